@@ -1,0 +1,328 @@
+"""Benchmark of the B200 explicit residual-and-update path (one JSON line).
+
+Workload (default): the batched multiblock 3D Euler bump duct -- about 30 M
+cells in 24 blocks of uneven sizes (seeded 2x3x4 tensor partition with
+segment lengths from {24, ..., 160}), M = 0.6, 4-stage RK, CFL 2, Roe + MUSCL
+(kappa = 1/3, smooth limiter), FP64 state.  A step is one RK cycle (4 stages)
+over all cells; the metric is Mcell-stage/s = cells * 4 * steps / time.
+
+Our arm times cosa_gpu_smooth (fused halo + tile kernels replayed from a
+CUDA graph, state resident in HBM) with CUDA events on the library's stream;
+inputs (the state, 1.4 GB) are larger than the 126 MB L2, so no flush is
+needed between steps.  It also reports the mixed-precision path (FP32 slopes
+and Roe dissipation on FP64 differences), the roofline of the tile kernel,
+an end-to-end number through cosa_gpu_smooth_host (state copied from pinned
+host memory and back every step) and the CPU oracle's throughput on a
+bounded sample of the same workload.
+
+--impl reference times the CPU restatement of the reference (oracle/; COSA
+itself is Fortran and cannot be built here) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# algorithmic bytes per cell-stage of the whole Euler stage (FP64): read q 40 +
+# read q^n 40 + write q 40 + face metrics of the 3 owned faces 96 + vol 8 +
+# dt/V 8 + dt/V write amortised 2
+B_ALG_STAGE = 234
+# tile kernel alone, per cell and launch: stages 2-4 read q, q^n, metrics and
+# dt/V and write q (224 B); stage 1 writes dt/V instead of reading it and
+# copies q^n (264 B): average over the 4 stages of a cycle
+B_TILE = (3 * 224 + 264) / 4.0
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if not self.proc:
+            return out
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+            os.unlink(self.path)
+        except Exception:
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1])); mx.append(float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                pass
+        if sm:
+            out = {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                   "samples": len(sm)}
+        return out
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def build_case(args):
+    from cosa_b200 import cases
+    if args.workload == "duct30m":
+        segs = cases.duct_segments(seed=args.seed)
+        return cases.duct3d(segs=segs), f"config3 bump duct, 24 blocks, segments {segs}"
+    if args.workload == "channel":
+        return cases.bump_channel(), "config1 bump channel 128x64x2 (1 block)"
+    raise SystemExit(f"unknown workload {args.workload}")
+
+
+def cpu_sample_case(args):
+    from cosa_b200 import cases
+    segs = cases.duct_segments(seed=args.seed + 100, lo=900_000, hi=1_300_000, choices=tuple(range(24, 65, 8)))
+    return cases.duct3d(segs=segs), segs
+
+
+def run_cpu_oracle(args, steps: int, warmup: int):
+    """The oracle (C++ restatement of the reference, OpenMP over blocks) on a
+    ~1 M-cell duct with the same generator: Mcell-stage/s on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    case, segs = cpu_sample_case(args)
+    O = oracle.OracleLevel(case.tables, case.params)
+    si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
+    q = case.q0.copy()
+    if warmup:
+        O.smooth(q, si, sj, sk, warmup, rms_every=10 ** 6)
+    t = time.perf_counter()
+    O.smooth(q, si, sj, sk, steps, rms_every=10 ** 6)
+    dt = time.perf_counter() - t
+    val = case.ncells * case.params.nstage * steps / dt / 1e6
+    return {"value": val, "unit": "Mcell-stage/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"{case.ncells} cells (24-block duct, segments {segs}), {steps} RK cycles, {dt:.2f} s"}, dt
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 8))
+    cb, dt = run_cpu_oracle(args, steps, min(args.warmup, 1))
+    line = {"impl": "reference", "metric": "Mcell-stage/s", "value": cb["value"], "unit": "Mcell-stage/s",
+            "n_gpus": ws, "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": dt / steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "config3 bump duct (bounded CPU sample)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "Mcell-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def time_smooth(ctx, steps: int, torch):
+    """Device time of `steps` fused cycles with CUDA events on the library's stream."""
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ctx.sync()
+    e0.record(stream)
+    hist, st = ctx.smooth(1, steps, 10 ** 6, 10 ** 6, want_hist=False)
+    e1.record(stream)
+    e1.synchronize()
+    if st:
+        raise RuntimeError(f"cosa_gpu_smooth status 0x{st:x}")
+    return e0.elapsed_time(e1)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="duct30m", choices=["duct30m", "channel"])
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    ws, rank, local = _dist()
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    dev = local if ws > 1 else 0
+    torch.cuda.set_device(dev)
+
+    from cosa_b200 import gpu
+    from cosa_b200.params import PREC_MIXED
+
+    case, desc = build_case(args)
+    p = case.params
+    ncells = case.ncells
+    ctx = gpu.Context([case.tables], p, device=dev)
+    X, Y, Z = (ctx.alloc_p2(ncomp=1).upload(a) for a in (case.x, case.y, case.z))
+    si, sj, sk = (ctx.alloc_p2() for _ in range(3))
+    vol = ctx.alloc_p1()
+    ctx.imetrix(1, X, Y, Z, si, sj, sk)
+    ctx.vols(1, X, Y, Z, vol)
+    q = ctx.alloc_p3().upload(case.q0)
+    qold = ctx.alloc_p3()
+    dtvol = ctx.alloc_p1()
+    ctx.bind_level(1, q=q, qold=qold, dtvol=dtvol, si=si, sj=sj, sk=sk, vol=vol)
+    nstage = p.nstage
+
+    # ---- FP64 fused path: warm-up then the timed region -------------------------
+    ctx.smooth(1, args.warmup, 1, 10 ** 6, want_hist=False)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    ctx.launch_count(reset=True)
+    clk = ClockSampler(dev)
+    clk.start()
+    ms = time_smooth(ctx, args.steps, torch)
+    clocks = clk.stop()
+    launches = ctx.launch_count(reset=True)
+    torch.cuda.synchronize()
+    ms_max = ms
+    if pg:
+        t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = ws * ncells * nstage * args.steps / (ms_max / 1e3) / 1e6
+
+    # ---- kernel roofline: event-timed pass right after the timed region ----------
+    kms, kcnt = ctx.profile(1, 3)
+    peak, peak_kind = _peaks()
+    tile_bytes = B_TILE * ncells
+    achieved = tile_bytes / (kms[1] / 1e3) / 1e9
+    stage_gbs = B_ALG_STAGE * ncells * nstage * args.steps / (ms / 1e3) / 1e9
+
+    # ---- mixed precision path on the same arrays -------------------------------------
+    from cosa_b200.params import CosaParams
+    pm = CosaParams.from_buffer_copy(bytes(memoryview(p)))
+    pm.precision = PREC_MIXED
+    ctx.set_params(pm)
+    q.upload(case.q0)
+    ctx.smooth(1, args.warmup, 1, 10 ** 6, want_hist=False)
+    ms_mixed = time_smooth(ctx, args.steps, torch)
+    kms_m, _ = ctx.profile(1, 3)
+    value_mixed = ws * ncells * nstage * args.steps / (ms_mixed / 1e3) / 1e6
+    ctx.set_params(p)
+
+    # ---- end to end through the host-buffer entry point --------------------------------
+    nq = q.n
+    hostq = torch.empty(nq, dtype=torch.float64, pin_memory=True)
+    hostq.numpy()[:] = case.q0
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ctx.sync()
+    import ctypes as C
+    hist = np.zeros((1, p.npde + 1))
+    e0.record(stream)
+    t0 = time.perf_counter()
+    for s in range(args.e2e_steps):
+        st = gpu.load().cosa_gpu_smooth_host(ctx.h, 1, C.c_void_p(hostq.data_ptr()), 1, s + 1, 1,
+                                             hist.ctypes.data_as(C.POINTER(C.c_double)))
+        if st:
+            raise RuntimeError(f"smooth_host status 0x{st:x}")
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = max(e0.elapsed_time(e1), wall * 1e3)
+    e2e_val = ws * ncells * nstage * args.e2e_steps / (e2e_ms / 1e3) / 1e6
+    state_bytes = nq * 8
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            cpu, _ = run_cpu_oracle(args, 2, 0)
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "error": str(e)}
+
+    if rank == 0:
+        line = {
+            "metric": "Mcell-stage/s", "value": value, "unit": "Mcell-stage/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "cells": ncells, "blocks": case.tables.nblocks, "stages_per_step": nstage,
+                       "scheme": "Roe FDS + MUSCL kappa=1/3 smooth limiter, 4-stage RK, CFL 2, M=0.6",
+                       "l2": "state 1.4 GB > L2 (126 MB): no flush needed",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "k_stage_tile<32,8,fp64>",
+                         "kernel_ms": kms[1], "halo_ms": kms[0], "bytes_per_cell": B_TILE,
+                         "peak_kind": peak_kind, "stage_gbs_alg": stage_gbs},
+            "mixed": {"value": value_mixed, "ms_per_step": ms_mixed / args.steps,
+                      "speedup_vs_fp64": value_mixed / value if value else None,
+                      "tile_kernel_ms": kms_m[1]},
+            "e2e": {"value": e2e_val, "unit": "Mcell-stage/s", "h2d_bytes_per_step": state_bytes,
+                    "d2h_bytes_per_step": state_bytes + 8 * (p.npde + 1)},
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

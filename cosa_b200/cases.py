@@ -1,0 +1,364 @@
+"""Synthetic multiblock cases in COSA's layout (grid, tables, parameters, state).
+
+COSA ships no meshes or inputs, so every case is generated from formulas:
+
+* ``bump_channel`` -- single-block quasi-2D channel with a 10%-thick
+  circular-arc bump (radius 1.3 through (0,0), (0.5,0.1), (1,0)) on the lower
+  wall; x uniform on [-1.5, 2.5], y linear between the wall and y=1, z two
+  cells of width 0.1.  BCs 21 (inlet) / 91 (outlet) / 14 (walls) / 80
+  (symmetry in z).
+* ``duct3d`` -- 3D duct x in [-1,2], y in [0,1], z in [-1,1] with the floor
+  bump h(x,z) = 0.1 sin^2(pi x) cos^2(pi z / 2) for x in [0,1]; a 2x3x4
+  tensor partition into 24 blocks whose segment lengths are drawn (seeded)
+  from {24, 32, ..., 160} until the cell count lies in a target window;
+  1-to-1 cuts between neighbours.
+* ``partitioned_channel`` -- the bump channel cut into several blocks, one of
+  them stored with cyclically permuted indices, to exercise cut_q's iord.
+
+Arrays are flat float64 in the reference layout (column-major per block,
+blocks concatenated with setoffs offsets).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+from .params import CosaParams, default_params, subsonic_inlet_total_state
+from .tables import BlockSpec, LevelTables, build_tables
+
+
+@dataclass
+class Case:
+    name: str
+    tables: LevelTables
+    params: CosaParams
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    q0: np.ndarray  # conservative initial state (P3 * npde * S)
+
+    @property
+    def ncells(self) -> int:
+        return self.tables.ncells()
+
+
+# ---- layout helpers -------------------------------------------------------------
+def p3_views(tables: LevelTables, arr: np.ndarray, npde: int, nsnap: int):
+    """Per-block views (I3,J3,K3,npde,S) Fortran-ordered into a flat P3 array."""
+    off, _ = tables.offsets()
+    views = []
+    for b, (im, jm, km) in enumerate(tables.dims):
+        n = (im + 3) * (jm + 3) * (km + 3) * npde * nsnap
+        s = off["p3"][b] * npde * nsnap
+        views.append(arr[s:s + n].reshape((im + 3, jm + 3, km + 3, npde, nsnap), order="F"))
+    return views
+
+
+def p2_views(tables: LevelTables, arr: np.ndarray, ncomp: int = 1):
+    off, _ = tables.offsets()
+    views = []
+    for b, (im, jm, km) in enumerate(tables.dims):
+        n = (im + 2) * (jm + 2) * (km + 2) * ncomp
+        s = off["p2"][b] * ncomp
+        if ncomp == 1:
+            views.append(arr[s:s + n].reshape((im + 2, jm + 2, km + 2), order="F"))
+        else:
+            views.append(arr[s:s + n].reshape((ncomp, im + 2, jm + 2, km + 2), order="F"))
+    return views
+
+
+def p1_views(tables: LevelTables, arr: np.ndarray, nsnap: int = 1):
+    off, _ = tables.offsets()
+    views = []
+    for b, (im, jm, km) in enumerate(tables.dims):
+        n = (im + 1) * (jm + 1) * (km + 1) * nsnap
+        s = off["p1"][b] * nsnap
+        views.append(arr[s:s + n].reshape((im + 1, jm + 1, km + 1, nsnap), order="F"))
+    return views
+
+
+def interior(v: np.ndarray) -> np.ndarray:
+    """Interior cells (1..imax-1, ...) of a P3 block view."""
+    return v[2:-2, 2:-2, 2:-2]
+
+
+def _embed_grid(nodes: np.ndarray, dst: np.ndarray):
+    """nodes (ni,nj,nk) at 1..imax -> dst (0:imax+1) with linear halo extrapolation."""
+    dst[1:-1, 1:-1, 1:-1] = nodes
+    dst[0, :, :] = 2 * dst[1, :, :] - dst[2, :, :]
+    dst[-1, :, :] = 2 * dst[-2, :, :] - dst[-3, :, :]
+    dst[:, 0, :] = 2 * dst[:, 1, :] - dst[:, 2, :]
+    dst[:, -1, :] = 2 * dst[:, -2, :] - dst[:, -3, :]
+    dst[:, :, 0] = 2 * dst[:, :, 1] - dst[:, :, 2]
+    dst[:, :, -1] = 2 * dst[:, :, -2] - dst[:, :, -3]
+
+
+def _freestream_state(tables: LevelTables, p: CosaParams) -> np.ndarray:
+    """init2fs (src/input.f90:4741-4775): conservative free stream everywhere."""
+    _, tot = tables.offsets()
+    S = 2 * p.nharms + 1
+    q = np.zeros(tot["p3"] * p.npde * S)
+    ca, sa = np.cos(p.alpha), np.sin(p.alpha)
+    cb, sb = np.cos(p.beta), np.sin(p.beta)
+    for v in p3_views(tables, q, p.npde, S):
+        v[..., 0, :] = p.rhoinf
+        v[..., 1, :] = p.rhoinf * p.machfs * ca * cb
+        v[..., 2, :] = p.rhoinf * p.machfs * sa * cb
+        v[..., 3, :] = p.rhoinf * p.machfs * sb
+        v[..., 4, :] = 1 / p.rhoinf / p.gamma / (p.gamma - 1) + 0.5 * p.machfs ** 2
+    return q
+
+
+def _assemble(name, blocks_nodes, specs, cuts, params) -> Case:
+    tables = build_tables(specs, cuts)
+    _, tot = tables.offsets()
+    x = np.zeros(tot["p2"]); y = np.zeros(tot["p2"]); z = np.zeros(tot["p2"])
+    for (X, Y, Z), vx, vy, vz in zip(blocks_nodes, p2_views(tables, x), p2_views(tables, y), p2_views(tables, z)):
+        _embed_grid(X, vx); _embed_grid(Y, vy); _embed_grid(Z, vz)
+    q0 = _freestream_state(tables, params)
+    return Case(name, tables, params, x, y, z, q0)
+
+
+def _face_bcs(ni, nj, nk, types):
+    """BC lines for the six faces of a block (node counts ni,nj,nk); types is
+    a dict face->bctype with faces 'imin','imax','jmin','jmax','kmin','kmax'."""
+    out = []
+    f = {
+        "imin": ((1, 1, 1), (1, nj, nk)), "imax": ((ni, 1, 1), (ni, nj, nk)),
+        "jmin": ((1, 1, 1), (ni, 1, nk)), "jmax": ((1, nj, 1), (ni, nj, nk)),
+        "kmin": ((1, 1, 1), (ni, nj, 1)), "kmax": ((1, 1, nk), (ni, nj, nk)),
+    }
+    for face in ("imin", "imax", "jmin", "jmax", "kmin", "kmax"):
+        if face in types:
+            s, e = f[face]
+            out.append((s, e, types[face]))
+    return out
+
+
+# ---- configuration 1: bump channel ------------------------------------------------
+def bump_wall(x: np.ndarray) -> np.ndarray:
+    r = 1.3
+    yb = np.sqrt(np.maximum(r * r - (x - 0.5) ** 2, 0.0)) - (r - 0.1)
+    return np.where((x >= 0.0) & (x <= 1.0), yb, 0.0)
+
+
+def channel_nodes(ni: int, nj: int, nk: int):
+    """Node coordinates (ni+1, nj+1, nk+1) of the bump channel."""
+    xs = -1.5 + 4.0 * np.arange(ni + 1) / ni
+    eta = np.arange(nj + 1) / nj
+    zs = 0.1 * np.arange(nk + 1)
+    X = np.broadcast_to(xs[:, None, None], (ni + 1, nj + 1, nk + 1)).copy()
+    yb = bump_wall(xs)[:, None, None]
+    Y = np.broadcast_to(yb + (1.0 - yb) * eta[None, :, None], (ni + 1, nj + 1, nk + 1)).copy()
+    Z = np.broadcast_to(zs[None, None, :], (ni + 1, nj + 1, nk + 1)).copy()
+    return X, Y, Z
+
+
+def channel_params(mach: float = 0.5) -> CosaParams:
+    p = default_params()
+    p.machfs = mach
+    p.alpha = 0.0
+    p.beta = 0.0
+    t0, p0 = subsonic_inlet_total_state(p.gamma, mach)
+    p.inlet_t0 = t0
+    p.inlet_p0 = p0
+    p.cfl = 2.0
+    p.irsop = 0
+    p.nstage = 4
+    return p
+
+
+def bump_channel(ni: int = 128, nj: int = 64, nk: int = 2, mach: float = 0.5, kface_bc: int = 80) -> Case:
+    X, Y, Z = channel_nodes(ni, nj, nk)
+    spec = BlockSpec(ni + 1, nj + 1, nk + 1, _face_bcs(ni + 1, nj + 1, nk + 1, {
+        "imin": 21, "imax": 91, "jmin": 14, "jmax": 14, "kmin": kface_bc, "kmax": kface_bc}))
+    return _assemble(f"bump_channel_{ni}x{nj}x{nk}", [(X, Y, Z)], [spec], [], channel_params(mach))
+
+
+def _permute_block(X, Y, Z):
+    """Store a block with cyclically permuted indices: new (i,j,k) = old (j,k,i)."""
+    return tuple(np.ascontiguousarray(np.transpose(A, (1, 2, 0))) for A in (X, Y, Z))
+
+
+def partitioned_channel(ni: int = 48, nj: int = 24, nk: int = 2, isplit=(20,), jsplit=(10,),
+                        permute_last: bool = True, mach: float = 0.5, kface_bc: int = 4) -> Case:
+    """Bump channel split at node planes isplit (i) and jsplit (j); the last
+    block is stored with permuted indices when permute_last.  The z faces
+    default to extrapolation (4): the reference's symmetry BC (80) reflects
+    the velocity component of the block's own index direction
+    (src/bc.f90:2684-2687), which is only the plane normal on blocks whose
+    axes follow x, y, z."""
+    X, Y, Z = channel_nodes(ni, nj, nk)
+    ib = [0] + list(isplit) + [ni]
+    jb = [0] + list(jsplit) + [nj]
+    nbi, nbj = len(ib) - 1, len(jb) - 1
+    nodes, specs, ids = [], [], {}
+    perm = {}
+    for bj in range(nbj):
+        for bi in range(nbi):
+            i0, i1, j0, j1 = ib[bi], ib[bi + 1], jb[bj], jb[bj + 1]
+            Xb, Yb, Zb = (A[i0:i1 + 1, j0:j1 + 1, :] for A in (X, Y, Z))
+            n = len(nodes)
+            ids[(bi, bj)] = n + 1
+            last = (bi == nbi - 1 and bj == nbj - 1)
+            ni_b, nj_b, nk_b = i1 - i0 + 1, j1 - j0 + 1, nk + 1
+            types = {}
+            if bi == 0: types["imin"] = 21
+            if bi == nbi - 1: types["imax"] = 91
+            if bj == 0: types["jmin"] = 14
+            if bj == nbj - 1: types["jmax"] = 14
+            types["kmin"] = kface_bc
+            types["kmax"] = kface_bc
+            if permute_last and last and (nbi * nbj > 1):
+                Xb, Yb, Zb = _permute_block(Xb, Yb, Zb)
+                # old face -> new face under new(i,j,k) = old(j,k,i)
+                fmap = {"imin": "kmin", "imax": "kmax", "jmin": "imin", "jmax": "imax",
+                        "kmin": "jmin", "kmax": "jmax"}
+                types = {fmap[f]: t for f, t in types.items()}
+                dims = (nj_b, nk_b, ni_b)
+                perm[n + 1] = True
+            else:
+                dims = (ni_b, nj_b, nk_b)
+            nodes.append((Xb, Yb, Zb))
+            specs.append(BlockSpec(*dims, _face_bcs(*dims, types)))
+    cuts = []
+
+    def face_nodes(b, face):
+        """input.dat node range of a face of block b, in b's own indices."""
+        ni_b, nj_b, nk_b = specs[b - 1].imax, specs[b - 1].jmax, specs[b - 1].kmax
+        if b in perm:
+            face = {"imin": "kmin", "imax": "kmax", "jmin": "imin", "jmax": "imax"}[face]
+        return {
+            "imin": ((1, 1, 1), (1, nj_b, nk_b)), "imax": ((ni_b, 1, 1), (ni_b, nj_b, nk_b)),
+            "jmin": ((1, 1, 1), (ni_b, 1, nk_b)), "jmax": ((1, nj_b, 1), (ni_b, nj_b, nk_b)),
+            "kmin": ((1, 1, 1), (ni_b, nj_b, 1)), "kmax": ((1, 1, nk_b), (ni_b, nj_b, nk_b)),
+        }[face]
+
+    def iord(b1, b2):
+        # index of block 2 matching index l of block 1 (both in own storage)
+        p1, p2 = b1 in perm, b2 in perm
+        # storage axis of the "physical" (i,j,k) of the unpermuted channel
+        ax = lambda p: (3, 1, 2) if p else (1, 2, 3)   # physical l -> storage axis
+        inv = lambda p: (2, 3, 1) if p else (1, 2, 3)  # storage axis -> physical
+        a1, a2 = inv(p1), ax(p2)
+        return tuple(a2[a1[l] - 1] for l in range(3))
+
+    for bj in range(nbj):
+        for bi in range(nbi):
+            b = ids[(bi, bj)]
+            if bi + 1 < nbi:
+                o = ids[(bi + 1, bj)]
+                s1, e1 = face_nodes(b, "imax")
+                s2, e2 = face_nodes(o, "imin")
+                cuts.append((b, s1, e1, o, s2, e2, iord(b, o)))
+            if bj + 1 < nbj:
+                o = ids[(bi, bj + 1)]
+                s1, e1 = face_nodes(b, "jmax")
+                s2, e2 = face_nodes(o, "jmin")
+                cuts.append((b, s1, e1, o, s2, e2, iord(b, o)))
+    return _assemble(f"partitioned_channel_{ni}x{nj}x{nk}", nodes, specs, cuts, channel_params(mach))
+
+
+# ---- configuration 3: 3D bump duct --------------------------------------------------
+def duct_segments(seed: int = 3, lo: int = 27_000_000, hi: int = 33_000_000, parts=(2, 3, 4),
+                  choices=tuple(range(24, 161, 8)), max_draws: int = 100000):
+    """Seeded draw of the tensor-partition segment lengths (cells) with
+    lo <= N <= hi."""
+    rng = np.random.default_rng(seed)
+    for _ in range(max_draws):
+        segs = [rng.choice(choices, size=n) for n in parts]
+        n = int(np.prod([s.sum() for s in segs]))
+        if lo <= n <= hi:
+            return [list(map(int, s)) for s in segs]
+    raise RuntimeError("no partition in the window")
+
+
+def duct_params(mach: float = 0.6) -> CosaParams:
+    return channel_params(mach)
+
+
+def duct3d(segs=None, seed: int = 3, lo: int = 27_000_000, hi: int = 33_000_000,
+           mach: float = 0.6, grid: bool = True) -> Case:
+    if segs is None:
+        segs = duct_segments(seed, lo, hi)
+    si, sj, sk = segs
+    NI, NJ, NK = sum(si), sum(sj), sum(sk)
+    xs = -1.0 + 3.0 * np.arange(NI + 1) / NI
+    eta = np.arange(NJ + 1) / NJ
+    zs = -1.0 + 2.0 * np.arange(NK + 1) / NK
+    ib = np.concatenate([[0], np.cumsum(si)]); jb = np.concatenate([[0], np.cumsum(sj)])
+    kb = np.concatenate([[0], np.cumsum(sk)])
+    nodes, specs, ids = [], [], {}
+    for bk in range(len(sk)):
+        for bj in range(len(sj)):
+            for bi in range(len(si)):
+                i0, i1, j0, j1, k0, k1 = ib[bi], ib[bi + 1], jb[bj], jb[bj + 1], kb[bk], kb[bk + 1]
+                ids[(bi, bj, bk)] = len(specs) + 1
+                types = {}
+                if bi == 0: types["imin"] = 21
+                if bi == len(si) - 1: types["imax"] = 91
+                if bj == 0: types["jmin"] = 14
+                if bj == len(sj) - 1: types["jmax"] = 14
+                if bk == 0: types["kmin"] = 14
+                if bk == len(sk) - 1: types["kmax"] = 14
+                dims = (i1 - i0 + 1, j1 - j0 + 1, k1 - k0 + 1)
+                specs.append(BlockSpec(*dims, _face_bcs(*dims, types)))
+                if grid:
+                    x = xs[i0:i1 + 1][:, None, None]
+                    z = zs[k0:k1 + 1][None, None, :]
+                    h = np.where((x >= 0) & (x <= 1), 0.1 * np.sin(np.pi * x) ** 2 * np.cos(np.pi * z / 2) ** 2, 0.0)
+                    e = eta[j0:j1 + 1][None, :, None]
+                    shp = (dims[0], dims[1], dims[2])
+                    X = np.broadcast_to(x, shp).copy()
+                    Y = np.broadcast_to(h + (1.0 - h) * e, shp).copy()
+                    Z = np.broadcast_to(z, shp).copy()
+                    nodes.append((X, Y, Z))
+    cuts = []
+    for (bi, bj, bk), b in ids.items():
+        d = specs[b - 1]
+        for axis, nb in ((0, (bi + 1, bj, bk)), (1, (bi, bj + 1, bk)), (2, (bi, bj, bk + 1))):
+            if nb not in ids:
+                continue
+            o = ids[nb]
+            od = specs[o - 1]
+            if axis == 0:
+                s1, e1 = (d.imax, 1, 1), (d.imax, d.jmax, d.kmax)
+                s2, e2 = (1, 1, 1), (1, od.jmax, od.kmax)
+            elif axis == 1:
+                s1, e1 = (1, d.jmax, 1), (d.imax, d.jmax, d.kmax)
+                s2, e2 = (1, 1, 1), (od.imax, 1, od.kmax)
+            else:
+                s1, e1 = (1, 1, d.kmax), (d.imax, d.jmax, d.kmax)
+                s2, e2 = (1, 1, 1), (od.imax, od.jmax, 1)
+            cuts.append((b, s1, e1, o, s2, e2, (1, 2, 3)))
+    p = duct_params(mach)
+    if not grid:
+        tables = build_tables(specs, cuts)
+        return Case(f"duct3d_{NI}x{NJ}x{NK}", tables, p, None, None, None, None)
+    return _assemble(f"duct3d_{NI}x{NJ}x{NK}", nodes, specs, cuts, p)
+
+
+def perturbed_state(case: Case, amp: float = 0.02, seed: int = 0) -> np.ndarray:
+    """Free stream plus a smooth seeded perturbation of every conservative
+    variable (keeps rho, p > 0); used to exercise limiters and all BC branches."""
+    rng = np.random.default_rng(seed)
+    q = case.q0.copy()
+    p = case.params
+    S = 2 * p.nharms + 1
+    for v in p3_views(case.tables, q, p.npde, S):
+        I, J, K = v.shape[:3]
+        ii = np.arange(I)[:, None, None] / max(I - 1, 1)
+        jj = np.arange(J)[None, :, None] / max(J - 1, 1)
+        kk = np.arange(K)[None, None, :] / max(K - 1, 1)
+        for var in range(p.npde):
+            a = rng.uniform(0.5, 1.5, size=3)
+            ph = rng.uniform(0, 2 * np.pi, size=3)
+            f = (np.sin(2 * np.pi * a[0] * ii + ph[0]) * np.cos(2 * np.pi * a[1] * jj + ph[1]) *
+                 (1.0 + 0.5 * np.sin(2 * np.pi * a[2] * kk + ph[2])))
+            noise = rng.standard_normal((I, J, K)) * 0.1
+            scale = amp * (abs(v[..., var, 0]).mean() + 0.1)
+            for n in range(S):
+                v[..., var, n] = v[..., var, n] + scale * (f + noise)
+    return q

@@ -1,0 +1,845 @@
+// C-ABI of the B200 path (include/cosa_gpu.h): context, level tables,
+// per-routine drop-in entry points and the fused smooth() loop.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "kernels_ref.cuh"
+#include "fused.cuh"
+
+namespace {
+
+constexpr int kTI = 32, kTJ = 8;  // tile of the fused stage kernel
+
+struct LevelState {
+  int nb = 0;
+  std::vector<DevBlock> hb;
+  std::vector<int> nbcs, bct, cut;
+  std::vector<int64_t> obct;
+  int ncuts = 0;
+  int64_t n3 = 0, n2 = 0, n1 = 0, n0 = 0, nm1 = 0;
+  DevBlock *d_blocks = nullptr;
+  int *d_bct = nullptr;
+  // halo work list: BC items first (table order), then cut items
+  std::vector<HaloItem> items;
+  int n_bc_items = 0;
+  HaloItem *d_items = nullptr;
+  uint8_t *d_strong = nullptr;
+  StrongMap *d_smap = nullptr;
+  Tile *d_tiles = nullptr;
+  int ntiles = 0, kchunk = 0;
+  bool bound = false;
+  cosa_level_ptrs ptrs{};
+  double *d_T = nullptr;      // second state buffer of the fused stages
+  double *d_part = nullptr;   // per-tile / per-CTA partial sums (8 doubles each)
+  int npart_cap = 0;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // iteration without / with rms
+};
+
+}  // namespace
+
+struct ProfState {
+  bool on = false;
+  cudaEvent_t ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [kind][start/stop]
+  double ms[2] = {0, 0};
+  long long n[2] = {0, 0};
+};
+
+struct cosa_ctx {
+  ProfState prof;
+  cosa_params p{};
+  cosa_params *d_p = nullptr;
+  int device = 0;
+  cudaStream_t s = nullptr;
+  int nlevels = 0;
+  LevelState L[COSA_MAX_LEVELS];
+  int *d_status = nullptr;
+  int *d_row = nullptr;
+  double *d_hist = nullptr;
+  int hist_cap = 0;
+  long long launches = 0;
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+int cuda_ok(cudaError_t e) {
+  if (e != cudaSuccess) {
+    fprintf(stderr, "cosa_gpu: CUDA error %s\n", cudaGetErrorString(e));
+    return COSA_ERR_CUDA;
+  }
+  return COSA_OK;
+}
+#define CK(x) do { int _r = cuda_ok(x); if (_r) return _r; } while (0)
+
+template <typename T>
+int dalloc(cosa_ctx *c, T **p, size_t n) {
+  void *v = nullptr;
+  CK(cudaMalloc(&v, std::max<size_t>(n, 1) * sizeof(T)));
+  c->allocs.push_back(v);
+  *p = static_cast<T *>(v);
+  return COSA_OK;
+}
+
+int grid_for(int64_t n, int threads = 256) {
+  int64_t g = (n + threads - 1) / threads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 16));
+}
+
+// index of cell (i,j,k) on the normal/tangential decomposition of a face
+inline void pcell(int idir, int nrm, int i2, int i3, int &i, int &j, int &k) {
+  const int ic1 = cyc3(idir, 1), ic2 = cyc3(idir, 2), ic3 = cyc3(idir, 3);
+  int v[4] = {0, 0, 0, 0};
+  v[ic1] = nrm; v[ic2] = i2; v[ic3] = i3;
+  i = v[1]; j = v[2]; k = v[3];
+}
+
+int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d) {
+  L.nb = d.nblocks;
+  int64_t a3 = 0, a2 = 0, a1 = 0, a0 = 0, am = 0, ab = 0;
+  for (int b = 0; b < L.nb; ++b) {
+    DevBlock x{};
+    x.im = d.dims[3 * b]; x.jm = d.dims[3 * b + 1]; x.km = d.dims[3 * b + 2];
+    if (x.im < 3 || x.jm < 3 || x.km < 2) return COSA_ERR_ARG;
+    x.I3 = x.im + 3; x.J3 = x.jm + 3;
+    x.P3 = (int64_t)(x.im + 3) * (x.jm + 3) * (x.km + 3);
+    x.op3 = a3; x.op2 = a2; x.op1 = a1; x.of0 = a0;
+    L.hb.push_back(x);
+    L.nbcs.push_back(d.nbcs[b]);
+    L.obct.push_back(ab);
+    a3 += x.P3;
+    a2 += (int64_t)(x.im + 2) * (x.jm + 2) * (x.km + 2);
+    a1 += (int64_t)(x.im + 1) * (x.jm + 1) * (x.km + 1);
+    a0 += (int64_t)x.im * x.jm * x.km;
+    am += (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1);
+    ab += 10 * d.nbcs[b];
+  }
+  L.n3 = a3; L.n2 = a2; L.n1 = a1; L.n0 = a0; L.nm1 = am;
+  L.bct.assign(d.bctopo, d.bctopo + ab);
+  L.ncuts = d.ncuts;
+  L.cut.assign(d.cutopo, d.cutopo + 21 * (int64_t)d.ncuts);
+
+  // ---- halo work list: bbc (src/bc.f90:35-121) then cut_q (src/bc.f90:1894-2141)
+  for (int b = 0; b < L.nb; ++b) {
+    const DevBlock &x = L.hb[b];
+    const int ijk[4] = {0, x.im, x.jm, x.km};
+    const int64_t I2 = x.im + 2, J2 = x.jm + 2;
+    for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
+      const int *r = L.bct.data() + L.obct[b] + 10 * ibc;
+      const int type = r[0], idir = r[1], inrout = r[2];
+      if (idir < 1 || idir > 3) return COSA_ERR_ARG;
+      const bool ok = type == 80 || type == 4 || type == 14 || type == 21 || type == 91 || type == 30;
+      if (!ok) return COSA_ERR_UNSUPPORTED;
+      int istrt[4] = {0, r[3], r[5], r[7]}, iend[4] = {0, r[4], r[6], r[8]};
+      const int ic2 = cyc3(idir, 2), ic3 = cyc3(idir, 3);
+      int ibcpt, ibcpt2, ibcn, ibcn2, ibcm;
+      if (inrout == 1) { ibcpt = 0; ibcpt2 = -1; ibcn = 1; ibcn2 = 2; ibcm = 1; }
+      else { ibcpt = ijk[idir]; ibcpt2 = ibcpt + 1; ibcn = ibcpt - 1; ibcn2 = ibcpt - 2; ibcm = ibcpt; }
+      int sgn = 1;
+      if (type == 21) sgn = inrout == 1 ? 1 : -1;       // bc_insub sgnm
+      else if (type == 30) sgn = inrout == 1 ? -1 : 1;  // bc_far0 sgnm
+      for (int i3 = istrt[ic3]; i3 <= iend[ic3]; ++i3)
+        for (int i2 = istrt[ic2]; i2 <= iend[ic2]; ++i2) {
+          HaloItem it{};
+          it.dblk = it.sblk = b; it.type = type; it.idir = idir; it.mask = 3; it.sgn = sgn;
+          int i, j, k;
+          pcell(idir, ibcpt, i2, i3, i, j, k); it.h1 = p3_cell(x, i, j, k);
+          pcell(idir, ibcpt2, i2, i3, i, j, k); it.h2 = p3_cell(x, i, j, k);
+          pcell(idir, ibcn, i2, i3, i, j, k); it.c1 = p3_cell(x, i, j, k);
+          pcell(idir, ibcn2, i2, i3, i, j, k); it.c2 = p3_cell(x, i, j, k);
+          pcell(idir, ibcm, i2, i3, i, j, k); it.mface = i + I2 * (j + J2 * (int64_t)k);
+          L.items.push_back(it);
+        }
+    }
+  }
+  L.n_bc_items = (int)L.items.size();
+  for (int ic = 0; ic < L.ncuts; ++ic) {
+    const int *cc = L.cut.data() + 21 * (int64_t)ic;
+    const int b1 = cc[0] - 1, b2 = cc[9] - 1;
+    if (b1 < 0 || b1 >= L.nb || b2 < 0 || b2 >= L.nb) return COSA_ERR_ARG;
+    const DevBlock &x1 = L.hb[b1], &x2 = L.hb[b2];
+    const int ijk1[4] = {0, x1.im, x1.jm, x1.km}, ijk2[4] = {0, x2.im, x2.jm, x2.km};
+    const int idir1 = cc[1], inout1 = cc[2], idir2 = cc[10], inout2 = cc[11];
+    const int istr1[4] = {0, cc[3], cc[5], cc[7]}, iend1[4] = {0, cc[4], cc[6], cc[8]};
+    const int istr2[4] = {0, cc[12], cc[14], cc[16]}, iend2[4] = {0, cc[13], cc[15], cc[17]};
+    const int iord[4] = {0, cc[18], cc[19], cc[20]};
+    int ibcpt, ibcinc, inr, inrinc;
+    if (inout1 == 1) { ibcpt = 0; ibcinc = -1; } else { ibcpt = ijk1[idir1]; ibcinc = 1; }
+    if (inout2 == 1) { inr = 1; inrinc = 1; } else { inr = ijk2[idir2] - 1; inrinc = -1; }
+    int len[4], isgn1[4], isgn2[4];
+    for (int l = 1; l <= 3; ++l) {
+      len[l] = std::abs(iend1[l] - istr1[l]);
+      isgn1[l] = iend1[l] > istr1[l] ? 1 : -1;
+      isgn2[l] = iend2[l] > istr2[l] ? 1 : -1;
+    }
+    const int ic1 = cyc3(idir1, 1), ic2 = cyc3(idir1, 2), ic3 = cyc3(idir1, 3);
+    const int jc1 = iord[ic1], jc2 = iord[ic2], jc3 = iord[ic3];
+    for (int i3 = 0; i3 <= len[ic3]; ++i3)
+      for (int i2 = 0; i2 <= len[ic2]; ++i2) {
+        int p1[4] = {0, 0, 0, 0}, p2[4] = {0, 0, 0, 0};
+        p1[ic1] = ibcpt; p1[ic2] = istr1[ic2] + isgn1[ic2] * i2; p1[ic3] = istr1[ic3] + isgn1[ic3] * i3;
+        p2[jc1] = inr; p2[jc2] = istr2[jc2] + isgn2[jc2] * i2; p2[jc3] = istr2[jc3] + isgn2[jc3] * i3;
+        HaloItem it{};
+        it.dblk = b1; it.sblk = b2; it.type = -1; it.idir = idir1; it.mask = 3; it.sgn = 1;
+        it.h1 = p3_cell(x1, p1[1], p1[2], p1[3]);
+        p1[ic1] += ibcinc;
+        it.h2 = p3_cell(x1, p1[1], p1[2], p1[3]);
+        it.c1 = p3_cell(x2, p2[1], p2[2], p2[3]);
+        p2[jc1] += inrinc;
+        it.c2 = p3_cell(x2, p2[1], p2[2], p2[3]);
+        it.mface = 0;
+        L.items.push_back(it);
+      }
+  }
+  // last writer of every halo cell keeps its write (reference order)
+  {
+    std::vector<int64_t> owner((size_t)L.n3, -1);
+    for (size_t t = 0; t < L.items.size(); ++t) {
+      const HaloItem &it = L.items[t];
+      const int64_t base = L.hb[it.dblk].op3;
+      owner[(size_t)(base + it.h1)] = (int64_t)t * 2;
+      owner[(size_t)(base + it.h2)] = (int64_t)t * 2 + 1;
+    }
+    for (size_t t = 0; t < L.items.size(); ++t) {
+      HaloItem &it = L.items[t];
+      const int64_t base = L.hb[it.dblk].op3;
+      int m = 0;
+      if (owner[(size_t)(base + it.h1)] == (int64_t)t * 2) m |= 1;
+      if (owner[(size_t)(base + it.h2)] == (int64_t)t * 2 + 1) m |= 2;
+      it.mask = m;
+    }
+  }
+  // ---- strong-boundary flags (muscl_b*, src/flux.f90:1318-1349, 1376-1406)
+  std::vector<uint8_t> flags;
+  std::vector<StrongMap> smap(L.nb);
+  for (int b = 0; b < L.nb; ++b) {
+    const DevBlock &x = L.hb[b];
+    const int nc[4] = {0, x.im - 1, x.jm - 1, x.km - 1};
+    StrongMap &m = smap[b];
+    for (int d = 1; d <= 3; ++d) {
+      const int t2d = d == 1 ? 2 : 1, t3d = d == 3 ? 2 : 3;
+      m.n2[d - 1] = nc[t2d];
+      for (int side = 0; side < 2; ++side) {
+        m.off[d - 1][side] = -1;
+        for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
+          const int *r = L.bct.data() + L.obct[b] + 10 * ibc;
+          if (r[1] != d || !((r[0] == 13 || r[0] == 14 || r[0] / 100 == 15 || r[0] == 22 || r[0] == 23 ||
+                               r[0] == 92 || r[0] == 93 || r[0] == 5)))
+            continue;
+          if ((r[2] == 1) != (side == 0)) continue;
+          if (m.off[d - 1][side] < 0) {
+            m.off[d - 1][side] = (int64_t)flags.size();
+            flags.resize(flags.size() + (size_t)nc[t2d] * nc[t3d], 0);
+          }
+          const int lo[4] = {0, r[3], r[5], r[7]}, hi[4] = {0, r[4], r[6], r[8]};
+          for (int t3 = std::max(1, lo[t3d]); t3 <= std::min(nc[t3d], hi[t3d]); ++t3)
+            for (int t2 = std::max(1, lo[t2d]); t2 <= std::min(nc[t2d], hi[t2d]); ++t2)
+              flags[(size_t)(m.off[d - 1][side] + (t2 - 1) + (int64_t)nc[t2d] * (t3 - 1))] = 1;
+        }
+      }
+    }
+  }
+  // ---- tiles of the fused stage kernel
+  std::vector<Tile> tiles;
+  const int S = 2 * c->p.nharms + 1;
+  const int kc = 32;
+  L.kchunk = kc;
+  for (int b = 0; b < L.nb; ++b) {
+    const DevBlock &x = L.hb[b];
+    for (int n = 0; n < S; ++n)
+      for (int k0 = 1; k0 <= x.km - 1; k0 += kc)
+        for (int j0 = 1; j0 <= x.jm - 1; j0 += kTJ)
+          for (int i0 = 1; i0 <= x.im - 1; i0 += kTI)
+            tiles.push_back(Tile{b, n, i0, j0, k0, std::min(k0 + kc - 1, x.km - 1)});
+  }
+  L.ntiles = (int)tiles.size();
+
+  int r = 0;
+  if ((r = dalloc(c, &L.d_blocks, L.hb.size()))) return r;
+  if ((r = dalloc(c, &L.d_bct, std::max<size_t>(L.bct.size(), 1)))) return r;
+  if ((r = dalloc(c, &L.d_items, std::max<size_t>(L.items.size(), 1)))) return r;
+  if ((r = dalloc(c, &L.d_strong, std::max<size_t>(flags.size(), 1)))) return r;
+  if ((r = dalloc(c, &L.d_smap, smap.size()))) return r;
+  if ((r = dalloc(c, &L.d_tiles, std::max<size_t>(tiles.size(), 1)))) return r;
+  CK(cudaMemcpy(L.d_blocks, L.hb.data(), L.hb.size() * sizeof(DevBlock), cudaMemcpyHostToDevice));
+  if (!L.bct.empty()) CK(cudaMemcpy(L.d_bct, L.bct.data(), L.bct.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (!L.items.empty())
+    CK(cudaMemcpy(L.d_items, L.items.data(), L.items.size() * sizeof(HaloItem), cudaMemcpyHostToDevice));
+  if (!flags.empty()) CK(cudaMemcpy(L.d_strong, flags.data(), flags.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(L.d_smap, smap.data(), smap.size() * sizeof(StrongMap), cudaMemcpyHostToDevice));
+  if (!tiles.empty()) CK(cudaMemcpy(L.d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  return COSA_OK;
+}
+
+LevelState *level(cosa_ctx *c, int nl) {
+  if (!c || nl < 1 || nl > c->nlevels) return nullptr;
+  return &c->L[nl - 1];
+}
+
+int after_launch(cosa_ctx *c) {
+  c->launches++;
+  return cuda_ok(cudaGetLastError());
+}
+
+// launch one per-block kernel for every block of the level
+template <typename F>
+int for_blocks(cosa_ctx *c, LevelState &L, int64_t (*count)(const DevBlock &, const cosa_params &), F launch) {
+  for (int b = 0; b < L.nb; ++b) {
+    const int64_t n = count(L.hb[b], c->p);
+    launch(b, L.hb[b], grid_for(n));
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int64_t cnt_interior(const DevBlock &b, const cosa_params &p) {
+  return (int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * (2 * p.nharms + 1) * p.npde;
+}
+int64_t cnt_all(const DevBlock &b, const cosa_params &p) {
+  return (int64_t)(b.im + 3) * (b.jm + 3) * (b.km + 3) * (2 * p.nharms + 1) * p.npde;
+}
+
+int set_smem_attrs() {
+  static bool done = false;
+  if (done) return COSA_OK;
+  CK(cudaFuncSetAttribute(k_stage_tile<kTI, kTJ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)stage_smem_bytes<kTI, kTJ>()));
+  CK(cudaFuncSetAttribute(k_stage_tile<kTI, kTJ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)stage_smem_bytes<kTI, kTJ>()));
+  done = true;
+  return COSA_OK;
+}
+
+int check_fused_supported(const cosa_params &p) {
+  if (p.npde != 5 || p.viscous || p.kom || p.kom_bsl || p.kom_sst || p.harbal || p.rkimp || p.moving ||
+      p.irsop != 0 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
+    return COSA_ERR_UNSUPPORTED;
+  return COSA_OK;
+}
+
+// profiling: close the event pair of kernel class `k` and accumulate its time
+void prof_stop(cosa_ctx *c, int k) {
+  cudaEventRecord(c->prof.ev[k][1], c->s);
+  cudaEventSynchronize(c->prof.ev[k][1]);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->prof.ev[k][0], c->prof.ev[k][1]);
+  c->prof.ms[k] += ms;
+  c->prof.n[k] += 1;
+}
+
+// one stage: halo fill + tile kernel (+ norm reduction)
+int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, const double *qold,
+                 double *qold_copy, int irk, int compute_dt, bool want_rms, int update, double *res_out) {
+  const cosa_params &p = c->p;
+  const int S = 2 * p.nharms + 1;
+  const cosa_level_ptrs &P = L.ptrs;
+  if (!L.items.empty()) {
+    const int64_t n = (int64_t)L.items.size() * S;
+    if (c->prof.on) cudaEventRecord(c->prof.ev[0][0], c->s);
+    k_halo<true><<<grid_for(n), 256, 0, c->s>>>(L.d_blocks, L.d_items, (int)L.items.size(), c->d_p, qin, P.si, P.sj,
+                                                P.sk, c->d_status);
+    int r = after_launch(c);
+    if (r) return r;
+    if (c->prof.on) prof_stop(c, 0);
+  }
+  StageArgs A{};
+  A.qin = qin; A.qout = qout; A.qold = qold; A.qold_copy = qold_copy;
+  A.dtvol = P.dtvol; A.si = P.si; A.sj = P.sj; A.sk = P.sk;
+  A.part = want_rms ? L.d_part : nullptr;
+  A.rhs = nullptr;
+  A.res_out = res_out;
+  A.strong = L.d_strong; A.smap = L.d_smap; A.status = c->d_status;
+  A.ar = p.alphas[irk - 1];
+  A.compute_dt = compute_dt;
+  A.first_order = nl >= p.nl_crs;
+  A.update = update;
+  const size_t smem = stage_smem_bytes<kTI, kTJ>();
+  if (c->prof.on) cudaEventRecord(c->prof.ev[1][0], c->s);
+  if (p.precision == COSA_PREC_MIXED)
+    k_stage_tile<kTI, kTJ, true><<<L.ntiles, kTI * kTJ, smem, c->s>>>(L.d_blocks, L.d_tiles, c->d_p, A);
+  else
+    k_stage_tile<kTI, kTJ, false><<<L.ntiles, kTI * kTJ, smem, c->s>>>(L.d_blocks, L.d_tiles, c->d_p, A);
+  int r = after_launch(c);
+  if (r) return r;
+  if (c->prof.on) prof_stop(c, 1);
+  if (want_rms) {
+    int64_t ncell = 0;
+    for (auto &b : L.hb) ncell += (int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1);
+    k_rms_final<<<1, 256, 0, c->s>>>(L.d_part, L.ntiles, p.npde, (double)ncell, c->d_hist, c->d_row, c->hist_cap);
+    r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+// one RK iteration (nstage stages) of the fused path
+int launch_iteration(cosa_ctx *c, int nl, LevelState &L, bool want_rms, int compute_dt) {
+  const cosa_params &p = c->p;
+  double *Q = L.ptrs.q, *T = L.d_T, *QO = L.ptrs.qold;
+  for (int irk = 1; irk <= p.nstage; ++irk) {
+    double *qin = (irk % 2 == 1) ? Q : T;
+    double *qout = (irk % 2 == 1) ? T : Q;
+    const double *qold = irk == 1 ? Q : QO;
+    double *qcopy = irk == 1 ? QO : nullptr;
+    int r = launch_stage(c, nl, L, qin, qout, qold, qcopy, irk, compute_dt && irk == 1, want_rms && irk == 1, 1,
+                         nullptr);
+    if (r) return r;
+  }
+  if (p.nstage % 2 == 1) {
+    // result landed in T: copy the interior back (whole array is simplest)
+    const int S = 2 * p.nharms + 1;
+    CK(cudaMemcpyAsync(Q, T, (size_t)L.n3 * p.npde * S * sizeof(double), cudaMemcpyDeviceToDevice, c->s));
+  }
+  return COSA_OK;
+}
+
+void drop_graphs(cosa_ctx *c) {
+  for (int l = 0; l < COSA_MAX_LEVELS; ++l)
+    for (auto &g : c->L[l].graph)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+int ensure_hist(cosa_ctx *c, int rows) {
+  if (rows <= c->hist_cap) return COSA_OK;
+  drop_graphs(c);  // captured graphs hold the old buffer address
+  int r = dalloc(c, &c->d_hist, (size_t)rows * 8);
+  if (r) return r;
+  c->hist_cap = rows;
+  return COSA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t cosa_gpu_params_size(void) { return (int64_t)sizeof(cosa_params); }
+
+int cosa_gpu_init(const cosa_params *p, int32_t nlevels, const cosa_level_desc *levels, int32_t device,
+                  cosa_ctx **out) {
+  if (!p || !levels || !out || nlevels < 1 || nlevels > COSA_MAX_LEVELS) return COSA_ERR_ARG;
+  if (p->npde != 5 && p->npde != 7) return COSA_ERR_ARG;
+  if (2 * p->nharms + 1 > COSA_MAX_SNAP) return COSA_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return COSA_ERR_CUDA;
+  CK(cudaSetDevice(device));
+  cosa_ctx *c = new (std::nothrow) cosa_ctx;
+  if (!c) return COSA_ERR_ARG;
+  c->p = *p;
+  c->device = device;
+  c->nlevels = nlevels;
+  int r = 0;
+  if ((r = cuda_ok(cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking))) ||
+      (r = dalloc(c, &c->d_p, 1)) || (r = dalloc(c, &c->d_status, 1)) || (r = dalloc(c, &c->d_row, 1)) ||
+      (r = set_smem_attrs())) {
+    cosa_gpu_finalize(c);
+    return r;
+  }
+  cudaMemcpy(c->d_p, p, sizeof(cosa_params), cudaMemcpyHostToDevice);
+  cudaMemset(c->d_status, 0, sizeof(int));
+  cudaMemset(c->d_row, 0, sizeof(int));
+  for (int l = 0; l < nlevels; ++l) {
+    if ((r = build_level(c, c->L[l], levels[l]))) {
+      cosa_gpu_finalize(c);
+      return r;
+    }
+  }
+  *out = c;
+  return COSA_OK;
+}
+
+int cosa_gpu_finalize(cosa_ctx *c) {
+  if (!c) return COSA_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (c->s) cudaStreamSynchronize(c->s);
+  for (int l = 0; l < COSA_MAX_LEVELS; ++l)
+    for (auto &g : c->L[l].graph)
+      if (g) cudaGraphExecDestroy(g);
+  for (auto &e2 : c->prof.ev)
+    for (auto &e : e2)
+      if (e) cudaEventDestroy(e);
+  for (void *v : c->allocs) cudaFree(v);
+  if (c->s) cudaStreamDestroy(c->s);
+  delete c;
+  return COSA_OK;
+}
+
+int cosa_gpu_set_params(cosa_ctx *c, const cosa_params *p) {
+  if (!c || !p) return COSA_ERR_ARG;
+  if (p->npde != c->p.npde || p->nharms != c->p.nharms) return COSA_ERR_ARG;
+  c->p = *p;
+  CK(cudaMemcpyAsync(c->d_p, p, sizeof(cosa_params), cudaMemcpyHostToDevice, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  for (int l = 0; l < COSA_MAX_LEVELS; ++l)
+    for (auto &g : c->L[l].graph)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return COSA_OK;
+}
+
+int cosa_gpu_level_sizes(cosa_ctx *c, int32_t nl, int64_t sizes[5]) {
+  LevelState *L = level(c, nl);
+  if (!L || !sizes) return COSA_ERR_ARG;
+  sizes[0] = L->n3; sizes[1] = L->n2; sizes[2] = L->n1; sizes[3] = L->n0; sizes[4] = L->nm1;
+  return COSA_OK;
+}
+
+int cosa_gpu_malloc(cosa_ctx *c, int64_t n, double **d) {
+  if (!c || !d || n < 0) return COSA_ERR_ARG;
+  cudaSetDevice(c->device);
+  int r = dalloc(c, d, (size_t)n);
+  if (r) return r;
+  CK(cudaMemset(*d, 0, std::max<size_t>(n, 1) * sizeof(double)));  // cosa_all zeroes (src/input.f90:5125)
+  return COSA_OK;
+}
+
+int cosa_gpu_memcpy_h2d(cosa_ctx *c, double *dst, const double *src, int64_t n) {
+  if (!c || n < 0) return COSA_ERR_ARG;
+  CK(cudaMemcpyAsync(dst, src, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->s));
+  return COSA_OK;
+}
+
+int cosa_gpu_memcpy_d2h(cosa_ctx *c, double *dst, const double *src, int64_t n) {
+  if (!c || n < 0) return COSA_ERR_ARG;
+  CK(cudaMemcpyAsync(dst, src, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  return COSA_OK;
+}
+
+int cosa_gpu_synchronize(cosa_ctx *c) {
+  if (!c) return COSA_ERR_ARG;
+  CK(cudaStreamSynchronize(c->s));
+  return COSA_OK;
+}
+
+int cosa_gpu_bind_level(cosa_ctx *c, int32_t nl, const cosa_level_ptrs *ptrs) {
+  LevelState *L = level(c, nl);
+  if (!L || !ptrs) return COSA_ERR_ARG;
+  L->ptrs = *ptrs;
+  const int S = 2 * c->p.nharms + 1;
+  int r = 0;
+  if (!L->d_T && (r = dalloc(c, &L->d_T, (size_t)L->n3 * c->p.npde * S))) return r;
+  CK(cudaMemset(L->d_T, 0, (size_t)L->n3 * c->p.npde * S * sizeof(double)));
+  const int need = std::max(L->ntiles, 148 * 16);
+  if (L->npart_cap < need) {
+    if ((r = dalloc(c, &L->d_part, (size_t)need * 8))) return r;
+    L->npart_cap = need;
+  }
+  for (auto &g : L->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  L->bound = true;
+  return COSA_OK;
+}
+
+// ---- level drivers --------------------------------------------------------------------
+int cosa_gpu_cons2prim(cosa_ctx *c, int32_t nl, int32_t xtnd, double *q) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || xtnd < 0 || xtnd > 1) return COSA_ERR_ARG;
+  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+    k_cons2prim<<<g, 256, 0, c->s>>>(b, c->d_p, q, xtnd);
+  });
+}
+
+int cosa_gpu_prim2cons(cosa_ctx *c, int32_t nl, double *q) {
+  LevelState *L = level(c, nl);
+  if (!L || !q) return COSA_ERR_ARG;
+  return for_blocks(c, *L, cnt_all, [&](int, const DevBlock &b, int g) {
+    k_prim2cons<<<g, 256, 0, c->s>>>(b, c->d_p, q);
+  });
+}
+
+int cosa_gpu_bc(cosa_ctx *c, int32_t nl, double *q, const double *si, const double *sj, const double *sk,
+                const double *) {
+  LevelState *L = level(c, nl);
+  if (!L || !q) return COSA_ERR_ARG;
+  if (L->n_bc_items == 0) return COSA_OK;
+  const int S = 2 * c->p.nharms + 1;
+  k_halo<false><<<grid_for((int64_t)L->n_bc_items * S), 256, 0, c->s>>>(L->d_blocks, L->d_items, L->n_bc_items,
+                                                                       c->d_p, q, si, sj, sk, c->d_status);
+  return after_launch(c);
+}
+
+int cosa_gpu_cutman_q(cosa_ctx *c, int32_t nl, double *q) {
+  LevelState *L = level(c, nl);
+  if (!L || !q) return COSA_ERR_ARG;
+  const int ncut = (int)L->items.size() - L->n_bc_items;
+  if (ncut == 0) return COSA_OK;
+  const int S = 2 * c->p.nharms + 1;
+  k_halo<false><<<grid_for((int64_t)ncut * S), 256, 0, c->s>>>(L->d_blocks, L->d_items + L->n_bc_items, ncut, c->d_p, q,
+                                                              nullptr, nullptr, nullptr, c->d_status);
+  return after_launch(c);
+}
+
+int cosa_gpu_prtest(cosa_ctx *c, int32_t nl, const double *q) {
+  LevelState *L = level(c, nl);
+  if (!L || !q) return COSA_ERR_ARG;
+  int r = for_blocks(c, *L, cnt_all, [&](int, const DevBlock &b, int g) {
+    k_prtest<<<g, 256, 0, c->s>>>(b, c->d_p, q, c->d_status);
+  });
+  if (r) return r;
+  return cosa_gpu_status(c, 0);
+}
+
+int cosa_gpu_lambda(cosa_ctx *c, int32_t nl, const double *q, const double *si, const double *sj,
+                    const double *sk, const double *, double *lam) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !lam) return COSA_ERR_ARG;
+  if (c->p.viscous || c->p.moving) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+    k_lambda<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, lam);
+  });
+}
+
+int cosa_gpu_deltat(cosa_ctx *c, int32_t nl, double *dtvol, const double *lam, double *bx, double *by, double *bz) {
+  LevelState *L = level(c, nl);
+  if (!L || !dtvol || !lam) return COSA_ERR_ARG;
+  if (c->p.viscous || c->p.kom || c->p.irsop == 5 || c->p.irsop == 6) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+    k_deltat<<<g, 256, 0, c->s>>>(b, c->d_p, dtvol, lam, bx, by, bz);
+  });
+}
+
+int cosa_gpu_muscl(cosa_ctx *c, int32_t idir, int32_t nl, const double *q, double *qp, double *qm, double *dq,
+                   double *dqp, double *dqm) {
+  LevelState *L = level(c, nl);
+  if (!L || idir < 1 || idir > 3 || !q || !qp || !qm || !dq || !dqp || !dqm) return COSA_ERR_ARG;
+  const cosa_params &p = c->p;
+  int so_beg = 1, so_end = p.npde;
+  if (nl >= p.nl_crs) { so_beg = 0; so_end = -1; }
+  else if (p.foturb) { so_beg = 1; so_end = 5; }
+  for (int b = 0; b < L->nb; ++b) {
+    const DevBlock &x = L->hb[b];
+    const int *bct = L->d_bct + L->obct[b];
+    if (so_end >= so_beg) {
+      k_muscl_dq<<<grid_for(cnt_all(x, p)), 256, 0, c->s>>>(x, c->d_p, idir, q, dq, bct, L->nbcs[b], so_beg, so_end);
+      int r = after_launch(c);
+      if (r) return r;
+    }
+    k_muscl_face<<<grid_for(cnt_all(x, p)), 256, 0, c->s>>>(x, c->d_p, idir, nl, q, qp, qm, dq, dqp, dqm, bct,
+                                                             L->nbcs[b]);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_roflux(cosa_ctx *c, int32_t idir, int32_t nl, const double *qr, const double *ql, double *flux,
+                    const double *sijk) {
+  LevelState *L = level(c, nl);
+  if (!L || idir < 1 || idir > 3 || !qr || !ql || !flux || !sijk) return COSA_ERR_ARG;
+  if (c->p.moving) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_all, [&](int, const DevBlock &b, int g) {
+    k_roflux<<<g, 256, 0, c->s>>>(b, c->d_p, idir, qr, ql, flux, sijk);
+  });
+}
+
+int cosa_gpu_resid(cosa_ctx *c, int32_t idir, int32_t nl, const double *flux, double *res) {
+  LevelState *L = level(c, nl);
+  if (!L || idir < 1 || idir > 3 || !flux || !res) return COSA_ERR_ARG;
+  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+    k_resid<<<g, 256, 0, c->s>>>(b, c->d_p, idir, flux, res);
+  });
+}
+
+int cosa_gpu_update(cosa_ctx *c, int32_t nl, const double *res, double *q, const double *qold, const double *dtvol,
+                    double ar) {
+  LevelState *L = level(c, nl);
+  if (!L || !res || !q || !qold || !dtvol) return COSA_ERR_ARG;
+  if (c->p.kom || c->p.harbal || c->p.rkimp) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+    k_update<<<g, 256, 0, c->s>>>(b, c->d_p, res, q, qold, dtvol, ar);
+  });
+}
+
+int cosa_gpu_zero(cosa_ctx *c, int32_t nl, double *a) {
+  LevelState *L = level(c, nl);
+  if (!L || !a) return COSA_ERR_ARG;
+  return for_blocks(c, *L, cnt_all, [&](int, const DevBlock &b, int g) {
+    k_zero_res<<<g, 256, 0, c->s>>>(b, c->d_p, a);
+  });
+}
+
+int cosa_gpu_resg_rms(cosa_ctx *c, int32_t nl, const double *res, const double *rhs, double *resrms) {
+  LevelState *L = level(c, nl);
+  if (!L || !res || !resrms) return COSA_ERR_ARG;
+  int r = 0;
+  if (L->npart_cap < L->nb * 64) {
+    drop_graphs(c);
+    if ((r = dalloc(c, &L->d_part, (size_t)L->nb * 64 * 8))) return r;
+    L->npart_cap = L->nb * 64;
+  }
+  for (int b = 0; b < L->nb; ++b) {
+    k_rms_partial<<<64, 256, 0, c->s>>>(L->hb[b], c->d_p, res, rhs, L->d_part + (int64_t)b * 64 * 8);
+    if ((r = after_launch(c))) return r;
+  }
+  if ((r = ensure_hist(c, 1))) return r;
+  int64_t ncell = 0;
+  for (auto &b : L->hb) ncell += (int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1);
+  k_rms_final<<<1, 256, 0, c->s>>>(L->d_part, L->nb * 64, c->p.npde, (double)ncell, c->d_hist, nullptr, 1);
+  if ((r = after_launch(c))) return r;
+  CK(cudaMemcpyAsync(resrms, c->d_hist, (c->p.npde + 1) * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  return COSA_OK;
+}
+
+// ---- fused smooth ------------------------------------------------------------------------
+int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32_t rms_every, double *hist) {
+  LevelState *L = level(c, nl);
+  if (!L || !L->bound || niter < 0 || rms_every < 1) return COSA_ERR_ARG;
+  int r = check_fused_supported(c->p);
+  if (r) return r;
+  const cosa_level_ptrs &P = L->ptrs;
+  if (!P.q || !P.qold || !P.dtvol || !P.si || !P.sj || !P.sk) return COSA_ERR_ARG;
+  cudaSetDevice(c->device);
+  const int npde = c->p.npde;
+  // schedule of printed iterations (src/cosa.f90:1925-1927)
+  std::vector<int> rows;
+  const int last = mgit0 + niter - 1;
+  for (int it = 0; it < niter; ++it) {
+    const int mgit = mgit0 + it;
+    if (hist && (mgit == 1 || mgit % rms_every == 0 || mgit == last)) rows.push_back(it);
+  }
+  if ((r = ensure_hist(c, std::max<int>(1, (int)rows.size())))) return r;
+  CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
+  const int iter = 1;
+  const int compute_dt = (iter / c->p.iupdt * c->p.iupdt == iter) ? 1 : 0;
+  size_t ri = 0;
+  for (int it = 0; it < niter; ++it) {
+    const bool want = ri < rows.size() && rows[ri] == it;
+    if (want) ++ri;
+    cudaGraphExec_t &g = L->graph[want ? 1 : 0];
+    if (!g) {
+      cudaGraph_t graph;
+      CK(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
+      const long long before = c->launches;
+      r = launch_iteration(c, nl, *L, want, compute_dt);
+      cudaError_t e = cudaStreamEndCapture(c->s, &graph);
+      if (r) return r;
+      CK(e);
+      CK(cudaGraphInstantiate(&g, graph, 0));
+      cudaGraphDestroy(graph);
+      c->launches = before;  // counted at replay
+    }
+    CK(cudaGraphLaunch(g, c->s));
+    c->launches += c->p.nstage * (L->items.empty() ? 1 : 2) + (want ? 1 : 0);
+  }
+  // reference state after smooth(): face halos of q in conservative form
+  if (niter > 0 && !L->items.empty()) {
+    double *last_in = (c->p.nstage % 2 == 0) ? L->d_T : L->ptrs.q;
+    const int S = 2 * c->p.nharms + 1;
+    k_halo_p2c<<<grid_for((int64_t)L->items.size() * S), 256, 0, c->s>>>(L->d_blocks, L->d_items,
+                                                                        (int)L->items.size(), c->d_p, last_in,
+                                                                        L->ptrs.q);
+    if ((r = after_launch(c))) return r;
+  }
+  if (hist) {
+    std::vector<double> h(rows.size() * (npde + 1));
+    if (!rows.empty())
+      CK(cudaMemcpyAsync(h.data(), c->d_hist, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    CK(cudaStreamSynchronize(c->s));
+    for (int it = 0; it < niter; ++it)
+      for (int v = 0; v <= npde; ++v) hist[(int64_t)it * (npde + 1) + v] = NAN;
+    for (size_t k = 0; k < rows.size(); ++k)
+      for (int v = 0; v <= npde; ++v) hist[(int64_t)rows[k] * (npde + 1) + v] = h[k * (npde + 1) + v];
+  }
+  return cosa_gpu_status(c, 0);
+}
+
+int cosa_gpu_smooth_host(cosa_ctx *c, int32_t nl, double *q_host, int32_t niter, int32_t mgit0, int32_t rms_every,
+                         double *hist) {
+  LevelState *L = level(c, nl);
+  if (!L || !L->bound || !q_host) return COSA_ERR_ARG;
+  const int64_t n = L->n3 * c->p.npde * (2 * c->p.nharms + 1);
+  int r = cosa_gpu_memcpy_h2d(c, L->ptrs.q, q_host, n);
+  if (r) return r;
+  r = cosa_gpu_smooth(c, nl, niter, mgit0, rms_every, hist);
+  int r2 = cosa_gpu_memcpy_d2h(c, q_host, L->ptrs.q, n);
+  return r ? r : r2;
+}
+
+int cosa_gpu_imetrix(cosa_ctx *c, int32_t nl, const double *x, const double *y, const double *z, double *si,
+                     double *sj, double *sk) {
+  LevelState *L = level(c, nl);
+  if (!L || !x || !y || !z || !si || !sj || !sk) return COSA_ERR_ARG;
+  if (c->p.hbmove || c->p.moving) return COSA_ERR_UNSUPPORTED;
+  double *s3[3] = {si, sj, sk};
+  for (int b = 0; b < L->nb; ++b)
+    for (int d = 1; d <= 3; ++d) {
+      const DevBlock &x_ = L->hb[b];
+      k_imetrix<<<grid_for((int64_t)(x_.im + 1) * (x_.jm + 1) * (x_.km + 1)), 256, 0, c->s>>>(x_, d, x, y, z, s3[d - 1]);
+      int r = after_launch(c);
+      if (r) return r;
+    }
+  return COSA_OK;
+}
+
+int cosa_gpu_vols(cosa_ctx *c, int32_t nl, const double *x, const double *y, const double *z, double *vol) {
+  LevelState *L = level(c, nl);
+  if (!L || !x || !y || !z || !vol) return COSA_ERR_ARG;
+  for (int b = 0; b < L->nb; ++b) {
+    const DevBlock &x_ = L->hb[b];
+    k_vols<<<grid_for((int64_t)x_.im * x_.jm * x_.km), 256, 0, c->s>>>(x_, x, y, z, vol);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_profile(cosa_ctx *c, int32_t nl, int32_t niter, double ms[3], int64_t counts[3]) {
+  LevelState *L = level(c, nl);
+  if (!L || !L->bound || niter < 1 || !ms || !counts) return COSA_ERR_ARG;
+  int r = check_fused_supported(c->p);
+  if (r) return r;
+  ProfState &pf = c->prof;
+  for (auto &e2 : pf.ev)
+    for (auto &e : e2)
+      if (!e) CK(cudaEventCreate(&e));
+  pf.ms[0] = pf.ms[1] = 0;
+  pf.n[0] = pf.n[1] = 0;
+  pf.on = true;
+  cudaEvent_t t0, t1;
+  CK(cudaEventCreate(&t0));
+  CK(cudaEventCreate(&t1));
+  const int compute_dt = (1 / c->p.iupdt * c->p.iupdt == 1) ? 1 : 0;
+  cudaEventRecord(t0, c->s);
+  for (int it = 0; it < niter && !r; ++it) r = launch_iteration(c, nl, *L, false, compute_dt);
+  cudaEventRecord(t1, c->s);
+  pf.on = false;
+  CK(cudaEventSynchronize(t1));
+  float tot = 0;
+  cudaEventElapsedTime(&tot, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (r) return r;
+  ms[0] = pf.n[0] ? pf.ms[0] / pf.n[0] : 0.0;
+  ms[1] = pf.n[1] ? pf.ms[1] / pf.n[1] : 0.0;
+  ms[2] = tot / niter;
+  counts[0] = pf.n[0];
+  counts[1] = pf.n[1];
+  counts[2] = niter;
+  return cosa_gpu_status(c, 0);
+}
+
+void *cosa_gpu_stream(cosa_ctx *c) { return c ? (void *)c->s : nullptr; }
+
+int64_t cosa_gpu_launch_count(cosa_ctx *c, int32_t reset) {
+  if (!c) return -1;
+  const long long v = c->launches;
+  if (reset) c->launches = 0;
+  return v;
+}
+
+int cosa_gpu_status(cosa_ctx *c, int32_t reset) {
+  if (!c) return COSA_ERR_ARG;
+  int st = 0;
+  if (cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->s) != cudaSuccess) return COSA_ERR_CUDA;
+  if (cudaStreamSynchronize(c->s) != cudaSuccess) return COSA_ERR_CUDA;
+  if (reset) cudaMemsetAsync(c->d_status, 0, sizeof(int), c->s);
+  return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,410 @@
+// Fused RK stage for sm_100a: halo fill + tiled residual/update kernel.
+//
+// One RK stage of smooth() (src/cosa.f90:1719-2016) for the explicit Euler
+// path is cons2prim -> bc -> cutman_q -> prtest -> [lambda, deltat] ->
+// muscl/roflux/resid x3 -> prim2cons -> [resg_rms] -> update: about 25
+// full-array sweeps.  Here it is two kernels:
+//
+//  k_halo        one thread per boundary/cut face cell and snapshot: reads
+//                the conservative interior next to the face, converts it to
+//                primitive form, applies the BC (or the cut copy) and writes
+//                the primitive halo values into the halo slots of the same
+//                state array.  Halo cells written twice in the reference keep
+//                the reference's last writer (mask computed on the host).
+//  k_stage_tile  a CTA owns a TI x TJ column of cells of one block and
+//                marches along k.  Planes of the state are staged in a 4-deep
+//                shared-memory ring (interior cells converted cons->prim on
+//                the way in, halo cells taken as written by k_halo); every
+//                i-, j- and k-face of the tile is reconstructed (MUSCL +
+//                limiter) and Roe-fluxed once per tile, the k-face flux is
+//                carried in registers between planes, the flux divergence is
+//                summed in the reference order, and the stage update
+//                q = qold - alpha dt/V R is written directly.  On stage 1 it
+//                also computes the local time step (lambda/deltat) and the
+//                per-tile residual sums of squares for resg_rms.
+#pragma once
+#include "physics.cuh"
+
+struct HaloItem {
+  int dblk, sblk;   // destination / source block (0-based)
+  int type;         // BC type, -1 = cut copy
+  int idir;         // direction of the face (1..3)
+  int mask;         // bit0: write first halo layer, bit1: second
+  int sgn;          // sign applied to the face normal
+  int64_t h1, h2;   // halo cells (p3 cell index in dblk)
+  int64_t c1, c2;   // interior cells (p3 cell index in sblk)
+  int64_t mface;    // metric cell index (i + I2*(j + J2*k)) of the face in dblk
+};
+
+struct Tile {
+  int blk, n, i0, j0, k0, k1;  // first cell (i0,j0), planes k0..k1 (inclusive)
+};
+
+// strong-boundary flags of one block: for each direction d and side s
+// (0 = min, 1 = max) a byte per tangential cell (t2,t3), t2 fastest, with
+// (t2,t3) = (j,k) for d=1, (i,k) for d=2, (i,j) for d=3 (1-based cells).
+struct StrongMap {
+  int64_t off[3][2];
+  int n2[3];
+};
+
+__device__ __forceinline__ bool strong_at(const uint8_t *flags, const StrongMap &m, int d, int side, int t2, int t3) {
+  const int64_t o = m.off[d][side];
+  if (o < 0) return false;
+  return flags[o + (t2 - 1) + (int64_t)m.n2[d] * (t3 - 1)] != 0;
+}
+
+// ---- k_halo ------------------------------------------------------------------------
+template <bool CONS>
+__global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__restrict__ items, int nitems,
+                       const cosa_params *__restrict__ Pp, double *__restrict__ q,
+                       const double *__restrict__ si, const double *__restrict__ sj,
+                       const double *__restrict__ sk, int *status) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
+  const int64_t total = (int64_t)nitems * S;
+  int st = 0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const HaloItem it = items[t % nitems];
+    const int n = (int)(t / nitems);
+    const DevBlock sb = blocks[it.sblk], db = blocks[it.dblk];
+    double c1[7], c2[7], h1[7], h2[7];
+    for (int v = 0; v < npde; ++v) {
+      const int64_t base = p3_var(sb, npde, S, v + 1, n);
+      c1[v] = q[base + it.c1];
+      c2[v] = q[base + it.c2];
+    }
+    if (CONS) {
+      if (npde > 5) { c2p7(P.gamma, c1); c2p7(P.gamma, c2); }
+      else { c2p5(P.gamma, c1); c2p5(P.gamma, c2); }
+    }
+    int mask = 0;
+    if (it.type < 0) {
+      for (int v = 0; v < npde; ++v) { h1[v] = c1[v]; h2[v] = c2[v]; }
+      mask = 3;
+    } else {
+      double nx = 0, ny = 0, nz = 0;
+      if (it.type == 14 || it.type == 21 || it.type == 30) {
+        const double *s = it.idir == 1 ? si : (it.idir == 2 ? sj : sk);
+        const int nh = n * P.hbmove;
+        const int64_t I2 = db.im + 2, J2 = db.jm + 2, K2 = db.km + 2;
+        const int64_t e = ((db.op2 * S2) + (int64_t)nh * I2 * J2 * K2 + it.mface) * 4;
+        nx = s[e] * it.sgn; ny = s[e + 1] * it.sgn; nz = s[e + 2] * it.sgn;
+      }
+      const BcPar B = make_bcpar(P);
+      int err = 0;
+      switch (it.type) {
+        case 80: mask = bc_sym(it.idir, npde, c1, c2, h1, h2); break;
+        case 4: mask = bc_extrapol(npde, c1, h1, h2); break;
+        case 14: mask = bc_walinv(npde, nx, ny, nz, c1, c2, h1, h2); break;
+        case 21: mask = bc_insub(B, nx, ny, nz, c1, c2, h1, h2, &err); break;
+        case 91: mask = bc_outsub(B, c1, c2, h1, h2); break;
+        case 30: mask = bc_far0(B, nx, ny, nz, c1, h1, h2); break;
+        default: st |= COSA_ERR_UNSUPPORTED; break;
+      }
+      if (err) st |= COSA_ERR_INFLOW;
+    }
+    mask &= it.mask;
+    for (int v = 0; v < npde; ++v) {
+      const int64_t base = p3_var(db, npde, S, v + 1, n);
+      if (mask & 1) q[base + it.h1] = h1[v];
+      if (mask & 2) q[base + it.h2] = h2[v];
+    }
+    if (it.idir == 1) {  // bprtest also checks the i halos (src/cosa.f90:1000)
+      if (mask & 1) { if (h1[4] <= P.qmin[4]) st |= COSA_ERR_NEG_P; else if (h1[0] <= P.qmin[0]) st |= COSA_ERR_NEG_RHO; }
+      if (mask & 2) { if (h2[4] <= P.qmin[4]) st |= COSA_ERR_NEG_P; else if (h2[0] <= P.qmin[0]) st |= COSA_ERR_NEG_RHO; }
+    }
+  }
+  if (st) atomicOr(status, st);
+}
+
+// ---- k_stage_tile ------------------------------------------------------------------
+struct StageArgs {
+  const double *qin;     // stage input: interior conservative, halos primitive
+  double *qout;          // stage output (interior written)
+  const double *qold;    // RK base state q^n
+  double *qold_copy;     // if set, q^n interior is copied here (stage 1)
+  double *dtvol;         // Delta t / V, written when compute_dt, read otherwise
+  const double *si, *sj, *sk;
+  double *part;          // per-tile residual sums of squares (npde) or null
+  const double *rhs;     // multigrid forcing or null
+  double *res_out;       // if set, the residual is stored here (P3 layout)
+  const uint8_t *strong; // strong-boundary flags
+  const StrongMap *smap; // per block
+  int *status;
+  double ar;
+  int compute_dt;
+  int first_order;
+  int update;            // 0: residual only (restriction pass)
+};
+
+template <int TI, int TJ, bool MIXED>
+__global__ void __launch_bounds__(TI *TJ, 2)
+k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles, const cosa_params *__restrict__ Pp,
+             StageArgs A) {
+  constexpr int NT = TI * TJ;
+  constexpr int PI = TI + 4, PJ = TJ + 4, PL = PI * PJ;  // padded plane
+  extern __shared__ double smem[];
+  double *ring = smem;                     // [4][5][PJ][PI]
+  double *fi = ring + 4 * 5 * PL;          // [5][TJ][TI+1]
+  double *fj = fi + 5 * TJ * (TI + 1);     // [5][TJ+1][TI]
+  double *red = fj + 5 * (TJ + 1) * TI;    // [5][NT/32]
+
+  const cosa_params &P = *Pp;
+  const Tile T = tiles[blockIdx.x];
+  const DevBlock b = blocks[T.blk];
+  const int npde = 5, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
+  const int n = T.n, nh = n * P.hbmove;
+  const PhysPar ph = make_phys(P);
+  const double g = P.gamma;
+  const int tid = threadIdx.x;
+  const int ti = tid % TI, tj = tid / TI;
+  const int ci = T.i0 + ti, cj = T.j0 + tj;          // this thread's cell column
+  const bool cvalid = ci <= b.im - 1 && cj <= b.jm - 1;
+  const int64_t vstride = b.P3;
+  const double *qin = A.qin + p3_var(b, npde, S, 1, n);
+  const StrongMap sm = A.smap[T.blk];
+  int st = 0;
+
+  auto slot_of = [](int k) { return ((k % 4) + 4) % 4; };
+
+  // load plane k (all cells of the padded plane that the stencils touch)
+  auto load_plane = [&](int k) {
+    double *dst = ring + slot_of(k) * 5 * PL;
+    const bool kin = k >= 1 && k <= b.km - 1;
+    for (int c = tid; c < PL; c += NT) {
+      const int pi = c % PI, pj = c / PI;
+      const int i = T.i0 - 2 + pi, j = T.j0 - 2 + pj;
+      const bool iin = i >= 1 && i <= b.im - 1, jin = j >= 1 && j <= b.jm - 1;
+      const int nout = (!iin) + (!jin) + (!kin);
+      if (nout > 1 || i > b.im + 1 || j > b.jm + 1) continue;  // corners/edges: never read
+      const int64_t cell = p3_cell(b, i, j, k);
+      double v[5];
+#pragma unroll
+      for (int m = 0; m < 5; ++m) v[m] = qin[m * vstride + cell];
+      if (nout == 0) {
+        c2p5(g, v);
+        if (v[4] <= P.qmin[4]) st |= COSA_ERR_NEG_P;
+        else if (v[0] <= P.qmin[0]) st |= COSA_ERR_NEG_RHO;
+      }
+#pragma unroll
+      for (int m = 0; m < 5; ++m) dst[m * PL + c] = v[m];
+    }
+  };
+
+  // face flux along a line: w0..w3 = cells f-2..f+1 (pointers into the ring
+  // with stride `ls` between consecutive cells and PL between variables)
+  auto face = [&](const double *w1p, const double *w0p, const double *w2p, const double *w3p, int f, int mx,
+                  bool slo, bool shi, const double *met, double *F) {
+    double qr[5], ql[5];
+    const bool ovr_lo = (f == 1 && slo), ovr_hi = (f == mx && shi);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      const double a0 = w0p[m * PL], a1 = w1p[m * PL], a2 = w2p[m * PL], a3 = w3p[m * PL];
+      if (A.first_order) {
+        qr[m] = a2; ql[m] = a1;
+      } else {
+        double dlo = a1 - a0, dmid = a2 - a1, dhi = a3 - a2;
+        if ((f - 1 == 1 && slo) || (f - 1 == mx && shi)) dlo = (a1 - a0) * 2;
+        if ((f == 1 && slo) || (f == mx && shi)) dmid = (a2 - a1) * 2;
+        if ((f + 1 == 1 && slo) || (f + 1 == mx && shi)) dhi = (a3 - a2) * 2;
+        if (MIXED) {
+          float dp, dm;
+          limit_face<float>(ph.ilimf, (float)ph.epslimf, (float)ph.rkap, (float)dlo, (float)dmid, (float)dhi, dp, dm);
+          qr[m] = a2 + (double)dp; ql[m] = a1 + (double)dm;
+        } else {
+          double dp, dm;
+          limit_face<double>(ph.ilimf, ph.epslimf, ph.rkap, dlo, dmid, dhi, dp, dm);
+          qr[m] = a2 + dp; ql[m] = a1 + dm;
+        }
+      }
+      if (ovr_lo) { qr[m] = a1; ql[m] = a1; }
+      if (ovr_hi) { qr[m] = a2; ql[m] = a2; }
+    }
+    if (MIXED) roe_flux_mixed(ph, met[0], met[1], met[2], met[3], qr, ql, F);
+    else roe_flux_fp64(ph, met[0], met[1], met[2], met[3], qr, ql, 0.0, 0.0, F);
+  };
+
+  auto metric = [&](const double *s, int i, int j, int k, double *m4) {
+    const int64_t e = p2_idx(b, S2, 1, i, j, k, nh);
+    const double2 a = *reinterpret_cast<const double2 *>(s + e);
+    const double2 c = *reinterpret_cast<const double2 *>(s + e + 2);
+    m4[0] = a.x; m4[1] = a.y; m4[2] = c.x; m4[3] = c.y;
+  };
+
+  // k-face flux at face kf (between planes kf-1 and kf) for this column
+  auto kface = [&](int kf, double *F) {
+    const int pc = (tj + 2) * PI + (ti + 2);
+    const double *w0 = ring + slot_of(kf - 2) * 5 * PL + pc;
+    const double *w1 = ring + slot_of(kf - 1) * 5 * PL + pc;
+    const double *w2 = ring + slot_of(kf) * 5 * PL + pc;
+    const double *w3 = ring + slot_of(kf + 1) * 5 * PL + pc;
+    double m4[4];
+    metric(A.sk, ci, cj, kf, m4);
+    const bool slo = (kf <= 2) && strong_at(A.strong, sm, 2, 0, ci, cj);
+    const bool shi = (kf >= b.km - 1) && strong_at(A.strong, sm, 2, 1, ci, cj);
+    face(w1, w0, w2, w3, kf, b.km, slo, shi, m4, F);
+  };
+
+  double acc[5] = {0, 0, 0, 0, 0};
+  // prologue: planes k0-2 .. k0+1 and the k-face at k0
+  for (int k = T.k0 - 2; k <= T.k0 + 1; ++k) load_plane(k);
+  __syncthreads();
+  double fk_lo[5];
+  if (cvalid) kface(T.k0, fk_lo);
+
+  for (int k = T.k0; k <= T.k1; ++k) {
+    load_plane(k + 2);
+    __syncthreads();
+    double fk_hi[5];
+    if (cvalid) kface(k + 1, fk_hi);
+    const double *pl = ring + slot_of(k) * 5 * PL;
+    // i-faces: left faces of the tile's cells plus the right face of the row
+    for (int f = tid; f < (TI + 1) * TJ; f += NT) {
+      const int fi_ = f % (TI + 1), fj_ = f / (TI + 1);
+      const int i = T.i0 + fi_, j = T.j0 + fj_;
+      if (i > b.im || j > b.jm - 1) continue;
+      const int pc = (fj_ + 2) * PI + (fi_ + 2);
+      double m4[4], F[5];
+      metric(A.si, i, j, k, m4);
+      const bool slo = (i <= 2) && strong_at(A.strong, sm, 0, 0, j, k);
+      const bool shi = (i >= b.im - 1) && strong_at(A.strong, sm, 0, 1, j, k);
+      face(pl + pc - 1, pl + pc - 2, pl + pc, pl + pc + 1, i, b.im, slo, shi, m4, F);
+#pragma unroll
+      for (int m = 0; m < 5; ++m) fi[(m * TJ + fj_) * (TI + 1) + fi_] = F[m];
+    }
+    // j-faces
+    for (int f = tid; f < TI * (TJ + 1); f += NT) {
+      const int fi_ = f % TI, fj_ = f / TI;
+      const int i = T.i0 + fi_, j = T.j0 + fj_;
+      if (i > b.im - 1 || j > b.jm) continue;
+      const int pc = (fj_ + 2) * PI + (fi_ + 2);
+      double m4[4], F[5];
+      metric(A.sj, i, j, k, m4);
+      const bool slo = (j <= 2) && strong_at(A.strong, sm, 1, 0, i, k);
+      const bool shi = (j >= b.jm - 1) && strong_at(A.strong, sm, 1, 1, i, k);
+      face(pl + pc - PI, pl + pc - 2 * PI, pl + pc, pl + pc + PI, j, b.jm, slo, shi, m4, F);
+#pragma unroll
+      for (int m = 0; m < 5; ++m) fj[(m * (TJ + 1) + fj_) * TI + fi_] = F[m];
+    }
+    __syncthreads();
+    if (cvalid) {
+      const int64_t cell = p3_cell(b, ci, cj, k);
+      const int64_t o1 = p1_idx(b, S, ci, cj, k, n);
+      double dt;
+      if (A.compute_dt) {
+        // lambdab + bdeltat (src/cosa.f90:1293-1323, 4860-4870)
+        double qc[5], sim[4], sip[4], sjm[4], sjp[4], skm[4], skp[4];
+        const int pc = (tj + 2) * PI + (ti + 2);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) qc[m] = pl[m * PL + pc];
+        metric(A.si, ci, cj, k, sim); metric(A.si, ci + 1, cj, k, sip);
+        metric(A.sj, ci, cj, k, sjm); metric(A.sj, ci, cj + 1, k, sjp);
+        metric(A.sk, ci, cj, k, skm); metric(A.sk, ci, cj, k + 1, skp);
+        double li, lj, lk;
+        eig_eul(g, qc, sim, sip, sjm, sjp, skm, skp, li, lj, lk);
+        dt = P.cfl / (li + lj + lk);
+        A.dtvol[o1] = dt;
+      } else {
+        dt = A.dtvol[o1];
+      }
+      const double *qo = A.qold + p3_var(b, npde, S, 1, n);
+      double *qw = A.qout + p3_var(b, npde, S, 1, n);
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        // bresid order: i, then j, then k (src/cosa.f90:1800-1876)
+        double r = fi[(m * TJ + tj) * (TI + 1) + ti + 1] - fi[(m * TJ + tj) * (TI + 1) + ti];
+        r = r + fj[(m * (TJ + 1) + tj + 1) * TI + ti] - fj[(m * (TJ + 1) + tj) * TI + ti];
+        r = r + fk_hi[m] - fk_lo[m];
+        if (A.res_out) A.res_out[p3_var(b, npde, S, m + 1, n) + cell] = r;
+        if (A.part) {
+          const double rr = r - (A.rhs ? A.rhs[p3_var(b, npde, S, m + 1, n) + cell] : 0.0);
+          acc[m] += rr * rr;
+        }
+        if (A.update) {
+          const double q0 = qo[m * vstride + cell];
+          if (A.qold_copy) A.qold_copy[p3_var(b, npde, S, m + 1, n) + cell] = q0;
+          qw[m * vstride + cell] = q0 - A.ar * r * dt;
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 5; ++m) fk_lo[m] = fk_hi[m];
+    }
+    __syncthreads();
+  }
+  if (A.part) {
+    // deterministic per-tile sums: warp shuffle then fixed-order warp sums
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      double x = acc[m];
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if ((tid & 31) == 0) red[m * (NT / 32) + (tid >> 5)] = x;
+    }
+    __syncthreads();
+    if (tid < 5) {
+      double x = 0;
+      for (int w = 0; w < NT / 32; ++w) x += red[tid * (NT / 32) + w];
+      A.part[(int64_t)blockIdx.x * 8 + tid] = x;
+    }
+  }
+  if (st) atomicOr(A.status, st);
+}
+
+template <int TI, int TJ>
+constexpr size_t stage_smem_bytes() {
+  return sizeof(double) * (4 * 5 * (TI + 4) * (TJ + 4) + 5 * TJ * (TI + 1) + 5 * (TJ + 1) * TI + 5 * (TI * TJ / 32));
+}
+
+// ---- deterministic reduction of per-tile / per-CTA partials -> resrms ------------------
+// resg_rms (src/cosa.f90:4458-4501): sqrt(sum/ncell), total sqrt(sum/ncell/npde)
+__global__ void k_rms_final(const double *__restrict__ part, int nparts, int npde, double ncell,
+                            double *__restrict__ out, int *row_counter, int nrows_max) {
+  __shared__ double red[8][32];
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int p = threadIdx.x; p < nparts; p += blockDim.x)
+    for (int v = 0; v < npde; ++v) acc[v] += part[(int64_t)p * 8 + v];
+  for (int v = 0; v < npde; ++v) {
+    double x = acc[v];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) red[v][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    double tot[8], all = 0;
+    for (int v = 0; v < npde; ++v) {
+      double x = 0;
+      for (int w = 0; w < nw; ++w) x += red[v][w];
+      tot[v] = x;
+      all = all + x;
+    }
+    int row = 0;
+    if (row_counter) { row = *row_counter; if (row < nrows_max) *row_counter = row + 1; else row = nrows_max - 1; }
+    double *o = out + (int64_t)row * (npde + 1);
+    for (int v = 0; v < npde; ++v) o[v] = sqrt(tot[v] / ncell);
+    o[npde] = sqrt(all / ncell / npde);
+  }
+}
+
+// ---- stage finalisation: face halos of q in conservative form ----------------------------
+// After smooth(), the reference's q holds prim2cons of the last stage's
+// halo values (src/cosa.f90:1908).  src holds those values in primitive form.
+__global__ void k_halo_p2c(const DevBlock *__restrict__ blocks, const HaloItem *__restrict__ items, int nitems,
+                           const cosa_params *__restrict__ Pp, const double *__restrict__ src, double *__restrict__ dst) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int64_t total = (int64_t)nitems * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const HaloItem it = items[t % nitems];
+    const int n = (int)(t / nitems);
+    const DevBlock db = blocks[it.dblk];
+    for (int layer = 0; layer < 2; ++layer) {
+      if (!((it.mask >> layer) & 1)) continue;
+      const int64_t c = layer ? it.h2 : it.h1;
+      double v[7];
+      for (int m = 0; m < npde; ++m) v[m] = src[p3_var(db, npde, S, m + 1, n) + c];
+      p2c(P.gamma, v, npde);
+      for (int m = 0; m < npde; ++m) dst[p3_var(db, npde, S, m + 1, n) + c] = v[m];
+    }
+  }
+}

@@ -1,0 +1,440 @@
+// Per-routine kernels: one CUDA kernel per reference routine, with the
+// reference's array contract (the level drivers of include/cosa_gpu.h).
+// Each kernel covers one block; the host loops over the blocks of a level
+// exactly like the Fortran drivers' `do iblock = 1,mynblocks`.
+#pragma once
+#include "physics.cuh"
+
+// ---- cons2prim_b (src/update.f90:2112-2188) ----------------------------------------
+__global__ void k_cons2prim(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ q, int xtnd) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ni = b.im - 1 + 2 * xtnd, nj = b.jm - 1 + 2 * xtnd, nk = b.km - 1 + 2 * xtnd;
+  const int64_t ncell = (int64_t)ni * nj * nk * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1 - xtnd; r /= ni;
+    const int j = (int)(r % nj) + 1 - xtnd; r /= nj;
+    const int k = (int)(r % nk) + 1 - xtnd; r /= nk;
+    const int n = (int)r;
+    const int64_t c = p3_cell(b, i, j, k);
+    double v[7];
+    for (int m = 0; m < npde; ++m) v[m] = q[p3_var(b, npde, S, m + 1, n) + c];
+    if (npde > 5) c2p7(P.gamma, v); else c2p5(P.gamma, v);
+    for (int m = 0; m < npde; ++m) q[p3_var(b, npde, S, m + 1, n) + c] = v[m];
+  }
+}
+
+// ---- prim2cons_b (src/update.f90:1875-2084): interior + face halos ------------------
+__global__ void k_prim2cons(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ q) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  // domain: i in -1..im+1, j,k in -1..jm+1/-1..km+1 restricted to the
+  // interior plus the six face-halo slabs (no edges, no corners)
+  const int ni = b.im + 3, nj = b.jm + 3, nk = b.km + 3;
+  const int64_t ncell = (int64_t)ni * nj * nk * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) - 1; r /= ni;
+    const int j = (int)(r % nj) - 1; r /= nj;
+    const int k = (int)(r % nk) - 1; r /= nk;
+    const int n = (int)r;
+    const int oi = (i < 1 || i > b.im - 1), oj = (j < 1 || j > b.jm - 1), ok = (k < 1 || k > b.km - 1);
+    if (oi + oj + ok > 1) continue;
+    const int64_t c = p3_cell(b, i, j, k);
+    double v[7];
+    for (int m = 0; m < npde; ++m) v[m] = q[p3_var(b, npde, S, m + 1, n) + c];
+    p2c(P.gamma, v, npde);
+    for (int m = 0; m < npde; ++m) q[p3_var(b, npde, S, m + 1, n) + c] = v[m];
+  }
+}
+
+// ---- bprtest (src/cosa.f90:960-1120): status bits instead of stop -----------------
+__global__ void k_prtest(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ q, int *status) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ni = b.im + 3, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t ncell = (int64_t)ni * nj * nk * S;
+  int st = 0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) - 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)(r % nk) + 1; r /= nk;
+    const int n = (int)r;
+    const int64_t c = p3_cell(b, i, j, k);
+    const double rho = q[p3_var(b, npde, S, 1, n) + c], pr = q[p3_var(b, npde, S, 5, n) + c];
+    if (pr <= P.qmin[4]) st |= COSA_ERR_NEG_P;
+    else if (rho <= P.qmin[0]) st |= COSA_ERR_NEG_RHO;
+  }
+  if (st) atomicOr(status, st);
+}
+
+// ---- lambdab inviscid (src/cosa.f90:1248-1330) --------------------------------------
+__global__ void k_lambda(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
+                         const double *__restrict__ si, const double *__restrict__ sj,
+                         const double *__restrict__ sk, double *__restrict__ lam) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t ncell = (int64_t)ni * nj * nk * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)(r % nk) + 1; r /= nk;
+    const int n = (int)r, nh = n * P.hbmove;
+    const int64_t c = p3_cell(b, i, j, k);
+    double qc[5], sim[4], sip[4], sjm[4], sjp[4], skm[4], skp[4];
+    for (int m = 0; m < 5; ++m) qc[m] = q[p3_var(b, npde, S, m + 1, n) + c];
+    for (int m = 0; m < 4; ++m) {
+      sim[m] = si[p2_idx(b, S2, m + 1, i, j, k, nh)]; sip[m] = si[p2_idx(b, S2, m + 1, i + 1, j, k, nh)];
+      sjm[m] = sj[p2_idx(b, S2, m + 1, i, j, k, nh)]; sjp[m] = sj[p2_idx(b, S2, m + 1, i, j + 1, k, nh)];
+      skm[m] = sk[p2_idx(b, S2, m + 1, i, j, k, nh)]; skp[m] = sk[p2_idx(b, S2, m + 1, i, j, k + 1, nh)];
+    }
+    double li, lj, lk;
+    eig_eul(P.gamma, qc, sim, sip, sjm, sjp, skm, skp, li, lj, lk);
+    lam[p3_var(b, npde, S, 1, n) + c] = li;
+    lam[p3_var(b, npde, S, 2, n) + c] = lj;
+    lam[p3_var(b, npde, S, 3, n) + c] = lk;
+  }
+}
+
+// ---- bdeltat (src/cosa.f90:4733-5203): dtvol and IRS beta, inviscid ---------------
+__global__ void k_deltat(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ dtv,
+                         const double *__restrict__ lam, double *bx, double *by, double *bz) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t ncell = (int64_t)ni * nj * nk * S;
+  const double zeta = 0.4;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)(r % nk) + 1; r /= nk;
+    const int n = (int)r;
+    const int64_t c = p3_cell(b, i, j, k);
+    const double lami = lam[p3_var(b, npde, S, 1, n) + c];
+    const double lamj = lam[p3_var(b, npde, S, 2, n) + c];
+    const double lamk = lam[p3_var(b, npde, S, 3, n) + c];
+    const int64_t o = p1_idx(b, S, i, j, k, n);
+    dtv[o] = P.cfl / (lami + lamj + lamk);
+    if (P.irsop == 2 && bx) {
+      const double phixi = 1 + pow(lamj / lami, zeta) + pow(lamk / lami, zeta);
+      const double phieta = 1 + pow(lami / lamj, zeta) + pow(lamk / lamj, zeta);
+      const double phizeta = 1 + pow(lami / lamk, zeta) + pow(lamj / lamk, zeta);
+      double tt;
+      tt = (P.rat * lami * phixi / (lami + lamj + lamk)); bx[o] = fmax(0.0, (tt * tt - 1) / 4);
+      tt = (P.rat * lamj * phieta / (lami + lamj + lamk)); by[o] = fmax(0.0, (tt * tt - 1) / 4);
+      tt = (P.rat * lamk * phizeta / (lami + lamj + lamk)); bz[o] = fmax(0.0, (tt * tt - 1) / 4);
+    } else if (P.irsop == 3 && bx) {
+      const double rji = lamj / lami, rki = lamk / lami, rij = lami / lamj;
+      const double rkj = lamk / lamj, rik = lami / lamk, rjk = lamj / lamk;
+      double tt;
+      tt = P.rat / (1 + P.psirs * (rji + rki)); bx[o] = fmax(0.0, 0.25 * (tt * tt - 1));
+      tt = P.rat / (1 + P.psirs * (rij + rkj)); by[o] = fmax(0.0, 0.25 * (tt * tt - 1));
+      tt = P.rat / (1 + P.psirs * (rik + rjk)); bz[o] = fmax(0.0, 0.25 * (tt * tt - 1));
+    }
+  }
+}
+
+// ---- muscl_b{i,j,k} (src/flux.f90:1221-1810) ---------------------------------------
+// Pass 1: dq along d over the reference's range, with strong-boundary doubling.
+__global__ void k_muscl_dq(DevBlock b, const cosa_params *__restrict__ Pp, int d, const double *__restrict__ q,
+                           double *__restrict__ dq, const int *__restrict__ bct, int nbcs, int vs, int ve) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
+  int lo[3] = {1, 1, 1}, n_[3] = {b.im - 1, b.jm - 1, b.km - 1};
+  lo[d - 1] = 0; n_[d - 1] = mx + 2;
+  const int nv = ve - vs + 1;
+  const int64_t ncell = (int64_t)n_[0] * n_[1] * n_[2] * nv * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % n_[0]) + lo[0]; r /= n_[0];
+    const int j = (int)(r % n_[1]) + lo[1]; r /= n_[1];
+    const int k = (int)(r % n_[2]) + lo[2]; r /= n_[2];
+    const int v = (int)(r % nv) + vs; r /= nv;
+    const int n = (int)r;
+    const int im1 = i - (d == 1), jm1 = j - (d == 2), km1 = k - (d == 3);
+    const int64_t base = p3_var(b, npde, S, v, n);
+    double val = q[base + p3_cell(b, i, j, k)] - q[base + p3_cell(b, im1, jm1, km1)];
+    const int e = d == 1 ? i : (d == 2 ? j : k);
+    if (e == 1 || e == mx) {
+      for (int ib = 0; ib < nbcs; ++ib) {
+        const int *rw = bct + 10 * ib;
+        if (rw[1] != d || !strong_bc(rw[0])) continue;
+        const int bcpt = rw[2] == 1 ? 1 : mx;
+        if (e != bcpt) continue;
+        const int t2 = d == 1 ? j : i, t3 = d == 3 ? j : k;
+        const int s2 = d == 1 ? rw[5] : rw[3], e2 = d == 1 ? rw[6] : rw[4];
+        const int s3 = d == 3 ? rw[5] : rw[7], e3 = d == 3 ? rw[6] : rw[8];
+        if (t2 >= s2 && t2 <= e2 && t3 >= s3 && t3 <= e3) {
+          val = (q[base + p3_cell(b, i, j, k)] - q[base + p3_cell(b, im1, jm1, km1)]) * 2;
+          break;
+        }
+      }
+    }
+    dq[base + p3_cell(b, i, j, k)] = val;
+  }
+}
+
+// Pass 2: limiter + construction of qp/qm on the faces, then the
+// strong-boundary override (qp = qm = q(halo)).
+__global__ void k_muscl_face(DevBlock b, const cosa_params *__restrict__ Pp, int d, int nl,
+                             const double *__restrict__ q, double *__restrict__ qp, double *__restrict__ qm,
+                             const double *__restrict__ dq, double *__restrict__ dqp, double *__restrict__ dqm,
+                             const int *__restrict__ bct, int nbcs) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
+  int n_[3] = {b.im - 1, b.jm - 1, b.km - 1};
+  n_[d - 1] = mx;
+  const int64_t ncell = (int64_t)n_[0] * n_[1] * n_[2] * npde * S;
+  const bool first_all = nl >= P.nl_crs;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % n_[0]) + 1; r /= n_[0];
+    const int j = (int)(r % n_[1]) + 1; r /= n_[1];
+    const int k = (int)(r % n_[2]) + 1; r /= n_[2];
+    const int v = (int)(r % npde) + 1; r /= npde;
+    const int n = (int)r;
+    const int di = (d == 1), dj = (d == 2), dk = (d == 3);
+    const int64_t base = p3_var(b, npde, S, v, n);
+    const int64_t c0 = p3_cell(b, i, j, k), cm = p3_cell(b, i - di, j - dj, k - dk);
+    const bool fo = first_all || (P.foturb && v >= 6);
+    double vp, vm;
+    if (fo) {
+      vp = q[base + c0];
+      vm = q[base + cm];
+    } else {
+      const double dlo = dq[base + cm], dmid = dq[base + c0], dhi = dq[base + p3_cell(b, i + di, j + dj, k + dk)];
+      double a, bq;
+      const int ilim = v <= 5 ? P.ilimf : P.ilimt;
+      const double eps = v <= 5 ? P.epslimf : P.epslimt;
+      limit_face<double>(ilim, eps, P.rkap, dlo, dmid, dhi, a, bq);
+      dqp[base + c0] = a;
+      dqm[base + c0] = bq;
+      vp = q[base + c0] + a;
+      vm = q[base + cm] + bq;
+    }
+    const int e = d == 1 ? i : (d == 2 ? j : k);
+    if (e == 1 || e == mx) {
+      for (int ib = 0; ib < nbcs; ++ib) {
+        const int *rw = bct + 10 * ib;
+        if (rw[1] != d || !strong_bc(rw[0])) continue;
+        const int qpm = rw[2] == 1 ? 1 : mx;
+        if (e != qpm) continue;
+        const int t2 = d == 1 ? j : i, t3 = d == 3 ? j : k;
+        const int s2 = d == 1 ? rw[5] : rw[3], e2 = d == 1 ? rw[6] : rw[4];
+        const int s3 = d == 3 ? rw[5] : rw[7], e3 = d == 3 ? rw[6] : rw[8];
+        if (t2 >= s2 && t2 <= e2 && t3 >= s3 && t3 <= e3) {
+          const int64_t cb = rw[2] == 1 ? cm : c0;  // q(0) at the min face, q(mx) at the max face
+          vp = q[base + cb];
+          vm = q[base + cb];
+        }
+      }
+    }
+    qp[base + c0] = vp;
+    qm[base + c0] = vm;
+  }
+}
+
+// ---- roflux_b (src/flux.f90:45-238) --------------------------------------------------
+__global__ void k_roflux(DevBlock b, const cosa_params *__restrict__ Pp, int d, const double *__restrict__ qr,
+                         const double *__restrict__ ql, double *__restrict__ flux, const double *__restrict__ sijk) {
+  const cosa_params &P = *Pp;
+  const PhysPar ph = make_phys(P);
+  const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
+  const int ic = d == 1 ? b.im : b.im - 1, jc = d == 2 ? b.jm : b.jm - 1, kc = d == 3 ? b.km : b.km - 1;
+  const int64_t ncell = (int64_t)ic * jc * kc * S;
+  const bool kom = npde > 5;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ic) + 1; r /= ic;
+    const int j = (int)(r % jc) + 1; r /= jc;
+    const int k = (int)(r % kc) + 1; r /= kc;
+    const int n = (int)r, nh = n * P.hbmove;
+    const int64_t c = p3_cell(b, i, j, k);
+    double vr[5], vl[5], f[5];
+    for (int m = 0; m < 5; ++m) {
+      vr[m] = qr[p3_var(b, npde, S, m + 1, n) + c];
+      vl[m] = ql[p3_var(b, npde, S, m + 1, n) + c];
+    }
+    const double tker = kom ? qr[p3_var(b, npde, S, 6, n) + c] : 0.0;
+    const double tkel = kom ? ql[p3_var(b, npde, S, 6, n) + c] : 0.0;
+    roe_flux_fp64(ph, sijk[p2_idx(b, S2, 1, i, j, k, nh)], sijk[p2_idx(b, S2, 2, i, j, k, nh)],
+                  sijk[p2_idx(b, S2, 3, i, j, k, nh)], sijk[p2_idx(b, S2, 4, i, j, k, nh)], vr, vl, tker, tkel, f);
+    for (int m = 0; m < 5; ++m) flux[f0_idx(b, npde, S, i, j, k, m + 1, n)] = f[m];
+  }
+}
+
+// ---- bresid (src/cosa.f90:1149-1211) --------------------------------------------------
+__global__ void k_resid(DevBlock b, const cosa_params *__restrict__ Pp, int d, const double *__restrict__ flux,
+                        double *__restrict__ res) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t ncell = (int64_t)ni * nj * nk * npde * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)(r % nk) + 1; r /= nk;
+    const int v = (int)(r % npde) + 1; r /= npde;
+    const int n = (int)r;
+    const int64_t o = p3_var(b, npde, S, v, n) + p3_cell(b, i, j, k);
+    res[o] = res[o] + flux[f0_idx(b, npde, S, i + (d == 1), j + (d == 2), k + (d == 3), v, n)] -
+             flux[f0_idx(b, npde, S, i, j, k, v, n)];
+  }
+}
+
+// ---- update_b explicit, mean flow (src/update.f90:568-640) ---------------------------
+__global__ void k_update(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
+                         double *__restrict__ q, const double *__restrict__ qold, const double *__restrict__ dtv,
+                         double ar) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t ncell = (int64_t)ni * nj * nk * 5 * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)(r % nk) + 1; r /= nk;
+    const int v = (int)(r % 5) + 1; r /= 5;
+    const int n = (int)r;
+    const int64_t o = p3_var(b, npde, S, v, n) + p3_cell(b, i, j, k);
+    q[o] = qold[o] - ar * res[o] * dtv[p1_idx(b, S, i, j, k, n)];
+  }
+}
+
+// ---- zero (src/util.f90), extent 1: 0..imax etc. ---------------------------------------
+__global__ void k_zero_res(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ res) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ni = b.im + 1, nj = b.jm + 1, nk = b.km + 1;
+  const int64_t ncell = (int64_t)ni * nj * nk * npde * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni); r /= ni;
+    const int j = (int)(r % nj); r /= nj;
+    const int k = (int)(r % nk); r /= nk;
+    const int v = (int)(r % npde) + 1; r /= npde;
+    const int n = (int)r;
+    res[p3_var(b, npde, S, v, n) + p3_cell(b, i, j, k)] = 0.0;
+  }
+}
+
+// ---- resg_brms partial sums (src/cosa.f90:4503-4582): one partial per CTA -----------
+__global__ void k_rms_partial(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
+                              const double *__restrict__ rhs, double *__restrict__ part) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t ncell = (int64_t)ni * nj * nk;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)r + 1;
+    const int64_t c = p3_cell(b, i, j, k);
+    for (int v = 0; v < npde; ++v) {
+      const double tt = res[p3_var(b, npde, S, v + 1, 0) + c] - (rhs ? rhs[p3_var(b, npde, S, v + 1, 0) + c] : 0.0);
+      acc[v] += tt * tt;
+    }
+  }
+  __shared__ double red[7][32];
+  for (int v = 0; v < npde; ++v) {
+    double x = acc[v];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) red[v][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int nw = blockDim.x >> 5;
+    for (int v = 0; v < npde; ++v) {
+      double x = threadIdx.x < nw ? red[v][threadIdx.x] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (threadIdx.x == 0) part[(int64_t)blockIdx.x * 8 + v] = x;
+    }
+  }
+}
+
+// ---- imetrix_b (src/grid.f90:847-1010): face unit normals and areas, fixed grid ----
+// One thread per face of family d; x/y/z are P2 grid arrays (0:imax+1, ...).
+__global__ void k_imetrix(DevBlock b, int d, const double *__restrict__ x, const double *__restrict__ y,
+                          const double *__restrict__ z, double *__restrict__ s) {
+  const int64_t I2 = b.im + 2, J2 = b.jm + 2;
+  const int ni = d == 1 ? b.im : b.im - 1, nj = d == 2 ? b.jm : b.jm - 1, nk = d == 3 ? b.km : b.km - 1;
+  const int64_t nf = (int64_t)ni * nj * nk;
+  const double *X = x + b.op2, *Y = y + b.op2, *Z = z + b.op2;
+  auto at = [&](const double *A, int i, int j, int k) { return A[i + I2 * (j + J2 * (int64_t)k)]; };
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nf; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)r + 1;
+    // the two diagonals of the face: (p1 -> p3) and (p2 -> p4)
+    int a0[3], a1[3], b0[3], b1[3];
+    if (d == 1) { a0[0] = i; a0[1] = j; a0[2] = k; a1[0] = i; a1[1] = j + 1; a1[2] = k + 1;
+                  b0[0] = i; b0[1] = j + 1; b0[2] = k; b1[0] = i; b1[1] = j; b1[2] = k + 1; }
+    else if (d == 2) { a0[0] = i; a0[1] = j; a0[2] = k; a1[0] = i + 1; a1[1] = j; a1[2] = k + 1;
+                       b0[0] = i + 1; b0[1] = j; b0[2] = k; b1[0] = i; b1[1] = j; b1[2] = k + 1; }
+    else { a0[0] = i; a0[1] = j; a0[2] = k; a1[0] = i + 1; a1[1] = j + 1; a1[2] = k;
+           b0[0] = i + 1; b0[1] = j; b0[2] = k; b1[0] = i; b1[1] = j + 1; b1[2] = k; }
+    const double dxa = at(X, a1[0], a1[1], a1[2]) - at(X, a0[0], a0[1], a0[2]);
+    const double dya = at(Y, a1[0], a1[1], a1[2]) - at(Y, a0[0], a0[1], a0[2]);
+    const double dza = at(Z, a1[0], a1[1], a1[2]) - at(Z, a0[0], a0[1], a0[2]);
+    const double dxb = at(X, b1[0], b1[1], b1[2]) - at(X, b0[0], b0[1], b0[2]);
+    const double dyb = at(Y, b1[0], b1[1], b1[2]) - at(Y, b0[0], b0[1], b0[2]);
+    const double dzb = at(Z, b1[0], b1[1], b1[2]) - at(Z, b0[0], b0[1], b0[2]);
+    double n1, n2, n3;
+    if (d == 2) {  // eta faces: the reference takes the cross product in the other order
+      n1 = (dza * dyb - dya * dzb) / 2;
+      n2 = (dxa * dzb - dza * dxb) / 2;
+      n3 = (dya * dxb - dxa * dyb) / 2;
+    } else {
+      n1 = (dya * dzb - dza * dyb) / 2;
+      n2 = (dza * dxb - dxa * dzb) / 2;
+      n3 = (dxa * dyb - dya * dxb) / 2;
+    }
+    const double area = sqrt(n1 * n1 + n2 * n2 + n3 * n3);
+    const int64_t e = (b.op2 + i + I2 * (j + J2 * (int64_t)k)) * 4;
+    s[e] = n1 / area; s[e + 1] = n2 / area; s[e + 2] = n3 / area; s[e + 3] = area;
+  }
+}
+
+// ---- bvols (src/grid.f90:2160-2230): cell volumes (Kordulla-Vinokur) ---------------------
+__global__ void k_vols(DevBlock b, const double *__restrict__ x, const double *__restrict__ y,
+                       const double *__restrict__ z, double *__restrict__ vol) {
+  const int64_t I2 = b.im + 2, J2 = b.jm + 2, I1 = b.im + 1, J1 = b.jm + 1;
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t nc = (int64_t)ni * nj * nk;
+  const double *X = x + b.op2, *Y = y + b.op2, *Z = z + b.op2;
+  auto at = [&](const double *A, int i, int j, int k) { return A[i + I2 * (j + J2 * (int64_t)k)]; };
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nc; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)r + 1;
+    // components c of the (unnormalised) face vectors of the xi, eta, zeta faces at the cell's min corner
+    auto sface = [&](int d, const double *P, const double *Q, int c) {
+      // c-th component of the cross product of the two face diagonals
+      int a0i = i, a0j = j, a0k = k, a1i, a1j, a1k, b0i, b0j, b0k, b1i, b1j, b1k;
+      if (d == 1) { a1i = i; a1j = j + 1; a1k = k + 1; b0i = i; b0j = j + 1; b0k = k; b1i = i; b1j = j; b1k = k + 1; }
+      else if (d == 2) { a1i = i + 1; a1j = j; a1k = k + 1; b0i = i + 1; b0j = j; b0k = k; b1i = i; b1j = j; b1k = k + 1; }
+      else { a1i = i + 1; a1j = j + 1; a1k = k; b0i = i + 1; b0j = j; b0k = k; b1i = i; b1j = j + 1; b1k = k; }
+      const double pa = at(P, a1i, a1j, a1k) - at(P, a0i, a0j, a0k), pb = at(P, b1i, b1j, b1k) - at(P, b0i, b0j, b0k);
+      const double qa = at(Q, a1i, a1j, a1k) - at(Q, a0i, a0j, a0k), qb = at(Q, b1i, b1j, b1k) - at(Q, b0i, b0j, b0k);
+      (void)c;
+      return d == 2 ? (qa * pb - pa * qb) / 2 : (pa * qb - qa * pb) / 2;
+    };
+    const double dx = (sface(1, Y, Z, 1) + sface(2, Y, Z, 1) + sface(3, Y, Z, 1)) * (at(X, i + 1, j + 1, k + 1) - at(X, i, j, k));
+    const double dy = (sface(1, Z, X, 2) + sface(2, Z, X, 2) + sface(3, Z, X, 2)) * (at(Y, i + 1, j + 1, k + 1) - at(Y, i, j, k));
+    const double dz = (sface(1, X, Y, 3) + sface(2, X, Y, 3) + sface(3, X, Y, 3)) * (at(Z, i + 1, j + 1, k + 1) - at(Z, i, j, k));
+    vol[b.op1 + i + I1 * (j + J1 * (int64_t)k)] = (dx + dy + dz) / 3;
+  }
+}

@@ -1,0 +1,477 @@
+// Pointwise physics of COSA's explicit residual path as device functions.
+//
+// Every function restates a Fortran routine (cited) with the same operation
+// order and parenthesisation, so an FP64 build differs from the reference
+// only by FMA contraction.  The MIXED variants keep the FP64 state and take
+// the slopes and the Roe dissipation in FP32 on FP64 differences.
+#pragma once
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+struct PhysPar {
+  double g, gm1, g_gm1;       // gamma, gamma-1, gamma/(gamma-1)
+  double rkap, epslimf, epslimt;
+  int ilimf, ilimt;
+  int efx_setup_f, efx_all_f, eig_limit_f, eig_lim_all_f;
+  double cntrpy_f, entfxctf_f, eig_cutoff_f;
+  double w1, w2, w3;          // entfx_f_w(1:3) as reals
+};
+
+__device__ __forceinline__ PhysPar make_phys(const cosa_params &P) {
+  PhysPar q;
+  q.g = P.gamma; q.gm1 = P.gamma - 1; q.g_gm1 = P.gamma / (P.gamma - 1);
+  q.rkap = P.rkap; q.epslimf = P.epslimf; q.epslimt = P.epslimt;
+  q.ilimf = P.ilimf; q.ilimt = P.ilimt;
+  q.efx_setup_f = P.efx_setup_f; q.efx_all_f = P.efx_all_f;
+  q.eig_limit_f = P.eig_limit_f; q.eig_lim_all_f = P.eig_lim_all_f;
+  q.cntrpy_f = P.cntrpy_f; q.entfxctf_f = P.entfxctf_f; q.eig_cutoff_f = P.eig_cutoff_f;
+  q.w1 = P.entfx_f_w[0]; q.w2 = P.entfx_f_w[1]; q.w3 = P.entfx_f_w[2];
+  return q;
+}
+
+// ---- cons2prim_b / prim2cons_b cell formulas (src/update.f90:2135-2188, 1875-2084)
+// q[0..4] = (rho, rho u, rho v, rho w, rho E) -> (rho, u, v, w, p); Euler
+__device__ __forceinline__ void c2p5(double g, double *q) {
+  const double rho = q[0];
+  const double u = q[1] / rho, v = q[2] / rho, w = q[3] / rho;
+  q[1] = u; q[2] = v; q[3] = w;
+  q[4] = (g - 1) * (q[4] - rho * (u * u + v * v + w * w) / 2);
+}
+// with k-omega: q[5] = rho k, q[6] = rho omega (divided by rho as well)
+__device__ __forceinline__ void c2p7(double g, double *q) {
+  const double rho = q[0];
+  const double u = q[1] / rho, v = q[2] / rho, w = q[3] / rho;
+  const double tke = q[5] / rho;
+  q[1] = u; q[2] = v; q[3] = w; q[5] = tke; q[6] = q[6] / rho;
+  q[4] = (g - 1) * (q[4] - rho * (u * u + v * v + w * w) / 2 - rho * tke);
+}
+__device__ __forceinline__ void p2c(double g, double *q, int npde) {
+  const double tke = npde > 5 ? q[5] : 0.0;
+  const double rho = q[0];
+  for (int v = 1; v < npde; ++v)
+    if (v != 4) q[v] = q[v] * rho;
+  const double ru = q[1], rv = q[2], rw = q[3], p = q[4];
+  double e = p / (g - 1) + (ru * ru + rv * rv + rw * rw) / 2 / rho;
+  if (npde > 5) e = e + rho * tke;
+  q[4] = e;
+}
+
+// ---- limiters limit_i/j/k (src/flux.f90:3472-3888) -----------------------------
+// For face f of a line: dlo = dq(f-1), dmid = dq(f), dhi = dq(f+1).
+// dqp(f) depends on (dq(f), dq(f+1)), dqm(f) on (dq(f-1), dq(f)).
+template <typename T>
+__device__ __forceinline__ void limit_face(int ilim, T eps, T rkap, T dlo, T dmid, T dhi, T &dqp, T &dqm) {
+  if (ilim == 1) {
+    T s = (2 * dhi * dmid + eps) / (dhi * dhi + dmid * dmid + eps);
+    T rkp = 1 + rkap * s, rkm = 1 - rkap * s;
+    dqp = -s * (rkp * dmid + rkm * dhi) / 4;
+    s = (2 * dmid * dlo + eps) / (dmid * dmid + dlo * dlo + eps);
+    rkp = 1 + rkap * s; rkm = 1 - rkap * s;
+    dqm = s * (rkm * dlo + rkp * dmid) / 4;
+  } else if (ilim == 0) {
+    const T rkp = 1 + rkap, rkm = 1 - rkap;
+    dqp = -(rkp * dmid + rkm * dhi) / 4;
+    dqm = (rkm * dlo + rkp * dmid) / 4;
+  } else if (ilim == 2) {
+    const T rkp = 1 + rkap, rkm = 1 - rkap;
+    const T bb = (T(3) - rkap) / (T(1) - rkap);
+    // pair (d0,d1) = (dq(f), dq(f+1)) gives dqp(f)
+    T d0 = dmid, d1 = dhi;
+    T dqmx = (copysign(T(1), d0) + copysign(T(1), d1)) / 2 * fmin(fabs(d0), fabs(d1) * bb);
+    T dqpx = (copysign(T(1), d1) + copysign(T(1), d0)) / 2 * fmin(fabs(d1), fabs(d0) * bb);
+    dqp = -(rkp * dqmx + rkm * dqpx) / 4;
+    // pair (dq(f-1), dq(f)) gives dqm(f)
+    d0 = dlo; d1 = dmid;
+    dqmx = (copysign(T(1), d0) + copysign(T(1), d1)) / 2 * fmin(fabs(d0), fabs(d1) * bb);
+    dqpx = (copysign(T(1), d1) + copysign(T(1), d0)) / 2 * fmin(fabs(d1), fabs(d0) * bb);
+    dqm = (rkm * dqmx + rkp * dqpx) / 4;
+  } else if (ilim == 3) {
+    const T epsq = eps * eps;
+    T d1 = dhi, d2 = dmid;
+    T dqpx = (d2 * (d1 * d1 + 2 * epsq) + d1 * (2 * (d2 * d2) + epsq)) /
+             (2 * (d2 * d2) - d2 * d1 + 2 * (d1 * d1) + 3 * epsq);
+    dqp = -dqpx / 2;
+    d1 = dmid; d2 = dlo;
+    T dqmx = (d1 * (d2 * d2 + 2 * epsq) + d2 * (2 * (d1 * d1) + epsq)) /
+             (2 * (d1 * d1) - d1 * d2 + 2 * (d2 * d2) + 3 * epsq);
+    dqm = dqmx / 2;
+  } else {  // ilim == 4
+    const T epsq = eps * eps;
+    T d1 = dhi, d2 = dmid;
+    T dqpx = (d1 * (d2 * d2 + epsq) + d2 * (d1 * d1 + epsq)) / (d1 * d1 + d2 * d2 + 2 * epsq);
+    dqp = -dqpx / 2;
+    d1 = dmid; d2 = dlo;
+    T dqmx = (d1 * (d2 * d2 + epsq) + d2 * (d1 * d1 + epsq)) / (d1 * d1 + d2 * d2 + 2 * epsq);
+    dqm = dqmx / 2;
+  }
+}
+
+// ---- roflux_b mean-flow face flux (src/flux.f90:45-238), fixed grid ---------------
+// qr/ql: primitive right/left states (rho,u,v,w,p); tker/tkel: TKE (0 for Euler)
+__device__ __forceinline__ void roe_flux_fp64(const PhysPar &P, double kx, double ky, double kz, double ds,
+                                              const double *qr, const double *ql, double tker, double tkel,
+                                              double *flux) {
+  const double g = P.g;
+  const double ubn = 0.0;
+  const double rhor = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
+  const double unr = ur * kx + vr * ky + wr * kz - ubn;
+  const double q2r = ur * ur + vr * vr + wr * wr;
+  const double h0r = g / (g - 1) * pr / rhor + q2r / 2 + tker;
+  const double rh0r = rhor * h0r;
+  const double rhol = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4];
+  const double unl = ul * kx + vl * ky + wl * kz - ubn;
+  const double q2l = ul * ul + vl * vl + wl * wl;
+  const double h0l = g / (g - 1) * pl / rhol + q2l / 2 + tkel;
+  const double rh0l = rhol * h0l;
+  const double drho = rhor - rhol, dp = pr - pl, du = ur - ul, dv = vr - vl, dw = wr - wl;
+  const double dun = unr - unl, dtke = tker - tkel;
+  const double rhols = sqrt(rhol), rhors = sqrt(rhor);
+  const double rho = rhols * rhors, denom = rhols + rhors;
+  const double u = (rhols * ul + rhors * ur) / denom;
+  const double v = (rhols * vl + rhors * vr) / denom;
+  const double w = (rhols * wl + rhors * wr) / denom;
+  const double un = u * kx + v * ky + w * kz;
+  const double h0 = (rhols * h0l + rhors * h0r) / denom;
+  const double tke = (rhols * tkel + rhors * tker) / denom;
+  const double q2 = u * u + v * v + w * w;
+  const double a2 = (g - 1) * (h0 - q2 / 2 - tke);
+  const double a = sqrt(a2);
+  double rm123 = fabs(un - ubn), rm4 = fabs(un + a - ubn), rm5 = fabs(un - a - ubn);
+  if (P.efx_setup_f) {
+    double rdelta = P.cntrpy_f * (P.w1 * P.entfxctf_f + P.w2 * (sqrt(u * u + v * v + w * w) + a) +
+                                  P.w3 * 0.2 * (fabs(un) + a + fabs(ubn)));
+    rdelta = fmax(rdelta, 1.0e-12);
+    if (rm123 <= rdelta && P.efx_all_f) rm123 = 0.5 * (rm123 * rm123 + rdelta * rdelta) / rdelta;
+    if (rm4 <= rdelta) rm4 = 0.5 * (rm4 * rm4 + rdelta * rdelta) / rdelta;
+    if (rm5 <= rdelta) rm5 = 0.5 * (rm5 * rm5 + rdelta * rdelta) / rdelta;
+  }
+  if (P.eig_limit_f) {
+    if (rm123 <= P.eig_cutoff_f) rm123 = P.eig_cutoff_f;
+    if (P.eig_lim_all_f && rm4 <= P.eig_cutoff_f) rm4 = P.eig_cutoff_f;
+    if (P.eig_lim_all_f && rm5 <= P.eig_cutoff_f) rm5 = P.eig_cutoff_f;
+  }
+  const double dpa2 = dp / a2, rdua = rho * dun / a;
+  const double al1 = rm123 * (drho - dpa2);
+  const double al2 = rm123 * rho;
+  const double al3 = rm4 * (dpa2 + rdua) / 2;
+  const double al4 = rm5 * (dpa2 - rdua) / 2;
+  const double df1 = al1 + al3 + al4;
+  const double df2 = al1 * u + al2 * (du - dun * kx) + al3 * (u + a * kx) + al4 * (u - a * kx);
+  const double df3 = al1 * v + al2 * (dv - dun * ky) + al3 * (v + a * ky) + al4 * (v - a * ky);
+  const double df4 = al1 * w + al2 * (dw - dun * kz) + al3 * (w + a * kz) + al4 * (w - a * kz);
+  const double df5 = al1 * (q2 / 2 + tke) + al2 * (u * du + v * dv + w * dw - un * dun + dtke) +
+                     al3 * (h0 + a * un) + al4 * (h0 - a * un);
+  const double fr1 = rhor * unr, fl1 = rhol * unl;
+  const double fr2 = (rhor * ur * unr + pr * kx), fl2 = (rhol * ul * unl + pl * kx);
+  const double fr3 = (rhor * vr * unr + pr * ky), fl3 = (rhol * vl * unl + pl * ky);
+  const double fr4 = (rhor * wr * unr + pr * kz), fl4 = (rhol * wl * unl + pl * kz);
+  const double fr5 = (rh0r * unr + pr * ubn), fl5 = (rh0l * unl + pl * ubn);
+  flux[0] = (fr1 + fl1 - df1) / 2 * ds;
+  flux[1] = (fr2 + fl2 - df2) / 2 * ds;
+  flux[2] = (fr3 + fl3 - df3) / 2 * ds;
+  flux[3] = (fr4 + fl4 - df4) / 2 * ds;
+  flux[4] = (fr5 + fl5 - df5) / 2 * ds;
+}
+
+// Mixed precision: the central part (fr + fl) in FP64 from the FP64 face
+// states, the Roe dissipation df in FP32 from FP32 copies of the states and
+// of their FP64 differences.  Same algebra as roe_flux_fp64.
+__device__ __forceinline__ void roe_flux_mixed(const PhysPar &P, double kx, double ky, double kz, double ds,
+                                               const double *qr, const double *ql, double *flux) {
+  const double g = P.g;
+  const double rhor = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
+  const double rhol = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4];
+  const double unr = ur * kx + vr * ky + wr * kz;
+  const double unl = ul * kx + vl * ky + wl * kz;
+  const double q2r = ur * ur + vr * vr + wr * wr;
+  const double q2l = ul * ul + vl * vl + wl * wl;
+  const double h0r = g / (g - 1) * pr / rhor + q2r / 2;
+  const double h0l = g / (g - 1) * pl / rhol + q2l / 2;
+  // FP32 dissipation on FP64 differences
+  const float fkx = (float)kx, fky = (float)ky, fkz = (float)kz;
+  const float drho = (float)(rhor - rhol), dp = (float)(pr - pl);
+  const float du = (float)(ur - ul), dv = (float)(vr - vl), dw = (float)(wr - wl);
+  const float dun = (float)(unr - unl);
+  const float frl = (float)rhol, frr = (float)rhor;
+  const float rhols = sqrtf(frl), rhors = sqrtf(frr);
+  const float rho = rhols * rhors;
+  const float rden = 1.0f / (rhols + rhors);
+  const float u = (rhols * (float)ul + rhors * (float)ur) * rden;
+  const float v = (rhols * (float)vl + rhors * (float)vr) * rden;
+  const float w = (rhols * (float)wl + rhors * (float)wr) * rden;
+  const float un = u * fkx + v * fky + w * fkz;
+  const float h0 = (rhols * (float)h0l + rhors * (float)h0r) * rden;
+  const float q2 = u * u + v * v + w * w;
+  const float a2 = (float)(g - 1) * (h0 - q2 * 0.5f);
+  const float a = sqrtf(a2);
+  float rm123 = fabsf(un), rm4 = fabsf(un + a), rm5 = fabsf(un - a);
+  if (P.efx_setup_f) {
+    float rdelta = (float)P.cntrpy_f * ((float)P.w1 * (float)P.entfxctf_f + (float)P.w2 * (sqrtf(q2) + a) +
+                                        (float)P.w3 * 0.2f * (fabsf(un) + a));
+    rdelta = fmaxf(rdelta, 1.0e-12f);
+    if (rm123 <= rdelta && P.efx_all_f) rm123 = 0.5f * (rm123 * rm123 + rdelta * rdelta) / rdelta;
+    if (rm4 <= rdelta) rm4 = 0.5f * (rm4 * rm4 + rdelta * rdelta) / rdelta;
+    if (rm5 <= rdelta) rm5 = 0.5f * (rm5 * rm5 + rdelta * rdelta) / rdelta;
+  }
+  if (P.eig_limit_f) {
+    const float c = (float)P.eig_cutoff_f;
+    if (rm123 <= c) rm123 = c;
+    if (P.eig_lim_all_f && rm4 <= c) rm4 = c;
+    if (P.eig_lim_all_f && rm5 <= c) rm5 = c;
+  }
+  const float ia2 = 1.0f / a2;
+  const float dpa2 = dp * ia2, rdua = rho * dun / a;
+  const float al1 = rm123 * (drho - dpa2);
+  const float al2 = rm123 * rho;
+  const float al3 = rm4 * (dpa2 + rdua) * 0.5f;
+  const float al4 = rm5 * (dpa2 - rdua) * 0.5f;
+  const float df1 = al1 + al3 + al4;
+  const float df2 = al1 * u + al2 * (du - dun * fkx) + al3 * (u + a * fkx) + al4 * (u - a * fkx);
+  const float df3 = al1 * v + al2 * (dv - dun * fky) + al3 * (v + a * fky) + al4 * (v - a * fky);
+  const float df4 = al1 * w + al2 * (dw - dun * fkz) + al3 * (w + a * fkz) + al4 * (w - a * fkz);
+  const float df5 = al1 * (q2 * 0.5f) + al2 * (u * du + v * dv + w * dw - un * dun) + al3 * (h0 + a * un) +
+                    al4 * (h0 - a * un);
+  const double hds = 0.5 * ds;
+  flux[0] = (rhor * unr + rhol * unl - (double)df1) * hds;
+  flux[1] = ((rhor * ur * unr + pr * kx) + (rhol * ul * unl + pl * kx) - (double)df2) * hds;
+  flux[2] = ((rhor * vr * unr + pr * ky) + (rhol * vl * unl + pl * ky) - (double)df3) * hds;
+  flux[3] = ((rhor * wr * unr + pr * kz) + (rhol * wl * unl + pl * kz) - (double)df4) * hds;
+  flux[4] = (rhor * h0r * unr + rhol * h0l * unl - (double)df5) * hds;
+}
+
+// ---- eig_eul (src/cosa.f90:4183-4233), fixed grid ---------------------------------
+__device__ __forceinline__ void eig_eul(double g, const double *qc, const double *sim, const double *sip,
+                                        const double *sjm, const double *sjp, const double *skm,
+                                        const double *skp, double &lami, double &lamj, double &lamk) {
+  const double rho = qc[0], u = qc[1], v = qc[2], w = qc[3], p = qc[4];
+  const double a = sqrt(g * p / rho);
+  const double xix = 0.5 * (sim[0] * sim[3] + sip[0] * sip[3]);
+  const double xiy = 0.5 * (sim[1] * sim[3] + sip[1] * sip[3]);
+  const double xiz = 0.5 * (sim[2] * sim[3] + sip[2] * sip[3]);
+  const double etax = 0.5 * (sjm[0] * sjm[3] + sjp[0] * sjp[3]);
+  const double etay = 0.5 * (sjm[1] * sjm[3] + sjp[1] * sjp[3]);
+  const double etaz = 0.5 * (sjm[2] * sjm[3] + sjp[2] * sjp[3]);
+  const double zetax = 0.5 * (skm[0] * skm[3] + skp[0] * skp[3]);
+  const double zetay = 0.5 * (skm[1] * skm[3] + skp[1] * skp[3]);
+  const double zetaz = 0.5 * (skm[2] * skm[3] + skp[2] * skp[3]);
+  const double axi = (sim[3] + sip[3]) / 2;
+  const double aeta = (sjm[3] + sjp[3]) / 2;
+  const double azeta = (skm[3] + skp[3]) / 2;
+  lami = fabs(u * xix + v * xiy + w * xiz) + a * axi;
+  lamj = fabs(u * etax + v * etay + w * etaz) + a * aeta;
+  lamk = fabs(u * zetax + v * zetay + w * zetaz) + a * azeta;
+}
+
+// ---- boundary conditions (src/bc.f90) --------------------------------------------
+// Each BC maps the primitive interior values next to the face (c1 = first
+// interior cell, c2 = second) and the face normal to the two halo layers
+// (h1 = first halo, h2 = second).  Returned mask: bit0 h1 set, bit1 h2 set.
+struct BcPar {
+  double g, rhoinf, ainf, pinf, sinf;
+  double qfst[5];
+  double t0, p0, sx, sy, sz;
+  double pout1, pout3;
+  double tkefar, omefar, qmin6, qmin7;
+  int npde;
+};
+
+__device__ __forceinline__ BcPar make_bcpar(const cosa_params &P) {
+  BcPar b;
+  b.g = P.gamma; b.rhoinf = P.rhoinf; b.ainf = P.ainf; b.pinf = P.pinf;
+  b.sinf = P.pinf / pow(P.rhoinf, P.gamma);
+  b.qfst[0] = P.rhoinf;
+  b.qfst[1] = P.machfs * cos(P.alpha) * cos(P.beta);
+  b.qfst[2] = P.machfs * sin(P.alpha) * cos(P.beta);
+  b.qfst[3] = P.machfs * sin(P.beta);
+  b.qfst[4] = P.pinf;
+  b.t0 = P.inlet_t0; b.p0 = P.inlet_p0;
+  b.sx = P.inlet_dir[0]; b.sy = P.inlet_dir[1]; b.sz = P.inlet_dir[2];
+  b.pout1 = P.outlet_p[0]; b.pout3 = P.outlet_p[2];
+  b.tkefar = P.tkefar; b.omefar = P.omefar; b.qmin6 = P.qmin[5]; b.qmin7 = P.qmin[6];
+  b.npde = P.npde;
+  return b;
+}
+
+// bc_sym (src/bc.f90:2595-2710)
+__device__ __forceinline__ int bc_sym(int idir, int npde, const double *c1, const double *c2, double *h1, double *h2) {
+  for (int v = 0; v < npde; ++v) {
+    const double s = (v == idir) ? -1.0 : 1.0;
+    h1[v] = s * c1[v];
+    h2[v] = s * c2[v];
+  }
+  return 3;
+}
+// bc_extrapol (src/bc.f90:2494-2592)
+__device__ __forceinline__ int bc_extrapol(int npde, const double *c1, double *h1, double *h2) {
+  for (int v = 0; v < npde; ++v) { h1[v] = c1[v]; h2[v] = c1[v]; }
+  return 3;
+}
+// bc_walinv_14 (src/bc.f90:1457-1675), fixed grid; n = face metric at ibcm
+__device__ __forceinline__ int bc_walinv(int npde, double nx, double ny, double nz, const double *c1,
+                                         const double *c2, double *h1, double *h2) {
+  const double rhow = (3 * c1[0] - c2[0]) / 2, uw = (3 * c1[1] - c2[1]) / 2;
+  const double vw = (3 * c1[2] - c2[2]) / 2, ww = (3 * c1[3] - c2[3]) / 2, pw = (3 * c1[4] - c2[4]) / 2;
+  const double un1 = c1[1] * nx + c1[2] * ny + c1[3] * nz;
+  const double un2 = c2[1] * nx + c2[2] * ny + c2[3] * nz;
+  const double unw = (3 * un1 - un2) / 2;
+  h1[0] = rhow; h1[1] = uw - unw * nx; h1[2] = vw - unw * ny; h1[3] = ww - unw * nz; h1[4] = pw;
+  if (npde > 5) { h1[5] = c1[5]; h1[6] = c1[6]; }
+  for (int v = 0; v < npde; ++v) h2[v] = h1[v];
+  return 3;
+}
+// bc_insub (src/bc.f90:875-1175): subsonic inlet, Newton on the normal
+// velocity; n already multiplied by sgnm.  Returns mask, sets *err on a
+// Newton iteration count of 10 (the reference stops there).
+__device__ __forceinline__ int bc_insub(const BcPar &B, double nx, double ny, double nz, const double *c1,
+                                        const double *c2, double *h1, double *h2, int *err) {
+  const double g = B.g;
+  const double rho1 = c1[0], rho2 = c2[0];
+  const double un1 = c1[1] * nx + c1[2] * ny + c1[3] * nz;
+  const double un2 = c2[1] * nx + c2[2] * ny + c2[3] * nz;
+  const double p1 = c1[4], p2 = c2[4];
+  const double rc1 = sqrt(g * p1 * rho1);
+  const double rc2 = sqrt(g * p2 * rho2);
+  const double rcun1 = rc1 * un1, rcun2 = rc2 * un2;
+  const double h0inl = 1 / (g - 1) * B.t0;
+  const double dot = B.sx * nx + B.sy * ny + B.sz * nz;
+  const double con1 = 0.5 / (h0inl * (dot * dot));
+  const double con2 = 2 * con1 * g / (g - 1);
+  for (int icell = 1; icell <= 2; ++icell) {
+    double p, un, rc, rcun;
+    if (icell == 1) {
+      p = 2 * p1 - p2; un = 2 * un1 - un2; rc = 2 * rc1 - rc2; rcun = 2 * rcun1 - rcun2;
+    } else {
+      p = 3 * p1 - 2 * p2; un = 3 * un1 - 2 * un2; rc = 3 * rc1 - 2 * rc2; rcun = 3 * rcun1 - 2 * rcun2;
+    }
+    const double con3 = p - rcun;
+    double dun = 1.0;
+    int count = 0;
+    while (fabs(dun) > 1.0e-10) {
+      count = count + 1;
+      if (count == 10) { *err = 1; break; }
+      const double par = 1.0 - con1 * (un * un);
+      p = B.p0 * pow(par, g / (g - 1));
+      const double f = p - rc * un - con3;
+      const double fp = -con2 * un * p / par - rc;
+      dun = -f / fp;
+      un = un + dun;
+    }
+    p = +rc * un + con3;
+    const double modv = un / dot;
+    double *h = icell == 1 ? h1 : h2;
+    h[0] = g * p / ((g - 1) * (h0inl - 0.5 * (modv * modv)));
+    h[1] = modv * B.sx; h[2] = modv * B.sy; h[3] = modv * B.sz; h[4] = p;
+    if (B.npde > 5) { h[5] = B.tkefar; h[6] = B.omefar; }
+  }
+  return 3;
+}
+// bc_outsub (src/bc.f90:1178-1455): static-pressure outlet
+__device__ __forceinline__ int bc_outsub(const BcPar &B, const double *c1, const double *c2, double *h1, double *h2) {
+  const double g = B.g;
+  const int npde = B.npde;
+  const bool kom = npde > 5;
+  double qc1[7], qc2[7];
+  const double tke1 = kom ? c1[5] : 0.0, tke2 = kom ? c2[5] : 0.0;
+  qc1[0] = c1[0]; qc2[0] = c2[0];
+  for (int v = 1; v < npde; ++v)
+    if (v != 4) { qc1[v] = c1[v] * c1[0]; qc2[v] = c2[v] * c2[0]; }
+  {
+    const double rho = qc1[0], ru = qc1[1], rv = qc1[2], rw = qc1[3];
+    qc1[4] = c1[4] / (g - 1) + (ru * ru + rv * rv + rw * rw) / 2 / rho + rho * tke1;
+  }
+  {
+    const double rho = qc2[0], ru = qc2[1], rv = qc2[2], rw = qc2[3];
+    qc2[4] = c2[4] / (g - 1) + (ru * ru + rv * rv + rw * rw) / 2 / rho + rho * tke2;
+  }
+  double a[7], b[7];  // conservative halo values
+  for (int v = 0; v < npde; ++v)
+    if (v != 4) a[v] = 2 * qc1[v] - qc2[v];
+  double rhotke0 = 0.0;
+  if (kom) {
+    a[5] = fmax(a[5], a[0] * B.qmin6);
+    a[6] = fmax(a[6], a[0] * B.qmin7);
+    rhotke0 = a[5];
+  }
+  a[4] = B.pout1 / (g - 1) + (a[1] * a[1] + a[2] * a[2] + a[3] * a[3]) / 2 / a[0] + rhotke0;
+  for (int v = 0; v < npde; ++v)
+    if (v != 4) b[v] = 3 * qc1[v] - 2 * qc2[v];
+  double rhotke2 = 0.0, rhotke1 = 0.0, rhotkem1 = 0.0;
+  if (kom) {
+    b[5] = fmax(b[5], b[0] * B.qmin6);
+    b[6] = fmax(b[6], b[0] * B.qmin7);
+    rhotke2 = qc2[5]; rhotke1 = qc1[5]; rhotkem1 = b[5];
+  }
+  const double rhol = (3 * qc1[0] - qc2[0]) / 2;
+  const double rhor = (3 * a[0] - b[0]) / 2;
+  const double pp1 = (g - 1) * (qc1[4] - rhotke1 - (qc1[1] * qc1[1] + qc1[2] * qc1[2] + qc1[3] * qc1[3]) / 2 / qc1[0]);
+  const double pp2 = (g - 1) * (qc2[4] - rhotke2 - (qc2[1] * qc2[1] + qc2[2] * qc2[2] + qc2[3] * qc2[3]) / 2 / qc2[0]);
+  const double pl = (3 * pp1 - pp2) / 2;
+  const double pr = (B.pout3 * (sqrt(rhol) + sqrt(rhor)) - pl * sqrt(rhol)) / sqrt(rhor);
+  const double pm1 = 3 * B.pout1 - 2 * pr;
+  b[4] = pm1 / (g - 1) + (b[1] * b[1] + b[2] * b[2] + b[3] * b[3]) / 2 / b[0] + rhotkem1;
+  for (int v = 1; v < npde; ++v)
+    if (v != 4) { a[v] = a[v] / a[0]; b[v] = b[v] / b[0]; }
+  const double tk1 = kom ? a[5] : 0.0, tk2 = kom ? b[5] : 0.0;
+  {
+    const double r1 = a[0], u1 = a[1], v1 = a[2], w1 = a[3], e1 = a[4];
+    a[4] = (g - 1) * (e1 - r1 * (u1 * u1 + v1 * v1 + w1 * w1) / 2 - r1 * tk1);
+  }
+  {
+    const double r2 = b[0], u2 = b[1], v2 = b[2], w2 = b[3], e2 = b[4];
+    b[4] = (g - 1) * (e2 - r2 * (u2 * u2 + v2 * v2 + w2 * w2) / 2 - r2 * tk2);
+  }
+  for (int v = 0; v < npde; ++v) { h1[v] = a[v]; h2[v] = b[v]; }
+  return 3;
+}
+// bc_far0 (src/bc.f90:124-483): Riemann-invariant far field, aircraft free
+// stream; s = face normal times sgnm
+__device__ __forceinline__ int bc_far0(const BcPar &B, double sx, double sy, double sz, const double *c1,
+                                       double *h1, double *h2) {
+  const double g = B.g;
+  const double qext = c1[1] * sx + c1[2] * sy + c1[3] * sz;
+  const double qinf = B.qfst[1] * sx + B.qfst[2] * sy + B.qfst[3] * sz;
+  const double rhoext = c1[0], pext = c1[4];
+  const double aext = sqrt(g * pext / rhoext);
+  const double rext = qext + 2 * aext / (g - 1);
+  const double rinf = qinf - 2 * B.ainf / (g - 1);
+  const double qdotn = (rext + rinf) / 2;
+  const double a = (g - 1) * (rext - rinf) / 4;
+  const double mach = qdotn / a;
+  const double sext = pext / pow(rhoext, g);
+  int mask = 0;
+  if (qdotn <= 0.0) {
+    if (fabs(mach) >= 1.0) {
+      for (int v = 0; v < 5; ++v) h1[v] = B.qfst[v];
+    } else {
+      const double rhobc = pow(a * a / (g * B.sinf), 1.0 / (g - 1));
+      const double p = rhobc * a * a / g;
+      h1[0] = rhobc;
+      h1[1] = B.qfst[1] + (qdotn - qinf) * sx;
+      h1[2] = B.qfst[2] + (qdotn - qinf) * sy;
+      h1[3] = B.qfst[3] + (qdotn - qinf) * sz;
+      h1[4] = p;
+    }
+    mask = 3;
+    if (B.npde > 5) { h1[5] = B.tkefar; h1[6] = B.omefar; }
+  } else if (qdotn > 0.0) {
+    if (fabs(mach) >= 1.0) {
+      for (int v = 0; v < 5; ++v) h1[v] = c1[v];
+    } else {
+      const double rhobc = pow(a * a / (g * sext), 1.0 / (g - 1));
+      const double p = rhobc * a * a / g;
+      h1[0] = rhobc;
+      h1[1] = c1[1] + (qdotn - qext) * sx;
+      h1[2] = c1[2] + (qdotn - qext) * sy;
+      h1[3] = c1[3] + (qdotn - qext) * sz;
+      h1[4] = p;
+    }
+    mask = 3;
+    if (B.npde > 5) { h1[5] = c1[5]; h1[6] = c1[6]; }
+  }
+  for (int v = 0; v < B.npde; ++v) h2[v] = h1[v];
+  return mask;
+}
+
+__device__ __forceinline__ bool strong_bc(int t) {
+  return t == 13 || t == 14 || t / 100 == 15 || t == 22 || t == 23 || t == 92 || t == 93 || t == 5;
+}

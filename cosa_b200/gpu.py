@@ -1,0 +1,300 @@
+"""ctypes binding of libcosa_gpu.so (include/cosa_gpu.h) and a small host driver.
+
+This is the Python mirror of the Fortran side of the boundary: the same
+entry points a Fortran ``interface ... bind(C)`` block would declare, called
+with device pointers to arrays in COSA's layout.  There is no CPU fallback:
+if the CUDA library or a GPU is missing, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import build as _build
+from .params import CosaParams
+from .tables import LevelTables
+
+_lib = None
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+ERR = {0x001: "NEG_P", 0x002: "NEG_RHO", 0x004: "INFLOW", 0x008: "NAN", 0x010: "ARG", 0x020: "CUDA",
+       0x040: "TIMEOUT", 0x080: "UNSUPPORTED"}
+
+
+class CosaError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        names = [v for k, v in ERR.items() if code & k]
+        super().__init__(f"{what}: status 0x{code:x} ({'|'.join(names) or '?'})")
+        self.code = code
+
+
+class LevelDesc(C.Structure):
+    _fields_ = [("nblocks", C.c_int32), ("dims", _ip), ("nbcs", _ip), ("bctopo", _ip),
+                ("ncuts", C.c_int32), ("cutopo", _ip)]
+
+
+class LevelPtrs(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in (
+        "q", "qold", "res", "rhs", "dtvol", "dtvolt", "si", "sj", "sk", "vol",
+        "qp", "qm", "dq", "dqp", "dqm", "flux", "betaxi", "betaeta", "betazeta",
+        "mut", "dist", "xdot", "ydot", "zdot")]
+
+
+# public symbols of include/cosa_gpu.h
+SYMBOLS = [
+    "cosa_gpu_params_size", "cosa_gpu_init", "cosa_gpu_finalize", "cosa_gpu_set_params",
+    "cosa_gpu_level_sizes", "cosa_gpu_malloc", "cosa_gpu_memcpy_h2d", "cosa_gpu_memcpy_d2h",
+    "cosa_gpu_synchronize", "cosa_gpu_bind_level", "cosa_gpu_cons2prim", "cosa_gpu_prim2cons",
+    "cosa_gpu_bc", "cosa_gpu_cutman_q", "cosa_gpu_prtest", "cosa_gpu_lambda", "cosa_gpu_deltat",
+    "cosa_gpu_muscl", "cosa_gpu_roflux", "cosa_gpu_resid", "cosa_gpu_update", "cosa_gpu_resg_rms",
+    "cosa_gpu_zero", "cosa_gpu_smooth", "cosa_gpu_smooth_host", "cosa_gpu_launch_count",
+    "cosa_gpu_status", "cosa_gpu_imetrix", "cosa_gpu_vols", "cosa_gpu_profile", "cosa_gpu_stream",
+]
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True):
+    """Load libcosa_gpu.so (building it in-tree first if needed)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise OSError(f"{path} missing: run cosa_b200.build.build()")
+        _build.build()
+    L = C.CDLL(path)
+    L.cosa_gpu_params_size.restype = C.c_int64
+    L.cosa_gpu_launch_count.restype = C.c_int64
+    L.cosa_gpu_stream.restype = C.c_void_p
+    L.cosa_gpu_init.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]
+    for name in SYMBOLS:
+        if name not in ("cosa_gpu_params_size", "cosa_gpu_launch_count", "cosa_gpu_stream"):
+            getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def _ptr(x) -> C.c_void_p:
+    return C.c_void_p(int(x)) if x is not None else C.c_void_p(0)
+
+
+class DevArray:
+    """A device float64 array owned by a Context."""
+
+    def __init__(self, ctx: "Context", n: int):
+        self.ctx = ctx
+        self.n = int(n)
+        p = C.c_void_p()
+        ctx._check(load().cosa_gpu_malloc(ctx.h, C.c_int64(self.n), C.byref(p)), "cosa_gpu_malloc")
+        self.ptr = p.value
+
+    def upload(self, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.size == self.n, (a.size, self.n)
+        self.ctx._check(load().cosa_gpu_memcpy_h2d(self.ctx.h, _ptr(self.ptr), a.ctypes.data_as(C.c_void_p),
+                                                   C.c_int64(self.n)), "h2d")
+        self.ctx.sync()
+        return self
+
+    def download(self) -> np.ndarray:
+        out = np.empty(self.n)
+        self.ctx._check(load().cosa_gpu_memcpy_d2h(self.ctx.h, out.ctypes.data_as(C.c_void_p), _ptr(self.ptr),
+                                                   C.c_int64(self.n)), "d2h")
+        return out
+
+
+class Context:
+    """cosa_ctx: module state of one solve on one GPU."""
+
+    def __init__(self, levels: Sequence[LevelTables], params: CosaParams, device: int = 0):
+        L = load()
+        if L.cosa_gpu_params_size() != C.sizeof(CosaParams):
+            raise RuntimeError("cosa_params ABI mismatch between Python and libcosa_gpu.so")
+        self.params = params
+        self.levels = list(levels)
+        self._keep = []
+        descs = (LevelDesc * len(self.levels))()
+        for i, t in enumerate(self.levels):
+            arrs = [np.ascontiguousarray(t.dims.ravel(), dtype=np.int32),
+                    np.ascontiguousarray(t.nbcs, dtype=np.int32),
+                    np.ascontiguousarray(t.bctopo.ravel(), dtype=np.int32),
+                    np.ascontiguousarray(t.cutopo.ravel(), dtype=np.int32)]
+            self._keep.append(arrs)
+            ip = lambda a: a.ctypes.data_as(_ip)
+            descs[i] = LevelDesc(t.nblocks, ip(arrs[0]), ip(arrs[1]), ip(arrs[2]), t.ncuts, ip(arrs[3]))
+        h = C.c_void_p()
+        self.h = None
+        self._check(L.cosa_gpu_init(C.byref(params), len(self.levels), descs, device, C.byref(h)), "cosa_gpu_init")
+        self.h = h
+        self.S = 2 * params.nharms + 1
+
+    def _check(self, st: int, what: str):
+        if st != 0:
+            raise CosaError(st, what)
+
+    def close(self):
+        if self.h is not None:
+            load().cosa_gpu_finalize(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        self._check(load().cosa_gpu_synchronize(self.h), "sync")
+
+    def sizes(self, nl: int = 1):
+        s = (C.c_int64 * 5)()
+        self._check(load().cosa_gpu_level_sizes(self.h, nl, s), "level_sizes")
+        return list(s)
+
+    def set_params(self, p: CosaParams):
+        self._check(load().cosa_gpu_set_params(self.h, C.byref(p)), "set_params")
+        self.params = p
+
+    def alloc_p3(self, nl=1, nvar=None):
+        n3 = self.sizes(nl)[0]
+        return DevArray(self, n3 * (nvar or self.params.npde) * self.S)
+
+    def alloc_p2(self, nl=1, ncomp=4):
+        return DevArray(self, self.sizes(nl)[1] * ncomp)
+
+    def alloc_p1(self, nl=1, nsnap=1):
+        return DevArray(self, self.sizes(nl)[2] * nsnap)
+
+    def alloc_f0(self, nl=1):
+        return DevArray(self, self.sizes(nl)[3] * self.params.npde * self.S)
+
+    def status(self, reset: bool = False) -> int:
+        return load().cosa_gpu_status(self.h, 1 if reset else 0)
+
+    def launch_count(self, reset: bool = False) -> int:
+        return int(load().cosa_gpu_launch_count(self.h, 1 if reset else 0))
+
+    # ---- level drivers -------------------------------------------------------
+    def cons2prim(self, nl, q, xtnd=0):
+        self._check(load().cosa_gpu_cons2prim(self.h, nl, xtnd, _ptr(q.ptr)), "cons2prim")
+
+    def prim2cons(self, nl, q):
+        self._check(load().cosa_gpu_prim2cons(self.h, nl, _ptr(q.ptr)), "prim2cons")
+
+    def bc(self, nl, q, si, sj, sk):
+        self._check(load().cosa_gpu_bc(self.h, nl, _ptr(q.ptr), _ptr(si.ptr), _ptr(sj.ptr), _ptr(sk.ptr),
+                                       _ptr(None)), "bc")
+
+    def cutman_q(self, nl, q):
+        self._check(load().cosa_gpu_cutman_q(self.h, nl, _ptr(q.ptr)), "cutman_q")
+
+    def prtest(self, nl, q) -> int:
+        return load().cosa_gpu_prtest(self.h, nl, _ptr(q.ptr))
+
+    def lambda_(self, nl, q, si, sj, sk, vol, lam):
+        self._check(load().cosa_gpu_lambda(self.h, nl, _ptr(q.ptr), _ptr(si.ptr), _ptr(sj.ptr), _ptr(sk.ptr),
+                                           _ptr(vol.ptr if vol else None), _ptr(lam.ptr)), "lambda")
+
+    def deltat(self, nl, dtvol, lam, bx=None, by=None, bz=None):
+        self._check(load().cosa_gpu_deltat(self.h, nl, _ptr(dtvol.ptr), _ptr(lam.ptr),
+                                           _ptr(bx.ptr if bx else None), _ptr(by.ptr if by else None),
+                                           _ptr(bz.ptr if bz else None)), "deltat")
+
+    def muscl(self, idir, nl, q, qp, qm, dq, dqp, dqm):
+        self._check(load().cosa_gpu_muscl(self.h, idir, nl, _ptr(q.ptr), _ptr(qp.ptr), _ptr(qm.ptr), _ptr(dq.ptr),
+                                          _ptr(dqp.ptr), _ptr(dqm.ptr)), "muscl")
+
+    def roflux(self, idir, nl, qr, ql, flux, sijk):
+        self._check(load().cosa_gpu_roflux(self.h, idir, nl, _ptr(qr.ptr), _ptr(ql.ptr), _ptr(flux.ptr),
+                                           _ptr(sijk.ptr)), "roflux")
+
+    def resid(self, idir, nl, flux, res):
+        self._check(load().cosa_gpu_resid(self.h, idir, nl, _ptr(flux.ptr), _ptr(res.ptr)), "resid")
+
+    def update(self, nl, res, q, qold, dtvol, ar):
+        self._check(load().cosa_gpu_update(self.h, nl, _ptr(res.ptr), _ptr(q.ptr), _ptr(qold.ptr), _ptr(dtvol.ptr),
+                                           C.c_double(ar)), "update")
+
+    def zero(self, nl, a):
+        self._check(load().cosa_gpu_zero(self.h, nl, _ptr(a.ptr)), "zero")
+
+    def resg_rms(self, nl, res, rhs=None):
+        out = np.zeros(self.params.npde + 1)
+        self._check(load().cosa_gpu_resg_rms(self.h, nl, _ptr(res.ptr), _ptr(rhs.ptr if rhs else None),
+                                             out.ctypes.data_as(_dp)), "resg_rms")
+        return out
+
+    def imetrix(self, nl, x, y, z, si, sj, sk):
+        self._check(load().cosa_gpu_imetrix(self.h, nl, _ptr(x.ptr), _ptr(y.ptr), _ptr(z.ptr), _ptr(si.ptr),
+                                            _ptr(sj.ptr), _ptr(sk.ptr)), "imetrix")
+
+    def vols(self, nl, x, y, z, vol):
+        self._check(load().cosa_gpu_vols(self.h, nl, _ptr(x.ptr), _ptr(y.ptr), _ptr(z.ptr), _ptr(vol.ptr)), "vols")
+
+    def profile(self, nl, niter):
+        ms = (C.c_double * 3)()
+        cnt = (C.c_int64 * 3)()
+        self._check(load().cosa_gpu_profile(self.h, nl, niter, ms, cnt), "profile")
+        return list(ms), list(cnt)
+
+    def stream(self) -> int:
+        return int(load().cosa_gpu_stream(self.h) or 0)
+
+    def bind_level(self, nl, **arrays):
+        p = LevelPtrs()
+        for k, v in arrays.items():
+            setattr(p, k, v.ptr if v is not None else None)
+        self._check(load().cosa_gpu_bind_level(self.h, nl, C.byref(p)), "bind_level")
+
+    def smooth(self, nl, niter, mgit0=1, rms_every=1, want_hist=True):
+        hist = np.full((max(niter, 1), self.params.npde + 1), np.nan) if want_hist else None
+        st = load().cosa_gpu_smooth(self.h, nl, niter, mgit0, rms_every,
+                                    hist.ctypes.data_as(_dp) if want_hist else _dp())
+        return (hist[:niter] if want_hist else None), st
+
+    def smooth_host(self, nl, q_host: np.ndarray, niter, mgit0=1, rms_every=1, want_hist=True):
+        hist = np.full((max(niter, 1), self.params.npde + 1), np.nan) if want_hist else None
+        st = load().cosa_gpu_smooth_host(self.h, nl, q_host.ctypes.data_as(_dp), niter, mgit0, rms_every,
+                                         hist.ctypes.data_as(_dp) if want_hist else _dp())
+        return (hist[:niter] if want_hist else None), st
+
+
+class Solver:
+    """Single-level explicit RK solve on one GPU (mg() with nlevel = 1):
+    device-resident state, metrics uploaded once, smooth() iterations fused."""
+
+    def __init__(self, tables: LevelTables, params: CosaParams, si: np.ndarray, sj: np.ndarray, sk: np.ndarray,
+                 vol: Optional[np.ndarray], q0: np.ndarray, device: int = 0):
+        self.ctx = Context([tables], params, device)
+        c = self.ctx
+        self.q = c.alloc_p3().upload(q0)
+        self.qold = c.alloc_p3()
+        self.dtvol = c.alloc_p1(nsnap=c.S)
+        self.si = c.alloc_p2().upload(si)
+        self.sj = c.alloc_p2().upload(sj)
+        self.sk = c.alloc_p2().upload(sk)
+        self.vol = c.alloc_p1().upload(vol) if vol is not None else None
+        c.bind_level(1, q=self.q, qold=self.qold, dtvol=self.dtvol, si=self.si, sj=self.sj, sk=self.sk,
+                     vol=self.vol)
+        self.mgit = 1
+
+    def run(self, ncycles: int, rms_every: int = 1):
+        hist, st = self.ctx.smooth(1, ncycles, self.mgit, rms_every)
+        if st:
+            raise CosaError(st, "cosa_gpu_smooth")
+        self.mgit += ncycles
+        return hist
+
+    def state(self) -> np.ndarray:
+        return self.q.download()
+
+    def close(self):
+        self.ctx.close()

@@ -1,0 +1,126 @@
+"""cosa_params: the module globals of COSA's hot path as a ctypes struct.
+
+Mirrors ``struct cosa_params`` in ``include/cosa_gpu.h`` field for field.
+Defaults follow ``input()`` (src/input.f90:2400-2540): RK coefficients
+``ar4 = (0.25, 0.333333, 0.5, 1.0)`` (the literal 0.333333, read as FP64
+because every build uses -fdefault-real-8), k-omega constants, qmin, and the
+boundary values the reference hard-wires in bc_insub / bc_outsub
+(src/bc.f90:996-1000, 1310-1312).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+MAX_SNAP = 15
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+
+class CosaParams(C.Structure):
+    _fields_ = [
+        ("gamma", C.c_double), ("machfs", C.c_double), ("alpha", C.c_double),
+        ("beta", C.c_double), ("reyno", C.c_double), ("pranl", C.c_double),
+        ("prant", C.c_double), ("stemp", C.c_double),
+        ("pinf", C.c_double), ("rhoinf", C.c_double), ("ainf", C.c_double),
+        ("tinf", C.c_double),
+        ("rkap", C.c_double), ("epslimf", C.c_double), ("epslimt", C.c_double),
+        ("ilimf", C.c_int32), ("ilimt", C.c_int32),
+        ("nl_crs", C.c_int32), ("foturb", C.c_int32),
+        ("efx_setup_f", C.c_int32), ("efx_all_f", C.c_int32),
+        ("eig_limit_f", C.c_int32), ("eig_lim_all_f", C.c_int32),
+        ("efx_setup_t", C.c_int32), ("efx_all_t", C.c_int32),
+        ("eig_limit_t", C.c_int32), ("eig_lim_all_t", C.c_int32),
+        ("entfx_f_w", C.c_int32 * 3), ("entfx_t_w", C.c_int32 * 3),
+        ("cntrpy_f", C.c_double), ("entfxctf_f", C.c_double), ("eig_cutoff_f", C.c_double),
+        ("cntrpy_t", C.c_double), ("entfxctf_t", C.c_double), ("eig_cutoff_t", C.c_double),
+        ("cfl", C.c_double), ("cflt", C.c_double), ("cdff", C.c_double),
+        ("rat", C.c_double), ("ratt", C.c_double), ("psirs", C.c_double),
+        ("irsop", C.c_int32), ("cutcirs", C.c_int32), ("iupdt", C.c_int32),
+        ("nstage", C.c_int32),
+        ("alphas", C.c_double * 5),
+        ("npde", C.c_int32), ("nharms", C.c_int32), ("hbmove", C.c_int32),
+        ("lmet", C.c_int32),
+        ("viscous", C.c_int32), ("kom", C.c_int32), ("kom_bsl", C.c_int32),
+        ("kom_sst", C.c_int32), ("harbal", C.c_int32), ("rkimp", C.c_int32),
+        ("moving", C.c_int32),
+        ("aircraft", C.c_int32), ("rgkuns", C.c_int32), ("dualt", C.c_int32),
+        ("nlevel", C.c_int32),
+        ("qmin", C.c_double * 7),
+        ("tkefar", C.c_double), ("omefar", C.c_double), ("mutfar", C.c_double),
+        ("cmu", C.c_double), ("bstrkw", C.c_double), ("gkw", C.c_double),
+        ("bkw", C.c_double), ("sigk", C.c_double), ("sigw", C.c_double),
+        ("epst", C.c_double), ("kappa", C.c_double),
+        ("inlet_t0", C.c_double), ("inlet_p0", C.c_double), ("inlet_dir", C.c_double * 3),
+        ("outlet_p", C.c_double * 3),
+        ("omega", C.c_double),
+        ("dhb", C.c_double * (MAX_SNAP * MAX_SNAP)),
+        ("precision", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+
+def default_params() -> CosaParams:
+    """A CosaParams holding input()'s defaults (src/input.f90:2400-2540)."""
+    p = CosaParams()
+    p.gamma = 1.4
+    p.pranl = 0.72
+    p.prant = 0.9
+    p.stemp = 110.4 / 288.15
+    p.rhoinf = 1.0
+    p.ainf = 1.0
+    p.tinf = 1.0
+    p.pinf = 1.0 / p.gamma
+    p.rkap = 1.0 / 3.0
+    p.epslimf = 1.0e-6
+    p.epslimt = 1.0e-6
+    p.ilimf = 1
+    p.ilimt = 1
+    p.nl_crs = 99
+    p.cfl = 2.0
+    p.cflt = 2.0
+    p.cdff = 1.0
+    p.rat = 1.0
+    p.ratt = 1.0
+    p.iupdt = 1
+    p.nstage = 4
+    for i, a in enumerate((0.25, 0.333333, 0.5, 1.0, 0.0)):
+        p.alphas[i] = a
+    p.npde = 5
+    p.lmet = 4
+    p.aircraft = 1
+    p.nlevel = 1
+    for i, v in enumerate((1.0e-8, 1.0, 1.0, 1.0, 1.0e-8, 1.0e-12, 1.0e-8)):
+        p.qmin[i] = v
+    # k-omega (src/input.f90:2513-2521)
+    p.epst = 1.0e-12
+    p.kappa = 0.41
+    p.cmu = 1.0
+    p.sigk = 0.5
+    p.sigw = 0.5
+    p.bkw = 3.0 / 40.0
+    p.bstrkw = 0.09
+    p.gkw = p.bkw / p.bstrkw - p.sigw * p.kappa ** 2 / math.sqrt(p.bstrkw)
+    # reference hard-wired inlet / outlet values (src/bc.f90:996-1000, 1310-1312)
+    p.inlet_t0 = 1.008
+    p.inlet_p0 = 0.734486515085076
+    p.inlet_dir[0] = 1.0
+    p.inlet_dir[1] = 0.0
+    p.inlet_dir[2] = 0.0
+    for i in range(3):
+        p.outlet_p[i] = 0.714285714285714
+    p.precision = PREC_FP64
+    return p
+
+
+def subsonic_inlet_total_state(gamma: float, mach: float):
+    """T0 and p0 of the subsonic inlet for a free stream at `mach` with the
+    non-dimensionalisation rho=1, p=1/gamma, a=1 (T = gamma p / rho = a^2)."""
+    t0 = 1.0 + 0.5 * (gamma - 1.0) * mach * mach
+    p0 = (1.0 / gamma) * t0 ** (gamma / (gamma - 1.0))
+    return t0, p0
+
+
+def params_bytes(p: CosaParams) -> bytes:
+    return bytes(memoryview(p))

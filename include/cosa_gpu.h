@@ -1,0 +1,228 @@
+/*
+ * cosa_gpu.h -- C-ABI of the B200 (sm_100a) explicit residual-and-update
+ * path of COSA (LANCASTER-CFD/COSA, Fortran 90).
+ *
+ * COSA's hot routines are external Fortran procedures with implicit
+ * interfaces that receive flat real(8) arrays (Cray pointers p_q(nl), ...,
+ * src/cosa_variables.f90:184-211) and read every scalar from module
+ * globals (src/common_variables.f90:11-129).  This header replaces them
+ * one-for-one:
+ *
+ *   - the module globals become the POD struct cosa_params (uploaded once
+ *     per solve) plus per-level block/BC/cut tables (cosa_level_desc);
+ *   - every array argument is a DEVICE pointer to an array with exactly the
+ *     reference's shape and block concatenation (offsets as in setoffs,
+ *     src/input.f90:5502-5585), so the Fortran driver's arrays map 1:1;
+ *   - every entry point returns an int status (0 = ok, COSA_ERR_* bits)
+ *     instead of calling `stop` (src/cosa.f90:985-1000, src/bc.f90:1100-1105).
+ *
+ * Array shapes per block (node counts imax,jmax,kmax of the level; S =
+ * 2*nharms+1 snapshots), all column-major with i fastest:
+ *   P3 arrays (q, qold, res, rhs, qp, qm, dq, dqp, dqm, lambdas):
+ *       (-1:imax+1,-1:jmax+1,-1:kmax+1, npde, 0:S-1)
+ *   P2 metric arrays (si, sj, sk):   (lmet=4, 0:imax+1,0:jmax+1,0:kmax+1, 0:S*hbmove-1... )
+ *   P1 arrays (vol):                 (0:imax,0:jmax,0:kmax)
+ *   P1 x S arrays (dtvol, dtvolt, beta*):  (0:imax,0:jmax,0:kmax, 0:S-1)
+ *   F0 arrays (flux):                (imax,jmax,kmax, npde, 0:S-1)
+ *   Grid (x, y, z):                  (0:imax+1,0:jmax+1,0:kmax+1)
+ */
+#ifndef COSA_GPU_H
+#define COSA_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define COSA_MAX_SNAP 15   /* 2*NH+1 for NH <= 7 */
+#define COSA_MAX_LEVELS 3  /* nlevel <= 3 in mg(), src/cosa.f90:806-930 */
+
+/* status bits (replace the reference's fatal stops) */
+#define COSA_OK              0
+#define COSA_ERR_NEG_P       0x001 /* p <= qmin(5): bprtest, src/cosa.f90:1000-1040 */
+#define COSA_ERR_NEG_RHO     0x002 /* rho <= qmin(1): bprtest */
+#define COSA_ERR_INFLOW      0x004 /* inlet Newton > 10 iterations, src/bc.f90:1100-1105 */
+#define COSA_ERR_NAN         0x008 /* non-finite residual norm */
+#define COSA_ERR_ARG         0x010 /* bad argument / size / level */
+#define COSA_ERR_CUDA        0x020 /* CUDA runtime error */
+#define COSA_ERR_TIMEOUT     0x040 /* a bounded device wait ran out */
+#define COSA_ERR_UNSUPPORTED 0x080 /* option outside the implemented path */
+
+/* precision of the reconstruction / Roe flux (state always FP64) */
+#define COSA_PREC_FP64  0
+#define COSA_PREC_MIXED 1
+
+/*
+ * Physics and scheme parameters: the common_variables module globals the
+ * hot path reads (src/common_variables.f90:19-50), with the defaults of
+ * input() (src/input.f90:2400-2540).  Boolean flags are int32 0/1.
+ */
+typedef struct cosa_params {
+  /* flow */
+  double gamma, machfs, alpha, beta, reyno, pranl, prant, stemp;
+  double pinf, rhoinf, ainf, tinf;
+  /* MUSCL + limiters (src/flux.f90:1221-1810, 3472-3888) */
+  double rkap, epslimf, epslimt;
+  int32_t ilimf, ilimt;
+  int32_t nl_crs;       /* first-order on levels nl >= nl_crs */
+  int32_t foturb;       /* first-order turbulence equations */
+  /* Roe entropy fix / eigenvalue cut-off (src/flux.f90:162-200) */
+  int32_t efx_setup_f, efx_all_f, eig_limit_f, eig_lim_all_f;
+  int32_t efx_setup_t, efx_all_t, eig_limit_t, eig_lim_all_t;
+  int32_t entfx_f_w[3], entfx_t_w[3];
+  double cntrpy_f, entfxctf_f, eig_cutoff_f;
+  double cntrpy_t, entfxctf_t, eig_cutoff_t;
+  /* local time step, IRS (src/cosa.f90:4733-5203, 2035-2443) */
+  double cfl, cflt, cdff, rat, ratt, psirs;
+  int32_t irsop, cutcirs, iupdt, nstage;
+  double alphas[5];     /* RK coefficients: ar4 = (0.25,0.333333,0.5,1.0) */
+  /* equation set / flags */
+  int32_t npde, nharms, hbmove, lmet;
+  int32_t viscous, kom, kom_bsl, kom_sst, harbal, rkimp, moving;
+  int32_t aircraft, rgkuns, dualt, nlevel;
+  double qmin[7];
+  /* k-omega (src/input.f90:2513-2540) */
+  double tkefar, omefar, mutfar, cmu, bstrkw, gkw, bkw, sigk, sigw, epst, kappa;
+  /* boundary values hard-wired in the reference, parameterised here;
+     defaults are the reference literals:
+       inlet  T0=1.008, p0=0.734486515085076, dir=(1,0,0)  (src/bc.f90:996-1000)
+       outlet p=0.714285714285714 in both halo layers and on the face
+                                                          (src/bc.f90:1310-1312) */
+  double inlet_t0, inlet_p0, inlet_dir[3];
+  double outlet_p[3];
+  /* harmonic balance: omega and D (src/input.f90:5206-5284) */
+  double omega;
+  double dhb[COSA_MAX_SNAP * COSA_MAX_SNAP]; /* dhb[n*S + m] = D(n,m) */
+  /* GPU-only knobs */
+  int32_t precision;    /* COSA_PREC_FP64 | COSA_PREC_MIXED */
+  int32_t reserved[7];
+} cosa_params;
+
+/*
+ * One multigrid level of the block table.  dims/nbcs/bctopo/cutopo are the
+ * reference's per-level tables: i_imax/j_jmax/k_kmax (src/input.f90:4426),
+ * bctopo(10,nbcs) (src/input.f90:3839-3872) and cutopo(21,ncuts) with the
+ * cut pairs already doubled (src/input.f90:3903-4000).
+ */
+typedef struct cosa_level_desc {
+  int32_t nblocks;
+  const int32_t *dims;    /* 3*nblocks: imax, jmax, kmax (node counts) */
+  const int32_t *nbcs;    /* nblocks */
+  const int32_t *bctopo;  /* 10 * sum(nbcs), block after block */
+  int32_t ncuts;          /* number of cutopo records (2 per input cut) */
+  const int32_t *cutopo;  /* 21 * ncuts */
+} cosa_level_desc;
+
+/*
+ * Device pointer table of one level: the Cray-pointer bases p_*(nl) that
+ * smooth() binds at its top (src/cosa.f90:1650-1703).
+ */
+typedef struct cosa_level_ptrs {
+  double *q, *qold, *res, *rhs, *dtvol, *dtvolt;
+  double *si, *sj, *sk, *vol;
+  double *qp, *qm, *dq, *dqp, *dqm, *flux;           /* unfused scratch */
+  double *betaxi, *betaeta, *betazeta;               /* IRS coefficients */
+  double *mut, *dist;                                /* RANS */
+  double *xdot, *ydot, *zdot;                        /* moving grids */
+} cosa_level_ptrs;
+
+typedef struct cosa_ctx cosa_ctx;
+
+/* sizeof(cosa_params) as compiled into the library (ABI check) */
+int64_t cosa_gpu_params_size(void);
+
+/* ---- context: replaces the module state set up by input()/alloc() ---- */
+int cosa_gpu_init(const cosa_params *p, int32_t nlevels,
+                  const cosa_level_desc *levels, int32_t device,
+                  cosa_ctx **out);
+int cosa_gpu_finalize(cosa_ctx *ctx);
+int cosa_gpu_set_params(cosa_ctx *ctx, const cosa_params *p);
+/* sizes in doubles of the level's arrays: [P3 cells, P2 cells, P1 cells,
+   F0 cells, interior cells]; a P3 array holds P3*npde*S doubles */
+int cosa_gpu_level_sizes(cosa_ctx *ctx, int32_t nl, int64_t sizes[5]);
+/* cosa_all replacement (src/input.f90:5072-5133): device allocation owned
+   by the context, freed by cosa_gpu_finalize */
+int cosa_gpu_malloc(cosa_ctx *ctx, int64_t ndoubles, double **dptr);
+int cosa_gpu_memcpy_h2d(cosa_ctx *ctx, double *dst, const double *src, int64_t n);
+int cosa_gpu_memcpy_d2h(cosa_ctx *ctx, double *dst, const double *src, int64_t n);
+int cosa_gpu_synchronize(cosa_ctx *ctx);
+int cosa_gpu_bind_level(cosa_ctx *ctx, int32_t nl, const cosa_level_ptrs *ptrs);
+
+/* ---- level drivers: one per reference routine, device arrays ---- */
+/* cons2prim (src/update.f90:2112-2188), xtnd as in the reference */
+int cosa_gpu_cons2prim(cosa_ctx *ctx, int32_t nl, int32_t xtnd, double *q);
+/* prim2cons (src/update.f90:1851-2084) */
+int cosa_gpu_prim2cons(cosa_ctx *ctx, int32_t nl, double *q);
+/* bc (src/bc.f90:2-121): every patch of every block, in table order */
+int cosa_gpu_bc(cosa_ctx *ctx, int32_t nl, double *q, const double *si,
+                const double *sj, const double *sk, const double *dist);
+/* cutman_q (src/bc.f90:1801-1891), in-process branch of cut_q */
+int cosa_gpu_cutman_q(cosa_ctx *ctx, int32_t nl, double *q);
+/* prtest (src/cosa.f90:933-1120): status bits instead of stop */
+int cosa_gpu_prtest(cosa_ctx *ctx, int32_t nl, const double *q);
+/* lambda (src/cosa.f90:1214-1591): lambdas(.,1:3,n) */
+int cosa_gpu_lambda(cosa_ctx *ctx, int32_t nl, const double *q,
+                    const double *si, const double *sj, const double *sk,
+                    const double *vol, double *lambdas);
+/* deltat (src/cosa.f90:4701-5203): dtvol and IRS beta */
+int cosa_gpu_deltat(cosa_ctx *ctx, int32_t nl, double *dtvol,
+                    const double *lambdas, double *betaxi, double *betaeta,
+                    double *betazeta);
+/* muscl (src/flux.f90:1183-1810) */
+int cosa_gpu_muscl(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *q,
+                   double *qp, double *qm, double *dq, double *dqp, double *dqm);
+/* roflux (src/flux.f90:2-387); flux is an F0 array */
+int cosa_gpu_roflux(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *qr,
+                    const double *ql, double *flux, const double *sijk);
+/* resid (src/cosa.f90:1123-1211) */
+int cosa_gpu_resid(cosa_ctx *ctx, int32_t idir, int32_t nl,
+                   const double *flux, double *res);
+/* update (src/update.f90:2-100, 568-762), explicit branch */
+int cosa_gpu_update(cosa_ctx *ctx, int32_t nl, const double *res, double *q,
+                    const double *qold, const double *dtvol, double ar);
+/* resg_rms (src/cosa.f90:4458-4582): resrms[0..npde] */
+int cosa_gpu_resg_rms(cosa_ctx *ctx, int32_t nl, const double *res,
+                      const double *rhs, double *resrms);
+/* zero (src/util.f90) of a P3 array including halo layer `ext` */
+int cosa_gpu_zero(cosa_ctx *ctx, int32_t nl, double *a);
+
+/* imetrix (src/grid.f90:820-1255): face unit normals and areas into si/sj/sk
+   (lmet = 4) from the grid x,y,z; fixed grids */
+int cosa_gpu_imetrix(cosa_ctx *ctx, int32_t nl, const double *x, const double *y,
+                     const double *z, double *si, double *sj, double *sk);
+/* vols (src/grid.f90:2133-2230): cell volumes */
+int cosa_gpu_vols(cosa_ctx *ctx, int32_t nl, const double *x, const double *y,
+                  const double *z, double *vol);
+
+/* ---- fused: what smooth() calls when the GPU path is on ---- */
+/*
+ * One RK iteration sequence of smooth() (src/cosa.f90:1711-2029) on the
+ * level bound with cosa_gpu_bind_level, niter iterations of nstage stages.
+ * For every iteration whose number is listed in want_rms (mgit values;
+ * iteration numbering starts at mgit0), the stage-1 residual RMS is written
+ * to hist[(it-mgit0)*(npde+1) + 0..npde].  The state stays on the device.
+ */
+int cosa_gpu_smooth(cosa_ctx *ctx, int32_t nl, int32_t niter, int32_t mgit0,
+                    int32_t rms_every, double *hist);
+/* same, with the state q passed in HOST memory (copied in and out) */
+int cosa_gpu_smooth_host(cosa_ctx *ctx, int32_t nl, double *q_host,
+                         int32_t niter, int32_t mgit0, int32_t rms_every,
+                         double *hist);
+/* niter fused iterations without graphs, with CUDA events around every
+   kernel: ms[0] = mean halo-kernel time, ms[1] = mean tile-kernel time,
+   ms[2] = mean iteration time; counts = launches timed */
+int cosa_gpu_profile(cosa_ctx *ctx, int32_t nl, int32_t niter, double ms[3],
+                     int64_t counts[3]);
+/* the context's CUDA stream (cudaStream_t), for callers that time with
+   their own events */
+void *cosa_gpu_stream(cosa_ctx *ctx);
+/* number of this library's kernels launched since the last call */
+int64_t cosa_gpu_launch_count(cosa_ctx *ctx, int32_t reset);
+/* latched device status bits (COSA_ERR_*), cleared when reset != 0 */
+int cosa_gpu_status(cosa_ctx *ctx, int32_t reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* COSA_GPU_H */

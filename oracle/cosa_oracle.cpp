@@ -1,0 +1,1246 @@
+// ORACLE -- test infrastructure only.
+//
+// CPU FP64 restatement of COSA's explicit residual-and-update hot path
+// (LANCASTER-CFD/COSA, Fortran 90), used by tests/ as the parity checker
+// and by bench.py's cpu_baseline / --impl reference leg as the timed CPU
+// implementation.  Nothing in the product (cosa_b200/) links or calls it.
+//
+// COSA itself cannot be compiled here (no Fortran compiler; it also needs
+// CGNS, TecIO and LAPACK), so this file restates the reference routines
+// loop for loop, keeping their operation order and parenthesisation so
+// that an FP64 build with -ffp-contract=off reproduces the reference's
+// rounding.  Each function cites the Fortran it follows.  The reference
+// ships no tests, inputs or golden vectors for this path, so the only
+// pins are the known-answer tests in tests/test_oracle_kat.py (Roe
+// consistency, free-stream preservation, conservation, symmetry, limiter
+// hand values) -- "parity unpinned" against a running reference.
+//
+// Array layout is the reference's: column-major, i fastest, per-block
+// arrays concatenated with the setoffs() offsets (src/input.f90:5502-5585).
+
+#include "../include/cosa_gpu.h"
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+struct Level {
+  int nb = 0, npde = 5, S = 1, lmet = 4, dim5h = 1;
+  std::vector<int> im, jm, km, nbcs;
+  std::vector<int64_t> op3, op2, op1, of0, om1, obct;
+  std::vector<int> bct;   // 10 * sum(nbcs)
+  int ncuts = 0;
+  std::vector<int> cut;   // 21 * ncuts
+  int64_t n3 = 0, n2 = 0, n1 = 0, n0 = 0, nm1 = 0;
+};
+
+// cyc / krd tables of input() (src/input.f90:2409-2410), 1-based
+inline int cyc(int idir, int m) {
+  static const int t[3][3] = {{1, 2, 3}, {2, 3, 1}, {3, 1, 2}};
+  return t[idir - 1][m - 1];
+}
+inline int krd(int a, int b) { return a == b ? 1 : 0; }
+
+// ---- per-block views -------------------------------------------------------
+struct B3 {  // (-1:im+1,-1:jm+1,-1:km+1, npde, 0:S-1)
+  double *p; int I, J, K; int64_t P; int npde;
+  B3(double *base, const Level &L, int b)
+      : I(L.im[b] + 3), J(L.jm[b] + 3), K(L.km[b] + 3), npde(L.npde) {
+    P = (int64_t)I * J * K;
+    p = base + L.op3[b] * L.npde * L.S;
+  }
+  inline double &operator()(int i, int j, int k, int v, int n) const {
+    return p[((int64_t)n * npde + (v - 1)) * P + (i + 1) + (int64_t)I * ((j + 1) + (int64_t)J * (k + 1))];
+  }
+};
+struct B3s {  // scalar P3 (-1:im+1,...,0:S-1) (mut, pr)
+  double *p; int I, J, K; int64_t P;
+  B3s(double *base, const Level &L, int b) : I(L.im[b] + 3), J(L.jm[b] + 3), K(L.km[b] + 3) {
+    P = (int64_t)I * J * K;
+    p = base + L.op3[b] * L.S;
+  }
+  inline double &operator()(int i, int j, int k, int n) const {
+    return p[(int64_t)n * P + (i + 1) + (int64_t)I * ((j + 1) + (int64_t)J * (k + 1))];
+  }
+};
+struct B2 {  // (lmet, 0:im+1, 0:jm+1, 0:km+1, 0:dim5h-1)
+  const double *p; int I, J, K, lmet; int64_t P;
+  B2(const double *base, const Level &L, int b)
+      : I(L.im[b] + 2), J(L.jm[b] + 2), K(L.km[b] + 2), lmet(L.lmet) {
+    P = (int64_t)I * J * K;
+    p = base + L.op2[b] * L.lmet * L.dim5h;
+  }
+  inline double operator()(int c, int i, int j, int k, int nh) const {
+    return p[((int64_t)nh * P + i + (int64_t)I * (j + (int64_t)J * k)) * lmet + (c - 1)];
+  }
+};
+struct B2w {  // writable metric view
+  double *p; int I, J, K, lmet; int64_t P;
+  B2w(double *base, const Level &L, int b)
+      : I(L.im[b] + 2), J(L.jm[b] + 2), K(L.km[b] + 2), lmet(L.lmet) {
+    P = (int64_t)I * J * K;
+    p = base + L.op2[b] * L.lmet * L.dim5h;
+  }
+  inline double &operator()(int c, int i, int j, int k, int nh) const {
+    return p[((int64_t)nh * P + i + (int64_t)I * (j + (int64_t)J * k)) * lmet + (c - 1)];
+  }
+};
+struct BG {  // grid (0:im+1, 0:jm+1, 0:km+1)
+  const double *p; int I, J;
+  BG(const double *base, const Level &L, int b) : I(L.im[b] + 2), J(L.jm[b] + 2) {
+    p = base + L.op2[b];
+  }
+  inline double operator()(int i, int j, int k) const {
+    return p[i + (int64_t)I * (j + (int64_t)J * k)];
+  }
+};
+struct B1 {  // (0:im, 0:jm, 0:km [, 0:S-1])
+  double *p; int I, J, K; int64_t P;
+  B1(double *base, const Level &L, int b, int nsnap)
+      : I(L.im[b] + 1), J(L.jm[b] + 1), K(L.km[b] + 1) {
+    P = (int64_t)I * J * K;
+    p = base + L.op1[b] * nsnap;
+  }
+  inline double &operator()(int i, int j, int k, int n = 0) const {
+    return p[(int64_t)n * P + i + (int64_t)I * (j + (int64_t)J * k)];
+  }
+};
+struct B0 {  // flux (im, jm, km, npde, 0:S-1), 1-based
+  double *p; int I, J, K, npde; int64_t P;
+  B0(double *base, const Level &L, int b) : I(L.im[b]), J(L.jm[b]), K(L.km[b]), npde(L.npde) {
+    P = (int64_t)I * J * K;
+    p = base + L.of0[b] * L.npde * L.S;
+  }
+  inline double &operator()(int i, int j, int k, int v, int n) const {
+    return p[((int64_t)n * npde + (v - 1)) * P + (i - 1) + (int64_t)I * ((j - 1) + (int64_t)J * (k - 1))];
+  }
+};
+
+inline bool is_kom(const cosa_params &p) { return p.kom || p.kom_bsl || p.kom_sst; }
+
+// ---- cons2prim_b (src/update.f90:2135-2188) --------------------------------
+void cons2prim_b(const Level &L, int b, double *qa, int xtnd, const cosa_params &P) {
+  B3 q(qa, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  const int is = 1 - xtnd, ie = im - 1 + xtnd, js = 1 - xtnd, je = jm - 1 + xtnd;
+  const int ks = 1 - xtnd, ke = km - 1 + xtnd;
+  const double g = P.gamma;
+  const bool kom = is_kom(P);
+  for (int n = 0; n < L.S; ++n)
+    for (int k = ks; k <= ke; ++k)
+      for (int j = js; j <= je; ++j)
+        for (int i = is; i <= ie; ++i) {
+          double rho = q(i, j, k, 1, n);
+          for (int v = 2; v <= L.npde; ++v)
+            if (v != 5) q(i, j, k, v, n) = q(i, j, k, v, n) / rho;
+          double tke = kom ? q(i, j, k, 6, n) : 0.0;
+          double u = q(i, j, k, 2, n), vv = q(i, j, k, 3, n), w = q(i, j, k, 4, n);
+          double rhoe = q(i, j, k, 5, n);
+          q(i, j, k, 5, n) = (g - 1) * (rhoe - rho * (u * u + vv * vv + w * w) / 2 - rho * tke);
+        }
+}
+
+// ---- prim2cons_b (src/update.f90:1875-2084): interior + face halos ---------
+inline void p2c_cell(B3 &q, int i, int j, int k, int n, int npde, double g, bool kom) {
+  double tke = kom ? q(i, j, k, 6, n) : 0.0;
+  double rho = q(i, j, k, 1, n);
+  for (int v = 2; v <= npde; ++v)
+    if (v != 5) q(i, j, k, v, n) = q(i, j, k, v, n) * rho;
+  double rhou = q(i, j, k, 2, n), rhov = q(i, j, k, 3, n), rhow = q(i, j, k, 4, n);
+  double p = q(i, j, k, 5, n);
+  q(i, j, k, 5, n) = p / (g - 1) + (rhou * rhou + rhov * rhov + rhow * rhow) / 2 / rho + rho * tke;
+}
+void prim2cons_b(const Level &L, int b, double *qa, const cosa_params &P) {
+  B3 q(qa, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  const double g = P.gamma;
+  const bool kom = is_kom(P);
+  for (int n = 0; n < L.S; ++n) {
+    for (int k = 1; k <= km - 1; ++k)
+      for (int j = 1; j <= jm - 1; ++j)
+        for (int i = -1; i <= im + 1; ++i) p2c_cell(q, i, j, k, n, L.npde, g, kom);
+    for (int k = 1; k <= km - 1; ++k)
+      for (int j : {-1, 0, jm, jm + 1})
+        for (int i = 1; i <= im - 1; ++i) p2c_cell(q, i, j, k, n, L.npde, g, kom);
+    for (int k : {-1, 0, km, km + 1})
+      for (int j = 1; j <= jm - 1; ++j)
+        for (int i = 1; i <= im - 1; ++i) p2c_cell(q, i, j, k, n, L.npde, g, kom);
+  }
+}
+
+// ---- boundary conditions (src/bc.f90) --------------------------------------
+struct Patch {
+  int bctyp, idir, inrout, istrt[4], iend[4];  // 1-based index arrays
+  int ijk[4];
+  int ic1, ic2, ic3;
+};
+inline Patch patch_of(const int *t, int im, int jm, int km) {
+  Patch pa;
+  pa.bctyp = t[0]; pa.idir = t[1]; pa.inrout = t[2];
+  pa.istrt[1] = t[3]; pa.iend[1] = t[4];
+  pa.istrt[2] = t[5]; pa.iend[2] = t[6];
+  pa.istrt[3] = t[7]; pa.iend[3] = t[8];
+  pa.ijk[1] = im; pa.ijk[2] = jm; pa.ijk[3] = km;
+  pa.ic1 = cyc(pa.idir, 1); pa.ic2 = cyc(pa.idir, 2); pa.ic3 = cyc(pa.idir, 3);
+  return pa;
+}
+// index (i,j,k) of the point at normal position `nrm` and tangential (i2,i3)
+inline void pidx(const Patch &pa, int nrm, int i2, int i3, int &i, int &j, int &k) {
+  i = nrm * krd(pa.ic1, 1) + i2 * krd(pa.ic2, 1) + i3 * krd(pa.ic3, 1);
+  j = nrm * krd(pa.ic1, 2) + i2 * krd(pa.ic2, 2) + i3 * krd(pa.ic3, 2);
+  k = nrm * krd(pa.ic1, 3) + i2 * krd(pa.ic2, 3) + i3 * krd(pa.ic3, 3);
+}
+
+// bc_sym (src/bc.f90:2595-2710)
+void bc_sym(const Patch &pa, B3 &q, const Level &L) {
+  int ibcpt, ibcpt2, ibcn, ibcn2;
+  if (pa.inrout == 1) { ibcpt = 0; ibcpt2 = -1; ibcn = 1; ibcn2 = 2; }
+  else { ibcpt = pa.ijk[pa.idir]; ibcpt2 = ibcpt + 1; ibcn = ibcpt - 1; ibcn2 = ibcpt - 2; }
+  int isym[8];
+  for (int v = 1; v <= L.npde; ++v) isym[v] = 1;
+  isym[pa.idir + 1] = -1;
+  for (int n = 0; n < L.S; ++n)
+    for (int v = 1; v <= L.npde; ++v)
+      for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+        for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+          int a, bb, c, a2, b2, c2, an, bn, cn, an2, bn2, cn2;
+          pidx(pa, ibcpt, i2, i3, a, bb, c); pidx(pa, ibcpt2, i2, i3, a2, b2, c2);
+          pidx(pa, ibcn, i2, i3, an, bn, cn); pidx(pa, ibcn2, i2, i3, an2, bn2, cn2);
+          q(a, bb, c, v, n) = isym[v] * q(an, bn, cn, v, n);
+          q(a2, b2, c2, v, n) = isym[v] * q(an2, bn2, cn2, v, n);
+        }
+}
+
+// bc_extrapol (src/bc.f90:2494-2592)
+void bc_extrapol(const Patch &pa, B3 &q, const Level &L) {
+  int ibcpt, ibcpt2, ibcn;
+  if (pa.inrout == 1) { ibcpt = 0; ibcpt2 = -1; ibcn = 1; }
+  else { ibcpt = pa.ijk[pa.idir]; ibcpt2 = ibcpt + 1; ibcn = ibcpt - 1; }
+  for (int n = 0; n < L.S; ++n)
+    for (int v = 1; v <= L.npde; ++v)
+      for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+        for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+          int a, bb, c, a2, b2, c2, an, bn, cn;
+          pidx(pa, ibcpt, i2, i3, a, bb, c); pidx(pa, ibcpt2, i2, i3, a2, b2, c2);
+          pidx(pa, ibcn, i2, i3, an, bn, cn);
+          q(a, bb, c, v, n) = q(an, bn, cn, v, n);
+          q(a2, b2, c2, v, n) = q(an, bn, cn, v, n);
+        }
+}
+
+inline void face_normal(const Patch &pa, const B2 &si, const B2 &sj, const B2 &sk, int a,
+                        int bb, int c, int nh, double &nx, double &ny, double &nz) {
+  const B2 &s = pa.idir == 1 ? si : (pa.idir == 2 ? sj : sk);
+  nx = s(1, a, bb, c, nh); ny = s(2, a, bb, c, nh); nz = s(3, a, bb, c, nh);
+}
+
+// bc_walinv_14 (src/bc.f90:1457-1675), fixed grid
+void bc_walinv_14(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
+                  const Level &L, const cosa_params &P) {
+  int ibcpt, ibcpt2, ibcn, ibcn2, ibcm;
+  if (pa.inrout == 1) { ibcpt = 0; ibcpt2 = -1; ibcn = 1; ibcn2 = 2; ibcm = 1; }
+  else { ibcpt = pa.ijk[pa.idir]; ibcpt2 = ibcpt + 1; ibcn = ibcpt - 1; ibcn2 = ibcpt - 2; ibcm = ibcpt; }
+  for (int n = 0; n < L.S; ++n) {
+    const int nh = n * P.hbmove;
+    for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+      for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+        int a, bb, c, a2, b2, c2, an, bn, cn, an2, bn2, cn2, am, bm, cm;
+        pidx(pa, ibcpt, i2, i3, a, bb, c); pidx(pa, ibcpt2, i2, i3, a2, b2, c2);
+        pidx(pa, ibcn, i2, i3, an, bn, cn); pidx(pa, ibcn2, i2, i3, an2, bn2, cn2);
+        pidx(pa, ibcm, i2, i3, am, bm, cm);
+        double nx, ny, nz;
+        face_normal(pa, si, sj, sk, am, bm, cm, nh, nx, ny, nz);
+        double rho1 = q(an, bn, cn, 1, n), u1 = q(an, bn, cn, 2, n), v1 = q(an, bn, cn, 3, n);
+        double w1 = q(an, bn, cn, 4, n), p1 = q(an, bn, cn, 5, n);
+        double rho2 = q(an2, bn2, cn2, 1, n), u2 = q(an2, bn2, cn2, 2, n), v2 = q(an2, bn2, cn2, 3, n);
+        double w2 = q(an2, bn2, cn2, 4, n), p2 = q(an2, bn2, cn2, 5, n);
+        double rhow = (3 * rho1 - rho2) / 2, uw = (3 * u1 - u2) / 2, vw = (3 * v1 - v2) / 2;
+        double ww = (3 * w1 - w2) / 2, pw = (3 * p1 - p2) / 2;
+        double un1 = u1 * nx + v1 * ny + w1 * nz;
+        double un2 = u2 * nx + v2 * ny + w2 * nz;
+        double unw = (3 * un1 - un2) / 2;
+        q(a, bb, c, 1, n) = rhow;
+        q(a, bb, c, 2, n) = uw - unw * nx;
+        q(a, bb, c, 3, n) = vw - unw * ny;
+        q(a, bb, c, 4, n) = ww - unw * nz;
+        q(a, bb, c, 5, n) = pw;
+        for (int v = 1; v <= 5; ++v) q(a2, b2, c2, v, n) = q(a, bb, c, v, n);
+        if (is_kom(P)) {
+          q(a, bb, c, 6, n) = q(an, bn, cn, 6, n);
+          q(a, bb, c, 7, n) = q(an, bn, cn, 7, n);
+          q(a2, b2, c2, 6, n) = q(a, bb, c, 6, n);
+          q(a2, b2, c2, 7, n) = q(a, bb, c, 7, n);
+        }
+      }
+  }
+}
+
+// bc_insub (src/bc.f90:875-1175); total state and direction are parameters
+// whose defaults are the reference's hard-wired values.
+int bc_insub(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
+             const Level &L, const cosa_params &P) {
+  int status = 0;
+  int ibcpt, ibcpt2, ibcn, ibcn2, ibcm;
+  double sgnm;
+  if (pa.inrout == 1) { ibcpt = 0; ibcpt2 = -1; ibcn = 1; ibcn2 = 2; ibcm = 1; sgnm = 1.0; }
+  else { ibcpt = pa.ijk[pa.idir]; ibcpt2 = ibcpt + 1; ibcn = ibcpt - 1; ibcn2 = ibcpt - 2; ibcm = ibcpt; sgnm = -1.0; }
+  const double g = P.gamma;
+  for (int icell = 1; icell <= 2; ++icell)
+    for (int n = 0; n < L.S; ++n) {
+      const int nh = n * P.hbmove;
+      for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+        for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+          int a, bb, c, a2, b2, c2, an, bn, cn, an2, bn2, cn2, am, bm, cm;
+          pidx(pa, ibcpt, i2, i3, a, bb, c); pidx(pa, ibcpt2, i2, i3, a2, b2, c2);
+          pidx(pa, ibcn, i2, i3, an, bn, cn); pidx(pa, ibcn2, i2, i3, an2, bn2, cn2);
+          pidx(pa, ibcm, i2, i3, am, bm, cm);
+          double nx, ny, nz;
+          face_normal(pa, si, sj, sk, am, bm, cm, nh, nx, ny, nz);
+          nx = sgnm * nx; ny = sgnm * ny; nz = sgnm * nz;
+          double rho1 = q(an, bn, cn, 1, n), rho2 = q(an2, bn2, cn2, 1, n);
+          double u1 = q(an, bn, cn, 2, n), u2 = q(an2, bn2, cn2, 2, n);
+          double v1 = q(an, bn, cn, 3, n), v2 = q(an2, bn2, cn2, 3, n);
+          double w1 = q(an, bn, cn, 4, n), w2 = q(an2, bn2, cn2, 4, n);
+          double p1 = q(an, bn, cn, 5, n), p2 = q(an2, bn2, cn2, 5, n);
+          double un1 = u1 * nx + v1 * ny + w1 * nz;
+          double un2 = u2 * nx + v2 * ny + w2 * nz;
+          double rc1 = std::sqrt(g * p1 * rho1);
+          double rc2 = std::sqrt(g * p2 * rho2);
+          double rcun1 = rc1 * un1, rcun2 = rc2 * un2;
+          double p, un, rc, rcun;
+          if (icell == 1) {
+            p = 2 * p1 - p2; un = 2 * un1 - un2; rc = 2 * rc1 - rc2; rcun = 2 * rcun1 - rcun2;
+          } else {
+            p = 3 * p1 - 2 * p2; un = 3 * un1 - 2 * un2; rc = 3 * rc1 - 2 * rc2; rcun = 3 * rcun1 - 2 * rcun2;
+          }
+          double t0 = P.inlet_t0, p0 = P.inlet_p0;
+          double h0inl = 1 / (g - 1) * t0;
+          double sx = P.inlet_dir[0], sy = P.inlet_dir[1], sz = P.inlet_dir[2];
+          double dot = sx * nx + sy * ny + sz * nz;
+          double con1 = 0.5 / (h0inl * (dot * dot));
+          double con2 = 2 * con1 * g / (g - 1);
+          double con3 = p - rcun;
+          double dun = 1.0;
+          int count = 0;
+          while (std::fabs(dun) > 1.0e-10) {
+            count = count + 1;
+            if (count == 10) { status |= COSA_ERR_INFLOW; break; }
+            double par = 1.0 - con1 * (un * un);
+            p = p0 * std::pow(par, g / (g - 1));
+            double f = p - rc * un - con3;
+            double fp = -con2 * un * p / par - rc;
+            dun = -f / fp;
+            un = un + dun;
+          }
+          p = +rc * un + con3;
+          double modv = un / dot;
+          double u = modv * sx, v = modv * sy, w = modv * sz;
+          double rho = g * p / ((g - 1) * (h0inl - 0.5 * (modv * modv)));
+          if (icell == 1) {
+            q(a, bb, c, 1, n) = rho; q(a, bb, c, 2, n) = u; q(a, bb, c, 3, n) = v;
+            q(a, bb, c, 4, n) = w; q(a, bb, c, 5, n) = p;
+          } else {
+            q(a2, b2, c2, 1, n) = rho; q(a2, b2, c2, 2, n) = u; q(a2, b2, c2, 3, n) = v;
+            q(a2, b2, c2, 4, n) = w; q(a2, b2, c2, 5, n) = p;
+          }
+        }
+    }
+  if (is_kom(P))
+    for (int n = 0; n < L.S; ++n)
+      for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+        for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+          int a, bb, c, a2, b2, c2;
+          pidx(pa, ibcpt, i2, i3, a, bb, c); pidx(pa, ibcpt2, i2, i3, a2, b2, c2);
+          q(a, bb, c, 6, n) = P.tkefar; q(a, bb, c, 7, n) = P.omefar;
+          q(a2, b2, c2, 6, n) = q(a, bb, c, 6, n); q(a2, b2, c2, 7, n) = q(a, bb, c, 7, n);
+        }
+  return status;
+}
+
+// bc_outsub (src/bc.f90:1178-1455); pressures are parameters whose defaults
+// are the reference's hard-wired 0.714285714285714.
+void bc_outsub(const Patch &pa, B3 &q, const Level &L, const cosa_params &P) {
+  int ibcpt, ibcpt2, ibcn, ibcn2;
+  if (pa.inrout == 1) { ibcpt = 0; ibcpt2 = -1; ibcn = 1; ibcn2 = 2; }
+  else { ibcpt = pa.ijk[pa.idir]; ibcpt2 = ibcpt + 1; ibcn = ibcpt - 1; ibcn2 = ibcpt - 2; }
+  const double g = P.gamma;
+  const bool kom = is_kom(P);
+  const int npde = L.npde;
+  for (int n = 0; n < L.S; ++n)
+    for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+      for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+        int a, bb, c, a2, b2, c2, an, bn, cn, an2, bn2, cn2;
+        pidx(pa, ibcpt, i2, i3, a, bb, c); pidx(pa, ibcpt2, i2, i3, a2, b2, c2);
+        pidx(pa, ibcn, i2, i3, an, bn, cn); pidx(pa, ibcn2, i2, i3, an2, bn2, cn2);
+        const double pout1 = P.outlet_p[0], pout3 = P.outlet_p[2];
+        double tke[3], pp[3], qc[8][3];
+        tke[1] = kom ? q(an, bn, cn, 6, n) : 0.0;
+        tke[2] = kom ? q(an2, bn2, cn2, 6, n) : 0.0;
+        for (int v = 1; v <= npde; ++v) {
+          if (v == 1) { qc[v][1] = q(an, bn, cn, v, n); qc[v][2] = q(an2, bn2, cn2, v, n); }
+          else if (v == 5) { pp[1] = q(an, bn, cn, v, n); pp[2] = q(an2, bn2, cn2, v, n); }
+          else {
+            qc[v][1] = q(an, bn, cn, v, n) * q(an, bn, cn, 1, n);
+            qc[v][2] = q(an2, bn2, cn2, v, n) * q(an2, bn2, cn2, 1, n);
+          }
+        }
+        for (int ic = 1; ic <= 2; ++ic) {
+          double rho = qc[1][ic], rhou = qc[2][ic], rhov = qc[3][ic], rhow = qc[4][ic];
+          qc[5][ic] = pp[ic] / (g - 1) + (rhou * rhou + rhov * rhov + rhow * rhow) / 2 / rho + rho * tke[ic];
+        }
+        for (int v = 1; v <= npde; ++v)
+          if (v != 5) q(a, bb, c, v, n) = 2 * qc[v][1] - qc[v][2];
+        double rhotke0 = 0.0;
+        if (kom) {
+          q(a, bb, c, 6, n) = std::max(q(a, bb, c, 6, n), q(a, bb, c, 1, n) * P.qmin[5]);
+          q(a, bb, c, 7, n) = std::max(q(a, bb, c, 7, n), q(a, bb, c, 1, n) * P.qmin[6]);
+          rhotke0 = q(a, bb, c, 6, n);
+        }
+        q(a, bb, c, 5, n) = pout1 / (g - 1) +
+                            (q(a, bb, c, 2, n) * q(a, bb, c, 2, n) + q(a, bb, c, 3, n) * q(a, bb, c, 3, n) +
+                             q(a, bb, c, 4, n) * q(a, bb, c, 4, n)) / 2 / q(a, bb, c, 1, n) + rhotke0;
+        for (int v = 1; v <= npde; ++v)
+          if (v != 5) q(a2, b2, c2, v, n) = 3 * qc[v][1] - 2 * qc[v][2];
+        double rhotke2 = 0.0, rhotke1 = 0.0, rhotkem1 = 0.0;
+        if (kom) {
+          q(a2, b2, c2, 6, n) = std::max(q(a2, b2, c2, 6, n), q(a2, b2, c2, 1, n) * P.qmin[5]);
+          q(a2, b2, c2, 7, n) = std::max(q(a2, b2, c2, 7, n), q(a2, b2, c2, 1, n) * P.qmin[6]);
+          rhotke2 = qc[6][2]; rhotke1 = qc[6][1]; rhotkem1 = q(a2, b2, c2, 6, n);
+        }
+        double rhol = (3 * qc[1][1] - qc[1][2]) / 2;
+        double rhor = (3 * q(a, bb, c, 1, n) - q(a2, b2, c2, 1, n)) / 2;
+        double p1 = (g - 1) * (qc[5][1] - rhotke1 -
+                               (qc[2][1] * qc[2][1] + qc[3][1] * qc[3][1] + qc[4][1] * qc[4][1]) / 2 / qc[1][1]);
+        double p2 = (g - 1) * (qc[5][2] - rhotke2 -
+                               (qc[2][2] * qc[2][2] + qc[3][2] * qc[3][2] + qc[4][2] * qc[4][2]) / 2 / qc[1][2]);
+        double pl = (3 * p1 - p2) / 2;
+        double pr = (pout3 * (std::sqrt(rhol) + std::sqrt(rhor)) - pl * std::sqrt(rhol)) / std::sqrt(rhor);
+        double pm1 = 3 * pout1 - 2 * pr;
+        q(a2, b2, c2, 5, n) = pm1 / (g - 1) +
+                              (q(a2, b2, c2, 2, n) * q(a2, b2, c2, 2, n) + q(a2, b2, c2, 3, n) * q(a2, b2, c2, 3, n) +
+                               q(a2, b2, c2, 4, n) * q(a2, b2, c2, 4, n)) / 2 / q(a2, b2, c2, 1, n) + rhotkem1;
+        for (int v = 2; v <= npde; ++v)
+          if (v != 5) {
+            q(a, bb, c, v, n) = q(a, bb, c, v, n) / q(a, bb, c, 1, n);
+            q(a2, b2, c2, v, n) = q(a2, b2, c2, v, n) / q(a2, b2, c2, 1, n);
+          }
+        double tk1 = kom ? q(a, bb, c, 6, n) : 0.0, tk2 = kom ? q(a2, b2, c2, 6, n) : 0.0;
+        double r1 = q(a, bb, c, 1, n), r2 = q(a2, b2, c2, 1, n);
+        double uu1 = q(a, bb, c, 2, n), uu2 = q(a2, b2, c2, 2, n);
+        double vv1 = q(a, bb, c, 3, n), vv2 = q(a2, b2, c2, 3, n);
+        double ww1 = q(a, bb, c, 4, n), ww2 = q(a2, b2, c2, 4, n);
+        double e1 = q(a, bb, c, 5, n), e2 = q(a2, b2, c2, 5, n);
+        q(a, bb, c, 5, n) = (g - 1) * (e1 - r1 * (uu1 * uu1 + vv1 * vv1 + ww1 * ww1) / 2 - r1 * tk1);
+        q(a2, b2, c2, 5, n) = (g - 1) * (e2 - r2 * (uu2 * uu2 + vv2 * vv2 + ww2 * ww2) / 2 - r2 * tk2);
+      }
+}
+
+// bc_far0 (src/bc.f90:124-483), fixed grid, aircraft free stream
+void bc_far0(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
+             const Level &L, const cosa_params &P) {
+  int ibcpt, ibcpt2, ibcn, ibcm;
+  double sgnm;
+  if (pa.inrout == 1) { ibcpt = 0; ibcpt2 = -1; ibcn = 1; ibcm = 1; sgnm = -1.0; }
+  else { ibcpt = pa.ijk[pa.idir]; ibcpt2 = ibcpt + 1; ibcn = ibcpt - 1; ibcm = ibcpt; sgnm = 1.0; }
+  const double g = P.gamma;
+  double qfst[6];
+  qfst[1] = P.rhoinf;
+  qfst[2] = P.machfs * std::cos(P.alpha) * std::cos(P.beta);
+  qfst[3] = P.machfs * std::sin(P.alpha) * std::cos(P.beta);
+  qfst[4] = P.machfs * std::sin(P.beta);
+  qfst[5] = P.pinf;
+  const double sinf = P.pinf / std::pow(P.rhoinf, g);
+  for (int n = 0; n < L.S; ++n) {
+    const int nh = n * P.hbmove;
+    for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+      for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+        int a, bb, c, a2, b2, c2, an, bn, cn, am, bm, cm;
+        pidx(pa, ibcpt, i2, i3, a, bb, c); pidx(pa, ibcpt2, i2, i3, a2, b2, c2);
+        pidx(pa, ibcn, i2, i3, an, bn, cn); pidx(pa, ibcm, i2, i3, am, bm, cm);
+        double sx, sy, sz;
+        face_normal(pa, si, sj, sk, am, bm, cm, nh, sx, sy, sz);
+        sx = sx * sgnm; sy = sy * sgnm; sz = sz * sgnm;
+        double qext = q(an, bn, cn, 2, n) * sx + q(an, bn, cn, 3, n) * sy + q(an, bn, cn, 4, n) * sz;
+        double qinf = qfst[2] * sx + qfst[3] * sy + qfst[4] * sz;
+        double rhoext = q(an, bn, cn, 1, n), pext = q(an, bn, cn, 5, n);
+        double aext = std::sqrt(g * pext / rhoext);
+        double rext = qext + 2 * aext / (g - 1);
+        double rinf = qinf - 2 * P.ainf / (g - 1);
+        double qdotn = (rext + rinf) / 2;
+        double a_ = (g - 1) * (rext - rinf) / 4;
+        double mach = qdotn / a_;
+        double sext = pext / std::pow(rhoext, g);
+        double out[6];
+        bool set = true;
+        if (qdotn <= 0.0) {
+          if (std::fabs(mach) >= 1.0) {
+            for (int v = 1; v <= 5; ++v) out[v] = qfst[v];
+          } else {
+            double rhobc = std::pow(a_ * a_ / (g * sinf), 1.0 / (g - 1));
+            double p = rhobc * a_ * a_ / g;
+            out[1] = rhobc;
+            out[2] = qfst[2] + (qdotn - qinf) * sx;
+            out[3] = qfst[3] + (qdotn - qinf) * sy;
+            out[4] = qfst[4] + (qdotn - qinf) * sz;
+            out[5] = p;
+          }
+        } else if (qdotn > 0.0) {
+          if (std::fabs(mach) >= 1.0) {
+            for (int v = 1; v <= 5; ++v) out[v] = q(an, bn, cn, v, n);
+          } else {
+            double rhobc = std::pow(a_ * a_ / (g * sext), 1.0 / (g - 1));
+            double p = rhobc * a_ * a_ / g;
+            out[1] = rhobc;
+            out[2] = q(an, bn, cn, 2, n) + (qdotn - qext) * sx;
+            out[3] = q(an, bn, cn, 3, n) + (qdotn - qext) * sy;
+            out[4] = q(an, bn, cn, 4, n) + (qdotn - qext) * sz;
+            out[5] = p;
+          }
+        } else {
+          set = false;  // NaN qdotn: the reference leaves the halo untouched
+        }
+        if (set)
+          for (int v = 1; v <= 5; ++v) { q(a, bb, c, v, n) = out[v]; q(a2, b2, c2, v, n) = out[v]; }
+        if (is_kom(P)) {
+          if (qdotn <= 0.0) {
+            q(a, bb, c, 6, n) = P.tkefar; q(a, bb, c, 7, n) = P.omefar;
+          } else if (qdotn > 0.0) {
+            q(a, bb, c, 6, n) = q(an, bn, cn, 6, n); q(a, bb, c, 7, n) = q(an, bn, cn, 7, n);
+          }
+          q(a2, b2, c2, 6, n) = q(a, bb, c, 6, n); q(a2, b2, c2, 7, n) = q(a, bb, c, 7, n);
+        }
+      }
+  }
+}
+
+// bbc dispatch (src/bc.f90:35-121): patches in table order
+int bc_level(const Level &L, double *qa, const double *si, const double *sj, const double *sk,
+             const cosa_params &P) {
+  int status = 0;
+#pragma omp parallel for reduction(| : status) schedule(dynamic)
+  for (int b = 0; b < L.nb; ++b) {
+    B3 q(qa, L, b);
+    B2 vi(si, L, b), vj(sj, L, b), vk(sk, L, b);
+    const int *t = L.bct.data() + L.obct[b];
+    for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
+      Patch pa = patch_of(t + 10 * ibc, L.im[b], L.jm[b], L.km[b]);
+      switch (pa.bctyp) {
+        case 80: bc_sym(pa, q, L); break;
+        case 4: bc_extrapol(pa, q, L); break;
+        case 30: bc_far0(pa, q, vi, vj, vk, L, P); break;
+        case 14: bc_walinv_14(pa, q, vi, vj, vk, L, P); break;
+        case 21: status |= bc_insub(pa, q, vi, vj, vk, L, P); break;
+        case 91: bc_outsub(pa, q, L, P); break;
+        default:
+          if (pa.bctyp / 100 == 15 || pa.bctyp == 31) status |= COSA_ERR_UNSUPPORTED;
+          break;
+      }
+    }
+  }
+  return status;
+}
+
+// ---- cut_q, in-process branch (src/bc.f90:1894-2141) -----------------------
+void cutman_q_level(const Level &L, double *qa, int nvar_override = 0) {
+  const int nv = nvar_override ? nvar_override : L.npde;
+  for (int icut = 0; icut < L.ncuts; ++icut) {
+    const int *c = L.cut.data() + 21 * icut;
+    const int b1 = c[0] - 1, b2 = c[9] - 1;
+    B3 q1(qa, L, b1), q2(qa, L, b2);
+    int ijk1[4] = {0, L.im[b1], L.jm[b1], L.km[b1]};
+    int ijk2[4] = {0, L.im[b2], L.jm[b2], L.km[b2]};
+    int idir1 = c[1], inout1 = c[2], idir2 = c[10], inout2 = c[11];
+    int istr1[4] = {0, c[3], c[5], c[7]}, iend1[4] = {0, c[4], c[6], c[8]};
+    int istr2[4] = {0, c[12], c[14], c[16]}, iend2[4] = {0, c[13], c[15], c[17]};
+    int iord[4] = {0, c[18], c[19], c[20]};
+    (void)idir2;
+    int ibcpt, ibcinc, inr, inrinc;
+    if (inout1 == 1) { ibcpt = 0; ibcinc = -1; } else { ibcpt = ijk1[idir1]; ibcinc = 1; }
+    if (inout2 == 1) { inr = 1; inrinc = 1; } else { inr = ijk2[idir2] - 1; inrinc = -1; }
+    int len[4], isgn1[4], isgn2[4];
+    for (int l = 1; l <= 3; ++l) {
+      len[l] = std::abs(iend1[l] - istr1[l]);
+      isgn1[l] = iend1[l] > istr1[l] ? 1 : -1;
+      isgn2[l] = iend2[l] > istr2[l] ? 1 : -1;
+    }
+    int ic1 = cyc(idir1, 1), ic2 = cyc(idir1, 2), ic3 = cyc(idir1, 3);
+    int jc1 = iord[ic1], jc2 = iord[ic2], jc3 = iord[ic3];
+    for (int i3 = 0; i3 <= len[ic3]; ++i3)
+      for (int i2 = 0; i2 <= len[ic2]; ++i2) {
+        int a2_ = istr1[ic2] + isgn1[ic2] * i2, a3_ = istr1[ic3] + isgn1[ic3] * i3;
+        int ii1 = ibcpt * krd(ic1, 1) + a2_ * krd(ic2, 1) + a3_ * krd(ic3, 1);
+        int jj1 = ibcpt * krd(ic1, 2) + a2_ * krd(ic2, 2) + a3_ * krd(ic3, 2);
+        int kk1 = ibcpt * krd(ic1, 3) + a2_ * krd(ic2, 3) + a3_ * krd(ic3, 3);
+        int ii2 = ii1 + ibcinc * krd(ic1, 1), jj2 = jj1 + ibcinc * krd(ic1, 2), kk2 = kk1 + ibcinc * krd(ic1, 3);
+        int b2_ = istr2[jc2] + isgn2[jc2] * i2, b3_ = istr2[jc3] + isgn2[jc3] * i3;
+        int in1 = inr * krd(jc1, 1) + b2_ * krd(jc2, 1) + b3_ * krd(jc3, 1);
+        int jn1 = inr * krd(jc1, 2) + b2_ * krd(jc2, 2) + b3_ * krd(jc3, 2);
+        int kn1 = inr * krd(jc1, 3) + b2_ * krd(jc2, 3) + b3_ * krd(jc3, 3);
+        int in2 = in1 + inrinc * krd(jc1, 1), jn2 = jn1 + inrinc * krd(jc1, 2), kn2 = kn1 + inrinc * krd(jc1, 3);
+        for (int n = 0; n < L.S; ++n)
+          for (int v = 1; v <= nv; ++v) {
+            q1(ii1, jj1, kk1, v, n) = q2(in1, jn1, kn1, v, n);
+            q1(ii2, jj2, kk2, v, n) = q2(in2, jn2, kn2, v, n);
+          }
+      }
+  }
+}
+
+// ---- prtest (src/cosa.f90:960-1120) -----------------------------------------
+int prtest_level(const Level &L, const double *qa, const cosa_params &P) {
+  int status = 0;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 q(const_cast<double *>(qa), L, b);
+    for (int n = 0; n < L.S; ++n)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = -1; i <= L.im[b] + 1; ++i) {
+            double rho = q(i, j, k, 1, n), pr = q(i, j, k, 5, n);
+            if (pr <= P.qmin[4]) status |= COSA_ERR_NEG_P;
+            else if (rho <= P.qmin[0]) status |= COSA_ERR_NEG_RHO;
+          }
+  }
+  return status;
+}
+
+// ---- lambdab + eig_eul (src/cosa.f90:1248-1330, 4183-4233), inviscid -------
+void lambda_level(const Level &L, const double *qa, const double *si, const double *sj,
+                  const double *sk, double *lam, const cosa_params &P) {
+  for (int b = 0; b < L.nb; ++b) {
+    B3 q(const_cast<double *>(qa), L, b), lm(lam, L, b);
+    B2 vi(si, L, b), vj(sj, L, b), vk(sk, L, b);
+    const double g = P.gamma;
+    for (int n = 0; n < L.S; ++n) {
+      const int nh = n * P.hbmove;
+#pragma omp parallel for schedule(static)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            double rho = q(i, j, k, 1, n), u = q(i, j, k, 2, n), v = q(i, j, k, 3, n);
+            double w = q(i, j, k, 4, n), p = q(i, j, k, 5, n);
+            double a = std::sqrt(g * p / rho);
+            double sim[5], sip[5], sjm[5], sjp[5], skm[5], skp[5];
+            for (int c = 1; c <= 4; ++c) {
+              sim[c] = vi(c, i, j, k, nh); sip[c] = vi(c, i + 1, j, k, nh);
+              sjm[c] = vj(c, i, j, k, nh); sjp[c] = vj(c, i, j + 1, k, nh);
+              skm[c] = vk(c, i, j, k, nh); skp[c] = vk(c, i, j, k + 1, nh);
+            }
+            double xix = 0.5 * (sim[1] * sim[4] + sip[1] * sip[4]);
+            double xiy = 0.5 * (sim[2] * sim[4] + sip[2] * sip[4]);
+            double xiz = 0.5 * (sim[3] * sim[4] + sip[3] * sip[4]);
+            double etax = 0.5 * (sjm[1] * sjm[4] + sjp[1] * sjp[4]);
+            double etay = 0.5 * (sjm[2] * sjm[4] + sjp[2] * sjp[4]);
+            double etaz = 0.5 * (sjm[3] * sjm[4] + sjp[3] * sjp[4]);
+            double zetax = 0.5 * (skm[1] * skm[4] + skp[1] * skp[4]);
+            double zetay = 0.5 * (skm[2] * skm[4] + skp[2] * skp[4]);
+            double zetaz = 0.5 * (skm[3] * skm[4] + skp[3] * skp[4]);
+            double axi = (sim[4] + sip[4]) / 2;
+            double aeta = (sjm[4] + sjp[4]) / 2;
+            double azeta = (skm[4] + skp[4]) / 2;
+            lm(i, j, k, 1, n) = std::fabs(u * xix + v * xiy + w * xiz) + a * axi;
+            lm(i, j, k, 2, n) = std::fabs(u * etax + v * etay + w * etaz) + a * aeta;
+            lm(i, j, k, 3, n) = std::fabs(u * zetax + v * zetay + w * zetaz) + a * azeta;
+          }
+    }
+  }
+}
+
+// ---- bdeltat (src/cosa.f90:4733-5203), inviscid, no CFL ramping ------------
+void deltat_level(const Level &L, double *dtv, const double *lam, double *bx_, double *by_,
+                  double *bz_, const cosa_params &P) {
+  const double zeta = 0.4, c1 = 40.0;
+  (void)c1;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 lm(const_cast<double *>(lam), L, b);
+    B1 dt(dtv, L, b, L.S);
+    for (int n = 0; n < L.S; ++n)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i)
+            dt(i, j, k, n) = P.cfl / (lm(i, j, k, 1, n) + lm(i, j, k, 2, n) + lm(i, j, k, 3, n));
+    if (P.irsop == 0 || !bx_) continue;
+    B1 bx(bx_, L, b, L.S), by(by_, L, b, L.S), bz(bz_, L, b, L.S);
+    const double rat = P.rat, psirs = P.psirs;
+    for (int n = 0; n < L.S; ++n)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            double lami = lm(i, j, k, 1, n), lamj = lm(i, j, k, 2, n), lamk = lm(i, j, k, 3, n);
+            if (P.irsop == 2) {
+              double phixi = 1 + std::pow(lamj / lami, zeta) + std::pow(lamk / lami, zeta);
+              double phieta = 1 + std::pow(lami / lamj, zeta) + std::pow(lamk / lamj, zeta);
+              double phizeta = 1 + std::pow(lami / lamk, zeta) + std::pow(lamj / lamk, zeta);
+              double t;
+              t = (rat * lami * phixi / (lami + lamj + lamk));
+              bx(i, j, k, n) = std::max(0.0, (t * t - 1) / 4);
+              t = (rat * lamj * phieta / (lami + lamj + lamk));
+              by(i, j, k, n) = std::max(0.0, (t * t - 1) / 4);
+              t = (rat * lamk * phizeta / (lami + lamj + lamk));
+              bz(i, j, k, n) = std::max(0.0, (t * t - 1) / 4);
+            } else if (P.irsop == 3) {
+              double rji = lamj / lami, rki = lamk / lami, rij = lami / lamj;
+              double rkj = lamk / lamj, rik = lami / lamk, rjk = lamj / lamk;
+              double t;
+              t = rat / (1 + psirs * (rji + rki));
+              bx(i, j, k, n) = std::max(0.0, 0.25 * (t * t - 1));
+              t = rat / (1 + psirs * (rij + rkj));
+              by(i, j, k, n) = std::max(0.0, 0.25 * (t * t - 1));
+              t = rat / (1 + psirs * (rik + rjk));
+              bz(i, j, k, n) = std::max(0.0, 0.25 * (t * t - 1));
+            }
+          }
+  }
+}
+
+// ---- limiters limit_i/j/k (src/flux.f90:3472-3888) -------------------------
+// The three directions are the same loops with the stencil along `d`; the
+// helpers below take the line accessor dq(., m) = dq at offset m along d.
+struct Line {
+  B3 *a; int d;
+  inline double &at(int i, int j, int k, int m, int v, int n) const {
+    return d == 1 ? (*a)(i + m, j, k, v, n) : (d == 2 ? (*a)(i, j + m, k, v, n) : (*a)(i, j, k + m, v, n));
+  }
+};
+
+void limit_dir(B3 &dq, B3 &dqp, B3 &dqm, int d, double epslim, double rkap, int vs, int ve,
+               int ilim, int im, int jm, int km, int S) {
+  // loop ranges per direction: along d, faces 1..max (ilim 0/1) or 0..max (2..4)
+  Line Lq{&dq, d}, Lp{&dqp, d}, Lm{&dqm, d};
+  int lo[4] = {0, 1, 1, 1}, hi[4] = {0, im - 1, jm - 1, km - 1};
+  const int nmax = d == 1 ? im : (d == 2 ? jm : km);
+  for (int n = 0; n < S; ++n)
+    for (int v = vs; v <= ve; ++v) {
+      int l0[4], h0[4];
+      for (int e = 1; e <= 3; ++e) { l0[e] = lo[e]; h0[e] = hi[e]; }
+      l0[d] = (ilim <= 1) ? 1 : 0;
+      h0[d] = nmax;
+      for (int k = l0[3]; k <= h0[3]; ++k)
+        for (int j = l0[2]; j <= h0[2]; ++j)
+          for (int i = l0[1]; i <= h0[1]; ++i) {
+            if (ilim == 0) {
+              double rkp = 1 + rkap, rkm = 1 - rkap;
+              Lp.at(i, j, k, 0, v, n) = -(rkp * Lq.at(i, j, k, 0, v, n) + rkm * Lq.at(i, j, k, 1, v, n)) / 4;
+              Lm.at(i, j, k, 0, v, n) = (rkm * Lq.at(i, j, k, -1, v, n) + rkp * Lq.at(i, j, k, 0, v, n)) / 4;
+            } else if (ilim == 1) {
+              double d0 = Lq.at(i, j, k, 0, v, n), dp1 = Lq.at(i, j, k, 1, v, n), dm1 = Lq.at(i, j, k, -1, v, n);
+              double s = (2 * dp1 * d0 + epslim) / (dp1 * dp1 + d0 * d0 + epslim);
+              double rkp = 1 + rkap * s, rkm = 1 - rkap * s;
+              Lp.at(i, j, k, 0, v, n) = -s * (rkp * d0 + rkm * dp1) / 4;
+              s = (2 * d0 * dm1 + epslim) / (d0 * d0 + dm1 * dm1 + epslim);
+              rkp = 1 + rkap * s; rkm = 1 - rkap * s;
+              Lm.at(i, j, k, 0, v, n) = s * (rkm * dm1 + rkp * d0) / 4;
+            } else if (ilim == 2) {
+              double rkp = 1 + rkap, rkm = 1 - rkap;
+              double bb = (3.0 - rkap) / (1.0 - rkap);
+              double d0 = Lq.at(i, j, k, 0, v, n), d1 = Lq.at(i, j, k, 1, v, n);
+              double dqmx = (std::copysign(1.0, d0) + std::copysign(1.0, d1)) / 2 *
+                            std::min(std::fabs(d0), std::fabs(d1) * bb);
+              double dqpx = (std::copysign(1.0, d1) + std::copysign(1.0, d0)) / 2 *
+                            std::min(std::fabs(d1), std::fabs(d0) * bb);
+              Lp.at(i, j, k, 0, v, n) = -(rkp * dqmx + rkm * dqpx) / 4;
+              Lm.at(i, j, k, 1, v, n) = (rkm * dqmx + rkp * dqpx) / 4;
+            } else if (ilim == 3) {
+              double epsq = epslim * epslim;
+              double d1 = Lq.at(i, j, k, 1, v, n), d2 = Lq.at(i, j, k, 0, v, n);
+              double dqmx = (d1 * (d2 * d2 + 2 * epsq) + d2 * (2 * (d1 * d1) + epsq)) /
+                            (2 * (d1 * d1) - d1 * d2 + 2 * (d2 * d2) + 3 * epsq);
+              double dqpx = (d2 * (d1 * d1 + 2 * epsq) + d1 * (2 * (d2 * d2) + epsq)) /
+                            (2 * (d2 * d2) - d2 * d1 + 2 * (d1 * d1) + 3 * epsq);
+              Lp.at(i, j, k, 0, v, n) = -dqpx / 2;
+              Lm.at(i, j, k, 1, v, n) = dqmx / 2;
+            } else if (ilim == 4) {
+              double epsq = epslim * epslim;
+              double d1 = Lq.at(i, j, k, 1, v, n), d2 = Lq.at(i, j, k, 0, v, n);
+              double dqmx = (d1 * (d2 * d2 + epsq) + d2 * (d1 * d1 + epsq)) / (d1 * d1 + d2 * d2 + 2 * epsq);
+              double dqpx = dqmx;
+              Lp.at(i, j, k, 0, v, n) = -dqpx / 2;
+              Lm.at(i, j, k, 1, v, n) = dqmx / 2;
+            }
+          }
+    }
+}
+
+inline bool strong_bc(int t) {
+  return t == 13 || t == 14 || t / 100 == 15 || t == 22 || t == 23 || t == 92 || t == 93 || t == 5;
+}
+
+// ---- muscl_bi/bj/bk (src/flux.f90:1221-1810) ------------------------------
+void muscl_b(const Level &L, int b, int d, int nl, double *qa, double *qpa, double *qma,
+             double *dqa, double *dqpa, double *dqma, const cosa_params &P) {
+  B3 q(qa, L, b), qp(qpa, L, b), qm(qma, L, b), dq(dqa, L, b), dqp(dqpa, L, b), dqm(dqma, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b], npde = L.npde, S = L.S;
+  int fo_beg = 0, fo_end = -1, so_beg = 1, so_end = npde;
+  bool dofirst = false, doscnd = true;
+  if (nl >= P.nl_crs) { fo_beg = 1; fo_end = npde; so_beg = 0; so_end = -1; dofirst = true; doscnd = false; }
+  else if (P.foturb) { fo_beg = 6; fo_end = npde; so_beg = 1; so_end = 5; dofirst = true; doscnd = true; }
+  // face ranges: along d 1..max, others 1..max-1
+  int flo[4] = {0, 1, 1, 1}, fhi[4] = {0, im - 1, jm - 1, km - 1};
+  fhi[d] = d == 1 ? im : (d == 2 ? jm : km);
+  auto off = [&](int e) { return e == d ? 1 : 0; };
+  if (dofirst)
+    for (int n = 0; n < S; ++n)
+      for (int v = fo_beg; v <= fo_end; ++v)
+        for (int k = flo[3]; k <= fhi[3]; ++k)
+          for (int j = flo[2]; j <= fhi[2]; ++j)
+            for (int i = flo[1]; i <= fhi[1]; ++i) {
+              qp(i, j, k, v, n) = q(i, j, k, v, n);
+              qm(i, j, k, v, n) = q(i - off(1), j - off(2), k - off(3), v, n);
+            }
+  const int *t = L.bct.data() + L.obct[b];
+  if (doscnd) {
+    int dlo[4] = {0, 1, 1, 1}, dhi[4] = {0, im - 1, jm - 1, km - 1};
+    dlo[d] = 0;
+    dhi[d] = (d == 1 ? im : (d == 2 ? jm : km)) + 1;
+    for (int n = 0; n < S; ++n)
+      for (int v = so_beg; v <= so_end; ++v)
+        for (int k = dlo[3]; k <= dhi[3]; ++k)
+          for (int j = dlo[2]; j <= dhi[2]; ++j)
+            for (int i = dlo[1]; i <= dhi[1]; ++i)
+              dq(i, j, k, v, n) = q(i, j, k, v, n) - q(i - off(1), j - off(2), k - off(3), v, n);
+    for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
+      const int *r = t + 10 * ibc;
+      if (r[1] != d || !strong_bc(r[0])) continue;
+      int bcpt = r[2] == 1 ? 1 : (d == 1 ? im : (d == 2 ? jm : km));
+      int s[4] = {0, r[3], r[5], r[7]}, e[4] = {0, r[4], r[6], r[8]};
+      s[d] = e[d] = bcpt;
+      for (int n = 0; n < S; ++n)
+        for (int v = so_beg; v <= so_end; ++v)
+          for (int k = s[3]; k <= e[3]; ++k)
+            for (int j = s[2]; j <= e[2]; ++j)
+              for (int i = s[1]; i <= e[1]; ++i)
+                dq(i, j, k, v, n) = (q(i, j, k, v, n) - q(i - off(1), j - off(2), k - off(3), v, n)) * 2;
+    }
+    limit_dir(dq, dqp, dqm, d, P.epslimf, P.rkap, 1, 5, P.ilimf, im, jm, km, S);
+    limit_dir(dq, dqp, dqm, d, P.epslimt, P.rkap, 6, npde, P.ilimt, im, jm, km, S);
+    for (int n = 0; n < S; ++n)
+      for (int v = so_beg; v <= so_end; ++v)
+        for (int k = flo[3]; k <= fhi[3]; ++k)
+          for (int j = flo[2]; j <= fhi[2]; ++j)
+            for (int i = flo[1]; i <= fhi[1]; ++i) {
+              qp(i, j, k, v, n) = q(i, j, k, v, n) + dqp(i, j, k, v, n);
+              qm(i, j, k, v, n) = q(i - off(1), j - off(2), k - off(3), v, n) + dqm(i, j, k, v, n);
+            }
+  }
+  for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
+    const int *r = t + 10 * ibc;
+    if (r[1] != d || !strong_bc(r[0])) continue;
+    const int mx = d == 1 ? im : (d == 2 ? jm : km);
+    int qpm = r[2] == 1 ? 1 : mx, bcpt = r[2] == 1 ? 0 : mx;
+    int s[4] = {0, r[3], r[5], r[7]}, e[4] = {0, r[4], r[6], r[8]};
+    s[d] = e[d] = 0;
+    for (int n = 0; n < S; ++n)
+      for (int v = 1; v <= npde; ++v)
+        for (int k = s[3]; k <= e[3]; ++k)
+          for (int j = s[2]; j <= e[2]; ++j)
+            for (int i = s[1]; i <= e[1]; ++i) {
+              int a = i, bb = j, c = k, a2 = i, b2 = j, c2 = k;
+              if (d == 1) { a = qpm; a2 = bcpt; } else if (d == 2) { bb = qpm; b2 = bcpt; } else { c = qpm; c2 = bcpt; }
+              qp(a, bb, c, v, n) = q(a2, b2, c2, v, n);
+              qm(a, bb, c, v, n) = q(a2, b2, c2, v, n);
+            }
+  }
+}
+
+// ---- roflux_b mean-flow part (src/flux.f90:45-238) --------------------------
+struct RoeOut { double f[6]; };
+inline void roe_face(const cosa_params &P, double kx, double ky, double kz, double ds, double ubn,
+                     const double *qr, const double *ql, double tker, double tkel, double *flux) {
+  const double g = P.gamma;
+  double rhor = qr[1], ur = qr[2], vr = qr[3], wr = qr[4], pr = qr[5];
+  double unr = ur * kx + vr * ky + wr * kz - ubn;
+  double q2r = ur * ur + vr * vr + wr * wr;
+  double h0r = g / (g - 1) * pr / rhor + q2r / 2 + tker;
+  double rh0r = rhor * h0r;
+  double fr[6], fl[6], df[6];
+  fr[1] = rhor * unr;
+  fr[2] = (rhor * ur * unr + pr * kx);
+  fr[3] = (rhor * vr * unr + pr * ky);
+  fr[4] = (rhor * wr * unr + pr * kz);
+  fr[5] = (rh0r * unr + pr * ubn);
+  double rhol = ql[1], ul = ql[2], vl = ql[3], wl = ql[4], pl = ql[5];
+  double unl = ul * kx + vl * ky + wl * kz - ubn;
+  double q2l = ul * ul + vl * vl + wl * wl;
+  double h0l = g / (g - 1) * pl / rhol + q2l / 2 + tkel;
+  double rh0l = rhol * h0l;
+  fl[1] = rhol * unl;
+  fl[2] = (rhol * ul * unl + pl * kx);
+  fl[3] = (rhol * vl * unl + pl * ky);
+  fl[4] = (rhol * wl * unl + pl * kz);
+  fl[5] = (rh0l * unl + pl * ubn);
+  double drho = rhor - rhol, dp = pr - pl, du = ur - ul, dv = vr - vl, dw = wr - wl;
+  double dun = unr - unl, dtke = tker - tkel;
+  double rhols = std::sqrt(rhol), rhors = std::sqrt(rhor);
+  double rho = rhols * rhors, denom = rhols + rhors;
+  double u = (rhols * ul + rhors * ur) / denom;
+  double v = (rhols * vl + rhors * vr) / denom;
+  double w = (rhols * wl + rhors * wr) / denom;
+  double un = u * kx + v * ky + w * kz;
+  double h0 = (rhols * h0l + rhors * h0r) / denom;
+  double tke = (rhols * tkel + rhors * tker) / denom;
+  double q2 = u * u + v * v + w * w;
+  double a2 = (g - 1) * (h0 - q2 / 2 - tke);
+  double a = std::sqrt(a2);
+  double rm123 = std::fabs(un - ubn), rm4 = std::fabs(un + a - ubn), rm5 = std::fabs(un - a - ubn);
+  if (P.efx_setup_f) {
+    double rdelta = P.cntrpy_f * (P.entfx_f_w[0] * P.entfxctf_f +
+                                  P.entfx_f_w[1] * (std::sqrt(u * u + v * v + w * w) + a) +
+                                  P.entfx_f_w[2] * 0.2 * (std::fabs(un) + a + std::fabs(ubn)));
+    rdelta = std::max(rdelta, 1.0e-12);
+    if (rm123 <= rdelta && P.efx_all_f) rm123 = 0.5 * (rm123 * rm123 + rdelta * rdelta) / rdelta;
+    if (rm4 <= rdelta) rm4 = 0.5 * (rm4 * rm4 + rdelta * rdelta) / rdelta;
+    if (rm5 <= rdelta) rm5 = 0.5 * (rm5 * rm5 + rdelta * rdelta) / rdelta;
+  }
+  if (P.eig_limit_f) {
+    if (rm123 <= P.eig_cutoff_f) rm123 = P.eig_cutoff_f;
+    if (P.eig_lim_all_f && rm4 <= P.eig_cutoff_f) rm4 = P.eig_cutoff_f;
+    if (P.eig_lim_all_f && rm5 <= P.eig_cutoff_f) rm5 = P.eig_cutoff_f;
+  }
+  double al1 = rm123 * (drho - dp / a2);
+  double al2 = rm123 * rho;
+  double al3 = rm4 * (dp / a2 + rho * dun / a) / 2;
+  double al4 = rm5 * (dp / a2 - rho * dun / a) / 2;
+  df[1] = al1 + al3 + al4;
+  df[2] = al1 * u + al2 * (du - dun * kx) + al3 * (u + a * kx) + al4 * (u - a * kx);
+  df[3] = al1 * v + al2 * (dv - dun * ky) + al3 * (v + a * ky) + al4 * (v - a * ky);
+  df[4] = al1 * w + al2 * (dw - dun * kz) + al3 * (w + a * kz) + al4 * (w - a * kz);
+  df[5] = al1 * (q2 / 2 + tke) + al2 * (u * du + v * dv + w * dw - un * dun + dtke) +
+          al3 * (h0 + a * un) + al4 * (h0 - a * un);
+  for (int m = 1; m <= 5; ++m) flux[m] = (fr[m] + fl[m] - df[m]) / 2 * ds;
+}
+
+void roflux_b(const Level &L, int b, int d, double *qra, double *qla, double *fa, const double *sijk,
+              const cosa_params &P) {
+  B3 qr(qra, L, b), ql(qla, L, b);
+  B0 flux(fa, L, b);
+  B2 s(sijk, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  int ic = d == 1 ? im : im - 1, jc = d == 2 ? jm : jm - 1, kc = d == 3 ? km : km - 1;
+  const bool kom = is_kom(P);
+  for (int n = 0; n < L.S; ++n) {
+    const int nh = n * P.hbmove;
+#pragma omp parallel for schedule(static)
+    for (int k = 1; k <= kc; ++k)
+      for (int j = 1; j <= jc; ++j)
+        for (int i = 1; i <= ic; ++i) {
+          double kx = s(1, i, j, k, nh), ky = s(2, i, j, k, nh), kz = s(3, i, j, k, nh), ds = s(4, i, j, k, nh);
+          double vr[6], vl[6], f[6];
+          for (int v = 1; v <= 5; ++v) { vr[v] = qr(i, j, k, v, n); vl[v] = ql(i, j, k, v, n); }
+          double tker = kom ? qr(i, j, k, 6, n) : 0.0, tkel = kom ? ql(i, j, k, 6, n) : 0.0;
+          roe_face(P, kx, ky, kz, ds, 0.0, vr, vl, tker, tkel, f);
+          for (int v = 1; v <= 5; ++v) flux(i, j, k, v, n) = f[v];
+        }
+  }
+}
+
+// ---- bresid (src/cosa.f90:1149-1211) ----------------------------------------
+void resid_b(const Level &L, int b, int d, double *fa, double *ra) {
+  B0 flux(fa, L, b);
+  B3 res(ra, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  const int oi = d == 1, oj = d == 2, ok = d == 3;
+  for (int n = 0; n < L.S; ++n)
+    for (int v = 1; v <= L.npde; ++v)
+      for (int k = 1; k <= km - 1; ++k)
+        for (int j = 1; j <= jm - 1; ++j)
+          for (int i = 1; i <= im - 1; ++i)
+            res(i, j, k, v, n) = res(i, j, k, v, n) + flux(i + oi, j + oj, k + ok, v, n) - flux(i, j, k, v, n);
+}
+
+// ---- update_b explicit, non-k-omega (src/update.f90:568-640) ---------------
+void update_b(const Level &L, int b, double *ra, double *qa, double *qoa, double *dta, double ar) {
+  B3 res(ra, L, b), q(qa, L, b), qold(qoa, L, b);
+  B1 dt(dta, L, b, L.S);
+  for (int n = 0; n < L.S; ++n)
+    for (int v = 1; v <= 5; ++v)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i)
+            q(i, j, k, v, n) = qold(i, j, k, v, n) - ar * res(i, j, k, v, n) * dt(i, j, k, n);
+}
+
+// ---- resg_brms (src/cosa.f90:4503-4582), explicit steady branch ------------
+void resg_rms_level(const Level &L, double *ra, double *rha, double *out) {
+  double acc[8] = {0};
+  int64_t ncell = 0;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 res(ra, L, b), rhs(rha, L, b);
+    double rb[8] = {0};
+    for (int v = 1; v <= L.npde; ++v)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            double t = res(i, j, k, v, 0) - rhs(i, j, k, v, 0);
+            rb[v] = rb[v] + t * t;
+          }
+    for (int v = 1; v <= L.npde; ++v) rb[L.npde + 1] = rb[L.npde + 1] + rb[v];
+    for (int v = 1; v <= L.npde + 1; ++v) acc[v] = acc[v] + rb[v];
+    ncell += (int64_t)(L.im[b] - 1) * (L.jm[b] - 1) * (L.km[b] - 1);
+  }
+  for (int v = 1; v <= L.npde; ++v) out[v - 1] = std::sqrt(acc[v] / ncell);
+  out[L.npde] = std::sqrt(acc[L.npde + 1] / ncell / L.npde);
+}
+
+void zero_res(const Level &L, double *ra) {
+  for (int b = 0; b < L.nb; ++b) {
+    B3 r(ra, L, b);
+    for (int n = 0; n < L.S; ++n)
+      for (int v = 1; v <= L.npde; ++v)
+        for (int k = 0; k <= L.km[b]; ++k)
+          for (int j = 0; j <= L.jm[b]; ++j)
+            for (int i = 0; i <= L.im[b]; ++i) r(i, j, k, v, n) = 0.0;
+  }
+}
+
+void copy_interior(const Level &L, double *dst, const double *src) {
+  for (int b = 0; b < L.nb; ++b) {
+    B3 d(dst, L, b), s(const_cast<double *>(src), L, b);
+    for (int n = 0; n < L.S; ++n)
+      for (int v = 1; v <= L.npde; ++v)
+        for (int k = 1; k <= L.km[b] - 1; ++k)
+          for (int j = 1; j <= L.jm[b] - 1; ++j)
+            for (int i = 1; i <= L.im[b] - 1; ++i) d(i, j, k, v, n) = s(i, j, k, v, n);
+  }
+}
+
+// ---- imetrix_b / bvols (src/grid.f90:847-1010, 2160-2230), fixed grid -------
+void imetrix_b(const Level &L, int b, const double *xa, const double *ya, const double *za,
+               double *sia, double *sja, double *ska) {
+  BG x(xa, L, b), y(ya, L, b), z(za, L, b);
+  B2w si(sia, L, b), sj(sja, L, b), sk(ska, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  const int n = 0;
+  for (int k = 1; k <= km - 1; ++k)
+    for (int j = 1; j <= jm - 1; ++j)
+      for (int i = 1; i <= im; ++i) {
+        double a1 = ((y(i, j + 1, k + 1) - y(i, j, k)) * (z(i, j, k + 1) - z(i, j + 1, k)) -
+                     (z(i, j + 1, k + 1) - z(i, j, k)) * (y(i, j, k + 1) - y(i, j + 1, k))) / 2;
+        double a2 = ((z(i, j + 1, k + 1) - z(i, j, k)) * (x(i, j, k + 1) - x(i, j + 1, k)) -
+                     (x(i, j + 1, k + 1) - x(i, j, k)) * (z(i, j, k + 1) - z(i, j + 1, k))) / 2;
+        double a3 = ((x(i, j + 1, k + 1) - x(i, j, k)) * (y(i, j, k + 1) - y(i, j + 1, k)) -
+                     (y(i, j + 1, k + 1) - y(i, j, k)) * (x(i, j, k + 1) - x(i, j + 1, k))) / 2;
+        double a4 = std::sqrt(a1 * a1 + a2 * a2 + a3 * a3);
+        si(1, i, j, k, n) = a1 / a4; si(2, i, j, k, n) = a2 / a4; si(3, i, j, k, n) = a3 / a4; si(4, i, j, k, n) = a4;
+      }
+  for (int k = 1; k <= km - 1; ++k)
+    for (int i = 1; i <= im - 1; ++i)
+      for (int j = 1; j <= jm; ++j) {
+        double a1 = ((z(i + 1, j, k + 1) - z(i, j, k)) * (y(i, j, k + 1) - y(i + 1, j, k)) -
+                     (y(i + 1, j, k + 1) - y(i, j, k)) * (z(i, j, k + 1) - z(i + 1, j, k))) / 2;
+        double a2 = ((x(i + 1, j, k + 1) - x(i, j, k)) * (z(i, j, k + 1) - z(i + 1, j, k)) -
+                     (z(i + 1, j, k + 1) - z(i, j, k)) * (x(i, j, k + 1) - x(i + 1, j, k))) / 2;
+        double a3 = ((y(i + 1, j, k + 1) - y(i, j, k)) * (x(i, j, k + 1) - x(i + 1, j, k)) -
+                     (x(i + 1, j, k + 1) - x(i, j, k)) * (y(i, j, k + 1) - y(i + 1, j, k))) / 2;
+        double a4 = std::sqrt(a1 * a1 + a2 * a2 + a3 * a3);
+        sj(1, i, j, k, n) = a1 / a4; sj(2, i, j, k, n) = a2 / a4; sj(3, i, j, k, n) = a3 / a4; sj(4, i, j, k, n) = a4;
+      }
+  for (int j = 1; j <= jm - 1; ++j)
+    for (int i = 1; i <= im - 1; ++i)
+      for (int k = 1; k <= km; ++k) {
+        double a1 = ((y(i + 1, j + 1, k) - y(i, j, k)) * (z(i, j + 1, k) - z(i + 1, j, k)) -
+                     (z(i + 1, j + 1, k) - z(i, j, k)) * (y(i, j + 1, k) - y(i + 1, j, k))) / 2;
+        double a2 = ((z(i + 1, j + 1, k) - z(i, j, k)) * (x(i, j + 1, k) - x(i + 1, j, k)) -
+                     (x(i + 1, j + 1, k) - x(i, j, k)) * (z(i, j + 1, k) - z(i + 1, j, k))) / 2;
+        double a3 = ((x(i + 1, j + 1, k) - x(i, j, k)) * (y(i, j + 1, k) - y(i + 1, j, k)) -
+                     (y(i + 1, j + 1, k) - y(i, j, k)) * (x(i, j + 1, k) - x(i + 1, j, k))) / 2;
+        double a4 = std::sqrt(a1 * a1 + a2 * a2 + a3 * a3);
+        sk(1, i, j, k, n) = a1 / a4; sk(2, i, j, k, n) = a2 / a4; sk(3, i, j, k, n) = a3 / a4; sk(4, i, j, k, n) = a4;
+      }
+}
+
+void bvols(const Level &L, int b, const double *xa, const double *ya, const double *za, double *va) {
+  BG x(xa, L, b), y(ya, L, b), z(za, L, b);
+  B1 vol(va, L, b, 1);
+  for (int k = 1; k <= L.km[b] - 1; ++k)
+    for (int j = 1; j <= L.jm[b] - 1; ++j)
+      for (int i = 1; i <= L.im[b] - 1; ++i) {
+        double si1 = ((y(i, j + 1, k + 1) - y(i, j, k)) * (z(i, j, k + 1) - z(i, j + 1, k)) -
+                      (z(i, j + 1, k + 1) - z(i, j, k)) * (y(i, j, k + 1) - y(i, j + 1, k))) / 2;
+        double sj1 = ((z(i + 1, j, k + 1) - z(i, j, k)) * (y(i, j, k + 1) - y(i + 1, j, k)) -
+                      (y(i + 1, j, k + 1) - y(i, j, k)) * (z(i, j, k + 1) - z(i + 1, j, k))) / 2;
+        double sk1 = ((y(i + 1, j + 1, k) - y(i, j, k)) * (z(i, j + 1, k) - z(i + 1, j, k)) -
+                      (z(i + 1, j + 1, k) - z(i, j, k)) * (y(i, j + 1, k) - y(i + 1, j, k))) / 2;
+        double dx = (si1 + sj1 + sk1) * (x(i + 1, j + 1, k + 1) - x(i, j, k));
+        double si2 = ((z(i, j + 1, k + 1) - z(i, j, k)) * (x(i, j, k + 1) - x(i, j + 1, k)) -
+                      (x(i, j + 1, k + 1) - x(i, j, k)) * (z(i, j, k + 1) - z(i, j + 1, k))) / 2;
+        double sj2 = ((x(i + 1, j, k + 1) - x(i, j, k)) * (z(i, j, k + 1) - z(i + 1, j, k)) -
+                      (z(i + 1, j, k + 1) - z(i, j, k)) * (x(i, j, k + 1) - x(i + 1, j, k))) / 2;
+        double sk2 = ((z(i + 1, j + 1, k) - z(i, j, k)) * (x(i, j + 1, k) - x(i + 1, j, k)) -
+                      (x(i + 1, j + 1, k) - x(i, j, k)) * (z(i, j + 1, k) - z(i + 1, j, k))) / 2;
+        double dy = (si2 + sj2 + sk2) * (y(i + 1, j + 1, k + 1) - y(i, j, k));
+        double si3 = ((x(i, j + 1, k + 1) - x(i, j, k)) * (y(i, j, k + 1) - y(i, j + 1, k)) -
+                      (y(i, j + 1, k + 1) - y(i, j, k)) * (x(i, j, k + 1) - x(i, j + 1, k))) / 2;
+        double sj3 = ((y(i + 1, j, k + 1) - y(i, j, k)) * (x(i, j, k + 1) - x(i + 1, j, k)) -
+                      (x(i + 1, j, k + 1) - x(i, j, k)) * (y(i, j, k + 1) - y(i + 1, j, k))) / 2;
+        double sk3 = ((x(i + 1, j + 1, k) - x(i, j, k)) * (y(i, j + 1, k) - y(i + 1, j, k)) -
+                      (y(i + 1, j + 1, k) - y(i, j, k)) * (x(i, j + 1, k) - x(i + 1, j, k))) / 2;
+        double dz = (si3 + sj3 + sk3) * (z(i + 1, j + 1, k + 1) - z(i, j, k));
+        vol(i, j, k) = (dx + dy + dz) / 3;
+      }
+}
+
+}  // namespace
+
+// ============================================================================
+// extern "C" surface used by tests/ (ctypes)
+// ============================================================================
+struct orc_level { Level L; };
+
+extern "C" {
+
+orc_level *orc_level_new(const cosa_level_desc *d, int npde, int nharms) {
+  auto *h = new orc_level;
+  Level &L = h->L;
+  L.nb = d->nblocks; L.npde = npde; L.S = 2 * nharms + 1; L.lmet = 4; L.dim5h = 1;
+  int64_t a3 = 0, a2 = 0, a1 = 0, a0 = 0, am = 0, ab = 0;
+  for (int b = 0; b < L.nb; ++b) {
+    int im = d->dims[3 * b], jm = d->dims[3 * b + 1], km = d->dims[3 * b + 2];
+    L.im.push_back(im); L.jm.push_back(jm); L.km.push_back(km);
+    L.nbcs.push_back(d->nbcs[b]);
+    L.op3.push_back(a3); L.op2.push_back(a2); L.op1.push_back(a1);
+    L.of0.push_back(a0); L.om1.push_back(am); L.obct.push_back(ab);
+    a3 += (int64_t)(im + 3) * (jm + 3) * (km + 3);
+    a2 += (int64_t)(im + 2) * (jm + 2) * (km + 2);
+    a1 += (int64_t)(im + 1) * (jm + 1) * (km + 1);
+    a0 += (int64_t)im * jm * km;
+    am += (int64_t)(im - 1) * (jm - 1) * (km - 1);
+    ab += 10 * d->nbcs[b];
+  }
+  L.n3 = a3; L.n2 = a2; L.n1 = a1; L.n0 = a0; L.nm1 = am;
+  L.bct.assign(d->bctopo, d->bctopo + ab);
+  L.ncuts = d->ncuts;
+  L.cut.assign(d->cutopo, d->cutopo + 21 * d->ncuts);
+  return h;
+}
+void orc_level_free(orc_level *h) { delete h; }
+void orc_level_sizes(orc_level *h, int64_t *s) {
+  s[0] = h->L.n3; s[1] = h->L.n2; s[2] = h->L.n1; s[3] = h->L.n0; s[4] = h->L.nm1;
+}
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+void orc_imetrix(orc_level *h, const double *x, const double *y, const double *z, double *si,
+                 double *sj, double *sk) {
+  for (int b = 0; b < h->L.nb; ++b) imetrix_b(h->L, b, x, y, z, si, sj, sk);
+}
+void orc_vols(orc_level *h, const double *x, const double *y, const double *z, double *vol) {
+  for (int b = 0; b < h->L.nb; ++b) bvols(h->L, b, x, y, z, vol);
+}
+void orc_cons2prim(orc_level *h, const cosa_params *p, int xtnd, double *q) {
+  for (int b = 0; b < h->L.nb; ++b) cons2prim_b(h->L, b, q, xtnd, *p);
+}
+void orc_prim2cons(orc_level *h, const cosa_params *p, double *q) {
+  for (int b = 0; b < h->L.nb; ++b) prim2cons_b(h->L, b, q, *p);
+}
+int orc_bc(orc_level *h, const cosa_params *p, double *q, const double *si, const double *sj,
+           const double *sk) {
+  return bc_level(h->L, q, si, sj, sk, *p);
+}
+void orc_cutman_q(orc_level *h, double *q) { cutman_q_level(h->L, q); }
+int orc_prtest(orc_level *h, const cosa_params *p, const double *q) { return prtest_level(h->L, q, *p); }
+void orc_lambda(orc_level *h, const cosa_params *p, const double *q, const double *si,
+                const double *sj, const double *sk, double *lam) {
+  lambda_level(h->L, q, si, sj, sk, lam, *p);
+}
+void orc_deltat(orc_level *h, const cosa_params *p, double *dtvol, const double *lam, double *bx,
+                double *by, double *bz) {
+  deltat_level(h->L, dtvol, lam, bx, by, bz, *p);
+}
+void orc_muscl(orc_level *h, const cosa_params *p, int idir, int nl, double *q, double *qp,
+               double *qm, double *dq, double *dqp, double *dqm) {
+  for (int b = 0; b < h->L.nb; ++b) muscl_b(h->L, b, idir, nl, q, qp, qm, dq, dqp, dqm, *p);
+}
+void orc_roflux(orc_level *h, const cosa_params *p, int idir, double *qr, double *ql, double *flux,
+                const double *sijk) {
+  for (int b = 0; b < h->L.nb; ++b) roflux_b(h->L, b, idir, qr, ql, flux, sijk, *p);
+}
+void orc_resid(orc_level *h, int idir, double *flux, double *res) {
+  for (int b = 0; b < h->L.nb; ++b) resid_b(h->L, b, idir, flux, res);
+}
+void orc_update(orc_level *h, double *res, double *q, double *qold, double *dtvol, double ar) {
+  for (int b = 0; b < h->L.nb; ++b) update_b(h->L, b, res, q, qold, dtvol, ar);
+}
+void orc_resg_rms(orc_level *h, double *res, double *rhs, double *out) { resg_rms_level(h->L, res, rhs, out); }
+void orc_zero_res(orc_level *h, double *res) { zero_res(h->L, res); }
+void orc_copy_interior(orc_level *h, double *dst, const double *src) { copy_interior(h->L, dst, src); }
+// Roe face flux on single states (for KATs): q = (rho,u,v,w,p) prim
+void orc_roe_face(const cosa_params *p, const double *nrm, const double *qr, const double *ql,
+                  double *f) {
+  double vr[6], vl[6], out[6];
+  for (int m = 0; m < 5; ++m) { vr[m + 1] = qr[m]; vl[m + 1] = ql[m]; }
+  roe_face(*p, nrm[0], nrm[1], nrm[2], nrm[3], 0.0, vr, vl, 0.0, 0.0, out);
+  for (int m = 0; m < 5; ++m) f[m] = out[m + 1];
+}
+
+/*
+ * One residual evaluation as smooth() performs it at stage 1 (src/cosa.f90:
+ * 1721-1908), leaving res (conservative residual), q back in conservative
+ * form, and lambdas/dtvol when want_dt.  Work arrays are caller-owned P3/F0.
+ */
+int orc_residual(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
+                 const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
+                 double *dqp, double *dqm, double *flux, double *dtvol, int want_dt) {
+  Level &L = h->L;
+  for (int b = 0; b < L.nb; ++b) cons2prim_b(L, b, q, 0, *p);
+  int status = bc_level(L, q, si, sj, sk, *p);
+  cutman_q_level(L, q);
+  status |= prtest_level(L, q, *p);
+  if (want_dt) {
+    lambda_level(L, q, si, sj, sk, qp, *p);
+    deltat_level(L, dtvol, qp, nullptr, nullptr, nullptr, *p);
+  }
+  zero_res(L, res);
+  const double *sd[4] = {nullptr, si, sj, sk};
+  for (int d = 1; d <= 3; ++d) {
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < L.nb; ++b) muscl_b(L, b, d, nl, q, qp, qm, dq, dqp, dqm, *p);
+    for (int b = 0; b < L.nb; ++b) roflux_b(L, b, d, qp, qm, flux, sd[d], *p);
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < L.nb; ++b) resid_b(L, b, d, flux, res);
+  }
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < L.nb; ++b) prim2cons_b(L, b, q, *p);
+  return status;
+}
+
+/*
+ * Single-level explicit RK driver: mg() with nlevel=1 calls smooth(1,...,
+ * niter=1) once per cycle (src/cosa.f90:817-840); this runs `ncycles` such
+ * cycles.  hist receives, for cycles with (mgit==1 || mgit%rms_every==0 ||
+ * mgit==last), the stage-1 resrms(1..npde+1) at row (mgit-mgit0).
+ */
+int orc_smooth(orc_level *h, const cosa_params *p, int ncycles, int mgit0, int rms_every, double *q,
+               double *qold, const double *si, const double *sj, const double *sk, double *res,
+               double *rhs, double *qp, double *qm, double *dq, double *dqp, double *dqm, double *flux,
+               double *dtvol, double *hist) {
+  Level &L = h->L;
+  int status = 0;
+  const int last = mgit0 + ncycles - 1;
+  for (int mgit = mgit0; mgit <= last; ++mgit) {
+    const int iter = 1;
+    copy_interior(L, qold, q);
+    for (int irk = 1; irk <= p->nstage; ++irk) {
+      const bool want_dt = (iter / p->iupdt * p->iupdt == iter) && irk == 1;
+      status |= orc_residual(h, p, 1, q, si, sj, sk, res, qp, qm, dq, dqp, dqm, flux, dtvol, want_dt);
+      if (irk == 1 && (mgit == 1 || mgit % rms_every == 0 || mgit == last) && hist) {
+        resg_rms_level(L, res, rhs, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
+      }
+#pragma omp parallel for schedule(dynamic)
+      for (int b = 0; b < L.nb; ++b) update_b(L, b, res, q, qold, dtvol, p->alphas[irk - 1]);
+    }
+  }
+  return status;
+}
+
+}  // extern "C"

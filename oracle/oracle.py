@@ -1,0 +1,184 @@
+"""ORACLE -- test infrastructure only (ctypes wrapper of liboracle_cosa.so).
+
+Used by tests/, by __graft_entry__.smoke() as the checker, and by bench.py's
+cpu_baseline / --impl reference legs.  The product (cosa_b200) never imports
+this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle_cosa.so")
+_lib = None
+
+_dp = C.POINTER(C.c_double)
+
+
+class _LevelDesc(C.Structure):
+    _fields_ = [("nblocks", C.c_int32), ("dims", C.POINTER(C.c_int32)),
+                ("nbcs", C.POINTER(C.c_int32)), ("bctopo", C.POINTER(C.c_int32)),
+                ("ncuts", C.c_int32), ("cutopo", C.POINTER(C.c_int32))]
+
+
+def build(force: bool = False) -> str:
+    if force or not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(os.path.join(_HERE, "cosa_oracle.cpp")):
+        subprocess.run(["make", "-C", _HERE], check=True, stdout=subprocess.DEVNULL)
+    return _LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(_LIB)
+        _lib.orc_level_new.restype = C.c_void_p
+        _lib.orc_level_new.argtypes = [C.POINTER(_LevelDesc), C.c_int, C.c_int]
+        _lib.orc_level_free.argtypes = [C.c_void_p]
+        _lib.orc_level_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def _par(p):
+    return C.byref(p)
+
+
+class OracleLevel:
+    """One level of the oracle with its own copy of the block tables."""
+
+    def __init__(self, tables, params):
+        self.t = tables
+        self.p = params
+        self._keep = [np.ascontiguousarray(tables.dims.ravel(), dtype=np.int32),
+                      np.ascontiguousarray(tables.nbcs, dtype=np.int32),
+                      np.ascontiguousarray(tables.bctopo.ravel(), dtype=np.int32),
+                      np.ascontiguousarray(tables.cutopo.ravel(), dtype=np.int32)]
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        d = _LevelDesc(tables.nblocks, ip(self._keep[0]), ip(self._keep[1]), ip(self._keep[2]),
+                       tables.ncuts, ip(self._keep[3]))
+        self.h = C.c_void_p(lib().orc_level_new(C.byref(d), params.npde, params.nharms))
+        s = (C.c_int64 * 5)()
+        lib().orc_level_sizes(self.h, s)
+        self.n3, self.n2, self.n1, self.n0, self.nm1 = list(s)
+        self.S = 2 * params.nharms + 1
+
+    def __del__(self):
+        try:
+            lib().orc_level_free(self.h)
+        except Exception:
+            pass
+
+    # allocation helpers (zeroed, like cosa_all)
+    def p3(self):
+        return np.zeros(self.n3 * self.p.npde * self.S)
+
+    def p2(self, ncomp=4):
+        return np.zeros(self.n2 * ncomp)
+
+    def p1(self, nsnap=1):
+        return np.zeros(self.n1 * nsnap)
+
+    def f0(self):
+        return np.zeros(self.n0 * self.p.npde * self.S)
+
+    def metrics(self, x, y, z):
+        si, sj, sk = self.p2(), self.p2(), self.p2()
+        vol = self.p1()
+        lib().orc_imetrix(self.h, _p(x), _p(y), _p(z), _p(si), _p(sj), _p(sk))
+        lib().orc_vols(self.h, _p(x), _p(y), _p(z), _p(vol))
+        return si, sj, sk, vol
+
+    def cons2prim(self, q, xtnd=0):
+        lib().orc_cons2prim(self.h, _par(self.p), C.c_int(xtnd), _p(q))
+
+    def prim2cons(self, q):
+        lib().orc_prim2cons(self.h, _par(self.p), _p(q))
+
+    def bc(self, q, si, sj, sk):
+        return lib().orc_bc(self.h, _par(self.p), _p(q), _p(si), _p(sj), _p(sk))
+
+    def cutman_q(self, q):
+        lib().orc_cutman_q(self.h, _p(q))
+
+    def prtest(self, q):
+        return lib().orc_prtest(self.h, _par(self.p), _p(q))
+
+    def lambda_(self, q, si, sj, sk, lam):
+        lib().orc_lambda(self.h, _par(self.p), _p(q), _p(si), _p(sj), _p(sk), _p(lam))
+
+    def deltat(self, dtvol, lam, bx=None, by=None, bz=None):
+        nul = C.cast(None, _dp)
+        lib().orc_deltat(self.h, _par(self.p), _p(dtvol), _p(lam),
+                         _p(bx) if bx is not None else nul, _p(by) if by is not None else nul,
+                         _p(bz) if bz is not None else nul)
+
+    def muscl(self, idir, nl, q, qp, qm, dq, dqp, dqm):
+        lib().orc_muscl(self.h, _par(self.p), C.c_int(idir), C.c_int(nl), _p(q), _p(qp), _p(qm),
+                        _p(dq), _p(dqp), _p(dqm))
+
+    def roflux(self, idir, qr, ql, flux, sijk):
+        lib().orc_roflux(self.h, _par(self.p), C.c_int(idir), _p(qr), _p(ql), _p(flux), _p(sijk))
+
+    def resid(self, idir, flux, res):
+        lib().orc_resid(self.h, C.c_int(idir), _p(flux), _p(res))
+
+    def update(self, res, q, qold, dtvol, ar):
+        lib().orc_update(self.h, _p(res), _p(q), _p(qold), _p(dtvol), C.c_double(ar))
+
+    def resg_rms(self, res, rhs):
+        out = np.zeros(self.p.npde + 1)
+        lib().orc_resg_rms(self.h, _p(res), _p(rhs), _p(out))
+        return out
+
+    def zero_res(self, res):
+        lib().orc_zero_res(self.h, _p(res))
+
+    def copy_interior(self, dst, src):
+        lib().orc_copy_interior(self.h, _p(dst), _p(src))
+
+    def residual(self, q, si, sj, sk, nl=1, want_dt=True, work=None):
+        """Stage-1 residual as smooth() computes it; returns (res, dtvol, status).
+        q is modified in place exactly as smooth() modifies it."""
+        w = work or {k: self.p3() for k in ("res", "qp", "qm", "dq", "dqp", "dqm")}
+        flux = self.f0()
+        dtvol = self.p1(self.S)
+        st = lib().orc_residual(self.h, _par(self.p), C.c_int(nl), _p(q), _p(si), _p(sj), _p(sk),
+                                _p(w["res"]), _p(w["qp"]), _p(w["qm"]), _p(w["dq"]), _p(w["dqp"]),
+                                _p(w["dqm"]), _p(flux), _p(dtvol), C.c_int(1 if want_dt else 0))
+        return w["res"], dtvol, st
+
+    def smooth(self, q, si, sj, sk, ncycles, mgit0=1, rms_every=1):
+        """ncycles single-level cycles of smooth(); q updated in place.
+        Returns (hist[ncycles, npde+1], status)."""
+        qold = self.p3()
+        res, rhs = self.p3(), self.p3()
+        qp, qm, dq, dqp, dqm = (self.p3() for _ in range(5))
+        flux = self.f0()
+        dtvol = self.p1(self.S)
+        hist = np.full((ncycles, self.p.npde + 1), np.nan)
+        st = lib().orc_smooth(self.h, _par(self.p), C.c_int(ncycles), C.c_int(mgit0), C.c_int(rms_every),
+                              _p(q), _p(qold), _p(si), _p(sj), _p(sk), _p(res), _p(rhs), _p(qp), _p(qm),
+                              _p(dq), _p(dqp), _p(dqm), _p(flux), _p(dtvol), _p(hist))
+        return hist, st
+
+
+def roe_face(params, nrm, qr, ql):
+    f = np.zeros(5)
+    n = np.ascontiguousarray(nrm, dtype=np.float64)
+    a = np.ascontiguousarray(qr, dtype=np.float64)
+    b = np.ascontiguousarray(ql, dtype=np.float64)
+    lib().orc_roe_face(C.byref(params), _p(n), _p(a), _p(b), _p(f))
+    return f
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())

@@ -1,0 +1,36 @@
+"""Test helpers: small cases, oracle metrics, and error measures."""
+from __future__ import annotations
+
+import numpy as np
+
+from cosa_b200 import cases
+from cosa_b200.cases import p3_views, interior
+
+
+def small_channel(ni=48, nj=24, nk=2):
+    return cases.bump_channel(ni, nj, nk)
+
+
+def small_partitioned(ni=48, nj=24, nk=2, permute=True):
+    return cases.partitioned_channel(ni, nj, nk, isplit=(20,), jsplit=(10,), permute_last=permute)
+
+
+def small_duct(seed=5):
+    # 2x3x4 partition with small segments (same generator as the 30M-cell case)
+    segs = cases.duct_segments(seed=seed, lo=20_000, hi=60_000, choices=tuple(range(8, 33, 8)))
+    return cases.duct3d(segs=segs)
+
+
+def interior_cells(case, arr, nvar, nsnap=1):
+    """Concatenated interior cells of every block: (ncells_total, nvar, nsnap)."""
+    out = []
+    for v in p3_views(case.tables, arr, nvar, nsnap):
+        iv = interior(v)
+        out.append(iv.reshape(-1, nvar, nsnap, order="F"))
+    return np.concatenate(out, axis=0)
+
+
+def scaled_err(gpu, ref, scale):
+    """max |gpu - ref| / scale (scale per variable, broadcast on axis 1)."""
+    d = np.abs(gpu - ref)
+    return float((d / scale[None, :, None]).max())

@@ -1,0 +1,222 @@
+"""Parity of the sm_100a path (through the C-ABI) with the CPU oracle.
+
+Tolerance (FP64 path): the GPU build contracts multiply-adds (FMA) where the
+oracle keeps the Fortran operation order, so results differ by rounding only.
+Per-cell errors are measured relative to the magnitude of the terms being
+combined: for fluxes and residuals, relative to the largest face flux of the
+same equation (a residual is a sum of face fluxes); for states, relative to
+the largest value of the same variable.  The bar is 1e-12.
+"""
+import numpy as np
+import pytest
+
+from cosa_b200 import cases, gpu
+from cosa_b200.cases import p3_views
+from cosa_b200.params import PREC_MIXED
+
+import casekit
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def _setup(case, oracle_mod, seed=3, perturb=True):
+    O = oracle_mod.OracleLevel(case.tables, case.params)
+    si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
+    q = cases.perturbed_state(case, seed=seed) if perturb else case.q0.copy()
+    ctx = gpu.Context([case.tables], case.params)
+    return O, ctx, (si, sj, sk, vol), q
+
+
+def _rel(a, b, case, nvar=5, scale=None):
+    A = casekit.interior_cells(case, a, nvar)
+    B = casekit.interior_cells(case, b, nvar)
+    if scale is None:
+        scale = np.abs(B).reshape(-1, nvar).max(axis=0) + 1e-300
+    return float((np.abs(A - B) / scale[None, :, None]).max())
+
+
+def _flux_scale(flux, case):
+    nvar = 5
+    F = flux.reshape(nvar, -1)  # one block of F0 is (i,j,k,v): use per-variable max over all
+    return np.array([np.abs(f).max() for f in F]) + 1e-300
+
+
+@pytest.mark.parametrize("which", ["channel", "partitioned"])
+def test_routines_match_oracle(oracle_mod, which):
+    """Each level driver against the oracle routine it replaces, chained as
+    smooth() chains them for one stage (src/cosa.f90:1721-2000)."""
+    case = casekit.small_channel() if which == "channel" else casekit.small_partitioned()
+    O, ctx, (si, sj, sk, vol), q = _setup(case, oracle_mod)
+    d = {k: ctx.alloc_p2().upload(v) for k, v in (("si", si), ("sj", sj), ("sk", sk))}
+    dq_ = ctx.alloc_p3().upload(q)
+    qh = q.copy()
+    # cons2prim
+    O.cons2prim(qh)
+    ctx.cons2prim(1, dq_)
+    assert _rel(dq_.download(), qh, case) <= TOL
+    # bc + cutman_q (+ prtest): full arrays, halos included
+    O.bc(qh, si, sj, sk)
+    O.cutman_q(qh)
+    ctx.bc(1, dq_, d["si"], d["sj"], d["sk"])
+    ctx.cutman_q(1, dq_)
+    assert ctx.prtest(1, dq_) == 0 and O.prtest(qh) == 0
+    g = dq_.download()
+    for vg, vo in zip(p3_views(case.tables, g, 5, 1), p3_views(case.tables, qh, 5, 1)):
+        sc = np.abs(vo).reshape(-1, 5).max(axis=0)
+        assert (np.abs(vg - vo) / sc[None, None, None, :, None]).max() <= TOL
+    # lambda + deltat
+    lam_o, lam_g = O.p3(), ctx.alloc_p3()
+    O.lambda_(qh, si, sj, sk, lam_o)
+    ctx.lambda_(1, dq_, d["si"], d["sj"], d["sk"], None, lam_g)
+    dt_o, dt_g = O.p1(), ctx.alloc_p1()
+    O.deltat(dt_o, lam_o)
+    ctx.deltat(1, dt_g, lam_g)
+    np.testing.assert_allclose(dt_g.download(), dt_o, rtol=TOL, atol=0)
+    # muscl + roflux + resid in the three directions
+    res_o, res_g = O.p3(), ctx.alloc_p3()
+    O.zero_res(res_o)
+    ctx.zero(1, res_g)
+    fscale = np.zeros(5)
+    for idir, s_o, s_g in ((1, si, d["si"]), (2, sj, d["sj"]), (3, sk, d["sk"])):
+        bufs_o = [O.p3() for _ in range(5)]
+        bufs_g = [ctx.alloc_p3() for _ in range(5)]
+        O.muscl(idir, 1, qh, *bufs_o)
+        ctx.muscl(idir, 1, dq_, *bufs_g)
+        for k in (0, 1):  # qp, qm on the faces
+            a, b = bufs_g[k].download(), bufs_o[k]
+            sc = np.abs(b).max()
+            # compare the face entries the reference writes (interior of the face range)
+            for vg, vo in zip(p3_views(case.tables, a, 5, 1), p3_views(case.tables, b, 5, 1)):
+                sl = [slice(2, -2)] * 3
+                sl[idir - 1] = slice(2, -1)
+                assert (np.abs(vg[tuple(sl)] - vo[tuple(sl)])).max() <= TOL * sc
+        fo, fg = O.f0(), ctx.alloc_f0()
+        O.roflux(idir, bufs_o[0], bufs_o[1], fo, s_o)
+        ctx.roflux(idir, 1, bufs_g[0], bufs_g[1], fg, s_g)
+        fgh = fg.download()
+        sc = np.abs(fo).max()
+        assert np.abs(fgh - fo).max() <= TOL * sc
+        fscale = np.maximum(fscale, sc)
+        O.resid(idir, fo, res_o)
+        ctx.resid(idir, 1, fg, res_g)
+    assert _rel(res_g.download(), res_o, case, scale=fscale) <= TOL
+    rms_o = O.resg_rms(res_o, O.p3())
+    rms_g = ctx.resg_rms(1, res_g)
+    np.testing.assert_allclose(rms_g, rms_o, rtol=1e-9)
+    # prim2cons + update
+    O.prim2cons(qh)
+    ctx.prim2cons(1, dq_)
+    qold_o = q.copy()
+    qold_g = ctx.alloc_p3().upload(q)
+    O.update(res_o, qh, qold_o, dt_o, 0.25)
+    ctx.update(1, res_g, dq_, qold_g, dt_g, 0.25)
+    assert _rel(dq_.download(), qh, case) <= TOL
+    ctx.close()
+
+
+@pytest.mark.parametrize("which", ["channel", "partitioned", "duct"])
+def test_fused_smooth_matches_oracle(oracle_mod, which):
+    """cosa_gpu_smooth (fused halo + tile kernels in a CUDA graph) against the
+    oracle's smooth() for several RK cycles: state, q^n copy, time step and
+    the residual history."""
+    if which == "channel":
+        case = casekit.small_channel()
+    elif which == "partitioned":
+        case = casekit.small_partitioned()
+    else:
+        case = casekit.small_duct()
+    O, ctx, (si, sj, sk, vol), q = _setup(case, oracle_mod, seed=11)
+    ncyc = 6
+    qo = q.copy()
+    hist_o, st_o = O.smooth(qo, si, sj, sk, ncyc, rms_every=2)
+    assert st_o == 0
+    dq_ = ctx.alloc_p3().upload(q)
+    qold = ctx.alloc_p3()
+    dtv = ctx.alloc_p1(nsnap=1)
+    m = [ctx.alloc_p2().upload(a) for a in (si, sj, sk)]
+    ctx.bind_level(1, q=dq_, qold=qold, dtvol=dtv, si=m[0], sj=m[1], sk=m[2])
+    hist_g, st = ctx.smooth(1, ncyc, 1, 2)
+    assert st == 0
+    err = _rel(dq_.download(), qo, case)
+    assert err <= TOL, err
+    rows = ~np.isnan(hist_o[:, 0])
+    assert np.array_equal(rows, ~np.isnan(hist_g[:, 0]))
+    np.testing.assert_allclose(hist_g[rows], hist_o[rows], rtol=1e-9)
+    ctx.close()
+
+
+def test_smooth_host_buffers_equal_device_path(oracle_mod):
+    """cosa_gpu_smooth_host (state copied in and out each call) gives the
+    device-resident result."""
+    case = casekit.small_partitioned()
+    O, ctx, (si, sj, sk, vol), q = _setup(case, oracle_mod, seed=2)
+    m = [ctx.alloc_p2().upload(a) for a in (si, sj, sk)]
+    dq_ = ctx.alloc_p3().upload(q)
+    ctx.bind_level(1, q=dq_, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(), si=m[0], sj=m[1], sk=m[2])
+    ctx.smooth(1, 3, 1, 1)
+    a = dq_.download()
+    qh = q.copy()
+    _, st = ctx.smooth_host(1, qh, 3, 1, 1)
+    assert st == 0
+    assert np.array_equal(casekit.interior_cells(case, a, 5), casekit.interior_cells(case, qh, 5))
+    ctx.close()
+
+
+def test_mixed_precision_close_to_fp64(oracle_mod):
+    """FP32 slopes + FP32 Roe dissipation on FP64 differences: after 20
+    cycles the state stays within 1e-6 (relative) of the FP64 path."""
+    case = casekit.small_partitioned()
+    O, ctx, (si, sj, sk, vol), q = _setup(case, oracle_mod, seed=4)
+    p = case.params
+    p.precision = PREC_MIXED
+    ctx2 = gpu.Context([case.tables], p)
+    out = []
+    for c in (ctx, ctx2):
+        m = [c.alloc_p2().upload(a) for a in (si, sj, sk)]
+        dq_ = c.alloc_p3().upload(q)
+        c.bind_level(1, q=dq_, qold=c.alloc_p3(), dtvol=c.alloc_p1(), si=m[0], sj=m[1], sk=m[2])
+        _, st = c.smooth(1, 20, 1, 20)
+        assert st == 0
+        out.append(dq_.download())
+    err = _rel(out[1], out[0], case)
+    assert 0 < err < 1e-6, err
+    ctx.close(); ctx2.close()
+
+
+def test_negative_pressure_sets_status_not_fault(oracle_mod):
+    """A state with a non-physical pressure is reported through the status
+    word (src/cosa.f90:1000-1040 stops there); the context stays usable."""
+    case = casekit.small_channel(16, 8, 2)
+    O, ctx, (si, sj, sk, vol), q = _setup(case, oracle_mod, perturb=False)
+    v = p3_views(case.tables, q, 5, 1)[0]
+    v[6, 4, 2, 4, 0] = -5.0  # rho*E far below the kinetic energy -> p < 0
+    m = [ctx.alloc_p2().upload(a) for a in (si, sj, sk)]
+    dq_ = ctx.alloc_p3().upload(q)
+    ctx.bind_level(1, q=dq_, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(), si=m[0], sj=m[1], sk=m[2])
+    _, st = ctx.smooth(1, 1, 1, 1)
+    assert st & 0x1
+    ctx.status(reset=True)
+    dq_.upload(case.q0)
+    _, st = ctx.smooth(1, 1, 1, 1)
+    assert st == 0
+    ctx.close()
+
+
+@pytest.mark.parametrize("which", ["channel", "duct"])
+def test_device_metrics_match_oracle(oracle_mod, which):
+    """imetrix / vols on the device against the oracle's restatement of
+    src/grid.f90 (the host precompute the GPU path replaces)."""
+    case = casekit.small_channel() if which == "channel" else casekit.small_duct()
+    O = oracle_mod.OracleLevel(case.tables, case.params)
+    si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
+    ctx = gpu.Context([case.tables], case.params)
+    X, Y, Z = (ctx.alloc_p2(ncomp=1).upload(a) for a in (case.x, case.y, case.z))
+    gs = [ctx.alloc_p2() for _ in range(3)]
+    gv = ctx.alloc_p1()
+    ctx.imetrix(1, X, Y, Z, *gs)
+    ctx.vols(1, X, Y, Z, gv)
+    for g, o in zip(gs, (si, sj, sk)):
+        np.testing.assert_allclose(g.download(), o, rtol=1e-13, atol=1e-15)
+    np.testing.assert_allclose(gv.download(), vol, rtol=1e-12, atol=1e-18)
+    ctx.close()
