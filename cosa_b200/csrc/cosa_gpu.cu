@@ -392,9 +392,16 @@ int launch_iteration(cosa_ctx *c, int nl, LevelState &L, bool want_rms, int comp
     if (r) return r;
   }
   if (p.nstage % 2 == 1) {
-    // result landed in T: copy the interior back (whole array is simplest)
+    // result landed in T: copy the interior back; Q keeps the last stage's
+    // halo values for the finalisation of smooth()
     const int S = 2 * p.nharms + 1;
-    CK(cudaMemcpyAsync(Q, T, (size_t)L.n3 * p.npde * S * sizeof(double), cudaMemcpyDeviceToDevice, c->s));
+    for (int b = 0; b < L.nb; ++b) {
+      const DevBlock &x = L.hb[b];
+      k_copy_interior<<<grid_for((int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * p.npde * S), 256, 0, c->s>>>(
+          x, p.npde * S, T, Q);
+      int r = after_launch(c);
+      if (r) return r;
+    }
   }
   return COSA_OK;
 }
@@ -725,7 +732,7 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
       c->launches = before;  // counted at replay
     }
     CK(cudaGraphLaunch(g, c->s));
-    c->launches += c->p.nstage * (L->items.empty() ? 1 : 2) + (want ? 1 : 0);
+    c->launches += c->p.nstage * (L->items.empty() ? 1 : 2) + (want ? 1 : 0) + (c->p.nstage % 2 ? L->nb : 0);
   }
   // reference state after smooth(): face halos of q in conservative form
   if (niter > 0 && !L->items.empty()) {

@@ -252,6 +252,7 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
   __syncthreads();
   double fk_lo[5];
   if (cvalid) kface(T.k0, fk_lo);
+  __syncthreads();  // the first load below overwrites the slot of plane k0-2
 
   for (int k = T.k0; k <= T.k1; ++k) {
     load_plane(k + 2);
@@ -383,6 +384,21 @@ __global__ void k_rms_final(const double *__restrict__ part, int nparts, int npd
     double *o = out + (int64_t)row * (npde + 1);
     for (int v = 0; v < npde; ++v) o[v] = sqrt(tot[v] / ncell);
     o[npde] = sqrt(all / ncell / npde);
+  }
+}
+
+// ---- interior copy (odd stage counts end in the second buffer) --------------------------
+__global__ void k_copy_interior(DevBlock b, int nvar_snap, const double *__restrict__ src, double *__restrict__ dst) {
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t n = (int64_t)ni * nj * nk * nvar_snap;
+  const int64_t base = b.op3 * nvar_snap;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)(r % nk) + 1; r /= nk;
+    const int64_t o = base + r * b.P3 + p3_cell(b, i, j, k);
+    dst[o] = src[o];
   }
 }
 

@@ -115,17 +115,23 @@ def test_routines_match_oracle(oracle_mod, which):
     ctx.close()
 
 
-@pytest.mark.parametrize("which", ["channel", "partitioned", "duct"])
+FUSED_CASES = {
+    "channel": lambda: casekit.small_channel(),
+    # extrapolated z faces and 5 k-planes: planes k0-2 and k0+2 differ, which
+    # a missing barrier between the first k-face and the ring refill exposes
+    "channel_extrap_nk5": lambda: cases.bump_channel(40, 20, 5, kface_bc=4),
+    "jsplit_10_14": lambda: cases.partitioned_channel(48, 24, 2, isplit=(), jsplit=(10,), permute_last=False),
+    "partitioned": lambda: casekit.small_partitioned(),
+    "duct": lambda: casekit.small_duct(),
+}
+
+
+@pytest.mark.parametrize("which", list(FUSED_CASES))
 def test_fused_smooth_matches_oracle(oracle_mod, which):
     """cosa_gpu_smooth (fused halo + tile kernels in a CUDA graph) against the
     oracle's smooth() for several RK cycles: state, q^n copy, time step and
     the residual history."""
-    if which == "channel":
-        case = casekit.small_channel()
-    elif which == "partitioned":
-        case = casekit.small_partitioned()
-    else:
-        case = casekit.small_duct()
+    case = FUSED_CASES[which]()
     O, ctx, (si, sj, sk, vol), q = _setup(case, oracle_mod, seed=11)
     ncyc = 6
     qo = q.copy()
