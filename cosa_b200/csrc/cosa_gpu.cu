@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -850,3 +851,59 @@ int cosa_gpu_status(cosa_ctx *c, int32_t reset) {
 }
 
 }  // extern "C"
+
+// ---- allocation-free residual norm ---------------------------------------------------
+// Scratch of cosa_gpu_resg_rms_noalloc: per-CTA partial sums, 8 doubles each,
+// COSA_NOALLOC_MAX_PARTS rows (256 KiB).  It lives in the library image, so
+// every device that loads the library holds it until the process exits.  Host
+// code must not pass the symbol itself to a kernel (on the host it is only a
+// stand-in); the device address is looked up once per device below.
+static __device__ __align__(256) double g_noalloc_rms_part[COSA_NOALLOC_MAX_PARTS * 8];
+
+namespace {
+constexpr int kMaxDevices = 64;
+double *g_noalloc_part_dev[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mu;
+
+int noalloc_scratch(double **out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return COSA_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_part_dev[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_rms_part) != cudaSuccess || !p) return COSA_ERR_CUDA;
+    g_noalloc_part_dev[dev] = static_cast<double *>(p);
+  }
+  *out = g_noalloc_part_dev[dev];
+  return COSA_OK;
+}
+}  // namespace
+
+extern "C" int cosa_gpu_resg_rms_noalloc(int32_t nblocks, const int32_t *dims, int32_t npde, int32_t nharms,
+                                         const double *res, const double *rhs, double *resrms, void *stream) {
+  if (nblocks < 1 || nblocks > COSA_NOALLOC_MAX_PARTS || !dims || !res || !resrms) return COSA_ERR_ARG;
+  if ((npde != 5 && npde != 7) || nharms < 0 || 2 * nharms + 1 > COSA_MAX_SNAP) return COSA_ERR_ARG;
+  for (int b = 0; b < nblocks; ++b)
+    if (dims[3 * b] < 3 || dims[3 * b + 1] < 3 || dims[3 * b + 2] < 2) return COSA_ERR_ARG;
+  double *part = nullptr;
+  int r = noalloc_scratch(&part);
+  if (r) return r;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int per_block = std::max(1, std::min(64, COSA_NOALLOC_MAX_PARTS / nblocks));
+  const int S = 2 * nharms + 1;
+  int64_t op3 = 0, ncell = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    DevBlock x{};
+    x.im = dims[3 * b]; x.jm = dims[3 * b + 1]; x.km = dims[3 * b + 2];
+    x.I3 = x.im + 3; x.J3 = x.jm + 3;
+    x.P3 = (int64_t)(x.im + 3) * (x.jm + 3) * (x.km + 3);
+    x.op3 = op3;
+    k_rms_partial_noalloc<<<per_block, 256, 0, s>>>(x, npde, S, res, rhs, part + (int64_t)b * per_block * 8);
+    if (cudaGetLastError() != cudaSuccess) return COSA_ERR_CUDA;
+    op3 += x.P3;
+    ncell += (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1);
+  }
+  k_rms_final<<<1, 256, 0, s>>>(part, nblocks * per_block, npde, (double)ncell, resrms, nullptr, 1);
+  if (cudaGetLastError() != cudaSuccess) return COSA_ERR_CUDA;
+  return COSA_OK;
+}

@@ -363,6 +363,41 @@ __global__ void k_rms_partial(DevBlock b, const cosa_params *__restrict__ Pp, co
   }
 }
 
+// Same partial sums as k_rms_partial with npde and the snapshot count passed
+// by value (the allocation-free entry point has no device parameter block).
+__global__ void k_rms_partial_noalloc(DevBlock b, int npde, int S, const double *__restrict__ res,
+                                      const double *__restrict__ rhs, double *__restrict__ part) {
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t ncell = (int64_t)ni * nj * nk;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)r + 1;
+    const int64_t c = p3_cell(b, i, j, k);
+    for (int v = 0; v < npde; ++v) {
+      const double tt = res[p3_var(b, npde, S, v + 1, 0) + c] - (rhs ? rhs[p3_var(b, npde, S, v + 1, 0) + c] : 0.0);
+      acc[v] += tt * tt;
+    }
+  }
+  __shared__ double red[7][32];
+  for (int v = 0; v < npde; ++v) {
+    double x = acc[v];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) red[v][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int nw = blockDim.x >> 5;
+    for (int v = 0; v < npde; ++v) {
+      double x = threadIdx.x < nw ? red[v][threadIdx.x] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (threadIdx.x == 0) part[(int64_t)blockIdx.x * 8 + v] = x;
+    }
+  }
+}
+
 // ---- imetrix_b (src/grid.f90:847-1010): face unit normals and areas, fixed grid ----
 // One thread per face of family d; x/y/z are P2 grid arrays (0:imax+1, ...).
 __global__ void k_imetrix(DevBlock b, int d, const double *__restrict__ x, const double *__restrict__ y,

@@ -53,6 +53,7 @@ SYMBOLS = [
     "cosa_gpu_muscl", "cosa_gpu_roflux", "cosa_gpu_resid", "cosa_gpu_update", "cosa_gpu_resg_rms",
     "cosa_gpu_zero", "cosa_gpu_smooth", "cosa_gpu_smooth_host", "cosa_gpu_launch_count",
     "cosa_gpu_status", "cosa_gpu_imetrix", "cosa_gpu_vols", "cosa_gpu_profile", "cosa_gpu_stream",
+    "cosa_gpu_resg_rms_noalloc",
 ]
 
 

@@ -222,6 +222,28 @@ int64_t cosa_gpu_launch_count(cosa_ctx *ctx, int32_t reset);
 /* latched device status bits (COSA_ERR_*), cleared when reset != 0 */
 int cosa_gpu_status(cosa_ctx *ctx, int32_t reset);
 
+/*
+ * Residual RMS that allocates nothing.  No counterpart in the reference: it
+ * is the resg_rms computation for callers that cannot call cudaMalloc, such
+ * as a Fortran driver whose device memory is owned and pooled by another
+ * runtime, or code running where a new allocation would fail or is not
+ * permitted.  It needs no context: the caller passes the block table (host
+ * array dims[3*nblocks], node counts as in cosa_level_desc), npde, nharms,
+ * the device arrays res and rhs (rhs may be NULL) in the P3 layout, a device
+ * output resrms[npde+1] (per-equation RMS, then the total as in resg_rms),
+ * and a CUDA stream (NULL = default stream).  The per-CTA partial sums go to
+ * a static device array of COSA_NOALLOC_MAX_PARTS rows of 8 doubles
+ * (256 KiB) that every GPU loading the library holds until exit.  The first
+ * call on a device looks up that array's device address; make that first
+ * call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race.  nblocks above COSA_NOALLOC_MAX_PARTS returns
+ * COSA_ERR_ARG.
+ */
+#define COSA_NOALLOC_MAX_PARTS 4096
+int cosa_gpu_resg_rms_noalloc(int32_t nblocks, const int32_t *dims, int32_t npde,
+                              int32_t nharms, const double *res, const double *rhs,
+                              double *resrms, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
