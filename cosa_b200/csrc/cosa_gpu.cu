@@ -15,7 +15,7 @@
 
 namespace {
 
-constexpr int kTI = 32, kTJ = 8;  // tile of the fused stage kernel
+constexpr int kTI = 32, kTJ = 7;  // tile of the fused stage kernel (7 rows + the boundary-face warp = 256 threads)
 
 struct LevelState {
   int nb = 0;
@@ -363,9 +363,9 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   const size_t smem = stage_smem_bytes<kTI, kTJ>();
   if (c->prof.on) cudaEventRecord(c->prof.ev[1][0], c->s);
   if (p.precision == COSA_PREC_MIXED)
-    k_stage_tile<kTI, kTJ, true><<<L.ntiles, kTI * kTJ, smem, c->s>>>(L.d_blocks, L.d_tiles, c->d_p, A);
+    k_stage_tile<kTI, kTJ, true><<<L.ntiles, stage_threads<kTI, kTJ>(), smem, c->s>>>(L.d_blocks, L.d_tiles, c->d_p, A);
   else
-    k_stage_tile<kTI, kTJ, false><<<L.ntiles, kTI * kTJ, smem, c->s>>>(L.d_blocks, L.d_tiles, c->d_p, A);
+    k_stage_tile<kTI, kTJ, false><<<L.ntiles, stage_threads<kTI, kTJ>(), smem, c->s>>>(L.d_blocks, L.d_tiles, c->d_p, A);
   int r = after_launch(c);
   if (r) return r;
   if (c->prof.on) prof_stop(c, 1);

@@ -23,6 +23,8 @@
 //                also computes the local time step (lambda/deltat) and the
 //                per-tile residual sums of squares for resg_rms.
 #pragma once
+#include <cuda_pipeline.h>
+
 #include "physics.cuh"
 
 struct HaloItem {
@@ -138,17 +140,26 @@ struct StageArgs {
   int update;            // 0: residual only (restriction pass)
 };
 
+// Thread layout: TJ main warps, warp w holds row j0+w of the tile (lane =
+// i - i0) and computes that cell's left i-face, left j-face and upper k-face
+// of every plane, then updates the cell; one extra warp computes the tile's
+// boundary faces (the j-faces above the last row and the i-faces right of the
+// last column), so every warp does a balanced share of the Roe fluxes.
 template <int TI, int TJ, bool MIXED>
-__global__ void __launch_bounds__(TI *TJ, 2)
+__global__ void __launch_bounds__(TI *TJ + 32, 2)
 k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles, const cosa_params *__restrict__ Pp,
              StageArgs A) {
-  constexpr int NT = TI * TJ;
+  static_assert(TI == 32, "a main warp is one row of the tile");
+  constexpr int NM = TI * TJ;                             // main threads (one per cell)
+  constexpr int NT = NM + 32;                             // + the boundary-face warp
   constexpr int PI = TI + 4, PJ = TJ + 4, PL = PI * PJ;  // padded plane
+  constexpr int NSLOT = 5;                                // planes k-1..k+2 + the one in flight
+  constexpr int CPT = (PL + NT - 1) / NT;                 // plane cells per thread
   extern __shared__ double smem[];
-  double *ring = smem;                     // [4][5][PJ][PI]
-  double *fi = ring + 4 * 5 * PL;          // [5][TJ][TI+1]
-  double *fj = fi + 5 * TJ * (TI + 1);     // [5][TJ+1][TI]
-  double *red = fj + 5 * (TJ + 1) * TI;    // [5][NT/32]
+  double *ring = smem;                        // [NSLOT][5][PJ][PI]
+  double *fi = ring + NSLOT * 5 * PL;         // [5][TJ][TI+1]
+  double *fj = fi + 5 * TJ * (TI + 1);        // [5][TJ+1][TI]
+  double *red = fj + 5 * (TJ + 1) * TI;       // [5][TJ]
 
   const cosa_params &P = *Pp;
   const Tile T = tiles[blockIdx.x];
@@ -158,46 +169,68 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
   const PhysPar ph = make_phys(P);
   const double g = P.gamma;
   const int tid = threadIdx.x;
-  const int ti = tid % TI, tj = tid / TI;
+  const bool main_warp = tid < NM;
+  const int ti = tid % TI, tj = main_warp ? tid / TI : 0;
   const int ci = T.i0 + ti, cj = T.j0 + tj;          // this thread's cell column
-  const bool cvalid = ci <= b.im - 1 && cj <= b.jm - 1;
+  const bool cvalid = main_warp && ci <= b.im - 1 && cj <= b.jm - 1;
   const int64_t vstride = b.P3;
   const double *qin = A.qin + p3_var(b, npde, S, 1, n);
   const StrongMap sm = A.smap[T.blk];
+  // metric plane strides (fixed grid per snapshot)
+  const int64_t I2 = b.im + 2, J2 = b.jm + 2;
+  const int64_t mbase = (b.op2 * S2 + (int64_t)nh * I2 * J2 * (b.km + 2)) * 4;
   int st = 0;
 
-  auto slot_of = [](int k) { return ((k % 4) + 4) % 4; };
+  auto slot = [](int k) { return ((k % NSLOT) + NSLOT) % NSLOT; };
 
-  // load plane k (all cells of the padded plane that the stencils touch)
-  auto load_plane = [&](int k) {
-    double *dst = ring + slot_of(k) * 5 * PL;
-    const bool kin = k >= 1 && k <= b.km - 1;
-    for (int c = tid; c < PL; c += NT) {
-      const int pi = c % PI, pj = c / PI;
-      const int i = T.i0 - 2 + pi, j = T.j0 - 2 + pj;
-      const bool iin = i >= 1 && i <= b.im - 1, jin = j >= 1 && j <= b.jm - 1;
-      const int nout = (!iin) + (!jin) + (!kin);
-      if (nout > 1 || i > b.im + 1 || j > b.jm + 1) continue;  // corners/edges: never read
-      const int64_t cell = p3_cell(b, i, j, k);
+  auto cell_kind = [&](int c, int k, int64_t &gcell) -> int {
+    if (c >= PL) return 0;
+    const int pi = c % PI, pj = c / PI;
+    const int i = T.i0 - 2 + pi, j = T.j0 - 2 + pj;
+    const bool iin = i >= 1 && i <= b.im - 1, jin = j >= 1 && j <= b.jm - 1, kin = k >= 1 && k <= b.km - 1;
+    const int nout = (!iin) + (!jin) + (!kin);
+    if (nout > 1 || i > b.im + 1 || j > b.jm + 1) return 0;  // corners, edges, outside
+    gcell = p3_cell(b, i, j, k);
+    return nout == 0 ? 1 : 2;
+  };
+  auto prefetch = [&](int k) {
+    double *dst = ring + slot(k) * 5 * PL;
+#pragma unroll
+    for (int r = 0; r < CPT; ++r) {
+      const int c = tid + r * NT;
+      int64_t gc;
+      if (!cell_kind(c, k, gc)) continue;
+#pragma unroll
+      for (int m = 0; m < 5; ++m) __pipeline_memcpy_async(dst + m * PL + c, qin + m * vstride + gc, sizeof(double));
+    }
+    __pipeline_commit();
+  };
+  auto convert = [&](int k) {
+    double *dst = ring + slot(k) * 5 * PL;
+#pragma unroll
+    for (int r = 0; r < CPT; ++r) {
+      const int c = tid + r * NT;
+      int64_t gc;
+      if (cell_kind(c, k, gc) != 1) continue;
       double v[5];
 #pragma unroll
-      for (int m = 0; m < 5; ++m) v[m] = qin[m * vstride + cell];
-      if (nout == 0) {
-        c2p5(g, v);
-        if (v[4] <= P.qmin[4]) st |= COSA_ERR_NEG_P;
-        else if (v[0] <= P.qmin[0]) st |= COSA_ERR_NEG_RHO;
-      }
+      for (int m = 0; m < 5; ++m) v[m] = dst[m * PL + c];
+      c2p5(g, v);
+      if (v[4] <= P.qmin[4]) st |= COSA_ERR_NEG_P;
+      else if (v[0] <= P.qmin[0]) st |= COSA_ERR_NEG_RHO;
 #pragma unroll
       for (int m = 0; m < 5; ++m) dst[m * PL + c] = v[m];
     }
   };
 
-  // face flux along a line: w0..w3 = cells f-2..f+1 (pointers into the ring
-  // with stride `ls` between consecutive cells and PL between variables)
-  auto face = [&](const double *w1p, const double *w0p, const double *w2p, const double *w3p, int f, int mx,
+  // MUSCL + limiter + Roe flux of face f along a line: w0..w3 = cells f-2..f+1
+  auto face = [&](const double *w0p, const double *w1p, const double *w2p, const double *w3p, int f, int mx,
                   bool slo, bool shi, const double *met, double *F) {
     double qr[5], ql[5];
     const bool ovr_lo = (f == 1 && slo), ovr_hi = (f == mx && shi);
+    const bool d_lo = (f - 1 == 1 && slo) || (f - 1 == mx && shi);
+    const bool d_mid = (f == 1 && slo) || (f == mx && shi);
+    const bool d_hi = (f + 1 == 1 && slo) || (f + 1 == mx && shi);
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
       const double a0 = w0p[m * PL], a1 = w1p[m * PL], a2 = w2p[m * PL], a3 = w3p[m * PL];
@@ -205,12 +238,12 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
         qr[m] = a2; ql[m] = a1;
       } else {
         double dlo = a1 - a0, dmid = a2 - a1, dhi = a3 - a2;
-        if ((f - 1 == 1 && slo) || (f - 1 == mx && shi)) dlo = (a1 - a0) * 2;
-        if ((f == 1 && slo) || (f == mx && shi)) dmid = (a2 - a1) * 2;
-        if ((f + 1 == 1 && slo) || (f + 1 == mx && shi)) dhi = (a3 - a2) * 2;
+        if (d_lo) dlo = (a1 - a0) * 2;
+        if (d_mid) dmid = (a2 - a1) * 2;
+        if (d_hi) dhi = (a3 - a2) * 2;
         if (MIXED) {
           float dp, dm;
-          limit_face<float>(ph.ilimf, (float)ph.epslimf, (float)ph.rkap, (float)dlo, (float)dmid, (float)dhi, dp, dm);
+          limit_face_fast(ph.ilimf, (float)ph.epslimf, (float)ph.rkap, (float)dlo, (float)dmid, (float)dhi, dp, dm);
           qr[m] = a2 + (double)dp; ql[m] = a1 + (double)dm;
         } else {
           double dp, dm;
@@ -222,72 +255,97 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
       if (ovr_hi) { qr[m] = a2; ql[m] = a2; }
     }
     if (MIXED) roe_flux_mixed(ph, met[0], met[1], met[2], met[3], qr, ql, F);
-    else roe_flux_fp64(ph, met[0], met[1], met[2], met[3], qr, ql, 0.0, 0.0, F);
+    else roe_flux_euler(ph, met[0], met[1], met[2], met[3], qr, ql, F);
   };
 
-  auto metric = [&](const double *s, int i, int j, int k, double *m4) {
-    const int64_t e = p2_idx(b, S2, 1, i, j, k, nh);
-    const double2 a = *reinterpret_cast<const double2 *>(s + e);
-    const double2 c = *reinterpret_cast<const double2 *>(s + e + 2);
+  auto load_metric = [&](const double *s, int i, int j, int k, double *m4) {
+    const int64_t e = mbase + (i + I2 * (j + J2 * (int64_t)k)) * 4;
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(s + e));
+    const double2 c = __ldg(reinterpret_cast<const double2 *>(s + e + 2));
     m4[0] = a.x; m4[1] = a.y; m4[2] = c.x; m4[3] = c.y;
   };
 
-  // k-face flux at face kf (between planes kf-1 and kf) for this column
+  // k-face flux at face kf (between planes kf-1 and kf) of this column
   auto kface = [&](int kf, double *F) {
     const int pc = (tj + 2) * PI + (ti + 2);
-    const double *w0 = ring + slot_of(kf - 2) * 5 * PL + pc;
-    const double *w1 = ring + slot_of(kf - 1) * 5 * PL + pc;
-    const double *w2 = ring + slot_of(kf) * 5 * PL + pc;
-    const double *w3 = ring + slot_of(kf + 1) * 5 * PL + pc;
     double m4[4];
-    metric(A.sk, ci, cj, kf, m4);
+    load_metric(A.sk, ci, cj, kf, m4);
     const bool slo = (kf <= 2) && strong_at(A.strong, sm, 2, 0, ci, cj);
     const bool shi = (kf >= b.km - 1) && strong_at(A.strong, sm, 2, 1, ci, cj);
-    face(w1, w0, w2, w3, kf, b.km, slo, shi, m4, F);
+    face(ring + slot(kf - 2) * 5 * PL + pc, ring + slot(kf - 1) * 5 * PL + pc, ring + slot(kf) * 5 * PL + pc,
+         ring + slot(kf + 1) * 5 * PL + pc, kf, b.km, slo, shi, m4, F);
+  };
+
+  // the (up to) two in-plane faces of this thread: task t = 0, 1
+  //   main warps: t = 0 i-face (ci, cj), t = 1 j-face (ci, cj)
+  //   extra warp: t = 0 j-face (i0+lane, j0+TJ), t = 1 i-face (i0+TI, j0+lane) for lane < TJ
+  struct InTask { int dir, i, j; bool valid; };
+  auto task = [&](int t) -> InTask {
+    InTask r;
+    if (main_warp) {
+      r.dir = t; r.i = ci; r.j = cj;
+      r.valid = t == 0 ? (ci <= b.im && cj <= b.jm - 1) : (ci <= b.im - 1 && cj <= b.jm);
+    } else if (t == 0) {
+      r.dir = 1; r.i = T.i0 + ti; r.j = T.j0 + TJ;
+      r.valid = r.i <= b.im - 1 && r.j <= b.jm;
+    } else {
+      r.dir = 0; r.i = T.i0 + TI; r.j = T.j0 + ti;
+      r.valid = ti < TJ && r.i <= b.im && r.j <= b.jm - 1;
+    }
+    return r;
   };
 
   double acc[5] = {0, 0, 0, 0, 0};
-  // prologue: planes k0-2 .. k0+1 and the k-face at k0
-  for (int k = T.k0 - 2; k <= T.k0 + 1; ++k) load_plane(k);
+  for (int k = T.k0 - 2; k <= T.k0 + 2; ++k) prefetch(k);
+  __pipeline_wait_prior(0);
+  for (int k = T.k0 - 2; k <= T.k0 + 2; ++k) convert(k);
   __syncthreads();
   double fk_lo[5];
   if (cvalid) kface(T.k0, fk_lo);
-  __syncthreads();  // the first load below overwrites the slot of plane k0-2
 
   for (int k = T.k0; k <= T.k1; ++k) {
-    load_plane(k + 2);
+    if (k > T.k0) {
+      __pipeline_wait_prior(0);  // plane k+2, issued during the previous face phase
+      convert(k + 2);
+    }
     __syncthreads();
+    // the slot of plane k+3 held plane k-2, last read before the barrier above
+    if (k + 3 <= T.k1 + 2) prefetch(k + 3);
+    const double *pl = ring + slot(k) * 5 * PL;
+    {
+      InTask tk = task(0);
+      double mcur[4], mnext[4];
+      if (tk.valid) load_metric(tk.dir == 0 ? A.si : A.sj, tk.i, tk.j, k, mcur);
+#pragma unroll 1
+      for (int t = 0; t < 2; ++t) {
+        const InTask tn = task(1);
+        if (t == 0 && tn.valid) load_metric(tn.dir == 0 ? A.si : A.sj, tn.i, tn.j, k, mnext);
+        if (tk.valid) {
+          const int pc = (tk.j - T.j0 + 2) * PI + (tk.i - T.i0 + 2);
+          const int stride = tk.dir == 0 ? 1 : PI;
+          const int f = tk.dir == 0 ? tk.i : tk.j, mx = tk.dir == 0 ? b.im : b.jm;
+          const int t2 = tk.dir == 0 ? tk.j : tk.i;
+          const bool slo = (f <= 2) && strong_at(A.strong, sm, tk.dir, 0, t2, k);
+          const bool shi = (f >= mx - 1) && strong_at(A.strong, sm, tk.dir, 1, t2, k);
+          double F[5];
+          face(pl + pc - 2 * stride, pl + pc - stride, pl + pc, pl + pc + stride, f, mx, slo, shi, mcur, F);
+          if (tk.dir == 0) {
+            const int a = tk.i - T.i0, r = tk.j - T.j0;
+#pragma unroll
+            for (int m = 0; m < 5; ++m) fi[(m * TJ + r) * (TI + 1) + a] = F[m];
+          } else {
+            const int a = tk.i - T.i0, r = tk.j - T.j0;
+#pragma unroll
+            for (int m = 0; m < 5; ++m) fj[(m * (TJ + 1) + r) * TI + a] = F[m];
+          }
+        }
+        tk = tn;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) mcur[m] = mnext[m];
+      }
+    }
     double fk_hi[5];
     if (cvalid) kface(k + 1, fk_hi);
-    const double *pl = ring + slot_of(k) * 5 * PL;
-    // i-faces: left faces of the tile's cells plus the right face of the row
-    for (int f = tid; f < (TI + 1) * TJ; f += NT) {
-      const int fi_ = f % (TI + 1), fj_ = f / (TI + 1);
-      const int i = T.i0 + fi_, j = T.j0 + fj_;
-      if (i > b.im || j > b.jm - 1) continue;
-      const int pc = (fj_ + 2) * PI + (fi_ + 2);
-      double m4[4], F[5];
-      metric(A.si, i, j, k, m4);
-      const bool slo = (i <= 2) && strong_at(A.strong, sm, 0, 0, j, k);
-      const bool shi = (i >= b.im - 1) && strong_at(A.strong, sm, 0, 1, j, k);
-      face(pl + pc - 1, pl + pc - 2, pl + pc, pl + pc + 1, i, b.im, slo, shi, m4, F);
-#pragma unroll
-      for (int m = 0; m < 5; ++m) fi[(m * TJ + fj_) * (TI + 1) + fi_] = F[m];
-    }
-    // j-faces
-    for (int f = tid; f < TI * (TJ + 1); f += NT) {
-      const int fi_ = f % TI, fj_ = f / TI;
-      const int i = T.i0 + fi_, j = T.j0 + fj_;
-      if (i > b.im - 1 || j > b.jm) continue;
-      const int pc = (fj_ + 2) * PI + (fi_ + 2);
-      double m4[4], F[5];
-      metric(A.sj, i, j, k, m4);
-      const bool slo = (j <= 2) && strong_at(A.strong, sm, 1, 0, i, k);
-      const bool shi = (j >= b.jm - 1) && strong_at(A.strong, sm, 1, 1, i, k);
-      face(pl + pc - PI, pl + pc - 2 * PI, pl + pc, pl + pc + PI, j, b.jm, slo, shi, m4, F);
-#pragma unroll
-      for (int m = 0; m < 5; ++m) fj[(m * (TJ + 1) + fj_) * TI + fi_] = F[m];
-    }
     __syncthreads();
     if (cvalid) {
       const int64_t cell = p3_cell(b, ci, cj, k);
@@ -299,9 +357,9 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
         const int pc = (tj + 2) * PI + (ti + 2);
 #pragma unroll
         for (int m = 0; m < 5; ++m) qc[m] = pl[m * PL + pc];
-        metric(A.si, ci, cj, k, sim); metric(A.si, ci + 1, cj, k, sip);
-        metric(A.sj, ci, cj, k, sjm); metric(A.sj, ci, cj + 1, k, sjp);
-        metric(A.sk, ci, cj, k, skm); metric(A.sk, ci, cj, k + 1, skp);
+        load_metric(A.si, ci, cj, k, sim); load_metric(A.si, ci + 1, cj, k, sip);
+        load_metric(A.sj, ci, cj, k, sjm); load_metric(A.sj, ci, cj + 1, k, sjp);
+        load_metric(A.sk, ci, cj, k, skm); load_metric(A.sk, ci, cj, k + 1, skp);
         double li, lj, lk;
         eig_eul(g, qc, sim, sip, sjm, sjp, skm, skp, li, lj, lk);
         dt = P.cfl / (li + lj + lk);
@@ -331,20 +389,22 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
 #pragma unroll
       for (int m = 0; m < 5; ++m) fk_lo[m] = fk_hi[m];
     }
-    __syncthreads();
   }
   if (A.part) {
+    __syncthreads();
     // deterministic per-tile sums: warp shuffle then fixed-order warp sums
+    if (main_warp) {
 #pragma unroll
-    for (int m = 0; m < 5; ++m) {
-      double x = acc[m];
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-      if ((tid & 31) == 0) red[m * (NT / 32) + (tid >> 5)] = x;
+      for (int m = 0; m < 5; ++m) {
+        double x = acc[m];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if ((tid & 31) == 0) red[m * TJ + (tid >> 5)] = x;
+      }
     }
     __syncthreads();
     if (tid < 5) {
       double x = 0;
-      for (int w = 0; w < NT / 32; ++w) x += red[tid * (NT / 32) + w];
+      for (int w = 0; w < TJ; ++w) x += red[tid * TJ + w];
       A.part[(int64_t)blockIdx.x * 8 + tid] = x;
     }
   }
@@ -353,8 +413,10 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
 
 template <int TI, int TJ>
 constexpr size_t stage_smem_bytes() {
-  return sizeof(double) * (4 * 5 * (TI + 4) * (TJ + 4) + 5 * TJ * (TI + 1) + 5 * (TJ + 1) * TI + 5 * (TI * TJ / 32));
+  return sizeof(double) * (5 * 5 * (TI + 4) * (TJ + 4) + 5 * TJ * (TI + 1) + 5 * (TJ + 1) * TI + 5 * TJ);
 }
+template <int TI, int TJ>
+constexpr int stage_threads() { return TI * TJ + 32; }
 
 // ---- deterministic reduction of per-tile / per-CTA partials -> resrms ------------------
 // resg_rms (src/cosa.f90:4458-4501): sqrt(sum/ncell), total sqrt(sum/ncell/npde)

@@ -106,6 +106,19 @@ __device__ __forceinline__ void limit_face(int ilim, T eps, T rkap, T dlo, T dmi
   }
 }
 
+// FP32 limiter of the mixed path: limit_face's algebra with fast division
+__device__ __forceinline__ void limit_face_fast(int ilim, float eps, float rkap, float dlo, float dmid, float dhi,
+                                                float &dqp, float &dqm) {
+  if (ilim == 1) {
+    float s = __fdividef(2.0f * dhi * dmid + eps, dhi * dhi + dmid * dmid + eps);
+    dqp = -s * ((1.0f + rkap * s) * dmid + (1.0f - rkap * s) * dhi) * 0.25f;
+    s = __fdividef(2.0f * dmid * dlo + eps, dmid * dmid + dlo * dlo + eps);
+    dqm = s * ((1.0f - rkap * s) * dlo + (1.0f + rkap * s) * dmid) * 0.25f;
+  } else {
+    limit_face<float>(ilim, eps, rkap, dlo, dmid, dhi, dqp, dqm);
+  }
+}
+
 // ---- roflux_b mean-flow face flux (src/flux.f90:45-238), fixed grid ---------------
 // qr/ql: primitive right/left states (rho,u,v,w,p); tker/tkel: TKE (0 for Euler)
 __device__ __forceinline__ void roe_flux_fp64(const PhysPar &P, double kx, double ky, double kz, double ds,
@@ -173,6 +186,65 @@ __device__ __forceinline__ void roe_flux_fp64(const PhysPar &P, double kx, doubl
   flux[4] = (fr5 + fl5 - df5) / 2 * ds;
 }
 
+// Euler face flux for the fused stage: roflux_b's algebra with the TKE terms
+// (zero for Euler) dropped and the four Roe averages taken with one
+// reciprocal of rhols + rhors (a last-bit difference from the divisions).
+__device__ __forceinline__ void roe_flux_euler(const PhysPar &P, double kx, double ky, double kz, double ds,
+                                               const double *qr, const double *ql, double *flux) {
+  const double g = P.g, g_gm1 = P.g_gm1, gm1 = P.gm1;
+  const double rhor = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
+  const double unr = ur * kx + vr * ky + wr * kz;
+  const double q2r = ur * ur + vr * vr + wr * wr;
+  const double h0r = g_gm1 * pr / rhor + q2r / 2;
+  const double rhol = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4];
+  const double unl = ul * kx + vl * ky + wl * kz;
+  const double q2l = ul * ul + vl * vl + wl * wl;
+  const double h0l = g_gm1 * pl / rhol + q2l / 2;
+  const double drho = rhor - rhol, dp = pr - pl, du = ur - ul, dv = vr - vl, dw = wr - wl;
+  const double dun = unr - unl;
+  const double rhols = sqrt(rhol), rhors = sqrt(rhor);
+  const double rho = rhols * rhors;
+  const double rden = 1.0 / (rhols + rhors);
+  const double u = (rhols * ul + rhors * ur) * rden;
+  const double v = (rhols * vl + rhors * vr) * rden;
+  const double w = (rhols * wl + rhors * wr) * rden;
+  const double un = u * kx + v * ky + w * kz;
+  const double h0 = (rhols * h0l + rhors * h0r) * rden;
+  const double q2 = u * u + v * v + w * w;
+  const double a2 = gm1 * (h0 - q2 / 2);
+  const double a = sqrt(a2);
+  double rm123 = fabs(un), rm4 = fabs(un + a), rm5 = fabs(un - a);
+  if (P.efx_setup_f) {
+    double rdelta = P.cntrpy_f * (P.w1 * P.entfxctf_f + P.w2 * (sqrt(q2) + a) + P.w3 * 0.2 * (fabs(un) + a));
+    rdelta = fmax(rdelta, 1.0e-12);
+    if (rm123 <= rdelta && P.efx_all_f) rm123 = 0.5 * (rm123 * rm123 + rdelta * rdelta) / rdelta;
+    if (rm4 <= rdelta) rm4 = 0.5 * (rm4 * rm4 + rdelta * rdelta) / rdelta;
+    if (rm5 <= rdelta) rm5 = 0.5 * (rm5 * rm5 + rdelta * rdelta) / rdelta;
+  }
+  if (P.eig_limit_f) {
+    if (rm123 <= P.eig_cutoff_f) rm123 = P.eig_cutoff_f;
+    if (P.eig_lim_all_f && rm4 <= P.eig_cutoff_f) rm4 = P.eig_cutoff_f;
+    if (P.eig_lim_all_f && rm5 <= P.eig_cutoff_f) rm5 = P.eig_cutoff_f;
+  }
+  const double dpa2 = dp / a2, rdua = rho * dun / a;
+  const double al1 = rm123 * (drho - dpa2);
+  const double al2 = rm123 * rho;
+  const double al3 = rm4 * (dpa2 + rdua) / 2;
+  const double al4 = rm5 * (dpa2 - rdua) / 2;
+  const double df1 = al1 + al3 + al4;
+  const double df2 = al1 * u + al2 * (du - dun * kx) + al3 * (u + a * kx) + al4 * (u - a * kx);
+  const double df3 = al1 * v + al2 * (dv - dun * ky) + al3 * (v + a * ky) + al4 * (v - a * ky);
+  const double df4 = al1 * w + al2 * (dw - dun * kz) + al3 * (w + a * kz) + al4 * (w - a * kz);
+  const double df5 = al1 * (q2 / 2) + al2 * (u * du + v * dv + w * dw - un * dun) + al3 * (h0 + a * un) +
+                     al4 * (h0 - a * un);
+  const double hds = ds / 2;
+  flux[0] = (rhor * unr + rhol * unl - df1) * hds;
+  flux[1] = ((rhor * ur * unr + pr * kx) + (rhol * ul * unl + pl * kx) - df2) * hds;
+  flux[2] = ((rhor * vr * unr + pr * ky) + (rhol * vl * unl + pl * ky) - df3) * hds;
+  flux[3] = ((rhor * wr * unr + pr * kz) + (rhol * wl * unl + pl * kz) - df4) * hds;
+  flux[4] = (rhor * h0r * unr + rhol * h0l * unl - df5) * hds;
+}
+
 // Mixed precision: the central part (fr + fl) in FP64 from the FP64 face
 // states, the Roe dissipation df in FP32 from FP32 copies of the states and
 // of their FP64 differences.  Same algebra as roe_flux_fp64.
@@ -193,9 +265,9 @@ __device__ __forceinline__ void roe_flux_mixed(const PhysPar &P, double kx, doub
   const float du = (float)(ur - ul), dv = (float)(vr - vl), dw = (float)(wr - wl);
   const float dun = (float)(unr - unl);
   const float frl = (float)rhol, frr = (float)rhor;
-  const float rhols = sqrtf(frl), rhors = sqrtf(frr);
+  const float rhols = frl * rsqrtf(frl), rhors = frr * rsqrtf(frr);
   const float rho = rhols * rhors;
-  const float rden = 1.0f / (rhols + rhors);
+  const float rden = __fdividef(1.0f, rhols + rhors);
   const float u = (rhols * (float)ul + rhors * (float)ur) * rden;
   const float v = (rhols * (float)vl + rhors * (float)vr) * rden;
   const float w = (rhols * (float)wl + rhors * (float)wr) * rden;
@@ -203,7 +275,8 @@ __device__ __forceinline__ void roe_flux_mixed(const PhysPar &P, double kx, doub
   const float h0 = (rhols * (float)h0l + rhors * (float)h0r) * rden;
   const float q2 = u * u + v * v + w * w;
   const float a2 = (float)(g - 1) * (h0 - q2 * 0.5f);
-  const float a = sqrtf(a2);
+  const float ria = rsqrtf(a2);
+  const float a = a2 * ria;
   float rm123 = fabsf(un), rm4 = fabsf(un + a), rm5 = fabsf(un - a);
   if (P.efx_setup_f) {
     float rdelta = (float)P.cntrpy_f * ((float)P.w1 * (float)P.entfxctf_f + (float)P.w2 * (sqrtf(q2) + a) +
@@ -219,8 +292,8 @@ __device__ __forceinline__ void roe_flux_mixed(const PhysPar &P, double kx, doub
     if (P.eig_lim_all_f && rm4 <= c) rm4 = c;
     if (P.eig_lim_all_f && rm5 <= c) rm5 = c;
   }
-  const float ia2 = 1.0f / a2;
-  const float dpa2 = dp * ia2, rdua = rho * dun / a;
+  const float ia2 = ria * ria;
+  const float dpa2 = dp * ia2, rdua = rho * dun * ria;
   const float al1 = rm123 * (drho - dpa2);
   const float al2 = rm123 * rho;
   const float al3 = rm4 * (dpa2 + rdua) * 0.5f;
