@@ -38,8 +38,13 @@ struct LevelState {
   cosa_level_ptrs ptrs{};
   double *d_T = nullptr;      // second state buffer of the fused stages
   double *d_part = nullptr;   // per-tile / per-CTA partial sums (8 doubles each)
+  double *d_res = nullptr;    // residual of the IRS path (P3, zero halos)
+  double *d_ores = nullptr;   // right-hand side copy of the cut-aware IRS
+  double *d_irs_scr = nullptr;  // tridiagonal pivots, 2 doubles per P3 cell and snapshot
+  double *d_beta[3] = {nullptr, nullptr, nullptr};  // IRS coefficients when not bound
   int npart_cap = 0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // iteration without / with rms
+  long long graph_launches[2] = {0, 0};           // kernels per replay of each graph
 };
 
 }  // namespace
@@ -319,9 +324,83 @@ int set_smem_attrs() {
 
 int check_fused_supported(const cosa_params &p) {
   if (p.npde != 5 || p.viscous || p.kom || p.kom_bsl || p.kom_sst || p.harbal || p.rkimp || p.moving ||
-      p.irsop != 0 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
+      p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
   return COSA_OK;
+}
+
+int ensure_irs_scratch(cosa_ctx *c, LevelState &L) {
+  const int S = 2 * c->p.nharms + 1;
+  const size_t n = (size_t)L.n3 * c->p.npde * S;
+  int r = 0;
+  if (!L.d_irs_scr && (r = dalloc(c, &L.d_irs_scr, (size_t)L.n3 * S * 2))) return r;
+  if (!L.d_res) {
+    if ((r = dalloc(c, &L.d_res, n))) return r;
+    CK(cudaMemset(L.d_res, 0, n * sizeof(double)));
+  }
+  if (!L.d_ores && (r = dalloc(c, &L.d_ores, n))) return r;
+  for (auto &bt : L.d_beta)
+    if (!bt && (r = dalloc(c, &bt, (size_t)L.n1 * S))) return r;
+  return COSA_OK;
+}
+
+// the three Thomas sweeps of cirs_b / ccirs_b on `res` for variables vs..ve
+int irs_sweeps(cosa_ctx *c, LevelState &L, double *res, const double *ores, const double *const beta[3], double eps,
+               int vs, int ve, int with_halo) {
+  const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
+  for (int b = 0; b < L.nb; ++b) {
+    const DevBlock &x = L.hb[b];
+    for (int d = 1; d <= 3; ++d) {
+      const int64_t nl = d == 1 ? (int64_t)(x.jm - 1) * (x.km - 1) : (d == 2 ? (int64_t)(x.im - 1) * (x.km - 1)
+                                                                            : (int64_t)(x.im - 1) * (x.jm - 1));
+      const int g = grid_for(nl * S, 128);
+      const double *bt = beta ? beta[d - 1] : nullptr;
+      if (d == 1) k_irs_line<1><<<g, 128, 0, c->s>>>(x, npde, S, res, ores, bt, eps, vs, ve, with_halo, L.d_irs_scr);
+      else if (d == 2) k_irs_line<2><<<g, 128, 0, c->s>>>(x, npde, S, res, nullptr, bt, eps, vs, ve, with_halo, L.d_irs_scr);
+      else k_irs_line<3><<<g, 128, 0, c->s>>>(x, npde, S, res, nullptr, bt, eps, vs, ve, with_halo, L.d_irs_scr);
+      int r = after_launch(c);
+      if (r) return r;
+    }
+  }
+  return COSA_OK;
+}
+
+int irs_scale(cosa_ctx *c, LevelState &L, double *res, const double *dtv, const double *dtvt, int forward) {
+  const int S = 2 * c->p.nharms + 1;
+  for (int b = 0; b < L.nb; ++b) {
+    const DevBlock &x = L.hb[b];
+    k_irs_scale<<<grid_for((int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * S), 256, 0, c->s>>>(x, c->p.npde, S, res, dtv,
+                                                                                               dtvt, forward);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+// cirs (cutcirs = 0) or scalef + 2 x (cutman_q + ccirs) + scaleb (cutcirs = 1)
+// of smooth() (src/cosa.f90:1977-1998) for the mean-flow equations
+int irs_apply(cosa_ctx *c, LevelState &L, double *res, double *ores, const double *dtv, const double *const beta[3]) {
+  const cosa_params &p = c->p;
+  const double eps = 0.25 * (p.rat * p.rat - 1.0);
+  const bool const_eps = p.irsop == 1;
+  const int S = 2 * p.nharms + 1;
+  int r = irs_scale(c, L, res, dtv, nullptr, 1);
+  if (r) return r;
+  if (p.cutcirs == 0) {
+    if ((r = irs_sweeps(c, L, res, nullptr, const_eps ? nullptr : beta, eps, 1, 5, 0))) return r;
+  } else {
+    CK(cudaMemcpyAsync(ores, res, (size_t)L.n3 * p.npde * S * sizeof(double), cudaMemcpyDeviceToDevice, c->s));
+    const int ncut = (int)L.items.size() - L.n_bc_items;
+    for (int its = 0; its < 2; ++its) {
+      if (ncut > 0) {
+        k_halo<false><<<grid_for((int64_t)ncut * S), 256, 0, c->s>>>(L.d_blocks, L.d_items + L.n_bc_items, ncut, c->d_p,
+                                                                    res, nullptr, nullptr, nullptr, c->d_status);
+        if ((r = after_launch(c))) return r;
+      }
+      if ((r = irs_sweeps(c, L, res, ores, const_eps ? nullptr : beta, eps, 1, 5, 1))) return r;
+    }
+  }
+  return irs_scale(c, L, res, dtv, nullptr, 0);
 }
 
 // profiling: close the event pair of kernel class `k` and accumulate its time
@@ -355,6 +434,11 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   A.part = want_rms ? L.d_part : nullptr;
   A.rhs = nullptr;
   A.res_out = res_out;
+  if (compute_dt && p.irsop >= 2) {
+    A.bx = P.betaxi ? P.betaxi : L.d_beta[0];
+    A.by = P.betaeta ? P.betaeta : L.d_beta[1];
+    A.bz = P.betazeta ? P.betazeta : L.d_beta[2];
+  }
   A.strong = L.d_strong; A.smap = L.d_smap; A.status = c->d_status;
   A.ar = p.alphas[irk - 1];
   A.compute_dt = compute_dt;
@@ -383,14 +467,32 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
 int launch_iteration(cosa_ctx *c, int nl, LevelState &L, bool want_rms, int compute_dt) {
   const cosa_params &p = c->p;
   double *Q = L.ptrs.q, *T = L.d_T, *QO = L.ptrs.qold;
+  const int S = 2 * p.nharms + 1;
   for (int irk = 1; irk <= p.nstage; ++irk) {
     double *qin = (irk % 2 == 1) ? Q : T;
     double *qout = (irk % 2 == 1) ? T : Q;
     const double *qold = irk == 1 ? Q : QO;
     double *qcopy = irk == 1 ? QO : nullptr;
-    int r = launch_stage(c, nl, L, qin, qout, qold, qcopy, irk, compute_dt && irk == 1, want_rms && irk == 1, 1,
-                         nullptr);
-    if (r) return r;
+    if (p.irsop == 0) {
+      int r = launch_stage(c, nl, L, qin, qout, qold, qcopy, irk, compute_dt && irk == 1, want_rms && irk == 1, 1,
+                           nullptr);
+      if (r) return r;
+    } else {
+      // residual (no update) -> implicit smoothing -> update
+      int r = launch_stage(c, nl, L, qin, qout, qold, nullptr, irk, compute_dt && irk == 1, want_rms && irk == 1, 0,
+                           L.d_res);
+      if (r) return r;
+      const double *beta[3] = {L.ptrs.betaxi ? L.ptrs.betaxi : L.d_beta[0],
+                               L.ptrs.betaeta ? L.ptrs.betaeta : L.d_beta[1],
+                               L.ptrs.betazeta ? L.ptrs.betazeta : L.d_beta[2]};
+      if ((r = irs_apply(c, L, L.d_res, L.d_ores, L.ptrs.dtvol, beta))) return r;
+      for (int b = 0; b < L.nb; ++b) {
+        const DevBlock &x = L.hb[b];
+        k_update_stage<<<grid_for((int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * S), 256, 0, c->s>>>(
+            x, p.npde, S, L.d_res, qold, qout, qcopy, L.ptrs.dtvol, p.alphas[irk - 1]);
+        if ((r = after_launch(c))) return r;
+      }
+    }
   }
   if (p.nstage % 2 == 1) {
     // result landed in T: copy the interior back; Q keeps the last stage's
@@ -712,6 +814,7 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
     if (hist && (mgit == 1 || mgit % rms_every == 0 || mgit == last)) rows.push_back(it);
   }
   if ((r = ensure_hist(c, std::max<int>(1, (int)rows.size())))) return r;
+  if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, *L))) return r;
   CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
   const int iter = 1;
   const int compute_dt = (iter / c->p.iupdt * c->p.iupdt == iter) ? 1 : 0;
@@ -730,10 +833,11 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
       CK(e);
       CK(cudaGraphInstantiate(&g, graph, 0));
       cudaGraphDestroy(graph);
+      L->graph_launches[want ? 1 : 0] = c->launches - before;
       c->launches = before;  // counted at replay
     }
     CK(cudaGraphLaunch(g, c->s));
-    c->launches += c->p.nstage * (L->items.empty() ? 1 : 2) + (want ? 1 : 0) + (c->p.nstage % 2 ? L->nb : 0);
+    c->launches += L->graph_launches[want ? 1 : 0];
   }
   // reference state after smooth(): face halos of q in conservative form
   if (niter > 0 && !L->items.empty()) {
@@ -767,6 +871,46 @@ int cosa_gpu_smooth_host(cosa_ctx *c, int32_t nl, double *q_host, int32_t niter,
   r = cosa_gpu_smooth(c, nl, niter, mgit0, rms_every, hist);
   int r2 = cosa_gpu_memcpy_d2h(c, q_host, L->ptrs.q, n);
   return r ? r : r2;
+}
+
+int cosa_gpu_scalef(cosa_ctx *c, int32_t nl, double *res, const double *dtvol, const double *dtvolt) {
+  LevelState *L = level(c, nl);
+  if (!L || !res || !dtvol) return COSA_ERR_ARG;
+  return irs_scale(c, *L, res, dtvol, c->p.npde > 5 ? dtvolt : nullptr, 1);
+}
+
+int cosa_gpu_scaleb(cosa_ctx *c, int32_t nl, double *res, const double *dtvol, const double *dtvolt) {
+  LevelState *L = level(c, nl);
+  if (!L || !res || !dtvol) return COSA_ERR_ARG;
+  return irs_scale(c, *L, res, dtvol, c->p.npde > 5 ? dtvolt : nullptr, 0);
+}
+
+int cosa_gpu_cirs(cosa_ctx *c, int32_t nl, double *res, const double *dtvol, const double *betaxi,
+                  const double *betaeta, const double *betazeta) {
+  LevelState *L = level(c, nl);
+  if (!L || !res || !dtvol) return COSA_ERR_ARG;
+  if (c->p.irsop < 1 || c->p.npde != 5) return COSA_ERR_UNSUPPORTED;
+  int r = ensure_irs_scratch(c, *L);
+  if (r) return r;
+  const double *beta[3] = {betaxi, betaeta, betazeta};
+  if (c->p.irsop >= 2 && (!betaxi || !betaeta || !betazeta)) return COSA_ERR_ARG;
+  const double eps = 0.25 * (c->p.rat * c->p.rat - 1.0);
+  if ((r = irs_scale(c, *L, res, dtvol, nullptr, 1))) return r;
+  if ((r = irs_sweeps(c, *L, res, nullptr, c->p.irsop == 1 ? nullptr : beta, eps, 1, 5, 0))) return r;
+  return irs_scale(c, *L, res, dtvol, nullptr, 0);
+}
+
+int cosa_gpu_ccirs(cosa_ctx *c, int32_t nl, double *res, const double *ores, const double *betaxi,
+                   const double *betaeta, const double *betazeta) {
+  LevelState *L = level(c, nl);
+  if (!L || !res || !ores) return COSA_ERR_ARG;
+  if (c->p.irsop < 1 || c->p.npde != 5) return COSA_ERR_UNSUPPORTED;
+  int r = ensure_irs_scratch(c, *L);
+  if (r) return r;
+  const double *beta[3] = {betaxi, betaeta, betazeta};
+  if (c->p.irsop >= 2 && (!betaxi || !betaeta || !betazeta)) return COSA_ERR_ARG;
+  const double eps = 0.25 * (c->p.rat * c->p.rat - 1.0);
+  return irs_sweeps(c, *L, res, ores, c->p.irsop == 1 ? nullptr : beta, eps, 1, 5, 1);
 }
 
 int cosa_gpu_imetrix(cosa_ctx *c, int32_t nl, const double *x, const double *y, const double *z, double *si,
@@ -813,6 +957,7 @@ int cosa_gpu_profile(cosa_ctx *c, int32_t nl, int32_t niter, double ms[3], int64
   CK(cudaEventCreate(&t0));
   CK(cudaEventCreate(&t1));
   const int compute_dt = (1 / c->p.iupdt * c->p.iupdt == 1) ? 1 : 0;
+  if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, *L))) return r;
   cudaEventRecord(t0, c->s);
   for (int it = 0; it < niter && !r; ++it) r = launch_iteration(c, nl, *L, false, compute_dt);
   cudaEventRecord(t1, c->s);

@@ -26,6 +26,7 @@
 #include <cuda_pipeline.h>
 
 #include "physics.cuh"
+#include "kernels_ref.cuh"
 
 struct HaloItem {
   int dblk, sblk;   // destination / source block (0-based)
@@ -112,7 +113,7 @@ __global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__re
       if (mask & 1) q[base + it.h1] = h1[v];
       if (mask & 2) q[base + it.h2] = h2[v];
     }
-    if (it.idir == 1) {  // bprtest also checks the i halos (src/cosa.f90:1000)
+    if (CONS && it.idir == 1) {  // bprtest also checks the i halos of the state (src/cosa.f90:1000)
       if (mask & 1) { if (h1[4] <= P.qmin[4]) st |= COSA_ERR_NEG_P; else if (h1[0] <= P.qmin[0]) st |= COSA_ERR_NEG_RHO; }
       if (mask & 2) { if (h2[4] <= P.qmin[4]) st |= COSA_ERR_NEG_P; else if (h2[0] <= P.qmin[0]) st |= COSA_ERR_NEG_RHO; }
     }
@@ -131,6 +132,7 @@ struct StageArgs {
   double *part;          // per-tile residual sums of squares (npde) or null
   const double *rhs;     // multigrid forcing or null
   double *res_out;       // if set, the residual is stored here (P3 layout)
+  double *bx, *by, *bz;  // IRS coefficients written with the time step (irsop >= 2)
   const uint8_t *strong; // strong-boundary flags
   const StrongMap *smap; // per block
   int *status;
@@ -364,6 +366,11 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
         eig_eul(g, qc, sim, sip, sjm, sjp, skm, skp, li, lj, lk);
         dt = P.cfl / (li + lj + lk);
         A.dtvol[o1] = dt;
+        if (A.bx) {
+          double ba, bb_, bc;
+          irs_beta(P.irsop, P.rat, P.psirs, li, lj, lk, ba, bb_, bc);
+          A.bx[o1] = ba; A.by[o1] = bb_; A.bz[o1] = bc;
+        }
       } else {
         dt = A.dtvol[o1];
       }

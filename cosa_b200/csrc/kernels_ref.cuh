@@ -5,6 +5,30 @@
 #pragma once
 #include "physics.cuh"
 
+// IRS coefficients beta of bdeltat (src/cosa.f90:4882-5180), inviscid lambdas
+// (irsop 5/6 reduce to 2/3 when the viscous spectral radii are zero)
+__device__ __forceinline__ void irs_beta(int irsop, double rat, double psirs, double lami, double lamj, double lamk,
+                                         double &bx, double &by, double &bz) {
+  if (irsop == 2 || irsop == 5) {
+    const double zeta = 0.4;
+    const double phixi = 1 + pow(lamj / lami, zeta) + pow(lamk / lami, zeta);
+    const double phieta = 1 + pow(lami / lamj, zeta) + pow(lamk / lamj, zeta);
+    const double phizeta = 1 + pow(lami / lamk, zeta) + pow(lamj / lamk, zeta);
+    double tt;
+    tt = (rat * lami * phixi / (lami + lamj + lamk)); bx = fmax(0.0, (tt * tt - 1) / 4);
+    tt = (rat * lamj * phieta / (lami + lamj + lamk)); by = fmax(0.0, (tt * tt - 1) / 4);
+    tt = (rat * lamk * phizeta / (lami + lamj + lamk)); bz = fmax(0.0, (tt * tt - 1) / 4);
+  } else {
+    const double rji = lamj / lami, rki = lamk / lami, rij = lami / lamj;
+    const double rkj = lamk / lamj, rik = lami / lamk, rjk = lamj / lamk;
+    double tt;
+    tt = rat / (1 + psirs * (rji + rki)); bx = fmax(0.0, 0.25 * (tt * tt - 1));
+    tt = rat / (1 + psirs * (rij + rkj)); by = fmax(0.0, 0.25 * (tt * tt - 1));
+    tt = rat / (1 + psirs * (rik + rjk)); bz = fmax(0.0, 0.25 * (tt * tt - 1));
+  }
+}
+
+
 // ---- cons2prim_b (src/update.f90:2112-2188) ----------------------------------------
 __global__ void k_cons2prim(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ q, int xtnd) {
   const cosa_params &P = *Pp;
@@ -120,21 +144,10 @@ __global__ void k_deltat(DevBlock b, const cosa_params *__restrict__ Pp, double 
     const double lamk = lam[p3_var(b, npde, S, 3, n) + c];
     const int64_t o = p1_idx(b, S, i, j, k, n);
     dtv[o] = P.cfl / (lami + lamj + lamk);
-    if (P.irsop == 2 && bx) {
-      const double phixi = 1 + pow(lamj / lami, zeta) + pow(lamk / lami, zeta);
-      const double phieta = 1 + pow(lami / lamj, zeta) + pow(lamk / lamj, zeta);
-      const double phizeta = 1 + pow(lami / lamk, zeta) + pow(lamj / lamk, zeta);
-      double tt;
-      tt = (P.rat * lami * phixi / (lami + lamj + lamk)); bx[o] = fmax(0.0, (tt * tt - 1) / 4);
-      tt = (P.rat * lamj * phieta / (lami + lamj + lamk)); by[o] = fmax(0.0, (tt * tt - 1) / 4);
-      tt = (P.rat * lamk * phizeta / (lami + lamj + lamk)); bz[o] = fmax(0.0, (tt * tt - 1) / 4);
-    } else if (P.irsop == 3 && bx) {
-      const double rji = lamj / lami, rki = lamk / lami, rij = lami / lamj;
-      const double rkj = lamk / lamj, rik = lami / lamk, rjk = lamj / lamk;
-      double tt;
-      tt = P.rat / (1 + P.psirs * (rji + rki)); bx[o] = fmax(0.0, 0.25 * (tt * tt - 1));
-      tt = P.rat / (1 + P.psirs * (rij + rkj)); by[o] = fmax(0.0, 0.25 * (tt * tt - 1));
-      tt = P.rat / (1 + P.psirs * (rik + rjk)); bz[o] = fmax(0.0, 0.25 * (tt * tt - 1));
+    if (bx && P.irsop >= 2 && P.irsop != 4) {
+      double a, c2, d;
+      irs_beta(P.irsop, P.rat, P.psirs, lami, lamj, lamk, a, c2, d);
+      bx[o] = a; by[o] = c2; bz[o] = d;
     }
   }
 }
@@ -471,5 +484,132 @@ __global__ void k_vols(DevBlock b, const double *__restrict__ x, const double *_
     const double dy = (sface(1, Z, X, 2) + sface(2, Z, X, 2) + sface(3, Z, X, 2)) * (at(Y, i + 1, j + 1, k + 1) - at(Y, i, j, k));
     const double dz = (sface(1, X, Y, 3) + sface(2, X, Y, 3) + sface(3, X, Y, 3)) * (at(Z, i + 1, j + 1, k + 1) - at(Z, i, j, k));
     vol[b.op1 + i + I1 * (j + J1 * (int64_t)k)] = (dx + dy + dz) / 3;
+  }
+}
+
+// ---- implicit residual smoothing (src/cosa.f90:2035-2443, 5206-5773) -------------
+// scalef_b / scaleb_b (src/cosa.f90:5652-5773): res *= or /= dt/V
+__global__ void k_irs_scale(DevBlock b, int npde, int S, double *__restrict__ res, const double *__restrict__ dtv,
+                            const double *__restrict__ dtvt, int forward) {
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t n = (int64_t)ni * nj * nk * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)(r % nk) + 1; r /= nk;
+    const int s = (int)r;
+    const int64_t c = p3_cell(b, i, j, k), o = p1_idx(b, S, i, j, k, s);
+    const double d = dtv[o], dt2 = dtvt ? dtvt[o] : d;
+    for (int v = 1; v <= npde; ++v) {
+      if (v >= 6 && !dtvt) continue;
+      const double f = v >= 6 ? dt2 : d;
+      double &x = res[p3_var(b, npde, S, v, s) + c];
+      x = forward ? x * f : x / f;
+    }
+  }
+}
+
+// One direction D of cirs_b / ccirs_b: a thread solves every variable vs..ve
+// of one grid line with tridi (src/cosa.f90:2418-2443).  The line's pivots
+// den(m) = b(m) - r(m-1) a(m) and ratios r(m) depend only on the coefficients,
+// so they are computed once into `scr` (2 doubles per cell) and reused for
+// each variable.  ores (if set) is the right-hand side of the i sweep of the
+// cut variant; with_halo adds eps * res(halo) on the first and last rows.
+template <int D>
+__global__ void k_irs_line(DevBlock b, int npde, int S, double *__restrict__ res, const double *__restrict__ ores,
+                           const double *__restrict__ beta, double eps, int vs, int ve, int with_halo,
+                           double *__restrict__ scr) {
+  const int im = b.im - 1, jm = b.jm - 1, km = b.km - 1;
+  const int len = D == 1 ? im : (D == 2 ? jm : km);
+  const int n2 = D == 1 ? jm : im, n3 = D == 3 ? jm : km;
+  const int64_t nlines = (int64_t)n2 * n3 * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nlines; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r_ = t;
+    const int t2 = (int)(r_ % n2) + 1; r_ /= n2;
+    const int t3 = (int)(r_ % n3) + 1; r_ /= n3;
+    const int s = (int)r_;
+    auto ijk = [&](int m, int &i, int &j, int &k) {
+      if (D == 1) { i = m; j = t2; k = t3; }
+      else if (D == 2) { i = t2; j = m; k = t3; }
+      else { i = t2; j = t3; k = m; }
+    };
+    auto coef = [&](int m) {
+      int i, j, k;
+      ijk(m, i, j, k);
+      return beta ? beta[p1_idx(b, S, i, j, k, s)] : eps;
+    };
+    // pivots
+    double rprev = 0.0;
+    for (int m = 1; m <= len; ++m) {
+      int i, j, k;
+      ijk(m, i, j, k);
+      const double e = coef(m);
+      const double a = m == 1 ? 0.0 : -e, bb = 1 + 2 * e, c = m == len ? 0.0 : -e;
+      const double den = m == 1 ? bb : bb - rprev * a;
+      const double rr = c / den;
+      const int64_t o = 2 * (b.op3 * S + (int64_t)s * b.P3 + p3_cell(b, i, j, k));
+      scr[o] = rr;
+      scr[o + 1] = den;
+      rprev = rr;
+    }
+    for (int v = vs; v <= ve; ++v) {
+      const int64_t base = p3_var(b, npde, S, v, s);
+      const double *src = ores ? ores + base : res + base;
+      double *x = res + base;
+      double tprev = 0.0;
+      for (int m = 1; m <= len; ++m) {
+        int i, j, k;
+        ijk(m, i, j, k);
+        const int64_t c = p3_cell(b, i, j, k);
+        const double e = coef(m);
+        double rhs = src[c];
+        if (with_halo && (m == 1 || m == len)) {
+          // the last-row assignment wins on a single-cell line, as in ccirs_b
+          int hi, hj, hk;
+          ijk(m == len ? len + 1 : 0, hi, hj, hk);
+          rhs = src[c] + e * x[p3_cell(b, hi, hj, hk)];
+        }
+        const double a = m == 1 ? 0.0 : -e;
+        const int64_t o = 2 * (b.op3 * S + (int64_t)s * b.P3 + c);
+        const double tt = m == 1 ? rhs / scr[o + 1] : (rhs - tprev * a) / scr[o + 1];
+        x[c] = tt;
+        tprev = tt;
+      }
+      double xnext = tprev;
+      for (int m = len - 1; m >= 1; --m) {
+        int i, j, k;
+        ijk(m, i, j, k);
+        const int64_t c = p3_cell(b, i, j, k);
+        const int64_t o = 2 * (b.op3 * S + (int64_t)s * b.P3 + c);
+        const double xm = x[c] - xnext * scr[o];
+        x[c] = xm;
+        xnext = xm;
+      }
+    }
+  }
+}
+
+// RK update of the stage from a stored residual (IRS path):
+// q_out = q^n - alpha dt/V R, optional copy of q^n (stage 1)
+__global__ void k_update_stage(DevBlock b, int npde, int S, const double *__restrict__ res,
+                               const double *__restrict__ qold, double *__restrict__ qout, double *__restrict__ qcopy,
+                               const double *__restrict__ dtv, double ar) {
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t n = (int64_t)ni * nj * nk * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)(r % nk) + 1; r /= nk;
+    const int s = (int)r;
+    const int64_t c = p3_cell(b, i, j, k);
+    const double dt = dtv[p1_idx(b, S, i, j, k, s)];
+    for (int v = 1; v <= 5; ++v) {
+      const int64_t o = p3_var(b, npde, S, v, s) + c;
+      const double q0 = qold[o];
+      if (qcopy) qcopy[o] = q0;
+      qout[o] = q0 - ar * res[o] * dt;
+    }
   }
 }

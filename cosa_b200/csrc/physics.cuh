@@ -191,7 +191,7 @@ __device__ __forceinline__ void roe_flux_fp64(const PhysPar &P, double kx, doubl
 // reciprocal of rhols + rhors (a last-bit difference from the divisions).
 __device__ __forceinline__ void roe_flux_euler(const PhysPar &P, double kx, double ky, double kz, double ds,
                                                const double *qr, const double *ql, double *flux) {
-  const double g = P.g, g_gm1 = P.g_gm1, gm1 = P.gm1;
+  const double g_gm1 = P.g_gm1, gm1 = P.gm1;
   const double rhor = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
   const double unr = ur * kx + vr * ky + wr * kz;
   const double q2r = ur * ur + vr * vr + wr * wr;

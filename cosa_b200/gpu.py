@@ -53,7 +53,7 @@ SYMBOLS = [
     "cosa_gpu_muscl", "cosa_gpu_roflux", "cosa_gpu_resid", "cosa_gpu_update", "cosa_gpu_resg_rms",
     "cosa_gpu_zero", "cosa_gpu_smooth", "cosa_gpu_smooth_host", "cosa_gpu_launch_count",
     "cosa_gpu_status", "cosa_gpu_imetrix", "cosa_gpu_vols", "cosa_gpu_profile", "cosa_gpu_stream",
-    "cosa_gpu_resg_rms_noalloc",
+    "cosa_gpu_resg_rms_noalloc", "cosa_gpu_scalef", "cosa_gpu_scaleb", "cosa_gpu_cirs", "cosa_gpu_ccirs",
 ]
 
 
@@ -232,6 +232,22 @@ class Context:
         self._check(load().cosa_gpu_resg_rms(self.h, nl, _ptr(res.ptr), _ptr(rhs.ptr if rhs else None),
                                              out.ctypes.data_as(_dp)), "resg_rms")
         return out
+
+    def scalef(self, nl, res, dtvol, dtvolt=None):
+        self._check(load().cosa_gpu_scalef(self.h, nl, _ptr(res.ptr), _ptr(dtvol.ptr),
+                                           _ptr(dtvolt.ptr if dtvolt else None)), "scalef")
+
+    def scaleb(self, nl, res, dtvol, dtvolt=None):
+        self._check(load().cosa_gpu_scaleb(self.h, nl, _ptr(res.ptr), _ptr(dtvol.ptr),
+                                           _ptr(dtvolt.ptr if dtvolt else None)), "scaleb")
+
+    def cirs(self, nl, res, dtvol, bx=None, by=None, bz=None):
+        self._check(load().cosa_gpu_cirs(self.h, nl, _ptr(res.ptr), _ptr(dtvol.ptr), _ptr(bx.ptr if bx else None),
+                                         _ptr(by.ptr if by else None), _ptr(bz.ptr if bz else None)), "cirs")
+
+    def ccirs(self, nl, res, ores, bx=None, by=None, bz=None):
+        self._check(load().cosa_gpu_ccirs(self.h, nl, _ptr(res.ptr), _ptr(ores.ptr), _ptr(bx.ptr if bx else None),
+                                          _ptr(by.ptr if by else None), _ptr(bz.ptr if bz else None)), "ccirs")
 
     def imetrix(self, nl, x, y, z, si, sj, sk):
         self._check(load().cosa_gpu_imetrix(self.h, nl, _ptr(x.ptr), _ptr(y.ptr), _ptr(z.ptr), _ptr(si.ptr),

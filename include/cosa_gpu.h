@@ -187,6 +187,22 @@ int cosa_gpu_resg_rms(cosa_ctx *ctx, int32_t nl, const double *res,
 /* zero (src/util.f90) of a P3 array including halo layer `ext` */
 int cosa_gpu_zero(cosa_ctx *ctx, int32_t nl, double *a);
 
+/* scalef / scaleb (src/cosa.f90:5626-5773): res *= / res /= dt/V (dtvolt
+   for the turbulence equations when npde = 7) */
+int cosa_gpu_scalef(cosa_ctx *ctx, int32_t nl, double *res, const double *dtvol,
+                    const double *dtvolt);
+int cosa_gpu_scaleb(cosa_ctx *ctx, int32_t nl, double *res, const double *dtvol,
+                    const double *dtvolt);
+/* cirs (src/cosa.f90:5206-5623): central implicit residual smoothing with
+   constant (irsop 1) or per-cell (irsop 2,3,5,6) coefficients, including
+   the scaling by dt/V; Thomas sweeps in i, j, k */
+int cosa_gpu_cirs(cosa_ctx *ctx, int32_t nl, double *res, const double *dtvol,
+                  const double *betaxi, const double *betaeta, const double *betazeta);
+/* ccirs (src/cosa.f90:2035-2443): the cut-aware sweeps (right-hand side of
+   the i sweep from ores, halo values of res on the boundary rows); called by
+   smooth() twice after cutman_q on res, between scalef and scaleb */
+int cosa_gpu_ccirs(cosa_ctx *ctx, int32_t nl, double *res, const double *ores,
+                   const double *betaxi, const double *betaeta, const double *betazeta);
 /* imetrix (src/grid.f90:820-1255): face unit normals and areas into si/sj/sk
    (lmet = 4) from the grid x,y,z; fixed grids */
 int cosa_gpu_imetrix(cosa_ctx *ctx, int32_t nl, const double *x, const double *y,

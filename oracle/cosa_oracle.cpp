@@ -673,7 +673,7 @@ void deltat_level(const Level &L, double *dtv, const double *lam, double *bx_, d
         for (int j = 1; j <= L.jm[b] - 1; ++j)
           for (int i = 1; i <= L.im[b] - 1; ++i) {
             double lami = lm(i, j, k, 1, n), lamj = lm(i, j, k, 2, n), lamk = lm(i, j, k, 3, n);
-            if (P.irsop == 2) {
+            if (P.irsop == 2 || P.irsop == 5) {
               double phixi = 1 + std::pow(lamj / lami, zeta) + std::pow(lamk / lami, zeta);
               double phieta = 1 + std::pow(lami / lamj, zeta) + std::pow(lamk / lamj, zeta);
               double phizeta = 1 + std::pow(lami / lamk, zeta) + std::pow(lamj / lamk, zeta);
@@ -684,7 +684,7 @@ void deltat_level(const Level &L, double *dtv, const double *lam, double *bx_, d
               by(i, j, k, n) = std::max(0.0, (t * t - 1) / 4);
               t = (rat * lamk * phizeta / (lami + lamj + lamk));
               bz(i, j, k, n) = std::max(0.0, (t * t - 1) / 4);
-            } else if (P.irsop == 3) {
+            } else if (P.irsop == 3 || P.irsop == 6) {
               double rji = lamj / lami, rki = lamk / lami, rij = lami / lamj;
               double rkj = lamk / lamj, rik = lami / lamk, rjk = lamj / lamk;
               double t;
@@ -965,6 +965,132 @@ void update_b(const Level &L, int b, double *ra, double *qa, double *qoa, double
             q(i, j, k, v, n) = qold(i, j, k, v, n) - ar * res(i, j, k, v, n) * dt(i, j, k, n);
 }
 
+
+// ---- implicit residual smoothing (src/cosa.f90:2035-2443, 5206-5773) -------
+// tridi (src/cosa.f90:2418-2443): Thomas algorithm, x overwritten by the solution
+void tridi(const double *a, const double *b, const double *c, double *x, int dim) {
+  std::vector<double> r(dim + 1), t(dim + 1);
+  if (dim == 1) { x[0] = x[0] / b[0]; return; }
+  r[0] = c[0] / b[0];
+  t[0] = x[0] / b[0];
+  for (int j = 1; j < dim - 1; ++j) {
+    r[j] = c[j] / (b[j] - r[j - 1] * a[j]);
+    t[j] = (x[j] - t[j - 1] * a[j]) / (b[j] - r[j - 1] * a[j]);
+  }
+  t[dim - 1] = (x[dim - 1] - t[dim - 2] * a[dim - 1]) / (b[dim - 1] - r[dim - 2] * a[dim - 1]);
+  x[dim - 1] = t[dim - 1];
+  for (int j = dim - 2; j >= 0; --j) x[j] = t[j] - x[j + 1] * r[j];
+}
+
+// one direction of cirs_b / ccirs_b for variables vs..ve: line solves with
+// coefficient eps (irsop 1) or beta(i,j,k) (irsop >= 2); for the cut
+// variant (rhs_src = ores for d = 1) the boundary rows take eps * halo.
+void irs_dir(const Level &L, int b, int d, double *ra, const double *rhs_src, const double *beta_a,
+             double epsc, int vs, int ve, bool with_halo) {
+  B3 res(ra, L, b);
+  B3 src(const_cast<double *>(rhs_src ? rhs_src : ra), L, b);
+  const int im = L.im[b] - 1, jm = L.jm[b] - 1, km = L.km[b] - 1;
+  const int len = d == 1 ? im : (d == 2 ? jm : km);
+  const int n2 = d == 1 ? jm : im, n3 = d == 3 ? jm : km;
+  std::vector<double> A(len), Bv(len), Cv(len), X(len);
+  for (int n = 0; n < L.S; ++n)
+    for (int v = vs; v <= ve; ++v)
+      for (int t3 = 1; t3 <= n3; ++t3)
+        for (int t2 = 1; t2 <= n2; ++t2) {
+          auto at = [&](int m, int &i, int &j, int &k) {
+            if (d == 1) { i = m; j = t2; k = t3; }
+            else if (d == 2) { i = t2; j = m; k = t3; }
+            else { i = t2; j = t3; k = m; }
+          };
+          for (int m = 1; m <= len; ++m) {
+            int i, j, k;
+            at(m, i, j, k);
+            double e = epsc;
+            if (beta_a) { B1 bt(const_cast<double *>(beta_a), L, b, L.S); e = bt(i, j, k, n); }
+            A[m - 1] = m == 1 ? 0 : -e;
+            Bv[m - 1] = 1 + 2 * e;
+            Cv[m - 1] = m == len ? 0 : -e;
+            X[m - 1] = src(i, j, k, v, n);
+            if (with_halo && m == 1) {
+              int hi, hj, hk; at(0, hi, hj, hk);
+              X[0] = src(i, j, k, v, n) + e * res(hi, hj, hk, v, n);
+            }
+            if (with_halo && m == len) {
+              int hi, hj, hk; at(len + 1, hi, hj, hk);
+              X[len - 1] = src(i, j, k, v, n) + e * res(hi, hj, hk, v, n);
+            }
+          }
+          tridi(A.data(), Bv.data(), Cv.data(), X.data(), len);
+          for (int m = 1; m <= len; ++m) {
+            int i, j, k;
+            at(m, i, j, k);
+            res(i, j, k, v, n) = X[m - 1];
+          }
+        }
+}
+
+// scalef_b / scaleb_b (src/cosa.f90:5652-5773): res *= or /= dtvol (dtvolt for k-omega)
+void scale_res(const Level &L, double *ra, const double *dtv, const double *dtvt, bool forward, const cosa_params &P) {
+  for (int b = 0; b < L.nb; ++b) {
+    B3 res(ra, L, b);
+    B1 dt(const_cast<double *>(dtv), L, b, L.S);
+    for (int n = 0; n < L.S; ++n)
+      for (int v = 1; v <= L.npde; ++v) {
+        const bool turb = v >= 6;
+        if (turb && !dtvt) continue;
+        B1 dtt(const_cast<double *>(turb ? dtvt : dtv), L, b, L.S);
+        for (int k = 1; k <= L.km[b] - 1; ++k)
+          for (int j = 1; j <= L.jm[b] - 1; ++j)
+            for (int i = 1; i <= L.im[b] - 1; ++i)
+              res(i, j, k, v, n) = forward ? res(i, j, k, v, n) * dtt(i, j, k, n) : res(i, j, k, v, n) / dtt(i, j, k, n);
+      }
+  }
+}
+
+// cirs (cutcirs = 0) and the ccirs loop (cutcirs = 1) of smooth()
+// (src/cosa.f90:1977-1998)
+void irs_level(const Level &L, double *res, const double *dtv, const double *dtvt, const double *bx,
+               const double *by, const double *bz, const double *tbx, const double *tby, const double *tbz,
+               const cosa_params &P) {
+  const double epsc = 0.25 * (P.rat * P.rat - 1.0);
+  const bool kom = is_kom(P);
+  const double *bet[4] = {nullptr, bx, by, bz}, *tbet[4] = {nullptr, tbx, tby, tbz};
+  auto sweep3 = [&](double *r, const double *ores, bool with_halo) {
+    for (int b = 0; b < L.nb; ++b)
+      for (int d = 1; d <= 3; ++d) {
+        const double *src = (d == 1) ? ores : nullptr;
+        if (P.irsop == 1) {
+          irs_dir(L, b, d, r, src, nullptr, epsc, 1, L.npde, with_halo);
+        } else {
+          irs_dir(L, b, d, r, src, bet[d], 0.0, 1, 5, with_halo);
+          if (kom) irs_dir(L, b, d, r, src, tbet[d], 0.0, 6, L.npde, with_halo);
+        }
+      }
+  };
+  if (P.cutcirs == 0) {
+    scale_res(L, res, dtv, kom ? dtvt : nullptr, true, P);
+    // cirs_b does i, j, k per block with the residual itself as right-hand side
+    for (int b = 0; b < L.nb; ++b)
+      for (int d = 1; d <= 3; ++d) {
+        if (P.irsop == 1) irs_dir(L, b, d, res, nullptr, nullptr, epsc, 1, L.npde, false);
+        else {
+          irs_dir(L, b, d, res, nullptr, bet[d], 0.0, 1, 5, false);
+          if (kom) irs_dir(L, b, d, res, nullptr, tbet[d], 0.0, 6, L.npde, false);
+        }
+      }
+    scale_res(L, res, dtv, kom ? dtvt : nullptr, false, P);
+  } else {
+    scale_res(L, res, dtv, kom ? dtvt : nullptr, true, P);
+    // work1 = res over 0..imax (copy_array extent 1)
+    std::vector<double> ores(res, res + L.n3 * L.npde * L.S);
+    for (int its = 0; its < 2; ++its) {
+      cutman_q_level(L, res);
+      sweep3(res, ores.data(), true);
+    }
+    scale_res(L, res, dtv, kom ? dtvt : nullptr, false, P);
+  }
+}
+
 // ---- resg_brms (src/cosa.f90:4503-4582), explicit steady branch ------------
 void resg_rms_level(const Level &L, double *ra, double *rha, double *out) {
   double acc[8] = {0};
@@ -1188,9 +1314,22 @@ void orc_roe_face(const cosa_params *p, const double *nrm, const double *qr, con
  * 1721-1908), leaving res (conservative residual), q back in conservative
  * form, and lambdas/dtvol when want_dt.  Work arrays are caller-owned P3/F0.
  */
+int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
+                  const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
+                  double *dqp, double *dqm, double *flux, double *dtvol, int want_dt, double *bx, double *by,
+                  double *bz);
+
 int orc_residual(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
                  const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
                  double *dqp, double *dqm, double *flux, double *dtvol, int want_dt) {
+  return residual_impl(h, p, nl, q, si, sj, sk, res, qp, qm, dq, dqp, dqm, flux, dtvol, want_dt, nullptr, nullptr,
+                       nullptr);
+}
+
+int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
+                  const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
+                  double *dqp, double *dqm, double *flux, double *dtvol, int want_dt, double *bx, double *by,
+                  double *bz) {
   Level &L = h->L;
   for (int b = 0; b < L.nb; ++b) cons2prim_b(L, b, q, 0, *p);
   int status = bc_level(L, q, si, sj, sk, *p);
@@ -1198,7 +1337,7 @@ int orc_residual(orc_level *h, const cosa_params *p, int nl, double *q, const do
   status |= prtest_level(L, q, *p);
   if (want_dt) {
     lambda_level(L, q, si, sj, sk, qp, *p);
-    deltat_level(L, dtvol, qp, nullptr, nullptr, nullptr, *p);
+    deltat_level(L, dtvol, qp, bx, by, bz, *p);
   }
   zero_res(L, res);
   const double *sd[4] = {nullptr, si, sj, sk};
@@ -1220,10 +1359,16 @@ int orc_residual(orc_level *h, const cosa_params *p, int nl, double *q, const do
  * cycles.  hist receives, for cycles with (mgit==1 || mgit%rms_every==0 ||
  * mgit==last), the stage-1 resrms(1..npde+1) at row (mgit-mgit0).
  */
+int orc_smooth_irs(orc_level *h, const cosa_params *p, int ncycles, int mgit0, int rms_every, double *q,
+                   double *qold, const double *si, const double *sj, const double *sk, double *res,
+                   double *rhs, double *qp, double *qm, double *dq, double *dqp, double *dqm, double *flux,
+                   double *dtvol, double *bx, double *by, double *bz, double *hist);
+
 int orc_smooth(orc_level *h, const cosa_params *p, int ncycles, int mgit0, int rms_every, double *q,
                double *qold, const double *si, const double *sj, const double *sk, double *res,
                double *rhs, double *qp, double *qm, double *dq, double *dqp, double *dqm, double *flux,
                double *dtvol, double *hist) {
+  if (p->irsop > 0) return -1;
   Level &L = h->L;
   int status = 0;
   const int last = mgit0 + ncycles - 1;
@@ -1242,5 +1387,34 @@ int orc_smooth(orc_level *h, const cosa_params *p, int ncycles, int mgit0, int r
   }
   return status;
 }
+
+int orc_smooth_irs(orc_level *h, const cosa_params *p, int ncycles, int mgit0, int rms_every, double *q,
+                   double *qold, const double *si, const double *sj, const double *sk, double *res,
+                   double *rhs, double *qp, double *qm, double *dq, double *dqp, double *dqm, double *flux,
+                   double *dtvol, double *bx, double *by, double *bz, double *hist) {
+  Level &L = h->L;
+  int status = 0;
+  const int last = mgit0 + ncycles - 1;
+  for (int mgit = mgit0; mgit <= last; ++mgit) {
+    const int iter = 1;
+    copy_interior(L, qold, q);
+    for (int irk = 1; irk <= p->nstage; ++irk) {
+      const bool want_dt = (iter / p->iupdt * p->iupdt == iter) && irk == 1;
+      status |= residual_impl(h, p, 1, q, si, sj, sk, res, qp, qm, dq, dqp, dqm, flux, dtvol, want_dt, bx, by, bz);
+      if (irk == 1 && (mgit == 1 || mgit % rms_every == 0 || mgit == last) && hist)
+        resg_rms_level(L, res, rhs, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
+      if (p->irsop > 0) irs_level(L, res, dtvol, nullptr, bx, by, bz, nullptr, nullptr, nullptr, *p);
+#pragma omp parallel for schedule(dynamic)
+      for (int b = 0; b < L.nb; ++b) update_b(L, b, res, q, qold, dtvol, p->alphas[irk - 1]);
+    }
+  }
+  return status;
+}
+
+void orc_irs(orc_level *h, const cosa_params *p, double *res, const double *dtvol, const double *bx,
+             const double *by, const double *bz) {
+  irs_level(h->L, res, dtvol, nullptr, bx, by, bz, nullptr, nullptr, nullptr, *p);
+}
+void orc_tridi(const double *a, const double *b, const double *c, double *x, int dim) { tridi(a, b, c, x, dim); }
 
 }  // extern "C"

@@ -171,6 +171,32 @@ class OracleLevel:
         return hist, st
 
 
+def smooth_irs(O, q, si, sj, sk, ncycles, mgit0=1, rms_every=1):
+    """Single-level cycles with implicit residual smoothing (irsop > 0)."""
+    qold = O.p3()
+    res, rhs = O.p3(), O.p3()
+    qp, qm, dq, dqp, dqm = (O.p3() for _ in range(5))
+    flux = O.f0()
+    dtvol = O.p1(O.S)
+    bx, by, bz = (O.p1(O.S) for _ in range(3))
+    hist = np.full((ncycles, O.p.npde + 1), np.nan)
+    st = lib().orc_smooth_irs(O.h, _par(O.p), C.c_int(ncycles), C.c_int(mgit0), C.c_int(rms_every),
+                              _p(q), _p(qold), _p(si), _p(sj), _p(sk), _p(res), _p(rhs), _p(qp), _p(qm),
+                              _p(dq), _p(dqp), _p(dqm), _p(flux), _p(dtvol), _p(bx), _p(by), _p(bz), _p(hist))
+    return hist, st, dtvol, (bx, by, bz)
+
+
+def irs(O, res, dtvol, bx, by, bz):
+    lib().orc_irs(O.h, _par(O.p), _p(res), _p(dtvol), _p(bx), _p(by), _p(bz))
+
+
+def tridi(a, b, c, x):
+    x = np.ascontiguousarray(x, dtype=np.float64).copy()
+    lib().orc_tridi(_p(np.ascontiguousarray(a, dtype=np.float64)), _p(np.ascontiguousarray(b, dtype=np.float64)),
+                    _p(np.ascontiguousarray(c, dtype=np.float64)), _p(x), C.c_int(len(x)))
+    return x
+
+
 def roe_face(params, nrm, qr, ql):
     f = np.zeros(5)
     n = np.ascontiguousarray(nrm, dtype=np.float64)
