@@ -255,12 +255,14 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d) {
   const int S = 2 * c->p.nharms + 1;
   const int kc = 32;
   L.kchunk = kc;
+  // snapshots innermost: the S tiles of one region run together, so the
+  // harmonic-balance coupling re-reads the other snapshots from L2
   for (int b = 0; b < L.nb; ++b) {
     const DevBlock &x = L.hb[b];
-    for (int n = 0; n < S; ++n)
-      for (int k0 = 1; k0 <= x.km - 1; k0 += kc)
-        for (int j0 = 1; j0 <= x.jm - 1; j0 += kTJ)
-          for (int i0 = 1; i0 <= x.im - 1; i0 += kTI)
+    for (int k0 = 1; k0 <= x.km - 1; k0 += kc)
+      for (int j0 = 1; j0 <= x.jm - 1; j0 += kTJ)
+        for (int i0 = 1; i0 <= x.im - 1; i0 += kTI)
+          for (int n = 0; n < S; ++n)
             tiles.push_back(Tile{b, n, i0, j0, k0, std::min(k0 + kc - 1, x.km - 1)});
   }
   L.ntiles = (int)tiles.size();
@@ -323,7 +325,7 @@ int set_smem_attrs() {
 }
 
 int check_fused_supported(const cosa_params &p) {
-  if (p.npde != 5 || p.viscous || p.kom || p.kom_bsl || p.kom_sst || p.harbal || p.rkimp || p.moving ||
+  if (p.npde != 5 || p.viscous || p.kom || p.kom_bsl || p.kom_sst || p.rkimp || p.moving ||
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
   return COSA_OK;
@@ -441,6 +443,7 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   }
   A.strong = L.d_strong; A.smap = L.d_smap; A.status = c->d_status;
   A.ar = p.alphas[irk - 1];
+  A.vol = p.harbal ? P.vol : nullptr;
   A.compute_dt = compute_dt;
   A.first_order = nl >= p.nl_crs;
   A.update = update;
@@ -456,7 +459,9 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   if (want_rms) {
     int64_t ncell = 0;
     for (auto &b : L.hb) ncell += (int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1);
-    k_rms_final<<<1, 256, 0, c->s>>>(L.d_part, L.ntiles, p.npde, (double)ncell, c->d_hist, c->d_row, c->hist_cap);
+    // resg_rms_hb averages over the snapshots as well (src/cosa.f90:4620-4626)
+    const double cnt = (double)ncell * (p.harbal ? (2 * p.nharms + 1) : 1);
+    k_rms_final<<<1, 256, 0, c->s>>>(L.d_part, L.ntiles, p.npde, cnt, c->d_hist, c->d_row, c->hist_cap);
     r = after_launch(c);
     if (r) return r;
   }
@@ -804,6 +809,7 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
   if (r) return r;
   const cosa_level_ptrs &P = L->ptrs;
   if (!P.q || !P.qold || !P.dtvol || !P.si || !P.sj || !P.sk) return COSA_ERR_ARG;
+  if (c->p.harbal && !P.vol) return COSA_ERR_ARG;
   cudaSetDevice(c->device);
   const int npde = c->p.npde;
   // schedule of printed iterations (src/cosa.f90:1925-1927)
@@ -871,6 +877,14 @@ int cosa_gpu_smooth_host(cosa_ctx *c, int32_t nl, double *q_host, int32_t niter,
   r = cosa_gpu_smooth(c, nl, niter, mgit0, rms_every, hist);
   int r2 = cosa_gpu_memcpy_d2h(c, q_host, L->ptrs.q, n);
   return r ? r : r2;
+}
+
+int cosa_gpu_src_hb(cosa_ctx *c, int32_t nl, const double *q, const double *vol, double *res) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !vol || !res) return COSA_ERR_ARG;
+  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+    k_src_hb<<<g, 256, 0, c->s>>>(b, c->d_p, q, vol, res);
+  });
 }
 
 int cosa_gpu_scalef(cosa_ctx *c, int32_t nl, double *res, const double *dtvol, const double *dtvolt) {

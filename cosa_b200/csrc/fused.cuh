@@ -133,6 +133,7 @@ struct StageArgs {
   const double *rhs;     // multigrid forcing or null
   double *res_out;       // if set, the residual is stored here (P3 layout)
   double *bx, *by, *bz;  // IRS coefficients written with the time step (irsop >= 2)
+  const double *vol;     // cell volumes when the harmonic-balance source is on
   const uint8_t *strong; // strong-boundary flags
   const StrongMap *smap; // per block
   int *status;
@@ -382,6 +383,14 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
         double r = fi[(m * TJ + tj) * (TI + 1) + ti + 1] - fi[(m * TJ + tj) * (TI + 1) + ti];
         r = r + fj[(m * (TJ + 1) + tj + 1) * TI + ti] - fj[(m * (TJ + 1) + tj) * TI + ti];
         r = r + fk_hi[m] - fk_lo[m];
+        if (A.vol) {
+          // src_bhb (src/src.f90:556-613): harmonic-balance coupling of the snapshots
+          const double ov = P.omega * A.vol[p1_idx(b, 1, ci, cj, k, 0)];
+          double qhb = 0.0;
+          for (int nj2 = 0; nj2 < S; ++nj2)
+            qhb = qhb + ov * P.dhb[n * S + nj2] * A.qin[p3_var(b, npde, S, m + 1, nj2) + cell];
+          r = r + qhb;
+        }
         if (A.res_out) A.res_out[p3_var(b, npde, S, m + 1, n) + cell] = r;
         if (A.part) {
           const double rr = r - (A.rhs ? A.rhs[p3_var(b, npde, S, m + 1, n) + cell] : 0.0);

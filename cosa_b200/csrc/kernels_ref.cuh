@@ -613,3 +613,29 @@ __global__ void k_update_stage(DevBlock b, int npde, int S, const double *__rest
     }
   }
 }
+
+// ---- src_bhb (src/src.f90:556-613): res(n) += sum_m omega V D(n,m) q(m) -------------
+__global__ void k_src_hb(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
+                         const double *__restrict__ vol, double *__restrict__ res) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t n = (int64_t)ni * nj * nk * npde;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)(r % nk) + 1; r /= nk;
+    const int v = (int)r + 1;
+    const int64_t c = p3_cell(b, i, j, k);
+    const double ov = P.omega * vol[p1_idx(b, 1, i, j, k, 0)];
+    double qs[COSA_MAX_SNAP];
+    for (int m = 0; m < S; ++m) qs[m] = q[p3_var(b, npde, S, v, m) + c];
+    for (int s = 0; s < S; ++s) {
+      double qhb = 0.0;
+      for (int m = 0; m < S; ++m) qhb = qhb + ov * P.dhb[s * S + m] * qs[m];
+      double &x = res[p3_var(b, npde, S, v, s) + c];
+      x = x + qhb;
+    }
+  }
+}

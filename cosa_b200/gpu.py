@@ -54,6 +54,7 @@ SYMBOLS = [
     "cosa_gpu_zero", "cosa_gpu_smooth", "cosa_gpu_smooth_host", "cosa_gpu_launch_count",
     "cosa_gpu_status", "cosa_gpu_imetrix", "cosa_gpu_vols", "cosa_gpu_profile", "cosa_gpu_stream",
     "cosa_gpu_resg_rms_noalloc", "cosa_gpu_scalef", "cosa_gpu_scaleb", "cosa_gpu_cirs", "cosa_gpu_ccirs",
+    "cosa_gpu_src_hb",
 ]
 
 
@@ -232,6 +233,9 @@ class Context:
         self._check(load().cosa_gpu_resg_rms(self.h, nl, _ptr(res.ptr), _ptr(rhs.ptr if rhs else None),
                                              out.ctypes.data_as(_dp)), "resg_rms")
         return out
+
+    def src_hb(self, nl, q, vol, res):
+        self._check(load().cosa_gpu_src_hb(self.h, nl, _ptr(q.ptr), _ptr(vol.ptr), _ptr(res.ptr)), "src_hb")
 
     def scalef(self, nl, res, dtvol, dtvolt=None):
         self._check(load().cosa_gpu_scalef(self.h, nl, _ptr(res.ptr), _ptr(dtvol.ptr),

@@ -12,6 +12,8 @@ from __future__ import annotations
 import ctypes as C
 import math
 
+import numpy as np
+
 MAX_SNAP = 15
 
 PREC_FP64 = 0
@@ -120,6 +122,63 @@ def subsonic_inlet_total_state(gamma: float, mach: float):
     t0 = 1.0 + 0.5 * (gamma - 1.0) * mach * mach
     p0 = (1.0 / gamma) * t0 ** (gamma / (gamma - 1.0))
     return t0, p0
+
+
+def hb_matrix(nharms: int, omega: float) -> np.ndarray:
+    """Time-spectral operator D = E^-1 A E of mathb (src/input.f90:5206-5284)
+    on the 2*nharms+1 equispaced instants zeit(n) = n * 2 pi / omega / S
+    (src/input.f90:3180-3193); D @ u(t_n) is d/dt u at the instants for
+    every Fourier mode up to nharms."""
+    S = 2 * nharms + 1
+    dt = 2 * math.pi / omega / S
+    zeit = [n * dt for n in range(S)]
+    ahb = np.zeros((S, S)); eihb = np.zeros((S, S)); ehb = np.zeros((S, S))
+    for i in range(1, nharms + 1):
+        ahb[2 * (i - 1) + 1, 2 * (i - 1) + 2] = i
+        ahb[2 * (i - 1) + 2, 2 * (i - 1) + 1] = -i
+    for i in range(S):
+        eihb[i, 0] = 1.0
+    for j in range(1, nharms + 1):
+        for i in range(S):
+            eihb[i, 2 * (j - 1) + 1] = math.cos(j * omega * zeit[i])
+            eihb[i, 2 * (j - 1) + 2] = math.sin(j * omega * zeit[i])
+    fact = 2.0 / S
+    for j in range(S):
+        ehb[0, j] = fact / 2
+    for i in range(1, nharms + 1):
+        for j in range(S):
+            ehb[2 * (i - 1) + 1, j] = fact * math.cos(i * omega * zeit[j])
+            ehb[2 * (i - 1) + 2, j] = fact * math.sin(i * omega * zeit[j])
+    # the reference accumulates the two products with explicit k loops
+    t = np.zeros((S, S))
+    for i in range(S):
+        for j in range(S):
+            acc = 0.0
+            for k in range(S):
+                acc = acc + ahb[i, k] * ehb[k, j]
+            t[i, j] = acc
+    d = np.zeros((S, S))
+    for i in range(S):
+        for j in range(S):
+            acc = 0.0
+            for k in range(S):
+                acc = acc + eihb[i, k] * t[k, j]
+            d[i, j] = acc
+    return d
+
+
+def set_harmonic_balance(p: CosaParams, nharms: int, omega: float) -> CosaParams:
+    """Switch p to harmonic balance with nharms harmonics at frequency omega
+    (rad per unit time): S = 2 nharms + 1 snapshots and D in p.dhb."""
+    p.harbal = 1
+    p.nharms = nharms
+    p.omega = omega
+    d = hb_matrix(nharms, omega)
+    S = 2 * nharms + 1
+    for i in range(S):
+        for j in range(S):
+            p.dhb[i * S + j] = d[i, j]
+    return p
 
 
 def params_bytes(p: CosaParams) -> bytes:

@@ -187,6 +187,9 @@ int cosa_gpu_resg_rms(cosa_ctx *ctx, int32_t nl, const double *res,
 /* zero (src/util.f90) of a P3 array including halo layer `ext` */
 int cosa_gpu_zero(cosa_ctx *ctx, int32_t nl, double *a);
 
+/* src_hb (src/src.f90:530-613): harmonic-balance source
+   res(n) += omega * vol * sum_m D(n,m) q(m), q conservative, D from params */
+int cosa_gpu_src_hb(cosa_ctx *ctx, int32_t nl, const double *q, const double *vol, double *res);
 /* scalef / scaleb (src/cosa.f90:5626-5773): res *= / res /= dt/V (dtvolt
    for the turbulence equations when npde = 7) */
 int cosa_gpu_scalef(cosa_ctx *ctx, int32_t nl, double *res, const double *dtvol,

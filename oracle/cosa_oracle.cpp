@@ -1091,6 +1091,46 @@ void irs_level(const Level &L, double *res, const double *dtv, const double *dtv
   }
 }
 
+// ---- src_bhb (src/src.f90:556-613): res(n) += omega V sum_m D(n,m) q(m) --------
+void src_hb_level(const Level &L, const double *qa, const double *va, double *ra, const cosa_params &P) {
+  const int S = L.S;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 q(const_cast<double *>(qa), L, b), res(ra, L, b);
+    B1 vol(const_cast<double *>(va), L, b, 1);
+    for (int v = 1; v <= L.npde; ++v)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            double qhb[COSA_MAX_SNAP];
+            for (int ni = 0; ni < S; ++ni) qhb[ni] = 0.0;
+            for (int ni = 0; ni < S; ++ni)
+              for (int nj = 0; nj < S; ++nj)
+                qhb[ni] = qhb[ni] + P.omega * vol(i, j, k) * P.dhb[ni * S + nj] * q(i, j, k, v, nj);
+            for (int ni = 0; ni < S; ++ni) res(i, j, k, v, ni) = res(i, j, k, v, ni) + qhb[ni];
+          }
+  }
+}
+
+// resg_rms_hb / resg_brms_hb (src/cosa.f90:4584-4697), explicit branch
+void resg_rms_hb_level(const Level &L, double *ra, double *out) {
+  double acc[8] = {0};
+  int64_t ncell = 0;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 res(ra, L, b);
+    double rb[8] = {0};
+    for (int n = 0; n < L.S; ++n)
+      for (int v = 1; v <= L.npde; ++v)
+        for (int k = 1; k <= L.km[b] - 1; ++k)
+          for (int j = 1; j <= L.jm[b] - 1; ++j)
+            for (int i = 1; i <= L.im[b] - 1; ++i) rb[v] = rb[v] + res(i, j, k, v, n) * res(i, j, k, v, n);
+    for (int v = 1; v <= L.npde; ++v) rb[L.npde + 1] = rb[L.npde + 1] + rb[v];
+    for (int v = 1; v <= L.npde + 1; ++v) acc[v] = acc[v] + rb[v];
+    ncell += (int64_t)(L.im[b] - 1) * (L.jm[b] - 1) * (L.km[b] - 1);
+  }
+  for (int v = 1; v <= L.npde; ++v) out[v - 1] = std::sqrt(acc[v] / ncell / L.S);
+  out[L.npde] = std::sqrt(acc[L.npde + 1] / ncell / L.S / L.npde);
+}
+
 // ---- resg_brms (src/cosa.f90:4503-4582), explicit steady branch ------------
 void resg_rms_level(const Level &L, double *ra, double *rha, double *out) {
   double acc[8] = {0};
@@ -1317,7 +1357,7 @@ void orc_roe_face(const cosa_params *p, const double *nrm, const double *qr, con
 int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
                   const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
                   double *dqp, double *dqm, double *flux, double *dtvol, int want_dt, double *bx, double *by,
-                  double *bz);
+                  double *bz, const double *vol = nullptr);
 
 int orc_residual(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
                  const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
@@ -1329,7 +1369,7 @@ int orc_residual(orc_level *h, const cosa_params *p, int nl, double *q, const do
 int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
                   const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
                   double *dqp, double *dqm, double *flux, double *dtvol, int want_dt, double *bx, double *by,
-                  double *bz) {
+                  double *bz, const double *vol) {
   Level &L = h->L;
   for (int b = 0; b < L.nb; ++b) cons2prim_b(L, b, q, 0, *p);
   int status = bc_level(L, q, si, sj, sk, *p);
@@ -1350,6 +1390,7 @@ int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const d
   }
 #pragma omp parallel for schedule(dynamic)
   for (int b = 0; b < L.nb; ++b) prim2cons_b(L, b, q, *p);
+  if (p->harbal && vol) src_hb_level(L, q, vol, res, *p);
   return status;
 }
 
@@ -1409,6 +1450,33 @@ int orc_smooth_irs(orc_level *h, const cosa_params *p, int ncycles, int mgit0, i
     }
   }
   return status;
+}
+
+int orc_smooth_hb(orc_level *h, const cosa_params *p, int ncycles, int mgit0, int rms_every, double *q,
+                  double *qold, const double *si, const double *sj, const double *sk, const double *vol,
+                  double *res, double *qp, double *qm, double *dq, double *dqp, double *dqm, double *flux,
+                  double *dtvol, double *hist) {
+  Level &L = h->L;
+  int status = 0;
+  const int last = mgit0 + ncycles - 1;
+  for (int mgit = mgit0; mgit <= last; ++mgit) {
+    const int iter = 1;
+    copy_interior(L, qold, q);
+    for (int irk = 1; irk <= p->nstage; ++irk) {
+      const bool want_dt = (iter / p->iupdt * p->iupdt == iter) && irk == 1;
+      status |= residual_impl(h, p, 1, q, si, sj, sk, res, qp, qm, dq, dqp, dqm, flux, dtvol, want_dt, nullptr,
+                              nullptr, nullptr, vol);
+      if (irk == 1 && (mgit == 1 || mgit % rms_every == 0 || mgit == last) && hist)
+        resg_rms_hb_level(L, res, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
+#pragma omp parallel for schedule(dynamic)
+      for (int b = 0; b < L.nb; ++b) update_b(L, b, res, q, qold, dtvol, p->alphas[irk - 1]);
+    }
+  }
+  return status;
+}
+
+void orc_src_hb(orc_level *h, const cosa_params *p, const double *q, const double *vol, double *res) {
+  src_hb_level(h->L, q, vol, res, *p);
 }
 
 void orc_irs(orc_level *h, const cosa_params *p, double *res, const double *dtvol, const double *bx,

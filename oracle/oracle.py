@@ -186,6 +186,24 @@ def smooth_irs(O, q, si, sj, sk, ncycles, mgit0=1, rms_every=1):
     return hist, st, dtvol, (bx, by, bz)
 
 
+def smooth_hb(O, q, si, sj, sk, vol, ncycles, mgit0=1, rms_every=1):
+    """Explicit harmonic-balance cycles (src_hb in the residual, resg_rms_hb)."""
+    qold = O.p3()
+    res = O.p3()
+    qp, qm, dq, dqp, dqm = (O.p3() for _ in range(5))
+    flux = O.f0()
+    dtvol = O.p1(O.S)
+    hist = np.full((ncycles, O.p.npde + 1), np.nan)
+    st = lib().orc_smooth_hb(O.h, _par(O.p), C.c_int(ncycles), C.c_int(mgit0), C.c_int(rms_every),
+                             _p(q), _p(qold), _p(si), _p(sj), _p(sk), _p(vol), _p(res), _p(qp), _p(qm),
+                             _p(dq), _p(dqp), _p(dqm), _p(flux), _p(dtvol), _p(hist))
+    return hist, st
+
+
+def src_hb(O, q, vol, res):
+    lib().orc_src_hb(O.h, _par(O.p), _p(q), _p(vol), _p(res))
+
+
 def irs(O, res, dtvol, bx, by, bz):
     lib().orc_irs(O.h, _par(O.p), _p(res), _p(dtvol), _p(bx), _p(by), _p(bz))
 

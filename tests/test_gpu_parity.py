@@ -291,3 +291,71 @@ def test_fused_smooth_irs_matches_oracle(oracle_mod, irsop, cutcirs):
     rows = ~np.isnan(hist_o[:, 0])
     np.testing.assert_allclose(hist_g[rows], hist_o[rows], rtol=1e-9)
     ctx.close()
+
+
+def _hb_case(nharms):
+    from cosa_b200.params import set_harmonic_balance
+    case = casekit.small_partitioned()
+    p = set_harmonic_balance(case.params, nharms, 0.16)
+    case.q0 = cases._freestream_state(case.tables, p)
+    return case
+
+
+def _hb_state(case, seed):
+    """Snapshot-dependent perturbation of the free stream."""
+    p = case.params
+    S = 2 * p.nharms + 1
+    q = cases.perturbed_state(case, seed=seed)
+    base = case.q0
+    for v, v0 in zip(p3_views(case.tables, q, 5, S), p3_views(case.tables, base, 5, S)):
+        for n in range(S):
+            v[..., n] = v0[..., n] + (v[..., n] - v0[..., n]) * (1.0 + 0.5 * np.sin(2 * np.pi * n / S + 0.3))
+    return q
+
+
+def test_src_hb_matches_oracle(oracle_mod):
+    case = _hb_case(2)
+    O = oracle_mod.OracleLevel(case.tables, case.params)
+    si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
+    q = _hb_state(case, 5)
+    res = np.random.default_rng(1).standard_normal(q.size) * 1e-3
+    ro = res.copy()
+    oracle_mod.src_hb(O, q, vol, ro)
+    ctx = gpu.Context([case.tables], case.params)
+    rg = ctx.alloc_p3().upload(res)
+    ctx.src_hb(1, ctx.alloc_p3().upload(q), ctx.alloc_p1().upload(vol), rg)
+    S = 5
+    a = casekit.interior_cells(case, rg.download(), 5, S)
+    b = casekit.interior_cells(case, ro, 5, S)
+    scale = np.abs(b).max()
+    assert np.abs(a - b).max() <= TOL * scale
+    ctx.close()
+
+
+@pytest.mark.parametrize("nharms", [1, 3])
+def test_fused_smooth_hb_matches_oracle(oracle_mod, nharms):
+    """Harmonic balance with all snapshots batched in the tile launch:
+    per-snapshot time steps, the coupling source and the snapshot-averaged
+    residual norm (resg_rms_hb) against the oracle for 4 cycles."""
+    case = _hb_case(nharms)
+    S = 2 * nharms + 1
+    O = oracle_mod.OracleLevel(case.tables, case.params)
+    si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
+    q = _hb_state(case, 21)
+    qo = q.copy()
+    hist_o, st_o = oracle_mod.smooth_hb(O, qo, si, sj, sk, vol, 4, rms_every=2)
+    assert st_o == 0
+    ctx = gpu.Context([case.tables], case.params)
+    dq_ = ctx.alloc_p3().upload(q)
+    m = [ctx.alloc_p2().upload(a) for a in (si, sj, sk)]
+    ctx.bind_level(1, q=dq_, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(nsnap=S), si=m[0], sj=m[1], sk=m[2],
+                   vol=ctx.alloc_p1().upload(vol))
+    hist_g, st = ctx.smooth(1, 4, 1, 2)
+    assert st == 0
+    a = casekit.interior_cells(case, dq_.download(), 5, S)
+    b = casekit.interior_cells(case, qo, 5, S)
+    scale = np.abs(b).reshape(-1, 5, S).max(axis=(0, 2))
+    assert (np.abs(a - b) / scale[None, :, None]).max() <= TOL
+    rows = ~np.isnan(hist_o[:, 0])
+    np.testing.assert_allclose(hist_g[rows], hist_o[rows], rtol=1e-9)
+    ctx.close()

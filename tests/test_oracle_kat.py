@@ -231,3 +231,31 @@ def test_prtest_flags_negative_pressure(oracle_mod):
     v = p3_views(case.tables, q, 5, 1)[0]
     v[5, 3, 2, 4, 0] = -1.0
     assert O.prtest(q) & 0x1
+
+
+@pytest.mark.parametrize("nharms", [1, 2, 3])
+def test_hb_operator_differentiates_harmonics(nharms):
+    """omega * D u(t_n) = du/dt(t_n) exactly for every harmonic up to nharms,
+    and D annihilates constants, so a steady state has src_hb = 0
+    (mathb, src/input.f90:5206-5284)."""
+    from cosa_b200.params import hb_matrix
+    omega = 0.08 * 2 / 0.5 * 0.5  # reduced frequency 0.08 at M = 0.5, c = 1
+    D = hb_matrix(nharms, omega)
+    S = 2 * nharms + 1
+    t = np.arange(S) * 2 * np.pi / omega / S
+    np.testing.assert_allclose(D @ np.ones(S), 0.0, atol=1e-13)
+    for k in range(1, nharms + 1):
+        np.testing.assert_allclose(omega * D @ np.cos(k * omega * t), -k * omega * np.sin(k * omega * t), atol=1e-12)
+        np.testing.assert_allclose(omega * D @ np.sin(k * omega * t), k * omega * np.cos(k * omega * t), atol=1e-12)
+
+
+def test_src_hb_vanishes_on_identical_snapshots(oracle_mod):
+    from cosa_b200.params import set_harmonic_balance
+    case = cases.bump_channel(16, 8, 2)
+    p = set_harmonic_balance(case.params, 2, 0.16)
+    O = oracle_mod.OracleLevel(case.tables, p)
+    si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
+    q = cases._freestream_state(case.tables, p)
+    res = O.p3()
+    oracle_mod.src_hb(O, q, vol, res)
+    assert np.abs(res).max() < 1e-14

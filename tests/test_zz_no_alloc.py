@@ -25,12 +25,13 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-9
 
 
-def _noalloc(lib, tables, npde, nharms, res, rhs, out):
+def _noalloc(lib, tables, npde, nharms, res, rhs, out, stream):
+    # the result is read back on `stream`, so the call must be issued on it too
     dims = np.ascontiguousarray(tables.dims.ravel(), dtype=np.int32)
     st = lib.cosa_gpu_resg_rms_noalloc(
         C.c_int32(tables.nblocks), dims.ctypes.data_as(C.POINTER(C.c_int32)), C.c_int32(npde),
         C.c_int32(nharms), C.c_void_p(res.ptr), C.c_void_p(rhs.ptr if rhs is not None else None),
-        C.c_void_p(out.ptr), C.c_void_p(None))
+        C.c_void_p(out.ptr), C.c_void_p(stream))
     assert st == 0, st
     return out.download()
 
@@ -49,8 +50,7 @@ def test_noalloc_rms_matches_context_rms():
         res.upload(rng.standard_normal(n) * 10.0 ** -(3 + call))
         rhs.upload(rng.standard_normal(n) * 1e-4)
         want = ctx.resg_rms(1, res, rhs if with_rhs else None)
-        got = _noalloc(lib, case.tables, p.npde, p.nharms, res, rhs if with_rhs else None, out)
-        ctx.sync()
+        got = _noalloc(lib, case.tables, p.npde, p.nharms, res, rhs if with_rhs else None, out, ctx.stream())
         np.testing.assert_allclose(got, want, rtol=RTOL, atol=0)
     ctx.close()
 
