@@ -26,7 +26,7 @@ from typing import List, Optional, Tuple
 import numpy as np
 
 from .params import CosaParams, default_params, subsonic_inlet_total_state
-from .tables import BlockSpec, LevelTables, build_tables
+from .tables import BlockSpec, LevelTables, build_tables, coarsen
 
 
 @dataclass
@@ -134,6 +134,27 @@ def _face_bcs(ni, nj, nk, types):
         if face in types:
             s, e = f[face]
             out.append((s, e, types[face]))
+    return out
+
+
+def mg_levels(case: Case, nlevel: int):
+    """[(tables, x, y, z)] of levels 1..nlevel: the coarsen() tables and the
+    grid of every other node (coarsen_b, src/cosa.f90:2609-2670), halo nodes
+    extrapolated as on the fine level."""
+    out = [(case.tables, case.x, case.y, case.z)]
+    for nl in range(2, nlevel + 1):
+        f = 2 ** (nl - 1)
+        if ((case.tables.dims - 1) % f).any():
+            raise ValueError(f"cell counts not divisible by {f} for {nlevel} levels")
+        t = coarsen(case.tables, nl)
+        _, tot = t.offsets()
+        grids = []
+        for a in (case.x, case.y, case.z):
+            dst = np.zeros(tot["p2"])
+            for vf, vc in zip(p2_views(case.tables, a), p2_views(t, dst)):
+                _embed_grid(vf[1:-1:f, 1:-1:f, 1:-1:f], vc)
+            grids.append(dst)
+        out.append((t, *grids))
     return out
 
 

@@ -6,12 +6,14 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <vector>
 
 #include "kernels_ref.cuh"
 #include "fused.cuh"
+#include "mg.cuh"
 
 namespace {
 
@@ -56,8 +58,14 @@ struct ProfState {
   long long n[2] = {0, 0};
 };
 
+struct GraphEntry {
+  cudaGraphExec_t exec = nullptr;
+  long long launches = 0;  // kernels per replay
+};
+
 struct cosa_ctx {
   ProfState prof;
+  std::map<uint64_t, GraphEntry> graphs;  // captured launch sequences by key
   cosa_params p{};
   cosa_params *d_p = nullptr;
   int device = 0;
@@ -331,6 +339,32 @@ int check_fused_supported(const cosa_params &p) {
   return COSA_OK;
 }
 
+// A block with a single cell along a direction: the reference's BCs on the
+// faces normal to it read "interior cell 2", which is the opposite face's
+// halo, still holding the previous stage's value in conservative form
+// (src/bc.f90 bc_* with ibcn2, after prim2cons of src/cosa.f90:1908).  The
+// fused halo kernel fills all faces at once from primitive data, so it
+// matches the reference there only where that second cell is never used:
+// first-order reconstruction on the level (the second halo layer unread)
+// and BCs whose first halo layer depends on the first interior cell alone
+// (80 symmetry, 4 extrapolation, 30 far field).
+int check_thin_blocks(const cosa_ctx *c, int nl) {
+  const LevelState &L = c->L[nl - 1];
+  for (int b = 0; b < L.nb; ++b) {
+    const DevBlock &x = L.hb[b];
+    const int nc[4] = {0, x.im - 1, x.jm - 1, x.km - 1};
+    for (int d = 1; d <= 3; ++d) {
+      if (nc[d] > 1) continue;
+      if (nl < c->p.nl_crs) return COSA_ERR_UNSUPPORTED;
+      for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
+        const int *r = L.bct.data() + L.obct[b] + 10 * ibc;
+        if (r[1] == d && r[0] != 80 && r[0] != 4 && r[0] != 30) return COSA_ERR_UNSUPPORTED;
+      }
+    }
+  }
+  return COSA_OK;
+}
+
 int ensure_irs_scratch(cosa_ctx *c, LevelState &L) {
   const int S = 2 * c->p.nharms + 1;
   const size_t n = (size_t)L.n3 * c->p.npde * S;
@@ -417,7 +451,8 @@ void prof_stop(cosa_ctx *c, int k) {
 
 // one stage: halo fill + tile kernel (+ norm reduction)
 int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, const double *qold,
-                 double *qold_copy, int irk, int compute_dt, bool want_rms, int update, double *res_out) {
+                 double *qold_copy, int irk, int compute_dt, bool want_rms, int update, double *res_out,
+                 double *rhs = nullptr, int rhs_mode = 0) {
   const cosa_params &p = c->p;
   const int S = 2 * p.nharms + 1;
   const cosa_level_ptrs &P = L.ptrs;
@@ -434,7 +469,8 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   A.qin = qin; A.qout = qout; A.qold = qold; A.qold_copy = qold_copy;
   A.dtvol = P.dtvol; A.si = P.si; A.sj = P.sj; A.sk = P.sk;
   A.part = want_rms ? L.d_part : nullptr;
-  A.rhs = nullptr;
+  A.rhs = rhs;
+  A.rhs_mode = rhs ? rhs_mode : 0;
   A.res_out = res_out;
   if (compute_dt && p.irsop >= 2) {
     A.bx = P.betaxi ? P.betaxi : L.d_beta[0];
@@ -468,24 +504,39 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   return COSA_OK;
 }
 
+// what one RK iteration of smooth() does besides the stages themselves
+struct IterOpts {
+  bool want_rms = false;       // stage-1 residual norm (fine level, printed cycle)
+  int compute_dt = 0;          // stage-1 local time step
+  double *rhs = nullptr;       // coarse-level forcing: res -= rhs at every stage
+  bool force = false;          // rhs += res at stage 1 (first iteration of a from_fine visit)
+  bool copy_qold = true;       // qold = q at stage 1 (iter <= niter)
+  double *res_only = nullptr;  // residual pass of to_coarse: stage-1 residual here, no update
+};
+
 // one RK iteration (nstage stages) of the fused path
-int launch_iteration(cosa_ctx *c, int nl, LevelState &L, bool want_rms, int compute_dt) {
+int launch_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
   const cosa_params &p = c->p;
   double *Q = L.ptrs.q, *T = L.d_T, *QO = L.ptrs.qold;
   const int S = 2 * p.nharms + 1;
+  if (o.res_only) {
+    return launch_stage(c, nl, L, Q, T, Q, nullptr, 1, o.compute_dt, false, 0, o.res_only, o.rhs,
+                        o.force ? 2 : 1);
+  }
   for (int irk = 1; irk <= p.nstage; ++irk) {
     double *qin = (irk % 2 == 1) ? Q : T;
     double *qout = (irk % 2 == 1) ? T : Q;
     const double *qold = irk == 1 ? Q : QO;
-    double *qcopy = irk == 1 ? QO : nullptr;
+    double *qcopy = (irk == 1 && o.copy_qold) ? QO : nullptr;
+    const int rmode = (irk == 1 && o.force) ? 2 : 1;
     if (p.irsop == 0) {
-      int r = launch_stage(c, nl, L, qin, qout, qold, qcopy, irk, compute_dt && irk == 1, want_rms && irk == 1, 1,
-                           nullptr);
+      int r = launch_stage(c, nl, L, qin, qout, qold, qcopy, irk, o.compute_dt && irk == 1, o.want_rms && irk == 1, 1,
+                           nullptr, o.rhs, rmode);
       if (r) return r;
     } else {
       // residual (no update) -> implicit smoothing -> update
-      int r = launch_stage(c, nl, L, qin, qout, qold, nullptr, irk, compute_dt && irk == 1, want_rms && irk == 1, 0,
-                           L.d_res);
+      int r = launch_stage(c, nl, L, qin, qout, qold, nullptr, irk, o.compute_dt && irk == 1, o.want_rms && irk == 1,
+                           0, L.d_res, o.rhs, rmode);
       if (r) return r;
       const double *beta[3] = {L.ptrs.betaxi ? L.ptrs.betaxi : L.d_beta[0],
                                L.ptrs.betaeta ? L.ptrs.betaeta : L.d_beta[1],
@@ -518,6 +569,41 @@ void drop_graphs(cosa_ctx *c) {
   for (int l = 0; l < COSA_MAX_LEVELS; ++l)
     for (auto &g : c->L[l].graph)
       if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (auto &kv : c->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  c->graphs.clear();
+}
+
+// replay the graph stored under `key`, capturing `issue` into it first if
+// absent; the launch counter advances by the graph's kernel count
+template <typename F>
+int run_graph(cosa_ctx *c, uint64_t key, F &&issue) {
+  GraphEntry &g = c->graphs[key];
+  if (!g.exec) {
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
+    const long long before = c->launches;
+    const int r = issue();
+    const long long n = c->launches - before;
+    const cudaError_t e = cudaStreamEndCapture(c->s, &graph);
+    c->launches = before;  // counted at replay
+    if (r || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      c->graphs.erase(key);
+      return r ? r : cuda_ok(e);
+    }
+    const cudaError_t e2 = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) {
+      c->graphs.erase(key);
+      return cuda_ok(e2);
+    }
+    g.launches = n;
+  }
+  const long long per = g.launches;
+  CK(cudaGraphLaunch(g.exec, c->s));
+  c->launches += per;
+  return COSA_OK;
 }
 
 int ensure_hist(cosa_ctx *c, int rows) {
@@ -572,9 +658,7 @@ int cosa_gpu_finalize(cosa_ctx *c) {
   if (!c) return COSA_ERR_ARG;
   cudaSetDevice(c->device);
   if (c->s) cudaStreamSynchronize(c->s);
-  for (int l = 0; l < COSA_MAX_LEVELS; ++l)
-    for (auto &g : c->L[l].graph)
-      if (g) cudaGraphExecDestroy(g);
+  drop_graphs(c);
   for (auto &e2 : c->prof.ev)
     for (auto &e : e2)
       if (e) cudaEventDestroy(e);
@@ -590,9 +674,7 @@ int cosa_gpu_set_params(cosa_ctx *c, const cosa_params *p) {
   c->p = *p;
   CK(cudaMemcpyAsync(c->d_p, p, sizeof(cosa_params), cudaMemcpyHostToDevice, c->s));
   CK(cudaStreamSynchronize(c->s));
-  for (int l = 0; l < COSA_MAX_LEVELS; ++l)
-    for (auto &g : c->L[l].graph)
-      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  drop_graphs(c);
   return COSA_OK;
 }
 
@@ -644,8 +726,7 @@ int cosa_gpu_bind_level(cosa_ctx *c, int32_t nl, const cosa_level_ptrs *ptrs) {
     if ((r = dalloc(c, &L->d_part, (size_t)need * 8))) return r;
     L->npart_cap = need;
   }
-  for (auto &g : L->graph)
-    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  drop_graphs(c);  // graphs hold the previous pointers
   L->bound = true;
   return COSA_OK;
 }
@@ -806,7 +887,7 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
   LevelState *L = level(c, nl);
   if (!L || !L->bound || niter < 0 || rms_every < 1) return COSA_ERR_ARG;
   int r = check_fused_supported(c->p);
-  if (r) return r;
+  if (r || (r = check_thin_blocks(c, nl))) return r;
   const cosa_level_ptrs &P = L->ptrs;
   if (!P.q || !P.qold || !P.dtvol || !P.si || !P.sj || !P.sk) return COSA_ERR_ARG;
   if (c->p.harbal && !P.vol) return COSA_ERR_ARG;
@@ -833,7 +914,10 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
       cudaGraph_t graph;
       CK(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
       const long long before = c->launches;
-      r = launch_iteration(c, nl, *L, want, compute_dt);
+      IterOpts o;
+      o.want_rms = want;
+      o.compute_dt = compute_dt;
+      r = launch_iteration(c, nl, *L, o);
       cudaError_t e = cudaStreamEndCapture(c->s, &graph);
       if (r) return r;
       CK(e);
@@ -955,11 +1039,362 @@ int cosa_gpu_vols(cosa_ctx *c, int32_t nl, const double *x, const double *y, con
   return COSA_OK;
 }
 
+}  // extern "C"
+
+// ---- multigrid ---------------------------------------------------------------------------
+namespace {
+
+// levels nl and nl+1 hold the same blocks with twice the cells per direction
+int level_pair(cosa_ctx *c, int nl, LevelState *&L1, LevelState *&L2) {
+  L1 = level(c, nl);
+  L2 = level(c, nl + 1);
+  if (!L1 || !L2 || L1->nb != L2->nb) return COSA_ERR_ARG;
+  for (int b = 0; b < L1->nb; ++b) {
+    const DevBlock &f = L1->hb[b], &g = L2->hb[b];
+    if (f.im - 1 != 2 * (g.im - 1) || f.jm - 1 != 2 * (g.jm - 1) || f.km - 1 != 2 * (g.km - 1)) return COSA_ERR_ARG;
+  }
+  return COSA_OK;
+}
+
+int launch_edges(cosa_ctx *c, LevelState &L, double *q, double *mut) {
+  const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
+  for (int b = 0; b < L.nb; ++b) {
+    const DevBlock &x = L.hb[b];
+    const int64_t per = 4 * ((int64_t)(x.im - 1) + (x.jm - 1) + (x.km - 1));
+    k_edges<<<grid_for(per * npde * S), 256, 0, c->s>>>(x, npde, S, q, x.op3 * npde * S);
+    int r = after_launch(c);
+    if (r) return r;
+    if (mut) {
+      k_edges<<<grid_for(per * S), 256, 0, c->s>>>(x, 1, S, mut, x.op3 * S);
+      if ((r = after_launch(c))) return r;
+    }
+  }
+  return COSA_OK;
+}
+
+int launch_corns(cosa_ctx *c, LevelState &L, double *q, double *mut) {
+  const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
+  for (int b = 0; b < L.nb; ++b) {
+    const DevBlock &x = L.hb[b];
+    k_corns<<<1, 128, 0, c->s>>>(x, npde, S, q, x.op3 * npde * S);
+    int r = after_launch(c);
+    if (r) return r;
+    if (mut) {
+      k_corns<<<1, 128, 0, c->s>>>(x, 1, S, mut, x.op3 * S);
+      if ((r = after_launch(c))) return r;
+    }
+  }
+  return COSA_OK;
+}
+
+int launch_rest1(cosa_ctx *c, LevelState &L1, LevelState &L2, const double *q1, double *q2, const double *v1,
+                 const double *v2) {
+  const int S = 2 * c->p.nharms + 1;
+  for (int b = 0; b < L1.nb; ++b) {
+    const DevBlock &g = L2.hb[b];
+    k_rest1<<<grid_for((int64_t)(g.im - 1) * (g.jm - 1) * (g.km - 1) * S), 256, 0, c->s>>>(L1.hb[b], g, c->p.npde, S,
+                                                                                          q1, q2, v1, v2);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int launch_rest2(cosa_ctx *c, LevelState &L1, LevelState &L2, double *rhs2, const double *res1) {
+  const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
+  for (int b = 0; b < L1.nb; ++b) {
+    const DevBlock &g = L2.hb[b];
+    k_rest2<<<grid_for((int64_t)(g.im - 1) * (g.jm - 1) * (g.km - 1) * npde * S), 256, 0, c->s>>>(L1.hb[b], g, npde,
+                                                                                                 S, rhs2, res1);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int launch_prol(cosa_ctx *c, LevelState &L1, LevelState &L2, double *q1, const double *q2, const double *vol1,
+                bool bilinear) {
+  const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
+  for (int b = 0; b < L1.nb; ++b) {
+    const DevBlock &g = L2.hb[b];
+    const int64_t n = (int64_t)g.im * g.jm * g.km * npde * S;
+    if (bilinear)
+      k_prol_bln<<<grid_for(n), 256, 0, c->s>>>(L1.hb[b], g, npde, S, q1, q2, c->p.lim_corr);
+    else
+      k_prol_lin<<<grid_for(n), 256, 0, c->s>>>(L1.hb[b], g, npde, S, q1, q2, vol1);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+// restrict(nl), Euler branch (src/cosa.f90:2672-2755)
+int issue_restrict(cosa_ctx *c, int nl) {
+  LevelState *L1, *L2;
+  int r = level_pair(c, nl, L1, L2);
+  if (r) return r;
+  const cosa_level_ptrs &A = L1->ptrs, &B = L2->ptrs;
+  if (!A.q || !A.vol || !A.res || !B.q || !B.vol || !B.rhs) return COSA_ERR_ARG;
+  if (c->p.kom || c->p.kom_bsl || c->p.kom_sst) return COSA_ERR_UNSUPPORTED;
+  if ((r = launch_rest1(c, *L1, *L2, A.q, B.q, A.vol, B.vol))) return r;
+  return launch_rest2(c, *L1, *L2, B.rhs, A.res);
+}
+
+// prolong(nl) (src/cosa.f90:3167-3250)
+int issue_prolong(cosa_ctx *c, int nl) {
+  LevelState *L1, *L2;
+  int r = level_pair(c, nl, L1, L2);
+  if (r) return r;
+  const cosa_level_ptrs &A = L1->ptrs, &B = L2->ptrs;
+  if (!A.q || !A.vol || !B.q || !B.qold || !B.vol || !B.si || !B.sj || !B.sk) return COSA_ERR_ARG;
+  if ((r = launch_rest1(c, *L1, *L2, A.q, B.qold, A.vol, B.vol))) return r;
+  for (double *a : {B.qold, B.q}) {
+    if ((r = cosa_gpu_cons2prim(c, nl + 1, 0, a)) || (r = cosa_gpu_bc(c, nl + 1, a, B.si, B.sj, B.sk, B.dist)) ||
+        (r = cosa_gpu_cutman_q(c, nl + 1, a)) || (r = cosa_gpu_prim2cons(c, nl + 1, a)) ||
+        (r = launch_edges(c, *L2, a, nullptr)) || (r = launch_corns(c, *L2, a, nullptr)))
+      return r;
+  }
+  const int nvs = c->p.npde * (2 * c->p.nharms + 1);
+  for (int b = 0; b < L2->nb; ++b) {
+    const DevBlock &g = L2->hb[b];
+    k_add_ext1<<<grid_for((int64_t)(g.im + 1) * (g.jm + 1) * (g.km + 1) * nvs), 256, 0, c->s>>>(g, nvs, B.q, B.qold,
+                                                                                               -1.0);
+    if ((r = after_launch(c))) return r;
+  }
+  if ((r = launch_prol(c, *L1, *L2, A.q, B.q, A.vol, c->p.bln_prol != 0))) return r;
+  if (c->p.lim_corr == 1 || c->p.lim_corr == 3) return cosa_gpu_fixq(c, nl, A.q);
+  return COSA_OK;
+}
+
+// smooth(nl, from_fine, to_coarse, done, niter) of the fused path
+int issue_smooth_level(cosa_ctx *c, int nl, int niter, bool from_fine, bool to_coarse, bool want_rms) {
+  LevelState &L = *level(c, nl);
+  const cosa_params &p = c->p;
+  const int niterp = to_coarse ? niter + 1 : niter;
+  int r = 0;
+  for (int iter = 1; iter <= niterp; ++iter) {
+    IterOpts o;
+    o.compute_dt = (iter / p.iupdt * p.iupdt == iter) ? 1 : 0;
+    o.rhs = nl > 1 ? L.ptrs.rhs : nullptr;
+    o.force = from_fine && iter == 1;
+    o.copy_qold = iter <= niter;
+    o.want_rms = want_rms && nl == 1 && iter == niter;
+    o.res_only = iter == niter + 1 ? L.ptrs.res : nullptr;
+    if ((r = launch_iteration(c, nl, L, o))) return r;
+  }
+  // reference state after smooth(): face halos of q in conservative form
+  if (niterp > 0 && !L.items.empty()) {
+    double *last_in = (to_coarse || p.nstage % 2 == 1) ? L.ptrs.q : L.d_T;
+    const int S = 2 * p.nharms + 1;
+    k_halo_p2c<<<grid_for((int64_t)L.items.size() * S), 256, 0, c->s>>>(L.d_blocks, L.d_items, (int)L.items.size(),
+                                                                       c->d_p, last_in, L.ptrs.q);
+    if ((r = after_launch(c))) return r;
+  }
+  return COSA_OK;
+}
+
+// one cycle of mg() (src/cosa.f90:822-912)
+int issue_mg_cycle(cosa_ctx *c, int mgit, bool want_rms) {
+  const cosa_params &p = c->p;
+  const int nlevel = p.nlevel;
+  int r = 0;
+  int niter = nlevel == 1 ? 1 : (mgit == 1 ? p.nstart : p.npost);
+  if ((r = issue_smooth_level(c, 1, niter, false, nlevel > 1, want_rms))) return r;
+  if (nlevel == 1) return COSA_OK;
+  if ((r = issue_restrict(c, 1))) return r;
+  niter = nlevel == 2 ? p.ncrs : p.npre;
+  if ((r = issue_smooth_level(c, 2, niter, true, nlevel > 2, false))) return r;
+  if (nlevel == 3) {
+    if ((r = issue_restrict(c, 2)) || (r = issue_smooth_level(c, 3, p.ncrs, true, false, false)) ||
+        (r = issue_prolong(c, 2)) || (r = issue_smooth_level(c, 2, p.npost, false, false, false)))
+      return r;
+  }
+  return issue_prolong(c, 1);
+}
+
+// the bound levels' arrays that smoothing and the transfers of nlevel levels need
+int check_mg_levels(cosa_ctx *c, int nlevel) {
+  for (int nl = 1; nl <= nlevel; ++nl) {
+    LevelState *L = level(c, nl);
+    if (!L || !L->bound) return COSA_ERR_ARG;
+    const cosa_level_ptrs &P = L->ptrs;
+    if (!P.q || !P.qold || !P.dtvol || !P.si || !P.sj || !P.sk) return COSA_ERR_ARG;
+    if ((c->p.harbal || nlevel > 1) && !P.vol) return COSA_ERR_ARG;
+    if (nl < nlevel && !P.res) return COSA_ERR_ARG;
+    if (nl > 1 && !P.rhs) return COSA_ERR_ARG;
+    if (nl < nlevel) {
+      LevelState *L1, *L2;
+      if (level_pair(c, nl, L1, L2)) return COSA_ERR_ARG;
+    }
+  }
+  return COSA_OK;
+}
+
+uint64_t graph_key(int kind, int nl, int niter, int flags) {
+  return ((uint64_t)kind << 56) | ((uint64_t)(nl & 0xff) << 48) | ((uint64_t)(uint32_t)niter << 16) |
+         (uint64_t)(flags & 0xffff);
+}
+
+}  // namespace
+
+extern "C" {
+
+int cosa_gpu_q_edges(cosa_ctx *c, int32_t nl, double *q, double *mut) {
+  LevelState *L = level(c, nl);
+  if (!L || !q) return COSA_ERR_ARG;
+  return launch_edges(c, *L, q, mut);
+}
+
+int cosa_gpu_q_corns(cosa_ctx *c, int32_t nl, double *q, double *mut) {
+  LevelState *L = level(c, nl);
+  if (!L || !q) return COSA_ERR_ARG;
+  return launch_corns(c, *L, q, mut);
+}
+
+int cosa_gpu_fixq(cosa_ctx *c, int32_t nl, double *q) {
+  LevelState *L = level(c, nl);
+  if (!L || !q) return COSA_ERR_ARG;
+  if (c->p.npde < 7) return COSA_OK;  // the reference calls it for k-omega only
+  const int S = 2 * c->p.nharms + 1;
+  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int) {
+    k_fixq<<<grid_for((int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * S), 256, 0, c->s>>>(b, c->d_p, q);
+  });
+}
+
+int cosa_gpu_tur_vis(cosa_ctx *c, int32_t nl, const double *q, double *mut) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !mut || c->p.npde < 7) return COSA_ERR_ARG;
+  const int S = 2 * c->p.nharms + 1;
+  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int) {
+    k_tur_vis<<<grid_for((int64_t)(b.im + 1) * (b.jm + 1) * (b.km + 1) * S), 256, 0, c->s>>>(b, c->d_p, q, mut);
+  });
+}
+
+int cosa_gpu_rest1(cosa_ctx *c, int32_t nl, const double *q1, double *q2, const double *vol1, const double *vol2) {
+  LevelState *L1, *L2;
+  int r = level_pair(c, nl, L1, L2);
+  if (r) return r;
+  if (!q1 || !q2 || !vol1 || !vol2) return COSA_ERR_ARG;
+  return launch_rest1(c, *L1, *L2, q1, q2, vol1, vol2);
+}
+
+int cosa_gpu_rest2(cosa_ctx *c, int32_t nl, double *rhs2, const double *res1) {
+  LevelState *L1, *L2;
+  int r = level_pair(c, nl, L1, L2);
+  if (r) return r;
+  if (!rhs2 || !res1) return COSA_ERR_ARG;
+  return launch_rest2(c, *L1, *L2, rhs2, res1);
+}
+
+int cosa_gpu_prol_bln(cosa_ctx *c, int32_t nl, double *q1, const double *q2) {
+  LevelState *L1, *L2;
+  int r = level_pair(c, nl, L1, L2);
+  if (r) return r;
+  if (!q1 || !q2) return COSA_ERR_ARG;
+  return launch_prol(c, *L1, *L2, q1, q2, nullptr, true);
+}
+
+int cosa_gpu_prol_lin(cosa_ctx *c, int32_t nl, double *q1, const double *q2, const double *vol1) {
+  LevelState *L1, *L2;
+  int r = level_pair(c, nl, L1, L2);
+  if (r) return r;
+  if (!q1 || !q2 || !vol1) return COSA_ERR_ARG;
+  return launch_prol(c, *L1, *L2, q1, q2, vol1, false);
+}
+
+int cosa_gpu_restrict(cosa_ctx *c, int32_t nl) {
+  if (!c) return COSA_ERR_ARG;
+  cudaSetDevice(c->device);
+  return issue_restrict(c, nl);
+}
+
+int cosa_gpu_prolong(cosa_ctx *c, int32_t nl) {
+  if (!c) return COSA_ERR_ARG;
+  cudaSetDevice(c->device);
+  int r = issue_prolong(c, nl);
+  if (r) return r;
+  return cosa_gpu_status(c, 0);
+}
+
+int cosa_gpu_smooth_level(cosa_ctx *c, int32_t nl, int32_t niter, int32_t from_fine, int32_t to_coarse, int32_t mgit,
+                          int32_t ncycle, int32_t rms_every, double *resrms) {
+  LevelState *L = level(c, nl);
+  if (!L || !L->bound || niter < 0 || rms_every < 1) return COSA_ERR_ARG;
+  int r = check_fused_supported(c->p);
+  if (r || (r = check_thin_blocks(c, nl))) return r;
+  const cosa_level_ptrs &P = L->ptrs;
+  if (!P.q || !P.qold || !P.dtvol || !P.si || !P.sj || !P.sk) return COSA_ERR_ARG;
+  if ((c->p.harbal && !P.vol) || (to_coarse && !P.res) || (nl > 1 && !P.rhs)) return COSA_ERR_ARG;
+  cudaSetDevice(c->device);
+  const bool want = resrms && nl == 1 && niter > 0 && (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle);
+  if ((r = ensure_hist(c, 1))) return r;
+  if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, *L))) return r;
+  CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
+  const int flags = (from_fine ? 1 : 0) | (to_coarse ? 2 : 0) | (want ? 4 : 0);
+  r = run_graph(c, graph_key(1, nl, niter, flags),
+                [&] { return issue_smooth_level(c, nl, niter, from_fine != 0, to_coarse != 0, want); });
+  if (r) return r;
+  if (want) CK(cudaMemcpyAsync(resrms, c->d_hist, (c->p.npde + 1) * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  return cosa_gpu_status(c, 0);
+}
+
+int cosa_gpu_mg(cosa_ctx *c, int32_t mgit0, int32_t ncycles, int32_t ncycle, int32_t rms_every, double *hist) {
+  if (!c || ncycles < 0 || rms_every < 1 || mgit0 < 1) return COSA_ERR_ARG;
+  const int nlevel = c->p.nlevel;
+  if (nlevel < 1 || nlevel > c->nlevels) return COSA_ERR_ARG;
+  int r = check_fused_supported(c->p);
+  if (r) return r;
+  if ((r = check_mg_levels(c, nlevel))) return r;
+  for (int nl = 1; nl <= nlevel; ++nl)
+    if ((r = check_thin_blocks(c, nl))) return r;
+  cudaSetDevice(c->device);
+  const int npde = c->p.npde;
+  std::vector<int> rows;
+  for (int it = 0; it < ncycles; ++it) {
+    const int mgit = mgit0 + it;
+    if (hist && (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle)) rows.push_back(it);
+  }
+  if ((r = ensure_hist(c, std::max<int>(1, (int)rows.size())))) return r;
+  for (int nl = 1; nl <= nlevel; ++nl)
+    if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, *level(c, nl)))) return r;
+  CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
+  size_t ri = 0;
+  int last = mgit0 - 1;
+  for (int it = 0; it < ncycles; ++it) {
+    const int mgit = mgit0 + it;
+    const bool want = ri < rows.size() && rows[ri] == it;
+    if (want) ++ri;
+    const int flags = (mgit == 1 ? 1 : 0) | (want ? 2 : 0);
+    r = run_graph(c, graph_key(2, nlevel, 0, flags), [&] { return issue_mg_cycle(c, mgit, want); });
+    if (r) return r;
+    last = mgit;
+  }
+  if (nlevel > 1 && last == ncycle) {
+    r = run_graph(c, graph_key(1, 1, c->p.npost, 0),
+                  [&] { return issue_smooth_level(c, 1, c->p.npost, false, false, false); });
+    if (r) return r;
+  }
+  if (hist) {
+    std::vector<double> h(rows.size() * (npde + 1));
+    if (!rows.empty())
+      CK(cudaMemcpyAsync(h.data(), c->d_hist, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    CK(cudaStreamSynchronize(c->s));
+    for (int it = 0; it < ncycles; ++it)
+      for (int v = 0; v <= npde; ++v) hist[(int64_t)it * (npde + 1) + v] = NAN;
+    for (size_t k = 0; k < rows.size(); ++k)
+      for (int v = 0; v <= npde; ++v) hist[(int64_t)rows[k] * (npde + 1) + v] = h[k * (npde + 1) + v];
+  } else {
+    CK(cudaStreamSynchronize(c->s));
+  }
+  return cosa_gpu_status(c, 0);
+}
+
 int cosa_gpu_profile(cosa_ctx *c, int32_t nl, int32_t niter, double ms[3], int64_t counts[3]) {
   LevelState *L = level(c, nl);
   if (!L || !L->bound || niter < 1 || !ms || !counts) return COSA_ERR_ARG;
   int r = check_fused_supported(c->p);
-  if (r) return r;
+  if (r || (r = check_thin_blocks(c, nl))) return r;
   ProfState &pf = c->prof;
   for (auto &e2 : pf.ev)
     for (auto &e : e2)
@@ -973,7 +1408,9 @@ int cosa_gpu_profile(cosa_ctx *c, int32_t nl, int32_t niter, double ms[3], int64
   const int compute_dt = (1 / c->p.iupdt * c->p.iupdt == 1) ? 1 : 0;
   if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, *L))) return r;
   cudaEventRecord(t0, c->s);
-  for (int it = 0; it < niter && !r; ++it) r = launch_iteration(c, nl, *L, false, compute_dt);
+  IterOpts o;
+  o.compute_dt = compute_dt;
+  for (int it = 0; it < niter && !r; ++it) r = launch_iteration(c, nl, *L, o);
   cudaEventRecord(t1, c->s);
   pf.on = false;
   CK(cudaEventSynchronize(t1));

@@ -130,7 +130,8 @@ struct StageArgs {
   double *dtvol;         // Delta t / V, written when compute_dt, read otherwise
   const double *si, *sj, *sk;
   double *part;          // per-tile residual sums of squares (npde) or null
-  const double *rhs;     // multigrid forcing or null
+  double *rhs;           // multigrid forcing term of a coarse level, or null
+  int rhs_mode;          // 1: r -= rhs; 2: rhs += r first (forcing), then r -= rhs
   double *res_out;       // if set, the residual is stored here (P3 layout)
   double *bx, *by, *bz;  // IRS coefficients written with the time step (irsop >= 2)
   const double *vol;     // cell volumes when the harmonic-balance source is on
@@ -391,11 +392,20 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
             qhb = qhb + ov * P.dhb[n * S + nj2] * A.qin[p3_var(b, npde, S, m + 1, nj2) + cell];
           r = r + qhb;
         }
-        if (A.res_out) A.res_out[p3_var(b, npde, S, m + 1, n) + cell] = r;
-        if (A.part) {
-          const double rr = r - (A.rhs ? A.rhs[p3_var(b, npde, S, m + 1, n) + cell] : 0.0);
-          acc[m] += rr * rr;
+        // resg_rms of the fine level, where rhs is zero (src/cosa.f90:1925-1936)
+        if (A.part) acc[m] += r * r;
+        if (A.rhs_mode) {
+          // multigrid forcing on coarse levels (src/cosa.f90:1950-1960)
+          double *rh = A.rhs + p3_var(b, npde, S, m + 1, n) + cell;
+          if (A.rhs_mode == 2) {
+            const double rn = *rh + r;
+            *rh = rn;
+            r = r - rn;
+          } else {
+            r = r - *rh;
+          }
         }
+        if (A.res_out) A.res_out[p3_var(b, npde, S, m + 1, n) + cell] = r;
         if (A.update) {
           const double q0 = qo[m * vstride + cell];
           if (A.qold_copy) A.qold_copy[p3_var(b, npde, S, m + 1, n) + cell] = q0;

@@ -1,0 +1,328 @@
+// Multigrid transfer kernels and the halo edge/corner extrapolation.
+//
+// Level nl (fine, blocks b1) and nl+1 (coarse, blocks b2) hold the same
+// blocks with (imax1-1) = 2 (imax2-1) cells per direction.  Every kernel is
+// a grid-stride loop over independent outputs (no atomics, no ordering
+// between threads), so results do not depend on the launch shape.  Threads
+// run fastest along i, which keeps the P3 reads and writes coalesced.
+#pragma once
+#include "physics.cuh"
+
+// ---- rest1_b (src/cosa.f90:2788-2833) ---------------------------------------------
+__global__ void k_rest1(DevBlock b1, DevBlock b2, int npde, int S, const double *__restrict__ q1,
+                        double *__restrict__ q2, const double *__restrict__ vol1, const double *__restrict__ vol2) {
+  const int ni = b2.im - 1, nj = b2.jm - 1, nk = b2.km - 1;
+  const int64_t total = (int64_t)ni * nj * nk * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i2 = (int)(r % ni) + 1; r /= ni;
+    const int j2 = (int)(r % nj) + 1; r /= nj;
+    const int k2 = (int)(r % nk) + 1; r /= nk;
+    const int n = (int)r;
+    const int i1 = 2 * i2 - 1, j1 = 2 * j2 - 1, k1 = 2 * k2 - 1;
+    // the eight fine cells in the reference's summation order
+    int64_t c[8];
+    double w[8];
+    const int di[8] = {0, 0, 1, 1, 0, 0, 1, 1}, dj[8] = {0, 1, 0, 1, 0, 1, 0, 1}, dk[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      c[s] = p3_cell(b1, i1 + di[s], j1 + dj[s], k1 + dk[s]);
+      w[s] = vol1[p1_idx(b1, 1, i1 + di[s], j1 + dj[s], k1 + dk[s], 0)];
+    }
+    const double v2 = vol2[p1_idx(b2, 1, i2, j2, k2, 0)];
+    const int64_t c2 = p3_cell(b2, i2, j2, k2);
+    for (int v = 1; v <= npde; ++v) {
+      const double *a = q1 + p3_var(b1, npde, S, v, n);
+      double s = w[0] * a[c[0]];
+#pragma unroll
+      for (int m = 1; m < 8; ++m) s = s + w[m] * a[c[m]];
+      q2[p3_var(b2, npde, S, v, n) + c2] = s / v2;
+    }
+  }
+}
+
+// ---- rest2_lo_b (src/cosa.f90:2955-3012) ------------------------------------------
+__global__ void k_rest2(DevBlock b1, DevBlock b2, int npde, int S, double *__restrict__ rhs2,
+                        const double *__restrict__ res1) {
+  const int ni = b2.im - 1, nj = b2.jm - 1, nk = b2.km - 1;
+  const int64_t total = (int64_t)ni * nj * nk * npde * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i2 = (int)(r % ni) + 1; r /= ni;
+    const int j2 = (int)(r % nj) + 1; r /= nj;
+    const int k2 = (int)(r % nk) + 1; r /= nk;
+    const int v = (int)(r % npde) + 1; r /= npde;
+    const int n = (int)r;
+    const int i1 = 2 * i2 - 1, j1 = 2 * j2 - 1, k1 = 2 * k2 - 1;
+    const double *a = res1 + p3_var(b1, npde, S, v, n);
+    const double s = a[p3_cell(b1, i1, j1, k1)] + a[p3_cell(b1, i1, j1 + 1, k1)] + a[p3_cell(b1, i1 + 1, j1, k1)] +
+                     a[p3_cell(b1, i1 + 1, j1 + 1, k1)] + a[p3_cell(b1, i1, j1, k1 + 1)] +
+                     a[p3_cell(b1, i1, j1 + 1, k1 + 1)] + a[p3_cell(b1, i1 + 1, j1, k1 + 1)] +
+                     a[p3_cell(b1, i1 + 1, j1 + 1, k1 + 1)];
+    rhs2[p3_var(b2, npde, S, v, n) + p3_cell(b2, i2, j2, k2)] = -s;
+  }
+}
+
+// ---- q_bedges (src/flux.f90:3913-4263) --------------------------------------------
+// edge ic of a family: target point 0 and fit points 1..3 in the two cross
+// coordinates (x, y) of the family: (i,j) along k, (i,k) along j, (j,k) along i
+__device__ __forceinline__ void edge_pts(int ic, int m1, int m2, int x[4], int y[4]) {
+  const int lo1 = (ic == 0 || ic == 3), lo2 = (ic <= 1);
+  const int e1 = lo1 ? 0 : m1, n1 = lo1 ? 1 : m1 - 1;
+  const int e2 = lo2 ? 0 : m2, n2 = lo2 ? 1 : m2 - 1;
+  x[0] = e1; x[1] = e1; x[2] = n1; x[3] = n1;
+  y[0] = e2; y[1] = n2; y[2] = e2; y[3] = n2;
+}
+__device__ __forceinline__ double edge_fit(const int x[4], const int y[4], double q1, double q2, double q3) {
+  const double b = ((q3 - q1) * (double)(x[2] - x[1]) - (q2 - q1) * (double)(x[3] - x[1])) /
+                   (double)((y[3] - y[1]) * (x[2] - x[1]) - (y[2] - y[1]) * (x[3] - x[1]));
+  const double a = (q2 - q1 - b * (double)(y[2] - y[1])) / (double)(x[2] - x[1]);
+  const double c = q1 - a * (double)x[1] - b * (double)y[1];
+  return a * (double)x[0] + b * (double)y[0] + c;
+}
+// one thread per (edge cell, variable, snapshot); nvar variables of stride
+// P3 per snapshot (q: npde, mut: 1)
+__global__ void k_edges(DevBlock b, int nvar, int S, double *__restrict__ q, int64_t base) {
+  const int nk = b.km - 1, nj = b.jm - 1;
+  const int64_t per = 4 * ((int64_t)nk + nj + (b.im - 1));
+  const int64_t total = per * nvar * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t % per;
+    const int64_t vn = t / per;
+    double *a = q + base + vn * b.P3;
+    int fam;
+    if (r < 4 * (int64_t)nk) fam = 0;
+    else if ((r -= 4 * (int64_t)nk) < 4 * (int64_t)nj) fam = 1;
+    else { r -= 4 * (int64_t)nj; fam = 2; }
+    const int ic = (int)(r % 4), tt = (int)(r / 4) + 1;
+    const int m1 = fam == 2 ? b.jm : b.im, m2 = fam == 0 ? b.jm : b.km;
+    int x[4], y[4];
+    edge_pts(ic, m1, m2, x, y);
+    auto at = [&](int p) -> int64_t {
+      if (fam == 0) return p3_cell(b, x[p], y[p], tt);
+      if (fam == 1) return p3_cell(b, x[p], tt, y[p]);
+      return p3_cell(b, tt, x[p], y[p]);
+    };
+    a[at(0)] = edge_fit(x, y, a[at(1)], a[at(2)], a[at(3)]);
+  }
+}
+
+// ---- q_bcorns (src/flux.f90:3156-3469) --------------------------------------------
+__device__ __forceinline__ void corner_pts(int ic, int im, int jm, int km, int x[5], int y[5], int z[5]) {
+  // ic 0..7: (i,j) = (0,0), (im,0), (im,jm), (0,jm) at k = 0 (ic < 4) or km
+  const int c4 = ic & 3;
+  const int hi = (c4 == 1 || c4 == 2), hj = (c4 == 2 || c4 == 3), hk = ic >= 4;
+  const int e1 = hi ? im : 0, n1 = hi ? im - 1 : 1;
+  const int e2 = hj ? jm : 0, n2 = hj ? jm - 1 : 1;
+  const int e3 = hk ? km : 0, n3 = hk ? km - 1 : 1;
+  x[0] = e1; y[0] = e2; z[0] = e3;
+  x[1] = e1; y[1] = n2; z[1] = n3;
+  x[2] = n1; y[2] = n2; z[2] = e3;
+  x[3] = n1; y[3] = e2; z[3] = n3;
+  x[4] = n1; y[4] = n2; z[4] = n3;
+}
+__device__ __forceinline__ double corner_fit(const int x[5], const int y[5], const int z[5], double q1, double q2,
+                                             double q3, double q4) {
+  // integer coefficient expressions of the reference (divisions by +-1)
+  const int dz = z[2] - z[1];
+  const int t1 = ((z[3] - z[1]) * (y[4] - y[1]) - (z[4] - z[1]) * (y[3] - y[1])) / dz;
+  const int t2 = ((z[2] - z[1]) * (y[1] - y[4]) + (z[4] - z[1]) * (y[2] - y[1])) / dz;
+  const int t3 = ((z[2] - z[1]) * (y[3] - y[1]) + (z[3] - z[1]) * (y[1] - y[2])) / dz;
+  const int den = ((x[4] - x[1]) * (y[3] - y[1]) + (x[1] - x[3]) * (y[4] - y[1])) +
+                  ((x[4] - x[1]) * (y[1] - y[2]) + (x[2] - x[1]) * (y[4] - y[1])) * (z[3] - z[1]) / dz +
+                  ((x[1] - x[2]) * (y[3] - y[1]) + (x[1] - x[3]) * (y[1] - y[2])) * (z[4] - z[1]) / dz;
+  const double a = ((double)t1 * (q2 - q1) + (double)t2 * (q3 - q1) + (double)t3 * (q4 - q1)) / (double)den;
+  const int e1 = (x[1] - x[3]) + (x[2] - x[1]) * (z[3] - z[1]) / dz;
+  const int f1 = (z[3] - z[1]) / dz;
+  const int g1 = (y[3] - y[1]) + (y[1] - y[2]) * (z[3] - z[1]) / dz;
+  const double bb = ((double)e1 * a + (double)f1 * (q1 - q2) + (q3 - q1)) / (double)g1;
+  const double c = ((double)(x[1] - x[2]) * a + (double)(y[1] - y[2]) * bb + (q2 - q1)) / (double)dz;
+  const double d = q1 - a * (double)x[1] - bb * (double)y[1] - c * (double)z[1];
+  return a * (double)x[0] + bb * (double)y[0] + c * (double)z[0] + d;
+}
+__global__ void k_corns(DevBlock b, int nvar, int S, double *__restrict__ q, int64_t base) {
+  const int total = 8 * nvar * S;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int ic = t % 8, vn = t / 8;
+    double *a = q + base + (int64_t)vn * b.P3;
+    int x[5], y[5], z[5];
+    corner_pts(ic, b.im, b.jm, b.km, x, y, z);
+    a[p3_cell(b, x[0], y[0], z[0])] =
+        corner_fit(x, y, z, a[p3_cell(b, x[1], y[1], z[1])], a[p3_cell(b, x[2], y[2], z[2])],
+                   a[p3_cell(b, x[3], y[3], z[3])], a[p3_cell(b, x[4], y[4], z[4])]);
+  }
+}
+
+// ---- add_array over cells 0..imax (src/util.f90:137-222, off_l = 1) -------------------
+__global__ void k_add_ext1(DevBlock b, int nvs, double *__restrict__ v1, const double *__restrict__ v2, double fact) {
+  const int ni = b.im + 1, nj = b.jm + 1, nk = b.km + 1;
+  const int64_t total = (int64_t)ni * nj * nk * nvs;
+  const int64_t base = b.op3 * nvs;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni); r /= ni;
+    const int j = (int)(r % nj); r /= nj;
+    const int k = (int)(r % nk); r /= nk;
+    const int64_t o = base + r * b.P3 + p3_cell(b, i, j, k);
+    v1[o] = v1[o] + v2[o] * fact;
+  }
+}
+
+// ---- prol_bln_b (src/cosa.f90:3478-3888) ------------------------------------------
+__device__ __forceinline__ double prol_w(double a, double b, double c, double d, double e, double f, double g,
+                                         double h) {
+  return (27 * a + 9 * b + 9 * c + 3 * d + 9 * e + 3 * f + 3 * g + h) / 64;
+}
+__device__ __forceinline__ double prol_lim2(double q, double c) {
+  if ((q + c) <= 0) {
+    if ((q + c / 2) > 0) return c / 2;
+    if ((q + c / 4) > 0) return c / 4;
+    return 0.0;
+  }
+  return c;
+}
+// one thread per (2x2x2 group of fine cells, variable, snapshot)
+__global__ void k_prol_bln(DevBlock b1, DevBlock b2, int npde, int S, double *__restrict__ q1,
+                           const double *__restrict__ q2, int lim_corr) {
+  const int gi = b2.im, gj = b2.jm, gk = b2.km;  // groups i1 = 0, 2, .., imax1-1
+  const int nv = lim_corr ? npde : (npde < 5 ? npde : 5);
+  const int64_t total = (int64_t)gi * gj * gk * nv * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i2 = (int)(r % gi); r /= gi;
+    const int j2 = (int)(r % gj); r /= gj;
+    const int k2 = (int)(r % gk); r /= gk;
+    const int v = (int)(r % nv) + 1; r /= nv;
+    const int n = (int)r;
+    const int i1 = 2 * i2, j1 = 2 * j2, k1 = 2 * k2;
+    const double *c = q2 + p3_var(b2, npde, S, v, n);
+    const double nel = c[p3_cell(b2, i2 + 1, j2 + 1, k2)], nwl = c[p3_cell(b2, i2, j2 + 1, k2)];
+    const double sel = c[p3_cell(b2, i2 + 1, j2, k2)], swl = c[p3_cell(b2, i2, j2, k2)];
+    const double neu = c[p3_cell(b2, i2 + 1, j2 + 1, k2 + 1)], nwu = c[p3_cell(b2, i2, j2 + 1, k2 + 1)];
+    const double seu = c[p3_cell(b2, i2 + 1, j2, k2 + 1)], swu = c[p3_cell(b2, i2, j2, k2 + 1)];
+    double f[8];  // sw_l, se_l, ne_l, nw_l, sw_u, se_u, ne_u, nw_u
+    f[0] = prol_w(swl, sel, nwl, nel, swu, seu, nwu, neu);
+    f[1] = prol_w(sel, swl, nel, nwl, seu, swu, neu, nwu);
+    f[2] = prol_w(nel, nwl, sel, swl, neu, nwu, seu, swu);
+    f[3] = prol_w(nwl, nel, swl, sel, nwu, neu, swu, seu);
+    f[4] = prol_w(swu, seu, nwu, neu, swl, sel, nwl, nel);
+    f[5] = prol_w(seu, swu, neu, nwu, sel, swl, nel, nwl);
+    f[6] = prol_w(neu, nwu, seu, swu, nel, nwl, sel, swl);
+    f[7] = prol_w(nwu, neu, swu, seu, nwl, nel, swl, sel);
+    double *a = q1 + p3_var(b1, npde, S, v, n);
+    int64_t o[8];
+    const int di[8] = {0, 1, 1, 0, 0, 1, 1, 0}, dj[8] = {0, 0, 1, 1, 0, 0, 1, 1}, dk[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+#pragma unroll
+    for (int s = 0; s < 8; ++s) o[s] = p3_cell(b1, i1 + di[s], j1 + dj[s], k1 + dk[s]);
+    double qv[8];
+#pragma unroll
+    for (int s = 0; s < 8; ++s) qv[s] = a[o[s]];
+    if (v >= 6 && lim_corr == 2) {
+      // lim_corr2: halve / quarter / drop a correction that makes the value
+      // non-positive; the NE tests read the SE values as the reference does
+      f[0] = prol_lim2(qv[0], f[0]);
+      f[1] = prol_lim2(qv[1], f[1]);
+      if ((qv[2] + f[2]) <= 0) {
+        if ((qv[2] + f[2] / 2) > 0) f[2] = f[2] / 2;
+        else if ((qv[1] + f[1] / 4) > 0) f[2] = f[2] / 4;
+        else f[2] = 0.0;
+      }
+      f[3] = prol_lim2(qv[3], f[3]);
+      f[4] = prol_lim2(qv[4], f[4]);
+      f[5] = prol_lim2(qv[5], f[5]);
+      if ((qv[6] + f[6]) <= 0) {
+        if ((qv[6] + f[6] / 2) > 0) f[6] = f[6] / 2;
+        else if ((qv[5] + f[5] / 4) > 0) f[6] = f[6] / 4;
+        else f[6] = 0.0;
+      }
+      f[7] = prol_lim2(qv[7], f[7]);
+    }
+    if (v >= 6 && lim_corr == 3) {
+#pragma unroll
+      for (int s = 0; s < 8; ++s) a[o[s]] = qv[s] + f[s] / (1 - 100.0 * fmin(f[s] / (qv[s] + 1.0e-12), 0.0));
+    } else {
+#pragma unroll
+      for (int s = 0; s < 8; ++s) a[o[s]] = qv[s] + f[s];
+    }
+  }
+}
+
+// ---- prol_lin_b (src/cosa.f90:3315-3476) ------------------------------------------
+__global__ void k_prol_lin(DevBlock b1, DevBlock b2, int npde, int S, double *__restrict__ q1,
+                           const double *__restrict__ q2, const double *__restrict__ vol1) {
+  const int gi = b2.im, gj = b2.jm, gk = b2.km;
+  const int64_t total = (int64_t)gi * gj * gk * npde * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i2 = (int)(r % gi); r /= gi;
+    const int j2 = (int)(r % gj); r /= gj;
+    const int k2 = (int)(r % gk); r /= gk;
+    const int v = (int)(r % npde) + 1; r /= npde;
+    const int n = (int)r;
+    const int i1 = 2 * i2, j1 = 2 * j2, k1 = 2 * k2;
+    const double *c = q2 + p3_var(b2, npde, S, v, n);
+    auto vol = [&](int i, int j, int k) { return vol1[p1_idx(b1, 1, i, j, k, 0)]; };
+    double f[2][4];  // [plane][sw, se, nw, ne]
+#pragma unroll
+    for (int pl = 0; pl < 2; ++pl) {
+      const int kc = k2 + pl, kf = k1 + pl;
+      const double cne = c[p3_cell(b2, i2 + 1, j2 + 1, kc)], cnw = c[p3_cell(b2, i2, j2 + 1, kc)];
+      const double cse = c[p3_cell(b2, i2 + 1, j2, kc)], csw = c[p3_cell(b2, i2, j2, kc)];
+      const double dn = cne - cnw, ds = cse - csw, de = cne - cse, dw = cnw - csw;
+      const double v00 = vol(i1, j1, kf), v10 = vol(i1 + 1, j1, kf), v01 = vol(i1, j1 + 1, kf),
+                   v11 = vol(i1 + 1, j1 + 1, kf);
+      f[pl][0] = csw + ds / 2 * v00 / (v00 + v10) + dw / 2 * v00 / (v00 + v01);
+      f[pl][1] = cse - ds / 2 * v10 / (v00 + v10) + de / 2 * v10 / (v10 + v11);
+      f[pl][2] = cnw + dn / 2 * v01 / (v01 + v11) - dw / 2 * v01 / (v00 + v01);
+      f[pl][3] = cne - dn / 2 * v11 / (v11 + v01) - de / 2 * v11 / (v11 + v10);
+    }
+    double *a = q1 + p3_var(b1, npde, S, v, n);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int ii = i1 + (s & 1), jj = j1 + (s >> 1);
+      const double fact = vol(ii, jj, k1) / 2 / (vol(ii, jj, k1) + vol(ii, jj, k1 + 1));
+      const int64_t lo = p3_cell(b1, ii, jj, k1), hi = p3_cell(b1, ii, jj, k1 + 1);
+      a[lo] = a[lo] + f[0][s] + fact / 2 * (f[1][s] - f[0][s]);
+      a[hi] = a[hi] + f[1][s] - (1 - fact) / 2 * (f[1][s] - f[0][s]);
+    }
+  }
+}
+
+// ---- fixq_b (src/update.f90:2216-2269) / tur_vis_b (2297-2337) --------------------------
+__global__ void k_fixq(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ q) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t total = (int64_t)ni * nj * nk * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)(r % nk) + 1; r /= nk;
+    const int n = (int)r;
+    const int64_t c = p3_cell(b, i, j, k);
+    const double rho = q[p3_var(b, npde, S, 1, n) + c];
+    double *qk = q + p3_var(b, npde, S, 6, n) + c, *qw = q + p3_var(b, npde, S, 7, n) + c;
+    const double tke = *qk / rho, ome = *qw / rho;
+    if (tke < P.qmin[5]) *qk = rho * P.qmin[5];
+    if (ome < P.qmin[6]) *qw = rho * P.qmin[6];
+  }
+}
+__global__ void k_tur_vis(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
+                          double *__restrict__ mut) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ni = b.im + 1, nj = b.jm + 1, nk = b.km + 1;
+  const int64_t total = (int64_t)ni * nj * nk * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni); r /= ni;
+    const int j = (int)(r % nj); r /= nj;
+    const int k = (int)(r % nk); r /= nk;
+    const int n = (int)r;
+    const int64_t c = p3_cell(b, i, j, k);
+    const double rho = q[p3_var(b, npde, S, 1, n) + c], tke = q[p3_var(b, npde, S, 6, n) + c];
+    const double ome = q[p3_var(b, npde, S, 7, n) + c];
+    mut[b.op3 * S + (int64_t)n * b.P3 + c] = P.cmu * rho * tke / (ome + P.epst) * P.reyno / P.machfs;
+  }
+}

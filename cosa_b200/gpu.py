@@ -54,7 +54,9 @@ SYMBOLS = [
     "cosa_gpu_zero", "cosa_gpu_smooth", "cosa_gpu_smooth_host", "cosa_gpu_launch_count",
     "cosa_gpu_status", "cosa_gpu_imetrix", "cosa_gpu_vols", "cosa_gpu_profile", "cosa_gpu_stream",
     "cosa_gpu_resg_rms_noalloc", "cosa_gpu_scalef", "cosa_gpu_scaleb", "cosa_gpu_cirs", "cosa_gpu_ccirs",
-    "cosa_gpu_src_hb",
+    "cosa_gpu_src_hb", "cosa_gpu_q_edges", "cosa_gpu_q_corns", "cosa_gpu_fixq", "cosa_gpu_tur_vis",
+    "cosa_gpu_rest1", "cosa_gpu_rest2", "cosa_gpu_prol_bln", "cosa_gpu_prol_lin", "cosa_gpu_restrict",
+    "cosa_gpu_prolong", "cosa_gpu_smooth_level", "cosa_gpu_mg",
 ]
 
 
@@ -280,6 +282,50 @@ class Context:
         st = load().cosa_gpu_smooth(self.h, nl, niter, mgit0, rms_every,
                                     hist.ctypes.data_as(_dp) if want_hist else _dp())
         return (hist[:niter] if want_hist else None), st
+
+    # ---- multigrid ---------------------------------------------------------------
+    def q_edges(self, nl, q, mut=None):
+        self._check(load().cosa_gpu_q_edges(self.h, nl, _ptr(q.ptr), _ptr(mut.ptr if mut else None)), "q_edges")
+
+    def q_corns(self, nl, q, mut=None):
+        self._check(load().cosa_gpu_q_corns(self.h, nl, _ptr(q.ptr), _ptr(mut.ptr if mut else None)), "q_corns")
+
+    def fixq(self, nl, q):
+        self._check(load().cosa_gpu_fixq(self.h, nl, _ptr(q.ptr)), "fixq")
+
+    def tur_vis(self, nl, q, mut):
+        self._check(load().cosa_gpu_tur_vis(self.h, nl, _ptr(q.ptr), _ptr(mut.ptr)), "tur_vis")
+
+    def rest1(self, nl, q1, q2, vol1, vol2):
+        self._check(load().cosa_gpu_rest1(self.h, nl, _ptr(q1.ptr), _ptr(q2.ptr), _ptr(vol1.ptr), _ptr(vol2.ptr)),
+                    "rest1")
+
+    def rest2(self, nl, rhs2, res1):
+        self._check(load().cosa_gpu_rest2(self.h, nl, _ptr(rhs2.ptr), _ptr(res1.ptr)), "rest2")
+
+    def prol_bln(self, nl, q1, q2):
+        self._check(load().cosa_gpu_prol_bln(self.h, nl, _ptr(q1.ptr), _ptr(q2.ptr)), "prol_bln")
+
+    def prol_lin(self, nl, q1, q2, vol1):
+        self._check(load().cosa_gpu_prol_lin(self.h, nl, _ptr(q1.ptr), _ptr(q2.ptr), _ptr(vol1.ptr)), "prol_lin")
+
+    def restrict(self, nl):
+        self._check(load().cosa_gpu_restrict(self.h, nl), "restrict")
+
+    def prolong(self, nl) -> int:
+        return load().cosa_gpu_prolong(self.h, nl)
+
+    def smooth_level(self, nl, niter, from_fine, to_coarse, mgit=1, ncycle=1, rms_every=1, want_rms=True):
+        out = np.full(self.params.npde + 1, np.nan)
+        st = load().cosa_gpu_smooth_level(self.h, nl, niter, int(from_fine), int(to_coarse), mgit, ncycle, rms_every,
+                                          out.ctypes.data_as(_dp) if want_rms else _dp())
+        return out, st
+
+    def mg(self, mgit0, ncycles, ncycle, rms_every=1, want_hist=True):
+        hist = np.full((max(ncycles, 1), self.params.npde + 1), np.nan) if want_hist else None
+        st = load().cosa_gpu_mg(self.h, mgit0, ncycles, ncycle, rms_every,
+                                hist.ctypes.data_as(_dp) if want_hist else _dp())
+        return (hist[:ncycles] if want_hist else None), st
 
     def smooth_host(self, nl, q_host: np.ndarray, niter, mgit0=1, rms_every=1, want_hist=True):
         hist = np.full((max(niter, 1), self.params.npde + 1), np.nan) if want_hist else None

@@ -59,7 +59,9 @@ class CosaParams(C.Structure):
         ("omega", C.c_double),
         ("dhb", C.c_double * (MAX_SNAP * MAX_SNAP)),
         ("precision", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("nstart", C.c_int32), ("npre", C.c_int32), ("npost", C.c_int32), ("ncrs", C.c_int32),
+        ("bln_prol", C.c_int32), ("lim_corr", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -113,6 +115,10 @@ def default_params() -> CosaParams:
     for i in range(3):
         p.outlet_p[i] = 0.714285714285714
     p.precision = PREC_FP64
+    # multigrid: one smoothing iteration per visit, bilinear prolongation
+    p.nstart = p.npre = p.npost = p.ncrs = 1
+    p.bln_prol = 1
+    p.lim_corr = 0
     return p
 
 

@@ -96,7 +96,12 @@ typedef struct cosa_params {
   double dhb[COSA_MAX_SNAP * COSA_MAX_SNAP]; /* dhb[n*S + m] = D(n,m) */
   /* GPU-only knobs */
   int32_t precision;    /* COSA_PREC_FP64 | COSA_PREC_MIXED */
-  int32_t reserved[7];
+  /* multigrid controls (src/input.f90:3509-3570, common/mgpars):
+     iterations per visit nstart (fine, first cycle), npre, npost, ncrs
+     (coarsest); bln_prol 1 = bilinear prol_bln, 0 = linear prol_lin;
+     lim_corr 0..3 = none / lim_corr1..3 of prol_bln (turbulence only) */
+  int32_t nstart, npre, npost, ncrs, bln_prol, lim_corr;
+  int32_t reserved[6];
 } cosa_params;
 
 /*
@@ -214,6 +219,44 @@ int cosa_gpu_imetrix(cosa_ctx *ctx, int32_t nl, const double *x, const double *y
 int cosa_gpu_vols(cosa_ctx *ctx, int32_t nl, const double *x, const double *y,
                   const double *z, double *vol);
 
+/* q_edges / q_corns (src/flux.f90:3889-4263, 3132-3469): linear
+   extrapolation of q (and of mut when mut != NULL, calmut) into the halo
+   edge cells (plane through three neighbours) and the 8 halo corner cells
+   (plane through four neighbours) of every block */
+int cosa_gpu_q_edges(cosa_ctx *ctx, int32_t nl, double *q, double *mut);
+int cosa_gpu_q_corns(cosa_ctx *ctx, int32_t nl, double *q, double *mut);
+/* fixq (src/update.f90:2191-2269): k and omega floors qmin(6:7), npde = 7 */
+int cosa_gpu_fixq(cosa_ctx *ctx, int32_t nl, double *q);
+/* tur_vis (src/update.f90:2271-2337): mut = cmu rho k/(omega+epst) Re/M
+   over cells 0..imax of every block (q conservative) */
+int cosa_gpu_tur_vis(cosa_ctx *ctx, int32_t nl, const double *q, double *mut);
+
+/* ---- multigrid transfers between level nl (fine) and nl+1 (coarse) ---- */
+/* rest1 (src/cosa.f90:2757-2833): q2 = volume-weighted mean of the 8 fine
+   cells of each coarse interior cell */
+int cosa_gpu_rest1(cosa_ctx *ctx, int32_t nl, const double *q1, double *q2,
+                   const double *vol1, const double *vol2);
+/* rest2 with lo_rest (src/cosa.f90:2835-2869, 2955-3012):
+   rhs2 = -(sum of the 8 fine residuals) */
+int cosa_gpu_rest2(cosa_ctx *ctx, int32_t nl, double *rhs2, const double *res1);
+/* prol_bln (src/cosa.f90:3282-3313, 3478-3888): q1 += trilinear
+   27/9/3/1 interpolation of the coarse correction q2 on fine cells
+   0..imax (one halo layer), lim_corr from params for npde = 7 */
+int cosa_gpu_prol_bln(cosa_ctx *ctx, int32_t nl, double *q1, const double *q2);
+/* prol_lin (src/cosa.f90:3252-3280, 3315-3476): volume-weighted variant;
+   vol1 must hold the halo volumes (volex/cutman_v/vol_edges) */
+int cosa_gpu_prol_lin(cosa_ctx *ctx, int32_t nl, double *q1, const double *q2,
+                      const double *vol1);
+/* restrict (src/cosa.f90:2672-2755), Euler branch, on bound levels nl and
+   nl+1: rest1 of q into q(nl+1), rest2 of res(nl) into rhs(nl+1) */
+int cosa_gpu_restrict(cosa_ctx *ctx, int32_t nl);
+/* prolong (src/cosa.f90:3167-3250) on bound levels nl and nl+1:
+   qold(nl+1) = rest1(q(nl)); both coarse states through cons2prim, bc,
+   cutman_q, prim2cons, q_edges, q_corns; q(nl+1) -= qold(nl+1) over cells
+   0..imax; then prol_bln (bln_prol) or prol_lin into q(nl); fixq for
+   lim_corr 1 and 3 */
+int cosa_gpu_prolong(cosa_ctx *ctx, int32_t nl);
+
 /* ---- fused: what smooth() calls when the GPU path is on ---- */
 /*
  * One RK iteration sequence of smooth() (src/cosa.f90:1711-2029) on the
@@ -228,6 +271,28 @@ int cosa_gpu_smooth(cosa_ctx *ctx, int32_t nl, int32_t niter, int32_t mgit0,
 int cosa_gpu_smooth_host(cosa_ctx *ctx, int32_t nl, double *q_host,
                          int32_t niter, int32_t mgit0, int32_t rms_every,
                          double *hist);
+/*
+ * smooth(nl, from_fine, to_coarse, done, niter) (src/cosa.f90:1594-2032) on
+ * the bound level nl: niter RK iterations; with to_coarse one more stage-1
+ * residual pass whose result (res - rhs on coarse levels) is left in the
+ * level's res array for restrict; on coarse levels the forcing rhs += res at
+ * the first stage of a from_fine visit and res -= rhs at every stage.  mgit
+ * and ncycle select the printed cycle (mgit == 1, mgit % rms_every == 0 or
+ * mgit == ncycle) whose fine-level resrms[0..npde] goes to resrms (NULL:
+ * none).  The convergence test `done` is left to the caller.
+ */
+int cosa_gpu_smooth_level(cosa_ctx *ctx, int32_t nl, int32_t niter, int32_t from_fine,
+                          int32_t to_coarse, int32_t mgit, int32_t ncycle,
+                          int32_t rms_every, double *resrms);
+/*
+ * mg() (src/cosa.f90:806-930): cycles mgit0 .. mgit0+ncycles-1 of a run of
+ * ncycle multigrid V-cycles on the nlevel (params) bound levels; smoothing
+ * counts nstart/npre/npost/ncrs from params.  When the last cycle run is
+ * ncycle, the final npost fine-level smoothing follows.  hist as in
+ * cosa_gpu_smooth, one row per cycle.
+ */
+int cosa_gpu_mg(cosa_ctx *ctx, int32_t mgit0, int32_t ncycles, int32_t ncycle,
+                int32_t rms_every, double *hist);
 /* niter fused iterations without graphs, with CUDA events around every
    kernel: ms[0] = mean halo-kernel time, ms[1] = mean tile-kernel time,
    ms[2] = mean iteration time; counts = launches timed */

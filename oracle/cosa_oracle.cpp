@@ -1251,6 +1251,317 @@ void bvols(const Level &L, int b, const double *xa, const double *ya, const doub
       }
 }
 
+// ---- multigrid transfers ---------------------------------------------------
+// rest1_b (src/cosa.f90:2788-2833): volume-weighted restriction of the
+// solution onto the coarse interior cells
+void rest1_b(const Level &L1, const Level &L2, int b, const double *q1a, double *q2a, const double *v1a,
+             const double *v2a) {
+  B3 q1(const_cast<double *>(q1a), L1, b), q2(q2a, L2, b);
+  B1 v1(const_cast<double *>(v1a), L1, b, 1), v2(const_cast<double *>(v2a), L2, b, 1);
+  const int im1 = L1.im[b], jm1 = L1.jm[b], km1 = L1.km[b];
+  for (int n = 0; n < L1.S; ++n)
+    for (int k1 = 1; k1 <= km1 - 2; k1 += 2)
+      for (int j1 = 1; j1 <= jm1 - 2; j1 += 2)
+        for (int i1 = 1; i1 <= im1 - 2; i1 += 2) {
+          const int i2 = 1 + i1 / 2, j2 = 1 + j1 / 2, k2 = 1 + k1 / 2;
+          for (int v = 1; v <= L1.npde; ++v)
+            q2(i2, j2, k2, v, n) =
+                (v1(i1, j1, k1) * q1(i1, j1, k1, v, n) + v1(i1, j1 + 1, k1) * q1(i1, j1 + 1, k1, v, n) +
+                 v1(i1 + 1, j1, k1) * q1(i1 + 1, j1, k1, v, n) + v1(i1 + 1, j1 + 1, k1) * q1(i1 + 1, j1 + 1, k1, v, n) +
+                 v1(i1, j1, k1 + 1) * q1(i1, j1, k1 + 1, v, n) + v1(i1, j1 + 1, k1 + 1) * q1(i1, j1 + 1, k1 + 1, v, n) +
+                 v1(i1 + 1, j1, k1 + 1) * q1(i1 + 1, j1, k1 + 1, v, n) +
+                 v1(i1 + 1, j1 + 1, k1 + 1) * q1(i1 + 1, j1 + 1, k1 + 1, v, n)) /
+                v2(i2, j2, k2);
+        }
+}
+
+// rest2_lo_b (src/cosa.f90:2955-3012): rhs2 = -(sum of the 8 fine residuals)
+void rest2_lo_b(const Level &L1, const Level &L2, int b, double *rhs2a, const double *res1a) {
+  B3 r1(const_cast<double *>(res1a), L1, b), rhs2(rhs2a, L2, b);
+  const int im1 = L1.im[b], jm1 = L1.jm[b], km1 = L1.km[b];
+  for (int n = 0; n < L1.S; ++n)
+    for (int v = 1; v <= L1.npde; ++v)
+      for (int k1 = 1; k1 <= km1 - 2; k1 += 2)
+        for (int j1 = 1; j1 <= jm1 - 2; j1 += 2)
+          for (int i1 = 1; i1 <= im1 - 2; i1 += 2) {
+            const int i2 = 1 + i1 / 2, j2 = 1 + j1 / 2, k2 = 1 + k1 / 2;
+            rhs2(i2, j2, k2, v, n) =
+                -(r1(i1, j1, k1, v, n) + r1(i1, j1 + 1, k1, v, n) + r1(i1 + 1, j1, k1, v, n) +
+                  r1(i1 + 1, j1 + 1, k1, v, n) + r1(i1, j1, k1 + 1, v, n) + r1(i1, j1 + 1, k1 + 1, v, n) +
+                  r1(i1 + 1, j1, k1 + 1, v, n) + r1(i1 + 1, j1 + 1, k1 + 1, v, n));
+          }
+}
+
+// q_bedges (src/flux.f90:3913-4263): the plane through three neighbours of
+// each halo edge cell, evaluated at the edge cell.  Edge families: (i,j) at
+// every interior k, (i,k) at every interior j, (j,k) at every interior i.
+struct Edge2 { int x[4], y[4]; };
+inline void edge_fit(double q1, double q2, double q3, const Edge2 &e, double &out) {
+  const int x0 = e.x[0], y0 = e.y[0], x1 = e.x[1], y1 = e.y[1], x2 = e.x[2], y2 = e.y[2], x3 = e.x[3], y3 = e.y[3];
+  const double b = ((q3 - q1) * (double)(x2 - x1) - (q2 - q1) * (double)(x3 - x1)) /
+                   (double)((y3 - y1) * (x2 - x1) - (y2 - y1) * (x3 - x1));
+  const double a = (q2 - q1 - b * (double)(y2 - y1)) / (double)(x2 - x1);
+  const double c = q1 - a * (double)x1 - b * (double)y1;
+  out = a * (double)x0 + b * (double)y0 + c;
+}
+// the 4 edges of one family: points 0 (target), 1, 2, 3 in the reference's order
+inline void edge_table(int m1, int m2, Edge2 e[4]) {
+  e[0] = {{0, 0, 1, 1}, {0, 1, 0, 1}};
+  e[1] = {{m1, m1, m1 - 1, m1 - 1}, {0, 1, 0, 1}};
+  e[2] = {{m1, m1, m1 - 1, m1 - 1}, {m2, m2 - 1, m2, m2 - 1}};
+  e[3] = {{0, 0, 1, 1}, {m2, m2 - 1, m2, m2 - 1}};
+}
+void q_bedges(const Level &L, int b, double *qa, double *muta) {
+  B3 q(qa, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  Edge2 eij[4], eik[4], ejk[4];
+  edge_table(im, jm, eij);
+  edge_table(im, km, eik);
+  edge_table(jm, km, ejk);
+  auto fam = [&](auto &&at, int nv, int nsnap, const Edge2 *E, int lo, int hi) {
+    for (int n = 0; n < nsnap; ++n)
+      for (int v = 1; v <= nv; ++v)
+        for (int t = lo; t <= hi; ++t)
+          for (int ic = 0; ic < 4; ++ic) {
+            const Edge2 &e = E[ic];
+            double o;
+            edge_fit(at(e.x[1], e.y[1], t, v, n), at(e.x[2], e.y[2], t, v, n), at(e.x[3], e.y[3], t, v, n), e, o);
+            at(e.x[0], e.y[0], t, v, n) = o;
+          }
+  };
+  auto qij = [&](int a, int c, int t, int v, int n) -> double & { return q(a, c, t, v, n); };
+  auto qik = [&](int a, int c, int t, int v, int n) -> double & { return q(a, t, c, v, n); };
+  auto qjk = [&](int a, int c, int t, int v, int n) -> double & { return q(t, a, c, v, n); };
+  if (muta) {
+    B3s mu(muta, L, b);
+    auto mij = [&](int a, int c, int t, int, int n) -> double & { return mu(a, c, t, n); };
+    auto mik = [&](int a, int c, int t, int, int n) -> double & { return mu(a, t, c, n); };
+    auto mjk = [&](int a, int c, int t, int, int n) -> double & { return mu(t, a, c, n); };
+    fam(qij, L.npde, L.S, eij, 1, km - 1); fam(mij, 1, L.S, eij, 1, km - 1);
+    fam(qik, L.npde, L.S, eik, 1, jm - 1); fam(mik, 1, L.S, eik, 1, jm - 1);
+    fam(qjk, L.npde, L.S, ejk, 1, im - 1); fam(mjk, 1, L.S, ejk, 1, im - 1);
+  } else {
+    fam(qij, L.npde, L.S, eij, 1, km - 1);
+    fam(qik, L.npde, L.S, eik, 1, jm - 1);
+    fam(qjk, L.npde, L.S, ejk, 1, im - 1);
+  }
+}
+
+// q_bcorns (src/flux.f90:3156-3469): the plane a i + b j + c k + d through
+// four neighbours of each of the 8 halo corner cells.  The coefficient
+// expressions are integer arithmetic in the reference (every integer
+// division is by +-1, so exact); they are kept as ints here.
+struct Corner { int x[5], y[5], z[5]; };
+inline void corner_table(int im, int jm, int km, Corner c[8]) {
+  // points 0 (target), 1..4 in the reference's order (ijkc(:,0:4,ic))
+  c[0] = {{0, 0, 1, 1, 1}, {0, 1, 1, 0, 1}, {0, 1, 0, 1, 1}};
+  c[1] = {{im, im, im - 1, im - 1, im - 1}, {0, 1, 1, 0, 1}, {0, 1, 0, 1, 1}};
+  c[2] = {{im, im, im - 1, im - 1, im - 1}, {jm, jm - 1, jm - 1, jm, jm - 1}, {0, 1, 0, 1, 1}};
+  c[3] = {{0, 0, 1, 1, 1}, {jm, jm - 1, jm - 1, jm, jm - 1}, {0, 1, 0, 1, 1}};
+  c[4] = {{0, 0, 1, 1, 1}, {0, 1, 1, 0, 1}, {km, km - 1, km, km - 1, km - 1}};
+  c[5] = {{im, im, im - 1, im - 1, im - 1}, {0, 1, 1, 0, 1}, {km, km - 1, km, km - 1, km - 1}};
+  c[6] = {{im, im, im - 1, im - 1, im - 1}, {jm, jm - 1, jm - 1, jm, jm - 1}, {km, km - 1, km, km - 1, km - 1}};
+  c[7] = {{0, 0, 1, 1, 1}, {jm, jm - 1, jm - 1, jm, jm - 1}, {km, km - 1, km, km - 1, km - 1}};
+}
+inline double corner_fit(const Corner &C, double q1, double q2, double q3, double q4) {
+  const int *x = C.x, *y = C.y, *z = C.z;
+  const int dz = z[2] - z[1];
+  const int t1 = ((z[3] - z[1]) * (y[4] - y[1]) - (z[4] - z[1]) * (y[3] - y[1])) / dz;
+  const int t2 = ((z[2] - z[1]) * (y[1] - y[4]) + (z[4] - z[1]) * (y[2] - y[1])) / dz;
+  const int t3 = ((z[2] - z[1]) * (y[3] - y[1]) + (z[3] - z[1]) * (y[1] - y[2])) / dz;
+  const int den = ((x[4] - x[1]) * (y[3] - y[1]) + (x[1] - x[3]) * (y[4] - y[1])) +
+                  ((x[4] - x[1]) * (y[1] - y[2]) + (x[2] - x[1]) * (y[4] - y[1])) * (z[3] - z[1]) / dz +
+                  ((x[1] - x[2]) * (y[3] - y[1]) + (x[1] - x[3]) * (y[1] - y[2])) * (z[4] - z[1]) / dz;
+  const double a = ((double)t1 * (q2 - q1) + (double)t2 * (q3 - q1) + (double)t3 * (q4 - q1)) / (double)den;
+  const int e1 = (x[1] - x[3]) + (x[2] - x[1]) * (z[3] - z[1]) / dz;
+  const int f1 = (z[3] - z[1]) / dz;
+  const int g1 = (y[3] - y[1]) + (y[1] - y[2]) * (z[3] - z[1]) / dz;
+  const double bb = ((double)e1 * a + (double)f1 * (q1 - q2) + (q3 - q1)) / (double)g1;
+  const double c = ((double)(x[1] - x[2]) * a + (double)(y[1] - y[2]) * bb + (q2 - q1)) / (double)dz;
+  const double d = q1 - a * (double)x[1] - bb * (double)y[1] - c * (double)z[1];
+  return a * (double)x[0] + bb * (double)y[0] + c * (double)z[0] + d;
+}
+void q_bcorns(const Level &L, int b, double *qa, double *muta) {
+  B3 q(qa, L, b);
+  Corner C[8];
+  corner_table(L.im[b], L.jm[b], L.km[b], C);
+  for (int n = 0; n < L.S; ++n)
+    for (int v = 1; v <= L.npde; ++v)
+      for (int ic = 0; ic < 8; ++ic) {
+        const Corner &c = C[ic];
+        q(c.x[0], c.y[0], c.z[0], v, n) =
+            corner_fit(c, q(c.x[1], c.y[1], c.z[1], v, n), q(c.x[2], c.y[2], c.z[2], v, n),
+                       q(c.x[3], c.y[3], c.z[3], v, n), q(c.x[4], c.y[4], c.z[4], v, n));
+      }
+  if (muta) {
+    B3s mu(muta, L, b);
+    for (int n = 0; n < L.S; ++n)
+      for (int ic = 0; ic < 8; ++ic) {
+        const Corner &c = C[ic];
+        mu(c.x[0], c.y[0], c.z[0], n) = corner_fit(c, mu(c.x[1], c.y[1], c.z[1], n), mu(c.x[2], c.y[2], c.z[2], n),
+                                                   mu(c.x[3], c.y[3], c.z[3], n), mu(c.x[4], c.y[4], c.z[4], n));
+      }
+  }
+}
+
+// prol_bln_b (src/cosa.f90:3478-3888): trilinear (27/9/3/1)/64 prolongation
+// of the coarse correction onto fine cells 0..imax1 (one halo layer
+// included); turbulence variables only with one of the three positivity
+// options (lim_corr 1..3).
+inline double prol_w(double a, double b, double c, double d, double e, double f, double g, double h) {
+  return (27 * a + 9 * b + 9 * c + 3 * d + 9 * e + 3 * f + 3 * g + h) / 64;
+}
+inline double lim2(double q, double c) {
+  if ((q + c) <= 0) {
+    if ((q + c / 2) > 0) return c / 2;
+    if ((q + c / 4) > 0) return c / 4;
+    return 0.0;
+  }
+  return c;
+}
+void prol_bln_b(const Level &L1, const Level &L2, int b, double *q1a, const double *q2a, int lim_corr) {
+  B3 q1(q1a, L1, b), q2(const_cast<double *>(q2a), L2, b);
+  const int im1 = L1.im[b], jm1 = L1.jm[b], km1 = L1.km[b];
+  const double beta = 100.0, epsl = 1.0e-12;
+  for (int n = 0; n < L1.S; ++n)
+    for (int v = 1; v <= L1.npde; ++v) {
+      if (v >= 6 && lim_corr == 0) continue;
+      for (int k1 = 0; k1 <= km1 - 1; k1 += 2)
+        for (int j1 = 0; j1 <= jm1 - 1; j1 += 2)
+          for (int i1 = 0; i1 <= im1 - 1; i1 += 2) {
+            const int i2 = i1 / 2, j2 = j1 / 2, k2 = k1 / 2;
+            const double nel = q2(i2 + 1, j2 + 1, k2, v, n), nwl = q2(i2, j2 + 1, k2, v, n);
+            const double sel = q2(i2 + 1, j2, k2, v, n), swl = q2(i2, j2, k2, v, n);
+            const double neu = q2(i2 + 1, j2 + 1, k2 + 1, v, n), nwu = q2(i2, j2 + 1, k2 + 1, v, n);
+            const double seu = q2(i2 + 1, j2, k2 + 1, v, n), swu = q2(i2, j2, k2 + 1, v, n);
+            double swf_l = prol_w(swl, sel, nwl, nel, swu, seu, nwu, neu);
+            double sef_l = prol_w(sel, swl, nel, nwl, seu, swu, neu, nwu);
+            double nef_l = prol_w(nel, nwl, sel, swl, neu, nwu, seu, swu);
+            double nwf_l = prol_w(nwl, nel, swl, sel, nwu, neu, swu, seu);
+            double swf_u = prol_w(swu, seu, nwu, neu, swl, sel, nwl, nel);
+            double sef_u = prol_w(seu, swu, neu, nwu, sel, swl, nel, nwl);
+            double nef_u = prol_w(neu, nwu, seu, swu, nel, nwl, sel, swl);
+            double nwf_u = prol_w(nwu, neu, swu, seu, nwl, nel, swl, sel);
+            double &a0 = q1(i1, j1, k1, v, n), &a1 = q1(i1 + 1, j1, k1, v, n);
+            double &a2 = q1(i1 + 1, j1 + 1, k1, v, n), &a3 = q1(i1, j1 + 1, k1, v, n);
+            double &a4 = q1(i1, j1, k1 + 1, v, n), &a5 = q1(i1 + 1, j1, k1 + 1, v, n);
+            double &a6 = q1(i1 + 1, j1 + 1, k1 + 1, v, n), &a7 = q1(i1, j1 + 1, k1 + 1, v, n);
+            if (v >= 6 && lim_corr == 2) {
+              // the NE limits test the SE values in the reference (kept)
+              const double qsw_l = a0, qse_l = a1, qne_l = a2, qnw_l = a3;
+              const double qsw_u = a4, qse_u = a5, qne_u = a6, qnw_u = a7;
+              swf_l = lim2(qsw_l, swf_l);
+              sef_l = lim2(qse_l, sef_l);
+              if ((qne_l + nef_l) <= 0) {
+                if ((qne_l + nef_l / 2) > 0) nef_l = nef_l / 2;
+                else if ((qse_l + sef_l / 4) > 0) nef_l = nef_l / 4;
+                else nef_l = 0.0;
+              }
+              nwf_l = lim2(qnw_l, nwf_l);
+              swf_u = lim2(qsw_u, swf_u);
+              sef_u = lim2(qse_u, sef_u);
+              if ((qne_u + nef_u) <= 0) {
+                if ((qne_u + nef_u / 2) > 0) nef_u = nef_u / 2;
+                else if ((qse_u + sef_u / 4) > 0) nef_u = nef_u / 4;
+                else nef_u = 0.0;
+              }
+              nwf_u = lim2(qnw_u, nwf_u);
+            }
+            if (v >= 6 && lim_corr == 3) {
+              auto el = [&](double &q, double c) { q = q + c / (1 - beta * std::min(c / (q + epsl), 0.0)); };
+              el(a0, swf_l); el(a1, sef_l); el(a2, nef_l); el(a3, nwf_l);
+              el(a4, swf_u); el(a5, sef_u); el(a6, nef_u); el(a7, nwf_u);
+            } else {
+              a0 = a0 + swf_l; a1 = a1 + sef_l; a2 = a2 + nef_l; a3 = a3 + nwf_l;
+              a4 = a4 + swf_u; a5 = a5 + sef_u; a6 = a6 + nef_u; a7 = a7 + nwf_u;
+            }
+          }
+    }
+}
+
+// prol_lin_b (src/cosa.f90:3315-3476): volume-weighted bilinear interpolation
+// in each coarse k plane, then a volume-weighted blend between the planes
+void prol_lin_b(const Level &L1, const Level &L2, int b, double *q1a, const double *q2a, const double *v1a) {
+  B3 q1(q1a, L1, b), q2(const_cast<double *>(q2a), L2, b);
+  B1 vol(const_cast<double *>(v1a), L1, b, 1);
+  const int im1 = L1.im[b], jm1 = L1.jm[b], km1 = L1.km[b];
+  for (int n = 0; n < L1.S; ++n)
+    for (int v = 1; v <= L1.npde; ++v)
+      for (int k1 = 0; k1 <= km1 - 1; k1 += 2)
+        for (int j1 = 0; j1 <= jm1 - 1; j1 += 2)
+          for (int i1 = 0; i1 <= im1 - 1; i1 += 2) {
+            const int i2 = i1 / 2, j2 = j1 / 2, k2 = k1 / 2;
+            double f[2][4];  // [plane][sw, se, nw, ne]
+            for (int pl = 0; pl < 2; ++pl) {
+              const int kc = k2 + pl, kf = k1 + pl;
+              const double cne = q2(i2 + 1, j2 + 1, kc, v, n), cnw = q2(i2, j2 + 1, kc, v, n);
+              const double cse = q2(i2 + 1, j2, kc, v, n), csw = q2(i2, j2, kc, v, n);
+              const double dn = cne - cnw, ds = cse - csw, de = cne - cse, dw = cnw - csw;
+              const double v00 = vol(i1, j1, kf), v10 = vol(i1 + 1, j1, kf), v01 = vol(i1, j1 + 1, kf),
+                           v11 = vol(i1 + 1, j1 + 1, kf);
+              f[pl][0] = csw + ds / 2 * v00 / (v00 + v10) + dw / 2 * v00 / (v00 + v01);
+              f[pl][1] = cse - ds / 2 * v10 / (v00 + v10) + de / 2 * v10 / (v10 + v11);
+              f[pl][2] = cnw + dn / 2 * v01 / (v01 + v11) - dw / 2 * v01 / (v00 + v01);
+              f[pl][3] = cne - dn / 2 * v11 / (v11 + v01) - de / 2 * v11 / (v11 + v10);
+            }
+            const int di[4] = {0, 1, 0, 1}, dj[4] = {0, 0, 1, 1};
+            // reference order of the corrections: sw, se, ne, nw
+            const int ord[4] = {0, 1, 3, 2};
+            for (int t = 0; t < 4; ++t) {
+              const int c = ord[t], ii = i1 + di[c], jj = j1 + dj[c];
+              const double fact = vol(ii, jj, k1) / 2 / (vol(ii, jj, k1) + vol(ii, jj, k1 + 1));
+              q1(ii, jj, k1, v, n) = q1(ii, jj, k1, v, n) + f[0][c] + fact / 2 * (f[1][c] - f[0][c]);
+              q1(ii, jj, k1 + 1, v, n) = q1(ii, jj, k1 + 1, v, n) + f[1][c] - (1 - fact) / 2 * (f[1][c] - f[0][c]);
+            }
+          }
+}
+
+// add_array over cells 0..imax (off_l = 1) or the interior (off_l = -1)
+// (src/util.f90:137-222)
+void add_level(const Level &L, double *v1a, const double *v2a, double fact, int off_l) {
+  const int lo = off_l == 1 ? 0 : 1, hi_off = off_l == 1 ? 0 : -1;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 a(v1a, L, b), c(const_cast<double *>(v2a), L, b);
+    for (int n = 0; n < L.S; ++n)
+      for (int v = 1; v <= L.npde; ++v)
+        for (int k = lo; k <= L.km[b] + hi_off; ++k)
+          for (int j = lo; j <= L.jm[b] + hi_off; ++j)
+            for (int i = lo; i <= L.im[b] + hi_off; ++i) a(i, j, k, v, n) = a(i, j, k, v, n) + c(i, j, k, v, n) * fact;
+  }
+}
+
+// fixq_b (src/update.f90:2216-2269): floors of k and omega
+void fixq_level(const Level &L, double *qa, const cosa_params &P) {
+  if (L.npde < 7) return;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 q(qa, L, b);
+    for (int n = 0; n < L.S; ++n)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            const double rho = q(i, j, k, 1, n);
+            double tke = q(i, j, k, 6, n) / rho, ome = q(i, j, k, 7, n) / rho;
+            if (tke < P.qmin[5]) { tke = P.qmin[5]; q(i, j, k, 6, n) = rho * tke; }
+            if (ome < P.qmin[6]) { ome = P.qmin[6]; q(i, j, k, 7, n) = rho * ome; }
+          }
+  }
+}
+
+// tur_vis_b (src/update.f90:2297-2337): mut over cells 0..imax
+void tur_vis_level(const Level &L, const double *qa, double *muta, const cosa_params &P) {
+  for (int b = 0; b < L.nb; ++b) {
+    B3 q(const_cast<double *>(qa), L, b);
+    B3s mu(muta, L, b);
+    for (int n = 0; n < L.S; ++n)
+      for (int k = 0; k <= L.km[b]; ++k)
+        for (int j = 0; j <= L.jm[b]; ++j)
+          for (int i = 0; i <= L.im[b]; ++i) {
+            const double rho = q(i, j, k, 1, n), tke = q(i, j, k, 6, n), ome = q(i, j, k, 7, n);
+            mu(i, j, k, n) = P.cmu * rho * tke / (ome + P.epst) * P.reyno / P.machfs;
+          }
+  }
+}
+
 }  // namespace
 
 // ============================================================================
@@ -1484,5 +1795,128 @@ void orc_irs(orc_level *h, const cosa_params *p, double *res, const double *dtvo
   irs_level(h->L, res, dtvol, nullptr, bx, by, bz, nullptr, nullptr, nullptr, *p);
 }
 void orc_tridi(const double *a, const double *b, const double *c, double *x, int dim) { tridi(a, b, c, x, dim); }
+
+// ---- multigrid -------------------------------------------------------------
+void orc_q_edges(orc_level *h, double *q, double *mut) {
+  for (int b = 0; b < h->L.nb; ++b) q_bedges(h->L, b, q, mut);
+}
+void orc_q_corns(orc_level *h, double *q, double *mut) {
+  for (int b = 0; b < h->L.nb; ++b) q_bcorns(h->L, b, q, mut);
+}
+void orc_fixq(orc_level *h, const cosa_params *p, double *q) { fixq_level(h->L, q, *p); }
+void orc_tur_vis(orc_level *h, const cosa_params *p, const double *q, double *mut) {
+  tur_vis_level(h->L, q, mut, *p);
+}
+void orc_add_array(orc_level *h, double *v1, const double *v2, double fact, int off_l) {
+  add_level(h->L, v1, v2, fact, off_l);
+}
+void orc_rest1(orc_level *f, orc_level *c, const double *q1, double *q2, const double *vol1, const double *vol2) {
+  for (int b = 0; b < f->L.nb; ++b) rest1_b(f->L, c->L, b, q1, q2, vol1, vol2);
+}
+void orc_rest2(orc_level *f, orc_level *c, double *rhs2, const double *res1) {
+  for (int b = 0; b < f->L.nb; ++b) rest2_lo_b(f->L, c->L, b, rhs2, res1);
+}
+void orc_prol_bln(orc_level *f, orc_level *c, double *q1, const double *q2, int lim_corr) {
+  for (int b = 0; b < f->L.nb; ++b) prol_bln_b(f->L, c->L, b, q1, q2, lim_corr);
+}
+void orc_prol_lin(orc_level *f, orc_level *c, double *q1, const double *q2, const double *vol1) {
+  for (int b = 0; b < f->L.nb; ++b) prol_lin_b(f->L, c->L, b, q1, q2, vol1);
+}
+
+// restrict (src/cosa.f90:2672-2755), Euler branch
+int orc_restrict(orc_level *f, orc_level *c, const cosa_params *p, const cosa_level_ptrs *P1,
+                 const cosa_level_ptrs *P2) {
+  if (is_kom(*p)) return COSA_ERR_UNSUPPORTED;
+  orc_rest1(f, c, P1->q, P2->q, P1->vol, P2->vol);
+  orc_rest2(f, c, P2->rhs, P1->res);
+  return 0;
+}
+
+// prolong (src/cosa.f90:3167-3250)
+int orc_prolong(orc_level *f, orc_level *c, const cosa_params *p, const cosa_level_ptrs *P1,
+                const cosa_level_ptrs *P2) {
+  const Level &L2 = c->L;
+  int status = 0;
+  orc_rest1(f, c, P1->q, P2->qold, P1->vol, P2->vol);
+  for (double *a : {P2->qold, P2->q}) {
+    for (int b = 0; b < L2.nb; ++b) cons2prim_b(L2, b, a, 0, *p);
+    status |= bc_level(L2, a, P2->si, P2->sj, P2->sk, *p);
+    cutman_q_level(L2, a);
+    for (int b = 0; b < L2.nb; ++b) prim2cons_b(L2, b, a, *p);
+    for (int b = 0; b < L2.nb; ++b) q_bedges(L2, b, a, nullptr);
+    for (int b = 0; b < L2.nb; ++b) q_bcorns(L2, b, a, nullptr);
+  }
+  add_level(L2, P2->q, P2->qold, -1.0, 1);
+  if (p->bln_prol) orc_prol_bln(f, c, P1->q, P2->q, p->lim_corr);
+  else orc_prol_lin(f, c, P1->q, P2->q, P1->vol);
+  if (p->lim_corr == 1 || p->lim_corr == 3) fixq_level(f->L, P1->q, *p);
+  return status;
+}
+
+// smooth(nl, from_fine, to_coarse, done, niter) (src/cosa.f90:1594-2032):
+// explicit Euler branch with the multigrid forcing; `done` is not evaluated.
+// hist_row receives the fine-level resrms of printed cycles (last iteration).
+int orc_smooth_level(orc_level *h, const cosa_params *p, int nl, const cosa_level_ptrs *P, int niter,
+                     int from_fine, int to_coarse, int mgit, int ncycle, int rms_every, double *hist_row) {
+  Level &L = h->L;
+  int status = 0;
+  const int niterp = to_coarse ? niter + 1 : niter;
+  std::vector<double> work;
+  for (int iter = 1; iter <= niterp; ++iter) {
+    if (iter <= niter) copy_interior(L, P->qold, P->q);
+    for (int irk = 1; irk <= p->nstage; ++irk) {
+      const bool want_dt = (iter / p->iupdt * p->iupdt == iter) && irk == 1;
+      status |= residual_impl(h, p, nl, P->q, P->si, P->sj, P->sk, P->res, P->qp, P->qm, P->dq, P->dqp, P->dqm,
+                              P->flux, P->dtvol, want_dt, P->betaxi, P->betaeta, P->betazeta,
+                              p->harbal ? P->vol : nullptr);
+      if (nl == 1 && irk == 1 && iter != niter + 1 && hist_row &&
+          (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle)) {
+        if (p->harbal) {
+          work.assign(P->res, P->res + L.n3 * L.npde * L.S);
+          resg_rms_hb_level(L, work.data(), hist_row);
+        } else {
+          resg_rms_level(L, P->res, P->rhs, hist_row);
+        }
+      }
+      if (from_fine && iter == 1 && irk == 1) add_level(L, P->rhs, P->res, 1.0, -1);
+      if (nl > 1) add_level(L, P->res, P->rhs, -1.0, -1);
+      if (iter == niter + 1) return status;
+      if (p->irsop > 0)
+        irs_level(L, P->res, P->dtvol, nullptr, P->betaxi, P->betaeta, P->betazeta, nullptr, nullptr, nullptr, *p);
+#pragma omp parallel for schedule(dynamic)
+      for (int b = 0; b < L.nb; ++b) update_b(L, b, P->res, P->q, P->qold, P->dtvol, p->alphas[irk - 1]);
+    }
+  }
+  return status;
+}
+
+// mg() (src/cosa.f90:806-930) for cycles mgit0..mgit0+ncycles-1 of ncycle
+int orc_mg(orc_level **lv, int nlevel, const cosa_params *p, const cosa_level_ptrs *P, int mgit0, int ncycles,
+           int ncycle, int rms_every, double *hist) {
+  int status = 0;
+  const int npde = p->npde;
+  int last = mgit0 - 1;
+  for (int mgit = mgit0; mgit < mgit0 + ncycles; ++mgit) {
+    last = mgit;
+    double *row = hist ? hist + (int64_t)(mgit - mgit0) * (npde + 1) : nullptr;
+    int niter = nlevel == 1 ? 1 : (mgit == 1 ? p->nstart : p->npost);
+    status |= orc_smooth_level(lv[0], p, 1, &P[0], niter, 0, nlevel > 1, mgit, ncycle, rms_every, row);
+    if (nlevel > 1) {
+      status |= orc_restrict(lv[0], lv[1], p, &P[0], &P[1]);
+      niter = nlevel == 2 ? p->ncrs : p->npre;
+      status |= orc_smooth_level(lv[1], p, 2, &P[1], niter, 1, nlevel > 2, mgit, ncycle, rms_every, nullptr);
+      if (nlevel == 3) {
+        status |= orc_restrict(lv[1], lv[2], p, &P[1], &P[2]);
+        status |= orc_smooth_level(lv[2], p, 3, &P[2], p->ncrs, 1, 0, mgit, ncycle, rms_every, nullptr);
+        status |= orc_prolong(lv[1], lv[2], p, &P[1], &P[2]);
+        status |= orc_smooth_level(lv[1], p, 2, &P[1], p->npost, 0, 0, mgit, ncycle, rms_every, nullptr);
+      }
+      status |= orc_prolong(lv[0], lv[1], p, &P[0], &P[1]);
+    }
+  }
+  if (nlevel > 1 && last == ncycle)
+    status |= orc_smooth_level(lv[0], p, 1, &P[0], p->npost, 0, 0, ncycle + 1, ncycle, rms_every, nullptr);
+  return status;
+}
 
 }  // extern "C"

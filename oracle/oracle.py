@@ -25,6 +25,14 @@ class _LevelDesc(C.Structure):
                 ("ncuts", C.c_int32), ("cutopo", C.POINTER(C.c_int32))]
 
 
+class _LevelPtrs(C.Structure):
+    # cosa_level_ptrs of include/cosa_gpu.h
+    _fields_ = [(n, _dp) for n in (
+        "q", "qold", "res", "rhs", "dtvol", "dtvolt", "si", "sj", "sk", "vol",
+        "qp", "qm", "dq", "dqp", "dqm", "flux", "betaxi", "betaeta", "betazeta",
+        "mut", "dist", "xdot", "ydot", "zdot")]
+
+
 def build(force: bool = False) -> str:
     if force or not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(os.path.join(_HERE, "cosa_oracle.cpp")):
         subprocess.run(["make", "-C", _HERE], check=True, stdout=subprocess.DEVNULL)
@@ -226,3 +234,99 @@ def roe_face(params, nrm, qr, ql):
 
 def num_threads() -> int:
     return int(lib().orc_num_threads())
+
+
+# ---- multigrid ---------------------------------------------------------------------
+def _opt(a):
+    return _p(a) if a is not None else C.cast(None, _dp)
+
+
+def q_edges(O, q, mut=None):
+    lib().orc_q_edges(O.h, _p(q), _opt(mut))
+
+
+def q_corns(O, q, mut=None):
+    lib().orc_q_corns(O.h, _p(q), _opt(mut))
+
+
+def fixq(O, q):
+    lib().orc_fixq(O.h, _par(O.p), _p(q))
+
+
+def tur_vis(O, q, mut):
+    lib().orc_tur_vis(O.h, _par(O.p), _p(q), _p(mut))
+
+
+def add_array(O, v1, v2, fact, off_l):
+    lib().orc_add_array(O.h, _p(v1), _p(v2), C.c_double(fact), C.c_int(off_l))
+
+
+def rest1(Of, Oc, q1, q2, vol1, vol2):
+    lib().orc_rest1(Of.h, Oc.h, _p(q1), _p(q2), _p(vol1), _p(vol2))
+
+
+def rest2(Of, Oc, rhs2, res1):
+    lib().orc_rest2(Of.h, Oc.h, _p(rhs2), _p(res1))
+
+
+def prol_bln(Of, Oc, q1, q2, lim_corr=0):
+    lib().orc_prol_bln(Of.h, Oc.h, _p(q1), _p(q2), C.c_int(lim_corr))
+
+
+def prol_lin(Of, Oc, q1, q2, vol1):
+    lib().orc_prol_lin(Of.h, Oc.h, _p(q1), _p(q2), _p(vol1))
+
+
+class LevelArrays:
+    """The arrays smooth()/restrict()/prolong() touch on one level, zeroed like
+    cosa_all; q, si, sj, sk, vol are set by the caller."""
+
+    P3 = ("q", "qold", "res", "rhs", "qp", "qm", "dq", "dqp", "dqm")
+
+    def __init__(self, O):
+        self.O = O
+        for n in self.P3:
+            setattr(self, n, O.p3())
+        self.flux = O.f0()
+        self.dtvol = O.p1(O.S)
+        self.betaxi, self.betaeta, self.betazeta = (O.p1(O.S) for _ in range(3))
+        self.si = self.sj = self.sk = self.vol = None
+
+    def ptrs(self):
+        p = _LevelPtrs()
+        for n in self.P3 + ("flux", "dtvol", "betaxi", "betaeta", "betazeta", "si", "sj", "sk", "vol"):
+            a = getattr(self, n)
+            if a is not None:
+                setattr(p, n, _p(a))
+        return p
+
+
+def restrict(Of, Oc, A1, A2):
+    p1, p2 = A1.ptrs(), A2.ptrs()
+    return lib().orc_restrict(Of.h, Oc.h, _par(Of.p), C.byref(p1), C.byref(p2))
+
+
+def prolong(Of, Oc, A1, A2):
+    p1, p2 = A1.ptrs(), A2.ptrs()
+    return lib().orc_prolong(Of.h, Oc.h, _par(Of.p), C.byref(p1), C.byref(p2))
+
+
+def smooth_level(O, nl, A, niter, from_fine, to_coarse, mgit=1, ncycle=1, rms_every=1):
+    row = np.full(O.p.npde + 1, np.nan)
+    pt = A.ptrs()
+    st = lib().orc_smooth_level(O.h, _par(O.p), C.c_int(nl), C.byref(pt), C.c_int(niter), C.c_int(int(from_fine)),
+                                C.c_int(int(to_coarse)), C.c_int(mgit), C.c_int(ncycle), C.c_int(rms_every),
+                                _p(row))
+    return row, st
+
+
+def mg(levels, arrays, mgit0, ncycles, ncycle, rms_every=1):
+    """mg() cycles on oracle levels (levels[0] finest) with LevelArrays each."""
+    n = len(levels)
+    hs = (C.c_void_p * n)(*[O.h.value for O in levels])
+    ps = (_LevelPtrs * n)(*[A.ptrs() for A in arrays])
+    p = levels[0].p
+    hist = np.full((max(ncycles, 1), p.npde + 1), np.nan)
+    st = lib().orc_mg(hs, C.c_int(n), _par(p), ps, C.c_int(mgit0), C.c_int(ncycles), C.c_int(ncycle),
+                      C.c_int(rms_every), _p(hist))
+    return hist[:ncycles], st

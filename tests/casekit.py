@@ -34,3 +34,20 @@ def scaled_err(gpu, ref, scale):
     """max |gpu - ref| / scale (scale per variable, broadcast on axis 1)."""
     d = np.abs(gpu - ref)
     return float((d / scale[None, :, None]).max())
+
+
+def mg_oracle(case, nlevel, params, oracle_mod, q_fine=None):
+    """Oracle levels + LevelArrays of an nlevel multigrid set-up of `case`;
+    coarse states start at the free stream (init2fs on every level)."""
+    lv = cases.mg_levels(case, nlevel)
+    Os, As = [], []
+    for i, (t, x, y, z) in enumerate(lv):
+        O = oracle_mod.OracleLevel(t, params)
+        A = oracle_mod.LevelArrays(O)
+        A.si, A.sj, A.sk, A.vol = O.metrics(x, y, z)
+        A.q[:] = case.q0 if i == 0 else cases._freestream_state(t, params)
+        Os.append(O)
+        As.append(A)
+    if q_fine is not None:
+        As[0].q[:] = q_fine
+    return lv, Os, As

@@ -1,0 +1,279 @@
+"""Parity of the multigrid path (restrict, prolong, coarse-level smoothing
+with the FAS forcing, the V-cycle driver mg()) and of the halo edge/corner
+extrapolation with the CPU oracle, through the C-ABI.
+
+Tolerance as for the single-level path: 1e-12 relative to the largest value
+of each variable for states and corrections, 1e-9 relative for residual
+norms.
+"""
+import numpy as np
+import pytest
+
+from cosa_b200 import cases, gpu
+from cosa_b200.cases import p3_views
+from cosa_b200.params import PREC_MIXED
+
+import casekit
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def _rel_max(a, b, npde, S):
+    """max |a-b| / max|b| per variable; a non-finite value counts as inf."""
+    if not (np.isfinite(a).all() and np.isfinite(b).all()):
+        return float("inf")
+    sc = np.abs(b).reshape(-1, npde, S).max(axis=0).max(axis=1) + 1e-300
+    return float((np.abs(a - b) / sc[None, None, None, :, None]).max())
+
+
+def _full_rel(a, b, tables, npde, S):
+    """max over every cell (halos included) of |a-b| / max|b| per variable."""
+    worst = 0.0
+    for va, vb in zip(p3_views(tables, a, npde, S), p3_views(tables, b, npde, S)):
+        worst = max(worst, _rel_max(va, vb, npde, S))
+    return worst
+
+
+def _interior_rel(a, b, tables, npde, S):
+    worst = 0.0
+    for va, vb in zip(p3_views(tables, a, npde, S), p3_views(tables, b, npde, S)):
+        worst = max(worst, _rel_max(cases.interior(va), cases.interior(vb), npde, S))
+    return worst
+
+
+def _gpu_levels(lv, params, As):
+    """Context over all levels with every array of the oracle set-up uploaded
+    and bound."""
+    ctx = gpu.Context([t for (t, _, _, _) in lv], params)
+    D = []
+    for nl, A in enumerate(As, start=1):
+        d = {
+            "q": ctx.alloc_p3(nl).upload(A.q), "qold": ctx.alloc_p3(nl), "res": ctx.alloc_p3(nl),
+            "rhs": ctx.alloc_p3(nl).upload(A.rhs), "dtvol": ctx.alloc_p1(nl, ctx.S),
+            "si": ctx.alloc_p2(nl).upload(A.si), "sj": ctx.alloc_p2(nl).upload(A.sj),
+            "sk": ctx.alloc_p2(nl).upload(A.sk), "vol": ctx.alloc_p1(nl).upload(A.vol),
+        }
+        if params.irsop >= 2:
+            for k in ("betaxi", "betaeta", "betazeta"):
+                d[k] = ctx.alloc_p1(nl, ctx.S)
+        ctx.bind_level(nl, **d)
+        D.append(d)
+    return ctx, D
+
+
+def test_edges_corners_match_oracle(oracle_mod):
+    case = casekit.small_partitioned(permute=True)
+    p = case.params
+    O = oracle_mod.OracleLevel(case.tables, p)
+    q = cases.perturbed_state(case, seed=7)
+    mut = np.random.default_rng(2).uniform(0.5, 1.5, O.n3)
+    qo, mo = q.copy(), mut.copy()
+    oracle_mod.q_edges(O, qo, mo)
+    oracle_mod.q_corns(O, qo, mo)
+    ctx = gpu.Context([case.tables], p)
+    dq, dm = ctx.alloc_p3().upload(q), ctx.alloc_p3(nvar=1).upload(mut)
+    ctx.q_edges(1, dq, dm)
+    ctx.q_corns(1, dq, dm)
+    assert _full_rel(dq.download(), qo, case.tables, 5, 1) <= TOL
+    np.testing.assert_allclose(dm.download(), mo, rtol=TOL, atol=0)
+    ctx.close()
+
+
+def test_transfer_operators_match_oracle(oracle_mod):
+    """rest1, rest2, prol_bln, prol_lin on random fields, whole arrays."""
+    case = casekit.small_partitioned(32, 16, 4)
+    p = case.params
+    lv = cases.mg_levels(case, 2)
+    Of, Oc = (oracle_mod.OracleLevel(t, p) for (t, _, _, _) in lv)
+    rng = np.random.default_rng(11)
+    q1 = rng.uniform(0.5, 2.0, Of.p3().size)
+    r1 = rng.standard_normal(Of.p3().size)
+    q2c = rng.standard_normal(Oc.p3().size) * 1e-2
+    v1 = rng.uniform(0.5, 1.5, Of.p1().size)
+    v2 = rng.uniform(4.0, 12.0, Oc.p1().size)
+    ctx = gpu.Context([lv[0][0], lv[1][0]], p)
+    g = {k: ctx.alloc_p3(nl).upload(a) for k, nl, a in (("q1", 1, q1), ("r1", 1, r1), ("c2", 2, q2c))}
+    gv1, gv2 = ctx.alloc_p1(1).upload(v1), ctx.alloc_p1(2).upload(v2)
+    # rest1 / rest2 into zeroed coarse arrays
+    q2o, rhs2o = Oc.p3(), Oc.p3()
+    oracle_mod.rest1(Of, Oc, q1, q2o, v1, v2)
+    oracle_mod.rest2(Of, Oc, rhs2o, r1)
+    gq2, grhs2 = ctx.alloc_p3(2), ctx.alloc_p3(2)
+    ctx.rest1(1, g["q1"], gq2, gv1, gv2)
+    ctx.rest2(1, grhs2, g["r1"])
+    assert _full_rel(gq2.download(), q2o, lv[1][0], 5, 1) <= TOL
+    assert _full_rel(grhs2.download(), rhs2o, lv[1][0], 5, 1) <= TOL
+    # prolongations of a coarse correction into the fine state
+    for kind in ("bln", "lin"):
+        qo = q1.copy()
+        gq = ctx.alloc_p3(1).upload(q1)
+        if kind == "bln":
+            oracle_mod.prol_bln(Of, Oc, qo, q2c)
+            ctx.prol_bln(1, gq, g["c2"])
+        else:
+            oracle_mod.prol_lin(Of, Oc, qo, q2c, v1)
+            ctx.prol_lin(1, gq, g["c2"], gv1)
+        # relative to the correction's size: the state is O(1), corrections O(1e-2)
+        d = np.abs(gq.download() - qo).max()
+        assert d <= TOL * np.abs(q2c).max() * 4, (kind, d)
+    ctx.close()
+
+
+@pytest.mark.parametrize("which", ["channel", "partitioned"])
+def test_restrict_smooth_prolong_match_oracle(oracle_mod, which):
+    """One two-level cycle step by step: fine smoothing with the to_coarse
+    residual pass, restrict, forced coarse smoothing, prolong."""
+    case = casekit.small_channel(32, 16, 4) if which == "channel" else casekit.small_partitioned(32, 16, 4)
+    p = case.params
+    p.nlevel = 2
+    p.cfl = 1.0
+    q = cases.perturbed_state(case, amp=0.01, seed=5)
+    lv, Os, As = casekit.mg_oracle(case, 2, p, oracle_mod, q_fine=q)
+    ctx, D = _gpu_levels(lv, p, As)
+    Of, Oc = Os
+    t1, t2 = lv[0][0], lv[1][0]
+    # fine level: 2 iterations + residual pass
+    ro, st = oracle_mod.smooth_level(Of, 1, As[0], 2, False, True, mgit=1, ncycle=5)
+    rg, stg = ctx.smooth_level(1, 2, False, True, mgit=1, ncycle=5)
+    assert st == 0 and stg == 0
+    np.testing.assert_allclose(rg, ro, rtol=1e-9)
+    assert _interior_rel(D[0]["q"].download(), As[0].q, t1, 5, 1) <= TOL
+    assert _interior_rel(D[0]["res"].download(), As[0].res, t1, 5, 1) <= TOL * 10
+    # restrict
+    assert oracle_mod.restrict(Of, Oc, As[0], As[1]) == 0
+    ctx.restrict(1)
+    assert _interior_rel(D[1]["q"].download(), As[1].q, t2, 5, 1) <= TOL
+    assert _interior_rel(D[1]["rhs"].download(), As[1].rhs, t2, 5, 1) <= TOL * 10
+    # coarse level: forced smoothing, 2 iterations
+    _, st = oracle_mod.smooth_level(Oc, 2, As[1], 2, True, False)
+    _, stg = ctx.smooth_level(2, 2, True, False, want_rms=False)
+    assert st == 0 and stg == 0
+    assert _interior_rel(D[1]["q"].download(), As[1].q, t2, 5, 1) <= TOL
+    assert _interior_rel(D[1]["rhs"].download(), As[1].rhs, t2, 5, 1) <= TOL * 10
+    # prolong
+    assert oracle_mod.prolong(Of, Oc, As[0], As[1]) == 0
+    assert ctx.prolong(1) == 0
+    assert _interior_rel(D[0]["q"].download(), As[0].q, t1, 5, 1) <= TOL
+    # the restricted fine state through the coarse BCs, cells 0..imax
+    assert _full_rel(D[1]["qold"].download(), As[1].qold, t2, 5, 1) <= 1e-11
+    ctx.close()
+
+
+MG_CASES = {
+    "channel_2lev": (lambda: casekit.small_channel(32, 16, 4), 2, {}),
+    "channel_2lev_npost2": (lambda: casekit.small_channel(32, 16, 4), 2, {"npost": 2}),
+    # level 3 has one k cell: first order there (nl_crs = 3), second order above
+    "channel_3lev": (lambda: casekit.small_channel(32, 16, 4), 3, {"ncrs": 2, "npost": 2, "nl_crs": 3}),
+    "channel_3lev_fo": (lambda: casekit.small_channel(32, 16, 4), 3, {"nl_crs": 2, "nstart": 2}),
+    "channel_3lev_k8": (lambda: casekit.small_channel(32, 16, 8), 3, {"npre": 2}),
+    "partitioned_2lev": (lambda: casekit.small_partitioned(32, 16, 4), 2, {"npre": 2}),
+    "duct_2lev": (lambda: casekit.small_duct(), 2, {}),
+    "channel_lin": (lambda: casekit.small_channel(32, 16, 4), 2, {"bln_prol": 0}),
+}
+
+
+@pytest.mark.parametrize("which", list(MG_CASES))
+def test_mg_cycles_match_oracle(oracle_mod, which):
+    make, nlevel, opts = MG_CASES[which]
+    case = make()
+    p = case.params
+    p.nlevel = nlevel
+    p.cfl = 1.0
+    for k, v in opts.items():
+        setattr(p, k, v)
+    q = cases.perturbed_state(case, amp=0.01, seed=9)
+    lv, Os, As = casekit.mg_oracle(case, nlevel, p, oracle_mod, q_fine=q)
+    if not p.bln_prol:
+        # prol_lin reads halo volumes: give every level halo volumes (volex-like copy)
+        for A, (t, _, _, _) in zip(As, lv):
+            for v in cases.p1_views(t, A.vol):
+                v[0, :, :] = v[1, :, :]; v[-1, :, :] = v[-2, :, :]
+                v[:, 0, :] = v[:, 1, :]; v[:, -1, :] = v[:, -2, :]
+                v[:, :, 0] = v[:, :, 1]; v[:, :, -1] = v[:, :, -2]
+    ctx, D = _gpu_levels(lv, p, As)
+    ncyc = 4
+    ho, st = oracle_mod.mg(Os, As, 1, ncyc, ncyc, rms_every=2)
+    hg, stg = ctx.mg(1, ncyc, ncyc, rms_every=2)
+    assert st == 0 and stg == 0
+    for nl in range(nlevel):
+        err = _interior_rel(D[nl]["q"].download(), As[nl].q, lv[nl][0], 5, 1)
+        assert err <= TOL * (10 if nl else 1), (nl, err)
+    rows = ~np.isnan(ho[:, 0])
+    assert (rows == ~np.isnan(hg[:, 0])).all(), (ho, hg)
+    np.testing.assert_allclose(hg[rows], ho[rows], rtol=1e-9)
+    ctx.close()
+
+
+def test_thin_level_needs_first_order(oracle_mod):
+    """A level whose blocks are one cell thick runs only first order: at
+    second order the reference's BCs read the opposite face's stale halo,
+    which the fused halo fill does not reproduce, so the call is refused."""
+    case = casekit.small_channel(32, 16, 4)
+    p = case.params
+    p.nlevel = 3
+    p.cfl = 1.0
+    lv, Os, As = casekit.mg_oracle(case, 3, p, oracle_mod)
+    ctx, D = _gpu_levels(lv, p, As)
+    _, st = ctx.mg(1, 1, 1)
+    assert st & 0x080
+    ctx.close()
+
+
+def test_mg_irs_matches_oracle(oracle_mod):
+    """Two-level cycles with central IRS (irsop 3, cut-aware) on every level."""
+    case = casekit.small_partitioned(32, 16, 4)
+    p = case.params
+    p.nlevel = 2
+    p.irsop = 3
+    p.cutcirs = 1
+    p.psirs = 0.125
+    p.rat = float(np.sqrt(1 + 4 * 0.6))
+    p.cfl = 1.0 * p.rat
+    q = cases.perturbed_state(case, amp=0.01, seed=12)
+    lv, Os, As = casekit.mg_oracle(case, 2, p, oracle_mod, q_fine=q)
+    ctx, D = _gpu_levels(lv, p, As)
+    ho, st = oracle_mod.mg(Os, As, 1, 3, 3)
+    hg, stg = ctx.mg(1, 3, 3)
+    assert st == 0 and stg == 0
+    assert _interior_rel(D[0]["q"].download(), As[0].q, lv[0][0], 5, 1) <= TOL
+    np.testing.assert_allclose(hg, ho, rtol=1e-9)
+    ctx.close()
+
+
+def test_mg_harmonic_balance_matches_oracle(oracle_mod):
+    """Two-level cycles of a harmonic-balance case (S = 3): the coupling
+    source on both levels, snapshot-averaged norms on the fine level."""
+    from cosa_b200.params import set_harmonic_balance
+    case = casekit.small_partitioned(32, 16, 4)
+    p = set_harmonic_balance(case.params, 1, 0.16)
+    p.nlevel = 2
+    p.cfl = 1.0
+    case.q0 = cases._freestream_state(case.tables, p)
+    S = 3
+    q = cases.perturbed_state(case, amp=0.01, seed=14)
+    lv, Os, As = casekit.mg_oracle(case, 2, p, oracle_mod, q_fine=q)
+    ctx, D = _gpu_levels(lv, p, As)
+    ho, st = oracle_mod.mg(Os, As, 1, 3, 3)
+    hg, stg = ctx.mg(1, 3, 3)
+    assert st == 0 and stg == 0
+    assert _interior_rel(D[0]["q"].download(), As[0].q, lv[0][0], 5, S) <= TOL
+    np.testing.assert_allclose(hg, ho, rtol=1e-9)
+    ctx.close()
+
+
+def test_mg_mixed_precision_close(oracle_mod):
+    case = casekit.small_channel(32, 16, 4)
+    p = case.params
+    p.nlevel = 2
+    p.cfl = 1.0
+    q = cases.perturbed_state(case, amp=0.01, seed=15)
+    lv, Os, As = casekit.mg_oracle(case, 2, p, oracle_mod, q_fine=q)
+    pm = type(p).from_buffer_copy(p)
+    pm.precision = PREC_MIXED
+    ctx, D = _gpu_levels(lv, pm, As)
+    ho, st = oracle_mod.mg(Os, As, 1, 5, 5)
+    hg, stg = ctx.mg(1, 5, 5)
+    assert st == 0 and stg == 0
+    assert _interior_rel(D[0]["q"].download(), As[0].q, lv[0][0], 5, 1) <= 1e-6
+    ctx.close()
