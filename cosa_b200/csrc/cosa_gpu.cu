@@ -324,10 +324,11 @@ int64_t cnt_all(const DevBlock &b, const cosa_params &p) {
 int set_smem_attrs() {
   static bool done = false;
   if (done) return COSA_OK;
-  CK(cudaFuncSetAttribute(k_stage_tile<kTI, kTJ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)stage_smem_bytes<kTI, kTJ>()));
-  CK(cudaFuncSetAttribute(k_stage_tile<kTI, kTJ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)stage_smem_bytes<kTI, kTJ>()));
+  const int smem = (int)stage_smem_bytes<kTI, kTJ>();
+  CK(cudaFuncSetAttribute(k_stage_tile<kTI, kTJ, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CK(cudaFuncSetAttribute(k_stage_tile<kTI, kTJ, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CK(cudaFuncSetAttribute(k_stage_tile<kTI, kTJ, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CK(cudaFuncSetAttribute(k_stage_tile<kTI, kTJ, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   done = true;
   return COSA_OK;
 }
@@ -485,10 +486,18 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   A.update = update;
   const size_t smem = stage_smem_bytes<kTI, kTJ>();
   if (c->prof.on) cudaEventRecord(c->prof.ev[1][0], c->s);
-  if (p.precision == COSA_PREC_MIXED)
-    k_stage_tile<kTI, kTJ, true><<<L.ntiles, stage_threads<kTI, kTJ>(), smem, c->s>>>(L.d_blocks, L.d_tiles, c->d_p, A);
+  // the residual-norm partials are a separate instantiation: their
+  // accumulators would otherwise hold registers in every launch
+  const int nthr = stage_threads<kTI, kTJ>();
+  const bool mixed = p.precision == COSA_PREC_MIXED;
+  if (mixed && want_rms)
+    k_stage_tile<kTI, kTJ, true, true><<<L.ntiles, nthr, smem, c->s>>>(L.d_blocks, L.d_tiles, c->d_p, A);
+  else if (mixed)
+    k_stage_tile<kTI, kTJ, true, false><<<L.ntiles, nthr, smem, c->s>>>(L.d_blocks, L.d_tiles, c->d_p, A);
+  else if (want_rms)
+    k_stage_tile<kTI, kTJ, false, true><<<L.ntiles, nthr, smem, c->s>>>(L.d_blocks, L.d_tiles, c->d_p, A);
   else
-    k_stage_tile<kTI, kTJ, false><<<L.ntiles, stage_threads<kTI, kTJ>(), smem, c->s>>>(L.d_blocks, L.d_tiles, c->d_p, A);
+    k_stage_tile<kTI, kTJ, false, false><<<L.ntiles, nthr, smem, c->s>>>(L.d_blocks, L.d_tiles, c->d_p, A);
   int r = after_launch(c);
   if (r) return r;
   if (c->prof.on) prof_stop(c, 1);

@@ -149,7 +149,7 @@ struct StageArgs {
 // of every plane, then updates the cell; one extra warp computes the tile's
 // boundary faces (the j-faces above the last row and the i-faces right of the
 // last column), so every warp does a balanced share of the Roe fluxes.
-template <int TI, int TJ, bool MIXED>
+template <int TI, int TJ, bool MIXED, bool RMS>
 __global__ void __launch_bounds__(TI *TJ + 32, 2)
 k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles, const cosa_params *__restrict__ Pp,
              StageArgs A) {
@@ -219,7 +219,7 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
       double v[5];
 #pragma unroll
       for (int m = 0; m < 5; ++m) v[m] = dst[m * PL + c];
-      c2p5(g, v);
+      c2p5_nr(g, v);
       if (v[4] <= P.qmin[4]) st |= COSA_ERR_NEG_P;
       else if (v[0] <= P.qmin[0]) st |= COSA_ERR_NEG_RHO;
 #pragma unroll
@@ -251,7 +251,7 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
           qr[m] = a2 + (double)dp; ql[m] = a1 + (double)dm;
         } else {
           double dp, dm;
-          limit_face<double>(ph.ilimf, ph.epslimf, ph.rkap, dlo, dmid, dhi, dp, dm);
+          limit_face_nr(ph.ilimf, ph.epslimf, ph.rkap, dlo, dmid, dhi, dp, dm);
           qr[m] = a2 + dp; ql[m] = a1 + dm;
         }
       }
@@ -393,7 +393,7 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
           r = r + qhb;
         }
         // resg_rms of the fine level, where rhs is zero (src/cosa.f90:1925-1936)
-        if (A.part) acc[m] += r * r;
+        if (RMS) acc[m] += r * r;
         if (A.rhs_mode) {
           // multigrid forcing on coarse levels (src/cosa.f90:1950-1960)
           double *rh = A.rhs + p3_var(b, npde, S, m + 1, n) + cell;
@@ -416,7 +416,7 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
       for (int m = 0; m < 5; ++m) fk_lo[m] = fk_hi[m];
     }
   }
-  if (A.part) {
+  if (RMS) {
     __syncthreads();
     // deterministic per-tile sums: warp shuffle then fixed-order warp sums
     if (main_warp) {

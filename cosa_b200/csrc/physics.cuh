@@ -2,8 +2,13 @@
 //
 // Every function restates a Fortran routine (cited) with the same operation
 // order and parenthesisation, so an FP64 build differs from the reference
-// only by FMA contraction.  The MIXED variants keep the FP64 state and take
-// the slopes and the Roe dissipation in FP32 on FP64 differences.
+// only by FMA contraction.  The variants used by the fused stage kernel
+// (limit_face_nr, roe_flux_euler, c2p5_nr) take the reciprocals and
+// reciprocal square roots on their dependency chains from rcp_nr / rsqrt_nr
+// below: results differ from the IEEE division and square root by at most a
+// couple of ulp, far inside the parity bound, and each chain gets shorter.
+// The MIXED variants keep the FP64 state and take the slopes and the Roe
+// dissipation in FP32 on FP64 differences.
 #pragma once
 #include <cuda_runtime.h>
 #include "common.cuh"
@@ -29,11 +34,43 @@ __device__ __forceinline__ PhysPar make_phys(const cosa_params &P) {
   return q;
 }
 
+// ---- Newton-Raphson reciprocal and reciprocal square root -------------------------
+// Seeds from the PTX approximations rcp.approx.ftz.f64 / rsqrt.approx.ftz.f64
+// (relative error around 2^-22), then two Newton-Raphson steps each:
+//   1/x:        r <- r + r (1 - x r)              (error e -> e^2)
+//   1/sqrt(x):  y <- y (3/2 - (x/2) y^2)          (error e -> 3 e^2 / 2)
+// which leaves only the rounding of the last operations (a few ulp at most).
+// Inputs are positive normal numbers here (densities, speeds of sound squared,
+// sums of squares plus a positive epsilon); no zero, denormal or infinity
+// handling is needed or done.
+__device__ __forceinline__ double rcp_nr(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double h = 0.5 * x;
+  y = y * fma(-h * y, y, 1.5);
+  return y * fma(-h * y, y, 1.5);
+}
+
 // ---- cons2prim_b / prim2cons_b cell formulas (src/update.f90:2135-2188, 1875-2084)
 // q[0..4] = (rho, rho u, rho v, rho w, rho E) -> (rho, u, v, w, p); Euler
 __device__ __forceinline__ void c2p5(double g, double *q) {
   const double rho = q[0];
   const double u = q[1] / rho, v = q[2] / rho, w = q[3] / rho;
+  q[1] = u; q[2] = v; q[3] = w;
+  q[4] = (g - 1) * (q[4] - rho * (u * u + v * v + w * w) / 2);
+}
+// c2p5 with one reciprocal of rho (fused stage kernel)
+__device__ __forceinline__ void c2p5_nr(double g, double *q) {
+  const double rho = q[0], ri = rcp_nr(rho);
+  const double u = q[1] * ri, v = q[2] * ri, w = q[3] * ri;
   q[1] = u; q[2] = v; q[3] = w;
   q[4] = (g - 1) * (q[4] - rho * (u * u + v * v + w * w) / 2);
 }
@@ -103,6 +140,22 @@ __device__ __forceinline__ void limit_face(int ilim, T eps, T rkap, T dlo, T dmi
     d1 = dmid; d2 = dlo;
     T dqmx = (d1 * (d2 * d2 + epsq) + d2 * (d1 * d1 + epsq)) / (d1 * d1 + d2 * d2 + 2 * epsq);
     dqm = dqmx / 2;
+  }
+}
+
+// limit_face with the sensor's division taken as a Newton-Raphson reciprocal
+// (ilim 1, the smooth van Albada-type sensor), fused stage kernel
+__device__ __forceinline__ void limit_face_nr(int ilim, double eps, double rkap, double dlo, double dmid, double dhi,
+                                              double &dqp, double &dqm) {
+  if (ilim == 1) {
+    double s = (2 * dhi * dmid + eps) * rcp_nr(dhi * dhi + dmid * dmid + eps);
+    double rkp = 1 + rkap * s, rkm = 1 - rkap * s;
+    dqp = -s * (rkp * dmid + rkm * dhi) / 4;
+    s = (2 * dmid * dlo + eps) * rcp_nr(dmid * dmid + dlo * dlo + eps);
+    rkp = 1 + rkap * s; rkm = 1 - rkap * s;
+    dqm = s * (rkm * dlo + rkp * dmid) / 4;
+  } else {
+    limit_face<double>(ilim, eps, rkap, dlo, dmid, dhi, dqp, dqm);
   }
 }
 
@@ -187,24 +240,27 @@ __device__ __forceinline__ void roe_flux_fp64(const PhysPar &P, double kx, doubl
 }
 
 // Euler face flux for the fused stage: roflux_b's algebra with the TKE terms
-// (zero for Euler) dropped and the four Roe averages taken with one
-// reciprocal of rhols + rhors (a last-bit difference from the divisions).
+// (zero for Euler) dropped; sqrt(rho), 1/rho, the Roe-average weights, the
+// speed of sound and its inverse come from rsqrt_nr / rcp_nr instead of
+// separate square roots and divisions (last-bit differences).
 __device__ __forceinline__ void roe_flux_euler(const PhysPar &P, double kx, double ky, double kz, double ds,
                                                const double *qr, const double *ql, double *flux) {
   const double g_gm1 = P.g_gm1, gm1 = P.gm1;
   const double rhor = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
   const double unr = ur * kx + vr * ky + wr * kz;
   const double q2r = ur * ur + vr * vr + wr * wr;
-  const double h0r = g_gm1 * pr / rhor + q2r / 2;
+  const double rsr = rsqrt_nr(rhor);  // 1/sqrt(rho_R): sqrt(rho_R) and 1/rho_R from it
+  const double h0r = g_gm1 * pr * (rsr * rsr) + q2r / 2;
   const double rhol = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4];
   const double unl = ul * kx + vl * ky + wl * kz;
   const double q2l = ul * ul + vl * vl + wl * wl;
-  const double h0l = g_gm1 * pl / rhol + q2l / 2;
+  const double rsl = rsqrt_nr(rhol);
+  const double h0l = g_gm1 * pl * (rsl * rsl) + q2l / 2;
   const double drho = rhor - rhol, dp = pr - pl, du = ur - ul, dv = vr - vl, dw = wr - wl;
   const double dun = unr - unl;
-  const double rhols = sqrt(rhol), rhors = sqrt(rhor);
+  const double rhols = rhol * rsl, rhors = rhor * rsr;
   const double rho = rhols * rhors;
-  const double rden = 1.0 / (rhols + rhors);
+  const double rden = rcp_nr(rhols + rhors);
   const double u = (rhols * ul + rhors * ur) * rden;
   const double v = (rhols * vl + rhors * vr) * rden;
   const double w = (rhols * wl + rhors * wr) * rden;
@@ -212,7 +268,8 @@ __device__ __forceinline__ void roe_flux_euler(const PhysPar &P, double kx, doub
   const double h0 = (rhols * h0l + rhors * h0r) * rden;
   const double q2 = u * u + v * v + w * w;
   const double a2 = gm1 * (h0 - q2 / 2);
-  const double a = sqrt(a2);
+  const double ra = rsqrt_nr(a2);  // 1/a
+  const double a = a2 * ra;
   double rm123 = fabs(un), rm4 = fabs(un + a), rm5 = fabs(un - a);
   if (P.efx_setup_f) {
     double rdelta = P.cntrpy_f * (P.w1 * P.entfxctf_f + P.w2 * (sqrt(q2) + a) + P.w3 * 0.2 * (fabs(un) + a));
@@ -226,7 +283,7 @@ __device__ __forceinline__ void roe_flux_euler(const PhysPar &P, double kx, doub
     if (P.eig_lim_all_f && rm4 <= P.eig_cutoff_f) rm4 = P.eig_cutoff_f;
     if (P.eig_lim_all_f && rm5 <= P.eig_cutoff_f) rm5 = P.eig_cutoff_f;
   }
-  const double dpa2 = dp / a2, rdua = rho * dun / a;
+  const double dpa2 = dp * (ra * ra), rdua = rho * dun * ra;
   const double al1 = rm123 * (drho - dpa2);
   const double al2 = rm123 * rho;
   const double al3 = rm4 * (dpa2 + rdua) / 2;
@@ -257,8 +314,8 @@ __device__ __forceinline__ void roe_flux_mixed(const PhysPar &P, double kx, doub
   const double unl = ul * kx + vl * ky + wl * kz;
   const double q2r = ur * ur + vr * vr + wr * wr;
   const double q2l = ul * ul + vl * vl + wl * wl;
-  const double h0r = g / (g - 1) * pr / rhor + q2r / 2;
-  const double h0l = g / (g - 1) * pl / rhol + q2l / 2;
+  const double h0r = P.g_gm1 * pr * rcp_nr(rhor) + q2r / 2;
+  const double h0l = P.g_gm1 * pl * rcp_nr(rhol) + q2l / 2;
   // FP32 dissipation on FP64 differences
   const float fkx = (float)kx, fky = (float)ky, fkz = (float)kz;
   const float drho = (float)(rhor - rhol), dp = (float)(pr - pl);
