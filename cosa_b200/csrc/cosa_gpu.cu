@@ -1439,6 +1439,44 @@ int cosa_gpu_profile(cosa_ctx *c, int32_t nl, int32_t niter, double ms[3], int64
 
 void *cosa_gpu_stream(cosa_ctx *c) { return c ? (void *)c->s : nullptr; }
 
+}  // extern "C"
+
+namespace {
+__global__ void k_nr_selftest(int64_t n, const double *__restrict__ x, double *__restrict__ e) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const double v = x[t];
+    const double r = 1.0 / v, s = 1.0 / sqrt(v);
+    e[2 * t] = fabs(rcp_nr(v) - r) / r;
+    e[2 * t + 1] = fabs(rsqrt_nr(v) - s) / s;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int cosa_gpu_nr_selftest(int64_t n, const double *x, double err[2]) {
+  if (n < 1 || !x || !err) return COSA_ERR_ARG;
+  double *dx = nullptr, *de = nullptr;
+  CK(cudaMalloc(&dx, n * sizeof(double)));
+  if (cudaMalloc(&de, 2 * n * sizeof(double)) != cudaSuccess) { cudaFree(dx); return COSA_ERR_CUDA; }
+  std::vector<double> h(2 * n);
+  int r = cuda_ok(cudaMemcpy(dx, x, n * sizeof(double), cudaMemcpyHostToDevice));
+  if (!r) {
+    k_nr_selftest<<<grid_for(n), 256>>>(n, dx, de);
+    r = cuda_ok(cudaGetLastError());
+  }
+  if (!r) r = cuda_ok(cudaMemcpy(h.data(), de, 2 * n * sizeof(double), cudaMemcpyDeviceToHost));
+  cudaFree(dx);
+  cudaFree(de);
+  if (r) return r;
+  err[0] = err[1] = 0.0;
+  for (int64_t t = 0; t < n; ++t) {
+    err[0] = std::max(err[0], h[2 * t]);
+    err[1] = std::max(err[1], h[2 * t + 1]);
+  }
+  return COSA_OK;
+}
+
 int64_t cosa_gpu_launch_count(cosa_ctx *c, int32_t reset) {
   if (!c) return -1;
   const long long v = c->launches;

@@ -56,7 +56,7 @@ SYMBOLS = [
     "cosa_gpu_resg_rms_noalloc", "cosa_gpu_scalef", "cosa_gpu_scaleb", "cosa_gpu_cirs", "cosa_gpu_ccirs",
     "cosa_gpu_src_hb", "cosa_gpu_q_edges", "cosa_gpu_q_corns", "cosa_gpu_fixq", "cosa_gpu_tur_vis",
     "cosa_gpu_rest1", "cosa_gpu_rest2", "cosa_gpu_prol_bln", "cosa_gpu_prol_lin", "cosa_gpu_restrict",
-    "cosa_gpu_prolong", "cosa_gpu_smooth_level", "cosa_gpu_mg",
+    "cosa_gpu_prolong", "cosa_gpu_smooth_level", "cosa_gpu_mg", "cosa_gpu_nr_selftest",
 ]
 
 
@@ -332,6 +332,17 @@ class Context:
         st = load().cosa_gpu_smooth_host(self.h, nl, q_host.ctypes.data_as(_dp), niter, mgit0, rms_every,
                                          hist.ctypes.data_as(_dp) if want_hist else _dp())
         return (hist[:niter] if want_hist else None), st
+
+
+def nr_selftest(x: np.ndarray):
+    """Largest relative differences of the fused kernel's Newton-Raphson 1/x
+    and 1/sqrt(x) from IEEE division and square root, on the GPU."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    err = (C.c_double * 2)()
+    st = load().cosa_gpu_nr_selftest(C.c_int64(x.size), x.ctypes.data_as(_dp), err)
+    if st:
+        raise CosaError(st, "cosa_gpu_nr_selftest")
+    return float(err[0]), float(err[1])
 
 
 class Solver:

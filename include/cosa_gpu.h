@@ -298,6 +298,11 @@ int cosa_gpu_mg(cosa_ctx *ctx, int32_t mgit0, int32_t ncycles, int32_t ncycle,
    ms[2] = mean iteration time; counts = launches timed */
 int cosa_gpu_profile(cosa_ctx *ctx, int32_t nl, int32_t niter, double ms[3],
                      int64_t counts[3]);
+/* diagnostics: evaluates the fused kernel's Newton-Raphson reciprocal and
+   reciprocal square root on n host values x (positive normal numbers) on
+   the current device and returns in err[0], err[1] the largest relative
+   differences from IEEE 1/x and 1/sqrt(x) computed there */
+int cosa_gpu_nr_selftest(int64_t n, const double *x, double err[2]);
 /* the context's CUDA stream (cudaStream_t), for callers that time with
    their own events */
 void *cosa_gpu_stream(cosa_ctx *ctx);

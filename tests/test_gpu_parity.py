@@ -359,3 +359,16 @@ def test_fused_smooth_hb_matches_oracle(oracle_mod, nharms):
     rows = ~np.isnan(hist_o[:, 0])
     np.testing.assert_allclose(hist_g[rows], hist_o[rows], rtol=1e-9)
     ctx.close()
+
+
+def test_newton_raphson_reciprocals_within_ulps():
+    """The tile kernel's 1/x and 1/sqrt(x) (Newton-Raphson on the PTX
+    approximations) stay within a few ulp of IEEE division and square root
+    over the range of densities, sound speeds and limiter denominators."""
+    rng = np.random.default_rng(0)
+    x = np.exp(rng.uniform(np.log(1e-8), np.log(1e8), 200_000))
+    x = np.concatenate([x, [1.0, 2.0, 0.5, 1.4, 1e-6, 3.0e5]])
+    e_rcp, e_rsq = gpu.nr_selftest(x)
+    eps = np.finfo(np.float64).eps
+    assert e_rcp <= 4 * eps, e_rcp / eps
+    assert e_rsq <= 4 * eps, e_rsq / eps
