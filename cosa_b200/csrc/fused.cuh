@@ -320,7 +320,7 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
       InTask tk = task(0);
       double mcur[4], mnext[4];
       if (tk.valid) load_metric(tk.dir == 0 ? A.si : A.sj, tk.i, tk.j, k, mcur);
-#pragma unroll 1
+#pragma unroll
       for (int t = 0; t < 2; ++t) {
         const InTask tn = task(1);
         if (t == 0 && tn.valid) load_metric(tn.dir == 0 ? A.si : A.sj, tn.i, tn.j, k, mnext);
