@@ -9,6 +9,7 @@
 #include <map>
 #include <mutex>
 #include <new>
+#include <unordered_map>
 #include <vector>
 
 #include "kernels_ref.cuh"
@@ -75,6 +76,12 @@ struct cosa_ctx {
   int *d_status = nullptr;
   int *d_row = nullptr;
   double *d_hist = nullptr;
+  const cosa_params *d_halo_p = nullptr;  // flow-condition slots read by k_halo (default: d_p)
+  // residual norms reduced per segment of tiles (one per served solve) when
+  // set: segment s = tiles [d_seg[2s], +d_seg[2s+1]) with seg_ncell[s] cells
+  int nseg = 0;
+  int *d_seg = nullptr;
+  double *d_seg_ncell = nullptr;
   int hist_cap = 0;
   long long launches = 0;
   std::vector<void *> allocs;
@@ -113,7 +120,11 @@ inline void pcell(int idir, int nrm, int i2, int i3, int &i, int &j, int &k) {
   i = v[1]; j = v[2]; k = v[3];
 }
 
-int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d) {
+// offs (optional): per block the P3, P2 and P1 offsets in cells to use
+// instead of the setoffs() concatenation (blocks placed in a shared pool);
+// bps (optional): per block the slot of its flow conditions for k_halo
+int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int64_t *offs = nullptr,
+                const int *bps = nullptr) {
   L.nb = d.nblocks;
   int64_t a3 = 0, a2 = 0, a1 = 0, a0 = 0, am = 0, ab = 0;
   for (int b = 0; b < L.nb; ++b) {
@@ -123,6 +134,7 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d) {
     x.I3 = x.im + 3; x.J3 = x.jm + 3;
     x.P3 = (int64_t)(x.im + 3) * (x.jm + 3) * (x.km + 3);
     x.op3 = a3; x.op2 = a2; x.op1 = a1; x.of0 = a0;
+    if (offs) { x.op3 = offs[3 * b]; x.op2 = offs[3 * b + 1]; x.op1 = offs[3 * b + 2]; }
     L.hb.push_back(x);
     L.nbcs.push_back(d.nbcs[b]);
     L.obct.push_back(ab);
@@ -134,6 +146,14 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d) {
     ab += 10 * d.nbcs[b];
   }
   L.n3 = a3; L.n2 = a2; L.n1 = a1; L.n0 = a0; L.nm1 = am;
+  if (offs) {  // pool placement: array extents reach the furthest block end
+    L.n3 = L.n2 = L.n1 = 0;
+    for (const DevBlock &x : L.hb) {
+      L.n3 = std::max(L.n3, x.op3 + x.P3);
+      L.n2 = std::max(L.n2, x.op2 + (int64_t)(x.im + 2) * (x.jm + 2) * (x.km + 2));
+      L.n1 = std::max(L.n1, x.op1 + (int64_t)(x.im + 1) * (x.jm + 1) * (x.km + 1));
+    }
+  }
   L.bct.assign(d.bctopo, d.bctopo + ab);
   L.ncuts = d.ncuts;
   L.cut.assign(d.cutopo, d.cutopo + 21 * (int64_t)d.ncuts);
@@ -210,21 +230,24 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d) {
         L.items.push_back(it);
       }
   }
+  if (bps)
+    for (HaloItem &it : L.items) it.ps = bps[it.dblk];
   // last writer of every halo cell keeps its write (reference order)
   {
-    std::vector<int64_t> owner((size_t)L.n3, -1);
+    std::unordered_map<int64_t, int64_t> owner;
+    owner.reserve(L.items.size() * 2);
     for (size_t t = 0; t < L.items.size(); ++t) {
       const HaloItem &it = L.items[t];
       const int64_t base = L.hb[it.dblk].op3;
-      owner[(size_t)(base + it.h1)] = (int64_t)t * 2;
-      owner[(size_t)(base + it.h2)] = (int64_t)t * 2 + 1;
+      owner[base + it.h1] = (int64_t)t * 2;
+      owner[base + it.h2] = (int64_t)t * 2 + 1;
     }
     for (size_t t = 0; t < L.items.size(); ++t) {
       HaloItem &it = L.items[t];
       const int64_t base = L.hb[it.dblk].op3;
       int m = 0;
-      if (owner[(size_t)(base + it.h1)] == (int64_t)t * 2) m |= 1;
-      if (owner[(size_t)(base + it.h2)] == (int64_t)t * 2 + 1) m |= 2;
+      if (owner[base + it.h1] == (int64_t)t * 2) m |= 1;
+      if (owner[base + it.h2] == (int64_t)t * 2 + 1) m |= 2;
       it.mask = m;
     }
   }
@@ -460,8 +483,9 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   if (!L.items.empty()) {
     const int64_t n = (int64_t)L.items.size() * S;
     if (c->prof.on) cudaEventRecord(c->prof.ev[0][0], c->s);
-    k_halo<true><<<grid_for(n), 256, 0, c->s>>>(L.d_blocks, L.d_items, (int)L.items.size(), c->d_p, qin, P.si, P.sj,
-                                                P.sk, c->d_status);
+    k_halo<true><<<grid_for(n), 256, 0, c->s>>>(L.d_blocks, L.d_items, (int)L.items.size(),
+                                                c->d_halo_p ? c->d_halo_p : c->d_p, qin, P.si, P.sj, P.sk,
+                                                c->d_status);
     int r = after_launch(c);
     if (r) return r;
     if (c->prof.on) prof_stop(c, 0);
@@ -501,7 +525,11 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   int r = after_launch(c);
   if (r) return r;
   if (c->prof.on) prof_stop(c, 1);
-  if (want_rms) {
+  if (want_rms && c->nseg > 0) {
+    k_rms_seg<<<c->nseg, 256, 0, c->s>>>(L.d_part, c->d_seg, c->d_seg_ncell, p.npde, c->d_hist);
+    r = after_launch(c);
+    if (r) return r;
+  } else if (want_rms) {
     int64_t ncell = 0;
     for (auto &b : L.hb) ncell += (int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1);
     // resg_rms_hb averages over the snapshots as well (src/cosa.f90:4620-4626)
@@ -1550,3 +1578,5 @@ extern "C" int cosa_gpu_resg_rms_noalloc(int32_t nblocks, const int32_t *dims, i
   if (cudaGetLastError() != cudaSuccess) return COSA_ERR_CUDA;
   return COSA_OK;
 }
+
+#include "serve.cuh"

@@ -37,6 +37,7 @@ struct HaloItem {
   int64_t h1, h2;   // halo cells (p3 cell index in dblk)
   int64_t c1, c2;   // interior cells (p3 cell index in sblk)
   int64_t mface;    // metric cell index (i + I2*(j + J2*k)) of the face in dblk
+  int ps;           // slot of the flow conditions (BC values) in the params array
 };
 
 struct Tile {
@@ -94,7 +95,7 @@ __global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__re
         const int64_t e = ((db.op2 * S2) + (int64_t)nh * I2 * J2 * K2 + it.mface) * 4;
         nx = s[e] * it.sgn; ny = s[e + 1] * it.sgn; nz = s[e + 2] * it.sgn;
       }
-      const BcPar B = make_bcpar(P);
+      const BcPar B = make_bcpar(Pp[it.ps]);
       int err = 0;
       switch (it.type) {
         case 80: mask = bc_sym(it.idir, npde, c1, c2, h1, h2); break;
@@ -470,6 +471,39 @@ __global__ void k_rms_final(const double *__restrict__ part, int nparts, int npd
     int row = 0;
     if (row_counter) { row = *row_counter; if (row < nrows_max) *row_counter = row + 1; else row = nrows_max - 1; }
     double *o = out + (int64_t)row * (npde + 1);
+    for (int v = 0; v < npde; ++v) o[v] = sqrt(tot[v] / ncell);
+    o[npde] = sqrt(all / ncell / npde);
+  }
+}
+
+// per-segment version of k_rms_final: CTA s reduces tiles [seg[2s], +seg[2s+1])
+// in the same fixed order into out[s * (npde + 1) ...]
+__global__ void k_rms_seg(const double *__restrict__ part, const int *__restrict__ seg,
+                          const double *__restrict__ seg_ncell, int npde, double *__restrict__ out) {
+  __shared__ double red[8][32];
+  const int s = blockIdx.x;
+  const double *pp = part + (int64_t)seg[2 * s] * 8;
+  const int nparts = seg[2 * s + 1];
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int p = threadIdx.x; p < nparts; p += blockDim.x)
+    for (int v = 0; v < npde; ++v) acc[v] += pp[(int64_t)p * 8 + v];
+  for (int v = 0; v < npde; ++v) {
+    double x = acc[v];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) red[v][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    const double ncell = seg_ncell[s];
+    double tot[8], all = 0;
+    for (int v = 0; v < npde; ++v) {
+      double x = 0;
+      for (int w = 0; w < nw; ++w) x += red[v][w];
+      tot[v] = x;
+      all = all + x;
+    }
+    double *o = out + (int64_t)s * (npde + 1);
     for (int v = 0; v < npde; ++v) o[v] = sqrt(tot[v] / ncell);
     o[npde] = sqrt(all / ncell / npde);
   }

@@ -57,6 +57,8 @@ SYMBOLS = [
     "cosa_gpu_src_hb", "cosa_gpu_q_edges", "cosa_gpu_q_corns", "cosa_gpu_fixq", "cosa_gpu_tur_vis",
     "cosa_gpu_rest1", "cosa_gpu_rest2", "cosa_gpu_prol_bln", "cosa_gpu_prol_lin", "cosa_gpu_restrict",
     "cosa_gpu_prolong", "cosa_gpu_smooth_level", "cosa_gpu_mg", "cosa_gpu_nr_selftest",
+    "cosa_serve_create", "cosa_serve_destroy", "cosa_serve_submit", "cosa_serve_step", "cosa_serve_result",
+    "cosa_serve_free_slots",
 ]
 
 
@@ -78,9 +80,10 @@ def load(build_if_missing: bool = True):
     L.cosa_gpu_params_size.restype = C.c_int64
     L.cosa_gpu_launch_count.restype = C.c_int64
     L.cosa_gpu_stream.restype = C.c_void_p
+    L.cosa_serve_free_slots.restype = C.c_int64
     L.cosa_gpu_init.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]
     for name in SYMBOLS:
-        if name not in ("cosa_gpu_params_size", "cosa_gpu_launch_count", "cosa_gpu_stream"):
+        if name not in ("cosa_gpu_params_size", "cosa_gpu_launch_count", "cosa_gpu_stream", "cosa_serve_free_slots"):
             getattr(L, name).restype = C.c_int
     _lib = L
     return L
@@ -332,6 +335,73 @@ class Context:
         st = load().cosa_gpu_smooth_host(self.h, nl, q_host.ctypes.data_as(_dp), niter, mgit0, rms_every,
                                          hist.ctypes.data_as(_dp) if want_hist else _dp())
         return (hist[:niter] if want_hist else None), st
+
+
+SOLVE_STATES = {0: "queued", 1: "active", 2: "converged", 3: "stopped", 4: "failed"}
+
+
+class Server:
+    """cosa_serve: steady solves of different grids and flow conditions
+    resident on one GPU and advanced together (continuous batching)."""
+
+    def __init__(self, scheme: CosaParams, budget_bytes: int, device: int = 0, check_every: int = 10):
+        L = load()
+        h = C.c_void_p()
+        st = L.cosa_serve_create(C.byref(scheme), C.c_int64(int(budget_bytes)), device, check_every, C.byref(h))
+        if st:
+            raise CosaError(st, "cosa_serve_create")
+        self.h = h
+        self.npde = scheme.npde
+        self._sizes = {}
+
+    def close(self):
+        if self.h is not None:
+            load().cosa_serve_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, tables: LevelTables, x, y, z, q0, flow: CosaParams, tol: float, max_iter: int) -> int:
+        arrs = [np.ascontiguousarray(tables.dims.ravel(), dtype=np.int32),
+                np.ascontiguousarray(tables.nbcs, dtype=np.int32),
+                np.ascontiguousarray(tables.bctopo.ravel(), dtype=np.int32),
+                np.ascontiguousarray(tables.cutopo.ravel(), dtype=np.int32)]
+        ip = lambda a: a.ctypes.data_as(_ip)
+        d = LevelDesc(tables.nblocks, ip(arrs[0]), ip(arrs[1]), ip(arrs[2]), tables.ncuts, ip(arrs[3]))
+        dp = lambda a: np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(_dp)
+        xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, q0)]
+        rid = C.c_int64()
+        st = load().cosa_serve_submit(self.h, C.byref(d), *(a.ctypes.data_as(_dp) for a in xs), C.byref(flow),
+                                      C.c_double(tol), C.c_int32(max_iter), C.byref(rid))
+        if st:
+            raise CosaError(st, "cosa_serve_submit")
+        self._sizes[rid.value] = xs[3].size
+        return rid.value
+
+    def step(self, niter: int):
+        na, nq = C.c_int32(), C.c_int32()
+        st = load().cosa_serve_step(self.h, niter, C.byref(na), C.byref(nq))
+        if st:
+            raise CosaError(st, "cosa_serve_step")
+        return na.value, nq.value
+
+    def result(self, rid: int, want_state: bool = False):
+        s, it, drop = C.c_int32(), C.c_int32(), C.c_double()
+        t = (C.c_double * 3)()
+        q = np.zeros(self._sizes[rid]) if want_state else None
+        st = load().cosa_serve_result(self.h, C.c_int64(rid), C.byref(s), C.byref(it), C.byref(drop), t,
+                                      q.ctypes.data_as(_dp) if want_state else _dp())
+        if st:
+            raise CosaError(st, "cosa_serve_result")
+        return {"state": SOLVE_STATES[s.value], "iters": it.value, "rms_drop": drop.value,
+                "t_submit": t[0], "t_admit": t[1], "t_done": t[2], "q": q}
+
+    def free_slots(self) -> int:
+        return int(load().cosa_serve_free_slots(self.h))
 
 
 def nr_selftest(x: np.ndarray):

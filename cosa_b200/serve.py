@@ -1,0 +1,132 @@
+"""Serving sweep over the cosa_serve engine (continuous batching on one GPU).
+
+A seeded Poisson stream of steady solves arrives; each request is the bump
+channel at one of three in-plane scales with its own free-stream Mach
+number (and the matching inlet total state).  Requests are submitted when
+they arrive, admitted by the engine as device memory allows, advanced
+together with whatever else is on the GPU, and retired at convergence.
+Reports throughput (solves per hour) and p50/p99 latency (arrival to
+retirement).  The reference has no serving mode: each of its runs is one
+solve; this is the batched counterpart of running those one after another.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import cases
+from .gpu import Server
+from .params import CosaParams, subsonic_inlet_total_state
+
+
+@dataclass
+class Request:
+    scale: float
+    mach: float
+    arrival: float
+    case: Optional[cases.Case] = None
+    flow: Optional[CosaParams] = None
+
+
+def channel_request(scale: float, mach: float, arrival: float = 0.0) -> Request:
+    """Bump channel 128 x 64 x 2 cells scaled by `scale` in i and j, free
+    stream and inlet total state at `mach`."""
+    ni, nj = max(8, int(round(128 * scale))), max(4, int(round(64 * scale)))
+    case = cases.bump_channel(ni, nj, 2, mach=mach)
+    return Request(scale, mach, arrival, case, case.params)
+
+
+def engine_scheme() -> CosaParams:
+    """The engine's scheme: Roe + MUSCL (kappa 1/3, smooth limiter), 4-stage
+    RK at CFL 2; flow conditions come with each request."""
+    return cases.channel_params(0.5)
+
+
+def poisson_requests(n: int, rate: float, seed: int, scales=(0.5, 1.0, 2.0), mach_range=(0.3, 0.7)) -> List[Request]:
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    t -= t[0]
+    out = []
+    for k in range(n):
+        out.append(channel_request(float(rng.choice(scales)), float(rng.uniform(*mach_range)), float(t[k])))
+    return out
+
+
+@dataclass
+class SweepResult:
+    n: int
+    wall_s: float
+    solves_per_hour: float
+    p50_s: float
+    p99_s: float
+    iters: List[int] = field(default_factory=list)
+    states: List[str] = field(default_factory=list)
+    latencies: List[float] = field(default_factory=list)
+    cell_stages: float = 0.0
+
+    def summary(self) -> Dict:
+        return {"requests": self.n, "wall_s": self.wall_s, "solves_per_hour": self.solves_per_hour,
+                "p50_latency_s": self.p50_s, "p99_latency_s": self.p99_s,
+                "converged": sum(s == "converged" for s in self.states),
+                "mean_iters": float(np.mean(self.iters)) if self.iters else 0.0,
+                "mcell_stages_per_s": self.cell_stages / self.wall_s / 1e6 if self.wall_s else 0.0}
+
+
+def run_sweep(requests: List[Request], budget_bytes: float = 150e9, tol: float = 1e-8, max_iter: int = 200_000,
+              check_every: int = 10, iters_per_step: int = 50, device: int = 0) -> SweepResult:
+    """Feed `requests` at their arrival times (seconds after the start) and
+    run the engine until every one has retired."""
+    srv = Server(engine_scheme(), int(budget_bytes), device=device, check_every=check_every)
+    try:
+        ids: List[int] = []
+        pending = sorted(range(len(requests)), key=lambda k: requests[k].arrival)
+        order: Dict[int, int] = {}
+        t0 = time.perf_counter()
+        done = 0
+        nxt = 0
+        while done < len(requests):
+            now = time.perf_counter() - t0
+            while nxt < len(pending) and requests[pending[nxt]].arrival <= now:
+                r = requests[pending[nxt]]
+                rid = srv.submit(r.case.tables, r.case.x, r.case.y, r.case.z, r.case.q0, r.flow, tol, max_iter)
+                order[rid] = pending[nxt]
+                ids.append(rid)
+                nxt += 1
+            na, nq = srv.step(iters_per_step) if ids else (0, 0)
+            done = sum(srv.result(rid)["state"] not in ("queued", "active") for rid in ids)
+            if na == 0 and nq == 0 and nxt < len(pending) and done == len(ids):
+                wait = requests[pending[nxt]].arrival - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+        wall = time.perf_counter() - t0
+        res = [srv.result(rid) for rid in ids]
+        lat = [r["t_done"] - r["t_submit"] for r in res]
+        cs = 0.0
+        for rid, r in zip(ids, res):
+            cs += requests[order[rid]].case.ncells * 4 * r["iters"]
+        return SweepResult(len(ids), wall, len(ids) / wall * 3600.0, float(np.percentile(lat, 50)),
+                           float(np.percentile(lat, 99)), [r["iters"] for r in res], [r["state"] for r in res], lat,
+                           cs)
+    finally:
+        srv.close()
+
+
+def main():
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--requests", type=int, default=20)
+    ap.add_argument("--rate", type=float, default=2.0)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--tol", type=float, default=0.1)
+    ap.add_argument("--budget-gb", type=float, default=150.0)
+    a = ap.parse_args()
+    reqs = poisson_requests(a.requests, a.rate, a.seed)
+    print(json.dumps(run_sweep(reqs, a.budget_gb * 1e9, a.tol).summary()))
+
+
+if __name__ == "__main__":
+    main()

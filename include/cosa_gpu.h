@@ -333,6 +333,44 @@ int cosa_gpu_resg_rms_noalloc(int32_t nblocks, const int32_t *dims, int32_t npde
                               int32_t nharms, const double *res, const double *rhs,
                               double *resrms, void *stream);
 
+/*
+ * ---- serving: several steady solves resident on one GPU ----
+ * No counterpart in the reference, which runs one solve per process.  An
+ * engine holds device pools sized by budget_bytes; submitted solves (grid
+ * tables, node coordinates in the P2 layout, initial P3 state, flow
+ * conditions) wait in a first-come queue, are admitted when their arrays fit
+ * in the pools, are advanced together (every RK stage of every active solve
+ * in the same halo and tile launches) and retire when their total residual
+ * norm falls below tol times its first-iteration value (checked every
+ * check_every of their own iterations) or after max_iter iterations.  The
+ * scheme (gamma, limiter, CFL, RK coefficients) is the engine's; machfs,
+ * alpha, beta, the free stream, the inlet total state and the outlet
+ * pressure come from each request.  Explicit Euler, single grid, S = 1,
+ * blocks of at least two cells per direction.
+ */
+#define COSA_SOLVE_QUEUED    0
+#define COSA_SOLVE_ACTIVE    1
+#define COSA_SOLVE_CONVERGED 2
+#define COSA_SOLVE_STOPPED   3  /* max_iter reached */
+#define COSA_SOLVE_FAILED    4  /* non-finite residual norm */
+typedef struct cosa_serve cosa_serve;
+int cosa_serve_create(const cosa_params *scheme, int64_t budget_bytes, int32_t device,
+                      int32_t check_every, cosa_serve **out);
+int cosa_serve_destroy(cosa_serve *e);
+int cosa_serve_submit(cosa_serve *e, const cosa_level_desc *grid, const double *x,
+                      const double *y, const double *z, const double *q0,
+                      const cosa_params *flow, double tol, int32_t max_iter, int64_t *id);
+/* admit what fits, then advance the active solves by up to niter iterations
+   (fewer when none is left); retired solves free their pool slots */
+int cosa_serve_step(cosa_serve *e, int32_t niter, int32_t *nactive, int32_t *nqueued);
+/* state, own iteration count, last residual drop, times (submitted,
+   admitted, done; seconds since the engine was created) and, once retired,
+   the P3 state (q_out may be NULL) */
+int cosa_serve_result(cosa_serve *e, int64_t id, int32_t *state, int32_t *iters, double *rms_drop,
+                      double times[3], double *q_out);
+/* free pool slots (one slot holds one P3 cell of every pool) */
+int64_t cosa_serve_free_slots(cosa_serve *e);
+
 #ifdef __cplusplus
 }
 #endif

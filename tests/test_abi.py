@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _declared():
     src = open(os.path.join(ROOT, "include", "cosa_gpu.h")).read()
-    return sorted(set(re.findall(r"\b(cosa_gpu_\w+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(cosa_(?:gpu|serve)_\w+)\s*\(", src)))
 
 
 def test_library_builds_and_loads():
