@@ -42,6 +42,10 @@ B_ALG_STAGE = 234
 # dt/V and write q (224 B); stage 1 writes dt/V instead of reading it and
 # copies q^n (264 B): average over the 4 stages of a cycle
 B_TILE = (3 * 224 + 264) / 4.0
+# DRAM bytes (read + write) per cell of one tile launch, from the ncu capture
+# summarised in profiles/k_stage_tile_fp64_duct4m.md (a stage-3 launch on the
+# 4.1 M-cell duct, scaled by the cells of the launch)
+TILE_TRAFFIC_B_PER_CELL = 257.8
 
 
 def _peaks():
@@ -193,6 +197,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed, e2e and CPU legs (profiling runs)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving sweep")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="precision of the main timed leg (profiling runs; the default line reports both)")
     args = ap.parse_args()
@@ -305,6 +310,18 @@ def main():
     e2e_val = ws * ncells * nstage * args.e2e_steps / (e2e_ms / 1e3) / 1e6
     state_bytes = nq * 8
 
+    serving = None
+    if rank == 0 and ws == 1 and not args.no_serve:
+        # continuous batching: 20 Poisson arrivals at 2 req/s of bump channels
+        # at three scales and random Mach numbers, each to a residual drop of
+        # 0.1 (single-grid explicit scheme), on this GPU after the duct runs
+        from cosa_b200 import serve
+        try:
+            serving = serve.run_sweep(serve.poisson_requests(20, 2.0, 0), 40e9, 0.1).summary()
+            serving["workload"] = "bump channel x{0.5,1,2} in-plane, M~U[0.3,0.7], Euler, Poisson 2 req/s"
+        except Exception as e:  # reported, not fatal
+            serving = {"error": str(e)}
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         try:
@@ -322,7 +339,9 @@ def main():
                        "l2": "state 1.4 GB > L2 (126 MB): no flush needed",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": "k_stage_tile<32,7,fp64>",
+                         "frac": achieved / peak, "traffic": TILE_TRAFFIC_B_PER_CELL * ncells,
+                         "traffic_source": "ncu dram bytes per cell of the 4.1 M-cell duct x cells",
+                         "kernel": "k_stage_tile<32,7,fp64>",
                          "kernel_ms": kms[1], "halo_ms": kms[0], "bytes_per_cell": B_TILE,
                          "peak_kind": peak_kind, "stage_gbs_alg": stage_gbs},
             "mixed": {"value": value_mixed, "ms_per_step": ms_mixed / args.steps,
@@ -331,6 +350,7 @@ def main():
             "e2e": {"value": e2e_val, "unit": "Mcell-stage/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes + 8 * (p.npde + 1)},
             "cpu_baseline": cpu,
+            "serving": serving,
             "gpu_launches": launches,
             "clocks": clocks,
         }
