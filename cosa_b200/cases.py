@@ -79,6 +79,36 @@ def p1_views(tables: LevelTables, arr: np.ndarray, nsnap: int = 1):
     return views
 
 
+def f0_views(tables: LevelTables, arr: np.ndarray, npde: int, nsnap: int = 1):
+    """Per-block views (im, jm, km, npde, S) of a face-flux (F0) array."""
+    off, _ = tables.offsets()
+    views = []
+    for b, (im, jm, km) in enumerate(tables.dims):
+        n = im * jm * km * npde * nsnap
+        s = off["f0"][b] * npde * nsnap
+        views.append(arr[s:s + n].reshape((im, jm, km, npde, nsnap), order="F"))
+    return views
+
+
+def vm_views(tables: LevelTables, vm: np.ndarray):
+    """Per-block views of the face inverse metrics: vm[b][d-1][m] is the
+    (3, im, jm, km) array of the derivatives of xi (m=0), eta (1), zeta (2)
+    on the faces of family d; array (d, m) starts at ((d-1)*3 + m)*3*n0."""
+    off, tot = tables.offsets()
+    n0 = tot["f0"]
+    out = []
+    for b, (im, jm, km) in enumerate(tables.dims):
+        per = []
+        for d in range(3):
+            row = []
+            for m in range(3):
+                s = (d * 3 + m) * 3 * n0 + off["f0"][b] * 3
+                row.append(vm[s:s + 3 * im * jm * km].reshape((3, im, jm, km), order="F"))
+            per.append(row)
+        out.append(per)
+    return out
+
+
 def interior(v: np.ndarray) -> np.ndarray:
     """Interior cells (1..imax-1, ...) of a P3 block view."""
     return v[2:-2, 2:-2, 2:-2]
@@ -204,7 +234,8 @@ def _permute_block(X, Y, Z):
 
 
 def partitioned_channel(ni: int = 48, nj: int = 24, nk: int = 2, isplit=(20,), jsplit=(10,),
-                        permute_last: bool = True, mach: float = 0.5, kface_bc: int = 4) -> Case:
+                        permute_last: bool = True, mach: float = 0.5, kface_bc: int = 4, wall: int = 14,
+                        params: CosaParams = None) -> Case:
     """Bump channel split at node planes isplit (i) and jsplit (j); the last
     block is stored with permuted indices when permute_last.  The z faces
     default to extrapolation (4): the reference's symmetry BC (80) reflects
@@ -228,8 +259,8 @@ def partitioned_channel(ni: int = 48, nj: int = 24, nk: int = 2, isplit=(20,), j
             types = {}
             if bi == 0: types["imin"] = 21
             if bi == nbi - 1: types["imax"] = 91
-            if bj == 0: types["jmin"] = 14
-            if bj == nbj - 1: types["jmax"] = 14
+            if bj == 0: types["jmin"] = wall
+            if bj == nbj - 1: types["jmax"] = wall
             types["kmin"] = kface_bc
             types["kmax"] = kface_bc
             if permute_last and last and (nbi * nbj > 1):
@@ -279,7 +310,39 @@ def partitioned_channel(ni: int = 48, nj: int = 24, nk: int = 2, isplit=(20,), j
                 s1, e1 = face_nodes(b, "jmax")
                 s2, e2 = face_nodes(o, "jmin")
                 cuts.append((b, s1, e1, o, s2, e2, iord(b, o)))
-    return _assemble(f"partitioned_channel_{ni}x{nj}x{nk}", nodes, specs, cuts, channel_params(mach))
+    return _assemble(f"partitioned_channel_{ni}x{nj}x{nk}", nodes, specs, cuts,
+                     params if params is not None else channel_params(mach))
+
+
+# ---- laminar channel: viscous walls (bctyp 15xx) on the bump channel -----------------
+VISCOUS_WALL = 1500
+
+
+def laminar_params(mach: float = 0.3, reyno: float = 500.0) -> CosaParams:
+    """Channel scheme with the laminar Navier-Stokes terms (viscous = .true.,
+    no turbulence model) at Reynolds number reyno."""
+    p = channel_params(mach)
+    p.viscous = 1
+    p.reyno = reyno
+    p.cfl = 1.5
+    return p
+
+
+def laminar_channel(ni: int = 48, nj: int = 24, nk: int = 2, mach: float = 0.3, reyno: float = 500.0,
+                    kface_bc: int = 80) -> Case:
+    """The bump channel with no-slip adiabatic walls at j = 1 and j = jmax."""
+    X, Y, Z = channel_nodes(ni, nj, nk)
+    spec = BlockSpec(ni + 1, nj + 1, nk + 1, _face_bcs(ni + 1, nj + 1, nk + 1, {
+        "imin": 21, "imax": 91, "jmin": VISCOUS_WALL, "jmax": VISCOUS_WALL, "kmin": kface_bc, "kmax": kface_bc}))
+    return _assemble(f"laminar_channel_{ni}x{nj}x{nk}", [(X, Y, Z)], [spec], [], laminar_params(mach, reyno))
+
+
+def partitioned_laminar_channel(ni: int = 48, nj: int = 24, nk: int = 2, isplit=(20,), jsplit=(10,),
+                                permute_last: bool = True, mach: float = 0.3, reyno: float = 500.0) -> Case:
+    """laminar_channel split into blocks joined by cuts (the last block stored
+    with permuted indices), z faces extrapolated."""
+    return partitioned_channel(ni, nj, nk, isplit, jsplit, permute_last, mach, kface_bc=4, wall=VISCOUS_WALL,
+                               params=laminar_params(mach, reyno))
 
 
 # ---- configuration 3: 3D bump duct --------------------------------------------------

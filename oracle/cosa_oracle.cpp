@@ -520,6 +520,8 @@ void bc_far0(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
   }
 }
 
+void bc_walvis_15(const Patch &pa, B3 &q, const Level &L, const cosa_params &P);
+
 // bbc dispatch (src/bc.f90:35-121): patches in table order
 int bc_level(const Level &L, double *qa, const double *si, const double *sj, const double *sk,
              const cosa_params &P) {
@@ -539,7 +541,8 @@ int bc_level(const Level &L, double *qa, const double *si, const double *sj, con
         case 21: status |= bc_insub(pa, q, vi, vj, vk, L, P); break;
         case 91: bc_outsub(pa, q, L, P); break;
         default:
-          if (pa.bctyp / 100 == 15 || pa.bctyp == 31) status |= COSA_ERR_UNSUPPORTED;
+          if (pa.bctyp / 100 == 15 && !is_kom(P) && !P.moving) bc_walvis_15(pa, q, L, P);
+          else if (pa.bctyp / 100 == 15 || pa.bctyp == 31) status |= COSA_ERR_UNSUPPORTED;
           break;
       }
     }
@@ -1562,6 +1565,558 @@ void tur_vis_level(const Level &L, const double *qa, double *muta, const cosa_pa
   }
 }
 
+// ---- viscous set-up (src/grid.f90) -----------------------------------------
+struct BGw {  // writable grid view (0:im+1, 0:jm+1, 0:km+1)
+  double *p; int I, J;
+  BGw(double *base, const Level &L, int b) : I(L.im[b] + 2), J(L.jm[b] + 2) { p = base + L.op2[b]; }
+  inline double &operator()(int i, int j, int k) const { return p[i + (int64_t)I * (j + (int64_t)J * k)]; }
+};
+struct BV {  // face inverse metrics (3, imax, jmax, kmax), 1-based face index
+  double *p; int I, J;
+  BV(double *base, const Level &L, int b) : I(L.im[b]), J(L.jm[b]) { p = base + L.of0[b] * 3; }
+  inline double &operator()(int c, int i, int j, int k) const {
+    return p[((i - 1) + (int64_t)I * ((j - 1) + (int64_t)J * (k - 1))) * 3 + (c - 1)];
+  }
+};
+
+// cordex_b (src/grid.f90:20-80): ghost nodes repeat the boundary nodes
+void coordex_level(const Level &L, double *xa, double *ya, double *za) {
+  for (int b = 0; b < L.nb; ++b) {
+    const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+    for (double *a : {xa, ya, za}) {
+      BGw X(a, L, b);
+      for (int k = 1; k <= km; ++k) {
+        for (int i = 1; i <= im; ++i) { X(i, 0, k) = X(i, 1, k); X(i, jm + 1, k) = X(i, jm, k); }
+        for (int j = 1; j <= jm; ++j) { X(0, j, k) = X(1, j, k); X(im + 1, j, k) = X(im, j, k); }
+      }
+      for (int j = 1; j <= jm; ++j)
+        for (int i = 1; i <= im; ++i) { X(i, j, 0) = X(i, j, 1); X(i, j, km + 1) = X(i, j, km); }
+    }
+  }
+}
+
+// cut_x, in-process branch (src/grid.f90:242-523): the ghost node plane of
+// block 1 takes the nodes one plane inside block 2
+void cutman_x_level(const Level &L, double *xa, double *ya, double *za) {
+  for (int icut = 0; icut < L.ncuts; ++icut) {
+    const int *c = L.cut.data() + 21 * icut;
+    const int b1 = c[0] - 1, b2 = c[9] - 1;
+    int ijk1[4] = {0, L.im[b1], L.jm[b1], L.km[b1]}, ijk2[4] = {0, L.im[b2], L.jm[b2], L.km[b2]};
+    const int idir1 = c[1], inout1 = c[2], idir2 = c[10], inout2 = c[11];
+    int istr1[4] = {0, c[3], c[5], c[7]}, iend1[4] = {0, c[4], c[6], c[8]};
+    int istr2[4] = {0, c[12], c[14], c[16]}, iend2[4] = {0, c[13], c[15], c[17]};
+    const int iord[4] = {0, c[18], c[19], c[20]};
+    const int ibcpt = inout1 == 1 ? 0 : ijk1[idir1] + 1;
+    const int inr = inout2 == 1 ? 2 : ijk2[idir2] - 1;
+    for (int l = 1; l <= 3; ++l)
+      if (l != idir1) { if (iend1[l] > istr1[l]) iend1[l] += 1; else istr1[l] += 1; }
+    for (int l = 1; l <= 3; ++l)
+      if (l != idir2) { if (iend2[l] > istr2[l]) iend2[l] += 1; else istr2[l] += 1; }
+    int len[4], isgn1[4], isgn2[4];
+    for (int l = 1; l <= 3; ++l) {
+      len[l] = std::abs(iend1[l] - istr1[l]);
+      isgn1[l] = iend1[l] > istr1[l] ? 1 : -1;
+      isgn2[l] = iend2[l] > istr2[l] ? 1 : -1;
+    }
+    const int ic1 = cyc(idir1, 1), ic2 = cyc(idir1, 2), ic3 = cyc(idir1, 3);
+    const int jc1 = iord[ic1], jc2 = iord[ic2], jc3 = iord[ic3];
+    for (double *a : {xa, ya, za}) {
+      BGw X1(a, L, b1), X2(a, L, b2);
+      for (int i3 = 0; i3 <= len[ic3]; ++i3)
+        for (int i2 = 0; i2 <= len[ic2]; ++i2) {
+          const int a2_ = istr1[ic2] + isgn1[ic2] * i2, a3_ = istr1[ic3] + isgn1[ic3] * i3;
+          const int ii1 = ibcpt * krd(ic1, 1) + a2_ * krd(ic2, 1) + a3_ * krd(ic3, 1);
+          const int jj1 = ibcpt * krd(ic1, 2) + a2_ * krd(ic2, 2) + a3_ * krd(ic3, 2);
+          const int kk1 = ibcpt * krd(ic1, 3) + a2_ * krd(ic2, 3) + a3_ * krd(ic3, 3);
+          const int b2_ = istr2[jc2] + isgn2[jc2] * i2, b3_ = istr2[jc3] + isgn2[jc3] * i3;
+          const int in1 = inr * krd(jc1, 1) + b2_ * krd(jc2, 1) + b3_ * krd(jc3, 1);
+          const int jn1 = inr * krd(jc1, 2) + b2_ * krd(jc2, 2) + b3_ * krd(jc3, 2);
+          const int kn1 = inr * krd(jc1, 3) + b2_ * krd(jc2, 3) + b3_ * krd(jc3, 3);
+          X1(ii1, jj1, kk1) = X2(in1, jn1, kn1);
+        }
+    }
+  }
+}
+
+// volex_b (src/grid.f90:110-136): face-halo volumes repeat the first cell
+void volex_level(const Level &L, double *va) {
+  for (int b = 0; b < L.nb; ++b) {
+    B1 vol(va, L, b, 1);
+    const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+    for (int k = 1; k <= km - 1; ++k) {
+      for (int i = 1; i <= im - 1; ++i) { vol(i, 0, k) = vol(i, 1, k); vol(i, jm, k) = vol(i, jm - 1, k); }
+      for (int j = 1; j <= jm - 1; ++j) { vol(0, j, k) = vol(1, j, k); vol(im, j, k) = vol(im - 1, j, k); }
+    }
+    for (int j = 1; j <= jm - 1; ++j)
+      for (int i = 1; i <= im - 1; ++i) { vol(i, j, 0) = vol(i, j, 1); vol(i, j, km) = vol(i, j, km - 1); }
+  }
+}
+
+// cut_v, in-process branch (src/grid.f90:612-700): one halo layer of volumes
+void cutman_v_level(const Level &L, double *va) {
+  for (int icut = 0; icut < L.ncuts; ++icut) {
+    const int *c = L.cut.data() + 21 * icut;
+    const int b1 = c[0] - 1, b2 = c[9] - 1;
+    int ijk1[4] = {0, L.im[b1], L.jm[b1], L.km[b1]}, ijk2[4] = {0, L.im[b2], L.jm[b2], L.km[b2]};
+    const int idir1 = c[1], inout1 = c[2], idir2 = c[10], inout2 = c[11];
+    const int istr1[4] = {0, c[3], c[5], c[7]}, iend1[4] = {0, c[4], c[6], c[8]};
+    const int istr2[4] = {0, c[12], c[14], c[16]}, iend2[4] = {0, c[13], c[15], c[17]};
+    const int iord[4] = {0, c[18], c[19], c[20]};
+    const int ibcpt = inout1 == 1 ? 0 : ijk1[idir1];
+    const int inr = inout2 == 1 ? 1 : ijk2[idir2] - 1;
+    int len[4], isgn1[4], isgn2[4];
+    for (int l = 1; l <= 3; ++l) {
+      len[l] = std::abs(iend1[l] - istr1[l]);
+      isgn1[l] = iend1[l] > istr1[l] ? 1 : -1;
+      isgn2[l] = iend2[l] > istr2[l] ? 1 : -1;
+    }
+    const int ic1 = cyc(idir1, 1), ic2 = cyc(idir1, 2), ic3 = cyc(idir1, 3);
+    const int jc1 = iord[ic1], jc2 = iord[ic2], jc3 = iord[ic3];
+    B1 v1(va, L, b1, 1), v2(va, L, b2, 1);
+    for (int i3 = 0; i3 <= len[ic3]; ++i3)
+      for (int i2 = 0; i2 <= len[ic2]; ++i2) {
+        const int a2_ = istr1[ic2] + isgn1[ic2] * i2, a3_ = istr1[ic3] + isgn1[ic3] * i3;
+        const int ii1 = ibcpt * krd(ic1, 1) + a2_ * krd(ic2, 1) + a3_ * krd(ic3, 1);
+        const int jj1 = ibcpt * krd(ic1, 2) + a2_ * krd(ic2, 2) + a3_ * krd(ic3, 2);
+        const int kk1 = ibcpt * krd(ic1, 3) + a2_ * krd(ic2, 3) + a3_ * krd(ic3, 3);
+        const int b2_ = istr2[jc2] + isgn2[jc2] * i2, b3_ = istr2[jc3] + isgn2[jc3] * i3;
+        const int in1 = inr * krd(jc1, 1) + b2_ * krd(jc2, 1) + b3_ * krd(jc3, 1);
+        const int jn1 = inr * krd(jc1, 2) + b2_ * krd(jc2, 2) + b3_ * krd(jc3, 2);
+        const int kn1 = inr * krd(jc1, 3) + b2_ * krd(jc2, 3) + b3_ * krd(jc3, 3);
+        v1(ii1, jj1, kk1) = v2(in1, jn1, kn1);
+      }
+  }
+}
+
+// vmetrix_b (src/grid.f90:3150-3582): the inverse metrics xi_x .. zeta_z on
+// the faces of family d from node differences averaged over the face, with
+// one-sided differences doubled where a ghost node coincides with its node
+// (coordex), divided by the mean volume of the two cells of the face.
+// vm[m] receives (xi, eta, zeta)_(x, y, z) for m = xi, eta, zeta.
+void vmetrix_b(const Level &L, int b, int d, const double *xa, const double *ya, const double *za,
+               const double *va, double *vm0, double *vm1, double *vm2) {
+  BGw X(const_cast<double *>(xa), L, b), Y(const_cast<double *>(ya), L, b), Z(const_cast<double *>(za), L, b);
+  B1 vol(const_cast<double *>(va), L, b, 1);
+  BV o0(vm0, L, b), o1(vm1, L, b), o2(vm2, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  const int ni = d == 1 ? im : im - 1, nj = d == 2 ? jm : jm - 1, nk = d == 3 ? km : km - 1;
+  const int ijkm[4] = {0, im, jm, km};
+  // unit offsets and the corner lists of the reference
+  auto e = [](int dir, int o[3]) { o[0] = dir == 1; o[1] = dir == 2; o[2] = dir == 3; };
+  for (int k = 1; k <= nk; ++k)
+    for (int j = 1; j <= nj; ++j)
+      for (int i = 1; i <= ni; ++i) {
+        const int p[3] = {i, j, k};
+        double g[4][3][5];  // g[dir][xyz][0..4]
+        for (int dir = 1; dir <= 3; ++dir) {
+          int ed[3];
+          e(dir, ed);
+          if (dir == d) {
+            // 4 corners of the face in the reference's order
+            int cr[4][3];
+            if (d == 1) { int t[4][3] = {{0,0,0},{0,1,0},{0,1,1},{0,0,1}}; std::memcpy(cr, t, sizeof t); }
+            else if (d == 2) { int t[4][3] = {{0,0,0},{0,0,1},{1,0,1},{1,0,0}}; std::memcpy(cr, t, sizeof t); }
+            else { int t[4][3] = {{0,0,0},{1,0,0},{1,1,0},{0,1,0}}; std::memcpy(cr, t, sizeof t); }
+            const int pos = p[d - 1];
+            for (int m = 0; m < 4; ++m) {
+              const int a0 = p[0] + cr[m][0], a1 = p[1] + cr[m][1], a2 = p[2] + cr[m][2];
+              const int hp[3] = {a0 + ed[0], a1 + ed[1], a2 + ed[2]}, hm[3] = {a0 - ed[0], a1 - ed[1], a2 - ed[2]};
+              double v3[3];
+              int c = 0;
+              for (BGw *A : {&X, &Y, &Z}) {
+                v3[c] = ((*A)(hp[0], hp[1], hp[2]) - (*A)(hm[0], hm[1], hm[2])) / 2;
+                ++c;
+              }
+              if (pos == 1 || pos == ijkm[d]) {
+                const int *gh = pos == 1 ? hm : hp;
+                const double dx = X(gh[0], gh[1], gh[2]) - X(a0, a1, a2);
+                const double dy = Y(gh[0], gh[1], gh[2]) - Y(a0, a1, a2);
+                const double dz = Z(gh[0], gh[1], gh[2]) - Z(a0, a1, a2);
+                const double dist = std::sqrt(dx * dx + dy * dy + dz * dz);
+                if (dist < 1.0e-14) for (int c2 = 0; c2 < 3; ++c2) v3[c2] = 2 * v3[c2];
+              }
+              for (int c2 = 0; c2 < 3; ++c2) g[dir][c2][m + 1] = v3[c2];
+            }
+            for (int c2 = 0; c2 < 3; ++c2)
+              g[dir][c2][0] = (g[dir][c2][1] + g[dir][c2][2] + g[dir][c2][3] + g[dir][c2][4]) / 4;
+          } else {
+            // two edge differences along dir, at the reference's positions
+            int s[2][3];
+            const int other = 6 - d - dir;  // the remaining direction
+            int eo[3];
+            e(other, eo);
+            s[0][0] = 0; s[0][1] = 0; s[0][2] = 0;
+            s[1][0] = eo[0]; s[1][1] = eo[1]; s[1][2] = eo[2];
+            for (int m = 0; m < 2; ++m) {
+              const int a0 = p[0] + s[m][0], a1 = p[1] + s[m][1], a2 = p[2] + s[m][2];
+              int c = 0;
+              for (BGw *A : {&X, &Y, &Z}) {
+                g[dir][c][m + 1] = (*A)(a0 + ed[0], a1 + ed[1], a2 + ed[2]) - (*A)(a0, a1, a2);
+                ++c;
+              }
+            }
+            for (int c2 = 0; c2 < 3; ++c2) g[dir][c2][0] = (g[dir][c2][1] + g[dir][c2][2]) / 2;
+          }
+        }
+        double volvisc;
+        if (d == 1) volvisc = (vol(i - 1, j, k) + vol(i, j, k)) / 2;
+        else if (d == 2) volvisc = (vol(i, j, k) + vol(i, j - 1, k)) / 2;
+        else volvisc = (vol(i, j, k) + vol(i, j, k - 1)) / 2;
+        const double x_xi = g[1][0][0], y_xi = g[1][1][0], z_xi = g[1][2][0];
+        const double x_eta = g[2][0][0], y_eta = g[2][1][0], z_eta = g[2][2][0];
+        const double x_zeta = g[3][0][0], y_zeta = g[3][1][0], z_zeta = g[3][2][0];
+        o0(1, i, j, k) = (z_zeta * y_eta - z_eta * y_zeta) / volvisc;
+        o0(2, i, j, k) = (x_zeta * z_eta - x_eta * z_zeta) / volvisc;
+        o0(3, i, j, k) = (y_zeta * x_eta - y_eta * x_zeta) / volvisc;
+        o1(1, i, j, k) = (z_xi * y_zeta - z_zeta * y_xi) / volvisc;
+        o1(2, i, j, k) = (x_xi * z_zeta - x_zeta * z_xi) / volvisc;
+        o1(3, i, j, k) = (y_xi * x_zeta - y_zeta * x_xi) / volvisc;
+        o2(1, i, j, k) = (z_eta * y_xi - z_xi * y_eta) / volvisc;
+        o2(2, i, j, k) = (x_eta * z_xi - x_xi * z_eta) / volvisc;
+        o2(3, i, j, k) = (y_eta * x_xi - y_xi * x_eta) / volvisc;
+      }
+}
+
+// ---- viscous residual (src/flux.f90) ----------------------------------------
+// bq_face_* (src/flux.f90:2432-2801): face averages of the primitive state,
+// the halo (wall) value on strong-boundary faces
+void q_face_b(const Level &L, int b, int d, const double *qa, double *qfa) {
+  B3 q(const_cast<double *>(qa), L, b), qf(qfa, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  const int ni = d == 1 ? im : im - 1, nj = d == 2 ? jm : jm - 1, nk = d == 3 ? km : km - 1;
+  const int di = d == 1, dj = d == 2, dk = d == 3;
+  for (int n = 0; n < L.S; ++n)
+    for (int v = 1; v <= L.npde; ++v)
+      for (int k = 1; k <= nk; ++k)
+        for (int j = 1; j <= nj; ++j)
+          for (int i = 1; i <= ni; ++i)
+            qf(i, j, k, v, n) = (q(i - di, j - dj, k - dk, v, n) + q(i, j, k, v, n)) / 2;
+  const int *t = L.bct.data() + L.obct[b];
+  for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
+    Patch pa = patch_of(t + 10 * ibc, im, jm, km);
+    if (pa.idir != d || !strong_bc(pa.bctyp)) continue;
+    const int ibcpt = pa.inrout == 1 ? 0 : pa.ijk[d], iface = pa.inrout == 1 ? 1 : pa.ijk[d];
+    for (int n = 0; n < L.S; ++n)
+      for (int v = 1; v <= L.npde; ++v)
+        for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+          for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+            int a, bb, c, e, f, g;
+            pidx(pa, iface, i2, i3, a, bb, c);
+            pidx(pa, ibcpt, i2, i3, e, f, g);
+            qf(a, bb, c, v, n) = q(e, f, g, v, n);
+          }
+  }
+}
+
+// bq_der_* (src/flux.f90:1848-2390): face gradients in computational
+// coordinates; one-sided three-point normal derivative and tangential
+// derivatives along the halo (wall) line on strong-boundary faces
+void q_der_b(const Level &L, int b, int d, const double *qa, double *dxa, double *dya, double *dza) {
+  B3 q(const_cast<double *>(qa), L, b);
+  B3 dqs[3] = {B3(dxa, L, b), B3(dya, L, b), B3(dza, L, b)};
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  const int ni = d == 1 ? im : im - 1, nj = d == 2 ? jm : jm - 1, nk = d == 3 ? km : km - 1;
+  const int ed[3] = {d == 1, d == 2, d == 3};
+  for (int n = 0; n < L.S; ++n)
+    for (int v = 1; v <= L.npde; ++v)
+      for (int k = 1; k <= nk; ++k)
+        for (int j = 1; j <= nj; ++j)
+          for (int i = 1; i <= ni; ++i) {
+            const int mi = i - ed[0], mj = j - ed[1], mk = k - ed[2];
+            for (int t = 1; t <= 3; ++t) {
+              if (t == d) {
+                dqs[t - 1](i, j, k, v, n) = q(i, j, k, v, n) - q(mi, mj, mk, v, n);
+                continue;
+              }
+              const int ti = t == 1, tj = t == 2, tk = t == 3;
+              const double q2 = (q(mi, mj, mk, v, n) + q(i, j, k, v, n) + q(i + ti, j + tj, k + tk, v, n) +
+                                 q(mi + ti, mj + tj, mk + tk, v, n)) / 4;
+              const double q1 = (q(mi - ti, mj - tj, mk - tk, v, n) + q(i - ti, j - tj, k - tk, v, n) +
+                                 q(i, j, k, v, n) + q(mi, mj, mk, v, n)) / 4;
+              dqs[t - 1](i, j, k, v, n) = q2 - q1;
+            }
+          }
+  const int *tb = L.bct.data() + L.obct[b];
+  for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
+    Patch pa = patch_of(tb + 10 * ibc, im, jm, km);
+    if (pa.idir != d || !strong_bc(pa.bctyp)) continue;
+    const bool lo = pa.inrout == 1;
+    const int iaux = lo ? 0 : pa.ijk[d], in1 = lo ? 1 : pa.ijk[d] - 1, in2 = lo ? 2 : pa.ijk[d] - 2;
+    const int iface = lo ? 1 : pa.ijk[d];
+    const double sgnm = lo ? 1.0 : -1.0;
+    for (int n = 0; n < L.S; ++n)
+      for (int v = 1; v <= L.npde; ++v)
+        for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+          for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+            int fi, fj, fk, ai, aj, ak, n1i, n1j, n1k, n2i, n2j, n2k;
+            pidx(pa, iface, i2, i3, fi, fj, fk);
+            pidx(pa, iaux, i2, i3, ai, aj, ak);
+            pidx(pa, in1, i2, i3, n1i, n1j, n1k);
+            pidx(pa, in2, i2, i3, n2i, n2j, n2k);
+            dqs[d - 1](fi, fj, fk, v, n) = sgnm / 3 *
+                (-q(ai, aj, ak, v, n) * 8 + q(n1i, n1j, n1k, v, n) * 9 - q(n2i, n2j, n2k, v, n));
+            for (int t = 1; t <= 3; ++t) {
+              if (t == d) continue;
+              const int ti = t == 1, tj = t == 2, tk = t == 3;
+              const int pos = t == 1 ? ai : (t == 2 ? aj : ak);
+              auto Q = [&](int s) { return q(ai + s * ti, aj + s * tj, ak + s * tk, v, n); };
+              double q2, q1;
+              if (pos == pa.istrt[t]) { q2 = (Q(0) + Q(1)) / 2; q1 = (Q(0) * 3 - Q(1)) / 2; }
+              else if (pos == pa.iend[t]) { q2 = (Q(0) * 3 - Q(-1)) / 2; q1 = (Q(0) + Q(-1)) / 2; }
+              else { q2 = (Q(0) + Q(1)) / 2; q1 = (Q(-1) + Q(0)) / 2; }
+              dqs[t - 1](fi, fj, fk, v, n) = q2 - q1;
+            }
+          }
+  }
+}
+
+// vflux_b, laminar branch (src/flux.f90:878-1180): viscous stresses and heat
+// flux on the faces of family d; the energy row keeps the reference's terms
+void vflux_b(const Level &L, int b, int d, const double *qfa, const double *dxa, const double *dya,
+             const double *dza, const double *xd, const double *ed, const double *zd, const double *sijk,
+             double *fa, const cosa_params &P) {
+  B3 qf(const_cast<double *>(qfa), L, b), dqx(const_cast<double *>(dxa), L, b);
+  B3 dqe(const_cast<double *>(dya), L, b), dqz(const_cast<double *>(dza), L, b);
+  BV xv(const_cast<double *>(xd), L, b), ev(const_cast<double *>(ed), L, b), zv(const_cast<double *>(zd), L, b);
+  B2 s(sijk, L, b);
+  B0 flux(fa, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  const int ni = d == 1 ? im : im - 1, nj = d == 2 ? jm : jm - 1, nk = d == 3 ? km : km - 1;
+  const double g = P.gamma, mr = P.machfs / P.reyno;
+  for (int n = 0; n < L.S; ++n)
+    for (int k = 1; k <= nk; ++k)
+      for (int j = 1; j <= nj; ++j)
+        for (int i = 1; i <= ni; ++i)
+          for (int v = 1; v <= 5; ++v) flux(i, j, k, v, n) = 0;
+  for (int n = 0; n < L.S; ++n) {
+    const int nh = n * P.hbmove;
+    for (int k = 1; k <= nk; ++k)
+      for (int j = 1; j <= nj; ++j)
+        for (int i = 1; i <= ni; ++i) {
+          const double kx = s(1, i, j, k, nh), ky = s(2, i, j, k, nh), kz = s(3, i, j, k, nh), ds = s(4, i, j, k, nh);
+          const double rho = qf(i, j, k, 1, n), u = qf(i, j, k, 2, n), v = qf(i, j, k, 3, n), w = qf(i, j, k, 4, n);
+          const double p = qf(i, j, k, 5, n);
+          const double t = g * p / rho;
+          const double mu = (P.stemp + 1) / (t + P.stemp) * std::pow(t, 1.5);
+          const double mut = flux(i, j, k, 1, n);
+          const double xix = xv(1, i, j, k), xiy = xv(2, i, j, k), xiz = xv(3, i, j, k);
+          const double etax = ev(1, i, j, k), etay = ev(2, i, j, k), etaz = ev(3, i, j, k);
+          const double zetax = zv(1, i, j, k), zetay = zv(2, i, j, k), zetaz = zv(3, i, j, k);
+          const double uxi = dqx(i, j, k, 2, n), ueta = dqe(i, j, k, 2, n), uzeta = dqz(i, j, k, 2, n);
+          const double vxi = dqx(i, j, k, 3, n), veta = dqe(i, j, k, 3, n), vzeta = dqz(i, j, k, 3, n);
+          const double wxi = dqx(i, j, k, 4, n), weta = dqe(i, j, k, 4, n), wzeta = dqz(i, j, k, 4, n);
+          const double txi = t * (dqx(i, j, k, 5, n) / p - dqx(i, j, k, 1, n) / rho);
+          const double teta = t * (dqe(i, j, k, 5, n) / p - dqe(i, j, k, 1, n) / rho);
+          const double tzeta = t * (dqz(i, j, k, 5, n) / p - dqz(i, j, k, 1, n) / rho);
+          const double dudx = uxi * xix + ueta * etax + uzeta * zetax;
+          const double dudy = uxi * xiy + ueta * etay + uzeta * zetay;
+          const double dudz = uxi * xiz + ueta * etaz + uzeta * zetaz;
+          const double dvdx = vxi * xix + veta * etax + vzeta * zetax;
+          const double dvdy = vxi * xiy + veta * etay + vzeta * zetay;
+          const double dvdz = vxi * xiz + veta * etaz + vzeta * zetaz;
+          const double dwdx = wxi * xix + weta * etax + wzeta * zetax;
+          const double dwdy = wxi * xiy + weta * etay + wzeta * zetay;
+          const double dwdz = wxi * xiz + weta * etaz + wzeta * zetaz;
+          const double dtdx = txi * xix + teta * etax + tzeta * zetax;
+          const double dtdy = txi * xiy + teta * etay + tzeta * zetay;
+          const double dtdz = txi * xiz + teta * etaz + tzeta * zetaz;
+          const double divv = dudx + dvdy + dwdz;
+          const double txx = mr * 2 * mu * (dudx - divv / 3);
+          const double txy = mr * mu * (dudy + dvdx);
+          const double txz = mr * mu * (dudz + dwdx);
+          const double tyy = mr * 2 * mu * (dvdy - divv / 3);
+          const double tyz = mr * mu * (dvdz + dwdy);
+          const double tzz = mr * 2 * mu * (dwdz - divv / 3);
+          const double cq = mr * (mu / P.pranl + mut / P.prant) / (g - 1);
+          const double qx = -(cq * dtdx), qy = -(cq * dtdy), qz = -(cq * dtdz);
+          flux(i, j, k, 1, n) = 0;
+          flux(i, j, k, 2, n) = flux(i, j, k, 2, n) - (txx * kx + txy * ky + txz * kz) * ds;
+          flux(i, j, k, 3, n) = flux(i, j, k, 3, n) - (txy * kx + tyy * ky + tyz * kz) * ds;
+          flux(i, j, k, 4, n) = flux(i, j, k, 4, n) - (txz * kx + tyz * ky + tzz * kz) * ds;
+          flux(i, j, k, 5, n) = flux(i, j, k, 5, n) -
+                                ((u * txx + v * txy + w * txz) * kx + (u * txy + v * tyy + w * tyz) * ky +
+                                 (u * txy + v * tyy + w * tyz) * kz) * ds +
+                                (qx * kx + qy * ky + qz * kz) * ds;
+        }
+  }
+}
+
+// bc_walvis_15, laminar part (src/bc.f90:2144-2300): no-slip wall on a fixed
+// grid; the wall pressure extrapolated, the density isentropic from cell 1
+void bc_walvis_15(const Patch &pa, B3 &q, const Level &L, const cosa_params &P) {
+  const int ibcpt = pa.inrout == 1 ? 0 : pa.ijk[pa.idir], ibcpt2 = pa.inrout == 1 ? -1 : pa.ijk[pa.idir] + 1;
+  const int ibcn = pa.inrout == 1 ? 1 : pa.ijk[pa.idir] - 1, ibcn2 = pa.inrout == 1 ? 2 : pa.ijk[pa.idir] - 2;
+  for (int n = 0; n < L.S; ++n)
+    for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+      for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+        int hi, hj, hk, h2i, h2j, h2k, ni_, nj_, nk_, n2i, n2j, n2k;
+        pidx(pa, ibcpt, i2, i3, hi, hj, hk);
+        pidx(pa, ibcpt2, i2, i3, h2i, h2j, h2k);
+        pidx(pa, ibcn, i2, i3, ni_, nj_, nk_);
+        pidx(pa, ibcn2, i2, i3, n2i, n2j, n2k);
+        const double p1 = q(ni_, nj_, nk_, 5, n), p2 = q(n2i, n2j, n2k, 5, n);
+        const double pw = 0.5 * (3 * p1 - p2);
+        const double rhow = std::pow(pw / p1, 1 / P.gamma) * q(ni_, nj_, nk_, 1, n);
+        q(hi, hj, hk, 1, n) = rhow;
+        q(hi, hj, hk, 2, n) = 0.0;
+        q(hi, hj, hk, 3, n) = 0.0;
+        q(hi, hj, hk, 4, n) = 0.0;
+        q(hi, hj, hk, 5, n) = pw;
+        for (int v = 1; v <= 5; ++v) q(h2i, h2j, h2k, v, n) = q(hi, hj, hk, v, n);
+      }
+}
+
+// lambdab viscous branch + eig_ns (src/cosa.f90:1335-1423, 4236-4297): the
+// convective lambdas and the viscous ones (kept in lamv(.,1:3)); the
+// neighbour temperatures on the + side use rho of the - side, as the
+// reference does
+void lambda_ns_level(const Level &L, const double *qa, const double *si, const double *sj, const double *sk,
+                     const double *va, const double *muta, double *lam, double *lamv, const cosa_params &P) {
+  const double g = P.gamma, st = P.stemp;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 q(const_cast<double *>(qa), L, b), lm(lam, L, b), lv(lamv, L, b);
+    B2 vi(si, L, b), vj(sj, L, b), vk(sk, L, b);
+    B1 vol(const_cast<double *>(va), L, b, 1);
+    for (int n = 0; n < L.S; ++n) {
+      const int nh = n * P.hbmove;
+      auto MUT = [&](int i, int j, int k) -> double {
+        if (!muta) return 0.0;
+        B3s mu(const_cast<double *>(muta), L, b);
+        return mu(i, j, k, n);
+      };
+      auto MU = [&](double t) { return (st + 1.0) / (t + st) * std::pow(t, 1.5); };
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            const double rho = q(i, j, k, 1, n), p = q(i, j, k, 5, n);
+            const double t = g * p / rho, mu = MU(t), mutc = MUT(i, j, k);
+            double mud[3], mutd[3];
+            const int dd[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+            for (int d = 0; d < 3; ++d) {
+              const int a = dd[d][0], bq = dd[d][1], c = dd[d][2];
+              const double rhom = q(i - a, j - bq, k - c, 1, n), pm = q(i - a, j - bq, k - c, 5, n);
+              const double tm = g * pm / rhom, mum = MU(tm), mutm = MUT(i - a, j - bq, k - c);
+              const double pp = q(i + a, j + bq, k + c, 5, n);
+              const double tp = g * pp / rhom, mup = MU(tp), mutp = MUT(i + a, j + bq, k + c);
+              mud[d] = (mum + 2 * mu + mup) / 4;
+              mutd[d] = (mutm + 2 * mutc + mutp) / 4;
+            }
+            double sim[5], sip[5], sjm[5], sjp[5], skm[5], skp[5];
+            for (int c = 1; c <= 4; ++c) {
+              sim[c] = vi(c, i, j, k, nh); sip[c] = vi(c, i + 1, j, k, nh);
+              sjm[c] = vj(c, i, j, k, nh); sjp[c] = vj(c, i, j + 1, k, nh);
+              skm[c] = vk(c, i, j, k, nh); skp[c] = vk(c, i, j, k + 1, nh);
+            }
+            const double u = q(i, j, k, 2, n), v = q(i, j, k, 3, n), w = q(i, j, k, 4, n);
+            const double a = std::sqrt(t);
+            const double xix = 0.5 * (sim[1] * sim[4] + sip[1] * sip[4]);
+            const double xiy = 0.5 * (sim[2] * sim[4] + sip[2] * sip[4]);
+            const double xiz = 0.5 * (sim[3] * sim[4] + sip[3] * sip[4]);
+            const double etax = 0.5 * (sjm[1] * sjm[4] + sjp[1] * sjp[4]);
+            const double etay = 0.5 * (sjm[2] * sjm[4] + sjp[2] * sjp[4]);
+            const double etaz = 0.5 * (sjm[3] * sjm[4] + sjp[3] * sjp[4]);
+            const double zetax = 0.5 * (skm[1] * skm[4] + skp[1] * skp[4]);
+            const double zetay = 0.5 * (skm[2] * skm[4] + skp[2] * skp[4]);
+            const double zetaz = 0.5 * (skm[3] * skm[4] + skp[3] * skp[4]);
+            const double axi = (sim[4] + sip[4]) / 2, aeta = (sjm[4] + sjp[4]) / 2, azeta = (skm[4] + skp[4]) / 2;
+            lm(i, j, k, 1, n) = std::fabs(u * xix + v * xiy + w * xiz) + a * axi;
+            lm(i, j, k, 2, n) = std::fabs(u * etax + v * etay + w * etaz) + a * aeta;
+            lm(i, j, k, 3, n) = std::fabs(u * zetax + v * zetay + w * zetaz) + a * azeta;
+            const double volc = vol(i, j, k), cm = P.cdff;
+            lv(i, j, k, 1, n) = cm * axi * axi * g * P.machfs / P.reyno * (mud[0] / P.pranl + mutd[0] / P.prant) /
+                                (rho * volc);
+            lv(i, j, k, 2, n) = cm * aeta * aeta * g * P.machfs / P.reyno * (mud[1] / P.pranl + mutd[1] / P.prant) /
+                                (rho * volc);
+            lv(i, j, k, 3, n) = cm * azeta * azeta * g * P.machfs / P.reyno * (mud[2] / P.pranl + mutd[2] / P.prant) /
+                                (rho * volc);
+          }
+    }
+  }
+}
+
+
+// bdeltat, viscous branch (src/cosa.f90:4861-4876, 4895-5010): the viscous
+// lambdas join the time step unless irsop is 5 or 6, where they raise the
+// smoothing coefficients instead
+void deltat_ns_level(const Level &L, double *dtv, const double *lam, const double *lamv, double *bx_, double *by_,
+                     double *bz_, const cosa_params &P) {
+  const double zeta = 0.4, c1 = 40.0;
+  const bool dt_visc = P.irsop != 5 && P.irsop != 6;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 lm(const_cast<double *>(lam), L, b), lv(const_cast<double *>(lamv), L, b);
+    B1 dt(dtv, L, b, L.S);
+    for (int n = 0; n < L.S; ++n)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            if (dt_visc)
+              dt(i, j, k, n) = P.cfl / (lm(i, j, k, 1, n) + lm(i, j, k, 2, n) + lm(i, j, k, 3, n) +
+                                        lv(i, j, k, 1, n) + lv(i, j, k, 2, n) + lv(i, j, k, 3, n));
+            else
+              dt(i, j, k, n) = P.cfl / (lm(i, j, k, 1, n) + lm(i, j, k, 2, n) + lm(i, j, k, 3, n));
+          }
+    if (P.irsop == 0 || !bx_) continue;
+    B1 bx(bx_, L, b, L.S), by(by_, L, b, L.S), bz(bz_, L, b, L.S);
+    const double rat = P.rat, psirs = P.psirs;
+    for (int n = 0; n < L.S; ++n)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            const double lami = lm(i, j, k, 1, n), lamj = lm(i, j, k, 2, n), lamk = lm(i, j, k, 3, n);
+            const double lamvi = lv(i, j, k, 1, n), lamvj = lv(i, j, k, 2, n), lamvk = lv(i, j, k, 3, n);
+            double ba = 0, bb = 0, bc = 0;
+            if (P.irsop == 2 || P.irsop == 5) {
+              const double phixi = 1 + std::pow(lamj / lami, zeta) + std::pow(lamk / lami, zeta);
+              const double phieta = 1 + std::pow(lami / lamj, zeta) + std::pow(lamk / lamj, zeta);
+              const double phizeta = 1 + std::pow(lami / lamk, zeta) + std::pow(lamj / lamk, zeta);
+              double t;
+              t = (rat * lami * phixi / (lami + lamj + lamk));
+              ba = std::max(0.0, (t * t - 1) / 4);
+              t = (rat * lamj * phieta / (lami + lamj + lamk));
+              bb = std::max(0.0, (t * t - 1) / 4);
+              t = (rat * lamk * phizeta / (lami + lamj + lamk));
+              bc = std::max(0.0, (t * t - 1) / 4);
+              if (P.irsop == 5) {
+                ba = std::max(ba, c1 / 4 * lamvi / (lami + lamj + lamk));
+                bb = std::max(bb, c1 / 4 * lamvj / (lami + lamj + lamk));
+                bc = std::max(bc, c1 / 4 * lamvk / (lami + lamj + lamk));
+              }
+            } else if (P.irsop == 3 || P.irsop == 6) {
+              const double rji = lamj / lami, rki = lamk / lami, rij = lami / lamj;
+              const double rkj = lamk / lamj, rik = lami / lamk, rjk = lamj / lamk;
+              double t;
+              t = rat / (1 + psirs * (rji + rki));
+              ba = std::max(0.0, 0.25 * (t * t - 1));
+              t = rat / (1 + psirs * (rij + rkj));
+              bb = std::max(0.0, 0.25 * (t * t - 1));
+              t = rat / (1 + psirs * (rik + rjk));
+              bc = std::max(0.0, 0.25 * (t * t - 1));
+              if (P.irsop == 6) {
+                ba = std::max(ba, 0.25 * c1 * lamvi / (lami + lamj + lamk));
+                bb = std::max(bb, 0.25 * c1 * lamvj / (lami + lamj + lamk));
+                bc = std::max(bc, 0.25 * c1 * lamvk / (lami + lamj + lamk));
+              }
+            }
+            bx(i, j, k, n) = ba; by(i, j, k, n) = bb; bz(i, j, k, n) = bc;
+          }
+  }
+}
+
+// viscous set-up of a level as the solver start does it (src/cosa.f90:
+// 300-322): volume and node halos, then the face inverse metrics.
+// vm holds the 9 arrays (xi, eta, zeta derivatives on i-, j-, k-faces),
+// array (d, m) at vm + ((d-1)*3 + m) * 3 * n0.
+void viscous_setup_level(const Level &L, double *x, double *y, double *z, double *vol, double *vm) {
+  volex_level(L, vol);
+  cutman_v_level(L, vol);
+  coordex_level(L, x, y, z);
+  cutman_x_level(L, x, y, z);
+  for (int d = 1; d <= 3; ++d) {
+    double *a = vm + (int64_t)(d - 1) * 9 * L.n0;
+    for (int b = 0; b < L.nb; ++b) vmetrix_b(L, b, d, x, y, z, vol, a, a + 3 * L.n0, a + 6 * L.n0);
+  }
+}
+
 }  // namespace
 
 // ============================================================================
@@ -1668,7 +2223,7 @@ void orc_roe_face(const cosa_params *p, const double *nrm, const double *qr, con
 int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
                   const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
                   double *dqp, double *dqm, double *flux, double *dtvol, int want_dt, double *bx, double *by,
-                  double *bz, const double *vol = nullptr);
+                  double *bz, const double *vol = nullptr, const double *vm = nullptr);
 
 int orc_residual(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
                  const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
@@ -1680,17 +2235,26 @@ int orc_residual(orc_level *h, const cosa_params *p, int nl, double *q, const do
 int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
                   const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
                   double *dqp, double *dqm, double *flux, double *dtvol, int want_dt, double *bx, double *by,
-                  double *bz, const double *vol) {
+                  double *bz, const double *vol, const double *vm) {
   Level &L = h->L;
+  const bool visc = p->viscous != 0;
+  if (visc && (!vol || !vm)) return COSA_ERR_ARG;
   for (int b = 0; b < L.nb; ++b) cons2prim_b(L, b, q, 0, *p);
   int status = bc_level(L, q, si, sj, sk, *p);
   cutman_q_level(L, q);
   status |= prtest_level(L, q, *p);
   if (want_dt) {
-    lambda_level(L, q, si, sj, sk, qp, *p);
-    deltat_level(L, dtvol, qp, bx, by, bz, *p);
+    if (visc) {
+      lambda_ns_level(L, q, si, sj, sk, vol, nullptr, qp, dq, *p);
+      deltat_ns_level(L, dtvol, qp, dq, bx, by, bz, *p);
+    } else {
+      lambda_level(L, q, si, sj, sk, qp, *p);
+      deltat_level(L, dtvol, qp, bx, by, bz, *p);
+    }
   }
   zero_res(L, res);
+  if (visc)
+    for (int b = 0; b < L.nb; ++b) q_bedges(L, b, q, nullptr);
   const double *sd[4] = {nullptr, si, sj, sk};
   for (int d = 1; d <= 3; ++d) {
 #pragma omp parallel for schedule(dynamic)
@@ -1698,6 +2262,17 @@ int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const d
     for (int b = 0; b < L.nb; ++b) roflux_b(L, b, d, qp, qm, flux, sd[d], *p);
 #pragma omp parallel for schedule(dynamic)
     for (int b = 0; b < L.nb; ++b) resid_b(L, b, d, flux, res);
+    if (visc) {
+      // q_face / q_der / vflux / resid (src/cosa.f90:1809-1824)
+      const double *a = vm + (int64_t)(d - 1) * 9 * L.n0;
+#pragma omp parallel for schedule(dynamic)
+      for (int b = 0; b < L.nb; ++b) {
+        q_face_b(L, b, d, q, dq);
+        q_der_b(L, b, d, q, qp, qm, dqm);
+        vflux_b(L, b, d, dq, qp, qm, dqm, a, a + 3 * L.n0, a + 6 * L.n0, sd[d], flux, *p);
+        resid_b(L, b, d, flux, res);
+      }
+    }
   }
 #pragma omp parallel for schedule(dynamic)
   for (int b = 0; b < L.nb; ++b) prim2cons_b(L, b, q, *p);
@@ -1919,4 +2494,77 @@ int orc_mg(orc_level **lv, int nlevel, const cosa_params *p, const cosa_level_pt
   return status;
 }
 
+
+// ---- viscous path ----------------------------------------------------------
+void orc_coordex(orc_level *h, double *x, double *y, double *z) { coordex_level(h->L, x, y, z); }
+void orc_cutman_x(orc_level *h, double *x, double *y, double *z) { cutman_x_level(h->L, x, y, z); }
+void orc_volex(orc_level *h, double *vol) { volex_level(h->L, vol); }
+void orc_cutman_v(orc_level *h, double *vol) { cutman_v_level(h->L, vol); }
+void orc_vmetrix(orc_level *h, const double *x, const double *y, const double *z, const double *vol, double *vm) {
+  for (int d = 1; d <= 3; ++d) {
+    double *a = vm + (int64_t)(d - 1) * 9 * h->L.n0;
+    for (int b = 0; b < h->L.nb; ++b) vmetrix_b(h->L, b, d, x, y, z, vol, a, a + 3 * h->L.n0, a + 6 * h->L.n0);
+  }
+}
+void orc_viscous_setup(orc_level *h, double *x, double *y, double *z, double *vol, double *vm) {
+  viscous_setup_level(h->L, x, y, z, vol, vm);
+}
+void orc_q_face(orc_level *h, int idir, const double *q, double *qf) {
+  for (int b = 0; b < h->L.nb; ++b) q_face_b(h->L, b, idir, q, qf);
+}
+void orc_q_der(orc_level *h, int idir, const double *q, double *dqxi, double *dqeta, double *dqzeta) {
+  for (int b = 0; b < h->L.nb; ++b) q_der_b(h->L, b, idir, q, dqxi, dqeta, dqzeta);
+}
+void orc_vflux(orc_level *h, const cosa_params *p, int idir, const double *qf, const double *dqxi,
+               const double *dqeta, const double *dqzeta, const double *vm, const double *sijk, double *flux) {
+  const double *a = vm + (int64_t)(idir - 1) * 9 * h->L.n0;
+  for (int b = 0; b < h->L.nb; ++b)
+    vflux_b(h->L, b, idir, qf, dqxi, dqeta, dqzeta, a, a + 3 * h->L.n0, a + 6 * h->L.n0, sijk, flux, *p);
+}
+void orc_lambda_ns(orc_level *h, const cosa_params *p, const double *q, const double *si, const double *sj,
+                   const double *sk, const double *vol, const double *mut, double *lam, double *lamv) {
+  lambda_ns_level(h->L, q, si, sj, sk, vol, mut, lam, lamv, *p);
+}
+void orc_deltat_ns(orc_level *h, const cosa_params *p, double *dtvol, const double *lam, const double *lamv,
+                   double *bx, double *by, double *bz) {
+  deltat_ns_level(h->L, dtvol, lam, lamv, bx, by, bz, *p);
+}
+int orc_residual_ns(orc_level *h, const cosa_params *p, int nl, double *q, const double *si, const double *sj,
+                    const double *sk, const double *vol, const double *vm, double *res, double *qp, double *qm,
+                    double *dq, double *dqp, double *dqm, double *flux, double *dtvol, int want_dt, double *bx,
+                    double *by, double *bz) {
+  return residual_impl(h, p, nl, q, si, sj, sk, res, qp, qm, dq, dqp, dqm, flux, dtvol, want_dt, bx, by, bz, vol,
+                       vm);
+}
+/*
+ * Viscous explicit RK driver (smooth() with viscous = .true., one level):
+ * like orc_smooth_irs with the viscous residual; vol and vm come from
+ * orc_viscous_setup.
+ */
+int orc_smooth_ns(orc_level *h, const cosa_params *p, int ncycles, int mgit0, int rms_every, double *q,
+                  double *qold, const double *si, const double *sj, const double *sk, const double *vol,
+                  const double *vm, double *res, double *rhs, double *qp, double *qm, double *dq, double *dqp,
+                  double *dqm, double *flux, double *dtvol, double *bx, double *by, double *bz, double *hist) {
+  Level &L = h->L;
+  int status = 0;
+  const int last = mgit0 + ncycles - 1;
+  for (int mgit = mgit0; mgit <= last; ++mgit) {
+    const int iter = 1;
+    copy_interior(L, qold, q);
+    for (int irk = 1; irk <= p->nstage; ++irk) {
+      const bool want_dt = (iter / p->iupdt * p->iupdt == iter) && irk == 1;
+      status |= residual_impl(h, p, 1, q, si, sj, sk, res, qp, qm, dq, dqp, dqm, flux, dtvol, want_dt, bx, by, bz,
+                              vol, vm);
+      if (status & COSA_ERR_ARG) return status;
+      if (irk == 1 && (mgit == 1 || mgit % rms_every == 0 || mgit == last) && hist) {
+        if (p->harbal) resg_rms_hb_level(L, res, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
+        else resg_rms_level(L, res, rhs, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
+      }
+      if (p->irsop > 0) irs_level(L, res, dtvol, nullptr, bx, by, bz, nullptr, nullptr, nullptr, *p);
+#pragma omp parallel for schedule(dynamic)
+      for (int b = 0; b < L.nb; ++b) update_b(L, b, res, q, qold, dtvol, p->alphas[irk - 1]);
+    }
+  }
+  return status;
+}
 }  // extern "C"

@@ -330,3 +330,86 @@ def mg(levels, arrays, mgit0, ncycles, ncycle, rms_every=1):
     st = lib().orc_mg(hs, C.c_int(n), _par(p), ps, C.c_int(mgit0), C.c_int(ncycles), C.c_int(ncycle),
                       C.c_int(rms_every), _p(hist))
     return hist[:ncycles], st
+
+
+# ---- viscous path ------------------------------------------------------------------
+def vm_alloc(O):
+    """The 9 face inverse-metric arrays (3 x imax x jmax x kmax each) of a level
+    in one buffer: array (d, m) at offset ((d-1)*3 + m) * 3 * n0."""
+    return np.zeros(27 * O.n0)
+
+
+def coordex(O, x, y, z):
+    lib().orc_coordex(O.h, _p(x), _p(y), _p(z))
+
+
+def cutman_x(O, x, y, z):
+    lib().orc_cutman_x(O.h, _p(x), _p(y), _p(z))
+
+
+def volex(O, vol):
+    lib().orc_volex(O.h, _p(vol))
+
+
+def cutman_v(O, vol):
+    lib().orc_cutman_v(O.h, _p(vol))
+
+
+def vmetrix(O, x, y, z, vol, vm):
+    lib().orc_vmetrix(O.h, _p(x), _p(y), _p(z), _p(vol), _p(vm))
+
+
+def viscous_setup(O, x, y, z, vol):
+    """volex + cutman_v + coordex + cutman_x (x, y, z, vol updated in place)
+    and vmetrix; returns vm."""
+    vm = vm_alloc(O)
+    lib().orc_viscous_setup(O.h, _p(x), _p(y), _p(z), _p(vol), _p(vm))
+    return vm
+
+
+def q_face(O, idir, q, qf):
+    lib().orc_q_face(O.h, C.c_int(idir), _p(q), _p(qf))
+
+
+def q_der(O, idir, q, dqxi, dqeta, dqzeta):
+    lib().orc_q_der(O.h, C.c_int(idir), _p(q), _p(dqxi), _p(dqeta), _p(dqzeta))
+
+
+def vflux(O, idir, qf, dqxi, dqeta, dqzeta, vm, sijk, flux):
+    lib().orc_vflux(O.h, _par(O.p), C.c_int(idir), _p(qf), _p(dqxi), _p(dqeta), _p(dqzeta), _p(vm), _p(sijk),
+                    _p(flux))
+
+
+def lambda_ns(O, q, si, sj, sk, vol, lam, lamv, mut=None):
+    lib().orc_lambda_ns(O.h, _par(O.p), _p(q), _p(si), _p(sj), _p(sk), _p(vol), _opt(mut), _p(lam), _p(lamv))
+
+
+def deltat_ns(O, dtvol, lam, lamv, bx=None, by=None, bz=None):
+    lib().orc_deltat_ns(O.h, _par(O.p), _p(dtvol), _p(lam), _p(lamv), _opt(bx), _opt(by), _opt(bz))
+
+
+def residual_ns(O, q, si, sj, sk, vol, vm, nl=1, want_dt=True):
+    """Stage-1 viscous residual; returns (res, dtvol, status), q modified in
+    place as smooth() modifies it."""
+    w = {k: O.p3() for k in ("res", "qp", "qm", "dq", "dqp", "dqm")}
+    flux = O.f0()
+    dtvol = O.p1(O.S)
+    bx, by, bz = (O.p1(O.S) for _ in range(3))
+    st = lib().orc_residual_ns(O.h, _par(O.p), C.c_int(nl), _p(q), _p(si), _p(sj), _p(sk), _p(vol), _p(vm),
+                               _p(w["res"]), _p(w["qp"]), _p(w["qm"]), _p(w["dq"]), _p(w["dqp"]), _p(w["dqm"]),
+                               _p(flux), _p(dtvol), C.c_int(1 if want_dt else 0), _p(bx), _p(by), _p(bz))
+    return w["res"], dtvol, st
+
+
+def smooth_ns(O, q, si, sj, sk, vol, vm, ncycles, mgit0=1, rms_every=1):
+    """Single-level viscous cycles; q updated in place.  Returns (hist, status)."""
+    qold, res, rhs = O.p3(), O.p3(), O.p3()
+    qp, qm, dq, dqp, dqm = (O.p3() for _ in range(5))
+    flux = O.f0()
+    dtvol = O.p1(O.S)
+    bx, by, bz = (O.p1(O.S) for _ in range(3))
+    hist = np.full((ncycles, O.p.npde + 1), np.nan)
+    st = lib().orc_smooth_ns(O.h, _par(O.p), C.c_int(ncycles), C.c_int(mgit0), C.c_int(rms_every), _p(q),
+                             _p(qold), _p(si), _p(sj), _p(sk), _p(vol), _p(vm), _p(res), _p(rhs), _p(qp), _p(qm),
+                             _p(dq), _p(dqp), _p(dqm), _p(flux), _p(dtvol), _p(bx), _p(by), _p(bz), _p(hist))
+    return hist, st
