@@ -15,6 +15,7 @@
 #include "kernels_ref.cuh"
 #include "fused.cuh"
 #include "mg.cuh"
+#include "visc.cuh"
 
 namespace {
 
@@ -48,6 +49,17 @@ struct LevelState {
   int npart_cap = 0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // iteration without / with rms
   long long graph_launches[2] = {0, 0};           // kernels per replay of each graph
+  // viscous terms: strong-boundary faces, cut_x / cut_v copy lists, the
+  // face inverse metrics (caller-owned, bound by cosa_gpu_viscous_setup) and
+  // the per-stage work arrays
+  std::vector<WallFace> walls;
+  WallFace *d_walls = nullptr;
+  CopyItem *d_cutx = nullptr, *d_cutv = nullptr;
+  int ncutx = 0, ncutv = 0;
+  const double *d_vm = nullptr;
+  double *d_qprim = nullptr;  // primitive stage state (P3)
+  double *d_vflux = nullptr;  // viscous face fluxes of the three families (3 x F0)
+  double *d_vres = nullptr;   // viscous flux balance (P3)
 };
 
 }  // namespace
@@ -167,7 +179,9 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
       const int *r = L.bct.data() + L.obct[b] + 10 * ibc;
       const int type = r[0], idir = r[1], inrout = r[2];
       if (idir < 1 || idir > 3) return COSA_ERR_ARG;
-      const bool ok = type == 80 || type == 4 || type == 14 || type == 21 || type == 91 || type == 30;
+      // viscous walls: the laminar, fixed-grid branch of bc_walvis_15
+      const bool wall15 = type / 100 == 15 && c->p.npde == 5 && !c->p.moving;
+      const bool ok = type == 80 || type == 4 || type == 14 || type == 21 || type == 91 || type == 30 || wall15;
       if (!ok) return COSA_ERR_UNSUPPORTED;
       int istrt[4] = {0, r[3], r[5], r[7]}, iend[4] = {0, r[4], r[6], r[8]};
       const int ic2 = cyc3(idir, 2), ic3 = cyc3(idir, 3);
@@ -281,6 +295,103 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
       }
     }
   }
+  // ---- strong-boundary faces of q_face / q_der (src/flux.f90:1884-1962, 2075-2143,
+  // 2256-2324, 2466-2488): patches in table order, a later patch's values
+  // replacing an earlier one's on a shared face
+  L.walls.clear();
+  {
+    std::unordered_map<int64_t, size_t> wpos;
+    for (int b = 0; b < L.nb; ++b) {
+      const DevBlock &x = L.hb[b];
+      const int ijk[4] = {0, x.im, x.jm, x.km};
+      for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
+        const int *r = L.bct.data() + L.obct[b] + 10 * ibc;
+        if (!((r[0] == 13 || r[0] == 14 || r[0] / 100 == 15 || r[0] == 22 || r[0] == 23 || r[0] == 92 ||
+               r[0] == 93 || r[0] == 5)))
+          continue;
+        const int d = r[1], inrout = r[2];
+        const int lo[4] = {0, r[3], r[5], r[7]}, hi[4] = {0, r[4], r[6], r[8]};
+        const int ic2 = cyc3(d, 2), ic3 = cyc3(d, 3);
+        for (int l = 1; l <= 3; ++l)
+          if (l != d && (lo[l] < 1 || hi[l] > ijk[l] - 1 || lo[l] > hi[l])) return COSA_ERR_ARG;
+        if (ijk[d] < 3) return COSA_ERR_ARG;
+        const int iface = inrout == 1 ? 1 : ijk[d];
+        for (int i3 = lo[ic3]; i3 <= hi[ic3]; ++i3)
+          for (int i2 = lo[ic2]; i2 <= hi[ic2]; ++i2) {
+            WallFace w{};
+            w.blk = b; w.d = d; w.inrout = inrout;
+            int pp[4] = {0, 0, 0, 0};
+            pp[d] = iface; pp[ic2] = i2; pp[ic3] = i3;
+            w.fi = pp[1]; w.fj = pp[2]; w.fk = pp[3];
+            for (int l = 1; l <= 3; ++l) { w.lo[l - 1] = lo[l]; w.hi[l - 1] = hi[l]; }
+            const int64_t key = (((int64_t)b * 4 + d) << 40) +
+                                (w.fi + (int64_t)(x.im + 1) * (w.fj + (int64_t)(x.jm + 1) * w.fk));
+            auto f = wpos.find(key);
+            if (f != wpos.end()) L.walls[f->second] = w;
+            else { wpos[key] = L.walls.size(); L.walls.push_back(w); }
+          }
+      }
+    }
+  }
+  // ---- cut_x / cut_v copy lists (src/grid.f90:242-523, 612-700), last writer kept
+  std::vector<CopyItem> cutx, cutv;
+  {
+    std::unordered_map<int64_t, size_t> px, pv;
+    auto put = [](std::vector<CopyItem> &v, std::unordered_map<int64_t, size_t> &pos, CopyItem it) {
+      auto f = pos.find(it.dst);
+      if (f != pos.end()) v[f->second] = it;
+      else { pos[it.dst] = v.size(); v.push_back(it); }
+    };
+    for (int ic = 0; ic < L.ncuts; ++ic) {
+      const int *cc = L.cut.data() + 21 * (int64_t)ic;
+      const int b1 = cc[0] - 1, b2 = cc[9] - 1;
+      const DevBlock &x1 = L.hb[b1], &x2 = L.hb[b2];
+      const int ijk1[4] = {0, x1.im, x1.jm, x1.km}, ijk2[4] = {0, x2.im, x2.jm, x2.km};
+      const int idir1 = cc[1], inout1 = cc[2], idir2 = cc[10], inout2 = cc[11];
+      const int iord[4] = {0, cc[18], cc[19], cc[20]};
+      const int ic1 = cyc3(idir1, 1), ic2 = cyc3(idir1, 2), ic3 = cyc3(idir1, 3);
+      const int jc1 = iord[ic1], jc2 = iord[ic2], jc3 = iord[ic3];
+      if (jc1 < 1 || jc1 > 3 || jc2 < 1 || jc2 > 3 || jc3 < 1 || jc3 > 3) return COSA_ERR_ARG;
+      for (int pass = 0; pass < 2; ++pass) {  // 0: nodes (cut_x), 1: volumes (cut_v)
+        int s1[4] = {0, cc[3], cc[5], cc[7]}, e1[4] = {0, cc[4], cc[6], cc[8]};
+        int s2[4] = {0, cc[12], cc[14], cc[16]}, e2[4] = {0, cc[13], cc[15], cc[17]};
+        int ibcpt, inr;
+        if (pass == 0) {
+          ibcpt = inout1 == 1 ? 0 : ijk1[idir1] + 1;
+          inr = inout2 == 1 ? 2 : ijk2[idir2] - 1;
+          for (int l = 1; l <= 3; ++l)
+            if (l != idir1) { if (e1[l] > s1[l]) e1[l] += 1; else s1[l] += 1; }
+          for (int l = 1; l <= 3; ++l)
+            if (l != idir2) { if (e2[l] > s2[l]) e2[l] += 1; else s2[l] += 1; }
+        } else {
+          ibcpt = inout1 == 1 ? 0 : ijk1[idir1];
+          inr = inout2 == 1 ? 1 : ijk2[idir2] - 1;
+        }
+        int len[4], g1[4], g2[4];
+        for (int l = 1; l <= 3; ++l) {
+          len[l] = std::abs(e1[l] - s1[l]);
+          g1[l] = e1[l] > s1[l] ? 1 : -1;
+          g2[l] = e2[l] > s2[l] ? 1 : -1;
+        }
+        const int top = pass == 0 ? 1 : 0;  // nodes 0..ijk+1, volumes 0..ijk
+        for (int i3 = 0; i3 <= len[ic3]; ++i3)
+          for (int i2 = 0; i2 <= len[ic2]; ++i2) {
+            int p1[4] = {0, 0, 0, 0}, p2[4] = {0, 0, 0, 0};
+            p1[ic1] = ibcpt; p1[ic2] = s1[ic2] + g1[ic2] * i2; p1[ic3] = s1[ic3] + g1[ic3] * i3;
+            p2[jc1] = inr; p2[jc2] = s2[jc2] + g2[jc2] * i2; p2[jc3] = s2[jc3] + g2[jc3] * i3;
+            for (int l = 1; l <= 3; ++l)
+              if (p1[l] < 0 || p1[l] > ijk1[l] + top || p2[l] < 0 || p2[l] > ijk2[l] + top) return COSA_ERR_ARG;
+            if (pass == 0)
+              put(cutx, px, CopyItem{g2_idx(x1, p1[1], p1[2], p1[3]), g2_idx(x2, p2[1], p2[2], p2[3])});
+            else
+              put(cutv, pv, CopyItem{p1_idx(x1, 1, p1[1], p1[2], p1[3], 0), p1_idx(x2, 1, p2[1], p2[2], p2[3], 0)});
+          }
+      }
+    }
+  }
+  L.ncutx = (int)cutx.size();
+  L.ncutv = (int)cutv.size();
+
   // ---- tiles of the fused stage kernel
   std::vector<Tile> tiles;
   const int S = 2 * c->p.nharms + 1;
@@ -312,6 +423,13 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
   if (!flags.empty()) CK(cudaMemcpy(L.d_strong, flags.data(), flags.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(L.d_smap, smap.data(), smap.size() * sizeof(StrongMap), cudaMemcpyHostToDevice));
   if (!tiles.empty()) CK(cudaMemcpy(L.d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  if ((r = dalloc(c, &L.d_walls, std::max<size_t>(L.walls.size(), 1)))) return r;
+  if ((r = dalloc(c, &L.d_cutx, std::max<size_t>(cutx.size(), 1)))) return r;
+  if ((r = dalloc(c, &L.d_cutv, std::max<size_t>(cutv.size(), 1)))) return r;
+  if (!L.walls.empty())
+    CK(cudaMemcpy(L.d_walls, L.walls.data(), L.walls.size() * sizeof(WallFace), cudaMemcpyHostToDevice));
+  if (!cutx.empty()) CK(cudaMemcpy(L.d_cutx, cutx.data(), cutx.size() * sizeof(CopyItem), cudaMemcpyHostToDevice));
+  if (!cutv.empty()) CK(cudaMemcpy(L.d_cutv, cutv.data(), cutv.size() * sizeof(CopyItem), cudaMemcpyHostToDevice));
   return COSA_OK;
 }
 
@@ -357,7 +475,7 @@ int set_smem_attrs() {
 }
 
 int check_fused_supported(const cosa_params &p) {
-  if (p.npde != 5 || p.viscous || p.kom || p.kom_bsl || p.kom_sst || p.rkimp || p.moving ||
+  if (p.npde != 5 || p.kom || p.kom_bsl || p.kom_sst || p.rkimp || p.moving ||
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
   return COSA_OK;
@@ -379,6 +497,8 @@ int check_thin_blocks(const cosa_ctx *c, int nl) {
     const int nc[4] = {0, x.im - 1, x.jm - 1, x.km - 1};
     for (int d = 1; d <= 3; ++d) {
       if (nc[d] > 1) continue;
+      // the viscous face stencils and q_edges read across such a block too
+      if (c->p.viscous) return COSA_ERR_UNSUPPORTED;
       if (nl < c->p.nl_crs) return COSA_ERR_UNSUPPORTED;
       for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
         const int *r = L.bct.data() + L.obct[b] + 10 * ibc;
@@ -473,6 +593,48 @@ void prof_stop(cosa_ctx *c, int k) {
   c->prof.n[k] += 1;
 }
 
+int launch_edges(cosa_ctx *c, LevelState &L, double *q, double *mut);
+
+// x extent of a (x, nblocks[, 3]) grid covering `n` items per block
+int grid_x(int64_t n, int nb) {
+  const int64_t g = (n + 255) / 256;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, std::max(148 * 16 / std::max(nb, 1), 148)));
+}
+
+// viscous part of one stage on the halo-filled state qin: primitive copy,
+// q_edges, [time step], face fluxes, wall faces, flux balance -> L.d_vres
+int launch_visc(cosa_ctx *c, LevelState &L, const double *qin, bool dt, double *bx, double *by, double *bz) {
+  const cosa_params &p = c->p;
+  const int S = 2 * p.nharms + 1;
+  int64_t m3 = 0, mc = 0, mf = 0;
+  for (const DevBlock &x : L.hb) {
+    m3 = std::max<int64_t>(m3, x.P3 * S);
+    mc = std::max<int64_t>(mc, (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * S);
+    mf = std::max<int64_t>(mf, (int64_t)x.im * x.jm * x.km * S);
+  }
+  k_prim<<<dim3(grid_x(m3, L.nb), L.nb), 256, 0, c->s>>>(L.d_blocks, c->d_p, qin, L.d_qprim);
+  int r = after_launch(c);
+  if (r) return r;
+  if ((r = launch_edges(c, L, L.d_qprim, nullptr))) return r;
+  const cosa_level_ptrs &P = L.ptrs;
+  if (dt) {
+    k_dt_ns<<<dim3(grid_x(mc, L.nb), L.nb), 256, 0, c->s>>>(L.d_blocks, c->d_p, L.d_qprim, P.si, P.sj, P.sk, P.vol,
+                                                            P.dtvol, bx, by, bz);
+    if ((r = after_launch(c))) return r;
+  }
+  k_vface<<<dim3(grid_x(mf, L.nb), L.nb, 3), 256, 0, c->s>>>(L.d_blocks, c->d_p, L.d_qprim, P.si, P.sj, P.sk, L.d_vm,
+                                                             L.n0, L.d_vflux);
+  if ((r = after_launch(c))) return r;
+  if (!L.walls.empty()) {
+    const int nw = (int)L.walls.size();
+    k_vwall<<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L.d_blocks, L.d_walls, nw, c->d_p, L.d_qprim, P.si, P.sj,
+                                                         P.sk, L.d_vm, L.n0, L.d_vflux);
+    if ((r = after_launch(c))) return r;
+  }
+  k_vdiv<<<dim3(grid_x(mc, L.nb), L.nb), 256, 0, c->s>>>(L.d_blocks, c->d_p, L.d_vflux, L.n0, L.d_vres);
+  return after_launch(c);
+}
+
 // one stage: halo fill + tile kernel (+ norm reduction)
 int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, const double *qold,
                  double *qold_copy, int irk, int compute_dt, bool want_rms, int update, double *res_out,
@@ -506,6 +668,15 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   A.ar = p.alphas[irk - 1];
   A.vol = p.harbal ? P.vol : nullptr;
   A.compute_dt = compute_dt;
+  if (p.viscous) {
+    // the viscous terms and, on stage 1, the viscous time step come first
+    if (!L.d_vm || !L.d_vres || !P.vol) return COSA_ERR_ARG;
+    int r = launch_visc(c, L, qin, compute_dt != 0, A.bx, A.by, A.bz);
+    if (r) return r;
+    A.vres = L.d_vres;
+    A.compute_dt = 0;
+    A.bx = A.by = A.bz = nullptr;
+  }
   A.first_order = nl >= p.nl_crs;
   A.update = update;
   const size_t smem = stage_smem_bytes<kTI, kTJ>();
@@ -928,6 +1099,7 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
   const cosa_level_ptrs &P = L->ptrs;
   if (!P.q || !P.qold || !P.dtvol || !P.si || !P.sj || !P.sk) return COSA_ERR_ARG;
   if (c->p.harbal && !P.vol) return COSA_ERR_ARG;
+  if (c->p.viscous && (!P.vol || !L->d_vm)) return COSA_ERR_ARG;
   cudaSetDevice(c->device);
   const int npde = c->p.npde;
   // schedule of printed iterations (src/cosa.f90:1925-1927)
@@ -1256,7 +1428,8 @@ int check_mg_levels(cosa_ctx *c, int nlevel) {
     if (!L || !L->bound) return COSA_ERR_ARG;
     const cosa_level_ptrs &P = L->ptrs;
     if (!P.q || !P.qold || !P.dtvol || !P.si || !P.sj || !P.sk) return COSA_ERR_ARG;
-    if ((c->p.harbal || nlevel > 1) && !P.vol) return COSA_ERR_ARG;
+    if ((c->p.harbal || nlevel > 1 || c->p.viscous) && !P.vol) return COSA_ERR_ARG;
+    if (c->p.viscous && !L->d_vm) return COSA_ERR_ARG;  // cosa_gpu_viscous_setup on every level
     if (nl < nlevel && !P.res) return COSA_ERR_ARG;
     if (nl > 1 && !P.rhs) return COSA_ERR_ARG;
     if (nl < nlevel) {
@@ -1578,5 +1751,161 @@ extern "C" int cosa_gpu_resg_rms_noalloc(int32_t nblocks, const int32_t *dims, i
   if (cudaGetLastError() != cudaSuccess) return COSA_ERR_CUDA;
   return COSA_OK;
 }
+
+// ---- laminar viscous path ---------------------------------------------------------------
+extern "C" {
+
+int cosa_gpu_coordex(cosa_ctx *c, int32_t nl, double *x, double *y, double *z) {
+  LevelState *L = level(c, nl);
+  if (!L || !x || !y || !z) return COSA_ERR_ARG;
+  for (const DevBlock &b : L->hb) {
+    const int64_t n = 2 * ((int64_t)b.im * b.km + (int64_t)b.jm * b.km + (int64_t)b.im * b.jm);
+    k_coordex<<<grid_for(n), 256, 0, c->s>>>(b, x, y, z);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_cutman_x(cosa_ctx *c, int32_t nl, double *x, double *y, double *z) {
+  LevelState *L = level(c, nl);
+  if (!L || !x || !y || !z) return COSA_ERR_ARG;
+  if (L->ncutx == 0) return COSA_OK;
+  k_copy_list<<<grid_for(L->ncutx), 256, 0, c->s>>>(L->d_cutx, L->ncutx, x, y, z);
+  return after_launch(c);
+}
+
+int cosa_gpu_volex(cosa_ctx *c, int32_t nl, double *vol) {
+  LevelState *L = level(c, nl);
+  if (!L || !vol) return COSA_ERR_ARG;
+  for (const DevBlock &b : L->hb) {
+    const int64_t n = 2 * ((int64_t)(b.im - 1) * (b.km - 1) + (int64_t)(b.jm - 1) * (b.km - 1) +
+                           (int64_t)(b.im - 1) * (b.jm - 1));
+    k_volex<<<grid_for(n), 256, 0, c->s>>>(b, vol);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_cutman_v(cosa_ctx *c, int32_t nl, double *vol) {
+  LevelState *L = level(c, nl);
+  if (!L || !vol) return COSA_ERR_ARG;
+  if (L->ncutv == 0) return COSA_OK;
+  k_copy_list<<<grid_for(L->ncutv), 256, 0, c->s>>>(L->d_cutv, L->ncutv, vol, nullptr, nullptr);
+  return after_launch(c);
+}
+
+int cosa_gpu_vmetrix(cosa_ctx *c, int32_t nl, const double *x, const double *y, const double *z, const double *vol,
+                     double *vm) {
+  LevelState *L = level(c, nl);
+  if (!L || !x || !y || !z || !vol || !vm) return COSA_ERR_ARG;
+  if (c->p.moving) return COSA_ERR_UNSUPPORTED;
+  for (const DevBlock &b : L->hb)
+    for (int d = 1; d <= 3; ++d) {
+      k_vmetrix<<<grid_for((int64_t)b.im * b.jm * b.km), 256, 0, c->s>>>(b, d, x, y, z, vol, vm, L->n0);
+      int r = after_launch(c);
+      if (r) return r;
+    }
+  return COSA_OK;
+}
+
+int cosa_gpu_viscous_setup(cosa_ctx *c, int32_t nl, double *x, double *y, double *z, double *vol, double *vm) {
+  LevelState *L = level(c, nl);
+  if (!L || !x || !y || !z || !vol || !vm) return COSA_ERR_ARG;
+  int r = 0;
+  if ((r = cosa_gpu_volex(c, nl, vol)) || (r = cosa_gpu_cutman_v(c, nl, vol)) || (r = cosa_gpu_coordex(c, nl, x, y, z)) ||
+      (r = cosa_gpu_cutman_x(c, nl, x, y, z)) || (r = cosa_gpu_vmetrix(c, nl, x, y, z, vol, vm)))
+    return r;
+  const int S = 2 * c->p.nharms + 1;
+  const size_t n3 = (size_t)L->n3 * 5 * S;
+  if (!L->d_qprim && (r = dalloc(c, &L->d_qprim, n3))) return r;
+  if (!L->d_vres && (r = dalloc(c, &L->d_vres, n3))) return r;
+  if (!L->d_vflux && (r = dalloc(c, &L->d_vflux, (size_t)3 * L->n0 * 5 * S))) return r;
+  CK(cudaMemsetAsync(L->d_qprim, 0, n3 * sizeof(double), c->s));
+  CK(cudaMemsetAsync(L->d_vres, 0, n3 * sizeof(double), c->s));
+  CK(cudaMemsetAsync(L->d_vflux, 0, (size_t)3 * L->n0 * 5 * S * sizeof(double), c->s));
+  L->d_vm = vm;
+  drop_graphs(c);
+  return COSA_OK;
+}
+
+int cosa_gpu_q_face(cosa_ctx *c, int32_t idir, int32_t nl, const double *q, double *qf) {
+  LevelState *L = level(c, nl);
+  if (!L || idir < 1 || idir > 3 || !q || !qf) return COSA_ERR_ARG;
+  if (c->p.npde != 5) return COSA_ERR_UNSUPPORTED;
+  const int S = 2 * c->p.nharms + 1;
+  for (const DevBlock &b : L->hb) {
+    const int g = grid_for((int64_t)b.im * b.jm * b.km * S);
+    if (idir == 1) k_qface_qder<1><<<g, 256, 0, c->s>>>(b, S, q, qf, nullptr, nullptr, nullptr);
+    else if (idir == 2) k_qface_qder<2><<<g, 256, 0, c->s>>>(b, S, q, qf, nullptr, nullptr, nullptr);
+    else k_qface_qder<3><<<g, 256, 0, c->s>>>(b, S, q, qf, nullptr, nullptr, nullptr);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  if (L->walls.empty()) return COSA_OK;
+  const int nw = (int)L->walls.size();
+  k_qwall<<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L->d_blocks, L->d_walls, nw, idir, S, q, qf, nullptr, nullptr,
+                                                       nullptr);
+  return after_launch(c);
+}
+
+int cosa_gpu_q_der(cosa_ctx *c, int32_t idir, int32_t nl, const double *q, double *dqxi, double *dqeta,
+                   double *dqzeta) {
+  LevelState *L = level(c, nl);
+  if (!L || idir < 1 || idir > 3 || !q || !dqxi || !dqeta || !dqzeta) return COSA_ERR_ARG;
+  if (c->p.npde != 5) return COSA_ERR_UNSUPPORTED;
+  const int S = 2 * c->p.nharms + 1;
+  for (const DevBlock &b : L->hb) {
+    const int g = grid_for((int64_t)b.im * b.jm * b.km * S);
+    if (idir == 1) k_qface_qder<1><<<g, 256, 0, c->s>>>(b, S, q, nullptr, dqxi, dqeta, dqzeta);
+    else if (idir == 2) k_qface_qder<2><<<g, 256, 0, c->s>>>(b, S, q, nullptr, dqxi, dqeta, dqzeta);
+    else k_qface_qder<3><<<g, 256, 0, c->s>>>(b, S, q, nullptr, dqxi, dqeta, dqzeta);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  if (L->walls.empty()) return COSA_OK;
+  const int nw = (int)L->walls.size();
+  k_qwall<<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L->d_blocks, L->d_walls, nw, idir, S, q, nullptr, dqxi, dqeta,
+                                                       dqzeta);
+  return after_launch(c);
+}
+
+int cosa_gpu_vflux(cosa_ctx *c, int32_t idir, int32_t nl, const double *qf, const double *dqxi, const double *dqeta,
+                   const double *dqzeta, const double *vm, const double *sijk, double *flux) {
+  LevelState *L = level(c, nl);
+  if (!L || idir < 1 || idir > 3 || !qf || !dqxi || !dqeta || !dqzeta || !vm || !sijk || !flux) return COSA_ERR_ARG;
+  if (c->p.npde != 5 || c->p.moving) return COSA_ERR_UNSUPPORTED;
+  const int S = 2 * c->p.nharms + 1;
+  for (const DevBlock &b : L->hb) {
+    k_vflux_ref<<<grid_for((int64_t)b.im * b.jm * b.km * S), 256, 0, c->s>>>(b, idir, c->d_p, qf, dqxi, dqeta, dqzeta,
+                                                                            vm, L->n0, sijk, flux);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_lambda_ns(cosa_ctx *c, int32_t nl, const double *q, const double *si, const double *sj, const double *sk,
+                       const double *vol, double *lam, double *lamv) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !si || !sj || !sk || !vol || !lam || !lamv) return COSA_ERR_ARG;
+  if (c->p.npde != 5 || c->p.moving) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+    k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, vol, lam, lamv);
+  });
+}
+
+int cosa_gpu_deltat_ns(cosa_ctx *c, int32_t nl, double *dtvol, const double *lam, const double *lamv, double *bx,
+                       double *by, double *bz) {
+  LevelState *L = level(c, nl);
+  if (!L || !dtvol || !lam || !lamv) return COSA_ERR_ARG;
+  if (c->p.npde != 5) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+    k_deltat_ns<<<g, 256, 0, c->s>>>(b, c->d_p, dtvol, lam, lamv, bx, by, bz);
+  });
+}
+
+}  // extern "C"
 
 #include "serve.cuh"

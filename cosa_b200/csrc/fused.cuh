@@ -104,7 +104,10 @@ __global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__re
         case 21: mask = bc_insub(B, nx, ny, nz, c1, c2, h1, h2, &err); break;
         case 91: mask = bc_outsub(B, c1, c2, h1, h2); break;
         case 30: mask = bc_far0(B, nx, ny, nz, c1, h1, h2); break;
-        default: st |= COSA_ERR_UNSUPPORTED; break;
+        default:
+          if (it.type / 100 == 15) mask = bc_walvis(P.gamma, c1, c2, h1, h2);
+          else st |= COSA_ERR_UNSUPPORTED;
+          break;
       }
       if (err) st |= COSA_ERR_INFLOW;
     }
@@ -136,6 +139,7 @@ struct StageArgs {
   double *res_out;       // if set, the residual is stored here (P3 layout)
   double *bx, *by, *bz;  // IRS coefficients written with the time step (irsop >= 2)
   const double *vol;     // cell volumes when the harmonic-balance source is on
+  const double *vres;    // viscous flux balance of each cell (P3 layout), added to the residual, or null
   const uint8_t *strong; // strong-boundary flags
   const StrongMap *smap; // per block
   int *status;
@@ -385,6 +389,8 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
         double r = fi[(m * TJ + tj) * (TI + 1) + ti + 1] - fi[(m * TJ + tj) * (TI + 1) + ti];
         r = r + fj[(m * (TJ + 1) + tj + 1) * TI + ti] - fj[(m * (TJ + 1) + tj) * TI + ti];
         r = r + fk_hi[m] - fk_lo[m];
+        // viscous terms (q_face/q_der/vflux/resid, src/cosa.f90:1809-1876)
+        if (A.vres) r = r + A.vres[p3_var(b, npde, S, m + 1, n) + cell];
         if (A.vol) {
           // src_bhb (src/src.f90:556-613): harmonic-balance coupling of the snapshots
           const double ov = P.omega * A.vol[p1_idx(b, 1, ci, cj, k, 0)];

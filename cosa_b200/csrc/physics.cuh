@@ -602,6 +602,19 @@ __device__ __forceinline__ int bc_far0(const BcPar &B, double sx, double sy, dou
   return mask;
 }
 
+// bc_walvis_15, laminar part on a fixed grid (src/bc.f90:2144-2300): no-slip
+// wall; wall pressure extrapolated linearly from the first two cells, wall
+// density from cell 1 along the isentrope; both halo layers take the wall state
+__device__ __forceinline__ int bc_walvis(double g, const double *c1, const double *c2, double *h1, double *h2) {
+  const double p1 = c1[4], p2 = c2[4];
+  const double pw = 0.5 * (3 * p1 - p2);
+  h1[0] = pow(pw / p1, 1 / g) * c1[0];
+  h1[1] = 0.0; h1[2] = 0.0; h1[3] = 0.0;
+  h1[4] = pw;
+  for (int v = 0; v < 5; ++v) h2[v] = h1[v];
+  return 3;
+}
+
 __device__ __forceinline__ bool strong_bc(int t) {
   return t == 13 || t == 14 || t / 100 == 15 || t == 22 || t == 23 || t == 92 || t == 93 || t == 5;
 }

@@ -295,7 +295,7 @@ extern "C" {
 int cosa_serve_create(const cosa_params *scheme, int64_t budget_bytes, int32_t device, int32_t check_every,
                       cosa_serve **out) {
   if (!scheme || !out || budget_bytes < kSlotBytes || check_every < 1) return COSA_ERR_ARG;
-  if (scheme->npde != 5 || scheme->nharms != 0 || scheme->irsop != 0 || scheme->iupdt != 1)
+  if (scheme->npde != 5 || scheme->nharms != 0 || scheme->irsop != 0 || scheme->iupdt != 1 || scheme->viscous)
     return COSA_ERR_UNSUPPORTED;
   int r = check_fused_supported(*scheme);
   if (r) return r;

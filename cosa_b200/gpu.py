@@ -58,7 +58,9 @@ SYMBOLS = [
     "cosa_gpu_rest1", "cosa_gpu_rest2", "cosa_gpu_prol_bln", "cosa_gpu_prol_lin", "cosa_gpu_restrict",
     "cosa_gpu_prolong", "cosa_gpu_smooth_level", "cosa_gpu_mg", "cosa_gpu_nr_selftest",
     "cosa_serve_create", "cosa_serve_destroy", "cosa_serve_submit", "cosa_serve_step", "cosa_serve_result",
-    "cosa_serve_free_slots",
+    "cosa_serve_free_slots", "cosa_gpu_coordex", "cosa_gpu_cutman_x", "cosa_gpu_volex", "cosa_gpu_cutman_v",
+    "cosa_gpu_vmetrix", "cosa_gpu_viscous_setup", "cosa_gpu_q_face", "cosa_gpu_q_der", "cosa_gpu_vflux",
+    "cosa_gpu_lambda_ns", "cosa_gpu_deltat_ns",
 ]
 
 
@@ -285,6 +287,51 @@ class Context:
         st = load().cosa_gpu_smooth(self.h, nl, niter, mgit0, rms_every,
                                     hist.ctypes.data_as(_dp) if want_hist else _dp())
         return (hist[:niter] if want_hist else None), st
+
+    # ---- laminar viscous terms -------------------------------------------------------
+    def alloc_vm(self, nl=1):
+        """The nine face inverse-metric arrays of level nl (27 * n0 doubles)."""
+        return DevArray(self, self.sizes(nl)[3] * 27)
+
+    def coordex(self, nl, x, y, z):
+        self._check(load().cosa_gpu_coordex(self.h, nl, _ptr(x.ptr), _ptr(y.ptr), _ptr(z.ptr)), "coordex")
+
+    def cutman_x(self, nl, x, y, z):
+        self._check(load().cosa_gpu_cutman_x(self.h, nl, _ptr(x.ptr), _ptr(y.ptr), _ptr(z.ptr)), "cutman_x")
+
+    def volex(self, nl, vol):
+        self._check(load().cosa_gpu_volex(self.h, nl, _ptr(vol.ptr)), "volex")
+
+    def cutman_v(self, nl, vol):
+        self._check(load().cosa_gpu_cutman_v(self.h, nl, _ptr(vol.ptr)), "cutman_v")
+
+    def vmetrix(self, nl, x, y, z, vol, vm):
+        self._check(load().cosa_gpu_vmetrix(self.h, nl, _ptr(x.ptr), _ptr(y.ptr), _ptr(z.ptr), _ptr(vol.ptr),
+                                            _ptr(vm.ptr)), "vmetrix")
+
+    def viscous_setup(self, nl, x, y, z, vol, vm):
+        self._check(load().cosa_gpu_viscous_setup(self.h, nl, _ptr(x.ptr), _ptr(y.ptr), _ptr(z.ptr), _ptr(vol.ptr),
+                                                  _ptr(vm.ptr)), "viscous_setup")
+
+    def q_face(self, idir, nl, q, qf):
+        self._check(load().cosa_gpu_q_face(self.h, idir, nl, _ptr(q.ptr), _ptr(qf.ptr)), "q_face")
+
+    def q_der(self, idir, nl, q, dqxi, dqeta, dqzeta):
+        self._check(load().cosa_gpu_q_der(self.h, idir, nl, _ptr(q.ptr), _ptr(dqxi.ptr), _ptr(dqeta.ptr),
+                                          _ptr(dqzeta.ptr)), "q_der")
+
+    def vflux(self, idir, nl, qf, dqxi, dqeta, dqzeta, vm, sijk, flux):
+        self._check(load().cosa_gpu_vflux(self.h, idir, nl, _ptr(qf.ptr), _ptr(dqxi.ptr), _ptr(dqeta.ptr),
+                                          _ptr(dqzeta.ptr), _ptr(vm.ptr), _ptr(sijk.ptr), _ptr(flux.ptr)), "vflux")
+
+    def lambda_ns(self, nl, q, si, sj, sk, vol, lam, lamv):
+        self._check(load().cosa_gpu_lambda_ns(self.h, nl, _ptr(q.ptr), _ptr(si.ptr), _ptr(sj.ptr), _ptr(sk.ptr),
+                                              _ptr(vol.ptr), _ptr(lam.ptr), _ptr(lamv.ptr)), "lambda_ns")
+
+    def deltat_ns(self, nl, dtvol, lam, lamv, bx=None, by=None, bz=None):
+        self._check(load().cosa_gpu_deltat_ns(self.h, nl, _ptr(dtvol.ptr), _ptr(lam.ptr), _ptr(lamv.ptr),
+                                              _ptr(bx.ptr if bx else None), _ptr(by.ptr if by else None),
+                                              _ptr(bz.ptr if bz else None)), "deltat_ns")
 
     # ---- multigrid ---------------------------------------------------------------
     def q_edges(self, nl, q, mut=None):

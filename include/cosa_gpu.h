@@ -257,6 +257,57 @@ int cosa_gpu_restrict(cosa_ctx *ctx, int32_t nl);
    lim_corr 1 and 3 */
 int cosa_gpu_prolong(cosa_ctx *ctx, int32_t nl);
 
+/* ---- laminar viscous terms (viscous = .true., no turbulence model, fixed
+   grid); q in primitive form where the reference has it so ---- */
+/* coordex (src/grid.f90:2-80): ghost nodes 0 and imax+1 (j, k alike)
+   repeat the boundary nodes; x, y, z are node arrays of cosa_level_desc's
+   P2 extent (no lmet factor) */
+int cosa_gpu_coordex(cosa_ctx *ctx, int32_t nl, double *x, double *y, double *z);
+/* cutman_x / cut_x (src/grid.f90:242-523): ghost nodes of cut faces from
+   the neighbour block's nodes one plane inside */
+int cosa_gpu_cutman_x(cosa_ctx *ctx, int32_t nl, double *x, double *y, double *z);
+/* volex (src/grid.f90:83-136): face-halo volumes repeat the first cell */
+int cosa_gpu_volex(cosa_ctx *ctx, int32_t nl, double *vol);
+/* cutman_v / cut_v (src/grid.f90:612-700): cut-face halo volumes from the
+   neighbour block */
+int cosa_gpu_cutman_v(cosa_ctx *ctx, int32_t nl, double *vol);
+/* vmetrix (src/grid.f90:3118-3582): face inverse metrics.  vm holds the
+   reference's nine arrays xideri, etaderi, zetaderi, xiderj, ... zetaderk,
+   each (3, imax, jmax, kmax) per block at offset off_0*3 of a 3*n0 slab:
+   array (d, m) (d = face family 1..3, m = 0 xi, 1 eta, 2 zeta) starts at
+   ((d-1)*3 + m)*3*n0, n0 = sizes[3] of cosa_gpu_level_sizes */
+int cosa_gpu_vmetrix(cosa_ctx *ctx, int32_t nl, const double *x, const double *y,
+                     const double *z, const double *vol, double *vm);
+/* the viscous start-up of the solver (src/cosa.f90:300-322): volex,
+   cutman_v, coordex, cutman_x, vmetrix; binds vm (27*n0 doubles, kept by
+   the caller) to level nl for cosa_gpu_smooth / smooth_level / mg */
+int cosa_gpu_viscous_setup(cosa_ctx *ctx, int32_t nl, double *x, double *y, double *z,
+                           double *vol, double *vm);
+/* q_face (src/flux.f90:2391-2801), calmut = .false.: face averages of the
+   primitive state, the halo (wall) value on strong-boundary faces; qf P3 */
+int cosa_gpu_q_face(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *q, double *qf);
+/* q_der (src/flux.f90:1813-2390): face gradients along xi, eta, zeta (P3
+   each), one-sided three-point normal derivative and tangential
+   derivatives along the halo line on strong-boundary faces */
+int cosa_gpu_q_der(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *q, double *dqxi,
+                   double *dqeta, double *dqzeta);
+/* vflux (src/flux.f90:831-1180), laminar: flux = viscous face flux (F0) of
+   face family idir with the family's metrics sijk and vm as above */
+int cosa_gpu_vflux(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *qf, const double *dqxi,
+                   const double *dqeta, const double *dqzeta, const double *vm,
+                   const double *sijk, double *flux);
+/* lambda with viscous = .true. (src/cosa.f90:1349-1423, eig_ns
+   4239-4297): lam(.,1:3) convective and lamv(.,1:3) viscous spectral radii
+   (P3 layout, q primitive with halos) */
+int cosa_gpu_lambda_ns(cosa_ctx *ctx, int32_t nl, const double *q, const double *si,
+                       const double *sj, const double *sk, const double *vol, double *lam,
+                       double *lamv);
+/* deltat with viscous = .true. (src/cosa.f90:4831-5180): dtvol with the
+   viscous radii (irsop other than 5, 6), IRS coefficients with the viscous
+   floor for irsop 5 and 6 */
+int cosa_gpu_deltat_ns(cosa_ctx *ctx, int32_t nl, double *dtvol, const double *lam,
+                       const double *lamv, double *bx, double *by, double *bz);
+
 /* ---- fused: what smooth() calls when the GPU path is on ---- */
 /*
  * One RK iteration sequence of smooth() (src/cosa.f90:1711-2029) on the
