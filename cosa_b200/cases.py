@@ -138,6 +138,10 @@ def _freestream_state(tables: LevelTables, p: CosaParams) -> np.ndarray:
         v[..., 2, :] = p.rhoinf * p.machfs * sa * cb
         v[..., 3, :] = p.rhoinf * p.machfs * sb
         v[..., 4, :] = 1 / p.rhoinf / p.gamma / (p.gamma - 1) + 0.5 * p.machfs ** 2
+        if p.kom:
+            # interior cells only (src/input.f90:4826-4836)
+            v[2:-2, 2:-2, 2:-2, 5, :] = p.rhoinf * p.tkefar
+            v[2:-2, 2:-2, 2:-2, 6, :] = p.rhoinf * p.omefar
     return q
 
 
@@ -343,6 +347,87 @@ def partitioned_laminar_channel(ni: int = 48, nj: int = 24, nk: int = 2, isplit=
     with permuted indices), z faces extrapolated."""
     return partitioned_channel(ni, nj, nk, isplit, jsplit, permute_last, mach, kface_bc=4, wall=VISCOUS_WALL,
                                params=laminar_params(mach, reyno))
+
+
+# ---- turbulent channel: Wilcox k-omega on the bump channel with viscous walls ---------
+def kom_params(mach: float = 0.3, reyno: float = 1.0e5, tu2: float = 1.0e-6, mutfar: float = 1.0,
+               wall: str = "menter", roughk: float = 0.0) -> CosaParams:
+    """laminar_params plus the Wilcox k-omega model (npde = 7): far-field
+    k and omega from the turbulence intensity squared tu2 and the viscosity
+    ratio mutfar (src/input.f90:2696-2720), omega wall value after Menter
+    or Wilcox (rough wall, roughk)."""
+    p = laminar_params(mach, reyno)
+    p.npde = 7
+    p.kom = 1
+    p.mutfar = mutfar
+    p.tkefar = tu2 * mach ** 2
+    p.omefar = p.cmu * p.rhoinf * p.tkefar / mutfar * p.reyno / p.machfs
+    p.wallwilc = 1 if wall == "wilcox" else 0
+    p.roughk = roughk
+    p.turcmp = 1.0
+    p.lim_prodtke = 0
+    p.lim_prodomega = 0
+    p.prdlim = 20.0
+    p.ifixq = 1
+    p.cflt = p.cfl
+    p.ratt = p.rat
+    return p
+
+
+def turbulent_channel(ni: int = 48, nj: int = 24, nk: int = 2, mach: float = 0.3, reyno: float = 1.0e5,
+                      wall: str = "menter", kface_bc: int = 80) -> Case:
+    """laminar_channel with the k-omega model (npde = 7)."""
+    X, Y, Z = channel_nodes(ni, nj, nk)
+    spec = BlockSpec(ni + 1, nj + 1, nk + 1, _face_bcs(ni + 1, nj + 1, nk + 1, {
+        "imin": 21, "imax": 91, "jmin": VISCOUS_WALL, "jmax": VISCOUS_WALL, "kmin": kface_bc, "kmax": kface_bc}))
+    return _assemble(f"turbulent_channel_{ni}x{nj}x{nk}", [(X, Y, Z)], [spec], [],
+                     kom_params(mach, reyno, wall=wall))
+
+
+def partitioned_turbulent_channel(ni: int = 48, nj: int = 24, nk: int = 2, isplit=(20,), jsplit=(10,),
+                                  permute_last: bool = True, mach: float = 0.3, reyno: float = 1.0e5,
+                                  wall: str = "menter") -> Case:
+    return partitioned_channel(ni, nj, nk, isplit, jsplit, permute_last, mach, kface_bc=4, wall=VISCOUS_WALL,
+                               params=kom_params(mach, reyno, wall=wall))
+
+
+def wall_distance(case: Case) -> np.ndarray:
+    """Wall distance of every cell (P1 array): the distance of each grid
+    node to the nearest node of a viscous-wall (15xx) patch, averaged over
+    the cell's eight nodes; halo cells repeat their neighbour.  Stands in for
+    the solver's set-up routine dist2wall (outside the hot path) in the test
+    cases."""
+    t = case.tables
+    gx, gy, gz = (p2_views(t, a) for a in (case.x, case.y, case.z))
+    walls = []
+    rows = t.bctopo
+    ob = np.concatenate([[0], np.cumsum(t.nbcs)[:-1]])
+    for b, (im, jm, km) in enumerate(t.dims):
+        for r in rows[ob[b]:ob[b] + t.nbcs[b]]:
+            if r[0] // 100 != 15:
+                continue
+            d, inrout = r[1], r[2]
+            sl = [slice(r[3], r[4] + 2), slice(r[5], r[6] + 2), slice(r[7], r[8] + 2)]
+            sl[d - 1] = slice(1, 2) if inrout == 1 else slice((im, jm, km)[d - 1], (im, jm, km)[d - 1] + 1)
+            walls.append(np.stack([gx[b][tuple(sl)].ravel(), gy[b][tuple(sl)].ravel(), gz[b][tuple(sl)].ravel()], 1))
+    W = np.concatenate(walls, 0) if walls else np.zeros((0, 3))
+    _, tot = t.offsets()
+    out = np.zeros(tot["p1"])
+    for b, (v, X, Y, Z) in enumerate(zip(p1_views(t, out, 1), gx, gy, gz)):
+        N = np.stack([X[1:-1, 1:-1, 1:-1].ravel(), Y[1:-1, 1:-1, 1:-1].ravel(), Z[1:-1, 1:-1, 1:-1].ravel()], 1)
+        dn = np.full(len(N), 1e20)
+        for c in range(0, len(W), 256):
+            dd = ((N[:, None, :] - W[None, c:c + 256, :]) ** 2).sum(-1).min(1)
+            dn = np.minimum(dn, dd)
+        dn = np.sqrt(dn).reshape(X[1:-1, 1:-1, 1:-1].shape, order="F")
+        cell = (dn[:-1, :-1, :-1] + dn[1:, :-1, :-1] + dn[:-1, 1:, :-1] + dn[1:, 1:, :-1] +
+                dn[:-1, :-1, 1:] + dn[1:, :-1, 1:] + dn[:-1, 1:, 1:] + dn[1:, 1:, 1:]) / 8
+        V = v[..., 0]
+        V[1:-1, 1:-1, 1:-1] = cell
+        V[0, :, :] = V[1, :, :]; V[-1, :, :] = V[-2, :, :]
+        V[:, 0, :] = V[:, 1, :]; V[:, -1, :] = V[:, -2, :]
+        V[:, :, 0] = V[:, :, 1]; V[:, :, -1] = V[:, :, -2]
+    return out
 
 
 # ---- configuration 3: 3D bump duct --------------------------------------------------

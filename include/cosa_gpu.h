@@ -101,7 +101,14 @@ typedef struct cosa_params {
      (coarsest); bln_prol 1 = bilinear prol_bln, 0 = linear prol_lin;
      lim_corr 0..3 = none / lim_corr1..3 of prol_bln (turbulence only) */
   int32_t nstart, npre, npost, ncrs, bln_prol, lim_corr;
-  int32_t reserved[6];
+  /* k-omega options (src/input.f90:2722-2765, 3565-3575): production
+     limiter on k (lim_prodtke) and omega (lim_prodomega) with factor prdlim;
+     production on every MG level (prd_all_lvls); k/omega floors after each
+     update (ifixq); compressibility term switch turcmp (0 or 1); omega wall
+     value (wallwilc 1: Wilcox rough wall with roughness roughk, 0: Menter) */
+  int32_t lim_prodtke, lim_prodomega, prd_all_lvls, ifixq, wallwilc, reserved_i;
+  double turcmp, prdlim, roughk;
+  double reserved[4];
 } cosa_params;
 
 /*

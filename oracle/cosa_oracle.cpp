@@ -521,10 +521,13 @@ void bc_far0(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
 }
 
 void bc_walvis_15(const Patch &pa, B3 &q, const Level &L, const cosa_params &P);
+void bc_walvis_15_kom(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk, const double *dista,
+                      const Level &L, int b, const cosa_params &P);
 
-// bbc dispatch (src/bc.f90:35-121): patches in table order
+// bbc dispatch (src/bc.f90:35-121): patches in table order; dist (wall
+// distance, P1) is read by the k-omega wall
 int bc_level(const Level &L, double *qa, const double *si, const double *sj, const double *sk,
-             const cosa_params &P) {
+             const cosa_params &P, const double *dist = nullptr) {
   int status = 0;
 #pragma omp parallel for reduction(| : status) schedule(dynamic)
   for (int b = 0; b < L.nb; ++b) {
@@ -541,8 +544,12 @@ int bc_level(const Level &L, double *qa, const double *si, const double *sj, con
         case 21: status |= bc_insub(pa, q, vi, vj, vk, L, P); break;
         case 91: bc_outsub(pa, q, L, P); break;
         default:
-          if (pa.bctyp / 100 == 15 && !is_kom(P) && !P.moving) bc_walvis_15(pa, q, L, P);
-          else if (pa.bctyp / 100 == 15 || pa.bctyp == 31) status |= COSA_ERR_UNSUPPORTED;
+          if (pa.bctyp / 100 == 15 && !P.moving && (!is_kom(P) || dist)) {
+            bc_walvis_15(pa, q, L, P);
+            if (is_kom(P)) bc_walvis_15_kom(pa, q, vi, vj, vk, dist, L, b, P);
+          } else if (pa.bctyp / 100 == 15 || pa.bctyp == 31) {
+            status |= COSA_ERR_UNSUPPORTED;
+          }
           break;
       }
     }
@@ -918,6 +925,70 @@ inline void roe_face(const cosa_params &P, double kx, double ky, double kz, doub
   for (int m = 1; m <= 5; ++m) flux[m] = (fr[m] + fl[m] - df[m]) / 2 * ds;
 }
 
+// roflux_b, turbulence fluxes (src/flux.f90:249-380): upwinded rho k u_n and
+// rho omega u_n with the mean-flow wave strengths.  The Roe-averaged total
+// enthalpy uses h0l/h0r as the mean-flow loop left them, i.e. those of the
+// block's last face (ic,jc,kc) of the snapshot: the reference does not
+// recompute them in this loop, and the restatement keeps that.
+void roflux_turb(const Level &L, int b, int d, B3 &qr, B3 &ql, B0 &flux, const B2 &s, const cosa_params &P, int n,
+                 int ic, int jc, int kc) {
+  const double g = P.gamma;
+  const int nh = n * P.hbmove;
+  double h0r_last, h0l_last;
+  {
+    const double ur = qr(ic, jc, kc, 2, n), vr = qr(ic, jc, kc, 3, n), wr = qr(ic, jc, kc, 4, n);
+    const double ul = ql(ic, jc, kc, 2, n), vl = ql(ic, jc, kc, 3, n), wl = ql(ic, jc, kc, 4, n);
+    h0r_last = g / (g - 1) * qr(ic, jc, kc, 5, n) / qr(ic, jc, kc, 1, n) + (ur * ur + vr * vr + wr * wr) / 2 +
+               qr(ic, jc, kc, 6, n);
+    h0l_last = g / (g - 1) * ql(ic, jc, kc, 5, n) / ql(ic, jc, kc, 1, n) + (ul * ul + vl * vl + wl * wl) / 2 +
+               ql(ic, jc, kc, 6, n);
+  }
+  for (int k = 1; k <= kc; ++k)
+    for (int j = 1; j <= jc; ++j)
+      for (int i = 1; i <= ic; ++i) {
+        const double kx = s(1, i, j, k, nh), ky = s(2, i, j, k, nh), kz = s(3, i, j, k, nh), ds = s(4, i, j, k, nh);
+        const double rhor = qr(i, j, k, 1, n), ur = qr(i, j, k, 2, n), vr = qr(i, j, k, 3, n), wr = qr(i, j, k, 4, n);
+        const double pr = qr(i, j, k, 5, n), omer = qr(i, j, k, 7, n), tker = qr(i, j, k, 6, n);
+        const double unr = ur * kx + vr * ky + wr * kz;
+        const double frk = rhor * unr * tker, frw = rhor * unr * omer;
+        const double rhol = ql(i, j, k, 1, n), ul = ql(i, j, k, 2, n), vl = ql(i, j, k, 3, n), wl = ql(i, j, k, 4, n);
+        const double pl = ql(i, j, k, 5, n), omel = ql(i, j, k, 7, n), tkel = ql(i, j, k, 6, n);
+        const double unl = ul * kx + vl * ky + wl * kz;
+        const double flk = rhol * unl * tkel, flw = rhol * unl * omel;
+        const double drho = rhor - rhol, dp = pr - pl, dun = unr - unl, dtke = tker - tkel, dome = omer - omel;
+        const double rhols = std::sqrt(rhol), rhors = std::sqrt(rhor);
+        const double rho = rhols * rhors, denom = rhols + rhors;
+        const double u = (rhols * ul + rhors * ur) / denom, v = (rhols * vl + rhors * vr) / denom;
+        const double w = (rhols * wl + rhors * wr) / denom;
+        const double un = u * kx + v * ky + w * kz;
+        const double h0 = (rhols * h0l_last + rhors * h0r_last) / denom;
+        const double tke = (rhols * tkel + rhors * tker) / denom, ome = (rhols * omel + rhors * omer) / denom;
+        const double q2 = u * u + v * v + w * w;
+        const double a2 = (g - 1) * (h0 - q2 / 2 - tke);
+        const double a = std::sqrt(a2);
+        double rm123 = std::fabs(un), rm4 = std::fabs(un + a), rm5 = std::fabs(un - a);
+        if (P.efx_setup_t) {
+          double rdelta = P.cntrpy_t * (P.entfx_t_w[0] * P.entfxctf_t + P.entfx_t_w[1] * (std::sqrt(q2) + a) +
+                                        P.entfx_t_w[2] * 0.2 * (std::fabs(un) + a + 0.0));
+          rdelta = std::max(rdelta, 1.0e-12);
+          if (rm123 <= rdelta && P.efx_all_t) rm123 = 0.5 * (rm123 * rm123 + rdelta * rdelta) / rdelta;
+          if (rm4 <= rdelta) rm4 = 0.5 * (rm4 * rm4 + rdelta * rdelta) / rdelta;
+          if (rm5 <= rdelta) rm5 = 0.5 * (rm5 * rm5 + rdelta * rdelta) / rdelta;
+        }
+        if (P.eig_limit_t) {
+          if (rm123 <= P.eig_cutoff_t) rm123 = P.eig_cutoff_t;
+          if (P.eig_lim_all_t && rm4 <= P.eig_cutoff_t) rm4 = P.eig_cutoff_t;
+          if (P.eig_lim_all_t && rm5 <= P.eig_cutoff_t) rm5 = P.eig_cutoff_t;
+        }
+        const double al1 = rm123 * (drho - dp / a2), al2 = rm123 * rho;
+        const double al3 = rm4 * (dp / a2 + rho * dun / a) / 2, al4 = rm5 * (dp / a2 - rho * dun / a) / 2;
+        const double dfk = (al1 + al3 + al4) * tke + al2 * dtke;
+        const double dfw = (al1 + al3 + al4) * ome + al2 * dome;
+        flux(i, j, k, 6, n) = (frk + flk - dfk) / 2 * ds;
+        flux(i, j, k, 7, n) = (frw + flw - dfw) / 2 * ds;
+      }
+}
+
 void roflux_b(const Level &L, int b, int d, double *qra, double *qla, double *fa, const double *sijk,
               const cosa_params &P) {
   B3 qr(qra, L, b), ql(qla, L, b);
@@ -939,6 +1010,7 @@ void roflux_b(const Level &L, int b, int d, double *qra, double *qla, double *fa
           roe_face(P, kx, ky, kz, ds, 0.0, vr, vl, tker, tkel, f);
           for (int v = 1; v <= 5; ++v) flux(i, j, k, v, n) = f[v];
         }
+    if (kom) roflux_turb(L, b, d, qr, ql, flux, s, P, n, ic, jc, kc);
   }
 }
 
@@ -1116,11 +1188,11 @@ void src_hb_level(const Level &L, const double *qa, const double *va, double *ra
 
 // resg_rms_hb / resg_brms_hb (src/cosa.f90:4584-4697), explicit branch
 void resg_rms_hb_level(const Level &L, double *ra, double *out) {
-  double acc[8] = {0};
+  double acc[10] = {0};
   int64_t ncell = 0;
   for (int b = 0; b < L.nb; ++b) {
     B3 res(ra, L, b);
-    double rb[8] = {0};
+    double rb[10] = {0};
     for (int n = 0; n < L.S; ++n)
       for (int v = 1; v <= L.npde; ++v)
         for (int k = 1; k <= L.km[b] - 1; ++k)
@@ -1136,11 +1208,11 @@ void resg_rms_hb_level(const Level &L, double *ra, double *out) {
 
 // ---- resg_brms (src/cosa.f90:4503-4582), explicit steady branch ------------
 void resg_rms_level(const Level &L, double *ra, double *rha, double *out) {
-  double acc[8] = {0};
+  double acc[10] = {0};
   int64_t ncell = 0;
   for (int b = 0; b < L.nb; ++b) {
     B3 res(ra, L, b), rhs(rha, L, b);
-    double rb[8] = {0};
+    double rb[10] = {0};
     for (int v = 1; v <= L.npde; ++v)
       for (int k = 1; k <= L.km[b] - 1; ++k)
         for (int j = 1; j <= L.jm[b] - 1; ++j)
@@ -1874,7 +1946,7 @@ void q_der_b(const Level &L, int b, int d, const double *qa, double *dxa, double
 // flux on the faces of family d; the energy row keeps the reference's terms
 void vflux_b(const Level &L, int b, int d, const double *qfa, const double *dxa, const double *dya,
              const double *dza, const double *xd, const double *ed, const double *zd, const double *sijk,
-             double *fa, const cosa_params &P) {
+             double *fa, const cosa_params &P, bool kom = false) {
   B3 qf(const_cast<double *>(qfa), L, b), dqx(const_cast<double *>(dxa), L, b);
   B3 dqe(const_cast<double *>(dya), L, b), dqz(const_cast<double *>(dza), L, b);
   BV xv(const_cast<double *>(xd), L, b), ev(const_cast<double *>(ed), L, b), zv(const_cast<double *>(zd), L, b);
@@ -1883,11 +1955,12 @@ void vflux_b(const Level &L, int b, int d, const double *qfa, const double *dxa,
   const int im = L.im[b], jm = L.jm[b], km = L.km[b];
   const int ni = d == 1 ? im : im - 1, nj = d == 2 ? jm : jm - 1, nk = d == 3 ? km : km - 1;
   const double g = P.gamma, mr = P.machfs / P.reyno;
-  for (int n = 0; n < L.S; ++n)
-    for (int k = 1; k <= nk; ++k)
-      for (int j = 1; j <= nj; ++j)
-        for (int i = 1; i <= ni; ++i)
-          for (int v = 1; v <= 5; ++v) flux(i, j, k, v, n) = 0;
+  if (!kom)  // laminar: the flux starts from zero (src/flux.f90:1073-1087)
+    for (int n = 0; n < L.S; ++n)
+      for (int k = 1; k <= nk; ++k)
+        for (int j = 1; j <= nj; ++j)
+          for (int i = 1; i <= ni; ++i)
+            for (int v = 1; v <= 5; ++v) flux(i, j, k, v, n) = 0;
   for (int n = 0; n < L.S; ++n) {
     const int nh = n * P.hbmove;
     for (int k = 1; k <= nk; ++k)
@@ -2035,12 +2108,49 @@ void lambda_ns_level(const Level &L, const double *qa, const double *si, const d
 }
 
 
-// bdeltat, viscous branch (src/cosa.f90:4861-4876, 4895-5010): the viscous
-// lambdas join the time step unless irsop is 5 or 6, where they raise the
-// smoothing coefficients instead
-void deltat_ns_level(const Level &L, double *dtv, const double *lam, const double *lamv, double *bx_, double *by_,
-                     double *bz_, const cosa_params &P) {
+// IRS coefficients of bdeltat (src/cosa.f90:4896-5200) for one cell with
+// ratio `rat` (rat for the mean flow, ratt for k-omega); irsop 5 and 6 add
+// the viscous floor c1/4 lamv / sum(lam)
+void irs_coef(int irsop, double rat, double psirs, const double lam[3], const double lamv[3], double out[3]) {
   const double zeta = 0.4, c1 = 40.0;
+  const double lami = lam[0], lamj = lam[1], lamk = lam[2];
+  if (irsop == 2 || irsop == 5) {
+    const double phixi = 1 + std::pow(lamj / lami, zeta) + std::pow(lamk / lami, zeta);
+    const double phieta = 1 + std::pow(lami / lamj, zeta) + std::pow(lamk / lamj, zeta);
+    const double phizeta = 1 + std::pow(lami / lamk, zeta) + std::pow(lamj / lamk, zeta);
+    double t;
+    t = (rat * lami * phixi / (lami + lamj + lamk));
+    out[0] = std::max(0.0, (t * t - 1) / 4);
+    t = (rat * lamj * phieta / (lami + lamj + lamk));
+    out[1] = std::max(0.0, (t * t - 1) / 4);
+    t = (rat * lamk * phizeta / (lami + lamj + lamk));
+    out[2] = std::max(0.0, (t * t - 1) / 4);
+    if (irsop == 5)
+      for (int c = 0; c < 3; ++c) out[c] = std::max(out[c], c1 / 4 * lamv[c] / (lami + lamj + lamk));
+  } else if (irsop == 3 || irsop == 6) {
+    const double rji = lamj / lami, rki = lamk / lami, rij = lami / lamj;
+    const double rkj = lamk / lamj, rik = lami / lamk, rjk = lamj / lamk;
+    double t;
+    t = rat / (1 + psirs * (rji + rki));
+    out[0] = std::max(0.0, 0.25 * (t * t - 1));
+    t = rat / (1 + psirs * (rij + rkj));
+    out[1] = std::max(0.0, 0.25 * (t * t - 1));
+    t = rat / (1 + psirs * (rik + rjk));
+    out[2] = std::max(0.0, 0.25 * (t * t - 1));
+    if (irsop == 6)
+      for (int c = 0; c < 3; ++c) out[c] = std::max(out[c], 0.25 * c1 * lamv[c] / (lami + lamj + lamk));
+  } else {
+    out[0] = out[1] = out[2] = 0.0;
+  }
+}
+
+// bdeltat, viscous branch (src/cosa.f90:4861-4876, 4895-5200): the viscous
+// lambdas join the time step unless irsop is 5 or 6, where they raise the
+// smoothing coefficients instead; k-omega: dtvolt = cflt/cfl dtvol and the
+// turbulence coefficients with ratt
+void deltat_ns_level(const Level &L, double *dtv, const double *lam, const double *lamv, double *bx_, double *by_,
+                     double *bz_, const cosa_params &P, double *dtt_ = nullptr, double *tbx_ = nullptr,
+                     double *tby_ = nullptr, double *tbz_ = nullptr) {
   const bool dt_visc = P.irsop != 5 && P.irsop != 6;
   for (int b = 0; b < L.nb; ++b) {
     B3 lm(const_cast<double *>(lam), L, b), lv(const_cast<double *>(lamv), L, b);
@@ -2054,51 +2164,360 @@ void deltat_ns_level(const Level &L, double *dtv, const double *lam, const doubl
                                         lv(i, j, k, 1, n) + lv(i, j, k, 2, n) + lv(i, j, k, 3, n));
             else
               dt(i, j, k, n) = P.cfl / (lm(i, j, k, 1, n) + lm(i, j, k, 2, n) + lm(i, j, k, 3, n));
+            if (dtt_) {
+              B1 dtt(dtt_, L, b, L.S);
+              dtt(i, j, k, n) = P.cflt / P.cfl * dt(i, j, k, n);
+            }
           }
-    if (P.irsop == 0 || !bx_) continue;
-    B1 bx(bx_, L, b, L.S), by(by_, L, b, L.S), bz(bz_, L, b, L.S);
-    const double rat = P.rat, psirs = P.psirs;
+    if (P.irsop < 2 || P.irsop == 4) continue;
     for (int n = 0; n < L.S; ++n)
       for (int k = 1; k <= L.km[b] - 1; ++k)
         for (int j = 1; j <= L.jm[b] - 1; ++j)
           for (int i = 1; i <= L.im[b] - 1; ++i) {
-            const double lami = lm(i, j, k, 1, n), lamj = lm(i, j, k, 2, n), lamk = lm(i, j, k, 3, n);
-            const double lamvi = lv(i, j, k, 1, n), lamvj = lv(i, j, k, 2, n), lamvk = lv(i, j, k, 3, n);
-            double ba = 0, bb = 0, bc = 0;
-            if (P.irsop == 2 || P.irsop == 5) {
-              const double phixi = 1 + std::pow(lamj / lami, zeta) + std::pow(lamk / lami, zeta);
-              const double phieta = 1 + std::pow(lami / lamj, zeta) + std::pow(lamk / lamj, zeta);
-              const double phizeta = 1 + std::pow(lami / lamk, zeta) + std::pow(lamj / lamk, zeta);
-              double t;
-              t = (rat * lami * phixi / (lami + lamj + lamk));
-              ba = std::max(0.0, (t * t - 1) / 4);
-              t = (rat * lamj * phieta / (lami + lamj + lamk));
-              bb = std::max(0.0, (t * t - 1) / 4);
-              t = (rat * lamk * phizeta / (lami + lamj + lamk));
-              bc = std::max(0.0, (t * t - 1) / 4);
-              if (P.irsop == 5) {
-                ba = std::max(ba, c1 / 4 * lamvi / (lami + lamj + lamk));
-                bb = std::max(bb, c1 / 4 * lamvj / (lami + lamj + lamk));
-                bc = std::max(bc, c1 / 4 * lamvk / (lami + lamj + lamk));
-              }
-            } else if (P.irsop == 3 || P.irsop == 6) {
-              const double rji = lamj / lami, rki = lamk / lami, rij = lami / lamj;
-              const double rkj = lamk / lamj, rik = lami / lamk, rjk = lamj / lamk;
-              double t;
-              t = rat / (1 + psirs * (rji + rki));
-              ba = std::max(0.0, 0.25 * (t * t - 1));
-              t = rat / (1 + psirs * (rij + rkj));
-              bb = std::max(0.0, 0.25 * (t * t - 1));
-              t = rat / (1 + psirs * (rik + rjk));
-              bc = std::max(0.0, 0.25 * (t * t - 1));
-              if (P.irsop == 6) {
-                ba = std::max(ba, 0.25 * c1 * lamvi / (lami + lamj + lamk));
-                bb = std::max(bb, 0.25 * c1 * lamvj / (lami + lamj + lamk));
-                bc = std::max(bc, 0.25 * c1 * lamvk / (lami + lamj + lamk));
-              }
+            const double l[3] = {lm(i, j, k, 1, n), lm(i, j, k, 2, n), lm(i, j, k, 3, n)};
+            const double v[3] = {lv(i, j, k, 1, n), lv(i, j, k, 2, n), lv(i, j, k, 3, n)};
+            double o[3];
+            if (bx_) {
+              irs_coef(P.irsop, P.rat, P.psirs, l, v, o);
+              B1 bx(bx_, L, b, L.S), by(by_, L, b, L.S), bz(bz_, L, b, L.S);
+              bx(i, j, k, n) = o[0]; by(i, j, k, n) = o[1]; bz(i, j, k, n) = o[2];
             }
-            bx(i, j, k, n) = ba; by(i, j, k, n) = bb; bz(i, j, k, n) = bc;
+            if (tbx_) {
+              irs_coef(P.irsop, P.ratt, P.psirs, l, v, o);
+              B1 bx(tbx_, L, b, L.S), by(tby_, L, b, L.S), bz(tbz_, L, b, L.S);
+              bx(i, j, k, n) = o[0]; by(i, j, k, n) = o[1]; bz(i, j, k, n) = o[2];
+            }
           }
+  }
+}
+
+// ---- k-omega (Wilcox), src/flux.f90, src/src.f90, src/update.f90, src/bc.f90 --
+// bc_walvis_15, k-omega part (src/bc.f90:2309-2470): k = 0 at the wall and
+// omega from Wilcox's rough-wall law (wallwilc) or Menter's near-wall
+// solution, both from the wall distance of the first cell
+void bc_walvis_15_kom(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk, const double *dista,
+                      const Level &L, int b, const cosa_params &P) {
+  const double small = 1.0e-12, smasq = 1.0e-24, mor = P.machfs / P.reyno;
+  const int ibcpt = pa.inrout == 1 ? 0 : pa.ijk[pa.idir], ibcpt2 = pa.inrout == 1 ? -1 : pa.ijk[pa.idir] + 1;
+  const int ibcn = pa.inrout == 1 ? 1 : pa.ijk[pa.idir] - 1, ibcm = pa.inrout == 1 ? 1 : pa.ijk[pa.idir];
+  B1 dist(const_cast<double *>(dista), L, b, 1);
+  const B2 &sf = pa.idir == 1 ? si : (pa.idir == 2 ? sj : sk);
+  for (int n = 0; n < L.S; ++n) {
+    const int nh = n * P.hbmove;
+    for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+      for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+        int hi, hj, hk, h2i, h2j, h2k, ni_, nj_, nk_, mi, mj, mk;
+        pidx(pa, ibcpt, i2, i3, hi, hj, hk);
+        pidx(pa, ibcpt2, i2, i3, h2i, h2j, h2k);
+        pidx(pa, ibcn, i2, i3, ni_, nj_, nk_);
+        pidx(pa, ibcm, i2, i3, mi, mj, mk);
+        const double rhow = q(hi, hj, hk, 1, n), pw = q(hi, hj, hk, 5, n);
+        const double tw = pw * P.gamma / rhow;
+        const double muw = (P.stemp + 1) / (tw + P.stemp) * std::pow(tw, 1.5);
+        const double d = dist(ni_, nj_, nk_);
+        double omew;
+        if (P.wallwilc) {
+          const double nx = sf(1, mi, mj, mk, nh), ny = sf(2, mi, mj, mk, nh), nz = sf(3, mi, mj, mk, nh);
+          const double uc = q(ni_, nj_, nk_, 2, n), vc = q(ni_, nj_, nk_, 3, n), wc = q(ni_, nj_, nk_, 4, n);
+          const double uorth = nx * uc + ny * vc + nz * wc;
+          const double a = uc - uorth * nx, bb = vc - uorth * ny, c = wc - uorth * nz;
+          const double upar = std::sqrt(a * a + bb * bb + c * c);
+          const double dupardn = upar / (d + small);
+          const double tauw = muw * std::fabs(dupardn);
+          const double rkrpls = P.roughk > 0.0 ? std::max(1.0, std::sqrt(rhow * tauw / mor) * P.roughk / muw) : 1.0;
+          const double sr = rkrpls >= 25.0 ? 100.0 / rkrpls : 2500.0 / (rkrpls * rkrpls);
+          omew = std::fabs(dupardn) * sr;
+        } else {
+          omew = 60.0 * muw / (P.bkw * rhow * (d * d) + smasq) * P.machfs / P.reyno;
+        }
+        q(hi, hj, hk, 6, n) = 0.0;
+        q(hi, hj, hk, 7, n) = omew;
+        q(h2i, h2j, h2k, 6, n) = q(hi, hj, hk, 6, n);
+        q(h2i, h2j, h2k, 7, n) = q(hi, hj, hk, 7, n);
+      }
+  }
+}
+
+// bq_face_* with calmut (src/flux.f90:2495-2540 and the j, k counterparts):
+// face turbulent viscosity into flux(.,1), the halo value on strong faces
+void q_face_mut_b(const Level &L, int b, int d, const double *muta, double *fa) {
+  B3s mu(const_cast<double *>(muta), L, b);
+  B0 f(fa, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  const int ni = d == 1 ? im : im - 1, nj = d == 2 ? jm : jm - 1, nk = d == 3 ? km : km - 1;
+  const int di = d == 1, dj = d == 2, dk = d == 3;
+  for (int n = 0; n < L.S; ++n)
+    for (int k = 1; k <= nk; ++k)
+      for (int j = 1; j <= nj; ++j)
+        for (int i = 1; i <= ni; ++i) f(i, j, k, 1, n) = (mu(i - di, j - dj, k - dk, n) + mu(i, j, k, n)) / 2;
+  const int *t = L.bct.data() + L.obct[b];
+  for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
+    Patch pa = patch_of(t + 10 * ibc, im, jm, km);
+    if (pa.idir != d || !strong_bc(pa.bctyp)) continue;
+    const int ibcpt = pa.inrout == 1 ? 0 : pa.ijk[d], iface = pa.inrout == 1 ? 1 : pa.ijk[d];
+    for (int n = 0; n < L.S; ++n)
+      for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+        for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+          int a, bb, c, e, g, h;
+          pidx(pa, iface, i2, i3, a, bb, c);
+          pidx(pa, ibcpt, i2, i3, e, g, h);
+          f(a, bb, c, 1, n) = mu(e, g, h, n);
+        }
+  }
+}
+
+// b_rtst (src/flux.f90:2846-2946): Reynolds stresses on the faces of family
+// d, tau1(.,1..6) = txx, txy, txz, tyy, tyz, tzz, with -2/3 rho k on the
+// diagonal
+void rtst_b(const Level &L, int b, int d, const double *qfa, const double *dxa, const double *dya, const double *dza,
+            const double *xd, const double *ed, const double *zd, double *taua, const double *fa,
+            const cosa_params &P) {
+  B3 qf(const_cast<double *>(qfa), L, b), dqx(const_cast<double *>(dxa), L, b);
+  B3 dqe(const_cast<double *>(dya), L, b), dqz(const_cast<double *>(dza), L, b), tau(taua, L, b);
+  BV xv(const_cast<double *>(xd), L, b), ev(const_cast<double *>(ed), L, b), zv(const_cast<double *>(zd), L, b);
+  B0 f(const_cast<double *>(fa), L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  const int ni = d == 1 ? im : im - 1, nj = d == 2 ? jm : jm - 1, nk = d == 3 ? km : km - 1;
+  const double fact = 2.0 / 3.0;
+  for (int n = 0; n < L.S; ++n)
+    for (int k = 1; k <= nk; ++k)
+      for (int j = 1; j <= nj; ++j)
+        for (int i = 1; i <= ni; ++i) {
+          const double rho = qf(i, j, k, 1, n), tke = qf(i, j, k, 6, n), mut = f(i, j, k, 1, n);
+          const double xix = xv(1, i, j, k), xiy = xv(2, i, j, k), xiz = xv(3, i, j, k);
+          const double etax = ev(1, i, j, k), etay = ev(2, i, j, k), etaz = ev(3, i, j, k);
+          const double zetax = zv(1, i, j, k), zetay = zv(2, i, j, k), zetaz = zv(3, i, j, k);
+          const double uxi = dqx(i, j, k, 2, n), ueta = dqe(i, j, k, 2, n), uzeta = dqz(i, j, k, 2, n);
+          const double vxi = dqx(i, j, k, 3, n), veta = dqe(i, j, k, 3, n), vzeta = dqz(i, j, k, 3, n);
+          const double wxi = dqx(i, j, k, 4, n), weta = dqe(i, j, k, 4, n), wzeta = dqz(i, j, k, 4, n);
+          const double dudx = uxi * xix + ueta * etax + uzeta * zetax;
+          const double dudy = uxi * xiy + ueta * etay + uzeta * zetay;
+          const double dudz = uxi * xiz + ueta * etaz + uzeta * zetaz;
+          const double dvdx = vxi * xix + veta * etax + vzeta * zetax;
+          const double dvdy = vxi * xiy + veta * etay + vzeta * zetay;
+          const double dvdz = vxi * xiz + veta * etaz + vzeta * zetaz;
+          const double dwdx = wxi * xix + weta * etax + wzeta * zetax;
+          const double dwdy = wxi * xiy + weta * etay + wzeta * zetay;
+          const double dwdz = wxi * xiz + weta * etaz + wzeta * zetaz;
+          const double divv = (dudx + dvdy + dwdz) * P.turcmp;
+          const double txx = 2 * mut * (dudx - divv / 3), txy = mut * (dudy + dvdx), txz = mut * (dudz + dwdx);
+          const double tyy = 2 * mut * (dvdy - divv / 3), tyz = mut * (dvdz + dwdy);
+          const double tzz = 2 * mut * (dwdz - divv / 3);
+          const double mr = P.machfs / P.reyno;
+          tau(i, j, k, 1, n) = mr * txx - fact * rho * tke;
+          tau(i, j, k, 2, n) = mr * txy;
+          tau(i, j, k, 3, n) = mr * txz;
+          tau(i, j, k, 4, n) = mr * tyy - fact * rho * tke;
+          tau(i, j, k, 5, n) = mr * tyz;
+          tau(i, j, k, 6, n) = mr * tzz - fact * rho * tke;
+        }
+}
+
+// vflux_b, Wilcox k-omega branch (src/flux.f90:915-983): Reynolds-stress
+// momentum flux and the k / omega diffusion, before the laminar terms; the
+// omega row keeps the reference's dk/dz in place of domega/dz
+void vflux_kom_b(const Level &L, int b, int d, const double *qfa, const double *dxa, const double *dya,
+                 const double *dza, const double *taua, const double *xd, const double *ed, const double *zd,
+                 const double *sijk, double *fa, const cosa_params &P) {
+  B3 qf(const_cast<double *>(qfa), L, b), dqx(const_cast<double *>(dxa), L, b);
+  B3 dqe(const_cast<double *>(dya), L, b), dqz(const_cast<double *>(dza), L, b), tau(const_cast<double *>(taua), L, b);
+  BV xv(const_cast<double *>(xd), L, b), ev(const_cast<double *>(ed), L, b), zv(const_cast<double *>(zd), L, b);
+  B2 s(sijk, L, b);
+  B0 flux(fa, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  const int ni = d == 1 ? im : im - 1, nj = d == 2 ? jm : jm - 1, nk = d == 3 ? km : km - 1;
+  for (int n = 0; n < L.S; ++n) {
+    const int nh = n * P.hbmove;
+    for (int k = 1; k <= nk; ++k)
+      for (int j = 1; j <= nj; ++j)
+        for (int i = 1; i <= ni; ++i) {
+          const double kx = s(1, i, j, k, nh), ky = s(2, i, j, k, nh), kz = s(3, i, j, k, nh), ds = s(4, i, j, k, nh);
+          const double rho = qf(i, j, k, 1, n), p = qf(i, j, k, 5, n);
+          const double t = P.gamma * p / rho;
+          const double mu = (P.stemp + 1) / (t + P.stemp) * std::pow(t, 1.5);
+          const double mut = flux(i, j, k, 1, n);
+          const double xix = xv(1, i, j, k), xiy = xv(2, i, j, k), xiz = xv(3, i, j, k);
+          const double etax = ev(1, i, j, k), etay = ev(2, i, j, k), etaz = ev(3, i, j, k);
+          const double zetax = zv(1, i, j, k), zetay = zv(2, i, j, k), zetaz = zv(3, i, j, k);
+          const double tkexi = dqx(i, j, k, 6, n), tkeeta = dqe(i, j, k, 6, n), tkezeta = dqz(i, j, k, 6, n);
+          const double omexi = dqx(i, j, k, 7, n), omeeta = dqe(i, j, k, 7, n), omezeta = dqz(i, j, k, 7, n);
+          const double dtkedx = tkexi * xix + tkeeta * etax + tkezeta * zetax;
+          const double dtkedy = tkexi * xiy + tkeeta * etay + tkezeta * zetay;
+          const double dtkedz = tkexi * xiz + tkeeta * etaz + tkezeta * zetaz;
+          const double domedx = omexi * xix + omeeta * etax + omezeta * zetax;
+          const double domedy = omexi * xiy + omeeta * etay + omezeta * zetay;
+          const double txx = tau(i, j, k, 1, n), txy = tau(i, j, k, 2, n), txz = tau(i, j, k, 3, n);
+          const double tyy = tau(i, j, k, 4, n), tyz = tau(i, j, k, 5, n), tzz = tau(i, j, k, 6, n);
+          flux(i, j, k, 2, n) = -(txx * kx + txy * ky + txz * kz) * ds;
+          flux(i, j, k, 3, n) = -(txy * kx + tyy * ky + tyz * kz) * ds;
+          flux(i, j, k, 4, n) = -(txz * kx + tyz * ky + tzz * kz) * ds;
+          const double ctke = (mu + P.sigk * mut) * P.machfs / P.reyno;
+          const double come = (mu + P.sigw * mut) * P.machfs / P.reyno;
+          flux(i, j, k, 5, n) = -ctke * (dtkedx * kx + dtkedy * ky + dtkedz * kz) * ds;
+          flux(i, j, k, 6, n) = -ctke * (dtkedx * kx + dtkedy * ky + dtkedz * kz) * ds;
+          flux(i, j, k, 7, n) = -come * (domedx * kx + domedy * ky + dtkedz * kz) * ds;
+        }
+  }
+}
+
+// bq_der_ci/cj/ck (src/flux.f90:2979-3130): cell-centred differences of the
+// face values of family d for the velocity components
+void q_der_c_b(const Level &L, int b, int d, const double *qfa, double *dca) {
+  B3 qf(const_cast<double *>(qfa), L, b), dc(dca, L, b);
+  const int di = d == 1, dj = d == 2, dk = d == 3;
+  for (int n = 0; n < L.S; ++n)
+    for (int v = 2; v <= 4; ++v)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i)
+            dc(i, j, k, v, n) = qf(i + di, j + dj, k + dk, v, n) - qf(i, j, k, v, n);
+}
+
+// turprod_b (src/src.f90:40-177): production P_d (alternative form), div u,
+// delta+ = 2/3 max(div u, 0); the cell-centre metrics average the two faces
+// of the family matching each Cartesian component, as the reference does
+void turprod_b(const Level &L, int b, const double *qa, const double *dxa, const double *dya, const double *dza,
+               const double *vm, double *prda, double *diva, double *dpla, const cosa_params &P) {
+  B3 q(const_cast<double *>(qa), L, b), dqx(const_cast<double *>(dxa), L, b);
+  B3 dqe(const_cast<double *>(dya), L, b), dqz(const_cast<double *>(dza), L, b);
+  B3s prd(prda, L, b), dvv(diva, L, b), dpl(dpla, L, b);
+  // vm array (d, m): derivative m on faces of family d
+  auto V = [&](int d, int m) { return BV(const_cast<double *>(vm) + (int64_t)((d - 1) * 3 + m) * 3 * L.n0, L, b); };
+  BV xi_i = V(1, 0), xi_j = V(2, 0), xi_k = V(3, 0);
+  BV et_i = V(1, 1), et_j = V(2, 1), et_k = V(3, 1);
+  BV ze_i = V(1, 2), ze_j = V(2, 2), ze_k = V(3, 2);
+  const double fact = 2.0 / 3.0;
+  for (int n = 0; n < L.S; ++n)
+    for (int k = 1; k <= L.km[b] - 1; ++k)
+      for (int j = 1; j <= L.jm[b] - 1; ++j)
+        for (int i = 1; i <= L.im[b] - 1; ++i) {
+          const double xix = (xi_i(1, i + 1, j, k) + xi_i(1, i, j, k)) / 2;
+          const double xiy = (xi_j(2, i, j + 1, k) + xi_j(2, i, j, k)) / 2;
+          const double xiz = (xi_k(3, i, j, k + 1) + xi_k(3, i, j, k)) / 2;
+          const double etax = (et_i(1, i + 1, j, k) + et_i(1, i, j, k)) / 2;
+          const double etay = (et_j(2, i, j + 1, k) + et_j(2, i, j, k)) / 2;
+          const double etaz = (et_k(3, i, j, k + 1) + et_k(3, i, j, k)) / 2;
+          const double zetax = (ze_i(1, i + 1, j, k) + ze_i(1, i, j, k)) / 2;
+          const double zetay = (ze_j(2, i, j + 1, k) + ze_j(2, i, j, k)) / 2;
+          const double zetaz = (ze_k(3, i, j, k + 1) + ze_k(3, i, j, k)) / 2;
+          const double uxi = dqx(i, j, k, 2, n), ueta = dqe(i, j, k, 2, n), uzeta = dqz(i, j, k, 2, n);
+          const double vxi = dqx(i, j, k, 3, n), veta = dqe(i, j, k, 3, n), vzeta = dqz(i, j, k, 3, n);
+          const double wxi = dqx(i, j, k, 4, n), weta = dqe(i, j, k, 4, n), wzeta = dqz(i, j, k, 4, n);
+          const double dudx = uxi * xix + ueta * etax + uzeta * zetax;
+          const double dudy = uxi * xiy + ueta * etay + uzeta * zetay;
+          const double dudz = uxi * xiz + ueta * etaz + uzeta * zetaz;
+          const double dvdx = vxi * xix + veta * etax + vzeta * zetax;
+          const double dvdy = vxi * xiy + veta * etay + vzeta * zetay;
+          const double dvdz = vxi * xiz + veta * etaz + vzeta * zetaz;
+          const double dwdx = wxi * xix + weta * etax + wzeta * zetax;
+          const double dwdy = wxi * xiy + weta * etay + wzeta * zetay;
+          const double dwdz = wxi * xiz + weta * etaz + wzeta * zetaz;
+          const double divv = (dudx + dvdy + dwdz) * P.turcmp;
+          const double txx = dudx, txy = (dudy + dvdx) / 2, txz = (dudz + dwdx) / 2;
+          const double tyy = dvdy, tyz = (dvdz + dwdy) / 2, tzz = dwdz;
+          const double prod = 2 * (txx * txx + tyy * tyy + tzz * tzz + 2 * (txy * txy + txz * txz + tyz * tyz) -
+                                   divv * divv / 3);
+          (void)q;
+          prd(i, j, k, n) = prod;
+          dvv(i, j, k, n) = divv;
+          dpl(i, j, k, n) = fact * std::max(divv, 0.0);
+        }
+}
+
+// srckw_b (src/src.f90:196-272): k and omega sources into res(6:7)
+void srckw_b(const Level &L, int b, int nl, const double *qa, const double *muta, const double *prda,
+             const double *diva, double *ra, const double *va, const cosa_params &P) {
+  B3 q(const_cast<double *>(qa), L, b), res(ra, L, b);
+  B3s mu(const_cast<double *>(muta), L, b), prd(const_cast<double *>(prda), L, b), dvv(const_cast<double *>(diva), L, b);
+  B1 vol(const_cast<double *>(va), L, b, 1);
+  const double fact = 2.0 / 3.0, mor = P.machfs / P.reyno;
+  for (int n = 0; n < L.S; ++n)
+    for (int k = 1; k <= L.km[b] - 1; ++k)
+      for (int j = 1; j <= L.jm[b] - 1; ++j)
+        for (int i = 1; i <= L.im[b] - 1; ++i) {
+          const double rho = q(i, j, k, 1, n), tke = q(i, j, k, 6, n), ome = q(i, j, k, 7, n);
+          const double mut = mu(i, j, k, n), divv = dvv(i, j, k, n);
+          double prod = prd(i, j, k, n), prodw = prd(i, j, k, n);
+          if (P.lim_prodtke && (nl == 1 || P.prd_all_lvls)) {
+            const double tstdis = P.prdlim * P.bstrkw * rho * tke * ome;
+            if (mor * mut * prod > tstdis) {
+              prod = tstdis / mor / mut;
+              if (P.lim_prodomega) prodw = prod;
+            }
+          }
+          res(i, j, k, 6, n) = res(i, j, k, 6, n) -
+                               vol(i, j, k) * (mor * mut * prod - fact * divv * rho * tke - P.bstrkw * rho * tke * ome);
+          res(i, j, k, 7, n) = res(i, j, k, 7, n) - vol(i, j, k) * (P.gkw * P.cmu * rho * prodw -
+                                                                    P.gkw * fact * divv * rho * ome -
+                                                                    P.bkw * rho * (ome * ome));
+        }
+}
+
+// update_b, explicit k-omega part (src/update.f90:601-640): point-implicit
+// rho*omega then rho*k with the destruction terms, omega floored by the
+// production; ttrm = (0, gkw, bkw) for the Wilcox model (update_ttrm_b)
+void update_kom_b(const Level &L, int b, const double *ra, double *qa, const double *qoa, const double *va,
+                  const double *dtta, const double *dpla, const double *prda, double ar, const cosa_params &P) {
+  B3 res(const_cast<double *>(ra), L, b), q(qa, L, b), qold(const_cast<double *>(qoa), L, b);
+  B1 vol(const_cast<double *>(va), L, b, 1), dtt(const_cast<double *>(dtta), L, b, L.S);
+  B3s dpl(const_cast<double *>(dpla), L, b), prd(const_cast<double *>(prda), L, b);
+  const double gav = P.gkw, bav = P.bkw;
+  for (int n = 0; n < L.S; ++n)
+    for (int k = 1; k <= L.km[b] - 1; ++k)
+      for (int j = 1; j <= L.jm[b] - 1; ++j)
+        for (int i = 1; i <= L.im[b] - 1; ++i) {
+          const double rho = q(i, j, k, 1, n);
+          const double ome = q(i, j, k, 7, n) / q(i, j, k, 1, n);
+          const double tke = q(i, j, k, 6, n) / q(i, j, k, 1, n);
+          const double dtau = dtt(i, j, k, n) * vol(i, j, k);
+          double rhomega = (qold(i, j, k, 7, n) - ar * res(i, j, k, 7, n) * dtt(i, j, k, n) +
+                            ar * dtau * rho * ome * (gav * dpl(i, j, k, n) + 2 * bav * ome)) /
+                           (1 + ar * dtau * (gav * dpl(i, j, k, n) + 2 * bav * ome));
+          const double rhomegamin = gav * P.cmu * rho * std::sqrt(prd(i, j, k, n));
+          if (rhomega < rhomegamin) rhomega = rhomegamin;
+          q(i, j, k, 7, n) = rhomega;
+          const double drhomega = q(i, j, k, 7, n) - rho * ome;
+          q(i, j, k, 6, n) = (qold(i, j, k, 6, n) - ar * res(i, j, k, 6, n) * dtt(i, j, k, n) +
+                              ar * dtau * rho * tke * (dpl(i, j, k, n) + P.bstrkw * ome) -
+                              ar * dtau * P.bstrkw * tke * drhomega) /
+                             (1 + ar * dtau * (dpl(i, j, k, n) + P.bstrkw * ome));
+        }
+}
+
+// cutman_mut (src/bc.f90:2713-2799): cut_q on the turbulent viscosity
+void cutman_mut_level(const Level &L, double *muta) {
+  for (int icut = 0; icut < L.ncuts; ++icut) {
+    const int *c = L.cut.data() + 21 * icut;
+    const int b1 = c[0] - 1, b2 = c[9] - 1;
+    B3s m1(muta, L, b1), m2(muta, L, b2);
+    const int ijk1[4] = {0, L.im[b1], L.jm[b1], L.km[b1]}, ijk2[4] = {0, L.im[b2], L.jm[b2], L.km[b2]};
+    const int idir1 = c[1], inout1 = c[2], idir2 = c[10], inout2 = c[11];
+    const int istr1[4] = {0, c[3], c[5], c[7]}, iend1[4] = {0, c[4], c[6], c[8]};
+    const int istr2[4] = {0, c[12], c[14], c[16]}, iend2[4] = {0, c[13], c[15], c[17]};
+    const int iord[4] = {0, c[18], c[19], c[20]};
+    int ibcpt, ibcinc, inr, inrinc;
+    if (inout1 == 1) { ibcpt = 0; ibcinc = -1; } else { ibcpt = ijk1[idir1]; ibcinc = 1; }
+    if (inout2 == 1) { inr = 1; inrinc = 1; } else { inr = ijk2[idir2] - 1; inrinc = -1; }
+    int len[4], isgn1[4], isgn2[4];
+    for (int l = 1; l <= 3; ++l) {
+      len[l] = std::abs(iend1[l] - istr1[l]);
+      isgn1[l] = iend1[l] > istr1[l] ? 1 : -1;
+      isgn2[l] = iend2[l] > istr2[l] ? 1 : -1;
+    }
+    const int ic1 = cyc(idir1, 1), ic2 = cyc(idir1, 2), ic3 = cyc(idir1, 3);
+    const int jc1 = iord[ic1], jc2 = iord[ic2], jc3 = iord[ic3];
+    for (int i3 = 0; i3 <= len[ic3]; ++i3)
+      for (int i2 = 0; i2 <= len[ic2]; ++i2) {
+        int p1[4] = {0, 0, 0, 0}, p2[4] = {0, 0, 0, 0};
+        p1[ic1] = ibcpt; p1[ic2] = istr1[ic2] + isgn1[ic2] * i2; p1[ic3] = istr1[ic3] + isgn1[ic3] * i3;
+        p2[jc1] = inr; p2[jc2] = istr2[jc2] + isgn2[jc2] * i2; p2[jc3] = istr2[jc3] + isgn2[jc3] * i3;
+        for (int n = 0; n < L.S; ++n) {
+          m1(p1[1], p1[2], p1[3], n) = m2(p2[1], p2[2], p2[3], n);
+          int a1[4] = {0, p1[1], p1[2], p1[3]}, a2[4] = {0, p2[1], p2[2], p2[3]};
+          a1[ic1] += ibcinc; a2[jc1] += inrinc;
+          m1(a1[1], a1[2], a1[3], n) = m2(a2[1], a2[2], a2[3], n);
+        }
+      }
   }
 }
 
@@ -2225,6 +2644,17 @@ int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const d
                   double *dqp, double *dqm, double *flux, double *dtvol, int want_dt, double *bx, double *by,
                   double *bz, const double *vol = nullptr, const double *vm = nullptr);
 
+// arrays of the viscous / k-omega residual beyond cosa_level_ptrs: the face
+// inverse metrics, production, div u, delta+ and the turbulence IRS
+// coefficients
+struct VExtra {
+  const double *vm;
+  double *prd, *divvel, *delpls;
+  double *tbx, *tby, *tbz;
+};
+int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_ptrs &A, const VExtra &X,
+                  int want_dt);
+
 int orc_residual(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
                  const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
                  double *dqp, double *dqm, double *flux, double *dtvol, int want_dt) {
@@ -2236,47 +2666,90 @@ int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const d
                   const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
                   double *dqp, double *dqm, double *flux, double *dtvol, int want_dt, double *bx, double *by,
                   double *bz, const double *vol, const double *vm) {
+  cosa_level_ptrs A{};
+  A.q = q; A.res = res; A.dtvol = dtvol;
+  A.si = const_cast<double *>(si); A.sj = const_cast<double *>(sj); A.sk = const_cast<double *>(sk);
+  A.vol = const_cast<double *>(vol);
+  A.qp = qp; A.qm = qm; A.dq = dq; A.dqp = dqp; A.dqm = dqm; A.flux = flux;
+  A.betaxi = bx; A.betaeta = by; A.betazeta = bz;
+  VExtra X{};
+  X.vm = vm;
+  return residual_full(h, p, nl, A, X, want_dt);
+}
+
+/*
+ * One residual evaluation of smooth() (src/cosa.f90:1721-1908) on the
+ * arrays of A: Euler, laminar (viscous) or Wilcox k-omega (viscous + kom,
+ * with A.mut, A.dist, A.dtvolt and the source arrays of X).  q is left in
+ * conservative form, res holds the residual, and on want_dt the time steps
+ * (and IRS coefficients when the beta arrays are set).
+ */
+int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_ptrs &A, const VExtra &X,
+                  int want_dt) {
   Level &L = h->L;
-  const bool visc = p->viscous != 0;
-  if (visc && (!vol || !vm)) return COSA_ERR_ARG;
+  const bool visc = p->viscous != 0, kom = is_kom(*p);
+  if (p->kom_bsl || p->kom_sst) return COSA_ERR_UNSUPPORTED;
+  if (visc && (!A.vol || !X.vm)) return COSA_ERR_ARG;
+  if (kom && (!visc || !A.mut || !A.dist || !A.dtvolt || !X.prd || !X.divvel || !X.delpls)) return COSA_ERR_ARG;
+  double *q = A.q;
   for (int b = 0; b < L.nb; ++b) cons2prim_b(L, b, q, 0, *p);
-  int status = bc_level(L, q, si, sj, sk, *p);
+  int status = bc_level(L, q, A.si, A.sj, A.sk, *p, A.dist);
   cutman_q_level(L, q);
   status |= prtest_level(L, q, *p);
   if (want_dt) {
     if (visc) {
-      lambda_ns_level(L, q, si, sj, sk, vol, nullptr, qp, dq, *p);
-      deltat_ns_level(L, dtvol, qp, dq, bx, by, bz, *p);
+      lambda_ns_level(L, q, A.si, A.sj, A.sk, A.vol, kom ? A.mut : nullptr, A.qp, A.dq, *p);
+      deltat_ns_level(L, A.dtvol, A.qp, A.dq, A.betaxi, A.betaeta, A.betazeta, *p, kom ? A.dtvolt : nullptr,
+                      kom ? X.tbx : nullptr, kom ? X.tby : nullptr, kom ? X.tbz : nullptr);
     } else {
-      lambda_level(L, q, si, sj, sk, qp, *p);
-      deltat_level(L, dtvol, qp, bx, by, bz, *p);
+      lambda_level(L, q, A.si, A.sj, A.sk, A.qp, *p);
+      deltat_level(L, A.dtvol, A.qp, A.betaxi, A.betaeta, A.betazeta, *p);
     }
   }
-  zero_res(L, res);
+  zero_res(L, A.res);
   if (visc)
-    for (int b = 0; b < L.nb; ++b) q_bedges(L, b, q, nullptr);
-  const double *sd[4] = {nullptr, si, sj, sk};
+    for (int b = 0; b < L.nb; ++b) q_bedges(L, b, q, kom ? A.mut : nullptr);
+  const double *sd[4] = {nullptr, A.si, A.sj, A.sk};
   for (int d = 1; d <= 3; ++d) {
 #pragma omp parallel for schedule(dynamic)
-    for (int b = 0; b < L.nb; ++b) muscl_b(L, b, d, nl, q, qp, qm, dq, dqp, dqm, *p);
-    for (int b = 0; b < L.nb; ++b) roflux_b(L, b, d, qp, qm, flux, sd[d], *p);
+    for (int b = 0; b < L.nb; ++b) muscl_b(L, b, d, nl, q, A.qp, A.qm, A.dq, A.dqp, A.dqm, *p);
+    for (int b = 0; b < L.nb; ++b) roflux_b(L, b, d, A.qp, A.qm, A.flux, sd[d], *p);
 #pragma omp parallel for schedule(dynamic)
-    for (int b = 0; b < L.nb; ++b) resid_b(L, b, d, flux, res);
+    for (int b = 0; b < L.nb; ++b) resid_b(L, b, d, A.flux, A.res);
     if (visc) {
-      // q_face / q_der / vflux / resid (src/cosa.f90:1809-1824)
-      const double *a = vm + (int64_t)(d - 1) * 9 * L.n0;
+      // q_face / q_der / [rtst] / vflux / resid (src/cosa.f90:1809-1824)
+      const double *a = X.vm + (int64_t)(d - 1) * 9 * L.n0;
 #pragma omp parallel for schedule(dynamic)
       for (int b = 0; b < L.nb; ++b) {
-        q_face_b(L, b, d, q, dq);
-        q_der_b(L, b, d, q, qp, qm, dqm);
-        vflux_b(L, b, d, dq, qp, qm, dqm, a, a + 3 * L.n0, a + 6 * L.n0, sd[d], flux, *p);
-        resid_b(L, b, d, flux, res);
+        q_face_b(L, b, d, q, A.dq);
+        if (kom) q_face_mut_b(L, b, d, A.mut, A.flux);
+        q_der_b(L, b, d, q, A.qp, A.qm, A.dqm);
+        if (kom) {
+          rtst_b(L, b, d, A.dq, A.qp, A.qm, A.dqm, a, a + 3 * L.n0, a + 6 * L.n0, A.dqp, A.flux, *p);
+          vflux_kom_b(L, b, d, A.dq, A.qp, A.qm, A.dqm, A.dqp, a, a + 3 * L.n0, a + 6 * L.n0, sd[d], A.flux, *p);
+        }
+        vflux_b(L, b, d, A.dq, A.qp, A.qm, A.dqm, a, a + 3 * L.n0, a + 6 * L.n0, sd[d], A.flux, *p, kom);
+        resid_b(L, b, d, A.flux, A.res);
       }
     }
   }
+  if (kom) {
+    // cell-centred velocity gradients, production and the k-omega sources
+    // (src/cosa.f90:1878-1896)
+    double *dc[3] = {A.qp, A.qm, A.dqm};
+    for (int d = 1; d <= 3; ++d)
+      for (int b = 0; b < L.nb; ++b) {
+        q_face_b(L, b, d, q, A.dq);
+        q_der_c_b(L, b, d, A.dq, dc[d - 1]);
+      }
+    if (nl == 1 || p->prd_all_lvls)
+      for (int b = 0; b < L.nb; ++b)
+        turprod_b(L, b, q, A.qp, A.qm, A.dqm, X.vm, X.prd, X.divvel, X.delpls, *p);
+    for (int b = 0; b < L.nb; ++b) srckw_b(L, b, nl, q, A.mut, X.prd, X.divvel, A.res, A.vol, *p);
+  }
 #pragma omp parallel for schedule(dynamic)
   for (int b = 0; b < L.nb; ++b) prim2cons_b(L, b, q, *p);
-  if (p->harbal && vol) src_hb_level(L, q, vol, res, *p);
+  if (p->harbal && A.vol) src_hb_level(L, q, A.vol, A.res, *p);
   return status;
 }
 
@@ -2566,5 +3039,98 @@ int orc_smooth_ns(orc_level *h, const cosa_params *p, int ncycles, int mgit0, in
     }
   }
   return status;
+}
+
+// ---- k-omega ---------------------------------------------------------------
+/*
+ * Single-level RK cycles of smooth() for the viscous path with the Wilcox
+ * k-omega model (or laminar, when kom is off): residual_full per stage,
+ * implicit residual smoothing with the turbulence coefficients, the
+ * point-implicit k/omega update (update_b), fixq, and tur_vis + cutman_mut
+ * after the last stage (src/cosa.f90:1994-2016).  A.mut must hold the
+ * turbulent viscosity of the initial state (tur_vis + cutman_mut).
+ */
+int orc_smooth_rans(orc_level *h, const cosa_params *p, int ncycles, int mgit0, int rms_every,
+                    const cosa_level_ptrs *Ap, const double *vm, double *prd, double *divvel, double *delpls,
+                    double *tbx, double *tby, double *tbz, double *hist) {
+  Level &L = h->L;
+  const cosa_level_ptrs &A = *Ap;
+  VExtra X{vm, prd, divvel, delpls, tbx, tby, tbz};
+  const bool kom = is_kom(*p);
+  int status = 0;
+  const int last = mgit0 + ncycles - 1;
+  for (int mgit = mgit0; mgit <= last; ++mgit) {
+    const int iter = 1;
+    copy_interior(L, A.qold, A.q);
+    for (int irk = 1; irk <= p->nstage; ++irk) {
+      const bool want_dt = (iter / p->iupdt * p->iupdt == iter) && irk == 1;
+      status |= residual_full(h, p, 1, A, X, want_dt);
+      if (status & (COSA_ERR_ARG | COSA_ERR_UNSUPPORTED)) return status;
+      if (irk == 1 && (mgit == 1 || mgit % rms_every == 0 || mgit == last) && hist) {
+        if (p->harbal) resg_rms_hb_level(L, A.res, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
+        else resg_rms_level(L, A.res, A.rhs, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
+      }
+      if (p->irsop > 0)
+        irs_level(L, A.res, A.dtvol, kom ? A.dtvolt : nullptr, A.betaxi, A.betaeta, A.betazeta, X.tbx, X.tby, X.tbz,
+                  *p);
+#pragma omp parallel for schedule(dynamic)
+      for (int b = 0; b < L.nb; ++b) {
+        if (kom) update_kom_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p);
+        update_b(L, b, A.res, A.q, A.qold, A.dtvol, p->alphas[irk - 1]);
+      }
+      if (kom) {
+        if (p->ifixq) fixq_level(L, A.q, *p);
+        if (irk == p->nstage) {
+          tur_vis_level(L, A.q, A.mut, *p);
+          cutman_mut_level(L, A.mut);
+        }
+      }
+    }
+  }
+  return status;
+}
+int orc_residual_rans(orc_level *h, const cosa_params *p, int nl, const cosa_level_ptrs *A, const double *vm,
+                      double *prd, double *divvel, double *delpls, double *tbx, double *tby, double *tbz,
+                      int want_dt) {
+  VExtra X{vm, prd, divvel, delpls, tbx, tby, tbz};
+  return residual_full(h, p, nl, *A, X, want_dt);
+}
+void orc_cutman_mut(orc_level *h, double *mut) { cutman_mut_level(h->L, mut); }
+int orc_bc_dist(orc_level *h, const cosa_params *p, double *q, const double *si, const double *sj, const double *sk,
+                const double *dist) {
+  return bc_level(h->L, q, si, sj, sk, *p, dist);
+}
+void orc_q_face_mut(orc_level *h, int idir, const double *mut, double *flux) {
+  for (int b = 0; b < h->L.nb; ++b) q_face_mut_b(h->L, b, idir, mut, flux);
+}
+void orc_rtst(orc_level *h, const cosa_params *p, int idir, const double *qf, const double *dqxi, const double *dqeta,
+              const double *dqzeta, const double *vm, double *tau1, const double *flux) {
+  const double *a = vm + (int64_t)(idir - 1) * 9 * h->L.n0;
+  for (int b = 0; b < h->L.nb; ++b)
+    rtst_b(h->L, b, idir, qf, dqxi, dqeta, dqzeta, a, a + 3 * h->L.n0, a + 6 * h->L.n0, tau1, flux, *p);
+}
+void orc_vflux_kom(orc_level *h, const cosa_params *p, int idir, const double *qf, const double *dqxi,
+                   const double *dqeta, const double *dqzeta, const double *tau1, const double *vm,
+                   const double *sijk, double *flux) {
+  const double *a = vm + (int64_t)(idir - 1) * 9 * h->L.n0;
+  for (int b = 0; b < h->L.nb; ++b) {
+    vflux_kom_b(h->L, b, idir, qf, dqxi, dqeta, dqzeta, tau1, a, a + 3 * h->L.n0, a + 6 * h->L.n0, sijk, flux, *p);
+    vflux_b(h->L, b, idir, qf, dqxi, dqeta, dqzeta, a, a + 3 * h->L.n0, a + 6 * h->L.n0, sijk, flux, *p, true);
+  }
+}
+void orc_q_der_c(orc_level *h, int idir, const double *qf, double *dqc) {
+  for (int b = 0; b < h->L.nb; ++b) q_der_c_b(h->L, b, idir, qf, dqc);
+}
+void orc_turprod(orc_level *h, const cosa_params *p, const double *q, const double *dqxi, const double *dqeta,
+                 const double *dqzeta, const double *vm, double *prd, double *divvel, double *delpls) {
+  for (int b = 0; b < h->L.nb; ++b) turprod_b(h->L, b, q, dqxi, dqeta, dqzeta, vm, prd, divvel, delpls, *p);
+}
+void orc_srckw(orc_level *h, const cosa_params *p, int nl, const double *q, const double *mut, const double *prd,
+               const double *divvel, double *res, const double *vol) {
+  for (int b = 0; b < h->L.nb; ++b) srckw_b(h->L, b, nl, q, mut, prd, divvel, res, vol, *p);
+}
+void orc_update_kom(orc_level *h, const cosa_params *p, const double *res, double *q, const double *qold,
+                    const double *vol, const double *dtvolt, const double *delpls, const double *prd, double ar) {
+  for (int b = 0; b < h->L.nb; ++b) update_kom_b(h->L, b, res, q, qold, vol, dtvolt, delpls, prd, ar, *p);
 }
 }  // extern "C"

@@ -413,3 +413,82 @@ def smooth_ns(O, q, si, sj, sk, vol, vm, ncycles, mgit0=1, rms_every=1):
                              _p(qold), _p(si), _p(sj), _p(sk), _p(vol), _p(vm), _p(res), _p(rhs), _p(qp), _p(qm),
                              _p(dq), _p(dqp), _p(dqm), _p(flux), _p(dtvol), _p(bx), _p(by), _p(bz), _p(hist))
     return hist, st
+
+
+# ---- k-omega (Wilcox) ------------------------------------------------------------
+class RansArrays(LevelArrays):
+    """LevelArrays plus what the viscous / k-omega residual reads: mut (P3
+    scalar), dist (P1), dtvolt, the turbulence IRS coefficients, production,
+    div u, delta+ and the face inverse metrics vm (set by the caller)."""
+
+    def __init__(self, O):
+        super().__init__(O)
+        n3s = O.n3 * O.S
+        self.mut = np.zeros(n3s)
+        self.dist = O.p1()
+        self.dtvolt = O.p1(O.S)
+        self.prd, self.divvel, self.delpls = (np.zeros(n3s) for _ in range(3))
+        self.tbx, self.tby, self.tbz = (O.p1(O.S) for _ in range(3))
+        self.vm = None
+
+    def ptrs(self):
+        p = super().ptrs()
+        for n in ("mut", "dist", "dtvolt"):
+            setattr(p, n, _p(getattr(self, n)))
+        return p
+
+    def extras(self):
+        return (_p(self.vm), _p(self.prd), _p(self.divvel), _p(self.delpls), _p(self.tbx), _p(self.tby), _p(self.tbz))
+
+
+def smooth_rans(O, A, ncycles, mgit0=1, rms_every=1):
+    hist = np.full((ncycles, O.p.npde + 1), np.nan)
+    pt = A.ptrs()
+    st = lib().orc_smooth_rans(O.h, _par(O.p), C.c_int(ncycles), C.c_int(mgit0), C.c_int(rms_every), C.byref(pt),
+                               *A.extras(), _p(hist))
+    return hist, st
+
+
+def residual_rans(O, A, nl=1, want_dt=True):
+    pt = A.ptrs()
+    return lib().orc_residual_rans(O.h, _par(O.p), C.c_int(nl), C.byref(pt), *A.extras(), C.c_int(int(want_dt)))
+
+
+def cutman_mut(O, mut):
+    lib().orc_cutman_mut(O.h, _p(mut))
+
+
+def bc_dist(O, q, si, sj, sk, dist):
+    return lib().orc_bc_dist(O.h, _par(O.p), _p(q), _p(si), _p(sj), _p(sk), _p(dist))
+
+
+def q_face_mut(O, idir, mut, flux):
+    lib().orc_q_face_mut(O.h, C.c_int(idir), _p(mut), _p(flux))
+
+
+def rtst(O, idir, qf, dqxi, dqeta, dqzeta, vm, tau1, flux):
+    lib().orc_rtst(O.h, _par(O.p), C.c_int(idir), _p(qf), _p(dqxi), _p(dqeta), _p(dqzeta), _p(vm), _p(tau1),
+                   _p(flux))
+
+
+def vflux_kom(O, idir, qf, dqxi, dqeta, dqzeta, tau1, vm, sijk, flux):
+    lib().orc_vflux_kom(O.h, _par(O.p), C.c_int(idir), _p(qf), _p(dqxi), _p(dqeta), _p(dqzeta), _p(tau1), _p(vm),
+                        _p(sijk), _p(flux))
+
+
+def q_der_c(O, idir, qf, dqc):
+    lib().orc_q_der_c(O.h, C.c_int(idir), _p(qf), _p(dqc))
+
+
+def turprod(O, q, dqxi, dqeta, dqzeta, vm, prd, divvel, delpls):
+    lib().orc_turprod(O.h, _par(O.p), _p(q), _p(dqxi), _p(dqeta), _p(dqzeta), _p(vm), _p(prd), _p(divvel),
+                      _p(delpls))
+
+
+def srckw(O, nl, q, mut, prd, divvel, res, vol):
+    lib().orc_srckw(O.h, _par(O.p), C.c_int(nl), _p(q), _p(mut), _p(prd), _p(divvel), _p(res), _p(vol))
+
+
+def update_kom(O, res, q, qold, vol, dtvolt, delpls, prd, ar):
+    lib().orc_update_kom(O.h, _par(O.p), _p(res), _p(q), _p(qold), _p(vol), _p(dtvolt), _p(delpls), _p(prd),
+                         C.c_double(ar))
