@@ -16,6 +16,7 @@
 #include "fused.cuh"
 #include "mg.cuh"
 #include "visc.cuh"
+#include "kom.cuh"
 
 namespace {
 
@@ -60,6 +61,10 @@ struct LevelState {
   double *d_qprim = nullptr;  // primitive stage state (P3)
   double *d_vflux = nullptr;  // viscous face fluxes of the three families (3 x F0)
   double *d_vres = nullptr;   // viscous flux balance (P3)
+  // k-omega: production, div u, delta+ (scalar P3) and the turbulence IRS
+  // coefficients (P1 x S)
+  double *d_prd = nullptr, *d_divvel = nullptr, *d_delpls = nullptr;
+  double *d_tbeta[3] = {nullptr, nullptr, nullptr};
 };
 
 }  // namespace
@@ -180,7 +185,7 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
       const int type = r[0], idir = r[1], inrout = r[2];
       if (idir < 1 || idir > 3) return COSA_ERR_ARG;
       // viscous walls: the laminar, fixed-grid branch of bc_walvis_15
-      const bool wall15 = type / 100 == 15 && c->p.npde == 5 && !c->p.moving;
+      const bool wall15 = type / 100 == 15 && !c->p.moving;
       const bool ok = type == 80 || type == 4 || type == 14 || type == 21 || type == 91 || type == 30 || wall15;
       if (!ok) return COSA_ERR_UNSUPPORTED;
       int istrt[4] = {0, r[3], r[5], r[7]}, iend[4] = {0, r[4], r[6], r[8]};
@@ -474,7 +479,16 @@ int set_smem_attrs() {
   return COSA_OK;
 }
 
+// the k-omega stage runs routine by routine (launch_rans_iteration)
+int check_rans_supported(const cosa_params &p) {
+  if (p.npde != 7 || !p.kom || p.kom_bsl || p.kom_sst || !p.viscous || p.rkimp || p.moving || p.harbal ||
+      p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
+    return COSA_ERR_UNSUPPORTED;
+  return COSA_OK;
+}
+
 int check_fused_supported(const cosa_params &p) {
+  if (p.kom) return check_rans_supported(p);
   if (p.npde != 5 || p.kom || p.kom_bsl || p.kom_sst || p.rkimp || p.moving ||
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
@@ -559,15 +573,25 @@ int irs_scale(cosa_ctx *c, LevelState &L, double *res, const double *dtv, const 
 
 // cirs (cutcirs = 0) or scalef + 2 x (cutman_q + ccirs) + scaleb (cutcirs = 1)
 // of smooth() (src/cosa.f90:1977-1998) for the mean-flow equations
-int irs_apply(cosa_ctx *c, LevelState &L, double *res, double *ores, const double *dtv, const double *const beta[3]) {
+// k-omega (npde 7): dtvt scales the turbulence equations and their sweeps
+// use tbeta (irsop >= 2) or the constant coefficient (irsop 1)
+int irs_apply(cosa_ctx *c, LevelState &L, double *res, double *ores, const double *dtv, const double *const beta[3],
+              const double *dtvt = nullptr, const double *const tbeta[3] = nullptr) {
   const cosa_params &p = c->p;
   const double eps = 0.25 * (p.rat * p.rat - 1.0);
   const bool const_eps = p.irsop == 1;
+  const bool kom = p.npde > 5;
   const int S = 2 * p.nharms + 1;
-  int r = irs_scale(c, L, res, dtv, nullptr, 1);
+  auto sweeps = [&](const double *src, int with_halo) -> int {
+    if (const_eps) return irs_sweeps(c, L, res, src, nullptr, eps, 1, p.npde, with_halo);
+    int r2 = irs_sweeps(c, L, res, src, beta, eps, 1, 5, with_halo);
+    if (!r2 && kom) r2 = irs_sweeps(c, L, res, src, tbeta, 0.0, 6, p.npde, with_halo);
+    return r2;
+  };
+  int r = irs_scale(c, L, res, dtv, kom ? dtvt : nullptr, 1);
   if (r) return r;
   if (p.cutcirs == 0) {
-    if ((r = irs_sweeps(c, L, res, nullptr, const_eps ? nullptr : beta, eps, 1, 5, 0))) return r;
+    if ((r = sweeps(nullptr, 0))) return r;
   } else {
     CK(cudaMemcpyAsync(ores, res, (size_t)L.n3 * p.npde * S * sizeof(double), cudaMemcpyDeviceToDevice, c->s));
     const int ncut = (int)L.items.size() - L.n_bc_items;
@@ -577,10 +601,10 @@ int irs_apply(cosa_ctx *c, LevelState &L, double *res, double *ores, const doubl
                                                                     res, nullptr, nullptr, nullptr, c->d_status);
         if ((r = after_launch(c))) return r;
       }
-      if ((r = irs_sweeps(c, L, res, ores, const_eps ? nullptr : beta, eps, 1, 5, 1))) return r;
+      if ((r = sweeps(ores, 1))) return r;
     }
   }
-  return irs_scale(c, L, res, dtv, nullptr, 0);
+  return irs_scale(c, L, res, dtv, kom ? dtvt : nullptr, 0);
 }
 
 // profiling: close the event pair of kernel class `k` and accumulate its time
@@ -722,9 +746,12 @@ struct IterOpts {
   double *res_only = nullptr;  // residual pass of to_coarse: stage-1 residual here, no update
 };
 
+int launch_rans_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o);
+
 // one RK iteration (nstage stages) of the fused path
 int launch_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
   const cosa_params &p = c->p;
+  if (p.kom) return launch_rans_iteration(c, nl, L, o);
   double *Q = L.ptrs.q, *T = L.d_T, *QO = L.ptrs.qold;
   const int S = 2 * p.nharms + 1;
   if (o.res_only) {
@@ -811,6 +838,30 @@ int run_graph(cosa_ctx *c, uint64_t key, F &&issue) {
   const long long per = g.launches;
   CK(cudaGraphLaunch(g.exec, c->s));
   c->launches += per;
+  return COSA_OK;
+}
+
+// the k-omega work arrays beyond the bound level pointers
+int ensure_rans(cosa_ctx *c, LevelState &L) {
+  const cosa_level_ptrs &P = L.ptrs;
+  if (!P.res || !P.dtvolt || !P.qp || !P.qm || !P.dq || !P.dqp || !P.dqm || !P.flux || !P.mut || !P.dist ||
+      !P.vol || !L.d_vm)
+    return COSA_ERR_ARG;
+  const int S = 2 * c->p.nharms + 1;
+  int r = 0;
+  for (double **a : {&L.d_prd, &L.d_divvel, &L.d_delpls})
+    if (!*a) {
+      if ((r = dalloc(c, a, (size_t)L.n3 * S))) return r;
+      CK(cudaMemset(*a, 0, (size_t)L.n3 * S * sizeof(double)));
+    }
+  for (auto &t : L.d_tbeta)
+    if (!t && (r = dalloc(c, &t, (size_t)L.n1 * S))) return r;
+  if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, L))) return r;
+  if (L.npart_cap < L.nb * 64) {  // per-block norm partials of the routine-by-routine stage
+    drop_graphs(c);
+    if ((r = dalloc(c, &L.d_part, (size_t)L.nb * 64 * 8))) return r;
+    L.npart_cap = L.nb * 64;
+  }
   return COSA_OK;
 }
 
@@ -957,13 +1008,13 @@ int cosa_gpu_prim2cons(cosa_ctx *c, int32_t nl, double *q) {
 }
 
 int cosa_gpu_bc(cosa_ctx *c, int32_t nl, double *q, const double *si, const double *sj, const double *sk,
-                const double *) {
+                const double *dist) {
   LevelState *L = level(c, nl);
   if (!L || !q) return COSA_ERR_ARG;
   if (L->n_bc_items == 0) return COSA_OK;
   const int S = 2 * c->p.nharms + 1;
   k_halo<false><<<grid_for((int64_t)L->n_bc_items * S), 256, 0, c->s>>>(L->d_blocks, L->d_items, L->n_bc_items,
-                                                                       c->d_p, q, si, sj, sk, c->d_status);
+                                                                       c->d_p, q, si, sj, sk, c->d_status, dist);
   return after_launch(c);
 }
 
@@ -1053,7 +1104,7 @@ int cosa_gpu_update(cosa_ctx *c, int32_t nl, const double *res, double *q, const
                     double ar) {
   LevelState *L = level(c, nl);
   if (!L || !res || !q || !qold || !dtvol) return COSA_ERR_ARG;
-  if (c->p.kom || c->p.harbal || c->p.rkimp) return COSA_ERR_UNSUPPORTED;
+  if (c->p.harbal || c->p.rkimp) return COSA_ERR_UNSUPPORTED;
   return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
     k_update<<<g, 256, 0, c->s>>>(b, c->d_p, res, q, qold, dtvol, ar);
   });
@@ -1100,6 +1151,7 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
   if (!P.q || !P.qold || !P.dtvol || !P.si || !P.sj || !P.sk) return COSA_ERR_ARG;
   if (c->p.harbal && !P.vol) return COSA_ERR_ARG;
   if (c->p.viscous && (!P.vol || !L->d_vm)) return COSA_ERR_ARG;
+  if (c->p.kom && (r = ensure_rans(c, *L))) return r;
   cudaSetDevice(c->device);
   const int npde = c->p.npde;
   // schedule of printed iterations (src/cosa.f90:1925-1927)
@@ -1833,20 +1885,31 @@ int cosa_gpu_viscous_setup(cosa_ctx *c, int32_t nl, double *x, double *y, double
 int cosa_gpu_q_face(cosa_ctx *c, int32_t idir, int32_t nl, const double *q, double *qf) {
   LevelState *L = level(c, nl);
   if (!L || idir < 1 || idir > 3 || !q || !qf) return COSA_ERR_ARG;
-  if (c->p.npde != 5) return COSA_ERR_UNSUPPORTED;
   const int S = 2 * c->p.nharms + 1;
   for (const DevBlock &b : L->hb) {
     const int g = grid_for((int64_t)b.im * b.jm * b.km * S);
-    if (idir == 1) k_qface_qder<1><<<g, 256, 0, c->s>>>(b, S, q, qf, nullptr, nullptr, nullptr);
-    else if (idir == 2) k_qface_qder<2><<<g, 256, 0, c->s>>>(b, S, q, qf, nullptr, nullptr, nullptr);
-    else k_qface_qder<3><<<g, 256, 0, c->s>>>(b, S, q, qf, nullptr, nullptr, nullptr);
+    const bool k7 = c->p.npde == 7;
+    if (idir == 1) {
+      if (k7) k_qface_qder<1, 7><<<g, 256, 0, c->s>>>(b, S, q, qf, nullptr, nullptr, nullptr);
+      else k_qface_qder<1, 5><<<g, 256, 0, c->s>>>(b, S, q, qf, nullptr, nullptr, nullptr);
+    } else if (idir == 2) {
+      if (k7) k_qface_qder<2, 7><<<g, 256, 0, c->s>>>(b, S, q, qf, nullptr, nullptr, nullptr);
+      else k_qface_qder<2, 5><<<g, 256, 0, c->s>>>(b, S, q, qf, nullptr, nullptr, nullptr);
+    } else {
+      if (k7) k_qface_qder<3, 7><<<g, 256, 0, c->s>>>(b, S, q, qf, nullptr, nullptr, nullptr);
+      else k_qface_qder<3, 5><<<g, 256, 0, c->s>>>(b, S, q, qf, nullptr, nullptr, nullptr);
+    }
     int r = after_launch(c);
     if (r) return r;
   }
   if (L->walls.empty()) return COSA_OK;
   const int nw = (int)L->walls.size();
-  k_qwall<<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L->d_blocks, L->d_walls, nw, idir, S, q, qf, nullptr, nullptr,
-                                                       nullptr);
+  if (c->p.npde == 7)
+    k_qwall<7><<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L->d_blocks, L->d_walls, nw, idir, S, q, qf, nullptr,
+                                                            nullptr, nullptr);
+  else
+    k_qwall<5><<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L->d_blocks, L->d_walls, nw, idir, S, q, qf, nullptr,
+                                                            nullptr, nullptr);
   return after_launch(c);
 }
 
@@ -1854,20 +1917,31 @@ int cosa_gpu_q_der(cosa_ctx *c, int32_t idir, int32_t nl, const double *q, doubl
                    double *dqzeta) {
   LevelState *L = level(c, nl);
   if (!L || idir < 1 || idir > 3 || !q || !dqxi || !dqeta || !dqzeta) return COSA_ERR_ARG;
-  if (c->p.npde != 5) return COSA_ERR_UNSUPPORTED;
   const int S = 2 * c->p.nharms + 1;
   for (const DevBlock &b : L->hb) {
     const int g = grid_for((int64_t)b.im * b.jm * b.km * S);
-    if (idir == 1) k_qface_qder<1><<<g, 256, 0, c->s>>>(b, S, q, nullptr, dqxi, dqeta, dqzeta);
-    else if (idir == 2) k_qface_qder<2><<<g, 256, 0, c->s>>>(b, S, q, nullptr, dqxi, dqeta, dqzeta);
-    else k_qface_qder<3><<<g, 256, 0, c->s>>>(b, S, q, nullptr, dqxi, dqeta, dqzeta);
+    const bool k7 = c->p.npde == 7;
+    if (idir == 1) {
+      if (k7) k_qface_qder<1, 7><<<g, 256, 0, c->s>>>(b, S, q, nullptr, dqxi, dqeta, dqzeta);
+      else k_qface_qder<1, 5><<<g, 256, 0, c->s>>>(b, S, q, nullptr, dqxi, dqeta, dqzeta);
+    } else if (idir == 2) {
+      if (k7) k_qface_qder<2, 7><<<g, 256, 0, c->s>>>(b, S, q, nullptr, dqxi, dqeta, dqzeta);
+      else k_qface_qder<2, 5><<<g, 256, 0, c->s>>>(b, S, q, nullptr, dqxi, dqeta, dqzeta);
+    } else {
+      if (k7) k_qface_qder<3, 7><<<g, 256, 0, c->s>>>(b, S, q, nullptr, dqxi, dqeta, dqzeta);
+      else k_qface_qder<3, 5><<<g, 256, 0, c->s>>>(b, S, q, nullptr, dqxi, dqeta, dqzeta);
+    }
     int r = after_launch(c);
     if (r) return r;
   }
   if (L->walls.empty()) return COSA_OK;
   const int nw = (int)L->walls.size();
-  k_qwall<<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L->d_blocks, L->d_walls, nw, idir, S, q, nullptr, dqxi, dqeta,
-                                                       dqzeta);
+  if (c->p.npde == 7)
+    k_qwall<7><<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L->d_blocks, L->d_walls, nw, idir, S, q, nullptr, dqxi,
+                                                            dqeta, dqzeta);
+  else
+    k_qwall<5><<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L->d_blocks, L->d_walls, nw, idir, S, q, nullptr, dqxi,
+                                                            dqeta, dqzeta);
   return after_launch(c);
 }
 
@@ -1887,25 +1961,266 @@ int cosa_gpu_vflux(cosa_ctx *c, int32_t idir, int32_t nl, const double *qf, cons
 }
 
 int cosa_gpu_lambda_ns(cosa_ctx *c, int32_t nl, const double *q, const double *si, const double *sj, const double *sk,
-                       const double *vol, double *lam, double *lamv) {
+                       const double *vol, const double *mut, double *lam, double *lamv) {
   LevelState *L = level(c, nl);
   if (!L || !q || !si || !sj || !sk || !vol || !lam || !lamv) return COSA_ERR_ARG;
-  if (c->p.npde != 5 || c->p.moving) return COSA_ERR_UNSUPPORTED;
+  if (c->p.moving) return COSA_ERR_UNSUPPORTED;
   return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
-    k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, vol, lam, lamv);
+    k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, vol, c->p.kom ? mut : nullptr, lam, lamv);
   });
 }
 
 int cosa_gpu_deltat_ns(cosa_ctx *c, int32_t nl, double *dtvol, const double *lam, const double *lamv, double *bx,
-                       double *by, double *bz) {
+                       double *by, double *bz, double *dtvolt, double *tbx, double *tby, double *tbz) {
   LevelState *L = level(c, nl);
   if (!L || !dtvol || !lam || !lamv) return COSA_ERR_ARG;
-  if (c->p.npde != 5) return COSA_ERR_UNSUPPORTED;
   return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
-    k_deltat_ns<<<g, 256, 0, c->s>>>(b, c->d_p, dtvol, lam, lamv, bx, by, bz);
+    k_deltat_ns<<<g, 256, 0, c->s>>>(b, c->d_p, dtvol, lam, lamv, bx, by, bz, c->p.kom ? dtvolt : nullptr,
+                                     c->p.kom ? tbx : nullptr, tby, tbz);
   });
 }
 
 }  // extern "C"
+
+// ---- Wilcox k-omega path ------------------------------------------------------------------
+extern "C" {
+
+int cosa_gpu_q_face_mut(cosa_ctx *c, int32_t idir, int32_t nl, const double *mut, double *flux) {
+  LevelState *L = level(c, nl);
+  if (!L || idir < 1 || idir > 3 || !mut || !flux) return COSA_ERR_ARG;
+  const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
+  for (const DevBlock &b : L->hb) {
+    const int g = grid_for((int64_t)b.im * b.jm * b.km * S);
+    if (idir == 1) k_qface_mut<1><<<g, 256, 0, c->s>>>(b, npde, S, mut, flux);
+    else if (idir == 2) k_qface_mut<2><<<g, 256, 0, c->s>>>(b, npde, S, mut, flux);
+    else k_qface_mut<3><<<g, 256, 0, c->s>>>(b, npde, S, mut, flux);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  if (L->walls.empty()) return COSA_OK;
+  const int nw = (int)L->walls.size();
+  k_qwall_mut<<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L->d_blocks, L->d_walls, nw, idir, npde, S, mut, flux);
+  return after_launch(c);
+}
+
+int cosa_gpu_rtst(cosa_ctx *c, int32_t idir, int32_t nl, const double *qf, const double *dqxi, const double *dqeta,
+                  const double *dqzeta, const double *vm, const double *flux, double *tau1) {
+  LevelState *L = level(c, nl);
+  if (!L || idir < 1 || idir > 3 || !qf || !dqxi || !dqeta || !dqzeta || !vm || !flux || !tau1) return COSA_ERR_ARG;
+  if (c->p.npde != 7) return COSA_ERR_UNSUPPORTED;
+  for (const DevBlock &b : L->hb) {
+    k_rtst<<<grid_for((int64_t)b.im * b.jm * b.km * (2 * c->p.nharms + 1)), 256, 0, c->s>>>(
+        b, idir, c->d_p, qf, dqxi, dqeta, dqzeta, vm, L->n0, flux, tau1);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_vflux_kom(cosa_ctx *c, int32_t idir, int32_t nl, const double *qf, const double *dqxi,
+                       const double *dqeta, const double *dqzeta, const double *tau1, const double *vm,
+                       const double *sijk, double *flux) {
+  LevelState *L = level(c, nl);
+  if (!L || idir < 1 || idir > 3 || !qf || !dqxi || !dqeta || !dqzeta || !tau1 || !vm || !sijk || !flux)
+    return COSA_ERR_ARG;
+  if (c->p.npde != 7 || !c->p.kom || c->p.moving) return COSA_ERR_UNSUPPORTED;
+  for (const DevBlock &b : L->hb) {
+    k_vflux_kom<<<grid_for((int64_t)b.im * b.jm * b.km * (2 * c->p.nharms + 1)), 256, 0, c->s>>>(
+        b, idir, c->d_p, qf, dqxi, dqeta, dqzeta, tau1, vm, L->n0, sijk, flux);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_q_der_c(cosa_ctx *c, int32_t idir, int32_t nl, const double *qf, double *dqc) {
+  LevelState *L = level(c, nl);
+  if (!L || idir < 1 || idir > 3 || !qf || !dqc) return COSA_ERR_ARG;
+  const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
+  for (const DevBlock &b : L->hb) {
+    const int g = grid_for((int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * S);
+    if (idir == 1) k_qder_c<1><<<g, 256, 0, c->s>>>(b, npde, S, qf, dqc);
+    else if (idir == 2) k_qder_c<2><<<g, 256, 0, c->s>>>(b, npde, S, qf, dqc);
+    else k_qder_c<3><<<g, 256, 0, c->s>>>(b, npde, S, qf, dqc);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_turprod(cosa_ctx *c, int32_t nl, const double *dqxi, const double *dqeta, const double *dqzeta,
+                     const double *vm, double *prd, double *divvel, double *delpls) {
+  LevelState *L = level(c, nl);
+  if (!L || !dqxi || !dqeta || !dqzeta || !vm || !prd || !divvel || !delpls) return COSA_ERR_ARG;
+  for (const DevBlock &b : L->hb) {
+    k_turprod<<<grid_for((int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * (2 * c->p.nharms + 1)), 256, 0, c->s>>>(
+        b, c->d_p, dqxi, dqeta, dqzeta, vm, L->n0, prd, divvel, delpls);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_srckw(cosa_ctx *c, int32_t nl, const double *q, const double *mut, const double *prd,
+                   const double *divvel, double *res, const double *vol) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !mut || !prd || !divvel || !res || !vol) return COSA_ERR_ARG;
+  if (c->p.npde != 7) return COSA_ERR_UNSUPPORTED;
+  for (const DevBlock &b : L->hb) {
+    k_srckw<<<grid_for((int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * (2 * c->p.nharms + 1)), 256, 0, c->s>>>(
+        b, c->d_p, nl, q, mut, prd, divvel, res, vol);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_update_kom(cosa_ctx *c, int32_t nl, const double *res, double *q, const double *qold, const double *vol,
+                        const double *dtvolt, const double *delpls, const double *prd, double ar) {
+  LevelState *L = level(c, nl);
+  if (!L || !res || !q || !qold || !vol || !dtvolt || !delpls || !prd) return COSA_ERR_ARG;
+  if (c->p.npde != 7 || c->p.rkimp) return COSA_ERR_UNSUPPORTED;
+  for (const DevBlock &b : L->hb) {
+    k_update_kom<<<grid_for((int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * (2 * c->p.nharms + 1)), 256, 0, c->s>>>(
+        b, c->d_p, res, q, qold, vol, dtvolt, delpls, prd, ar);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_cutman_mut(cosa_ctx *c, int32_t nl, double *mut) {
+  LevelState *L = level(c, nl);
+  if (!L || !mut) return COSA_ERR_ARG;
+  const int ncut = (int)L->items.size() - L->n_bc_items;
+  if (ncut == 0) return COSA_OK;
+  const int S = 2 * c->p.nharms + 1;
+  k_cut_scalar<<<grid_for((int64_t)ncut * S), 256, 0, c->s>>>(L->d_blocks, L->d_items + L->n_bc_items, ncut, S, mut);
+  return after_launch(c);
+}
+
+}  // extern "C"
+
+namespace {
+
+// q_face (calmut off) of family d into qf and, when g0 is set, q_der into
+// g0..g2, bulk faces then strong-boundary faces, for npde = 7
+int rans_face_state(cosa_ctx *c, LevelState &L, int d, const double *q, double *qf, double *g0, double *g1,
+                    double *g2) {
+  const int S = 2 * c->p.nharms + 1;
+  for (const DevBlock &b : L.hb) {
+    const int g = grid_for((int64_t)b.im * b.jm * b.km * S);
+    if (d == 1) k_qface_qder<1, 7><<<g, 256, 0, c->s>>>(b, S, q, qf, g0, g1, g2);
+    else if (d == 2) k_qface_qder<2, 7><<<g, 256, 0, c->s>>>(b, S, q, qf, g0, g1, g2);
+    else k_qface_qder<3, 7><<<g, 256, 0, c->s>>>(b, S, q, qf, g0, g1, g2);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  if (L.walls.empty()) return COSA_OK;
+  const int nw = (int)L.walls.size();
+  k_qwall<7><<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L.d_blocks, L.d_walls, nw, d, S, q, qf, g0, g1, g2);
+  return after_launch(c);
+}
+
+// one RK stage of the k-omega path, routine by routine as smooth() runs it
+// (src/cosa.f90:1719-2016): every kernel is a full-array pass with the
+// reference's arrays, captured with the rest of the iteration in a graph
+int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, bool compute_dt, bool want_rms, bool copy_qold) {
+  const cosa_params &p = c->p;
+  const int S = 2 * p.nharms + 1, npde = p.npde;
+  const cosa_level_ptrs &P = L.ptrs;
+  double *q = P.q;
+  int r = 0;
+  if (irk == 1 && copy_qold)
+    for (const DevBlock &x : L.hb) {
+      k_copy_interior<<<grid_for((int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * npde * S), 256, 0, c->s>>>(
+          x, npde * S, q, P.qold);
+      if ((r = after_launch(c))) return r;
+    }
+  if ((r = cosa_gpu_cons2prim(c, nl, 0, q))) return r;
+  if (!L.items.empty()) {
+    // BC patches then cuts, last writers as in the reference
+    k_halo<false><<<grid_for((int64_t)L.items.size() * S), 256, 0, c->s>>>(
+        L.d_blocks, L.d_items, (int)L.items.size(), c->d_p, q, P.si, P.sj, P.sk, c->d_status, P.dist);
+    if ((r = after_launch(c))) return r;
+  }
+  for (const DevBlock &b : L.hb) {
+    k_prtest<<<grid_for(cnt_all(b, p)), 256, 0, c->s>>>(b, c->d_p, q, c->d_status);
+    if ((r = after_launch(c))) return r;
+  }
+  if (compute_dt) {
+    for (const DevBlock &b : L.hb) {
+      const int g = grid_for(cnt_interior(b, p));
+      k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.si, P.sj, P.sk, P.vol, P.mut, P.qp, P.dq);
+      if ((r = after_launch(c))) return r;
+      const bool irs = p.irsop >= 2 && p.irsop != 4;
+      k_deltat_ns<<<g, 256, 0, c->s>>>(b, c->d_p, P.dtvol, P.qp, P.dq, irs ? P.betaxi : nullptr, P.betaeta,
+                                       P.betazeta, P.dtvolt, irs ? L.d_tbeta[0] : nullptr, L.d_tbeta[1],
+                                       L.d_tbeta[2]);
+      if ((r = after_launch(c))) return r;
+    }
+  }
+  if ((r = cosa_gpu_zero(c, nl, P.res))) return r;
+  if ((r = launch_edges(c, L, q, P.mut))) return r;
+  const double *sd[4] = {nullptr, P.si, P.sj, P.sk};
+  for (int d = 1; d <= 3; ++d) {
+    if ((r = cosa_gpu_muscl(c, d, nl, q, P.qp, P.qm, P.dq, P.dqp, P.dqm))) return r;
+    if ((r = cosa_gpu_roflux(c, d, nl, P.qp, P.qm, P.flux, sd[d]))) return r;
+    if ((r = cosa_gpu_resid(c, d, nl, P.flux, P.res))) return r;
+    // q_face (+ face mut) / q_der / rtst / vflux / resid (src/cosa.f90:1809-1824)
+    if ((r = rans_face_state(c, L, d, q, P.dq, nullptr, nullptr, nullptr))) return r;
+    if ((r = cosa_gpu_q_face_mut(c, d, nl, P.mut, P.flux))) return r;
+    if ((r = rans_face_state(c, L, d, q, nullptr, P.qp, P.qm, P.dqm))) return r;
+    if ((r = cosa_gpu_rtst(c, d, nl, P.dq, P.qp, P.qm, P.dqm, L.d_vm, P.flux, P.dqp))) return r;
+    if ((r = cosa_gpu_vflux_kom(c, d, nl, P.dq, P.qp, P.qm, P.dqm, P.dqp, L.d_vm, sd[d], P.flux))) return r;
+    if ((r = cosa_gpu_resid(c, d, nl, P.flux, P.res))) return r;
+  }
+  // cell-centred velocity gradients, production and sources (src/cosa.f90:1878-1896)
+  double *dc[3] = {P.qp, P.qm, P.dqm};
+  for (int d = 1; d <= 3; ++d) {
+    if ((r = rans_face_state(c, L, d, q, P.dq, nullptr, nullptr, nullptr))) return r;
+    if ((r = cosa_gpu_q_der_c(c, d, nl, P.dq, dc[d - 1]))) return r;
+  }
+  if (nl == 1 || p.prd_all_lvls)
+    if ((r = cosa_gpu_turprod(c, nl, P.qp, P.qm, P.dqm, L.d_vm, L.d_prd, L.d_divvel, L.d_delpls))) return r;
+  if ((r = cosa_gpu_srckw(c, nl, q, P.mut, L.d_prd, L.d_divvel, P.res, P.vol))) return r;
+  if ((r = cosa_gpu_prim2cons(c, nl, q))) return r;
+  if (want_rms) {
+    for (int b = 0; b < L.nb; ++b) {
+      k_rms_partial<<<64, 256, 0, c->s>>>(L.hb[b], c->d_p, P.res, nullptr, L.d_part + (int64_t)b * 64 * 8);
+      if ((r = after_launch(c))) return r;
+    }
+    int64_t ncell = 0;
+    for (auto &b : L.hb) ncell += (int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1);
+    k_rms_final<<<1, 256, 0, c->s>>>(L.d_part, L.nb * 64, npde, (double)ncell, c->d_hist, c->d_row, c->hist_cap);
+    if ((r = after_launch(c))) return r;
+  }
+  if (p.irsop > 0) {
+    const double *beta[3] = {P.betaxi ? P.betaxi : L.d_beta[0], P.betaeta ? P.betaeta : L.d_beta[1],
+                             P.betazeta ? P.betazeta : L.d_beta[2]};
+    const double *tbeta[3] = {L.d_tbeta[0], L.d_tbeta[1], L.d_tbeta[2]};
+    if ((r = irs_apply(c, L, P.res, L.d_ores, P.dtvol, beta, P.dtvolt, tbeta))) return r;
+  }
+  if ((r = cosa_gpu_update_kom(c, nl, P.res, q, P.qold, P.vol, P.dtvolt, L.d_delpls, L.d_prd, p.alphas[irk - 1])))
+    return r;
+  if ((r = cosa_gpu_update(c, nl, P.res, q, P.qold, P.dtvol, p.alphas[irk - 1]))) return r;
+  if (p.ifixq && (r = cosa_gpu_fixq(c, nl, q))) return r;
+  if (irk == p.nstage && (nl == 1 || !p.prd_all_lvls)) {
+    if ((r = cosa_gpu_tur_vis(c, nl, q, P.mut))) return r;
+    if ((r = cosa_gpu_cutman_mut(c, nl, P.mut))) return r;
+  }
+  return COSA_OK;
+}
+
+int launch_rans_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
+  if (o.rhs || o.res_only) return COSA_ERR_UNSUPPORTED;  // k-omega multigrid is not on this path
+  for (int irk = 1; irk <= c->p.nstage; ++irk) {
+    int r = launch_rans_stage(c, nl, L, irk, o.compute_dt && irk == 1, o.want_rms && irk == 1, o.copy_qold);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+}  // namespace
 
 #include "serve.cuh"

@@ -63,7 +63,7 @@ template <bool CONS>
 __global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__restrict__ items, int nitems,
                        const cosa_params *__restrict__ Pp, double *__restrict__ q,
                        const double *__restrict__ si, const double *__restrict__ sj,
-                       const double *__restrict__ sk, int *status) {
+                       const double *__restrict__ sk, int *status, const double *__restrict__ dist = nullptr) {
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
   const int64_t total = (int64_t)nitems * S;
@@ -88,7 +88,7 @@ __global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__re
       mask = 3;
     } else {
       double nx = 0, ny = 0, nz = 0;
-      if (it.type == 14 || it.type == 21 || it.type == 30) {
+      if (it.type == 14 || it.type == 21 || it.type == 30 || (it.type / 100 == 15 && npde > 5)) {
         const double *s = it.idir == 1 ? si : (it.idir == 2 ? sj : sk);
         const int nh = n * P.hbmove;
         const int64_t I2 = db.im + 2, J2 = db.jm + 2, K2 = db.km + 2;
@@ -105,8 +105,19 @@ __global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__re
         case 91: mask = bc_outsub(B, c1, c2, h1, h2); break;
         case 30: mask = bc_far0(B, nx, ny, nz, c1, h1, h2); break;
         default:
-          if (it.type / 100 == 15) mask = bc_walvis(P.gamma, c1, c2, h1, h2);
-          else st |= COSA_ERR_UNSUPPORTED;
+          if (it.type / 100 == 15) {
+            mask = bc_walvis(P.gamma, c1, c2, h1, h2);
+            if (npde > 5) {
+              // k-omega wall values from the wall distance of the first cell
+              if (!dist) { st |= COSA_ERR_ARG; break; }
+              const int64_t I3 = db.I3, J3 = db.J3;
+              const int ci = (int)(it.c1 % I3) - 1, cj = (int)((it.c1 / I3) % J3) - 1;
+              const int ck = (int)(it.c1 / (I3 * J3)) - 1;
+              bc_walvis_kom(P, nx, ny, nz, dist[p1_idx(db, 1, ci, cj, ck, 0)], c1, h1, h2);
+            }
+          } else {
+            st |= COSA_ERR_UNSUPPORTED;
+          }
           break;
       }
       if (err) st |= COSA_ERR_INFLOW;

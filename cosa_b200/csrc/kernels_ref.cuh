@@ -280,6 +280,26 @@ __global__ void k_roflux(DevBlock b, const cosa_params *__restrict__ Pp, int d, 
     roe_flux_fp64(ph, sijk[p2_idx(b, S2, 1, i, j, k, nh)], sijk[p2_idx(b, S2, 2, i, j, k, nh)],
                   sijk[p2_idx(b, S2, 3, i, j, k, nh)], sijk[p2_idx(b, S2, 4, i, j, k, nh)], vr, vl, tker, tkel, f);
     for (int m = 0; m < 5; ++m) flux[f0_idx(b, npde, S, i, j, k, m + 1, n)] = f[m];
+    if (kom) {
+      // turbulence fluxes (src/flux.f90:249-380) with the mean-flow loop's
+      // final h0l/h0r: those of the last face (ic,jc,kc) of this snapshot
+      double a7[7], b7[7], tr[7], tl[7];
+      const int64_t cl = p3_cell(b, ic, jc, kc);
+      for (int m = 0; m < 6; ++m) {
+        a7[m] = qr[p3_var(b, npde, S, m + 1, n) + cl];
+        b7[m] = ql[p3_var(b, npde, S, m + 1, n) + cl];
+      }
+      for (int m = 0; m < 7; ++m) {
+        tr[m] = qr[p3_var(b, npde, S, m + 1, n) + c];
+        tl[m] = ql[p3_var(b, npde, S, m + 1, n) + c];
+      }
+      double fk, fw;
+      roe_turb(P, sijk[p2_idx(b, S2, 1, i, j, k, nh)], sijk[p2_idx(b, S2, 2, i, j, k, nh)],
+               sijk[p2_idx(b, S2, 3, i, j, k, nh)], sijk[p2_idx(b, S2, 4, i, j, k, nh)], tr, tl,
+               face_h0(P.gamma, a7), face_h0(P.gamma, b7), fk, fw);
+      flux[f0_idx(b, npde, S, i, j, k, 6, n)] = fk;
+      flux[f0_idx(b, npde, S, i, j, k, 7, n)] = fw;
+    }
   }
 }
 

@@ -1,0 +1,272 @@
+// Wilcox k-omega terms of the B200 path (kom = .true., viscous, fixed grid),
+// with the reference's array contract (one kernel per routine, the level
+// drivers in cosa_gpu.cu loop over blocks like the Fortran drivers).
+//
+//   k_qface_mut       q_face with calmut: face mut into flux(.,1)
+//   k_rtst            b_rtst: Reynolds stresses on the faces
+//   k_vflux_kom       vflux_b, k-omega branch + laminar terms
+//   k_qder_c          q_der_c: cell-centred velocity differences
+//   k_turprod         turprod_b: production, div u, delta+
+//   k_srckw           srckw_b: k and omega sources into res
+//   k_update_kom      update_b's point-implicit k / omega update
+//   k_cut_scalar      cut_q on a scalar P3 array (cutman_mut)
+#pragma once
+#include "visc.cuh"
+
+// ---- per-routine kernels ---------------------------------------------------------------
+// one thread per face (i,j,k) of family D and snapshot
+#define KOM_FACE_LOOP(D)                                                                                    \
+  const int ni = (D) == 1 ? b.im : b.im - 1, nj = (D) == 2 ? b.jm : b.jm - 1, nk = (D) == 3 ? b.km : b.km - 1; \
+  const int64_t total = (int64_t)ni * nj * nk * S;                                                          \
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;                              \
+       t += (int64_t)gridDim.x * blockDim.x) {                                                              \
+    int64_t r_ = t;                                                                                         \
+    const int i = (int)(r_ % ni) + 1; r_ /= ni;                                                             \
+    const int j = (int)(r_ % nj) + 1; r_ /= nj;                                                             \
+    const int k = (int)(r_ % nk) + 1;                                                                       \
+    const int n = (int)(r_ / nk);
+
+#define KOM_CELL_LOOP                                                                                       \
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;                                                    \
+  const int64_t total = (int64_t)ni * nj * nk * S;                                                          \
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;                              \
+       t += (int64_t)gridDim.x * blockDim.x) {                                                              \
+    int64_t r_ = t;                                                                                         \
+    const int i = (int)(r_ % ni) + 1; r_ /= ni;                                                             \
+    const int j = (int)(r_ % nj) + 1; r_ /= nj;                                                             \
+    const int k = (int)(r_ % nk) + 1;                                                                       \
+    const int n = (int)(r_ / nk);
+
+__device__ __forceinline__ int64_t p3s_idx(const DevBlock &b, int S, int i, int j, int k, int n) {
+  return b.op3 * S + (int64_t)n * b.P3 + p3_cell(b, i, j, k);
+}
+
+// mut on the faces of family D into flux(.,1) (bq_face_* calmut part)
+template <int D>
+__global__ void k_qface_mut(DevBlock b, int npde, int S, const double *__restrict__ mut, double *__restrict__ flux) {
+  KOM_FACE_LOOP(D)
+    const int di = D == 1, dj = D == 2, dk = D == 3;
+    flux[f0_idx(b, npde, S, i, j, k, 1, n)] =
+        (mut[p3s_idx(b, S, i - di, j - dj, k - dk, n)] + mut[p3s_idx(b, S, i, j, k, n)]) / 2;
+  }
+}
+__global__ void k_qwall_mut(const DevBlock *__restrict__ blocks, const WallFace *__restrict__ walls, int nw, int d,
+                            int npde, int S, const double *__restrict__ mut, double *__restrict__ flux) {
+  const int64_t total = (int64_t)nw * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const WallFace w = walls[t % nw];
+    if (w.d != d) continue;
+    const int n = (int)(t / nw);
+    const DevBlock b = blocks[w.blk];
+    int pa[3] = {w.fi, w.fj, w.fk};
+    pa[d - 1] = w.inrout == 1 ? 0 : (d == 1 ? b.im : (d == 2 ? b.jm : b.km));
+    flux[f0_idx(b, npde, S, w.fi, w.fj, w.fk, 1, n)] = mut[p3s_idx(b, S, pa[0], pa[1], pa[2], n)];
+  }
+}
+
+// b_rtst (src/flux.f90:2846-2946): tau1(.,1..6) on the faces of family d
+__global__ void k_rtst(DevBlock b, int d, const cosa_params *__restrict__ Pp, const double *__restrict__ qf,
+                       const double *__restrict__ g0, const double *__restrict__ g1, const double *__restrict__ g2,
+                       const double *__restrict__ vm, int64_t n0, const double *__restrict__ flux,
+                       double *__restrict__ tau) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const double fact = 2.0 / 3.0, mr = P.machfs / P.reyno;
+  KOM_FACE_LOOP(d)
+    const int64_t c = p3_cell(b, i, j, k);
+    auto Q = [&](const double *a, int v) { return a[p3_var(b, npde, S, v, n) + c]; };
+    const double rho = Q(qf, 1), tke = Q(qf, 6), mut = flux[f0_idx(b, npde, S, i, j, k, 1, n)];
+    double vmf[9];
+    load_vm(vm, b, n0, d, i, j, k, vmf);
+    double gr[3][3];  // gr[var u,v,w][xi, eta, zeta]
+#pragma unroll
+    for (int m = 0; m < 3; ++m) { gr[m][0] = Q(g0, m + 2); gr[m][1] = Q(g1, m + 2); gr[m][2] = Q(g2, m + 2); }
+    double dv[3][3];  // dv[var][x, y, z]
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+      for (int c3 = 0; c3 < 3; ++c3) dv[m][c3] = gr[m][0] * vmf[c3] + gr[m][1] * vmf[3 + c3] + gr[m][2] * vmf[6 + c3];
+    const double divv = (dv[0][0] + dv[1][1] + dv[2][2]) * P.turcmp;
+    const double txx = 2 * mut * (dv[0][0] - divv / 3), txy = mut * (dv[0][1] + dv[1][0]);
+    const double txz = mut * (dv[0][2] + dv[2][0]), tyy = 2 * mut * (dv[1][1] - divv / 3);
+    const double tyz = mut * (dv[1][2] + dv[2][1]), tzz = 2 * mut * (dv[2][2] - divv / 3);
+    tau[p3_var(b, npde, S, 1, n) + c] = mr * txx - fact * rho * tke;
+    tau[p3_var(b, npde, S, 2, n) + c] = mr * txy;
+    tau[p3_var(b, npde, S, 3, n) + c] = mr * txz;
+    tau[p3_var(b, npde, S, 4, n) + c] = mr * tyy - fact * rho * tke;
+    tau[p3_var(b, npde, S, 5, n) + c] = mr * tyz;
+    tau[p3_var(b, npde, S, 6, n) + c] = mr * tzz - fact * rho * tke;
+  }
+}
+
+// vflux_b with kom: the k-omega branch (Reynolds stresses, k and omega
+// diffusion; the omega row keeps the reference's dk/dz) followed by the
+// laminar terms with the face mut of flux(.,1)
+__global__ void k_vflux_kom(DevBlock b, int d, const cosa_params *__restrict__ Pp, const double *__restrict__ qf,
+                            const double *__restrict__ g0, const double *__restrict__ g1,
+                            const double *__restrict__ g2, const double *__restrict__ tau,
+                            const double *__restrict__ vm, int64_t n0, const double *__restrict__ s,
+                            double *__restrict__ flux) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
+  const ViscPar V = make_visc(P);
+  KOM_FACE_LOOP(d)
+    const int nh = n * P.hbmove;
+    const int64_t c = p3_cell(b, i, j, k);
+    auto Q = [&](const double *a, int v) { return a[p3_var(b, npde, S, v, n) + c]; };
+    const int64_t e = p2_idx(b, S2, 1, i, j, k, nh);
+    const double kx = s[e], ky = s[e + 1], kz = s[e + 2], ds = s[e + 3];
+    double vmf[9];
+    load_vm(vm, b, n0, d, i, j, k, vmf);
+    const double rho = Q(qf, 1), p = Q(qf, 5);
+    const double tt = P.gamma * p / rho;
+    const double mu = sutherland(tt, P.stemp);
+    const double mut = flux[f0_idx(b, npde, S, i, j, k, 1, n)];
+    const double tkexi = Q(g0, 6), tkeeta = Q(g1, 6), tkezeta = Q(g2, 6);
+    const double omexi = Q(g0, 7), omeeta = Q(g1, 7), omezeta = Q(g2, 7);
+    const double dtkedx = tkexi * vmf[0] + tkeeta * vmf[3] + tkezeta * vmf[6];
+    const double dtkedy = tkexi * vmf[1] + tkeeta * vmf[4] + tkezeta * vmf[7];
+    const double dtkedz = tkexi * vmf[2] + tkeeta * vmf[5] + tkezeta * vmf[8];
+    const double domedx = omexi * vmf[0] + omeeta * vmf[3] + omezeta * vmf[6];
+    const double domedy = omexi * vmf[1] + omeeta * vmf[4] + omezeta * vmf[7];
+    const double txx = Q(tau, 1), txy = Q(tau, 2), txz = Q(tau, 3), tyy = Q(tau, 4), tyz = Q(tau, 5), tzz = Q(tau, 6);
+    double Fk[7];
+    Fk[1] = -(txx * kx + txy * ky + txz * kz) * ds;
+    Fk[2] = -(txy * kx + tyy * ky + tyz * kz) * ds;
+    Fk[3] = -(txz * kx + tyz * ky + tzz * kz) * ds;
+    const double ctke = (mu + P.sigk * mut) * P.machfs / P.reyno;
+    const double come = (mu + P.sigw * mut) * P.machfs / P.reyno;
+    Fk[4] = -ctke * (dtkedx * kx + dtkedy * ky + dtkedz * kz) * ds;
+    Fk[5] = -ctke * (dtkedx * kx + dtkedy * ky + dtkedz * kz) * ds;
+    Fk[6] = -come * (domedx * kx + domedy * ky + dtkedz * kz) * ds;
+    // laminar terms with the face mut in the heat flux
+    double f5[5], g[3][5], F[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) { f5[m] = Q(qf, m + 1); g[0][m] = Q(g0, m + 1); g[1][m] = Q(g1, m + 1); g[2][m] = Q(g2, m + 1); }
+    vflux_face(V, f5, g, vmf, kx, ky, kz, ds, mut, F);
+    flux[f0_idx(b, npde, S, i, j, k, 1, n)] = 0.0;
+#pragma unroll
+    for (int m = 1; m < 5; ++m) flux[f0_idx(b, npde, S, i, j, k, m + 1, n)] = Fk[m] + F[m];
+    flux[f0_idx(b, npde, S, i, j, k, 6, n)] = Fk[5];
+    flux[f0_idx(b, npde, S, i, j, k, 7, n)] = Fk[6];
+  }
+}
+
+// q_der_c (src/flux.f90:2979-3130): velocity differences of the face values
+template <int D>
+__global__ void k_qder_c(DevBlock b, int npde, int S, const double *__restrict__ qf, double *__restrict__ dc) {
+  KOM_CELL_LOOP
+    const int di = D == 1, dj = D == 2, dk = D == 3;
+    const int64_t c0 = p3_cell(b, i, j, k), c1 = p3_cell(b, i + di, j + dj, k + dk);
+#pragma unroll
+    for (int v = 2; v <= 4; ++v) {
+      const int64_t o = p3_var(b, npde, S, v, n);
+      dc[o + c0] = qf[o + c1] - qf[o + c0];
+    }
+  }
+}
+
+// turprod_b (src/src.f90:40-177)
+__global__ void k_turprod(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ dx,
+                          const double *__restrict__ de, const double *__restrict__ dz, const double *__restrict__ vm,
+                          int64_t n0, double *__restrict__ prd, double *__restrict__ divvel,
+                          double *__restrict__ delpls) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  KOM_CELL_LOOP
+    // cell metrics: derivative m, component c from the two faces of family c+1
+    double met[3][3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      met[m][0] = (vm[vm_idx(b, n0, 1, m, 0, i + 1, j, k)] + vm[vm_idx(b, n0, 1, m, 0, i, j, k)]) / 2;
+      met[m][1] = (vm[vm_idx(b, n0, 2, m, 1, i, j + 1, k)] + vm[vm_idx(b, n0, 2, m, 1, i, j, k)]) / 2;
+      met[m][2] = (vm[vm_idx(b, n0, 3, m, 2, i, j, k + 1)] + vm[vm_idx(b, n0, 3, m, 2, i, j, k)]) / 2;
+    }
+    const int64_t c = p3_cell(b, i, j, k);
+    double dv[3][3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const int64_t o = p3_var(b, npde, S, v + 2, n) + c;
+      const double a = dx[o], e = de[o], f = dz[o];
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) dv[v][cc] = a * met[0][cc] + e * met[1][cc] + f * met[2][cc];
+    }
+    const double divv = (dv[0][0] + dv[1][1] + dv[2][2]) * P.turcmp;
+    const double txx = dv[0][0], txy = (dv[0][1] + dv[1][0]) / 2, txz = (dv[0][2] + dv[2][0]) / 2;
+    const double tyy = dv[1][1], tyz = (dv[1][2] + dv[2][1]) / 2, tzz = dv[2][2];
+    const double prod = 2 * (txx * txx + tyy * tyy + tzz * tzz + 2 * (txy * txy + txz * txz + tyz * tyz) - divv * divv / 3);
+    const int64_t o = p3s_idx(b, S, i, j, k, n);
+    prd[o] = prod;
+    divvel[o] = divv;
+    delpls[o] = 2.0 / 3.0 * fmax(divv, 0.0);
+  }
+}
+
+// srckw_b (src/src.f90:196-272)
+__global__ void k_srckw(DevBlock b, const cosa_params *__restrict__ Pp, int nl, const double *__restrict__ q,
+                        const double *__restrict__ mut, const double *__restrict__ prd,
+                        const double *__restrict__ divvel, double *__restrict__ res, const double *__restrict__ vol) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const double fact = 2.0 / 3.0, mor = P.machfs / P.reyno;
+  KOM_CELL_LOOP
+    const int64_t c = p3_cell(b, i, j, k), o = p3s_idx(b, S, i, j, k, n);
+    const double rho = q[p3_var(b, npde, S, 1, n) + c], tke = q[p3_var(b, npde, S, 6, n) + c];
+    const double ome = q[p3_var(b, npde, S, 7, n) + c];
+    const double mt = mut[o], divv = divvel[o];
+    double prod = prd[o], prodw = prd[o];
+    if (P.lim_prodtke && (nl == 1 || P.prd_all_lvls)) {
+      const double tstdis = P.prdlim * P.bstrkw * rho * tke * ome;
+      if (mor * mt * prod > tstdis) {
+        prod = tstdis / mor / mt;
+        if (P.lim_prodomega) prodw = prod;
+      }
+    }
+    const double v = vol[p1_idx(b, 1, i, j, k, 0)];
+    double *r6 = res + p3_var(b, npde, S, 6, n) + c, *r7 = res + p3_var(b, npde, S, 7, n) + c;
+    *r6 = *r6 - v * (mor * mt * prod - fact * divv * rho * tke - P.bstrkw * rho * tke * ome);
+    *r7 = *r7 - v * (P.gkw * P.cmu * rho * prodw - P.gkw * fact * divv * rho * ome - P.bkw * rho * (ome * ome));
+  }
+}
+
+// update_b, explicit k-omega part (src/update.f90:601-640)
+__global__ void k_update_kom(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
+                             double *__restrict__ q, const double *__restrict__ qold, const double *__restrict__ vol,
+                             const double *__restrict__ dtt, const double *__restrict__ delpls,
+                             const double *__restrict__ prd, double ar) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const double gav = P.gkw, bav = P.bkw;
+  KOM_CELL_LOOP
+    const int64_t c = p3_cell(b, i, j, k), o = p3s_idx(b, S, i, j, k, n);
+    const int64_t i1 = p3_var(b, npde, S, 1, n) + c, i6 = p3_var(b, npde, S, 6, n) + c, i7 = p3_var(b, npde, S, 7, n) + c;
+    const double rho = q[i1], ome = q[i7] / q[i1], tke = q[i6] / q[i1];
+    const double dt = dtt[p1_idx(b, S, i, j, k, n)];
+    const double dtau = dt * vol[p1_idx(b, 1, i, j, k, 0)];
+    const double dp = delpls[o];
+    double rhomega = (qold[i7] - ar * res[i7] * dt + ar * dtau * rho * ome * (gav * dp + 2 * bav * ome)) /
+                     (1 + ar * dtau * (gav * dp + 2 * bav * ome));
+    const double rhomegamin = gav * P.cmu * rho * sqrt(prd[o]);
+    if (rhomega < rhomegamin) rhomega = rhomegamin;
+    q[i7] = rhomega;
+    const double drhomega = rhomega - rho * ome;
+    q[i6] = (qold[i6] - ar * res[i6] * dt + ar * dtau * rho * tke * (dp + P.bstrkw * ome) -
+             ar * dtau * P.bstrkw * tke * drhomega) /
+            (1 + ar * dtau * (dp + P.bstrkw * ome));
+  }
+}
+
+// cut_q on a scalar P3 array with S snapshots (cutman_mut, src/bc.f90:2713-2799)
+__global__ void k_cut_scalar(const DevBlock *__restrict__ blocks, const HaloItem *__restrict__ items, int nitems,
+                             int S, double *__restrict__ a) {
+  const int64_t total = (int64_t)nitems * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const HaloItem it = items[t % nitems];
+    const int n = (int)(t / nitems);
+    const DevBlock db = blocks[it.dblk], sb = blocks[it.sblk];
+    const int64_t bd = db.op3 * S + (int64_t)n * db.P3, bs = sb.op3 * S + (int64_t)n * sb.P3;
+    // the cut of the reference's last write keeps each halo cell (host mask)
+    if (it.mask & 1) a[bd + it.h1] = a[bs + it.c1];
+    if (it.mask & 2) a[bd + it.h2] = a[bs + it.c2];
+  }
+}

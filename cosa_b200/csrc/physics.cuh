@@ -615,6 +615,85 @@ __device__ __forceinline__ int bc_walvis(double g, const double *c1, const doubl
   return 3;
 }
 
+// ---- roflux_b turbulence fluxes ----------------------------------------------------
+// Upwinded rho k u_n and rho omega u_n with the mean-flow wave strengths and
+// the turbulence entropy-fix settings.  h0l/h0r are the values the
+// mean-flow loop left behind, those of the block's last face (ic,jc,kc) of
+// the snapshot (the reference does not recompute them in this loop).
+__device__ __forceinline__ void roe_turb(const cosa_params &P, double kx, double ky, double kz, double ds,
+                                         const double *qr, const double *ql, double h0r_last, double h0l_last,
+                                         double &fk, double &fw) {
+  const double g = P.gamma;
+  const double rhor = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4], tker = qr[5], omer = qr[6];
+  const double rhol = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4], tkel = ql[5], omel = ql[6];
+  const double unr = ur * kx + vr * ky + wr * kz, unl = ul * kx + vl * ky + wl * kz;
+  const double frk = rhor * unr * tker, frw = rhor * unr * omer;
+  const double flk = rhol * unl * tkel, flw = rhol * unl * omel;
+  const double drho = rhor - rhol, dp = pr - pl, dun = unr - unl, dtke = tker - tkel, dome = omer - omel;
+  const double rhols = sqrt(rhol), rhors = sqrt(rhor);
+  const double rho = rhols * rhors, denom = rhols + rhors;
+  const double u = (rhols * ul + rhors * ur) / denom, v = (rhols * vl + rhors * vr) / denom;
+  const double w = (rhols * wl + rhors * wr) / denom;
+  const double un = u * kx + v * ky + w * kz;
+  const double h0 = (rhols * h0l_last + rhors * h0r_last) / denom;
+  const double tke = (rhols * tkel + rhors * tker) / denom, ome = (rhols * omel + rhors * omer) / denom;
+  const double q2 = u * u + v * v + w * w;
+  const double a2 = (g - 1) * (h0 - q2 / 2 - tke);
+  const double a = sqrt(a2);
+  double rm123 = fabs(un), rm4 = fabs(un + a), rm5 = fabs(un - a);
+  if (P.efx_setup_t) {
+    double rdelta = P.cntrpy_t * (P.entfx_t_w[0] * P.entfxctf_t + P.entfx_t_w[1] * (sqrt(q2) + a) +
+                                  P.entfx_t_w[2] * 0.2 * (fabs(un) + a + 0.0));
+    rdelta = fmax(rdelta, 1.0e-12);
+    if (rm123 <= rdelta && P.efx_all_t) rm123 = 0.5 * (rm123 * rm123 + rdelta * rdelta) / rdelta;
+    if (rm4 <= rdelta) rm4 = 0.5 * (rm4 * rm4 + rdelta * rdelta) / rdelta;
+    if (rm5 <= rdelta) rm5 = 0.5 * (rm5 * rm5 + rdelta * rdelta) / rdelta;
+  }
+  if (P.eig_limit_t) {
+    if (rm123 <= P.eig_cutoff_t) rm123 = P.eig_cutoff_t;
+    if (P.eig_lim_all_t && rm4 <= P.eig_cutoff_t) rm4 = P.eig_cutoff_t;
+    if (P.eig_lim_all_t && rm5 <= P.eig_cutoff_t) rm5 = P.eig_cutoff_t;
+  }
+  const double al1 = rm123 * (drho - dp / a2), al2 = rm123 * rho;
+  const double al3 = rm4 * (dp / a2 + rho * dun / a) / 2, al4 = rm5 * (dp / a2 - rho * dun / a) / 2;
+  const double dfk = (al1 + al3 + al4) * tke + al2 * dtke;
+  const double dfw = (al1 + al3 + al4) * ome + al2 * dome;
+  fk = (frk + flk - dfk) / 2 * ds;
+  fw = (frw + flw - dfw) / 2 * ds;
+}
+
+// h0 of a face state (rho, u, v, w, p, k)
+__device__ __forceinline__ double face_h0(double g, const double *q) {
+  return g / (g - 1) * q[4] / q[0] + (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) / 2 + q[5];
+}
+
+// ---- bc_walvis_15, k-omega part (src/bc.f90:2309-2470) ---------------------------
+// h1 holds the wall state (laminar part already applied), c1 the first
+// cell; d = wall distance of the first cell, (nx, ny, nz) the face normal
+__device__ __forceinline__ void bc_walvis_kom(const cosa_params &P, double nx, double ny, double nz, double d,
+                                              const double *c1, double *h1, double *h2) {
+  const double small = 1.0e-12, smasq = 1.0e-24, mor = P.machfs / P.reyno;
+  const double rhow = h1[0], pw = h1[4];
+  const double tw = pw * P.gamma / rhow;
+  const double muw = (P.stemp + 1) / (tw + P.stemp) * pow(tw, 1.5);
+  double omew;
+  if (P.wallwilc) {
+    const double uc = c1[1], vc = c1[2], wc = c1[3];
+    const double uorth = nx * uc + ny * vc + nz * wc;
+    const double a = uc - uorth * nx, b = vc - uorth * ny, c = wc - uorth * nz;
+    const double upar = sqrt(a * a + b * b + c * c);
+    const double dupardn = upar / (d + small);
+    const double tauw = muw * fabs(dupardn);
+    const double rkrpls = P.roughk > 0.0 ? fmax(1.0, sqrt(rhow * tauw / mor) * P.roughk / muw) : 1.0;
+    const double sr = rkrpls >= 25.0 ? 100.0 / rkrpls : 2500.0 / (rkrpls * rkrpls);
+    omew = fabs(dupardn) * sr;
+  } else {
+    omew = 60.0 * muw / (P.bkw * rhow * (d * d) + smasq) * P.machfs / P.reyno;
+  }
+  h1[5] = 0.0; h1[6] = omew;
+  h2[5] = h1[5]; h2[6] = h1[6];
+}
+
 __device__ __forceinline__ bool strong_bc(int t) {
   return t == 13 || t == 14 || t / 100 == 15 || t == 22 || t == 23 || t == 92 || t == 93 || t == 5;
 }

@@ -209,20 +209,20 @@ struct QView {
     return q[m * P3 + (i + 1) + (int64_t)I3 * ((j + 1) + (int64_t)J3 * (k + 1))];
   }
 };
-__device__ __forceinline__ QView qview(const DevBlock &b, const double *q, int S, int n) {
+__device__ __forceinline__ QView qview(const DevBlock &b, const double *q, int S, int n, int npde = 5) {
   QView v;
-  v.q = q + p3_var(b, 5, S, 1, n);
+  v.q = q + p3_var(b, npde, S, 1, n);
   v.P3 = b.P3; v.I3 = b.I3; v.J3 = b.J3;
   return v;
 }
 
 // bq_face_* / bq_der_* bulk loops (src/flux.f90:1848-1880, 2029-2070, 2210-2250,
 // 2432-2450): face (i,j,k) of family D between cells c-e_D and c
-template <int D>
-__device__ __forceinline__ void face_interior(const QView &Q, int i, int j, int k, double qf[5], double g[3][5]) {
+template <int D, int NV = 5>
+__device__ __forceinline__ void face_interior(const QView &Q, int i, int j, int k, double qf[NV], double g[3][NV]) {
   constexpr int di = D == 1, dj = D == 2, dk = D == 3;
 #pragma unroll
-  for (int m = 0; m < 5; ++m) {
+  for (int m = 0; m < NV; ++m) {
     const double c = Q(i, j, k, m), cm = Q(i - di, j - dj, k - dk, m);
     qf[m] = (cm + c) / 2;
     g[D - 1][m] = c - cm;
@@ -241,7 +241,8 @@ __device__ __forceinline__ void face_interior(const QView &Q, int i, int j, int 
 // counterparts; 2466-2488): face state = the halo (wall) value, three-point
 // one-sided normal derivative, tangential derivatives along the halo line,
 // one-sided at the ends of the patch
-__device__ __forceinline__ void face_wall(const QView &Q, const WallFace &w, int mx, double qf[5], double g[3][5]) {
+template <int NV = 5>
+__device__ __forceinline__ void face_wall(const QView &Q, const WallFace &w, int mx, double qf[NV], double g[3][NV]) {
   const int d = w.d;
   const bool lo = w.inrout == 1;
   const int aux = lo ? 0 : mx, in1 = lo ? 1 : mx - 1, in2 = lo ? 2 : mx - 2;
@@ -252,7 +253,7 @@ __device__ __forceinline__ void face_wall(const QView &Q, const WallFace &w, int
   pa[d - 1] = aux; p1[d - 1] = in1; p2[d - 1] = in2;
   const int fpos[3] = {w.fi, w.fj, w.fk};
 #pragma unroll
-  for (int m = 0; m < 5; ++m) {
+  for (int m = 0; m < NV; ++m) {
     const double qa = Q(pa[0], pa[1], pa[2], m);
     qf[m] = qa;
     g[d - 1][m] = sgnm / 3 * (-qa * 8 + Q(p1[0], p1[1], p1[2], m) * 9 - Q(p2[0], p2[1], p2[2], m));
@@ -470,7 +471,8 @@ __global__ void k_vdiv(const DevBlock *__restrict__ blocks, const cosa_params *_
 __device__ __forceinline__ void eig_ns_cell(const DevBlock &b, const cosa_params &P, const QView &Q,
                                             const double *__restrict__ si, const double *__restrict__ sj,
                                             const double *__restrict__ sk, int S2, int nh, double volc, int i, int j,
-                                            int k, double lam[3], double lamv[3]) {
+                                            int k, double lam[3], double lamv[3], const double *mut = nullptr,
+                                            int S = 1, int n = 0) {
   const double g = P.gamma, st = P.stemp;
   double qc[5], sm[3][4], sp[3][4];
 #pragma unroll
@@ -484,6 +486,8 @@ __device__ __forceinline__ void eig_ns_cell(const DevBlock &b, const cosa_params
   eig_eul(g, qc, sm[0], sp[0], sm[1], sp[1], sm[2], sp[2], lam[0], lam[1], lam[2]);
   const double rho = qc[0];
   const double mu = sutherland(g * qc[4] / rho, st);
+  auto MUT = [&](int a, int c, int e) { return mut ? mut[b.op3 * S + (int64_t)n * b.P3 + p3_cell(b, a, c, e)] : 0.0; };
+  const double mutc = MUT(i, j, k);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const int a = d == 0, c = d == 1, e = d == 2;
@@ -492,28 +496,34 @@ __device__ __forceinline__ void eig_ns_cell(const DevBlock &b, const cosa_params
     const double tp = g * Q(i + a, j + c, k + e, 4) / rhom;
     const double mum = sutherland(tm, st), mup = sutherland(tp, st);
     const double mud = (mum + 2 * mu + mup) / 4;
+    const double mutd = (MUT(i - a, j - c, k - e) + 2 * mutc + MUT(i + a, j + c, k + e)) / 4;
     const double area = (sm[d][3] + sp[d][3]) / 2;
-    // laminar: the turbulent viscosity term mut/prant is zero
-    lamv[d] = P.cdff * area * area * g * P.machfs / P.reyno * (mud / P.pranl) / (rho * volc);
+    lamv[d] = P.cdff * area * area * g * P.machfs / P.reyno * (mud / P.pranl + mutd / P.prant) / (rho * volc);
+  }
+}
+
+// IRS coefficients of bdeltat for ratio rat (rat: mean flow, ratt: k-omega),
+// with the viscous floor c1/4 lamv / sum(lam) for irsop 5 and 6
+__device__ __forceinline__ void irs_coef_ns(int irsop, double rat, double psirs, const double lam[3],
+                                            const double lamv[3], double &bx, double &by, double &bz) {
+  const double c1 = 40.0;
+  bx = by = bz = 0.0;
+  if (irsop < 2 || irsop == 4) return;
+  irs_beta(irsop, rat, psirs, lam[0], lam[1], lam[2], bx, by, bz);
+  const double sl = lam[0] + lam[1] + lam[2];
+  if (irsop == 5) {
+    bx = fmax(bx, c1 / 4 * lamv[0] / sl); by = fmax(by, c1 / 4 * lamv[1] / sl); bz = fmax(bz, c1 / 4 * lamv[2] / sl);
+  } else if (irsop == 6) {
+    bx = fmax(bx, 0.25 * c1 * lamv[0] / sl); by = fmax(by, 0.25 * c1 * lamv[1] / sl);
+    bz = fmax(bz, 0.25 * c1 * lamv[2] / sl);
   }
 }
 
 __device__ __forceinline__ void deltat_ns_cell(const cosa_params &P, const double lam[3], const double lamv[3],
                                                double &dt, double &bx, double &by, double &bz) {
-  const double c1 = 40.0;
   if (P.irsop == 5 || P.irsop == 6) dt = P.cfl / (lam[0] + lam[1] + lam[2]);
   else dt = P.cfl / (lam[0] + lam[1] + lam[2] + lamv[0] + lamv[1] + lamv[2]);
-  bx = by = bz = 0.0;
-  if (P.irsop >= 2 && P.irsop != 4) {
-    irs_beta(P.irsop, P.rat, P.psirs, lam[0], lam[1], lam[2], bx, by, bz);
-    const double sl = lam[0] + lam[1] + lam[2];
-    if (P.irsop == 5) {
-      bx = fmax(bx, c1 / 4 * lamv[0] / sl); by = fmax(by, c1 / 4 * lamv[1] / sl); bz = fmax(bz, c1 / 4 * lamv[2] / sl);
-    } else if (P.irsop == 6) {
-      bx = fmax(bx, 0.25 * c1 * lamv[0] / sl); by = fmax(by, 0.25 * c1 * lamv[1] / sl);
-      bz = fmax(bz, 0.25 * c1 * lamv[2] / sl);
-    }
-  }
+  irs_coef_ns(P.irsop, P.rat, P.psirs, lam, lamv, bx, by, bz);
 }
 
 // time step (and IRS coefficients) of the fused viscous path, from the
@@ -548,10 +558,10 @@ __global__ void k_dt_ns(const DevBlock *__restrict__ blocks, const cosa_params *
 // lambda with viscous = .true.: lam(.,1:3) convective, lamv(.,1:3) viscous
 __global__ void k_lambda_ns(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
                             const double *__restrict__ si, const double *__restrict__ sj,
-                            const double *__restrict__ sk, const double *__restrict__ vol, double *__restrict__ lam,
-                            double *__restrict__ lamv) {
+                            const double *__restrict__ sk, const double *__restrict__ vol,
+                            const double *__restrict__ mut, double *__restrict__ lam, double *__restrict__ lamv) {
   const cosa_params &P = *Pp;
-  const int S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
+  const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
   const int64_t total = (int64_t)ni * nj * nk * S;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
@@ -560,23 +570,23 @@ __global__ void k_lambda_ns(DevBlock b, const cosa_params *__restrict__ Pp, cons
     const int j = (int)(r % nj) + 1; r /= nj;
     const int k = (int)(r % nk) + 1;
     const int n = (int)(r / nk), nh = n * P.hbmove;
-    const QView Q = qview(b, q, S, n);
+    const QView Q = qview(b, q, S, n, npde);
     double l[3], lv[3];
-    eig_ns_cell(b, P, Q, si, sj, sk, S2, nh, vol[p1_idx(b, 1, i, j, k, 0)], i, j, k, l, lv);
+    eig_ns_cell(b, P, Q, si, sj, sk, S2, nh, vol[p1_idx(b, 1, i, j, k, 0)], i, j, k, l, lv, mut, S, n);
     const int64_t c = p3_cell(b, i, j, k);
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
-      lam[p3_var(b, 5, S, m + 1, n) + c] = l[m];
-      lamv[p3_var(b, 5, S, m + 1, n) + c] = lv[m];
+      lam[p3_var(b, npde, S, m + 1, n) + c] = l[m];
+      lamv[p3_var(b, npde, S, m + 1, n) + c] = lv[m];
     }
   }
 }
 
 __global__ void k_deltat_ns(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ dtv,
                             const double *__restrict__ lam, const double *__restrict__ lamv, double *bx, double *by,
-                            double *bz) {
+                            double *bz, double *dtt, double *tbx, double *tby, double *tbz) {
   const cosa_params &P = *Pp;
-  const int S = 2 * P.nharms + 1;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
   const int64_t total = (int64_t)ni * nj * nk * S;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
@@ -589,19 +599,25 @@ __global__ void k_deltat_ns(DevBlock b, const cosa_params *__restrict__ Pp, doub
     double l[3], lv[3];
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
-      l[m] = lam[p3_var(b, 5, S, m + 1, n) + c];
-      lv[m] = lamv[p3_var(b, 5, S, m + 1, n) + c];
+      l[m] = lam[p3_var(b, npde, S, m + 1, n) + c];
+      lv[m] = lamv[p3_var(b, npde, S, m + 1, n) + c];
     }
     double dt, a, e, f;
     deltat_ns_cell(P, l, lv, dt, a, e, f);
     const int64_t o = p1_idx(b, S, i, j, k, n);
     dtv[o] = dt;
     if (bx && P.irsop >= 2 && P.irsop != 4) { bx[o] = a; by[o] = e; bz[o] = f; }
+    // k-omega: dtvolt = cflt/cfl dtvol and the turbulence coefficients with ratt
+    if (dtt) dtt[o] = P.cflt / P.cfl * dt;
+    if (tbx && P.irsop >= 2 && P.irsop != 4) {
+      irs_coef_ns(P.irsop, P.ratt, P.psirs, l, lv, a, e, f);
+      tbx[o] = a; tby[o] = e; tbz[o] = f;
+    }
   }
 }
 
 // q_face / q_der bulk loops with the reference's P3 outputs
-template <int D>
+template <int D, int NV>
 __global__ void k_qface_qder(DevBlock b, int S, const double *__restrict__ q, double *__restrict__ qf,
                              double *__restrict__ g0, double *__restrict__ g1, double *__restrict__ g2) {
   const int ni = D == 1 ? b.im : b.im - 1, nj = D == 2 ? b.jm : b.jm - 1, nk = D == 3 ? b.km : b.km - 1;
@@ -612,19 +628,20 @@ __global__ void k_qface_qder(DevBlock b, int S, const double *__restrict__ q, do
     const int j = (int)(r % nj) + 1; r /= nj;
     const int k = (int)(r % nk) + 1;
     const int n = (int)(r / nk);
-    const QView Q = qview(b, q, S, n);
-    double f[5], g[3][5];
-    face_interior<D>(Q, i, j, k, f, g);
+    const QView Q = qview(b, q, S, n, NV);
+    double f[NV], g[3][NV];
+    face_interior<D, NV>(Q, i, j, k, f, g);
     const int64_t c = p3_cell(b, i, j, k);
 #pragma unroll
-    for (int m = 0; m < 5; ++m) {
-      const int64_t o = p3_var(b, 5, S, m + 1, n) + c;
+    for (int m = 0; m < NV; ++m) {
+      const int64_t o = p3_var(b, NV, S, m + 1, n) + c;
       if (qf) qf[o] = f[m];
       if (g0) { g0[o] = g[0][m]; g1[o] = g[1][m]; g2[o] = g[2][m]; }
     }
   }
 }
 
+template <int NV>
 __global__ void k_qwall(const DevBlock *__restrict__ blocks, const WallFace *__restrict__ walls, int nw, int d, int S,
                         const double *__restrict__ q, double *__restrict__ qf, double *__restrict__ g0,
                         double *__restrict__ g1, double *__restrict__ g2) {
@@ -634,14 +651,14 @@ __global__ void k_qwall(const DevBlock *__restrict__ blocks, const WallFace *__r
     if (w.d != d) continue;
     const int n = (int)(t / nw);
     const DevBlock b = blocks[w.blk];
-    const QView Q = qview(b, q, S, n);
+    const QView Q = qview(b, q, S, n, NV);
     const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
-    double f[5], g[3][5];
-    face_wall(Q, w, mx, f, g);
+    double f[NV], g[3][NV];
+    face_wall<NV>(Q, w, mx, f, g);
     const int64_t c = p3_cell(b, w.fi, w.fj, w.fk);
 #pragma unroll
-    for (int m = 0; m < 5; ++m) {
-      const int64_t o = p3_var(b, 5, S, m + 1, n) + c;
+    for (int m = 0; m < NV; ++m) {
+      const int64_t o = p3_var(b, NV, S, m + 1, n) + c;
       if (qf) qf[o] = f[m];
       if (g0) { g0[o] = g[0][m]; g1[o] = g[1][m]; g2[o] = g[2][m]; }
     }

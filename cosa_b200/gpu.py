@@ -60,7 +60,8 @@ SYMBOLS = [
     "cosa_serve_create", "cosa_serve_destroy", "cosa_serve_submit", "cosa_serve_step", "cosa_serve_result",
     "cosa_serve_free_slots", "cosa_gpu_coordex", "cosa_gpu_cutman_x", "cosa_gpu_volex", "cosa_gpu_cutman_v",
     "cosa_gpu_vmetrix", "cosa_gpu_viscous_setup", "cosa_gpu_q_face", "cosa_gpu_q_der", "cosa_gpu_vflux",
-    "cosa_gpu_lambda_ns", "cosa_gpu_deltat_ns",
+    "cosa_gpu_lambda_ns", "cosa_gpu_deltat_ns", "cosa_gpu_q_face_mut", "cosa_gpu_rtst", "cosa_gpu_vflux_kom",
+    "cosa_gpu_q_der_c", "cosa_gpu_turprod", "cosa_gpu_srckw", "cosa_gpu_update_kom", "cosa_gpu_cutman_mut",
 ]
 
 
@@ -324,14 +325,56 @@ class Context:
         self._check(load().cosa_gpu_vflux(self.h, idir, nl, _ptr(qf.ptr), _ptr(dqxi.ptr), _ptr(dqeta.ptr),
                                           _ptr(dqzeta.ptr), _ptr(vm.ptr), _ptr(sijk.ptr), _ptr(flux.ptr)), "vflux")
 
-    def lambda_ns(self, nl, q, si, sj, sk, vol, lam, lamv):
+    def lambda_ns(self, nl, q, si, sj, sk, vol, lam, lamv, mut=None):
         self._check(load().cosa_gpu_lambda_ns(self.h, nl, _ptr(q.ptr), _ptr(si.ptr), _ptr(sj.ptr), _ptr(sk.ptr),
-                                              _ptr(vol.ptr), _ptr(lam.ptr), _ptr(lamv.ptr)), "lambda_ns")
+                                              _ptr(vol.ptr), _ptr(mut.ptr if mut else None), _ptr(lam.ptr),
+                                              _ptr(lamv.ptr)), "lambda_ns")
 
-    def deltat_ns(self, nl, dtvol, lam, lamv, bx=None, by=None, bz=None):
-        self._check(load().cosa_gpu_deltat_ns(self.h, nl, _ptr(dtvol.ptr), _ptr(lam.ptr), _ptr(lamv.ptr),
-                                              _ptr(bx.ptr if bx else None), _ptr(by.ptr if by else None),
-                                              _ptr(bz.ptr if bz else None)), "deltat_ns")
+    def deltat_ns(self, nl, dtvol, lam, lamv, bx=None, by=None, bz=None, dtvolt=None, tbx=None, tby=None, tbz=None):
+        o = lambda a: _ptr(a.ptr if a else None)
+        self._check(load().cosa_gpu_deltat_ns(self.h, nl, _ptr(dtvol.ptr), _ptr(lam.ptr), _ptr(lamv.ptr), o(bx), o(by),
+                                              o(bz), o(dtvolt), o(tbx), o(tby), o(tbz)), "deltat_ns")
+
+    # ---- Wilcox k-omega ---------------------------------------------------------------
+    def alloc_p3s(self, nl=1):
+        """A scalar P3 array (mut, prd, divvel, delpls) with S snapshots."""
+        return DevArray(self, self.sizes(nl)[0] * self.S)
+
+    def bc_dist(self, nl, q, si, sj, sk, dist):
+        self._check(load().cosa_gpu_bc(self.h, nl, _ptr(q.ptr), _ptr(si.ptr), _ptr(sj.ptr), _ptr(sk.ptr),
+                                       _ptr(dist.ptr)), "bc")
+
+    def q_face_mut(self, idir, nl, mut, flux):
+        self._check(load().cosa_gpu_q_face_mut(self.h, idir, nl, _ptr(mut.ptr), _ptr(flux.ptr)), "q_face_mut")
+
+    def rtst(self, idir, nl, qf, dqxi, dqeta, dqzeta, vm, flux, tau1):
+        self._check(load().cosa_gpu_rtst(self.h, idir, nl, _ptr(qf.ptr), _ptr(dqxi.ptr), _ptr(dqeta.ptr),
+                                         _ptr(dqzeta.ptr), _ptr(vm.ptr), _ptr(flux.ptr), _ptr(tau1.ptr)), "rtst")
+
+    def vflux_kom(self, idir, nl, qf, dqxi, dqeta, dqzeta, tau1, vm, sijk, flux):
+        self._check(load().cosa_gpu_vflux_kom(self.h, idir, nl, _ptr(qf.ptr), _ptr(dqxi.ptr), _ptr(dqeta.ptr),
+                                              _ptr(dqzeta.ptr), _ptr(tau1.ptr), _ptr(vm.ptr), _ptr(sijk.ptr),
+                                              _ptr(flux.ptr)), "vflux_kom")
+
+    def q_der_c(self, idir, nl, qf, dqc):
+        self._check(load().cosa_gpu_q_der_c(self.h, idir, nl, _ptr(qf.ptr), _ptr(dqc.ptr)), "q_der_c")
+
+    def turprod(self, nl, dqxi, dqeta, dqzeta, vm, prd, divvel, delpls):
+        self._check(load().cosa_gpu_turprod(self.h, nl, _ptr(dqxi.ptr), _ptr(dqeta.ptr), _ptr(dqzeta.ptr),
+                                            _ptr(vm.ptr), _ptr(prd.ptr), _ptr(divvel.ptr), _ptr(delpls.ptr)),
+                    "turprod")
+
+    def srckw(self, nl, q, mut, prd, divvel, res, vol):
+        self._check(load().cosa_gpu_srckw(self.h, nl, _ptr(q.ptr), _ptr(mut.ptr), _ptr(prd.ptr), _ptr(divvel.ptr),
+                                          _ptr(res.ptr), _ptr(vol.ptr)), "srckw")
+
+    def update_kom(self, nl, res, q, qold, vol, dtvolt, delpls, prd, ar):
+        self._check(load().cosa_gpu_update_kom(self.h, nl, _ptr(res.ptr), _ptr(q.ptr), _ptr(qold.ptr), _ptr(vol.ptr),
+                                               _ptr(dtvolt.ptr), _ptr(delpls.ptr), _ptr(prd.ptr), C.c_double(ar)),
+                    "update_kom")
+
+    def cutman_mut(self, nl, mut):
+        self._check(load().cosa_gpu_cutman_mut(self.h, nl, _ptr(mut.ptr)), "cutman_mut")
 
     # ---- multigrid ---------------------------------------------------------------
     def q_edges(self, nl, q, mut=None):

@@ -190,7 +190,8 @@ int cosa_gpu_roflux(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *qr,
 /* resid (src/cosa.f90:1123-1211) */
 int cosa_gpu_resid(cosa_ctx *ctx, int32_t idir, int32_t nl,
                    const double *flux, double *res);
-/* update (src/update.f90:2-100, 568-762), explicit branch */
+/* update (src/update.f90:2-100, 568-762), explicit branch: variables 1..5
+   (with k-omega, cosa_gpu_update_kom first) */
 int cosa_gpu_update(cosa_ctx *ctx, int32_t nl, const double *res, double *q,
                     const double *qold, const double *dtvol, double ar);
 /* resg_rms (src/cosa.f90:4458-4582): resrms[0..npde] */
@@ -307,13 +308,48 @@ int cosa_gpu_vflux(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *qf, co
    4239-4297): lam(.,1:3) convective and lamv(.,1:3) viscous spectral radii
    (P3 layout, q primitive with halos) */
 int cosa_gpu_lambda_ns(cosa_ctx *ctx, int32_t nl, const double *q, const double *si,
-                       const double *sj, const double *sk, const double *vol, double *lam,
-                       double *lamv);
+                       const double *sj, const double *sk, const double *vol, const double *mut,
+                       double *lam, double *lamv);
 /* deltat with viscous = .true. (src/cosa.f90:4831-5180): dtvol with the
    viscous radii (irsop other than 5, 6), IRS coefficients with the viscous
-   floor for irsop 5 and 6 */
+   floor for irsop 5 and 6; with k-omega also dtvolt = cflt/cfl dtvol and
+   the turbulence coefficients tb* (ratt).  NULL pointers are skipped. */
 int cosa_gpu_deltat_ns(cosa_ctx *ctx, int32_t nl, double *dtvol, const double *lam,
-                       const double *lamv, double *bx, double *by, double *bz);
+                       const double *lamv, double *bx, double *by, double *bz,
+                       double *dtvolt, double *tbx, double *tby, double *tbz);
+
+/* ---- Wilcox k-omega (kom = .true., npde = 7); mut, prd, divvel, delpls
+   are scalar P3 arrays (-1:imax+1,...,0:S-1) ---- */
+/* q_face with calmut (src/flux.f90:2495-2540): face mut into flux(.,1) */
+int cosa_gpu_q_face_mut(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *mut, double *flux);
+/* rtst (src/flux.f90:2803-2946): Reynolds stresses tau1(.,1..6) on the faces
+   from q_face/q_der output, vm and the face mut in flux(.,1) */
+int cosa_gpu_rtst(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *qf, const double *dqxi,
+                  const double *dqeta, const double *dqzeta, const double *vm,
+                  const double *flux, double *tau1);
+/* vflux with kom (src/flux.f90:915-1180): Reynolds-stress and k/omega
+   diffusion fluxes plus the laminar terms; flux(.,1) holds the face mut on
+   entry */
+int cosa_gpu_vflux_kom(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *qf, const double *dqxi,
+                       const double *dqeta, const double *dqzeta, const double *tau1,
+                       const double *vm, const double *sijk, double *flux);
+/* q_der_c (src/flux.f90:2949-3130): cell-centred velocity differences of
+   the face values of family idir */
+int cosa_gpu_q_der_c(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *qf, double *dqc);
+/* turprod (src/src.f90:2-177): production, div u and delta+ */
+int cosa_gpu_turprod(cosa_ctx *ctx, int32_t nl, const double *dqxi, const double *dqeta,
+                     const double *dqzeta, const double *vm, double *prd, double *divvel,
+                     double *delpls);
+/* srckw (src/src.f90:179-272): k and omega sources into res(6:7) */
+int cosa_gpu_srckw(cosa_ctx *ctx, int32_t nl, const double *q, const double *mut, const double *prd,
+                   const double *divvel, double *res, const double *vol);
+/* update_b, k-omega part (src/update.f90:601-640): point-implicit rho omega
+   and rho k; call before cosa_gpu_update (which updates variables 1..5) */
+int cosa_gpu_update_kom(cosa_ctx *ctx, int32_t nl, const double *res, double *q, const double *qold,
+                        const double *vol, const double *dtvolt, const double *delpls,
+                        const double *prd, double ar);
+/* cutman_mut (src/bc.f90:2713-2799) */
+int cosa_gpu_cutman_mut(cosa_ctx *ctx, int32_t nl, double *mut);
 
 /* ---- fused: what smooth() calls when the GPU path is on ---- */
 /*

@@ -3133,4 +3133,8 @@ void orc_update_kom(orc_level *h, const cosa_params *p, const double *res, doubl
                     const double *vol, const double *dtvolt, const double *delpls, const double *prd, double ar) {
   for (int b = 0; b < h->L.nb; ++b) update_kom_b(h->L, b, res, q, qold, vol, dtvolt, delpls, prd, ar, *p);
 }
+void orc_deltat_ns_full(orc_level *h, const cosa_params *p, double *dtvol, const double *lam, const double *lamv,
+                        double *bx, double *by, double *bz, double *dtvolt, double *tbx, double *tby, double *tbz) {
+  deltat_ns_level(h->L, dtvol, lam, lamv, bx, by, bz, *p, dtvolt, tbx, tby, tbz);
+}
 }  // extern "C"

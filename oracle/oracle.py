@@ -492,3 +492,8 @@ def srckw(O, nl, q, mut, prd, divvel, res, vol):
 def update_kom(O, res, q, qold, vol, dtvolt, delpls, prd, ar):
     lib().orc_update_kom(O.h, _par(O.p), _p(res), _p(q), _p(qold), _p(vol), _p(dtvolt), _p(delpls), _p(prd),
                          C.c_double(ar))
+
+
+def deltat_ns_full(O, dtvol, lam, lamv, bx, by, bz, dtvolt, tbx, tby, tbz):
+    lib().orc_deltat_ns_full(O.h, _par(O.p), _p(dtvol), _p(lam), _p(lamv), _opt(bx), _opt(by), _opt(bz),
+                             _opt(dtvolt), _opt(tbx), _opt(tby), _opt(tbz))
