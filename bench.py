@@ -42,6 +42,9 @@ B_ALG_STAGE = 234
 # dt/V and write q (224 B); stage 1 writes dt/V instead of reading it and
 # copies q^n (264 B): average over the 4 stages of a cycle
 B_TILE = (3 * 224 + 264) / 4.0
+# face-split schedule: k_faces per cell (three face families) reads the
+# primitive state 40 + face metrics 96 and writes the face fluxes 120
+B_FACES = 256
 # DRAM bytes (read + write) per cell of one tile launch, from the ncu capture
 # summarised in profiles/k_stage_tile_fp64_duct4m.md (a stage-3 launch on the
 # 4.1 M-cell duct, scaled by the cells of the launch)
@@ -186,6 +189,48 @@ def time_smooth(ctx, steps: int, torch):
     return e0.elapsed_time(e1)
 
 
+def viscous_leg(kind: str, steps: int, warmup: int, dev: int, torch):
+    """FP64 throughput of the laminar (fused stage + viscous face kernels) or
+    Wilcox k-omega (routine by routine) path on the duct generator with
+    no-slip walls: Mcell-stage/s, device-timed like the main leg."""
+    from cosa_b200 import cases, gpu
+    if kind == "laminar":
+        segs = cases.duct_segments(seed=3, lo=3_500_000, hi=4_500_000, choices=tuple(range(24, 97, 8)))
+        p = cases.laminar_params(0.6, 1.0e4)
+    else:
+        segs = cases.duct_segments(seed=3, lo=900_000, hi=1_300_000, choices=tuple(range(24, 65, 8)))
+        p = cases.kom_params(0.6, 1.0e5)
+    case = cases.duct3d(segs=segs, wall=cases.VISCOUS_WALL, params=p)
+    ctx = gpu.Context([case.tables], p, device=dev)
+    X, Y, Z = (ctx.alloc_p2(ncomp=1).upload(a) for a in (case.x, case.y, case.z))
+    si, sj, sk = (ctx.alloc_p2() for _ in range(3))
+    vol = ctx.alloc_p1()
+    ctx.imetrix(1, X, Y, Z, si, sj, sk)
+    ctx.vols(1, X, Y, Z, vol)
+    vm = ctx.alloc_vm()
+    ctx.viscous_setup(1, X, Y, Z, vol, vm)
+    q = ctx.alloc_p3().upload(case.q0)
+    arrays = dict(q=q, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(), si=si, sj=sj, sk=sk, vol=vol)
+    if kind == "kom":
+        mut = ctx.alloc_p3s()
+        dist = ctx.alloc_p1().upload(cases.wall_distance(case))
+        arrays.update(res=ctx.alloc_p3(), dtvolt=ctx.alloc_p1(), qp=ctx.alloc_p3(), qm=ctx.alloc_p3(),
+                      dq=ctx.alloc_p3(), dqp=ctx.alloc_p3(), dqm=ctx.alloc_p3(), flux=ctx.alloc_f0(), mut=mut,
+                      dist=dist)
+        # the free stream's turbulent viscosity (tur_vis of the initial state)
+        ctx.tur_vis(1, q, mut)
+    ctx.bind_level(1, **arrays)
+    ctx.smooth(1, warmup, 1, 10 ** 6, want_hist=False)
+    ctx.launch_count(reset=True)
+    ms = time_smooth(ctx, steps, torch)
+    launches = ctx.launch_count(reset=True)
+    ctx.close()
+    return {"value": case.ncells * p.nstage * steps / (ms / 1e3) / 1e6, "unit": "Mcell-stage/s",
+            "ms_per_step": ms / steps, "cells": case.ncells, "steps": steps, "gpu_launches": launches,
+            "workload": f"bump duct, segments {segs}, no-slip walls (1500), "
+                        + ("laminar Re=1e4" if kind == "laminar" else "Wilcox k-omega Re=1e5") + ", M=0.6, FP64"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -198,6 +243,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed, e2e and CPU legs (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving sweep")
+    ap.add_argument("--no-viscous", action="store_true", help="skip the laminar and k-omega legs")
+    ap.add_argument("--schedule", type=int, default=0, choices=[0, 1, 2],
+                    help="0: autotune the stage schedule, 1: fused tile kernel, 2: face-split")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="precision of the main timed leg (profiling runs; the default line reports both)")
     args = ap.parse_args()
@@ -239,7 +287,13 @@ def main():
     ctx.bind_level(1, q=q, qold=qold, dtvol=dtvol, si=si, sj=sj, sk=sk, vol=vol)
     nstage = p.nstage
 
-    # ---- FP64 fused path: warm-up then the timed region -------------------------
+    # ---- stage schedule: the autotuner times the fused tile kernel and the
+    # face-split schedule on this grid and keeps the faster (state restored)
+    sched_fp64 = ctx.autotune(1, 3) if not args.schedule else (None, None, args.schedule - 1)
+    if args.schedule:
+        ctx.set_schedule(1, args.schedule - 1)
+
+    # ---- FP64 path: warm-up then the timed region -------------------------------
     ctx.smooth(1, args.warmup, 1, 10 ** 6, want_hist=False)
     if pg:
         pg.barrier()
@@ -261,8 +315,9 @@ def main():
     # ---- kernel roofline: event-timed pass right after the timed region ----------
     kms, kcnt = ctx.profile(1, 3)
     peak, peak_kind = _peaks()
-    tile_bytes = B_TILE * ncells
-    achieved = tile_bytes / (kms[1] / 1e3) / 1e9
+    split = sched_fp64[2] == 1
+    main_bytes = (B_FACES if split else B_TILE) * ncells
+    achieved = main_bytes / (kms[1] / 1e3) / 1e9
     stage_gbs = B_ALG_STAGE * ncells * nstage * args.steps / (ms / 1e3) / 1e9
 
     if args.no_extras:
@@ -270,7 +325,8 @@ def main():
             print(json.dumps({"metric": "Mcell-stage/s", "value": value, "unit": "Mcell-stage/s", "n_gpus": ws,
                               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
                               "higher_is_better": True, "dtype": "f64", "config": {"workload": desc},
-                              "tile_kernel_ms": kms[1], "halo_ms": kms[0], "gpu_launches": launches}), flush=True)
+                              "main_kernel_ms": kms[1], "halo_ms": kms[0], "cells_kernel_ms": kms[3],
+                              "schedule": sched_fp64, "gpu_launches": launches}), flush=True)
         ctx.close()
         return
 
@@ -280,11 +336,13 @@ def main():
     pm.precision = PREC_MIXED
     ctx.set_params(pm)
     q.upload(case.q0)
+    sched_mixed = ctx.autotune(1, 3) if not args.schedule else (None, None, args.schedule - 1)
     ctx.smooth(1, args.warmup, 1, 10 ** 6, want_hist=False)
     ms_mixed = time_smooth(ctx, args.steps, torch)
     kms_m, _ = ctx.profile(1, 3)
     value_mixed = ws * ncells * nstage * args.steps / (ms_mixed / 1e3) / 1e6
     ctx.set_params(p)
+    ctx.set_schedule(1, sched_fp64[2])
 
     # ---- end to end through the host-buffer entry point --------------------------------
     nq = q.n
@@ -309,6 +367,14 @@ def main():
     e2e_ms = max(e0.elapsed_time(e1), wall * 1e3)
     e2e_val = ws * ncells * nstage * args.e2e_steps / (e2e_ms / 1e3) / 1e6
     state_bytes = nq * 8
+
+    viscous = {}
+    if rank == 0 and ws == 1 and not args.no_viscous:
+        for kind in ("laminar", "kom"):
+            try:
+                viscous[kind] = viscous_leg(kind, min(args.steps, 10), 3, dev, torch)
+            except Exception as e:  # reported, not fatal
+                viscous[kind] = {"error": str(e)}
 
     serving = None
     if rank == 0 and ws == 1 and not args.no_serve:
@@ -339,17 +405,25 @@ def main():
                        "l2": "state 1.4 GB > L2 (126 MB): no flush needed",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": TILE_TRAFFIC_B_PER_CELL * ncells,
-                         "traffic_source": "ncu dram bytes per cell of the 4.1 M-cell duct x cells",
-                         "kernel": "k_stage_tile<32,7,fp64>",
-                         "kernel_ms": kms[1], "halo_ms": kms[0], "bytes_per_cell": B_TILE,
+                         "frac": achieved / peak,
+                         "traffic": None if split else TILE_TRAFFIC_B_PER_CELL * ncells,
+                         "traffic_source": None if split else
+                         "ncu dram bytes per cell of the 4.1 M-cell duct x cells",
+                         "kernel": "k_faces<fp64>" if split else "k_stage_tile<32,7,fp64>",
+                         "kernel_ms": kms[1], "halo_ms": kms[0], "cells_kernel_ms": kms[3] if split else None,
+                         "bytes_per_cell": B_FACES if split else B_TILE,
                          "peak_kind": peak_kind, "stage_gbs_alg": stage_gbs},
+            "schedule": {"fp64": {"tile_ms_per_step": sched_fp64[0], "split_ms_per_step": sched_fp64[1],
+                                  "chosen": ["tile", "split"][sched_fp64[2]]},
+                         "mixed": {"tile_ms_per_step": sched_mixed[0], "split_ms_per_step": sched_mixed[1],
+                                   "chosen": ["tile", "split"][sched_mixed[2]]}},
             "mixed": {"value": value_mixed, "ms_per_step": ms_mixed / args.steps,
                       "speedup_vs_fp64": value_mixed / value if value else None,
-                      "tile_kernel_ms": kms_m[1]},
+                      "main_kernel_ms": kms_m[1], "cells_kernel_ms": kms_m[3]},
             "e2e": {"value": e2e_val, "unit": "Mcell-stage/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes + 8 * (p.npde + 1)},
             "cpu_baseline": cpu,
+            "viscous": viscous or None,
             "serving": serving,
             "gpu_launches": launches,
             "clocks": clocks,

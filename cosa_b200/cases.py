@@ -415,11 +415,12 @@ def wall_distance(case: Case) -> np.ndarray:
     out = np.zeros(tot["p1"])
     for b, (v, X, Y, Z) in enumerate(zip(p1_views(t, out, 1), gx, gy, gz)):
         N = np.stack([X[1:-1, 1:-1, 1:-1].ravel(), Y[1:-1, 1:-1, 1:-1].ravel(), Z[1:-1, 1:-1, 1:-1].ravel()], 1)
-        dn = np.full(len(N), 1e20)
-        for c in range(0, len(W), 256):
-            dd = ((N[:, None, :] - W[None, c:c + 256, :]) ** 2).sum(-1).min(1)
-            dn = np.minimum(dn, dd)
-        dn = np.sqrt(dn).reshape(X[1:-1, 1:-1, 1:-1].shape, order="F")
+        if len(W):
+            from scipy.spatial import cKDTree
+            dn, _ = cKDTree(W).query(N, workers=-1)
+        else:
+            dn = np.full(len(N), 1e20)
+        dn = np.asarray(dn).reshape(X[1:-1, 1:-1, 1:-1].shape, order="F")
         cell = (dn[:-1, :-1, :-1] + dn[1:, :-1, :-1] + dn[:-1, 1:, :-1] + dn[1:, 1:, :-1] +
                 dn[:-1, :-1, 1:] + dn[1:, :-1, 1:] + dn[:-1, 1:, 1:] + dn[1:, 1:, 1:]) / 8
         V = v[..., 0]
@@ -449,7 +450,7 @@ def duct_params(mach: float = 0.6) -> CosaParams:
 
 
 def duct3d(segs=None, seed: int = 3, lo: int = 27_000_000, hi: int = 33_000_000,
-           mach: float = 0.6, grid: bool = True) -> Case:
+           mach: float = 0.6, grid: bool = True, wall: int = 14, params: CosaParams = None) -> Case:
     if segs is None:
         segs = duct_segments(seed, lo, hi)
     si, sj, sk = segs
@@ -468,10 +469,10 @@ def duct3d(segs=None, seed: int = 3, lo: int = 27_000_000, hi: int = 33_000_000,
                 types = {}
                 if bi == 0: types["imin"] = 21
                 if bi == len(si) - 1: types["imax"] = 91
-                if bj == 0: types["jmin"] = 14
-                if bj == len(sj) - 1: types["jmax"] = 14
-                if bk == 0: types["kmin"] = 14
-                if bk == len(sk) - 1: types["kmax"] = 14
+                if bj == 0: types["jmin"] = wall
+                if bj == len(sj) - 1: types["jmax"] = wall
+                if bk == 0: types["kmin"] = wall
+                if bk == len(sk) - 1: types["kmax"] = wall
                 dims = (i1 - i0 + 1, j1 - j0 + 1, k1 - k0 + 1)
                 specs.append(BlockSpec(*dims, _face_bcs(*dims, types)))
                 if grid:
@@ -502,7 +503,7 @@ def duct3d(segs=None, seed: int = 3, lo: int = 27_000_000, hi: int = 33_000_000,
                 s1, e1 = (1, 1, d.kmax), (d.imax, d.jmax, d.kmax)
                 s2, e2 = (1, 1, 1), (od.imax, od.jmax, 1)
             cuts.append((b, s1, e1, o, s2, e2, (1, 2, 3)))
-    p = duct_params(mach)
+    p = params if params is not None else duct_params(mach)
     if not grid:
         tables = build_tables(specs, cuts)
         return Case(f"duct3d_{NI}x{NJ}x{NK}", tables, p, None, None, None, None)

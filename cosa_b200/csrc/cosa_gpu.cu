@@ -17,6 +17,7 @@
 #include "mg.cuh"
 #include "visc.cuh"
 #include "kom.cuh"
+#include "split.cuh"
 
 namespace {
 
@@ -65,15 +66,21 @@ struct LevelState {
   // coefficients (P1 x S)
   double *d_prd = nullptr, *d_divvel = nullptr, *d_delpls = nullptr;
   double *d_tbeta[3] = {nullptr, nullptr, nullptr};
+  // stage schedule: 0 = fused tile kernel, 1 = face-split (k_faces + k_cells),
+  // set by cosa_gpu_autotune
+  int schedule = 0;
+  double *d_cflux = nullptr;  // convective face fluxes of the split schedule (3 x F0)
 };
 
 }  // namespace
 
 struct ProfState {
   bool on = false;
-  cudaEvent_t ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [kind][start/stop]
-  double ms[2] = {0, 0};
-  long long n[2] = {0, 0};
+  // kinds: 0 halo fill, 1 main kernel (k_stage_tile, or k_faces of the split
+  // schedule), 2 the split schedule's k_cells
+  cudaEvent_t ev[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};  // [kind][start/stop]
+  double ms[3] = {0, 0, 0};
+  long long n[3] = {0, 0, 0};
 };
 
 struct GraphEntry {
@@ -627,7 +634,8 @@ int grid_x(int64_t n, int nb) {
 
 // viscous part of one stage on the halo-filled state qin: primitive copy,
 // q_edges, [time step], face fluxes, wall faces, flux balance -> L.d_vres
-int launch_visc(cosa_ctx *c, LevelState &L, const double *qin, bool dt, double *bx, double *by, double *bz) {
+int launch_visc(cosa_ctx *c, LevelState &L, const double *qin, bool dt, double *bx, double *by, double *bz,
+                bool have_prim = false) {
   const cosa_params &p = c->p;
   const int S = 2 * p.nharms + 1;
   int64_t m3 = 0, mc = 0, mf = 0;
@@ -636,9 +644,11 @@ int launch_visc(cosa_ctx *c, LevelState &L, const double *qin, bool dt, double *
     mc = std::max<int64_t>(mc, (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * S);
     mf = std::max<int64_t>(mf, (int64_t)x.im * x.jm * x.km * S);
   }
-  k_prim<<<dim3(grid_x(m3, L.nb), L.nb), 256, 0, c->s>>>(L.d_blocks, c->d_p, qin, L.d_qprim);
-  int r = after_launch(c);
-  if (r) return r;
+  int r = 0;
+  if (!have_prim) {
+    k_prim<<<dim3(grid_x(m3, L.nb), L.nb), 256, 0, c->s>>>(L.d_blocks, c->d_p, qin, L.d_qprim);
+    if ((r = after_launch(c))) return r;
+  }
   if ((r = launch_edges(c, L, L.d_qprim, nullptr))) return r;
   const cosa_level_ptrs &P = L.ptrs;
   if (dt) {
@@ -657,6 +667,54 @@ int launch_visc(cosa_ctx *c, LevelState &L, const double *qin, bool dt, double *
   }
   k_vdiv<<<dim3(grid_x(mc, L.nb), L.nb), 256, 0, c->s>>>(L.d_blocks, c->d_p, L.d_vflux, L.n0, L.d_vres);
   return after_launch(c);
+}
+
+constexpr int kCellsGX = 64;  // CTAs per block of k_cells (fixed: deterministic norm partials)
+
+// split schedule after the halo fill and the primitive copy: face fluxes,
+// cell epilogue, norm reduction
+int launch_split_tail(cosa_ctx *c, int nl, LevelState &L, StageArgs &A, bool want_rms) {
+  const cosa_params &p = c->p;
+  const int S = 2 * p.nharms + 1;
+  int64_t mf = 0;
+  for (const DevBlock &x : L.hb) mf = std::max<int64_t>(mf, (int64_t)x.im * x.jm * x.km * S);
+  const bool mixed = p.precision == COSA_PREC_MIXED;
+  const dim3 gf(grid_x(mf, L.nb), L.nb, 3);
+  if (c->prof.on) cudaEventRecord(c->prof.ev[1][0], c->s);
+  if (mixed)
+    k_faces<true><<<gf, 128, 0, c->s>>>(L.d_blocks, c->d_p, L.d_qprim, A.si, A.sj, A.sk, L.d_strong, L.d_smap,
+                                         A.first_order, L.n0, L.d_cflux);
+  else
+    k_faces<false><<<gf, 128, 0, c->s>>>(L.d_blocks, c->d_p, L.d_qprim, A.si, A.sj, A.sk, L.d_strong, L.d_smap,
+                                          A.first_order, L.n0, L.d_cflux);
+  int r = after_launch(c);
+  if (r) return r;
+  if (c->prof.on) {
+    prof_stop(c, 1);
+    cudaEventRecord(c->prof.ev[2][0], c->s);
+  }
+  A.part = want_rms ? L.d_part : nullptr;
+  const dim3 gc(kCellsGX, L.nb);
+  if (A.compute_dt) {
+    int64_t mc = 0;
+    for (const DevBlock &x : L.hb) mc = std::max<int64_t>(mc, (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * S);
+    k_dt_euler<<<dim3(grid_x(mc, L.nb), L.nb), 256, 0, c->s>>>(L.d_blocks, c->d_p, L.d_qprim, A.si, A.sj, A.sk,
+                                                               A.dtvol, A.bx, A.by, A.bz);
+    if ((r = after_launch(c))) return r;
+  }
+  if (want_rms) k_cells<true><<<gc, 256, 0, c->s>>>(L.d_blocks, c->d_p, A, L.d_qprim, L.d_cflux, L.n0);
+  else k_cells<false><<<gc, 256, 0, c->s>>>(L.d_blocks, c->d_p, A, L.d_qprim, L.d_cflux, L.n0);
+  if ((r = after_launch(c))) return r;
+  if (c->prof.on) prof_stop(c, 2);
+  if (want_rms) {
+    int64_t ncell = 0;
+    for (auto &b : L.hb) ncell += (int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1);
+    const double cnt = (double)ncell * (p.harbal ? S : 1);
+    k_rms_final<<<1, 256, 0, c->s>>>(L.d_part, L.nb * kCellsGX, p.npde, cnt, c->d_hist, c->d_row, c->hist_cap);
+    if ((r = after_launch(c))) return r;
+  }
+  (void)nl;
+  return COSA_OK;
 }
 
 // one stage: halo fill + tile kernel (+ norm reduction)
@@ -692,17 +750,27 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   A.ar = p.alphas[irk - 1];
   A.vol = p.harbal ? P.vol : nullptr;
   A.compute_dt = compute_dt;
+  A.first_order = nl >= p.nl_crs;
+  A.update = update;
+  const bool split = L.schedule == 1 && c->nseg == 0 && L.d_cflux && L.d_qprim;
+  if (split) {
+    // primitive copy (with bprtest) shared by the viscous and convective faces
+    int64_t m3 = 0;
+    for (const DevBlock &x : L.hb) m3 = std::max<int64_t>(m3, x.P3 * S);
+    k_prim<<<dim3(grid_x(m3, L.nb), L.nb), 256, 0, c->s>>>(L.d_blocks, c->d_p, qin, L.d_qprim, c->d_status);
+    int r = after_launch(c);
+    if (r) return r;
+  }
   if (p.viscous) {
     // the viscous terms and, on stage 1, the viscous time step come first
     if (!L.d_vm || !L.d_vres || !P.vol) return COSA_ERR_ARG;
-    int r = launch_visc(c, L, qin, compute_dt != 0, A.bx, A.by, A.bz);
+    int r = launch_visc(c, L, qin, compute_dt != 0, A.bx, A.by, A.bz, split);
     if (r) return r;
     A.vres = L.d_vres;
     A.compute_dt = 0;
     A.bx = A.by = A.bz = nullptr;
   }
-  A.first_order = nl >= p.nl_crs;
-  A.update = update;
+  if (split) return launch_split_tail(c, nl, L, A, want_rms);
   const size_t smem = stage_smem_bytes<kTI, kTJ>();
   if (c->prof.on) cudaEventRecord(c->prof.ev[1][0], c->s);
   // the residual-norm partials are a separate instantiation: their
@@ -1652,7 +1720,7 @@ int cosa_gpu_mg(cosa_ctx *c, int32_t mgit0, int32_t ncycles, int32_t ncycle, int
   return cosa_gpu_status(c, 0);
 }
 
-int cosa_gpu_profile(cosa_ctx *c, int32_t nl, int32_t niter, double ms[3], int64_t counts[3]) {
+int cosa_gpu_profile(cosa_ctx *c, int32_t nl, int32_t niter, double ms[4], int64_t counts[4]) {
   LevelState *L = level(c, nl);
   if (!L || !L->bound || niter < 1 || !ms || !counts) return COSA_ERR_ARG;
   int r = check_fused_supported(c->p);
@@ -1661,8 +1729,8 @@ int cosa_gpu_profile(cosa_ctx *c, int32_t nl, int32_t niter, double ms[3], int64
   for (auto &e2 : pf.ev)
     for (auto &e : e2)
       if (!e) CK(cudaEventCreate(&e));
-  pf.ms[0] = pf.ms[1] = 0;
-  pf.n[0] = pf.n[1] = 0;
+  pf.ms[0] = pf.ms[1] = pf.ms[2] = 0;
+  pf.n[0] = pf.n[1] = pf.n[2] = 0;
   pf.on = true;
   cudaEvent_t t0, t1;
   CK(cudaEventCreate(&t0));
@@ -1684,9 +1752,11 @@ int cosa_gpu_profile(cosa_ctx *c, int32_t nl, int32_t niter, double ms[3], int64
   ms[0] = pf.n[0] ? pf.ms[0] / pf.n[0] : 0.0;
   ms[1] = pf.n[1] ? pf.ms[1] / pf.n[1] : 0.0;
   ms[2] = tot / niter;
+  ms[3] = pf.n[2] ? pf.ms[2] / pf.n[2] : 0.0;
   counts[0] = pf.n[0];
   counts[1] = pf.n[1];
   counts[2] = niter;
+  counts[3] = pf.n[2];
   return cosa_gpu_status(c, 0);
 }
 
@@ -2222,5 +2292,79 @@ int launch_rans_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o)
 }
 
 }  // namespace
+
+// ---- stage schedule autotuner -----------------------------------------------------------
+namespace {
+int ensure_split(cosa_ctx *c, LevelState &L) {
+  const int S = 2 * c->p.nharms + 1;
+  int r = 0;
+  if (!L.d_qprim && (r = dalloc(c, &L.d_qprim, (size_t)L.n3 * 5 * S))) return r;
+  if (!L.d_cflux && (r = dalloc(c, &L.d_cflux, (size_t)3 * L.n0 * 5 * S))) return r;
+  if (L.npart_cap < L.nb * kCellsGX) {
+    drop_graphs(c);
+    if ((r = dalloc(c, &L.d_part, (size_t)L.nb * kCellsGX * 8))) return r;
+    L.npart_cap = L.nb * kCellsGX;
+  }
+  return COSA_OK;
+}
+}  // namespace
+
+extern "C" int cosa_gpu_autotune(cosa_ctx *c, int32_t nl, int32_t niter, double ms[2], int32_t *choice) {
+  LevelState *L = level(c, nl);
+  if (!L || !L->bound || niter < 1 || !ms) return COSA_ERR_ARG;
+  int r = check_fused_supported(c->p);
+  if (r) return r;
+  ms[0] = ms[1] = 0.0;
+  if (c->p.kom) {  // the k-omega stage has one schedule
+    L->schedule = 0;
+    if (choice) *choice = 0;
+    return COSA_OK;
+  }
+  cudaSetDevice(c->device);
+  if ((r = ensure_split(c, *L))) return r;
+  const int S = 2 * c->p.nharms + 1;
+  const size_t nq = (size_t)L->n3 * c->p.npde * S;
+  double *save = nullptr;
+  CK(cudaMalloc(&save, nq * sizeof(double)));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaMemcpyAsync(save, L->ptrs.q, nq * sizeof(double), cudaMemcpyDeviceToDevice, c->s);
+  for (int sched = 0; sched < 2 && !r; ++sched) {
+    L->schedule = sched;
+    drop_graphs(c);
+    if ((r = cosa_gpu_smooth(c, nl, 1, 1 << 30, 1 << 30, nullptr))) break;  // capture + warm-up
+    cudaEventRecord(e0, c->s);
+    if ((r = cosa_gpu_smooth(c, nl, niter, 1 << 30, 1 << 30, nullptr))) break;
+    cudaEventRecord(e1, c->s);
+    cudaEventSynchronize(e1);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    ms[sched] = t / niter;
+    cudaMemcpyAsync(L->ptrs.q, save, nq * sizeof(double), cudaMemcpyDeviceToDevice, c->s);
+  }
+  const int best = (!r && ms[1] > 0.0 && ms[1] < ms[0]) ? 1 : 0;
+  L->schedule = best;
+  drop_graphs(c);
+  cudaStreamSynchronize(c->s);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(save);
+  if (choice) *choice = best;
+  return r ? r : cuda_ok(cudaGetLastError());
+}
+
+/* force a schedule (0 tile, 1 split) without timing */
+extern "C" int cosa_gpu_set_schedule(cosa_ctx *c, int32_t nl, int32_t schedule) {
+  LevelState *L = level(c, nl);
+  if (!L || schedule < 0 || schedule > 1) return COSA_ERR_ARG;
+  if (schedule == 1) {
+    int r = ensure_split(c, *L);
+    if (r) return r;
+  }
+  L->schedule = schedule;
+  drop_graphs(c);
+  return COSA_OK;
+}
 
 #include "serve.cuh"

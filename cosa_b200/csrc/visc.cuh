@@ -347,7 +347,8 @@ __device__ __forceinline__ void load_vm(const double *__restrict__ vm, const Dev
 // ---- per-stage kernels of the fused viscous path -------------------------------------
 // primitive copy of a stage state (interior conservative, halos primitive)
 __global__ void k_prim(const DevBlock *__restrict__ blocks, const cosa_params *__restrict__ Pp,
-                       const double *__restrict__ q, double *__restrict__ qp) {
+                       const double *__restrict__ q, double *__restrict__ qp, int *status = nullptr) {
+  int st = 0;
   const DevBlock b = blocks[blockIdx.y];
   const cosa_params &P = *Pp;
   const int S = 2 * P.nharms + 1;
@@ -360,10 +361,16 @@ __global__ void k_prim(const DevBlock *__restrict__ blocks, const cosa_params *_
     double v[5];
 #pragma unroll
     for (int m = 0; m < 5; ++m) v[m] = q[base + m * b.P3];
-    if (i >= 1 && i <= b.im - 1 && j >= 1 && j <= b.jm - 1 && k >= 1 && k <= b.km - 1) c2p5_nr(P.gamma, v);
+    if (i >= 1 && i <= b.im - 1 && j >= 1 && j <= b.jm - 1 && k >= 1 && k <= b.km - 1) {
+      c2p5_nr(P.gamma, v);
+      // bprtest on the interior (src/cosa.f90:1000-1040)
+      if (v[4] <= P.qmin[4]) st |= COSA_ERR_NEG_P;
+      else if (v[0] <= P.qmin[0]) st |= COSA_ERR_NEG_RHO;
+    }
 #pragma unroll
     for (int m = 0; m < 5; ++m) qp[base + m * b.P3] = v[m];
   }
+  if (st && status) atomicOr(status, st);
 }
 
 // viscous flux of every face: grid (x, nblocks, 3 families)

@@ -62,6 +62,7 @@ SYMBOLS = [
     "cosa_gpu_vmetrix", "cosa_gpu_viscous_setup", "cosa_gpu_q_face", "cosa_gpu_q_der", "cosa_gpu_vflux",
     "cosa_gpu_lambda_ns", "cosa_gpu_deltat_ns", "cosa_gpu_q_face_mut", "cosa_gpu_rtst", "cosa_gpu_vflux_kom",
     "cosa_gpu_q_der_c", "cosa_gpu_turprod", "cosa_gpu_srckw", "cosa_gpu_update_kom", "cosa_gpu_cutman_mut",
+    "cosa_gpu_autotune", "cosa_gpu_set_schedule",
 ]
 
 
@@ -269,10 +270,21 @@ class Context:
         self._check(load().cosa_gpu_vols(self.h, nl, _ptr(x.ptr), _ptr(y.ptr), _ptr(z.ptr), _ptr(vol.ptr)), "vols")
 
     def profile(self, nl, niter):
-        ms = (C.c_double * 3)()
-        cnt = (C.c_int64 * 3)()
+        ms = (C.c_double * 4)()
+        cnt = (C.c_int64 * 4)()
         self._check(load().cosa_gpu_profile(self.h, nl, niter, ms, cnt), "profile")
         return list(ms), list(cnt)
+
+    def autotune(self, nl=1, niter=5):
+        """Time the fused-tile and face-split stage schedules on level nl and
+        keep the faster; returns (ms_tile, ms_split, choice)."""
+        ms = (C.c_double * 2)()
+        ch = C.c_int32()
+        self._check(load().cosa_gpu_autotune(self.h, nl, niter, ms, C.byref(ch)), "autotune")
+        return ms[0], ms[1], ch.value
+
+    def set_schedule(self, nl, schedule):
+        self._check(load().cosa_gpu_set_schedule(self.h, nl, schedule), "set_schedule")
 
     def stream(self) -> int:
         return int(load().cosa_gpu_stream(self.h) or 0)

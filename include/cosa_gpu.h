@@ -387,11 +387,20 @@ int cosa_gpu_smooth_level(cosa_ctx *ctx, int32_t nl, int32_t niter, int32_t from
  */
 int cosa_gpu_mg(cosa_ctx *ctx, int32_t mgit0, int32_t ncycles, int32_t ncycle,
                 int32_t rms_every, double *hist);
+/* stage-schedule autotuner (no reference counterpart): times niter
+   iterations of level nl with the fused tile kernel (schedule 0) and with
+   the face-split schedule (1: face fluxes through HBM, then a cell pass),
+   keeps the faster for the level and returns the ms per iteration of each;
+   the level's state is restored afterwards.  set_schedule forces one. */
+int cosa_gpu_autotune(cosa_ctx *ctx, int32_t nl, int32_t niter, double ms[2], int32_t *choice);
+int cosa_gpu_set_schedule(cosa_ctx *ctx, int32_t nl, int32_t schedule);
 /* niter fused iterations without graphs, with CUDA events around every
-   kernel: ms[0] = mean halo-kernel time, ms[1] = mean tile-kernel time,
-   ms[2] = mean iteration time; counts = launches timed */
-int cosa_gpu_profile(cosa_ctx *ctx, int32_t nl, int32_t niter, double ms[3],
-                     int64_t counts[3]);
+   kernel: ms[0] = mean halo-kernel time, ms[1] = mean time of the main
+   kernel (k_stage_tile, or k_faces under the split schedule), ms[2] = mean
+   iteration time, ms[3] = mean k_cells time (split schedule);
+   counts = launches timed */
+int cosa_gpu_profile(cosa_ctx *ctx, int32_t nl, int32_t niter, double ms[4],
+                     int64_t counts[4]);
 /* diagnostics: evaluates the fused kernel's Newton-Raphson reciprocal and
    reciprocal square root on n host values x (positive normal numbers) on
    the current device and returns in err[0], err[1] the largest relative

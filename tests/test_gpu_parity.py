@@ -372,3 +372,40 @@ def test_newton_raphson_reciprocals_within_ulps():
     eps = np.finfo(np.float64).eps
     assert e_rcp <= 4 * eps, e_rcp / eps
     assert e_rsq <= 4 * eps, e_rsq / eps
+
+
+@pytest.mark.parametrize("which", ["channel", "partitioned", "duct"])
+def test_split_schedule_matches_oracle(oracle_mod, which):
+    """The face-split stage schedule (face fluxes through HBM, then the cell
+    pass) against the oracle, like the fused tile kernel."""
+    case = FUSED_CASES[which]()
+    O, ctx, (si, sj, sk, vol), q = _setup(case, oracle_mod, seed=11)
+    ncyc = 6
+    qo = q.copy()
+    hist_o, st_o = O.smooth(qo, si, sj, sk, ncyc, rms_every=2)
+    assert st_o == 0
+    dq_ = ctx.alloc_p3().upload(q)
+    m = [ctx.alloc_p2().upload(a) for a in (si, sj, sk)]
+    ctx.bind_level(1, q=dq_, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(), si=m[0], sj=m[1], sk=m[2])
+    ctx.set_schedule(1, 1)
+    hist_g, st = ctx.smooth(1, ncyc, 1, 2)
+    assert st == 0
+    assert _rel(dq_.download(), qo, case) <= TOL
+    rows = ~np.isnan(hist_o[:, 0])
+    np.testing.assert_allclose(hist_g[rows], hist_o[rows], rtol=1e-9)
+    ctx.close()
+
+
+def test_autotune_restores_state_and_picks_a_schedule(oracle_mod):
+    case = casekit.small_duct()
+    O, ctx, (si, sj, sk, vol), q = _setup(case, oracle_mod, seed=3)
+    dq_ = ctx.alloc_p3().upload(q)
+    m = [ctx.alloc_p2().upload(a) for a in (si, sj, sk)]
+    ctx.bind_level(1, q=dq_, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(), si=m[0], sj=m[1], sk=m[2])
+    t0, t1, choice = ctx.autotune(1, 3)
+    assert t0 > 0 and t1 > 0 and choice in (0, 1)
+    assert choice == (1 if t1 < t0 else 0)
+    assert np.array_equal(dq_.download(), q)
+    _, st = ctx.smooth(1, 2, 1, 1)
+    assert st == 0
+    ctx.close()
