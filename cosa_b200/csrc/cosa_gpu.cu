@@ -679,7 +679,7 @@ int launch_split_tail(cosa_ctx *c, int nl, LevelState &L, StageArgs &A, bool wan
   int64_t mf = 0;
   for (const DevBlock &x : L.hb) mf = std::max<int64_t>(mf, (int64_t)x.im * x.jm * x.km * S);
   const bool mixed = p.precision == COSA_PREC_MIXED;
-  const dim3 gf(grid_x(mf, L.nb), L.nb, 3);
+  const dim3 gf(grid_x(mf, L.nb), 3, L.nb);
   if (c->prof.on) cudaEventRecord(c->prof.ev[1][0], c->s);
   if (mixed)
     k_faces<true><<<gf, 128, 0, c->s>>>(L.d_blocks, c->d_p, L.d_qprim, A.si, A.sj, A.sk, L.d_strong, L.d_smap,
@@ -2298,6 +2298,8 @@ namespace {
 int ensure_split(cosa_ctx *c, LevelState &L) {
   const int S = 2 * c->p.nharms + 1;
   int r = 0;
+  for (const DevBlock &x : L.hb)  // the split kernels index faces of a block in 32 bits
+    if ((int64_t)x.im * x.jm * x.km * S >= (int64_t)1 << 31) return COSA_ERR_UNSUPPORTED;
   if (!L.d_qprim && (r = dalloc(c, &L.d_qprim, (size_t)L.n3 * 5 * S))) return r;
   if (!L.d_cflux && (r = dalloc(c, &L.d_cflux, (size_t)3 * L.n0 * 5 * S))) return r;
   if (L.npart_cap < L.nb * kCellsGX) {

@@ -56,28 +56,30 @@ __device__ __forceinline__ void split_face(const PhysPar &ph, bool first_order, 
   else roe_flux_euler(ph, met[0], met[1], met[2], met[3], qr, ql, F);
 }
 
-// grid (x, nblocks, 3 families); face flux of family d into cf + (d-1)*n0*5*S
-// (F0 layout per family)
+// grid (x, 3 families, nblocks): the three families of a block run one after
+// the other, so the block's state stays in L2 across them; face flux of
+// family d into cf + (d-1)*n0*5*S (F0 layout per family)
 template <bool MIXED>
 __global__ void __launch_bounds__(128, 5) k_faces(const DevBlock *__restrict__ blocks, const cosa_params *__restrict__ Pp,
                                                const double *__restrict__ qp, const double *__restrict__ si,
                                                const double *__restrict__ sj, const double *__restrict__ sk,
                                                const uint8_t *__restrict__ strong, const StrongMap *__restrict__ smap,
                                                int first_order, int64_t n0, double *__restrict__ cf) {
-  const DevBlock b = blocks[blockIdx.y];
-  const int d = blockIdx.z + 1;
+  const DevBlock b = blocks[blockIdx.z];
+  const int d = blockIdx.y + 1;
   const cosa_params &P = *Pp;
   const PhysPar ph = make_phys(P);
   const int S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
-  const int ni = d == 1 ? b.im : b.im - 1, nj = d == 2 ? b.jm : b.jm - 1, nk = d == 3 ? b.km : b.km - 1;
-  const int64_t total = (int64_t)ni * nj * nk * S;
+  const unsigned ni = d == 1 ? b.im : b.im - 1, nj = d == 2 ? b.jm : b.jm - 1, nk = d == 3 ? b.km : b.km - 1;
+  const unsigned total = ni * nj * nk * S;  // < 2^31 per block and family (checked on the host)
   const double *s = d == 1 ? si : (d == 2 ? sj : sk);
   double *F0 = cf + (int64_t)(d - 1) * n0 * 5 * S;
-  const StrongMap sm = smap[blockIdx.y];
+  const StrongMap sm = smap[blockIdx.z];
   const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
   const int64_t step = d == 1 ? 1 : (d == 2 ? (int64_t)b.I3 : (int64_t)b.I3 * b.J3);
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = t;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    // 32-bit decomposition (64-bit division costs several times more instructions)
+    unsigned r = t;
     const int i = (int)(r % ni) + 1; r /= ni;
     const int j = (int)(r % nj) + 1; r /= nj;
     const int k = (int)(r % nk) + 1;
