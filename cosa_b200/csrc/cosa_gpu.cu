@@ -679,22 +679,7 @@ int launch_split_tail(cosa_ctx *c, int nl, LevelState &L, StageArgs &A, bool wan
   int64_t mf = 0;
   for (const DevBlock &x : L.hb) mf = std::max<int64_t>(mf, (int64_t)x.im * x.jm * x.km * S);
   const bool mixed = p.precision == COSA_PREC_MIXED;
-  const dim3 gf(grid_x(mf, L.nb), 3, L.nb);
-  if (c->prof.on) cudaEventRecord(c->prof.ev[1][0], c->s);
-  if (mixed)
-    k_faces<true><<<gf, 128, 0, c->s>>>(L.d_blocks, c->d_p, L.d_qprim, A.si, A.sj, A.sk, L.d_strong, L.d_smap,
-                                         A.first_order, L.n0, L.d_cflux);
-  else
-    k_faces<false><<<gf, 128, 0, c->s>>>(L.d_blocks, c->d_p, L.d_qprim, A.si, A.sj, A.sk, L.d_strong, L.d_smap,
-                                          A.first_order, L.n0, L.d_cflux);
-  int r = after_launch(c);
-  if (r) return r;
-  if (c->prof.on) {
-    prof_stop(c, 1);
-    cudaEventRecord(c->prof.ev[2][0], c->s);
-  }
-  A.part = want_rms ? L.d_part : nullptr;
-  const dim3 gc(kCellsGX, L.nb);
+  int r = 0;
   if (A.compute_dt) {
     int64_t mc = 0;
     for (const DevBlock &x : L.hb) mc = std::max<int64_t>(mc, (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * S);
@@ -702,8 +687,32 @@ int launch_split_tail(cosa_ctx *c, int nl, LevelState &L, StageArgs &A, bool wan
                                                                A.dtvol, A.bx, A.by, A.bz);
     if ((r = after_launch(c))) return r;
   }
-  if (want_rms) k_cells<true><<<gc, 256, 0, c->s>>>(L.d_blocks, c->d_p, A, L.d_qprim, L.d_cflux, L.n0);
-  else k_cells<false><<<gc, 256, 0, c->s>>>(L.d_blocks, c->d_p, A, L.d_qprim, L.d_cflux, L.n0);
+  A.part = want_rms ? L.d_part : nullptr;
+  auto faces = [&](int b0, int nb, cudaStream_t st) {
+    const dim3 gf(grid_x(mf, nb), 3, nb);
+    if (mixed)
+      k_faces<true><<<gf, 128, 0, st>>>(L.d_blocks, c->d_p, L.d_qprim, A.si, A.sj, A.sk, L.d_strong, L.d_smap,
+                                         A.first_order, L.n0, L.d_cflux, b0);
+    else
+      k_faces<false><<<gf, 128, 0, st>>>(L.d_blocks, c->d_p, L.d_qprim, A.si, A.sj, A.sk, L.d_strong, L.d_smap,
+                                          A.first_order, L.n0, L.d_cflux, b0);
+  };
+  auto cells = [&](int b0, int nb, cudaStream_t st) {
+    const dim3 gc(kCellsGX, nb);
+    if (want_rms) k_cells<true><<<gc, 256, 0, st>>>(L.d_blocks, c->d_p, A, L.d_qprim, L.d_cflux, L.n0, b0);
+    else k_cells<false><<<gc, 256, 0, st>>>(L.d_blocks, c->d_p, A, L.d_qprim, L.d_cflux, L.n0, b0);
+  };
+  // one launch per kernel over all blocks: per-block launches on two streams
+  // (cell pass of block b beside the faces of block b+1) measured slower, the
+  // small blocks underfill the GPU
+  if (c->prof.on) cudaEventRecord(c->prof.ev[1][0], c->s);
+  faces(0, L.nb, c->s);
+  if ((r = after_launch(c))) return r;
+  if (c->prof.on) {
+    prof_stop(c, 1);
+    cudaEventRecord(c->prof.ev[2][0], c->s);
+  }
+  cells(0, L.nb, c->s);
   if ((r = after_launch(c))) return r;
   if (c->prof.on) prof_stop(c, 2);
   if (want_rms) {

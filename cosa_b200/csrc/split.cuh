@@ -56,16 +56,16 @@ __device__ __forceinline__ void split_face(const PhysPar &ph, bool first_order, 
   else roe_flux_euler(ph, met[0], met[1], met[2], met[3], qr, ql, F);
 }
 
-// grid (x, 3 families, nblocks): the three families of a block run one after
-// the other, so the block's state stays in L2 across them; face flux of
-// family d into cf + (d-1)*n0*5*S (F0 layout per family)
+// grid (x, 3 families, blocks from blk0): the three families of a block run
+// one after the other, so the block's state stays in L2 across them; face
+// flux of family d into cf + (d-1)*n0*5*S (F0 layout per family)
 template <bool MIXED>
 __global__ void __launch_bounds__(128, 5) k_faces(const DevBlock *__restrict__ blocks, const cosa_params *__restrict__ Pp,
                                                const double *__restrict__ qp, const double *__restrict__ si,
                                                const double *__restrict__ sj, const double *__restrict__ sk,
                                                const uint8_t *__restrict__ strong, const StrongMap *__restrict__ smap,
-                                               int first_order, int64_t n0, double *__restrict__ cf) {
-  const DevBlock b = blocks[blockIdx.z];
+                                               int first_order, int64_t n0, double *__restrict__ cf, int blk0) {
+  const DevBlock b = blocks[blk0 + blockIdx.z];
   const int d = blockIdx.y + 1;
   const cosa_params &P = *Pp;
   const PhysPar ph = make_phys(P);
@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(128, 5) k_faces(const DevBlock *__restrict__ b
   const unsigned total = ni * nj * nk * S;  // < 2^31 per block and family (checked on the host)
   const double *s = d == 1 ? si : (d == 2 ? sj : sk);
   double *F0 = cf + (int64_t)(d - 1) * n0 * 5 * S;
-  const StrongMap sm = smap[blockIdx.z];
+  const StrongMap sm = smap[blk0 + blockIdx.z];
   const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
   const int64_t step = d == 1 ? 1 : (d == 2 ? (int64_t)b.I3 : (int64_t)b.I3 * b.J3);
   for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
@@ -144,15 +144,15 @@ __global__ void k_dt_euler(const DevBlock *__restrict__ blocks, const cosa_param
   }
 }
 
-// grid (x, nblocks): flux balance, norms, forcing and update of every
-// interior cell (the tile kernel's epilogue; the time step is already in
-// dtvol); per-CTA norm partials at part[(blockIdx.y * gridDim.x + blockIdx.x) * 8 + m]
+// grid (x, blocks from blk0): flux balance, norms, forcing and update of
+// every interior cell (the tile kernel's epilogue; the time step is already
+// in dtvol); per-CTA norm partials at part[(block * gridDim.x + blockIdx.x) * 8 + m]
 template <bool RMS>
 __global__ void __launch_bounds__(256, 2) k_cells(const DevBlock *__restrict__ blocks, const cosa_params *__restrict__ Pp,
                                                StageArgs A, const double *__restrict__ qp,
-                                               const double *__restrict__ cf, int64_t n0) {
+                                               const double *__restrict__ cf, int64_t n0, int blk0) {
   __shared__ double red[8][8];
-  const DevBlock b = blocks[blockIdx.y];
+  const DevBlock b = blocks[blk0 + blockIdx.y];
   const cosa_params &P = *Pp;
   const int npde = 5, S = 2 * P.nharms + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(256, 2) k_cells(const DevBlock *__restrict__ b
     if (threadIdx.x < 5) {
       double x = 0;
       for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += red[threadIdx.x][w];
-      A.part[((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * 8 + threadIdx.x] = x;
+      A.part[((int64_t)(blk0 + blockIdx.y) * gridDim.x + blockIdx.x) * 8 + threadIdx.x] = x;
     }
   }
 }
