@@ -45,6 +45,9 @@ B_TILE = (3 * 224 + 264) / 4.0
 # face-split schedule: k_faces per cell (three face families) reads the
 # primitive state 40 + face metrics 96 and writes the face fluxes 120
 B_FACES = 256
+# DRAM bytes per cell of one k_faces launch, from the ncu capture summarised
+# in profiles/k_faces_k_cells_duct4m.md (4.2 M-cell duct, scaled by cells)
+FACES_TRAFFIC_B_PER_CELL = 373.3
 # DRAM bytes (read + write) per cell of one tile launch, from the ncu capture
 # summarised in profiles/k_stage_tile_fp64_duct4m.md (a stage-3 launch on the
 # 4.1 M-cell duct, scaled by the cells of the launch)
@@ -406,9 +409,8 @@ def main():
                        "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": None if split else TILE_TRAFFIC_B_PER_CELL * ncells,
-                         "traffic_source": None if split else
-                         "ncu dram bytes per cell of the 4.1 M-cell duct x cells",
+                         "traffic": (FACES_TRAFFIC_B_PER_CELL if split else TILE_TRAFFIC_B_PER_CELL) * ncells,
+                         "traffic_source": "ncu dram bytes per cell of the 4.2 M-cell duct x cells",
                          "kernel": "k_faces<fp64>" if split else "k_stage_tile<32,7,fp64>",
                          "kernel_ms": kms[1], "halo_ms": kms[0], "cells_kernel_ms": kms[3] if split else None,
                          "bytes_per_cell": B_FACES if split else B_TILE,
