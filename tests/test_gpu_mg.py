@@ -277,3 +277,31 @@ def test_mg_mixed_precision_close(oracle_mod):
     assert st == 0 and stg == 0
     assert _interior_rel(D[0]["q"].download(), As[0].q, lv[0][0], 5, 1) <= 1e-6
     ctx.close()
+
+
+@pytest.mark.parametrize("which", ["channel_3lev", "duct_2lev"])
+def test_mg_cycles_split_schedule_match_oracle(oracle_mod, which):
+    """mg() with every level on the face-split stage schedule (residual-only
+    passes, forcing terms and first-order coarse levels in the cell pass)."""
+    make, nlevel, opts = MG_CASES[which]
+    case = make()
+    p = case.params
+    p.nlevel = nlevel
+    p.cfl = 1.0
+    for k, v in opts.items():
+        setattr(p, k, v)
+    q = cases.perturbed_state(case, amp=0.01, seed=9)
+    lv, Os, As = casekit.mg_oracle(case, nlevel, p, oracle_mod, q_fine=q)
+    ctx, D = _gpu_levels(lv, p, As)
+    for nl in range(1, nlevel + 1):
+        ctx.set_schedule(nl, 1)
+    ncyc = 4
+    ho, st = oracle_mod.mg(Os, As, 1, ncyc, ncyc, rms_every=2)
+    hg, stg = ctx.mg(1, ncyc, ncyc, rms_every=2)
+    assert st == 0 and stg == 0
+    for nl in range(nlevel):
+        err = _interior_rel(D[nl]["q"].download(), As[nl].q, lv[nl][0], 5, 1)
+        assert err <= TOL * (10 if nl else 1), (nl, err)
+    rows = ~np.isnan(ho[:, 0])
+    np.testing.assert_allclose(hg[rows], ho[rows], rtol=1e-9)
+    ctx.close()

@@ -147,7 +147,7 @@ def _rel3(case, a, b):
     return float((np.abs(A - B) / sc[None, :, None]).max())
 
 
-def _smooth_pair(oracle_mod, case, ncyc, seed, params=None):
+def _smooth_pair(oracle_mod, case, ncyc, seed, params=None, schedule=0):
     p = params or case.params
     O, _, (si, sj, sk), vol, vm = _oracle_setup(oracle_mod, case)
     O.p = p
@@ -160,6 +160,7 @@ def _smooth_pair(oracle_mod, case, ncyc, seed, params=None):
     betas = [ctx.alloc_p1() for _ in range(3)]
     ctx.bind_level(1, q=dq_, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(), si=m[0], sj=m[1], sk=m[2], vol=gvol,
                    betaxi=betas[0], betaeta=betas[1], betazeta=betas[2])
+    ctx.set_schedule(1, schedule)
     hist_g, st = ctx.smooth(1, ncyc, 1, 2)
     assert st == 0
     out = dq_.download()
@@ -175,10 +176,11 @@ def _state_err(case, a, b):
     return float(np.inf if not np.isfinite(d).all() else d.max())
 
 
+@pytest.mark.parametrize("schedule", [0, 1])
 @pytest.mark.parametrize("which", list(CASES))
-def test_fused_viscous_smooth_matches_oracle(oracle_mod, which):
+def test_fused_viscous_smooth_matches_oracle(oracle_mod, which, schedule):
     case = CASES[which]()
-    qo, hist_o, qg, hist_g = _smooth_pair(oracle_mod, case, 6, seed=5)
+    qo, hist_o, qg, hist_g = _smooth_pair(oracle_mod, case, 6, seed=5, schedule=schedule)
     assert _state_err(case, qg, qo) <= TOL
     rows = ~np.isnan(hist_o[:, 0])
     assert np.array_equal(rows, ~np.isnan(hist_g[:, 0]))
