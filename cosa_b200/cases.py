@@ -14,6 +14,10 @@ COSA ships no meshes or inputs, so every case is generated from formulas:
   1-to-1 cuts between neighbours.
 * ``partitioned_channel`` -- the bump channel cut into several blocks, one of
   them stored with cyclically permuted indices, to exercise cut_q's iord.
+* ``naca0012_ogrid`` -- O-grid around the NACA 0012 (4-digit formula, closed
+  trailing edge), 512 x 128 x 2 cells in four blocks of 96/160/160/96 cells
+  along the contour, far field 50 chords, first spacing of y+ ~ 1 at Re 6e6;
+  BCs 1500 (wall, force surface 1) / 30 (far field) / 80 (k faces).
 
 Arrays are flat float64 in the reference layout (column-major per block,
 blocks concatenated with setoffs offsets).
@@ -509,6 +513,129 @@ def duct3d(segs=None, seed: int = 3, lo: int = 27_000_000, hi: int = 33_000_000,
         return Case(f"duct3d_{NI}x{NJ}x{NK}", tables, p, None, None, None, None)
     return _assemble(f"duct3d_{NI}x{NJ}x{NK}", nodes, specs, cuts, p)
 
+
+
+# ---- configuration 2/4: NACA 0012 O-grid --------------------------------------------
+FAR_FIELD = 30
+
+
+def naca0012_thickness(x: np.ndarray) -> np.ndarray:
+    """Half thickness of the NACA 0012 from the 4-digit formula with the
+    closed-trailing-edge last coefficient (-0.1036), chord 1."""
+    x = np.clip(x, 0.0, 1.0)
+    return 0.6 * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1036 * x ** 4)
+
+
+def _geometric_distances(n: int, h1: float, total: float) -> np.ndarray:
+    """n+1 distances 0, h1, h1(1+r), ... ending at total (ratio r by bisection)."""
+    lo, hi = 1.0 + 1e-12, 2.0
+    for _ in range(200):
+        r = 0.5 * (lo + hi)
+        if h1 * (r ** n - 1) / (r - 1) > total:
+            hi = r
+        else:
+            lo = r
+    r = 0.5 * (lo + hi)
+    d = np.concatenate([[0.0], h1 * np.cumsum(r ** np.arange(n))])
+    return d * (total / d[-1])
+
+
+def naca0012_nodes(ni: int = 512, nj: int = 128, nk: int = 2, rfar: float = 50.0, h1: float = 4.5e-6,
+                   span: float = 0.1, blend: float = 1.0):
+    """Node coordinates (ni+1, nj+1, nk+1) of an O-grid around the NACA 0012.
+
+    i runs clockwise from the trailing edge (i = 0 and i = ni coincide) over
+    the lower surface, the leading edge (i = ni/2) and the upper surface,
+    with cosine clustering at both edges; j runs from the wall to a circle of
+    radius rfar about mid-chord with first spacing h1 (geometric); k spans
+    z in [0, span].  Grid line i leaves the wall along the surface normal and
+    bends over a length ~blend (chords) to the radial direction of its
+    far-field point."""
+    beta = 2 * np.pi * np.arange(ni + 1) / ni
+    xs = 0.5 * (1 + np.cos(beta))
+    ys = np.where(beta < np.pi, -1.0, 1.0) * naca0012_thickness(xs)
+    ys[0] = ys[-1] = 0.0
+    ys[ni // 2] = 0.0
+    P = np.stack([xs, ys], 1)
+    # outward normal of the clockwise contour: the tangent turned by +90 deg
+    Pp = np.roll(P[:-1], -1, 0); Pm = np.roll(P[:-1], 1, 0)
+    t = Pp - Pm
+    t = np.concatenate([t, t[:1]], 0)
+    Nrm = np.stack([-t[:, 1], t[:, 0]], 1)
+    Nrm /= np.linalg.norm(Nrm, axis=1, keepdims=True)
+    c = np.array([0.5, 0.0])
+    R = P - c
+    U0 = R / np.linalg.norm(R, axis=1, keepdims=True)
+    Cfar = c + rfar * U0
+    L = np.linalg.norm(Cfar - P, axis=1)
+    U = (Cfar - P) / L[:, None]
+    d = _geometric_distances(nj, h1, rfar)
+    s = d / d[-1]
+    w = 1.0 - np.exp(-d / blend)
+    D = (1 - w)[None, :, None] * Nrm[:, None, :] + w[None, :, None] * U[:, None, :]
+    D /= np.linalg.norm(D, axis=2, keepdims=True)
+    XY = P[:, None, :] + (s[None, :, None] * L[:, None, None]) * D
+    XY[:, -1, :] = Cfar
+    zs = span * np.arange(nk + 1) / nk
+    X = np.repeat(XY[:, :, 0:1], nk + 1, axis=2)
+    Y = np.repeat(XY[:, :, 1:2], nk + 1, axis=2)
+    Z = np.broadcast_to(zs[None, None, :], X.shape).copy()
+    return X, Y, Z
+
+
+def naca_params(model: str = "kom", mach: float = 0.3, alpha_deg: float = 4.0, reyno: float = 6.0e6,
+                cfl: float = 3.0, eps_irs: float = 0.6, nlevel: int = 1) -> CosaParams:
+    """Free stream at incidence alpha for the aerofoil cases: model "euler",
+    "laminar" or "kom"; constant-coefficient IRS (irsop 1) with smoothing
+    coefficient eps_irs (rat = sqrt(1 + 4 eps)) when eps_irs > 0."""
+    if model == "kom":
+        p = kom_params(mach, reyno)
+    elif model == "laminar":
+        p = laminar_params(mach, reyno)
+    else:
+        p = channel_params(mach)
+    p.alpha = np.deg2rad(alpha_deg)
+    p.beta = 0.0
+    p.aircraft = 1
+    p.cfl = cfl
+    p.cflt = cfl
+    p.nlevel = nlevel
+    if eps_irs > 0:
+        p.irsop = 1
+        p.rat = float(np.sqrt(1 + 4 * eps_irs))
+        p.ratt = p.rat
+    return p
+
+
+def naca0012_ogrid(blocks=(96, 160, 160, 96), nj: int = 128, nk: int = 2, rfar: float = 50.0,
+                   h1: float = 4.5e-6, span: float = 0.1, params: CosaParams = None,
+                   wall: int = VISCOUS_WALL, kface_bc: int = 80) -> Case:
+    """NACA 0012 O-grid split along i into len(blocks) blocks of the given
+    cell counts (default 96/160/160/96, 512 x nj x nk cells), 1-to-1 cuts
+    between consecutive blocks and across the trailing-edge seam (last block
+    imax to first block imin).  BCs: wall (default 1500, the force surface)
+    on jmin, far field (30) on jmax, kface_bc on the k faces.  h1 = 4.5e-6
+    chords is the first spacing of y+ ~ 1 at Re = 6e6 (flat-plate skin
+    friction)."""
+    ni = int(sum(blocks))
+    X, Y, Z = naca0012_nodes(ni, nj, nk, rfar, h1, span)
+    ib = np.concatenate([[0], np.cumsum(blocks)])
+    nodes, specs = [], []
+    for b in range(len(blocks)):
+        i0, i1 = ib[b], ib[b + 1]
+        nodes.append(tuple(A[i0:i1 + 1].copy() for A in (X, Y, Z)))
+        dims = (i1 - i0 + 1, nj + 1, nk + 1)
+        specs.append(BlockSpec(*dims, _face_bcs(*dims, {
+            "jmin": wall, "jmax": FAR_FIELD, "kmin": kface_bc, "kmax": kface_bc})))
+    cuts = []
+    nb = len(blocks)
+    for b in range(nb):
+        o = (b + 1) % nb
+        d, od = specs[b], specs[o]
+        cuts.append((b + 1, (d.imax, 1, 1), (d.imax, d.jmax, d.kmax), o + 1, (1, 1, 1), (1, od.jmax, od.kmax),
+                     (1, 2, 3)))
+    p = params if params is not None else naca_params()
+    return _assemble(f"naca0012_{ni}x{nj}x{nk}", nodes, specs, cuts, p)
 
 def perturbed_state(case: Case, amp: float = 0.02, seed: int = 0) -> np.ndarray:
     """Free stream plus a smooth seeded perturbation of every conservative

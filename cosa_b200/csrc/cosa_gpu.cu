@@ -18,6 +18,7 @@
 #include "visc.cuh"
 #include "kom.cuh"
 #include "split.cuh"
+#include "force.cuh"
 
 namespace {
 
@@ -70,6 +71,14 @@ struct LevelState {
   // set by cosa_gpu_autotune
   int schedule = 0;
   double *d_cflux = nullptr;  // convective face fluxes of the split schedule (3 x F0)
+  // wall faces of each force surface (key: surface number), built on first use
+  struct ForceList {
+    ForceFace *d_faces = nullptr;
+    int nfaces = 0;
+    int *d_bstart = nullptr;
+    double *d_buf = nullptr, *d_sums = nullptr;
+  };
+  std::map<int, ForceList> forces;
 };
 
 }  // namespace
@@ -545,7 +554,15 @@ int ensure_irs_scratch(cosa_ctx *c, LevelState &L) {
   return COSA_OK;
 }
 
-// the three Thomas sweeps of cirs_b / ccirs_b on `res` for variables vs..ve
+// lines of kPcrMinLen..kPcrMaxLen cells are solved by cyclic reduction in
+// shared memory (at most kPcrSmemBytes per CTA, within the 48 KB default);
+// shorter lines (a warp per line would idle) and longer ones by the Thomas
+// sweeps, one thread per line
+constexpr int kPcrSmemBytes = 48 * 1024;
+constexpr int kPcrMaxLen = kPcrSmemBytes / 64;
+constexpr int kPcrMinLen = 16;
+
+// the three line sweeps of cirs_b / ccirs_b on `res` for variables vs..ve
 int irs_sweeps(cosa_ctx *c, LevelState &L, double *res, const double *ores, const double *const beta[3], double eps,
                int vs, int ve, int with_halo) {
   const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
@@ -554,8 +571,23 @@ int irs_sweeps(cosa_ctx *c, LevelState &L, double *res, const double *ores, cons
     for (int d = 1; d <= 3; ++d) {
       const int64_t nl = d == 1 ? (int64_t)(x.jm - 1) * (x.km - 1) : (d == 2 ? (int64_t)(x.im - 1) * (x.km - 1)
                                                                             : (int64_t)(x.im - 1) * (x.jm - 1));
-      const int g = grid_for(nl * S, 128);
       const double *bt = beta ? beta[d - 1] : nullptr;
+      const int len = d == 1 ? x.im - 1 : (d == 2 ? x.jm - 1 : x.km - 1);
+      if (len >= kPcrMinLen && len <= kPcrMaxLen) {
+        // parallel cyclic reduction, one warp per line and variable
+        const int nmax = std::max(len, 1);
+        const int wpc = std::max(1, std::min(4, kPcrSmemBytes / (64 * nmax)));
+        const int g = grid_for(nl * S * (ve - vs + 1) * 32, 32 * wpc);  // one warp per line and variable
+        const size_t sm = (size_t)wpc * 8 * nmax * sizeof(double);
+        const double *src = d == 1 ? ores : nullptr;
+        if (d == 1) k_irs_pcr<1><<<g, 32 * wpc, sm, c->s>>>(x, npde, S, res, src, bt, eps, vs, ve, with_halo, nmax);
+        else if (d == 2) k_irs_pcr<2><<<g, 32 * wpc, sm, c->s>>>(x, npde, S, res, src, bt, eps, vs, ve, with_halo, nmax);
+        else k_irs_pcr<3><<<g, 32 * wpc, sm, c->s>>>(x, npde, S, res, src, bt, eps, vs, ve, with_halo, nmax);
+        int r = after_launch(c);
+        if (r) return r;
+        continue;
+      }
+      const int g = grid_for(nl * S, 128);
       if (d == 1) k_irs_line<1><<<g, 128, 0, c->s>>>(x, npde, S, res, ores, bt, eps, vs, ve, with_halo, L.d_irs_scr);
       else if (d == 2) k_irs_line<2><<<g, 128, 0, c->s>>>(x, npde, S, res, nullptr, bt, eps, vs, ve, with_halo, L.d_irs_scr);
       else k_irs_line<3><<<g, 128, 0, c->s>>>(x, npde, S, res, nullptr, bt, eps, vs, ve, with_halo, L.d_irs_scr);
@@ -1135,8 +1167,34 @@ int cosa_gpu_deltat(cosa_ctx *c, int32_t nl, double *dtvol, const double *lam, d
   });
 }
 
+}  // extern "C"
+
+namespace {
+// muscl / roflux of the routine-by-routine (k-omega) stage; mixed: limiter
+// and Roe dissipation in FP32 on FP64 differences
+int muscl_impl(cosa_ctx *c, int32_t idir, int32_t nl, const double *q, double *qp, double *qm, double *dq,
+               double *dqp, double *dqm, int mixed);
+int roflux_impl(cosa_ctx *c, int32_t idir, int32_t nl, const double *qr, const double *ql, double *flux,
+                const double *sijk, int mixed);
+}  // namespace
+
+extern "C" {
+
 int cosa_gpu_muscl(cosa_ctx *c, int32_t idir, int32_t nl, const double *q, double *qp, double *qm, double *dq,
                    double *dqp, double *dqm) {
+  return muscl_impl(c, idir, nl, q, qp, qm, dq, dqp, dqm, 0);
+}
+
+int cosa_gpu_roflux(cosa_ctx *c, int32_t idir, int32_t nl, const double *qr, const double *ql, double *flux,
+                    const double *sijk) {
+  return roflux_impl(c, idir, nl, qr, ql, flux, sijk, 0);
+}
+
+}  // extern "C"
+
+namespace {
+int muscl_impl(cosa_ctx *c, int32_t idir, int32_t nl, const double *q, double *qp, double *qm, double *dq,
+               double *dqp, double *dqm, int mixed) {
   LevelState *L = level(c, nl);
   if (!L || idir < 1 || idir > 3 || !q || !qp || !qm || !dq || !dqp || !dqm) return COSA_ERR_ARG;
   const cosa_params &p = c->p;
@@ -1152,22 +1210,25 @@ int cosa_gpu_muscl(cosa_ctx *c, int32_t idir, int32_t nl, const double *q, doubl
       if (r) return r;
     }
     k_muscl_face<<<grid_for(cnt_all(x, p)), 256, 0, c->s>>>(x, c->d_p, idir, nl, q, qp, qm, dq, dqp, dqm, bct,
-                                                             L->nbcs[b]);
+                                                             L->nbcs[b], mixed);
     int r = after_launch(c);
     if (r) return r;
   }
   return COSA_OK;
 }
 
-int cosa_gpu_roflux(cosa_ctx *c, int32_t idir, int32_t nl, const double *qr, const double *ql, double *flux,
-                    const double *sijk) {
+int roflux_impl(cosa_ctx *c, int32_t idir, int32_t nl, const double *qr, const double *ql, double *flux,
+                const double *sijk, int mixed) {
   LevelState *L = level(c, nl);
   if (!L || idir < 1 || idir > 3 || !qr || !ql || !flux || !sijk) return COSA_ERR_ARG;
   if (c->p.moving) return COSA_ERR_UNSUPPORTED;
   return for_blocks(c, *L, cnt_all, [&](int, const DevBlock &b, int g) {
-    k_roflux<<<g, 256, 0, c->s>>>(b, c->d_p, idir, qr, ql, flux, sijk);
+    k_roflux<<<g, 256, 0, c->s>>>(b, c->d_p, idir, qr, ql, flux, sijk, mixed);
   });
 }
+}  // namespace
+
+extern "C" {
 
 int cosa_gpu_resid(cosa_ctx *c, int32_t idir, int32_t nl, const double *flux, double *res) {
   LevelState *L = level(c, nl);
@@ -1268,7 +1329,8 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
     c->launches += L->graph_launches[want ? 1 : 0];
   }
   // reference state after smooth(): face halos of q in conservative form
-  if (niter > 0 && !L->items.empty()) {
+  // (the k-omega stage converts them itself, src/update.f90:1875-2084)
+  if (niter > 0 && !L->items.empty() && !c->p.kom) {
     double *last_in = (c->p.nstage % 2 == 0) ? L->d_T : L->ptrs.q;
     const int S = 2 * c->p.nharms + 1;
     k_halo_p2c<<<grid_for((int64_t)L->items.size() * S), 256, 0, c->s>>>(L->d_blocks, L->d_items,
@@ -1521,7 +1583,8 @@ int issue_smooth_level(cosa_ctx *c, int nl, int niter, bool from_fine, bool to_c
     if ((r = launch_iteration(c, nl, L, o))) return r;
   }
   // reference state after smooth(): face halos of q in conservative form
-  if (niterp > 0 && !L.items.empty()) {
+  // (the k-omega stage converts them itself)
+  if (niterp > 0 && !L.items.empty() && !p.kom) {
     double *last_in = (to_coarse || p.nstage % 2 == 1) ? L.ptrs.q : L.d_T;
     const int S = 2 * p.nharms + 1;
     k_halo_p2c<<<grid_for((int64_t)L.items.size() * S), 256, 0, c->s>>>(L.d_blocks, L.d_items, (int)L.items.size(),
@@ -2168,6 +2231,107 @@ int cosa_gpu_update_kom(cosa_ctx *c, int32_t nl, const double *res, double *q, c
   return COSA_OK;
 }
 
+int cosa_gpu_force(cosa_ctx *c, int32_t nl, const double *q, const double *x, const double *y, const double *z,
+                   const double *si, const double *sj, const double *sk, const double *vm, int32_t isurf,
+                   const double *xmom, const double *lngth, double *coef) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !x || !y || !z || !si || !sj || !sk || !xmom || !lngth || !coef || isurf < 1) return COSA_ERR_ARG;
+  const cosa_params &P = c->p;
+  if (P.viscous && !vm) return COSA_ERR_ARG;
+  if (P.moving) return COSA_ERR_UNSUPPORTED;
+  if (lngth[0] == 0.0 || lngth[1] == 0.0 || lngth[2] == 0.0) return COSA_ERR_ARG;
+  const int S = 2 * P.nharms + 1, nb = L->nb;
+  auto it = L->forces.find(isurf);
+  if (it == L->forces.end()) {
+    // faces of the patches with bctopo(1) == 1500 + isurf - 1, block after
+    // block, patches and faces in table order
+    std::vector<ForceFace> faces;
+    std::vector<int> bstart(nb + 1, 0);
+    for (int b = 0; b < nb; ++b) {
+      bstart[b] = (int)faces.size();
+      const DevBlock &db = L->hb[b];
+      const int ijk[4] = {0, db.im, db.jm, db.km};
+      for (int ib = 0; ib < L->nbcs[b]; ++ib) {
+        const int *t = &L->bct[L->obct[b] + 10 * ib];
+        if (t[0] != 1500 + isurf - 1) continue;
+        const int d = t[1], inrout = t[2];
+        if (d < 1 || d > 3 || (inrout != 1 && inrout != 2)) return COSA_ERR_ARG;
+        const int c2 = cyc3(d, 2), c3 = cyc3(d, 3);
+        const int lo[4] = {0, t[3], t[5], t[7]}, hi[4] = {0, t[4], t[6], t[8]};
+        for (int a : {c2, c3})
+          if (lo[a] < 1 || hi[a] > ijk[a] - 1) return COSA_ERR_ARG;
+        if (ijk[d] < 3) return COSA_ERR_ARG;  // the wall stencil reads two cells in
+        const int h = inrout == 1 ? 0 : ijk[d];
+        for (int i3 = lo[c3]; i3 <= hi[c3]; ++i3)
+          for (int i2 = lo[c2]; i2 <= hi[c2]; ++i2) {
+            int idx[4];
+            idx[d] = h; idx[c2] = i2; idx[c3] = i3;
+            faces.push_back(ForceFace{b, d, inrout == 1 ? 1 : -1, idx[1], idx[2], idx[3]});
+          }
+      }
+    }
+    bstart[nb] = (int)faces.size();
+    LevelState::ForceList fl;
+    fl.nfaces = (int)faces.size();
+    int r;
+    if ((r = dalloc(c, &fl.d_faces, faces.size())) || (r = dalloc(c, &fl.d_bstart, bstart.size())) ||
+        (r = dalloc(c, &fl.d_buf, (size_t)fl.nfaces * 12 * S)) || (r = dalloc(c, &fl.d_sums, (size_t)nb * 12 * S)))
+      return r;
+    if (!faces.empty())
+      CK(cudaMemcpyAsync(fl.d_faces, faces.data(), faces.size() * sizeof(ForceFace), cudaMemcpyHostToDevice, c->s));
+    CK(cudaMemcpyAsync(fl.d_bstart, bstart.data(), bstart.size() * sizeof(int), cudaMemcpyHostToDevice, c->s));
+    CK(cudaStreamSynchronize(c->s));
+    it = L->forces.emplace(isurf, fl).first;
+  }
+  const LevelState::ForceList &fl = it->second;
+  std::vector<double> sums((size_t)nb * 12 * S, 0.0);
+  if (fl.nfaces > 0) {
+    k_force_faces<<<grid_for((int64_t)fl.nfaces * S), 256, 0, c->s>>>(L->d_blocks, c->d_p, fl.d_faces, fl.nfaces, q, x,
+                                                                       y, z, si, sj, sk, vm, L->n0, xmom[0], xmom[1],
+                                                                       xmom[2], fl.d_buf);
+    int r = after_launch(c);
+    if (r) return r;
+    k_force_sum<<<dim3(nb, S), 256, 0, c->s>>>(fl.d_bstart, fl.nfaces, fl.d_buf, fl.d_sums);
+    if ((r = after_launch(c))) return r;
+    CK(cudaMemcpyAsync(sums.data(), fl.d_sums, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    CK(cudaStreamSynchronize(c->s));
+  }
+  // coefficients of each block, summed in block order (src/output.f90:4870-4893, 4283-4320)
+  const double mach = P.machfs > 1e-14 ? P.machfs : 1.0;
+  double ss[3], aa[3], bb[3];
+  if (P.aircraft) {
+    const double ca = std::cos(P.alpha), sa = std::sin(P.alpha), cb = std::cos(P.beta), sb = std::sin(P.beta);
+    ss[0] = ca * cb; ss[1] = sa * cb; ss[2] = sb;
+    const double den = std::sqrt(sb * sb + ca * ca * cb * cb);
+    aa[0] = -sa * ca * cb * cb / den; aa[1] = den; aa[2] = sa * sb * cb / den;
+    bb[0] = -sb / den; bb[1] = 0.0; bb[2] = ca * cb / den;
+  } else {
+    ss[0] = 0; ss[1] = 1; ss[2] = 0;
+    aa[0] = 1; aa[1] = 0; aa[2] = 0;
+    bb[0] = 0; bb[1] = 0; bb[2] = 1;
+  }
+  const double cf = 2 / (lngth[0] * lngth[1] * mach * mach);
+  const double cmf = 2 / (lngth[0] * lngth[1] * lngth[2] * mach * mach);
+  for (int n = 0; n < S; ++n) {
+    double *o = coef + (size_t)n * 12;
+    for (int k = 0; k < 12; ++k) o[k] = 0.0;
+    for (int b = 0; b < nb; ++b) {
+      const double *g0 = &sums[((size_t)n * nb + b) * 12];
+      for (int pv = 0; pv < 2; ++pv) {
+        const double *g = g0 + 6 * pv;
+        double *cc = o + 6 * pv;
+        cc[0] += (g[0] * aa[0] + g[1] * aa[1] + g[2] * aa[2]) * cf;
+        cc[1] += (g[0] * ss[0] + g[1] * ss[1] + g[2] * ss[2]) * cf;
+        cc[2] += (g[0] * bb[0] + g[1] * bb[1] + g[2] * bb[2]) * cf;
+        cc[3] += g[3] * cmf;
+        cc[4] += g[4] * cmf;
+        cc[5] += g[5] * cmf;
+      }
+    }
+  }
+  return COSA_OK;
+}
+
 int cosa_gpu_cutman_mut(cosa_ctx *c, int32_t nl, double *mut) {
   LevelState *L = level(c, nl);
   if (!L || !mut) return COSA_ERR_ARG;
@@ -2243,8 +2407,9 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, bool compute_
   if ((r = launch_edges(c, L, q, P.mut))) return r;
   const double *sd[4] = {nullptr, P.si, P.sj, P.sk};
   for (int d = 1; d <= 3; ++d) {
-    if ((r = cosa_gpu_muscl(c, d, nl, q, P.qp, P.qm, P.dq, P.dqp, P.dqm))) return r;
-    if ((r = cosa_gpu_roflux(c, d, nl, P.qp, P.qm, P.flux, sd[d]))) return r;
+    const int mixed = p.precision == COSA_PREC_MIXED;
+    if ((r = muscl_impl(c, d, nl, q, P.qp, P.qm, P.dq, P.dqp, P.dqm, mixed))) return r;
+    if ((r = roflux_impl(c, d, nl, P.qp, P.qm, P.flux, sd[d], mixed))) return r;
     if ((r = cosa_gpu_resid(c, d, nl, P.flux, P.res))) return r;
     // q_face (+ face mut) / q_der / rtst / vflux / resid (src/cosa.f90:1809-1824)
     if ((r = rans_face_state(c, L, d, q, P.dq, nullptr, nullptr, nullptr))) return r;

@@ -198,7 +198,7 @@ __global__ void k_muscl_dq(DevBlock b, const cosa_params *__restrict__ Pp, int d
 __global__ void k_muscl_face(DevBlock b, const cosa_params *__restrict__ Pp, int d, int nl,
                              const double *__restrict__ q, double *__restrict__ qp, double *__restrict__ qm,
                              const double *__restrict__ dq, double *__restrict__ dqp, double *__restrict__ dqm,
-                             const int *__restrict__ bct, int nbcs) {
+                             const int *__restrict__ bct, int nbcs, int mixed = 0) {
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
@@ -226,7 +226,14 @@ __global__ void k_muscl_face(DevBlock b, const cosa_params *__restrict__ Pp, int
       double a, bq;
       const int ilim = v <= 5 ? P.ilimf : P.ilimt;
       const double eps = v <= 5 ? P.epslimf : P.epslimt;
-      limit_face<double>(ilim, eps, P.rkap, dlo, dmid, dhi, a, bq);
+      if (mixed) {
+        // the limited slopes in FP32 on the FP64 differences
+        float fa, fb;
+        limit_face_fast(ilim, (float)eps, (float)P.rkap, (float)dlo, (float)dmid, (float)dhi, fa, fb);
+        a = fa; bq = fb;
+      } else {
+        limit_face<double>(ilim, eps, P.rkap, dlo, dmid, dhi, a, bq);
+      }
       dqp[base + c0] = a;
       dqm[base + c0] = bq;
       vp = q[base + c0] + a;
@@ -256,7 +263,8 @@ __global__ void k_muscl_face(DevBlock b, const cosa_params *__restrict__ Pp, int
 
 // ---- roflux_b (src/flux.f90:45-238) --------------------------------------------------
 __global__ void k_roflux(DevBlock b, const cosa_params *__restrict__ Pp, int d, const double *__restrict__ qr,
-                         const double *__restrict__ ql, double *__restrict__ flux, const double *__restrict__ sijk) {
+                         const double *__restrict__ ql, double *__restrict__ flux, const double *__restrict__ sijk,
+                         int mixed = 0) {
   const cosa_params &P = *Pp;
   const PhysPar ph = make_phys(P);
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
@@ -277,8 +285,13 @@ __global__ void k_roflux(DevBlock b, const cosa_params *__restrict__ Pp, int d, 
     }
     const double tker = kom ? qr[p3_var(b, npde, S, 6, n) + c] : 0.0;
     const double tkel = kom ? ql[p3_var(b, npde, S, 6, n) + c] : 0.0;
-    roe_flux_fp64(ph, sijk[p2_idx(b, S2, 1, i, j, k, nh)], sijk[p2_idx(b, S2, 2, i, j, k, nh)],
-                  sijk[p2_idx(b, S2, 3, i, j, k, nh)], sijk[p2_idx(b, S2, 4, i, j, k, nh)], vr, vl, tker, tkel, f);
+    if (mixed)
+      roe_flux_mixed_tke(ph, sijk[p2_idx(b, S2, 1, i, j, k, nh)], sijk[p2_idx(b, S2, 2, i, j, k, nh)],
+                         sijk[p2_idx(b, S2, 3, i, j, k, nh)], sijk[p2_idx(b, S2, 4, i, j, k, nh)], vr, vl, tker, tkel,
+                         f);
+    else
+      roe_flux_fp64(ph, sijk[p2_idx(b, S2, 1, i, j, k, nh)], sijk[p2_idx(b, S2, 2, i, j, k, nh)],
+                    sijk[p2_idx(b, S2, 3, i, j, k, nh)], sijk[p2_idx(b, S2, 4, i, j, k, nh)], vr, vl, tker, tkel, f);
     for (int m = 0; m < 5; ++m) flux[f0_idx(b, npde, S, i, j, k, m + 1, n)] = f[m];
     if (kom) {
       // turbulence fluxes (src/flux.f90:249-380) with the mean-flow loop's
@@ -607,6 +620,89 @@ __global__ void k_irs_line(DevBlock b, int npde, int S, double *__restrict__ res
         xnext = xm;
       }
     }
+  }
+}
+
+// The same line solves by parallel cyclic reduction: one warp per (line,
+// snapshot, variable), the line's four diagonals/right-hand side in shared
+// memory (ping-pong, 8 * nmax doubles per warp).  Row m of the system is
+// -e_m x_{m-1} + (1 + 2 e_m) x_m - e_m x_{m+1} = r_m (first and last rows
+// without the outer term), as in the Thomas sweeps above; step s eliminates
+// x_{m-s} and x_{m+s} from row m, so after ceil(log2 len) steps x_m = r_m /
+// b_m.  The chain of dependent steps is log2(len) instead of 2 len; the
+// result differs from the Thomas sweeps by rounding only (the matrix is
+// strictly diagonally dominant).
+template <int D>
+__global__ void __launch_bounds__(128) k_irs_pcr(DevBlock b, int npde, int S, double *__restrict__ res,
+                                                 const double *__restrict__ ores, const double *__restrict__ beta,
+                                                 double eps, int vs, int ve, int with_halo, int nmax) {
+  extern __shared__ double irs_sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int im = b.im - 1, jm = b.jm - 1, km = b.km - 1;
+  const int len = D == 1 ? im : (D == 2 ? jm : km);
+  const int n2 = D == 1 ? jm : im, n3 = D == 3 ? jm : km;
+  const int nv = ve - vs + 1;
+  const int64_t nwork = (int64_t)n2 * n3 * S * nv;
+  double *buf = irs_sm + (size_t)warp * 8 * nmax;
+  for (int64_t w = blockIdx.x * (int64_t)nw + warp; w < nwork; w += (int64_t)gridDim.x * nw) {
+    int64_t r_ = w;
+    const int t2 = (int)(r_ % n2) + 1; r_ /= n2;
+    const int t3 = (int)(r_ % n3) + 1; r_ /= n3;
+    const int s = (int)(r_ % S); r_ /= S;
+    const int v = vs + (int)r_;
+    auto cell = [&](int m) {
+      if (D == 1) return p3_cell(b, m, t2, t3);
+      if (D == 2) return p3_cell(b, t2, m, t3);
+      return p3_cell(b, t2, t3, m);
+    };
+    auto coef = [&](int m) {
+      if (!beta) return eps;
+      if (D == 1) return beta[p1_idx(b, S, m, t2, t3, s)];
+      if (D == 2) return beta[p1_idx(b, S, t2, m, t3, s)];
+      return beta[p1_idx(b, S, t2, t3, m, s)];
+    };
+    const int64_t base = p3_var(b, npde, S, v, s);
+    const double *src = ores ? ores + base : res + base;
+    double *x = res + base;
+    double *a0 = buf, *b0 = buf + nmax, *c0 = buf + 2 * nmax, *r0 = buf + 3 * nmax;
+    double *a1 = buf + 4 * nmax, *b1 = buf + 5 * nmax, *c1 = buf + 6 * nmax, *r1 = buf + 7 * nmax;
+    for (int m = lane + 1; m <= len; m += 32) {
+      const double e = coef(m);
+      double rhs = src[cell(m)];
+      if (with_halo && (m == 1 || m == len)) rhs = src[cell(m)] + e * x[cell(m == len ? len + 1 : 0)];
+      a0[m - 1] = m == 1 ? 0.0 : -e;
+      b0[m - 1] = 1 + 2 * e;
+      c0[m - 1] = m == len ? 0.0 : -e;
+      r0[m - 1] = rhs;
+    }
+    __syncwarp();
+    for (int st = 1; st < len; st <<= 1) {
+      for (int m = lane; m < len; m += 32) {
+        double am = a0[m], bm = b0[m], cm = c0[m], rm = r0[m];
+        double an = 0.0, cn = 0.0;
+        if (m - st >= 0) {
+          const double al = -am / b0[m - st];
+          an = al * a0[m - st];
+          bm += al * c0[m - st];
+          rm += al * r0[m - st];
+        }
+        if (m + st < len) {
+          const double ga = -cm / b0[m + st];
+          cn = ga * c0[m + st];
+          bm += ga * a0[m + st];
+          rm += ga * r0[m + st];
+        }
+        a1[m] = an; b1[m] = bm; c1[m] = cn; r1[m] = rm;
+      }
+      __syncwarp();
+      double *t;
+      t = a0; a0 = a1; a1 = t;
+      t = b0; b0 = b1; b1 = t;
+      t = c0; c0 = c1; c1 = t;
+      t = r0; r0 = r1; r1 = t;
+    }
+    for (int m = lane + 1; m <= len; m += 32) x[cell(m)] = r0[m - 1] / b0[m - 1];
+    __syncwarp();
   }
 }
 

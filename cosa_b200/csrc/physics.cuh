@@ -369,6 +369,72 @@ __device__ __forceinline__ void roe_flux_mixed(const PhysPar &P, double kx, doub
   flux[4] = (rhor * h0r * unr + rhol * h0l * unl - (double)df5) * hds;
 }
 
+// roflux_b's mean-flow flux with the turbulent kinetic energy terms
+// (roe_flux_fp64's algebra) in mixed precision: central part in FP64, the
+// Roe dissipation in FP32 from FP32 copies of the states and of their FP64
+// differences (the k-omega path's counterpart of roe_flux_mixed).
+__device__ __forceinline__ void roe_flux_mixed_tke(const PhysPar &P, double kx, double ky, double kz, double ds,
+                                                   const double *qr, const double *ql, double tker, double tkel,
+                                                   double *flux) {
+  const double g = P.g;
+  const double rhor = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
+  const double rhol = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4];
+  const double unr = ur * kx + vr * ky + wr * kz;
+  const double unl = ul * kx + vl * ky + wl * kz;
+  const double q2r = ur * ur + vr * vr + wr * wr;
+  const double q2l = ul * ul + vl * vl + wl * wl;
+  const double h0r = g / (g - 1) * pr / rhor + q2r / 2 + tker;
+  const double h0l = g / (g - 1) * pl / rhol + q2l / 2 + tkel;
+  const float fkx = (float)kx, fky = (float)ky, fkz = (float)kz;
+  const float drho = (float)(rhor - rhol), dp = (float)(pr - pl);
+  const float du = (float)(ur - ul), dv = (float)(vr - vl), dw = (float)(wr - wl);
+  const float dun = (float)(unr - unl), dtke = (float)(tker - tkel);
+  const float frl = (float)rhol, frr = (float)rhor;
+  const float rhols = sqrtf(frl), rhors = sqrtf(frr);
+  const float rho = rhols * rhors;
+  const float rden = 1.0f / (rhols + rhors);
+  const float u = (rhols * (float)ul + rhors * (float)ur) * rden;
+  const float v = (rhols * (float)vl + rhors * (float)vr) * rden;
+  const float w = (rhols * (float)wl + rhors * (float)wr) * rden;
+  const float un = u * fkx + v * fky + w * fkz;
+  const float h0 = (rhols * (float)h0l + rhors * (float)h0r) * rden;
+  const float tke = (rhols * (float)tkel + rhors * (float)tker) * rden;
+  const float q2 = u * u + v * v + w * w;
+  const float a2 = (float)(g - 1) * (h0 - q2 * 0.5f - tke);
+  const float a = sqrtf(a2);
+  float rm123 = fabsf(un), rm4 = fabsf(un + a), rm5 = fabsf(un - a);
+  if (P.efx_setup_f) {
+    float rdelta = (float)P.cntrpy_f * ((float)P.w1 * (float)P.entfxctf_f + (float)P.w2 * (sqrtf(q2) + a) +
+                                        (float)P.w3 * 0.2f * (fabsf(un) + a));
+    rdelta = fmaxf(rdelta, 1.0e-12f);
+    if (rm123 <= rdelta && P.efx_all_f) rm123 = 0.5f * (rm123 * rm123 + rdelta * rdelta) / rdelta;
+    if (rm4 <= rdelta) rm4 = 0.5f * (rm4 * rm4 + rdelta * rdelta) / rdelta;
+    if (rm5 <= rdelta) rm5 = 0.5f * (rm5 * rm5 + rdelta * rdelta) / rdelta;
+  }
+  if (P.eig_limit_f) {
+    const float c = (float)P.eig_cutoff_f;
+    if (rm123 <= c) rm123 = c;
+    if (P.eig_lim_all_f && rm4 <= c) rm4 = c;
+    if (P.eig_lim_all_f && rm5 <= c) rm5 = c;
+  }
+  const float dpa2 = dp / a2, rdua = rho * dun / a;
+  const float al1 = rm123 * (drho - dpa2);
+  const float al2 = rm123 * rho;
+  const float al3 = rm4 * (dpa2 + rdua) * 0.5f;
+  const float al4 = rm5 * (dpa2 - rdua) * 0.5f;
+  const float df1 = al1 + al3 + al4;
+  const float df2 = al1 * u + al2 * (du - dun * fkx) + al3 * (u + a * fkx) + al4 * (u - a * fkx);
+  const float df3 = al1 * v + al2 * (dv - dun * fky) + al3 * (v + a * fky) + al4 * (v - a * fky);
+  const float df4 = al1 * w + al2 * (dw - dun * fkz) + al3 * (w + a * fkz) + al4 * (w - a * fkz);
+  const float df5 = al1 * (q2 * 0.5f + tke) + al2 * (u * du + v * dv + w * dw - un * dun + dtke) +
+                    al3 * (h0 + a * un) + al4 * (h0 - a * un);
+  flux[0] = (rhor * unr + rhol * unl - (double)df1) / 2 * ds;
+  flux[1] = ((rhor * ur * unr + pr * kx) + (rhol * ul * unl + pl * kx) - (double)df2) / 2 * ds;
+  flux[2] = ((rhor * vr * unr + pr * ky) + (rhol * vl * unl + pl * ky) - (double)df3) / 2 * ds;
+  flux[3] = ((rhor * wr * unr + pr * kz) + (rhol * wl * unl + pl * kz) - (double)df4) / 2 * ds;
+  flux[4] = (rhor * h0r * unr + rhol * h0l * unl - (double)df5) / 2 * ds;
+}
+
 // ---- eig_eul (src/cosa.f90:4183-4233), fixed grid ---------------------------------
 __device__ __forceinline__ void eig_eul(double g, const double *qc, const double *sim, const double *sip,
                                         const double *sjm, const double *sjp, const double *skm,

@@ -62,7 +62,7 @@ SYMBOLS = [
     "cosa_gpu_vmetrix", "cosa_gpu_viscous_setup", "cosa_gpu_q_face", "cosa_gpu_q_der", "cosa_gpu_vflux",
     "cosa_gpu_lambda_ns", "cosa_gpu_deltat_ns", "cosa_gpu_q_face_mut", "cosa_gpu_rtst", "cosa_gpu_vflux_kom",
     "cosa_gpu_q_der_c", "cosa_gpu_turprod", "cosa_gpu_srckw", "cosa_gpu_update_kom", "cosa_gpu_cutman_mut",
-    "cosa_gpu_autotune", "cosa_gpu_set_schedule",
+    "cosa_gpu_autotune", "cosa_gpu_set_schedule", "cosa_gpu_force",
 ]
 
 
@@ -387,6 +387,20 @@ class Context:
 
     def cutman_mut(self, nl, mut):
         self._check(load().cosa_gpu_cutman_mut(self.h, nl, _ptr(mut.ptr)), "cutman_mut")
+
+    # ---- wall forces -------------------------------------------------------------
+    def force(self, nl, q, x, y, z, si, sj, sk, vm=None, isurf=1, xmom=(0.25, 0.0, 0.0), lngth=(1.0, 1.0, 1.0)):
+        """(S, 12) force and moment coefficients of surface isurf, columns
+        cl_p, cd_p, cz_p, cmx_p, cmy_p, cm_p, then the viscous six."""
+        S = self.S
+        out = (C.c_double * (12 * S))()
+        xm = (C.c_double * 3)(*xmom)
+        ln = (C.c_double * 3)(*lngth)
+        self._check(load().cosa_gpu_force(self.h, nl, _ptr(q.ptr), _ptr(x.ptr), _ptr(y.ptr), _ptr(z.ptr),
+                                          _ptr(si.ptr), _ptr(sj.ptr), _ptr(sk.ptr),
+                                          _ptr(vm.ptr if vm is not None else None), C.c_int32(isurf), xm, ln, out),
+                    "force")
+        return np.array(out[:], dtype=np.float64).reshape(S, 12)
 
     # ---- multigrid ---------------------------------------------------------------
     def q_edges(self, nl, q, mut=None):

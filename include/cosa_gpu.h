@@ -351,6 +351,23 @@ int cosa_gpu_update_kom(cosa_ctx *ctx, int32_t nl, const double *res, double *q,
 /* cutman_mut (src/bc.f90:2713-2799) */
 int cosa_gpu_cutman_mut(cosa_ctx *ctx, int32_t nl, double *mut);
 
+/* ---- wall forces ---- */
+/* force (src/output.f90:4027-4387) over force_b (src/output.f90:4388-4900):
+   pressure and skin-friction force and moment coefficients of surface isurf
+   (the patches with bctopo(1) == 1500 + isurf - 1) of level nl, per block
+   in the reference's order and summed over blocks.  q conservative with the
+   halos of the last bc (as smooth() leaves them); x, y, z the P2 node arrays
+   with the ghost nodes of coordex (the moment arm of an inrout = 1 patch is
+   the ghost node); vm the face inverse metrics (viscous flows; may be NULL
+   otherwise); xmom the moment centre, lngth = lref1..3 of the input file.
+   coef (host, 12 * S doubles): snapshot n at coef[12n ..] = cl_p, cd_p,
+   cz_p, cmx_p, cmy_p, cm_p, cl_v, cd_v, cz_v, cmx_v, cmy_v, cm_v.  Moving
+   grids (the rotated moment centre) return COSA_ERR_UNSUPPORTED. */
+int cosa_gpu_force(cosa_ctx *ctx, int32_t nl, const double *q, const double *x, const double *y,
+                   const double *z, const double *si, const double *sj, const double *sk,
+                   const double *vm, int32_t isurf, const double *xmom, const double *lngth,
+                   double *coef);
+
 /* ---- fused: what smooth() calls when the GPU path is on ---- */
 /*
  * One RK iteration sequence of smooth() (src/cosa.f90:1711-2029) on the

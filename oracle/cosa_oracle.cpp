@@ -2536,6 +2536,141 @@ void viscous_setup_level(const Level &L, double *x, double *y, double *z, double
   }
 }
 
+// force frame of force_b (src/output.f90:4448-4470): drag (ss), lift (aa)
+// and side (bb) directions; the aircraft frame, else the turbine one
+void force_frame(const cosa_params &P, double ss[3], double aa[3], double bb[3]) {
+  if (P.aircraft) {
+    const double ca = std::cos(P.alpha), sa = std::sin(P.alpha), cb = std::cos(P.beta), sb = std::sin(P.beta);
+    ss[0] = ca * cb; ss[1] = sa * cb; ss[2] = sb;
+    const double den = std::sqrt(sb * sb + ca * ca * cb * cb);
+    aa[0] = -sa * ca * cb * cb / den; aa[1] = den; aa[2] = sa * sb * cb / den;
+    bb[0] = -sb / den; bb[1] = 0.0; bb[2] = ca * cb / den;
+  } else {
+    ss[0] = 0; ss[1] = 1; ss[2] = 0;
+    aa[0] = 1; aa[1] = 0; aa[2] = 0;
+    bb[0] = 0; bb[1] = 0; bb[2] = 1;
+  }
+}
+
+// force_b (src/output.f90:4388-4900) of every block, summed over blocks in
+// block order as force() does (src/output.f90:4283-4320).  Surface isurf
+// (1-based) is the patches with bctopo(1) == 1500 + isurf - 1.  The wall
+// state is the halo cell's conservative q; the moment arm is the node at
+// face index ibcw (0 on inrout = 1 patches: the ghost node written by
+// coordex).  The viscous part (P.viscous) uses the wall-face inverse
+// metric of the patch's own direction (xideri, etaderj, zetaderk: vm arrays
+// (1,xi), (2,eta), (3,zeta)).  out[n*12 + c], c = cl_p, cd_p, cz_p, cmx_p,
+// cmy_p, cm_p, cl_v, cd_v, cz_v, cmx_v, cmy_v, cm_v; a non-moving grid, so
+// the moment centre is xmom itself.
+void force_level(const Level &L, const double *qa, const double *xa, const double *ya, const double *za,
+                 const double *si, const double *sj, const double *sk, const double *vm, const cosa_params &P,
+                 int isurf, const double xmom[3], const double lngth[3], double *out) {
+  const double mach = P.machfs > 1e-14 ? P.machfs : 1.0;
+  double ss[3], aa[3], bb[3];
+  force_frame(P, ss, aa, bb);
+  const double cf = 2 / (lngth[0] * lngth[1] * mach * mach);
+  const double cmf = 2 / (lngth[0] * lngth[1] * lngth[2] * mach * mach);
+  const double mor = P.machfs / P.reyno;
+  for (int n = 0; n < L.S * 12; ++n) out[n] = 0.0;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 q(const_cast<double *>(qa), L, b);
+    BG X(xa, L, b), Y(ya, L, b), Z(za, L, b);
+    const B2 sd[3] = {B2(si, L, b), B2(sj, L, b), B2(sk, L, b)};
+    const int ijk[4] = {0, L.im[b], L.jm[b], L.km[b]};
+    for (int n = 0; n < L.S; ++n) {
+      double fp[6] = {0, 0, 0, 0, 0, 0}, fv[6] = {0, 0, 0, 0, 0, 0};
+      for (int ib = 0; ib < L.nbcs[b]; ++ib) {
+        const int *t = &L.bct[L.obct[b] + 10 * ib];
+        if (t[0] != 1500 + isurf - 1) continue;
+        Patch pa = patch_of(t, L.im[b], L.jm[b], L.km[b]);
+        const int d = pa.idir, in1 = pa.inrout == 1;
+        const int ibcpt = in1 ? 0 : ijk[d], ibcm = in1 ? 1 : ijk[d], ibcw = in1 ? 0 : ijk[d];
+        const int sgn = in1 ? 1 : -1;  // (-1)**(1+1/inrout)
+        const B2 &s = sd[d - 1];
+        BV vd(vm ? const_cast<double *>(vm) + (int64_t)((d - 1) * 3 + (d - 1)) * 3 * L.n0 : nullptr, L, b);
+        auto pw_of = [&](int i, int j, int k) {
+          const double r = q(i, j, k, 1, n);
+          return (P.gamma - 1) * (q(i, j, k, 5, n) - q(i, j, k, 2, n) * q(i, j, k, 2, n) / r / 2 -
+                                  q(i, j, k, 3, n) * q(i, j, k, 3, n) / r / 2 - q(i, j, k, 4, n) * q(i, j, k, 4, n) / r / 2);
+        };
+        // pressure force and moment (src/output.f90:4660-4700)
+        for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+          for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+            int hi, hj, hk, mi, mj, mk, wi, wj, wk;
+            pidx(pa, ibcpt, i2, i3, hi, hj, hk);
+            pidx(pa, ibcm, i2, i3, mi, mj, mk);
+            pidx(pa, ibcw, i2, i3, wi, wj, wk);
+            const double kx = sgn * s(1, mi, mj, mk, 0), ky = sgn * s(2, mi, mj, mk, 0);
+            const double kz = sgn * s(3, mi, mj, mk, 0), ds = s(4, mi, mj, mk, 0);
+            const double pw = pw_of(hi, hj, hk);
+            fp[0] = fp[0] - pw * kx * ds;
+            fp[1] = fp[1] - pw * ky * ds;
+            fp[2] = fp[2] - pw * kz * ds;
+            const double xr = X(wi, wj, wk) - xmom[0], yr = Y(wi, wj, wk) - xmom[1], zr = Z(wi, wj, wk) - xmom[2];
+            fp[3] = fp[3] + (ky * zr - kz * yr) * pw * ds;
+            fp[4] = fp[4] + (kz * xr - kx * zr) * pw * ds;
+            fp[5] = fp[5] + (kx * yr - ky * xr) * pw * ds;
+          }
+        if (!P.viscous) continue;
+        // skin friction from the one-sided three-point wall derivative
+        // (src/output.f90:4703-4860)
+        for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+          for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+            int hi, hj, hk, mi, mj, mk, wi, wj, wk;
+            pidx(pa, ibcpt, i2, i3, hi, hj, hk);
+            pidx(pa, ibcm, i2, i3, mi, mj, mk);
+            pidx(pa, ibcw, i2, i3, wi, wj, wk);
+            const int o1[3] = {sgn * krd(d, 1), sgn * krd(d, 2), sgn * krd(d, 3)};
+            const double kx = sgn * s(1, mi, mj, mk, 0), ky = sgn * s(2, mi, mj, mk, 0);
+            const double kz = sgn * s(3, mi, mj, mk, 0), ds = s(4, mi, mj, mk, 0);
+            const double ex = vd(1, mi, mj, mk), ey = vd(2, mi, mj, mk), ez = vd(3, mi, mj, mk);
+            const double rhow = q(hi, hj, hk, 1, n);
+            const double pw = pw_of(hi, hj, hk);
+            const double tw = pw * P.gamma / rhow;
+            const double muw = (P.stemp + 1) / (tw + P.stemp) * std::pow(tw, 1.5);
+            double eta[3];
+            for (int m = 0; m < 3; ++m) {
+              const double uw = q(hi, hj, hk, m + 2, n) / q(hi, hj, hk, 1, n);
+              const double u1 = q(hi + o1[0], hj + o1[1], hk + o1[2], m + 2, n) / q(hi + o1[0], hj + o1[1], hk + o1[2], 1, n);
+              const double u2 = q(hi + 2 * o1[0], hj + 2 * o1[1], hk + 2 * o1[2], m + 2, n) /
+                                q(hi + 2 * o1[0], hj + 2 * o1[1], hk + 2 * o1[2], 1, n);
+              eta[m] = sgn * (-8 * uw + 9 * u1 - u2) / 3;
+            }
+            const double dudx = eta[0] * ex, dudy = eta[0] * ey, dudz = eta[0] * ez;
+            const double dvdx = eta[1] * ex, dvdy = eta[1] * ey, dvdz = eta[1] * ez;
+            const double dwdx = eta[2] * ex, dwdy = eta[2] * ey, dwdz = eta[2] * ez;
+            const double divv = dudx + dvdy + dwdz;
+            const double txx = 2 * muw * (dudx - divv / 3), txy = muw * (dudy + dvdx), txz = muw * (dudz + dwdx);
+            const double tyy = 2 * muw * (dvdy - divv / 3), tyz = muw * (dvdz + dwdy), tzz = 2 * muw * (dwdz - divv / 3);
+            const double tx = txx * kx + txy * ky + txz * kz;
+            const double ty = txy * kx + tyy * ky + tyz * kz;
+            const double tz = txz * kx + tyz * ky + tzz * kz;
+            fv[0] = fv[0] + mor * ds * tx;
+            fv[1] = fv[1] + mor * ds * ty;
+            fv[2] = fv[2] + mor * ds * tz;
+            const double xr = X(wi, wj, wk) - xmom[0], yr = Y(wi, wj, wk) - xmom[1], zr = Z(wi, wj, wk) - xmom[2];
+            fv[3] = fv[3] + mor * ds * (-ty * zr + tz * yr);
+            fv[4] = fv[4] + mor * ds * (-tz * xr + tx * zr);
+            fv[5] = fv[5] + mor * ds * (-tx * yr + ty * xr);
+          }
+      }
+      // block coefficients (src/output.f90:4870-4893), summed over blocks
+      double *o = out + n * 12;
+      const double *f[2] = {fp, fv};
+      for (int pv = 0; pv < 2; ++pv) {
+        const double *g = f[pv];
+        double *c = o + 6 * pv;
+        c[0] += (g[0] * aa[0] + g[1] * aa[1] + g[2] * aa[2]) * cf;
+        c[1] += (g[0] * ss[0] + g[1] * ss[1] + g[2] * ss[2]) * cf;
+        c[2] += (g[0] * bb[0] + g[1] * bb[1] + g[2] * bb[2]) * cf;
+        c[3] += g[3] * cmf;
+        c[4] += g[4] * cmf;
+        c[5] += g[5] * cmf;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 // ============================================================================
@@ -3136,5 +3271,10 @@ void orc_update_kom(orc_level *h, const cosa_params *p, const double *res, doubl
 void orc_deltat_ns_full(orc_level *h, const cosa_params *p, double *dtvol, const double *lam, const double *lamv,
                         double *bx, double *by, double *bz, double *dtvolt, double *tbx, double *tby, double *tbz) {
   deltat_ns_level(h->L, dtvol, lam, lamv, bx, by, bz, *p, dtvolt, tbx, tby, tbz);
+}
+void orc_force(orc_level *h, const cosa_params *p, const double *q, const double *x, const double *y,
+               const double *z, const double *si, const double *sj, const double *sk, const double *vm, int isurf,
+               const double *xmom, const double *lngth, double *out) {
+  force_level(h->L, q, x, y, z, si, sj, sk, vm, *p, isurf, xmom, lngth, out);
 }
 }  // extern "C"

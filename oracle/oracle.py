@@ -497,3 +497,18 @@ def update_kom(O, res, q, qold, vol, dtvolt, delpls, prd, ar):
 def deltat_ns_full(O, dtvol, lam, lamv, bx, by, bz, dtvolt, tbx, tby, tbz):
     lib().orc_deltat_ns_full(O.h, _par(O.p), _p(dtvol), _p(lam), _p(lamv), _opt(bx), _opt(by), _opt(bz),
                              _opt(dtvolt), _opt(tbx), _opt(tby), _opt(tbz))
+
+
+FORCE_NAMES = ("cl_p", "cd_p", "cz_p", "cmx_p", "cmy_p", "cm_p",
+               "cl_v", "cd_v", "cz_v", "cmx_v", "cmy_v", "cm_v")
+
+
+def force(O, q, x, y, z, si, sj, sk, vm, isurf=1, xmom=(0.25, 0.0, 0.0), lngth=(1.0, 1.0, 1.0)):
+    """force_b summed over blocks (src/output.f90:4283-4900): (S, 12) force
+    and moment coefficients of wall surface isurf, columns FORCE_NAMES."""
+    out = np.zeros(O.S * 12)
+    xm = np.ascontiguousarray(xmom, dtype=np.float64)
+    ln = np.ascontiguousarray(lngth, dtype=np.float64)
+    lib().orc_force(O.h, _par(O.p), _p(q), _p(x), _p(y), _p(z), _p(si), _p(sj), _p(sk), _opt(vm),
+                    C.c_int(isurf), _p(xm), _p(ln), _p(out))
+    return out.reshape(O.S, 12)

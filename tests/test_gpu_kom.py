@@ -259,3 +259,4 @@ def test_rans_smooth_with_irs_matches_oracle(oracle_mod, irsop, cutcirs):
     assert _state_err(case, qg, qo) <= TOL
     rows = ~np.isnan(ho[:, 0])
     np.testing.assert_allclose(hg[rows], ho[rows], rtol=1e-9)
+

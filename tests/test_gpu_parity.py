@@ -228,8 +228,10 @@ def test_device_metrics_match_oracle(oracle_mod, which):
     ctx.close()
 
 
-def _irs_case(irsop, cutcirs):
-    case = casekit.small_partitioned()
+def _irs_case(irsop, cutcirs, long_lines=False):
+    # long_lines: 800-cell i-lines, above the cyclic-reduction limit (768),
+    # so the i sweeps take the Thomas kernel
+    case = cases.bump_channel(800, 6, 2) if long_lines else casekit.small_partitioned()
     p = case.params
     p.irsop = irsop
     p.cutcirs = cutcirs
@@ -239,12 +241,14 @@ def _irs_case(irsop, cutcirs):
     return case
 
 
-@pytest.mark.parametrize("irsop,cutcirs", [(1, 0), (1, 1), (3, 0), (3, 1), (2, 1)])
-def test_irs_routines_match_oracle(oracle_mod, irsop, cutcirs):
+@pytest.mark.parametrize("irsop,cutcirs,long_lines", [(1, 0, False), (1, 1, False), (3, 0, False), (3, 1, False),
+                                                      (2, 1, False), (3, 0, True)])
+def test_irs_routines_match_oracle(oracle_mod, irsop, cutcirs, long_lines):
     """cirs (cutcirs 0) and scalef + 2 x (cutman_q + ccirs) + scaleb (cutcirs 1)
     on a residual field, against the oracle's restatement of
-    src/cosa.f90:1977-1998, 2035-2443, 5206-5773."""
-    case = _irs_case(irsop, cutcirs)
+    src/cosa.f90:1977-1998, 2035-2443, 5206-5773 (cyclic reduction on the
+    device up to 768-cell lines, Thomas sweeps beyond)."""
+    case = _irs_case(irsop, cutcirs, long_lines)
     O, ctx, (si, sj, sk, vol), q = _setup(case, oracle_mod, seed=9)
     qh = q.copy()
     res_o, dt_o, st = O.residual(qh, si, sj, sk)
