@@ -192,37 +192,40 @@ def time_smooth(ctx, steps: int, torch):
     return e0.elapsed_time(e1)
 
 
-def viscous_leg(kind: str, steps: int, warmup: int, dev: int, torch):
-    """FP64 throughput of the laminar (fused stage + viscous face kernels) or
-    Wilcox k-omega (routine by routine) path on the duct generator with
-    no-slip walls: Mcell-stage/s, device-timed like the main leg."""
+def viscous_leg(kind: str, steps: int, warmup: int, dev: int, torch, precision: str = "fp64"):
+    """FP64 (or mixed) throughput of the laminar path (fused stage + viscous
+    face kernels) on the duct generator with no-slip walls, or of the Wilcox
+    k-omega path (routine by routine, IRS) on the NACA 0012 O-grid of the
+    RANS configuration: Mcell-stage/s, device-timed like the main leg."""
     from cosa_b200 import cases, gpu
-    if kind == "laminar":
+    from cosa_b200.params import PREC_MIXED
+    if kind == "kom":
+        from cosa_b200.solver import SteadySolver
+        p = cases.naca_params("kom", mach=0.3, alpha_deg=4.0, reyno=6.0e6, cfl=3.0, eps_irs=0.6)
+        if precision == "mixed":
+            p.precision = PREC_MIXED
+        case = cases.naca0012_ogrid(params=p)
+        s = SteadySolver(case, device=dev)
+        ctx = s.ctx
+        workload = ("NACA 0012 O-grid 512x128x2 (blocks 96/160/160/96), Wilcox k-omega, M=0.3, alpha=4, Re=6e6, "
+                    "CFL 3, IRS eps 0.6, single grid, " + precision.upper())
+    else:
         segs = cases.duct_segments(seed=3, lo=3_500_000, hi=4_500_000, choices=tuple(range(24, 97, 8)))
         p = cases.laminar_params(0.6, 1.0e4)
-    else:
-        segs = cases.duct_segments(seed=3, lo=900_000, hi=1_300_000, choices=tuple(range(24, 65, 8)))
-        p = cases.kom_params(0.6, 1.0e5)
-    case = cases.duct3d(segs=segs, wall=cases.VISCOUS_WALL, params=p)
-    ctx = gpu.Context([case.tables], p, device=dev)
-    X, Y, Z = (ctx.alloc_p2(ncomp=1).upload(a) for a in (case.x, case.y, case.z))
-    si, sj, sk = (ctx.alloc_p2() for _ in range(3))
-    vol = ctx.alloc_p1()
-    ctx.imetrix(1, X, Y, Z, si, sj, sk)
-    ctx.vols(1, X, Y, Z, vol)
-    vm = ctx.alloc_vm()
-    ctx.viscous_setup(1, X, Y, Z, vol, vm)
-    q = ctx.alloc_p3().upload(case.q0)
-    arrays = dict(q=q, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(), si=si, sj=sj, sk=sk, vol=vol)
-    if kind == "kom":
-        mut = ctx.alloc_p3s()
-        dist = ctx.alloc_p1().upload(cases.wall_distance(case))
-        arrays.update(res=ctx.alloc_p3(), dtvolt=ctx.alloc_p1(), qp=ctx.alloc_p3(), qm=ctx.alloc_p3(),
-                      dq=ctx.alloc_p3(), dqp=ctx.alloc_p3(), dqm=ctx.alloc_p3(), flux=ctx.alloc_f0(), mut=mut,
-                      dist=dist)
-        # the free stream's turbulent viscosity (tur_vis of the initial state)
-        ctx.tur_vis(1, q, mut)
-    ctx.bind_level(1, **arrays)
+        if precision == "mixed":
+            p.precision = PREC_MIXED
+        case = cases.duct3d(segs=segs, wall=cases.VISCOUS_WALL, params=p)
+        ctx = gpu.Context([case.tables], p, device=dev)
+        X, Y, Z = (ctx.alloc_p2(ncomp=1).upload(a) for a in (case.x, case.y, case.z))
+        si, sj, sk = (ctx.alloc_p2() for _ in range(3))
+        vol = ctx.alloc_p1()
+        ctx.imetrix(1, X, Y, Z, si, sj, sk)
+        ctx.vols(1, X, Y, Z, vol)
+        vm = ctx.alloc_vm()
+        ctx.viscous_setup(1, X, Y, Z, vol, vm)
+        q = ctx.alloc_p3().upload(case.q0)
+        ctx.bind_level(1, q=q, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(), si=si, sj=sj, sk=sk, vol=vol)
+        workload = f"bump duct, segments {segs}, no-slip walls (1500), laminar Re=1e4, M=0.6, " + precision.upper()
     ctx.smooth(1, warmup, 1, 10 ** 6, want_hist=False)
     ctx.launch_count(reset=True)
     ms = time_smooth(ctx, steps, torch)
@@ -230,8 +233,7 @@ def viscous_leg(kind: str, steps: int, warmup: int, dev: int, torch):
     ctx.close()
     return {"value": case.ncells * p.nstage * steps / (ms / 1e3) / 1e6, "unit": "Mcell-stage/s",
             "ms_per_step": ms / steps, "cells": case.ncells, "steps": steps, "gpu_launches": launches,
-            "workload": f"bump duct, segments {segs}, no-slip walls (1500), "
-                        + ("laminar Re=1e4" if kind == "laminar" else "Wilcox k-omega Re=1e5") + ", M=0.6, FP64"}
+            "workload": workload}
 
 
 def main():
@@ -251,8 +253,17 @@ def main():
                     help="0: autotune the stage schedule, 1: fused tile kernel, 2: face-split")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="precision of the main timed leg (profiling runs; the default line reports both)")
+    ap.add_argument("--leg", default="all", choices=["all", "laminar", "kom"],
+                    help="laminar / kom: time only that viscous leg and print its line (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+
+    if args.leg != "all":
+        import torch
+        torch.cuda.set_device(0)
+        r = viscous_leg(args.leg, args.steps, args.warmup, 0, torch, args.precision)
+        print(json.dumps({"metric": "Mcell-stage/s", "leg": args.leg, "precision": args.precision, **r}), flush=True)
+        return
 
     if args.impl == "reference":
         run_reference(args)
@@ -376,6 +387,7 @@ def main():
         for kind in ("laminar", "kom"):
             try:
                 viscous[kind] = viscous_leg(kind, min(args.steps, 10), 3, dev, torch)
+                viscous[kind]["mixed"] = viscous_leg(kind, min(args.steps, 10), 3, dev, torch, "mixed")["value"]
             except Exception as e:  # reported, not fatal
                 viscous[kind] = {"error": str(e)}
 

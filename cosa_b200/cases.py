@@ -418,7 +418,8 @@ def wall_distance(case: Case) -> np.ndarray:
     _, tot = t.offsets()
     out = np.zeros(tot["p1"])
     for b, (v, X, Y, Z) in enumerate(zip(p1_views(t, out, 1), gx, gy, gz)):
-        N = np.stack([X[1:-1, 1:-1, 1:-1].ravel(), Y[1:-1, 1:-1, 1:-1].ravel(), Z[1:-1, 1:-1, 1:-1].ravel()], 1)
+        N = np.stack([X[1:-1, 1:-1, 1:-1].ravel(order="F"), Y[1:-1, 1:-1, 1:-1].ravel(order="F"),
+                      Z[1:-1, 1:-1, 1:-1].ravel(order="F")], 1)
         if len(W):
             from scipy.spatial import cKDTree
             dn, _ = cKDTree(W).query(N, workers=-1)
