@@ -853,6 +853,7 @@ struct IterOpts {
   bool force = false;          // rhs += res at stage 1 (first iteration of a from_fine visit)
   bool copy_qold = true;       // qold = q at stage 1 (iter <= niter)
   double *res_only = nullptr;  // residual pass of to_coarse: stage-1 residual here, no update
+  bool first_cycle = false;    // mgit == 1 (k-omega: coarse-level mut at the first visit)
 };
 
 int launch_rans_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o);
@@ -1535,8 +1536,28 @@ int issue_restrict(cosa_ctx *c, int nl) {
   if (r) return r;
   const cosa_level_ptrs &A = L1->ptrs, &B = L2->ptrs;
   if (!A.q || !A.vol || !A.res || !B.q || !B.vol || !B.rhs) return COSA_ERR_ARG;
-  if (c->p.kom || c->p.kom_bsl || c->p.kom_sst) return COSA_ERR_UNSUPPORTED;
+  if (c->p.kom_bsl || c->p.kom_sst) return COSA_ERR_UNSUPPORTED;
   if ((r = launch_rest1(c, *L1, *L2, A.q, B.q, A.vol, B.vol))) return r;
+  if (c->p.kom) {
+    // production terms (or mut with prd_all_lvls) restricted as well
+    // (src/cosa.f90:2733-2741); ho_rest is not on this path
+    const int S = 2 * c->p.nharms + 1;
+    std::vector<std::pair<const double *, double *>> fields;
+    if (!c->p.prd_all_lvls) {
+      if (!L1->d_prd || !L2->d_prd) return COSA_ERR_ARG;
+      fields = {{L1->d_prd, L2->d_prd}, {L1->d_delpls, L2->d_delpls}, {L1->d_divvel, L2->d_divvel}};
+    } else {
+      if (!A.mut || !B.mut) return COSA_ERR_ARG;
+      fields = {{A.mut, B.mut}};
+    }
+    for (auto &f : fields)
+      for (int b = 0; b < L2->nb; ++b) {
+        const DevBlock &g = L2->hb[b];
+        k_rest4<<<grid_for((int64_t)(g.im - 1) * (g.jm - 1) * (g.km - 1) * S), 256, 0, c->s>>>(
+            L1->hb[b], g, S, f.first, f.second, A.vol, B.vol);
+        if ((r = after_launch(c))) return r;
+      }
+  }
   return launch_rest2(c, *L1, *L2, B.rhs, A.res);
 }
 
@@ -1567,7 +1588,8 @@ int issue_prolong(cosa_ctx *c, int nl) {
 }
 
 // smooth(nl, from_fine, to_coarse, done, niter) of the fused path
-int issue_smooth_level(cosa_ctx *c, int nl, int niter, bool from_fine, bool to_coarse, bool want_rms) {
+int issue_smooth_level(cosa_ctx *c, int nl, int niter, bool from_fine, bool to_coarse, bool want_rms,
+                       bool first_cycle = false) {
   LevelState &L = *level(c, nl);
   const cosa_params &p = c->p;
   const int niterp = to_coarse ? niter + 1 : niter;
@@ -1580,6 +1602,7 @@ int issue_smooth_level(cosa_ctx *c, int nl, int niter, bool from_fine, bool to_c
     o.copy_qold = iter <= niter;
     o.want_rms = want_rms && nl == 1 && iter == niter;
     o.res_only = iter == niter + 1 ? L.ptrs.res : nullptr;
+    o.first_cycle = first_cycle;
     if ((r = launch_iteration(c, nl, L, o))) return r;
   }
   // reference state after smooth(): face halos of q in conservative form
@@ -1599,15 +1622,16 @@ int issue_mg_cycle(cosa_ctx *c, int mgit, bool want_rms) {
   const cosa_params &p = c->p;
   const int nlevel = p.nlevel;
   int r = 0;
+  const bool first = mgit == 1;
   int niter = nlevel == 1 ? 1 : (mgit == 1 ? p.nstart : p.npost);
-  if ((r = issue_smooth_level(c, 1, niter, false, nlevel > 1, want_rms))) return r;
+  if ((r = issue_smooth_level(c, 1, niter, false, nlevel > 1, want_rms, first))) return r;
   if (nlevel == 1) return COSA_OK;
   if ((r = issue_restrict(c, 1))) return r;
   niter = nlevel == 2 ? p.ncrs : p.npre;
-  if ((r = issue_smooth_level(c, 2, niter, true, nlevel > 2, false))) return r;
+  if ((r = issue_smooth_level(c, 2, niter, true, nlevel > 2, false, first))) return r;
   if (nlevel == 3) {
-    if ((r = issue_restrict(c, 2)) || (r = issue_smooth_level(c, 3, p.ncrs, true, false, false)) ||
-        (r = issue_prolong(c, 2)) || (r = issue_smooth_level(c, 2, p.npost, false, false, false)))
+    if ((r = issue_restrict(c, 2)) || (r = issue_smooth_level(c, 3, p.ncrs, true, false, false, first)) ||
+        (r = issue_prolong(c, 2)) || (r = issue_smooth_level(c, 2, p.npost, false, false, false, first)))
       return r;
   }
   return issue_prolong(c, 1);
@@ -1732,9 +1756,11 @@ int cosa_gpu_smooth_level(cosa_ctx *c, int32_t nl, int32_t niter, int32_t from_f
   if ((r = ensure_hist(c, 1))) return r;
   if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, *L))) return r;
   CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
-  const int flags = (from_fine ? 1 : 0) | (to_coarse ? 2 : 0) | (want ? 4 : 0);
+  if (c->p.kom && (r = ensure_rans(c, *L))) return r;
+  const bool first = mgit == 1;
+  const int flags = (from_fine ? 1 : 0) | (to_coarse ? 2 : 0) | (want ? 4 : 0) | (first ? 8 : 0);
   r = run_graph(c, graph_key(1, nl, niter, flags),
-                [&] { return issue_smooth_level(c, nl, niter, from_fine != 0, to_coarse != 0, want); });
+                [&] { return issue_smooth_level(c, nl, niter, from_fine != 0, to_coarse != 0, want, first); });
   if (r) return r;
   if (want) CK(cudaMemcpyAsync(resrms, c->d_hist, (c->p.npde + 1) * sizeof(double), cudaMemcpyDeviceToHost, c->s));
   CK(cudaStreamSynchronize(c->s));
@@ -1758,8 +1784,10 @@ int cosa_gpu_mg(cosa_ctx *c, int32_t mgit0, int32_t ncycles, int32_t ncycle, int
     if (hist && (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle)) rows.push_back(it);
   }
   if ((r = ensure_hist(c, std::max<int>(1, (int)rows.size())))) return r;
-  for (int nl = 1; nl <= nlevel; ++nl)
+  for (int nl = 1; nl <= nlevel; ++nl) {
     if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, *level(c, nl)))) return r;
+    if (c->p.kom && (r = ensure_rans(c, *level(c, nl)))) return r;
+  }
   CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
   size_t ri = 0;
   int last = mgit0 - 1;
@@ -2368,7 +2396,8 @@ int rans_face_state(cosa_ctx *c, LevelState &L, int d, const double *q, double *
 // one RK stage of the k-omega path, routine by routine as smooth() runs it
 // (src/cosa.f90:1719-2016): every kernel is a full-array pass with the
 // reference's arrays, captured with the rest of the iteration in a graph
-int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, bool compute_dt, bool want_rms, bool copy_qold) {
+int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpts &o) {
+  const bool compute_dt = o.compute_dt && irk == 1, want_rms = o.want_rms && irk == 1, copy_qold = o.copy_qold;
   const cosa_params &p = c->p;
   const int S = 2 * p.nharms + 1, npde = p.npde;
   const cosa_level_ptrs &P = L.ptrs;
@@ -2386,6 +2415,11 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, bool compute_
     k_halo<false><<<grid_for((int64_t)L.items.size() * S), 256, 0, c->s>>>(
         L.d_blocks, L.d_items, (int)L.items.size(), c->d_p, q, P.si, P.sj, P.sk, c->d_status, P.dist);
     if ((r = after_launch(c))) return r;
+  }
+  if (o.first_cycle && o.force && irk == 1 && !p.prd_all_lvls) {
+    // coarse-level mut from the restricted (primitive) state at the first
+    // stage of the first cycle's visit (src/cosa.f90:1727-1760)
+    if ((r = cosa_gpu_tur_vis(c, nl, q, P.mut)) || (r = cosa_gpu_cutman_mut(c, nl, P.mut))) return r;
   }
   for (const DevBlock &b : L.hb) {
     k_prtest<<<grid_for(cnt_all(b, p)), 256, 0, c->s>>>(b, c->d_p, q, c->d_status);
@@ -2439,6 +2473,33 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, bool compute_
     k_rms_final<<<1, 256, 0, c->s>>>(L.d_part, L.nb * 64, npde, (double)ncell, c->d_hist, c->d_row, c->hist_cap);
     if ((r = after_launch(c))) return r;
   }
+  // multigrid forcing: rhs += res at the first stage of a visit from the
+  // finer level, then res -= rhs on coarse levels (src/cosa.f90:1950-1960)
+  const int nvs = npde * S;
+  if (o.rhs && o.force && irk == 1)
+    for (const DevBlock &b : L.hb) {
+      k_add_interior<<<grid_for(cnt_interior(b, p)), 256, 0, c->s>>>(b, nvs, o.rhs, P.res, 1.0);
+      if ((r = after_launch(c))) return r;
+    }
+  if (o.rhs && nl > 1)
+    for (const DevBlock &b : L.hb) {
+      k_add_interior<<<grid_for(cnt_interior(b, p)), 256, 0, c->s>>>(b, nvs, P.res, o.rhs, -1.0);
+      if ((r = after_launch(c))) return r;
+    }
+  if (o.res_only) {
+    // residual pass before the restriction (src/cosa.f90:1963-1975)
+    if (p.nlevel > 1 && nl != p.nlevel && !p.prd_all_lvls && p.lim_prodtke)
+      for (const DevBlock &b : L.hb) {
+        k_lim_prod_mg<<<grid_for(cnt_interior(b, p)), 256, 0, c->s>>>(b, c->d_p, q, L.d_prd, P.mut);
+        if ((r = after_launch(c))) return r;
+      }
+    for (const DevBlock &b : L.hb) {
+      k_lim_res_ome<<<grid_for(cnt_interior(b, p)), 256, 0, c->s>>>(b, c->d_p, P.res, q, P.vol, P.dtvolt,
+                                                                   L.d_delpls, L.d_prd, p.alphas[irk - 1]);
+      if ((r = after_launch(c))) return r;
+    }
+    return COSA_OK;
+  }
   if (p.irsop > 0) {
     const double *beta[3] = {P.betaxi ? P.betaxi : L.d_beta[0], P.betaeta ? P.betaeta : L.d_beta[1],
                              P.betazeta ? P.betazeta : L.d_beta[2]};
@@ -2457,9 +2518,10 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, bool compute_
 }
 
 int launch_rans_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
-  if (o.rhs || o.res_only) return COSA_ERR_UNSUPPORTED;  // k-omega multigrid is not on this path
+  if (o.res_only && o.res_only != L.ptrs.res) return COSA_ERR_ARG;  // the residual pass leaves R in res
+  if (o.res_only) return launch_rans_stage(c, nl, L, 1, o);
   for (int irk = 1; irk <= c->p.nstage; ++irk) {
-    int r = launch_rans_stage(c, nl, L, irk, o.compute_dt && irk == 1, o.want_rms && irk == 1, o.copy_qold);
+    int r = launch_rans_stage(c, nl, L, irk, o);
     if (r) return r;
   }
   return COSA_OK;

@@ -10,6 +10,10 @@
 //   k_srckw           srckw_b: k and omega sources into res
 //   k_update_kom      update_b's point-implicit k / omega update
 //   k_cut_scalar      cut_q on a scalar P3 array (cutman_mut)
+//   k_rest4           rest4_b: volume-weighted restriction of a scalar field
+//   k_lim_prod_mg     lim_prod_mg_b: production limiter before restriction
+//   k_lim_res_ome     lim_res_ome_b: omega residual limiter (residual pass)
+//   k_add_interior    add_array over the interior cells (multigrid forcing)
 #pragma once
 #include "visc.cuh"
 
@@ -268,5 +272,88 @@ __global__ void k_cut_scalar(const DevBlock *__restrict__ blocks, const HaloItem
     // the cut of the reference's last write keeps each halo cell (host mask)
     if (it.mask & 1) a[bd + it.h1] = a[bs + it.c1];
     if (it.mask & 2) a[bd + it.h2] = a[bs + it.c2];
+  }
+}
+
+// ---- k-omega multigrid (src/cosa.f90:2672-2755, 3122-3160; src/src.f90:708-745;
+// src/update.f90:2585-2835) --------------------------------------------------------------
+// rest4_b: coarse cell = volume-weighted mean of its 8 fine cells, the
+// reference's summation order (one thread per coarse cell and snapshot)
+__global__ void k_rest4(DevBlock b1, DevBlock b2, int S, const double *__restrict__ f1, double *__restrict__ f2,
+                        const double *__restrict__ vol1, const double *__restrict__ vol2) {
+  const int ni = b2.im - 1, nj = b2.jm - 1, nk = b2.km - 1;
+  const int64_t total = (int64_t)ni * nj * nk * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i2 = (int)(r % ni) + 1; r /= ni;
+    const int j2 = (int)(r % nj) + 1; r /= nj;
+    const int k2 = (int)(r % nk) + 1; r /= nk;
+    const int n = (int)r;
+    const int i1 = 2 * i2 - 1, j1 = 2 * j2 - 1, k1 = 2 * k2 - 1;
+    const int di[8] = {0, 0, 1, 1, 0, 0, 1, 1}, dj[8] = {0, 1, 0, 1, 0, 1, 0, 1}, dk[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+    double s = 0.0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const double w = vol1[p1_idx(b1, 1, i1 + di[m], j1 + dj[m], k1 + dk[m], 0)];
+      const double a = f1[p3s_idx(b1, S, i1 + di[m], j1 + dj[m], k1 + dk[m], n)];
+      s = m == 0 ? w * a : s + w * a;
+    }
+    f2[p3s_idx(b2, S, i2, j2, k2, n)] = s / vol2[p1_idx(b2, 1, i2, j2, k2, 0)];
+  }
+}
+
+// lim_prod_mg_b: q conservative (tke, ome are rho k, rho omega), as the
+// reference's residual pass leaves it
+__global__ void k_lim_prod_mg(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
+                              double *__restrict__ prd, const double *__restrict__ mut) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const double mor = P.machfs / P.reyno;
+  KOM_CELL_LOOP
+    const int64_t c = p3_cell(b, i, j, k), o = p3s_idx(b, S, i, j, k, n);
+    const double rho = q[p3_var(b, npde, S, 1, n) + c], tke = q[p3_var(b, npde, S, 6, n) + c];
+    const double ome = q[p3_var(b, npde, S, 7, n) + c];
+    const double mt = mut[o], prod = prd[o];
+    const double tstdis = P.prdlim * P.bstrkw * rho * tke * ome;
+    if (mor * mt * prod > tstdis) prd[o] = tstdis / mor / mt;
+  }
+}
+
+// lim_res_ome_b, explicit branch without low-speed preconditioning
+// (ttrm = (0, gkw, bkw) for the Wilcox model)
+__global__ void k_lim_res_ome(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ res,
+                              const double *__restrict__ q, const double *__restrict__ vol,
+                              const double *__restrict__ dtt, const double *__restrict__ delpls,
+                              const double *__restrict__ prd, double ar) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const double gav = P.gkw, bav = P.bkw;
+  KOM_CELL_LOOP
+    const int64_t c = p3_cell(b, i, j, k), o = p3s_idx(b, S, i, j, k, n);
+    const int64_t i1 = p3_var(b, npde, S, 1, n) + c, i7 = p3_var(b, npde, S, 7, n) + c;
+    const double dt = dtt[p1_idx(b, S, i, j, k, n)];
+    const double dtau = dt * vol[p1_idx(b, 1, i, j, k, 0)];
+    const double rho = q[i1], ome = q[i7] / q[i1];
+    const double den1 = 1 + ar * dtau * (gav * delpls[o] + 2 * bav * ome);
+    const double rhomega = q[i7] - ar * res[i7] * dt / den1;
+    const double rhomegamin = gav * P.cmu * rho * sqrt(prd[o]);
+    if (rhomega < rhomegamin) res[i7] = den1 * (q[i7] - rhomegamin) / dt / ar;
+  }
+}
+
+// add_array over the interior cells (off_l = -1, src/util.f90:137-222):
+// v1 += fact v2 for all nvs = npde * S variable planes
+__global__ void k_add_interior(DevBlock b, int nvs, double *__restrict__ v1, const double *__restrict__ v2,
+                               double fact) {
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t total = (int64_t)ni * nj * nk * nvs;
+  const int64_t base = b.op3 * nvs;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)(r % nk) + 1; r /= nk;
+    const int64_t o = base + r * b.P3 + p3_cell(b, i, j, k);
+    v1[o] = v1[o] + v2[o] * fact;
   }
 }

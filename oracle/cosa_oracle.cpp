@@ -1367,6 +1367,70 @@ void rest2_lo_b(const Level &L1, const Level &L2, int b, double *rhs2a, const do
           }
 }
 
+// rest4_b (src/cosa.f90:3122-3160): volume-weighted restriction of a
+// scalar P3 field (prd, delpls, divvel or mut)
+void rest4_b(const Level &L1, const Level &L2, int b, const double *f1a, double *f2a, const double *v1a,
+             const double *v2a) {
+  B3s f1(const_cast<double *>(f1a), L1, b), f2(f2a, L2, b);
+  B1 v1(const_cast<double *>(v1a), L1, b, 1), v2(const_cast<double *>(v2a), L2, b, 1);
+  const int im1 = L1.im[b], jm1 = L1.jm[b], km1 = L1.km[b];
+  for (int n = 0; n < L1.S; ++n)
+    for (int k1 = 1; k1 <= km1 - 2; k1 += 2)
+      for (int j1 = 1; j1 <= jm1 - 2; j1 += 2)
+        for (int i1 = 1; i1 <= im1 - 2; i1 += 2) {
+          const int i2 = 1 + i1 / 2, j2 = 1 + j1 / 2, k2 = 1 + k1 / 2;
+          f2(i2, j2, k2, n) =
+              (v1(i1, j1, k1) * f1(i1, j1, k1, n) + v1(i1, j1 + 1, k1) * f1(i1, j1 + 1, k1, n) +
+               v1(i1 + 1, j1, k1) * f1(i1 + 1, j1, k1, n) + v1(i1 + 1, j1 + 1, k1) * f1(i1 + 1, j1 + 1, k1, n) +
+               v1(i1, j1, k1 + 1) * f1(i1, j1, k1 + 1, n) + v1(i1, j1 + 1, k1 + 1) * f1(i1, j1 + 1, k1 + 1, n) +
+               v1(i1 + 1, j1, k1 + 1) * f1(i1 + 1, j1, k1 + 1, n) +
+               v1(i1 + 1, j1 + 1, k1 + 1) * f1(i1 + 1, j1 + 1, k1 + 1, n)) /
+              v2(i2, j2, k2);
+        }
+}
+
+// lim_prod_mg_b (src/src.f90:708-745): the production limiter applied to
+// prd before it is restricted; q is conservative here (the residual pass
+// has converted it back), so tke and ome are rho k and rho omega
+void lim_prod_mg_b(const Level &L, int b, const double *qa, double *prda, const double *muta,
+                   const cosa_params &P) {
+  B3 q(const_cast<double *>(qa), L, b);
+  B3s prd(prda, L, b), mu(const_cast<double *>(muta), L, b);
+  const double mor = P.machfs / P.reyno;
+  for (int n = 0; n < L.S; ++n)
+    for (int k = 1; k <= L.km[b] - 1; ++k)
+      for (int j = 1; j <= L.jm[b] - 1; ++j)
+        for (int i = 1; i <= L.im[b] - 1; ++i) {
+          const double rho = q(i, j, k, 1, n), tke = q(i, j, k, 6, n), ome = q(i, j, k, 7, n);
+          const double mut = mu(i, j, k, n), prod = prd(i, j, k, n);
+          const double tstdis = P.prdlim * P.bstrkw * rho * tke * ome;
+          if (mor * mut * prod > tstdis) prd(i, j, k, n) = tstdis / mor / mut;
+        }
+}
+
+// lim_res_ome_b (src/update.f90:2585-2835), explicit branch without
+// low-speed preconditioning: the omega residual is limited so that the
+// point-implicit update cannot take rho omega below gkw cmu rho sqrt(prd);
+// ttrm = (0, gkw, bkw) for the Wilcox model
+void lim_res_ome_b(const Level &L, int b, double *ra, const double *qa, const double *va, const double *dtta,
+                   const double *dpla, const double *prda, double ar, const cosa_params &P) {
+  B3 res(ra, L, b), q(const_cast<double *>(qa), L, b);
+  B1 vol(const_cast<double *>(va), L, b, 1), dtt(const_cast<double *>(dtta), L, b, L.S);
+  B3s dpl(const_cast<double *>(dpla), L, b), prd(const_cast<double *>(prda), L, b);
+  const double gav = P.gkw, bav = P.bkw;
+  for (int n = 0; n < L.S; ++n)
+    for (int k = 1; k <= L.km[b] - 1; ++k)
+      for (int j = 1; j <= L.jm[b] - 1; ++j)
+        for (int i = 1; i <= L.im[b] - 1; ++i) {
+          const double dtau = dtt(i, j, k, n) * vol(i, j, k);
+          const double rho = q(i, j, k, 1, n), ome = q(i, j, k, 7, n) / q(i, j, k, 1, n);
+          const double den1 = 1 + ar * dtau * (gav * dpl(i, j, k, n) + 2 * bav * ome);
+          const double rhomega = q(i, j, k, 7, n) - ar * res(i, j, k, 7, n) * dtt(i, j, k, n) / den1;
+          const double rhomegamin = gav * P.cmu * rho * std::sqrt(prd(i, j, k, n));
+          if (rhomega < rhomegamin) res(i, j, k, 7, n) = den1 * (q(i, j, k, 7, n) - rhomegamin) / dtt(i, j, k, n) / ar;
+        }
+}
+
 // q_bedges (src/flux.f90:3913-4263): the plane through three neighbours of
 // each halo edge cell, evaluated at the edge cell.  Edge families: (i,j) at
 // every interior k, (i,k) at every interior j, (j,k) at every interior i.
@@ -2788,7 +2852,7 @@ struct VExtra {
   double *tbx, *tby, *tbz;
 };
 int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_ptrs &A, const VExtra &X,
-                  int want_dt);
+                  int want_dt, bool mut_first = false);
 
 int orc_residual(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
                  const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
@@ -2820,7 +2884,7 @@ int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const d
  * (and IRS coefficients when the beta arrays are set).
  */
 int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_ptrs &A, const VExtra &X,
-                  int want_dt) {
+                  int want_dt, bool mut_first) {
   Level &L = h->L;
   const bool visc = p->viscous != 0, kom = is_kom(*p);
   if (p->kom_bsl || p->kom_sst) return COSA_ERR_UNSUPPORTED;
@@ -2830,6 +2894,12 @@ int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_p
   for (int b = 0; b < L.nb; ++b) cons2prim_b(L, b, q, 0, *p);
   int status = bc_level(L, q, A.si, A.sj, A.sk, *p, A.dist);
   cutman_q_level(L, q);
+  if (mut_first) {
+    // coarse-level mut from the restricted (primitive) state at the first
+    // stage of the first cycle's visit (src/cosa.f90:1727-1760)
+    tur_vis_level(L, q, A.mut, *p);
+    cutman_mut_level(L, A.mut);
+  }
   status |= prtest_level(L, q, *p);
   if (want_dt) {
     if (visc) {
@@ -3023,7 +3093,7 @@ int orc_prolong(orc_level *f, orc_level *c, const cosa_params *p, const cosa_lev
   orc_rest1(f, c, P1->q, P2->qold, P1->vol, P2->vol);
   for (double *a : {P2->qold, P2->q}) {
     for (int b = 0; b < L2.nb; ++b) cons2prim_b(L2, b, a, 0, *p);
-    status |= bc_level(L2, a, P2->si, P2->sj, P2->sk, *p);
+    status |= bc_level(L2, a, P2->si, P2->sj, P2->sk, *p, P2->dist);
     cutman_q_level(L2, a);
     for (int b = 0; b < L2.nb; ++b) prim2cons_b(L2, b, a, *p);
     for (int b = 0; b < L2.nb; ++b) q_bedges(L2, b, a, nullptr);
@@ -3268,6 +3338,124 @@ void orc_update_kom(orc_level *h, const cosa_params *p, const double *res, doubl
                     const double *vol, const double *dtvolt, const double *delpls, const double *prd, double ar) {
   for (int b = 0; b < h->L.nb; ++b) update_kom_b(h->L, b, res, q, qold, vol, dtvolt, delpls, prd, ar, *p);
 }
+// ---- k-omega multigrid ------------------------------------------------------
+// per-level arrays of the k-omega residual beyond cosa_level_ptrs
+struct orc_vextra {
+  const double *vm;
+  double *prd, *divvel, *delpls, *tbx, *tby, *tbz;
+};
+static VExtra vx(const orc_vextra &e) { return VExtra{e.vm, e.prd, e.divvel, e.delpls, e.tbx, e.tby, e.tbz}; }
+
+void orc_rest4(orc_level *f, orc_level *c, const double *f1, double *f2, const double *vol1, const double *vol2) {
+  for (int b = 0; b < f->L.nb; ++b) rest4_b(f->L, c->L, b, f1, f2, vol1, vol2);
+}
+void orc_lim_prod_mg(orc_level *h, const cosa_params *p, const double *q, double *prd, const double *mut) {
+  for (int b = 0; b < h->L.nb; ++b) lim_prod_mg_b(h->L, b, q, prd, mut, *p);
+}
+void orc_lim_res_ome(orc_level *h, const cosa_params *p, double *res, const double *q, const double *vol,
+                     const double *dtvolt, const double *delpls, const double *prd, double ar) {
+  for (int b = 0; b < h->L.nb; ++b) lim_res_ome_b(h->L, b, res, q, vol, dtvolt, delpls, prd, ar, *p);
+}
+
+// smooth(nl, from_fine, to_coarse, done, niter) with the k-omega terms
+// (src/cosa.f90:1594-2032): mut of the coarse level from its restricted
+// state at the first stage of the first cycle's visit, the forcing, and on
+// the residual pass (to_coarse) lim_prod_mg and lim_res_ome
+int orc_smooth_level_rans(orc_level *h, const cosa_params *p, int nl, int nlevel, const cosa_level_ptrs *Ap,
+                          const orc_vextra *E, int niter, int from_fine, int to_coarse, int mgit, int ncycle,
+                          int rms_every, double *hist_row) {
+  Level &L = h->L;
+  const cosa_level_ptrs &A = *Ap;
+  const VExtra X = vx(*E);
+  int status = 0;
+  const int niterp = to_coarse ? niter + 1 : niter;
+  for (int iter = 1; iter <= niterp; ++iter) {
+    if (iter <= niter) copy_interior(L, A.qold, A.q);
+    for (int irk = 1; irk <= p->nstage; ++irk) {
+      const bool want_dt = (iter / p->iupdt * p->iupdt == iter) && irk == 1;
+      const bool mut_first = mgit == 1 && iter == 1 && irk == 1 && from_fine && !p->prd_all_lvls;
+      status |= residual_full(h, p, nl, A, X, want_dt, mut_first);
+      if (status & (COSA_ERR_ARG | COSA_ERR_UNSUPPORTED)) return status;
+      if (nl == 1 && irk == 1 && iter != niter + 1 && hist_row &&
+          (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle))
+        resg_rms_level(L, A.res, A.rhs, hist_row);
+      if (from_fine && iter == 1 && irk == 1) add_level(L, A.rhs, A.res, 1.0, -1);
+      if (nl > 1) add_level(L, A.res, A.rhs, -1.0, -1);
+      if (iter == niter + 1) {
+        if (nlevel > 1 && nl != nlevel && !p->prd_all_lvls && p->lim_prodtke)
+          for (int b = 0; b < L.nb; ++b) lim_prod_mg_b(L, b, A.q, X.prd, A.mut, *p);
+        for (int b = 0; b < L.nb; ++b)
+          lim_res_ome_b(L, b, A.res, A.q, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p);
+        return status;
+      }
+      if (p->irsop > 0)
+        irs_level(L, A.res, A.dtvol, A.dtvolt, A.betaxi, A.betaeta, A.betazeta, X.tbx, X.tby, X.tbz, *p);
+#pragma omp parallel for schedule(dynamic)
+      for (int b = 0; b < L.nb; ++b) {
+        update_kom_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p);
+        update_b(L, b, A.res, A.q, A.qold, A.dtvol, p->alphas[irk - 1]);
+      }
+      if (p->ifixq) fixq_level(L, A.q, *p);
+      if (irk == p->nstage && (nl == 1 || !p->prd_all_lvls)) {
+        tur_vis_level(L, A.q, A.mut, *p);
+        cutman_mut_level(L, A.mut);
+      }
+    }
+  }
+  return status;
+}
+
+// restrict (src/cosa.f90:2672-2755), k-omega branch without ho_rest: q, the
+// production terms (or mut with prd_all_lvls) and the residual sums
+int orc_restrict_rans(orc_level *f, orc_level *c, const cosa_params *p, const cosa_level_ptrs *P1,
+                      const cosa_level_ptrs *P2, const orc_vextra *E1, const orc_vextra *E2) {
+  orc_rest1(f, c, P1->q, P2->q, P1->vol, P2->vol);
+  if (!p->prd_all_lvls) {
+    orc_rest4(f, c, E1->prd, E2->prd, P1->vol, P2->vol);
+    orc_rest4(f, c, E1->delpls, E2->delpls, P1->vol, P2->vol);
+    orc_rest4(f, c, E1->divvel, E2->divvel, P1->vol, P2->vol);
+  } else {
+    orc_rest4(f, c, P1->mut, P2->mut, P1->vol, P2->vol);
+  }
+  orc_rest2(f, c, P2->rhs, P1->res);
+  return 0;
+}
+
+// mg() (src/cosa.f90:806-930) with the k-omega smoothing and restriction
+int orc_mg_rans(orc_level **lv, int nlevel, const cosa_params *p, const cosa_level_ptrs *P, const orc_vextra *E,
+                int mgit0, int ncycles, int ncycle, int rms_every, double *hist) {
+  int status = 0;
+  const int npde = p->npde;
+  int last = mgit0 - 1;
+  for (int mgit = mgit0; mgit < mgit0 + ncycles; ++mgit) {
+    last = mgit;
+    double *row = hist ? hist + (int64_t)(mgit - mgit0) * (npde + 1) : nullptr;
+    int niter = nlevel == 1 ? 1 : (mgit == 1 ? p->nstart : p->npost);
+    status |= orc_smooth_level_rans(lv[0], p, 1, nlevel, &P[0], &E[0], niter, 0, nlevel > 1, mgit, ncycle,
+                                    rms_every, row);
+    if (nlevel > 1) {
+      status |= orc_restrict_rans(lv[0], lv[1], p, &P[0], &P[1], &E[0], &E[1]);
+      niter = nlevel == 2 ? p->ncrs : p->npre;
+      status |= orc_smooth_level_rans(lv[1], p, 2, nlevel, &P[1], &E[1], niter, 1, nlevel > 2, mgit, ncycle,
+                                      rms_every, nullptr);
+      if (nlevel == 3) {
+        status |= orc_restrict_rans(lv[1], lv[2], p, &P[1], &P[2], &E[1], &E[2]);
+        status |= orc_smooth_level_rans(lv[2], p, 3, nlevel, &P[2], &E[2], p->ncrs, 1, 0, mgit, ncycle, rms_every,
+                                        nullptr);
+        status |= orc_prolong(lv[1], lv[2], p, &P[1], &P[2]);
+        status |= orc_smooth_level_rans(lv[1], p, 2, nlevel, &P[1], &E[1], p->npost, 0, 0, mgit, ncycle,
+                                        rms_every, nullptr);
+      }
+      status |= orc_prolong(lv[0], lv[1], p, &P[0], &P[1]);
+    }
+    if (status & (COSA_ERR_ARG | COSA_ERR_UNSUPPORTED)) return status;
+  }
+  if (nlevel > 1 && last == ncycle)
+    status |= orc_smooth_level_rans(lv[0], p, 1, nlevel, &P[0], &E[0], p->npost, 0, 0, ncycle + 1, ncycle,
+                                    rms_every, nullptr);
+  return status;
+}
+
 void orc_deltat_ns_full(orc_level *h, const cosa_params *p, double *dtvol, const double *lam, const double *lamv,
                         double *bx, double *by, double *bz, double *dtvolt, double *tbx, double *tby, double *tbz) {
   deltat_ns_level(h->L, dtvol, lam, lamv, bx, by, bz, *p, dtvolt, tbx, tby, tbz);

@@ -512,3 +512,52 @@ def force(O, q, x, y, z, si, sj, sk, vm, isurf=1, xmom=(0.25, 0.0, 0.0), lngth=(
     lib().orc_force(O.h, _par(O.p), _p(q), _p(x), _p(y), _p(z), _p(si), _p(sj), _p(sk), _opt(vm),
                     C.c_int(isurf), _p(xm), _p(ln), _p(out))
     return out.reshape(O.S, 12)
+
+
+# ---- k-omega multigrid ---------------------------------------------------------------
+class _VExtra(C.Structure):
+    _fields_ = [(n, _dp) for n in ("vm", "prd", "divvel", "delpls", "tbx", "tby", "tbz")]
+
+
+def _vextra(A):
+    return _VExtra(*A.extras())
+
+
+def rest4(Of, Oc, f1, f2, vol1, vol2):
+    lib().orc_rest4(Of.h, Oc.h, _p(f1), _p(f2), _p(vol1), _p(vol2))
+
+
+def lim_prod_mg(O, q, prd, mut):
+    lib().orc_lim_prod_mg(O.h, _par(O.p), _p(q), _p(prd), _p(mut))
+
+
+def lim_res_ome(O, res, q, vol, dtvolt, delpls, prd, ar):
+    lib().orc_lim_res_ome(O.h, _par(O.p), _p(res), _p(q), _p(vol), _p(dtvolt), _p(delpls), _p(prd), C.c_double(ar))
+
+
+def smooth_level_rans(O, nl, nlevel, A, niter, from_fine, to_coarse, mgit=1, ncycle=1, rms_every=1):
+    row = np.full(O.p.npde + 1, np.nan)
+    pt, ex = A.ptrs(), _vextra(A)
+    st = lib().orc_smooth_level_rans(O.h, _par(O.p), C.c_int(nl), C.c_int(nlevel), C.byref(pt), C.byref(ex),
+                                     C.c_int(niter), C.c_int(int(from_fine)), C.c_int(int(to_coarse)), C.c_int(mgit),
+                                     C.c_int(ncycle), C.c_int(rms_every), _p(row))
+    return row, st
+
+
+def restrict_rans(Of, Oc, A1, A2):
+    p1, p2, e1, e2 = A1.ptrs(), A2.ptrs(), _vextra(A1), _vextra(A2)
+    return lib().orc_restrict_rans(Of.h, Oc.h, _par(Of.p), C.byref(p1), C.byref(p2), C.byref(e1), C.byref(e2))
+
+
+def mg_rans(levels, arrays, mgit0, ncycles, ncycle, rms_every=1):
+    """mg() cycles of the k-omega path on oracle levels (levels[0] finest)
+    with RansArrays each."""
+    n = len(levels)
+    hs = (C.c_void_p * n)(*[O.h.value for O in levels])
+    ps = (_LevelPtrs * n)(*[A.ptrs() for A in arrays])
+    es = (_VExtra * n)(*[_vextra(A) for A in arrays])
+    p = levels[0].p
+    hist = np.full((max(ncycles, 1), p.npde + 1), np.nan)
+    st = lib().orc_mg_rans(hs, C.c_int(n), _par(p), ps, es, C.c_int(mgit0), C.c_int(ncycles), C.c_int(ncycle),
+                           C.c_int(rms_every), _p(hist))
+    return hist[:ncycles], st

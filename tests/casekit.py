@@ -51,3 +51,31 @@ def mg_oracle(case, nlevel, params, oracle_mod, q_fine=None):
     if q_fine is not None:
         As[0].q[:] = q_fine
     return lv, Os, As
+
+
+def mg_rans_oracle(case, nlevel, params, oracle_mod):
+    """Oracle levels + RansArrays of an nlevel k-omega multigrid set-up of
+    `case`: metrics, viscous set-up and wall distance on every level, the
+    free stream on every level, the fine level's mut from its state after
+    the BCs (coarse mut is set by the first cycle's visit)."""
+    lv = cases.mg_levels(case, nlevel)
+    Os, As = [], []
+    for i, (t, x, y, z) in enumerate(lv):
+        O = oracle_mod.OracleLevel(t, params)
+        A = oracle_mod.RansArrays(O)
+        x, y, z = x.copy(), y.copy(), z.copy()
+        A.si, A.sj, A.sk, A.vol = O.metrics(x, y, z)
+        A.vm = oracle_mod.viscous_setup(O, x, y, z, A.vol)
+        A.dist[:] = cases.wall_distance(cases.Case("level", t, params, x, y, z, None))
+        A.q[:] = case.q0 if i == 0 else cases._freestream_state(t, params)
+        Os.append(O)
+        As.append(A)
+    O, A = Os[0], As[0]
+    qq = A.q.copy()
+    O.cons2prim(qq)
+    oracle_mod.bc_dist(O, qq, A.si, A.sj, A.sk, A.dist)
+    O.cutman_q(qq)
+    O.prim2cons(qq)
+    oracle_mod.tur_vis(O, qq, A.mut)
+    oracle_mod.cutman_mut(O, A.mut)
+    return lv, Os, As

@@ -193,3 +193,73 @@ def test_rans_smooth_runs(oracle_mod):
     assert st == 0
     rows = hist[~np.isnan(hist[:, 0])]
     assert np.isfinite(rows).all() and (rows[:, [0, 1, 4, 5, 6]] > 0).all()
+
+
+def test_rest4_and_omega_residual_limiter(oracle_mod):
+    """rest4 restricts a constant to itself; lim_res_ome rewrites the omega
+    residual exactly where the point-implicit update would undercut
+    gkw cmu rho sqrt(prd), to the value that lands on that floor."""
+    case = cases.turbulent_channel(16, 8, 4)
+    p = case.params
+    lv = cases.mg_levels(case, 2)
+    Of, Oc = (oracle_mod.OracleLevel(t, p) for (t, _, _, _) in lv)
+    vf = np.random.default_rng(1).uniform(0.5, 2.0, Of.p1().size)
+    vc = np.zeros(Oc.p1().size)
+    # coarse volumes = sums of their 8 fine volumes, so a constant survives
+    for bf, bc in zip(p1_views(lv[0][0], vf, 1), p1_views(lv[1][0], vc, 1)):
+        f = bf[1:-1, 1:-1, 1:-1, 0]
+        bc[1:-1, 1:-1, 1:-1, 0] = (f[0::2, 0::2, 0::2] + f[1::2, 0::2, 0::2] + f[0::2, 1::2, 0::2] +
+                                   f[1::2, 1::2, 0::2] + f[0::2, 0::2, 1::2] + f[1::2, 0::2, 1::2] +
+                                   f[0::2, 1::2, 1::2] + f[1::2, 1::2, 1::2])
+    f1 = np.full(Of.n3 * Of.S, 3.25)
+    f2 = np.zeros(Oc.n3 * Oc.S)
+    oracle_mod.rest4(Of, Oc, f1, f2, vf, vc)
+    (im, jm, km), = lv[1][0].dims
+    f2v = f2.reshape(km + 3, jm + 3, im + 3)[2:-2, 2:-2, 2:-2]
+    np.testing.assert_allclose(f2v, 3.25, rtol=1e-14)
+    # lim_res_ome on a uniform conservative state
+    O = Of
+    rho, rk, rw = 1.1, 2e-4, 0.4
+    q = O.p3()
+    for v in p3_views(lv[0][0], q, 7, 1):
+        v[..., 0, 0] = rho
+        v[..., 5, 0] = rk
+        v[..., 6, 0] = rw
+    dtt = np.full(O.n1, 0.02)
+    vol = np.full(O.n1, 0.5)
+    dpl = np.zeros(O.n3)
+    prd = np.full(O.n3, 0.09)
+    res = O.p3()
+    r = p3_views(lv[0][0], res, 7, 1)[0]
+    r[..., 6, 0] = 100.0          # large positive residual: rho omega would drop below the floor
+    r[2:-2, 2:-2, 2, 6, 0] = -1.0  # negative residual on one k plane: untouched
+    ar = 0.25
+    oracle_mod.lim_res_ome(O, res, q, vol, dtt, dpl, prd, ar)
+    dtau = 0.02 * 0.5
+    den1 = 1 + ar * dtau * (2 * p.bkw * rw / rho)
+    floor = p.gkw * p.cmu * rho * np.sqrt(0.09)
+    assert rw - ar * 100.0 * 0.02 / den1 < floor
+    np.testing.assert_allclose(r[2:-2, 2:-2, 3:-2, 6, 0], den1 * (rw - floor) / 0.02 / ar, rtol=1e-13)
+    assert np.all(r[2:-2, 2:-2, 2, 6, 0] == -1.0)
+
+
+def test_kom_multigrid_accelerates(oracle_mod):
+    """Three-level k-omega V-cycles (forcing, restricted production terms,
+    lim_res_ome) reduce the density residual faster than single-grid
+    cycles from the same start."""
+    import casekit
+    out = {}
+    for nlevel in (1, 3):
+        p = cases.kom_params(0.3, 1e5)
+        p.cfl = p.cflt = 1.5
+        p.nlevel = nlevel
+        p.nstart = p.npre = p.npost = p.ncrs = 1
+        p.bln_prol = 1
+        case = cases.turbulent_channel(32, 16, 8)
+        lv, Os, As = casekit.mg_rans_oracle(case, nlevel, p, oracle_mod)
+        h, st = oracle_mod.mg_rans(Os, As, 1, 30, 30, rms_every=10)
+        assert st == 0
+        rows = h[~np.isnan(h[:, 0])]
+        assert np.isfinite(rows).all()
+        out[nlevel] = rows[-1, 0] / rows[0, 0]
+    assert out[3] < 0.5 * out[1], out
