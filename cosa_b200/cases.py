@@ -601,6 +601,10 @@ def naca_params(model: str = "kom", mach: float = 0.3, alpha_deg: float = 4.0, r
     p.cfl = cfl
     p.cflt = cfl
     p.nlevel = nlevel
+    if nlevel > 1:
+        # one pre-, post- and coarsest-level iteration, bilinear prolongation
+        p.nstart = p.npre = p.npost = p.ncrs = 1
+        p.bln_prol = 1
     if eps_irs > 0:
         p.irsop = 1
         p.rat = float(np.sqrt(1 + 4 * eps_irs))

@@ -1,14 +1,17 @@
-"""Single-level steady driver over the C-ABI: the part of COSA's main program
-(src/cosa.f90:300-322 viscous set-up, 780-840 the iteration loop of a
-one-level mg(), src/output.f90:4960-4990 the force output) that a solve of
-one synthetic case needs.
+"""Steady driver over the C-ABI: the part of COSA's main program
+(src/cosa.f90:300-322 viscous set-up, 780-930 the iteration loop of mg(),
+src/output.f90:4960-4990 the force output) that a solve of one synthetic
+case needs, on one level or on params.nlevel multigrid levels.
 
     s = SteadySolver(case)            # geometry, metrics, viscous set-up, wall distance
-    hist = s.run(2000, rms_every=100) # resrms rows of the printed iterations
+    hist = s.run(2000, rms_every=100) # resrms rows of the printed cycles
     c = s.forces()                    # (S, 12) force/moment coefficients of surface 1
 
-Every array lives on the device; the state is read back only by state()
-and forces() (12 doubles per snapshot).
+With params.nlevel > 1 every level gets its own coarsened grid (every other
+node), metrics, face inverse metrics and wall distance, its state starts at
+the free stream like the fine one (init2fs on every level), and run() calls
+cosa_gpu_mg.  Every array lives on the device; the state is read back only
+by state() and forces() (12 doubles per snapshot).
 """
 from __future__ import annotations
 
@@ -22,53 +25,79 @@ from .params import CosaParams
 
 class SteadySolver:
     def __init__(self, case: "cases.Case", params: Optional[CosaParams] = None, device: int = 0,
-                 q0: Optional[np.ndarray] = None):
+                 q0: Optional[np.ndarray] = None, ncycle: Optional[int] = None):
         self.case = case
         self.p = params if params is not None else case.params
         p = self.p
+        self.nlevel = max(1, int(p.nlevel))
+        self.ncycle = ncycle
         self.viscous = bool(p.viscous)
         self.kom = bool(p.kom)
-        ctx = gpu.Context([case.tables], p, device=device)
+        lv = cases.mg_levels(case, self.nlevel) if self.nlevel > 1 else [(case.tables, case.x, case.y, case.z)]
+        ctx = gpu.Context([t for (t, _, _, _) in lv], p, device=device)
         self.ctx = ctx
-        self.X, self.Y, self.Z = (ctx.alloc_p2(ncomp=1).upload(a) for a in (case.x, case.y, case.z))
-        self.si, self.sj, self.sk = (ctx.alloc_p2() for _ in range(3))
-        self.vol = ctx.alloc_p1()
-        ctx.imetrix(1, self.X, self.Y, self.Z, self.si, self.sj, self.sk)
-        ctx.vols(1, self.X, self.Y, self.Z, self.vol)
-        self.vm = None
-        if self.viscous:
-            self.vm = ctx.alloc_vm()
-            ctx.viscous_setup(1, self.X, self.Y, self.Z, self.vol, self.vm)
-        self.q = ctx.alloc_p3().upload(case.q0 if q0 is None else q0)
-        arrays = dict(q=self.q, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(), si=self.si, sj=self.sj, sk=self.sk,
-                      vol=self.vol)
-        if p.irsop > 0:
-            arrays.update(betaxi=ctx.alloc_p1(), betaeta=ctx.alloc_p1(), betazeta=ctx.alloc_p1())
-        self.mut = None
+        self.levels = []
+        for nl, (t, x, y, z) in enumerate(lv, start=1):
+            L = {}
+            L["X"], L["Y"], L["Z"] = (ctx.alloc_p2(nl, ncomp=1).upload(a) for a in (x, y, z))
+            si, sj, sk = (ctx.alloc_p2(nl) for _ in range(3))
+            vol = ctx.alloc_p1(nl)
+            ctx.imetrix(nl, L["X"], L["Y"], L["Z"], si, sj, sk)
+            ctx.vols(nl, L["X"], L["Y"], L["Z"], vol)
+            vm = None
+            if self.viscous:
+                vm = ctx.alloc_vm(nl)
+                ctx.viscous_setup(nl, L["X"], L["Y"], L["Z"], vol, vm)
+            if nl == 1:
+                qinit = case.q0 if q0 is None else q0
+            else:
+                qinit = cases._freestream_state(t, p)
+            q = ctx.alloc_p3(nl).upload(qinit)
+            arrays = dict(q=q, qold=ctx.alloc_p3(nl), dtvol=ctx.alloc_p1(nl, ctx.S), si=si, sj=sj, sk=sk, vol=vol)
+            if self.nlevel > 1:
+                arrays.update(res=ctx.alloc_p3(nl), rhs=ctx.alloc_p3(nl))
+            if p.irsop > 0:
+                arrays.update(betaxi=ctx.alloc_p1(nl, ctx.S), betaeta=ctx.alloc_p1(nl, ctx.S),
+                              betazeta=ctx.alloc_p1(nl, ctx.S))
+            if self.kom:
+                dist = cases.wall_distance(cases.Case("level", t, p, x, y, z, None))
+                if "res" not in arrays:
+                    arrays["res"] = ctx.alloc_p3(nl)
+                arrays.update(dtvolt=ctx.alloc_p1(nl, ctx.S), qp=ctx.alloc_p3(nl), qm=ctx.alloc_p3(nl), dq=ctx.alloc_p3(nl), dqp=ctx.alloc_p3(nl),
+                              dqm=ctx.alloc_p3(nl), flux=ctx.alloc_f0(nl), mut=ctx.alloc_p3s(nl),
+                              dist=ctx.alloc_p1(nl).upload(dist))
+            ctx.bind_level(nl, **arrays)
+            L.update(arrays)
+            L["vm"] = vm
+            self.levels.append(L)
+        fine = self.levels[0]
+        self.q, self.X, self.Y, self.Z = fine["q"], fine["X"], fine["Y"], fine["Z"]
+        self.si, self.sj, self.sk, self.vol, self.vm = fine["si"], fine["sj"], fine["sk"], fine["vol"], fine["vm"]
+        self.mut = fine.get("mut")
         if self.kom:
-            self.mut = ctx.alloc_p3s()
-            self.dist = ctx.alloc_p1().upload(cases.wall_distance(case))
-            arrays.update(res=ctx.alloc_p3(), dtvolt=ctx.alloc_p1(), qp=ctx.alloc_p3(), qm=ctx.alloc_p3(),
-                          dq=ctx.alloc_p3(), dqp=ctx.alloc_p3(), dqm=ctx.alloc_p3(), flux=ctx.alloc_f0(),
-                          mut=self.mut, dist=self.dist)
-            # the initial turbulent viscosity: tur_vis of the state after the
-            # BCs (src/cosa.f90:560-600), halos of the cuts copied
+            # the initial turbulent viscosity: tur_vis of the fine state after
+            # the BCs (src/cosa.f90:560-600), halos of the cuts copied; the
+            # coarse levels' mut is set by the first cycle's visit
             qq = ctx.alloc_p3()
             qq.upload(self.q.download())
             ctx.cons2prim(1, qq)
-            ctx.bc_dist(1, qq, self.si, self.sj, self.sk, self.dist)
+            ctx.bc_dist(1, qq, self.si, self.sj, self.sk, fine["dist"])
             ctx.cutman_q(1, qq)
             ctx.prim2cons(1, qq)
             ctx.tur_vis(1, qq, self.mut)
             ctx.cutman_mut(1, self.mut)
-        ctx.bind_level(1, **arrays)
-        self.arrays = arrays
         self.it = 0
 
     def run(self, niter: int, rms_every: int = 10, want_hist: bool = True):
-        """niter iterations (one-level mg cycles); returns the resrms rows of
-        the printed iterations (NaN rows elsewhere) and the status word."""
-        hist, st = self.ctx.smooth(1, niter, self.it + 1, rms_every, want_hist=want_hist)
+        """niter cycles of mg() (one-level: RK iterations); returns the resrms
+        rows of the printed cycles (NaN rows elsewhere) and the status word.
+        The solve's last cycle (ncycle, when given at construction) adds the
+        fine-level post-smoothing of mg()."""
+        if self.nlevel == 1:
+            hist, st = self.ctx.smooth(1, niter, self.it + 1, rms_every, want_hist=want_hist)
+        else:
+            ncycle = self.ncycle if self.ncycle is not None else 2 ** 30
+            hist, st = self.ctx.mg(self.it + 1, niter, ncycle, rms_every, want_hist=want_hist)
         self.it += niter
         return hist, st
 
