@@ -393,13 +393,15 @@ def main():
 
     serving = None
     if rank == 0 and ws == 1 and not args.no_serve:
-        # continuous batching: 20 Poisson arrivals at 2 req/s of bump channels
-        # at three scales and random Mach numbers, each to a residual drop of
+        # continuous batching: 20 Poisson arrivals at 2 req/s, half bump
+        # channels and half Euler NACA 0012 O-grids (alpha ~ U[-4, 8] deg), at
+        # three scales and random Mach numbers, each to a residual drop of
         # 0.1 (single-grid explicit scheme), on this GPU after the duct runs
         from cosa_b200 import serve
         try:
-            serving = serve.run_sweep(serve.poisson_requests(20, 2.0, 0), 40e9, 0.1).summary()
-            serving["workload"] = "bump channel x{0.5,1,2} in-plane, M~U[0.3,0.7], Euler, Poisson 2 req/s"
+            serving = serve.run_sweep(serve.poisson_requests(20, 2.0, 0, naca_fraction=0.5), 40e9, 0.1).summary()
+            serving["workload"] = ("bump channel 128x64x2 / Euler NACA 0012 256x64x2 (50/50) x{0.5,1,2} in-plane, "
+                                   "M~U[0.3,0.7], alpha~U[-4,8] deg, Poisson 2 req/s")
         except Exception as e:  # reported, not fatal
             serving = {"error": str(e)}
 

@@ -45,6 +45,34 @@ struct ServeSolve {
 
 constexpr int64_t kSlotBytes = (3 * 5 + 2 + 3 * 4) * 8;  // Q, T, QO (5 each), DT, VOL, SI, SJ, SK (4 each)
 
+// per block of the merged level: 1 when an interior cell of the conservative
+// state has rho <= qmin(1), p <= qmin(5) or a non-finite value (the
+// positivity test of bprtest, src/cosa.f90:960-1120, used to find the solve
+// that set the shared status word)
+__global__ void k_block_bad(const DevBlock *__restrict__ blocks, const cosa_params *__restrict__ Pp,
+                            const double *__restrict__ q, int *__restrict__ bad) {
+  const DevBlock b = blocks[blockIdx.y];
+  const cosa_params &P = *Pp;
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t total = (int64_t)ni * nj * nk;
+  int found = 0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1;
+    const int k = (int)(r / nj) + 1;
+    const int64_t c = p3_cell(b, i, j, k);
+    double v[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) v[m] = q[p3_var(b, 5, 1, m + 1, 0) + c];
+    const double pr = (P.gamma - 1) * (v[4] - 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / v[0]);
+    const bool ok = isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]) && isfinite(v[3]) && isfinite(v[4]) &&
+                    v[0] > P.qmin[0] && pr > P.qmin[4];
+    found |= ok ? 0 : 1;
+  }
+  if (__syncthreads_or(found) && threadIdx.x == 0) bad[blockIdx.y] = 1;
+}
+
 }  // namespace
 
 struct cosa_serve {
@@ -58,6 +86,8 @@ struct cosa_serve {
   std::vector<int64_t> active;       // ids in the merged level's block order
   cosa_params *d_ps = nullptr;
   int ps_cap = 0;
+  int *d_bad = nullptr;  // per-block positivity flags of the merged level
+  int bad_cap = 0;
   int check_every = 10;
   bool dirty = true;
   uint64_t gen = 0;
@@ -326,6 +356,7 @@ int cosa_serve_destroy(cosa_serve *e) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->s);
   if (e->d_ps) cudaFree(e->d_ps);
+  if (e->d_bad) cudaFree(e->d_bad);
   if (c->d_seg) cudaFree(c->d_seg);
   if (c->d_seg_ncell) cudaFree(c->d_seg_ncell);
   if (c->L[0].d_part) cudaFree(c->L[0].d_part);
@@ -414,7 +445,38 @@ int cosa_serve_step(cosa_serve *e, int32_t niter, int32_t *nactive, int32_t *nqu
     }
     if (!done.empty() && (r = serve_retire(e, done))) return r;
   }
-  if ((r = cosa_gpu_status(c, 1))) return r;
+  const int st = cosa_gpu_status(c, 1);
+  const int soft = COSA_ERR_NEG_P | COSA_ERR_NEG_RHO | COSA_ERR_NAN;
+  if (st & ~soft) return st;
+  if (st && !e->active.empty() && !e->dirty) {
+    // a solve lost positivity: the status word is shared, so find the
+    // solves whose blocks hold a bad cell and retire them as failed; the
+    // other solves never read their cells and go on
+    LevelState &L = c->L[0];
+    if (e->bad_cap < L.nb) {
+      if (e->d_bad) { cudaFree(e->d_bad); e->d_bad = nullptr; }
+      CK(cudaMalloc(&e->d_bad, (size_t)L.nb * sizeof(int)));
+      e->bad_cap = L.nb;
+    }
+    CK(cudaMemsetAsync(e->d_bad, 0, (size_t)L.nb * sizeof(int), c->s));
+    int64_t mc = 1;
+    for (const DevBlock &x : L.hb) mc = std::max<int64_t>(mc, (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1));
+    k_block_bad<<<dim3(grid_x(mc, L.nb), L.nb), 256, 0, c->s>>>(L.d_blocks, c->d_p, e->Q, e->d_bad);
+    if ((r = after_launch(c))) return r;
+    std::vector<int> bad((size_t)L.nb);
+    CK(cudaMemcpyAsync(bad.data(), e->d_bad, bad.size() * sizeof(int), cudaMemcpyDeviceToHost, c->s));
+    CK(cudaStreamSynchronize(c->s));
+    std::vector<int64_t> failed;
+    int b0 = 0;
+    for (int64_t id : e->active) {
+      ServeSolve &s = e->solves[(size_t)id];
+      bool any = false;
+      for (int b = 0; b < s.nb; ++b) any |= bad[(size_t)(b0 + b)] != 0;
+      b0 += s.nb;
+      if (any) { s.state = SOLVE_FAILED; failed.push_back(id); }
+    }
+    if (!failed.empty() && (r = serve_retire(e, failed))) return r;
+  }
   if (nactive) *nactive = (int32_t)e->active.size();
   if (nqueued) *nqueued = (int32_t)e->queue.size();
   return COSA_OK;

@@ -2,7 +2,8 @@
 
 A seeded Poisson stream of steady solves arrives; each request is the bump
 channel at one of three in-plane scales with its own free-stream Mach
-number (and the matching inlet total state).  Requests are submitted when
+number (and the matching inlet total state), or an Euler NACA 0012 O-grid
+at one of three scales with its own Mach number and incidence.  Requests are submitted when
 they arrive, admitted by the engine as device memory allows, advanced
 together with whatever else is on the GPU, and retired at convergence.
 Reports throughput (solves per hour) and p50/p99 latency (arrival to
@@ -29,6 +30,8 @@ class Request:
     arrival: float
     case: Optional[cases.Case] = None
     flow: Optional[CosaParams] = None
+    alpha_deg: float = 0.0
+    grid: str = "channel"
 
 
 def channel_request(scale: float, mach: float, arrival: float = 0.0) -> Request:
@@ -39,19 +42,40 @@ def channel_request(scale: float, mach: float, arrival: float = 0.0) -> Request:
     return Request(scale, mach, arrival, case, case.params)
 
 
+def naca_request(scale: float, mach: float, alpha_deg: float, arrival: float = 0.0) -> Request:
+    """Euler NACA 0012 O-grid of the harmonic-balance family, 256 x 64 x 2
+    cells in four blocks (3/16, 5/16, 5/16, 3/16 of the contour) scaled by
+    `scale` in i and j, slip wall (14), far field (30) at 20 chords, free
+    stream at `mach` and incidence `alpha_deg`."""
+    ni, nj = max(16, int(round(256 * scale)) // 16 * 16), max(8, int(round(64 * scale)))
+    blocks = (3 * ni // 16, 5 * ni // 16, 5 * ni // 16, 3 * ni // 16)
+    p = cases.channel_params(mach)
+    p.alpha = float(np.deg2rad(alpha_deg))
+    case = cases.naca0012_ogrid(blocks=blocks, nj=nj, nk=2, rfar=20.0, h1=2e-3 / scale, params=p, wall=14)
+    return Request(scale, mach, arrival, case, case.params, alpha_deg, "naca")
+
+
 def engine_scheme() -> CosaParams:
     """The engine's scheme: Roe + MUSCL (kappa 1/3, smooth limiter), 4-stage
     RK at CFL 2; flow conditions come with each request."""
     return cases.channel_params(0.5)
 
 
-def poisson_requests(n: int, rate: float, seed: int, scales=(0.5, 1.0, 2.0), mach_range=(0.3, 0.7)) -> List[Request]:
+def poisson_requests(n: int, rate: float, seed: int, scales=(0.5, 1.0, 2.0), mach_range=(0.3, 0.7),
+                     naca_fraction: float = 0.0, alpha_range=(-4.0, 8.0)) -> List[Request]:
+    """n arrivals at `rate` per second (seeded): the bump channel, or with
+    probability naca_fraction the Euler NACA 0012 at an incidence drawn from
+    alpha_range (degrees); scale and Mach number drawn uniformly."""
     rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1.0 / rate, size=n))
     t -= t[0]
     out = []
     for k in range(n):
-        out.append(channel_request(float(rng.choice(scales)), float(rng.uniform(*mach_range)), float(t[k])))
+        scale, mach = float(rng.choice(scales)), float(rng.uniform(*mach_range))
+        if rng.uniform() < naca_fraction:
+            out.append(naca_request(scale, mach, float(rng.uniform(*alpha_range)), float(t[k])))
+        else:
+            out.append(channel_request(scale, mach, float(t[k])))
     return out
 
 
@@ -123,8 +147,9 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--tol", type=float, default=0.1)
     ap.add_argument("--budget-gb", type=float, default=150.0)
+    ap.add_argument("--naca-fraction", type=float, default=0.5)
     a = ap.parse_args()
-    reqs = poisson_requests(a.requests, a.rate, a.seed)
+    reqs = poisson_requests(a.requests, a.rate, a.seed, naca_fraction=a.naca_fraction)
     print(json.dumps(run_sweep(reqs, a.budget_gb * 1e9, a.tol).summary()))
 
 

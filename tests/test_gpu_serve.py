@@ -110,3 +110,43 @@ def test_short_sweep_reports_latency():
     assert s["converged"] == 6
     assert 0 < s["p50_latency_s"] <= s["p99_latency_s"]
     assert s["solves_per_hour"] > 0
+
+
+def test_naca_requests_in_the_mix():
+    """Euler NACA 0012 requests (4 blocks with the trailing-edge seam cut,
+    far field at their own incidence) served among bump channels: the same
+    bits alone and in the mix, every request converged."""
+    reqs = [serve.naca_request(0.5, 0.5, 6.0), serve.channel_request(0.5, 0.45), serve.naca_request(0.5, 0.65, -3.0)]
+    alone = _run(reqs, [0], tol=0.3)[0]
+    mixed = _run(reqs, [1, 0, 2], tol=0.3)
+    m = mixed[0]
+    assert alone["state"] == m["state"] == "converged"
+    assert alone["iters"] == m["iters"]
+    assert np.array_equal(_interior(reqs[0].case, alone["q"]), _interior(reqs[0].case, m["q"]))
+    assert all(v["state"] == "converged" for v in mixed.values())
+
+
+def test_failed_solve_is_isolated():
+    """A request whose state loses positivity (Euler NACA at 7.7 deg on the
+    finer grid: the impulsive start drives p below qmin at the leading
+    edge) is retired as failed; the requests beside it converge with the
+    same bits as alone."""
+    bad = serve.naca_request(1.0, 0.417, 7.68)
+    reqs = [serve.channel_request(0.5, 0.45), bad, serve.naca_request(0.5, 0.5, 6.0)]
+    alone = {k: _run(reqs, [k], tol=0.3)[k] for k in (0, 2)}
+    assert _run(reqs, [1], tol=0.3)[1]["state"] == "failed"
+    mixed = _run(reqs, [0, 1, 2], tol=0.3)
+    assert mixed[1]["state"] == "failed"
+    for k in (0, 2):
+        assert mixed[k]["state"] == alone[k]["state"] == "converged"
+        assert mixed[k]["iters"] == alone[k]["iters"]
+        assert np.array_equal(_interior(reqs[k].case, alone[k]["q"]), _interior(reqs[k].case, mixed[k]["q"]))
+
+
+def test_short_mixed_sweep_reports_latency():
+    reqs = serve.poisson_requests(6, rate=20.0, seed=1, scales=(0.5, 1.0), naca_fraction=0.5, alpha_range=(-4.0, 4.0))
+    assert {r.grid for r in reqs} == {"channel", "naca"}
+    res = serve.run_sweep(reqs, budget_bytes=8e9, tol=0.3, max_iter=20000, iters_per_step=25)
+    s = res.summary()
+    assert s["requests"] == 6 and s["converged"] == 6, res.states
+    assert 0 < s["p50_latency_s"] <= s["p99_latency_s"]
