@@ -614,12 +614,13 @@ def naca_params(model: str = "kom", mach: float = 0.3, alpha_deg: float = 4.0, r
 
 def naca0012_ogrid(blocks=(96, 160, 160, 96), nj: int = 128, nk: int = 2, rfar: float = 50.0,
                    h1: float = 4.5e-6, span: float = 0.1, params: CosaParams = None,
-                   wall: int = VISCOUS_WALL, kface_bc: int = 80) -> Case:
+                   wall: int = VISCOUS_WALL, kface_bc: int = 80, far: int = FAR_FIELD) -> Case:
     """NACA 0012 O-grid split along i into len(blocks) blocks of the given
     cell counts (default 96/160/160/96, 512 x nj x nk cells), 1-to-1 cuts
     between consecutive blocks and across the trailing-edge seam (last block
     imax to first block imin).  BCs: wall (default 1500, the force surface)
-    on jmin, far field (30) on jmax, kface_bc on the k faces.  h1 = 4.5e-6
+    on jmin, far field `far` (30, or 31 for bc_far1) on jmax, kface_bc on
+    the k faces.  h1 = 4.5e-6
     chords is the first spacing of y+ ~ 1 at Re = 6e6 (flat-plate skin
     friction)."""
     ni = int(sum(blocks))
@@ -631,7 +632,7 @@ def naca0012_ogrid(blocks=(96, 160, 160, 96), nj: int = 128, nk: int = 2, rfar: 
         nodes.append(tuple(A[i0:i1 + 1].copy() for A in (X, Y, Z)))
         dims = (i1 - i0 + 1, nj + 1, nk + 1)
         specs.append(BlockSpec(*dims, _face_bcs(*dims, {
-            "jmin": wall, "jmax": FAR_FIELD, "kmin": kface_bc, "kmax": kface_bc})))
+            "jmin": wall, "jmax": far, "kmin": kface_bc, "kmax": kface_bc})))
     cuts = []
     nb = len(blocks)
     for b in range(nb):

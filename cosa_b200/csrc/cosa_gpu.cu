@@ -202,7 +202,8 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
       if (idir < 1 || idir > 3) return COSA_ERR_ARG;
       // viscous walls: the laminar, fixed-grid branch of bc_walvis_15
       const bool wall15 = type / 100 == 15 && !c->p.moving;
-      const bool ok = type == 80 || type == 4 || type == 14 || type == 21 || type == 91 || type == 30 || wall15;
+      const bool ok = type == 80 || type == 4 || type == 14 || type == 21 || type == 91 || type == 30 || type == 31 ||
+                      wall15;
       if (!ok) return COSA_ERR_UNSUPPORTED;
       int istrt[4] = {0, r[3], r[5], r[7]}, iend[4] = {0, r[4], r[6], r[8]};
       const int ic2 = cyc3(idir, 2), ic3 = cyc3(idir, 3);
@@ -211,7 +212,7 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
       else { ibcpt = ijk[idir]; ibcpt2 = ibcpt + 1; ibcn = ibcpt - 1; ibcn2 = ibcpt - 2; ibcm = ibcpt; }
       int sgn = 1;
       if (type == 21) sgn = inrout == 1 ? 1 : -1;       // bc_insub sgnm
-      else if (type == 30) sgn = inrout == 1 ? -1 : 1;  // bc_far0 sgnm
+      else if (type == 30 || type == 31) sgn = inrout == 1 ? -1 : 1;  // bc_far0 / bc_far1 sgnm
       for (int i3 = istrt[ic3]; i3 <= iend[ic3]; ++i3)
         for (int i2 = istrt[ic2]; i2 <= iend[ic2]; ++i2) {
           HaloItem it{};
@@ -532,7 +533,7 @@ int check_thin_blocks(const cosa_ctx *c, int nl) {
       if (nl < c->p.nl_crs) return COSA_ERR_UNSUPPORTED;
       for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
         const int *r = L.bct.data() + L.obct[b] + 10 * ibc;
-        if (r[1] == d && r[0] != 80 && r[0] != 4 && r[0] != 30) return COSA_ERR_UNSUPPORTED;
+        if (r[1] == d && r[0] != 80 && r[0] != 4 && r[0] != 30 && r[0] != 31) return COSA_ERR_UNSUPPORTED;
       }
     }
   }

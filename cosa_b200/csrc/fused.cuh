@@ -88,7 +88,7 @@ __global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__re
       mask = 3;
     } else {
       double nx = 0, ny = 0, nz = 0;
-      if (it.type == 14 || it.type == 21 || it.type == 30 || (it.type / 100 == 15 && npde > 5)) {
+      if (it.type == 14 || it.type == 21 || it.type == 30 || it.type == 31 || (it.type / 100 == 15 && npde > 5)) {
         const double *s = it.idir == 1 ? si : (it.idir == 2 ? sj : sk);
         const int nh = n * P.hbmove;
         const int64_t I2 = db.im + 2, J2 = db.jm + 2, K2 = db.km + 2;
@@ -104,6 +104,7 @@ __global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__re
         case 21: mask = bc_insub(B, nx, ny, nz, c1, c2, h1, h2, &err); break;
         case 91: mask = bc_outsub(B, c1, c2, h1, h2); break;
         case 30: mask = bc_far0(B, nx, ny, nz, c1, h1, h2); break;
+        case 31: mask = bc_far1(B, nx, ny, nz, c1, h1, h2); break;
         default:
           if (it.type / 100 == 15) {
             mask = bc_walvis(P.gamma, c1, c2, h1, h2);

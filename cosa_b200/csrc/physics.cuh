@@ -671,6 +671,50 @@ __device__ __forceinline__ int bc_far0(const BcPar &B, double sx, double sy, dou
 // bc_walvis_15, laminar part on a fixed grid (src/bc.f90:2144-2300): no-slip
 // wall; wall pressure extrapolated linearly from the first two cells, wall
 // density from cell 1 along the isentrope; both halo layers take the wall state
+// bc_far1 (src/bc.f90:486-870), aircraft free stream, no low-speed
+// preconditioning: boundary normal velocity and pressure from the mean of
+// the interior and free-stream states plus the acoustic jump, density from
+// the isentrope of the upwind side; s = face normal times sgnm
+__device__ __forceinline__ int bc_far1(const BcPar &B, double sx, double sy, double sz, const double *c1,
+                                       double *h1, double *h2) {
+  const double g = B.g;
+  const double qext = c1[1] * sx + c1[2] * sy + c1[3] * sz;
+  const double qinf = B.qfst[1] * sx + B.qfst[2] * sy + B.qfst[3] * sz;
+  const double pext = c1[4], pinf = B.qfst[4], rhoext = c1[0];
+  const double a = sqrt(g * pext / rhoext);
+  const double unb = (qext + qinf) / 2 + (pext - pinf) / (2 * rhoext * a);
+  const double pb = (pext + pinf) / 2 + rhoext * a * (qext - qinf) / 2;
+  const double mach = unb / a;
+  int mask = 0;
+  if (unb <= 0.0) {
+    if (fabs(mach) >= 1.0) {
+      for (int v = 0; v < 5; ++v) h1[v] = B.qfst[v];
+    } else {
+      h1[0] = B.qfst[0] * pow(pb / pinf, 1 / g);
+      h1[1] = B.qfst[1] + (unb - qinf) * sx;
+      h1[2] = B.qfst[2] + (unb - qinf) * sy;
+      h1[3] = B.qfst[3] + (unb - qinf) * sz;
+      h1[4] = pb;
+    }
+    mask = 3;
+    if (B.npde > 5) { h1[5] = B.tkefar; h1[6] = B.omefar; }
+  } else if (unb > 0.0) {
+    if (fabs(mach) >= 1.0) {
+      for (int v = 0; v < 5; ++v) h1[v] = c1[v];
+    } else {
+      h1[0] = c1[0] * pow(pb / pext, 1 / g);
+      h1[1] = c1[1] + (unb - qext) * sx;
+      h1[2] = c1[2] + (unb - qext) * sy;
+      h1[3] = c1[3] + (unb - qext) * sz;
+      h1[4] = pb;
+    }
+    mask = 3;
+    if (B.npde > 5) { h1[5] = c1[5]; h1[6] = c1[6]; }
+  }
+  for (int v = 0; v < B.npde; ++v) h2[v] = h1[v];
+  return mask;
+}
+
 __device__ __forceinline__ int bc_walvis(double g, const double *c1, const double *c2, double *h1, double *h2) {
   const double p1 = c1[4], p2 = c2[4];
   const double pw = 0.5 * (3 * p1 - p2);

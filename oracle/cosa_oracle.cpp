@@ -520,6 +520,82 @@ void bc_far0(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
   }
 }
 
+// bc_far1 (src/bc.f90:486-870), fixed grid, aircraft free stream, without
+// low-speed preconditioning: the boundary normal velocity and pressure from
+// the average of the interior and free-stream states plus the acoustic
+// jump, the density from the isentrope of the upwind side
+void bc_far1(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
+             const Level &L, const cosa_params &P) {
+  int ibcpt, ibcpt2, ibcn, ibcm;
+  double sgnm;
+  if (pa.inrout == 1) { ibcpt = 0; ibcpt2 = -1; ibcn = 1; ibcm = 1; sgnm = -1.0; }
+  else { ibcpt = pa.ijk[pa.idir]; ibcpt2 = ibcpt + 1; ibcn = ibcpt - 1; ibcm = ibcpt; sgnm = 1.0; }
+  const double g = P.gamma;
+  double qfst[6];
+  qfst[1] = P.rhoinf;
+  qfst[2] = P.machfs * std::cos(P.alpha) * std::cos(P.beta);
+  qfst[3] = P.machfs * std::sin(P.alpha) * std::cos(P.beta);
+  qfst[4] = P.machfs * std::sin(P.beta);
+  qfst[5] = P.pinf;
+  for (int n = 0; n < L.S; ++n) {
+    const int nh = n * P.hbmove;
+    for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+      for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+        int a, bb, c, a2, b2, c2, an, bn, cn, am, bm, cm;
+        pidx(pa, ibcpt, i2, i3, a, bb, c); pidx(pa, ibcpt2, i2, i3, a2, b2, c2);
+        pidx(pa, ibcn, i2, i3, an, bn, cn); pidx(pa, ibcm, i2, i3, am, bm, cm);
+        double sx, sy, sz;
+        face_normal(pa, si, sj, sk, am, bm, cm, nh, sx, sy, sz);
+        sx = sx * sgnm; sy = sy * sgnm; sz = sz * sgnm;
+        const double qext = q(an, bn, cn, 2, n) * sx + q(an, bn, cn, 3, n) * sy + q(an, bn, cn, 4, n) * sz;
+        const double qinf = qfst[2] * sx + qfst[3] * sy + qfst[4] * sz;
+        const double pext = q(an, bn, cn, 5, n), pinf = qfst[5];
+        const double rhoext = q(an, bn, cn, 1, n);
+        const double a_ = std::sqrt(g * pext / rhoext);
+        const double unb = (qext + qinf) / 2 + (pext - pinf) / (2 * rhoext * a_);
+        const double pb = (pext + pinf) / 2 + rhoext * a_ * (qext - qinf) / 2;
+        const double mach = unb / a_;
+        double out[6];
+        bool set = true;
+        if (unb <= 0.0) {
+          if (std::fabs(mach) >= 1.0) {
+            for (int v = 1; v <= 5; ++v) out[v] = qfst[v];
+          } else {
+            out[1] = qfst[1] * std::pow(pb / pinf, 1 / g);
+            out[2] = qfst[2] + (unb - qinf) * sx;
+            out[3] = qfst[3] + (unb - qinf) * sy;
+            out[4] = qfst[4] + (unb - qinf) * sz;
+            out[5] = pb;
+          }
+        } else if (unb > 0.0) {
+          if (std::fabs(mach) >= 1.0) {
+            for (int v = 1; v <= 5; ++v) out[v] = q(an, bn, cn, v, n);
+          } else {
+            out[1] = q(an, bn, cn, 1, n) * std::pow(pb / pext, 1 / g);
+            out[2] = q(an, bn, cn, 2, n) + (unb - qext) * sx;
+            out[3] = q(an, bn, cn, 3, n) + (unb - qext) * sy;
+            out[4] = q(an, bn, cn, 4, n) + (unb - qext) * sz;
+            out[5] = pb;
+          }
+        } else {
+          set = false;  // NaN unb: the reference leaves the halo untouched
+        }
+        if (set)
+          for (int v = 1; v <= 5; ++v) { q(a, bb, c, v, n) = out[v]; q(a2, b2, c2, v, n) = out[v]; }
+        if (is_kom(P)) {
+          // second pass of the reference, same unb (src/bc.f90:800-860)
+          if (unb <= 0.0) {
+            q(a, bb, c, 6, n) = P.tkefar; q(a, bb, c, 7, n) = P.omefar;
+            q(a2, b2, c2, 6, n) = q(a, bb, c, 6, n); q(a2, b2, c2, 7, n) = q(a, bb, c, 7, n);
+          } else if (unb > 0.0) {
+            q(a, bb, c, 6, n) = q(an, bn, cn, 6, n); q(a, bb, c, 7, n) = q(an, bn, cn, 7, n);
+            q(a2, b2, c2, 6, n) = q(a, bb, c, 6, n); q(a2, b2, c2, 7, n) = q(a, bb, c, 7, n);
+          }
+        }
+      }
+  }
+}
+
 void bc_walvis_15(const Patch &pa, B3 &q, const Level &L, const cosa_params &P);
 void bc_walvis_15_kom(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk, const double *dista,
                       const Level &L, int b, const cosa_params &P);
@@ -540,6 +616,7 @@ int bc_level(const Level &L, double *qa, const double *si, const double *sj, con
         case 80: bc_sym(pa, q, L); break;
         case 4: bc_extrapol(pa, q, L); break;
         case 30: bc_far0(pa, q, vi, vj, vk, L, P); break;
+        case 31: bc_far1(pa, q, vi, vj, vk, L, P); break;
         case 14: bc_walinv_14(pa, q, vi, vj, vk, L, P); break;
         case 21: status |= bc_insub(pa, q, vi, vj, vk, L, P); break;
         case 91: bc_outsub(pa, q, L, P); break;
@@ -547,7 +624,7 @@ int bc_level(const Level &L, double *qa, const double *si, const double *sj, con
           if (pa.bctyp / 100 == 15 && !P.moving && (!is_kom(P) || dist)) {
             bc_walvis_15(pa, q, L, P);
             if (is_kom(P)) bc_walvis_15_kom(pa, q, vi, vj, vk, dist, L, b, P);
-          } else if (pa.bctyp / 100 == 15 || pa.bctyp == 31) {
+          } else if (pa.bctyp / 100 == 15) {
             status |= COSA_ERR_UNSUPPORTED;
           }
           break;

@@ -259,3 +259,21 @@ def test_src_hb_vanishes_on_identical_snapshots(oracle_mod):
     res = O.p3()
     oracle_mod.src_hb(O, q, vol, res)
     assert np.abs(res).max() < 1e-14
+
+
+def test_far_field_bc_far1_keeps_the_free_stream(oracle_mod):
+    """bc_far1 (type 31) with the free stream inside writes the free stream
+    into both halo layers (unb = q_inf . n, pb = p_inf, rho from the
+    isentrope through p_inf), at inflow and outflow faces alike."""
+    p = cases.naca_params("euler", mach=0.5, alpha_deg=3.0, eps_irs=0.0)
+    case = cases.naca0012_ogrid(blocks=(8, 12, 12, 8), nj=8, nk=2, rfar=10.0, h1=5e-3, params=p, wall=14, far=31)
+    O = oracle_mod.OracleLevel(case.tables, p)
+    si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
+    q = case.q0.copy()
+    O.cons2prim(q)
+    assert O.bc(q, si, sj, sk) == 0
+    fs = np.array([p.rhoinf, p.machfs * np.cos(p.alpha), p.machfs * np.sin(p.alpha), 0.0, p.pinf])
+    for v in p3_views(case.tables, q, 5, 1):
+        jm = v.shape[1] - 3
+        h = v[2:-2, jm + 1:jm + 3, 2:-2, :, 0]   # far-field halo layers j = jmax, jmax+1
+        np.testing.assert_allclose(h, np.broadcast_to(fs, h.shape), rtol=1e-13, atol=1e-15)
