@@ -18,6 +18,16 @@ struct DevBlock {
   int I3, J3;              // im+3, jm+3
   int64_t P3;              // (im+3)(jm+3)(km+3)
   int64_t op3, op2, op1, of0;  // setoffs offsets in cells
+  int obct, nbcs;          // the block's rows of the level's BC table (offset in ints, count)
+  // a per-block kernel launched for this block alone
+  __host__ __device__ DevBlock get() const { return *this; }
+};
+
+// a per-block kernel launched once for all blocks of a level: block
+// blockIdx.y of the level's device table (grid-stride loops use x only)
+struct BlockList {
+  const DevBlock *p;
+  __device__ DevBlock get() const { return p[blockIdx.y]; }
 };
 
 // element (i,j,k) [Fortran indices] of the cell plane of a P3 block

@@ -168,6 +168,7 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
     x.P3 = (int64_t)(x.im + 3) * (x.jm + 3) * (x.km + 3);
     x.op3 = a3; x.op2 = a2; x.op1 = a1; x.of0 = a0;
     if (offs) { x.op3 = offs[3 * b]; x.op2 = offs[3 * b + 1]; x.op1 = offs[3 * b + 2]; }
+    x.obct = (int)ab; x.nbcs = d.nbcs[b];
     L.hb.push_back(x);
     L.nbcs.push_back(d.nbcs[b]);
     L.obct.push_back(ab);
@@ -465,18 +466,33 @@ int after_launch(cosa_ctx *c) {
   return cuda_ok(cudaGetLastError());
 }
 
-// launch one per-block kernel for every block of the level
-template <typename F>
-int for_blocks(cosa_ctx *c, LevelState &L, int64_t (*count)(const DevBlock &, const cosa_params &), F launch) {
-  for (int b = 0; b < L.nb; ++b) {
-    const int64_t n = count(L.hb[b], c->p);
-    launch(b, L.hb[b], grid_for(n));
-    int r = after_launch(c);
-    if (r) return r;
-  }
-  return COSA_OK;
+// CTAs along x for a multi-block launch over nb blocks of at most n items
+int grid_x(int64_t n, int nb) {
+  const int64_t g = (n + 255) / 256;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, std::max(148 * 16 / std::max(nb, 1), 148)));
 }
 
+// launch a per-block kernel once for all blocks of the level (grid y =
+// block, x sized for the largest block); launch(BlockList, dim3 grid)
+template <typename F>
+int for_blocks(cosa_ctx *c, LevelState &L, int64_t (*count)(const DevBlock &, const cosa_params &), F launch) {
+  int64_t m = 1;
+  for (const DevBlock &b : L.hb) m = std::max<int64_t>(m, count(b, c->p));
+  launch(BlockList{L.d_blocks}, dim3(grid_x(m, L.nb), L.nb));
+  return after_launch(c);
+}
+
+// per snapshot: one item per node-indexed face (i,j,k <= imax,jmax,kmax) or per interior cell
+int64_t cnt_faces(const DevBlock &b, const cosa_params &p) {
+  return (int64_t)b.im * b.jm * b.km * (2 * p.nharms + 1);
+}
+int64_t cnt_cells(const DevBlock &b, const cosa_params &p) {
+  return (int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * (2 * p.nharms + 1);
+}
+// halo edge cells of q_bedges, all variables
+int64_t cnt_edges(const DevBlock &b, const cosa_params &p) {
+  return 4 * ((int64_t)(b.im - 1) + (b.jm - 1) + (b.km - 1)) * (2 * p.nharms + 1) * p.npde;
+}
 int64_t cnt_interior(const DevBlock &b, const cosa_params &p) {
   return (int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * (2 * p.nharms + 1) * p.npde;
 }
@@ -566,33 +582,57 @@ constexpr int kPcrMinLen = 16;
 // the three line sweeps of cirs_b / ccirs_b on `res` for variables vs..ve
 int irs_sweeps(cosa_ctx *c, LevelState &L, double *res, const double *ores, const double *const beta[3], double eps,
                int vs, int ve, int with_halo) {
-  const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
-  for (int b = 0; b < L.nb; ++b) {
-    const DevBlock &x = L.hb[b];
-    for (int d = 1; d <= 3; ++d) {
-      const int64_t nl = d == 1 ? (int64_t)(x.jm - 1) * (x.km - 1) : (d == 2 ? (int64_t)(x.im - 1) * (x.km - 1)
-                                                                            : (int64_t)(x.im - 1) * (x.jm - 1));
-      const double *bt = beta ? beta[d - 1] : nullptr;
-      const int len = d == 1 ? x.im - 1 : (d == 2 ? x.jm - 1 : x.km - 1);
+  // blocks are independent here (each sweep writes its own block's interior,
+  // halos were filled before), so a direction can run for all blocks at once
+  const int S = 2 * c->p.nharms + 1, npde = c->p.npde, nv = ve - vs + 1;
+  for (int d = 1; d <= 3; ++d) {
+    const double *bt = beta ? beta[d - 1] : nullptr;
+    const double *src = d == 1 ? ores : nullptr;
+    auto len_of = [&](const DevBlock &x) { return d == 1 ? x.im - 1 : (d == 2 ? x.jm - 1 : x.km - 1); };
+    auto lines_of = [&](const DevBlock &x) {
+      return d == 1 ? (int64_t)(x.jm - 1) * (x.km - 1)
+                    : (d == 2 ? (int64_t)(x.im - 1) * (x.km - 1) : (int64_t)(x.im - 1) * (x.jm - 1));
+    };
+    bool all_pcr = true;
+    int nmax = 1;
+    int64_t wmax = 1;
+    for (const DevBlock &x : L.hb) {
+      const int len = len_of(x);
+      all_pcr &= len >= kPcrMinLen && len <= kPcrMaxLen;
+      nmax = std::max(nmax, len);
+      wmax = std::max<int64_t>(wmax, lines_of(x) * S * nv);
+    }
+    if (all_pcr) {
+      // parallel cyclic reduction, one warp per line and variable, all blocks
+      const int wpc = std::max(1, std::min(4, kPcrSmemBytes / (64 * nmax)));
+      const dim3 g((unsigned)grid_x(wmax * 32, L.nb) * 256 / (32 * wpc) + 1, L.nb);
+      const size_t sm = (size_t)wpc * 8 * nmax * sizeof(double);
+      const BlockList bl{L.d_blocks};
+      if (d == 1) k_irs_pcr<1><<<g, 32 * wpc, sm, c->s>>>(bl, npde, S, res, src, bt, eps, vs, ve, with_halo, nmax);
+      else if (d == 2) k_irs_pcr<2><<<g, 32 * wpc, sm, c->s>>>(bl, npde, S, res, src, bt, eps, vs, ve, with_halo, nmax);
+      else k_irs_pcr<3><<<g, 32 * wpc, sm, c->s>>>(bl, npde, S, res, src, bt, eps, vs, ve, with_halo, nmax);
+      const int r = after_launch(c);
+      if (r) return r;
+      continue;
+    }
+    for (const DevBlock &x : L.hb) {
+      const int len = len_of(x);
+      const int64_t nl = lines_of(x);
       if (len >= kPcrMinLen && len <= kPcrMaxLen) {
-        // parallel cyclic reduction, one warp per line and variable
-        const int nmax = std::max(len, 1);
-        const int wpc = std::max(1, std::min(4, kPcrSmemBytes / (64 * nmax)));
-        const int g = grid_for(nl * S * (ve - vs + 1) * 32, 32 * wpc);  // one warp per line and variable
-        const size_t sm = (size_t)wpc * 8 * nmax * sizeof(double);
-        const double *src = d == 1 ? ores : nullptr;
-        if (d == 1) k_irs_pcr<1><<<g, 32 * wpc, sm, c->s>>>(x, npde, S, res, src, bt, eps, vs, ve, with_halo, nmax);
-        else if (d == 2) k_irs_pcr<2><<<g, 32 * wpc, sm, c->s>>>(x, npde, S, res, src, bt, eps, vs, ve, with_halo, nmax);
-        else k_irs_pcr<3><<<g, 32 * wpc, sm, c->s>>>(x, npde, S, res, src, bt, eps, vs, ve, with_halo, nmax);
-        int r = after_launch(c);
-        if (r) return r;
-        continue;
+        const int nm = std::max(len, 1);
+        const int wpc = std::max(1, std::min(4, kPcrSmemBytes / (64 * nm)));
+        const int g = grid_for(nl * S * nv * 32, 32 * wpc);  // one warp per line and variable
+        const size_t sm = (size_t)wpc * 8 * nm * sizeof(double);
+        if (d == 1) k_irs_pcr<1><<<g, 32 * wpc, sm, c->s>>>(x, npde, S, res, src, bt, eps, vs, ve, with_halo, nm);
+        else if (d == 2) k_irs_pcr<2><<<g, 32 * wpc, sm, c->s>>>(x, npde, S, res, src, bt, eps, vs, ve, with_halo, nm);
+        else k_irs_pcr<3><<<g, 32 * wpc, sm, c->s>>>(x, npde, S, res, src, bt, eps, vs, ve, with_halo, nm);
+      } else {
+        const int g = grid_for(nl * S, 128);
+        if (d == 1) k_irs_line<1><<<g, 128, 0, c->s>>>(x, npde, S, res, src, bt, eps, vs, ve, with_halo, L.d_irs_scr);
+        else if (d == 2) k_irs_line<2><<<g, 128, 0, c->s>>>(x, npde, S, res, src, bt, eps, vs, ve, with_halo, L.d_irs_scr);
+        else k_irs_line<3><<<g, 128, 0, c->s>>>(x, npde, S, res, src, bt, eps, vs, ve, with_halo, L.d_irs_scr);
       }
-      const int g = grid_for(nl * S, 128);
-      if (d == 1) k_irs_line<1><<<g, 128, 0, c->s>>>(x, npde, S, res, ores, bt, eps, vs, ve, with_halo, L.d_irs_scr);
-      else if (d == 2) k_irs_line<2><<<g, 128, 0, c->s>>>(x, npde, S, res, nullptr, bt, eps, vs, ve, with_halo, L.d_irs_scr);
-      else k_irs_line<3><<<g, 128, 0, c->s>>>(x, npde, S, res, nullptr, bt, eps, vs, ve, with_halo, L.d_irs_scr);
-      int r = after_launch(c);
+      const int r = after_launch(c);
       if (r) return r;
     }
   }
@@ -601,14 +641,9 @@ int irs_sweeps(cosa_ctx *c, LevelState &L, double *res, const double *ores, cons
 
 int irs_scale(cosa_ctx *c, LevelState &L, double *res, const double *dtv, const double *dtvt, int forward) {
   const int S = 2 * c->p.nharms + 1;
-  for (int b = 0; b < L.nb; ++b) {
-    const DevBlock &x = L.hb[b];
-    k_irs_scale<<<grid_for((int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * S), 256, 0, c->s>>>(x, c->p.npde, S, res, dtv,
-                                                                                               dtvt, forward);
-    int r = after_launch(c);
-    if (r) return r;
-  }
-  return COSA_OK;
+  return for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+    k_irs_scale<<<g, 256, 0, c->s>>>(b, c->p.npde, S, res, dtv, dtvt, forward);
+  });
 }
 
 // cirs (cutcirs = 0) or scalef + 2 x (cutman_q + ccirs) + scaleb (cutcirs = 1)
@@ -660,11 +695,6 @@ void prof_stop(cosa_ctx *c, int k) {
 int launch_edges(cosa_ctx *c, LevelState &L, double *q, double *mut);
 
 // x extent of a (x, nblocks[, 3]) grid covering `n` items per block
-int grid_x(int64_t n, int nb) {
-  const int64_t g = (n + 255) / 256;
-  return (int)std::max<int64_t>(1, std::min<int64_t>(g, std::max(148 * 16 / std::max(nb, 1), 148)));
-}
-
 // viscous part of one stage on the halo-filled state qin: primitive copy,
 // q_edges, [time step], face fluxes, wall faces, flux balance -> L.d_vres
 int launch_visc(cosa_ctx *c, LevelState &L, const double *qin, bool dt, double *bx, double *by, double *bz,
@@ -1105,7 +1135,7 @@ int cosa_gpu_bind_level(cosa_ctx *c, int32_t nl, const cosa_level_ptrs *ptrs) {
 int cosa_gpu_cons2prim(cosa_ctx *c, int32_t nl, int32_t xtnd, double *q) {
   LevelState *L = level(c, nl);
   if (!L || !q || xtnd < 0 || xtnd > 1) return COSA_ERR_ARG;
-  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+  return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) {
     k_cons2prim<<<g, 256, 0, c->s>>>(b, c->d_p, q, xtnd);
   });
 }
@@ -1113,7 +1143,7 @@ int cosa_gpu_cons2prim(cosa_ctx *c, int32_t nl, int32_t xtnd, double *q) {
 int cosa_gpu_prim2cons(cosa_ctx *c, int32_t nl, double *q) {
   LevelState *L = level(c, nl);
   if (!L || !q) return COSA_ERR_ARG;
-  return for_blocks(c, *L, cnt_all, [&](int, const DevBlock &b, int g) {
+  return for_blocks(c, *L, cnt_all, [&](auto b, dim3 g) {
     k_prim2cons<<<g, 256, 0, c->s>>>(b, c->d_p, q);
   });
 }
@@ -1143,7 +1173,7 @@ int cosa_gpu_cutman_q(cosa_ctx *c, int32_t nl, double *q) {
 int cosa_gpu_prtest(cosa_ctx *c, int32_t nl, const double *q) {
   LevelState *L = level(c, nl);
   if (!L || !q) return COSA_ERR_ARG;
-  int r = for_blocks(c, *L, cnt_all, [&](int, const DevBlock &b, int g) {
+  int r = for_blocks(c, *L, cnt_all, [&](auto b, dim3 g) {
     k_prtest<<<g, 256, 0, c->s>>>(b, c->d_p, q, c->d_status);
   });
   if (r) return r;
@@ -1155,7 +1185,7 @@ int cosa_gpu_lambda(cosa_ctx *c, int32_t nl, const double *q, const double *si, 
   LevelState *L = level(c, nl);
   if (!L || !q || !lam) return COSA_ERR_ARG;
   if (c->p.viscous || c->p.moving) return COSA_ERR_UNSUPPORTED;
-  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+  return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) {
     k_lambda<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, lam);
   });
 }
@@ -1164,7 +1194,7 @@ int cosa_gpu_deltat(cosa_ctx *c, int32_t nl, double *dtvol, const double *lam, d
   LevelState *L = level(c, nl);
   if (!L || !dtvol || !lam) return COSA_ERR_ARG;
   if (c->p.viscous || c->p.kom || c->p.irsop == 5 || c->p.irsop == 6) return COSA_ERR_UNSUPPORTED;
-  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+  return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) {
     k_deltat<<<g, 256, 0, c->s>>>(b, c->d_p, dtvol, lam, bx, by, bz);
   });
 }
@@ -1203,20 +1233,16 @@ int muscl_impl(cosa_ctx *c, int32_t idir, int32_t nl, const double *q, double *q
   int so_beg = 1, so_end = p.npde;
   if (nl >= p.nl_crs) { so_beg = 0; so_end = -1; }
   else if (p.foturb) { so_beg = 1; so_end = 5; }
-  for (int b = 0; b < L->nb; ++b) {
-    const DevBlock &x = L->hb[b];
-    const int *bct = L->d_bct + L->obct[b];
-    if (so_end >= so_beg) {
-      k_muscl_dq<<<grid_for(cnt_all(x, p)), 256, 0, c->s>>>(x, c->d_p, idir, q, dq, bct, L->nbcs[b], so_beg, so_end);
-      int r = after_launch(c);
-      if (r) return r;
-    }
-    k_muscl_face<<<grid_for(cnt_all(x, p)), 256, 0, c->s>>>(x, c->d_p, idir, nl, q, qp, qm, dq, dqp, dqm, bct,
-                                                             L->nbcs[b], mixed);
-    int r = after_launch(c);
+  const int *bct = L->d_bct;
+  if (so_end >= so_beg) {
+    const int r = for_blocks(c, *L, cnt_all, [&](auto b, dim3 g) {
+      k_muscl_dq<<<g, 256, 0, c->s>>>(b, c->d_p, idir, q, dq, bct, so_beg, so_end);
+    });
     if (r) return r;
   }
-  return COSA_OK;
+  return for_blocks(c, *L, cnt_all, [&](auto b, dim3 g) {
+    k_muscl_face<<<g, 256, 0, c->s>>>(b, c->d_p, idir, nl, q, qp, qm, dq, dqp, dqm, bct, mixed);
+  });
 }
 
 int roflux_impl(cosa_ctx *c, int32_t idir, int32_t nl, const double *qr, const double *ql, double *flux,
@@ -1224,7 +1250,7 @@ int roflux_impl(cosa_ctx *c, int32_t idir, int32_t nl, const double *qr, const d
   LevelState *L = level(c, nl);
   if (!L || idir < 1 || idir > 3 || !qr || !ql || !flux || !sijk) return COSA_ERR_ARG;
   if (c->p.moving) return COSA_ERR_UNSUPPORTED;
-  return for_blocks(c, *L, cnt_all, [&](int, const DevBlock &b, int g) {
+  return for_blocks(c, *L, cnt_all, [&](auto b, dim3 g) {
     k_roflux<<<g, 256, 0, c->s>>>(b, c->d_p, idir, qr, ql, flux, sijk, mixed);
   });
 }
@@ -1235,7 +1261,7 @@ extern "C" {
 int cosa_gpu_resid(cosa_ctx *c, int32_t idir, int32_t nl, const double *flux, double *res) {
   LevelState *L = level(c, nl);
   if (!L || idir < 1 || idir > 3 || !flux || !res) return COSA_ERR_ARG;
-  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+  return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) {
     k_resid<<<g, 256, 0, c->s>>>(b, c->d_p, idir, flux, res);
   });
 }
@@ -1245,7 +1271,7 @@ int cosa_gpu_update(cosa_ctx *c, int32_t nl, const double *res, double *q, const
   LevelState *L = level(c, nl);
   if (!L || !res || !q || !qold || !dtvol) return COSA_ERR_ARG;
   if (c->p.harbal || c->p.rkimp) return COSA_ERR_UNSUPPORTED;
-  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+  return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) {
     k_update<<<g, 256, 0, c->s>>>(b, c->d_p, res, q, qold, dtvol, ar);
   });
 }
@@ -1253,7 +1279,7 @@ int cosa_gpu_update(cosa_ctx *c, int32_t nl, const double *res, double *q, const
 int cosa_gpu_zero(cosa_ctx *c, int32_t nl, double *a) {
   LevelState *L = level(c, nl);
   if (!L || !a) return COSA_ERR_ARG;
-  return for_blocks(c, *L, cnt_all, [&](int, const DevBlock &b, int g) {
+  return for_blocks(c, *L, cnt_all, [&](auto b, dim3 g) {
     k_zero_res<<<g, 256, 0, c->s>>>(b, c->d_p, a);
   });
 }
@@ -1368,7 +1394,7 @@ int cosa_gpu_smooth_host(cosa_ctx *c, int32_t nl, double *q_host, int32_t niter,
 int cosa_gpu_src_hb(cosa_ctx *c, int32_t nl, const double *q, const double *vol, double *res) {
   LevelState *L = level(c, nl);
   if (!L || !q || !vol || !res) return COSA_ERR_ARG;
-  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+  return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) {
     k_src_hb<<<g, 256, 0, c->s>>>(b, c->d_p, q, vol, res);
   });
 }
@@ -1460,18 +1486,9 @@ int level_pair(cosa_ctx *c, int nl, LevelState *&L1, LevelState *&L2) {
 
 int launch_edges(cosa_ctx *c, LevelState &L, double *q, double *mut) {
   const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
-  for (int b = 0; b < L.nb; ++b) {
-    const DevBlock &x = L.hb[b];
-    const int64_t per = 4 * ((int64_t)(x.im - 1) + (x.jm - 1) + (x.km - 1));
-    k_edges<<<grid_for(per * npde * S), 256, 0, c->s>>>(x, npde, S, q, x.op3 * npde * S);
-    int r = after_launch(c);
-    if (r) return r;
-    if (mut) {
-      k_edges<<<grid_for(per * S), 256, 0, c->s>>>(x, 1, S, mut, x.op3 * S);
-      if ((r = after_launch(c))) return r;
-    }
-  }
-  return COSA_OK;
+  int r = for_blocks(c, L, cnt_edges, [&](auto b, dim3 g) { k_edges<<<g, 256, 0, c->s>>>(b, npde, S, q, -1); });
+  if (r || !mut) return r;
+  return for_blocks(c, L, cnt_edges, [&](auto b, dim3 g) { k_edges<<<g, 256, 0, c->s>>>(b, 1, S, mut, -1); });
 }
 
 int launch_corns(cosa_ctx *c, LevelState &L, double *q, double *mut) {
@@ -1683,18 +1700,14 @@ int cosa_gpu_fixq(cosa_ctx *c, int32_t nl, double *q) {
   if (!L || !q) return COSA_ERR_ARG;
   if (c->p.npde < 7) return COSA_OK;  // the reference calls it for k-omega only
   const int S = 2 * c->p.nharms + 1;
-  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int) {
-    k_fixq<<<grid_for((int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * S), 256, 0, c->s>>>(b, c->d_p, q);
-  });
+  return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) { k_fixq<<<g, 256, 0, c->s>>>(b, c->d_p, q); });
 }
 
 int cosa_gpu_tur_vis(cosa_ctx *c, int32_t nl, const double *q, double *mut) {
   LevelState *L = level(c, nl);
   if (!L || !q || !mut || c->p.npde < 7) return COSA_ERR_ARG;
   const int S = 2 * c->p.nharms + 1;
-  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int) {
-    k_tur_vis<<<grid_for((int64_t)(b.im + 1) * (b.jm + 1) * (b.km + 1) * S), 256, 0, c->s>>>(b, c->d_p, q, mut);
-  });
+  return for_blocks(c, *L, cnt_all, [&](auto b, dim3 g) { k_tur_vis<<<g, 256, 0, c->s>>>(b, c->d_p, q, mut); });
 }
 
 int cosa_gpu_rest1(cosa_ctx *c, int32_t nl, const double *q1, double *q2, const double *vol1, const double *vol2) {
@@ -2136,7 +2149,7 @@ int cosa_gpu_lambda_ns(cosa_ctx *c, int32_t nl, const double *q, const double *s
   LevelState *L = level(c, nl);
   if (!L || !q || !si || !sj || !sk || !vol || !lam || !lamv) return COSA_ERR_ARG;
   if (c->p.moving) return COSA_ERR_UNSUPPORTED;
-  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+  return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) {
     k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, vol, c->p.kom ? mut : nullptr, lam, lamv);
   });
 }
@@ -2145,7 +2158,7 @@ int cosa_gpu_deltat_ns(cosa_ctx *c, int32_t nl, double *dtvol, const double *lam
                        double *by, double *bz, double *dtvolt, double *tbx, double *tby, double *tbz) {
   LevelState *L = level(c, nl);
   if (!L || !dtvol || !lam || !lamv) return COSA_ERR_ARG;
-  return for_blocks(c, *L, cnt_interior, [&](int, const DevBlock &b, int g) {
+  return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) {
     k_deltat_ns<<<g, 256, 0, c->s>>>(b, c->d_p, dtvol, lam, lamv, bx, by, bz, c->p.kom ? dtvolt : nullptr,
                                      c->p.kom ? tbx : nullptr, tby, tbz);
   });
@@ -2160,14 +2173,12 @@ int cosa_gpu_q_face_mut(cosa_ctx *c, int32_t idir, int32_t nl, const double *mut
   LevelState *L = level(c, nl);
   if (!L || idir < 1 || idir > 3 || !mut || !flux) return COSA_ERR_ARG;
   const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
-  for (const DevBlock &b : L->hb) {
-    const int g = grid_for((int64_t)b.im * b.jm * b.km * S);
+  int r = for_blocks(c, *L, cnt_faces, [&](auto b, dim3 g) {
     if (idir == 1) k_qface_mut<1><<<g, 256, 0, c->s>>>(b, npde, S, mut, flux);
     else if (idir == 2) k_qface_mut<2><<<g, 256, 0, c->s>>>(b, npde, S, mut, flux);
     else k_qface_mut<3><<<g, 256, 0, c->s>>>(b, npde, S, mut, flux);
-    int r = after_launch(c);
-    if (r) return r;
-  }
+  });
+  if (r) return r;
   if (L->walls.empty()) return COSA_OK;
   const int nw = (int)L->walls.size();
   k_qwall_mut<<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L->d_blocks, L->d_walls, nw, idir, npde, S, mut, flux);
@@ -2179,13 +2190,9 @@ int cosa_gpu_rtst(cosa_ctx *c, int32_t idir, int32_t nl, const double *qf, const
   LevelState *L = level(c, nl);
   if (!L || idir < 1 || idir > 3 || !qf || !dqxi || !dqeta || !dqzeta || !vm || !flux || !tau1) return COSA_ERR_ARG;
   if (c->p.npde != 7) return COSA_ERR_UNSUPPORTED;
-  for (const DevBlock &b : L->hb) {
-    k_rtst<<<grid_for((int64_t)b.im * b.jm * b.km * (2 * c->p.nharms + 1)), 256, 0, c->s>>>(
-        b, idir, c->d_p, qf, dqxi, dqeta, dqzeta, vm, L->n0, flux, tau1);
-    int r = after_launch(c);
-    if (r) return r;
-  }
-  return COSA_OK;
+  return for_blocks(c, *L, cnt_faces, [&](auto b, dim3 g) {
+    k_rtst<<<g, 256, 0, c->s>>>(b, idir, c->d_p, qf, dqxi, dqeta, dqzeta, vm, L->n0, flux, tau1);
+  });
 }
 
 int cosa_gpu_vflux_kom(cosa_ctx *c, int32_t idir, int32_t nl, const double *qf, const double *dqxi,
@@ -2195,41 +2202,29 @@ int cosa_gpu_vflux_kom(cosa_ctx *c, int32_t idir, int32_t nl, const double *qf, 
   if (!L || idir < 1 || idir > 3 || !qf || !dqxi || !dqeta || !dqzeta || !tau1 || !vm || !sijk || !flux)
     return COSA_ERR_ARG;
   if (c->p.npde != 7 || !c->p.kom || c->p.moving) return COSA_ERR_UNSUPPORTED;
-  for (const DevBlock &b : L->hb) {
-    k_vflux_kom<<<grid_for((int64_t)b.im * b.jm * b.km * (2 * c->p.nharms + 1)), 256, 0, c->s>>>(
-        b, idir, c->d_p, qf, dqxi, dqeta, dqzeta, tau1, vm, L->n0, sijk, flux);
-    int r = after_launch(c);
-    if (r) return r;
-  }
-  return COSA_OK;
+  return for_blocks(c, *L, cnt_faces, [&](auto b, dim3 g) {
+    k_vflux_kom<<<g, 256, 0, c->s>>>(b, idir, c->d_p, qf, dqxi, dqeta, dqzeta, tau1, vm, L->n0, sijk, flux);
+  });
 }
 
 int cosa_gpu_q_der_c(cosa_ctx *c, int32_t idir, int32_t nl, const double *qf, double *dqc) {
   LevelState *L = level(c, nl);
   if (!L || idir < 1 || idir > 3 || !qf || !dqc) return COSA_ERR_ARG;
   const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
-  for (const DevBlock &b : L->hb) {
-    const int g = grid_for((int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * S);
+  return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
     if (idir == 1) k_qder_c<1><<<g, 256, 0, c->s>>>(b, npde, S, qf, dqc);
     else if (idir == 2) k_qder_c<2><<<g, 256, 0, c->s>>>(b, npde, S, qf, dqc);
     else k_qder_c<3><<<g, 256, 0, c->s>>>(b, npde, S, qf, dqc);
-    int r = after_launch(c);
-    if (r) return r;
-  }
-  return COSA_OK;
+  });
 }
 
 int cosa_gpu_turprod(cosa_ctx *c, int32_t nl, const double *dqxi, const double *dqeta, const double *dqzeta,
                      const double *vm, double *prd, double *divvel, double *delpls) {
   LevelState *L = level(c, nl);
   if (!L || !dqxi || !dqeta || !dqzeta || !vm || !prd || !divvel || !delpls) return COSA_ERR_ARG;
-  for (const DevBlock &b : L->hb) {
-    k_turprod<<<grid_for((int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * (2 * c->p.nharms + 1)), 256, 0, c->s>>>(
-        b, c->d_p, dqxi, dqeta, dqzeta, vm, L->n0, prd, divvel, delpls);
-    int r = after_launch(c);
-    if (r) return r;
-  }
-  return COSA_OK;
+  return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
+    k_turprod<<<g, 256, 0, c->s>>>(b, c->d_p, dqxi, dqeta, dqzeta, vm, L->n0, prd, divvel, delpls);
+  });
 }
 
 int cosa_gpu_srckw(cosa_ctx *c, int32_t nl, const double *q, const double *mut, const double *prd,
@@ -2237,13 +2232,9 @@ int cosa_gpu_srckw(cosa_ctx *c, int32_t nl, const double *q, const double *mut, 
   LevelState *L = level(c, nl);
   if (!L || !q || !mut || !prd || !divvel || !res || !vol) return COSA_ERR_ARG;
   if (c->p.npde != 7) return COSA_ERR_UNSUPPORTED;
-  for (const DevBlock &b : L->hb) {
-    k_srckw<<<grid_for((int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * (2 * c->p.nharms + 1)), 256, 0, c->s>>>(
-        b, c->d_p, nl, q, mut, prd, divvel, res, vol);
-    int r = after_launch(c);
-    if (r) return r;
-  }
-  return COSA_OK;
+  return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
+    k_srckw<<<g, 256, 0, c->s>>>(b, c->d_p, nl, q, mut, prd, divvel, res, vol);
+  });
 }
 
 int cosa_gpu_update_kom(cosa_ctx *c, int32_t nl, const double *res, double *q, const double *qold, const double *vol,
@@ -2251,13 +2242,9 @@ int cosa_gpu_update_kom(cosa_ctx *c, int32_t nl, const double *res, double *q, c
   LevelState *L = level(c, nl);
   if (!L || !res || !q || !qold || !vol || !dtvolt || !delpls || !prd) return COSA_ERR_ARG;
   if (c->p.npde != 7 || c->p.rkimp) return COSA_ERR_UNSUPPORTED;
-  for (const DevBlock &b : L->hb) {
-    k_update_kom<<<grid_for((int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1) * (2 * c->p.nharms + 1)), 256, 0, c->s>>>(
-        b, c->d_p, res, q, qold, vol, dtvolt, delpls, prd, ar);
-    int r = after_launch(c);
-    if (r) return r;
-  }
-  return COSA_OK;
+  return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
+    k_update_kom<<<g, 256, 0, c->s>>>(b, c->d_p, res, q, qold, vol, dtvolt, delpls, prd, ar);
+  });
 }
 
 int cosa_gpu_force(cosa_ctx *c, int32_t nl, const double *q, const double *x, const double *y, const double *z,
@@ -2380,14 +2367,12 @@ namespace {
 int rans_face_state(cosa_ctx *c, LevelState &L, int d, const double *q, double *qf, double *g0, double *g1,
                     double *g2) {
   const int S = 2 * c->p.nharms + 1;
-  for (const DevBlock &b : L.hb) {
-    const int g = grid_for((int64_t)b.im * b.jm * b.km * S);
+  int r = for_blocks(c, L, cnt_faces, [&](auto b, dim3 g) {
     if (d == 1) k_qface_qder<1, 7><<<g, 256, 0, c->s>>>(b, S, q, qf, g0, g1, g2);
     else if (d == 2) k_qface_qder<2, 7><<<g, 256, 0, c->s>>>(b, S, q, qf, g0, g1, g2);
     else k_qface_qder<3, 7><<<g, 256, 0, c->s>>>(b, S, q, qf, g0, g1, g2);
-    int r = after_launch(c);
-    if (r) return r;
-  }
+  });
+  if (r) return r;
   if (L.walls.empty()) return COSA_OK;
   const int nw = (int)L.walls.size();
   k_qwall<7><<<grid_for((int64_t)nw * S), 256, 0, c->s>>>(L.d_blocks, L.d_walls, nw, d, S, q, qf, g0, g1, g2);
@@ -2404,12 +2389,10 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
   const cosa_level_ptrs &P = L.ptrs;
   double *q = P.q;
   int r = 0;
-  if (irk == 1 && copy_qold)
-    for (const DevBlock &x : L.hb) {
-      k_copy_interior<<<grid_for((int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * npde * S), 256, 0, c->s>>>(
-          x, npde * S, q, P.qold);
-      if ((r = after_launch(c))) return r;
-    }
+  if (irk == 1 && copy_qold &&
+      (r = for_blocks(c, L, cnt_interior,
+                      [&](auto b, dim3 g) { k_copy_interior<<<g, 256, 0, c->s>>>(b, npde * S, q, P.qold); })))
+    return r;
   if ((r = cosa_gpu_cons2prim(c, nl, 0, q))) return r;
   if (!L.items.empty()) {
     // BC patches then cuts, last writers as in the reference
@@ -2422,21 +2405,20 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
     // stage of the first cycle's visit (src/cosa.f90:1727-1760)
     if ((r = cosa_gpu_tur_vis(c, nl, q, P.mut)) || (r = cosa_gpu_cutman_mut(c, nl, P.mut))) return r;
   }
-  for (const DevBlock &b : L.hb) {
-    k_prtest<<<grid_for(cnt_all(b, p)), 256, 0, c->s>>>(b, c->d_p, q, c->d_status);
-    if ((r = after_launch(c))) return r;
-  }
+  if ((r = for_blocks(c, L, cnt_all, [&](auto b, dim3 g) { k_prtest<<<g, 256, 0, c->s>>>(b, c->d_p, q, c->d_status); })))
+    return r;
   if (compute_dt) {
-    for (const DevBlock &b : L.hb) {
-      const int g = grid_for(cnt_interior(b, p));
-      k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.si, P.sj, P.sk, P.vol, P.mut, P.qp, P.dq);
-      if ((r = after_launch(c))) return r;
-      const bool irs = p.irsop >= 2 && p.irsop != 4;
-      k_deltat_ns<<<g, 256, 0, c->s>>>(b, c->d_p, P.dtvol, P.qp, P.dq, irs ? P.betaxi : nullptr, P.betaeta,
-                                       P.betazeta, P.dtvolt, irs ? L.d_tbeta[0] : nullptr, L.d_tbeta[1],
-                                       L.d_tbeta[2]);
-      if ((r = after_launch(c))) return r;
-    }
+    if ((r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+           k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.si, P.sj, P.sk, P.vol, P.mut, P.qp, P.dq);
+         })))
+      return r;
+    const bool irs = p.irsop >= 2 && p.irsop != 4;
+    if ((r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+           k_deltat_ns<<<g, 256, 0, c->s>>>(b, c->d_p, P.dtvol, P.qp, P.dq, irs ? P.betaxi : nullptr, P.betaeta,
+                                            P.betazeta, P.dtvolt, irs ? L.d_tbeta[0] : nullptr, L.d_tbeta[1],
+                                            L.d_tbeta[2]);
+         })))
+      return r;
   }
   if ((r = cosa_gpu_zero(c, nl, P.res))) return r;
   if ((r = launch_edges(c, L, q, P.mut))) return r;
@@ -2477,29 +2459,24 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
   // multigrid forcing: rhs += res at the first stage of a visit from the
   // finer level, then res -= rhs on coarse levels (src/cosa.f90:1950-1960)
   const int nvs = npde * S;
-  if (o.rhs && o.force && irk == 1)
-    for (const DevBlock &b : L.hb) {
-      k_add_interior<<<grid_for(cnt_interior(b, p)), 256, 0, c->s>>>(b, nvs, o.rhs, P.res, 1.0);
-      if ((r = after_launch(c))) return r;
-    }
-  if (o.rhs && nl > 1)
-    for (const DevBlock &b : L.hb) {
-      k_add_interior<<<grid_for(cnt_interior(b, p)), 256, 0, c->s>>>(b, nvs, P.res, o.rhs, -1.0);
-      if ((r = after_launch(c))) return r;
-    }
+  if (o.rhs && o.force && irk == 1 &&
+      (r = for_blocks(c, L, cnt_interior,
+                      [&](auto b, dim3 g) { k_add_interior<<<g, 256, 0, c->s>>>(b, nvs, o.rhs, P.res, 1.0); })))
+    return r;
+  if (o.rhs && nl > 1 &&
+      (r = for_blocks(c, L, cnt_interior,
+                      [&](auto b, dim3 g) { k_add_interior<<<g, 256, 0, c->s>>>(b, nvs, P.res, o.rhs, -1.0); })))
+    return r;
   if (o.res_only) {
     // residual pass before the restriction (src/cosa.f90:1963-1975)
-    if (p.nlevel > 1 && nl != p.nlevel && !p.prd_all_lvls && p.lim_prodtke)
-      for (const DevBlock &b : L.hb) {
-        k_lim_prod_mg<<<grid_for(cnt_interior(b, p)), 256, 0, c->s>>>(b, c->d_p, q, L.d_prd, P.mut);
-        if ((r = after_launch(c))) return r;
-      }
-    for (const DevBlock &b : L.hb) {
-      k_lim_res_ome<<<grid_for(cnt_interior(b, p)), 256, 0, c->s>>>(b, c->d_p, P.res, q, P.vol, P.dtvolt,
-                                                                   L.d_delpls, L.d_prd, p.alphas[irk - 1]);
-      if ((r = after_launch(c))) return r;
-    }
-    return COSA_OK;
+    if (p.nlevel > 1 && nl != p.nlevel && !p.prd_all_lvls && p.lim_prodtke &&
+        (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+           k_lim_prod_mg<<<g, 256, 0, c->s>>>(b, c->d_p, q, L.d_prd, P.mut);
+         })))
+      return r;
+    return for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+      k_lim_res_ome<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, q, P.vol, P.dtvolt, L.d_delpls, L.d_prd, p.alphas[irk - 1]);
+    });
   }
   if (p.irsop > 0) {
     const double *beta[3] = {P.betaxi ? P.betaxi : L.d_beta[0], P.betaeta ? P.betaeta : L.d_beta[1],

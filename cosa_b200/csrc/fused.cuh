@@ -528,7 +528,9 @@ __global__ void k_rms_seg(const double *__restrict__ part, const int *__restrict
 }
 
 // ---- interior copy (odd stage counts end in the second buffer) --------------------------
-__global__ void k_copy_interior(DevBlock b, int nvar_snap, const double *__restrict__ src, double *__restrict__ dst) {
+template <class BS>
+__global__ void k_copy_interior(BS bs_, int nvar_snap, const double *__restrict__ src, double *__restrict__ dst) {
+  const DevBlock b = bs_.get();
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
   const int64_t n = (int64_t)ni * nj * nk * nvar_snap;
   const int64_t base = b.op3 * nvar_snap;

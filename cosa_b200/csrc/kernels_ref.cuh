@@ -30,7 +30,9 @@ __device__ __forceinline__ void irs_beta(int irsop, double rat, double psirs, do
 
 
 // ---- cons2prim_b (src/update.f90:2112-2188) ----------------------------------------
-__global__ void k_cons2prim(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ q, int xtnd) {
+template <class BS>
+__global__ void k_cons2prim(BS bs_, const cosa_params *__restrict__ Pp, double *__restrict__ q, int xtnd) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int ni = b.im - 1 + 2 * xtnd, nj = b.jm - 1 + 2 * xtnd, nk = b.km - 1 + 2 * xtnd;
@@ -50,7 +52,9 @@ __global__ void k_cons2prim(DevBlock b, const cosa_params *__restrict__ Pp, doub
 }
 
 // ---- prim2cons_b (src/update.f90:1875-2084): interior + face halos ------------------
-__global__ void k_prim2cons(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ q) {
+template <class BS>
+__global__ void k_prim2cons(BS bs_, const cosa_params *__restrict__ Pp, double *__restrict__ q) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   // domain: i in -1..im+1, j,k in -1..jm+1/-1..km+1 restricted to the
@@ -74,7 +78,9 @@ __global__ void k_prim2cons(DevBlock b, const cosa_params *__restrict__ Pp, doub
 }
 
 // ---- bprtest (src/cosa.f90:960-1120): status bits instead of stop -----------------
-__global__ void k_prtest(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ q, int *status) {
+template <class BS>
+__global__ void k_prtest(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ q, int *status) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int ni = b.im + 3, nj = b.jm - 1, nk = b.km - 1;
@@ -95,9 +101,11 @@ __global__ void k_prtest(DevBlock b, const cosa_params *__restrict__ Pp, const d
 }
 
 // ---- lambdab inviscid (src/cosa.f90:1248-1330) --------------------------------------
-__global__ void k_lambda(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
+template <class BS>
+__global__ void k_lambda(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
                          const double *__restrict__ si, const double *__restrict__ sj,
                          const double *__restrict__ sk, double *__restrict__ lam) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
@@ -125,8 +133,10 @@ __global__ void k_lambda(DevBlock b, const cosa_params *__restrict__ Pp, const d
 }
 
 // ---- bdeltat (src/cosa.f90:4733-5203): dtvol and IRS beta, inviscid ---------------
-__global__ void k_deltat(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ dtv,
+template <class BS>
+__global__ void k_deltat(BS bs_, const cosa_params *__restrict__ Pp, double *__restrict__ dtv,
                          const double *__restrict__ lam, double *bx, double *by, double *bz) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
@@ -154,8 +164,10 @@ __global__ void k_deltat(DevBlock b, const cosa_params *__restrict__ Pp, double 
 
 // ---- muscl_b{i,j,k} (src/flux.f90:1221-1810) ---------------------------------------
 // Pass 1: dq along d over the reference's range, with strong-boundary doubling.
-__global__ void k_muscl_dq(DevBlock b, const cosa_params *__restrict__ Pp, int d, const double *__restrict__ q,
-                           double *__restrict__ dq, const int *__restrict__ bct, int nbcs, int vs, int ve) {
+template <class BS>
+__global__ void k_muscl_dq(BS bs_, const cosa_params *__restrict__ Pp, int d, const double *__restrict__ q,
+                           double *__restrict__ dq, const int *__restrict__ bct, int vs, int ve) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
@@ -175,8 +187,8 @@ __global__ void k_muscl_dq(DevBlock b, const cosa_params *__restrict__ Pp, int d
     double val = q[base + p3_cell(b, i, j, k)] - q[base + p3_cell(b, im1, jm1, km1)];
     const int e = d == 1 ? i : (d == 2 ? j : k);
     if (e == 1 || e == mx) {
-      for (int ib = 0; ib < nbcs; ++ib) {
-        const int *rw = bct + 10 * ib;
+      for (int ib = 0; ib < b.nbcs; ++ib) {
+        const int *rw = bct + b.obct + 10 * ib;
         if (rw[1] != d || !strong_bc(rw[0])) continue;
         const int bcpt = rw[2] == 1 ? 1 : mx;
         if (e != bcpt) continue;
@@ -195,10 +207,12 @@ __global__ void k_muscl_dq(DevBlock b, const cosa_params *__restrict__ Pp, int d
 
 // Pass 2: limiter + construction of qp/qm on the faces, then the
 // strong-boundary override (qp = qm = q(halo)).
-__global__ void k_muscl_face(DevBlock b, const cosa_params *__restrict__ Pp, int d, int nl,
+template <class BS>
+__global__ void k_muscl_face(BS bs_, const cosa_params *__restrict__ Pp, int d, int nl,
                              const double *__restrict__ q, double *__restrict__ qp, double *__restrict__ qm,
                              const double *__restrict__ dq, double *__restrict__ dqp, double *__restrict__ dqm,
-                             const int *__restrict__ bct, int nbcs, int mixed = 0) {
+                             const int *__restrict__ bct, int mixed = 0) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
@@ -241,8 +255,8 @@ __global__ void k_muscl_face(DevBlock b, const cosa_params *__restrict__ Pp, int
     }
     const int e = d == 1 ? i : (d == 2 ? j : k);
     if (e == 1 || e == mx) {
-      for (int ib = 0; ib < nbcs; ++ib) {
-        const int *rw = bct + 10 * ib;
+      for (int ib = 0; ib < b.nbcs; ++ib) {
+        const int *rw = bct + b.obct + 10 * ib;
         if (rw[1] != d || !strong_bc(rw[0])) continue;
         const int qpm = rw[2] == 1 ? 1 : mx;
         if (e != qpm) continue;
@@ -262,9 +276,11 @@ __global__ void k_muscl_face(DevBlock b, const cosa_params *__restrict__ Pp, int
 }
 
 // ---- roflux_b (src/flux.f90:45-238) --------------------------------------------------
-__global__ void k_roflux(DevBlock b, const cosa_params *__restrict__ Pp, int d, const double *__restrict__ qr,
+template <class BS>
+__global__ void k_roflux(BS bs_, const cosa_params *__restrict__ Pp, int d, const double *__restrict__ qr,
                          const double *__restrict__ ql, double *__restrict__ flux, const double *__restrict__ sijk,
                          int mixed = 0) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const PhysPar ph = make_phys(P);
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
@@ -317,8 +333,10 @@ __global__ void k_roflux(DevBlock b, const cosa_params *__restrict__ Pp, int d, 
 }
 
 // ---- bresid (src/cosa.f90:1149-1211) --------------------------------------------------
-__global__ void k_resid(DevBlock b, const cosa_params *__restrict__ Pp, int d, const double *__restrict__ flux,
+template <class BS>
+__global__ void k_resid(BS bs_, const cosa_params *__restrict__ Pp, int d, const double *__restrict__ flux,
                         double *__restrict__ res) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
@@ -337,9 +355,11 @@ __global__ void k_resid(DevBlock b, const cosa_params *__restrict__ Pp, int d, c
 }
 
 // ---- update_b explicit, mean flow (src/update.f90:568-640) ---------------------------
-__global__ void k_update(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
+template <class BS>
+__global__ void k_update(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
                          double *__restrict__ q, const double *__restrict__ qold, const double *__restrict__ dtv,
                          double ar) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
@@ -357,7 +377,9 @@ __global__ void k_update(DevBlock b, const cosa_params *__restrict__ Pp, const d
 }
 
 // ---- zero (src/util.f90), extent 1: 0..imax etc. ---------------------------------------
-__global__ void k_zero_res(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ res) {
+template <class BS>
+__global__ void k_zero_res(BS bs_, const cosa_params *__restrict__ Pp, double *__restrict__ res) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int ni = b.im + 1, nj = b.jm + 1, nk = b.km + 1;
@@ -522,8 +544,10 @@ __global__ void k_vols(DevBlock b, const double *__restrict__ x, const double *_
 
 // ---- implicit residual smoothing (src/cosa.f90:2035-2443, 5206-5773) -------------
 // scalef_b / scaleb_b (src/cosa.f90:5652-5773): res *= or /= dt/V
-__global__ void k_irs_scale(DevBlock b, int npde, int S, double *__restrict__ res, const double *__restrict__ dtv,
+template <class BS>
+__global__ void k_irs_scale(BS bs_, int npde, int S, double *__restrict__ res, const double *__restrict__ dtv,
                             const double *__restrict__ dtvt, int forward) {
+  const DevBlock b = bs_.get();
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
   const int64_t n = (int64_t)ni * nj * nk * S;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
@@ -549,10 +573,11 @@ __global__ void k_irs_scale(DevBlock b, int npde, int S, double *__restrict__ re
 // so they are computed once into `scr` (2 doubles per cell) and reused for
 // each variable.  ores (if set) is the right-hand side of the i sweep of the
 // cut variant; with_halo adds eps * res(halo) on the first and last rows.
-template <int D>
-__global__ void k_irs_line(DevBlock b, int npde, int S, double *__restrict__ res, const double *__restrict__ ores,
+template <int D, class BS>
+__global__ void k_irs_line(BS bs_, int npde, int S, double *__restrict__ res, const double *__restrict__ ores,
                            const double *__restrict__ beta, double eps, int vs, int ve, int with_halo,
                            double *__restrict__ scr) {
+  const DevBlock b = bs_.get();
   const int im = b.im - 1, jm = b.jm - 1, km = b.km - 1;
   const int len = D == 1 ? im : (D == 2 ? jm : km);
   const int n2 = D == 1 ? jm : im, n3 = D == 3 ? jm : km;
@@ -632,10 +657,11 @@ __global__ void k_irs_line(DevBlock b, int npde, int S, double *__restrict__ res
 // b_m.  The chain of dependent steps is log2(len) instead of 2 len; the
 // result differs from the Thomas sweeps by rounding only (the matrix is
 // strictly diagonally dominant).
-template <int D>
-__global__ void __launch_bounds__(128) k_irs_pcr(DevBlock b, int npde, int S, double *__restrict__ res,
+template <int D, class BS>
+__global__ void __launch_bounds__(128) k_irs_pcr(BS bs_, int npde, int S, double *__restrict__ res,
                                                  const double *__restrict__ ores, const double *__restrict__ beta,
                                                  double eps, int vs, int ve, int with_halo, int nmax) {
+  const DevBlock b = bs_.get();
   extern __shared__ double irs_sm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int im = b.im - 1, jm = b.jm - 1, km = b.km - 1;
@@ -731,8 +757,10 @@ __global__ void k_update_stage(DevBlock b, int npde, int S, const double *__rest
 }
 
 // ---- src_bhb (src/src.f90:556-613): res(n) += sum_m omega V D(n,m) q(m) -------------
-__global__ void k_src_hb(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
+template <class BS>
+__global__ void k_src_hb(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
                          const double *__restrict__ vol, double *__restrict__ res) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;

@@ -46,8 +46,9 @@ __device__ __forceinline__ int64_t p3s_idx(const DevBlock &b, int S, int i, int 
 }
 
 // mut on the faces of family D into flux(.,1) (bq_face_* calmut part)
-template <int D>
-__global__ void k_qface_mut(DevBlock b, int npde, int S, const double *__restrict__ mut, double *__restrict__ flux) {
+template <int D, class BS>
+__global__ void k_qface_mut(BS bs_, int npde, int S, const double *__restrict__ mut, double *__restrict__ flux) {
+  const DevBlock b = bs_.get();
   KOM_FACE_LOOP(D)
     const int di = D == 1, dj = D == 2, dk = D == 3;
     flux[f0_idx(b, npde, S, i, j, k, 1, n)] =
@@ -69,10 +70,12 @@ __global__ void k_qwall_mut(const DevBlock *__restrict__ blocks, const WallFace 
 }
 
 // b_rtst (src/flux.f90:2846-2946): tau1(.,1..6) on the faces of family d
-__global__ void k_rtst(DevBlock b, int d, const cosa_params *__restrict__ Pp, const double *__restrict__ qf,
+template <class BS>
+__global__ void k_rtst(BS bs_, int d, const cosa_params *__restrict__ Pp, const double *__restrict__ qf,
                        const double *__restrict__ g0, const double *__restrict__ g1, const double *__restrict__ g2,
                        const double *__restrict__ vm, int64_t n0, const double *__restrict__ flux,
                        double *__restrict__ tau) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const double fact = 2.0 / 3.0, mr = P.machfs / P.reyno;
@@ -106,11 +109,13 @@ __global__ void k_rtst(DevBlock b, int d, const cosa_params *__restrict__ Pp, co
 // vflux_b with kom: the k-omega branch (Reynolds stresses, k and omega
 // diffusion; the omega row keeps the reference's dk/dz) followed by the
 // laminar terms with the face mut of flux(.,1)
-__global__ void k_vflux_kom(DevBlock b, int d, const cosa_params *__restrict__ Pp, const double *__restrict__ qf,
+template <class BS>
+__global__ void k_vflux_kom(BS bs_, int d, const cosa_params *__restrict__ Pp, const double *__restrict__ qf,
                             const double *__restrict__ g0, const double *__restrict__ g1,
                             const double *__restrict__ g2, const double *__restrict__ tau,
                             const double *__restrict__ vm, int64_t n0, const double *__restrict__ s,
                             double *__restrict__ flux) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
   const ViscPar V = make_visc(P);
@@ -157,8 +162,9 @@ __global__ void k_vflux_kom(DevBlock b, int d, const cosa_params *__restrict__ P
 }
 
 // q_der_c (src/flux.f90:2979-3130): velocity differences of the face values
-template <int D>
-__global__ void k_qder_c(DevBlock b, int npde, int S, const double *__restrict__ qf, double *__restrict__ dc) {
+template <int D, class BS>
+__global__ void k_qder_c(BS bs_, int npde, int S, const double *__restrict__ qf, double *__restrict__ dc) {
+  const DevBlock b = bs_.get();
   KOM_CELL_LOOP
     const int di = D == 1, dj = D == 2, dk = D == 3;
     const int64_t c0 = p3_cell(b, i, j, k), c1 = p3_cell(b, i + di, j + dj, k + dk);
@@ -171,10 +177,12 @@ __global__ void k_qder_c(DevBlock b, int npde, int S, const double *__restrict__
 }
 
 // turprod_b (src/src.f90:40-177)
-__global__ void k_turprod(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ dx,
+template <class BS>
+__global__ void k_turprod(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ dx,
                           const double *__restrict__ de, const double *__restrict__ dz, const double *__restrict__ vm,
                           int64_t n0, double *__restrict__ prd, double *__restrict__ divvel,
                           double *__restrict__ delpls) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   KOM_CELL_LOOP
@@ -207,9 +215,11 @@ __global__ void k_turprod(DevBlock b, const cosa_params *__restrict__ Pp, const 
 }
 
 // srckw_b (src/src.f90:196-272)
-__global__ void k_srckw(DevBlock b, const cosa_params *__restrict__ Pp, int nl, const double *__restrict__ q,
+template <class BS>
+__global__ void k_srckw(BS bs_, const cosa_params *__restrict__ Pp, int nl, const double *__restrict__ q,
                         const double *__restrict__ mut, const double *__restrict__ prd,
                         const double *__restrict__ divvel, double *__restrict__ res, const double *__restrict__ vol) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const double fact = 2.0 / 3.0, mor = P.machfs / P.reyno;
@@ -234,10 +244,12 @@ __global__ void k_srckw(DevBlock b, const cosa_params *__restrict__ Pp, int nl, 
 }
 
 // update_b, explicit k-omega part (src/update.f90:601-640)
-__global__ void k_update_kom(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
+template <class BS>
+__global__ void k_update_kom(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
                              double *__restrict__ q, const double *__restrict__ qold, const double *__restrict__ vol,
                              const double *__restrict__ dtt, const double *__restrict__ delpls,
                              const double *__restrict__ prd, double ar) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const double gav = P.gkw, bav = P.bkw;
@@ -304,8 +316,10 @@ __global__ void k_rest4(DevBlock b1, DevBlock b2, int S, const double *__restric
 
 // lim_prod_mg_b: q conservative (tke, ome are rho k, rho omega), as the
 // reference's residual pass leaves it
-__global__ void k_lim_prod_mg(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
+template <class BS>
+__global__ void k_lim_prod_mg(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
                               double *__restrict__ prd, const double *__restrict__ mut) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const double mor = P.machfs / P.reyno;
@@ -321,10 +335,12 @@ __global__ void k_lim_prod_mg(DevBlock b, const cosa_params *__restrict__ Pp, co
 
 // lim_res_ome_b, explicit branch without low-speed preconditioning
 // (ttrm = (0, gkw, bkw) for the Wilcox model)
-__global__ void k_lim_res_ome(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ res,
+template <class BS>
+__global__ void k_lim_res_ome(BS bs_, const cosa_params *__restrict__ Pp, double *__restrict__ res,
                               const double *__restrict__ q, const double *__restrict__ vol,
                               const double *__restrict__ dtt, const double *__restrict__ delpls,
                               const double *__restrict__ prd, double ar) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const double gav = P.gkw, bav = P.bkw;
@@ -343,8 +359,10 @@ __global__ void k_lim_res_ome(DevBlock b, const cosa_params *__restrict__ Pp, do
 
 // add_array over the interior cells (off_l = -1, src/util.f90:137-222):
 // v1 += fact v2 for all nvs = npde * S variable planes
-__global__ void k_add_interior(DevBlock b, int nvs, double *__restrict__ v1, const double *__restrict__ v2,
+template <class BS>
+__global__ void k_add_interior(BS bs_, int nvs, double *__restrict__ v1, const double *__restrict__ v2,
                                double fact) {
+  const DevBlock b = bs_.get();
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
   const int64_t total = (int64_t)ni * nj * nk * nvs;
   const int64_t base = b.op3 * nvs;

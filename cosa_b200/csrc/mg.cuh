@@ -82,7 +82,10 @@ __device__ __forceinline__ double edge_fit(const int x[4], const int y[4], doubl
 }
 // one thread per (edge cell, variable, snapshot); nvar variables of stride
 // P3 per snapshot (q: npde, mut: 1)
-__global__ void k_edges(DevBlock b, int nvar, int S, double *__restrict__ q, int64_t base) {
+template <class BS>
+__global__ void k_edges(BS bs_, int nvar, int S, double *__restrict__ q, int64_t base) {
+  const DevBlock b = bs_.get();
+  if (base < 0) base = b.op3 * nvar * S;  // multi-block launch: the block's own offset
   const int nk = b.km - 1, nj = b.jm - 1;
   const int64_t per = 4 * ((int64_t)nk + nj + (b.im - 1));
   const int64_t total = per * nvar * S;
@@ -289,7 +292,9 @@ __global__ void k_prol_lin(DevBlock b1, DevBlock b2, int npde, int S, double *__
 }
 
 // ---- fixq_b (src/update.f90:2216-2269) / tur_vis_b (2297-2337) --------------------------
-__global__ void k_fixq(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ q) {
+template <class BS>
+__global__ void k_fixq(BS bs_, const cosa_params *__restrict__ Pp, double *__restrict__ q) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
@@ -308,8 +313,10 @@ __global__ void k_fixq(DevBlock b, const cosa_params *__restrict__ Pp, double *_
     if (ome < P.qmin[6]) *qw = rho * P.qmin[6];
   }
 }
-__global__ void k_tur_vis(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
+template <class BS>
+__global__ void k_tur_vis(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
                           double *__restrict__ mut) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int ni = b.im + 1, nj = b.jm + 1, nk = b.km + 1;

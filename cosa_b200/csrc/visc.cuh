@@ -563,10 +563,12 @@ __global__ void k_dt_ns(const DevBlock *__restrict__ blocks, const cosa_params *
 
 // ---- per-routine kernels (reference array contract) ----------------------------------
 // lambda with viscous = .true.: lam(.,1:3) convective, lamv(.,1:3) viscous
-__global__ void k_lambda_ns(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
+template <class BS>
+__global__ void k_lambda_ns(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
                             const double *__restrict__ si, const double *__restrict__ sj,
                             const double *__restrict__ sk, const double *__restrict__ vol,
                             const double *__restrict__ mut, double *__restrict__ lam, double *__restrict__ lamv) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
@@ -589,9 +591,11 @@ __global__ void k_lambda_ns(DevBlock b, const cosa_params *__restrict__ Pp, cons
   }
 }
 
-__global__ void k_deltat_ns(DevBlock b, const cosa_params *__restrict__ Pp, double *__restrict__ dtv,
+template <class BS>
+__global__ void k_deltat_ns(BS bs_, const cosa_params *__restrict__ Pp, double *__restrict__ dtv,
                             const double *__restrict__ lam, const double *__restrict__ lamv, double *bx, double *by,
                             double *bz, double *dtt, double *tbx, double *tby, double *tbz) {
+  const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
@@ -624,9 +628,10 @@ __global__ void k_deltat_ns(DevBlock b, const cosa_params *__restrict__ Pp, doub
 }
 
 // q_face / q_der bulk loops with the reference's P3 outputs
-template <int D, int NV>
-__global__ void k_qface_qder(DevBlock b, int S, const double *__restrict__ q, double *__restrict__ qf,
+template <int D, int NV, class BS>
+__global__ void k_qface_qder(BS bs_, int S, const double *__restrict__ q, double *__restrict__ qf,
                              double *__restrict__ g0, double *__restrict__ g1, double *__restrict__ g2) {
+  const DevBlock b = bs_.get();
   const int ni = D == 1 ? b.im : b.im - 1, nj = D == 2 ? b.jm : b.jm - 1, nk = D == 3 ? b.km : b.km - 1;
   const int64_t total = (int64_t)ni * nj * nk * S;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
