@@ -522,7 +522,10 @@ int check_rans_supported(const cosa_params &p) {
 
 int check_fused_supported(const cosa_params &p) {
   if (p.kom) return check_rans_supported(p);
-  if (p.npde != 5 || p.kom || p.kom_bsl || p.kom_sst || p.rkimp || p.moving ||
+  // rkimp: the implicit time-spectral update of harmonic balance, branch
+  // without IRS on one level (update_bhb, src/update.f90:1564-1604)
+  if (p.rkimp && (!p.harbal || p.irsop != 0 || p.nlevel > 1)) return COSA_ERR_UNSUPPORTED;
+  if (p.npde != 5 || p.kom || p.kom_bsl || p.kom_sst || p.moving ||
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
   return COSA_OK;
@@ -820,11 +823,11 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   }
   A.strong = L.d_strong; A.smap = L.d_smap; A.status = c->d_status;
   A.ar = p.alphas[irk - 1];
-  A.vol = p.harbal ? P.vol : nullptr;
+  A.vol = p.harbal && !p.rkimp ? P.vol : nullptr;  // rkimp: the time-spectral term goes to update_bhb
   A.compute_dt = compute_dt;
   A.first_order = nl >= p.nl_crs;
   A.update = update;
-  const bool split = L.schedule == 1 && c->nseg == 0 && L.d_cflux && L.d_qprim;
+  const bool split = L.schedule == 1 && c->nseg == 0 && L.d_cflux && L.d_qprim && !p.rkimp;
   if (split) {
     // primitive copy (with bprtest) shared by the viscous and convective faces
     int64_t m3 = 0;
@@ -905,6 +908,32 @@ int launch_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
     const double *qold = irk == 1 ? Q : QO;
     double *qcopy = (irk == 1 && o.copy_qold) ? QO : nullptr;
     const int rmode = (irk == 1 && o.force) ? 2 : 1;
+    if (p.rkimp) {
+      // residual without the time-spectral term -> [norm with it] -> the
+      // per-cell snapshot solve of update_bhb
+      int r = launch_stage(c, nl, L, qin, qout, qold, nullptr, irk, o.compute_dt && irk == 1, false, 0, L.d_res,
+                           o.rhs, rmode);
+      if (r) return r;
+      if (o.want_rms && irk == 1) {
+        int64_t ncell = 0;
+        for (int b = 0; b < L.nb; ++b) {
+          const DevBlock &x = L.hb[b];
+          k_rms_bhb_partial<<<64, 256, 0, c->s>>>(x, c->d_p, L.d_res, qin, L.ptrs.vol, L.d_part + (int64_t)b * 64 * 8);
+          if ((r = after_launch(c))) return r;
+          ncell += (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1);
+        }
+        k_rms_final<<<1, 256, 0, c->s>>>(L.d_part, L.nb * 64, p.npde, (double)ncell * S, c->d_hist, c->d_row,
+                                         c->hist_cap);
+        if ((r = after_launch(c))) return r;
+      }
+      const double *QOLD = qold;
+      r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+        k_update_bhb<<<g, 256, 0, c->s>>>(b, c->d_p, L.d_res, QOLD, qout, qcopy, L.ptrs.dtvol, L.ptrs.vol,
+                                          p.alphas[irk - 1]);
+      });
+      if (r) return r;
+      continue;
+    }
     if (p.irsop == 0) {
       int r = launch_stage(c, nl, L, qin, qout, qold, qcopy, irk, o.compute_dt && irk == 1, o.want_rms && irk == 1, 1,
                            nullptr, o.rhs, rmode);
@@ -1328,7 +1357,12 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
     if (hist && (mgit == 1 || mgit % rms_every == 0 || mgit == last)) rows.push_back(it);
   }
   if ((r = ensure_hist(c, std::max<int>(1, (int)rows.size())))) return r;
-  if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, *L))) return r;
+  if ((c->p.irsop > 0 || c->p.rkimp) && (r = ensure_irs_scratch(c, *L))) return r;
+  if (c->p.rkimp && L->npart_cap < L->nb * 64) {  // per-block norm partials of the implicit HB norm
+    drop_graphs(c);
+    if ((r = dalloc(c, &L->d_part, (size_t)L->nb * 64 * 8))) return r;
+    L->npart_cap = L->nb * 64;
+  }
   CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
   const int iter = 1;
   const int compute_dt = (iter / c->p.iupdt * c->p.iupdt == iter) ? 1 : 0;
@@ -1768,7 +1802,12 @@ int cosa_gpu_smooth_level(cosa_ctx *c, int32_t nl, int32_t niter, int32_t from_f
   cudaSetDevice(c->device);
   const bool want = resrms && nl == 1 && niter > 0 && (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle);
   if ((r = ensure_hist(c, 1))) return r;
-  if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, *L))) return r;
+  if ((c->p.irsop > 0 || c->p.rkimp) && (r = ensure_irs_scratch(c, *L))) return r;
+  if (c->p.rkimp && L->npart_cap < L->nb * 64) {  // per-block norm partials of the implicit HB norm
+    drop_graphs(c);
+    if ((r = dalloc(c, &L->d_part, (size_t)L->nb * 64 * 8))) return r;
+    L->npart_cap = L->nb * 64;
+  }
   CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
   if (c->p.kom && (r = ensure_rans(c, *L))) return r;
   const bool first = mgit == 1;
@@ -1799,8 +1838,14 @@ int cosa_gpu_mg(cosa_ctx *c, int32_t mgit0, int32_t ncycles, int32_t ncycle, int
   }
   if ((r = ensure_hist(c, std::max<int>(1, (int)rows.size())))) return r;
   for (int nl = 1; nl <= nlevel; ++nl) {
-    if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, *level(c, nl)))) return r;
-    if (c->p.kom && (r = ensure_rans(c, *level(c, nl)))) return r;
+    LevelState &Lv = *level(c, nl);
+    if ((c->p.irsop > 0 || c->p.rkimp) && (r = ensure_irs_scratch(c, Lv))) return r;
+    if (c->p.rkimp && Lv.npart_cap < Lv.nb * 64) {  // per-block norm partials of the implicit HB norm
+      drop_graphs(c);
+      if ((r = dalloc(c, &Lv.d_part, (size_t)Lv.nb * 64 * 8))) return r;
+      Lv.npart_cap = Lv.nb * 64;
+    }
+    if (c->p.kom && (r = ensure_rans(c, Lv))) return r;
   }
   CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
   size_t ri = 0;

@@ -783,3 +783,128 @@ __global__ void k_src_hb(BS bs_, const cosa_params *__restrict__ Pp, const doubl
     }
   }
 }
+
+// ---- update_bhb, rkimp branch without IRS on one level (src/update.f90:1564-1604) ----
+// LU with partial pivoting of an n x n matrix (column-major a[i + n*j]) and
+// the solve for nrhs right-hand sides (b[i + n*m]), in the order of LAPACK's
+// unblocked DGETF2 (first largest pivot, whole rows swapped, column scaled by
+// the pivot's reciprocal, rank-1 update) and DGETRS 'N'
+__device__ __forceinline__ void hb_lu_solve(int n, double *a, double *bm, int nrhs) {
+  int ipiv[COSA_MAX_SNAP];
+  for (int j = 0; j < n; ++j) {
+    int pv = j;
+    double amax = fabs(a[j + n * j]);
+    for (int i = j + 1; i < n; ++i)
+      if (fabs(a[i + n * j]) > amax) { amax = fabs(a[i + n * j]); pv = i; }
+    ipiv[j] = pv;
+    if (a[pv + n * j] != 0.0) {
+      if (pv != j)
+        for (int k = 0; k < n; ++k) {
+          const double t = a[j + n * k];
+          a[j + n * k] = a[pv + n * k];
+          a[pv + n * k] = t;
+        }
+      const double r = 1.0 / a[j + n * j];
+      for (int i = j + 1; i < n; ++i) a[i + n * j] = a[i + n * j] * r;
+    }
+    for (int k = j + 1; k < n; ++k) {
+      const double t = -a[j + n * k];
+      for (int i = j + 1; i < n; ++i) a[i + n * k] = a[i + n * k] + a[i + n * j] * t;
+    }
+  }
+  for (int m = 0; m < nrhs; ++m) {
+    double *x = bm + n * m;
+    for (int j = 0; j < n; ++j)
+      if (ipiv[j] != j) {
+        const double t = x[j];
+        x[j] = x[ipiv[j]];
+        x[ipiv[j]] = t;
+      }
+    for (int k = 0; k < n; ++k)
+      if (x[k] != 0.0)
+        for (int i = k + 1; i < n; ++i) x[i] = x[i] - x[k] * a[i + n * k];
+    for (int k = n - 1; k >= 0; --k)
+      if (x[k] != 0.0) {
+        x[k] = x[k] / a[k + n * k];
+        for (int i = 0; i < k; ++i) x[i] = x[i] - x[k] * a[i + n * k];
+      }
+  }
+}
+
+// one thread per interior cell: (I + ar omega dtau D) q = qold - ar res dtvol
+// over the snapshots (dtau = dtvol V of the row's snapshot), the five
+// mean-flow equations as five right-hand sides; qcopy (stage 1) receives qold
+template <class BS>
+__global__ void k_update_bhb(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
+                             const double *__restrict__ qold, double *__restrict__ qout, double *__restrict__ qcopy,
+                             const double *__restrict__ dtv, const double *__restrict__ vol, double ar) {
+  const DevBlock b = bs_.get();
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ni_ = b.im - 1, nj_ = b.jm - 1, nk_ = b.km - 1;
+  const int64_t n = (int64_t)ni_ * nj_ * nk_;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni_) + 1; r /= ni_;
+    const int j = (int)(r % nj_) + 1;
+    const int k = (int)(r / nj_) + 1;
+    const int64_t c = p3_cell(b, i, j, k);
+    const double v = vol[p1_idx(b, 1, i, j, k, 0)];
+    double a[COSA_MAX_SNAP * COSA_MAX_SNAP], x[COSA_MAX_SNAP * 5];
+    for (int si = 0; si < S; ++si) {
+      const double dt = dtv[p1_idx(b, S, i, j, k, si)];
+      const double dtau = dt * v;
+      for (int sj = 0; sj < S; ++sj) a[si + S * sj] = (si == sj ? 1.0 : 0.0) + ar * P.omega * dtau * P.dhb[si * S + sj];
+      for (int m = 0; m < 5; ++m) {
+        const int64_t o = p3_var(b, npde, S, m + 1, si) + c;
+        const double q0 = qold[o];
+        if (qcopy) qcopy[o] = q0;
+        x[si + S * m] = q0 - ar * res[o] * dt;
+      }
+    }
+    hb_lu_solve(S, a, x, 5);
+    for (int si = 0; si < S; ++si)
+      for (int m = 0; m < 5; ++m) qout[p3_var(b, npde, S, m + 1, si) + c] = x[si + S * m];
+  }
+}
+
+// resg_brms_hb partial sums with rkimp (src/cosa.f90:4629-4697): the
+// residual plus omega D q V, one snapshot at a time, squared; 8 doubles per CTA
+__global__ void k_rms_bhb_partial(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
+                                  const double *__restrict__ q, const double *__restrict__ vol,
+                                  double *__restrict__ part) {
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t ncell = (int64_t)ni * nj * nk;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)r + 1;
+    const int64_t c = p3_cell(b, i, j, k);
+    const double v = vol[p1_idx(b, 1, i, j, k, 0)];
+    for (int n = 0; n < S; ++n)
+      for (int m = 0; m < npde; ++m) {
+        double w = res[p3_var(b, npde, S, m + 1, n) + c];
+        for (int s2 = 0; s2 < S; ++s2) w = w + P.omega * P.dhb[n * S + s2] * q[p3_var(b, npde, S, m + 1, s2) + c] * v;
+        acc[m] += w * w;
+      }
+  }
+  __shared__ double red[7][32];
+  for (int m = 0; m < npde; ++m) {
+    double x = acc[m];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) red[m][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int nw = blockDim.x >> 5;
+    for (int m = 0; m < npde; ++m) {
+      double x = threadIdx.x < nw ? red[m][threadIdx.x] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (threadIdx.x == 0) part[(int64_t)blockIdx.x * 8 + m] = x;
+    }
+  }
+}

@@ -1283,6 +1283,102 @@ void resg_rms_hb_level(const Level &L, double *ra, double *out) {
   out[L.npde] = std::sqrt(acc[L.npde + 1] / ncell / L.S / L.npde);
 }
 
+// resg_brms_hb with rkimp, no IRS and one level (src/cosa.f90:4629-4697):
+// the harmonic-balance term omega D q V is added to the residual, one
+// snapshot nj at a time, before the squares are summed
+void resg_rms_hbimp_level(const Level &L, const double *ra, const double *qa, const double *va, const cosa_params &P,
+                          double *out) {
+  const int S = L.S;
+  double acc[10] = {0};
+  int64_t ncell = 0;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 res(const_cast<double *>(ra), L, b), q(const_cast<double *>(qa), L, b);
+    B1 vol(const_cast<double *>(va), L, b, 1);
+    double rb[10] = {0};
+    for (int n = 0; n < S; ++n)
+      for (int v = 1; v <= L.npde; ++v)
+        for (int k = 1; k <= L.km[b] - 1; ++k)
+          for (int j = 1; j <= L.jm[b] - 1; ++j)
+            for (int i = 1; i <= L.im[b] - 1; ++i) {
+              double w = res(i, j, k, v, n);
+              for (int nj = 0; nj < S; ++nj) w = w + P.omega * P.dhb[n * S + nj] * q(i, j, k, v, nj) * vol(i, j, k);
+              rb[v] = rb[v] + w * w;
+            }
+    for (int v = 1; v <= L.npde; ++v) rb[L.npde + 1] = rb[L.npde + 1] + rb[v];
+    for (int v = 1; v <= L.npde + 1; ++v) acc[v] = acc[v] + rb[v];
+    ncell += (int64_t)(L.im[b] - 1) * (L.jm[b] - 1) * (L.km[b] - 1);
+  }
+  for (int v = 1; v <= L.npde; ++v) out[v - 1] = std::sqrt(acc[v] / ncell / S);
+  out[L.npde] = std::sqrt(acc[L.npde + 1] / ncell / S / L.npde);
+}
+
+// LU factorisation with partial pivoting of an n x n matrix (column-major,
+// a[i + n*j]) and the solve for nrhs right-hand sides (b[i + n*m]), in the
+// order of LAPACK's unblocked DGETF2 (pivot = first largest |a(i,j)|, whole
+// rows swapped, column scaled by the pivot's reciprocal, rank-1 update) and
+// DGETRS 'N' (row interchanges, unit-lower then upper triangular solves);
+// DGETRF's recursive variant may round differently.
+void lu_solve(int n, double *a, double *bm, int nrhs) {
+  int ipiv[COSA_MAX_SNAP];
+  for (int j = 0; j < n; ++j) {
+    int pv = j;
+    double amax = std::fabs(a[j + n * j]);
+    for (int i = j + 1; i < n; ++i)
+      if (std::fabs(a[i + n * j]) > amax) { amax = std::fabs(a[i + n * j]); pv = i; }
+    ipiv[j] = pv;
+    if (a[pv + n * j] != 0.0) {
+      if (pv != j)
+        for (int k = 0; k < n; ++k) std::swap(a[j + n * k], a[pv + n * k]);
+      const double r = 1.0 / a[j + n * j];
+      for (int i = j + 1; i < n; ++i) a[i + n * j] = a[i + n * j] * r;
+    }
+    for (int k = j + 1; k < n; ++k) {
+      const double t = -a[j + n * k];
+      for (int i = j + 1; i < n; ++i) a[i + n * k] = a[i + n * k] + a[i + n * j] * t;
+    }
+  }
+  for (int m = 0; m < nrhs; ++m) {
+    double *x = bm + n * m;
+    for (int j = 0; j < n; ++j)
+      if (ipiv[j] != j) std::swap(x[j], x[ipiv[j]]);
+    for (int k = 0; k < n; ++k)
+      if (x[k] != 0.0)
+        for (int i = k + 1; i < n; ++i) x[i] = x[i] - x[k] * a[i + n * k];
+    for (int k = n - 1; k >= 0; --k)
+      if (x[k] != 0.0) {
+        x[k] = x[k] / a[k + n * k];
+        for (int i = 0; i < k; ++i) x[i] = x[i] - x[k] * a[i + n * k];
+      }
+  }
+}
+
+// update_bhb, rkimp branch without IRS on one level, mean-flow equations
+// (src/update.f90:1564-1604): per cell the snapshots are coupled through
+// (I + ar omega dtau D) q = qold - ar res dtvol, dtau = dtvol V of the row's
+// snapshot
+void update_bhb_b(const Level &L, int b, const double *ra, double *qa, const double *qoa, const double *dta,
+                  const double *va, double ar, const cosa_params &P) {
+  const int S = L.S;
+  B3 res(const_cast<double *>(ra), L, b), q(qa, L, b), qold(const_cast<double *>(qoa), L, b);
+  B1 dtv(const_cast<double *>(dta), L, b, S), vol(const_cast<double *>(va), L, b, 1);
+  for (int k = 1; k <= L.km[b] - 1; ++k)
+    for (int j = 1; j <= L.jm[b] - 1; ++j)
+      for (int i = 1; i <= L.im[b] - 1; ++i) {
+        double a[COSA_MAX_SNAP * COSA_MAX_SNAP], x[COSA_MAX_SNAP * 5];
+        for (int ni = 0; ni < S; ++ni) {
+          const double dtau = dtv(i, j, k, ni) * vol(i, j, k);
+          for (int nj = 0; nj < S; ++nj)
+            a[ni + S * nj] = (ni == nj ? 1.0 : 0.0) + ar * P.omega * dtau * P.dhb[ni * S + nj];
+        }
+        for (int ni = 0; ni < S; ++ni)
+          for (int m = 0; m < 5; ++m)
+            x[ni + S * m] = qold(i, j, k, m + 1, ni) - ar * res(i, j, k, m + 1, ni) * dtv(i, j, k, ni);
+        lu_solve(S, a, x, 5);
+        for (int ni = 0; ni < S; ++ni)
+          for (int m = 0; m < 5; ++m) q(i, j, k, m + 1, ni) = x[ni + S * m];
+      }
+}
+
 // ---- resg_brms (src/cosa.f90:4503-4582), explicit steady branch ------------
 void resg_rms_level(const Level &L, double *ra, double *rha, double *out) {
   double acc[10] = {0};
@@ -3100,21 +3196,32 @@ int orc_smooth_hb(orc_level *h, const cosa_params *p, int ncycles, int mgit0, in
   Level &L = h->L;
   int status = 0;
   const int last = mgit0 + ncycles - 1;
+  // rkimp without IRS on one level: the time-spectral term is not added to
+  // the residual (src/cosa.f90:1918-1922) but solved in update_bhb
+  const bool imp = p->rkimp != 0;
+  if (imp && (p->irsop != 0 || p->nlevel > 1 || L.npde != 5)) return COSA_ERR_UNSUPPORTED;
   for (int mgit = mgit0; mgit <= last; ++mgit) {
     const int iter = 1;
     copy_interior(L, qold, q);
     for (int irk = 1; irk <= p->nstage; ++irk) {
       const bool want_dt = (iter / p->iupdt * p->iupdt == iter) && irk == 1;
       status |= residual_impl(h, p, 1, q, si, sj, sk, res, qp, qm, dq, dqp, dqm, flux, dtvol, want_dt, nullptr,
-                              nullptr, nullptr, vol);
-      if (irk == 1 && (mgit == 1 || mgit % rms_every == 0 || mgit == last) && hist)
-        resg_rms_hb_level(L, res, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
+                              nullptr, nullptr, imp ? nullptr : vol);
+      if (irk == 1 && (mgit == 1 || mgit % rms_every == 0 || mgit == last) && hist) {
+        if (imp) resg_rms_hbimp_level(L, res, q, vol, *p, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
+        else resg_rms_hb_level(L, res, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
+      }
 #pragma omp parallel for schedule(dynamic)
-      for (int b = 0; b < L.nb; ++b) update_b(L, b, res, q, qold, dtvol, p->alphas[irk - 1]);
+      for (int b = 0; b < L.nb; ++b) {
+        if (imp) update_bhb_b(L, b, res, q, qold, dtvol, vol, p->alphas[irk - 1], *p);
+        else update_b(L, b, res, q, qold, dtvol, p->alphas[irk - 1]);
+      }
     }
   }
   return status;
 }
+
+void orc_lu_solve(int n, double *a, double *b, int nrhs) { lu_solve(n, a, b, nrhs); }
 
 void orc_src_hb(orc_level *h, const cosa_params *p, const double *q, const double *vol, double *res) {
   src_hb_level(h->L, q, vol, res, *p);

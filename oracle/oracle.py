@@ -195,7 +195,9 @@ def smooth_irs(O, q, si, sj, sk, ncycles, mgit0=1, rms_every=1):
 
 
 def smooth_hb(O, q, si, sj, sk, vol, ncycles, mgit0=1, rms_every=1):
-    """Explicit harmonic-balance cycles (src_hb in the residual, resg_rms_hb)."""
+    """Harmonic-balance cycles: explicit (src_hb in the residual, resg_rms_hb)
+    or, with params.rkimp, the time-spectral term solved per cell in
+    update_bhb and added to the residual norm."""
     qold = O.p3()
     res = O.p3()
     qp, qm, dq, dqp, dqm = (O.p3() for _ in range(5))
@@ -561,3 +563,16 @@ def mg_rans(levels, arrays, mgit0, ncycles, ncycle, rms_every=1):
     st = lib().orc_mg_rans(hs, C.c_int(n), _par(p), ps, es, C.c_int(mgit0), C.c_int(ncycles), C.c_int(ncycle),
                            C.c_int(rms_every), _p(hist))
     return hist[:ncycles], st
+
+
+def lu_solve(a, b):
+    """x with a x = b (partial-pivot LU in DGETF2/DGETRS order); a (n, n),
+    b (n,) or (n, nrhs)."""
+    n = a.shape[0]
+    af = np.asfortranarray(a, dtype=np.float64).ravel(order="F").copy()
+    bb = np.asarray(b, dtype=np.float64)
+    nrhs = 1 if bb.ndim == 1 else bb.shape[1]
+    bf = bb.reshape(n, nrhs).ravel(order="F").copy()
+    lib().orc_lu_solve(C.c_int(n), _p(af), _p(bf), C.c_int(nrhs))
+    x = bf.reshape((n, nrhs), order="F")
+    return x[:, 0] if bb.ndim == 1 else x

@@ -191,3 +191,47 @@ def test_mg_beats_single_grid(oracle_mod):
     assert st1 == 0
     assert np.isfinite(h3[-1, -1])
     assert h3[-1, -1] < 0.7 * h1[-1, -1], (h3[-1, -1], h1[-1, -1])
+
+
+def test_lu_solve_matches_numpy(oracle_mod):
+    """The partial-pivot LU of update_bhb (DGETF2/DGETRS order) solves random
+    systems, pivoting included, to rounding."""
+    rng = np.random.default_rng(3)
+    for n in (3, 5, 7, 15):
+        a = rng.standard_normal((n, n))
+        b = rng.standard_normal((n, 5))
+        x = oracle_mod.lu_solve(a, b)
+        np.testing.assert_allclose(a @ x, b, rtol=0, atol=1e-12 * np.abs(b).max() * n)
+
+
+def test_implicit_hb_update(oracle_mod):
+    """rkimp (no IRS, one level): with every snapshot equal the time-spectral
+    term vanishes and the implicit update equals the explicit one; with
+    snapshot-dependent states both converge and differ on the way."""
+    from cosa_b200.params import set_harmonic_balance
+    case = casekit.small_partitioned()
+    p = set_harmonic_balance(case.params, 1, 0.16)
+    case.q0 = cases._freestream_state(case.tables, p)
+    O = oracle_mod.OracleLevel(case.tables, p)
+    si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
+    out = {}
+    for imp in (0, 1):
+        p.rkimp = imp
+        q = cases.perturbed_state(case, seed=4)  # the same perturbation in every snapshot
+        h, st = oracle_mod.smooth_hb(O, q, si, sj, sk, vol, 5, rms_every=1)
+        assert st == 0
+        out[imp] = (q, h)
+    np.testing.assert_allclose(out[1][0], out[0][0], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(out[1][1], out[0][1], rtol=1e-10)
+    qs = {}
+    for imp in (0, 1):
+        p.rkimp = imp
+        q = cases.perturbed_state(case, seed=4)
+        for v in cases.p3_views(case.tables, q, 5, 3):
+            for n in range(3):
+                v[..., 1, n] *= 1 + 0.05 * np.sin(2 * np.pi * n / 3)
+        h, st = oracle_mod.smooth_hb(O, q, si, sj, sk, vol, 300, rms_every=100)
+        rows = h[~np.isnan(h[:, 0])]
+        assert st == 0 and rows[-1, 0] < 0.5 * rows[0, 0]
+        qs[imp] = q
+    assert np.abs(qs[1] - qs[0]).max() > 1e-6
