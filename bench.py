@@ -412,6 +412,13 @@ def main():
                                    "M~U[0.3,0.7], alpha~U[-4,8] deg, Poisson 2 req/s; k-omega requests are not served")
         except Exception as e:  # reported, not fatal
             serving = {"error": str(e)}
+        # the same kind of solves batched in the engine (mixed precision)
+        # against the plain single-solve FP64 path, 400 RK cycles each
+        try:
+            reqs = serve.poisson_requests(12, 2.0, 5, naca_fraction=0.5, alpha_range=(-4.0, 4.0))
+            serving["batched_vs_plain"] = serve.batched_vs_plain(reqs, 400, device=dev)
+        except Exception as e:  # reported, not fatal
+            serving["batched_vs_plain"] = {"error": str(e)}
 
     cpu = None
     if rank == 0 and not args.no_cpu:
