@@ -23,14 +23,14 @@ from .solver import SteadySolver
 
 
 def run(model="kom", niter=20000, chunk=2000, cfl=3.0, eps=0.6, reyno=6.0e6, mach=0.3, alpha=4.0, nj=128,
-        h1=4.5e-6, nlevel=1, nk=2, verbose=True):
+        h1=4.5e-6, nlevel=1, nk=2, ramp=None, verbose=True):
     res = {}
     for prec in ("fp64", "mixed"):
         p = cases.naca_params(model, mach=mach, alpha_deg=alpha, reyno=reyno, cfl=cfl, eps_irs=eps, nlevel=nlevel)
         if prec == "mixed":
             p.precision = PREC_MIXED
         case = cases.naca0012_ogrid(nj=nj, nk=nk, h1=h1, params=p)
-        s = SteadySolver(case, ncycle=niter)
+        s = SteadySolver(case, ncycle=niter, ramp=ramp)
         hist, r0, t0 = [], None, time.time()
         for _ in range(0, niter, chunk):
             h, st = s.run(chunk, rms_every=chunk)
@@ -68,9 +68,17 @@ def main():
     ap.add_argument("--h1", type=float, default=4.5e-6, help="first wall spacing (chords)")
     ap.add_argument("--nlevel", type=int, default=1, help="multigrid levels (3 needs --nk 8)")
     ap.add_argument("--nk", type=int, default=2, help="cells in k (span 0.1)")
+    ap.add_argument("--ramp", default=None,
+                    help="k-omega CFL ramp 'mode:n0,n1,n2,n3:c1,c2' from c1 over c2 to --cfl (bdeltat ramping1/2)")
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
-    res = run(a.model, a.niter, a.chunk, a.cfl, a.eps, a.reyno, a.mach, a.alpha, a.nj, a.h1, a.nlevel, a.nk)
+    ramp = None
+    if a.ramp:
+        mode, ns, cs = a.ramp.split(":")
+        c1, c2 = (float(v) for v in cs.split(","))
+        ramp = dict(mode=int(mode), ncycr=tuple(int(v) for v in ns.split(",")), vcfli=(c1, c2, a.cfl),
+                    vcflit=(c1, c2, a.cfl))
+    res = run(a.model, a.niter, a.chunk, a.cfl, a.eps, a.reyno, a.mach, a.alpha, a.nj, a.h1, a.nlevel, a.nk, ramp)
     print(json.dumps(dict(final=res["final"], fp64=res["fp64"]["hist"][-1], mixed=res["mixed"]["hist"][-1],
                           sec_fp64=res["fp64"]["sec"], sec_mixed=res["mixed"]["sec"])))
     if a.out:

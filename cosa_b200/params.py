@@ -192,3 +192,41 @@ def set_harmonic_balance(p: CosaParams, nharms: int, omega: float) -> CosaParams
 
 def params_bytes(p: CosaParams) -> bytes:
     return bytes(memoryview(p))
+
+
+def cfl_ramp(mgit: int, mode: int, ncycr, vcfli, vcflit, current=None):
+    """(cfl, cflt) of cycle mgit under the k-omega CFL ramps of bdeltat
+    (src/cosa.f90:4763-4815).  mode 1: cubic then linear growth, re-evaluated
+    on cycle 1 and every 100th cycle (in between the previous value, passed
+    as `current`, holds); mode 2: constant, linear, constant, linear, every
+    cycle.  ncycr = (n0, n1, n2, n3), vcfli/vcflit = the three CFL levels of
+    the mean-flow and turbulence equations."""
+    n0, n1, n2, n3 = ncycr
+    if mode == 1:
+        if not (mgit == 1 or mgit % 100 == 0):
+            return current
+        s3 = 3.0 ** 0.5
+        d1, d2 = (vcfli[1] - vcfli[0]) * s3 ** 3, vcfli[2] - vcfli[1]
+        t1, t2 = (vcflit[1] - vcflit[0]) * s3 ** 3, vcflit[2] - vcflit[1]
+        if mgit <= n1:
+            return vcfli[0], vcflit[0]
+        if mgit <= n2:
+            f = (float(mgit - n1) / (n2 - n1) / s3) ** 3
+            return vcfli[0] + d1 * f, vcflit[0] + t1 * f
+        if mgit <= n3:
+            f = float(mgit - n2) / (n3 - n2)
+            return vcfli[1] + d2 * f, vcflit[1] + t2 * f
+        return vcfli[2], vcflit[2]
+    d1, d2 = vcfli[1] - vcfli[0], vcfli[2] - vcfli[1]
+    t1, t2 = vcflit[1] - vcflit[0], vcflit[2] - vcflit[1]
+    if mgit <= n0:
+        return vcfli[0], vcflit[0]
+    if mgit <= n1:
+        f = float(mgit - n0) / (n1 - n0)
+        return vcfli[0] + d1 * f, vcflit[0] + t1 * f
+    if mgit <= n2:
+        return vcfli[1], vcflit[1]
+    if mgit <= n3:
+        f = float(mgit - n2) / (n3 - n2)
+        return vcfli[1] + d2 * f, vcflit[1] + t2 * f
+    return vcfli[2], vcflit[2]

@@ -25,12 +25,15 @@ from .params import CosaParams
 
 class SteadySolver:
     def __init__(self, case: "cases.Case", params: Optional[CosaParams] = None, device: int = 0,
-                 q0: Optional[np.ndarray] = None, ncycle: Optional[int] = None):
+                 q0: Optional[np.ndarray] = None, ncycle: Optional[int] = None, ramp: Optional[dict] = None):
         self.case = case
         self.p = params if params is not None else case.params
         p = self.p
         self.nlevel = max(1, int(p.nlevel))
         self.ncycle = ncycle
+        # k-omega CFL ramp of bdeltat: dict(mode=1|2, ncycr=(n0..n3), vcfli=(3), vcflit=(3))
+        self.ramp = ramp if (ramp and p.kom) else None
+        self._cfl = None
         self.viscous = bool(p.viscous)
         self.kom = bool(p.kom)
         lv = cases.mg_levels(case, self.nlevel) if self.nlevel > 1 else [(case.tables, case.x, case.y, case.z)]
@@ -93,12 +96,48 @@ class SteadySolver:
         rows of the printed cycles (NaN rows elsewhere) and the status word.
         The solve's last cycle (ncycle, when given at construction) adds the
         fine-level post-smoothing of mg()."""
-        if self.nlevel == 1:
-            hist, st = self.ctx.smooth(1, niter, self.it + 1, rms_every, want_hist=want_hist)
-        else:
-            ncycle = self.ncycle if self.ncycle is not None else 2 ** 30
-            hist, st = self.ctx.mg(self.it + 1, niter, ncycle, rms_every, want_hist=want_hist)
+        if self.ramp:
+            return self._run_ramped(niter, rms_every, want_hist)
+        hist, st = self._cycles(niter, rms_every, want_hist)
         self.it += niter
+        return hist, st
+
+    def _cycles(self, niter, rms_every, want_hist):
+        if self.nlevel == 1:
+            return self.ctx.smooth(1, niter, self.it + 1, rms_every, want_hist=want_hist)
+        ncycle = self.ncycle if self.ncycle is not None else 2 ** 30
+        return self.ctx.mg(self.it + 1, niter, ncycle, rms_every, want_hist=want_hist)
+
+    def _run_ramped(self, niter, rms_every, want_hist):
+        """Cycles in runs of constant CFL: the parameters are uploaded where
+        the ramp changes cfl/cflt (cycle 1 and every 100th for mode 1, every
+        cycle of a ramp segment for mode 2)."""
+        from .params import cfl_ramp
+        r = self.ramp
+        rows, st = [], 0
+        end = self.it + niter
+        while self.it < end:
+            mgit = self.it + 1
+            c = cfl_ramp(mgit, r["mode"], r["ncycr"], r["vcfli"], r["vcflit"], self._cfl)
+            if c != self._cfl:
+                self._cfl = c
+                self.p.cfl, self.p.cflt = c
+                self.ctx.set_params(self.p)
+            # run until the next cycle where the ramp may change the CFL
+            n = 1
+            while self.it + n < end:
+                nxt = cfl_ramp(self.it + n + 1, r["mode"], r["ncycr"], r["vcfli"], r["vcflit"], c)
+                if nxt != c:
+                    break
+                n += 1
+            h, s_ = self._cycles(n, rms_every, want_hist)
+            st |= s_
+            if h is not None:
+                rows.append(h[:n])
+            self.it += n
+            if s_:
+                break
+        hist = np.concatenate(rows, axis=0) if rows else None
         return hist, st
 
     def forces(self, isurf: int = 1, xmom=(0.25, 0.0, 0.0), lngth=(1.0, None, 1.0)) -> np.ndarray:

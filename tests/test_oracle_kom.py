@@ -263,3 +263,27 @@ def test_kom_multigrid_accelerates(oracle_mod):
         assert np.isfinite(rows).all()
         out[nlevel] = rows[-1, 0] / rows[0, 0]
     assert out[3] < 0.5 * out[1], out
+
+
+def test_cfl_ramps():
+    """bdeltat's k-omega CFL ramps (src/cosa.f90:4763-4815): mode 1 holds its
+    value between cycle 1 and every 100th cycle and grows cubically then
+    linearly; mode 2 is piecewise linear; both are continuous at the
+    segment ends and reach the final CFL."""
+    from cosa_b200.params import cfl_ramp
+    nc, c, t = (0, 100, 600, 1200), (0.5, 1.5, 3.0), (0.4, 1.0, 2.0)
+    cur = None
+    seen = []
+    for m in range(1, 1401):
+        cur = cfl_ramp(m, 1, nc, c, t, cur)
+        seen.append(cur)
+    assert seen[0] == (0.5, 0.4) and seen[1399] == (3.0, 2.0)
+    assert seen[149] == seen[100]                       # held between updates (cycles 101..199)
+    np.testing.assert_allclose(cfl_ramp(600, 1, nc, c, t), (1.5, 1.0), rtol=1e-12)
+    np.testing.assert_allclose(cfl_ramp(900, 1, nc, c, t), (2.25, 1.5), rtol=1e-12)
+    nc2 = (50, 150, 300, 500)
+    np.testing.assert_allclose(cfl_ramp(50, 2, nc2, c, t), (0.5, 0.4))
+    np.testing.assert_allclose(cfl_ramp(100, 2, nc2, c, t), (1.0, 0.7), rtol=1e-12)
+    np.testing.assert_allclose(cfl_ramp(200, 2, nc2, c, t), (1.5, 1.0))
+    np.testing.assert_allclose(cfl_ramp(400, 2, nc2, c, t), (2.25, 1.5), rtol=1e-12)
+    np.testing.assert_allclose(cfl_ramp(600, 2, nc2, c, t), (3.0, 2.0))
