@@ -618,6 +618,21 @@ int irs_sweeps(cosa_ctx *c, LevelState &L, double *res, const double *ores, cons
       if (r) return r;
       continue;
     }
+    bool all_thomas = true;
+    for (const DevBlock &x : L.hb) all_thomas &= !(len_of(x) >= kPcrMinLen && len_of(x) <= kPcrMaxLen);
+    if (all_thomas) {
+      // Thomas sweeps, one thread per line, all blocks in one launch
+      int64_t lmax = 1;
+      for (const DevBlock &x : L.hb) lmax = std::max<int64_t>(lmax, lines_of(x) * S);
+      const dim3 g(grid_x(lmax, L.nb) * 2, L.nb);  // 128-thread CTAs
+      const BlockList bl{L.d_blocks};
+      if (d == 1) k_irs_line<1><<<g, 128, 0, c->s>>>(bl, npde, S, res, src, bt, eps, vs, ve, with_halo, L.d_irs_scr);
+      else if (d == 2) k_irs_line<2><<<g, 128, 0, c->s>>>(bl, npde, S, res, src, bt, eps, vs, ve, with_halo, L.d_irs_scr);
+      else k_irs_line<3><<<g, 128, 0, c->s>>>(bl, npde, S, res, src, bt, eps, vs, ve, with_halo, L.d_irs_scr);
+      const int r = after_launch(c);
+      if (r) return r;
+      continue;
+    }
     for (const DevBlock &x : L.hb) {
       const int len = len_of(x);
       const int64_t nl = lines_of(x);
@@ -1733,14 +1748,12 @@ int cosa_gpu_fixq(cosa_ctx *c, int32_t nl, double *q) {
   LevelState *L = level(c, nl);
   if (!L || !q) return COSA_ERR_ARG;
   if (c->p.npde < 7) return COSA_OK;  // the reference calls it for k-omega only
-  const int S = 2 * c->p.nharms + 1;
   return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) { k_fixq<<<g, 256, 0, c->s>>>(b, c->d_p, q); });
 }
 
 int cosa_gpu_tur_vis(cosa_ctx *c, int32_t nl, const double *q, double *mut) {
   LevelState *L = level(c, nl);
   if (!L || !q || !mut || c->p.npde < 7) return COSA_ERR_ARG;
-  const int S = 2 * c->p.nharms + 1;
   return for_blocks(c, *L, cnt_all, [&](auto b, dim3 g) { k_tur_vis<<<g, 256, 0, c->s>>>(b, c->d_p, q, mut); });
 }
 

@@ -141,7 +141,6 @@ __global__ void k_deltat(BS bs_, const cosa_params *__restrict__ Pp, double *__r
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
   const int64_t ncell = (int64_t)ni * nj * nk * S;
-  const double zeta = 0.4;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
     int64_t r = t;
     const int i = (int)(r % ni) + 1; r /= ni;
