@@ -62,7 +62,7 @@ def run(kind="duct", cells=4e6, seed=3, nlevel=3, drop=1e-8, max_cycles=20000, c
         s.close()
     a, b = fields["fp64"], fields["mixed"]
     # density, momentum (the vector: a component that is zero in a
-    # quasi-2D flow is judged against the momentum norm) and energy
+    # quasi-2D flow is measured against the momentum norm) and energy
     groups = {"rho": [0], "momentum": [1, 2, 3], "rhoE": [4]}
     out["l2_rel_diff"] = {k: float(np.linalg.norm(b[:, g] - a[:, g]) / np.linalg.norm(a[:, g]))
                           for k, g in groups.items()}

@@ -32,7 +32,7 @@ def _rel(a, b, case, nvar=5, scale=None):
     """max |a-b| over interior cells, relative to the largest value of each
     variable; the three momentum components share the momentum scale (the
     largest of the three), so a component that is small everywhere (rho w
-    of a quasi-2D flow) is not judged against its own tiny values."""
+    of a quasi-2D flow) is not measured against its own tiny values."""
     A = casekit.interior_cells(case, a, nvar)
     B = casekit.interior_cells(case, b, nvar)
     if scale is None:
