@@ -185,6 +185,20 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(ms: float, dist, torch, device: str) -> float:
+    """The slowest rank's device time: every rank takes part in the same
+    all-reduce (MAX) in the same order."""
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world_size: int, cell_stages_per_rank: float, ms_max: float) -> float:
+    """Whole-job Mcell-stage/s of `world_size` replicas that each did
+    cell_stages_per_rank in at most ms_max milliseconds (weak scaling)."""
+    return world_size * cell_stages_per_rank / (ms_max / 1e3) / 1e6
+
+
 def time_smooth(ctx, steps: int, torch):
     """Device time of `steps` fused cycles with CUDA events on the library's stream."""
     stream = torch.cuda.ExternalStream(ctx.stream())
@@ -327,12 +341,8 @@ def main():
     clocks = clk.stop()
     launches = ctx.launch_count(reset=True)
     torch.cuda.synchronize()
-    ms_max = ms
-    if pg:
-        t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = ws * ncells * nstage * args.steps / (ms_max / 1e3) / 1e6
+    ms_max = max_over_ranks(ms, pg, torch, f"cuda:{dev}") if pg else ms
+    value = replica_throughput(ws, ncells * nstage * args.steps, ms_max)
 
     # ---- kernel roofline: event-timed pass right after the timed region ----------
     kms, kcnt = ctx.profile(1, 3)
