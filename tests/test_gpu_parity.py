@@ -418,6 +418,50 @@ def test_split_schedule_matches_oracle(oracle_mod, which):
     ctx.close()
 
 
+def _schedule_run(case, q, schedule, ncyc, nsnap=1, vol=None, si=None, sj=None, sk=None):
+    ctx = gpu.Context([case.tables], case.params)
+    dq_ = ctx.alloc_p3().upload(q)
+    m = [ctx.alloc_p2().upload(a) for a in (si, sj, sk)]
+    extra = {} if vol is None else dict(vol=ctx.alloc_p1().upload(vol))
+    ctx.bind_level(1, q=dq_, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(nsnap=nsnap), si=m[0], sj=m[1], sk=m[2],
+                   **extra)
+    ctx.set_schedule(1, schedule)
+    hist, st = ctx.smooth(1, ncyc, 1, 1)
+    out = dq_.download()
+    ctx.close()
+    return out, hist, st
+
+
+@pytest.mark.parametrize("which", ["channel_extrap_nk5", "partitioned", "duct", "naca_far1", "hb1"])
+@pytest.mark.parametrize("ilimf", [1, 2, 3, 4])
+def test_split_schedule_bits_equal_tile(oracle_mod, which, ilimf):
+    """In FP64 the face-split schedule computes the tile kernel's arithmetic
+    with the same device functions in the same order: the states of both
+    schedules are bit for bit the same, for every limiter, strong
+    boundaries, cuts and harmonic-balance snapshots; the residual norms,
+    summed in a different order, agree to rounding.  (The mixed path is not
+    bit-equal across schedules; it is held to its own tolerance against
+    FP64 elsewhere.)"""
+    if which == "hb1":
+        case = _hb_case(1)
+        q = _hb_state(case, 21)
+        nsnap = 3
+    else:
+        case = FUSED_CASES[which]()
+        q = cases.perturbed_state(case, seed=13)
+        nsnap = 1
+    case.params.ilimf = ilimf
+    O = oracle_mod.OracleLevel(case.tables, case.params)
+    si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
+    kw = dict(nsnap=nsnap, vol=vol if which == "hb1" else None, si=si, sj=sj, sk=sk)
+    q0, h0, st0 = _schedule_run(case, q, 0, 3, **kw)
+    q1, h1, st1 = _schedule_run(case, q, 1, 3, **kw)
+    assert st0 == 0 and st1 == 0
+    assert np.array_equal(q0, q1)
+    # the norms' partial sums are reduced in a different order per schedule
+    np.testing.assert_allclose(h1, h0, rtol=1e-12, atol=0)
+
+
 def test_autotune_restores_state_and_picks_a_schedule(oracle_mod):
     case = casekit.small_duct()
     O, ctx, (si, sj, sk, vol), q = _setup(case, oracle_mod, seed=3)
