@@ -1344,7 +1344,9 @@ int cosa_gpu_resg_rms(cosa_ctx *c, int32_t nl, const double *res, const double *
   if ((r = ensure_hist(c, 1))) return r;
   int64_t ncell = 0;
   for (auto &b : L->hb) ncell += (int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1);
-  k_rms_final<<<1, 256, 0, c->s>>>(L->d_part, L->nb * 64, c->p.npde, (double)ncell, c->d_hist, nullptr, 1);
+  // resg_rms_hb: every snapshot, divided by ncell * dim5 (src/cosa.f90:4620-4626)
+  const double cnt = (double)ncell * (c->p.harbal ? 2 * c->p.nharms + 1 : 1);
+  k_rms_final<<<1, 256, 0, c->s>>>(L->d_part, L->nb * 64, c->p.npde, cnt, c->d_hist, nullptr, 1);
   if ((r = after_launch(c))) return r;
   CK(cudaMemcpyAsync(resrms, c->d_hist, (c->p.npde + 1) * sizeof(double), cudaMemcpyDeviceToHost, c->s));
   CK(cudaStreamSynchronize(c->s));
@@ -1596,7 +1598,46 @@ int launch_prol(cosa_ctx *c, LevelState &L1, LevelState &L2, double *q1, const d
   return COSA_OK;
 }
 
-// restrict(nl), Euler branch (src/cosa.f90:2672-2755)
+int launch_rest2_ho(cosa_ctx *c, LevelState &L1, LevelState &L2, double *rhs2, const double *res1) {
+  const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
+  for (int b = 0; b < L1.nb; ++b) {
+    const DevBlock &g = L2.hb[b];
+    k_rest2_ho<<<grid_for((int64_t)(g.im - 1) * (g.jm - 1) * (g.km - 1) * npde * S), 256, 0, c->s>>>(
+        L1.hb[b], g, npde, S, rhs2, res1);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int launch_bc_res(cosa_ctx *c, LevelState &L, double *res) {
+  if (L.n_bc_items == 0) return COSA_OK;
+  const int S = 2 * c->p.nharms + 1;
+  k_bc_res<<<grid_for((int64_t)L.n_bc_items * c->p.npde * S), 256, 0, c->s>>>(L.d_blocks, L.d_items, L.n_bc_items,
+                                                                            c->p.npde, S, res);
+  return after_launch(c);
+}
+
+// rest2 with ho_rest (src/cosa.f90:2742-2751): the fine residual's first halo
+// layer as smooth() leaves it (zeroed every stage, src/cosa.f90:1786-1792) or,
+// with k-omega, filled by cutman_q, bc_res, q_edges and q_corns
+int issue_rest2_ho(cosa_ctx *c, LevelState &L1, LevelState &L2, int nl, double *rhs2, double *res1) {
+  const int nvs = c->p.npde * (2 * c->p.nharms + 1);
+  int r = 0;
+  for (int b = 0; b < L1.nb; ++b) {
+    const DevBlock &x = L1.hb[b];
+    k_zero_shell1<<<grid_for((int64_t)(x.im + 1) * (x.jm + 1) * (x.km + 1) * nvs), 256, 0, c->s>>>(x, nvs, res1);
+    if ((r = after_launch(c))) return r;
+  }
+  if (c->p.kom) {
+    if ((r = cosa_gpu_cutman_q(c, nl, res1)) || (r = launch_bc_res(c, L1, res1)) ||
+        (r = launch_edges(c, L1, res1, nullptr)) || (r = launch_corns(c, L1, res1, nullptr)))
+      return r;
+  }
+  return launch_rest2_ho(c, L1, L2, rhs2, res1);
+}
+
+// restrict(nl) (src/cosa.f90:2672-2755)
 int issue_restrict(cosa_ctx *c, int nl) {
   LevelState *L1, *L2;
   int r = level_pair(c, nl, L1, L2);
@@ -1607,7 +1648,7 @@ int issue_restrict(cosa_ctx *c, int nl) {
   if ((r = launch_rest1(c, *L1, *L2, A.q, B.q, A.vol, B.vol))) return r;
   if (c->p.kom) {
     // production terms (or mut with prd_all_lvls) restricted as well
-    // (src/cosa.f90:2733-2741); ho_rest is not on this path
+    // (src/cosa.f90:2733-2741)
     const int S = 2 * c->p.nharms + 1;
     std::vector<std::pair<const double *, double *>> fields;
     if (!c->p.prd_all_lvls) {
@@ -1625,6 +1666,7 @@ int issue_restrict(cosa_ctx *c, int nl) {
         if ((r = after_launch(c))) return r;
       }
   }
+  if (c->p.ho_rest) return issue_rest2_ho(c, *L1, *L2, nl, B.rhs, A.res);
   return launch_rest2(c, *L1, *L2, B.rhs, A.res);
 }
 
@@ -1773,6 +1815,18 @@ int cosa_gpu_rest2(cosa_ctx *c, int32_t nl, double *rhs2, const double *res1) {
   return launch_rest2(c, *L1, *L2, rhs2, res1);
 }
 
+int cosa_gpu_rest2_ho(cosa_ctx *c, int32_t nl, double *rhs2, const double *res1) {
+  LevelState *L1, *L2;
+  int r = level_pair(c, nl, L1, L2);
+  if (r) return r;
+  if (!rhs2 || !res1) return COSA_ERR_ARG;
+  return launch_rest2_ho(c, *L1, *L2, rhs2, res1);
+}
+int cosa_gpu_bc_res(cosa_ctx *c, int32_t nl, double *res) {
+  LevelState *L = level(c, nl);
+  if (!L || !res) return COSA_ERR_ARG;
+  return launch_bc_res(c, *L, res);
+}
 int cosa_gpu_prol_bln(cosa_ctx *c, int32_t nl, double *q1, const double *q2) {
   LevelState *L1, *L2;
   int r = level_pair(c, nl, L1, L2);
@@ -2041,7 +2095,8 @@ extern "C" int cosa_gpu_resg_rms_noalloc(int32_t nblocks, const int32_t *dims, i
     op3 += x.P3;
     ncell += (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1);
   }
-  k_rms_final<<<1, 256, 0, s>>>(part, nblocks * per_block, npde, (double)ncell, resrms, nullptr, 1);
+  // resg_rms_hb divides by ncell * dim5 (src/cosa.f90:4620-4626)
+  k_rms_final<<<1, 256, 0, s>>>(part, nblocks * per_block, npde, (double)ncell * S, resrms, nullptr, 1);
   if (cudaGetLastError() != cudaSuccess) return COSA_ERR_CUDA;
   return COSA_OK;
 }

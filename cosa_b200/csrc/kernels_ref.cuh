@@ -394,25 +394,35 @@ __global__ void k_zero_res(BS bs_, const cosa_params *__restrict__ Pp, double *_
   }
 }
 
-// ---- resg_brms partial sums (src/cosa.f90:4503-4582): one partial per CTA -----------
+// ---- resg_brms / resg_brms_hb partial sums (src/cosa.f90:4503-4582, 4629-4697) -------
+// One partial per CTA.  Steady flows sum snapshot 0; harmonic balance sums
+// every snapshot (resg_brms_hb's loop over n = 0..2*nharms, :4680-4690), and
+// the caller divides by ncell * S.
+__device__ __forceinline__ void rms_accumulate(const DevBlock &b, int npde, int S, int nsnap,
+                                               const double *__restrict__ res, const double *__restrict__ rhs,
+                                               double acc[7]) {
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t ncell = (int64_t)ni * nj * nk, nall = ncell * nsnap;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nall; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni) + 1; r /= ni;
+    const int j = (int)(r % nj) + 1; r /= nj;
+    const int k = (int)(r % nk) + 1;
+    const int n = (int)(r / nk);
+    const int64_t c = p3_cell(b, i, j, k);
+    for (int v = 0; v < npde; ++v) {
+      const double tt = res[p3_var(b, npde, S, v + 1, n) + c] - (rhs ? rhs[p3_var(b, npde, S, v + 1, n) + c] : 0.0);
+      acc[v] += tt * tt;
+    }
+  }
+}
+
 __global__ void k_rms_partial(DevBlock b, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
                               const double *__restrict__ rhs, double *__restrict__ part) {
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
-  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
-  const int64_t ncell = (int64_t)ni * nj * nk;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = t;
-    const int i = (int)(r % ni) + 1; r /= ni;
-    const int j = (int)(r % nj) + 1; r /= nj;
-    const int k = (int)r + 1;
-    const int64_t c = p3_cell(b, i, j, k);
-    for (int v = 0; v < npde; ++v) {
-      const double tt = res[p3_var(b, npde, S, v + 1, 0) + c] - (rhs ? rhs[p3_var(b, npde, S, v + 1, 0) + c] : 0.0);
-      acc[v] += tt * tt;
-    }
-  }
+  rms_accumulate(b, npde, S, P.harbal ? S : 1, res, rhs, acc);
   __shared__ double red[7][32];
   for (int v = 0; v < npde; ++v) {
     double x = acc[v];
@@ -431,23 +441,12 @@ __global__ void k_rms_partial(DevBlock b, const cosa_params *__restrict__ Pp, co
 }
 
 // Same partial sums as k_rms_partial with npde and the snapshot count passed
-// by value (the allocation-free entry point has no device parameter block).
+// by value (the allocation-free entry point has no device parameter block);
+// S > 1 sums every snapshot, as resg_brms_hb does.
 __global__ void k_rms_partial_noalloc(DevBlock b, int npde, int S, const double *__restrict__ res,
                                       const double *__restrict__ rhs, double *__restrict__ part) {
-  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
-  const int64_t ncell = (int64_t)ni * nj * nk;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ncell; t += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = t;
-    const int i = (int)(r % ni) + 1; r /= ni;
-    const int j = (int)(r % nj) + 1; r /= nj;
-    const int k = (int)r + 1;
-    const int64_t c = p3_cell(b, i, j, k);
-    for (int v = 0; v < npde; ++v) {
-      const double tt = res[p3_var(b, npde, S, v + 1, 0) + c] - (rhs ? rhs[p3_var(b, npde, S, v + 1, 0) + c] : 0.0);
-      acc[v] += tt * tt;
-    }
-  }
+  rms_accumulate(b, npde, S, S, res, rhs, acc);
   __shared__ double red[7][32];
   for (int v = 0; v < npde; ++v) {
     double x = acc[v];

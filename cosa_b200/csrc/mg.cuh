@@ -63,6 +63,80 @@ __global__ void k_rest2(DevBlock b1, DevBlock b2, int npde, int S, double *__res
   }
 }
 
+// ---- rest2_ho_b (src/cosa.f90:2871-2954) --------------------------------------------
+// one thread per (coarse cell, variable, snapshot): -(27 x the 8 fine cells +
+// 9 x their 24 face neighbours + 3 x the 24 edge neighbours + the 8 corner
+// neighbours) / 64, each sum in the reference's term order
+__global__ void k_rest2_ho(DevBlock b1, DevBlock b2, int npde, int S, double *__restrict__ rhs2,
+                           const double *__restrict__ res1) {
+  const int ni = b2.im - 1, nj = b2.jm - 1, nk = b2.km - 1;
+  const int64_t total = (int64_t)ni * nj * nk * npde * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i2 = (int)(r % ni) + 1; r /= ni;
+    const int j2 = (int)(r % nj) + 1; r /= nj;
+    const int k2 = (int)(r % nk) + 1; r /= nk;
+    const int v = (int)(r % npde) + 1; r /= npde;
+    const int n = (int)r;
+    const int i = 2 * i2 - 1, j = 2 * j2 - 1, k = 2 * k2 - 1;
+    const double *a = res1 + p3_var(b1, npde, S, v, n);
+    auto R = [&](int ii, int jj, int kk) { return __ldg(a + p3_cell(b1, ii, jj, kk)); };
+    const double c27 = R(i, j, k) + R(i, j + 1, k) + R(i + 1, j, k) + R(i + 1, j + 1, k) + R(i, j, k + 1) +
+                       R(i, j + 1, k + 1) + R(i + 1, j, k + 1) + R(i + 1, j + 1, k + 1);
+    const double c9 = R(i - 1, j, k) + R(i - 1, j + 1, k) + R(i + 2, j, k) + R(i + 2, j + 1, k) + R(i - 1, j, k + 1) +
+                      R(i - 1, j + 1, k + 1) + R(i + 2, j, k + 1) + R(i + 2, j + 1, k + 1) + R(i, j - 1, k) +
+                      R(i + 1, j - 1, k) + R(i, j + 2, k) + R(i + 1, j + 2, k) + R(i, j - 1, k + 1) +
+                      R(i + 1, j - 1, k + 1) + R(i, j + 2, k + 1) + R(i + 1, j + 2, k + 1) + R(i, j, k - 1) +
+                      R(i, j + 1, k - 1) + R(i, j, k + 2) + R(i, j + 1, k + 2) + R(i + 1, j, k - 1) +
+                      R(i + 1, j + 1, k - 1) + R(i + 1, j, k + 2) + R(i + 1, j + 1, k + 2);
+    const double c3 = R(i, j - 1, k - 1) + R(i + 1, j - 1, k - 1) + R(i, j + 2, k - 1) + R(i + 1, j + 2, k - 1) +
+                      R(i - 1, j, k - 1) + R(i - 1, j + 1, k - 1) + R(i + 2, j, k - 1) + R(i + 2, j + 1, k - 1) +
+                      R(i, j - 1, k + 2) + R(i + 1, j - 1, k + 2) + R(i, j + 2, k + 2) + R(i + 1, j + 2, k + 2) +
+                      R(i - 1, j, k + 2) + R(i - 1, j + 1, k + 2) + R(i + 2, j, k + 2) + R(i + 2, j + 1, k + 2) +
+                      R(i - 1, j - 1, k) + R(i - 1, j - 1, k + 1) + R(i - 1, j + 2, k) + R(i - 1, j + 2, k + 1) +
+                      R(i + 2, j - 1, k) + R(i + 2, j - 1, k + 1) + R(i + 2, j + 2, k) + R(i + 2, j + 2, k + 1);
+    const double c1 = R(i - 1, j - 1, k - 1) + R(i + 2, j - 1, k - 1) + R(i - 1, j + 2, k - 1) +
+                      R(i + 2, j + 2, k - 1) + R(i - 1, j - 1, k + 2) + R(i + 2, j - 1, k + 2) +
+                      R(i - 1, j + 2, k + 2) + R(i + 2, j + 2, k + 2);
+    rhs2[p3_var(b2, npde, S, v, n) + p3_cell(b2, i2, j2, k2)] = -(27 * c27 + 9 * c9 + 3 * c3 + c1) / 64;
+  }
+}
+
+// zero the first halo layer (the shell i = 0 or imax, j = 0 or jmax, k = 0
+// or kmax of cells 0..imax) of every variable and snapshot of a P3 array
+__global__ void k_zero_shell1(DevBlock b, int nvs, double *__restrict__ a) {
+  const int ni = b.im + 1, nj = b.jm + 1, nk = b.km + 1;
+  const int64_t total = (int64_t)ni * nj * nk * nvs;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ni); r /= ni;
+    const int j = (int)(r % nj); r /= nj;
+    const int k = (int)(r % nk);
+    const int vn = (int)(r / nk);
+    if (i != 0 && i != b.im && j != 0 && j != b.jm && k != 0 && k != b.km) continue;
+    a[b.op3 * nvs + (int64_t)vn * b.P3 + p3_cell(b, i, j, k)] = 0.0;
+  }
+}
+
+// bc_res_bnd (src/bc.f90:2875-2995) over the boundary-condition items of the
+// halo work list: first halo cell = pm * first interior cell, pm = -1 on
+// 15xx walls; one thread per (item, variable, snapshot).  Patches of one
+// block cover distinct halo cells (or repeat the same value), so the items
+// need no ordering.
+__global__ void k_bc_res(const DevBlock *__restrict__ blocks, const HaloItem *__restrict__ items, int nitems,
+                         int npde, int S, double *__restrict__ res) {
+  const int64_t total = (int64_t)nitems * npde * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const HaloItem it = items[t % nitems];
+    const int vn = (int)(t / nitems);
+    const int v = vn % npde + 1, n = vn / npde;
+    const DevBlock b = blocks[it.dblk];
+    const double pm = it.type / 100 == 15 ? -1.0 : 1.0;
+    double *a = res + p3_var(b, npde, S, v, n);
+    a[it.h1] = pm * a[it.c1];
+  }
+}
+
 // ---- q_bedges (src/flux.f90:3913-4263) --------------------------------------------
 // edge ic of a family: target point 0 and fit points 1..3 in the two cross
 // coordinates (x, y) of the family: (i,j) along k, (i,k) along j, (j,k) along i

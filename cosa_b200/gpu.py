@@ -62,7 +62,7 @@ SYMBOLS = [
     "cosa_gpu_vmetrix", "cosa_gpu_viscous_setup", "cosa_gpu_q_face", "cosa_gpu_q_der", "cosa_gpu_vflux",
     "cosa_gpu_lambda_ns", "cosa_gpu_deltat_ns", "cosa_gpu_q_face_mut", "cosa_gpu_rtst", "cosa_gpu_vflux_kom",
     "cosa_gpu_q_der_c", "cosa_gpu_turprod", "cosa_gpu_srckw", "cosa_gpu_update_kom", "cosa_gpu_cutman_mut",
-    "cosa_gpu_autotune", "cosa_gpu_set_schedule", "cosa_gpu_force",
+    "cosa_gpu_autotune", "cosa_gpu_set_schedule", "cosa_gpu_force", "cosa_gpu_rest2_ho", "cosa_gpu_bc_res",
 ]
 
 
@@ -421,6 +421,12 @@ class Context:
 
     def rest2(self, nl, rhs2, res1):
         self._check(load().cosa_gpu_rest2(self.h, nl, _ptr(rhs2.ptr), _ptr(res1.ptr)), "rest2")
+
+    def rest2_ho(self, nl, rhs2, res1):
+        self._check(load().cosa_gpu_rest2_ho(self.h, nl, _ptr(rhs2.ptr), _ptr(res1.ptr)), "rest2_ho")
+
+    def bc_res(self, nl, res):
+        self._check(load().cosa_gpu_bc_res(self.h, nl, _ptr(res.ptr)), "bc_res")
 
     def prol_bln(self, nl, q1, q2):
         self._check(load().cosa_gpu_prol_bln(self.h, nl, _ptr(q1.ptr), _ptr(q2.ptr)), "prol_bln")

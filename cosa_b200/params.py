@@ -62,7 +62,7 @@ class CosaParams(C.Structure):
         ("nstart", C.c_int32), ("npre", C.c_int32), ("npost", C.c_int32), ("ncrs", C.c_int32),
         ("bln_prol", C.c_int32), ("lim_corr", C.c_int32),
         ("lim_prodtke", C.c_int32), ("lim_prodomega", C.c_int32), ("prd_all_lvls", C.c_int32),
-        ("ifixq", C.c_int32), ("wallwilc", C.c_int32), ("reserved_i", C.c_int32),
+        ("ifixq", C.c_int32), ("wallwilc", C.c_int32), ("ho_rest", C.c_int32),
         ("turcmp", C.c_double), ("prdlim", C.c_double), ("roughk", C.c_double),
         ("reserved", C.c_double * 4),
     ]

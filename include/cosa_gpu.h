@@ -105,8 +105,10 @@ typedef struct cosa_params {
      limiter on k (lim_prodtke) and omega (lim_prodomega) with factor prdlim;
      production on every MG level (prd_all_lvls); k/omega floors after each
      update (ifixq); compressibility term switch turcmp (0 or 1); omega wall
-     value (wallwilc 1: Wilcox rough wall with roughness roughk, 0: Menter) */
-  int32_t lim_prodtke, lim_prodomega, prd_all_lvls, ifixq, wallwilc, reserved_i;
+     value (wallwilc 1: Wilcox rough wall with roughness roughk, 0: Menter);
+     ho_rest 1: high-order residual restriction rest2_ho_b in restrict()
+     (src/cosa.f90:2742-2751, 2871-2954), 0: rest2_lo_b */
+  int32_t lim_prodtke, lim_prodomega, prd_all_lvls, ifixq, wallwilc, ho_rest;
   double turcmp, prdlim, roughk;
   double reserved[4];
 } cosa_params;
@@ -194,7 +196,9 @@ int cosa_gpu_resid(cosa_ctx *ctx, int32_t idir, int32_t nl,
    (with k-omega, cosa_gpu_update_kom first) */
 int cosa_gpu_update(cosa_ctx *ctx, int32_t nl, const double *res, double *q,
                     const double *qold, const double *dtvol, double ar);
-/* resg_rms (src/cosa.f90:4458-4582): resrms[0..npde] */
+/* resg_rms (src/cosa.f90:4458-4582): resrms[0..npde]; with harbal the
+   resg_rms_hb norm (src/cosa.f90:4585-4697): every snapshot of res - rhs,
+   divided by ncell * (2 nharms + 1) */
 int cosa_gpu_resg_rms(cosa_ctx *ctx, int32_t nl, const double *res,
                       const double *rhs, double *resrms);
 /* zero (src/util.f90) of a P3 array including halo layer `ext` */
@@ -247,6 +251,14 @@ int cosa_gpu_rest1(cosa_ctx *ctx, int32_t nl, const double *q1, double *q2,
 /* rest2 with lo_rest (src/cosa.f90:2835-2869, 2955-3012):
    rhs2 = -(sum of the 8 fine residuals) */
 int cosa_gpu_rest2(cosa_ctx *ctx, int32_t nl, double *rhs2, const double *res1);
+/* rest2 with ho_rest (src/cosa.f90:2871-2954): rhs2 = -(27/9/3/1-weighted
+   sum of the 4x4x4 fine residuals around each coarse cell) / 64; reads the
+   first halo layer of res1, edges and corners included */
+int cosa_gpu_rest2_ho(cosa_ctx *ctx, int32_t nl, double *rhs2, const double *res1);
+/* bc_res (src/bc.f90:2802-2995): first halo layer of a residual array at
+   every boundary patch = pm * first interior cell, pm = -1 on 15xx walls
+   and +1 elsewhere (all npde equations) */
+int cosa_gpu_bc_res(cosa_ctx *ctx, int32_t nl, double *res);
 /* prol_bln (src/cosa.f90:3282-3313, 3478-3888): q1 += trilinear
    27/9/3/1 interpolation of the coarse correction q2 on fine cells
    0..imax (one halo layer), lim_corr from params for npde = 7 */
@@ -255,8 +267,11 @@ int cosa_gpu_prol_bln(cosa_ctx *ctx, int32_t nl, double *q1, const double *q2);
    vol1 must hold the halo volumes (volex/cutman_v/vol_edges) */
 int cosa_gpu_prol_lin(cosa_ctx *ctx, int32_t nl, double *q1, const double *q2,
                       const double *vol1);
-/* restrict (src/cosa.f90:2672-2755), Euler branch, on bound levels nl and
-   nl+1: rest1 of q into q(nl+1), rest2 of res(nl) into rhs(nl+1) */
+/* restrict (src/cosa.f90:2672-2755) on bound levels nl and nl+1: rest1 of
+   q into q(nl+1), rest2 of res(nl) into rhs(nl+1); with ho_rest the
+   high-order rest2 on res(nl) whose first halo layer is zero (smooth()
+   zeroes it every stage) or, with k-omega, filled by cutman_q, bc_res,
+   q_edges and q_corns as restrict() does */
 int cosa_gpu_restrict(cosa_ctx *ctx, int32_t nl);
 /* prolong (src/cosa.f90:3167-3250) on bound levels nl and nl+1:
    qold(nl+1) = rest1(q(nl)); both coarse states through cons2prim, bc,
@@ -440,7 +455,10 @@ int cosa_gpu_status(cosa_ctx *ctx, int32_t reset);
  * array dims[3*nblocks], node counts as in cosa_level_desc), npde, nharms,
  * the device arrays res and rhs (rhs may be NULL) in the P3 layout, a device
  * output resrms[npde+1] (per-equation RMS, then the total as in resg_rms),
- * and a CUDA stream (NULL = default stream).  The per-CTA partial sums go to
+ * and a CUDA stream (NULL = default stream).  With nharms > 0 the norm is
+ * resg_rms_hb's (src/cosa.f90:4585-4697): the squares of every snapshot are
+ * summed and divided by ncell * (2 nharms + 1); res must then already hold
+ * any time-spectral term.  The per-CTA partial sums go to
  * a static device array of COSA_NOALLOC_MAX_PARTS rows of 8 doubles
  * (256 KiB) that every GPU loading the library holds until exit.  The first
  * call on a device looks up that array's device address; make that first

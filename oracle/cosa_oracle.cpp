@@ -1540,6 +1540,70 @@ void rest2_lo_b(const Level &L1, const Level &L2, int b, double *rhs2a, const do
           }
 }
 
+// rest2_ho_b (src/cosa.f90:2871-2954): rhs2 = -(27 x the 8 fine cells of the
+// coarse cell + 9 x their 24 face neighbours + 3 x the 24 edge neighbours +
+// the 8 corner neighbours) / 64, in the reference's summation order
+void rest2_ho_b(const Level &L1, const Level &L2, int b, double *rhs2a, const double *res1a) {
+  B3 r(const_cast<double *>(res1a), L1, b), rhs2(rhs2a, L2, b);
+  const int im1 = L1.im[b], jm1 = L1.jm[b], km1 = L1.km[b];
+  for (int n = 0; n < L1.S; ++n)
+    for (int v = 1; v <= L1.npde; ++v)
+      for (int k1 = 1; k1 <= km1 - 2; k1 += 2)
+        for (int j1 = 1; j1 <= jm1 - 2; j1 += 2)
+          for (int i1 = 1; i1 <= im1 - 2; i1 += 2) {
+            const int i2 = 1 + i1 / 2, j2 = 1 + j1 / 2, k2 = 1 + k1 / 2;
+            const int i = i1, j = j1, k = k1;
+            const double c27 = r(i, j, k, v, n) + r(i, j + 1, k, v, n) + r(i + 1, j, k, v, n) +
+                               r(i + 1, j + 1, k, v, n) + r(i, j, k + 1, v, n) + r(i, j + 1, k + 1, v, n) +
+                               r(i + 1, j, k + 1, v, n) + r(i + 1, j + 1, k + 1, v, n);
+            const double c9 = r(i - 1, j, k, v, n) + r(i - 1, j + 1, k, v, n) + r(i + 2, j, k, v, n) +
+                              r(i + 2, j + 1, k, v, n) + r(i - 1, j, k + 1, v, n) + r(i - 1, j + 1, k + 1, v, n) +
+                              r(i + 2, j, k + 1, v, n) + r(i + 2, j + 1, k + 1, v, n) + r(i, j - 1, k, v, n) +
+                              r(i + 1, j - 1, k, v, n) + r(i, j + 2, k, v, n) + r(i + 1, j + 2, k, v, n) +
+                              r(i, j - 1, k + 1, v, n) + r(i + 1, j - 1, k + 1, v, n) + r(i, j + 2, k + 1, v, n) +
+                              r(i + 1, j + 2, k + 1, v, n) + r(i, j, k - 1, v, n) + r(i, j + 1, k - 1, v, n) +
+                              r(i, j, k + 2, v, n) + r(i, j + 1, k + 2, v, n) + r(i + 1, j, k - 1, v, n) +
+                              r(i + 1, j + 1, k - 1, v, n) + r(i + 1, j, k + 2, v, n) + r(i + 1, j + 1, k + 2, v, n);
+            const double c3 = r(i, j - 1, k - 1, v, n) + r(i + 1, j - 1, k - 1, v, n) + r(i, j + 2, k - 1, v, n) +
+                              r(i + 1, j + 2, k - 1, v, n) + r(i - 1, j, k - 1, v, n) + r(i - 1, j + 1, k - 1, v, n) +
+                              r(i + 2, j, k - 1, v, n) + r(i + 2, j + 1, k - 1, v, n) + r(i, j - 1, k + 2, v, n) +
+                              r(i + 1, j - 1, k + 2, v, n) + r(i, j + 2, k + 2, v, n) + r(i + 1, j + 2, k + 2, v, n) +
+                              r(i - 1, j, k + 2, v, n) + r(i - 1, j + 1, k + 2, v, n) + r(i + 2, j, k + 2, v, n) +
+                              r(i + 2, j + 1, k + 2, v, n) + r(i - 1, j - 1, k, v, n) + r(i - 1, j - 1, k + 1, v, n) +
+                              r(i - 1, j + 2, k, v, n) + r(i - 1, j + 2, k + 1, v, n) + r(i + 2, j - 1, k, v, n) +
+                              r(i + 2, j - 1, k + 1, v, n) + r(i + 2, j + 2, k, v, n) + r(i + 2, j + 2, k + 1, v, n);
+            const double c1 = r(i - 1, j - 1, k - 1, v, n) + r(i + 2, j - 1, k - 1, v, n) +
+                              r(i - 1, j + 2, k - 1, v, n) + r(i + 2, j + 2, k - 1, v, n) +
+                              r(i - 1, j - 1, k + 2, v, n) + r(i + 2, j - 1, k + 2, v, n) +
+                              r(i - 1, j + 2, k + 2, v, n) + r(i + 2, j + 2, k + 2, v, n);
+            rhs2(i2, j2, k2, v, n) = -(27 * c27 + 9 * c9 + 3 * c3 + c1) / 64;
+          }
+}
+
+// bc_res / bbc_res / bc_res_bnd (src/bc.f90:2802-2995): at every patch the
+// first halo layer = pm * first interior cell, pm = -1 on 15xx walls
+void bc_res_level(const Level &L, double *ra) {
+  for (int b = 0; b < L.nb; ++b) {
+    B3 q(ra, L, b);
+    const int *t = L.bct.data() + L.obct[b];
+    for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
+      Patch pa = patch_of(t + 10 * ibc, L.im[b], L.jm[b], L.km[b]);
+      const double pm = pa.bctyp / 100 == 15 ? -1.0 : 1.0;
+      const int ibcpt = pa.inrout == 1 ? 0 : pa.ijk[pa.idir];
+      const int ibcn = pa.inrout == 1 ? 1 : pa.ijk[pa.idir] - 1;
+      for (int n = 0; n < L.S; ++n)
+        for (int v = 1; v <= L.npde; ++v)
+          for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+            for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+              int a, bb, c, an, bn, cn;
+              pidx(pa, ibcpt, i2, i3, a, bb, c);
+              pidx(pa, ibcn, i2, i3, an, bn, cn);
+              q(a, bb, c, v, n) = pm * q(an, bn, cn, v, n);
+            }
+    }
+  }
+}
+
 // rest4_b (src/cosa.f90:3122-3160): volume-weighted restriction of a
 // scalar P3 field (prd, delpls, divvel or mut)
 void rest4_b(const Level &L1, const Level &L2, int b, const double *f1a, double *f2a, const double *v1a,
@@ -3253,6 +3317,10 @@ void orc_rest1(orc_level *f, orc_level *c, const double *q1, double *q2, const d
 void orc_rest2(orc_level *f, orc_level *c, double *rhs2, const double *res1) {
   for (int b = 0; b < f->L.nb; ++b) rest2_lo_b(f->L, c->L, b, rhs2, res1);
 }
+void orc_rest2_ho(orc_level *f, orc_level *c, double *rhs2, const double *res1) {
+  for (int b = 0; b < f->L.nb; ++b) rest2_ho_b(f->L, c->L, b, rhs2, res1);
+}
+void orc_bc_res(orc_level *h, double *res) { bc_res_level(h->L, res); }
 void orc_prol_bln(orc_level *f, orc_level *c, double *q1, const double *q2, int lim_corr) {
   for (int b = 0; b < f->L.nb; ++b) prol_bln_b(f->L, c->L, b, q1, q2, lim_corr);
 }
@@ -3265,7 +3333,10 @@ int orc_restrict(orc_level *f, orc_level *c, const cosa_params *p, const cosa_le
                  const cosa_level_ptrs *P2) {
   if (is_kom(*p)) return COSA_ERR_UNSUPPORTED;
   orc_rest1(f, c, P1->q, P2->q, P1->vol, P2->vol);
-  orc_rest2(f, c, P2->rhs, P1->res);
+  // ho_rest reads res's first halo layer as smooth() left it (zeroed at
+  // every stage, src/cosa.f90:1786-1792)
+  if (p->ho_rest) orc_rest2_ho(f, c, P2->rhs, P1->res);
+  else orc_rest2(f, c, P2->rhs, P1->res);
   return 0;
 }
 
@@ -3589,8 +3660,8 @@ int orc_smooth_level_rans(orc_level *h, const cosa_params *p, int nl, int nlevel
   return status;
 }
 
-// restrict (src/cosa.f90:2672-2755), k-omega branch without ho_rest: q, the
-// production terms (or mut with prd_all_lvls) and the residual sums
+// restrict (src/cosa.f90:2672-2755), k-omega branch: q, the production terms
+// (or mut with prd_all_lvls) and the residual sums (high order with ho_rest)
 int orc_restrict_rans(orc_level *f, orc_level *c, const cosa_params *p, const cosa_level_ptrs *P1,
                       const cosa_level_ptrs *P2, const orc_vextra *E1, const orc_vextra *E2) {
   orc_rest1(f, c, P1->q, P2->q, P1->vol, P2->vol);
@@ -3601,7 +3672,16 @@ int orc_restrict_rans(orc_level *f, orc_level *c, const cosa_params *p, const co
   } else {
     orc_rest4(f, c, P1->mut, P2->mut, P1->vol, P2->vol);
   }
-  orc_rest2(f, c, P2->rhs, P1->res);
+  if (p->ho_rest) {
+    // halo of the fine residual for the 4x4x4 stencil (src/cosa.f90:2742-2749)
+    cutman_q_level(f->L, P1->res);
+    bc_res_level(f->L, P1->res);
+    orc_q_edges(f, P1->res, nullptr);
+    orc_q_corns(f, P1->res, nullptr);
+    orc_rest2_ho(f, c, P2->rhs, P1->res);
+  } else {
+    orc_rest2(f, c, P2->rhs, P1->res);
+  }
   return 0;
 }
 

@@ -271,6 +271,14 @@ def rest2(Of, Oc, rhs2, res1):
     lib().orc_rest2(Of.h, Oc.h, _p(rhs2), _p(res1))
 
 
+def rest2_ho(Of, Oc, rhs2, res1):
+    lib().orc_rest2_ho(Of.h, Oc.h, _p(rhs2), _p(res1))
+
+
+def bc_res(O, res):
+    lib().orc_bc_res(O.h, _p(res))
+
+
 def prol_bln(Of, Oc, q1, q2, lim_corr=0):
     lib().orc_prol_bln(Of.h, Oc.h, _p(q1), _p(q2), C.c_int(lim_corr))
 

@@ -104,6 +104,18 @@ def test_transfer_operators_match_oracle(oracle_mod):
     ctx.rest2(1, grhs2, g["r1"])
     assert _full_rel(gq2.download(), q2o, lv[1][0], 5, 1) <= TOL
     assert _full_rel(grhs2.download(), rhs2o, lv[1][0], 5, 1) <= TOL
+    # high-order residual restriction (ho_rest): the 4x4x4 stencil reads the
+    # first halo layer of the random fine residual
+    rhs2h = Oc.p3()
+    oracle_mod.rest2_ho(Of, Oc, rhs2h, r1)
+    grhs2h = ctx.alloc_p3(2)
+    ctx.rest2_ho(1, grhs2h, g["r1"])
+    assert _full_rel(grhs2h.download(), rhs2h, lv[1][0], 5, 1) <= TOL
+    # bc_res on the fine level: the whole array, halos included, bit for bit
+    rb = r1.copy()
+    oracle_mod.bc_res(Of, rb)
+    ctx.bc_res(1, g["r1"])
+    np.testing.assert_array_equal(g["r1"].download(), rb)
     # prolongations of a coarse correction into the fine state
     for kind in ("bln", "lin"):
         qo = q1.copy()
@@ -170,6 +182,9 @@ MG_CASES = {
     "partitioned_2lev": (lambda: casekit.small_partitioned(32, 16, 4), 2, {"npre": 2}),
     "duct_2lev": (lambda: casekit.small_duct(), 2, {}),
     "channel_lin": (lambda: casekit.small_channel(32, 16, 4), 2, {"bln_prol": 0}),
+    # high-order residual restriction on 4 blocks (one permuted), 3 levels
+    "partitioned_3lev_ho_rest": (lambda: cases.partitioned_channel(32, 16, 8, isplit=(16,), jsplit=(8,),
+                                                                  permute_last=True), 3, {"ho_rest": 1}),
 }
 
 
@@ -346,6 +361,10 @@ KOM_MG_CASES = {
                                  2, {"irsop": 1}),
     # mut restricted instead of the production terms
     "kom_channel_2lev_prd_all": (lambda: cases.turbulent_channel(32, 16, 4), 2, {"prd_all_lvls": 1}),
+    # high-order residual restriction: the fine residual's halo from cutman_q,
+    # bc_res (negated at the 1500 walls), q_edges and q_corns
+    "kom_partitioned_2lev_ho_rest": (lambda: cases.partitioned_turbulent_channel(32, 16, 4, isplit=(16,),
+                                                                                 jsplit=(8,)), 2, {"ho_rest": 1}),
 }
 
 

@@ -112,6 +112,68 @@ def test_rest1_rest2_values(oracle_mod):
                     np.testing.assert_allclose(R[i2 + 1, j2 + 1, k2 + 1, var, 0], -f.sum(), rtol=1e-14)
 
 
+def test_rest2_ho_weights(oracle_mod):
+    """rest2_ho_b (src/cosa.f90:2871-2954): the 27/9/3/1 weights sum to 512,
+    so a constant residual c restricts to -8 c like rest2_lo; the stencil is
+    symmetric about the centre of the 2x2x2 fine cells, so a field linear in
+    the cell indices (halos included) restricts to -8 x its value there."""
+    case = casekit.small_channel(32, 16, 8)
+    lv, (Of, Oc) = _two_levels(oracle_mod, case)
+    p = case.params
+    for kind in ("const", "linear"):
+        r1 = Of.p3()
+        for v in p3_views(lv[0][0], r1, p.npde, 1):
+            ii, jj, kk = np.meshgrid(*(np.arange(n) - 1.0 for n in v.shape[:3]), indexing="ij")
+            for var in range(p.npde):
+                v[..., var, 0] = 0.7 + var if kind == "const" else 0.3 + 0.11 * ii - 0.07 * jj + 0.05 * kk + var
+        rhs2 = Oc.p3()
+        oracle_mod.rest2_ho(Of, Oc, rhs2, r1)
+        R = p3_views(lv[1][0], rhs2, p.npde, 1)[0]
+        im2, jm2, km2 = lv[1][0].dims[0]
+        for i2 in range(1, im2):
+            for j2 in range(1, jm2):
+                for k2 in range(1, km2):
+                    ic, jc, kc = 2 * i2 - 0.5, 2 * j2 - 0.5, 2 * k2 - 0.5
+                    for var in range(p.npde):
+                        want = 0.7 + var if kind == "const" else 0.3 + 0.11 * ic - 0.07 * jc + 0.05 * kc + var
+                        np.testing.assert_allclose(R[i2 + 1, j2 + 1, k2 + 1, var, 0], -8 * want, rtol=1e-13)
+
+
+def test_bc_res_first_layer(oracle_mod):
+    """bc_res (src/bc.f90:2802-2995): the first halo layer of every patch is
+    the first interior cell, negated on 15xx walls; nothing else changes."""
+    case = cases.duct3d(segs=cases.duct_segments(seed=5, lo=20_000, hi=60_000, choices=tuple(range(8, 33, 8))),
+                        wall=cases.VISCOUS_WALL)
+    p = case.params
+    O = oracle_mod.OracleLevel(case.tables, p)
+    rng = np.random.default_rng(4)
+    r = rng.standard_normal(O.p3().size)
+    r0 = r.copy()
+    oracle_mod.bc_res(O, r)
+    t = case.tables
+    off = 0
+    changed = np.zeros(r.size, dtype=bool)
+    for b, (v, v0) in enumerate(zip(p3_views(t, r, p.npde, 1), p3_views(t, r0, p.npde, 1))):
+        for rec in t.bctopo[t.nbcs[:b].sum():t.nbcs[:b + 1].sum()]:
+            typ, idir, inrout = rec[0], rec[1], rec[2]
+            lo = [rec[3], rec[5], rec[7]]
+            hi = [rec[4], rec[6], rec[8]]
+            pm = -1.0 if typ // 100 == 15 else 1.0
+            dims = t.dims[b]
+            sl_h, sl_c = [], []
+            for d in range(3):
+                if d == idir - 1:
+                    h = 0 if inrout == 1 else dims[d]
+                    c = 1 if inrout == 1 else dims[d] - 1
+                    sl_h.append(slice(h + 1, h + 2)); sl_c.append(slice(c + 1, c + 2))
+                else:
+                    sl_h.append(slice(lo[d] + 1, hi[d] + 2)); sl_c.append(slice(lo[d] + 1, hi[d] + 2))
+            np.testing.assert_array_equal(v[tuple(sl_h)], pm * v0[tuple(sl_c)])
+    # interior cells untouched
+    for v, v0 in zip(p3_views(t, r, p.npde, 1), p3_views(t, r0, p.npde, 1)):
+        np.testing.assert_array_equal(cases.interior(v), cases.interior(v0))
+
+
 def test_prol_bln_reproduces_linear_corrections(oracle_mod):
     """27/9/3/1 weights: constant corrections pass unchanged and corrections
     linear in the coarse index reproduce the line through the fine centres."""
