@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libcosa_gpu.so")
 SOURCES = ["cosa_gpu.cu"]
-HEADERS = ["common.cuh", "physics.cuh", "kernels_ref.cuh", "fused.cuh", "mg.cuh", "visc.cuh", "kom.cuh", "split.cuh",
+HEADERS = ["common.cuh", "physics.cuh", "kernels_ref.cuh", "fused.cuh", "mg.cuh", "visc.cuh", "kom.cuh", "split.cuh", "faces.cuh",
            "force.cuh", "serve.cuh"]
 
 

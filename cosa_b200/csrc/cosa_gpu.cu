@@ -18,6 +18,7 @@
 #include "visc.cuh"
 #include "kom.cuh"
 #include "split.cuh"
+#include "faces.cuh"
 #include "force.cuh"
 
 namespace {
@@ -71,6 +72,8 @@ struct LevelState {
   // set by cosa_gpu_autotune
   int schedule = 0;
   double *d_cflux = nullptr;  // convective face fluxes of the split schedule (3 x F0)
+  FaceTask *d_ftasks = nullptr;  // warp tasks of k_faces_line: i-face tasks first
+  int nftasks = 0, nftasks1 = 0;
   // wall faces of each force surface (key: surface number), built on first use
   struct ForceList {
     ForceFace *d_faces = nullptr;
@@ -752,36 +755,46 @@ int launch_visc(cosa_ctx *c, LevelState &L, const double *qin, bool dt, double *
 
 constexpr int kCellsGX = 64;  // CTAs per block of k_cells (fixed: deterministic norm partials)
 
-// split schedule after the halo fill and the primitive copy: face fluxes,
-// cell epilogue, norm reduction
-int launch_split_tail(cosa_ctx *c, int nl, LevelState &L, StageArgs &A, bool want_rms) {
+// split schedule after the halo fill (and, for viscous flows, the primitive
+// copy): face fluxes, cell epilogue, norm reduction.  qsrc is the stage input
+// (conv: interior cells converted on load) or the primitive copy.
+int launch_split_tail(cosa_ctx *c, int nl, LevelState &L, StageArgs &A, bool want_rms, const double *qsrc,
+                      bool conv) {
   const cosa_params &p = c->p;
   const int S = 2 * p.nharms + 1;
-  int64_t mf = 0;
-  for (const DevBlock &x : L.hb) mf = std::max<int64_t>(mf, (int64_t)x.im * x.jm * x.km * S);
   const bool mixed = p.precision == COSA_PREC_MIXED;
   int r = 0;
   if (A.compute_dt) {
     int64_t mc = 0;
     for (const DevBlock &x : L.hb) mc = std::max<int64_t>(mc, (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * S);
-    k_dt_euler<<<dim3(grid_x(mc, L.nb), L.nb), 256, 0, c->s>>>(L.d_blocks, c->d_p, L.d_qprim, A.si, A.sj, A.sk,
-                                                               A.dtvol, A.bx, A.by, A.bz);
+    const dim3 g(grid_x(mc, L.nb), L.nb);
+    if (conv)
+      k_dt_euler<true><<<g, 256, 0, c->s>>>(L.d_blocks, c->d_p, qsrc, A.si, A.sj, A.sk, A.dtvol, A.bx, A.by, A.bz);
+    else
+      k_dt_euler<false><<<g, 256, 0, c->s>>>(L.d_blocks, c->d_p, qsrc, A.si, A.sj, A.sk, A.dtvol, A.bx, A.by, A.bz);
     if ((r = after_launch(c))) return r;
   }
   A.part = want_rms ? L.d_part : nullptr;
+  // i-face tasks, then the marching j- and k-face tasks
   auto faces = [&](int b0, int nb, cudaStream_t st) {
-    const dim3 gf(grid_x(mf, nb), 3, nb);
-    if (mixed)
-      k_faces<true><<<gf, 128, 0, st>>>(L.d_blocks, c->d_p, L.d_qprim, A.si, A.sj, A.sk, L.d_strong, L.d_smap,
-                                         A.first_order, L.n0, L.d_cflux, b0);
-    else
-      k_faces<false><<<gf, 128, 0, st>>>(L.d_blocks, c->d_p, L.d_qprim, A.si, A.sj, A.sk, L.d_strong, L.d_smap,
-                                          A.first_order, L.n0, L.d_cflux, b0);
+    (void)b0; (void)nb;
+    const FaceTask *tk[2] = {L.d_ftasks, L.d_ftasks + L.nftasks1};
+    const LinePar lp = make_line_par(p);
+    const int nt[2] = {L.nftasks1, L.nftasks - L.nftasks1};
+#define COSA_FACES_LINE(M, CV, IF)                                                                               \
+  k_faces_line<M, CV, IF><<<(nt[IF ? 0 : 1] + 3) / 4, 128, 0, st>>>(                                           \
+      L.d_blocks, tk[IF ? 0 : 1], nt[IF ? 0 : 1], lp, qsrc, A.si, A.sj, A.sk, L.d_strong, L.d_smap,              \
+      A.first_order, L.n0, L.d_cflux, c->d_status)
+    if (mixed && conv) { COSA_FACES_LINE(true, true, true); COSA_FACES_LINE(true, true, false); }
+    else if (mixed) { COSA_FACES_LINE(true, false, true); COSA_FACES_LINE(true, false, false); }
+    else if (conv) { COSA_FACES_LINE(false, true, true); COSA_FACES_LINE(false, true, false); }
+    else { COSA_FACES_LINE(false, false, true); COSA_FACES_LINE(false, false, false); }
+#undef COSA_FACES_LINE
   };
   auto cells = [&](int b0, int nb, cudaStream_t st) {
     const dim3 gc(kCellsGX, nb);
-    if (want_rms) k_cells<true><<<gc, 256, 0, st>>>(L.d_blocks, c->d_p, A, L.d_qprim, L.d_cflux, L.n0, b0);
-    else k_cells<false><<<gc, 256, 0, st>>>(L.d_blocks, c->d_p, A, L.d_qprim, L.d_cflux, L.n0, b0);
+    if (want_rms) k_cells<true><<<gc, 256, 0, st>>>(L.d_blocks, c->d_p, A, L.d_cflux, L.n0, b0);
+    else k_cells<false><<<gc, 256, 0, st>>>(L.d_blocks, c->d_p, A, L.d_cflux, L.n0, b0);
   };
   // one launch per kernel over all blocks: per-block launches on two streams
   // (cell pass of block b beside the faces of block b+1) measured slower, the
@@ -842,8 +855,9 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   A.compute_dt = compute_dt;
   A.first_order = nl >= p.nl_crs;
   A.update = update;
-  const bool split = L.schedule == 1 && c->nseg == 0 && L.d_cflux && L.d_qprim && !p.rkimp;
-  if (split) {
+  const bool split =
+      L.schedule == 1 && c->nseg == 0 && L.d_cflux && (L.d_qprim || !p.viscous) && L.d_ftasks && !p.rkimp;
+  if (split && p.viscous) {
     // primitive copy (with bprtest) shared by the viscous and convective faces
     int64_t m3 = 0;
     for (const DevBlock &x : L.hb) m3 = std::max<int64_t>(m3, x.P3 * S);
@@ -860,7 +874,7 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
     A.compute_dt = 0;
     A.bx = A.by = A.bz = nullptr;
   }
-  if (split) return launch_split_tail(c, nl, L, A, want_rms);
+  if (split) return launch_split_tail(c, nl, L, A, want_rms, p.viscous ? L.d_qprim : qin, !p.viscous);
   const size_t smem = stage_smem_bytes<kTI, kTJ>();
   if (c->prof.on) cudaEventRecord(c->prof.ev[1][0], c->s);
   // the residual-norm partials are a separate instantiation: their
@@ -2622,12 +2636,52 @@ int launch_rans_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o)
 
 // ---- stage schedule autotuner -----------------------------------------------------------
 namespace {
+// warp tasks of k_faces_line, block after block and snapshot after snapshot:
+// first every d = 1 task (rows in groups of kLineRows, 31 faces per warp),
+// then the d = 2, 3 tasks (lines of 32 lanes in segments of at most kLineSeg
+// faces, the two families of a block back to back)
+constexpr int kLineRows = 16, kLineSeg = 16;
+int build_face_tasks(cosa_ctx *c, LevelState &L) {
+  const int S = 2 * c->p.nharms + 1;
+  std::vector<FaceTask> t;
+  for (int b = 0; b < L.nb; ++b) {
+    const DevBlock &x = L.hb[b];
+    const int nj = x.jm - 1, nk = x.km - 1;
+    for (int n = 0; n < S; ++n)
+      for (int k = 1; k <= nk; ++k)
+        for (int j0 = 1; j0 <= nj; j0 += kLineRows)
+          for (int i0 = 1; i0 <= x.im; i0 += 31)
+            t.push_back(FaceTask{b, 1, n, i0, j0, k, 0, std::min(kLineRows, nj - j0 + 1)});
+  }
+  L.nftasks1 = (int)t.size();
+  for (int b = 0; b < L.nb; ++b) {
+    const DevBlock &x = L.hb[b];
+    const int ni = x.im - 1, nj = x.jm - 1, nk = x.km - 1;
+    for (int n = 0; n < S; ++n) {
+      for (int d = 2; d <= 3; ++d) {
+        const int mx = d == 2 ? x.jm : x.km, nt = d == 2 ? nk : nj;
+        const int nseg = (mx + kLineSeg - 1) / kLineSeg, len = (mx + nseg - 1) / nseg;
+        for (int tb = 1; tb <= nt; ++tb)
+          for (int f0 = 1; f0 <= mx; f0 += len)
+            for (int i0 = 1; i0 <= ni; i0 += 32)
+              t.push_back(FaceTask{b, d, n, i0, 0, tb, f0, std::min(len, mx - f0 + 1)});
+      }
+    }
+  }
+  if (t.size() >= (size_t)1 << 30) return COSA_ERR_UNSUPPORTED;
+  int r = dalloc(c, &L.d_ftasks, t.size());
+  if (r) return r;
+  CK(cudaMemcpy(L.d_ftasks, t.data(), t.size() * sizeof(FaceTask), cudaMemcpyHostToDevice));
+  L.nftasks = (int)t.size();
+  return COSA_OK;
+}
+
 int ensure_split(cosa_ctx *c, LevelState &L) {
   const int S = 2 * c->p.nharms + 1;
   int r = 0;
-  for (const DevBlock &x : L.hb)  // the split kernels index faces of a block in 32 bits
-    if ((int64_t)x.im * x.jm * x.km * S >= (int64_t)1 << 31) return COSA_ERR_UNSUPPORTED;
-  if (!L.d_qprim && (r = dalloc(c, &L.d_qprim, (size_t)L.n3 * 5 * S))) return r;
+  if (!L.d_ftasks && (r = build_face_tasks(c, L))) return r;
+  // the primitive copy only for viscous flows (the viscous set-up allocates it)
+  if (c->p.viscous && !L.d_qprim && (r = dalloc(c, &L.d_qprim, (size_t)L.n3 * 5 * S))) return r;
   if (!L.d_cflux && (r = dalloc(c, &L.d_cflux, (size_t)3 * L.n0 * 5 * S))) return r;
   if (L.npart_cap < L.nb * kCellsGX) {
     drop_graphs(c);

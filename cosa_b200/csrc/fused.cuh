@@ -269,7 +269,7 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
         } else {
           double dp, dm;
           limit_face_nr(ph.ilimf, ph.epslimf, ph.rkap, dlo, dmid, dhi, dp, dm);
-          qr[m] = a2 + dp; ql[m] = a1 + dm;
+          qr[m] = __dadd_rn(a2, dp); ql[m] = __dadd_rn(a1, dm);
         }
       }
       if (ovr_lo) { qr[m] = a1; ql[m] = a1; }

@@ -22,7 +22,7 @@ struct PhysPar {
   double w1, w2, w3;          // entfx_f_w(1:3) as reals
 };
 
-__device__ __forceinline__ PhysPar make_phys(const cosa_params &P) {
+__host__ __device__ __forceinline__ PhysPar make_phys(const cosa_params &P) {
   PhysPar q;
   q.g = P.gamma; q.gm1 = P.gamma - 1; q.g_gm1 = P.gamma / (P.gamma - 1);
   q.rkap = P.rkap; q.epslimf = P.epslimf; q.epslimt = P.epslimt;
@@ -67,12 +67,15 @@ __device__ __forceinline__ void c2p5(double g, double *q) {
   q[1] = u; q[2] = v; q[3] = w;
   q[4] = (g - 1) * (q[4] - rho * (u * u + v * v + w * w) / 2);
 }
-// c2p5 with one reciprocal of rho (fused stage kernel)
+// c2p5 with one reciprocal of rho (fused stage kernels); every rounding is
+// pinned with explicit intrinsics, so the result does not depend on how the
+// compiler contracts it in each kernel that inlines it
 __device__ __forceinline__ void c2p5_nr(double g, double *q) {
   const double rho = q[0], ri = rcp_nr(rho);
-  const double u = q[1] * ri, v = q[2] * ri, w = q[3] * ri;
+  const double u = __dmul_rn(q[1], ri), v = __dmul_rn(q[2], ri), w = __dmul_rn(q[3], ri);
   q[1] = u; q[2] = v; q[3] = w;
-  q[4] = (g - 1) * (q[4] - rho * (u * u + v * v + w * w) / 2);
+  const double q2 = __fma_rn(w, w, __fma_rn(v, v, __dmul_rn(u, u)));
+  q[4] = __dmul_rn(g - 1, __fma_rn(-__dmul_rn(rho, q2), 0.5, q[4]));
 }
 // with k-omega: q[5] = rho k, q[6] = rho omega (divided by rho as well)
 __device__ __forceinline__ void c2p7(double g, double *q) {
@@ -143,20 +146,64 @@ __device__ __forceinline__ void limit_face(int ilim, T eps, T rkap, T dlo, T dmi
   }
 }
 
-// limit_face with the sensor's division taken as a Newton-Raphson reciprocal
-// (ilim 1, the smooth van Albada-type sensor), fused stage kernel
+// The limiter of one cell from its two slopes a = dq(c), b = dq(c+1):
+// dqp(c), the offset to its lower face (limit_face's dqp with dmid = a,
+// dhi = b), and dqm(c+1), the offset to its upper face (limit_face's dqm with
+// dlo = a, dmid = b), in FP64 for the fused stage kernels.  The sensor's
+// division is a Newton-Raphson reciprocal; every rounding is pinned with
+// explicit intrinsics (fixed contraction), so the tile kernel (two cells per
+// face) and the line-marching face kernel (one cell at a time) give the same
+// bits.  ilim 1, 2 and 4 share their sensor between dqp and dqm, as the
+// reference's two expressions coincide (src/flux.f90:3561-3604).
+__device__ __forceinline__ double lim3_nr(double x, double y, double epsq) {
+  // (x (y^2 + 2 e) + y (2 x^2 + e)) / (2 x^2 - x y + 2 y^2 + 3 e), limit_i ilim 3
+  const double xx = __dmul_rn(x, x), yy = __dmul_rn(y, y);
+  const double num = __fma_rn(y, __fma_rn(2.0, xx, epsq), __dmul_rn(x, __fma_rn(2.0, epsq, yy)));
+  const double den = __fma_rn(3.0, epsq, __fma_rn(2.0, yy, __fma_rn(-x, y, __dmul_rn(2.0, xx))));
+  return __ddiv_rn(num, den);
+}
+__device__ __forceinline__ void limit_cell64(int ilim, double eps, double rkap, double a, double b, double &dqp,
+                                             double &dqm) {
+  if (ilim == 1) {
+    const double num = __fma_rn(__dmul_rn(2.0, b), a, eps);
+    const double den = __dadd_rn(__fma_rn(b, b, __dmul_rn(a, a)), eps);
+    const double s = __dmul_rn(num, rcp_nr(den));
+    const double rkp = __fma_rn(rkap, s, 1.0), rkm = __fma_rn(-rkap, s, 1.0);
+    dqp = __dmul_rn(__dmul_rn(-s, __fma_rn(rkp, a, __dmul_rn(rkm, b))), 0.25);
+    dqm = __dmul_rn(__dmul_rn(s, __fma_rn(rkm, a, __dmul_rn(rkp, b))), 0.25);
+  } else if (ilim == 0) {
+    const double rkp = 1 + rkap, rkm = 1 - rkap;
+    dqp = __dmul_rn(-__fma_rn(rkp, a, __dmul_rn(rkm, b)), 0.25);
+    dqm = __dmul_rn(__fma_rn(rkm, a, __dmul_rn(rkp, b)), 0.25);
+  } else if (ilim == 2) {
+    const double rkp = 1 + rkap, rkm = 1 - rkap;
+    const double bb = (3.0 - rkap) / (1.0 - rkap);
+    const double sg = (copysign(1.0, a) + copysign(1.0, b)) * 0.5;  // -1, 0 or 1: exact
+    const double dqmx = sg * fmin(fabs(a), __dmul_rn(fabs(b), bb));
+    const double dqpx = sg * fmin(fabs(b), __dmul_rn(fabs(a), bb));
+    dqp = __dmul_rn(-__fma_rn(rkp, dqmx, __dmul_rn(rkm, dqpx)), 0.25);
+    dqm = __dmul_rn(__fma_rn(rkm, dqmx, __dmul_rn(rkp, dqpx)), 0.25);
+  } else if (ilim == 3) {
+    const double epsq = __dmul_rn(eps, eps);
+    dqp = -0.5 * lim3_nr(a, b, epsq);
+    dqm = 0.5 * lim3_nr(b, a, epsq);
+  } else {  // ilim == 4
+    const double epsq = __dmul_rn(eps, eps);
+    const double num = __fma_rn(a, __fma_rn(b, b, epsq), __dmul_rn(b, __fma_rn(a, a, epsq)));
+    const double den = __fma_rn(2.0, epsq, __fma_rn(a, a, __dmul_rn(b, b)));
+    const double x = __ddiv_rn(num, den);
+    dqp = -0.5 * x;
+    dqm = 0.5 * x;
+  }
+}
+
+// limit_face on the fused stage kernels' arithmetic: the two cells' halves
+// of limit_cell64 (dqp from cell f, dqm from cell f-1)
 __device__ __forceinline__ void limit_face_nr(int ilim, double eps, double rkap, double dlo, double dmid, double dhi,
                                               double &dqp, double &dqm) {
-  if (ilim == 1) {
-    double s = (2 * dhi * dmid + eps) * rcp_nr(dhi * dhi + dmid * dmid + eps);
-    double rkp = 1 + rkap * s, rkm = 1 - rkap * s;
-    dqp = -s * (rkp * dmid + rkm * dhi) / 4;
-    s = (2 * dmid * dlo + eps) * rcp_nr(dmid * dmid + dlo * dlo + eps);
-    rkp = 1 + rkap * s; rkm = 1 - rkap * s;
-    dqm = s * (rkm * dlo + rkp * dmid) / 4;
-  } else {
-    limit_face<double>(ilim, eps, rkap, dlo, dmid, dhi, dqp, dqm);
-  }
+  double unused;
+  limit_cell64(ilim, eps, rkap, dmid, dhi, dqp, unused);
+  limit_cell64(ilim, eps, rkap, dlo, dmid, unused, dqm);
 }
 
 // FP32 limiter of the mixed path: limit_face's algebra with fast division

@@ -1,112 +1,29 @@
 // Face-split schedule of the explicit RK stage (an alternative to
 // k_stage_tile, picked per level by the autotuner in cosa_gpu.cu).
 //
-//   k_halo<true>     BC + cut halos (as for the tile kernel)
-//   k_prim           primitive copy of the stage state (visc.cuh)
-//   k_faces<P>       one thread per face of all three families of every
-//                    block: MUSCL + limiter + Roe flux from the primitive
-//                    copy (stencil reads hit L1/L2), face flux to HBM
-//   k_cells<P,RMS>   one thread per cell: flux balance in the reference's
-//                    order, [viscous balance, HB source], [lambda/deltat],
-//                    norms, multigrid forcing, the update
+//   k_halo<true>        BC + cut halos (as for the tile kernel)
+//   [k_prim]            primitive copy of the stage state, viscous flows
+//                       only (their face stencils read it too)
+//   k_faces_line<P>     MUSCL + limiter + Roe flux of every face of the three
+//                       families, threads marching along face lines
+//                       (faces.cuh), face fluxes to HBM
+//   [k_dt_euler]        local time step at stage 1
+//   k_cells<RMS>        one thread per cell: flux balance in the reference's
+//                       order, [viscous balance, HB source], norms, multigrid
+//                       forcing, the update
 //
-// The face and cell arithmetic is the tile kernel's (same device functions,
-// same order), so both schedules give the same bits.  The split schedule
-// moves 3 x 5 face fluxes per cell through HBM (240 B/cell written and read
-// back) but has no shared-memory ring, no barriers and far fewer registers
-// per thread, so many more warps hide the FP64 latency chains.
+// The face and cell arithmetic in FP64 is the tile kernel's (same device
+// functions, same order), so both schedules give the same bits.  The split
+// schedule moves 3 x 5 face fluxes per cell through HBM (120 B/cell written
+// and read back) but has no shared-memory ring and no barriers.
 #pragma once
 #include "fused.cuh"
 #include "visc.cuh"
 
-// MUSCL + limiter + Roe flux of face f along a line of 4 cells w[0..3] =
-// cells f-2..f+1 (the tile kernel's `face`)
-template <bool MIXED>
-__device__ __forceinline__ void split_face(const PhysPar &ph, bool first_order, const double w[4][5], int f, int mx,
-                                           bool slo, bool shi, const double *met, double *F) {
-  double qr[5], ql[5];
-  const bool ovr_lo = (f == 1 && slo), ovr_hi = (f == mx && shi);
-  const bool d_lo = (f - 1 == 1 && slo) || (f - 1 == mx && shi);
-  const bool d_mid = (f == 1 && slo) || (f == mx && shi);
-  const bool d_hi = (f + 1 == 1 && slo) || (f + 1 == mx && shi);
-#pragma unroll
-  for (int m = 0; m < 5; ++m) {
-    const double a0 = w[0][m], a1 = w[1][m], a2 = w[2][m], a3 = w[3][m];
-    if (first_order) {
-      qr[m] = a2; ql[m] = a1;
-    } else {
-      double dlo = a1 - a0, dmid = a2 - a1, dhi = a3 - a2;
-      if (d_lo) dlo = (a1 - a0) * 2;
-      if (d_mid) dmid = (a2 - a1) * 2;
-      if (d_hi) dhi = (a3 - a2) * 2;
-      if (MIXED) {
-        float dp, dm;
-        limit_face_fast(ph.ilimf, (float)ph.epslimf, (float)ph.rkap, (float)dlo, (float)dmid, (float)dhi, dp, dm);
-        qr[m] = a2 + (double)dp; ql[m] = a1 + (double)dm;
-      } else {
-        double dp, dm;
-        limit_face_nr(ph.ilimf, ph.epslimf, ph.rkap, dlo, dmid, dhi, dp, dm);
-        qr[m] = a2 + dp; ql[m] = a1 + dm;
-      }
-    }
-    if (ovr_lo) { qr[m] = a1; ql[m] = a1; }
-    if (ovr_hi) { qr[m] = a2; ql[m] = a2; }
-  }
-  if (MIXED) roe_flux_mixed(ph, met[0], met[1], met[2], met[3], qr, ql, F);
-  else roe_flux_euler(ph, met[0], met[1], met[2], met[3], qr, ql, F);
-}
-
-// grid (x, 3 families, blocks from blk0): the three families of a block run
-// one after the other, so the block's state stays in L2 across them; face
-// flux of family d into cf + (d-1)*n0*5*S (F0 layout per family)
-template <bool MIXED>
-__global__ void __launch_bounds__(128, 5) k_faces(const DevBlock *__restrict__ blocks, const cosa_params *__restrict__ Pp,
-                                               const double *__restrict__ qp, const double *__restrict__ si,
-                                               const double *__restrict__ sj, const double *__restrict__ sk,
-                                               const uint8_t *__restrict__ strong, const StrongMap *__restrict__ smap,
-                                               int first_order, int64_t n0, double *__restrict__ cf, int blk0) {
-  const DevBlock b = blocks[blk0 + blockIdx.z];
-  const int d = blockIdx.y + 1;
-  const cosa_params &P = *Pp;
-  const PhysPar ph = make_phys(P);
-  const int S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
-  const unsigned ni = d == 1 ? b.im : b.im - 1, nj = d == 2 ? b.jm : b.jm - 1, nk = d == 3 ? b.km : b.km - 1;
-  const unsigned total = ni * nj * nk * S;  // < 2^31 per block and family (checked on the host)
-  const double *s = d == 1 ? si : (d == 2 ? sj : sk);
-  double *F0 = cf + (int64_t)(d - 1) * n0 * 5 * S;
-  const StrongMap sm = smap[blk0 + blockIdx.z];
-  const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
-  const int64_t step = d == 1 ? 1 : (d == 2 ? (int64_t)b.I3 : (int64_t)b.I3 * b.J3);
-  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-    // 32-bit decomposition (64-bit division costs several times more instructions)
-    unsigned r = t;
-    const int i = (int)(r % ni) + 1; r /= ni;
-    const int j = (int)(r % nj) + 1; r /= nj;
-    const int k = (int)(r % nk) + 1;
-    const int n = (int)(r / nk), nh = n * P.hbmove;
-    const int f = d == 1 ? i : (d == 2 ? j : k);
-    const int t2 = d == 1 ? j : i, t3 = d == 3 ? j : k;
-    const bool slo = (f <= 2) && strong_at(strong, sm, d - 1, 0, t2, t3);
-    const bool shi = (f >= mx - 1) && strong_at(strong, sm, d - 1, 1, t2, t3);
-    const double *base = qp + p3_var(b, 5, S, 1, n) + p3_cell(b, i, j, k) - 2 * step;
-    double w[4][5];
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-#pragma unroll
-      for (int m = 0; m < 5; ++m) w[p][m] = __ldg(base + p * step + m * b.P3);
-    const int64_t e = p2_idx(b, S2, 1, i, j, k, nh);
-    const double2 a = __ldg(reinterpret_cast<const double2 *>(s + e));
-    const double2 c = __ldg(reinterpret_cast<const double2 *>(s + e + 2));
-    const double met[4] = {a.x, a.y, c.x, c.y};
-    double F[5];
-    split_face<MIXED>(ph, first_order != 0, w, f, mx, slo, shi, met, F);
-#pragma unroll
-    for (int m = 0; m < 5; ++m) F0[f0_idx(b, 5, S, i, j, k, m + 1, n)] = F[m];
-  }
-}
-
 // grid (x, nblocks): local time step of the stage-1 pass (lambdab + bdeltat,
-// src/cosa.f90:1293-1323, 4860-4870) from the primitive copy
+// src/cosa.f90:1293-1323, 4860-4870) from the primitive copy, or (CONV) from
+// the stage input's conservative interior cells converted on load
+template <bool CONV>
 __global__ void k_dt_euler(const DevBlock *__restrict__ blocks, const cosa_params *__restrict__ Pp,
                            const double *__restrict__ qp, const double *__restrict__ si,
                            const double *__restrict__ sj, const double *__restrict__ sk, double *__restrict__ dtv,
@@ -126,6 +43,7 @@ __global__ void k_dt_euler(const DevBlock *__restrict__ blocks, const cosa_param
     double qc[5], sim[4], sip[4], sjm[4], sjp[4], skm[4], skp[4];
 #pragma unroll
     for (int m = 0; m < 5; ++m) qc[m] = qp[p3_var(b, 5, S, m + 1, n) + cell];
+    if (CONV) c2p5_nr(P.gamma, qc);
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       sim[m] = si[p2_idx(b, S2, m + 1, i, j, k, nh)]; sip[m] = si[p2_idx(b, S2, m + 1, i + 1, j, k, nh)];
@@ -149,8 +67,8 @@ __global__ void k_dt_euler(const DevBlock *__restrict__ blocks, const cosa_param
 // in dtvol); per-CTA norm partials at part[(block * gridDim.x + blockIdx.x) * 8 + m]
 template <bool RMS>
 __global__ void __launch_bounds__(256, 2) k_cells(const DevBlock *__restrict__ blocks, const cosa_params *__restrict__ Pp,
-                                               StageArgs A, const double *__restrict__ qp,
-                                               const double *__restrict__ cf, int64_t n0, int blk0) {
+                                               StageArgs A, const double *__restrict__ cf, int64_t n0,
+                                               int blk0) {
   __shared__ double red[8][8];
   const DevBlock b = blocks[blk0 + blockIdx.y];
   const cosa_params &P = *Pp;

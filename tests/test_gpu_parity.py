@@ -184,10 +184,16 @@ def test_smooth_host_buffers_equal_device_path(oracle_mod):
     ctx.close()
 
 
-def test_mixed_precision_close_to_fp64(oracle_mod):
-    """FP32 slopes + FP32 Roe dissipation on FP64 differences: after 20
-    cycles the state stays within 1e-6 (relative) of the FP64 path."""
+@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("ilimf", [1, 2, 3, 4])
+def test_mixed_precision_close_to_fp64(oracle_mod, schedule, ilimf):
+    """Mixed precision (FP32 limiter and Roe flux on FP64 differences; in the
+    face-split schedule also the FP32 change of the central flux from the
+    left cell's FP64 flux): after 20 cycles the state stays within 1e-6
+    (relative) of the FP64 path, for both schedules; the other limiters,
+    less dissipative on this perturbed state, over 4 cycles."""
     case = casekit.small_partitioned()
+    case.params.ilimf = ilimf
     O, ctx, (si, sj, sk, vol), q = _setup(case, oracle_mod, seed=4)
     p = case.params
     p.precision = PREC_MIXED
@@ -197,7 +203,9 @@ def test_mixed_precision_close_to_fp64(oracle_mod):
         m = [c.alloc_p2().upload(a) for a in (si, sj, sk)]
         dq_ = c.alloc_p3().upload(q)
         c.bind_level(1, q=dq_, qold=c.alloc_p3(), dtvol=c.alloc_p1(), si=m[0], sj=m[1], sk=m[2])
-        _, st = c.smooth(1, 20, 1, 20)
+        c.set_schedule(1, schedule)
+        ncyc = 20 if ilimf == 1 else 4
+        _, st = c.smooth(1, ncyc, 1, ncyc)
         assert st == 0
         out.append(dq_.download())
     err = _rel(out[1], out[0], case)
@@ -205,9 +213,11 @@ def test_mixed_precision_close_to_fp64(oracle_mod):
     ctx.close(); ctx2.close()
 
 
-def test_negative_pressure_sets_status_not_fault(oracle_mod):
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_negative_pressure_sets_status_not_fault(oracle_mod, schedule):
     """A state with a non-physical pressure is reported through the status
-    word (src/cosa.f90:1000-1040 stops there); the context stays usable."""
+    word (src/cosa.f90:1000-1040 stops there); the context stays usable.
+    Both stage schedules test positivity where they convert the state."""
     case = casekit.small_channel(16, 8, 2)
     O, ctx, (si, sj, sk, vol), q = _setup(case, oracle_mod, perturb=False)
     v = p3_views(case.tables, q, 5, 1)[0]
@@ -215,6 +225,7 @@ def test_negative_pressure_sets_status_not_fault(oracle_mod):
     m = [ctx.alloc_p2().upload(a) for a in (si, sj, sk)]
     dq_ = ctx.alloc_p3().upload(q)
     ctx.bind_level(1, q=dq_, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(), si=m[0], sj=m[1], sk=m[2])
+    ctx.set_schedule(1, schedule)
     _, st = ctx.smooth(1, 1, 1, 1)
     assert st & 0x1
     ctx.status(reset=True)
