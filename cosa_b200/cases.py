@@ -643,6 +643,23 @@ def naca0012_ogrid(blocks=(96, 160, 160, 96), nj: int = 128, nk: int = 2, rfar: 
     p = params if params is not None else naca_params()
     return _assemble(f"naca0012_{ni}x{nj}x{nk}", nodes, specs, cuts, p)
 
+def naca_pitching(nharms: int = 1, blocks=(64, 64, 64, 64), nj: int = 64, nk: int = 2, mach: float = 0.5,
+                  alpha_deg: float = 0.0, amp_deg: float = 2.5, kred: float = 0.08, xh: float = 0.25,
+                  rfar: float = 30.0, h1: float = 2.0e-3, cfl: float = 2.0, model: str = "euler") -> Case:
+    """Harmonic balance of a NACA 0012 pitching about the quarter chord:
+    theta(t) = amp sin(omega t), omega = 2 kred M (chord 1, a_inf = 1), the
+    O-grid of naca0012_ogrid (default 256 x 64 x 2 cells in 4 blocks), every
+    snapshot on its own rotated grid.  The inviscid run keeps the 1500 wall
+    (force surface 1): its halo holds the wall velocity, and the strong
+    boundary face carries no mass flux.  Explicit 4-stage RK, no IRS."""
+    from .params import set_pitching
+    p = naca_params(model, mach=mach, alpha_deg=alpha_deg, reyno=1.0e6, cfl=cfl, eps_irs=0.0)
+    set_pitching(p, nharms, amp_deg, kred, xh, 0.0)
+    case = naca0012_ogrid(blocks=blocks, nj=nj, nk=nk, rfar=rfar, h1=h1, params=p)
+    case.q0 = _freestream_state(case.tables, p)
+    return case
+
+
 def perturbed_state(case: Case, amp: float = 0.02, seed: int = 0) -> np.ndarray:
     """Free stream plus a smooth seeded perturbation of every conservative
     variable (keeps rho, p > 0); used to exercise limiters and all BC branches."""

@@ -19,6 +19,7 @@
 #include "kom.cuh"
 #include "split.cuh"
 #include "faces.cuh"
+#include "moving.cuh"
 #include "force.cuh"
 
 namespace {
@@ -79,7 +80,7 @@ struct LevelState {
     ForceFace *d_faces = nullptr;
     int nfaces = 0;
     int *d_bstart = nullptr;
-    double *d_buf = nullptr, *d_sums = nullptr;
+    double *d_buf = nullptr, *d_sums = nullptr, *d_xmom = nullptr;
   };
   std::map<int, ForceList> forces;
 };
@@ -205,7 +206,7 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
       const int type = r[0], idir = r[1], inrout = r[2];
       if (idir < 1 || idir > 3) return COSA_ERR_ARG;
       // viscous walls: the laminar, fixed-grid branch of bc_walvis_15
-      const bool wall15 = type / 100 == 15 && !c->p.moving;
+      const bool wall15 = type / 100 == 15 && (!c->p.moving || !c->p.kom);
       const bool ok = type == 80 || type == 4 || type == 14 || type == 21 || type == 91 || type == 30 || type == 31 ||
                       wall15;
       if (!ok) return COSA_ERR_UNSUPPORTED;
@@ -464,6 +465,12 @@ LevelState *level(cosa_ctx *c, int nl) {
   return &c->L[nl - 1];
 }
 
+// face velocities of the bound level's moving grid (all null on fixed grids)
+FaceVel face_vel_of(const cosa_ctx *c, const LevelState &L) {
+  if (!c->p.moving) return FaceVel{{nullptr, nullptr, nullptr}};
+  return FaceVel{{L.ptrs.fvi, L.ptrs.fvj, L.ptrs.fvk}};
+}
+
 int after_launch(cosa_ctx *c) {
   c->launches++;
   return cuda_ok(cudaGetLastError());
@@ -528,9 +535,12 @@ int check_fused_supported(const cosa_params &p) {
   // rkimp: the implicit time-spectral update of harmonic balance, branch
   // without IRS on one level (update_bhb, src/update.f90:1564-1604)
   if (p.rkimp && (!p.harbal || p.irsop != 0 || p.nlevel > 1)) return COSA_ERR_UNSUPPORTED;
-  if (p.npde != 5 || p.kom || p.kom_bsl || p.kom_sst || p.moving ||
+  if (p.npde != 5 || p.kom || p.kom_bsl || p.kom_sst ||
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
+  // moving grids: inviscid harmonic balance of a pitching body, explicit
+  // (the face-split stage schedule carries the face speeds)
+  if (p.moving && (!p.harbal || !p.hbmove || p.viscous || p.rkimp || p.nlevel > 1)) return COSA_ERR_UNSUPPORTED;
   return COSA_OK;
 }
 
@@ -768,10 +778,13 @@ int launch_split_tail(cosa_ctx *c, int nl, LevelState &L, StageArgs &A, bool wan
     int64_t mc = 0;
     for (const DevBlock &x : L.hb) mc = std::max<int64_t>(mc, (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * S);
     const dim3 g(grid_x(mc, L.nb), L.nb);
+    const CellVel cv = p.moving ? CellVel{{L.ptrs.xdot, L.ptrs.ydot, L.ptrs.zdot}} : CellVel{{nullptr, nullptr, nullptr}};
     if (conv)
-      k_dt_euler<true><<<g, 256, 0, c->s>>>(L.d_blocks, c->d_p, qsrc, A.si, A.sj, A.sk, A.dtvol, A.bx, A.by, A.bz);
+      k_dt_euler<true><<<g, 256, 0, c->s>>>(L.d_blocks, c->d_p, qsrc, A.si, A.sj, A.sk, A.dtvol, A.bx, A.by, A.bz,
+                                            cv);
     else
-      k_dt_euler<false><<<g, 256, 0, c->s>>>(L.d_blocks, c->d_p, qsrc, A.si, A.sj, A.sk, A.dtvol, A.bx, A.by, A.bz);
+      k_dt_euler<false><<<g, 256, 0, c->s>>>(L.d_blocks, c->d_p, qsrc, A.si, A.sj, A.sk, A.dtvol, A.bx, A.by, A.bz,
+                                             cv);
     if ((r = after_launch(c))) return r;
   }
   A.part = want_rms ? L.d_part : nullptr;
@@ -785,11 +798,19 @@ int launch_split_tail(cosa_ctx *c, int nl, LevelState &L, StageArgs &A, bool wan
   k_faces_line<M, CV, IF><<<(nt[IF ? 0 : 1] + 3) / 4, 128, 0, st>>>(                                           \
       L.d_blocks, tk[IF ? 0 : 1], nt[IF ? 0 : 1], lp, qsrc, A.si, A.sj, A.sk, L.d_strong, L.d_smap,              \
       A.first_order, L.n0, L.d_cflux, c->d_status)
-    if (mixed && conv) { COSA_FACES_LINE(true, true, true); COSA_FACES_LINE(true, true, false); }
+#define COSA_FACES_MOVING(M, IF)                                                                                \
+  k_faces_line<M, true, IF, true><<<(nt[IF ? 0 : 1] + 3) / 4, 128, 0, st>>>(                                   \
+      L.d_blocks, tk[IF ? 0 : 1], nt[IF ? 0 : 1], lp, qsrc, A.si, A.sj, A.sk, L.d_strong, L.d_smap,              \
+      A.first_order, L.n0, L.d_cflux, c->d_status, fvel)
+    const FaceVel fvel = face_vel_of(c, L);
+    if (p.moving && conv && mixed) { COSA_FACES_MOVING(true, true); COSA_FACES_MOVING(true, false); }
+    else if (p.moving && conv) { COSA_FACES_MOVING(false, true); COSA_FACES_MOVING(false, false); }
+    else if (mixed && conv) { COSA_FACES_LINE(true, true, true); COSA_FACES_LINE(true, true, false); }
     else if (mixed) { COSA_FACES_LINE(true, false, true); COSA_FACES_LINE(true, false, false); }
     else if (conv) { COSA_FACES_LINE(false, true, true); COSA_FACES_LINE(false, true, false); }
     else { COSA_FACES_LINE(false, false, true); COSA_FACES_LINE(false, false, false); }
 #undef COSA_FACES_LINE
+#undef COSA_FACES_MOVING
   };
   auto cells = [&](int b0, int nb, cudaStream_t st) {
     const dim3 gc(kCellsGX, nb);
@@ -832,7 +853,7 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
     if (c->prof.on) cudaEventRecord(c->prof.ev[0][0], c->s);
     k_halo<true><<<grid_for(n), 256, 0, c->s>>>(L.d_blocks, L.d_items, (int)L.items.size(),
                                                 c->d_halo_p ? c->d_halo_p : c->d_p, qin, P.si, P.sj, P.sk,
-                                                c->d_status);
+                                                c->d_status, nullptr, face_vel_of(c, L));
     int r = after_launch(c);
     if (r) return r;
     if (c->prof.on) prof_stop(c, 0);
@@ -875,6 +896,7 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
     A.bx = A.by = A.bz = nullptr;
   }
   if (split) return launch_split_tail(c, nl, L, A, want_rms, p.viscous ? L.d_qprim : qin, !p.viscous);
+  if (p.moving) return COSA_ERR_UNSUPPORTED;  // the tile kernel has no face speeds
   const size_t smem = stage_smem_bytes<kTI, kTJ>();
   if (c->prof.on) cudaEventRecord(c->prof.ev[1][0], c->s);
   // the residual-norm partials are a separate instantiation: their
@@ -1075,6 +1097,10 @@ int ensure_hist(cosa_ctx *c, int rows) {
 
 }  // namespace
 
+namespace {
+int ensure_split(cosa_ctx *c, LevelState &L);
+}
+
 extern "C" {
 
 int64_t cosa_gpu_params_size(void) { return (int64_t)sizeof(cosa_params); }
@@ -1186,6 +1212,12 @@ int cosa_gpu_bind_level(cosa_ctx *c, int32_t nl, const cosa_level_ptrs *ptrs) {
   }
   drop_graphs(c);  // graphs hold the previous pointers
   L->bound = true;
+  if (c->p.moving) {
+    // moving grids run the face-split schedule (the tile kernel has no face speeds)
+    if (!ptrs->fvi || !ptrs->fvj || !ptrs->fvk || !ptrs->xdot || !ptrs->ydot || !ptrs->zdot) return COSA_ERR_ARG;
+    if ((r = ensure_split(c, *L))) return r;
+    L->schedule = 1;
+  }
   return COSA_OK;
 }
 
@@ -1213,7 +1245,8 @@ int cosa_gpu_bc(cosa_ctx *c, int32_t nl, double *q, const double *si, const doub
   if (L->n_bc_items == 0) return COSA_OK;
   const int S = 2 * c->p.nharms + 1;
   k_halo<false><<<grid_for((int64_t)L->n_bc_items * S), 256, 0, c->s>>>(L->d_blocks, L->d_items, L->n_bc_items,
-                                                                       c->d_p, q, si, sj, sk, c->d_status, dist);
+                                                                       c->d_p, q, si, sj, sk, c->d_status, dist,
+                                                                       face_vel_of(c, *L));
   return after_launch(c);
 }
 
@@ -1242,9 +1275,14 @@ int cosa_gpu_lambda(cosa_ctx *c, int32_t nl, const double *q, const double *si, 
                     const double *sk, const double *, double *lam) {
   LevelState *L = level(c, nl);
   if (!L || !q || !lam) return COSA_ERR_ARG;
-  if (c->p.viscous || c->p.moving) return COSA_ERR_UNSUPPORTED;
+  if (c->p.viscous) return COSA_ERR_UNSUPPORTED;
+  // moving grids: the cell grid velocities of the bound level
+  const cosa_level_ptrs &P = L->ptrs;
+  if (c->p.moving && (!P.xdot || !P.ydot || !P.zdot)) return COSA_ERR_ARG;
+  const double *cx = c->p.moving ? P.xdot : nullptr, *cy = c->p.moving ? P.ydot : nullptr;
+  const double *cz = c->p.moving ? P.zdot : nullptr;
   return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) {
-    k_lambda<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, lam);
+    k_lambda<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, lam, cx, cy, cz);
   });
 }
 
@@ -1307,9 +1345,15 @@ int roflux_impl(cosa_ctx *c, int32_t idir, int32_t nl, const double *qr, const d
                 const double *sijk, int mixed) {
   LevelState *L = level(c, nl);
   if (!L || idir < 1 || idir > 3 || !qr || !ql || !flux || !sijk) return COSA_ERR_ARG;
-  if (c->p.moving) return COSA_ERR_UNSUPPORTED;
+  // moving grids: the face velocities of the bound level (FP64 flux, inviscid)
+  const double *fv = nullptr;
+  if (c->p.moving) {
+    if (mixed || c->p.npde != 5) return COSA_ERR_UNSUPPORTED;
+    fv = idir == 1 ? L->ptrs.fvi : (idir == 2 ? L->ptrs.fvj : L->ptrs.fvk);
+    if (!fv) return COSA_ERR_ARG;
+  }
   return for_blocks(c, *L, cnt_all, [&](auto b, dim3 g) {
-    k_roflux<<<g, 256, 0, c->s>>>(b, c->d_p, idir, qr, ql, flux, sijk, mixed);
+    k_roflux<<<g, 256, 0, c->s>>>(b, c->d_p, idir, qr, ql, flux, sijk, mixed, fv);
   });
 }
 }  // namespace
@@ -1508,15 +1552,18 @@ int cosa_gpu_imetrix(cosa_ctx *c, int32_t nl, const double *x, const double *y, 
                      double *sj, double *sk) {
   LevelState *L = level(c, nl);
   if (!L || !x || !y || !z || !si || !sj || !sk) return COSA_ERR_ARG;
-  if (c->p.hbmove || c->p.moving) return COSA_ERR_UNSUPPORTED;
+  // one set of metrics per grid snapshot with hbmove (src/grid.f90:897-1062)
+  const int S2 = 2 * c->p.nharms * c->p.hbmove + 1;
   double *s3[3] = {si, sj, sk};
-  for (int b = 0; b < L->nb; ++b)
-    for (int d = 1; d <= 3; ++d) {
-      const DevBlock &x_ = L->hb[b];
-      k_imetrix<<<grid_for((int64_t)(x_.im + 1) * (x_.jm + 1) * (x_.km + 1)), 256, 0, c->s>>>(x_, d, x, y, z, s3[d - 1]);
-      int r = after_launch(c);
-      if (r) return r;
-    }
+  for (int nh = 0; nh < S2; ++nh)
+    for (int b = 0; b < L->nb; ++b)
+      for (int d = 1; d <= 3; ++d) {
+        const DevBlock &x_ = L->hb[b];
+        k_imetrix<<<grid_for((int64_t)(x_.im + 1) * (x_.jm + 1) * (x_.km + 1)), 256, 0, c->s>>>(x_, d, x, y, z,
+                                                                                                 s3[d - 1], S2, nh);
+        int r = after_launch(c);
+        if (r) return r;
+      }
   return COSA_OK;
 }
 
@@ -1525,10 +1572,80 @@ int cosa_gpu_vols(cosa_ctx *c, int32_t nl, const double *x, const double *y, con
   if (!L || !x || !y || !z || !vol) return COSA_ERR_ARG;
   for (int b = 0; b < L->nb; ++b) {
     const DevBlock &x_ = L->hb[b];
-    k_vols<<<grid_for((int64_t)x_.im * x_.jm * x_.km), 256, 0, c->s>>>(x_, x, y, z, vol);
+    k_vols<<<grid_for((int64_t)x_.im * x_.jm * x_.km), 256, 0, c->s>>>(x_, x, y, z, vol,
+                                                                       2 * c->p.nharms * c->p.hbmove + 1);
     int r = after_launch(c);
     if (r) return r;
   }
+  return COSA_OK;
+}
+
+// movegrid with pitch (src/grid.f90:1783-1966) for every snapshot
+int cosa_gpu_movegrid(cosa_ctx *c, int32_t nl, const double *x0, const double *y0, const double *z0,
+                      const double *dx, const double *dy, const double *dz, double *x, double *y, double *z,
+                      double *xdot, double *ydot, double *zdot) {
+  LevelState *L = level(c, nl);
+  if (!L || !x0 || !y0 || !z0 || !dx || !dy || !x || !y || !z || !xdot || !ydot || !zdot) return COSA_ERR_ARG;
+  (void)dz;
+  const cosa_params &p = c->p;
+  if (!p.moving || !p.harbal || !p.hbmove) return COSA_ERR_UNSUPPORTED;
+  const int S2 = 2 * p.nharms * p.hbmove + 1;
+  // snapshot times and angles (src/input.f90:3182-3192, src/grid.f90:4536-4541)
+  std::vector<PitchSnap> snap(S2);
+  const double pi = 3.14159265358979323846, omega = std::fabs(p.omegas);
+  const double dt = omega > 0 ? 2 * pi / omega / (2 * p.nharms + 1) : 0.0;
+  for (int n = 0; n < S2; ++n) {
+    const double zeit = n * dt, dth = p.dtheta0 * std::sin(p.omegas * zeit);
+    snap[n] = PitchSnap{std::cos(dth), std::sin(dth), std::cos(p.omegas * zeit)};
+  }
+  PitchSnap *d_snap = nullptr;
+  int r = dalloc(c, &d_snap, snap.size());
+  if (r) return r;
+  CK(cudaMemcpyAsync(d_snap, snap.data(), snap.size() * sizeof(PitchSnap), cudaMemcpyHostToDevice, c->s));
+  for (int b = 0; b < L->nb; ++b) {
+    const DevBlock &x_ = L->hb[b];
+    k_pitch<<<grid_for((int64_t)(x_.im + 2) * (x_.jm + 2) * (x_.km + 2) * S2), 256, 0, c->s>>>(
+        x_, S2, d_snap, p.xh, p.yh, p.dtheta0, p.omegas, x0, y0, z0, dx, dy, x, y, z, xdot, ydot, zdot);
+    if ((r = after_launch(c))) return r;
+  }
+  CK(cudaStreamSynchronize(c->s));
+  return COSA_OK;
+}
+
+// face velocities from the node velocities (imetrix_b's moving part)
+int cosa_gpu_face_vel(cosa_ctx *c, int32_t nl, const double *xdot, const double *ydot, const double *zdot,
+                      double *fvi, double *fvj, double *fvk) {
+  LevelState *L = level(c, nl);
+  if (!L || !xdot || !ydot || !zdot || !fvi || !fvj || !fvk) return COSA_ERR_ARG;
+  const int S2 = 2 * c->p.nharms * c->p.hbmove + 1;
+  double *f3[3] = {fvi, fvj, fvk};
+  for (int b = 0; b < L->nb; ++b)
+    for (int d = 1; d <= 3; ++d) {
+      const DevBlock &x_ = L->hb[b];
+      k_face_vel<<<grid_for((int64_t)(x_.im + 1) * (x_.jm + 1) * (x_.km + 1) * S2), 256, 0, c->s>>>(
+          x_, d, S2, xdot, ydot, zdot, f3[d - 1]);
+      int r = after_launch(c);
+      if (r) return r;
+    }
+  return COSA_OK;
+}
+
+// vert2cell_g (src/output.f90:3242-3480) of one node array, in place
+int cosa_gpu_vert2cell(cosa_ctx *c, int32_t nl, double *w) {
+  LevelState *L = level(c, nl);
+  if (!L || !w) return COSA_ERR_ARG;
+  const int S2 = 2 * c->p.nharms * c->p.hbmove + 1;
+  const size_t n = (size_t)L->n2 * S2;
+  double *tmp = nullptr;
+  int r = dalloc(c, &tmp, n);
+  if (r) return r;
+  CK(cudaMemcpyAsync(tmp, w, n * sizeof(double), cudaMemcpyDeviceToDevice, c->s));
+  for (int b = 0; b < L->nb; ++b) {
+    const DevBlock &x_ = L->hb[b];
+    k_vert2cell<<<grid_for((int64_t)(x_.im + 1) * (x_.jm + 1) * (x_.km + 1) * S2), 256, 0, c->s>>>(x_, S2, tmp, w);
+    if ((r = after_launch(c))) return r;
+  }
+  CK(cudaStreamSynchronize(c->s));
   return COSA_OK;
 }
 
@@ -2381,9 +2498,27 @@ int cosa_gpu_force(cosa_ctx *c, int32_t nl, const double *q, const double *x, co
   if (!L || !q || !x || !y || !z || !si || !sj || !sk || !xmom || !lngth || !coef || isurf < 1) return COSA_ERR_ARG;
   const cosa_params &P = c->p;
   if (P.viscous && !vm) return COSA_ERR_ARG;
-  if (P.moving) return COSA_ERR_UNSUPPORTED;
+  if (P.moving && P.viscous) return COSA_ERR_UNSUPPORTED;
   if (lngth[0] == 0.0 || lngth[1] == 0.0 || lngth[2] == 0.0) return COSA_ERR_ARG;
   const int S = 2 * P.nharms + 1, nb = L->nb;
+  // moment centre of every snapshot: on a pitching grid it moves with the
+  // body (src/output.f90:4476-4485), theta_n as in cosa_gpu_movegrid
+  std::vector<double> xms((size_t)3 * S);
+  {
+    const double pi = 3.14159265358979323846, omega = std::fabs(P.omegas);
+    const double dt = omega > 0 ? 2 * pi / omega / S : 0.0;
+    for (int n = 0; n < S; ++n) {
+      double xr = xmom[0], yr = xmom[1];
+      if (P.moving) {
+        const double dth = P.dtheta0 * std::sin(P.omegas * (n * dt));
+        const double dr1 = (xmom[0] - P.xh) * (std::cos(dth) - 1) - (xmom[1] - P.yh) * std::sin(dth);
+        const double dr2 = (xmom[0] - P.xh) * std::sin(dth) + (xmom[1] - P.yh) * (std::cos(dth) - 1);
+        xr = xmom[0] + dr1;
+        yr = xmom[1] + dr2;
+      }
+      xms[3 * n] = xr; xms[3 * n + 1] = yr; xms[3 * n + 2] = xmom[2];
+    }
+  }
   auto it = L->forces.find(isurf);
   if (it == L->forces.end()) {
     // faces of the patches with bctopo(1) == 1500 + isurf - 1, block after
@@ -2418,7 +2553,8 @@ int cosa_gpu_force(cosa_ctx *c, int32_t nl, const double *q, const double *x, co
     fl.nfaces = (int)faces.size();
     int r;
     if ((r = dalloc(c, &fl.d_faces, faces.size())) || (r = dalloc(c, &fl.d_bstart, bstart.size())) ||
-        (r = dalloc(c, &fl.d_buf, (size_t)fl.nfaces * 12 * S)) || (r = dalloc(c, &fl.d_sums, (size_t)nb * 12 * S)))
+        (r = dalloc(c, &fl.d_buf, (size_t)fl.nfaces * 12 * S)) || (r = dalloc(c, &fl.d_sums, (size_t)nb * 12 * S)) ||
+        (r = dalloc(c, &fl.d_xmom, (size_t)3 * S)))
       return r;
     if (!faces.empty())
       CK(cudaMemcpyAsync(fl.d_faces, faces.data(), faces.size() * sizeof(ForceFace), cudaMemcpyHostToDevice, c->s));
@@ -2429,9 +2565,10 @@ int cosa_gpu_force(cosa_ctx *c, int32_t nl, const double *q, const double *x, co
   const LevelState::ForceList &fl = it->second;
   std::vector<double> sums((size_t)nb * 12 * S, 0.0);
   if (fl.nfaces > 0) {
+    CK(cudaMemcpyAsync(fl.d_xmom, xms.data(), xms.size() * sizeof(double), cudaMemcpyHostToDevice, c->s));
     k_force_faces<<<grid_for((int64_t)fl.nfaces * S), 256, 0, c->s>>>(L->d_blocks, c->d_p, fl.d_faces, fl.nfaces, q, x,
-                                                                       y, z, si, sj, sk, vm, L->n0, xmom[0], xmom[1],
-                                                                       xmom[2], fl.d_buf);
+                                                                       y, z, si, sj, sk, vm, L->n0, fl.d_xmom,
+                                                                       fl.d_buf);
     int r = after_launch(c);
     if (r) return r;
     k_force_sum<<<dim3(nb, S), 256, 0, c->s>>>(fl.d_bstart, fl.nfaces, fl.d_buf, fl.d_sums);
@@ -2524,7 +2661,8 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
   if (!L.items.empty()) {
     // BC patches then cuts, last writers as in the reference
     k_halo<false><<<grid_for((int64_t)L.items.size() * S), 256, 0, c->s>>>(
-        L.d_blocks, L.d_items, (int)L.items.size(), c->d_p, q, P.si, P.sj, P.sk, c->d_status, P.dist);
+        L.d_blocks, L.d_items, (int)L.items.size(), c->d_p, q, P.si, P.sj, P.sk, c->d_status, P.dist,
+        face_vel_of(c, L));
     if ((r = after_launch(c))) return r;
   }
   if (o.first_cycle && o.force && irk == 1 && !p.prd_all_lvls) {

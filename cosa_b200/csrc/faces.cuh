@@ -79,15 +79,18 @@ __device__ __forceinline__ void limit_cell32(int ilim, float eps, float rkap, fl
 
 // g(q) . n of a primitive state (rho, u, v, w, p) in FP64: the unit-normal
 // Euler flux roflux_b builds from each face state (src/flux.f90:119-136)
-__device__ __forceinline__ void unit_flux64(double g_gm1, double kx, double ky, double kz, const double *q, double *g) {
-  const double un = q[1] * kx + q[2] * ky + q[3] * kz;
+// (MV: relative to a face moving with normal speed ubn, src/flux.f90:122-148)
+template <bool MV>
+__device__ __forceinline__ void unit_flux64(double g_gm1, double kx, double ky, double kz, const double *q, double *g,
+                                            double ubn) {
+  const double un = MV ? q[1] * kx + q[2] * ky + q[3] * kz - ubn : q[1] * kx + q[2] * ky + q[3] * kz;
   const double ru = q[0] * un;
   const double e = g_gm1 * q[4] + q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) / 2;
   g[0] = ru;
   g[1] = ru * q[1] + q[4] * kx;
   g[2] = ru * q[2] + q[4] * ky;
   g[3] = ru * q[3] + q[4] * kz;
-  g[4] = e * un;
+  g[4] = MV ? e * un + q[4] * ubn : e * un;
 }
 
 // base quantities of the FP32 expansions for the left cell: the state, its
@@ -110,8 +113,11 @@ __device__ __forceinline__ Base32 make_base32(float g_gm1, const float *b) {
 //   D(E)         = G dp + (drho q'^2 + rho (q'^2 - q^2)) / 2
 //   D(E U)       = D(E) U' + E dU
 // with primes for base + d and U = u.n
+// (U is the normal velocity relative to the face; MV adds the change of the
+// energy flux's p ubn term)
+template <bool MV>
 __device__ __forceinline__ void delta_flux32(float g_gm1, const Base32 &B, float U, float rU, float kx, float ky,
-                                             float kz, const float *d, float *dg) {
+                                             float kz, const float *d, float *dg, float ubn) {
   const float dU = d[1] * kx + d[2] * ky + d[3] * kz;
   const float r1 = B.r + d[0], U1 = U + dU;
   const float u1 = B.u + d[1], v1 = B.v + d[2], w1 = B.w + d[3];
@@ -122,13 +128,14 @@ __device__ __forceinline__ void delta_flux32(float g_gm1, const Base32 &B, float
   dg[3] = drU * w1 + rU * d[3] + d[4] * kz;
   const float dq2 = d[1] * (B.u + u1) + d[2] * (B.v + v1) + d[3] * (B.w + w1);
   const float de = g_gm1 * d[4] + 0.5f * (d[0] * (B.q2 + dq2) + B.r * dq2);
-  dg[4] = de * U1 + B.e * dU;
+  dg[4] = MV ? de * U1 + B.e * dU + d[4] * ubn : de * U1 + B.e * dU;
 }
 
 // Roe dissipation |A| (qR - qL) of roflux_b (src/flux.f90:137-230) in FP32
 // from the FP32 face states and their jump dq (computed from differences)
+template <bool MV>
 __device__ __forceinline__ void roe_diss32(const PhysPar &P, float g, float g_gm1, float kx, float ky, float kz,
-                                           const float *qr, const float *ql, const float *dq, float *df) {
+                                           const float *qr, const float *ql, const float *dq, float *df, float ubn) {
   const float rsr = rsqrtf(qr[0]), rsl = rsqrtf(ql[0]);
   const float h0r = g_gm1 * qr[4] * (rsr * rsr) + 0.5f * (qr[1] * qr[1] + qr[2] * qr[2] + qr[3] * qr[3]);
   const float h0l = g_gm1 * ql[4] * (rsl * rsl) + 0.5f * (ql[1] * ql[1] + ql[2] * ql[2] + ql[3] * ql[3]);
@@ -146,10 +153,11 @@ __device__ __forceinline__ void roe_diss32(const PhysPar &P, float g, float g_gm
   const float a = a2 * ria;
   const float drho = dq[0], du = dq[1], dv = dq[2], dw = dq[3], dp = dq[4];
   const float dun = du * kx + dv * ky + dw * kz;
-  float rm123 = fabsf(un), rm4 = fabsf(un + a), rm5 = fabsf(un - a);
+  const float unr = MV ? un - ubn : un;  // normal velocity relative to the face
+  float rm123 = fabsf(unr), rm4 = fabsf(unr + a), rm5 = fabsf(unr - a);
   if (P.efx_setup_f) {
     float rdelta = (float)P.cntrpy_f * ((float)P.w1 * (float)P.entfxctf_f + (float)P.w2 * (sqrtf(q2) + a) +
-                                        (float)P.w3 * 0.2f * (fabsf(un) + a));
+                                        (float)P.w3 * 0.2f * (fabsf(un) + a + (MV ? fabsf(ubn) : 0.0f)));
     rdelta = fmaxf(rdelta, 1.0e-12f);
     if (rm123 <= rdelta && P.efx_all_f) rm123 = 0.5f * (rm123 * rm123 + rdelta * rdelta) / rdelta;
     if (rm4 <= rdelta) rm4 = 0.5f * (rm4 * rm4 + rdelta * rdelta) / rdelta;
@@ -177,16 +185,18 @@ __device__ __forceinline__ void roe_diss32(const PhysPar &P, float g, float g_gm
 // mixed-precision face flux between cells L (FP64 state qL64, FP32 copy bL)
 // and R (FP32 copy bR): dqL / dqR the FP32 offsets of the face states from
 // their cells, dLR = (float)(qR64 - qL64)
+template <bool MV>
 __device__ __forceinline__ void face_flux_mixed(const PhysPar &P, float g, float g_gm1, const double *met,
                                                 const double *qL64, const float *bL, const float *bR,
                                                 const float *dLR, const float *dqL, const float *dqR,
-                                                double *F) {
+                                                double *F, double ubn = 0.0) {
   const double kx = met[0], ky = met[1], kz = met[2], ds = met[3];
-  const float fkx = (float)kx, fky = (float)ky, fkz = (float)kz;
+  const float fkx = (float)kx, fky = (float)ky, fkz = (float)kz, fub = (float)ubn;
   double g64[5];
-  unit_flux64(P.g_gm1, kx, ky, kz, qL64, g64);
+  unit_flux64<MV>(P.g_gm1, kx, ky, kz, qL64, g64, ubn);
   const Base32 B = make_base32(g_gm1, bL);
-  const float U = B.u * fkx + B.v * fky + B.w * fkz, rU = B.r * U;
+  const float U = MV ? B.u * fkx + B.v * fky + B.w * fkz - fub : B.u * fkx + B.v * fky + B.w * fkz;
+  const float rU = B.r * U;
   float dLs[5], dRs[5], ql[5], qr[5], jump[5];
 #pragma unroll
   for (int m = 0; m < 5; ++m) {
@@ -197,9 +207,9 @@ __device__ __forceinline__ void face_flux_mixed(const PhysPar &P, float g, float
     jump[m] = dRs[m] - dLs[m];    // face state R - face state L
   }
   float dgl[5], dgr[5], df[5];
-  delta_flux32(g_gm1, B, U, rU, fkx, fky, fkz, dLs, dgl);
-  delta_flux32(g_gm1, B, U, rU, fkx, fky, fkz, dRs, dgr);
-  roe_diss32(P, g, g_gm1, fkx, fky, fkz, qr, ql, jump, df);
+  delta_flux32<MV>(g_gm1, B, U, rU, fkx, fky, fkz, dLs, dgl, fub);
+  delta_flux32<MV>(g_gm1, B, U, rU, fkx, fky, fkz, dRs, dgr, fub);
+  roe_diss32<MV>(P, g, g_gm1, fkx, fky, fkz, qr, ql, jump, df, fub);
 #pragma unroll
   for (int m = 0; m < 5; ++m) {
     const float t = 0.5f * (dgl[m] + dgr[m] - df[m]);
@@ -294,16 +304,24 @@ __device__ __forceinline__ void ld_met(const double *__restrict__ sp, double *m4
 // the register allocation of each to its own code.  The next row's (IFAM) or
 // the next step's cells and face metrics are loaded one step ahead, and all
 // addresses advance by constant strides.
+// normal speed of face e (its metric record index p2_idx / 4) of family d:
+// sijk(5)*kx + sijk(6)*ky + sijk(7)*kz, roflux_b's order (src/flux.f90:110-113)
+__device__ __forceinline__ double face_ubn(const double *__restrict__ fv, int64_t rec, double kx, double ky,
+                                           double kz) {
+  const double *v = fv + rec * 3;
+  return __ldg(v) * kx + __ldg(v + 1) * ky + __ldg(v + 2) * kz;
+}
+
 #ifndef COSA_LINE_MINB64
 #define COSA_LINE_MINB64 3  // resident CTAs per SM the FP64 instantiations are compiled for
 #endif
-template <bool MIXED, bool CONV, bool IFAM>
+template <bool MIXED, bool CONV, bool IFAM, bool MV = false>
 __global__ void __launch_bounds__(128, MIXED ? 4 : COSA_LINE_MINB64)
 k_faces_line(const DevBlock *__restrict__ blocks, const FaceTask *__restrict__ tasks, int ntasks,
              const LinePar LP, const double *__restrict__ q, const double *__restrict__ si,
              const double *__restrict__ sj, const double *__restrict__ sk, const uint8_t *__restrict__ strong,
              const StrongMap *__restrict__ smap, int first_order, int64_t n0, double *__restrict__ cf,
-             int *status) {
+             int *status, FaceVel FV = FaceVel{{nullptr, nullptr, nullptr}}) {
   const int wid = blockIdx.x * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (wid >= ntasks) return;
   const FaceTask T = tasks[wid];
@@ -330,6 +348,7 @@ k_faces_line(const DevBlock *__restrict__ blocks, const FaceTask *__restrict__ t
                in_p = cl + 1 >= 1 && cl + 1 <= mx - 1;
     const double *pc = qv + p3_cell(b, cl, T.ta, k);
     const double *sp = s + p2_idx(b, S2, 1, cl, T.ta, k, nh);
+    const double *vp = MV ? FV.f[0] + p2_idx(b, S2, 1, cl, T.ta, k, nh) / 4 * 3 : nullptr;
     double *Fp = F0 + f0_idx(b, 5, S, max(cl, 1), T.ta, k, 1, n);  // lane 0 stores nothing
     const int64_t qrow = b.I3, mrow = (int64_t)(b.im + 2) * 4, frow = b.im;
     double A[3][5], met[4];
@@ -363,7 +382,10 @@ k_faces_line(const DevBlock *__restrict__ blocks, const FaceTask *__restrict__ t
         }
         double qr[5], ql[5];
         face_states64(fo, ovr_lo, ovr_hi, A[0], A[1], dqm, dqp, ql, qr);
-        if (face) roe_flux_euler(ph, met[0], met[1], met[2], met[3], qr, ql, Fv);
+        if (face) {
+          const double ubn = MV ? face_ubn(vp, 0, met[0], met[1], met[2]) : 0.0;
+          roe_flux_euler<MV>(ph, met[0], met[1], met[2], met[3], qr, ql, Fv, ubn);
+        }
       } else {
         float dqp[5], dqmn[5], dqm[5], b0[5], bm1[5], dlr[5];
 #pragma unroll
@@ -378,7 +400,10 @@ k_faces_line(const DevBlock *__restrict__ blocks, const FaceTask *__restrict__ t
         }
         float dqL[5], dqR[5];
         face_offsets32(ovr_lo, ovr_hi, dlr, dqm, dqp, dqL, dqR);
-        if (face) face_flux_mixed(ph, g32, gg32, met, A[0], bm1, b0, dlr, dqL, dqR, Fv);
+        if (face) {
+          const double ubn = MV ? face_ubn(vp, 0, met[0], met[1], met[2]) : 0.0;
+          face_flux_mixed<MV>(ph, g32, gg32, met, A[0], bm1, b0, dlr, dqL, dqR, Fv, ubn);
+        }
       }
       if (face) {
 #pragma unroll
@@ -389,6 +414,7 @@ k_faces_line(const DevBlock *__restrict__ blocks, const FaceTask *__restrict__ t
 #pragma unroll
       for (int m = 0; m < 4; ++m) met[m] = metn[m];
       pc += qrow; sp += mrow; Fp += frow;
+      if (MV) vp += mrow / 4 * 3;
     }
   } else {
     // lanes along i; march along d over faces f0 .. f0 + nf - 1
@@ -404,6 +430,7 @@ k_faces_line(const DevBlock *__restrict__ blocks, const FaceTask *__restrict__ t
       const double *p = qv + (d == 2 ? p3_cell(b, i, f0 - 2, tb) : p3_cell(b, i, tb, f0 - 2));
       const double *sp = s + (d == 2 ? p2_idx(b, S2, 1, i, f0, tb, nh) : p2_idx(b, S2, 1, i, tb, f0, nh));
       double *Fp = F0 + (d == 2 ? f0_idx(b, 5, S, i, f0, tb, 1, n) : f0_idx(b, 5, S, i, tb, f0, 1, n));
+      const double *vp = MV ? FV.f[d - 1] + (sp - s) / 4 * 3 : nullptr;  // face velocity of face f0
       auto inner = [&](int cc) { return cc >= 1 && cc <= mx - 1; };
       double qa[5], qb[5], qc[5];
       load_cell<CONV>(p, b.P3, inner(f0 - 2), LP, st, qa);
@@ -450,7 +477,9 @@ k_faces_line(const DevBlock *__restrict__ blocks, const FaceTask *__restrict__ t
           }
           double qr[5], ql[5], Fv[5];
           face_states64(fo, ovr_lo, ovr_hi, qb, qc, dqm, dqp, ql, qr);
-          roe_flux_euler(ph, met[0], met[1], met[2], met[3], qr, ql, Fv);
+          const double ubn = MV ? face_ubn(vp, 0, met[0], met[1], met[2]) : 0.0;
+          roe_flux_euler<MV>(ph, met[0], met[1], met[2], met[3], qr, ql, Fv, ubn);
+          if (MV) vp += mstep / 4 * 3;
 #pragma unroll
           for (int m = 0; m < 5; ++m) Fp[m * fv] = Fv[m];
           Fp += fstep;
@@ -494,7 +523,9 @@ k_faces_line(const DevBlock *__restrict__ blocks, const FaceTask *__restrict__ t
           float dqL[5], dqR[5];
           face_offsets32(ovr_lo, ovr_hi, sB, dqm, dqp, dqL, dqR);
           double Fv[5];
-          face_flux_mixed(ph, g32, gg32, met, qb, fb, fc, sB, dqL, dqR, Fv);
+          const double ubn = MV ? face_ubn(vp, 0, met[0], met[1], met[2]) : 0.0;
+          face_flux_mixed<MV>(ph, g32, gg32, met, qb, fb, fc, sB, dqL, dqR, Fv, ubn);
+          if (MV) vp += mstep / 4 * 3;
 #pragma unroll
           for (int m = 0; m < 5; ++m) Fp[m * fv] = Fv[m];
           Fp += fstep;

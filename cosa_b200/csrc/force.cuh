@@ -24,10 +24,13 @@ __global__ void k_force_faces(const DevBlock *__restrict__ blocks, const cosa_pa
                               const double *__restrict__ x, const double *__restrict__ y,
                               const double *__restrict__ z, const double *__restrict__ si,
                               const double *__restrict__ sj, const double *__restrict__ sk,
-                              const double *__restrict__ vm, int64_t n0, double xm0, double xm1, double xm2,
+                              const double *__restrict__ vm, int64_t n0, const double *__restrict__ xmoms,
                               double *__restrict__ buf) {
+  // xmoms: the moment centre of every snapshot (3 doubles each; on moving
+  // grids carried with the body, src/output.f90:4476-4485); metrics and
+  // nodes of snapshot n hbmove
   const cosa_params &P = *Pp;
-  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
   const int64_t total = (int64_t)nfaces * S;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
     const int f = (int)(t % nfaces), n = (int)(t / nfaces);
@@ -39,7 +42,9 @@ __global__ void k_force_faces(const DevBlock *__restrict__ blocks, const cosa_pa
     const int up = sgn > 0 ? 1 : 0;
     const int mi = F.i + up * di, mj = F.j + up * dj, mk = F.k + up * dk;
     const double *s = d == 1 ? si : (d == 2 ? sj : sk);
-    const int64_t e = p2_idx(b, 1, 1, mi, mj, mk, 0);
+    const int nh = n * P.hbmove;
+    const double xm0 = xmoms[3 * n], xm1 = xmoms[3 * n + 1], xm2 = xmoms[3 * n + 2];
+    const int64_t e = p2_idx(b, S2, 1, mi, mj, mk, nh);
     const double kx = sgn * s[e], ky = sgn * s[e + 1], kz = sgn * s[e + 2], ds = s[e + 3];
     const int64_t hc = p3_cell(b, F.i, F.j, F.k);
     auto Q = [&](int v, int64_t cell) { return q[p3_var(b, npde, S, v, n) + cell]; };
@@ -48,7 +53,7 @@ __global__ void k_force_faces(const DevBlock *__restrict__ blocks, const cosa_pa
     const double pw = (P.gamma - 1) * (Q(5, hc) - u2 * u2 / r / 2 - v2 * v2 / r / 2 - w2 * w2 / r / 2);
     // moment arm: node (ibcw) with the halo cell's index
     const int64_t I2 = b.im + 2, J2 = b.jm + 2;
-    const int64_t gw = b.op2 + F.i + I2 * (F.j + J2 * (int64_t)F.k);
+    const int64_t gw = b.op2 * S2 + (int64_t)nh * I2 * J2 * (b.km + 2) + F.i + I2 * (F.j + J2 * (int64_t)F.k);
     const double xr = x[gw] - xm0, yr = y[gw] - xm1, zr = z[gw] - xm2;
     double o[12];
     o[0] = -pw * kx * ds;

@@ -59,11 +59,18 @@ __device__ __forceinline__ bool strong_at(const uint8_t *flags, const StrongMap 
 }
 
 // ---- k_halo ------------------------------------------------------------------------
+// face velocities of a moving grid, the reference's sijk(5:7) of the three
+// families: (3, 0:imax+1, 0:jmax+1, 0:kmax+1, 0:S2-1) per block at op2*3*S2
+struct FaceVel {
+  const double *f[3];
+};
+
 template <bool CONS>
 __global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__restrict__ items, int nitems,
                        const cosa_params *__restrict__ Pp, double *__restrict__ q,
                        const double *__restrict__ si, const double *__restrict__ sj,
-                       const double *__restrict__ sk, int *status, const double *__restrict__ dist = nullptr) {
+                       const double *__restrict__ sk, int *status, const double *__restrict__ dist = nullptr,
+                       FaceVel fvel = FaceVel{{nullptr, nullptr, nullptr}}) {
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
   const int64_t total = (int64_t)nitems * S;
@@ -97,17 +104,27 @@ __global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__re
       }
       const BcPar B = make_bcpar(Pp[it.ps]);
       int err = 0;
+      // moving walls: the velocity of the wall face (snapshot nh)
+      double wv[3];
+      const double *wvp = nullptr;
+      if ((it.type == 14 || it.type / 100 == 15) && fvel.f[it.idir - 1]) {
+        const int64_t I2 = db.im + 2, J2 = db.jm + 2, K2 = db.km + 2;
+        const int64_t e = ((db.op2 * S2) + (int64_t)(n * P.hbmove) * I2 * J2 * K2 + it.mface) * 3;
+        const double *f = fvel.f[it.idir - 1];
+        wv[0] = f[e]; wv[1] = f[e + 1]; wv[2] = f[e + 2];
+        wvp = wv;
+      }
       switch (it.type) {
         case 80: mask = bc_sym(it.idir, npde, c1, c2, h1, h2); break;
         case 4: mask = bc_extrapol(npde, c1, h1, h2); break;
-        case 14: mask = bc_walinv(npde, nx, ny, nz, c1, c2, h1, h2); break;
+        case 14: mask = bc_walinv(npde, nx, ny, nz, c1, c2, h1, h2, wvp); break;
         case 21: mask = bc_insub(B, nx, ny, nz, c1, c2, h1, h2, &err); break;
         case 91: mask = bc_outsub(B, c1, c2, h1, h2); break;
         case 30: mask = bc_far0(B, nx, ny, nz, c1, h1, h2); break;
         case 31: mask = bc_far1(B, nx, ny, nz, c1, h1, h2); break;
         default:
           if (it.type / 100 == 15) {
-            mask = bc_walvis(P.gamma, c1, c2, h1, h2);
+            mask = bc_walvis(P.gamma, c1, c2, h1, h2, wvp);
             if (npde > 5) {
               // k-omega wall values from the wall distance of the first cell
               if (!dist) { st |= COSA_ERR_ARG; break; }

@@ -104,7 +104,8 @@ __global__ void k_prtest(BS bs_, const cosa_params *__restrict__ Pp, const doubl
 template <class BS>
 __global__ void k_lambda(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
                          const double *__restrict__ si, const double *__restrict__ sj,
-                         const double *__restrict__ sk, double *__restrict__ lam) {
+                         const double *__restrict__ sk, double *__restrict__ lam, const double *__restrict__ cvx = nullptr,
+                         const double *__restrict__ cvy = nullptr, const double *__restrict__ cvz = nullptr) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
@@ -124,8 +125,14 @@ __global__ void k_lambda(BS bs_, const cosa_params *__restrict__ Pp, const doubl
       sjm[m] = sj[p2_idx(b, S2, m + 1, i, j, k, nh)]; sjp[m] = sj[p2_idx(b, S2, m + 1, i, j + 1, k, nh)];
       skm[m] = sk[p2_idx(b, S2, m + 1, i, j, k, nh)]; skp[m] = sk[p2_idx(b, S2, m + 1, i, j, k + 1, nh)];
     }
-    double li, lj, lk;
-    eig_eul(P.gamma, qc, sim, sip, sjm, sjp, skm, skp, li, lj, lk);
+    double li, lj, lk, gv[3];
+    if (cvx) {
+      // cell grid velocity of a moving grid (node-array layout, snapshot nh)
+      const int64_t I2 = b.im + 2, J2 = b.jm + 2, K2 = b.km + 2;
+      const int64_t g = b.op2 * S2 + (int64_t)nh * I2 * J2 * K2 + i + I2 * (j + J2 * (int64_t)k);
+      gv[0] = cvx[g]; gv[1] = cvy[g]; gv[2] = cvz[g];
+    }
+    eig_eul(P.gamma, qc, sim, sip, sjm, sjp, skm, skp, li, lj, lk, cvx ? gv : nullptr);
     lam[p3_var(b, npde, S, 1, n) + c] = li;
     lam[p3_var(b, npde, S, 2, n) + c] = lj;
     lam[p3_var(b, npde, S, 3, n) + c] = lk;
@@ -278,7 +285,7 @@ __global__ void k_muscl_face(BS bs_, const cosa_params *__restrict__ Pp, int d, 
 template <class BS>
 __global__ void k_roflux(BS bs_, const cosa_params *__restrict__ Pp, int d, const double *__restrict__ qr,
                          const double *__restrict__ ql, double *__restrict__ flux, const double *__restrict__ sijk,
-                         int mixed = 0) {
+                         int mixed = 0, const double *__restrict__ fv = nullptr) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const PhysPar ph = make_phys(P);
@@ -304,9 +311,17 @@ __global__ void k_roflux(BS bs_, const cosa_params *__restrict__ Pp, int d, cons
       roe_flux_mixed_tke(ph, sijk[p2_idx(b, S2, 1, i, j, k, nh)], sijk[p2_idx(b, S2, 2, i, j, k, nh)],
                          sijk[p2_idx(b, S2, 3, i, j, k, nh)], sijk[p2_idx(b, S2, 4, i, j, k, nh)], vr, vl, tker, tkel,
                          f);
-    else
-      roe_flux_fp64(ph, sijk[p2_idx(b, S2, 1, i, j, k, nh)], sijk[p2_idx(b, S2, 2, i, j, k, nh)],
-                    sijk[p2_idx(b, S2, 3, i, j, k, nh)], sijk[p2_idx(b, S2, 4, i, j, k, nh)], vr, vl, tker, tkel, f);
+    else {
+      const double kx = sijk[p2_idx(b, S2, 1, i, j, k, nh)], ky = sijk[p2_idx(b, S2, 2, i, j, k, nh)];
+      const double kz = sijk[p2_idx(b, S2, 3, i, j, k, nh)];
+      double ubn = 0.0;
+      if (fv) {
+        // face velocity . normal, roflux_b's order (src/flux.f90:110-113)
+        const int64_t e = p2_idx(b, S2, 1, i, j, k, nh) / 4 * 3;
+        ubn = fv[e] * kx + fv[e + 1] * ky + fv[e + 2] * kz;
+      }
+      roe_flux_fp64(ph, kx, ky, kz, sijk[p2_idx(b, S2, 4, i, j, k, nh)], vr, vl, tker, tkel, f, ubn);
+    }
     for (int m = 0; m < 5; ++m) flux[f0_idx(b, npde, S, i, j, k, m + 1, n)] = f[m];
     if (kom) {
       // turbulence fluxes (src/flux.f90:249-380) with the mean-flow loop's
@@ -466,12 +481,15 @@ __global__ void k_rms_partial_noalloc(DevBlock b, int npde, int S, const double 
 
 // ---- imetrix_b (src/grid.f90:847-1010): face unit normals and areas, fixed grid ----
 // One thread per face of family d; x/y/z are P2 grid arrays (0:imax+1, ...).
+// S2 snapshots of the grid (node arrays (0:imax+1,...,0:S2-1) per block at
+// op2*S2), metrics of snapshot nh
 __global__ void k_imetrix(DevBlock b, int d, const double *__restrict__ x, const double *__restrict__ y,
-                          const double *__restrict__ z, double *__restrict__ s) {
-  const int64_t I2 = b.im + 2, J2 = b.jm + 2;
+                          const double *__restrict__ z, double *__restrict__ s, int S2 = 1, int nh = 0) {
+  const int64_t I2 = b.im + 2, J2 = b.jm + 2, K2 = b.km + 2;
   const int ni = d == 1 ? b.im : b.im - 1, nj = d == 2 ? b.jm : b.jm - 1, nk = d == 3 ? b.km : b.km - 1;
   const int64_t nf = (int64_t)ni * nj * nk;
-  const double *X = x + b.op2, *Y = y + b.op2, *Z = z + b.op2;
+  const int64_t g0 = b.op2 * S2 + (int64_t)nh * I2 * J2 * K2;
+  const double *X = x + g0, *Y = y + g0, *Z = z + g0;
   auto at = [&](const double *A, int i, int j, int k) { return A[i + I2 * (j + J2 * (int64_t)k)]; };
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nf; t += (int64_t)gridDim.x * blockDim.x) {
     int64_t r = t;
@@ -503,18 +521,19 @@ __global__ void k_imetrix(DevBlock b, int d, const double *__restrict__ x, const
       n3 = (dxa * dyb - dya * dxb) / 2;
     }
     const double area = sqrt(n1 * n1 + n2 * n2 + n3 * n3);
-    const int64_t e = (b.op2 + i + I2 * (j + J2 * (int64_t)k)) * 4;
+    const int64_t e = (g0 + i + I2 * (j + J2 * (int64_t)k)) * 4;
     s[e] = n1 / area; s[e + 1] = n2 / area; s[e + 2] = n3 / area; s[e + 3] = area;
   }
 }
 
 // ---- bvols (src/grid.f90:2160-2230): cell volumes (Kordulla-Vinokur) ---------------------
+// the volumes of the first grid snapshot (S2 snapshots stored; rigid motions keep them)
 __global__ void k_vols(DevBlock b, const double *__restrict__ x, const double *__restrict__ y,
-                       const double *__restrict__ z, double *__restrict__ vol) {
+                       const double *__restrict__ z, double *__restrict__ vol, int S2 = 1) {
   const int64_t I2 = b.im + 2, J2 = b.jm + 2, I1 = b.im + 1, J1 = b.jm + 1;
   const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
   const int64_t nc = (int64_t)ni * nj * nk;
-  const double *X = x + b.op2, *Y = y + b.op2, *Z = z + b.op2;
+  const double *X = x + b.op2 * S2, *Y = y + b.op2 * S2, *Z = z + b.op2 * S2;
   auto at = [&](const double *A, int i, int j, int k) { return A[i + I2 * (j + J2 * (int64_t)k)]; };
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nc; t += (int64_t)gridDim.x * blockDim.x) {
     int64_t r = t;

@@ -221,11 +221,11 @@ __device__ __forceinline__ void limit_face_fast(int ilim, float eps, float rkap,
 
 // ---- roflux_b mean-flow face flux (src/flux.f90:45-238), fixed grid ---------------
 // qr/ql: primitive right/left states (rho,u,v,w,p); tker/tkel: TKE (0 for Euler)
+// ubn: the face's normal grid speed on moving grids (src/flux.f90:110-113)
 __device__ __forceinline__ void roe_flux_fp64(const PhysPar &P, double kx, double ky, double kz, double ds,
                                               const double *qr, const double *ql, double tker, double tkel,
-                                              double *flux) {
+                                              double *flux, double ubn = 0.0) {
   const double g = P.g;
-  const double ubn = 0.0;
   const double rhor = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
   const double unr = ur * kx + vr * ky + wr * kz - ubn;
   const double q2r = ur * ur + vr * vr + wr * wr;
@@ -289,17 +289,22 @@ __device__ __forceinline__ void roe_flux_fp64(const PhysPar &P, double kx, doubl
 // Euler face flux for the fused stage: roflux_b's algebra with the TKE terms
 // (zero for Euler) dropped; sqrt(rho), 1/rho, the Roe-average weights, the
 // speed of sound and its inverse come from rsqrt_nr / rcp_nr instead of
-// separate square roots and divisions (last-bit differences).
+// separate square roots and divisions (last-bit differences).  MV: moving
+// face with normal grid speed ubn (src/flux.f90:110-113, 122-189): the normal
+// velocities relative to the face, the energy flux's p ubn and the shifted
+// eigenvalues; the fixed-grid instantiation has none of these terms.
+template <bool MV = false>
 __device__ __forceinline__ void roe_flux_euler(const PhysPar &P, double kx, double ky, double kz, double ds,
-                                               const double *qr, const double *ql, double *flux) {
+                                               const double *qr, const double *ql, double *flux,
+                                               double ubn = 0.0) {
   const double g_gm1 = P.g_gm1, gm1 = P.gm1;
   const double rhor = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
-  const double unr = ur * kx + vr * ky + wr * kz;
+  const double unr = MV ? ur * kx + vr * ky + wr * kz - ubn : ur * kx + vr * ky + wr * kz;
   const double q2r = ur * ur + vr * vr + wr * wr;
   const double rsr = rsqrt_nr(rhor);  // 1/sqrt(rho_R): sqrt(rho_R) and 1/rho_R from it
   const double h0r = g_gm1 * pr * (rsr * rsr) + q2r / 2;
   const double rhol = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4];
-  const double unl = ul * kx + vl * ky + wl * kz;
+  const double unl = MV ? ul * kx + vl * ky + wl * kz - ubn : ul * kx + vl * ky + wl * kz;
   const double q2l = ul * ul + vl * vl + wl * wl;
   const double rsl = rsqrt_nr(rhol);
   const double h0l = g_gm1 * pl * (rsl * rsl) + q2l / 2;
@@ -317,9 +322,11 @@ __device__ __forceinline__ void roe_flux_euler(const PhysPar &P, double kx, doub
   const double a2 = gm1 * (h0 - q2 / 2);
   const double ra = rsqrt_nr(a2);  // 1/a
   const double a = a2 * ra;
-  double rm123 = fabs(un), rm4 = fabs(un + a), rm5 = fabs(un - a);
+  double rm123 = MV ? fabs(un - ubn) : fabs(un), rm4 = MV ? fabs(un + a - ubn) : fabs(un + a);
+  double rm5 = MV ? fabs(un - a - ubn) : fabs(un - a);
   if (P.efx_setup_f) {
-    double rdelta = P.cntrpy_f * (P.w1 * P.entfxctf_f + P.w2 * (sqrt(q2) + a) + P.w3 * 0.2 * (fabs(un) + a));
+    double rdelta = P.cntrpy_f * (P.w1 * P.entfxctf_f + P.w2 * (sqrt(q2) + a) +
+                                  P.w3 * 0.2 * (MV ? fabs(un) + a + fabs(ubn) : fabs(un) + a));
     rdelta = fmax(rdelta, 1.0e-12);
     if (rm123 <= rdelta && P.efx_all_f) rm123 = 0.5 * (rm123 * rm123 + rdelta * rdelta) / rdelta;
     if (rm4 <= rdelta) rm4 = 0.5 * (rm4 * rm4 + rdelta * rdelta) / rdelta;
@@ -346,7 +353,8 @@ __device__ __forceinline__ void roe_flux_euler(const PhysPar &P, double kx, doub
   flux[1] = ((rhor * ur * unr + pr * kx) + (rhol * ul * unl + pl * kx) - df2) * hds;
   flux[2] = ((rhor * vr * unr + pr * ky) + (rhol * vl * unl + pl * ky) - df3) * hds;
   flux[3] = ((rhor * wr * unr + pr * kz) + (rhol * wl * unl + pl * kz) - df4) * hds;
-  flux[4] = (rhor * h0r * unr + rhol * h0l * unl - df5) * hds;
+  if (MV) flux[4] = ((rhor * h0r * unr + pr * ubn) + (rhol * h0l * unl + pl * ubn) - df5) * hds;
+  else flux[4] = (rhor * h0r * unr + rhol * h0l * unl - df5) * hds;
 }
 
 // Mixed precision: the central part (fr + fl) in FP64 from the FP64 face
@@ -482,11 +490,15 @@ __device__ __forceinline__ void roe_flux_mixed_tke(const PhysPar &P, double kx, 
   flux[4] = (rhor * h0r * unr + rhol * h0l * unl - (double)df5) / 2 * ds;
 }
 
-// ---- eig_eul (src/cosa.f90:4183-4233), fixed grid ---------------------------------
+// ---- eig_eul (src/cosa.f90:4183-4233); gv: the cell's grid velocity on
+// moving grids (src/cosa.f90:4225-4229), null on fixed grids ----------------------------
 __device__ __forceinline__ void eig_eul(double g, const double *qc, const double *sim, const double *sip,
                                         const double *sjm, const double *sjp, const double *skm,
-                                        const double *skp, double &lami, double &lamj, double &lamk) {
-  const double rho = qc[0], u = qc[1], v = qc[2], w = qc[3], p = qc[4];
+                                        const double *skp, double &lami, double &lamj, double &lamk,
+                                        const double *gv = nullptr) {
+  const double rho = qc[0], p = qc[4];
+  double u = qc[1], v = qc[2], w = qc[3];
+  if (gv) { u = u - gv[0]; v = v - gv[1]; w = w - gv[2]; }
   const double a = sqrt(g * p / rho);
   const double xix = 0.5 * (sim[0] * sim[3] + sip[0] * sip[3]);
   const double xiy = 0.5 * (sim[1] * sim[3] + sip[1] * sip[3]);
@@ -550,13 +562,16 @@ __device__ __forceinline__ int bc_extrapol(int npde, const double *c1, double *h
   return 3;
 }
 // bc_walinv_14 (src/bc.f90:1457-1675), fixed grid; n = face metric at ibcm
+// wv: the wall face's velocity on moving grids (src/bc.f90:1567-1614), null on
+// fixed grids
 __device__ __forceinline__ int bc_walinv(int npde, double nx, double ny, double nz, const double *c1,
-                                         const double *c2, double *h1, double *h2) {
+                                         const double *c2, double *h1, double *h2, const double *wv = nullptr) {
   const double rhow = (3 * c1[0] - c2[0]) / 2, uw = (3 * c1[1] - c2[1]) / 2;
   const double vw = (3 * c1[2] - c2[2]) / 2, ww = (3 * c1[3] - c2[3]) / 2, pw = (3 * c1[4] - c2[4]) / 2;
   const double un1 = c1[1] * nx + c1[2] * ny + c1[3] * nz;
   const double un2 = c2[1] * nx + c2[2] * ny + c2[3] * nz;
-  const double unw = (3 * un1 - un2) / 2;
+  double unw = (3 * un1 - un2) / 2;
+  if (wv) unw = unw - (wv[0] * nx + wv[1] * ny + wv[2] * nz);
   h1[0] = rhow; h1[1] = uw - unw * nx; h1[2] = vw - unw * ny; h1[3] = ww - unw * nz; h1[4] = pw;
   if (npde > 5) { h1[5] = c1[5]; h1[6] = c1[6]; }
   for (int v = 0; v < npde; ++v) h2[v] = h1[v];
@@ -762,11 +777,14 @@ __device__ __forceinline__ int bc_far1(const BcPar &B, double sx, double sy, dou
   return mask;
 }
 
-__device__ __forceinline__ int bc_walvis(double g, const double *c1, const double *c2, double *h1, double *h2) {
+// wv: the wall face's velocity on moving grids (src/bc.f90:2256-2283), null
+// on fixed grids
+__device__ __forceinline__ int bc_walvis(double g, const double *c1, const double *c2, double *h1, double *h2,
+                                         const double *wv = nullptr) {
   const double p1 = c1[4], p2 = c2[4];
   const double pw = 0.5 * (3 * p1 - p2);
   h1[0] = pow(pw / p1, 1 / g) * c1[0];
-  h1[1] = 0.0; h1[2] = 0.0; h1[3] = 0.0;
+  h1[1] = wv ? wv[0] : 0.0; h1[2] = wv ? wv[1] : 0.0; h1[3] = wv ? wv[2] : 0.0;
   h1[4] = pw;
   for (int v = 0; v < 5; ++v) h2[v] = h1[v];
   return 3;

@@ -23,11 +23,17 @@
 // grid (x, nblocks): local time step of the stage-1 pass (lambdab + bdeltat,
 // src/cosa.f90:1293-1323, 4860-4870) from the primitive copy, or (CONV) from
 // the stage input's conservative interior cells converted on load
+// cell grid velocities of a moving grid (the reference's xdot, ydot, zdot after
+// vert2cell_g: node-array layout, one set per snapshot); null on fixed grids
+struct CellVel {
+  const double *c[3];
+};
+
 template <bool CONV>
 __global__ void k_dt_euler(const DevBlock *__restrict__ blocks, const cosa_params *__restrict__ Pp,
                            const double *__restrict__ qp, const double *__restrict__ si,
                            const double *__restrict__ sj, const double *__restrict__ sk, double *__restrict__ dtv,
-                           double *bx, double *by, double *bz) {
+                           double *bx, double *by, double *bz, CellVel cv = CellVel{{nullptr, nullptr, nullptr}}) {
   const DevBlock b = blocks[blockIdx.y];
   const cosa_params &P = *Pp;
   const int S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
@@ -50,8 +56,13 @@ __global__ void k_dt_euler(const DevBlock *__restrict__ blocks, const cosa_param
       sjm[m] = sj[p2_idx(b, S2, m + 1, i, j, k, nh)]; sjp[m] = sj[p2_idx(b, S2, m + 1, i, j + 1, k, nh)];
       skm[m] = sk[p2_idx(b, S2, m + 1, i, j, k, nh)]; skp[m] = sk[p2_idx(b, S2, m + 1, i, j, k + 1, nh)];
     }
-    double li, lj, lk;
-    eig_eul(P.gamma, qc, sim, sip, sjm, sjp, skm, skp, li, lj, lk);
+    double li, lj, lk, gv[3];
+    if (cv.c[0]) {
+      const int64_t I2 = b.im + 2, J2 = b.jm + 2, K2 = b.km + 2;
+      const int64_t g = b.op2 * S2 + (int64_t)nh * I2 * J2 * K2 + i + I2 * (j + J2 * (int64_t)k);
+      gv[0] = cv.c[0][g]; gv[1] = cv.c[1][g]; gv[2] = cv.c[2][g];
+    }
+    eig_eul(P.gamma, qc, sim, sip, sjm, sjp, skm, skp, li, lj, lk, cv.c[0] ? gv : nullptr);
     const double dt = P.cfl / (li + lj + lk);
     dtv[o1] = dt;
     if (bx) {

@@ -41,7 +41,7 @@ class LevelPtrs(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in (
         "q", "qold", "res", "rhs", "dtvol", "dtvolt", "si", "sj", "sk", "vol",
         "qp", "qm", "dq", "dqp", "dqm", "flux", "betaxi", "betaeta", "betazeta",
-        "mut", "dist", "xdot", "ydot", "zdot")]
+        "mut", "dist", "xdot", "ydot", "zdot", "fvi", "fvj", "fvk")]
 
 
 # public symbols of include/cosa_gpu.h
@@ -63,6 +63,7 @@ SYMBOLS = [
     "cosa_gpu_lambda_ns", "cosa_gpu_deltat_ns", "cosa_gpu_q_face_mut", "cosa_gpu_rtst", "cosa_gpu_vflux_kom",
     "cosa_gpu_q_der_c", "cosa_gpu_turprod", "cosa_gpu_srckw", "cosa_gpu_update_kom", "cosa_gpu_cutman_mut",
     "cosa_gpu_autotune", "cosa_gpu_set_schedule", "cosa_gpu_force", "cosa_gpu_rest2_ho", "cosa_gpu_bc_res",
+    "cosa_gpu_movegrid", "cosa_gpu_face_vel", "cosa_gpu_vert2cell",
 ]
 
 
@@ -268,6 +269,42 @@ class Context:
 
     def vols(self, nl, x, y, z, vol):
         self._check(load().cosa_gpu_vols(self.h, nl, _ptr(x.ptr), _ptr(y.ptr), _ptr(z.ptr), _ptr(vol.ptr)), "vols")
+
+    # ---- moving grids (harmonic balance of a pitching body) -----------------------------
+    def movegrid(self, nl, x0, y0, z0, dx, dy, dz, x, y, z, xdot, ydot, zdot):
+        self._check(load().cosa_gpu_movegrid(self.h, nl, *(_ptr(a.ptr) for a in (x0, y0, z0, dx, dy, dz, x, y, z,
+                                                                                 xdot, ydot, zdot))), "movegrid")
+
+    def face_vel(self, nl, xdot, ydot, zdot, fvi, fvj, fvk):
+        self._check(load().cosa_gpu_face_vel(self.h, nl, *(_ptr(a.ptr) for a in (xdot, ydot, zdot, fvi, fvj, fvk))),
+                    "face_vel")
+
+    def vert2cell(self, nl, w):
+        self._check(load().cosa_gpu_vert2cell(self.h, nl, _ptr(w.ptr)), "vert2cell")
+
+    def pitching_setup(self, nl, case):
+        """The moving grid of a pitching harmonic-balance case in the
+        reference's set-up order: movegrid, vols, imetrix (per snapshot),
+        face velocities, vert2cell of the grid velocities.  Returns a dict of
+        device arrays (x, y, z, xdot, ydot, zdot, si, sj, sk, vol, fvi, fvj,
+        fvk); the displacement scales are 1 (rigid motion)."""
+        S = self.S
+        n1 = self.sizes(nl)[2]
+        x0, y0, z0 = (self.alloc_p2(nl, ncomp=1).upload(a) for a in (case.x, case.y, case.z))
+        dxyz = [self.alloc_p1(nl).upload(np.ones(n1)) for _ in range(3)]
+        m = {k: self.alloc_p2(nl, ncomp=S) for k in ("x", "y", "z", "xdot", "ydot", "zdot")}
+        self.movegrid(nl, x0, y0, z0, *dxyz, m["x"], m["y"], m["z"], m["xdot"], m["ydot"], m["zdot"])
+        m["vol"] = self.alloc_p1(nl)
+        self.vols(nl, m["x"], m["y"], m["z"], m["vol"])
+        for k in ("si", "sj", "sk"):
+            m[k] = self.alloc_p2(nl, ncomp=4 * S)
+        self.imetrix(nl, m["x"], m["y"], m["z"], m["si"], m["sj"], m["sk"])
+        for k in ("fvi", "fvj", "fvk"):
+            m[k] = self.alloc_p2(nl, ncomp=3 * S)
+        self.face_vel(nl, m["xdot"], m["ydot"], m["zdot"], m["fvi"], m["fvj"], m["fvk"])
+        for k in ("xdot", "ydot", "zdot"):
+            self.vert2cell(nl, m[k])
+        return m
 
     def profile(self, nl, niter):
         ms = (C.c_double * 4)()

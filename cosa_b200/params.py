@@ -64,7 +64,7 @@ class CosaParams(C.Structure):
         ("lim_prodtke", C.c_int32), ("lim_prodomega", C.c_int32), ("prd_all_lvls", C.c_int32),
         ("ifixq", C.c_int32), ("wallwilc", C.c_int32), ("ho_rest", C.c_int32),
         ("turcmp", C.c_double), ("prdlim", C.c_double), ("roughk", C.c_double),
-        ("reserved", C.c_double * 4),
+        ("dtheta0", C.c_double), ("omegas", C.c_double), ("xh", C.c_double), ("yh", C.c_double),
     ]
 
 
@@ -187,6 +187,41 @@ def set_harmonic_balance(p: CosaParams, nharms: int, omega: float) -> CosaParams
     for i in range(S):
         for j in range(S):
             p.dhb[i * S + j] = d[i, j]
+    return p
+
+
+def hb_harmonics(values, nharms: int, omega: float) -> np.ndarray:
+    """Fourier coefficients of a periodic quantity from its S = 2 nharms + 1
+    snapshot values through the matrix E of mathb (src/input.f90:5240-5251):
+    [a0, a1, b1, a2, b2, ...] with v(t) = a0 + sum a_i cos(i omega t) +
+    b_i sin(i omega t)."""
+    S = 2 * nharms + 1
+    dt = 2 * math.pi / omega / S
+    zeit = [n * dt for n in range(S)]
+    fact = 2.0 / S
+    e = np.zeros((S, S))
+    e[0, :] = fact / 2
+    for i in range(1, nharms + 1):
+        for j in range(S):
+            e[2 * (i - 1) + 1, j] = fact * math.cos(i * omega * zeit[j])
+            e[2 * (i - 1) + 2, j] = fact * math.sin(i * omega * zeit[j])
+    return e @ np.asarray(values, dtype=np.float64)
+
+
+def set_pitching(p: CosaParams, nharms: int, amp_deg: float, kred: float, xh: float = 0.25,
+                 yh: float = 0.0) -> CosaParams:
+    """Harmonic balance of a rigid pitching motion theta(t) = amp sin(omega t)
+    about (xh, yh): reduced frequency kred = omega c / (2 U) with chord 1 and
+    U = machfs (a_inf = 1), so omega = 2 kred machfs; every snapshot has its
+    own grid and metrics (moving = hbmove = 1)."""
+    omega = 2.0 * kred * p.machfs
+    set_harmonic_balance(p, nharms, omega)
+    p.moving = 1
+    p.hbmove = 1
+    p.omegas = omega
+    p.dtheta0 = math.radians(amp_deg)
+    p.xh = xh
+    p.yh = yh
     return p
 
 

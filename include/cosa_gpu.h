@@ -110,7 +110,11 @@ typedef struct cosa_params {
      (src/cosa.f90:2742-2751, 2871-2954), 0: rest2_lo_b */
   int32_t lim_prodtke, lim_prodomega, prd_all_lvls, ifixq, wallwilc, ho_rest;
   double turcmp, prdlim, roughk;
-  double reserved[4];
+  /* rigid pitching of the grid (moving = 1, harmonic balance, hbmove = 1):
+     theta(t) = dtheta0 sin(omegas t) about the hinge (xh, yh); dtheta0 in
+     radians, omegas = 2 pi x the input frequency (src/input.f90:2960-2980,
+     src/grid.f90:4540) */
+  double dtheta0, omegas, xh, yh;
 } cosa_params;
 
 /*
@@ -138,7 +142,13 @@ typedef struct cosa_level_ptrs {
   double *qp, *qm, *dq, *dqp, *dqm, *flux;           /* unfused scratch */
   double *betaxi, *betaeta, *betazeta;               /* IRS coefficients */
   double *mut, *dist;                                /* RANS */
-  double *xdot, *ydot, *zdot;                        /* moving grids */
+  /* moving grids: xdot, ydot, zdot the cell grid velocities (the node
+     arrays after vert2cell_g, P2 layout x S snapshots); fvi, fvj, fvk the
+     face velocities of the three families, the reference's sijk(5:7) kept
+     beside the lmet = 4 metric records: (3, 0:imax+1, 0:jmax+1, 0:kmax+1,
+     0:S-1) per block at offset op2*3*S */
+  double *xdot, *ydot, *zdot;
+  double *fvi, *fvj, *fvk;
 } cosa_level_ptrs;
 
 typedef struct cosa_ctx cosa_ctx;
@@ -227,6 +237,30 @@ int cosa_gpu_ccirs(cosa_ctx *ctx, int32_t nl, double *res, const double *ores,
    (lmet = 4) from the grid x,y,z; fixed grids */
 int cosa_gpu_imetrix(cosa_ctx *ctx, int32_t nl, const double *x, const double *y,
                      const double *z, double *si, double *sj, double *sk);
+/* ---- moving grids: harmonic balance of a rigidly pitching body (moving = 1,
+   hbmove = 1, lmet stays 4: the face velocities live in their own arrays).
+   Node arrays hold every snapshot: (0:imax+1,0:jmax+1,0:kmax+1,0:S-1) per
+   block at offset op2*S; imetrix then writes one set of metrics per
+   snapshot.  The set-up order is the reference's (src/cosa.f90:281-330):
+   movegrid, vols, imetrix, face_vel, vert2cell of xdot, ydot, zdot. ---- */
+/* movegrid + pitch (src/grid.f90:1783-1966): node positions x, y, z and
+   velocities xdot, ydot, zdot of every snapshot t_n = n 2 pi / (|omegas| S),
+   theta_n = dtheta0 sin(omegas t_n), from the reference grid x0, y0, z0 (P2
+   node arrays) and the displacement scales dx, dy (P1 arrays, nodes
+   1..imax; the mesh file's displacement record, src/input.f90:4562-4566).
+   Ghost nodes (index 0, imax+1) rotate rigidly (unit scales). */
+int cosa_gpu_movegrid(cosa_ctx *ctx, int32_t nl, const double *x0, const double *y0, const double *z0,
+                      const double *dx, const double *dy, const double *dz, double *x, double *y, double *z,
+                      double *xdot, double *ydot, double *zdot);
+/* face velocities (imetrix_b, src/grid.f90:1024-1062): the mean of each
+   face's four node velocities into fvi, fvj, fvk (layout as in
+   cosa_level_ptrs) */
+int cosa_gpu_face_vel(cosa_ctx *ctx, int32_t nl, const double *xdot, const double *ydot, const double *zdot,
+                      double *fvi, double *fvj, double *fvk);
+/* vert2cell_g (src/output.f90:3242-3480): node values of every snapshot to
+   cell values (cells 0..imax), in place; the cell grid velocities that
+   eig_eul reads */
+int cosa_gpu_vert2cell(cosa_ctx *ctx, int32_t nl, double *w);
 /* vols (src/grid.f90:2133-2230): cell volumes */
 int cosa_gpu_vols(cosa_ctx *ctx, int32_t nl, const double *x, const double *y,
                   const double *z, double *vol);
@@ -376,8 +410,10 @@ int cosa_gpu_cutman_mut(cosa_ctx *ctx, int32_t nl, double *mut);
    the ghost node); vm the face inverse metrics (viscous flows; may be NULL
    otherwise); xmom the moment centre, lngth = lref1..3 of the input file.
    coef (host, 12 * S doubles): snapshot n at coef[12n ..] = cl_p, cd_p,
-   cz_p, cmx_p, cmy_p, cm_p, cl_v, cd_v, cz_v, cmx_v, cmy_v, cm_v.  Moving
-   grids (the rotated moment centre) return COSA_ERR_UNSUPPORTED. */
+   cz_p, cmx_p, cmy_p, cm_p, cl_v, cd_v, cz_v, cmx_v, cmy_v, cm_v.  On a
+   pitching grid (moving) each snapshot uses its own metrics and nodes and
+   the moment centre carried with the body (src/output.f90:4476-4485);
+   inviscid only there. */
 int cosa_gpu_force(cosa_ctx *ctx, int32_t nl, const double *q, const double *x, const double *y,
                    const double *z, const double *si, const double *sj, const double *sk,
                    const double *vm, int32_t isurf, const double *xmom, const double *lngth,

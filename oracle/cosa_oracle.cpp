@@ -33,6 +33,12 @@ namespace {
 
 struct Level {
   int nb = 0, npde = 5, S = 1, lmet = 4, dim5h = 1;
+  // moving grids (harmonic balance of a pitching body): face velocities of
+  // the three families (3 components per face, the reference's sijk(5:7),
+  // P2 x dim5h layout) and cell-centred grid velocities (the node arrays
+  // xdot, ydot, zdot after vert2cell_g); null on fixed grids
+  const double *fv[3] = {nullptr, nullptr, nullptr};
+  const double *cv[3] = {nullptr, nullptr, nullptr};
   std::vector<int> im, jm, km, nbcs;
   std::vector<int64_t> op3, op2, op1, of0, om1, obct;
   std::vector<int> bct;   // 10 * sum(nbcs)
@@ -101,6 +107,32 @@ struct BG {  // grid (0:im+1, 0:jm+1, 0:km+1)
     return p[i + (int64_t)I * (j + (int64_t)J * k)];
   }
 };
+struct BGs {  // node array of snapshot nh: (0:im+1, 0:jm+1, 0:km+1, 0:dim5h-1)
+  double *p; int I, J;
+  BGs(const double *base, const Level &L, int b, int nh) : I(L.im[b] + 2), J(L.jm[b] + 2) {
+    p = const_cast<double *>(base) + L.op2[b] * L.dim5h + (int64_t)nh * I * J * (L.km[b] + 2);
+  }
+  inline double &operator()(int i, int j, int k) const { return p[i + (int64_t)I * (j + (int64_t)J * k)]; }
+};
+struct BFv {  // face velocities (3, 0:im+1, 0:jm+1, 0:km+1, 0:dim5h-1)
+  double *p; int I, J, K; int64_t P;
+  BFv(const double *base, const Level &L, int b)
+      : I(L.im[b] + 2), J(L.jm[b] + 2), K(L.km[b] + 2) {
+    P = (int64_t)I * J * K;
+    p = const_cast<double *>(base) + L.op2[b] * 3 * L.dim5h;
+  }
+  inline double &operator()(int c, int i, int j, int k, int nh) const {
+    return p[((int64_t)nh * P + i + (int64_t)I * (j + (int64_t)J * k)) * 3 + (c - 1)];
+  }
+};
+// face velocity . unit normal of face (i,j,k) of family d, snapshot nh, in
+// roflux_b's order: sijk(5)*kx + sijk(6)*ky + sijk(7)*kz (src/flux.f90:110-113)
+inline double face_ubn(const Level &L, int b, int d, int i, int j, int k, int nh, double kx, double ky, double kz) {
+  if (!L.fv[d - 1]) return 0.0;
+  BFv f(L.fv[d - 1], L, b);
+  return f(1, i, j, k, nh) * kx + f(2, i, j, k, nh) * ky + f(3, i, j, k, nh) * kz;
+}
+
 struct B1 {  // (0:im, 0:jm, 0:km [, 0:S-1])
   double *p; int I, J, K; int64_t P;
   B1(double *base, const Level &L, int b, int nsnap)
@@ -180,6 +212,7 @@ struct Patch {
   int bctyp, idir, inrout, istrt[4], iend[4];  // 1-based index arrays
   int ijk[4];
   int ic1, ic2, ic3;
+  int blk = 0;  // block of the patch (0-based)
 };
 inline Patch patch_of(const int *t, int im, int jm, int km) {
   Patch pa;
@@ -266,6 +299,11 @@ void bc_walinv_14(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &
         double un1 = u1 * nx + v1 * ny + w1 * nz;
         double un2 = u2 * nx + v2 * ny + w2 * nz;
         double unw = (3 * un1 - un2) / 2;
+        if (P.moving && L.fv[pa.idir - 1]) {
+          // wall face velocity (src/bc.f90:1567-1614)
+          BFv f(L.fv[pa.idir - 1], L, pa.blk);
+          unw = unw - (f(1, am, bm, cm, nh) * nx + f(2, am, bm, cm, nh) * ny + f(3, am, bm, cm, nh) * nz);
+        }
         q(a, bb, c, 1, n) = rhow;
         q(a, bb, c, 2, n) = uw - unw * nx;
         q(a, bb, c, 3, n) = vw - unw * ny;
@@ -612,6 +650,7 @@ int bc_level(const Level &L, double *qa, const double *si, const double *sj, con
     const int *t = L.bct.data() + L.obct[b];
     for (int ibc = 0; ibc < L.nbcs[b]; ++ibc) {
       Patch pa = patch_of(t + 10 * ibc, L.im[b], L.jm[b], L.km[b]);
+      pa.blk = b;
       switch (pa.bctyp) {
         case 80: bc_sym(pa, q, L); break;
         case 4: bc_extrapol(pa, q, L); break;
@@ -621,7 +660,7 @@ int bc_level(const Level &L, double *qa, const double *si, const double *sj, con
         case 21: status |= bc_insub(pa, q, vi, vj, vk, L, P); break;
         case 91: bc_outsub(pa, q, L, P); break;
         default:
-          if (pa.bctyp / 100 == 15 && !P.moving && (!is_kom(P) || dist)) {
+          if (pa.bctyp / 100 == 15 && (!P.moving || !is_kom(P)) && (!is_kom(P) || dist)) {
             bc_walvis_15(pa, q, L, P);
             if (is_kom(P)) bc_walvis_15_kom(pa, q, vi, vj, vk, dist, L, b, P);
           } else if (pa.bctyp / 100 == 15) {
@@ -731,6 +770,12 @@ void lambda_level(const Level &L, const double *qa, const double *si, const doub
             double axi = (sim[4] + sip[4]) / 2;
             double aeta = (sjm[4] + sjp[4]) / 2;
             double azeta = (skm[4] + skp[4]) / 2;
+            if (P.moving && L.cv[0]) {
+              // eig_eul: velocity relative to the cell's grid velocity (src/cosa.f90:4225-4229)
+              u = u - BGs(L.cv[0], L, b, nh)(i, j, k);
+              v = v - BGs(L.cv[1], L, b, nh)(i, j, k);
+              w = w - BGs(L.cv[2], L, b, nh)(i, j, k);
+            }
             lm(i, j, k, 1, n) = std::fabs(u * xix + v * xiy + w * xiz) + a * axi;
             lm(i, j, k, 2, n) = std::fabs(u * etax + v * etay + w * etaz) + a * aeta;
             lm(i, j, k, 3, n) = std::fabs(u * zetax + v * zetay + w * zetaz) + a * azeta;
@@ -1084,7 +1129,8 @@ void roflux_b(const Level &L, int b, int d, double *qra, double *qla, double *fa
           double vr[6], vl[6], f[6];
           for (int v = 1; v <= 5; ++v) { vr[v] = qr(i, j, k, v, n); vl[v] = ql(i, j, k, v, n); }
           double tker = kom ? qr(i, j, k, 6, n) : 0.0, tkel = kom ? ql(i, j, k, 6, n) : 0.0;
-          roe_face(P, kx, ky, kz, ds, 0.0, vr, vl, tker, tkel, f);
+          const double ubn = P.moving ? face_ubn(L, b, d, i, j, k, nh, kx, ky, kz) : 0.0;
+          roe_face(P, kx, ky, kz, ds, ubn, vr, vl, tker, tkel, f);
           for (int v = 1; v <= 5; ++v) flux(i, j, k, v, n) = f[v];
         }
     if (kom) roflux_turb(L, b, d, qr, ql, flux, s, P, n, ic, jc, kc);
@@ -1426,10 +1472,11 @@ void copy_interior(const Level &L, double *dst, const double *src) {
 // ---- imetrix_b / bvols (src/grid.f90:847-1010, 2160-2230), fixed grid -------
 void imetrix_b(const Level &L, int b, const double *xa, const double *ya, const double *za,
                double *sia, double *sja, double *ska) {
-  BG x(xa, L, b), y(ya, L, b), z(za, L, b);
+  // one set of metrics per grid snapshot (dim5h = 2 nharms hbmove + 1)
+  for (int n = 0; n < L.dim5h; ++n) {
+  BGs x(xa, L, b, n), y(ya, L, b, n), z(za, L, b, n);
   B2w si(sia, L, b), sj(sja, L, b), sk(ska, L, b);
   const int im = L.im[b], jm = L.jm[b], km = L.km[b];
-  const int n = 0;
   for (int k = 1; k <= km - 1; ++k)
     for (int j = 1; j <= jm - 1; ++j)
       for (int i = 1; i <= im; ++i) {
@@ -1466,10 +1513,122 @@ void imetrix_b(const Level &L, int b, const double *xa, const double *ya, const 
         double a4 = std::sqrt(a1 * a1 + a2 * a2 + a3 * a3);
         sk(1, i, j, k, n) = a1 / a4; sk(2, i, j, k, n) = a2 / a4; sk(3, i, j, k, n) = a3 / a4; sk(4, i, j, k, n) = a4;
       }
+  }
+}
+
+// ---- moving grids: rigid pitching (src/grid.f90:1783-1966) ------------------
+// movegrid_b + pitch: node positions and velocities of every snapshot n from
+// the reference grid x0 and the per-node displacement scales dx, dy (P1
+// arrays, nodes 1..imax), theta(n) = dtheta0 sin(omegas t_n).  The reference
+// moves nodes 1..imax; the ghost nodes 0 and imax+1 are rotated rigidly here as
+// well (the forces read them as moment arms).  The branch for |dx| or |dy| <=
+// 1e-4 keeps the reference's y0 (not y0 - yh) in its rotation terms.
+void pitch_b(const Level &L, int b, const double *x0a, const double *y0a, const double *z0a, const double *dxa,
+             const double *dya, const double *dza, double *xa, double *ya, double *za, double *xda, double *yda,
+             double *zda, const cosa_params &P, const double *zeit, const double *dth) {
+  BG x0(x0a, L, b), y0(y0a, L, b), z0(z0a, L, b);
+  B1 dx(const_cast<double *>(dxa), L, b, 1), dy(const_cast<double *>(dya), L, b, 1);
+  (void)dza;
+  const double xh = P.xh, yh = P.yh, dtheta0 = P.dtheta0, omegas = P.omegas;
+  for (int n = 0; n < L.dim5h; ++n) {
+    BGs x(xa, L, b, n), y(ya, L, b, n), z(za, L, b, n), xd(xda, L, b, n), yd(yda, L, b, n), zd(zda, L, b, n);
+    const double dtheta = dth[n], c = std::cos(dtheta), sn = std::sin(dtheta);
+    const double cw = std::cos(omegas * zeit[n]);
+    for (int k = 0; k <= L.km[b] + 1; ++k)
+      for (int i = 0; i <= L.im[b] + 1; ++i)
+        for (int j = 0; j <= L.jm[b] + 1; ++j) {
+          z(i, j, k) = z0(i, j, k);
+          zd(i, j, k) = 0.0;
+          // ghost nodes (index 0 or imax+1, read by the forces' moment arm)
+          // rotate rigidly: unit displacement scales
+          const bool ghost = i == 0 || j == 0 || k == 0 || i > L.im[b] || j > L.jm[b] || k > L.km[b];
+          const double X0 = x0(i, j, k), Y0 = y0(i, j, k);
+          const double DX = ghost ? 1.0 : dx(i, j, k), DY = ghost ? 1.0 : dy(i, j, k);
+          if (std::fabs(DX) > 1e-4 && std::fabs(DY) > 1e-4) {
+            const double d1 = ((X0 - xh) * (c - 1) - (Y0 - yh) * sn) / DX;
+            const double d2 = ((X0 - xh) * sn + (Y0 - yh) * (c - 1)) / DY;
+            x(i, j, k) = X0 + d1 * DX;
+            y(i, j, k) = Y0 + d2 * DY;
+            const double v1 = (-(X0 - xh) * sn - (Y0 - yh) * c) * dtheta0 * cw / DX;
+            const double v2 = ((X0 - xh) * c - (Y0 - yh) * sn) * dtheta0 * cw / DY;
+            xd(i, j, k) = omegas * v1 * DX;
+            yd(i, j, k) = omegas * v2 * DY;
+          } else {
+            const double d1 = ((X0 - xh) * (c - 1.0) - Y0 * sn);
+            const double d2 = ((X0 - xh) * sn + Y0 * (c - 1.0));
+            x(i, j, k) = X0 + d1;
+            y(i, j, k) = Y0 + d2;
+            const double v1 = dtheta0 * cw * (-(X0 - xh) * sn - Y0 * c);
+            const double v2 = dtheta0 * cw * ((X0 - xh) * c - Y0 * sn);
+            xd(i, j, k) = omegas * v1;
+            yd(i, j, k) = omegas * v2;
+          }
+        }
+  }
+}
+
+// imetrix_b, moving part (src/grid.f90:1024-1062): the velocity of each face
+// midpoint as the mean of its four nodes' velocities
+void face_vel_b(const Level &L, int b, const double *xda, const double *yda, const double *zda, double *fia,
+                double *fja, double *fka) {
+  BFv fi(fia, L, b), fj(fja, L, b), fk(fka, L, b);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  for (int n = 0; n < L.dim5h; ++n) {
+    BGs xd(xda, L, b, n), yd(yda, L, b, n), zd(zda, L, b, n);
+    const BGs *v[3] = {&xd, &yd, &zd};
+    for (int c = 0; c < 3; ++c) {
+      const BGs &a = *v[c];
+      for (int k = 1; k <= km - 1; ++k)
+        for (int j = 1; j <= jm - 1; ++j)
+          for (int i = 1; i <= im; ++i)
+            fi(c + 1, i, j, k, n) = (a(i, j + 1, k + 1) + a(i, j + 1, k) + a(i, j, k + 1) + a(i, j, k)) / 4;
+      for (int k = 1; k <= km - 1; ++k)
+        for (int i = 1; i <= im - 1; ++i)
+          for (int j = 1; j <= jm; ++j)
+            fj(c + 1, i, j, k, n) = (a(i + 1, j, k + 1) + a(i + 1, j, k) + a(i, j, k + 1) + a(i, j, k)) / 4;
+      for (int j = 1; j <= jm - 1; ++j)
+        for (int i = 1; i <= im - 1; ++i)
+          for (int k = 1; k <= km; ++k)
+            fk(c + 1, i, j, k, n) = (a(i + 1, j + 1, k) + a(i + 1, j, k) + a(i, j + 1, k) + a(i, j, k)) / 4;
+    }
+  }
+}
+
+// vert2cell_bg (src/output.f90:3276-3480): node values -> cell values in
+// place (cells 0..imax: the block's vertices, edges and bounding faces take
+// the nearest boundary nodes, interior cells the mean of their 8 nodes)
+void vert2cell_b(const Level &L, int b, double *wa) {
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  for (int n = 0; n < L.dim5h; ++n) {
+    BGs x(wa, L, b, n);
+    const int64_t np = (int64_t)(im + 2) * (jm + 2) * (km + 2);
+    std::vector<double> w(x.p, x.p + np);
+    auto W = [&](int i, int j, int k) { return w[i + (int64_t)(im + 2) * (j + (int64_t)(jm + 2) * k)]; };
+    auto bnd = [](int i, int m) { return i == 0 ? 1 : m; };
+    for (int k = 0; k <= km; ++k)
+      for (int j = 0; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i) {
+          const bool bi = i == 0 || i == im, bj = j == 0 || j == jm, bk = k == 0 || k == km;
+          const int i1 = bnd(i, im), j1 = bnd(j, jm), k1 = bnd(k, km);
+          double v;
+          if (bi && bj && bk) v = W(i1, j1, k1);
+          else if (bj && bk) v = (W(i, j1, k1) + W(i + 1, j1, k1)) / 2;
+          else if (bi && bk) v = (W(i1, j, k1) + W(i1, j + 1, k1)) / 2;
+          else if (bi && bj) v = (W(i1, j1, k) + W(i1, j1, k + 1)) / 2;
+          else if (bk) v = (W(i, j, k1) + W(i + 1, j, k1) + W(i, j + 1, k1) + W(i + 1, j + 1, k1)) / 4;
+          else if (bj) v = (W(i, j1, k) + W(i + 1, j1, k) + W(i, j1, k + 1) + W(i + 1, j1, k + 1)) / 4;
+          else if (bi) v = (W(i1, j, k) + W(i1, j, k + 1) + W(i1, j + 1, k) + W(i1, j + 1, k + 1)) / 4;
+          else
+            v = (W(i, j, k) + W(i + 1, j, k) + W(i, j + 1, k) + W(i + 1, j + 1, k) + W(i, j, k + 1) +
+                 W(i + 1, j, k + 1) + W(i, j + 1, k + 1) + W(i + 1, j + 1, k + 1)) / 8;
+          x(i, j, k) = v;
+        }
+  }
 }
 
 void bvols(const Level &L, int b, const double *xa, const double *ya, const double *za, double *va) {
-  BG x(xa, L, b), y(ya, L, b), z(za, L, b);
+  // the volumes of the first grid snapshot (rigid motions keep them)
+  BGs x(xa, L, b, 0), y(ya, L, b, 0), z(za, L, b, 0);
   B1 vol(va, L, b, 1);
   for (int k = 1; k <= L.km[b] - 1; ++k)
     for (int j = 1; j <= L.jm[b] - 1; ++j)
@@ -2331,10 +2490,19 @@ void bc_walvis_15(const Patch &pa, B3 &q, const Level &L, const cosa_params &P) 
         const double p1 = q(ni_, nj_, nk_, 5, n), p2 = q(n2i, n2j, n2k, 5, n);
         const double pw = 0.5 * (3 * p1 - p2);
         const double rhow = std::pow(pw / p1, 1 / P.gamma) * q(ni_, nj_, nk_, 1, n);
+        double uw = 0.0, vw = 0.0, ww = 0.0;
+        if (P.moving && L.fv[pa.idir - 1]) {
+          // the wall moves with its face (src/bc.f90:2256-2283)
+          int mi, mj, mk;
+          pidx(pa, pa.inrout == 1 ? 1 : pa.ijk[pa.idir], i2, i3, mi, mj, mk);
+          BFv f(L.fv[pa.idir - 1], L, pa.blk);
+          const int nh = n * P.hbmove;
+          uw = f(1, mi, mj, mk, nh); vw = f(2, mi, mj, mk, nh); ww = f(3, mi, mj, mk, nh);
+        }
         q(hi, hj, hk, 1, n) = rhow;
-        q(hi, hj, hk, 2, n) = 0.0;
-        q(hi, hj, hk, 3, n) = 0.0;
-        q(hi, hj, hk, 4, n) = 0.0;
+        q(hi, hj, hk, 2, n) = uw;
+        q(hi, hj, hk, 3, n) = vw;
+        q(hi, hj, hk, 4, n) = ww;
         q(hi, hj, hk, 5, n) = pw;
         for (int v = 1; v <= 5; ++v) q(h2i, h2j, h2k, v, n) = q(hi, hj, hk, v, n);
       }
@@ -2863,9 +3031,23 @@ void force_frame(const cosa_params &P, double ss[3], double aa[3], double bb[3])
 // (1,xi), (2,eta), (3,zeta)).  out[n*12 + c], c = cl_p, cd_p, cz_p, cmx_p,
 // cmy_p, cm_p, cl_v, cd_v, cz_v, cmx_v, cmy_v, cm_v; a non-moving grid, so
 // the moment centre is xmom itself.
+// snapshot times and pitch angles of harmonic balance (src/input.f90:3182-3192,
+// src/grid.f90:4536-4541): t_n = n 2 pi / (|omegas| S), theta_n = dtheta0 sin(omegas t_n)
+void hb_motion(const cosa_params &P, int S, double *zeit, double *dth) {
+  const double pi = 3.14159265358979323846;
+  const double omega = std::fabs(P.omegas);
+  const double dt = omega > 0 ? 2 * pi / omega / S : 0.0;
+  for (int n = 0; n < S; ++n) {
+    zeit[n] = n * dt;
+    dth[n] = P.dtheta0 * std::sin(P.omegas * zeit[n]);
+  }
+}
+
 void force_level(const Level &L, const double *qa, const double *xa, const double *ya, const double *za,
                  const double *si, const double *sj, const double *sk, const double *vm, const cosa_params &P,
-                 int isurf, const double xmom[3], const double lngth[3], double *out) {
+                 int isurf, const double xmom0[3], const double lngth[3], double *out) {
+  double zeit[COSA_MAX_SNAP], dth[COSA_MAX_SNAP];
+  hb_motion(P, L.S, zeit, dth);
   const double mach = P.machfs > 1e-14 ? P.machfs : 1.0;
   double ss[3], aa[3], bb[3];
   force_frame(P, ss, aa, bb);
@@ -2875,10 +3057,19 @@ void force_level(const Level &L, const double *qa, const double *xa, const doubl
   for (int n = 0; n < L.S * 12; ++n) out[n] = 0.0;
   for (int b = 0; b < L.nb; ++b) {
     B3 q(const_cast<double *>(qa), L, b);
-    BG X(xa, L, b), Y(ya, L, b), Z(za, L, b);
     const B2 sd[3] = {B2(si, L, b), B2(sj, L, b), B2(sk, L, b)};
     const int ijk[4] = {0, L.im[b], L.jm[b], L.km[b]};
     for (int n = 0; n < L.S; ++n) {
+      const int nh = n * P.hbmove;
+      BGs X(xa, L, b, nh), Y(ya, L, b, nh), Z(za, L, b, nh);
+      double xmom[3] = {xmom0[0], xmom0[1], xmom0[2]};
+      if (P.moving) {
+        // moment centre carried by the pitching motion (src/output.f90:4476-4485)
+        const double dr1 = (xmom0[0] - P.xh) * (std::cos(dth[n]) - 1) - (xmom0[1] - P.yh) * std::sin(dth[n]);
+        const double dr2 = (xmom0[0] - P.xh) * std::sin(dth[n]) + (xmom0[1] - P.yh) * (std::cos(dth[n]) - 1);
+        xmom[0] = xmom0[0] + dr1;
+        xmom[1] = xmom0[1] + dr2;
+      }
       double fp[6] = {0, 0, 0, 0, 0, 0}, fv[6] = {0, 0, 0, 0, 0, 0};
       for (int ib = 0; ib < L.nbcs[b]; ++ib) {
         const int *t = &L.bct[L.obct[b] + 10 * ib];
@@ -2901,8 +3092,8 @@ void force_level(const Level &L, const double *qa, const double *xa, const doubl
             pidx(pa, ibcpt, i2, i3, hi, hj, hk);
             pidx(pa, ibcm, i2, i3, mi, mj, mk);
             pidx(pa, ibcw, i2, i3, wi, wj, wk);
-            const double kx = sgn * s(1, mi, mj, mk, 0), ky = sgn * s(2, mi, mj, mk, 0);
-            const double kz = sgn * s(3, mi, mj, mk, 0), ds = s(4, mi, mj, mk, 0);
+            const double kx = sgn * s(1, mi, mj, mk, nh), ky = sgn * s(2, mi, mj, mk, nh);
+            const double kz = sgn * s(3, mi, mj, mk, nh), ds = s(4, mi, mj, mk, nh);
             const double pw = pw_of(hi, hj, hk);
             fp[0] = fp[0] - pw * kx * ds;
             fp[1] = fp[1] - pw * ky * ds;
@@ -3017,6 +3208,32 @@ int orc_num_threads(void) {
 #endif
 }
 
+// moving grid of harmonic balance: metrics, grid arrays and the face /
+// cell velocities of every snapshot (dim5h = S); null pointers turn the
+// face and cell velocities off again
+void orc_set_moving(orc_level *h, int hbmove, const double *fvi, const double *fvj, const double *fvk,
+                    const double *cvx, const double *cvy, const double *cvz) {
+  Level &L = h->L;
+  L.dim5h = hbmove ? L.S : 1;
+  L.fv[0] = fvi; L.fv[1] = fvj; L.fv[2] = fvk;
+  L.cv[0] = cvx; L.cv[1] = cvy; L.cv[2] = cvz;
+}
+void orc_pitch(orc_level *h, const cosa_params *p, const double *x0, const double *y0, const double *z0,
+               const double *dx, const double *dy, const double *dz, double *x, double *y, double *z, double *xd,
+               double *yd, double *zd) {
+  double zeit[COSA_MAX_SNAP], dth[COSA_MAX_SNAP];
+  hb_motion(*p, h->L.S, zeit, dth);
+  for (int b = 0; b < h->L.nb; ++b) pitch_b(h->L, b, x0, y0, z0, dx, dy, dz, x, y, z, xd, yd, zd, *p, zeit, dth);
+}
+void orc_face_vel(orc_level *h, const double *xd, const double *yd, const double *zd, double *fvi, double *fvj,
+                  double *fvk) {
+  for (int b = 0; b < h->L.nb; ++b) face_vel_b(h->L, b, xd, yd, zd, fvi, fvj, fvk);
+}
+void orc_vert2cell(orc_level *h, double *w) {
+  for (int b = 0; b < h->L.nb; ++b) vert2cell_b(h->L, b, w);
+}
+void orc_hb_motion(const cosa_params *p, int S, double *zeit, double *dth) { hb_motion(*p, S, zeit, dth); }
+
 void orc_imetrix(orc_level *h, const double *x, const double *y, const double *z, double *si,
                  double *sj, double *sk) {
   for (int b = 0; b < h->L.nb; ++b) imetrix_b(h->L, b, x, y, z, si, sj, sk);
@@ -3062,11 +3279,13 @@ void orc_resg_rms(orc_level *h, double *res, double *rhs, double *out) { resg_rm
 void orc_zero_res(orc_level *h, double *res) { zero_res(h->L, res); }
 void orc_copy_interior(orc_level *h, double *dst, const double *src) { copy_interior(h->L, dst, src); }
 // Roe face flux on single states (for KATs): q = (rho,u,v,w,p) prim
+// nrm = (kx, ky, kz, ds[, ubn]): with nrm5 != 0, nrm[4] is the face's normal
+// grid speed
 void orc_roe_face(const cosa_params *p, const double *nrm, const double *qr, const double *ql,
-                  double *f) {
+                  double *f, int nrm5) {
   double vr[6], vl[6], out[6];
   for (int m = 0; m < 5; ++m) { vr[m + 1] = qr[m]; vl[m + 1] = ql[m]; }
-  roe_face(*p, nrm[0], nrm[1], nrm[2], nrm[3], 0.0, vr, vl, 0.0, 0.0, out);
+  roe_face(*p, nrm[0], nrm[1], nrm[2], nrm[3], nrm5 ? nrm[4] : 0.0, vr, vl, 0.0, 0.0, out);
   for (int m = 0; m < 5; ++m) f[m] = out[m + 1];
 }
 

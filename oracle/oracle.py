@@ -30,7 +30,7 @@ class _LevelPtrs(C.Structure):
     _fields_ = [(n, _dp) for n in (
         "q", "qold", "res", "rhs", "dtvol", "dtvolt", "si", "sj", "sk", "vol",
         "qp", "qm", "dq", "dqp", "dqm", "flux", "betaxi", "betaeta", "betazeta",
-        "mut", "dist", "xdot", "ydot", "zdot")]
+        "mut", "dist", "xdot", "ydot", "zdot", "fvi", "fvj", "fvk")]
 
 
 def build(force: bool = False) -> str:
@@ -179,6 +179,39 @@ class OracleLevel:
         return hist, st
 
 
+def hb_motion(p, S):
+    """Snapshot times and pitch angles of harmonic balance."""
+    zeit, dth = np.zeros(S), np.zeros(S)
+    lib().orc_hb_motion(_par(p), C.c_int(S), _p(zeit), _p(dth))
+    return zeit, dth
+
+
+def moving_setup(O, x0, y0, z0, dx, dy, dz):
+    """The moving grid of a pitching harmonic-balance case as the reference's
+    set-up builds it (movegrid, imetrix with the face velocities, vols,
+    vert2cell_g of the grid velocities), bound to O: returns a dict with the
+    per-snapshot node arrays x, y, z, the cell grid velocities cx, cy, cz, the
+    face velocities fvi, fvj, fvk, the metrics si, sj, sk and vol."""
+    S = O.S
+    m = {k: np.zeros(O.n2 * S) for k in ("x", "y", "z", "cx", "cy", "cz")}
+    for k in ("fvi", "fvj", "fvk"):
+        m[k] = np.zeros(O.n2 * 3 * S)
+    lib().orc_set_moving(O.h, C.c_int(1), None, None, None, None, None, None)
+    lib().orc_pitch(O.h, _par(O.p), _p(x0), _p(y0), _p(z0), _p(dx), _p(dy), _p(dz), _p(m["x"]), _p(m["y"]),
+                    _p(m["z"]), _p(m["cx"]), _p(m["cy"]), _p(m["cz"]))
+    lib().orc_face_vel(O.h, _p(m["cx"]), _p(m["cy"]), _p(m["cz"]), _p(m["fvi"]), _p(m["fvj"]), _p(m["fvk"]))
+    for k in ("cx", "cy", "cz"):
+        lib().orc_vert2cell(O.h, _p(m[k]))
+    m["si"], m["sj"], m["sk"] = (np.zeros(O.n2 * 4 * S) for _ in range(3))
+    m["vol"] = O.p1()
+    lib().orc_imetrix(O.h, _p(m["x"]), _p(m["y"]), _p(m["z"]), _p(m["si"]), _p(m["sj"]), _p(m["sk"]))
+    lib().orc_vols(O.h, _p(m["x"]), _p(m["y"]), _p(m["z"]), _p(m["vol"]))
+    lib().orc_set_moving(O.h, C.c_int(1), _p(m["fvi"]), _p(m["fvj"]), _p(m["fvk"]), _p(m["cx"]), _p(m["cy"]),
+                         _p(m["cz"]))
+    O._moving = m  # keeps the arrays the oracle points to alive
+    return m
+
+
 def smooth_irs(O, q, si, sj, sk, ncycles, mgit0=1, rms_every=1):
     """Single-level cycles with implicit residual smoothing (irsop > 0)."""
     qold = O.p3()
@@ -226,11 +259,13 @@ def tridi(a, b, c, x):
 
 
 def roe_face(params, nrm, qr, ql):
+    """roflux_b's face flux; nrm = (kx, ky, kz, ds) or (kx, ky, kz, ds, ubn)
+    with the face's normal grid speed ubn."""
     f = np.zeros(5)
     n = np.ascontiguousarray(nrm, dtype=np.float64)
     a = np.ascontiguousarray(qr, dtype=np.float64)
     b = np.ascontiguousarray(ql, dtype=np.float64)
-    lib().orc_roe_face(C.byref(params), _p(n), _p(a), _p(b), _p(f))
+    lib().orc_roe_face(C.byref(params), _p(n), _p(a), _p(b), _p(f), C.c_int(1 if n.size > 4 else 0))
     return f
 
 
