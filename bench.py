@@ -6,17 +6,21 @@ segment lengths from {24, ..., 160}), M = 0.6, 4-stage RK, CFL 2, Roe + MUSCL
 (kappa = 1/3, smooth limiter), FP64 state.  A step is one RK cycle (4 stages)
 over all cells; the metric is Mcell-stage/s = cells * 4 * steps / time.
 
-Our arm times cosa_gpu_smooth (fused halo + tile kernels replayed from a
-CUDA graph, state resident in HBM) with CUDA events on the library's stream;
-inputs (the state, 1.4 GB) are larger than the 126 MB L2, so no flush is
-needed between steps.  It also reports the mixed-precision path (FP32 slopes
-and Roe dissipation on FP64 differences), the roofline of the tile kernel,
-an end-to-end number through cosa_gpu_smooth_host (state copied from pinned
-host memory and back every step) and the CPU oracle's throughput on a
-bounded sample of the same workload.
+Our arm times cosa_gpu_smooth (halo fill, line-marching face kernels and the
+cell pass of the face-split schedule, or the fused tile kernel, whichever the
+autotuner picks, replayed from a CUDA graph with the state resident in HBM)
+with CUDA events on the library's stream; the state (1.4 GB) is larger than
+the 126 MB L2, so no flush is needed between steps.  It also reports the
+mixed-precision path, the roofline of the dominant kernel and of the whole
+stage against the algorithmic bytes of the ideally fused stage, an
+end-to-end number through cosa_gpu_smooth_host (state copied from pinned
+host memory and back every step), the laminar and k-omega legs, the
+harmonic-balance pitching aerofoil (NH = 1..3, FP64 and mixed), the serving
+sweep and the CPU oracle's throughput on 2 cycles of the same workload.
 
 --impl reference times the CPU restatement of the reference (oracle/; COSA
-itself is Fortran and cannot be built here) on the host cores.
+itself is Fortran and cannot be built here) on the host cores, 2 RK cycles of
+the same 30.7 M-cell duct.
 """
 from __future__ import annotations
 
@@ -34,24 +38,22 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# algorithmic bytes per cell-stage of the whole Euler stage (FP64): read q 40 +
-# read q^n 40 + write q 40 + face metrics of the 3 owned faces 96 + vol 8 +
-# dt/V 8 + dt/V write amortised 2
+# algorithmic bytes per cell-stage of the ideally fused Euler stage (FP64):
+# read q 40 + read q^n 40 + write q 40 + face metrics of the 3 owned faces 96
+# + vol 8 + dt/V 8 + dt/V write amortised 2.  The roofline fractions below
+# charge every kernel with these bytes, whatever it moves itself.
 B_ALG_STAGE = 234
-# tile kernel alone, per cell and launch: stages 2-4 read q, q^n, metrics and
-# dt/V and write q (224 B); stage 1 writes dt/V instead of reading it and
-# copies q^n (264 B): average over the 4 stages of a cycle
-B_TILE = (3 * 224 + 264) / 4.0
-# face-split schedule: k_faces per cell (three face families) reads the
-# primitive state 40 + face metrics 96 and writes the face fluxes 120
-B_FACES = 256
-# DRAM bytes per cell of one k_faces launch, from the ncu capture summarised
-# in profiles/k_faces_k_cells_duct4m.md (4.2 M-cell duct, scaled by cells)
-FACES_TRAFFIC_B_PER_CELL = 373.3
-# DRAM bytes (read + write) per cell of one tile launch, from the ncu capture
-# summarised in profiles/k_stage_tile_fp64_duct4m.md (a stage-3 launch on the
-# 4.1 M-cell duct, scaled by the cells of the launch)
-TILE_TRAFFIC_B_PER_CELL = 257.8
+# harmonic balance of a pitching body, per cell-snapshot-stage: state 120 +
+# metrics 3 x 7 x 8 = 168 + cell grid velocity 24 + vol 8 + dt/V 8 + 2
+B_ALG_HB_MOVING = 330
+# bytes the face-split schedule's face kernels (k_faces_line, i-face and
+# marching launches) move per cell: state reads 3 x 40 (once per family) +
+# face metrics 96 + face fluxes written 120
+B_FACES_OWN = 336
+# DRAM bytes (read + write) per cell of one stage's two k_faces_line
+# launches in an ncu capture of the 4.2 M-cell duct (k_faces_line<fp64>,
+# scaled by the cells of the launch)
+FACES_TRAFFIC_B_PER_CELL = 311.7
 
 
 def _peaks():
@@ -137,49 +139,39 @@ def build_case(args):
     raise SystemExit(f"unknown workload {args.workload}")
 
 
-def cpu_sample_case(args):
-    from cosa_b200 import cases
-    segs = cases.duct_segments(seed=args.seed + 100, lo=900_000, hi=1_300_000, choices=tuple(range(24, 65, 8)))
-    return cases.duct3d(segs=segs), segs
-
-
-def run_cpu_oracle(args, steps: int, warmup: int, min_seconds: float = 0.0):
-    """The oracle (C++ restatement of the reference, OpenMP over blocks) on a
-    ~1 M-cell duct with the same generator: Mcell-stage/s on the host cores.
-    With min_seconds, RK cycles are added in chunks of `steps` until the
-    timed CPU work lasts at least that long."""
+def run_cpu_oracle(case, desc, steps: int, warmup: int):
+    """The oracle (C++ restatement of the reference, OpenMP over blocks and
+    k-planes) on the benchmark's own workload: `steps` RK cycles after
+    `warmup`, wall-timed around the cycles only (set-up and metrics
+    excluded).  Returns the cpu_baseline record and the seconds."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    case, segs = cpu_sample_case(args)
     O = oracle.OracleLevel(case.tables, case.params)
     si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
     q = case.q0.copy()
     if warmup:
         O.smooth(q, si, sj, sk, warmup, rms_every=10 ** 6)
     t = time.perf_counter()
-    done = 0
-    while True:
-        O.smooth(q, si, sj, sk, steps, rms_every=10 ** 6, mgit0=done + 1)
-        done += steps
-        if time.perf_counter() - t >= min_seconds:
-            break
+    O.smooth(q, si, sj, sk, steps, rms_every=10 ** 6, mgit0=warmup + 1)
     dt = time.perf_counter() - t
-    steps = done
     val = case.ncells * case.params.nstage * steps / dt / 1e6
     return {"value": val, "unit": "Mcell-stage/s", "cores": oracle.num_threads(), "kind": "port",
-            "sample": f"{case.ncells} cells (24-block duct, segments {segs}), {steps} RK cycles, {dt:.2f} s"}, dt
+            "sample": f"{desc}: {steps} RK cycles of the full workload after {warmup} warm-up, {dt:.2f} s"}, dt
 
 
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return
-    steps = max(1, min(args.steps, 8))
-    cb, dt = run_cpu_oracle(args, steps, min(args.warmup, 1))
+    # a bounded sample of the same workload: 2 cycles of the full grid
+    steps, warmup = max(1, min(args.steps, 2)), min(args.warmup, 1)
+    case, desc = build_case(args)
+    cb, dt = run_cpu_oracle(case, desc, steps, warmup)
     line = {"impl": "reference", "metric": "Mcell-stage/s", "value": cb["value"], "unit": "Mcell-stage/s",
-            "n_gpus": ws, "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": dt / steps * 1e3,
+            "n_gpus": ws, "steps": steps, "warmup": warmup, "ms_per_step": dt / steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": "config3 bump duct (bounded CPU sample)"},
+            "data": "synthetic", "config": {"workload": desc, "cells": case.ncells, "blocks": case.tables.nblocks,
+                                            "stages_per_step": case.params.nstage},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "Mcell-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -271,6 +263,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed, e2e and CPU legs (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving sweep")
     ap.add_argument("--no-viscous", action="store_true", help="skip the laminar and k-omega legs")
+    ap.add_argument("--no-hb", action="store_true", help="skip the pitching harmonic-balance leg")
+    ap.add_argument("--hb-cycles", type=int, default=400, help="RK cycles of each harmonic-balance run")
     ap.add_argument("--schedule", type=int, default=0, choices=[0, 1, 2],
                     help="0: autotune the stage schedule, 1: fused tile kernel, 2: face-split")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
@@ -345,11 +339,12 @@ def main():
     value = replica_throughput(ws, ncells * nstage * args.steps, ms_max)
 
     # ---- kernel roofline: event-timed pass right after the timed region ----------
+    # the dominant kernel is charged the whole stage's algorithmic bytes
     kms, kcnt = ctx.profile(1, 3)
     peak, peak_kind = _peaks()
     split = sched_fp64[2] == 1
-    main_bytes = (B_FACES if split else B_TILE) * ncells
-    achieved = main_bytes / (kms[1] / 1e3) / 1e9
+    alg_bytes = B_ALG_STAGE * ncells
+    achieved = alg_bytes / (kms[1] / 1e3) / 1e9
     stage_gbs = B_ALG_STAGE * ncells * nstage * args.steps / (ms / 1e3) / 1e9
 
     if args.no_extras:
@@ -430,10 +425,35 @@ def main():
         except Exception as e:  # reported, not fatal
             serving["batched_vs_plain"] = {"error": str(e)}
 
+    hb = None
+    if rank == 0 and ws == 1 and not args.no_hb:
+        # harmonic balance of the pitching NACA 0012 (256 x 64 x 2, NH = 1..3),
+        # FP64 and mixed: throughput, roofline and the CL/CM harmonics' gap
+        from cosa_b200 import pitching
+        hb = {}
+        for nh in (1, 2, 3):
+            try:
+                r = pitching.compare(nh, cycles=args.hb_cycles, chunk=args.hb_cycles, device=dev)
+                f, mx = r["fp64"], r["mixed"]
+                gbs = B_ALG_HB_MOVING * f["mcell_snapshot_stage_s"] * 1e6 / 1e9
+                hb[f"nh{nh}"] = {"snapshots": f["snapshots"], "cells": f["cells"], "cycles": f["cycles"],
+                                 "fp64_mcell_snapshot_stage_s": f["mcell_snapshot_stage_s"],
+                                 "mixed_mcell_snapshot_stage_s": mx["mcell_snapshot_stage_s"],
+                                 "mixed_speedup": r["mixed_speedup"],
+                                 "fp64_stage_gbs_alg": gbs, "fp64_stage_frac": gbs / peak,
+                                 "drop_rho_fp64": f["drop_rho"],
+                                 "cl_harmonics_fp64": f["cl_harmonics"], "cm_harmonics_fp64": f["cm_harmonics"],
+                                 "max_dcl_harmonic_mixed": r["max_dcl_harmonic"],
+                                 "max_dcm_harmonic_mixed": r["max_dcm_harmonic"]}
+            except Exception as e:  # reported, not fatal
+                hb[f"nh{nh}"] = {"error": str(e)}
+        hb["workload"] = ("NACA 0012 O-grid 256x64x2 (4 blocks), Euler, M=0.5, pitching 2.5 deg about c/4 at "
+                          "k=0.08, harmonic balance with one grid per snapshot, CFL 1, 4-stage RK")
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         try:
-            cpu, _ = run_cpu_oracle(args, 4, 0, min_seconds=10.0)
+            cpu, _ = run_cpu_oracle(case, desc, 2, 0)
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "error": str(e)}
 
@@ -448,12 +468,14 @@ def main():
                        "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": (FACES_TRAFFIC_B_PER_CELL if split else TILE_TRAFFIC_B_PER_CELL) * ncells,
-                         "traffic_source": "ncu dram bytes per cell of the 4.2 M-cell duct x cells",
-                         "kernel": "k_faces<fp64>" if split else "k_stage_tile<32,7,fp64>",
+                         "traffic": FACES_TRAFFIC_B_PER_CELL * ncells if split else None,
+                         "traffic_source": "ncu dram read+write of k_faces_line (both launches of a stage) per "
+                                           "cell on the 4.2 M-cell duct, x cells",
+                         "kernel": "k_faces_line<fp64> (i-face + marching launches)" if split
+                                   else "k_stage_tile<32,7,fp64>",
                          "kernel_ms": kms[1], "halo_ms": kms[0], "cells_kernel_ms": kms[3] if split else None,
-                         "bytes_per_cell": B_FACES if split else B_TILE,
-                         "peak_kind": peak_kind, "stage_gbs_alg": stage_gbs},
+                         "alg_bytes_per_cell": B_ALG_STAGE, "kernel_own_bytes_per_cell": B_FACES_OWN if split else None,
+                         "peak_kind": peak_kind, "stage_gbs_alg": stage_gbs, "stage_frac": stage_gbs / peak},
             "schedule": {"fp64": {"tile_ms_per_step": sched_fp64[0], "split_ms_per_step": sched_fp64[1],
                                   "chosen": ["tile", "split"][sched_fp64[2]]},
                          "mixed": {"tile_ms_per_step": sched_mixed[0], "split_ms_per_step": sched_mixed[1],
@@ -465,6 +487,7 @@ def main():
                     "d2h_bytes_per_step": state_bytes + 8 * (p.npde + 1)},
             "cpu_baseline": cpu,
             "viscous": viscous or None,
+            "harmonic_balance": hb,
             "serving": serving,
             "gpu_launches": launches,
             "clocks": clocks,

@@ -645,13 +645,15 @@ def naca0012_ogrid(blocks=(96, 160, 160, 96), nj: int = 128, nk: int = 2, rfar: 
 
 def naca_pitching(nharms: int = 1, blocks=(64, 64, 64, 64), nj: int = 64, nk: int = 2, mach: float = 0.5,
                   alpha_deg: float = 0.0, amp_deg: float = 2.5, kred: float = 0.08, xh: float = 0.25,
-                  rfar: float = 30.0, h1: float = 2.0e-3, cfl: float = 2.0, model: str = "euler") -> Case:
+                  rfar: float = 30.0, h1: float = 2.0e-3, cfl: float = 1.0, model: str = "euler") -> Case:
     """Harmonic balance of a NACA 0012 pitching about the quarter chord:
     theta(t) = amp sin(omega t), omega = 2 kred M (chord 1, a_inf = 1), the
     O-grid of naca0012_ogrid (default 256 x 64 x 2 cells in 4 blocks), every
     snapshot on its own rotated grid.  The inviscid run keeps the 1500 wall
     (force surface 1): its halo holds the wall velocity, and the strong
-    boundary face carries no mass flux.  Explicit 4-stage RK, no IRS."""
+    boundary face carries no mass flux.  Explicit 4-stage RK, no IRS, CFL 1
+    (at CFL 2 the explicit time-spectral cycles of this grid lose
+    positivity, in the oracle as on the device)."""
     from .params import set_pitching
     p = naca_params(model, mach=mach, alpha_deg=alpha_deg, reyno=1.0e6, cfl=cfl, eps_irs=0.0)
     set_pitching(p, nharms, amp_deg, kred, xh, 0.0)

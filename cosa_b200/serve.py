@@ -157,60 +157,73 @@ if __name__ == "__main__":
     main()
 
 
-def batched_vs_plain(requests: List[Request], niter: int = 400, device: int = 0, precision: int = 1) -> Dict:
+def batched_vs_plain(requests: List[Request], niter: int = 400, device: int = 0, precision: int = 1,
+                     repeats: int = 3) -> Dict:
     """Throughput of the same solves two ways, `niter` RK cycles each:
     plain -- one after another through the single-solve FP64 path
-    (cosa_gpu_smooth, one context per request, device-timed);
+    (cosa_gpu_smooth, one context per request);
     batched -- all resident in the serving engine at once in the given
-    precision (1 = mixed), advanced by shared stage launches (wall-timed
-    around the engine steps, which synchronise).  Mcell-stage/s of both and
-    their ratio."""
+    precision (1 = mixed), advanced by shared stage launches.
+    Both arms are timed the same way: host wall clock around one
+    synchronous library call per solve (plain) or per engine step of niter
+    cycles (batched), after a warm-up that captures the graphs; the work is
+    counted from the cycles each solve actually completed.  The median over
+    `repeats` measurements of each arm, Mcell-stage/s of both and their
+    ratio."""
     import torch
     from . import gpu as _gpu
     cells = [r.case.ncells for r in requests]
-    work = sum(cells) * 4 * niter
-    # plain FP64, request by request
-    ms = 0.0
-    for r in requests:
-        p = engine_scheme()
-        for k in ("machfs", "alpha", "beta", "rhoinf", "pinf", "ainf", "tinf", "inlet_t0", "inlet_p0"):
-            setattr(p, k, getattr(r.flow, k))
-        for i in range(3):
-            p.inlet_dir[i] = r.flow.inlet_dir[i]
-            p.outlet_p[i] = r.flow.outlet_p[i]
-        ctx = _gpu.Context([r.case.tables], p, device=device)
-        x, y, z = (ctx.alloc_p2(ncomp=1).upload(a) for a in (r.case.x, r.case.y, r.case.z))
-        si, sj, sk, vol = ctx.alloc_p2(), ctx.alloc_p2(), ctx.alloc_p2(), ctx.alloc_p1()
-        ctx.imetrix(1, x, y, z, si, sj, sk)
-        ctx.vols(1, x, y, z, vol)
-        q = ctx.alloc_p3().upload(r.case.q0)
-        ctx.bind_level(1, q=q, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(), si=si, sj=sj, sk=sk, vol=vol)
-        ctx.smooth(1, 5, 1, 10 ** 6, want_hist=False)  # warm-up and graph capture
-        stream = torch.cuda.ExternalStream(ctx.stream())
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ctx.sync()
-        e0.record(stream)
-        ctx.smooth(1, niter, 6, 10 ** 6, want_hist=False)
-        e1.record(stream)
-        e1.synchronize()
-        ms += e0.elapsed_time(e1)
-        ctx.close()
-    plain = work / (ms / 1e3) / 1e6
-    # batched in the serving engine
-    scheme = engine_scheme()
-    scheme.precision = precision
-    srv = Server(scheme, int(40e9), device=device, check_every=10 ** 6)
-    try:
-        ids = [srv.submit(r.case.tables, r.case.x, r.case.y, r.case.z, r.case.q0, r.flow, 0.0, niter + 5)
-               for r in requests]
-        srv.step(5)  # admission, table build and graph capture
-        t0 = time.perf_counter()
-        while any(srv.result(i)["state"] in ("queued", "active") for i in ids):
-            srv.step(50)
-        wall = time.perf_counter() - t0
-    finally:
-        srv.close()
-    batched = work / wall / 1e6
-    return {"requests": len(requests), "cells": int(sum(cells)), "cycles_each": niter,
+
+    def plain_once():
+        secs, work = 0.0, 0
+        for r, nc in zip(requests, cells):
+            p = engine_scheme()
+            for k in ("machfs", "alpha", "beta", "rhoinf", "pinf", "ainf", "tinf", "inlet_t0", "inlet_p0"):
+                setattr(p, k, getattr(r.flow, k))
+            for i in range(3):
+                p.inlet_dir[i] = r.flow.inlet_dir[i]
+                p.outlet_p[i] = r.flow.outlet_p[i]
+            ctx = _gpu.Context([r.case.tables], p, device=device)
+            x, y, z = (ctx.alloc_p2(ncomp=1).upload(a) for a in (r.case.x, r.case.y, r.case.z))
+            si, sj, sk, vol = ctx.alloc_p2(), ctx.alloc_p2(), ctx.alloc_p2(), ctx.alloc_p1()
+            ctx.imetrix(1, x, y, z, si, sj, sk)
+            ctx.vols(1, x, y, z, vol)
+            q = ctx.alloc_p3().upload(r.case.q0)
+            ctx.bind_level(1, q=q, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(), si=si, sj=sj, sk=sk, vol=vol)
+            ctx.smooth(1, 5, 1, 10 ** 6, want_hist=False)  # warm-up and graph capture
+            ctx.sync()
+            t0 = time.perf_counter()
+            _, st = ctx.smooth(1, niter, 6, 10 ** 6, want_hist=False)
+            ctx.sync()
+            secs += time.perf_counter() - t0
+            work += nc * 4 * niter
+            ctx.close()
+        return work / secs / 1e6
+
+    def batched_once():
+        scheme = engine_scheme()
+        scheme.precision = precision
+        srv = Server(scheme, int(40e9), device=device, check_every=10 ** 6)
+        try:
+            ids = [srv.submit(r.case.tables, r.case.x, r.case.y, r.case.z, r.case.q0, r.flow, 0.0, niter + 10)
+                   for r in requests]
+            srv.step(5)  # admission, table build and graph capture
+            before = [srv.result(i)["iters"] for i in ids]
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            srv.step(niter)
+            torch.cuda.synchronize(device)
+            secs = time.perf_counter() - t0
+            after = [srv.result(i)["iters"] for i in ids]
+        finally:
+            srv.close()
+        work = sum(nc * 4 * (b - a) for nc, a, b in zip(cells, before, after))
+        return work / secs / 1e6
+
+    plains = sorted(plain_once() for _ in range(repeats))
+    batches = sorted(batched_once() for _ in range(repeats))
+    plain, batched = plains[len(plains) // 2], batches[len(batches) // 2]
+    return {"requests": len(requests), "cells": int(sum(cells)), "cycles_each": niter, "repeats": repeats,
+            "timing": "host wall clock around synchronous library calls, both arms; median of repeats",
             "plain_fp64_mcell_stage_s": plain, "batched_mcell_stage_s": batched,
             "batched_precision": "mixed" if precision == 1 else "fp64", "speedup": batched / plain}
