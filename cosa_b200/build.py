@@ -15,9 +15,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libcosa_gpu.so")
-SOURCES = ["cosa_gpu.cu"]
+SOURCES = ["cosa_gpu.cu", "io.cpp"]
 HEADERS = ["common.cuh", "physics.cuh", "kernels_ref.cuh", "fused.cuh", "mg.cuh", "visc.cuh", "kom.cuh", "split.cuh", "faces.cuh",
-           "force.cuh", "serve.cuh"]
+           "moving.cuh", "force.cuh", "serve.cuh"]
 
 
 def nvcc() -> str:
@@ -40,7 +40,7 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "cosa_gpu.h")]
+    deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS] + [os.path.join(ROOT, "include", h) for h in ("cosa_gpu.h", "cosa_io.h")]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
