@@ -532,9 +532,10 @@ int check_rans_supported(const cosa_params &p) {
 
 int check_fused_supported(const cosa_params &p) {
   if (p.kom) return check_rans_supported(p);
-  // rkimp: the implicit time-spectral update of harmonic balance, branch
-  // without IRS on one level (update_bhb, src/update.f90:1564-1604)
-  if (p.rkimp && (!p.harbal || p.irsop != 0 || p.nlevel > 1)) return COSA_ERR_UNSUPPORTED;
+  // rkimp: the implicit time-spectral update of harmonic balance (update_bhb,
+  // src/update.f90:1564-1604 without IRS on one level, 1771-1836 with IRS or
+  // multigrid)
+  if (p.rkimp && !p.harbal) return COSA_ERR_UNSUPPORTED;
   if (p.npde != 5 || p.kom || p.kom_bsl || p.kom_sst ||
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
@@ -872,7 +873,10 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   }
   A.strong = L.d_strong; A.smap = L.d_smap; A.status = c->d_status;
   A.ar = p.alphas[irk - 1];
-  A.vol = p.harbal && !p.rkimp ? P.vol : nullptr;  // rkimp: the time-spectral term goes to update_bhb
+  // src_hb adds the time-spectral term to the residual except under rkimp
+  // without IRS on one level, where update_bhb takes it alone
+  // (src/cosa.f90:1918-1922)
+  A.vol = p.harbal && (!p.rkimp || p.irsop > 0 || p.nlevel > 1) ? P.vol : nullptr;
   A.compute_dt = compute_dt;
   A.first_order = nl >= p.nl_crs;
   A.update = update;
@@ -959,6 +963,26 @@ int launch_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
     const double *qold = irk == 1 ? Q : QO;
     double *qcopy = (irk == 1 && o.copy_qold) ? QO : nullptr;
     const int rmode = (irk == 1 && o.force) ? 2 : 1;
+    if (p.rkimp && (p.irsop > 0 || p.nlevel > 1)) {
+      // residual with the time-spectral term -> [IRS] -> update_bhb, which
+      // takes the unsmoothed term out again and solves for it implicitly
+      int r = launch_stage(c, nl, L, qin, qout, qold, nullptr, irk, o.compute_dt && irk == 1, o.want_rms && irk == 1,
+                           0, L.d_res, o.rhs, rmode);
+      if (r) return r;
+      if (p.irsop > 0) {
+        const double *beta[3] = {L.ptrs.betaxi ? L.ptrs.betaxi : L.d_beta[0],
+                                 L.ptrs.betaeta ? L.ptrs.betaeta : L.d_beta[1],
+                                 L.ptrs.betazeta ? L.ptrs.betazeta : L.d_beta[2]};
+        if ((r = irs_apply(c, L, L.d_res, L.d_ores, L.ptrs.dtvol, beta))) return r;
+      }
+      const double *QOLD = qold, *QSRC = qin;
+      r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+        k_update_bhb<<<g, 256, 0, c->s>>>(b, c->d_p, L.d_res, QOLD, qout, qcopy, L.ptrs.dtvol, L.ptrs.vol,
+                                          p.alphas[irk - 1], QSRC);
+      });
+      if (r) return r;
+      continue;
+    }
     if (p.rkimp) {
       // residual without the time-spectral term -> [norm with it] -> the
       // per-cell snapshot solve of update_bhb
@@ -980,7 +1004,7 @@ int launch_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
       const double *QOLD = qold;
       r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
         k_update_bhb<<<g, 256, 0, c->s>>>(b, c->d_p, L.d_res, QOLD, qout, qcopy, L.ptrs.dtvol, L.ptrs.vol,
-                                          p.alphas[irk - 1]);
+                                          p.alphas[irk - 1], nullptr);
       });
       if (r) return r;
       continue;

@@ -848,13 +848,19 @@ __device__ __forceinline__ void hb_lu_solve(int n, double *a, double *bm, int nr
   }
 }
 
-// one thread per interior cell: (I + ar omega dtau D) q = qold - ar res dtvol
-// over the snapshots (dtau = dtvol V of the row's snapshot), the five
-// mean-flow equations as five right-hand sides; qcopy (stage 1) receives qold
+// update_bhb (src/update.f90:1301-1848), mean-flow equations.  One thread
+// per interior cell: (I + ar omega dtau D) q = rhs over the snapshots (dtau =
+// dtvol V of the row's snapshot), the five equations as five right-hand
+// sides; qcopy (stage 1) receives qold.  qsrc null (no IRS, one level): the
+// residual holds no time-spectral term and rhs = qold - ar res dtvol.  qsrc
+// set (IRS or multigrid): the residual, smoothed, includes src_hb's
+// qhb = omega V D q of the stage state qsrc, and rhs = qold + (qhb - res) ar
+// dtvol with qhb recomputed from qsrc in src_bhb's order.
 template <class BS>
 __global__ void k_update_bhb(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
                              const double *__restrict__ qold, double *__restrict__ qout, double *__restrict__ qcopy,
-                             const double *__restrict__ dtv, const double *__restrict__ vol, double ar) {
+                             const double *__restrict__ dtv, const double *__restrict__ vol, double ar,
+                             const double *__restrict__ qsrc) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
@@ -876,7 +882,14 @@ __global__ void k_update_bhb(BS bs_, const cosa_params *__restrict__ Pp, const d
         const int64_t o = p3_var(b, npde, S, m + 1, si) + c;
         const double q0 = qold[o];
         if (qcopy) qcopy[o] = q0;
-        x[si + S * m] = q0 - ar * res[o] * dt;
+        if (qsrc) {
+          double qhb = 0.0;
+          for (int sj = 0; sj < S; ++sj)
+            qhb = qhb + P.omega * v * P.dhb[si * S + sj] * qsrc[p3_var(b, npde, S, m + 1, sj) + c];
+          x[si + S * m] = q0 + (qhb - res[o]) * ar * dt;
+        } else {
+          x[si + S * m] = q0 - ar * res[o] * dt;
+        }
       }
     }
     hb_lu_solve(S, a, x, 5);

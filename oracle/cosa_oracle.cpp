@@ -1398,12 +1398,16 @@ void lu_solve(int n, double *a, double *bm, int nrhs) {
   }
 }
 
-// update_bhb, rkimp branch without IRS on one level, mean-flow equations
-// (src/update.f90:1564-1604): per cell the snapshots are coupled through
-// (I + ar omega dtau D) q = qold - ar res dtvol, dtau = dtvol V of the row's
-// snapshot
+// update_bhb, rkimp, mean-flow equations: per cell the snapshots are coupled
+// through (I + ar omega dtau D) q = rhs, dtau = dtvol V of the row's snapshot.
+// Without IRS on one level (src/update.f90:1564-1604) the residual holds no
+// time-spectral term and rhs = qold - ar res dtvol.  With IRS or multigrid
+// (src/update.f90:1771-1836) src_hb has added qhb = omega V D q to the
+// residual before the smoothing (src/cosa.f90:1918-1922) and
+// rhs = qold + (qhb - res) ar dtvol, qhb recomputed here from the same q in
+// src_bhb's order (src/src.f90:556-600)
 void update_bhb_b(const Level &L, int b, const double *ra, double *qa, const double *qoa, const double *dta,
-                  const double *va, double ar, const cosa_params &P) {
+                  const double *va, double ar, const cosa_params &P, bool src_in_res) {
   const int S = L.S;
   B3 res(const_cast<double *>(ra), L, b), q(qa, L, b), qold(const_cast<double *>(qoa), L, b);
   B1 dtv(const_cast<double *>(dta), L, b, S), vol(const_cast<double *>(va), L, b, 1);
@@ -1417,8 +1421,16 @@ void update_bhb_b(const Level &L, int b, const double *ra, double *qa, const dou
             a[ni + S * nj] = (ni == nj ? 1.0 : 0.0) + ar * P.omega * dtau * P.dhb[ni * S + nj];
         }
         for (int ni = 0; ni < S; ++ni)
-          for (int m = 0; m < 5; ++m)
-            x[ni + S * m] = qold(i, j, k, m + 1, ni) - ar * res(i, j, k, m + 1, ni) * dtv(i, j, k, ni);
+          for (int m = 0; m < 5; ++m) {
+            if (src_in_res) {
+              double qhb = 0.0;
+              for (int nj = 0; nj < S; ++nj)
+                qhb = qhb + P.omega * vol(i, j, k) * P.dhb[ni * S + nj] * q(i, j, k, m + 1, nj);
+              x[ni + S * m] = qold(i, j, k, m + 1, ni) + (qhb - res(i, j, k, m + 1, ni)) * ar * dtv(i, j, k, ni);
+            } else {
+              x[ni + S * m] = qold(i, j, k, m + 1, ni) - ar * res(i, j, k, m + 1, ni) * dtv(i, j, k, ni);
+            }
+          }
         lu_solve(S, a, x, 5);
         for (int ni = 0; ni < S; ++ni)
           for (int m = 0; m < 5; ++m) q(i, j, k, m + 1, ni) = x[ni + S * m];
@@ -3480,23 +3492,32 @@ int orc_smooth_hb(orc_level *h, const cosa_params *p, int ncycles, int mgit0, in
   int status = 0;
   const int last = mgit0 + ncycles - 1;
   // rkimp without IRS on one level: the time-spectral term is not added to
-  // the residual (src/cosa.f90:1918-1922) but solved in update_bhb
+  // the residual (src/cosa.f90:1918-1922) but solved in update_bhb; with IRS
+  // src_hb adds it and update_bhb takes it out again
   const bool imp = p->rkimp != 0;
-  if (imp && (p->irsop != 0 || p->nlevel > 1 || L.npde != 5)) return COSA_ERR_UNSUPPORTED;
+  const bool src_in_res = !imp || p->irsop > 0 || p->nlevel > 1;
+  if (imp && L.npde != 5) return COSA_ERR_UNSUPPORTED;
+  std::vector<double> beta;
+  double *bx = nullptr, *by = nullptr, *bz = nullptr;
+  if (p->irsop > 0) {
+    beta.assign((size_t)3 * L.n1 * L.S, 0.0);
+    bx = beta.data(); by = bx + L.n1 * L.S; bz = by + L.n1 * L.S;
+  }
   for (int mgit = mgit0; mgit <= last; ++mgit) {
     const int iter = 1;
     copy_interior(L, qold, q);
     for (int irk = 1; irk <= p->nstage; ++irk) {
       const bool want_dt = (iter / p->iupdt * p->iupdt == iter) && irk == 1;
-      status |= residual_impl(h, p, 1, q, si, sj, sk, res, qp, qm, dq, dqp, dqm, flux, dtvol, want_dt, nullptr,
-                              nullptr, nullptr, imp ? nullptr : vol);
+      status |= residual_impl(h, p, 1, q, si, sj, sk, res, qp, qm, dq, dqp, dqm, flux, dtvol, want_dt, bx, by, bz,
+                              src_in_res ? vol : nullptr);
       if (irk == 1 && (mgit == 1 || mgit % rms_every == 0 || mgit == last) && hist) {
-        if (imp) resg_rms_hbimp_level(L, res, q, vol, *p, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
+        if (!src_in_res) resg_rms_hbimp_level(L, res, q, vol, *p, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
         else resg_rms_hb_level(L, res, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
       }
+      if (p->irsop > 0) irs_level(L, res, dtvol, nullptr, bx, by, bz, nullptr, nullptr, nullptr, *p);
 #pragma omp parallel for schedule(dynamic)
       for (int b = 0; b < L.nb; ++b) {
-        if (imp) update_bhb_b(L, b, res, q, qold, dtvol, vol, p->alphas[irk - 1], *p);
+        if (imp) update_bhb_b(L, b, res, q, qold, dtvol, vol, p->alphas[irk - 1], *p, src_in_res);
         else update_b(L, b, res, q, qold, dtvol, p->alphas[irk - 1]);
       }
     }
@@ -3589,16 +3610,23 @@ int orc_smooth_level(orc_level *h, const cosa_params *p, int nl, const cosa_leve
   int status = 0;
   const int niterp = to_coarse ? niter + 1 : niter;
   std::vector<double> work;
+  // harmonic balance: src_hb in the residual unless rkimp without IRS on one
+  // level (src/cosa.f90:1918-1922)
+  const bool imp = p->harbal && p->rkimp;
+  const bool src_in_res = p->harbal && (!p->rkimp || p->irsop > 0 || p->nlevel > 1);
+  if (imp && L.npde != 5) return COSA_ERR_UNSUPPORTED;
   for (int iter = 1; iter <= niterp; ++iter) {
     if (iter <= niter) copy_interior(L, P->qold, P->q);
     for (int irk = 1; irk <= p->nstage; ++irk) {
       const bool want_dt = (iter / p->iupdt * p->iupdt == iter) && irk == 1;
       status |= residual_impl(h, p, nl, P->q, P->si, P->sj, P->sk, P->res, P->qp, P->qm, P->dq, P->dqp, P->dqm,
                               P->flux, P->dtvol, want_dt, P->betaxi, P->betaeta, P->betazeta,
-                              p->harbal ? P->vol : nullptr);
+                              src_in_res ? P->vol : nullptr);
       if (nl == 1 && irk == 1 && iter != niter + 1 && hist_row &&
           (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle)) {
-        if (p->harbal) {
+        if (imp && !src_in_res) {
+          resg_rms_hbimp_level(L, P->res, P->q, P->vol, *p, hist_row);
+        } else if (p->harbal) {
           work.assign(P->res, P->res + L.n3 * L.npde * L.S);
           resg_rms_hb_level(L, work.data(), hist_row);
         } else {
@@ -3611,7 +3639,10 @@ int orc_smooth_level(orc_level *h, const cosa_params *p, int nl, const cosa_leve
       if (p->irsop > 0)
         irs_level(L, P->res, P->dtvol, nullptr, P->betaxi, P->betaeta, P->betazeta, nullptr, nullptr, nullptr, *p);
 #pragma omp parallel for schedule(dynamic)
-      for (int b = 0; b < L.nb; ++b) update_b(L, b, P->res, P->q, P->qold, P->dtvol, p->alphas[irk - 1]);
+      for (int b = 0; b < L.nb; ++b) {
+        if (imp) update_bhb_b(L, b, P->res, P->q, P->qold, P->dtvol, P->vol, p->alphas[irk - 1], *p, src_in_res);
+        else update_b(L, b, P->res, P->q, P->qold, P->dtvol, p->alphas[irk - 1]);
+      }
     }
   }
   return status;

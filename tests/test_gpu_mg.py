@@ -256,14 +256,17 @@ def test_mg_irs_matches_oracle(oracle_mod):
     ctx.close()
 
 
-def test_mg_harmonic_balance_matches_oracle(oracle_mod):
+@pytest.mark.parametrize("rkimp", [0, 1])
+def test_mg_harmonic_balance_matches_oracle(oracle_mod, rkimp):
     """Two-level cycles of a harmonic-balance case (S = 3): the coupling
-    source on both levels, snapshot-averaged norms on the fine level."""
+    source on both levels, snapshot-averaged norms on the fine level; with
+    rkimp the multigrid branch of update_bhb on both levels."""
     from cosa_b200.params import set_harmonic_balance
     case = casekit.small_partitioned(32, 16, 4)
     p = set_harmonic_balance(case.params, 1, 0.16)
     p.nlevel = 2
     p.cfl = 1.0
+    p.rkimp = rkimp
     case.q0 = cases._freestream_state(case.tables, p)
     S = 3
     q = cases.perturbed_state(case, amp=0.01, seed=14)

@@ -362,15 +362,21 @@ def test_src_hb_matches_oracle(oracle_mod):
     ctx.close()
 
 
-@pytest.mark.parametrize("nharms,rkimp", [(1, 0), (3, 0), (1, 1), (3, 1)])
-def test_fused_smooth_hb_matches_oracle(oracle_mod, nharms, rkimp):
+@pytest.mark.parametrize("nharms,rkimp,irsop,cutcirs", [(1, 0, 0, 0), (3, 0, 0, 0), (1, 1, 0, 0), (3, 1, 0, 0),
+                                                       (1, 1, 1, 0), (2, 1, 2, 1), (2, 0, 2, 1)])
+def test_fused_smooth_hb_matches_oracle(oracle_mod, nharms, rkimp, irsop, cutcirs):
     """Harmonic balance with all snapshots batched in the tile launch:
     per-snapshot time steps, the coupling source and the snapshot-averaged
     residual norm (resg_rms_hb) against the oracle for 4 cycles; with rkimp
     the time-spectral term leaves the residual and each cell's snapshots are
-    coupled by the LU solve of update_bhb (its norm adds the term back)."""
+    coupled by the LU solve of update_bhb (its norm adds the term back).
+    With IRS (rkimp or not) the term is in the smoothed residual and
+    update_bhb takes the unsmoothed term out again."""
     case = _hb_case(nharms)
-    case.params.rkimp = rkimp
+    p = case.params
+    p.rkimp = rkimp
+    if irsop:
+        p.irsop, p.cutcirs, p.rat = irsop, cutcirs, float(np.sqrt(1 + 4 * 0.6))
     S = 2 * nharms + 1
     O = oracle_mod.OracleLevel(case.tables, case.params)
     si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
@@ -381,8 +387,9 @@ def test_fused_smooth_hb_matches_oracle(oracle_mod, nharms, rkimp):
     ctx = gpu.Context([case.tables], case.params)
     dq_ = ctx.alloc_p3().upload(q)
     m = [ctx.alloc_p2().upload(a) for a in (si, sj, sk)]
+    extra = {k: ctx.alloc_p1(nsnap=S) for k in ("betaxi", "betaeta", "betazeta")} if irsop >= 2 else {}
     ctx.bind_level(1, q=dq_, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(nsnap=S), si=m[0], sj=m[1], sk=m[2],
-                   vol=ctx.alloc_p1().upload(vol))
+                   vol=ctx.alloc_p1().upload(vol), **extra)
     hist_g, st = ctx.smooth(1, 4, 1, 2)
     assert st == 0
     a = casekit.interior_cells(case, dq_.download(), 5, S)

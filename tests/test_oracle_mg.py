@@ -297,3 +297,44 @@ def test_implicit_hb_update(oracle_mod):
         assert st == 0 and rows[-1, 0] < 0.5 * rows[0, 0]
         qs[imp] = q
     assert np.abs(qs[1] - qs[0]).max() > 1e-6
+
+
+def test_implicit_hb_update_irs_branch(oracle_mod):
+    """rkimp with IRS (src/update.f90:1771-1836): src_hb's term enters the
+    residual and update_bhb takes it out again.  With a smoothing
+    coefficient of zero (rat = 1) IRS is the identity, so the IRS branch must
+    reproduce the branch without IRS to rounding; with rat > 1 both converge
+    and differ on the way."""
+    from cosa_b200.params import set_harmonic_balance
+    case = casekit.small_partitioned()
+    p = set_harmonic_balance(case.params, 1, 0.16)
+    p.rkimp = 1
+    case.q0 = cases._freestream_state(case.tables, p)
+    O = oracle_mod.OracleLevel(case.tables, p)
+    si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
+
+    def state():
+        q = cases.perturbed_state(case, seed=4)
+        for v in cases.p3_views(case.tables, q, 5, 3):
+            for n in range(3):
+                v[..., 1, n] *= 1 + 0.05 * np.sin(2 * np.pi * n / 3)
+        return q
+
+    out = {}
+    for irsop, rat in ((0, 1.0), (1, 1.0), (1, 1.6)):
+        p.irsop, p.rat, p.cutcirs = irsop, rat, 0
+        q = state()
+        h, st = oracle_mod.smooth_hb(O, q, si, sj, sk, vol, 40, rms_every=10)
+        assert st == 0
+        out[(irsop, rat)] = (q, h)
+    q0, h0 = out[(0, 1.0)]
+    q1, h1 = out[(1, 1.0)]
+    np.testing.assert_allclose(q1, q0, rtol=0, atol=1e-12)
+    rows = ~np.isnan(h0[:, 0])
+    # the norms differ by design: without IRS the term is added back to the
+    # unsmoothed residual, with IRS the residual already holds it
+    np.testing.assert_allclose(h1[rows], h0[rows], rtol=1e-8)
+    q2, h2 = out[(1, 1.6)]
+    assert np.isfinite(q2).all() and np.abs(q2 - q0).max() > 1e-8
+    r2 = h2[~np.isnan(h2[:, 0])]
+    assert r2[-1, 0] < r2[0, 0]
