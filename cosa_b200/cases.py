@@ -142,7 +142,7 @@ def _freestream_state(tables: LevelTables, p: CosaParams) -> np.ndarray:
         v[..., 2, :] = p.rhoinf * p.machfs * sa * cb
         v[..., 3, :] = p.rhoinf * p.machfs * sb
         v[..., 4, :] = 1 / p.rhoinf / p.gamma / (p.gamma - 1) + 0.5 * p.machfs ** 2
-        if p.kom:
+        if p.kom or p.kom_bsl or p.kom_sst:
             # interior cells only (src/input.f90:4826-4836)
             v[2:-2, 2:-2, 2:-2, 5, :] = p.rhoinf * p.tkefar
             v[2:-2, 2:-2, 2:-2, 6, :] = p.rhoinf * p.omefar

@@ -32,10 +32,10 @@ class SteadySolver:
         self.nlevel = max(1, int(p.nlevel))
         self.ncycle = ncycle
         # k-omega CFL ramp of bdeltat: dict(mode=1|2, ncycr=(n0..n3), vcfli=(3), vcflit=(3))
-        self.ramp = ramp if (ramp and p.kom) else None
+        self.ramp = ramp if (ramp and (p.kom or p.kom_bsl or p.kom_sst)) else None
         self._cfl = None
         self.viscous = bool(p.viscous)
-        self.kom = bool(p.kom)
+        self.kom = bool(p.kom or p.kom_bsl or p.kom_sst)
         lv = cases.mg_levels(case, self.nlevel) if self.nlevel > 1 else [(case.tables, case.x, case.y, case.z)]
         ctx = gpu.Context([t for (t, _, _, _) in lv], p, device=device)
         self.ctx = ctx

@@ -156,6 +156,47 @@ struct B0 {  // flux (im, jm, km, npde, 0:S-1), 1-based
 };
 
 inline bool is_kom(const cosa_params &p) { return p.kom || p.kom_bsl || p.kom_sst; }
+inline bool is_blend(const cosa_params &p) { return p.kom_bsl || p.kom_sst; }
+
+struct B3t {  // ttrm (-1:im+1,-1:jm+1,-1:km+1, 3, 0:S-1)
+  double *p; int I, J; int64_t P;
+  B3t(double *base, const Level &L, int b) : I(L.im[b] + 3), J(L.jm[b] + 3) {
+    P = (int64_t)I * J * (L.km[b] + 3);
+    p = base + L.op3[b] * 3 * L.S;
+  }
+  inline double &operator()(int i, int j, int k, int c, int n) const {
+    return p[((int64_t)n * 3 + (c - 1)) * P + (i + 1) + (int64_t)I * ((j + 1) + (int64_t)J * (k + 1))];
+  }
+};
+struct B0s {  // face distance (im, jm, km), 1-based
+  double *p; int I, J;
+  B0s(double *base, const Level &L, int b) : I(L.im[b]), J(L.jm[b]) { p = base + L.of0[b]; }
+  inline double &operator()(int i, int j, int k) const {
+    return p[(i - 1) + (int64_t)I * ((j - 1) + (int64_t)J * (k - 1))];
+  }
+};
+
+// the BSL/SST closure constants of input() (src/input.f90:2522-2539)
+struct Blend {
+  double sigk1, sigk2, sigw1, sigw2, b1, b2, bstr, g1, g2, a1;
+};
+inline Blend blend_of(const cosa_params &P) {
+  Blend c;
+  c.bstr = 0.09;
+  c.a1 = 0.31;
+  c.sigk1 = P.kom_sst ? 0.85 : 0.5;
+  c.sigk2 = 1.0;
+  c.sigw1 = 0.5;
+  c.b1 = 3.0 / 40.0;
+  c.g1 = c.b1 / c.bstr - c.sigw1 * (P.kappa * P.kappa) / std::sqrt(c.bstr);
+  c.sigw2 = 0.856;
+  c.b2 = 0.0828;
+  c.g2 = c.b2 / c.bstr - c.sigw2 * (P.kappa * P.kappa) / std::sqrt(c.bstr);
+  return c;
+}
+// x**4 and the blending tanh as the reference writes them
+inline double pow4(double x) { const double x2 = x * x; return x2 * x2; }
+inline double tanh_ref(double a) { return (std::exp(2 * a) - 1) / (std::exp(2 * a) + 1); }
 
 // ---- cons2prim_b (src/update.f90:2135-2188) --------------------------------
 void cons2prim_b(const Level &L, int b, double *qa, int xtnd, const cosa_params &P) {
@@ -1821,15 +1862,17 @@ void lim_prod_mg_b(const Level &L, int b, const double *qa, double *prda, const 
 // point-implicit update cannot take rho omega below gkw cmu rho sqrt(prd);
 // ttrm = (0, gkw, bkw) for the Wilcox model
 void lim_res_ome_b(const Level &L, int b, double *ra, const double *qa, const double *va, const double *dtta,
-                   const double *dpla, const double *prda, double ar, const cosa_params &P) {
+                   const double *dpla, const double *prda, double ar, const cosa_params &P,
+                   const double *ttrma = nullptr) {
   B3 res(ra, L, b), q(const_cast<double *>(qa), L, b);
   B1 vol(const_cast<double *>(va), L, b, 1), dtt(const_cast<double *>(dtta), L, b, L.S);
   B3s dpl(const_cast<double *>(dpla), L, b), prd(const_cast<double *>(prda), L, b);
-  const double gav = P.gkw, bav = P.bkw;
   for (int n = 0; n < L.S; ++n)
     for (int k = 1; k <= L.km[b] - 1; ++k)
       for (int j = 1; j <= L.jm[b] - 1; ++j)
         for (int i = 1; i <= L.im[b] - 1; ++i) {
+          const double gav = ttrma ? B3t(const_cast<double *>(ttrma), L, b)(i, j, k, 2, n) : P.gkw;
+          const double bav = ttrma ? B3t(const_cast<double *>(ttrma), L, b)(i, j, k, 3, n) : P.bkw;
           const double dtau = dtt(i, j, k, n) * vol(i, j, k);
           const double rho = q(i, j, k, 1, n), ome = q(i, j, k, 7, n) / q(i, j, k, 1, n);
           const double den1 = 1 + ar * dtau * (gav * dpl(i, j, k, n) + 2 * bav * ome);
@@ -2799,7 +2842,7 @@ void rtst_b(const Level &L, int b, int d, const double *qfa, const double *dxa, 
 // omega row keeps the reference's dk/dz in place of domega/dz
 void vflux_kom_b(const Level &L, int b, int d, const double *qfa, const double *dxa, const double *dya,
                  const double *dza, const double *taua, const double *xd, const double *ed, const double *zd,
-                 const double *sijk, double *fa, const cosa_params &P) {
+                 const double *sijk, double *fa, const cosa_params &P, const double *fdista = nullptr) {
   B3 qf(const_cast<double *>(qfa), L, b), dqx(const_cast<double *>(dxa), L, b);
   B3 dqe(const_cast<double *>(dya), L, b), dqz(const_cast<double *>(dza), L, b), tau(const_cast<double *>(taua), L, b);
   BV xv(const_cast<double *>(xd), L, b), ev(const_cast<double *>(ed), L, b), zv(const_cast<double *>(zd), L, b);
@@ -2832,8 +2875,25 @@ void vflux_kom_b(const Level &L, int b, int d, const double *qfa, const double *
           flux(i, j, k, 2, n) = -(txx * kx + txy * ky + txz * kz) * ds;
           flux(i, j, k, 3, n) = -(txy * kx + tyy * ky + tyz * kz) * ds;
           flux(i, j, k, 4, n) = -(txz * kx + tyz * ky + tzz * kz) * ds;
-          const double ctke = (mu + P.sigk * mut) * P.machfs / P.reyno;
-          const double come = (mu + P.sigw * mut) * P.machfs / P.reyno;
+          double sigk = P.sigk, sigw = P.sigw;
+          if (is_blend(P)) {
+            // BSL/SST (src/flux.f90:987-1061): sigma_k and sigma_omega blended by
+            // F1 of the face state and the face's wall distance
+            const Blend c = blend_of(P);
+            const double tke = qf(i, j, k, 6, n), ome = qf(i, j, k, 7, n);
+            const double domedz = omexi * xiz + omeeta * etaz + omezeta * zetaz;
+            const double fd = B0s(const_cast<double *>(fdista), L, b)(i, j, k) + P.epst;
+            double arg1 = std::max(std::sqrt(tke) / 0.09 / ome / fd, 500 * mu / rho / ome / (fd * fd) * P.machfs / P.reyno);
+            const double cdt = 2 * rho * c.sigw2 / ome * (dtkedx * domedx + dtkedy * domedy + dtkedz * domedz);
+            const double acdt = std::max(cdt, 1.0e-20);
+            arg1 = std::min(arg1, 4 * rho * c.sigw2 * tke / acdt / (fd * fd));
+            arg1 = std::min(pow4(arg1), 1.0e2);
+            const double f1 = tanh_ref(arg1);
+            sigk = f1 * c.sigk1 + (1 - f1) * c.sigk2;
+            sigw = f1 * c.sigw1 + (1 - f1) * c.sigw2;
+          }
+          const double ctke = (mu + sigk * mut) * P.machfs / P.reyno;
+          const double come = (mu + sigw * mut) * P.machfs / P.reyno;
           flux(i, j, k, 5, n) = -ctke * (dtkedx * kx + dtkedy * ky + dtkedz * kz) * ds;
           flux(i, j, k, 6, n) = -ctke * (dtkedx * kx + dtkedy * ky + dtkedz * kz) * ds;
           flux(i, j, k, 7, n) = -come * (domedx * kx + domedy * ky + dtkedz * kz) * ds;
@@ -2842,16 +2902,19 @@ void vflux_kom_b(const Level &L, int b, int d, const double *qfa, const double *
 }
 
 // bq_der_ci/cj/ck (src/flux.f90:2979-3130): cell-centred differences of the
-// face values of family d for the velocity components
-void q_der_c_b(const Level &L, int b, int d, const double *qfa, double *dca) {
+// face values of family d for the velocity components, and for k and omega
+// under BSL/SST
+void q_der_c_b(const Level &L, int b, int d, const double *qfa, double *dca, bool blend = false) {
   B3 qf(const_cast<double *>(qfa), L, b), dc(dca, L, b);
   const int di = d == 1, dj = d == 2, dk = d == 3;
   for (int n = 0; n < L.S; ++n)
-    for (int v = 2; v <= 4; ++v)
+    for (int v = 2; v <= (blend ? 7 : 4); ++v) {
+      if (v == 5) continue;
       for (int k = 1; k <= L.km[b] - 1; ++k)
         for (int j = 1; j <= L.jm[b] - 1; ++j)
           for (int i = 1; i <= L.im[b] - 1; ++i)
             dc(i, j, k, v, n) = qf(i + di, j + dj, k + dk, v, n) - qf(i, j, k, v, n);
+    }
 }
 
 // turprod_b (src/src.f90:40-177): production P_d (alternative form), div u,
@@ -2934,19 +2997,215 @@ void srckw_b(const Level &L, int b, int nl, const double *qa, const double *muta
         }
 }
 
-// update_b, explicit k-omega part (src/update.f90:601-640): point-implicit
-// rho*omega then rho*k with the destruction terms, omega floored by the
-// production; ttrm = (0, gkw, bkw) for the Wilcox model (update_ttrm_b)
-void update_kom_b(const Level &L, int b, const double *ra, double *qa, const double *qoa, const double *va,
-                  const double *dtta, const double *dpla, const double *prda, double ar, const cosa_params &P) {
-  B3 res(const_cast<double *>(ra), L, b), q(qa, L, b), qold(const_cast<double *>(qoa), L, b);
-  B1 vol(const_cast<double *>(va), L, b, 1), dtt(const_cast<double *>(dtta), L, b, L.S);
-  B3s dpl(const_cast<double *>(dpla), L, b), prd(const_cast<double *>(prda), L, b);
-  const double gav = P.gkw, bav = P.bkw;
+// ---- BSL / SST (src/update.f90:2340-2460, 3000-3161; src/src.f90:275-378;
+// src/grid.f90:2809-2870) ------------------------------------------------------
+// facedist_b: wall distance of the faces of each family, the mean of the
+// two cells' distances and the boundary cell's own on the block faces
+void facedist_level(const Level &L, const double *dista, double *fi, double *fj, double *fk) {
+  for (int b = 0; b < L.nb; ++b) {
+    B1 dist(const_cast<double *>(dista), L, b, 1);
+    B0s FI(fi, L, b), FJ(fj, L, b), FK(fk, L, b);
+    const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+    for (int k = 1; k <= km - 1; ++k)
+      for (int j = 1; j <= jm - 1; ++j) {
+        FI(1, j, k) = dist(0, j, k);
+        for (int i = 2; i <= im - 1; ++i) FI(i, j, k) = (dist(i - 1, j, k) + dist(i, j, k)) / 2;
+        FI(im, j, k) = dist(im, j, k);
+      }
+    for (int k = 1; k <= km - 1; ++k)
+      for (int i = 1; i <= im - 1; ++i) {
+        FJ(i, 1, k) = dist(i, 0, k);
+        for (int j = 2; j <= jm - 1; ++j) FJ(i, j, k) = (dist(i, j - 1, k) + dist(i, j, k)) / 2;
+        FJ(i, jm, k) = dist(i, jm, k);
+      }
+    for (int j = 1; j <= jm - 1; ++j)
+      for (int i = 1; i <= im - 1; ++i) {
+        FK(i, j, 1) = dist(i, j, 0);
+        for (int k = 2; k <= km - 1; ++k) FK(i, j, k) = (dist(i, j, k - 1) + dist(i, j, k)) / 2;
+        FK(i, j, km) = dist(i, j, km);
+      }
+  }
+}
+
+// the cell-centre inverse metrics of turprod_b / update_ttrm_b: each
+// Cartesian derivative of xi, eta, zeta averaged over the two faces of the
+// family it is stored on
+struct CellMet { double xix, xiy, xiz, etax, etay, etaz, zetax, zetay, zetaz; };
+inline CellMet cell_met(const Level &L, int b, const double *vm, int i, int j, int k) {
+  auto V = [&](int d, int m) { return BV(const_cast<double *>(vm) + (int64_t)((d - 1) * 3 + m) * 3 * L.n0, L, b); };
+  const BV xi_i = V(1, 0), xi_j = V(2, 0), xi_k = V(3, 0);
+  const BV et_i = V(1, 1), et_j = V(2, 1), et_k = V(3, 1);
+  const BV ze_i = V(1, 2), ze_j = V(2, 2), ze_k = V(3, 2);
+  CellMet m;
+  m.xix = (xi_i(1, i + 1, j, k) + xi_i(1, i, j, k)) / 2;
+  m.xiy = (xi_j(2, i, j + 1, k) + xi_j(2, i, j, k)) / 2;
+  m.xiz = (xi_k(3, i, j, k + 1) + xi_k(3, i, j, k)) / 2;
+  m.etax = (et_i(1, i + 1, j, k) + et_i(1, i, j, k)) / 2;
+  m.etay = (et_j(2, i, j + 1, k) + et_j(2, i, j, k)) / 2;
+  m.etaz = (et_k(3, i, j, k + 1) + et_k(3, i, j, k)) / 2;
+  m.zetax = (ze_i(1, i + 1, j, k) + ze_i(1, i, j, k)) / 2;
+  m.zetay = (ze_j(2, i, j + 1, k) + ze_j(2, i, j, k)) / 2;
+  m.zetaz = (ze_k(3, i, j, k + 1) + ze_k(3, i, j, k)) / 2;
+  return m;
+}
+
+// update_ttrm_b: ttrm = (cross diffusion (1 - F1) CD, gamma, beta) blended
+// by F1 from the primitive state, the cell-centred k and omega differences
+// and the cell wall distance; Wilcox: (0, gkw, bkw)
+void update_ttrm_b(const Level &L, int b, const double *qa, const double *dxa, const double *dya, const double *dza,
+                   const double *vm, double *ttrma, const double *dista, const cosa_params &P) {
+  B3 q(const_cast<double *>(qa), L, b), dqx(const_cast<double *>(dxa), L, b);
+  B3 dqe(const_cast<double *>(dya), L, b), dqz(const_cast<double *>(dza), L, b);
+  B3t ttrm(ttrma, L, b);
+  B1 dist(const_cast<double *>(dista), L, b, 1);
+  const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+  if (P.kom) {
+    for (int n = 0; n < L.S; ++n)
+      for (int k = 1; k <= km - 1; ++k)
+        for (int j = 1; j <= jm - 1; ++j)
+          for (int i = 1; i <= im - 1; ++i) {
+            ttrm(i, j, k, 1, n) = 0.0;
+            ttrm(i, j, k, 2, n) = P.gkw;
+            ttrm(i, j, k, 3, n) = P.bkw;
+          }
+    return;
+  }
+  const Blend c = blend_of(P);
+  for (int n = 0; n < L.S; ++n)
+    for (int k = 1; k <= km - 1; ++k)
+      for (int j = 1; j <= jm - 1; ++j)
+        for (int i = 1; i <= im - 1; ++i) {
+          const double rho = q(i, j, k, 1, n), tke = q(i, j, k, 6, n), ome = q(i, j, k, 7, n), p = q(i, j, k, 5, n);
+          const double t = P.gamma * p / rho;
+          const double mu = (P.stemp + 1) / (t + P.stemp) * std::pow(t, 1.5);
+          const CellMet m = cell_met(L, b, vm, i, j, k);
+          const double tkexi = dqx(i, j, k, 6, n), tkeeta = dqe(i, j, k, 6, n), tkezeta = dqz(i, j, k, 6, n);
+          const double omexi = dqx(i, j, k, 7, n), omeeta = dqe(i, j, k, 7, n), omezeta = dqz(i, j, k, 7, n);
+          const double dtkedx = tkexi * m.xix + tkeeta * m.etax + tkezeta * m.zetax;
+          const double dtkedy = tkexi * m.xiy + tkeeta * m.etay + tkezeta * m.zetay;
+          const double dtkedz = tkexi * m.xiz + tkeeta * m.etaz + tkezeta * m.zetaz;
+          const double domedx = omexi * m.xix + omeeta * m.etax + omezeta * m.zetax;
+          const double domedy = omexi * m.xiy + omeeta * m.etay + omezeta * m.zetay;
+          const double domedz = omexi * m.xiz + omeeta * m.etaz + omezeta * m.zetaz;
+          const double dd = dist(i, j, k) + P.epst;
+          double arg1 = std::max(std::sqrt(tke) / 0.09 / ome / dd, 500 * mu / rho / ome / (dd * dd) * P.machfs / P.reyno);
+          const double cdt = 2 * rho * c.sigw2 / ome * (dtkedx * domedx + dtkedy * domedy + dtkedz * domedz);
+          const double acdt = std::max(cdt, 1.0e-20);
+          arg1 = std::min(arg1, 4 * rho * c.sigw2 * tke / acdt / (dd * dd));
+          arg1 = pow4(arg1);
+          arg1 = std::min(arg1, 1.0e2);
+          const double f1 = tanh_ref(arg1);
+          ttrm(i, j, k, 1, n) = cdt * (1 - f1);
+          ttrm(i, j, k, 2, n) = f1 * c.g1 + (1 - f1) * c.g2;
+          ttrm(i, j, k, 3, n) = f1 * c.b1 + (1 - f1) * c.b2;
+        }
+}
+
+// srckw_sst_b: the k source of srckw_b and the omega source with the blended
+// gamma, beta and the cross-diffusion term
+void srckw_sst_b(const Level &L, int b, int nl, const double *qa, const double *muta, const double *prda,
+                 const double *diva, double *ra, const double *ttrma, const double *va, const cosa_params &P) {
+  B3 q(const_cast<double *>(qa), L, b), res(ra, L, b);
+  B3s mu(const_cast<double *>(muta), L, b), prd(const_cast<double *>(prda), L, b), dvv(const_cast<double *>(diva), L, b);
+  B3t ttrm(const_cast<double *>(ttrma), L, b);
+  B1 vol(const_cast<double *>(va), L, b, 1);
+  const double fact = 2.0 / 3.0, mor = P.machfs / P.reyno;
   for (int n = 0; n < L.S; ++n)
     for (int k = 1; k <= L.km[b] - 1; ++k)
       for (int j = 1; j <= L.jm[b] - 1; ++j)
         for (int i = 1; i <= L.im[b] - 1; ++i) {
+          const double rho = q(i, j, k, 1, n), tke = q(i, j, k, 6, n), ome = q(i, j, k, 7, n);
+          const double mut = mu(i, j, k, n), divv = dvv(i, j, k, n);
+          double prod = prd(i, j, k, n), prodw = prd(i, j, k, n);
+          const double cdif = ttrm(i, j, k, 1, n), gav = ttrm(i, j, k, 2, n), bav = ttrm(i, j, k, 3, n);
+          if (P.lim_prodtke && (nl == 1 || P.prd_all_lvls)) {
+            const double tstdis = P.prdlim * P.bstrkw * rho * tke * ome;
+            if (mor * mut * prod > tstdis) {
+              prod = tstdis / mor / mut;
+              if (P.lim_prodomega) prodw = prod;
+            }
+          }
+          res(i, j, k, 6, n) = res(i, j, k, 6, n) -
+                               vol(i, j, k) * (mor * mut * prod - fact * divv * rho * tke - P.bstrkw * rho * tke * ome);
+          res(i, j, k, 7, n) = res(i, j, k, 7, n) - vol(i, j, k) * (gav * P.cmu * rho * prodw - gav * fact * divv * rho * ome -
+                                                                    bav * rho * (ome * ome) + cdif);
+        }
+}
+
+// tur_vis_sst_b: mut = a1 rho k / max(a1 omega, sqrt(2 S) F2) of the
+// conservative state with the stage's cell-centred velocity differences;
+// the face halos copy the adjacent cell (edges and corners are left)
+void tur_vis_sst_level(const Level &L, const double *qa, double *muta, const double *dxa, const double *dya,
+                       const double *dza, const double *vm, const double *dista, const cosa_params &P) {
+  const Blend c = blend_of(P);
+  for (int b = 0; b < L.nb; ++b) {
+    B3 q(const_cast<double *>(qa), L, b), dqx(const_cast<double *>(dxa), L, b);
+    B3 dqe(const_cast<double *>(dya), L, b), dqz(const_cast<double *>(dza), L, b);
+    B3s mut(muta, L, b);
+    B1 dist(const_cast<double *>(dista), L, b, 1);
+    const int im = L.im[b], jm = L.jm[b], km = L.km[b];
+    for (int n = 0; n < L.S; ++n) {
+      for (int k = 1; k <= km - 1; ++k)
+        for (int j = 1; j <= jm - 1; ++j)
+          for (int i = 1; i <= im - 1; ++i) {
+            const double q1 = q(i, j, k, 1, n), q2 = q(i, j, k, 2, n), q3 = q(i, j, k, 3, n), q4 = q(i, j, k, 4, n);
+            const double p = (P.gamma - 1) * (q(i, j, k, 5, n) - (q2 * q2 + q3 * q3 + q4 * q4) / q1 / 2 - q(i, j, k, 6, n));
+            const double rho = q1, tke = q(i, j, k, 6, n) / rho, ome = q(i, j, k, 7, n) / rho;
+            const double t = P.gamma * p / rho;
+            const double mu = (P.stemp + 1) / (t + P.stemp) * std::pow(t, 1.5);
+            const CellMet m = cell_met(L, b, vm, i, j, k);
+            const double uxi = dqx(i, j, k, 2, n), ueta = dqe(i, j, k, 2, n), uzeta = dqz(i, j, k, 2, n);
+            const double vxi = dqx(i, j, k, 3, n), veta = dqe(i, j, k, 3, n), vzeta = dqz(i, j, k, 3, n);
+            const double wxi = dqx(i, j, k, 4, n), weta = dqe(i, j, k, 4, n), wzeta = dqz(i, j, k, 4, n);
+            const double dudx = uxi * m.xix + ueta * m.etax + uzeta * m.zetax;
+            const double dudy = uxi * m.xiy + ueta * m.etay + uzeta * m.zetay;
+            const double dudz = uxi * m.xiz + ueta * m.etaz + uzeta * m.zetaz;
+            const double dvdx = vxi * m.xix + veta * m.etax + vzeta * m.zetax;
+            const double dvdy = vxi * m.xiy + veta * m.etay + vzeta * m.zetay;
+            const double dvdz = vxi * m.xiz + veta * m.etaz + vzeta * m.zetaz;
+            const double dwdx = wxi * m.xix + weta * m.etax + wzeta * m.zetax;
+            const double dwdy = wxi * m.xiy + weta * m.etay + wzeta * m.zetay;
+            const double dwdz = wxi * m.xiz + weta * m.etaz + wzeta * m.zetaz;
+            const double sxx = dudx, sxy = (dudy + dvdx) / 2, sxz = (dudz + dwdx) / 2;
+            const double syy = dvdy, syz = (dvdz + dwdy) / 2, szz = dwdz;
+            const double sn = sxx * sxx + syy * syy + szz * szz + 2 * (sxy * sxy + sxz * sxz + syz * syz);
+            const double dd = dist(i, j, k) + P.epst;
+            double arg2 = std::max(2 * std::sqrt(tke) / 0.09 / ome / dd, 500 * mu / rho / ome / (dd * dd) * P.machfs / P.reyno);
+            arg2 = arg2 * arg2;
+            arg2 = std::min(arg2, 1.0e2);
+            const double f2 = tanh_ref(arg2);
+            const double fact = std::sqrt(2 * sn);
+            mut(i, j, k, n) = c.a1 * rho * tke / std::max(c.a1 * ome, fact * f2) * P.reyno / P.machfs;
+          }
+      for (int k = 0; k <= km; k += km)
+        for (int j = 1; j <= jm - 1; ++j)
+          for (int i = 1; i <= im - 1; ++i) mut(i, j, k, n) = mut(i, j, k == 0 ? 1 : km - 1, n);
+      for (int k = 1; k <= km - 1; ++k)
+        for (int j = 0; j <= jm; j += jm)
+          for (int i = 1; i <= im - 1; ++i) mut(i, j, k, n) = mut(i, j == 0 ? 1 : jm - 1, k, n);
+      for (int k = 1; k <= km - 1; ++k)
+        for (int j = 1; j <= jm - 1; ++j)
+          for (int i = 0; i <= im; i += im) mut(i, j, k, n) = mut(i == 0 ? 1 : im - 1, j, k, n);
+    }
+  }
+}
+
+// update_b, explicit k-omega part (src/update.f90:601-640): point-implicit
+// rho*omega then rho*k with the destruction terms, omega floored by the
+// production; ttrm = (0, gkw, bkw) for the Wilcox model (update_ttrm_b)
+void update_kom_b(const Level &L, int b, const double *ra, double *qa, const double *qoa, const double *va,
+                  const double *dtta, const double *dpla, const double *prda, double ar, const cosa_params &P,
+                  const double *ttrma = nullptr) {
+  B3 res(const_cast<double *>(ra), L, b), q(qa, L, b), qold(const_cast<double *>(qoa), L, b);
+  B1 vol(const_cast<double *>(va), L, b, 1), dtt(const_cast<double *>(dtta), L, b, L.S);
+  B3s dpl(const_cast<double *>(dpla), L, b), prd(const_cast<double *>(prda), L, b);
+  for (int n = 0; n < L.S; ++n)
+    for (int k = 1; k <= L.km[b] - 1; ++k)
+      for (int j = 1; j <= L.jm[b] - 1; ++j)
+        for (int i = 1; i <= L.im[b] - 1; ++i) {
+          // ttrm(2:3) per cell under BSL/SST, (gkw, bkw) for Wilcox
+          const double gav = ttrma ? B3t(const_cast<double *>(ttrma), L, b)(i, j, k, 2, n) : P.gkw;
+          const double bav = ttrma ? B3t(const_cast<double *>(ttrma), L, b)(i, j, k, 3, n) : P.bkw;
           const double rho = q(i, j, k, 1, n);
           const double ome = q(i, j, k, 7, n) / q(i, j, k, 1, n);
           const double tke = q(i, j, k, 6, n) / q(i, j, k, 1, n);
@@ -3318,6 +3577,8 @@ struct VExtra {
   const double *vm;
   double *prd, *divvel, *delpls;
   double *tbx, *tby, *tbz;
+  double *ttrm;         // BSL/SST: (cdif, gamma, beta) per cell, P3 x 3 x S
+  const double *fdist;  // BSL/SST: face wall distances, families 1..3 at 0, n0, 2 n0
 };
 int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_ptrs &A, const VExtra &X,
                   int want_dt, bool mut_first = false);
@@ -3355,17 +3616,31 @@ int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_p
                   int want_dt, bool mut_first) {
   Level &L = h->L;
   const bool visc = p->viscous != 0, kom = is_kom(*p);
-  if (p->kom_bsl || p->kom_sst) return COSA_ERR_UNSUPPORTED;
+  const bool blend = is_blend(*p);
   if (visc && (!A.vol || !X.vm)) return COSA_ERR_ARG;
   if (kom && (!visc || !A.mut || !A.dist || !A.dtvolt || !X.prd || !X.divvel || !X.delpls)) return COSA_ERR_ARG;
+  if (blend && (!X.ttrm || !X.fdist)) return COSA_ERR_ARG;
   double *q = A.q;
   for (int b = 0; b < L.nb; ++b) cons2prim_b(L, b, q, 0, *p);
   int status = bc_level(L, q, A.si, A.sj, A.sk, *p, A.dist);
   cutman_q_level(L, q);
   if (mut_first) {
     // coarse-level mut from the restricted (primitive) state at the first
-    // stage of the first cycle's visit (src/cosa.f90:1727-1760)
-    tur_vis_level(L, q, A.mut, *p);
+    // stage of the first cycle's visit (src/cosa.f90:1727-1760); SST takes
+    // the cell-centred differences of a copy, back in conservative form
+    if (p->kom_sst) {
+      std::vector<double> w(q, q + L.n3 * L.npde * L.S);
+      double *dc[3] = {A.qp, A.qm, A.dqm};
+      for (int d = 1; d <= 3; ++d)
+        for (int b = 0; b < L.nb; ++b) {
+          q_face_b(L, b, d, w.data(), A.dq);
+          q_der_c_b(L, b, d, A.dq, dc[d - 1], true);
+        }
+      for (int b = 0; b < L.nb; ++b) prim2cons_b(L, b, w.data(), *p);
+      tur_vis_sst_level(L, w.data(), A.mut, A.qp, A.qm, A.dqm, X.vm, A.dist, *p);
+    } else {
+      tur_vis_level(L, q, A.mut, *p);
+    }
     cutman_mut_level(L, A.mut);
   }
   status |= prtest_level(L, q, *p);
@@ -3399,7 +3674,8 @@ int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_p
         q_der_b(L, b, d, q, A.qp, A.qm, A.dqm);
         if (kom) {
           rtst_b(L, b, d, A.dq, A.qp, A.qm, A.dqm, a, a + 3 * L.n0, a + 6 * L.n0, A.dqp, A.flux, *p);
-          vflux_kom_b(L, b, d, A.dq, A.qp, A.qm, A.dqm, A.dqp, a, a + 3 * L.n0, a + 6 * L.n0, sd[d], A.flux, *p);
+          vflux_kom_b(L, b, d, A.dq, A.qp, A.qm, A.dqm, A.dqp, a, a + 3 * L.n0, a + 6 * L.n0, sd[d], A.flux, *p,
+                      blend ? X.fdist + (int64_t)(d - 1) * L.n0 : nullptr);
         }
         vflux_b(L, b, d, A.dq, A.qp, A.qm, A.dqm, a, a + 3 * L.n0, a + 6 * L.n0, sd[d], A.flux, *p, kom);
         resid_b(L, b, d, A.flux, A.res);
@@ -3413,12 +3689,19 @@ int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_p
     for (int d = 1; d <= 3; ++d)
       for (int b = 0; b < L.nb; ++b) {
         q_face_b(L, b, d, q, A.dq);
-        q_der_c_b(L, b, d, A.dq, dc[d - 1]);
+        q_der_c_b(L, b, d, A.dq, dc[d - 1], blend);
       }
     if (nl == 1 || p->prd_all_lvls)
       for (int b = 0; b < L.nb; ++b)
         turprod_b(L, b, q, A.qp, A.qm, A.dqm, X.vm, X.prd, X.divvel, X.delpls, *p);
-    for (int b = 0; b < L.nb; ++b) srckw_b(L, b, nl, q, A.mut, X.prd, X.divvel, A.res, A.vol, *p);
+    if (blend) {
+      for (int b = 0; b < L.nb; ++b) {
+        update_ttrm_b(L, b, q, A.qp, A.qm, A.dqm, X.vm, X.ttrm, A.dist, *p);
+        srckw_sst_b(L, b, nl, q, A.mut, X.prd, X.divvel, A.res, X.ttrm, A.vol, *p);
+      }
+    } else {
+      for (int b = 0; b < L.nb; ++b) srckw_b(L, b, nl, q, A.mut, X.prd, X.divvel, A.res, A.vol, *p);
+    }
   }
 #pragma omp parallel for schedule(dynamic)
   for (int b = 0; b < L.nb; ++b) prim2cons_b(L, b, q, *p);
@@ -3762,10 +4045,10 @@ int orc_smooth_ns(orc_level *h, const cosa_params *p, int ncycles, int mgit0, in
  */
 int orc_smooth_rans(orc_level *h, const cosa_params *p, int ncycles, int mgit0, int rms_every,
                     const cosa_level_ptrs *Ap, const double *vm, double *prd, double *divvel, double *delpls,
-                    double *tbx, double *tby, double *tbz, double *hist) {
+                    double *tbx, double *tby, double *tbz, double *ttrm, const double *fdist, double *hist) {
   Level &L = h->L;
   const cosa_level_ptrs &A = *Ap;
-  VExtra X{vm, prd, divvel, delpls, tbx, tby, tbz};
+  VExtra X{vm, prd, divvel, delpls, tbx, tby, tbz, ttrm, fdist};
   const bool kom = is_kom(*p);
   int status = 0;
   const int last = mgit0 + ncycles - 1;
@@ -3785,13 +4068,16 @@ int orc_smooth_rans(orc_level *h, const cosa_params *p, int ncycles, int mgit0, 
                   *p);
 #pragma omp parallel for schedule(dynamic)
       for (int b = 0; b < L.nb; ++b) {
-        if (kom) update_kom_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p);
+        if (kom)
+          update_kom_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p,
+                       is_blend(*p) ? X.ttrm : nullptr);
         update_b(L, b, A.res, A.q, A.qold, A.dtvol, p->alphas[irk - 1]);
       }
       if (kom) {
         if (p->ifixq) fixq_level(L, A.q, *p);
         if (irk == p->nstage) {
-          tur_vis_level(L, A.q, A.mut, *p);
+          if (p->kom_sst) tur_vis_sst_level(L, A.q, A.mut, A.qp, A.qm, A.dqm, X.vm, A.dist, *p);
+          else tur_vis_level(L, A.q, A.mut, *p);
           cutman_mut_level(L, A.mut);
         }
       }
@@ -3801,8 +4087,8 @@ int orc_smooth_rans(orc_level *h, const cosa_params *p, int ncycles, int mgit0, 
 }
 int orc_residual_rans(orc_level *h, const cosa_params *p, int nl, const cosa_level_ptrs *A, const double *vm,
                       double *prd, double *divvel, double *delpls, double *tbx, double *tby, double *tbz,
-                      int want_dt) {
-  VExtra X{vm, prd, divvel, delpls, tbx, tby, tbz};
+                      double *ttrm, const double *fdist, int want_dt) {
+  VExtra X{vm, prd, divvel, delpls, tbx, tby, tbz, ttrm, fdist};
   return residual_full(h, p, nl, *A, X, want_dt);
 }
 void orc_cutman_mut(orc_level *h, double *mut) { cutman_mut_level(h->L, mut); }
@@ -3821,15 +4107,32 @@ void orc_rtst(orc_level *h, const cosa_params *p, int idir, const double *qf, co
 }
 void orc_vflux_kom(orc_level *h, const cosa_params *p, int idir, const double *qf, const double *dqxi,
                    const double *dqeta, const double *dqzeta, const double *tau1, const double *vm,
-                   const double *sijk, double *flux) {
+                   const double *sijk, double *flux, const double *fdist) {
   const double *a = vm + (int64_t)(idir - 1) * 9 * h->L.n0;
   for (int b = 0; b < h->L.nb; ++b) {
-    vflux_kom_b(h->L, b, idir, qf, dqxi, dqeta, dqzeta, tau1, a, a + 3 * h->L.n0, a + 6 * h->L.n0, sijk, flux, *p);
+    vflux_kom_b(h->L, b, idir, qf, dqxi, dqeta, dqzeta, tau1, a, a + 3 * h->L.n0, a + 6 * h->L.n0, sijk, flux, *p,
+                fdist);
     vflux_b(h->L, b, idir, qf, dqxi, dqeta, dqzeta, a, a + 3 * h->L.n0, a + 6 * h->L.n0, sijk, flux, *p, true);
   }
 }
-void orc_q_der_c(orc_level *h, int idir, const double *qf, double *dqc) {
-  for (int b = 0; b < h->L.nb; ++b) q_der_c_b(h->L, b, idir, qf, dqc);
+void orc_q_der_c(orc_level *h, const cosa_params *p, int idir, const double *qf, double *dqc) {
+  for (int b = 0; b < h->L.nb; ++b) q_der_c_b(h->L, b, idir, qf, dqc, is_blend(*p));
+}
+void orc_facedist(orc_level *h, const double *dist, double *fdist) {
+  const int64_t n0 = h->L.n0;
+  facedist_level(h->L, dist, fdist, fdist + n0, fdist + 2 * n0);
+}
+void orc_update_ttrm(orc_level *h, const cosa_params *p, const double *q, const double *dqxi, const double *dqeta,
+                     const double *dqzeta, const double *vm, double *ttrm, const double *dist) {
+  for (int b = 0; b < h->L.nb; ++b) update_ttrm_b(h->L, b, q, dqxi, dqeta, dqzeta, vm, ttrm, dist, *p);
+}
+void orc_srckw_sst(orc_level *h, const cosa_params *p, int nl, const double *q, const double *mut, const double *prd,
+                   const double *divvel, double *res, const double *ttrm, const double *vol) {
+  for (int b = 0; b < h->L.nb; ++b) srckw_sst_b(h->L, b, nl, q, mut, prd, divvel, res, ttrm, vol, *p);
+}
+void orc_tur_vis_sst(orc_level *h, const cosa_params *p, const double *q, double *mut, const double *dqxi,
+                     const double *dqeta, const double *dqzeta, const double *vm, const double *dist) {
+  tur_vis_sst_level(h->L, q, mut, dqxi, dqeta, dqzeta, vm, dist, *p);
 }
 void orc_turprod(orc_level *h, const cosa_params *p, const double *q, const double *dqxi, const double *dqeta,
                  const double *dqzeta, const double *vm, double *prd, double *divvel, double *delpls) {
@@ -3840,16 +4143,20 @@ void orc_srckw(orc_level *h, const cosa_params *p, int nl, const double *q, cons
   for (int b = 0; b < h->L.nb; ++b) srckw_b(h->L, b, nl, q, mut, prd, divvel, res, vol, *p);
 }
 void orc_update_kom(orc_level *h, const cosa_params *p, const double *res, double *q, const double *qold,
-                    const double *vol, const double *dtvolt, const double *delpls, const double *prd, double ar) {
-  for (int b = 0; b < h->L.nb; ++b) update_kom_b(h->L, b, res, q, qold, vol, dtvolt, delpls, prd, ar, *p);
+                    const double *vol, const double *dtvolt, const double *delpls, const double *prd, double ar,
+                    const double *ttrm) {
+  for (int b = 0; b < h->L.nb; ++b) update_kom_b(h->L, b, res, q, qold, vol, dtvolt, delpls, prd, ar, *p, ttrm);
 }
 // ---- k-omega multigrid ------------------------------------------------------
 // per-level arrays of the k-omega residual beyond cosa_level_ptrs
 struct orc_vextra {
   const double *vm;
-  double *prd, *divvel, *delpls, *tbx, *tby, *tbz;
+  double *prd, *divvel, *delpls, *tbx, *tby, *tbz, *ttrm;
+  const double *fdist;
 };
-static VExtra vx(const orc_vextra &e) { return VExtra{e.vm, e.prd, e.divvel, e.delpls, e.tbx, e.tby, e.tbz}; }
+static VExtra vx(const orc_vextra &e) {
+  return VExtra{e.vm, e.prd, e.divvel, e.delpls, e.tbx, e.tby, e.tbz, e.ttrm, e.fdist};
+}
 
 void orc_rest4(orc_level *f, orc_level *c, const double *f1, double *f2, const double *vol1, const double *vol2) {
   for (int b = 0; b < f->L.nb; ++b) rest4_b(f->L, c->L, b, f1, f2, vol1, vol2);
@@ -3890,19 +4197,22 @@ int orc_smooth_level_rans(orc_level *h, const cosa_params *p, int nl, int nlevel
         if (nlevel > 1 && nl != nlevel && !p->prd_all_lvls && p->lim_prodtke)
           for (int b = 0; b < L.nb; ++b) lim_prod_mg_b(L, b, A.q, X.prd, A.mut, *p);
         for (int b = 0; b < L.nb; ++b)
-          lim_res_ome_b(L, b, A.res, A.q, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p);
+          lim_res_ome_b(L, b, A.res, A.q, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p,
+                        is_blend(*p) ? X.ttrm : nullptr);
         return status;
       }
       if (p->irsop > 0)
         irs_level(L, A.res, A.dtvol, A.dtvolt, A.betaxi, A.betaeta, A.betazeta, X.tbx, X.tby, X.tbz, *p);
 #pragma omp parallel for schedule(dynamic)
       for (int b = 0; b < L.nb; ++b) {
-        update_kom_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p);
+        update_kom_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p,
+                     is_blend(*p) ? X.ttrm : nullptr);
         update_b(L, b, A.res, A.q, A.qold, A.dtvol, p->alphas[irk - 1]);
       }
       if (p->ifixq) fixq_level(L, A.q, *p);
       if (irk == p->nstage && (nl == 1 || !p->prd_all_lvls)) {
-        tur_vis_level(L, A.q, A.mut, *p);
+        if (p->kom_sst) tur_vis_sst_level(L, A.q, A.mut, A.qp, A.qm, A.dqm, X.vm, A.dist, *p);
+        else tur_vis_level(L, A.q, A.mut, *p);
         cutman_mut_level(L, A.mut);
       }
     }

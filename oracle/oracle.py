@@ -475,6 +475,10 @@ class RansArrays(LevelArrays):
         self.prd, self.divvel, self.delpls = (np.zeros(n3s) for _ in range(3))
         self.tbx, self.tby, self.tbz = (O.p1(O.S) for _ in range(3))
         self.vm = None
+        # BSL/SST: blended coefficients per cell and the face wall distances
+        self.ttrm = np.zeros(O.n3 * 3 * O.S)
+        self.fdist = np.zeros(3 * O.n0)
+        self._O = O
 
     def ptrs(self):
         p = super().ptrs()
@@ -483,7 +487,10 @@ class RansArrays(LevelArrays):
         return p
 
     def extras(self):
-        return (_p(self.vm), _p(self.prd), _p(self.divvel), _p(self.delpls), _p(self.tbx), _p(self.tby), _p(self.tbz))
+        if self._O.p.kom_bsl or self._O.p.kom_sst:
+            facedist(self._O, self.dist, self.fdist)
+        return (_p(self.vm), _p(self.prd), _p(self.divvel), _p(self.delpls), _p(self.tbx), _p(self.tby), _p(self.tbz),
+                _p(self.ttrm), _p(self.fdist))
 
 
 def smooth_rans(O, A, ncycles, mgit0=1, rms_every=1):
@@ -516,13 +523,31 @@ def rtst(O, idir, qf, dqxi, dqeta, dqzeta, vm, tau1, flux):
                    _p(flux))
 
 
-def vflux_kom(O, idir, qf, dqxi, dqeta, dqzeta, tau1, vm, sijk, flux):
+def vflux_kom(O, idir, qf, dqxi, dqeta, dqzeta, tau1, vm, sijk, flux, fdist=None):
+    """fdist: the face wall distances of family idir (BSL/SST)."""
     lib().orc_vflux_kom(O.h, _par(O.p), C.c_int(idir), _p(qf), _p(dqxi), _p(dqeta), _p(dqzeta), _p(tau1), _p(vm),
-                        _p(sijk), _p(flux))
+                        _p(sijk), _p(flux), _opt(fdist))
 
 
 def q_der_c(O, idir, qf, dqc):
-    lib().orc_q_der_c(O.h, C.c_int(idir), _p(qf), _p(dqc))
+    lib().orc_q_der_c(O.h, _par(O.p), C.c_int(idir), _p(qf), _p(dqc))
+
+
+def facedist(O, dist, fdist):
+    """facedist_b: the three face-distance arrays (F0 each) into fdist (3 n0)."""
+    lib().orc_facedist(O.h, _p(dist), _p(fdist))
+
+
+def update_ttrm(O, q, dqxi, dqeta, dqzeta, vm, ttrm, dist):
+    lib().orc_update_ttrm(O.h, _par(O.p), _p(q), _p(dqxi), _p(dqeta), _p(dqzeta), _p(vm), _p(ttrm), _p(dist))
+
+
+def srckw_sst(O, nl, q, mut, prd, divvel, res, ttrm, vol):
+    lib().orc_srckw_sst(O.h, _par(O.p), C.c_int(nl), _p(q), _p(mut), _p(prd), _p(divvel), _p(res), _p(ttrm), _p(vol))
+
+
+def tur_vis_sst(O, q, mut, dqxi, dqeta, dqzeta, vm, dist):
+    lib().orc_tur_vis_sst(O.h, _par(O.p), _p(q), _p(mut), _p(dqxi), _p(dqeta), _p(dqzeta), _p(vm), _p(dist))
 
 
 def turprod(O, q, dqxi, dqeta, dqzeta, vm, prd, divvel, delpls):
@@ -534,9 +559,9 @@ def srckw(O, nl, q, mut, prd, divvel, res, vol):
     lib().orc_srckw(O.h, _par(O.p), C.c_int(nl), _p(q), _p(mut), _p(prd), _p(divvel), _p(res), _p(vol))
 
 
-def update_kom(O, res, q, qold, vol, dtvolt, delpls, prd, ar):
+def update_kom(O, res, q, qold, vol, dtvolt, delpls, prd, ar, ttrm=None):
     lib().orc_update_kom(O.h, _par(O.p), _p(res), _p(q), _p(qold), _p(vol), _p(dtvolt), _p(delpls), _p(prd),
-                         C.c_double(ar))
+                         C.c_double(ar), _opt(ttrm))
 
 
 def deltat_ns_full(O, dtvol, lam, lamv, bx, by, bz, dtvolt, tbx, tby, tbz):
@@ -561,7 +586,7 @@ def force(O, q, x, y, z, si, sj, sk, vm, isurf=1, xmom=(0.25, 0.0, 0.0), lngth=(
 
 # ---- k-omega multigrid ---------------------------------------------------------------
 class _VExtra(C.Structure):
-    _fields_ = [(n, _dp) for n in ("vm", "prd", "divvel", "delpls", "tbx", "tby", "tbz")]
+    _fields_ = [(n, _dp) for n in ("vm", "prd", "divvel", "delpls", "tbx", "tby", "tbz", "ttrm", "fdist")]
 
 
 def _vextra(A):
