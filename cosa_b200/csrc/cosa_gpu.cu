@@ -23,6 +23,9 @@
 #include "force.cuh"
 
 namespace {
+// any k-omega variant: Wilcox (kom), BSL (kom_bsl), SST (kom_sst)
+inline bool rans(const cosa_params &p) { return p.kom || p.kom_bsl || p.kom_sst; }
+inline bool blend(const cosa_params &p) { return p.kom_bsl || p.kom_sst; }
 
 constexpr int kTI = 32, kTJ = 7;  // tile of the fused stage kernel (7 rows + the boundary-face warp = 256 threads)
 
@@ -68,6 +71,8 @@ struct LevelState {
   // k-omega: production, div u, delta+ (scalar P3) and the turbulence IRS
   // coefficients (P1 x S)
   double *d_prd = nullptr, *d_divvel = nullptr, *d_delpls = nullptr;
+  double *d_ttrm = nullptr;   // BSL/SST: (cdif, gamma, beta) per cell (P3 x 3 x S)
+  double *d_fdist = nullptr;  // BSL/SST: face wall distances, families 1..3 at 0, n0, 2 n0
   double *d_tbeta[3] = {nullptr, nullptr, nullptr};
   // stage schedule: 0 = fused tile kernel, 1 = face-split (k_faces + k_cells),
   // set by cosa_gpu_autotune
@@ -206,7 +211,7 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
       const int type = r[0], idir = r[1], inrout = r[2];
       if (idir < 1 || idir > 3) return COSA_ERR_ARG;
       // viscous walls: the laminar, fixed-grid branch of bc_walvis_15
-      const bool wall15 = type / 100 == 15 && (!c->p.moving || !c->p.kom);
+      const bool wall15 = type / 100 == 15 && (!c->p.moving || !rans(c->p));
       const bool ok = type == 80 || type == 4 || type == 14 || type == 21 || type == 91 || type == 30 || type == 31 ||
                       wall15;
       if (!ok) return COSA_ERR_UNSUPPORTED;
@@ -522,16 +527,18 @@ int set_smem_attrs() {
   return COSA_OK;
 }
 
-// the k-omega stage runs routine by routine (launch_rans_iteration)
+// the k-omega stage runs routine by routine (launch_rans_iteration); Wilcox,
+// BSL and SST
 int check_rans_supported(const cosa_params &p) {
-  if (p.npde != 7 || !p.kom || p.kom_bsl || p.kom_sst || !p.viscous || p.rkimp || p.moving || p.harbal ||
+  if (p.npde != 7 || !rans(p) || (p.kom + p.kom_bsl + p.kom_sst) != 1 || !p.viscous || p.rkimp || p.moving ||
+      p.harbal ||
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
   return COSA_OK;
 }
 
 int check_fused_supported(const cosa_params &p) {
-  if (p.kom) return check_rans_supported(p);
+  if (rans(p)) return check_rans_supported(p);
   // rkimp: the implicit time-spectral update of harmonic balance (update_bhb,
   // src/update.f90:1564-1604 without IRS on one level, 1771-1836 with IRS or
   // multigrid)
@@ -950,7 +957,7 @@ int launch_rans_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o)
 // one RK iteration (nstage stages) of the fused path
 int launch_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
   const cosa_params &p = c->p;
-  if (p.kom) return launch_rans_iteration(c, nl, L, o);
+  if (rans(p)) return launch_rans_iteration(c, nl, L, o);
   double *Q = L.ptrs.q, *T = L.d_T, *QO = L.ptrs.qold;
   const int S = 2 * p.nharms + 1;
   if (o.res_only) {
@@ -1101,6 +1108,21 @@ int ensure_rans(cosa_ctx *c, LevelState &L) {
     }
   for (auto &t : L.d_tbeta)
     if (!t && (r = dalloc(c, &t, (size_t)L.n1 * S))) return r;
+  if (blend(c->p)) {
+    if (!L.d_ttrm) {
+      if ((r = dalloc(c, &L.d_ttrm, (size_t)L.n3 * 3 * S))) return r;
+      CK(cudaMemset(L.d_ttrm, 0, (size_t)L.n3 * 3 * S * sizeof(double)));
+    }
+    if (!L.d_fdist && (r = dalloc(c, &L.d_fdist, (size_t)3 * L.n0))) return r;
+    // the face distances of the bound wall distance (facedist, src/cosa.f90:209-211)
+    for (const DevBlock &x : L.hb) {
+      const int64_t nf = (int64_t)x.im * x.jm * x.km;
+      k_facedist<1><<<grid_for(nf), 256, 0, c->s>>>(x, P.dist, L.d_fdist);
+      k_facedist<2><<<grid_for(nf), 256, 0, c->s>>>(x, P.dist, L.d_fdist + L.n0);
+      k_facedist<3><<<grid_for(nf), 256, 0, c->s>>>(x, P.dist, L.d_fdist + 2 * L.n0);
+      if ((r = after_launch(c))) return r;
+    }
+  }
   if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, L))) return r;
   if (L.npart_cap < L.nb * 64) {  // per-block norm partials of the routine-by-routine stage
     drop_graphs(c);
@@ -1313,7 +1335,7 @@ int cosa_gpu_lambda(cosa_ctx *c, int32_t nl, const double *q, const double *si, 
 int cosa_gpu_deltat(cosa_ctx *c, int32_t nl, double *dtvol, const double *lam, double *bx, double *by, double *bz) {
   LevelState *L = level(c, nl);
   if (!L || !dtvol || !lam) return COSA_ERR_ARG;
-  if (c->p.viscous || c->p.kom || c->p.irsop == 5 || c->p.irsop == 6) return COSA_ERR_UNSUPPORTED;
+  if (c->p.viscous || rans(c->p) || c->p.irsop == 5 || c->p.irsop == 6) return COSA_ERR_UNSUPPORTED;
   return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) {
     k_deltat<<<g, 256, 0, c->s>>>(b, c->d_p, dtvol, lam, bx, by, bz);
   });
@@ -1445,7 +1467,7 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
   if (!P.q || !P.qold || !P.dtvol || !P.si || !P.sj || !P.sk) return COSA_ERR_ARG;
   if (c->p.harbal && !P.vol) return COSA_ERR_ARG;
   if (c->p.viscous && (!P.vol || !L->d_vm)) return COSA_ERR_ARG;
-  if (c->p.kom && (r = ensure_rans(c, *L))) return r;
+  if (rans(c->p) && (r = ensure_rans(c, *L))) return r;
   cudaSetDevice(c->device);
   const int npde = c->p.npde;
   // schedule of printed iterations (src/cosa.f90:1925-1927)
@@ -1491,7 +1513,7 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
   }
   // reference state after smooth(): face halos of q in conservative form
   // (the k-omega stage converts them itself, src/update.f90:1875-2084)
-  if (niter > 0 && !L->items.empty() && !c->p.kom) {
+  if (niter > 0 && !L->items.empty() && !rans(c->p)) {
     double *last_in = (c->p.nstage % 2 == 0) ? L->d_T : L->ptrs.q;
     const int S = 2 * c->p.nharms + 1;
     k_halo_p2c<<<grid_for((int64_t)L->items.size() * S), 256, 0, c->s>>>(L->d_blocks, L->d_items,
@@ -1784,7 +1806,7 @@ int issue_rest2_ho(cosa_ctx *c, LevelState &L1, LevelState &L2, int nl, double *
     k_zero_shell1<<<grid_for((int64_t)(x.im + 1) * (x.jm + 1) * (x.km + 1) * nvs), 256, 0, c->s>>>(x, nvs, res1);
     if ((r = after_launch(c))) return r;
   }
-  if (c->p.kom) {
+  if (rans(c->p)) {
     if ((r = cosa_gpu_cutman_q(c, nl, res1)) || (r = launch_bc_res(c, L1, res1)) ||
         (r = launch_edges(c, L1, res1, nullptr)) || (r = launch_corns(c, L1, res1, nullptr)))
       return r;
@@ -1799,9 +1821,8 @@ int issue_restrict(cosa_ctx *c, int nl) {
   if (r) return r;
   const cosa_level_ptrs &A = L1->ptrs, &B = L2->ptrs;
   if (!A.q || !A.vol || !A.res || !B.q || !B.vol || !B.rhs) return COSA_ERR_ARG;
-  if (c->p.kom_bsl || c->p.kom_sst) return COSA_ERR_UNSUPPORTED;
   if ((r = launch_rest1(c, *L1, *L2, A.q, B.q, A.vol, B.vol))) return r;
-  if (c->p.kom) {
+  if (rans(c->p)) {
     // production terms (or mut with prd_all_lvls) restricted as well
     // (src/cosa.f90:2733-2741)
     const int S = 2 * c->p.nharms + 1;
@@ -1871,7 +1892,7 @@ int issue_smooth_level(cosa_ctx *c, int nl, int niter, bool from_fine, bool to_c
   }
   // reference state after smooth(): face halos of q in conservative form
   // (the k-omega stage converts them itself)
-  if (niterp > 0 && !L.items.empty() && !p.kom) {
+  if (niterp > 0 && !L.items.empty() && !rans(p)) {
     double *last_in = (to_coarse || p.nstage % 2 == 1) ? L.ptrs.q : L.d_T;
     const int S = 2 * p.nharms + 1;
     k_halo_p2c<<<grid_for((int64_t)L.items.size() * S), 256, 0, c->s>>>(L.d_blocks, L.d_items, (int)L.items.size(),
@@ -2031,7 +2052,7 @@ int cosa_gpu_smooth_level(cosa_ctx *c, int32_t nl, int32_t niter, int32_t from_f
     L->npart_cap = L->nb * 64;
   }
   CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
-  if (c->p.kom && (r = ensure_rans(c, *L))) return r;
+  if (rans(c->p) && (r = ensure_rans(c, *L))) return r;
   const bool first = mgit == 1;
   const int flags = (from_fine ? 1 : 0) | (to_coarse ? 2 : 0) | (want ? 4 : 0) | (first ? 8 : 0);
   r = run_graph(c, graph_key(1, nl, niter, flags),
@@ -2067,7 +2088,7 @@ int cosa_gpu_mg(cosa_ctx *c, int32_t mgit0, int32_t ncycles, int32_t ncycle, int
       if ((r = dalloc(c, &Lv.d_part, (size_t)Lv.nb * 64 * 8))) return r;
       Lv.npart_cap = Lv.nb * 64;
     }
-    if (c->p.kom && (r = ensure_rans(c, Lv))) return r;
+    if (rans(c->p) && (r = ensure_rans(c, Lv))) return r;
   }
   CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
   size_t ri = 0;
@@ -2418,7 +2439,7 @@ int cosa_gpu_lambda_ns(cosa_ctx *c, int32_t nl, const double *q, const double *s
   if (!L || !q || !si || !sj || !sk || !vol || !lam || !lamv) return COSA_ERR_ARG;
   if (c->p.moving) return COSA_ERR_UNSUPPORTED;
   return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) {
-    k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, vol, c->p.kom ? mut : nullptr, lam, lamv);
+    k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, vol, rans(c->p) ? mut : nullptr, lam, lamv);
   });
 }
 
@@ -2427,8 +2448,8 @@ int cosa_gpu_deltat_ns(cosa_ctx *c, int32_t nl, double *dtvol, const double *lam
   LevelState *L = level(c, nl);
   if (!L || !dtvol || !lam || !lamv) return COSA_ERR_ARG;
   return for_blocks(c, *L, cnt_interior, [&](auto b, dim3 g) {
-    k_deltat_ns<<<g, 256, 0, c->s>>>(b, c->d_p, dtvol, lam, lamv, bx, by, bz, c->p.kom ? dtvolt : nullptr,
-                                     c->p.kom ? tbx : nullptr, tby, tbz);
+    k_deltat_ns<<<g, 256, 0, c->s>>>(b, c->d_p, dtvol, lam, lamv, bx, by, bz, rans(c->p) ? dtvolt : nullptr,
+                                     rans(c->p) ? tbx : nullptr, tby, tbz);
   });
 }
 
@@ -2465,24 +2486,79 @@ int cosa_gpu_rtst(cosa_ctx *c, int32_t idir, int32_t nl, const double *qf, const
 
 int cosa_gpu_vflux_kom(cosa_ctx *c, int32_t idir, int32_t nl, const double *qf, const double *dqxi,
                        const double *dqeta, const double *dqzeta, const double *tau1, const double *vm,
-                       const double *sijk, double *flux) {
+                       const double *sijk, double *flux, const double *fdist) {
   LevelState *L = level(c, nl);
   if (!L || idir < 1 || idir > 3 || !qf || !dqxi || !dqeta || !dqzeta || !tau1 || !vm || !sijk || !flux)
     return COSA_ERR_ARG;
-  if (c->p.npde != 7 || !c->p.kom || c->p.moving) return COSA_ERR_UNSUPPORTED;
+  if (c->p.npde != 7 || !rans(c->p) || c->p.moving) return COSA_ERR_UNSUPPORTED;
+  if (blend(c->p) != (fdist != nullptr)) return COSA_ERR_ARG;
   return for_blocks(c, *L, cnt_faces, [&](auto b, dim3 g) {
-    k_vflux_kom<<<g, 256, 0, c->s>>>(b, idir, c->d_p, qf, dqxi, dqeta, dqzeta, tau1, vm, L->n0, sijk, flux);
+    k_vflux_kom<<<g, 256, 0, c->s>>>(b, idir, c->d_p, qf, dqxi, dqeta, dqzeta, tau1, vm, L->n0, sijk, flux, fdist);
   });
+}
+
+int cosa_gpu_facedist(cosa_ctx *c, int32_t nl, const double *dist, double *fidist, double *fjdist, double *fkdist) {
+  LevelState *L = level(c, nl);
+  if (!L || !dist || !fidist || !fjdist || !fkdist) return COSA_ERR_ARG;
+  for (const DevBlock &x : L->hb) {
+    const int64_t nf = (int64_t)x.im * x.jm * x.km;
+    k_facedist<1><<<grid_for(nf), 256, 0, c->s>>>(x, dist, fidist);
+    k_facedist<2><<<grid_for(nf), 256, 0, c->s>>>(x, dist, fjdist);
+    k_facedist<3><<<grid_for(nf), 256, 0, c->s>>>(x, dist, fkdist);
+    int r = after_launch(c);
+    if (r) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_update_ttrm(cosa_ctx *c, int32_t nl, const double *q, const double *dqxi, const double *dqeta,
+                         const double *dqzeta, const double *vm, double *ttrm, const double *dist) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !dqxi || !dqeta || !dqzeta || !vm || !ttrm || !dist) return COSA_ERR_ARG;
+  if (c->p.npde != 7 || !rans(c->p)) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
+    k_update_ttrm<<<g, 256, 0, c->s>>>(b, c->d_p, q, dqxi, dqeta, dqzeta, vm, L->n0, ttrm, dist);
+  });
+}
+
+int cosa_gpu_srckw_sst(cosa_ctx *c, int32_t nl, const double *q, const double *prd, const double *divvel,
+                       double *res, const double *mut, const double *ttrm, const double *vol) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !prd || !divvel || !res || !mut || !ttrm || !vol) return COSA_ERR_ARG;
+  if (c->p.npde != 7 || !blend(c->p)) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
+    k_srckw<<<g, 256, 0, c->s>>>(b, c->d_p, nl, q, mut, prd, divvel, res, vol, ttrm);
+  });
+}
+
+int cosa_gpu_tur_vis_sst(cosa_ctx *c, int32_t nl, const double *q, double *mut, const double *dqxi,
+                         const double *dqeta, const double *dqzeta, const double *vm, const double *dist) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !mut || !dqxi || !dqeta || !dqzeta || !vm || !dist) return COSA_ERR_ARG;
+  if (c->p.npde != 7 || !c->p.kom_sst) return COSA_ERR_UNSUPPORTED;
+  const int S = 2 * c->p.nharms + 1;
+  int r = for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
+    k_tur_vis_sst<<<g, 256, 0, c->s>>>(b, c->d_p, q, mut, dqxi, dqeta, dqzeta, vm, L->n0, dist);
+  });
+  if (r) return r;
+  for (const DevBlock &x : L->hb) {
+    const int64_t nh = 2 * ((int64_t)(x.jm - 1) * (x.km - 1) + (int64_t)(x.im - 1) * (x.km - 1) +
+                            (int64_t)(x.im - 1) * (x.jm - 1)) * S;
+    k_tur_vis_sst_halo<<<grid_for(nh), 256, 0, c->s>>>(x, S, mut);
+    if ((r = after_launch(c))) return r;
+  }
+  return COSA_OK;
 }
 
 int cosa_gpu_q_der_c(cosa_ctx *c, int32_t idir, int32_t nl, const double *qf, double *dqc) {
   LevelState *L = level(c, nl);
   if (!L || idir < 1 || idir > 3 || !qf || !dqc) return COSA_ERR_ARG;
   const int S = 2 * c->p.nharms + 1, npde = c->p.npde;
+  const int vhi = blend(c->p) ? 7 : 4;  // k and omega too under BSL/SST
   return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
-    if (idir == 1) k_qder_c<1><<<g, 256, 0, c->s>>>(b, npde, S, qf, dqc);
-    else if (idir == 2) k_qder_c<2><<<g, 256, 0, c->s>>>(b, npde, S, qf, dqc);
-    else k_qder_c<3><<<g, 256, 0, c->s>>>(b, npde, S, qf, dqc);
+    if (idir == 1) k_qder_c<1><<<g, 256, 0, c->s>>>(b, npde, S, qf, dqc, vhi);
+    else if (idir == 2) k_qder_c<2><<<g, 256, 0, c->s>>>(b, npde, S, qf, dqc, vhi);
+    else k_qder_c<3><<<g, 256, 0, c->s>>>(b, npde, S, qf, dqc, vhi);
   });
 }
 
@@ -2501,17 +2577,19 @@ int cosa_gpu_srckw(cosa_ctx *c, int32_t nl, const double *q, const double *mut, 
   if (!L || !q || !mut || !prd || !divvel || !res || !vol) return COSA_ERR_ARG;
   if (c->p.npde != 7) return COSA_ERR_UNSUPPORTED;
   return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
-    k_srckw<<<g, 256, 0, c->s>>>(b, c->d_p, nl, q, mut, prd, divvel, res, vol);
+    k_srckw<<<g, 256, 0, c->s>>>(b, c->d_p, nl, q, mut, prd, divvel, res, vol, nullptr);
   });
 }
 
 int cosa_gpu_update_kom(cosa_ctx *c, int32_t nl, const double *res, double *q, const double *qold, const double *vol,
-                        const double *dtvolt, const double *delpls, const double *prd, double ar) {
+                        const double *dtvolt, const double *delpls, const double *prd, double ar,
+                        const double *ttrm) {
   LevelState *L = level(c, nl);
   if (!L || !res || !q || !qold || !vol || !dtvolt || !delpls || !prd) return COSA_ERR_ARG;
   if (c->p.npde != 7 || c->p.rkimp) return COSA_ERR_UNSUPPORTED;
+  if (blend(c->p) && !ttrm) return COSA_ERR_ARG;
   return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
-    k_update_kom<<<g, 256, 0, c->s>>>(b, c->d_p, res, q, qold, vol, dtvolt, delpls, prd, ar);
+    k_update_kom<<<g, 256, 0, c->s>>>(b, c->d_p, res, q, qold, vol, dtvolt, delpls, prd, ar, ttrm);
   });
 }
 
@@ -2691,8 +2769,25 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
   }
   if (o.first_cycle && o.force && irk == 1 && !p.prd_all_lvls) {
     // coarse-level mut from the restricted (primitive) state at the first
-    // stage of the first cycle's visit (src/cosa.f90:1727-1760)
-    if ((r = cosa_gpu_tur_vis(c, nl, q, P.mut)) || (r = cosa_gpu_cutman_mut(c, nl, P.mut))) return r;
+    // stage of the first cycle's visit (src/cosa.f90:1727-1760); SST takes
+    // the cell-centred differences of a copy of q in res, back in
+    // conservative form, and zeroes res after
+    if (p.kom_sst) {
+      const size_t bytes = (size_t)L.n3 * npde * S * sizeof(double);
+      CK(cudaMemcpyAsync(P.res, q, bytes, cudaMemcpyDeviceToDevice, c->s));
+      double *dc[3] = {P.qp, P.qm, P.dqm};
+      for (int d = 1; d <= 3; ++d) {
+        if ((r = rans_face_state(c, L, d, P.res, P.dq, nullptr, nullptr, nullptr))) return r;
+        if ((r = cosa_gpu_q_der_c(c, d, nl, P.dq, dc[d - 1]))) return r;
+      }
+      if ((r = cosa_gpu_prim2cons(c, nl, P.res)) ||
+          (r = cosa_gpu_tur_vis_sst(c, nl, P.res, P.mut, P.qp, P.qm, P.dqm, L.d_vm, P.dist)))
+        return r;
+      CK(cudaMemsetAsync(P.res, 0, bytes, c->s));
+    } else if ((r = cosa_gpu_tur_vis(c, nl, q, P.mut))) {
+      return r;
+    }
+    if ((r = cosa_gpu_cutman_mut(c, nl, P.mut))) return r;
   }
   if ((r = for_blocks(c, L, cnt_all, [&](auto b, dim3 g) { k_prtest<<<g, 256, 0, c->s>>>(b, c->d_p, q, c->d_status); })))
     return r;
@@ -2722,7 +2817,9 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
     if ((r = cosa_gpu_q_face_mut(c, d, nl, P.mut, P.flux))) return r;
     if ((r = rans_face_state(c, L, d, q, nullptr, P.qp, P.qm, P.dqm))) return r;
     if ((r = cosa_gpu_rtst(c, d, nl, P.dq, P.qp, P.qm, P.dqm, L.d_vm, P.flux, P.dqp))) return r;
-    if ((r = cosa_gpu_vflux_kom(c, d, nl, P.dq, P.qp, P.qm, P.dqm, P.dqp, L.d_vm, sd[d], P.flux))) return r;
+    if ((r = cosa_gpu_vflux_kom(c, d, nl, P.dq, P.qp, P.qm, P.dqm, P.dqp, L.d_vm, sd[d], P.flux,
+                                blend(p) ? L.d_fdist + (int64_t)(d - 1) * L.n0 : nullptr)))
+      return r;
     if ((r = cosa_gpu_resid(c, d, nl, P.flux, P.res))) return r;
   }
   // cell-centred velocity gradients, production and sources (src/cosa.f90:1878-1896)
@@ -2733,7 +2830,14 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
   }
   if (nl == 1 || p.prd_all_lvls)
     if ((r = cosa_gpu_turprod(c, nl, P.qp, P.qm, P.dqm, L.d_vm, L.d_prd, L.d_divvel, L.d_delpls))) return r;
-  if ((r = cosa_gpu_srckw(c, nl, q, P.mut, L.d_prd, L.d_divvel, P.res, P.vol))) return r;
+  if (blend(p)) {
+    // update_ttrm + srckw_sst (src/cosa.f90:1896-1901)
+    if ((r = cosa_gpu_update_ttrm(c, nl, q, P.qp, P.qm, P.dqm, L.d_vm, L.d_ttrm, P.dist)) ||
+        (r = cosa_gpu_srckw_sst(c, nl, q, L.d_prd, L.d_divvel, P.res, P.mut, L.d_ttrm, P.vol)))
+      return r;
+  } else if ((r = cosa_gpu_srckw(c, nl, q, P.mut, L.d_prd, L.d_divvel, P.res, P.vol))) {
+    return r;
+  }
   if ((r = cosa_gpu_prim2cons(c, nl, q))) return r;
   if (want_rms) {
     for (int b = 0; b < L.nb; ++b) {
@@ -2764,7 +2868,8 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
          })))
       return r;
     return for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
-      k_lim_res_ome<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, q, P.vol, P.dtvolt, L.d_delpls, L.d_prd, p.alphas[irk - 1]);
+      k_lim_res_ome<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, q, P.vol, P.dtvolt, L.d_delpls, L.d_prd, p.alphas[irk - 1],
+                                         blend(p) ? L.d_ttrm : nullptr);
     });
   }
   if (p.irsop > 0) {
@@ -2773,13 +2878,16 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
     const double *tbeta[3] = {L.d_tbeta[0], L.d_tbeta[1], L.d_tbeta[2]};
     if ((r = irs_apply(c, L, P.res, L.d_ores, P.dtvol, beta, P.dtvolt, tbeta))) return r;
   }
-  if ((r = cosa_gpu_update_kom(c, nl, P.res, q, P.qold, P.vol, P.dtvolt, L.d_delpls, L.d_prd, p.alphas[irk - 1])))
+  if ((r = cosa_gpu_update_kom(c, nl, P.res, q, P.qold, P.vol, P.dtvolt, L.d_delpls, L.d_prd, p.alphas[irk - 1],
+                               blend(p) ? L.d_ttrm : nullptr)))
     return r;
   if ((r = cosa_gpu_update(c, nl, P.res, q, P.qold, P.dtvol, p.alphas[irk - 1]))) return r;
   if (p.ifixq && (r = cosa_gpu_fixq(c, nl, q))) return r;
   if (irk == p.nstage && (nl == 1 || !p.prd_all_lvls)) {
-    if ((r = cosa_gpu_tur_vis(c, nl, q, P.mut))) return r;
-    if ((r = cosa_gpu_cutman_mut(c, nl, P.mut))) return r;
+    // SST: the stage's cell-centred differences are still in qp, qm, dqm
+    if (p.kom_sst) r = cosa_gpu_tur_vis_sst(c, nl, q, P.mut, P.qp, P.qm, P.dqm, L.d_vm, P.dist);
+    else r = cosa_gpu_tur_vis(c, nl, q, P.mut);
+    if (r || (r = cosa_gpu_cutman_mut(c, nl, P.mut))) return r;
   }
   return COSA_OK;
 }
@@ -2860,7 +2968,7 @@ extern "C" int cosa_gpu_autotune(cosa_ctx *c, int32_t nl, int32_t niter, double 
   int r = check_fused_supported(c->p);
   if (r) return r;
   ms[0] = ms[1] = 0.0;
-  if (c->p.kom) {  // the k-omega stage has one schedule
+  if (rans(c->p)) {  // the k-omega stage has one schedule
     L->schedule = 0;
     if (choice) *choice = 0;
     return COSA_OK;

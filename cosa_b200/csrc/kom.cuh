@@ -1,6 +1,7 @@
-// Wilcox k-omega terms of the B200 path (kom = .true., viscous, fixed grid),
-// with the reference's array contract (one kernel per routine, the level
-// drivers in cosa_gpu.cu loop over blocks like the Fortran drivers).
+// k-omega terms of the B200 path (Wilcox kom, BSL kom_bsl, SST kom_sst;
+// viscous, fixed grid), with the reference's array contract (one kernel per
+// routine, the level drivers in cosa_gpu.cu loop over blocks like the
+// Fortran drivers).
 //
 //   k_qface_mut       q_face with calmut: face mut into flux(.,1)
 //   k_rtst            b_rtst: Reynolds stresses on the faces
@@ -14,6 +15,14 @@
 //   k_lim_prod_mg     lim_prod_mg_b: production limiter before restriction
 //   k_lim_res_ome     lim_res_ome_b: omega residual limiter (residual pass)
 //   k_add_interior    add_array over the interior cells (multigrid forcing)
+//   k_facedist        facedist_b: face wall distances (BSL/SST)
+//   k_update_ttrm     update_ttrm_b: blended gamma, beta, cross diffusion
+//   k_tur_vis_sst     tur_vis_sst_b: SST eddy viscosity (+ k_tur_vis_sst_halo)
+//
+// BSL/SST: ttrm is (-1:imax+1,...,3,0:S-1) per block at op3*3*S; the face
+// distances are one F0 scalar per face family; k_srckw, k_update_kom and
+// k_lim_res_ome read gamma, beta (and the cross diffusion) from ttrm when it
+// is given, Wilcox's constants otherwise.
 #pragma once
 #include "visc.cuh"
 
@@ -43,6 +52,47 @@
 
 __device__ __forceinline__ int64_t p3s_idx(const DevBlock &b, int S, int i, int j, int k, int n) {
   return b.op3 * S + (int64_t)n * b.P3 + p3_cell(b, i, j, k);
+}
+// ttrm(i,j,k,c,n), c = 1..3
+__device__ __forceinline__ int64_t ttrm_idx(const DevBlock &b, int S, int i, int j, int k, int c, int n) {
+  return b.op3 * 3 * S + ((int64_t)n * 3 + (c - 1)) * b.P3 + p3_cell(b, i, j, k);
+}
+
+// the BSL/SST closure constants of input() (src/input.f90:2522-2539)
+struct BlendPar {
+  double sigk1, sigk2, sigw1, sigw2, b1, b2, g1, g2, a1;
+};
+__device__ __forceinline__ BlendPar make_blend(const cosa_params &P) {
+  BlendPar c;
+  const double bstr = 0.09;
+  c.a1 = 0.31;
+  c.sigk1 = P.kom_sst ? 0.85 : 0.5;
+  c.sigk2 = 1.0;
+  c.sigw1 = 0.5;
+  c.b1 = 3.0 / 40.0;
+  c.g1 = __dsub_rn(c.b1 / bstr, __dmul_rn(c.sigw1, P.kappa * P.kappa) / sqrt(bstr));
+  c.sigw2 = 0.856;
+  c.b2 = 0.0828;
+  c.g2 = __dsub_rn(c.b2 / bstr, __dmul_rn(c.sigw2, P.kappa * P.kappa) / sqrt(bstr));
+  return c;
+}
+// F1 (F2) as the reference writes tanh: (e^2a - 1) / (e^2a + 1)
+__device__ __forceinline__ double tanh_ref(double a) {
+  const double e = exp(2 * a);
+  return (e - 1) / (e + 1);
+}
+// F1 of update_ttrm_b / vflux from rho, k, omega, mu, the k.omega gradient
+// product and the wall distance; cdt out
+__device__ __forceinline__ double blend_f1(const BlendPar &c, const cosa_params &P, double rho, double tke, double ome,
+                                           double mu, double gradkw, double dist, double &cdt) {
+  const double dd = dist + P.epst, d2 = dd * dd;
+  double arg1 = fmax(sqrt(tke) / 0.09 / ome / dd, 500 * mu / rho / ome / d2 * P.machfs / P.reyno);
+  cdt = 2 * rho * c.sigw2 / ome * gradkw;
+  const double acdt = fmax(cdt, 1.0e-20);
+  arg1 = fmin(arg1, 4 * rho * c.sigw2 * tke / acdt / d2);
+  const double a2 = arg1 * arg1;
+  arg1 = fmin(a2 * a2, 1.0e2);
+  return tanh_ref(arg1);
 }
 
 // mut on the faces of family D into flux(.,1) (bq_face_* calmut part)
@@ -114,7 +164,7 @@ __global__ void k_vflux_kom(BS bs_, int d, const cosa_params *__restrict__ Pp, c
                             const double *__restrict__ g0, const double *__restrict__ g1,
                             const double *__restrict__ g2, const double *__restrict__ tau,
                             const double *__restrict__ vm, int64_t n0, const double *__restrict__ s,
-                            double *__restrict__ flux) {
+                            double *__restrict__ flux, const double *__restrict__ fdist) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
@@ -143,8 +193,20 @@ __global__ void k_vflux_kom(BS bs_, int d, const cosa_params *__restrict__ Pp, c
     Fk[1] = -(txx * kx + txy * ky + txz * kz) * ds;
     Fk[2] = -(txy * kx + tyy * ky + tyz * kz) * ds;
     Fk[3] = -(txz * kx + tyz * ky + tzz * kz) * ds;
-    const double ctke = (mu + P.sigk * mut) * P.machfs / P.reyno;
-    const double come = (mu + P.sigw * mut) * P.machfs / P.reyno;
+    double sigk = P.sigk, sigw = P.sigw;
+    if (fdist) {
+      // BSL/SST (src/flux.f90:987-1061): sigma_k, sigma_omega blended by F1 of
+      // the face state and the face's wall distance
+      const BlendPar c = make_blend(P);
+      const double domedz = omexi * vmf[2] + omeeta * vmf[5] + omezeta * vmf[8];
+      double cdt;
+      const double f1 = blend_f1(c, P, rho, Q(qf, 6), Q(qf, 7), mu, dtkedx * domedx + dtkedy * domedy + dtkedz * domedz,
+                                 fdist[f0_idx(b, 1, 1, i, j, k, 1, 0)], cdt);
+      sigk = f1 * c.sigk1 + (1 - f1) * c.sigk2;
+      sigw = f1 * c.sigw1 + (1 - f1) * c.sigw2;
+    }
+    const double ctke = (mu + sigk * mut) * P.machfs / P.reyno;
+    const double come = (mu + sigw * mut) * P.machfs / P.reyno;
     Fk[4] = -ctke * (dtkedx * kx + dtkedy * ky + dtkedz * kz) * ds;
     Fk[5] = -ctke * (dtkedx * kx + dtkedy * ky + dtkedz * kz) * ds;
     Fk[6] = -come * (domedx * kx + domedy * ky + dtkedz * kz) * ds;
@@ -161,15 +223,16 @@ __global__ void k_vflux_kom(BS bs_, int d, const cosa_params *__restrict__ Pp, c
   }
 }
 
-// q_der_c (src/flux.f90:2979-3130): velocity differences of the face values
+// q_der_c (src/flux.f90:2979-3130): velocity differences of the face
+// values, and of k and omega under BSL/SST (vhi = 7)
 template <int D, class BS>
-__global__ void k_qder_c(BS bs_, int npde, int S, const double *__restrict__ qf, double *__restrict__ dc) {
+__global__ void k_qder_c(BS bs_, int npde, int S, const double *__restrict__ qf, double *__restrict__ dc, int vhi) {
   const DevBlock b = bs_.get();
   KOM_CELL_LOOP
     const int di = D == 1, dj = D == 2, dk = D == 3;
     const int64_t c0 = p3_cell(b, i, j, k), c1 = p3_cell(b, i + di, j + dj, k + dk);
-#pragma unroll
-    for (int v = 2; v <= 4; ++v) {
+    for (int v = 2; v <= vhi; ++v) {
+      if (v == 5) continue;
       const int64_t o = p3_var(b, npde, S, v, n);
       dc[o + c0] = qf[o + c1] - qf[o + c0];
     }
@@ -218,7 +281,8 @@ __global__ void k_turprod(BS bs_, const cosa_params *__restrict__ Pp, const doub
 template <class BS>
 __global__ void k_srckw(BS bs_, const cosa_params *__restrict__ Pp, int nl, const double *__restrict__ q,
                         const double *__restrict__ mut, const double *__restrict__ prd,
-                        const double *__restrict__ divvel, double *__restrict__ res, const double *__restrict__ vol) {
+                        const double *__restrict__ divvel, double *__restrict__ res, const double *__restrict__ vol,
+                        const double *__restrict__ ttrm) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
@@ -239,7 +303,14 @@ __global__ void k_srckw(BS bs_, const cosa_params *__restrict__ Pp, int nl, cons
     const double v = vol[p1_idx(b, 1, i, j, k, 0)];
     double *r6 = res + p3_var(b, npde, S, 6, n) + c, *r7 = res + p3_var(b, npde, S, 7, n) + c;
     *r6 = *r6 - v * (mor * mt * prod - fact * divv * rho * tke - P.bstrkw * rho * tke * ome);
-    *r7 = *r7 - v * (P.gkw * P.cmu * rho * prodw - P.gkw * fact * divv * rho * ome - P.bkw * rho * (ome * ome));
+    if (ttrm) {
+      // srckw_sst_b (src/src.f90:306-378): blended gamma, beta and the cross diffusion
+      const double cdif = ttrm[ttrm_idx(b, S, i, j, k, 1, n)], gav = ttrm[ttrm_idx(b, S, i, j, k, 2, n)];
+      const double bav = ttrm[ttrm_idx(b, S, i, j, k, 3, n)];
+      *r7 = *r7 - v * (gav * P.cmu * rho * prodw - gav * fact * divv * rho * ome - bav * rho * (ome * ome) + cdif);
+    } else {
+      *r7 = *r7 - v * (P.gkw * P.cmu * rho * prodw - P.gkw * fact * divv * rho * ome - P.bkw * rho * (ome * ome));
+    }
   }
 }
 
@@ -248,12 +319,13 @@ template <class BS>
 __global__ void k_update_kom(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
                              double *__restrict__ q, const double *__restrict__ qold, const double *__restrict__ vol,
                              const double *__restrict__ dtt, const double *__restrict__ delpls,
-                             const double *__restrict__ prd, double ar) {
+                             const double *__restrict__ prd, double ar, const double *__restrict__ ttrm) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
-  const double gav = P.gkw, bav = P.bkw;
   KOM_CELL_LOOP
+    const double gav = ttrm ? ttrm[ttrm_idx(b, S, i, j, k, 2, n)] : P.gkw;
+    const double bav = ttrm ? ttrm[ttrm_idx(b, S, i, j, k, 3, n)] : P.bkw;
     const int64_t c = p3_cell(b, i, j, k), o = p3s_idx(b, S, i, j, k, n);
     const int64_t i1 = p3_var(b, npde, S, 1, n) + c, i6 = p3_var(b, npde, S, 6, n) + c, i7 = p3_var(b, npde, S, 7, n) + c;
     const double rho = q[i1], ome = q[i7] / q[i1], tke = q[i6] / q[i1];
@@ -339,12 +411,13 @@ template <class BS>
 __global__ void k_lim_res_ome(BS bs_, const cosa_params *__restrict__ Pp, double *__restrict__ res,
                               const double *__restrict__ q, const double *__restrict__ vol,
                               const double *__restrict__ dtt, const double *__restrict__ delpls,
-                              const double *__restrict__ prd, double ar) {
+                              const double *__restrict__ prd, double ar, const double *__restrict__ ttrm) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
-  const double gav = P.gkw, bav = P.bkw;
   KOM_CELL_LOOP
+    const double gav = ttrm ? ttrm[ttrm_idx(b, S, i, j, k, 2, n)] : P.gkw;
+    const double bav = ttrm ? ttrm[ttrm_idx(b, S, i, j, k, 3, n)] : P.bkw;
     const int64_t c = p3_cell(b, i, j, k), o = p3s_idx(b, S, i, j, k, n);
     const int64_t i1 = p3_var(b, npde, S, 1, n) + c, i7 = p3_var(b, npde, S, 7, n) + c;
     const double dt = dtt[p1_idx(b, S, i, j, k, n)];
@@ -373,5 +446,148 @@ __global__ void k_add_interior(BS bs_, int nvs, double *__restrict__ v1, const d
     const int k = (int)(r % nk) + 1; r /= nk;
     const int64_t o = base + r * b.P3 + p3_cell(b, i, j, k);
     v1[o] = v1[o] + v2[o] * fact;
+  }
+}
+
+// ---- BSL / SST ---------------------------------------------------------------------------
+// facedist_b (src/grid.f90:2833-2870): one thread per face of family D with
+// interior tangential indices; the mean of the two cells' wall distances,
+// the boundary cell's own on the block faces
+template <int D>
+__global__ void k_facedist(DevBlock b, const double *__restrict__ dist, double *__restrict__ fd) {
+  const int S = 1;
+  KOM_FACE_LOOP(D)
+    (void)n;
+    const int m = D == 1 ? i : (D == 2 ? j : k), mx = D == 1 ? b.im : (D == 2 ? b.jm : b.km);
+    const int di = D == 1, dj = D == 2, dk = D == 3;
+    double v;
+    if (m == 1) v = dist[p1_idx(b, 1, i - di, j - dj, k - dk, 0)];
+    else if (m == mx) v = dist[p1_idx(b, 1, i, j, k, 0)];
+    else v = (dist[p1_idx(b, 1, i - di, j - dj, k - dk, 0)] + dist[p1_idx(b, 1, i, j, k, 0)]) / 2;
+    fd[f0_idx(b, 1, 1, i, j, k, 1, 0)] = v;
+  }
+}
+
+// the cell-centre inverse metrics of turprod_b / update_ttrm_b / tur_vis_sst_b:
+// met[m][c] = d(xi_m)/d(x_c), averaged over the two faces of family c + 1
+__device__ __forceinline__ void cell_met(const double *__restrict__ vm, const DevBlock &b, int64_t n0, int i, int j,
+                                         int k, double met[3][3]) {
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    met[m][0] = (vm[vm_idx(b, n0, 1, m, 0, i + 1, j, k)] + vm[vm_idx(b, n0, 1, m, 0, i, j, k)]) / 2;
+    met[m][1] = (vm[vm_idx(b, n0, 2, m, 1, i, j + 1, k)] + vm[vm_idx(b, n0, 2, m, 1, i, j, k)]) / 2;
+    met[m][2] = (vm[vm_idx(b, n0, 3, m, 2, i, j, k + 1)] + vm[vm_idx(b, n0, 3, m, 2, i, j, k)]) / 2;
+  }
+}
+
+// update_ttrm_b (src/update.f90:3036-3161) on the primitive state with the
+// cell-centred k and omega differences; Wilcox: (0, gkw, bkw)
+template <class BS>
+__global__ void k_update_ttrm(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
+                              const double *__restrict__ dx, const double *__restrict__ de,
+                              const double *__restrict__ dz, const double *__restrict__ vm, int64_t n0,
+                              double *__restrict__ ttrm, const double *__restrict__ dist) {
+  const DevBlock b = bs_.get();
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const BlendPar cb = make_blend(P);
+  KOM_CELL_LOOP
+    if (P.kom) {
+      ttrm[ttrm_idx(b, S, i, j, k, 1, n)] = 0.0;
+      ttrm[ttrm_idx(b, S, i, j, k, 2, n)] = P.gkw;
+      ttrm[ttrm_idx(b, S, i, j, k, 3, n)] = P.bkw;
+      continue;
+    }
+    const int64_t c = p3_cell(b, i, j, k);
+    auto Q = [&](const double *a, int v) { return a[p3_var(b, npde, S, v, n) + c]; };
+    const double rho = Q(q, 1), tke = Q(q, 6), ome = Q(q, 7), p = Q(q, 5);
+    const double tt = P.gamma * p / rho;
+    const double mu = sutherland(tt, P.stemp);
+    double met[3][3];
+    cell_met(vm, b, n0, i, j, k, met);
+    const double tkexi = Q(dx, 6), tkeeta = Q(de, 6), tkezeta = Q(dz, 6);
+    const double omexi = Q(dx, 7), omeeta = Q(de, 7), omezeta = Q(dz, 7);
+    const double dtkedx = tkexi * met[0][0] + tkeeta * met[1][0] + tkezeta * met[2][0];
+    const double dtkedy = tkexi * met[0][1] + tkeeta * met[1][1] + tkezeta * met[2][1];
+    const double dtkedz = tkexi * met[0][2] + tkeeta * met[1][2] + tkezeta * met[2][2];
+    const double domedx = omexi * met[0][0] + omeeta * met[1][0] + omezeta * met[2][0];
+    const double domedy = omexi * met[0][1] + omeeta * met[1][1] + omezeta * met[2][1];
+    const double domedz = omexi * met[0][2] + omeeta * met[1][2] + omezeta * met[2][2];
+    double cdt;
+    const double f1 = blend_f1(cb, P, rho, tke, ome, mu, dtkedx * domedx + dtkedy * domedy + dtkedz * domedz,
+                               dist[p1_idx(b, 1, i, j, k, 0)], cdt);
+    ttrm[ttrm_idx(b, S, i, j, k, 1, n)] = cdt * (1 - f1);
+    ttrm[ttrm_idx(b, S, i, j, k, 2, n)] = f1 * cb.g1 + (1 - f1) * cb.g2;
+    ttrm[ttrm_idx(b, S, i, j, k, 3, n)] = f1 * cb.b1 + (1 - f1) * cb.b2;
+  }
+}
+
+// tur_vis_sst_b (src/update.f90:2375-2460), interior cells: mut = a1 rho k /
+// max(a1 omega, sqrt(2 S) F2) of the conservative state with the stage's
+// cell-centred velocity differences
+template <class BS>
+__global__ void k_tur_vis_sst(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
+                              double *__restrict__ mut, const double *__restrict__ dx,
+                              const double *__restrict__ de, const double *__restrict__ dz,
+                              const double *__restrict__ vm, int64_t n0, const double *__restrict__ dist) {
+  const DevBlock b = bs_.get();
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const BlendPar cb = make_blend(P);
+  KOM_CELL_LOOP
+    const int64_t c = p3_cell(b, i, j, k);
+    auto Q = [&](const double *a, int v) { return a[p3_var(b, npde, S, v, n) + c]; };
+    const double q1 = Q(q, 1), q2 = Q(q, 2), q3 = Q(q, 3), q4 = Q(q, 4);
+    const double p = (P.gamma - 1) * (Q(q, 5) - (q2 * q2 + q3 * q3 + q4 * q4) / q1 / 2 - Q(q, 6));
+    const double rho = q1, tke = Q(q, 6) / rho, ome = Q(q, 7) / rho;
+    const double tt = P.gamma * p / rho;
+    const double mu = sutherland(tt, P.stemp);
+    double met[3][3];
+    cell_met(vm, b, n0, i, j, k, met);
+    double dv[3][3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const double a = Q(dx, v + 2), e = Q(de, v + 2), f = Q(dz, v + 2);
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) dv[v][cc] = a * met[0][cc] + e * met[1][cc] + f * met[2][cc];
+    }
+    const double sxx = dv[0][0], sxy = (dv[0][1] + dv[1][0]) / 2, sxz = (dv[0][2] + dv[2][0]) / 2;
+    const double syy = dv[1][1], syz = (dv[1][2] + dv[2][1]) / 2, szz = dv[2][2];
+    const double sn = sxx * sxx + syy * syy + szz * szz + 2 * (sxy * sxy + sxz * sxz + syz * syz);
+    const double dd = dist[p1_idx(b, 1, i, j, k, 0)] + P.epst;
+    double arg2 = fmax(2 * sqrt(tke) / 0.09 / ome / dd, 500 * mu / rho / ome / (dd * dd) * P.machfs / P.reyno);
+    arg2 = fmin(arg2 * arg2, 1.0e2);
+    const double f2 = tanh_ref(arg2);
+    const double fact = sqrt(2 * sn);
+    mut[p3s_idx(b, S, i, j, k, n)] = cb.a1 * rho * tke / fmax(cb.a1 * ome, fact * f2) * P.reyno / P.machfs;
+  }
+}
+// the face halos of tur_vis_sst_b: mut of the adjacent interior cell, on the
+// six faces over the interior tangential ranges (edges and corners left)
+template <class BS>
+__global__ void k_tur_vis_sst_halo(BS bs_, int S, double *__restrict__ mut) {
+  const DevBlock b = bs_.get();
+  const int ni = b.im - 1, nj = b.jm - 1, nk = b.km - 1;
+  const int64_t fi = (int64_t)nj * nk, fj = (int64_t)ni * nk, fk = (int64_t)ni * nj;
+  const int64_t per = 2 * (fi + fj + fk), total = per * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int n = (int)(t / per);
+    int64_t r = t % per;
+    int i, j, k, si, sj, sk;
+    if (r < 2 * fk) {
+      const int side = (int)(r / fk); r %= fk;
+      i = (int)(r % ni) + 1; j = (int)(r / ni) + 1; k = side ? b.km : 0;
+      si = i; sj = j; sk = side ? b.km - 1 : 1;
+    } else if ((r -= 2 * fk) < 2 * fj) {
+      const int side = (int)(r / fj); r %= fj;
+      i = (int)(r % ni) + 1; k = (int)(r / ni) + 1; j = side ? b.jm : 0;
+      si = i; sj = side ? b.jm - 1 : 1; sk = k;
+    } else {
+      r -= 2 * fj;
+      const int side = (int)(r / fi); r %= fi;
+      j = (int)(r % nj) + 1; k = (int)(r / nj) + 1; i = side ? b.im : 0;
+      si = side ? b.im - 1 : 1; sj = j; sk = k;
+    }
+    mut[p3s_idx(b, S, i, j, k, n)] = mut[p3s_idx(b, S, si, sj, sk, n)];
   }
 }

@@ -63,7 +63,8 @@ SYMBOLS = [
     "cosa_gpu_lambda_ns", "cosa_gpu_deltat_ns", "cosa_gpu_q_face_mut", "cosa_gpu_rtst", "cosa_gpu_vflux_kom",
     "cosa_gpu_q_der_c", "cosa_gpu_turprod", "cosa_gpu_srckw", "cosa_gpu_update_kom", "cosa_gpu_cutman_mut",
     "cosa_gpu_autotune", "cosa_gpu_set_schedule", "cosa_gpu_force", "cosa_gpu_rest2_ho", "cosa_gpu_bc_res",
-    "cosa_gpu_movegrid", "cosa_gpu_face_vel", "cosa_gpu_vert2cell",
+    "cosa_gpu_movegrid", "cosa_gpu_face_vel", "cosa_gpu_vert2cell", "cosa_gpu_facedist", "cosa_gpu_update_ttrm",
+    "cosa_gpu_srckw_sst", "cosa_gpu_tur_vis_sst",
 ]
 
 
@@ -187,6 +188,10 @@ class Context:
 
     def alloc_f0(self, nl=1):
         return DevArray(self, self.sizes(nl)[3] * self.params.npde * self.S)
+
+    def alloc_f0s(self, nl=1):
+        """One F0 scalar (imax, jmax, kmax) per block, no snapshots (face wall distance)."""
+        return DevArray(self, self.sizes(nl)[3])
 
     def status(self, reset: bool = False) -> int:
         return load().cosa_gpu_status(self.h, 1 if reset else 0)
@@ -400,10 +405,12 @@ class Context:
         self._check(load().cosa_gpu_rtst(self.h, idir, nl, _ptr(qf.ptr), _ptr(dqxi.ptr), _ptr(dqeta.ptr),
                                          _ptr(dqzeta.ptr), _ptr(vm.ptr), _ptr(flux.ptr), _ptr(tau1.ptr)), "rtst")
 
-    def vflux_kom(self, idir, nl, qf, dqxi, dqeta, dqzeta, tau1, vm, sijk, flux):
+    def vflux_kom(self, idir, nl, qf, dqxi, dqeta, dqzeta, tau1, vm, sijk, flux, fdist=None):
+        """fdist: the face wall distances of family idir (BSL/SST)."""
         self._check(load().cosa_gpu_vflux_kom(self.h, idir, nl, _ptr(qf.ptr), _ptr(dqxi.ptr), _ptr(dqeta.ptr),
                                               _ptr(dqzeta.ptr), _ptr(tau1.ptr), _ptr(vm.ptr), _ptr(sijk.ptr),
-                                              _ptr(flux.ptr)), "vflux_kom")
+                                              _ptr(flux.ptr), _ptr(fdist.ptr if fdist is not None else None)),
+                    "vflux_kom")
 
     def q_der_c(self, idir, nl, qf, dqc):
         self._check(load().cosa_gpu_q_der_c(self.h, idir, nl, _ptr(qf.ptr), _ptr(dqc.ptr)), "q_der_c")
@@ -417,10 +424,28 @@ class Context:
         self._check(load().cosa_gpu_srckw(self.h, nl, _ptr(q.ptr), _ptr(mut.ptr), _ptr(prd.ptr), _ptr(divvel.ptr),
                                           _ptr(res.ptr), _ptr(vol.ptr)), "srckw")
 
-    def update_kom(self, nl, res, q, qold, vol, dtvolt, delpls, prd, ar):
+    def update_kom(self, nl, res, q, qold, vol, dtvolt, delpls, prd, ar, ttrm=None):
         self._check(load().cosa_gpu_update_kom(self.h, nl, _ptr(res.ptr), _ptr(q.ptr), _ptr(qold.ptr), _ptr(vol.ptr),
-                                               _ptr(dtvolt.ptr), _ptr(delpls.ptr), _ptr(prd.ptr), C.c_double(ar)),
-                    "update_kom")
+                                               _ptr(dtvolt.ptr), _ptr(delpls.ptr), _ptr(prd.ptr), C.c_double(ar),
+                                               _ptr(ttrm.ptr if ttrm is not None else None)), "update_kom")
+
+    def facedist(self, nl, dist, fidist, fjdist, fkdist):
+        self._check(load().cosa_gpu_facedist(self.h, nl, _ptr(dist.ptr), _ptr(fidist.ptr), _ptr(fjdist.ptr),
+                                             _ptr(fkdist.ptr)), "facedist")
+
+    def update_ttrm(self, nl, q, dqxi, dqeta, dqzeta, vm, ttrm, dist):
+        self._check(load().cosa_gpu_update_ttrm(self.h, nl, _ptr(q.ptr), _ptr(dqxi.ptr), _ptr(dqeta.ptr),
+                                                _ptr(dqzeta.ptr), _ptr(vm.ptr), _ptr(ttrm.ptr), _ptr(dist.ptr)),
+                    "update_ttrm")
+
+    def srckw_sst(self, nl, q, prd, divvel, res, mut, ttrm, vol):
+        self._check(load().cosa_gpu_srckw_sst(self.h, nl, _ptr(q.ptr), _ptr(prd.ptr), _ptr(divvel.ptr), _ptr(res.ptr),
+                                              _ptr(mut.ptr), _ptr(ttrm.ptr), _ptr(vol.ptr)), "srckw_sst")
+
+    def tur_vis_sst(self, nl, q, mut, dqxi, dqeta, dqzeta, vm, dist):
+        self._check(load().cosa_gpu_tur_vis_sst(self.h, nl, _ptr(q.ptr), _ptr(mut.ptr), _ptr(dqxi.ptr),
+                                                _ptr(dqeta.ptr), _ptr(dqzeta.ptr), _ptr(vm.ptr), _ptr(dist.ptr)),
+                    "tur_vis_sst")
 
     def cutman_mut(self, nl, mut):
         self._check(load().cosa_gpu_cutman_mut(self.h, nl, _ptr(mut.ptr)), "cutman_mut")

@@ -367,8 +367,10 @@ int cosa_gpu_deltat_ns(cosa_ctx *ctx, int32_t nl, double *dtvol, const double *l
                        const double *lamv, double *bx, double *by, double *bz,
                        double *dtvolt, double *tbx, double *tby, double *tbz);
 
-/* ---- Wilcox k-omega (kom = .true., npde = 7); mut, prd, divvel, delpls
-   are scalar P3 arrays (-1:imax+1,...,0:S-1) ---- */
+/* ---- k-omega: Wilcox (kom), BSL (kom_bsl), SST (kom_sst); npde = 7; mut,
+   prd, divvel, delpls are scalar P3 arrays (-1:imax+1,...,0:S-1); ttrm
+   (BSL/SST) is (-1:imax+1,...,3,0:S-1) per block at off_p3 * 3 * S; the face
+   wall distances are one F0 scalar array (imax,jmax,kmax) per face family ---- */
 /* q_face with calmut (src/flux.f90:2495-2540): face mut into flux(.,1) */
 int cosa_gpu_q_face_mut(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *mut, double *flux);
 /* rtst (src/flux.f90:2803-2946): Reynolds stresses tau1(.,1..6) on the faces
@@ -376,14 +378,15 @@ int cosa_gpu_q_face_mut(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *m
 int cosa_gpu_rtst(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *qf, const double *dqxi,
                   const double *dqeta, const double *dqzeta, const double *vm,
                   const double *flux, double *tau1);
-/* vflux with kom (src/flux.f90:915-1180): Reynolds-stress and k/omega
+/* vflux with k-omega (src/flux.f90:915-1180): Reynolds-stress and k/omega
    diffusion fluxes plus the laminar terms; flux(.,1) holds the face mut on
-   entry */
+   entry; fdist, the face wall distances of family idir, for BSL/SST (sigma
+   blended by F1, src/flux.f90:987-1061) and null for Wilcox */
 int cosa_gpu_vflux_kom(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *qf, const double *dqxi,
                        const double *dqeta, const double *dqzeta, const double *tau1,
-                       const double *vm, const double *sijk, double *flux);
+                       const double *vm, const double *sijk, double *flux, const double *fdist);
 /* q_der_c (src/flux.f90:2949-3130): cell-centred velocity differences of
-   the face values of family idir */
+   the face values of family idir (and of k, omega under BSL/SST) */
 int cosa_gpu_q_der_c(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *qf, double *dqc);
 /* turprod (src/src.f90:2-177): production, div u and delta+ */
 int cosa_gpu_turprod(cosa_ctx *ctx, int32_t nl, const double *dqxi, const double *dqeta,
@@ -393,10 +396,28 @@ int cosa_gpu_turprod(cosa_ctx *ctx, int32_t nl, const double *dqxi, const double
 int cosa_gpu_srckw(cosa_ctx *ctx, int32_t nl, const double *q, const double *mut, const double *prd,
                    const double *divvel, double *res, const double *vol);
 /* update_b, k-omega part (src/update.f90:601-640): point-implicit rho omega
-   and rho k; call before cosa_gpu_update (which updates variables 1..5) */
+   and rho k; call before cosa_gpu_update (which updates variables 1..5);
+   ttrm: gamma and beta per cell (BSL/SST), null for Wilcox's constants */
 int cosa_gpu_update_kom(cosa_ctx *ctx, int32_t nl, const double *res, double *q, const double *qold,
                         const double *vol, const double *dtvolt, const double *delpls,
-                        const double *prd, double ar);
+                        const double *prd, double ar, const double *ttrm);
+/* facedist (src/grid.f90:2809-2870): face wall distances of the three
+   families from the cell distances dist (P1) */
+int cosa_gpu_facedist(cosa_ctx *ctx, int32_t nl, const double *dist, double *fidist, double *fjdist,
+                      double *fkdist);
+/* update_ttrm (src/update.f90:3000-3161): ttrm = ((1 - F1) CD, gamma, beta)
+   blended by F1 from the primitive state, the cell-centred k and omega
+   differences of q_der_c and dist; Wilcox: (0, gkw, bkw) */
+int cosa_gpu_update_ttrm(cosa_ctx *ctx, int32_t nl, const double *q, const double *dqxi, const double *dqeta,
+                         const double *dqzeta, const double *vm, double *ttrm, const double *dist);
+/* srckw_sst (src/src.f90:275-378): BSL/SST k and omega sources into res(6:7) */
+int cosa_gpu_srckw_sst(cosa_ctx *ctx, int32_t nl, const double *q, const double *prd, const double *divvel,
+                       double *res, const double *mut, const double *ttrm, const double *vol);
+/* tur_vis_sst (src/update.f90:2340-2460): SST eddy viscosity of the
+   conservative state with the cell-centred velocity differences; the face
+   halos copy the adjacent cell */
+int cosa_gpu_tur_vis_sst(cosa_ctx *ctx, int32_t nl, const double *q, double *mut, const double *dqxi,
+                         const double *dqeta, const double *dqzeta, const double *vm, const double *dist);
 /* cutman_mut (src/bc.f90:2713-2799) */
 int cosa_gpu_cutman_mut(cosa_ctx *ctx, int32_t nl, double *mut);
 

@@ -3627,7 +3627,7 @@ int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_p
   if (mut_first) {
     // coarse-level mut from the restricted (primitive) state at the first
     // stage of the first cycle's visit (src/cosa.f90:1727-1760); SST takes
-    // the cell-centred differences of a copy, back in conservative form
+    // the cell-centred differences of a copy of q, back in conservative form
     if (p->kom_sst) {
       std::vector<double> w(q, q + L.n3 * L.npde * L.S);
       double *dc[3] = {A.qp, A.qm, A.dqm};
@@ -3638,6 +3638,8 @@ int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_p
         }
       for (int b = 0; b < L.nb; ++b) prim2cons_b(L, b, w.data(), *p);
       tur_vis_sst_level(L, w.data(), A.mut, A.qp, A.qm, A.dqm, X.vm, A.dist, *p);
+      // the reference works in res and zeroes all of it afterwards
+      std::fill(A.res, A.res + L.n3 * L.npde * L.S, 0.0);
     } else {
       tur_vis_level(L, q, A.mut, *p);
     }
