@@ -21,11 +21,15 @@
 #include "faces.cuh"
 #include "moving.cuh"
 #include "force.cuh"
+#include "unsteady.cuh"
 
 namespace {
 // any k-omega variant: Wilcox (kom), BSL (kom_bsl), SST (kom_sst)
 inline bool rans(const cosa_params &p) { return p.kom || p.kom_bsl || p.kom_sst; }
 inline bool blend(const cosa_params &p) { return p.kom_bsl || p.kom_sst; }
+// dual time: src_uns enters the residual unless rkimp without IRS on one
+// level, where update_b takes the physical-time term alone (src/cosa.f90:1910-1915)
+inline bool dual_src_in_res(const cosa_params &p) { return p.dualt && (!p.rkimp || p.irsop > 0 || p.nlevel > 1); }
 
 constexpr int kTI = 32, kTJ = 7;  // tile of the fused stage kernel (7 rows + the boundary-face warp = 256 threads)
 
@@ -530,8 +534,8 @@ int set_smem_attrs() {
 // the k-omega stage runs routine by routine (launch_rans_iteration); Wilcox,
 // BSL and SST
 int check_rans_supported(const cosa_params &p) {
-  if (p.npde != 7 || !rans(p) || (p.kom + p.kom_bsl + p.kom_sst) != 1 || !p.viscous || p.rkimp || p.moving ||
-      p.harbal ||
+  if (p.npde != 7 || !rans(p) || (p.kom + p.kom_bsl + p.kom_sst) != 1 || !p.viscous || (p.rkimp && !p.dualt) ||
+      p.moving || p.harbal || (p.dualt && p.dt <= 0) ||
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
   return COSA_OK;
@@ -542,7 +546,9 @@ int check_fused_supported(const cosa_params &p) {
   // rkimp: the implicit time-spectral update of harmonic balance (update_bhb,
   // src/update.f90:1564-1604 without IRS on one level, 1771-1836 with IRS or
   // multigrid)
-  if (p.rkimp && !p.harbal) return COSA_ERR_UNSUPPORTED;
+  if (p.rkimp && !p.harbal && !p.dualt) return COSA_ERR_UNSUPPORTED;
+  // dual time: one snapshot, fixed grid, a physical time step
+  if (p.dualt && (p.harbal || p.moving || p.dt <= 0)) return COSA_ERR_UNSUPPORTED;
   if (p.npde != 5 || p.kom || p.kom_bsl || p.kom_sst ||
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
@@ -943,7 +949,8 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
 
 // what one RK iteration of smooth() does besides the stages themselves
 struct IterOpts {
-  bool want_rms = false;       // stage-1 residual norm (fine level, printed cycle)
+  bool want_rms = false;       // residual norm (fine level, printed cycle) at stage rms_stage
+  int rms_stage = 1;           // 1 for smooth(); nstage for rkuns (the last stage's norm is kept)
   int compute_dt = 0;          // stage-1 local time step
   double *rhs = nullptr;       // coarse-level forcing: res -= rhs at every stage
   bool force = false;          // rhs += res at stage 1 (first iteration of a from_fine visit)
@@ -954,12 +961,101 @@ struct IterOpts {
 
 int launch_rans_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o);
 
+// residual norm partials of every block (64 CTAs each) and the final sum
+int launch_norm(cosa_ctx *c, LevelState &L, const double *res, const double *rhs, const double *q_imp) {
+  int r = 0;
+  int64_t ncell = 0;
+  for (int b = 0; b < L.nb; ++b) {
+    const DevBlock &x = L.hb[b];
+    double *part = L.d_part + (int64_t)b * 64 * 8;
+    if (q_imp) k_rms_dualimp<<<64, 256, 0, c->s>>>(x, c->d_p, res, rhs, q_imp, L.ptrs.vol, part);
+    else k_rms_partial<<<64, 256, 0, c->s>>>(x, c->d_p, res, rhs, part);
+    if ((r = after_launch(c))) return r;
+    ncell += (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1);
+  }
+  k_rms_final<<<1, 256, 0, c->s>>>(L.d_part, L.nb * 64, c->p.npde, (double)ncell, c->d_hist, c->d_row, c->hist_cap);
+  return after_launch(c);
+}
+
+// what follows the residual of a dual-time stage (src/cosa.f90:1908-1961):
+// src_uns, the fine-level norm (printed cycles), res -= rhs_uns on the fine
+// level, the multigrid forcing on coarse levels; q the stage state
+int dual_tail(cosa_ctx *c, int nl, LevelState &L, const double *q, double *R, const IterOpts &o, int irk) {
+  const cosa_params &p = c->p;
+  const cosa_level_ptrs &P = L.ptrs;
+  const int nvs = p.npde;
+  int r = 0;
+  if (dual_src_in_res(p) &&
+      (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) { k_src_uns<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.vol, R); })))
+    return r;
+  if (nl == 1 && o.want_rms && irk == o.rms_stage &&
+      (r = launch_norm(c, L, R, P.rhs, p.rkimp && !dual_src_in_res(p) ? q : nullptr)))
+    return r;
+  if (nl == 1 &&
+      (r = for_blocks(c, L, cnt_interior, [&](auto b, dim3 g) { k_add_interior<<<g, 256, 0, c->s>>>(b, nvs, R, P.rhs, -1.0); })))
+    return r;
+  if (o.rhs && o.force && irk == 1 &&
+      (r = for_blocks(c, L, cnt_interior, [&](auto b, dim3 g) { k_add_interior<<<g, 256, 0, c->s>>>(b, nvs, o.rhs, R, 1.0); })))
+    return r;
+  if (o.rhs &&
+      (r = for_blocks(c, L, cnt_interior, [&](auto b, dim3 g) { k_add_interior<<<g, 256, 0, c->s>>>(b, nvs, R, o.rhs, -1.0); })))
+    return r;
+  return COSA_OK;
+}
+
 // one RK iteration (nstage stages) of the fused path
 int launch_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
   const cosa_params &p = c->p;
   if (rans(p)) return launch_rans_iteration(c, nl, L, o);
   double *Q = L.ptrs.q, *T = L.d_T, *QO = L.ptrs.qold;
   const int S = 2 * p.nharms + 1;
+  if (p.dualt) {
+    // dual time: residual (no forcing, no update) -> dual_tail -> [IRS] ->
+    // update_b, explicit or with the physical-time term implicit (rkimp)
+    if (o.res_only) {
+      int r = launch_stage(c, nl, L, Q, T, Q, nullptr, 1, o.compute_dt, false, 0, o.res_only);
+      return r ? r : dual_tail(c, nl, L, Q, o.res_only, o, 1);
+    }
+    for (int irk = 1; irk <= p.nstage; ++irk) {
+      double *qin = (irk % 2 == 1) ? Q : T;
+      double *qout = (irk % 2 == 1) ? T : Q;
+      const double *qold = irk == 1 ? Q : QO;
+      double *qcopy = (irk == 1 && o.copy_qold) ? QO : nullptr;
+      int r = launch_stage(c, nl, L, qin, qout, qold, nullptr, irk, o.compute_dt && irk == 1, false, 0, L.d_res);
+      if (r || (r = dual_tail(c, nl, L, qin, L.d_res, o, irk))) return r;
+      if (p.irsop > 0) {
+        const double *beta[3] = {L.ptrs.betaxi ? L.ptrs.betaxi : L.d_beta[0],
+                                 L.ptrs.betaeta ? L.ptrs.betaeta : L.d_beta[1],
+                                 L.ptrs.betazeta ? L.ptrs.betazeta : L.d_beta[2]};
+        if ((r = irs_apply(c, L, L.d_res, L.d_ores, L.ptrs.dtvol, beta))) return r;
+      }
+      const double ar = p.alphas[irk - 1];
+      if (p.rkimp) {
+        const int sir = dual_src_in_res(p) ? 1 : 0;
+        r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+          k_update_dual<<<g, 256, 0, c->s>>>(b, c->d_p, L.d_res, qold, qin, qout, qcopy, L.ptrs.dtvol, L.ptrs.vol,
+                                             ar, sir);
+        });
+      } else {
+        for (int b = 0; b < L.nb && !r; ++b) {
+          const DevBlock &x = L.hb[b];
+          k_update_stage<<<grid_for((int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1)), 256, 0, c->s>>>(
+              x, p.npde, 1, L.d_res, qold, qout, qcopy, L.ptrs.dtvol, ar);
+          r = after_launch(c);
+        }
+      }
+      if (r) return r;
+    }
+    if (p.nstage % 2 == 1)
+      for (int b = 0; b < L.nb; ++b) {
+        const DevBlock &x = L.hb[b];
+        k_copy_interior<<<grid_for((int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1) * p.npde), 256, 0, c->s>>>(
+            x, p.npde, T, Q);
+        int r = after_launch(c);
+        if (r) return r;
+      }
+    return COSA_OK;
+  }
   if (o.res_only) {
     return launch_stage(c, nl, L, Q, T, Q, nullptr, 1, o.compute_dt, false, 0, o.res_only, o.rhs,
                         o.force ? 2 : 1);
@@ -973,7 +1069,7 @@ int launch_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
     if (p.rkimp && (p.irsop > 0 || p.nlevel > 1)) {
       // residual with the time-spectral term -> [IRS] -> update_bhb, which
       // takes the unsmoothed term out again and solves for it implicitly
-      int r = launch_stage(c, nl, L, qin, qout, qold, nullptr, irk, o.compute_dt && irk == 1, o.want_rms && irk == 1,
+      int r = launch_stage(c, nl, L, qin, qout, qold, nullptr, irk, o.compute_dt && irk == 1, o.want_rms && irk == o.rms_stage,
                            0, L.d_res, o.rhs, rmode);
       if (r) return r;
       if (p.irsop > 0) {
@@ -996,7 +1092,7 @@ int launch_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
       int r = launch_stage(c, nl, L, qin, qout, qold, nullptr, irk, o.compute_dt && irk == 1, false, 0, L.d_res,
                            o.rhs, rmode);
       if (r) return r;
-      if (o.want_rms && irk == 1) {
+      if (o.want_rms && irk == o.rms_stage) {
         int64_t ncell = 0;
         for (int b = 0; b < L.nb; ++b) {
           const DevBlock &x = L.hb[b];
@@ -1017,12 +1113,12 @@ int launch_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
       continue;
     }
     if (p.irsop == 0) {
-      int r = launch_stage(c, nl, L, qin, qout, qold, qcopy, irk, o.compute_dt && irk == 1, o.want_rms && irk == 1, 1,
+      int r = launch_stage(c, nl, L, qin, qout, qold, qcopy, irk, o.compute_dt && irk == 1, o.want_rms && irk == o.rms_stage, 1,
                            nullptr, o.rhs, rmode);
       if (r) return r;
     } else {
       // residual (no update) -> implicit smoothing -> update
-      int r = launch_stage(c, nl, L, qin, qout, qold, nullptr, irk, o.compute_dt && irk == 1, o.want_rms && irk == 1,
+      int r = launch_stage(c, nl, L, qin, qout, qold, nullptr, irk, o.compute_dt && irk == 1, o.want_rms && irk == o.rms_stage,
                            0, L.d_res, o.rhs, rmode);
       if (r) return r;
       const double *beta[3] = {L.ptrs.betaxi ? L.ptrs.betaxi : L.d_beta[0],
@@ -1424,6 +1520,29 @@ int cosa_gpu_update(cosa_ctx *c, int32_t nl, const double *res, double *q, const
   });
 }
 
+int cosa_gpu_src_uns(cosa_ctx *c, int32_t nl, const double *q, const double *vol, double *res) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !vol || !res) return COSA_ERR_ARG;
+  if (c->p.harbal || c->p.dt <= 0) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) { k_src_uns<<<g, 256, 0, c->s>>>(b, c->d_p, q, vol, res); });
+}
+
+int cosa_gpu_copy_interior(cosa_ctx *c, int32_t nl, double *dst, const double *src) {
+  LevelState *L = level(c, nl);
+  if (!L || !dst || !src) return COSA_ERR_ARG;
+  const int nvs = c->p.npde * (2 * c->p.nharms + 1);
+  return for_blocks(c, *L, cnt_interior,
+                    [&](auto b, dim3 g) { k_copy_interior<<<g, 256, 0, c->s>>>(b, nvs, src, dst); });
+}
+
+int cosa_gpu_rhs_uns(cosa_ctx *c, int32_t nl, double *rhs, const double *q1, const double *q2, const double *vol) {
+  LevelState *L = level(c, nl);
+  if (!L || !rhs || !q1 || !q2 || !vol) return COSA_ERR_ARG;
+  if (c->p.harbal || c->p.dt <= 0) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_cells,
+                    [&](auto b, dim3 g) { k_rhs_uns<<<g, 256, 0, c->s>>>(b, c->d_p, rhs, q1, q2, vol); });
+}
+
 int cosa_gpu_zero(cosa_ctx *c, int32_t nl, double *a) {
   LevelState *L = level(c, nl);
   if (!L || !a) return COSA_ERR_ARG;
@@ -1467,6 +1586,7 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
   if (!P.q || !P.qold || !P.dtvol || !P.si || !P.sj || !P.sk) return COSA_ERR_ARG;
   if (c->p.harbal && !P.vol) return COSA_ERR_ARG;
   if (c->p.viscous && (!P.vol || !L->d_vm)) return COSA_ERR_ARG;
+  if (c->p.dualt && (nl != 1 || !P.rhs || !P.vol)) return COSA_ERR_ARG;
   if (rans(c->p) && (r = ensure_rans(c, *L))) return r;
   cudaSetDevice(c->device);
   const int npde = c->p.npde;
@@ -1478,8 +1598,8 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
     if (hist && (mgit == 1 || mgit % rms_every == 0 || mgit == last)) rows.push_back(it);
   }
   if ((r = ensure_hist(c, std::max<int>(1, (int)rows.size())))) return r;
-  if ((c->p.irsop > 0 || c->p.rkimp) && (r = ensure_irs_scratch(c, *L))) return r;
-  if (c->p.rkimp && L->npart_cap < L->nb * 64) {  // per-block norm partials of the implicit HB norm
+  if ((c->p.irsop > 0 || c->p.rkimp || c->p.dualt) && (r = ensure_irs_scratch(c, *L))) return r;
+  if ((c->p.rkimp || c->p.dualt) && L->npart_cap < L->nb * 64) {  // per-block norm partials (implicit HB, dual time)
     drop_graphs(c);
     if ((r = dalloc(c, &L->d_part, (size_t)L->nb * 64 * 8))) return r;
     L->npart_cap = L->nb * 64;
@@ -2042,11 +2162,12 @@ int cosa_gpu_smooth_level(cosa_ctx *c, int32_t nl, int32_t niter, int32_t from_f
   const cosa_level_ptrs &P = L->ptrs;
   if (!P.q || !P.qold || !P.dtvol || !P.si || !P.sj || !P.sk) return COSA_ERR_ARG;
   if ((c->p.harbal && !P.vol) || (to_coarse && !P.res) || (nl > 1 && !P.rhs)) return COSA_ERR_ARG;
+  if (c->p.dualt && (!P.rhs || !P.vol)) return COSA_ERR_ARG;
   cudaSetDevice(c->device);
   const bool want = resrms && nl == 1 && niter > 0 && (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle);
   if ((r = ensure_hist(c, 1))) return r;
-  if ((c->p.irsop > 0 || c->p.rkimp) && (r = ensure_irs_scratch(c, *L))) return r;
-  if (c->p.rkimp && L->npart_cap < L->nb * 64) {  // per-block norm partials of the implicit HB norm
+  if ((c->p.irsop > 0 || c->p.rkimp || c->p.dualt) && (r = ensure_irs_scratch(c, *L))) return r;
+  if ((c->p.rkimp || c->p.dualt) && L->npart_cap < L->nb * 64) {  // per-block norm partials (implicit HB, dual time)
     drop_graphs(c);
     if ((r = dalloc(c, &L->d_part, (size_t)L->nb * 64 * 8))) return r;
     L->npart_cap = L->nb * 64;
@@ -2063,6 +2184,61 @@ int cosa_gpu_smooth_level(cosa_ctx *c, int32_t nl, int32_t niter, int32_t from_f
   return cosa_gpu_status(c, 0);
 }
 
+int cosa_gpu_rkuns(cosa_ctx *c, int32_t ntime, int32_t iprint, double *hist) {
+  LevelState *L = level(c, 1);
+  if (!L || !L->bound || ntime < 0 || iprint < 1) return COSA_ERR_ARG;
+  const cosa_params &p = c->p;
+  // fixed grids, Euler and laminar, no IRS (rkuns smooths nothing); the
+  // reference's k-omega variant advances k and omega with a dtvolt that
+  // rkuns never sets
+  if (!p.rgkuns || rans(p) || p.harbal || p.dualt || p.moving || p.irsop != 0 || p.dt <= 0)
+    return COSA_ERR_UNSUPPORTED;
+  int r = check_fused_supported(p);
+  if (r || (r = check_thin_blocks(c, 1))) return r;
+  const cosa_level_ptrs &P = L->ptrs;
+  if (!P.q || !P.qold || !P.dtvol || !P.si || !P.sj || !P.sk || !P.vol) return COSA_ERR_ARG;
+  if (p.viscous && !L->d_vm) return COSA_ERR_ARG;
+  cudaSetDevice(c->device);
+  std::vector<int> rows;
+  for (int it = 0; it < ntime; ++it)
+    if (hist && ((it + 1) % iprint == 0 || it + 1 == ntime)) rows.push_back(it);
+  if ((r = ensure_hist(c, std::max<int>(1, (int)rows.size())))) return r;
+  // deltat_urk: the global time step, once (src/cosa.f90:4039-4041)
+  if ((r = for_blocks(c, *L, cnt_cells,
+                      [&](auto b, dim3 g) { k_deltat_urk<<<g, 256, 0, c->s>>>(b, c->d_p, P.vol, P.dtvol); })))
+    return r;
+  CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
+  size_t ri = 0;
+  for (int it = 0; it < ntime; ++it) {
+    const bool want = ri < rows.size() && rows[ri] == it;
+    if (want) ++ri;
+    IterOpts o;
+    o.want_rms = want;
+    o.rms_stage = p.nstage;  // the norm of the last stage is the one kept
+    o.compute_dt = 0;
+    r = run_graph(c, graph_key(3, 1, 0, want ? 1 : 0), [&] { return launch_iteration(c, 1, *L, o); });
+    if (r) return r;
+  }
+  if (ntime > 0 && !L->items.empty()) {
+    double *last_in = (p.nstage % 2 == 0) ? L->d_T : L->ptrs.q;
+    k_halo_p2c<<<grid_for((int64_t)L->items.size()), 256, 0, c->s>>>(L->d_blocks, L->d_items, (int)L->items.size(),
+                                                                      c->d_p, last_in, L->ptrs.q);
+    if ((r = after_launch(c))) return r;
+  }
+  if (hist) {
+    const int npde = p.npde;
+    std::vector<double> h(rows.size() * (npde + 1));
+    if (!rows.empty())
+      CK(cudaMemcpyAsync(h.data(), c->d_hist, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    CK(cudaStreamSynchronize(c->s));
+    for (int it = 0; it < ntime; ++it)
+      for (int v = 0; v <= npde; ++v) hist[(int64_t)it * (npde + 1) + v] = NAN;
+    for (size_t k = 0; k < rows.size(); ++k)
+      for (int v = 0; v <= npde; ++v) hist[(int64_t)rows[k] * (npde + 1) + v] = h[k * (npde + 1) + v];
+  }
+  return cosa_gpu_status(c, 0);
+}
+
 int cosa_gpu_mg(cosa_ctx *c, int32_t mgit0, int32_t ncycles, int32_t ncycle, int32_t rms_every, double *hist) {
   if (!c || ncycles < 0 || rms_every < 1 || mgit0 < 1) return COSA_ERR_ARG;
   const int nlevel = c->p.nlevel;
@@ -2070,6 +2246,8 @@ int cosa_gpu_mg(cosa_ctx *c, int32_t mgit0, int32_t ncycles, int32_t ncycle, int
   int r = check_fused_supported(c->p);
   if (r) return r;
   if ((r = check_mg_levels(c, nlevel))) return r;
+  // dual time: the fine level's rhs holds rhs_uns, the BDF term needs vol
+  if (c->p.dualt && (!level(c, 1)->ptrs.rhs || !level(c, 1)->ptrs.vol)) return COSA_ERR_ARG;
   for (int nl = 1; nl <= nlevel; ++nl)
     if ((r = check_thin_blocks(c, nl))) return r;
   cudaSetDevice(c->device);
@@ -2082,8 +2260,8 @@ int cosa_gpu_mg(cosa_ctx *c, int32_t mgit0, int32_t ncycles, int32_t ncycle, int
   if ((r = ensure_hist(c, std::max<int>(1, (int)rows.size())))) return r;
   for (int nl = 1; nl <= nlevel; ++nl) {
     LevelState &Lv = *level(c, nl);
-    if ((c->p.irsop > 0 || c->p.rkimp) && (r = ensure_irs_scratch(c, Lv))) return r;
-    if (c->p.rkimp && Lv.npart_cap < Lv.nb * 64) {  // per-block norm partials of the implicit HB norm
+    if ((c->p.irsop > 0 || c->p.rkimp || c->p.dualt) && (r = ensure_irs_scratch(c, Lv))) return r;
+    if ((c->p.rkimp || c->p.dualt) && Lv.npart_cap < Lv.nb * 64) {  // per-block norm partials (implicit HB, dual time)
       drop_graphs(c);
       if ((r = dalloc(c, &Lv.d_part, (size_t)Lv.nb * 64 * 8))) return r;
       Lv.npart_cap = Lv.nb * 64;
@@ -2749,7 +2927,7 @@ int rans_face_state(cosa_ctx *c, LevelState &L, int d, const double *q, double *
 // (src/cosa.f90:1719-2016): every kernel is a full-array pass with the
 // reference's arrays, captured with the rest of the iteration in a graph
 int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpts &o) {
-  const bool compute_dt = o.compute_dt && irk == 1, want_rms = o.want_rms && irk == 1, copy_qold = o.copy_qold;
+  const bool compute_dt = o.compute_dt && irk == 1, want_rms = o.want_rms && irk == o.rms_stage, copy_qold = o.copy_qold;
   const cosa_params &p = c->p;
   const int S = 2 * p.nharms + 1, npde = p.npde;
   const cosa_level_ptrs &P = L.ptrs;
@@ -2839,19 +3017,21 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
     return r;
   }
   if ((r = cosa_gpu_prim2cons(c, nl, q))) return r;
-  if (want_rms) {
-    for (int b = 0; b < L.nb; ++b) {
-      k_rms_partial<<<64, 256, 0, c->s>>>(L.hb[b], c->d_p, P.res, nullptr, L.d_part + (int64_t)b * 64 * 8);
-      if ((r = after_launch(c))) return r;
-    }
-    int64_t ncell = 0;
-    for (auto &b : L.hb) ncell += (int64_t)(b.im - 1) * (b.jm - 1) * (b.km - 1);
-    k_rms_final<<<1, 256, 0, c->s>>>(L.d_part, L.nb * 64, npde, (double)ncell, c->d_hist, c->d_row, c->hist_cap);
-    if ((r = after_launch(c))) return r;
-  }
+  // dual time: src_uns, the norm with rhs_uns, res -= rhs_uns on the fine
+  // level (src/cosa.f90:1908-1941)
+  if (dual_src_in_res(p) &&
+      (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) { k_src_uns<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.vol, P.res); })))
+    return r;
+  if (want_rms && (r = launch_norm(c, L, P.res, p.dualt ? P.rhs : nullptr,
+                                   p.dualt && p.rkimp && !dual_src_in_res(p) ? q : nullptr)))
+    return r;
+  const int nvs = npde * S;
+  if (p.dualt && nl == 1 &&
+      (r = for_blocks(c, L, cnt_interior,
+                      [&](auto b, dim3 g) { k_add_interior<<<g, 256, 0, c->s>>>(b, nvs, P.res, P.rhs, -1.0); })))
+    return r;
   // multigrid forcing: rhs += res at the first stage of a visit from the
   // finer level, then res -= rhs on coarse levels (src/cosa.f90:1950-1960)
-  const int nvs = npde * S;
   if (o.rhs && o.force && irk == 1 &&
       (r = for_blocks(c, L, cnt_interior,
                       [&](auto b, dim3 g) { k_add_interior<<<g, 256, 0, c->s>>>(b, nvs, o.rhs, P.res, 1.0); })))
@@ -2878,10 +3058,25 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
     const double *tbeta[3] = {L.d_tbeta[0], L.d_tbeta[1], L.d_tbeta[2]};
     if ((r = irs_apply(c, L, P.res, L.d_ores, P.dtvol, beta, P.dtvolt, tbeta))) return r;
   }
-  if ((r = cosa_gpu_update_kom(c, nl, P.res, q, P.qold, P.vol, P.dtvolt, L.d_delpls, L.d_prd, p.alphas[irk - 1],
-                               blend(p) ? L.d_ttrm : nullptr)))
-    return r;
-  if ((r = cosa_gpu_update(c, nl, P.res, q, P.qold, P.dtvol, p.alphas[irk - 1]))) return r;
+  if (p.dualt && p.rkimp) {
+    // update_b with the physical-time term implicit (src/update.f90:650-738)
+    const int sir = dual_src_in_res(p) ? 1 : 0;
+    const double ar = p.alphas[irk - 1];
+    const double *tt = blend(p) ? L.d_ttrm : nullptr;
+    if ((r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+           k_update_kom_dual<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, q, P.qold, P.vol, P.dtvolt, L.d_delpls, L.d_prd, ar,
+                                                  tt, sir);
+         })) ||
+        (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+           k_update_dual<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, P.qold, q, q, nullptr, P.dtvol, P.vol, ar, sir);
+         })))
+      return r;
+  } else {
+    if ((r = cosa_gpu_update_kom(c, nl, P.res, q, P.qold, P.vol, P.dtvolt, L.d_delpls, L.d_prd, p.alphas[irk - 1],
+                                 blend(p) ? L.d_ttrm : nullptr)))
+      return r;
+    if ((r = cosa_gpu_update(c, nl, P.res, q, P.qold, P.dtvol, p.alphas[irk - 1]))) return r;
+  }
   if (p.ifixq && (r = cosa_gpu_fixq(c, nl, q))) return r;
   if (irk == p.nstage && (nl == 1 || !p.prd_all_lvls)) {
     // SST: the stage's cell-centred differences are still in qp, qm, dqm

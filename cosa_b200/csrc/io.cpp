@@ -212,6 +212,7 @@ int cosa_io_default_params(cosa_params *p) {
   p->precision = COSA_PREC_FP64;
   p->nstart = p->npre = p->npost = p->ncrs = 1;
   p->bln_prol = 1;
+  p->bdf1 = 1;
   return COSA_OK;
 }
 
@@ -630,6 +631,10 @@ int cosa_io_read_input(const char *path, cosa_params *pp, cosa_run_opts *rr, cos
     p.cfl = vcfl3;
     if (turb) p.cflt = vcflt3;
   }
+  if (p.dualt || p.rgkuns) p.dt = r.dt;
+  // first-order first step unless a dual-time restart holds two states
+  // (zeit.dat key 9992999, src/input.f90:5614-5620), which the caller knows
+  p.bdf1 = 1;
   *pp = p;
   *rr = r;
   *out = in;

@@ -423,6 +423,16 @@ __global__ void k_lim_res_ome(BS bs_, const cosa_params *__restrict__ Pp, double
     const double dt = dtt[p1_idx(b, S, i, j, k, n)];
     const double dtau = dt * vol[p1_idx(b, 1, i, j, k, 0)];
     const double rho = q[i1], ome = q[i7] / q[i1];
+    if (P.rkimp && P.dualt) {
+      // rkimp (src/update.f90:2781-2806): the physical-time term in the
+      // denominator; the reference's den1 has no ar here
+      const double den1 = 1 + dtau * (gav * delpls[o] + 2 * bav * ome);
+      const double den2 = ar * (P.bdf1 ? 1.0 : 1.5) * dtau / P.dt;
+      const double rhomega = q[i7] - ar * res[i7] * dt / (den1 + den2);
+      const double rhomegamin = gav * P.cmu * rho * sqrt(prd[o]);
+      if (rhomega < rhomegamin) res[i7] = ((den1 + den2) * (q[i7] - rhomegamin)) / dt / ar;
+      continue;
+    }
     const double den1 = 1 + ar * dtau * (gav * delpls[o] + 2 * bav * ome);
     const double rhomega = q[i7] - ar * res[i7] * dt / den1;
     const double rhomegamin = gav * P.cmu * rho * sqrt(prd[o]);

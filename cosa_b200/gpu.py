@@ -64,7 +64,8 @@ SYMBOLS = [
     "cosa_gpu_q_der_c", "cosa_gpu_turprod", "cosa_gpu_srckw", "cosa_gpu_update_kom", "cosa_gpu_cutman_mut",
     "cosa_gpu_autotune", "cosa_gpu_set_schedule", "cosa_gpu_force", "cosa_gpu_rest2_ho", "cosa_gpu_bc_res",
     "cosa_gpu_movegrid", "cosa_gpu_face_vel", "cosa_gpu_vert2cell", "cosa_gpu_facedist", "cosa_gpu_update_ttrm",
-    "cosa_gpu_srckw_sst", "cosa_gpu_tur_vis_sst",
+    "cosa_gpu_srckw_sst", "cosa_gpu_tur_vis_sst", "cosa_gpu_src_uns", "cosa_gpu_rhs_uns", "cosa_gpu_rkuns",
+    "cosa_gpu_copy_interior",
 ]
 
 
@@ -428,6 +429,23 @@ class Context:
         self._check(load().cosa_gpu_update_kom(self.h, nl, _ptr(res.ptr), _ptr(q.ptr), _ptr(qold.ptr), _ptr(vol.ptr),
                                                _ptr(dtvolt.ptr), _ptr(delpls.ptr), _ptr(prd.ptr), C.c_double(ar),
                                                _ptr(ttrm.ptr if ttrm is not None else None)), "update_kom")
+
+    # ---- time-accurate runs -------------------------------------------------------
+    def src_uns(self, nl, q, vol, res):
+        self._check(load().cosa_gpu_src_uns(self.h, nl, _ptr(q.ptr), _ptr(vol.ptr), _ptr(res.ptr)), "src_uns")
+
+    def rhs_uns(self, nl, rhs, q1, q2, vol):
+        self._check(load().cosa_gpu_rhs_uns(self.h, nl, _ptr(rhs.ptr), _ptr(q1.ptr), _ptr(q2.ptr), _ptr(vol.ptr)),
+                    "rhs_uns")
+
+    def copy_interior(self, nl, dst, src):
+        self._check(load().cosa_gpu_copy_interior(self.h, nl, _ptr(dst.ptr), _ptr(src.ptr)), "copy_interior")
+
+    def rkuns(self, ntime, iprint=1):
+        """rkuns on level 1: (hist (ntime, npde+1), status)."""
+        hist = np.full((max(ntime, 1), self.params.npde + 1), np.nan)
+        st = load().cosa_gpu_rkuns(self.h, ntime, iprint, hist.ctypes.data_as(C.c_void_p))
+        return hist[:ntime], st
 
     def facedist(self, nl, dist, fidist, fjdist, fkdist):
         self._check(load().cosa_gpu_facedist(self.h, nl, _ptr(dist.ptr), _ptr(fidist.ptr), _ptr(fjdist.ptr),

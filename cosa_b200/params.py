@@ -65,6 +65,7 @@ class CosaParams(C.Structure):
         ("ifixq", C.c_int32), ("wallwilc", C.c_int32), ("ho_rest", C.c_int32),
         ("turcmp", C.c_double), ("prdlim", C.c_double), ("roughk", C.c_double),
         ("dtheta0", C.c_double), ("omegas", C.c_double), ("xh", C.c_double), ("yh", C.c_double),
+        ("dt", C.c_double), ("bdf1", C.c_int32), ("reserved_t", C.c_int32),
     ]
 
 
@@ -122,6 +123,8 @@ def default_params() -> CosaParams:
     p.nstart = p.npre = p.npost = p.ncrs = 1
     p.bln_prol = 1
     p.lim_corr = 0
+    # time-accurate runs start with a first-order step (src/src.f90:420-432)
+    p.bdf1 = 1
     return p
 
 

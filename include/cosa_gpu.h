@@ -115,6 +115,13 @@ typedef struct cosa_params {
      radians, omegas = 2 pi x the input frequency (src/input.f90:2960-2980,
      src/grid.f90:4540) */
   double dtheta0, omegas, xh, yh;
+  /* time-accurate runs: the physical time step dt of dual time stepping
+     (dualt, BDF2 with src_uns / rhs_uns, src/src.f90:381-527) and of the
+     explicit RK integration (rgkuns, src/cosa.f90:3890-4180); bdf1 = 1 on
+     the first physical step of a run not started from a dual-time restart
+     (itime = 1 and not dual_prop_start: first-order backward difference) */
+  double dt;
+  int32_t bdf1, reserved_t;
 } cosa_params;
 
 /*
@@ -366,6 +373,26 @@ int cosa_gpu_lambda_ns(cosa_ctx *ctx, int32_t nl, const double *q, const double 
 int cosa_gpu_deltat_ns(cosa_ctx *ctx, int32_t nl, double *dtvol, const double *lam,
                        const double *lamv, double *bx, double *by, double *bz,
                        double *dtvolt, double *tbx, double *tby, double *tbz);
+
+/* ---- time-accurate runs (one snapshot; params.dt, params.bdf1) ---- */
+/* src_uns (src/src.f90:381-451): res += 3/2 q V / dt, or q V / dt with bdf1;
+   the dual-time stages of cosa_gpu_smooth / cosa_gpu_mg add it themselves
+   (and subtract the fine level's rhs, rhs_uns, src/cosa.f90:1908-1941) */
+int cosa_gpu_src_uns(cosa_ctx *ctx, int32_t nl, const double *q, const double *vol, double *res);
+/* rhs_uns (src/src.f90:453-527): rhs = (2 q1 - q2 / 2) V / dt, or q1 V / dt
+   with bdf1; q1 = q^n, q2 = q^(n-1).  One physical step of dual time is
+   q1 <- q, cosa_gpu_rhs_uns into the fine level's rhs, cosa_gpu_mg for the
+   pseudo-time cycles, q2 <- q1 (src/cosa.f90:548-667). */
+int cosa_gpu_rhs_uns(cosa_ctx *ctx, int32_t nl, double *rhs, const double *q1, const double *q2, const double *vol);
+/* copy_array over the interior cells of every variable and snapshot
+   (offset -1, src/util.f90:2-135): dst = src, e.g. q1 <- q */
+int cosa_gpu_copy_interior(cosa_ctx *ctx, int32_t nl, double *dst, const double *src);
+/* rkuns (src/cosa.f90:3890-4180) on level 1 of a fixed grid: ntime physical
+   steps of the nstage-stage RK scheme with dtvol = dt / V (deltat_urk);
+   hist receives (npde+1) values per step, the norm of the last stage's
+   residual on steps with itime % iprint == 0 and the last (NaN elsewhere).
+   Euler and laminar without IRS (COSA_ERR_UNSUPPORTED otherwise). */
+int cosa_gpu_rkuns(cosa_ctx *ctx, int32_t ntime, int32_t iprint, double *hist);
 
 /* ---- k-omega: Wilcox (kom), BSL (kom_bsl), SST (kom_sst); npde = 7; mut,
    prd, divvel, delpls are scalar P3 arrays (-1:imax+1,...,0:S-1); ttrm

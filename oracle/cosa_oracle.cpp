@@ -1478,18 +1478,140 @@ void update_bhb_b(const Level &L, int b, const double *ra, double *qa, const dou
       }
 }
 
-// ---- resg_brms (src/cosa.f90:4503-4582), explicit steady branch ------------
-void resg_rms_level(const Level &L, double *ra, double *rha, double *out) {
+// ---- dual time stepping (src/src.f90:381-527; src/update.f90:568-740;
+// src/cosa.f90:4503-4560) ---------------------------------------------------------
+// src_uns_b: res += 3/2 q V / dt (BDF2), q V / dt on a first-order first step
+void src_uns_level(const Level &L, const double *qa, const double *va, double *ra, const cosa_params &P) {
+  for (int b = 0; b < L.nb; ++b) {
+    B3 q(const_cast<double *>(qa), L, b), res(ra, L, b);
+    B1 vol(const_cast<double *>(va), L, b, 1);
+    for (int v = 1; v <= L.npde; ++v)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            if (P.bdf1) res(i, j, k, v, 0) = res(i, j, k, v, 0) + q(i, j, k, v, 0) * vol(i, j, k) / P.dt;
+            else res(i, j, k, v, 0) = res(i, j, k, v, 0) + 3 * q(i, j, k, v, 0) * vol(i, j, k) / 2 / P.dt;
+          }
+  }
+}
+// rhs_uns_b: rhs = q1 V / dt, or (2 q1 - q2 / 2) V / dt (q1 = q^n, q2 = q^(n-1))
+void rhs_uns_level(const Level &L, double *rha, const double *q1a, const double *q2a, const double *va,
+                   const cosa_params &P) {
+  for (int b = 0; b < L.nb; ++b) {
+    B3 rhs(rha, L, b), q1(const_cast<double *>(q1a), L, b), q2(const_cast<double *>(q2a), L, b);
+    B1 vol(const_cast<double *>(va), L, b, 1);
+    for (int v = 1; v <= L.npde; ++v)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            if (P.bdf1) rhs(i, j, k, v, 0) = q1(i, j, k, v, 0) * vol(i, j, k) / P.dt;
+            else rhs(i, j, k, v, 0) = (2 * q1(i, j, k, v, 0) - q2(i, j, k, v, 0) / 2) * vol(i, j, k) / P.dt;
+          }
+  }
+}
+// resg_brms with rkimp, no IRS, one level: the physical-time term fact q V /
+// dt added back to res - rhs
+void resg_rms_dualimp_level(const Level &L, const double *ra, const double *rha, const double *qa, const double *va,
+                            const cosa_params &P, double *out) {
+  const double fact = P.bdf1 ? 1.0 : 1.5;
   double acc[10] = {0};
   int64_t ncell = 0;
   for (int b = 0; b < L.nb; ++b) {
-    B3 res(ra, L, b), rhs(rha, L, b);
+    B3 res(const_cast<double *>(ra), L, b), rhs(const_cast<double *>(rha), L, b), q(const_cast<double *>(qa), L, b);
+    B1 vol(const_cast<double *>(va), L, b, 1);
     double rb[10] = {0};
     for (int v = 1; v <= L.npde; ++v)
       for (int k = 1; k <= L.km[b] - 1; ++k)
         for (int j = 1; j <= L.jm[b] - 1; ++j)
           for (int i = 1; i <= L.im[b] - 1; ++i) {
-            double t = res(i, j, k, v, 0) - rhs(i, j, k, v, 0);
+            const double t = fact * q(i, j, k, v, 0) * vol(i, j, k) / P.dt + res(i, j, k, v, 0) - rhs(i, j, k, v, 0);
+            rb[v] = rb[v] + t * t;
+          }
+    for (int v = 1; v <= L.npde; ++v) rb[L.npde + 1] = rb[L.npde + 1] + rb[v];
+    for (int v = 1; v <= L.npde + 1; ++v) acc[v] = acc[v] + rb[v];
+    ncell += (int64_t)(L.im[b] - 1) * (L.jm[b] - 1) * (L.km[b] - 1);
+  }
+  for (int v = 1; v <= L.npde; ++v) out[v - 1] = std::sqrt(acc[v] / ncell);
+  out[L.npde] = std::sqrt(acc[L.npde + 1] / ncell / L.npde);
+}
+// update_b with rkimp (src/update.f90:650-738): the physical-time term
+// implicit.  Without IRS on one level the residual holds no physical-time
+// term; with IRS or multigrid src_uns added it and it is taken out again.
+void update_dual_b(const Level &L, int b, const double *ra, double *qa, const double *qoa, const double *dta,
+                   const double *va, double ar, const cosa_params &P, bool src_in_res) {
+  B3 res(const_cast<double *>(ra), L, b), q(qa, L, b), qold(const_cast<double *>(qoa), L, b);
+  B1 dtv(const_cast<double *>(dta), L, b, 1), vol(const_cast<double *>(va), L, b, 1);
+  const double fact = P.bdf1 ? 1.0 : 1.5;
+  for (int v = 1; v <= 5; ++v)
+    for (int k = 1; k <= L.km[b] - 1; ++k)
+      for (int j = 1; j <= L.jm[b] - 1; ++j)
+        for (int i = 1; i <= L.im[b] - 1; ++i) {
+          const double den = 1 + fact * ar * dtv(i, j, k) * vol(i, j, k) / P.dt;
+          if (src_in_res)
+            q(i, j, k, v, 0) = (qold(i, j, k, v, 0) -
+                                ar * dtv(i, j, k) * (-fact * vol(i, j, k) / P.dt * q(i, j, k, v, 0) + res(i, j, k, v, 0))) /
+                               den;
+          else
+            q(i, j, k, v, 0) = (qold(i, j, k, v, 0) - ar * res(i, j, k, v, 0) * dtv(i, j, k)) / den;
+        }
+}
+// the k-omega part of update_b with rkimp (src/update.f90:655-732)
+void update_kom_dual_b(const Level &L, int b, const double *ra, double *qa, const double *qoa, const double *va,
+                       const double *dtta, const double *dpla, const double *prda, double ar, const cosa_params &P,
+                       const double *ttrma, bool src_in_res) {
+  B3 res(const_cast<double *>(ra), L, b), q(qa, L, b), qold(const_cast<double *>(qoa), L, b);
+  B1 vol(const_cast<double *>(va), L, b, 1), dtt(const_cast<double *>(dtta), L, b, 1);
+  B3s dpl(const_cast<double *>(dpla), L, b), prd(const_cast<double *>(prda), L, b);
+  const double fact = P.bdf1 ? 1.0 : 1.5;
+  for (int k = 1; k <= L.km[b] - 1; ++k)
+    for (int j = 1; j <= L.jm[b] - 1; ++j)
+      for (int i = 1; i <= L.im[b] - 1; ++i) {
+        const double gav = ttrma ? B3t(const_cast<double *>(ttrma), L, b)(i, j, k, 2, 0) : P.gkw;
+        const double bav = ttrma ? B3t(const_cast<double *>(ttrma), L, b)(i, j, k, 3, 0) : P.bkw;
+        const double rho = q(i, j, k, 1, 0);
+        const double ome = q(i, j, k, 7, 0) / q(i, j, k, 1, 0);
+        const double dtau = dtt(i, j, k) * vol(i, j, k);
+        const double dp = dpl(i, j, k, 0);
+        double rhomega;
+        if (src_in_res)
+          rhomega = (qold(i, j, k, 7, 0) + ar * fact * dtau / P.dt * q(i, j, k, 7, 0) -
+                     ar * res(i, j, k, 7, 0) * dtt(i, j, k) + ar * dtau * q(i, j, k, 7, 0) * (gav * dp + 2 * bav * ome)) /
+                    (1 + ar * dtau * (gav * dp + 2 * bav * ome) + ar * fact * dtau / P.dt);
+        else
+          rhomega = (qold(i, j, k, 7, 0) - ar * res(i, j, k, 7, 0) * dtt(i, j, k) +
+                     ar * dtau * q(i, j, k, 7, 0) * (gav * dp + 2 * bav * ome)) /
+                    (1 + ar * dtau * (gav * dp + 2 * bav * ome) + fact * ar * dtau / P.dt);
+        const double rhomegamin = gav * P.cmu * rho * std::sqrt(prd(i, j, k, 0));
+        if (rhomega < rhomegamin) rhomega = rhomegamin;
+        q(i, j, k, 7, 0) = rhomega;
+        const double drhomega = q(i, j, k, 7, 0) - rho * ome;
+        if (src_in_res)
+          q(i, j, k, 6, 0) = (qold(i, j, k, 6, 0) + ar * fact * dtau / P.dt * q(i, j, k, 6, 0) -
+                              ar * res(i, j, k, 6, 0) * dtt(i, j, k) +
+                              ar * dtau * q(i, j, k, 6, 0) * (dp + P.bstrkw * ome - P.bstrkw * drhomega / rho)) /
+                             (1 + ar * dtau * (dp + P.bstrkw * ome) + ar * fact * dtau / P.dt);
+        else
+          q(i, j, k, 6, 0) = (qold(i, j, k, 6, 0) - ar * res(i, j, k, 6, 0) * dtt(i, j, k) +
+                              ar * dtau * q(i, j, k, 6, 0) * (dp + P.bstrkw * ome - P.bstrkw * drhomega / rho)) /
+                             (1 + ar * dtau * (dp + P.bstrkw * ome) + ar * fact * dtau / P.dt);
+      }
+}
+// src_uns enters the residual unless rkimp without IRS on one level
+inline bool dual_src_in_res(const cosa_params &P) { return P.dualt && (!P.rkimp || P.irsop > 0 || P.nlevel > 1); }
+
+// ---- resg_brms (src/cosa.f90:4503-4582), explicit steady branch ------------
+void resg_rms_level(const Level &L, double *ra, double *rha, double *out) {
+  double acc[10] = {0};
+  int64_t ncell = 0;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 res(ra, L, b), rhs(rha ? rha : ra, L, b);
+    double rb[10] = {0};
+    for (int v = 1; v <= L.npde; ++v)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            // rkuns has no rhs (src/cosa.f90:4562-4571)
+            double t = rha ? res(i, j, k, v, 0) - rhs(i, j, k, v, 0) : res(i, j, k, v, 0);
             rb[v] = rb[v] + t * t;
           }
     for (int v = 1; v <= L.npde; ++v) rb[L.npde + 1] = rb[L.npde + 1] + rb[v];
@@ -1875,6 +1997,18 @@ void lim_res_ome_b(const Level &L, int b, double *ra, const double *qa, const do
           const double bav = ttrma ? B3t(const_cast<double *>(ttrma), L, b)(i, j, k, 3, n) : P.bkw;
           const double dtau = dtt(i, j, k, n) * vol(i, j, k);
           const double rho = q(i, j, k, 1, n), ome = q(i, j, k, 7, n) / q(i, j, k, 1, n);
+          if (P.rkimp && P.dualt) {
+            // rkimp (src/update.f90:2781-2806): the physical-time term in the
+            // denominator; the reference's den1 has no ar here
+            const double fact = P.bdf1 ? 1.0 : 1.5;
+            const double den1 = 1 + dtau * (gav * dpl(i, j, k, n) + 2 * bav * ome);
+            const double den2 = ar * fact * dtau / P.dt;
+            const double rhomega = q(i, j, k, 7, n) - ar * res(i, j, k, 7, n) * dtt(i, j, k, n) / (den1 + den2);
+            const double rhomegamin = gav * P.cmu * rho * std::sqrt(prd(i, j, k, n));
+            if (rhomega < rhomegamin)
+              res(i, j, k, 7, n) = ((den1 + den2) * (q(i, j, k, 7, n) - rhomegamin)) / dtt(i, j, k, n) / ar;
+            continue;
+          }
           const double den1 = 1 + ar * dtau * (gav * dpl(i, j, k, n) + 2 * bav * ome);
           const double rhomega = q(i, j, k, 7, n) - ar * res(i, j, k, 7, n) * dtt(i, j, k, n) / den1;
           const double rhomegamin = gav * P.cmu * rho * std::sqrt(prd(i, j, k, n));
@@ -3707,7 +3841,12 @@ int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_p
   }
 #pragma omp parallel for schedule(dynamic)
   for (int b = 0; b < L.nb; ++b) prim2cons_b(L, b, q, *p);
-  if (p->harbal && A.vol) src_hb_level(L, q, A.vol, A.res, *p);
+  if (dual_src_in_res(*p)) {
+    if (!A.vol) return COSA_ERR_ARG;
+    src_uns_level(L, q, A.vol, A.res, *p);
+  } else if (p->harbal && A.vol) {
+    src_hb_level(L, q, A.vol, A.res, *p);
+  }
   return status;
 }
 
@@ -3726,6 +3865,7 @@ int orc_smooth(orc_level *h, const cosa_params *p, int ncycles, int mgit0, int r
                double *qold, const double *si, const double *sj, const double *sk, double *res,
                double *rhs, double *qp, double *qm, double *dq, double *dqp, double *dqm, double *flux,
                double *dtvol, double *hist) {
+  if (p->dualt || p->rgkuns) return COSA_ERR_UNSUPPORTED;  // dual time: orc_mg / orc_mg_rans; rkuns: orc_rkuns
   if (p->irsop > 0) return -1;
   Level &L = h->L;
   int status = 0;
@@ -3750,6 +3890,7 @@ int orc_smooth_irs(orc_level *h, const cosa_params *p, int ncycles, int mgit0, i
                    double *qold, const double *si, const double *sj, const double *sk, double *res,
                    double *rhs, double *qp, double *qm, double *dq, double *dqp, double *dqm, double *flux,
                    double *dtvol, double *bx, double *by, double *bz, double *hist) {
+  if (p->dualt || p->rgkuns) return COSA_ERR_UNSUPPORTED;  // dual time: orc_mg / orc_mg_rans; rkuns: orc_rkuns
   Level &L = h->L;
   int status = 0;
   const int last = mgit0 + ncycles - 1;
@@ -3773,6 +3914,7 @@ int orc_smooth_hb(orc_level *h, const cosa_params *p, int ncycles, int mgit0, in
                   double *qold, const double *si, const double *sj, const double *sk, const double *vol,
                   double *res, double *qp, double *qm, double *dq, double *dqp, double *dqm, double *flux,
                   double *dtvol, double *hist) {
+  if (p->dualt || p->rgkuns) return COSA_ERR_UNSUPPORTED;  // dual time: orc_mg / orc_mg_rans; rkuns: orc_rkuns
   Level &L = h->L;
   int status = 0;
   const int last = mgit0 + ncycles - 1;
@@ -3811,6 +3953,51 @@ int orc_smooth_hb(orc_level *h, const cosa_params *p, int ncycles, int mgit0, in
 }
 
 void orc_lu_solve(int n, double *a, double *b, int nrhs) { lu_solve(n, a, b, nrhs); }
+
+void orc_src_uns(orc_level *h, const cosa_params *p, const double *q, const double *vol, double *res) {
+  src_uns_level(h->L, q, vol, res, *p);
+}
+void orc_rhs_uns(orc_level *h, const cosa_params *p, double *rhs, const double *q1, const double *q2,
+                 const double *vol) {
+  rhs_uns_level(h->L, rhs, q1, q2, vol, *p);
+}
+
+/*
+ * rkuns (src/cosa.f90:3890-4180) on a fixed grid: ntime physical steps of
+ * the nstage-stage RK scheme with the global time step dtvol = dt / V of
+ * deltat_urk (src/cosa.f90:2525-2572); on printed steps (itime % iprint == 0
+ * or the last) hist row itime - 1 receives the norm of the last stage's
+ * residual, as the reference overwrites resrms at every stage.  Euler and
+ * laminar: the k-omega variant of the reference advances k and omega with
+ * dtvolt, which rkuns never sets.
+ */
+int orc_rkuns(orc_level *h, const cosa_params *p, const cosa_level_ptrs *Ap, const double *vm, int ntime, int iprint,
+              double *hist) {
+  Level &L = h->L;
+  const cosa_level_ptrs &A = *Ap;
+  if (!p->rgkuns || is_kom(*p) || p->harbal || p->dualt) return COSA_ERR_UNSUPPORTED;
+  if (!A.vol || !A.dtvol || (p->viscous && !vm) || iprint < 1) return COSA_ERR_ARG;
+  for (int b = 0; b < L.nb; ++b) {
+    B1 dtv(A.dtvol, L, b, 1), vol(A.vol, L, b, 1);
+    for (int k = 1; k <= L.km[b] - 1; ++k)
+      for (int j = 1; j <= L.jm[b] - 1; ++j)
+        for (int i = 1; i <= L.im[b] - 1; ++i) dtv(i, j, k) = p->dt / vol(i, j, k);
+  }
+  int status = 0;
+  for (int itime = 1; itime <= ntime; ++itime) {
+    copy_interior(L, A.qold, A.q);
+    const bool printed = itime % iprint == 0 || itime == ntime;
+    for (int irk = 1; irk <= p->nstage; ++irk) {
+      status |= residual_impl(h, p, 1, A.q, A.si, A.sj, A.sk, A.res, A.qp, A.qm, A.dq, A.dqp, A.dqm, A.flux, A.dtvol,
+                              0, nullptr, nullptr, nullptr, A.vol, vm);
+      if (status & (COSA_ERR_ARG | COSA_ERR_UNSUPPORTED)) return status;
+      if (printed && hist) resg_rms_level(L, A.res, nullptr, hist + (int64_t)(itime - 1) * (L.npde + 1));
+#pragma omp parallel for schedule(dynamic)
+      for (int b = 0; b < L.nb; ++b) update_b(L, b, A.res, A.q, A.qold, A.dtvol, p->alphas[irk - 1]);
+    }
+  }
+  return status;
+}
 
 void orc_src_hb(orc_level *h, const cosa_params *p, const double *q, const double *vol, double *res) {
   src_hb_level(h->L, q, vol, res, *p);
@@ -3900,16 +4087,21 @@ int orc_smooth_level(orc_level *h, const cosa_params *p, int nl, const cosa_leve
   const bool imp = p->harbal && p->rkimp;
   const bool src_in_res = p->harbal && (!p->rkimp || p->irsop > 0 || p->nlevel > 1);
   if (imp && L.npde != 5) return COSA_ERR_UNSUPPORTED;
+  // dual time: src_uns in the residual (unless rkimp without IRS on one
+  // level), res -= rhs_uns on the fine level (src/cosa.f90:1910-1941)
+  const bool dual_imp = p->dualt && p->rkimp;
   for (int iter = 1; iter <= niterp; ++iter) {
     if (iter <= niter) copy_interior(L, P->qold, P->q);
     for (int irk = 1; irk <= p->nstage; ++irk) {
       const bool want_dt = (iter / p->iupdt * p->iupdt == iter) && irk == 1;
       status |= residual_impl(h, p, nl, P->q, P->si, P->sj, P->sk, P->res, P->qp, P->qm, P->dq, P->dqp, P->dqm,
                               P->flux, P->dtvol, want_dt, P->betaxi, P->betaeta, P->betazeta,
-                              src_in_res ? P->vol : nullptr);
+                              src_in_res || dual_src_in_res(*p) ? P->vol : nullptr);
       if (nl == 1 && irk == 1 && iter != niter + 1 && hist_row &&
           (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle)) {
-        if (imp && !src_in_res) {
+        if (dual_imp && !dual_src_in_res(*p)) {
+          resg_rms_dualimp_level(L, P->res, P->rhs, P->q, P->vol, *p, hist_row);
+        } else if (imp && !src_in_res) {
           resg_rms_hbimp_level(L, P->res, P->q, P->vol, *p, hist_row);
         } else if (p->harbal) {
           work.assign(P->res, P->res + L.n3 * L.npde * L.S);
@@ -3918,6 +4110,7 @@ int orc_smooth_level(orc_level *h, const cosa_params *p, int nl, const cosa_leve
           resg_rms_level(L, P->res, P->rhs, hist_row);
         }
       }
+      if (nl == 1 && p->dualt) add_level(L, P->res, P->rhs, -1.0, -1);
       if (from_fine && iter == 1 && irk == 1) add_level(L, P->rhs, P->res, 1.0, -1);
       if (nl > 1) add_level(L, P->res, P->rhs, -1.0, -1);
       if (iter == niter + 1) return status;
@@ -3926,6 +4119,8 @@ int orc_smooth_level(orc_level *h, const cosa_params *p, int nl, const cosa_leve
 #pragma omp parallel for schedule(dynamic)
       for (int b = 0; b < L.nb; ++b) {
         if (imp) update_bhb_b(L, b, P->res, P->q, P->qold, P->dtvol, P->vol, p->alphas[irk - 1], *p, src_in_res);
+        else if (dual_imp) update_dual_b(L, b, P->res, P->q, P->qold, P->dtvol, P->vol, p->alphas[irk - 1], *p,
+                                         dual_src_in_res(*p));
         else update_b(L, b, P->res, P->q, P->qold, P->dtvol, p->alphas[irk - 1]);
       }
     }
@@ -4013,6 +4208,7 @@ int orc_smooth_ns(orc_level *h, const cosa_params *p, int ncycles, int mgit0, in
                   double *qold, const double *si, const double *sj, const double *sk, const double *vol,
                   const double *vm, double *res, double *rhs, double *qp, double *qm, double *dq, double *dqp,
                   double *dqm, double *flux, double *dtvol, double *bx, double *by, double *bz, double *hist) {
+  if (p->dualt || p->rgkuns) return COSA_ERR_UNSUPPORTED;  // dual time: orc_mg / orc_mg_rans; rkuns: orc_rkuns
   Level &L = h->L;
   int status = 0;
   const int last = mgit0 + ncycles - 1;
@@ -4048,6 +4244,7 @@ int orc_smooth_ns(orc_level *h, const cosa_params *p, int ncycles, int mgit0, in
 int orc_smooth_rans(orc_level *h, const cosa_params *p, int ncycles, int mgit0, int rms_every,
                     const cosa_level_ptrs *Ap, const double *vm, double *prd, double *divvel, double *delpls,
                     double *tbx, double *tby, double *tbz, double *ttrm, const double *fdist, double *hist) {
+  if (p->dualt || p->rgkuns) return COSA_ERR_UNSUPPORTED;  // dual time: orc_mg / orc_mg_rans; rkuns: orc_rkuns
   Level &L = h->L;
   const cosa_level_ptrs &A = *Ap;
   VExtra X{vm, prd, divvel, delpls, tbx, tby, tbz, ttrm, fdist};
@@ -4191,8 +4388,11 @@ int orc_smooth_level_rans(orc_level *h, const cosa_params *p, int nl, int nlevel
       status |= residual_full(h, p, nl, A, X, want_dt, mut_first);
       if (status & (COSA_ERR_ARG | COSA_ERR_UNSUPPORTED)) return status;
       if (nl == 1 && irk == 1 && iter != niter + 1 && hist_row &&
-          (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle))
-        resg_rms_level(L, A.res, A.rhs, hist_row);
+          (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle)) {
+        if (p->dualt && p->rkimp && !dual_src_in_res(*p)) resg_rms_dualimp_level(L, A.res, A.rhs, A.q, A.vol, *p, hist_row);
+        else resg_rms_level(L, A.res, A.rhs, hist_row);
+      }
+      if (nl == 1 && p->dualt) add_level(L, A.res, A.rhs, -1.0, -1);
       if (from_fine && iter == 1 && irk == 1) add_level(L, A.rhs, A.res, 1.0, -1);
       if (nl > 1) add_level(L, A.res, A.rhs, -1.0, -1);
       if (iter == niter + 1) {
@@ -4207,9 +4407,15 @@ int orc_smooth_level_rans(orc_level *h, const cosa_params *p, int nl, int nlevel
         irs_level(L, A.res, A.dtvol, A.dtvolt, A.betaxi, A.betaeta, A.betazeta, X.tbx, X.tby, X.tbz, *p);
 #pragma omp parallel for schedule(dynamic)
       for (int b = 0; b < L.nb; ++b) {
-        update_kom_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p,
-                     is_blend(*p) ? X.ttrm : nullptr);
-        update_b(L, b, A.res, A.q, A.qold, A.dtvol, p->alphas[irk - 1]);
+        if (p->dualt && p->rkimp) {
+          update_kom_dual_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p,
+                            is_blend(*p) ? X.ttrm : nullptr, dual_src_in_res(*p));
+          update_dual_b(L, b, A.res, A.q, A.qold, A.dtvol, A.vol, p->alphas[irk - 1], *p, dual_src_in_res(*p));
+        } else {
+          update_kom_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p,
+                       is_blend(*p) ? X.ttrm : nullptr);
+          update_b(L, b, A.res, A.q, A.qold, A.dtvol, p->alphas[irk - 1]);
+        }
       }
       if (p->ifixq) fixq_level(L, A.q, *p);
       if (irk == p->nstage && (nl == 1 || !p->prd_all_lvls)) {

@@ -243,6 +243,26 @@ def smooth_hb(O, q, si, sj, sk, vol, ncycles, mgit0=1, rms_every=1):
     return hist, st
 
 
+def src_uns(O, q, vol, res):
+    lib().orc_src_uns(O.h, _par(O.p), _p(q), _p(vol), _p(res))
+
+
+def rhs_uns(O, rhs, q1, q2, vol):
+    lib().orc_rhs_uns(O.h, _par(O.p), _p(rhs), _p(q1), _p(q2), _p(vol))
+
+
+def rkuns(O, A, ntime, iprint=1, vm=None):
+    """rkuns on one level (LevelArrays with vol; vm for laminar): (hist, status)."""
+    hist = np.full((max(ntime, 1), O.p.npde + 1), np.nan)
+    pt = A.ptrs()
+    st = lib().orc_rkuns(O.h, _par(O.p), C.byref(pt), _opt(vm), C.c_int(ntime), C.c_int(iprint), _p(hist))
+    return hist[:ntime], st
+
+
+def copy_interior(O, dst, src):
+    lib().orc_copy_interior(O.h, _p(dst), _p(src))
+
+
 def src_hb(O, q, vol, res):
     lib().orc_src_hb(O.h, _par(O.p), _p(q), _p(vol), _p(res))
 
