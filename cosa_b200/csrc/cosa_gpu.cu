@@ -534,8 +534,8 @@ int set_smem_attrs() {
 // the k-omega stage runs routine by routine (launch_rans_iteration); Wilcox,
 // BSL and SST
 int check_rans_supported(const cosa_params &p) {
-  if (p.npde != 7 || !rans(p) || (p.kom + p.kom_bsl + p.kom_sst) != 1 || !p.viscous || (p.rkimp && !p.dualt) ||
-      p.moving || p.harbal || (p.dualt && p.dt <= 0) ||
+  if (p.npde != 7 || !rans(p) || (p.kom + p.kom_bsl + p.kom_sst) != 1 || !p.viscous ||
+      (p.rkimp && !p.dualt && !p.harbal) || p.moving || (p.dualt && (p.dt <= 0 || p.harbal)) ||
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
   return COSA_OK;
@@ -961,19 +961,24 @@ struct IterOpts {
 
 int launch_rans_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o);
 
-// residual norm partials of every block (64 CTAs each) and the final sum
+// residual norm partials of every block (64 CTAs each) and the final sum;
+// q_imp: the state whose implicit term is added back (dual time or harmonic
+// balance with rkimp, no IRS, one level); harmonic balance averages over
+// the snapshots
 int launch_norm(cosa_ctx *c, LevelState &L, const double *res, const double *rhs, const double *q_imp) {
   int r = 0;
   int64_t ncell = 0;
   for (int b = 0; b < L.nb; ++b) {
     const DevBlock &x = L.hb[b];
     double *part = L.d_part + (int64_t)b * 64 * 8;
-    if (q_imp) k_rms_dualimp<<<64, 256, 0, c->s>>>(x, c->d_p, res, rhs, q_imp, L.ptrs.vol, part);
+    if (q_imp && c->p.harbal) k_rms_bhb_partial<<<64, 256, 0, c->s>>>(x, c->d_p, res, q_imp, L.ptrs.vol, part);
+    else if (q_imp) k_rms_dualimp<<<64, 256, 0, c->s>>>(x, c->d_p, res, rhs, q_imp, L.ptrs.vol, part);
     else k_rms_partial<<<64, 256, 0, c->s>>>(x, c->d_p, res, rhs, part);
     if ((r = after_launch(c))) return r;
     ncell += (int64_t)(x.im - 1) * (x.jm - 1) * (x.km - 1);
   }
-  k_rms_final<<<1, 256, 0, c->s>>>(L.d_part, L.nb * 64, c->p.npde, (double)ncell, c->d_hist, c->d_row, c->hist_cap);
+  const double cnt = (double)ncell * (c->p.harbal ? 2 * c->p.nharms + 1 : 1);
+  k_rms_final<<<1, 256, 0, c->s>>>(L.d_part, L.nb * 64, c->p.npde, cnt, c->d_hist, c->d_row, c->hist_cap);
   return after_launch(c);
 }
 
@@ -3022,9 +3027,14 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
   if (dual_src_in_res(p) &&
       (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) { k_src_uns<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.vol, P.res); })))
     return r;
-  if (want_rms && (r = launch_norm(c, L, P.res, p.dualt ? P.rhs : nullptr,
-                                   p.dualt && p.rkimp && !dual_src_in_res(p) ? q : nullptr)))
+  // harmonic balance: src_hb unless rkimp without IRS on one level
+  // (src/cosa.f90:1918-1922)
+  const bool hb_sir = p.harbal && (!p.rkimp || p.irsop > 0 || p.nlevel > 1);
+  if (hb_sir &&
+      (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) { k_src_hb<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.vol, P.res); })))
     return r;
+  const bool imp_norm = p.rkimp && ((p.dualt && !dual_src_in_res(p)) || (p.harbal && !hb_sir));
+  if (want_rms && (r = launch_norm(c, L, P.res, p.dualt ? P.rhs : nullptr, imp_norm ? q : nullptr))) return r;
   const int nvs = npde * S;
   if (p.dualt && nl == 1 &&
       (r = for_blocks(c, L, cnt_interior,
@@ -3048,8 +3058,12 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
          })))
       return r;
     return for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
-      k_lim_res_ome<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, q, P.vol, P.dtvolt, L.d_delpls, L.d_prd, p.alphas[irk - 1],
-                                         blend(p) ? L.d_ttrm : nullptr);
+      if (p.harbal)
+        k_lim_res_ome_bhb<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, q, P.qold, P.vol, P.dtvolt, L.d_delpls, L.d_prd,
+                                               blend(p) ? L.d_ttrm : nullptr);
+      else
+        k_lim_res_ome<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, q, P.vol, P.dtvolt, L.d_delpls, L.d_prd,
+                                           p.alphas[irk - 1], blend(p) ? L.d_ttrm : nullptr);
     });
   }
   if (p.irsop > 0) {
@@ -3071,11 +3085,28 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
            k_update_dual<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, P.qold, q, q, nullptr, P.dtvol, P.vol, ar, sir);
          })))
       return r;
+  } else if (p.harbal && p.rkimp) {
+    // update_bhb: k-omega snapshots coupled per cell, then the mean flow
+    const int sir = hb_sir ? 1 : 0;
+    const double ar = p.alphas[irk - 1];
+    const double *tt = blend(p) ? L.d_ttrm : nullptr;
+    if ((r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+           k_update_bhb_kom<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, q, P.qold, P.vol, P.dtvolt, L.d_delpls, L.d_prd, ar,
+                                                 tt, sir);
+         })) ||
+        (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+           k_update_bhb<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, P.qold, q, nullptr, P.dtvol, P.vol, ar,
+                                             sir ? q : nullptr);
+         })))
+      return r;
   } else {
     if ((r = cosa_gpu_update_kom(c, nl, P.res, q, P.qold, P.vol, P.dtvolt, L.d_delpls, L.d_prd, p.alphas[irk - 1],
                                  blend(p) ? L.d_ttrm : nullptr)))
       return r;
-    if ((r = cosa_gpu_update(c, nl, P.res, q, P.qold, P.dtvol, p.alphas[irk - 1]))) return r;
+    const double ar = p.alphas[irk - 1];
+    if ((r = for_blocks(c, L, cnt_interior,
+                        [&](auto b, dim3 g) { k_update<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, q, P.qold, P.dtvol, ar); })))
+      return r;
   }
   if (p.ifixq && (r = cosa_gpu_fixq(c, nl, q))) return r;
   if (irk == p.nstage && (nl == 1 || !p.prd_all_lvls)) {

@@ -855,12 +855,13 @@ __device__ __forceinline__ void hb_lu_solve(int n, double *a, double *bm, int nr
 // residual holds no time-spectral term and rhs = qold - ar res dtvol.  qsrc
 // set (IRS or multigrid): the residual, smoothed, includes src_hb's
 // qhb = omega V D q of the stage state qsrc, and rhs = qold + (qhb - res) ar
-// dtvol with qhb recomputed from qsrc in src_bhb's order.
+// dtvol with qhb recomputed from qsrc in src_bhb's order.  qsrc may be qout
+// (the k-omega stage updates in place): a cell's values are all read first.
 template <class BS>
 __global__ void k_update_bhb(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
-                             const double *__restrict__ qold, double *__restrict__ qout, double *__restrict__ qcopy,
+                             const double *__restrict__ qold, double *qout, double *__restrict__ qcopy,
                              const double *__restrict__ dtv, const double *__restrict__ vol, double ar,
-                             const double *__restrict__ qsrc) {
+                             const double *qsrc) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;

@@ -1478,6 +1478,132 @@ void update_bhb_b(const Level &L, int b, const double *ra, double *qa, const dou
       }
 }
 
+// update_bhb's k-omega part with rkimp (src/update.f90:1427-1560 without IRS
+// on one level, 1633-1768 with IRS or multigrid): per cell the snapshots of
+// rho omega, then of rho k, coupled through (I (1 + ar dtau a_n) + ar omega
+// dtau D) x = rhs with the point-implicit destruction a_n; rho omega floored
+// by gav cmu rho sqrt(prd); the k equation takes omega before the update
+// and the change of rho omega.  Runs before update_bhb_b (variables 1..5).
+void update_bhb_kom_b(const Level &L, int b, const double *ra, double *qa, const double *qoa, const double *va,
+                      const double *dtta, const double *dpla, const double *prda, double ar, const cosa_params &P,
+                      const double *ttrma, bool src_in_res) {
+  const int S = L.S;
+  B3 res(const_cast<double *>(ra), L, b), q(qa, L, b), qold(const_cast<double *>(qoa), L, b);
+  B1 dtt(const_cast<double *>(dtta), L, b, S), vol(const_cast<double *>(va), L, b, 1);
+  B3s dpl(const_cast<double *>(dpla), L, b), prd(const_cast<double *>(prda), L, b);
+  for (int k = 1; k <= L.km[b] - 1; ++k)
+    for (int j = 1; j <= L.jm[b] - 1; ++j)
+      for (int i = 1; i <= L.im[b] - 1; ++i) {
+        auto gav_of = [&](int n) { return ttrma ? B3t(const_cast<double *>(ttrma), L, b)(i, j, k, 2, n) : P.gkw; };
+        auto bav_of = [&](int n) { return ttrma ? B3t(const_cast<double *>(ttrma), L, b)(i, j, k, 3, n) : P.bkw; };
+        auto hbsrc = [&](int v, int ni) {  // src_bhb's term of variable v, snapshot ni
+          double qhb = 0.0;
+          for (int nj = 0; nj < S; ++nj) qhb = qhb + P.omega * vol(i, j, k) * P.dhb[ni * S + nj] * q(i, j, k, v, nj);
+          return qhb;
+        };
+        double a[COSA_MAX_SNAP * COSA_MAX_SNAP], x[COSA_MAX_SNAP], w7[COSA_MAX_SNAP], dw[COSA_MAX_SNAP];
+        // rho omega
+        for (int ni = 0; ni < S; ++ni) {
+          const double gav = gav_of(ni), bav = bav_of(ni);
+          const double ome = q(i, j, k, 7, ni) / q(i, j, k, 1, ni);
+          const double dtau = dtt(i, j, k, ni) * vol(i, j, k);
+          const double dps = dpl(i, j, k, ni);
+          if (src_in_res)
+            x[ni] = qold(i, j, k, 7, ni) + ar * dtt(i, j, k, ni) * (hbsrc(7, ni) - res(i, j, k, 7, ni)) +
+                    ar * dtau * q(i, j, k, 7, ni) * (gav * dps + 2 * bav * ome);
+          else
+            x[ni] = qold(i, j, k, 7, ni) - ar * res(i, j, k, 7, ni) * dtt(i, j, k, ni) +
+                    ar * dtau * q(i, j, k, 7, ni) * (gav * dps + 2 * bav * ome);
+          w7[ni] = q(i, j, k, 7, ni);
+          for (int nj = 0; nj < S; ++nj)
+            a[ni + S * nj] = (ni == nj ? 1.0 : 0.0) * (1 + ar * dtau * (gav * dps + 2 * bav * ome)) +
+                             ar * P.omega * dtau * P.dhb[ni * S + nj];
+        }
+        // the k right-hand sides read rho k and the src_bhb terms before any update
+        double xk[COSA_MAX_SNAP], qk[COSA_MAX_SNAP], sk[COSA_MAX_SNAP];
+        for (int ni = 0; ni < S; ++ni) {
+          qk[ni] = q(i, j, k, 6, ni);
+          sk[ni] = src_in_res ? hbsrc(6, ni) : 0.0;
+        }
+        lu_solve(S, a, x, 1);
+        for (int ni = 0; ni < S; ++ni) {
+          const double rho = q(i, j, k, 1, ni);
+          const double rhomegamin = gav_of(ni) * P.cmu * rho * std::sqrt(prd(i, j, k, ni));
+          if (x[ni] < rhomegamin) x[ni] = rhomegamin;
+          q(i, j, k, 7, ni) = x[ni];
+          dw[ni] = q(i, j, k, 7, ni) - w7[ni];
+        }
+        // rho k
+        for (int ni = 0; ni < S; ++ni) {
+          const double rho = q(i, j, k, 1, ni);
+          const double ome = w7[ni] / q(i, j, k, 1, ni);
+          const double dtau = dtt(i, j, k, ni) * vol(i, j, k);
+          const double dps = dpl(i, j, k, ni);
+          if (src_in_res)
+            xk[ni] = (qold(i, j, k, 6, ni) + ar * dtt(i, j, k, ni) * (sk[ni] - res(i, j, k, 6, ni)) +
+                      ar * dtau * qk[ni] * (dps + P.bstrkw * ome - P.bstrkw * dw[ni] / rho));
+          else
+            xk[ni] = (qold(i, j, k, 6, ni) - ar * res(i, j, k, 6, ni) * dtt(i, j, k, ni) +
+                      ar * dtau * qk[ni] * (dps + P.bstrkw * ome - P.bstrkw * dw[ni] / rho));
+          for (int nj = 0; nj < S; ++nj)
+            a[ni + S * nj] = (ni == nj ? 1.0 : 0.0) * (1 + ar * dtau * (dps + P.bstrkw * ome)) +
+                             ar * P.omega * dtau * P.dhb[ni * S + nj];
+        }
+        lu_solve(S, a, xk, 1);
+        for (int ni = 0; ni < S; ++ni) q(i, j, k, 6, ni) = xk[ni];
+      }
+}
+
+// lim_res_ome_bhb (src/update.f90:2836-2999), without low-speed
+// preconditioning: the omega residual of the residual pass limited so that
+// rho omega cannot go below its floor; explicit per snapshot, with rkimp
+// through the snapshot-coupled system (I (1 + dtau a_n) + omega dtau D)
+void lim_res_ome_bhb_b(const Level &L, int b, double *ra, const double *qa, const double *qoa, const double *va,
+                       const double *dtta, const double *dpla, const double *prda, const cosa_params &P,
+                       const double *ttrma) {
+  const int S = L.S;
+  B3 res(ra, L, b), q(const_cast<double *>(qa), L, b), qold(const_cast<double *>(qoa), L, b);
+  B1 dtt(const_cast<double *>(dtta), L, b, S), vol(const_cast<double *>(va), L, b, 1);
+  B3s dpl(const_cast<double *>(dpla), L, b), prd(const_cast<double *>(prda), L, b);
+  for (int k = 1; k <= L.km[b] - 1; ++k)
+    for (int j = 1; j <= L.jm[b] - 1; ++j)
+      for (int i = 1; i <= L.im[b] - 1; ++i) {
+        auto gav_of = [&](int n) { return ttrma ? B3t(const_cast<double *>(ttrma), L, b)(i, j, k, 2, n) : P.gkw; };
+        auto bav_of = [&](int n) { return ttrma ? B3t(const_cast<double *>(ttrma), L, b)(i, j, k, 3, n) : P.bkw; };
+        if (!P.rkimp) {
+          for (int n = 0; n < S; ++n) {
+            const double gav = gav_of(n), bav = bav_of(n);
+            const double rho = q(i, j, k, 1, n), ome = q(i, j, k, 7, n) / q(i, j, k, 1, n);
+            const double dtau = dtt(i, j, k, n) * vol(i, j, k);
+            const double rhomega = qold(i, j, k, 7, n) -
+                                   res(i, j, k, 7, n) * dtt(i, j, k, n) / (1 + dtau * (gav * dpl(i, j, k, n) + 2 * bav * ome));
+            const double rhomegamin = gav * P.cmu * rho * std::sqrt(prd(i, j, k, n));
+            res(i, j, k, 7, n) = res(i, j, k, 7, n) - (1 + dtau * (gav * dpl(i, j, k, n) + 2 * bav * ome)) *
+                                                          std::max(0.0, (rhomegamin - rhomega) / dtt(i, j, k, n));
+          }
+          continue;
+        }
+        double a[COSA_MAX_SNAP * COSA_MAX_SNAP], x[COSA_MAX_SNAP];
+        for (int ni = 0; ni < S; ++ni) {
+          const double gav = gav_of(ni), bav = bav_of(ni);
+          const double dtau = dtt(i, j, k, ni) * vol(i, j, k);
+          const double ome = q(i, j, k, 7, ni) / q(i, j, k, 1, ni);
+          const double dps = dpl(i, j, k, ni);
+          for (int nj = 0; nj < S; ++nj)
+            a[ni + S * nj] = (ni == nj ? 1.0 : 0.0) * (1 + dtau * (gav * dps + 2 * bav * ome)) +
+                             P.omega * dtau * P.dhb[ni * S + nj];
+          x[ni] = res(i, j, k, 7, ni) * dtt(i, j, k, ni);
+        }
+        lu_solve(S, a, x, 1);
+        for (int n = 0; n < S; ++n) {
+          const double rho = q(i, j, k, 1, n);
+          const double rhomegamin = gav_of(n) * P.cmu * rho * std::sqrt(prd(i, j, k, n));
+          const double rhomeganew = qold(i, j, k, 7, n) - x[n];
+          res(i, j, k, 7, n) = res(i, j, k, 7, n) - std::max(0.0, (rhomegamin - rhomeganew)) / dtt(i, j, k, n);
+        }
+      }
+}
+
 // ---- dual time stepping (src/src.f90:381-527; src/update.f90:568-740;
 // src/cosa.f90:4503-4560) ---------------------------------------------------------
 // src_uns_b: res += 3/2 q V / dt (BDF2), q V / dt on a first-order first step
@@ -3844,7 +3970,9 @@ int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_p
   if (dual_src_in_res(*p)) {
     if (!A.vol) return COSA_ERR_ARG;
     src_uns_level(L, q, A.vol, A.res, *p);
-  } else if (p->harbal && A.vol) {
+  } else if (p->harbal && A.vol && (!kom || !p->rkimp || p->irsop > 0 || p->nlevel > 1)) {
+    // src_hb unless rkimp without IRS on one level (src/cosa.f90:1918-1922);
+    // the Euler callers pass no vol in that case
     src_hb_level(L, q, A.vol, A.res, *p);
   }
   return status;
@@ -4389,8 +4517,16 @@ int orc_smooth_level_rans(orc_level *h, const cosa_params *p, int nl, int nlevel
       if (status & (COSA_ERR_ARG | COSA_ERR_UNSUPPORTED)) return status;
       if (nl == 1 && irk == 1 && iter != niter + 1 && hist_row &&
           (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle)) {
-        if (p->dualt && p->rkimp && !dual_src_in_res(*p)) resg_rms_dualimp_level(L, A.res, A.rhs, A.q, A.vol, *p, hist_row);
-        else resg_rms_level(L, A.res, A.rhs, hist_row);
+        if (p->dualt && p->rkimp && !dual_src_in_res(*p)) {
+          resg_rms_dualimp_level(L, A.res, A.rhs, A.q, A.vol, *p, hist_row);
+        } else if (p->harbal && p->rkimp && p->irsop == 0 && p->nlevel == 1) {
+          resg_rms_hbimp_level(L, A.res, A.q, A.vol, *p, hist_row);
+        } else if (p->harbal) {
+          std::vector<double> w(A.res, A.res + L.n3 * L.npde * L.S);
+          resg_rms_hb_level(L, w.data(), hist_row);
+        } else {
+          resg_rms_level(L, A.res, A.rhs, hist_row);
+        }
       }
       if (nl == 1 && p->dualt) add_level(L, A.res, A.rhs, -1.0, -1);
       if (from_fine && iter == 1 && irk == 1) add_level(L, A.rhs, A.res, 1.0, -1);
@@ -4398,9 +4534,14 @@ int orc_smooth_level_rans(orc_level *h, const cosa_params *p, int nl, int nlevel
       if (iter == niter + 1) {
         if (nlevel > 1 && nl != nlevel && !p->prd_all_lvls && p->lim_prodtke)
           for (int b = 0; b < L.nb; ++b) lim_prod_mg_b(L, b, A.q, X.prd, A.mut, *p);
-        for (int b = 0; b < L.nb; ++b)
-          lim_res_ome_b(L, b, A.res, A.q, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p,
-                        is_blend(*p) ? X.ttrm : nullptr);
+        for (int b = 0; b < L.nb; ++b) {
+          if (p->harbal)
+            lim_res_ome_bhb_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, *p,
+                              is_blend(*p) ? X.ttrm : nullptr);
+          else
+            lim_res_ome_b(L, b, A.res, A.q, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p,
+                          is_blend(*p) ? X.ttrm : nullptr);
+        }
         return status;
       }
       if (p->irsop > 0)
@@ -4411,6 +4552,11 @@ int orc_smooth_level_rans(orc_level *h, const cosa_params *p, int nl, int nlevel
           update_kom_dual_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p,
                             is_blend(*p) ? X.ttrm : nullptr, dual_src_in_res(*p));
           update_dual_b(L, b, A.res, A.q, A.qold, A.dtvol, A.vol, p->alphas[irk - 1], *p, dual_src_in_res(*p));
+        } else if (p->harbal && p->rkimp) {
+          const bool sir = p->irsop > 0 || p->nlevel > 1;
+          update_bhb_kom_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p,
+                           is_blend(*p) ? X.ttrm : nullptr, sir);
+          update_bhb_b(L, b, A.res, A.q, A.qold, A.dtvol, A.vol, p->alphas[irk - 1], *p, sir);
         } else {
           update_kom_b(L, b, A.res, A.q, A.qold, A.vol, A.dtvolt, X.delpls, X.prd, p->alphas[irk - 1], *p,
                        is_blend(*p) ? X.ttrm : nullptr);
