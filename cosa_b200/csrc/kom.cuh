@@ -424,7 +424,7 @@ __global__ void k_lim_res_ome(BS bs_, const cosa_params *__restrict__ Pp, double
     const double dtau = dt * vol[p1_idx(b, 1, i, j, k, 0)];
     const double rho = q[i1], ome = q[i7] / q[i1];
     if (P.rkimp && P.dualt) {
-      // rkimp (src/update.f90:2781-2806): the physical-time term in the
+      // rkimp (src/update.f90:2785-2823): the physical-time term in the
       // denominator; the reference's den1 has no ar here
       const double den1 = 1 + dtau * (gav * delpls[o] + 2 * bav * ome);
       const double den2 = ar * (P.bdf1 ? 1.0 : 1.5) * dtau / P.dt;

@@ -2124,7 +2124,7 @@ void lim_res_ome_b(const Level &L, int b, double *ra, const double *qa, const do
           const double dtau = dtt(i, j, k, n) * vol(i, j, k);
           const double rho = q(i, j, k, 1, n), ome = q(i, j, k, 7, n) / q(i, j, k, 1, n);
           if (P.rkimp && P.dualt) {
-            // rkimp (src/update.f90:2781-2806): the physical-time term in the
+            // rkimp (src/update.f90:2785-2823): the physical-time term in the
             // denominator; the reference's den1 has no ar here
             const double fact = P.bdf1 ? 1.0 : 1.5;
             const double den1 = 1 + dtau * (gav * dpl(i, j, k, n) + 2 * bav * ome);
