@@ -77,6 +77,7 @@ struct LevelState {
   double *d_prd = nullptr, *d_divvel = nullptr, *d_delpls = nullptr;
   double *d_ttrm = nullptr;   // BSL/SST: (cdif, gamma, beta) per cell (P3 x 3 x S)
   double *d_fdist = nullptr;  // BSL/SST: face wall distances, families 1..3 at 0, n0, 2 n0
+  double *d_h0 = nullptr;     // k-omega: h0 of each family's last face (block x 3 x snapshot x 2)
   double *d_tbeta[3] = {nullptr, nullptr, nullptr};
   // stage schedule: 0 = fused tile kernel, 1 = face-split (k_faces + k_cells),
   // set by cosa_gpu_autotune
@@ -1209,6 +1210,7 @@ int ensure_rans(cosa_ctx *c, LevelState &L) {
     }
   for (auto &t : L.d_tbeta)
     if (!t && (r = dalloc(c, &t, (size_t)L.n1 * S))) return r;
+  if (!L.d_h0 && (r = dalloc(c, &L.d_h0, (size_t)L.nb * 3 * COSA_MAX_SNAP * 2))) return r;
   if (blend(c->p)) {
     if (!L.d_ttrm) {
       if ((r = dalloc(c, &L.d_ttrm, (size_t)L.n3 * 3 * S))) return r;
@@ -2990,27 +2992,44 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
   if ((r = cosa_gpu_zero(c, nl, P.res))) return r;
   if ((r = launch_edges(c, L, q, P.mut))) return r;
   const double *sd[4] = {nullptr, P.si, P.sj, P.sk};
+  const bool mixed = p.precision == COSA_PREC_MIXED;
+  const int *bct = L.d_bct;
+  const BlockList bl{L.d_blocks};
+  const int ntr = L.nb * 3 * S;
+  if (mixed) k_rans_h0<true><<<grid_for(ntr, 64), 64, 0, c->s>>>(L.d_blocks, L.nb, c->d_p, bct, q, nl, L.d_h0);
+  else k_rans_h0<false><<<grid_for(ntr, 64), 64, 0, c->s>>>(L.d_blocks, L.nb, c->d_p, bct, q, nl, L.d_h0);
+  if ((r = after_launch(c))) return r;
   for (int d = 1; d <= 3; ++d) {
-    const int mixed = p.precision == COSA_PREC_MIXED;
-    if ((r = muscl_impl(c, d, nl, q, P.qp, P.qm, P.dq, P.dqp, P.dqm, mixed))) return r;
-    if ((r = roflux_impl(c, d, nl, P.qp, P.qm, P.flux, sd[d], mixed))) return r;
-    if ((r = cosa_gpu_resid(c, d, nl, P.flux, P.res))) return r;
-    // q_face (+ face mut) / q_der / rtst / vflux / resid (src/cosa.f90:1809-1824)
-    if ((r = rans_face_state(c, L, d, q, P.dq, nullptr, nullptr, nullptr))) return r;
-    if ((r = cosa_gpu_q_face_mut(c, d, nl, P.mut, P.flux))) return r;
-    if ((r = rans_face_state(c, L, d, q, nullptr, P.qp, P.qm, P.dqm))) return r;
-    if ((r = cosa_gpu_rtst(c, d, nl, P.dq, P.qp, P.qm, P.dqm, L.d_vm, P.flux, P.dqp))) return r;
-    if ((r = cosa_gpu_vflux_kom(c, d, nl, P.dq, P.qp, P.qm, P.dqm, P.dqp, L.d_vm, sd[d], P.flux,
-                                blend(p) ? L.d_fdist + (int64_t)(d - 1) * L.n0 : nullptr)))
-      return r;
-    if ((r = cosa_gpu_resid(c, d, nl, P.flux, P.res))) return r;
+    // muscl + roflux, then q_face / q_der / rtst / vflux added to the same
+    // face fluxes, then resid (src/cosa.f90:1797-1824)
+    const double *sm = sd[d];
+    const double *fd = blend(p) ? L.d_fdist + (int64_t)(d - 1) * L.n0 : nullptr;
+    r = for_blocks(c, L, cnt_faces, [&](auto b, dim3 g) {
+      (void)b;
+      const dim3 g128(g.x * 2, g.y);
+#define COSA_RANS_CONV(DD, MM) \
+  k_rans_conv<DD, MM><<<g128, 128, 0, c->s>>>(bl, c->d_p, bct, q, nl, sm, L.d_h0, P.flux)
+      if (d == 1) { if (mixed) COSA_RANS_CONV(1, true); else COSA_RANS_CONV(1, false); }
+      else if (d == 2) { if (mixed) COSA_RANS_CONV(2, true); else COSA_RANS_CONV(2, false); }
+      else { if (mixed) COSA_RANS_CONV(3, true); else COSA_RANS_CONV(3, false); }
+#undef COSA_RANS_CONV
+    });
+    if (r) return r;
+    r = for_blocks(c, L, cnt_faces, [&](auto b, dim3 g) {
+      (void)b;
+      const dim3 g128(g.x * 2, g.y);
+      if (d == 1) k_rans_vface<1><<<g128, 128, 0, c->s>>>(bl, c->d_p, bct, q, P.mut, L.d_vm, L.n0, sm, fd, P.flux);
+      else if (d == 2) k_rans_vface<2><<<g128, 128, 0, c->s>>>(bl, c->d_p, bct, q, P.mut, L.d_vm, L.n0, sm, fd, P.flux);
+      else k_rans_vface<3><<<g128, 128, 0, c->s>>>(bl, c->d_p, bct, q, P.mut, L.d_vm, L.n0, sm, fd, P.flux);
+    });
+    if (r || (r = cosa_gpu_resid(c, d, nl, P.flux, P.res))) return r;
   }
   // cell-centred velocity gradients, production and sources (src/cosa.f90:1878-1896)
-  double *dc[3] = {P.qp, P.qm, P.dqm};
-  for (int d = 1; d <= 3; ++d) {
-    if ((r = rans_face_state(c, L, d, q, P.dq, nullptr, nullptr, nullptr))) return r;
-    if ((r = cosa_gpu_q_der_c(c, d, nl, P.dq, dc[d - 1]))) return r;
-  }
+  if ((r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+         (void)b;
+         k_rans_qder_c<<<g, 256, 0, c->s>>>(bl, c->d_p, bct, q, P.qp, P.qm, P.dqm, blend(p) ? 7 : 4);
+       })))
+    return r;
   if (nl == 1 || p.prd_all_lvls)
     if ((r = cosa_gpu_turprod(c, nl, P.qp, P.qm, P.dqm, L.d_vm, L.d_prd, L.d_divvel, L.d_delpls))) return r;
   if (blend(p)) {
@@ -3100,15 +3119,17 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
          })))
       return r;
   } else {
-    if ((r = cosa_gpu_update_kom(c, nl, P.res, q, P.qold, P.vol, P.dtvolt, L.d_delpls, L.d_prd, p.alphas[irk - 1],
-                                 blend(p) ? L.d_ttrm : nullptr)))
-      return r;
+    // point-implicit k / omega, the mean-flow update and fixq in one pass
     const double ar = p.alphas[irk - 1];
-    if ((r = for_blocks(c, L, cnt_interior,
-                        [&](auto b, dim3 g) { k_update<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, q, P.qold, P.dtvol, ar); })))
+    const double *tt = blend(p) ? L.d_ttrm : nullptr;
+    if ((r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+           k_update_rans<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, q, P.qold, P.vol, P.dtvolt, P.dtvol, L.d_delpls,
+                                              L.d_prd, ar, tt);
+         })))
       return r;
   }
-  if (p.ifixq && (r = cosa_gpu_fixq(c, nl, q))) return r;
+  // k_update_rans applies fixq itself
+  if (p.ifixq && p.rkimp && (p.dualt || p.harbal) && (r = cosa_gpu_fixq(c, nl, q))) return r;
   if (irk == p.nstage && (nl == 1 || !p.prd_all_lvls)) {
     // SST: the stage's cell-centred differences are still in qp, qm, dqm
     if (p.kom_sst) r = cosa_gpu_tur_vis_sst(c, nl, q, P.mut, P.qp, P.qm, P.dqm, L.d_vm, P.dist);

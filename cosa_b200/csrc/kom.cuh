@@ -119,6 +119,81 @@ __global__ void k_qwall_mut(const DevBlock *__restrict__ blocks, const WallFace 
   }
 }
 
+// b_rtst of one face (src/flux.f90:2846-2946): tau1(1..6) from the face
+// density and k, the velocity gradients gr[var u,v,w][xi, eta, zeta], the
+// face inverse metrics and the face mut
+__device__ __forceinline__ void rtst_face(const cosa_params &P, double rho, double tke, const double gr[3][3],
+                                          const double vmf[9], double mut, double tau[6]) {
+  const double fact = 2.0 / 3.0, mr = P.machfs / P.reyno;
+  double dv[3][3];  // dv[var][x, y, z]
+#pragma unroll
+  for (int m = 0; m < 3; ++m)
+#pragma unroll
+    for (int c3 = 0; c3 < 3; ++c3) dv[m][c3] = gr[m][0] * vmf[c3] + gr[m][1] * vmf[3 + c3] + gr[m][2] * vmf[6 + c3];
+  const double divv = (dv[0][0] + dv[1][1] + dv[2][2]) * P.turcmp;
+  const double txx = 2 * mut * (dv[0][0] - divv / 3), txy = mut * (dv[0][1] + dv[1][0]);
+  const double txz = mut * (dv[0][2] + dv[2][0]), tyy = 2 * mut * (dv[1][1] - divv / 3);
+  const double tyz = mut * (dv[1][2] + dv[2][1]), tzz = 2 * mut * (dv[2][2] - divv / 3);
+  tau[0] = mr * txx - fact * rho * tke;
+  tau[1] = mr * txy;
+  tau[2] = mr * txz;
+  tau[3] = mr * tyy - fact * rho * tke;
+  tau[4] = mr * tyz;
+  tau[5] = mr * tzz - fact * rho * tke;
+}
+
+// vflux_b with kom on one face: the k-omega branch (Reynolds stresses, k
+// and omega diffusion; the omega row keeps the reference's dk/dz) plus the
+// laminar terms with the face mut in the heat flux.  qf primitive face state
+// (7 variables), g[dir][var] its gradients, fd the face wall distance
+// (BSL/SST sigma blending) or negative for Wilcox's constants; F[0] = 0
+__device__ __forceinline__ void vflux_kom_face(const cosa_params &P, const ViscPar &V, const double qf[7],
+                                               const double g[3][7], const double tau[6], const double vmf[9],
+                                               double kx, double ky, double kz, double ds, double mut, double fd,
+                                               double F[7]) {
+  const double rho = qf[0], p = qf[4];
+  const double tt = P.gamma * p / rho;
+  const double mu = sutherland(tt, P.stemp);
+  const double tkexi = g[0][5], tkeeta = g[1][5], tkezeta = g[2][5];
+  const double omexi = g[0][6], omeeta = g[1][6], omezeta = g[2][6];
+  const double dtkedx = tkexi * vmf[0] + tkeeta * vmf[3] + tkezeta * vmf[6];
+  const double dtkedy = tkexi * vmf[1] + tkeeta * vmf[4] + tkezeta * vmf[7];
+  const double dtkedz = tkexi * vmf[2] + tkeeta * vmf[5] + tkezeta * vmf[8];
+  const double domedx = omexi * vmf[0] + omeeta * vmf[3] + omezeta * vmf[6];
+  const double domedy = omexi * vmf[1] + omeeta * vmf[4] + omezeta * vmf[7];
+  const double txx = tau[0], txy = tau[1], txz = tau[2], tyy = tau[3], tyz = tau[4], tzz = tau[5];
+  double Fk[7];
+  Fk[1] = -(txx * kx + txy * ky + txz * kz) * ds;
+  Fk[2] = -(txy * kx + tyy * ky + tyz * kz) * ds;
+  Fk[3] = -(txz * kx + tyz * ky + tzz * kz) * ds;
+  double sigk = P.sigk, sigw = P.sigw;
+  if (fd >= 0) {
+    // BSL/SST (src/flux.f90:987-1061): sigma_k, sigma_omega blended by F1 of
+    // the face state and the face's wall distance
+    const BlendPar c = make_blend(P);
+    const double domedz = omexi * vmf[2] + omeeta * vmf[5] + omezeta * vmf[8];
+    double cdt;
+    const double f1 = blend_f1(c, P, rho, qf[5], qf[6], mu, dtkedx * domedx + dtkedy * domedy + dtkedz * domedz, fd,
+                               cdt);
+    sigk = f1 * c.sigk1 + (1 - f1) * c.sigk2;
+    sigw = f1 * c.sigw1 + (1 - f1) * c.sigw2;
+  }
+  const double ctke = (mu + sigk * mut) * P.machfs / P.reyno;
+  const double come = (mu + sigw * mut) * P.machfs / P.reyno;
+  Fk[4] = -ctke * (dtkedx * kx + dtkedy * ky + dtkedz * kz) * ds;
+  Fk[5] = -ctke * (dtkedx * kx + dtkedy * ky + dtkedz * kz) * ds;
+  Fk[6] = -come * (domedx * kx + domedy * ky + dtkedz * kz) * ds;
+  double f5[5], g5[3][5], F5[5];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) { f5[m] = qf[m]; g5[0][m] = g[0][m]; g5[1][m] = g[1][m]; g5[2][m] = g[2][m]; }
+  vflux_face(V, f5, g5, vmf, kx, ky, kz, ds, mut, F5);
+  F[0] = 0.0;
+#pragma unroll
+  for (int m = 1; m < 5; ++m) F[m] = Fk[m] + F5[m];
+  F[5] = Fk[5];
+  F[6] = Fk[6];
+}
+
 // b_rtst (src/flux.f90:2846-2946): tau1(.,1..6) on the faces of family d
 template <class BS>
 __global__ void k_rtst(BS bs_, int d, const cosa_params *__restrict__ Pp, const double *__restrict__ qf,
@@ -128,7 +203,6 @@ __global__ void k_rtst(BS bs_, int d, const cosa_params *__restrict__ Pp, const 
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
-  const double fact = 2.0 / 3.0, mr = P.machfs / P.reyno;
   KOM_FACE_LOOP(d)
     const int64_t c = p3_cell(b, i, j, k);
     auto Q = [&](const double *a, int v) { return a[p3_var(b, npde, S, v, n) + c]; };
@@ -138,21 +212,10 @@ __global__ void k_rtst(BS bs_, int d, const cosa_params *__restrict__ Pp, const 
     double gr[3][3];  // gr[var u,v,w][xi, eta, zeta]
 #pragma unroll
     for (int m = 0; m < 3; ++m) { gr[m][0] = Q(g0, m + 2); gr[m][1] = Q(g1, m + 2); gr[m][2] = Q(g2, m + 2); }
-    double dv[3][3];  // dv[var][x, y, z]
+    double t6[6];
+    rtst_face(P, rho, tke, gr, vmf, mut, t6);
 #pragma unroll
-    for (int m = 0; m < 3; ++m)
-#pragma unroll
-      for (int c3 = 0; c3 < 3; ++c3) dv[m][c3] = gr[m][0] * vmf[c3] + gr[m][1] * vmf[3 + c3] + gr[m][2] * vmf[6 + c3];
-    const double divv = (dv[0][0] + dv[1][1] + dv[2][2]) * P.turcmp;
-    const double txx = 2 * mut * (dv[0][0] - divv / 3), txy = mut * (dv[0][1] + dv[1][0]);
-    const double txz = mut * (dv[0][2] + dv[2][0]), tyy = 2 * mut * (dv[1][1] - divv / 3);
-    const double tyz = mut * (dv[1][2] + dv[2][1]), tzz = 2 * mut * (dv[2][2] - divv / 3);
-    tau[p3_var(b, npde, S, 1, n) + c] = mr * txx - fact * rho * tke;
-    tau[p3_var(b, npde, S, 2, n) + c] = mr * txy;
-    tau[p3_var(b, npde, S, 3, n) + c] = mr * txz;
-    tau[p3_var(b, npde, S, 4, n) + c] = mr * tyy - fact * rho * tke;
-    tau[p3_var(b, npde, S, 5, n) + c] = mr * tyz;
-    tau[p3_var(b, npde, S, 6, n) + c] = mr * tzz - fact * rho * tke;
+    for (int m = 0; m < 6; ++m) tau[p3_var(b, npde, S, m + 1, n) + c] = t6[m];
   }
 }
 
@@ -177,49 +240,15 @@ __global__ void k_vflux_kom(BS bs_, int d, const cosa_params *__restrict__ Pp, c
     const double kx = s[e], ky = s[e + 1], kz = s[e + 2], ds = s[e + 3];
     double vmf[9];
     load_vm(vm, b, n0, d, i, j, k, vmf);
-    const double rho = Q(qf, 1), p = Q(qf, 5);
-    const double tt = P.gamma * p / rho;
-    const double mu = sutherland(tt, P.stemp);
     const double mut = flux[f0_idx(b, npde, S, i, j, k, 1, n)];
-    const double tkexi = Q(g0, 6), tkeeta = Q(g1, 6), tkezeta = Q(g2, 6);
-    const double omexi = Q(g0, 7), omeeta = Q(g1, 7), omezeta = Q(g2, 7);
-    const double dtkedx = tkexi * vmf[0] + tkeeta * vmf[3] + tkezeta * vmf[6];
-    const double dtkedy = tkexi * vmf[1] + tkeeta * vmf[4] + tkezeta * vmf[7];
-    const double dtkedz = tkexi * vmf[2] + tkeeta * vmf[5] + tkezeta * vmf[8];
-    const double domedx = omexi * vmf[0] + omeeta * vmf[3] + omezeta * vmf[6];
-    const double domedy = omexi * vmf[1] + omeeta * vmf[4] + omezeta * vmf[7];
-    const double txx = Q(tau, 1), txy = Q(tau, 2), txz = Q(tau, 3), tyy = Q(tau, 4), tyz = Q(tau, 5), tzz = Q(tau, 6);
-    double Fk[7];
-    Fk[1] = -(txx * kx + txy * ky + txz * kz) * ds;
-    Fk[2] = -(txy * kx + tyy * ky + tyz * kz) * ds;
-    Fk[3] = -(txz * kx + tyz * ky + tzz * kz) * ds;
-    double sigk = P.sigk, sigw = P.sigw;
-    if (fdist) {
-      // BSL/SST (src/flux.f90:987-1061): sigma_k, sigma_omega blended by F1 of
-      // the face state and the face's wall distance
-      const BlendPar c = make_blend(P);
-      const double domedz = omexi * vmf[2] + omeeta * vmf[5] + omezeta * vmf[8];
-      double cdt;
-      const double f1 = blend_f1(c, P, rho, Q(qf, 6), Q(qf, 7), mu, dtkedx * domedx + dtkedy * domedy + dtkedz * domedz,
-                                 fdist[f0_idx(b, 1, 1, i, j, k, 1, 0)], cdt);
-      sigk = f1 * c.sigk1 + (1 - f1) * c.sigk2;
-      sigw = f1 * c.sigw1 + (1 - f1) * c.sigw2;
-    }
-    const double ctke = (mu + sigk * mut) * P.machfs / P.reyno;
-    const double come = (mu + sigw * mut) * P.machfs / P.reyno;
-    Fk[4] = -ctke * (dtkedx * kx + dtkedy * ky + dtkedz * kz) * ds;
-    Fk[5] = -ctke * (dtkedx * kx + dtkedy * ky + dtkedz * kz) * ds;
-    Fk[6] = -come * (domedx * kx + domedy * ky + dtkedz * kz) * ds;
-    // laminar terms with the face mut in the heat flux
-    double f5[5], g[3][5], F[5];
+    double f7[7], g[3][7], t6[6], F[7];
 #pragma unroll
-    for (int m = 0; m < 5; ++m) { f5[m] = Q(qf, m + 1); g[0][m] = Q(g0, m + 1); g[1][m] = Q(g1, m + 1); g[2][m] = Q(g2, m + 1); }
-    vflux_face(V, f5, g, vmf, kx, ky, kz, ds, mut, F);
-    flux[f0_idx(b, npde, S, i, j, k, 1, n)] = 0.0;
+    for (int m = 0; m < 7; ++m) { f7[m] = Q(qf, m + 1); g[0][m] = Q(g0, m + 1); g[1][m] = Q(g1, m + 1); g[2][m] = Q(g2, m + 1); }
 #pragma unroll
-    for (int m = 1; m < 5; ++m) flux[f0_idx(b, npde, S, i, j, k, m + 1, n)] = Fk[m] + F[m];
-    flux[f0_idx(b, npde, S, i, j, k, 6, n)] = Fk[5];
-    flux[f0_idx(b, npde, S, i, j, k, 7, n)] = Fk[6];
+    for (int m = 0; m < 6; ++m) t6[m] = Q(tau, m + 1);
+    vflux_kom_face(P, V, f7, g, t6, vmf, kx, ky, kz, ds, mut, fdist ? fdist[f0_idx(b, 1, 1, i, j, k, 1, 0)] : -1.0, F);
+#pragma unroll
+    for (int m = 0; m < 7; ++m) flux[f0_idx(b, npde, S, i, j, k, m + 1, n)] = F[m];
   }
 }
 
@@ -599,5 +628,271 @@ __global__ void k_tur_vis_sst_halo(BS bs_, int S, double *__restrict__ mut) {
       si = side ? b.im - 1 : 1; sj = j; sk = k;
     }
     mut[p3s_idx(b, S, i, j, k, n)] = mut[p3s_idx(b, S, si, sj, sk, n)];
+  }
+}
+
+// ---- fused faces of the k-omega stage ---------------------------------------------------
+// the last strong-BC patch (row of bct) of block b whose face at position e
+// (1 or mx) along d covers the tangential indices (t2, t3); -1 if none.  A
+// later patch replaces an earlier one on a shared face, as the wall-face
+// list of q_face / q_der keeps it.
+__device__ __forceinline__ int strong_row(const DevBlock &b, const int *__restrict__ bct, int d, int e, int mx, int t2,
+                                          int t3) {
+  if (e != 1 && e != mx) return -1;
+  int row = -1;
+  for (int ib = 0; ib < b.nbcs; ++ib) {
+    const int *rw = bct + b.obct + 10 * ib;
+    if (rw[1] != d || !strong_bc(rw[0])) continue;
+    if (e != (rw[2] == 1 ? 1 : mx)) continue;
+    const int s2 = d == 1 ? rw[5] : rw[3], e2 = d == 1 ? rw[6] : rw[4];
+    const int s3 = d == 3 ? rw[5] : rw[7], e3 = d == 3 ? rw[6] : rw[8];
+    if (t2 >= s2 && t2 <= e2 && t3 >= s3 && t3 <= e3) row = ib;
+  }
+  return row;
+}
+// the inflow/outflow side (1 = min face, 2 = max face) of a strong-BC patch
+// covering position e along d; 0 if none
+__device__ __forceinline__ int strong_side(const DevBlock &b, const int *__restrict__ bct, int d, int e, int mx,
+                                           int t2, int t3) {
+  return strong_row(b, bct, d, e, mx, t2, t3) < 0 ? 0 : (e == 1 ? 1 : 2);
+}
+
+// muscl_b* (dq with the strong-BC doubling, limiter, first order on coarse
+// levels / foturb, the strong-BC override) of variables 1..nv at face
+// (i,j,k) of family d, snapshot n: vr = qp (cell side), vl = qm (minus side),
+// as k_muscl_dq + k_muscl_face compute them
+template <bool MIXED>
+__device__ __forceinline__ void rans_face_recon(const DevBlock &b, const cosa_params &P, const int *__restrict__ bct,
+                                                const double *__restrict__ q, int d, int nl, int i, int j, int k,
+                                                int n, int nv, double *vr, double *vl) {
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int di = d == 1, dj = d == 2, dk = d == 3;
+  const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
+  const int e = d == 1 ? i : (d == 2 ? j : k);
+  const int t2 = d == 1 ? j : i, t3 = d == 3 ? j : k;
+  const int64_t cm2 = p3_cell(b, i - 2 * di, j - 2 * dj, k - 2 * dk), cm = p3_cell(b, i - di, j - dj, k - dk);
+  const int64_t c0 = p3_cell(b, i, j, k), cp = p3_cell(b, i + di, j + dj, k + dk);
+  const bool first_all = nl >= P.nl_crs;
+  // doubling of the differences at strong-BC faces (index e-1, e, e+1)
+  const int side = strong_side(b, bct, d, e, mx, t2, t3);
+  const bool dlo2 = strong_side(b, bct, d, e - 1, mx, t2, t3) != 0;
+  const bool dmi2 = side != 0;
+  const bool dhi2 = strong_side(b, bct, d, e + 1, mx, t2, t3) != 0;
+#pragma unroll
+  for (int v = 1; v <= 7; ++v) {
+    if (v > nv) break;
+    const int64_t base = p3_var(b, npde, S, v, n);
+    const double qm2 = q[base + cm2], qm = q[base + cm], q0 = q[base + c0], qp = q[base + cp];
+    const bool fo = first_all || (P.foturb && v >= 6);
+    double a_ = 0.0, b_ = 0.0;
+    if (!fo) {
+      double dlo = qm - qm2, dmid = q0 - qm, dhi = qp - q0;
+      if (dlo2) dlo = dlo * 2;
+      if (dmi2) dmid = dmid * 2;
+      if (dhi2) dhi = dhi * 2;
+      const int ilim = v <= 5 ? P.ilimf : P.ilimt;
+      const double eps = v <= 5 ? P.epslimf : P.epslimt;
+      if (MIXED) {
+        float fa, fb;
+        limit_face_fast(ilim, (float)eps, (float)P.rkap, (float)dlo, (float)dmid, (float)dhi, fa, fb);
+        a_ = fa; b_ = fb;
+      } else {
+        limit_face<double>(ilim, eps, P.rkap, dlo, dmid, dhi, a_, b_);
+      }
+    }
+    double vp = fo ? q0 : q0 + a_, vm = fo ? qm : qm + b_;
+    if (side) vp = vm = side == 1 ? qm : q0;  // q(0) at the min face, q(mx) at the max face
+    vr[v - 1] = vp;
+    vl[v - 1] = vm;
+  }
+}
+
+// roflux_b's turbulence fluxes use h0 of the mean-flow loop's last face
+// (src/flux.f90:312): both sides' h0 at face (imax, jmax-1, kmax-1) of the i
+// family (and its j, k counterparts) per block, family and snapshot, into
+// h0[((block * 3 + d - 1) * S + n) * 2 + side]
+template <bool MIXED>
+__global__ void k_rans_h0(const DevBlock *__restrict__ blocks, int nb, const cosa_params *__restrict__ Pp,
+                          const int *__restrict__ bct, const double *__restrict__ q, int nl, double *__restrict__ h0) {
+  const cosa_params &P = *Pp;
+  const int S = 2 * P.nharms + 1;
+  const int64_t total = (int64_t)nb * 3 * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int n = (int)(t % S), d = (int)((t / S) % 3) + 1, ib = (int)(t / (3 * S));
+    const DevBlock b = blocks[ib];
+    const int ic = d == 1 ? b.im : b.im - 1, jc = d == 2 ? b.jm : b.jm - 1, kc = d == 3 ? b.km : b.km - 1;
+    double a7[7], b7[7];
+    rans_face_recon<MIXED>(b, P, bct, q, d, nl, ic, jc, kc, n, 6, a7, b7);
+    h0[t * 2] = face_h0(P.gamma, a7);
+    h0[t * 2 + 1] = face_h0(P.gamma, b7);
+  }
+}
+
+// muscl + roflux_b of one face family of the k-omega stage in one pass: the
+// reconstructed states stay in registers, the seven face fluxes go to flux
+template <int D, bool MIXED>
+__global__ void __launch_bounds__(128, 3) k_rans_conv(BlockList bs_, const cosa_params *__restrict__ Pp,
+                                                      const int *__restrict__ bct, const double *__restrict__ q,
+                                                      int nl, const double *__restrict__ s,
+                                                      const double *__restrict__ h0, double *__restrict__ flux) {
+  const DevBlock b = bs_.get();
+  const cosa_params &P = *Pp;
+  const PhysPar ph = make_phys(P);
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int ic = D == 1 ? b.im : b.im - 1, jc = D == 2 ? b.jm : b.jm - 1, kc = D == 3 ? b.km : b.km - 1;
+  const double *h0b = h0 + ((int64_t)blockIdx.y * 3 + (D - 1)) * S * 2;
+  const int64_t total = (int64_t)ic * jc * kc * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int i = (int)(r % ic) + 1; r /= ic;
+    const int j = (int)(r % jc) + 1; r /= jc;
+    const int k = (int)(r % kc) + 1;
+    const int n = (int)(r / kc);
+    double vr[7], vl[7], f[5];
+    rans_face_recon<MIXED>(b, P, bct, q, D, nl, i, j, k, n, npde, vr, vl);
+    const int64_t e4 = p2_idx(b, 1, 1, i, j, k, 0);
+    const double kx = s[e4], ky = s[e4 + 1], kz = s[e4 + 2], ds = s[e4 + 3];
+    if (MIXED) roe_flux_mixed_tke(ph, kx, ky, kz, ds, vr, vl, vr[5], vl[5], f);
+    else roe_flux_fp64(ph, kx, ky, kz, ds, vr, vl, vr[5], vl[5], f);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) flux[f0_idx(b, npde, S, i, j, k, m + 1, n)] = f[m];
+    double fk, fw;
+    roe_turb(P, kx, ky, kz, ds, vr, vl, h0b[2 * n], h0b[2 * n + 1], fk, fw);
+    flux[f0_idx(b, npde, S, i, j, k, 6, n)] = fk;
+    flux[f0_idx(b, npde, S, i, j, k, 7, n)] = fw;
+  }
+}
+
+// q_face (+ calmut) / q_der / b_rtst / vflux_b of one face family of the
+// k-omega stage in one pass, added to the convective fluxes in flux: the face
+// state and gradients of the bulk loops, or on strong-BC faces the one-sided
+// wall formulas with the halo mut (src/flux.f90:1848-1962, 2846-2946, 947-1180)
+template <int D>
+__global__ void __launch_bounds__(128, 3) k_rans_vface(BlockList bs_, const cosa_params *__restrict__ Pp,
+                                                       const int *__restrict__ bct, const double *__restrict__ q,
+                                                       const double *__restrict__ mut, const double *__restrict__ vm,
+                                                       int64_t n0, const double *__restrict__ s,
+                                                       const double *__restrict__ fdist, double *__restrict__ flux) {
+  const DevBlock b = bs_.get();
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const ViscPar V = make_visc(P);
+  constexpr int di = D == 1, dj = D == 2, dk = D == 3;
+  const int mx = D == 1 ? b.im : (D == 2 ? b.jm : b.km);
+  KOM_FACE_LOOP(D)
+    const QView Q = qview(b, q, S, n, npde);
+    const int e = D == 1 ? i : (D == 2 ? j : k);
+    const int row = strong_row(b, bct, D, e, mx, D == 1 ? j : i, D == 3 ? j : k);
+    double qf[7], g[3][7], mf;
+    if (row < 0) {
+      face_interior<D, 7>(Q, i, j, k, qf, g);
+      mf = (mut[p3s_idx(b, S, i - di, j - dj, k - dk, n)] + mut[p3s_idx(b, S, i, j, k, n)]) / 2;
+    } else {
+      const int *rw = bct + b.obct + 10 * row;
+      WallFace w;
+      w.blk = blockIdx.y; w.d = D; w.inrout = rw[2];
+      w.fi = i; w.fj = j; w.fk = k;
+      w.lo[0] = rw[3]; w.lo[1] = rw[5]; w.lo[2] = rw[7];
+      w.hi[0] = rw[4]; w.hi[1] = rw[6]; w.hi[2] = rw[8];
+      face_wall<7>(Q, w, mx, qf, g);
+      const int a = e == 1 ? 0 : mx;
+      mf = mut[p3s_idx(b, S, D == 1 ? a : i, D == 2 ? a : j, D == 3 ? a : k, n)];
+    }
+    double vmf[9];
+    load_vm(vm, b, n0, D, i, j, k, vmf);
+    double gr[3][3], t6[6], F[7];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) { gr[m][0] = g[0][m + 1]; gr[m][1] = g[1][m + 1]; gr[m][2] = g[2][m + 1]; }
+    rtst_face(P, qf[0], qf[5], gr, vmf, mf, t6);
+    const int64_t e4 = p2_idx(b, 1, 1, i, j, k, 0);
+    vflux_kom_face(P, V, qf, g, t6, vmf, s[e4], s[e4 + 1], s[e4 + 2], s[e4 + 3], mf,
+                   fdist ? fdist[f0_idx(b, 1, 1, i, j, k, 1, 0)] : -1.0, F);
+#pragma unroll
+    for (int m = 1; m < 7; ++m) {
+      const int64_t o = f0_idx(b, npde, S, i, j, k, m + 1, n);
+      flux[o] = flux[o] + F[m];
+    }
+  }
+}
+
+// q_face (face states only) + q_der_c of the three families in one pass over
+// the cells: dc_d = qf_d(face e+1) - qf_d(face e) for u, v, w (and k, omega
+// when vhi = 7), the face state the bulk average or, on strong-BC faces, the
+// halo value (src/flux.f90:2979-3130)
+__global__ void k_rans_qder_c(BlockList bs_, const cosa_params *__restrict__ Pp, const int *__restrict__ bct,
+                              const double *__restrict__ q, double *__restrict__ dx, double *__restrict__ dy,
+                              double *__restrict__ dz, int vhi) {
+  const DevBlock b = bs_.get();
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  KOM_CELL_LOOP
+#pragma unroll
+    for (int d = 1; d <= 3; ++d) {
+      const int di = d == 1, dj = d == 2, dk = d == 3;
+      const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
+      const int e = d == 1 ? i : (d == 2 ? j : k);
+      const int t2 = d == 1 ? j : i, t3 = d == 3 ? j : k;
+      const bool wlo = strong_row(b, bct, d, e, mx, t2, t3) >= 0;
+      const bool whi = strong_row(b, bct, d, e + 1, mx, t2, t3) >= 0;
+      const int64_t cm = p3_cell(b, i - di, j - dj, k - dk), c0 = p3_cell(b, i, j, k);
+      const int64_t cp = p3_cell(b, i + di, j + dj, k + dk);
+      double *dc = d == 1 ? dx : (d == 2 ? dy : dz);
+      for (int v = 2; v <= vhi; ++v) {
+        if (v == 5) continue;
+        const int64_t o = p3_var(b, npde, S, v, n);
+        const double qm = q[o + cm], q0 = q[o + c0], qp = q[o + cp];
+        const double flo = wlo ? qm : (qm + q0) / 2;
+        const double fhi = whi ? qp : (q0 + qp) / 2;
+        dc[o + c0] = fhi - flo;
+      }
+    }
+  }
+}
+
+// update_b of the k-omega stage in one pass (src/update.f90:568-640): the
+// point-implicit rho omega / rho k of k_update_kom, the mean-flow update
+// q = q^n - ar R dt/V, and with ifixq the floors of fixq_b
+template <class BS>
+__global__ void k_update_rans(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ res,
+                              double *__restrict__ q, const double *__restrict__ qold,
+                              const double *__restrict__ vol, const double *__restrict__ dtt,
+                              const double *__restrict__ dtv, const double *__restrict__ delpls,
+                              const double *__restrict__ prd, double ar, const double *__restrict__ ttrm) {
+  const DevBlock b = bs_.get();
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  KOM_CELL_LOOP
+    const double gav = ttrm ? ttrm[ttrm_idx(b, S, i, j, k, 2, n)] : P.gkw;
+    const double bav = ttrm ? ttrm[ttrm_idx(b, S, i, j, k, 3, n)] : P.bkw;
+    const int64_t c = p3_cell(b, i, j, k), o = p3s_idx(b, S, i, j, k, n);
+    const int64_t i1 = p3_var(b, npde, S, 1, n) + c, i6 = p3_var(b, npde, S, 6, n) + c, i7 = p3_var(b, npde, S, 7, n) + c;
+    const double rho = q[i1], ome = q[i7] / q[i1], tke = q[i6] / q[i1];
+    const double dt = dtt[p1_idx(b, S, i, j, k, n)];
+    const double dtau = dt * vol[p1_idx(b, 1, i, j, k, 0)];
+    const double dp = delpls[o];
+    double rhomega = (qold[i7] - ar * res[i7] * dt + ar * dtau * rho * ome * (gav * dp + 2 * bav * ome)) /
+                     (1 + ar * dtau * (gav * dp + 2 * bav * ome));
+    const double rhomegamin = gav * P.cmu * rho * sqrt(prd[o]);
+    if (rhomega < rhomegamin) rhomega = rhomegamin;
+    const double drhomega = rhomega - rho * ome;
+    double rk = (qold[i6] - ar * res[i6] * dt + ar * dtau * rho * tke * (dp + P.bstrkw * ome) -
+                 ar * dtau * P.bstrkw * tke * drhomega) /
+                (1 + ar * dtau * (dp + P.bstrkw * ome));
+    const double dm = dtv[p1_idx(b, S, i, j, k, n)];
+    double rho1 = rho;
+#pragma unroll
+    for (int m = 1; m <= 5; ++m) {
+      const int64_t om = p3_var(b, npde, S, m, n) + c;
+      const double v = qold[om] - ar * res[om] * dm;
+      q[om] = v;
+      if (m == 1) rho1 = v;
+    }
+    if (P.ifixq) {
+      // fixq_b (src/update.f90:2216-2269) on the updated cell
+      if (rk / rho1 < P.qmin[5]) rk = rho1 * P.qmin[5];
+      if (rhomega / rho1 < P.qmin[6]) rhomega = rho1 * P.qmin[6];
+    }
+    q[i6] = rk;
+    q[i7] = rhomega;
   }
 }
