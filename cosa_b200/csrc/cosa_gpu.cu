@@ -78,6 +78,8 @@ struct LevelState {
   double *d_ttrm = nullptr;   // BSL/SST: (cdif, gamma, beta) per cell (P3 x 3 x S)
   double *d_fdist = nullptr;  // BSL/SST: face wall distances, families 1..3 at 0, n0, 2 n0
   double *d_h0 = nullptr;     // k-omega: h0 of each family's last face (block x 3 x snapshot x 2)
+  double *d_rflux = nullptr;  // k-omega: convective and viscous face fluxes of the three families (6 x F0 x npde x S)
+  int rflux_S = 0;
   double *d_tbeta[3] = {nullptr, nullptr, nullptr};
   // stage schedule: 0 = fused tile kernel, 1 = face-split (k_faces + k_cells),
   // set by cosa_gpu_autotune
@@ -1211,6 +1213,11 @@ int ensure_rans(cosa_ctx *c, LevelState &L) {
   for (auto &t : L.d_tbeta)
     if (!t && (r = dalloc(c, &t, (size_t)L.n1 * S))) return r;
   if (!L.d_h0 && (r = dalloc(c, &L.d_h0, (size_t)L.nb * 3 * COSA_MAX_SNAP * 2))) return r;
+  if (L.rflux_S < S) {
+    drop_graphs(c);  // captured graphs hold the old buffer address
+    if ((r = dalloc(c, &L.d_rflux, (size_t)6 * L.n0 * c->p.npde * S))) return r;
+    L.rflux_S = S;
+  }
   if (blend(c->p)) {
     if (!L.d_ttrm) {
       if ((r = dalloc(c, &L.d_ttrm, (size_t)L.n3 * 3 * S))) return r;
@@ -2991,7 +2998,6 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
   }
   if ((r = cosa_gpu_zero(c, nl, P.res))) return r;
   if ((r = launch_edges(c, L, q, P.mut))) return r;
-  const double *sd[4] = {nullptr, P.si, P.sj, P.sk};
   const bool mixed = p.precision == COSA_PREC_MIXED;
   const int *bct = L.d_bct;
   const BlockList bl{L.d_blocks};
@@ -2999,47 +3005,36 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
   if (mixed) k_rans_h0<true><<<grid_for(ntr, 64), 64, 0, c->s>>>(L.d_blocks, L.nb, c->d_p, bct, q, nl, L.d_h0);
   else k_rans_h0<false><<<grid_for(ntr, 64), 64, 0, c->s>>>(L.d_blocks, L.nb, c->d_p, bct, q, nl, L.d_h0);
   if ((r = after_launch(c))) return r;
-  for (int d = 1; d <= 3; ++d) {
-    // muscl + roflux, then q_face / q_der / rtst / vflux added to the same
-    // face fluxes, then resid (src/cosa.f90:1797-1824)
-    const double *sm = sd[d];
-    const double *fd = blend(p) ? L.d_fdist + (int64_t)(d - 1) * L.n0 : nullptr;
-    r = for_blocks(c, L, cnt_faces, [&](auto b, dim3 g) {
-      (void)b;
-      const dim3 g128(g.x * 2, g.y);
-#define COSA_RANS_CONV(DD, MM) \
-  k_rans_conv<DD, MM><<<g128, 128, 0, c->s>>>(bl, c->d_p, bct, q, nl, sm, L.d_h0, P.flux)
-      if (d == 1) { if (mixed) COSA_RANS_CONV(1, true); else COSA_RANS_CONV(1, false); }
-      else if (d == 2) { if (mixed) COSA_RANS_CONV(2, true); else COSA_RANS_CONV(2, false); }
-      else { if (mixed) COSA_RANS_CONV(3, true); else COSA_RANS_CONV(3, false); }
-#undef COSA_RANS_CONV
-    });
-    if (r) return r;
-    r = for_blocks(c, L, cnt_faces, [&](auto b, dim3 g) {
-      (void)b;
-      const dim3 g128(g.x * 2, g.y);
-      if (d == 1) k_rans_vface<1><<<g128, 128, 0, c->s>>>(bl, c->d_p, bct, q, P.mut, L.d_vm, L.n0, sm, fd, P.flux);
-      else if (d == 2) k_rans_vface<2><<<g128, 128, 0, c->s>>>(bl, c->d_p, bct, q, P.mut, L.d_vm, L.n0, sm, fd, P.flux);
-      else k_rans_vface<3><<<g128, 128, 0, c->s>>>(bl, c->d_p, bct, q, P.mut, L.d_vm, L.n0, sm, fd, P.flux);
-    });
-    if (r || (r = cosa_gpu_resid(c, d, nl, P.flux, P.res))) return r;
-  }
-  // cell-centred velocity gradients, production and sources (src/cosa.f90:1878-1896)
-  if ((r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+  // muscl + roflux and q_face / q_der / rtst / vflux of the three families in
+  // one launch, then resid of their sums (src/cosa.f90:1797-1824)
+  if ((r = for_blocks(c, L, cnt_faces, [&](auto b, dim3 g) {
          (void)b;
-         k_rans_qder_c<<<g, 256, 0, c->s>>>(bl, c->d_p, bct, q, P.qp, P.qm, P.dqm, blend(p) ? 7 : 4);
+         const dim3 g6(g.x * 2, g.y, 6);
+         const double *fd = blend(p) ? L.d_fdist : nullptr;
+         if (mixed)
+           k_rans_faces<true><<<g6, 128, 0, c->s>>>(bl, c->d_p, bct, q, nl, P.si, P.sj, P.sk, L.d_h0, P.mut, L.d_vm,
+                                                    L.n0, fd, L.d_rflux);
+         else
+           k_rans_faces<false><<<g6, 128, 0, c->s>>>(bl, c->d_p, bct, q, nl, P.si, P.sj, P.sk, L.d_h0, P.mut, L.d_vm,
+                                                     L.n0, fd, L.d_rflux);
+       })) ||
+      (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+         (void)b;
+         k_rans_resid<<<g, 256, 0, c->s>>>(bl, c->d_p, L.n0, L.d_rflux, P.res);
        })))
     return r;
-  if (nl == 1 || p.prd_all_lvls)
-    if ((r = cosa_gpu_turprod(c, nl, P.qp, P.qm, P.dqm, L.d_vm, L.d_prd, L.d_divvel, L.d_delpls))) return r;
-  if (blend(p)) {
-    // update_ttrm + srckw_sst (src/cosa.f90:1896-1901)
-    if ((r = cosa_gpu_update_ttrm(c, nl, q, P.qp, P.qm, P.dqm, L.d_vm, L.d_ttrm, P.dist)) ||
-        (r = cosa_gpu_srckw_sst(c, nl, q, L.d_prd, L.d_divvel, P.res, P.mut, L.d_ttrm, P.vol)))
-      return r;
-  } else if ((r = cosa_gpu_srckw(c, nl, q, P.mut, L.d_prd, L.d_divvel, P.res, P.vol))) {
+  // cell-centred velocity gradients, production, BSL/SST blending and the
+  // sources in one pass over the cells (src/cosa.f90:1878-1901)
+  if ((r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+         (void)b;
+         if (blend(p))
+           k_rans_cellsrc<true><<<g, 256, 0, c->s>>>(bl, c->d_p, nl, bct, q, P.qp, P.qm, P.dqm, L.d_vm, L.n0, P.mut,
+                                                    P.dist, P.vol, L.d_prd, L.d_divvel, L.d_delpls, L.d_ttrm, P.res);
+         else
+           k_rans_cellsrc<false><<<g, 256, 0, c->s>>>(bl, c->d_p, nl, bct, q, P.qp, P.qm, P.dqm, L.d_vm, L.n0, P.mut,
+                                                     P.dist, P.vol, L.d_prd, L.d_divvel, L.d_delpls, nullptr, P.res);
+       })))
     return r;
-  }
   if ((r = cosa_gpu_prim2cons(c, nl, q))) return r;
   // dual time: src_uns, the norm with rhs_uns, res -= rhs_uns on the fine
   // level (src/cosa.f90:1908-1941)

@@ -728,26 +728,15 @@ __global__ void k_rans_h0(const DevBlock *__restrict__ blocks, int nb, const cos
   }
 }
 
-// muscl + roflux_b of one face family of the k-omega stage in one pass: the
-// reconstructed states stay in registers, the seven face fluxes go to flux
+// muscl + roflux_b of the faces of family D of block b: the reconstructed
+// states stay in registers, the seven convective face fluxes go to F
 template <int D, bool MIXED>
-__global__ void __launch_bounds__(128, 3) k_rans_conv(BlockList bs_, const cosa_params *__restrict__ Pp,
-                                                      const int *__restrict__ bct, const double *__restrict__ q,
-                                                      int nl, const double *__restrict__ s,
-                                                      const double *__restrict__ h0, double *__restrict__ flux) {
-  const DevBlock b = bs_.get();
-  const cosa_params &P = *Pp;
+__device__ __forceinline__ void rans_conv_faces(const DevBlock &b, const cosa_params &P, const int *__restrict__ bct,
+                                                const double *__restrict__ q, int nl, const double *__restrict__ s,
+                                                const double *__restrict__ h0b, double *__restrict__ F) {
   const PhysPar ph = make_phys(P);
   const int npde = P.npde, S = 2 * P.nharms + 1;
-  const int ic = D == 1 ? b.im : b.im - 1, jc = D == 2 ? b.jm : b.jm - 1, kc = D == 3 ? b.km : b.km - 1;
-  const double *h0b = h0 + ((int64_t)blockIdx.y * 3 + (D - 1)) * S * 2;
-  const int64_t total = (int64_t)ic * jc * kc * S;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = t;
-    const int i = (int)(r % ic) + 1; r /= ic;
-    const int j = (int)(r % jc) + 1; r /= jc;
-    const int k = (int)(r % kc) + 1;
-    const int n = (int)(r / kc);
+  KOM_FACE_LOOP(D)
     double vr[7], vl[7], f[5];
     rans_face_recon<MIXED>(b, P, bct, q, D, nl, i, j, k, n, npde, vr, vl);
     const int64_t e4 = p2_idx(b, 1, 1, i, j, k, 0);
@@ -755,26 +744,24 @@ __global__ void __launch_bounds__(128, 3) k_rans_conv(BlockList bs_, const cosa_
     if (MIXED) roe_flux_mixed_tke(ph, kx, ky, kz, ds, vr, vl, vr[5], vl[5], f);
     else roe_flux_fp64(ph, kx, ky, kz, ds, vr, vl, vr[5], vl[5], f);
 #pragma unroll
-    for (int m = 0; m < 5; ++m) flux[f0_idx(b, npde, S, i, j, k, m + 1, n)] = f[m];
+    for (int m = 0; m < 5; ++m) F[f0_idx(b, npde, S, i, j, k, m + 1, n)] = f[m];
     double fk, fw;
     roe_turb(P, kx, ky, kz, ds, vr, vl, h0b[2 * n], h0b[2 * n + 1], fk, fw);
-    flux[f0_idx(b, npde, S, i, j, k, 6, n)] = fk;
-    flux[f0_idx(b, npde, S, i, j, k, 7, n)] = fw;
+    F[f0_idx(b, npde, S, i, j, k, 6, n)] = fk;
+    F[f0_idx(b, npde, S, i, j, k, 7, n)] = fw;
   }
 }
 
-// q_face (+ calmut) / q_der / b_rtst / vflux_b of one face family of the
-// k-omega stage in one pass, added to the convective fluxes in flux: the face
-// state and gradients of the bulk loops, or on strong-BC faces the one-sided
-// wall formulas with the halo mut (src/flux.f90:1848-1962, 2846-2946, 947-1180)
+// q_face (+ calmut) / q_der / b_rtst / vflux_b of the faces of family D of
+// block ib: the face state and gradients of the bulk loops, or on strong-BC
+// faces the one-sided wall formulas with the halo mut (src/flux.f90:1848-1962,
+// 2846-2946, 947-1180); the seven viscous face fluxes go to F
 template <int D>
-__global__ void __launch_bounds__(128, 3) k_rans_vface(BlockList bs_, const cosa_params *__restrict__ Pp,
-                                                       const int *__restrict__ bct, const double *__restrict__ q,
-                                                       const double *__restrict__ mut, const double *__restrict__ vm,
-                                                       int64_t n0, const double *__restrict__ s,
-                                                       const double *__restrict__ fdist, double *__restrict__ flux) {
-  const DevBlock b = bs_.get();
-  const cosa_params &P = *Pp;
+__device__ __forceinline__ void rans_visc_faces(const DevBlock &b, int ib, const cosa_params &P,
+                                                const int *__restrict__ bct, const double *__restrict__ q,
+                                                const double *__restrict__ mut, const double *__restrict__ vm,
+                                                int64_t n0, const double *__restrict__ s,
+                                                const double *__restrict__ fdist, double *__restrict__ F) {
   const int npde = P.npde, S = 2 * P.nharms + 1;
   const ViscPar V = make_visc(P);
   constexpr int di = D == 1, dj = D == 2, dk = D == 3;
@@ -790,7 +777,7 @@ __global__ void __launch_bounds__(128, 3) k_rans_vface(BlockList bs_, const cosa
     } else {
       const int *rw = bct + b.obct + 10 * row;
       WallFace w;
-      w.blk = blockIdx.y; w.d = D; w.inrout = rw[2];
+      w.blk = ib; w.d = D; w.inrout = rw[2];
       w.fi = i; w.fj = j; w.fk = k;
       w.lo[0] = rw[3]; w.lo[1] = rw[5]; w.lo[2] = rw[7];
       w.hi[0] = rw[4]; w.hi[1] = rw[6]; w.hi[2] = rw[8];
@@ -800,51 +787,69 @@ __global__ void __launch_bounds__(128, 3) k_rans_vface(BlockList bs_, const cosa
     }
     double vmf[9];
     load_vm(vm, b, n0, D, i, j, k, vmf);
-    double gr[3][3], t6[6], F[7];
+    double gr[3][3], t6[6], Fv[7];
 #pragma unroll
     for (int m = 0; m < 3; ++m) { gr[m][0] = g[0][m + 1]; gr[m][1] = g[1][m + 1]; gr[m][2] = g[2][m + 1]; }
     rtst_face(P, qf[0], qf[5], gr, vmf, mf, t6);
     const int64_t e4 = p2_idx(b, 1, 1, i, j, k, 0);
     vflux_kom_face(P, V, qf, g, t6, vmf, s[e4], s[e4 + 1], s[e4 + 2], s[e4 + 3], mf,
-                   fdist ? fdist[f0_idx(b, 1, 1, i, j, k, 1, 0)] : -1.0, F);
+                   fdist ? fdist[f0_idx(b, 1, 1, i, j, k, 1, 0)] : -1.0, Fv);
 #pragma unroll
-    for (int m = 1; m < 7; ++m) {
-      const int64_t o = f0_idx(b, npde, S, i, j, k, m + 1, n);
-      flux[o] = flux[o] + F[m];
-    }
+    for (int m = 0; m < 7; ++m) F[f0_idx(b, npde, S, i, j, k, m + 1, n)] = Fv[m];
   }
 }
 
-// q_face (face states only) + q_der_c of the three families in one pass over
-// the cells: dc_d = qf_d(face e+1) - qf_d(face e) for u, v, w (and k, omega
-// when vhi = 7), the face state the bulk average or, on strong-BC faces, the
-// halo value (src/flux.f90:2979-3130)
-__global__ void k_rans_qder_c(BlockList bs_, const cosa_params *__restrict__ Pp, const int *__restrict__ bct,
-                              const double *__restrict__ q, double *__restrict__ dx, double *__restrict__ dy,
-                              double *__restrict__ dz, int vhi) {
+// every face flux of the k-omega stage in one launch: grid (x, block, 6),
+// z = family - 1 for the convective fluxes (muscl + roflux) and 3 + family - 1
+// for the viscous ones, each into its own plane of rf (n0 npde S doubles per
+// plane); fd holds the three families' face wall distances (BSL/SST) or is null
+template <bool MIXED>
+__global__ void __launch_bounds__(128, 3) k_rans_faces(BlockList bs_, const cosa_params *__restrict__ Pp,
+                                                       const int *__restrict__ bct, const double *__restrict__ q,
+                                                       int nl, const double *__restrict__ si,
+                                                       const double *__restrict__ sj, const double *__restrict__ sk,
+                                                       const double *__restrict__ h0, const double *__restrict__ mut,
+                                                       const double *__restrict__ vm, int64_t n0,
+                                                       const double *__restrict__ fd, double *__restrict__ rf) {
+  const DevBlock b = bs_.get();
+  const cosa_params &P = *Pp;
+  const int S = 2 * P.nharms + 1, z = blockIdx.z, d = z % 3 + 1;
+  const double *s = d == 1 ? si : (d == 2 ? sj : sk);
+  double *F = rf + (int64_t)z * n0 * P.npde * S;
+  if (z < 3) {
+    const double *h0b = h0 + ((int64_t)blockIdx.y * 3 + (d - 1)) * S * 2;
+    if (d == 1) rans_conv_faces<1, MIXED>(b, P, bct, q, nl, s, h0b, F);
+    else if (d == 2) rans_conv_faces<2, MIXED>(b, P, bct, q, nl, s, h0b, F);
+    else rans_conv_faces<3, MIXED>(b, P, bct, q, nl, s, h0b, F);
+  } else {
+    const double *fdd = fd ? fd + (int64_t)(d - 1) * n0 : nullptr;
+    if (d == 1) rans_visc_faces<1>(b, blockIdx.y, P, bct, q, mut, vm, n0, s, fdd, F);
+    else if (d == 2) rans_visc_faces<2>(b, blockIdx.y, P, bct, q, mut, vm, n0, s, fdd, F);
+    else rans_visc_faces<3>(b, blockIdx.y, P, bct, q, mut, vm, n0, s, fdd, F);
+  }
+}
+
+// bresid of the three families on the summed convective + viscous face
+// fluxes of k_rans_faces, families in the reference's order (src/cosa.f90:1149-1200)
+__global__ void k_rans_resid(BlockList bs_, const cosa_params *__restrict__ Pp, int64_t n0,
+                             const double *__restrict__ rf, double *__restrict__ res) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int64_t plane = n0 * npde * S;
   KOM_CELL_LOOP
+    const int64_t c = p3_cell(b, i, j, k);
+    for (int v = 1; v <= npde; ++v) {
+      const int64_t o = p3_var(b, npde, S, v, n) + c;
+      double x = res[o];
 #pragma unroll
-    for (int d = 1; d <= 3; ++d) {
-      const int di = d == 1, dj = d == 2, dk = d == 3;
-      const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
-      const int e = d == 1 ? i : (d == 2 ? j : k);
-      const int t2 = d == 1 ? j : i, t3 = d == 3 ? j : k;
-      const bool wlo = strong_row(b, bct, d, e, mx, t2, t3) >= 0;
-      const bool whi = strong_row(b, bct, d, e + 1, mx, t2, t3) >= 0;
-      const int64_t cm = p3_cell(b, i - di, j - dj, k - dk), c0 = p3_cell(b, i, j, k);
-      const int64_t cp = p3_cell(b, i + di, j + dj, k + dk);
-      double *dc = d == 1 ? dx : (d == 2 ? dy : dz);
-      for (int v = 2; v <= vhi; ++v) {
-        if (v == 5) continue;
-        const int64_t o = p3_var(b, npde, S, v, n);
-        const double qm = q[o + cm], q0 = q[o + c0], qp = q[o + cp];
-        const double flo = wlo ? qm : (qm + q0) / 2;
-        const double fhi = whi ? qp : (q0 + qp) / 2;
-        dc[o + c0] = fhi - flo;
+      for (int d = 1; d <= 3; ++d) {
+        const int64_t fp = f0_idx(b, npde, S, i + (d == 1), j + (d == 2), k + (d == 3), v, n);
+        const int64_t fm = f0_idx(b, npde, S, i, j, k, v, n);
+        const double *Fc = rf + (d - 1) * plane, *Fv = rf + (d + 2) * plane;
+        x = x + (Fc[fp] + Fv[fp]) - (Fc[fm] + Fv[fm]);
       }
+      res[o] = x;
     }
   }
 }
@@ -894,5 +899,116 @@ __global__ void k_update_rans(BS bs_, const cosa_params *__restrict__ Pp, const 
     }
     q[i6] = rk;
     q[i7] = rhomega;
+  }
+}
+
+// the cell side of the k-omega stage in one pass over the cells
+// (src/cosa.f90:1878-1901): q_face + q_der_c of the three families (the
+// differences still written to dx, dy, dz), turprod_b on the levels that
+// compute production (else the restricted prd and div u are read), under
+// BSL/SST update_ttrm_b, and srckw_b / srckw_sst_b into res; the state is
+// primitive
+template <bool BLEND>
+__global__ void k_rans_cellsrc(BlockList bs_, const cosa_params *__restrict__ Pp, int nl, const int *__restrict__ bct,
+                               const double *__restrict__ q, double *__restrict__ dx, double *__restrict__ dy,
+                               double *__restrict__ dz, const double *__restrict__ vm, int64_t n0,
+                               const double *__restrict__ mut, const double *__restrict__ dist,
+                               const double *__restrict__ vol, double *__restrict__ prd, double *__restrict__ divvel,
+                               double *__restrict__ delpls, double *__restrict__ ttrm, double *__restrict__ res) {
+  const DevBlock b = bs_.get();
+  const cosa_params &P = *Pp;
+  const int npde = P.npde, S = 2 * P.nharms + 1;
+  constexpr int vhi = BLEND ? 7 : 4;
+  const bool own_prod = nl == 1 || P.prd_all_lvls;
+  const double fact = 2.0 / 3.0, mor = P.machfs / P.reyno;
+  KOM_CELL_LOOP
+    const int64_t c0 = p3_cell(b, i, j, k), o = p3s_idx(b, S, i, j, k, n);
+    // dc[d][v - 2]: differences of u, v, w (and k, omega) across the cell
+    double dc[3][6];
+#pragma unroll
+    for (int d = 1; d <= 3; ++d) {
+      const int di = d == 1, dj = d == 2, dk = d == 3;
+      const int mx = d == 1 ? b.im : (d == 2 ? b.jm : b.km);
+      const int e = d == 1 ? i : (d == 2 ? j : k);
+      const int t2 = d == 1 ? j : i, t3 = d == 3 ? j : k;
+      const bool wlo = strong_row(b, bct, d, e, mx, t2, t3) >= 0;
+      const bool whi = strong_row(b, bct, d, e + 1, mx, t2, t3) >= 0;
+      const int64_t cm = p3_cell(b, i - di, j - dj, k - dk), cp = p3_cell(b, i + di, j + dj, k + dk);
+      double *dd = d == 1 ? dx : (d == 2 ? dy : dz);
+#pragma unroll
+      for (int v = 2; v <= vhi; ++v) {
+        if (v == 5) continue;
+        const int64_t ov = p3_var(b, npde, S, v, n);
+        const double qm = q[ov + cm], qc = q[ov + c0], qp = q[ov + cp];
+        const double flo = wlo ? qm : (qm + qc) / 2;
+        const double fhi = whi ? qp : (qc + qp) / 2;
+        dc[d - 1][v - 2] = fhi - flo;
+        dd[ov + c0] = dc[d - 1][v - 2];
+      }
+    }
+    double met[3][3];
+    if (own_prod || BLEND) cell_met(vm, b, n0, i, j, k, met);
+    double prod, divv;
+    if (own_prod) {
+      // turprod_b (src/src.f90:40-177)
+      double dv[3][3];
+#pragma unroll
+      for (int v = 0; v < 3; ++v)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) dv[v][cc] = dc[0][v] * met[0][cc] + dc[1][v] * met[1][cc] + dc[2][v] * met[2][cc];
+      divv = (dv[0][0] + dv[1][1] + dv[2][2]) * P.turcmp;
+      const double txx = dv[0][0], txy = (dv[0][1] + dv[1][0]) / 2, txz = (dv[0][2] + dv[2][0]) / 2;
+      const double tyy = dv[1][1], tyz = (dv[1][2] + dv[2][1]) / 2, tzz = dv[2][2];
+      prod = 2 * (txx * txx + tyy * tyy + tzz * tzz + 2 * (txy * txy + txz * txz + tyz * tyz) - divv * divv / 3);
+      prd[o] = prod;
+      divvel[o] = divv;
+      delpls[o] = 2.0 / 3.0 * fmax(divv, 0.0);
+    } else {
+      prod = prd[o];
+      divv = divvel[o];
+    }
+    auto Q = [&](int v) { return q[p3_var(b, npde, S, v, n) + c0]; };
+    const double rho = Q(1), tke = Q(6), ome = Q(7);
+    double cdif = 0.0, gav = P.gkw, bav = P.bkw;
+    if (BLEND) {
+      // update_ttrm_b (src/update.f90:3036-3161)
+      const BlendPar cb = make_blend(P);
+      const double tt = P.gamma * Q(5) / rho;
+      const double mu = sutherland(tt, P.stemp);
+      const double tkexi = dc[0][4], tkeeta = dc[1][4], tkezeta = dc[2][4];
+      const double omexi = dc[0][5], omeeta = dc[1][5], omezeta = dc[2][5];
+      const double dtkedx = tkexi * met[0][0] + tkeeta * met[1][0] + tkezeta * met[2][0];
+      const double dtkedy = tkexi * met[0][1] + tkeeta * met[1][1] + tkezeta * met[2][1];
+      const double dtkedz = tkexi * met[0][2] + tkeeta * met[1][2] + tkezeta * met[2][2];
+      const double domedx = omexi * met[0][0] + omeeta * met[1][0] + omezeta * met[2][0];
+      const double domedy = omexi * met[0][1] + omeeta * met[1][1] + omezeta * met[2][1];
+      const double domedz = omexi * met[0][2] + omeeta * met[1][2] + omezeta * met[2][2];
+      double cdt;
+      const double f1 = blend_f1(cb, P, rho, tke, ome, mu, dtkedx * domedx + dtkedy * domedy + dtkedz * domedz,
+                                 dist[p1_idx(b, 1, i, j, k, 0)], cdt);
+      cdif = cdt * (1 - f1);
+      gav = f1 * cb.g1 + (1 - f1) * cb.g2;
+      bav = f1 * cb.b1 + (1 - f1) * cb.b2;
+      ttrm[ttrm_idx(b, S, i, j, k, 1, n)] = cdif;
+      ttrm[ttrm_idx(b, S, i, j, k, 2, n)] = gav;
+      ttrm[ttrm_idx(b, S, i, j, k, 3, n)] = bav;
+    }
+    // srckw_b / srckw_sst_b (src/src.f90:196-378)
+    const double mt = mut[o];
+    double prodk = prod, prodw = prod;
+    if (P.lim_prodtke && own_prod) {
+      const double tstdis = P.prdlim * P.bstrkw * rho * tke * ome;
+      if (mor * mt * prodk > tstdis) {
+        prodk = tstdis / mor / mt;
+        if (P.lim_prodomega) prodw = prodk;
+      }
+    }
+    const double v = vol[p1_idx(b, 1, i, j, k, 0)];
+    double *r6 = res + p3_var(b, npde, S, 6, n) + c0, *r7 = res + p3_var(b, npde, S, 7, n) + c0;
+    *r6 = *r6 - v * (mor * mt * prodk - fact * divv * rho * tke - P.bstrkw * rho * tke * ome);
+    if (BLEND)
+      *r7 = *r7 - v * (gav * P.cmu * rho * prodw - gav * fact * divv * rho * ome - bav * rho * (ome * ome) + cdif);
+    else
+      *r7 = *r7 - v * (P.gkw * P.cmu * rho * prodw - P.gkw * fact * divv * rho * ome - P.bkw * rho * (ome * ome));
   }
 }
