@@ -213,6 +213,7 @@ int cosa_io_default_params(cosa_params *p) {
   p->nstart = p->npre = p->npost = p->ncrs = 1;
   p->bln_prol = 1;
   p->bdf1 = 1;
+  p->cutoff_type = 1;
   return COSA_OK;
 }
 
@@ -494,10 +495,44 @@ int cosa_io_read_input(const char *path, cosa_params *pp, cosa_run_opts *rr, cos
       if ((e = yn(W(line, 4), p.prd_all_lvls))) return e;
     }
   }
-  // low-speed preconditioning
+  // low-speed preconditioning control parameters (src/input.f90:3582-3700)
   L.skip();
   line = L.next();
-  if (W(line, 1) == "lomach") return COSA_ERR_UNSUPPORTED;
+  if (W(line, 1) == "lomach") {
+    p.lomach = 1;
+    if (!inum(W(line, 2), p.cutoff_type) || p.cutoff_type < 1 || p.cutoff_type > 3) return COSA_ERR_ARG;
+    const std::string vp = W(line, 3);
+    if (vp == "viscous") {
+      if (!p.viscous) return COSA_ERR_ARG;
+      p.visprec = 1;
+    } else if (vp == "inviscid") {
+      p.visprec = 0;
+    } else {
+      return COSA_ERR_ARG;
+    }
+    int lsp_vfr = 0;
+    if (p.moving && !unsteady && (!inum(W(line, 4), lsp_vfr) || lsp_vfr < 0 || lsp_vfr > 1)) return COSA_ERR_ARG;
+    if (unsteady) {
+      const std::string mx = W(line, 4);
+      if (mx == "standard") p.mixpi = 0;
+      else if (mx == "mixed") p.mixpi = 1;
+      else return COSA_ERR_ARG;
+      double lx = 0, ly = 0;
+      if (!num(W(line, 5), lx) || !num(W(line, 6), ly)) return COSA_ERR_ARG;
+      // the unsteady reference velocity
+      p.uprv = std::max(lx / (pi * r.dt), ly / (pi * r.dt));
+      if (p.moving && (!inum(W(line, 7), lsp_vfr) || lsp_vfr < 0 || lsp_vfr > 1)) return COSA_ERR_ARG;
+    }
+    // the preconditioner's Mach number in the frame of a moving grid is not built
+    if (lsp_vfr == 1) return COSA_ERR_UNSUPPORTED;
+    // entropy fix type 1 is inadmissible with preconditioning
+    if (p.entfx_f_w[1] == 1 || p.entfx_t_w[1] == 1) return COSA_ERR_ARG;
+    // the constant cut-off of every multigrid level
+    L.skip();
+    line = L.next();
+    for (int l = 0; l < p.nlevel; ++l)
+      if (!num(W(line, l + 1), p.epsp[l])) return COSA_ERR_ARG;
+  }
   if (p.viscous) {
     L.skip();
     line = L.next();
@@ -618,7 +653,10 @@ int cosa_io_read_input(const char *path, cosa_params *pp, cosa_run_opts *rr, cos
     in->ncuts = 2 * nc;
   }
   // compatibility tests (src/input.f90:4235-4275)
-  if ((p.machfs < 1e-14 && p.viscous) || (p.rgkuns && p.nlevel > 1)) return fail(COSA_ERR_ARG);
+  if ((p.machfs < 1e-14 && p.viscous) || (p.rgkuns && p.nlevel > 1) || (p.rgkuns && p.lomach))
+    return fail(COSA_ERR_ARG);
+  // IRS for the removal of the diffusion limit is not available with preconditioning
+  if (p.lomach && (p.irsop == 5 || p.irsop == 6)) return fail(COSA_ERR_ARG);
   if (turb && p.nlevel > 1 && (!p.bln_prol || (!p.prd_all_lvls && p.lim_prodtke && !p.lim_prodomega)))
     return fail(COSA_ERR_ARG);
   // derived CFL values (src/input.f90:4205-4221)
@@ -737,7 +775,18 @@ int cosa_io_write_input(const char *path, const cosa_params *pp, const cosa_run_
                            p.prd_all_lvls ? "y" : "n");
     std::fprintf(f, "\n");
   }
-  std::fprintf(f, "preconditioning\nnone\n");
+  if (p.lomach) {
+    std::fprintf(f, "preconditioning\nlomach %d %s", p.cutoff_type, p.visprec ? "viscous" : "inviscid");
+    if (p.harbal || p.dualt || p.rgkuns) {
+      const double l = p.uprv * pi * r.dt;
+      std::fprintf(f, " %s %.17g %.17g", p.mixpi ? "mixed" : "standard", l, l);
+    }
+    std::fprintf(f, "\nepsp\n");
+    for (int l = 0; l < p.nlevel; ++l) std::fprintf(f, "%s%.17g", l ? " " : "", p.epsp[l]);
+    std::fprintf(f, "\n");
+  } else {
+    std::fprintf(f, "preconditioning\nnone\n");
+  }
   if (p.viscous) std::fprintf(f, "tref\n%.17g\n", 110.4 / p.stemp);
   std::fprintf(f, "dgn_cell wri_res wri_tec\n%s %s %s\n", r.dgn_cell ? "y" : "n", r.wri_res ? "y" : "n",
                r.wri_tec ? "y" : "n");

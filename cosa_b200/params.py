@@ -15,6 +15,7 @@ import math
 import numpy as np
 
 MAX_SNAP = 15
+MAX_LEVELS = 3
 
 PREC_FP64 = 0
 PREC_MIXED = 1
@@ -66,6 +67,8 @@ class CosaParams(C.Structure):
         ("turcmp", C.c_double), ("prdlim", C.c_double), ("roughk", C.c_double),
         ("dtheta0", C.c_double), ("omegas", C.c_double), ("xh", C.c_double), ("yh", C.c_double),
         ("dt", C.c_double), ("bdf1", C.c_int32), ("reserved_t", C.c_int32),
+        ("lomach", C.c_int32), ("cutoff_type", C.c_int32), ("visprec", C.c_int32), ("mixpi", C.c_int32),
+        ("uprv", C.c_double), ("epsp", C.c_double * MAX_LEVELS),
     ]
 
 
@@ -125,6 +128,22 @@ def default_params() -> CosaParams:
     p.lim_corr = 0
     # time-accurate runs start with a first-order step (src/src.f90:420-432)
     p.bdf1 = 1
+    # low-speed preconditioning off; cut-off type 1 (none) when switched on
+    p.cutoff_type = 1
+    return p
+
+
+def set_low_speed(p: CosaParams, cutoff_type: int = 2, visprec: bool = False, epsp=(1.0e-5, 1.0e-5, 1.0e-5),
+                  mixpi: int = 0, uprv: float = 0.0) -> CosaParams:
+    """Switch on low-speed preconditioning (the input file's `lomach`
+    line and its constant cut-offs per level, src/input.f90:3585-3700)."""
+    p.lomach = 1
+    p.cutoff_type = cutoff_type
+    p.visprec = 1 if visprec else 0
+    p.mixpi = mixpi
+    p.uprv = uprv
+    for i in range(MAX_LEVELS):
+        p.epsp[i] = epsp[min(i, len(epsp) - 1)]
     return p
 
 

@@ -122,6 +122,16 @@ typedef struct cosa_params {
      (itime = 1 and not dual_prop_start: first-order backward difference) */
   double dt;
   int32_t bdf1, reserved_t;
+  /* low-speed preconditioning, lomach = 1 (src/losp.f90, src/flux.f90:390-830,
+     src/input.f90:3585-3700): cutoff_type 1 no pressure-gradient cut-off,
+     2 lm_cutoff_pg on every level, 3 on the fine level and restricted
+     (rest3) to the coarse ones; visprec 1 adds the viscous cut-off
+     lm_viscoff (viscous runs); mixpi 0 standard, 1 mixed preconditioner;
+     uprv the unsteady reference velocity (0 in steady runs); epsp[nl-1] the
+     constant cut-off of level nl */
+  int32_t lomach, cutoff_type, visprec, mixpi;
+  double uprv;
+  double epsp[COSA_MAX_LEVELS];
 } cosa_params;
 
 /*

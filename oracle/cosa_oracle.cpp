@@ -199,6 +199,8 @@ inline double pow4(double x) { const double x2 = x * x; return x2 * x2; }
 inline double tanh_ref(double a) { return (std::exp(2 * a) - 1) / (std::exp(2 * a) + 1); }
 
 // ---- cons2prim_b (src/update.f90:2135-2188) --------------------------------
+#include "lsp_oracle.inc"
+
 void cons2prim_b(const Level &L, int b, double *qa, int xtnd, const cosa_params &P) {
   B3 q(qa, L, b);
   const int im = L.im[b], jm = L.jm[b], km = L.km[b];
@@ -364,7 +366,7 @@ void bc_walinv_14(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &
 // bc_insub (src/bc.f90:875-1175); total state and direction are parameters
 // whose defaults are the reference's hard-wired values.
 int bc_insub(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
-             const Level &L, const cosa_params &P) {
+             const Level &L, const cosa_params &P, int nl = 1) {
   int status = 0;
   int ibcpt, ibcpt2, ibcn, ibcn2, ibcm;
   double sgnm;
@@ -392,6 +394,19 @@ int bc_insub(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
           double un2 = u2 * nx + v2 * ny + w2 * nz;
           double rc1 = std::sqrt(g * p1 * rho1);
           double rc2 = std::sqrt(g * p2 * rho2);
+          if (P.lomach) {
+            // the preconditioned outgoing characteristic (src/bc.f90:1032-1056)
+            auto rc_lsp = [&](double rho_, double u_, double v_, double w_, double p_, double un_) {
+              const double q2 = u_ * u_ + v_ * v_ + w_ * w_, a2 = g * p_ / rho_, a = std::sqrt(a2);
+              const double ump2 = (P.uprv / a) * (P.uprv / a);
+              const double mp2 = std::min(std::max(std::max(q2 / a2, ump2), lsp_eps2(P, nl)), 1.0);
+              const double lp3 = 0.5 * (un_ * (1. + mp2) + std::sqrt(un_ * un_ * ((1. - mp2) * (1. - mp2)) + 4. * a2 * mp2));
+              const double esse = un_ - lp3;
+              return -(rho_ * esse);
+            };
+            rc1 = rc_lsp(rho1, u1, v1, w1, p1, un1);
+            rc2 = rc_lsp(rho2, u2, v2, w2, p2, un2);
+          }
           double rcun1 = rc1 * un1, rcun2 = rc2 * un2;
           double p, un, rc, rcun;
           if (icell == 1) {
@@ -524,6 +539,27 @@ void bc_outsub(const Patch &pa, B3 &q, const Level &L, const cosa_params &P) {
 // bc_far0 (src/bc.f90:124-483), fixed grid, aircraft free stream
 void bc_far0(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
              const Level &L, const cosa_params &P) {
+  if (P.lomach) {
+    // low-speed preconditioning: both halo layers frozen at the free stream
+    // (src/bc.f90:264-276, 409-414)
+    int ibcpt, ibcpt2;
+    if (pa.inrout == 1) { ibcpt = 0; ibcpt2 = -1; }
+    else { ibcpt = pa.ijk[pa.idir]; ibcpt2 = ibcpt + 1; }
+    const double qf[6] = {0.0, P.rhoinf, P.machfs * std::cos(P.alpha) * std::cos(P.beta),
+                          P.machfs * std::sin(P.alpha) * std::cos(P.beta), P.machfs * std::sin(P.beta), P.pinf};
+    for (int n = 0; n < L.S; ++n)
+      for (int i3 = pa.istrt[pa.ic3]; i3 <= pa.iend[pa.ic3]; ++i3)
+        for (int i2 = pa.istrt[pa.ic2]; i2 <= pa.iend[pa.ic2]; ++i2) {
+          int a, bb, c, a2, b2, c2;
+          pidx(pa, ibcpt, i2, i3, a, bb, c); pidx(pa, ibcpt2, i2, i3, a2, b2, c2);
+          for (int v = 1; v <= 5; ++v) { q(a, bb, c, v, n) = qf[v]; q(a2, b2, c2, v, n) = q(a, bb, c, v, n); }
+          if (is_kom(P)) {
+            q(a, bb, c, 6, n) = P.tkefar; q(a, bb, c, 7, n) = P.omefar;
+            q(a2, b2, c2, 6, n) = q(a, bb, c, 6, n); q(a2, b2, c2, 7, n) = q(a, bb, c, 7, n);
+          }
+        }
+    return;
+  }
   int ibcpt, ibcpt2, ibcn, ibcm;
   double sgnm;
   if (pa.inrout == 1) { ibcpt = 0; ibcpt2 = -1; ibcn = 1; ibcm = 1; sgnm = -1.0; }
@@ -604,7 +640,7 @@ void bc_far0(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
 // the average of the interior and free-stream states plus the acoustic
 // jump, the density from the isentrope of the upwind side
 void bc_far1(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
-             const Level &L, const cosa_params &P) {
+             const Level &L, const cosa_params &P, int nl = 1) {
   int ibcpt, ibcpt2, ibcn, ibcm;
   double sgnm;
   if (pa.inrout == 1) { ibcpt = 0; ibcpt2 = -1; ibcn = 1; ibcm = 1; sgnm = -1.0; }
@@ -631,8 +667,21 @@ void bc_far1(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const B2 &sk,
         const double pext = q(an, bn, cn, 5, n), pinf = qfst[5];
         const double rhoext = q(an, bn, cn, 1, n);
         const double a_ = std::sqrt(g * pext / rhoext);
-        const double unb = (qext + qinf) / 2 + (pext - pinf) / (2 * rhoext * a_);
-        const double pb = (pext + pinf) / 2 + rhoext * a_ * (qext - qinf) / 2;
+        double unb = (qext + qinf) / 2 + (pext - pinf) / (2 * rhoext * a_);
+        double pb = (pext + pinf) / 2 + rhoext * a_ * (qext - qinf) / 2;
+        if (P.lomach) {
+          // preconditioned characteristics with the artificial sound speed
+          // apr (src/bc.f90:638-667)
+          const double u1 = q(an, bn, cn, 2, n), v1 = q(an, bn, cn, 3, n), w1 = q(an, bn, cn, 4, n);
+          const double q2 = u1 * u1 + v1 * v1 + w1 * w1;
+          const double a2 = g * pext / rhoext, a = std::sqrt(a2), un = qext;
+          const double m2 = q2 / a2, ump2 = (P.uprv / a) * (P.uprv / a);
+          const double mp2s = std::min(1.0, std::max(std::max(m2, (1 - P.mixpi) * ump2), lsp_eps2(P, nl)));
+          const double am = (1 - mp2s) / 2;
+          const double apr = std::sqrt(am * am * (un * un) + a2 * mp2s);
+          unb = (qext + qinf) / 2 + (pext - pinf) / (2 * rhoext * apr) + (qext - qinf) / 2 * am * un / apr;
+          pb = (pext + pinf) / 2 + rhoext * mp2s * a2 / apr * (qext - qinf) / 2 - (pext - pinf) / 2 * am * un / apr;
+        }
         const double mach = unb / a_;
         double out[6];
         bool set = true;
@@ -682,7 +731,7 @@ void bc_walvis_15_kom(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const 
 // bbc dispatch (src/bc.f90:35-121): patches in table order; dist (wall
 // distance, P1) is read by the k-omega wall
 int bc_level(const Level &L, double *qa, const double *si, const double *sj, const double *sk,
-             const cosa_params &P, const double *dist = nullptr) {
+             const cosa_params &P, const double *dist = nullptr, int nl = 1) {
   int status = 0;
 #pragma omp parallel for reduction(| : status) schedule(dynamic)
   for (int b = 0; b < L.nb; ++b) {
@@ -696,9 +745,9 @@ int bc_level(const Level &L, double *qa, const double *si, const double *sj, con
         case 80: bc_sym(pa, q, L); break;
         case 4: bc_extrapol(pa, q, L); break;
         case 30: bc_far0(pa, q, vi, vj, vk, L, P); break;
-        case 31: bc_far1(pa, q, vi, vj, vk, L, P); break;
+        case 31: bc_far1(pa, q, vi, vj, vk, L, P, nl); break;
         case 14: bc_walinv_14(pa, q, vi, vj, vk, L, P); break;
-        case 21: status |= bc_insub(pa, q, vi, vj, vk, L, P); break;
+        case 21: status |= bc_insub(pa, q, vi, vj, vk, L, P, nl); break;
         case 91: bc_outsub(pa, q, L, P); break;
         default:
           if (pa.bctyp / 100 == 15 && (!P.moving || !is_kom(P)) && (!is_kom(P) || dist)) {
@@ -778,8 +827,27 @@ int prtest_level(const Level &L, const double *qa, const cosa_params &P) {
 }
 
 // ---- lambdab + eig_eul (src/cosa.f90:1248-1330, 4183-4233), inviscid -------
+// preconditioned spectral radii of eig_eul_p / eig_ns_p (src/cosa.f90:4300-
+// 4460): the convective lambdas of the low-speed preconditioned system
+inline void lsp_lambdas(const cosa_params &P, int nl, double u, double v, double w, double a, double cutoff,
+                        double xix, double xiy, double xiz, double etax, double etay, double etaz, double zetax,
+                        double zetay, double zetaz, double axi, double aeta, double azeta, double *lam) {
+  const double q2 = u * u + v * v + w * w, a2 = a * a;
+  const double ump2 = (P.uprv / a) * (P.uprv / a);
+  const double mp2 = std::min(std::max(std::max(std::max(q2 / a2, ump2), cutoff), lsp_eps2(P, nl)), 1.0);
+  const double ui = u * xix + v * xiy + w * xiz, uj = u * etax + v * etay + w * etaz;
+  const double uk = u * zetax + v * zetay + w * zetaz;
+  lam[0] = ((1 + mp2) * std::fabs(ui) + std::sqrt(ui * ui * ((1 - mp2) * (1 - mp2)) + 4 * a2 * mp2 * (axi * axi))) / 2;
+  lam[1] = ((1 + mp2) * std::fabs(uj) + std::sqrt(uj * uj * ((1 - mp2) * (1 - mp2)) + 4 * a2 * mp2 * (aeta * aeta))) / 2;
+  lam[2] =
+      ((1 + mp2) * std::fabs(uk) + std::sqrt(uk * uk * ((1 - mp2) * (1 - mp2)) + 4 * a2 * mp2 * (azeta * azeta))) / 2;
+}
+
+// lambdab (src/cosa.f90:1309-1590), inviscid; with low-speed
+// preconditioning (cpg, cvs: the level's cut-offs, nl its index) eig_eul_p
 void lambda_level(const Level &L, const double *qa, const double *si, const double *sj,
-                  const double *sk, double *lam, const cosa_params &P) {
+                  const double *sk, double *lam, const cosa_params &P, const double *cpga = nullptr,
+                  const double *cvsa = nullptr, int nl = 1) {
   for (int b = 0; b < L.nb; ++b) {
     B3 q(const_cast<double *>(qa), L, b), lm(lam, L, b);
     B2 vi(si, L, b), vj(sj, L, b), vk(sk, L, b);
@@ -816,6 +884,14 @@ void lambda_level(const Level &L, const double *qa, const double *si, const doub
               u = u - BGs(L.cv[0], L, b, nh)(i, j, k);
               v = v - BGs(L.cv[1], L, b, nh)(i, j, k);
               w = w - BGs(L.cv[2], L, b, nh)(i, j, k);
+            }
+            if (P.lomach && cpga) {
+              B1m cpg(const_cast<double *>(cpga), L, b), cvs(const_cast<double *>(cvsa), L, b);
+              double l3[3];
+              lsp_lambdas(P, nl, u, v, w, a, std::max(cpg(i, j, k, n), cvs(i, j, k, n)), xix, xiy, xiz, etax, etay,
+                          etaz, zetax, zetay, zetaz, axi, aeta, azeta, l3);
+              for (int c = 0; c < 3; ++c) lm(i, j, k, c + 1, n) = l3[c];
+              continue;
             }
             lm(i, j, k, 1, n) = std::fabs(u * xix + v * xiy + w * xiz) + a * axi;
             lm(i, j, k, 2, n) = std::fabs(u * etax + v * etay + w * etaz) + a * aeta;
@@ -1191,6 +1267,7 @@ void resid_b(const Level &L, int b, int d, double *fa, double *ra) {
           for (int i = 1; i <= im - 1; ++i)
             res(i, j, k, v, n) = res(i, j, k, v, n) + flux(i + oi, j + oj, k + ok, v, n) - flux(i, j, k, v, n);
 }
+
 
 // ---- update_b explicit, non-k-omega (src/update.f90:568-640) ---------------
 void update_b(const Level &L, int b, double *ra, double *qa, double *qoa, double *dta, double ar) {
@@ -2828,7 +2905,8 @@ void bc_walvis_15(const Patch &pa, B3 &q, const Level &L, const cosa_params &P) 
 // neighbour temperatures on the + side use rho of the - side, as the
 // reference does
 void lambda_ns_level(const Level &L, const double *qa, const double *si, const double *sj, const double *sk,
-                     const double *va, const double *muta, double *lam, double *lamv, const cosa_params &P) {
+                     const double *va, const double *muta, double *lam, double *lamv, const cosa_params &P,
+                     const double *cpga = nullptr, const double *cvsa = nullptr, int nl = 1) {
   const double g = P.gamma, st = P.stemp;
   for (int b = 0; b < L.nb; ++b) {
     B3 q(const_cast<double *>(qa), L, b), lm(lam, L, b), lv(lamv, L, b);
@@ -2876,9 +2954,17 @@ void lambda_ns_level(const Level &L, const double *qa, const double *si, const d
             const double zetay = 0.5 * (skm[2] * skm[4] + skp[2] * skp[4]);
             const double zetaz = 0.5 * (skm[3] * skm[4] + skp[3] * skp[4]);
             const double axi = (sim[4] + sip[4]) / 2, aeta = (sjm[4] + sjp[4]) / 2, azeta = (skm[4] + skp[4]) / 2;
-            lm(i, j, k, 1, n) = std::fabs(u * xix + v * xiy + w * xiz) + a * axi;
-            lm(i, j, k, 2, n) = std::fabs(u * etax + v * etay + w * etaz) + a * aeta;
-            lm(i, j, k, 3, n) = std::fabs(u * zetax + v * zetay + w * zetaz) + a * azeta;
+            if (P.lomach && cpga) {
+              B1m cpg(const_cast<double *>(cpga), L, b), cvs(const_cast<double *>(cvsa), L, b);
+              double l3[3];
+              lsp_lambdas(P, nl, u, v, w, a, std::max(cpg(i, j, k, n), cvs(i, j, k, n)), xix, xiy, xiz, etax, etay,
+                          etaz, zetax, zetay, zetaz, axi, aeta, azeta, l3);
+              for (int c = 0; c < 3; ++c) lm(i, j, k, c + 1, n) = l3[c];
+            } else {
+              lm(i, j, k, 1, n) = std::fabs(u * xix + v * xiy + w * xiz) + a * axi;
+              lm(i, j, k, 2, n) = std::fabs(u * etax + v * etay + w * etaz) + a * aeta;
+              lm(i, j, k, 3, n) = std::fabs(u * zetax + v * zetay + w * zetaz) + a * azeta;
+            }
             const double volc = vol(i, j, k), cm = P.cdff;
             lv(i, j, k, 1, n) = cm * axi * axi * g * P.machfs / P.reyno * (mud[0] / P.pranl + mutd[0] / P.prant) /
                                 (rho * volc);
@@ -3699,7 +3785,22 @@ void force_level(const Level &L, const double *qa, const double *xa, const doubl
 // ============================================================================
 // extern "C" surface used by tests/ (ctypes)
 // ============================================================================
-struct orc_level { Level L; };
+// a level of the oracle: the block tables and the level's low-speed
+// cut-offs (p_cutoff_pgr / p_cutoff_vis of the reference, interior layout x S)
+struct orc_level {
+  Level L;
+  std::vector<double> cut_pgr, cut_vis;
+  int nl = 1;  // the level's index in the multigrid drivers
+};
+
+// rest3 of the low-speed cut-offs in restrict (src/cosa.f90:2724-2731)
+void lsp_restrict(orc_level *f, orc_level *c, const cosa_params *p, const double *vol1, const double *vol2) {
+  if (!p->lomach) return;
+  for (int b = 0; b < f->L.nb; ++b) {
+    if (p->cutoff_type == 3) rest3_b(f->L, c->L, b, f->cut_pgr.data(), c->cut_pgr.data(), vol1, vol2);
+    if (p->visprec) rest3_b(f->L, c->L, b, f->cut_vis.data(), c->cut_vis.data(), vol1, vol2);
+  }
+}
 
 extern "C" {
 
@@ -3722,6 +3823,8 @@ orc_level *orc_level_new(const cosa_level_desc *d, int npde, int nharms) {
     ab += 10 * d->nbcs[b];
   }
   L.n3 = a3; L.n2 = a2; L.n1 = a1; L.n0 = a0; L.nm1 = am;
+  h->cut_pgr.assign((size_t)am * L.S, 0.0);
+  h->cut_vis.assign((size_t)am * L.S, 0.0);
   L.bct.assign(d->bctopo, d->bctopo + ab);
   L.ncuts = d->ncuts;
   L.cut.assign(d->cutopo, d->cutopo + 21 * d->ncuts);
@@ -3828,7 +3931,7 @@ void orc_roe_face(const cosa_params *p, const double *nrm, const double *qr, con
 int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
                   const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
                   double *dqp, double *dqm, double *flux, double *dtvol, int want_dt, double *bx, double *by,
-                  double *bz, const double *vol = nullptr, const double *vm = nullptr);
+                  double *bz, const double *vol = nullptr, const double *vm = nullptr, int to_coarse = 0);
 
 // arrays of the viscous / k-omega residual beyond cosa_level_ptrs: the face
 // inverse metrics, production, div u, delta+ and the turbulence IRS
@@ -3839,6 +3942,7 @@ struct VExtra {
   double *tbx, *tby, *tbz;
   double *ttrm;         // BSL/SST: (cdif, gamma, beta) per cell, P3 x 3 x S
   const double *fdist;  // BSL/SST: face wall distances, families 1..3 at 0, n0, 2 n0
+  int to_coarse;        // smooth()'s to_coarse (the fine-level cut-offs of low-speed preconditioning)
 };
 int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_ptrs &A, const VExtra &X,
                   int want_dt, bool mut_first = false);
@@ -3853,7 +3957,7 @@ int orc_residual(orc_level *h, const cosa_params *p, int nl, double *q, const do
 int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const double *si,
                   const double *sj, const double *sk, double *res, double *qp, double *qm, double *dq,
                   double *dqp, double *dqm, double *flux, double *dtvol, int want_dt, double *bx, double *by,
-                  double *bz, const double *vol, const double *vm) {
+                  double *bz, const double *vol, const double *vm, int to_coarse) {
   cosa_level_ptrs A{};
   A.q = q; A.res = res; A.dtvol = dtvol;
   A.si = const_cast<double *>(si); A.sj = const_cast<double *>(sj); A.sk = const_cast<double *>(sk);
@@ -3862,6 +3966,7 @@ int residual_impl(orc_level *h, const cosa_params *p, int nl, double *q, const d
   A.betaxi = bx; A.betaeta = by; A.betazeta = bz;
   VExtra X{};
   X.vm = vm;
+  X.to_coarse = to_coarse;
   return residual_full(h, p, nl, A, X, want_dt);
 }
 
@@ -3880,9 +3985,11 @@ int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_p
   if (visc && (!A.vol || !X.vm)) return COSA_ERR_ARG;
   if (kom && (!visc || !A.mut || !A.dist || !A.dtvolt || !X.prd || !X.divvel || !X.delpls)) return COSA_ERR_ARG;
   if (blend && (!X.ttrm || !X.fdist)) return COSA_ERR_ARG;
+  // low-speed preconditioning of k-omega runs (ipkpi of update_lsp_b) is not restated
+  if (p->lomach && (kom || p->rkimp)) return COSA_ERR_UNSUPPORTED;
   double *q = A.q;
   for (int b = 0; b < L.nb; ++b) cons2prim_b(L, b, q, 0, *p);
-  int status = bc_level(L, q, A.si, A.sj, A.sk, *p, A.dist);
+  int status = bc_level(L, q, A.si, A.sj, A.sk, *p, A.dist, nl);
   cutman_q_level(L, q);
   if (mut_first) {
     // coarse-level mut from the restricted (primitive) state at the first
@@ -3906,13 +4013,23 @@ int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_p
     cutman_mut_level(L, A.mut);
   }
   status |= prtest_level(L, q, *p);
+  const double *cpg = p->lomach ? h->cut_pgr.data() : nullptr, *cvs = p->lomach ? h->cut_vis.data() : nullptr;
+  if (p->lomach) {
+    // Darmofal's pressure-gradient cut-off (every level, or the fine level
+    // of a cycle that restricts) and the viscous cut-off (src/cosa.f90:1763-1778)
+    const bool fine = (p->nlevel > 1 && nl == 1 && X.to_coarse) || p->nlevel == 1;
+    if ((p->cutoff_type == 3 && fine) || p->cutoff_type == 2)
+      for (int b = 0; b < L.nb; ++b) lm_bcutoff_pg(L, b, q, h->cut_pgr.data(), *p);
+    if (p->visprec && fine)
+      for (int b = 0; b < L.nb; ++b) lm_bviscoff(L, b, q, A.si, A.sj, A.sk, h->cut_vis.data(), *p);
+  }
   if (want_dt) {
     if (visc) {
-      lambda_ns_level(L, q, A.si, A.sj, A.sk, A.vol, kom ? A.mut : nullptr, A.qp, A.dq, *p);
+      lambda_ns_level(L, q, A.si, A.sj, A.sk, A.vol, kom ? A.mut : nullptr, A.qp, A.dq, *p, cpg, cvs, nl);
       deltat_ns_level(L, A.dtvol, A.qp, A.dq, A.betaxi, A.betaeta, A.betazeta, *p, kom ? A.dtvolt : nullptr,
                       kom ? X.tbx : nullptr, kom ? X.tby : nullptr, kom ? X.tbz : nullptr);
     } else {
-      lambda_level(L, q, A.si, A.sj, A.sk, A.qp, *p);
+      lambda_level(L, q, A.si, A.sj, A.sk, A.qp, *p, cpg, cvs, nl);
       deltat_level(L, A.dtvol, A.qp, A.betaxi, A.betaeta, A.betazeta, *p);
     }
   }
@@ -3923,7 +4040,12 @@ int residual_full(orc_level *h, const cosa_params *p, int nl, const cosa_level_p
   for (int d = 1; d <= 3; ++d) {
 #pragma omp parallel for schedule(dynamic)
     for (int b = 0; b < L.nb; ++b) muscl_b(L, b, d, nl, q, A.qp, A.qm, A.dq, A.dqp, A.dqm, *p);
-    for (int b = 0; b < L.nb; ++b) roflux_b(L, b, d, A.qp, A.qm, A.flux, sd[d], *p);
+    if (p->lomach) {
+#pragma omp parallel for schedule(dynamic)
+      for (int b = 0; b < L.nb; ++b) proflux_b(L, b, d, nl, A.qp, A.qm, A.flux, sd[d], cpg, cvs, *p);
+    } else {
+      for (int b = 0; b < L.nb; ++b) roflux_b(L, b, d, A.qp, A.qm, A.flux, sd[d], *p);
+    }
 #pragma omp parallel for schedule(dynamic)
     for (int b = 0; b < L.nb; ++b) resid_b(L, b, d, A.flux, A.res);
     if (visc) {
@@ -4007,6 +4129,7 @@ int orc_smooth(orc_level *h, const cosa_params *p, int ncycles, int mgit0, int r
       if (irk == 1 && (mgit == 1 || mgit % rms_every == 0 || mgit == last) && hist) {
         resg_rms_level(L, res, rhs, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
       }
+      if (p->lomach) lsp_precres_level(L, 1, q, res, h->cut_pgr.data(), h->cut_vis.data(), *p);
 #pragma omp parallel for schedule(dynamic)
       for (int b = 0; b < L.nb; ++b) update_b(L, b, res, q, qold, dtvol, p->alphas[irk - 1]);
     }
@@ -4030,6 +4153,7 @@ int orc_smooth_irs(orc_level *h, const cosa_params *p, int ncycles, int mgit0, i
       status |= residual_impl(h, p, 1, q, si, sj, sk, res, qp, qm, dq, dqp, dqm, flux, dtvol, want_dt, bx, by, bz);
       if (irk == 1 && (mgit == 1 || mgit % rms_every == 0 || mgit == last) && hist)
         resg_rms_level(L, res, rhs, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
+      if (p->lomach) lsp_precres_level(L, 1, q, res, h->cut_pgr.data(), h->cut_vis.data(), *p);
       if (p->irsop > 0) irs_level(L, res, dtvol, nullptr, bx, by, bz, nullptr, nullptr, nullptr, *p);
 #pragma omp parallel for schedule(dynamic)
       for (int b = 0; b < L.nb; ++b) update_b(L, b, res, q, qold, dtvol, p->alphas[irk - 1]);
@@ -4069,6 +4193,7 @@ int orc_smooth_hb(orc_level *h, const cosa_params *p, int ncycles, int mgit0, in
         if (!src_in_res) resg_rms_hbimp_level(L, res, q, vol, *p, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
         else resg_rms_hb_level(L, res, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
       }
+      if (p->lomach) lsp_precres_level(L, 1, q, res, h->cut_pgr.data(), h->cut_vis.data(), *p);
       if (p->irsop > 0) irs_level(L, res, dtvol, nullptr, bx, by, bz, nullptr, nullptr, nullptr, *p);
 #pragma omp parallel for schedule(dynamic)
       for (int b = 0; b < L.nb; ++b) {
@@ -4081,6 +4206,80 @@ int orc_smooth_hb(orc_level *h, const cosa_params *p, int ncycles, int mgit0, in
 }
 
 void orc_lu_solve(int n, double *a, double *b, int nrhs) { lu_solve(n, a, b, nrhs); }
+
+// ---- low-speed preconditioning, per routine (src/losp.f90, src/flux.f90:390-830) ----
+// cut-off arrays in the interior-cell layout (off_m1 x S); q primitive
+void orc_lm_cutoff_pg(orc_level *h, const cosa_params *p, const double *q, double *cut) {
+  for (int b = 0; b < h->L.nb; ++b) lm_bcutoff_pg(h->L, b, q, cut, *p);
+}
+void orc_lm_viscoff(orc_level *h, const cosa_params *p, const double *q, const double *si, const double *sj,
+                    const double *sk, double *cut) {
+  for (int b = 0; b < h->L.nb; ++b) lm_bviscoff(h->L, b, q, si, sj, sk, cut, *p);
+}
+void orc_proflux(orc_level *h, const cosa_params *p, int idir, int nl, double *qr, double *ql, double *flux,
+                 const double *sijk, const double *cpg, const double *cvs) {
+  for (int b = 0; b < h->L.nb; ++b) proflux_b(h->L, b, idir, nl, qr, ql, flux, sijk, cpg, cvs, *p);
+}
+// prec (imax-1, jmax-1, kmax-1, npde, npde, 0:S-1) per block at off_m1 npde^2 S,
+// from the conservative state
+void orc_lsp_prec(orc_level *h, const cosa_params *p, int nl, const double *q, const double *cpg, const double *cvs,
+                  double *prec) {
+  const Level &L = h->L;
+  const int npde = L.npde;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 qv(const_cast<double *>(q), L, b);
+    B1m cp(const_cast<double *>(cpg), L, b), cv(const_cast<double *>(cvs), L, b);
+    const int64_t nc = (int64_t)(L.im[b] - 1) * (L.jm[b] - 1) * (L.km[b] - 1);
+    double *pb = prec + L.om1[b] * npde * npde * L.S;
+    for (int n = 0; n < L.S; ++n)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            double qc[8], pm[49];
+            for (int v = 1; v <= npde; ++v) qc[v] = qv(i, j, k, v, n);
+            lsp_prec_cell(*p, nl, npde, qc, cp(i, j, k, n), cv(i, j, k, n), pm);
+            const int64_t c = (i - 1) + (int64_t)(L.im[b] - 1) * ((j - 1) + (int64_t)(L.jm[b] - 1) * (k - 1));
+            for (int r = 1; r <= npde; ++r)
+              for (int cc = 1; cc <= npde; ++cc)
+                pb[(((int64_t)n * npde + (cc - 1)) * npde + (r - 1)) * nc + c] = pm[(r - 1) * npde + (cc - 1)];
+          }
+  }
+}
+// precres / prec_bres (src/cosa.f90:2446-2521): res <- prec res
+void orc_precres(orc_level *h, double *res, const double *prec) {
+  const Level &L = h->L;
+  const int npde = L.npde;
+  for (int b = 0; b < L.nb; ++b) {
+    B3 r(res, L, b);
+    const int64_t nc = (int64_t)(L.im[b] - 1) * (L.jm[b] - 1) * (L.km[b] - 1);
+    const double *pb = prec + L.om1[b] * npde * npde * L.S;
+    for (int n = 0; n < L.S; ++n)
+      for (int k = 1; k <= L.km[b] - 1; ++k)
+        for (int j = 1; j <= L.jm[b] - 1; ++j)
+          for (int i = 1; i <= L.im[b] - 1; ++i) {
+            const int64_t c = (i - 1) + (int64_t)(L.im[b] - 1) * ((j - 1) + (int64_t)(L.jm[b] - 1) * (k - 1));
+            double w[8];
+            for (int a = 1; a <= npde; ++a) {
+              w[a] = 0.0;
+              for (int cc = 1; cc <= npde; ++cc)
+                w[a] = w[a] + pb[(((int64_t)n * npde + (cc - 1)) * npde + (a - 1)) * nc + c] * r(i, j, k, cc, n);
+            }
+            for (int a = 1; a <= npde; ++a) r(i, j, k, a, n) = w[a];
+          }
+  }
+}
+void orc_rest3(orc_level *f, orc_level *c, const double *c1, double *c2, const double *vol1, const double *vol2) {
+  for (int b = 0; b < f->L.nb; ++b) rest3_b(f->L, c->L, b, c1, c2, vol1, vol2);
+}
+// the level's own cut-off arrays (what smooth() computes and restricts)
+void orc_get_cutoffs(orc_level *h, double *pgr, double *vis) {
+  std::copy(h->cut_pgr.begin(), h->cut_pgr.end(), pgr);
+  std::copy(h->cut_vis.begin(), h->cut_vis.end(), vis);
+}
+void orc_set_cutoffs(orc_level *h, const double *pgr, const double *vis) {
+  std::copy(pgr, pgr + h->cut_pgr.size(), h->cut_pgr.begin());
+  std::copy(vis, vis + h->cut_vis.size(), h->cut_vis.begin());
+}
 
 void orc_src_uns(orc_level *h, const cosa_params *p, const double *q, const double *vol, double *res) {
   src_uns_level(h->L, q, vol, res, *p);
@@ -4173,6 +4372,7 @@ int orc_restrict(orc_level *f, orc_level *c, const cosa_params *p, const cosa_le
                  const cosa_level_ptrs *P2) {
   if (is_kom(*p)) return COSA_ERR_UNSUPPORTED;
   orc_rest1(f, c, P1->q, P2->q, P1->vol, P2->vol);
+  lsp_restrict(f, c, p, P1->vol, P2->vol);
   // ho_rest reads res's first halo layer as smooth() left it (zeroed at
   // every stage, src/cosa.f90:1786-1792)
   if (p->ho_rest) orc_rest2_ho(f, c, P2->rhs, P1->res);
@@ -4188,7 +4388,7 @@ int orc_prolong(orc_level *f, orc_level *c, const cosa_params *p, const cosa_lev
   orc_rest1(f, c, P1->q, P2->qold, P1->vol, P2->vol);
   for (double *a : {P2->qold, P2->q}) {
     for (int b = 0; b < L2.nb; ++b) cons2prim_b(L2, b, a, 0, *p);
-    status |= bc_level(L2, a, P2->si, P2->sj, P2->sk, *p, P2->dist);
+    status |= bc_level(L2, a, P2->si, P2->sj, P2->sk, *p, P2->dist, c->nl);
     cutman_q_level(L2, a);
     for (int b = 0; b < L2.nb; ++b) prim2cons_b(L2, b, a, *p);
     for (int b = 0; b < L2.nb; ++b) q_bedges(L2, b, a, nullptr);
@@ -4224,7 +4424,7 @@ int orc_smooth_level(orc_level *h, const cosa_params *p, int nl, const cosa_leve
       const bool want_dt = (iter / p->iupdt * p->iupdt == iter) && irk == 1;
       status |= residual_impl(h, p, nl, P->q, P->si, P->sj, P->sk, P->res, P->qp, P->qm, P->dq, P->dqp, P->dqm,
                               P->flux, P->dtvol, want_dt, P->betaxi, P->betaeta, P->betazeta,
-                              src_in_res || dual_src_in_res(*p) ? P->vol : nullptr);
+                              src_in_res || dual_src_in_res(*p) ? P->vol : nullptr, nullptr, to_coarse);
       if (nl == 1 && irk == 1 && iter != niter + 1 && hist_row &&
           (mgit == 1 || mgit % rms_every == 0 || mgit == ncycle)) {
         if (dual_imp && !dual_src_in_res(*p)) {
@@ -4239,6 +4439,8 @@ int orc_smooth_level(orc_level *h, const cosa_params *p, int nl, const cosa_leve
         }
       }
       if (nl == 1 && p->dualt) add_level(L, P->res, P->rhs, -1.0, -1);
+      // low-speed preconditioning of the residual (src/cosa.f90:1943-1947)
+      if (p->lomach) lsp_precres_level(L, nl, P->q, P->res, h->cut_pgr.data(), h->cut_vis.data(), *p);
       if (from_fine && iter == 1 && irk == 1) add_level(L, P->rhs, P->res, 1.0, -1);
       if (nl > 1) add_level(L, P->res, P->rhs, -1.0, -1);
       if (iter == niter + 1) return status;
@@ -4262,6 +4464,7 @@ int orc_mg(orc_level **lv, int nlevel, const cosa_params *p, const cosa_level_pt
   int status = 0;
   const int npde = p->npde;
   int last = mgit0 - 1;
+  for (int l = 0; l < nlevel; ++l) lv[l]->nl = l + 1;
   for (int mgit = mgit0; mgit < mgit0 + ncycles; ++mgit) {
     last = mgit;
     double *row = hist ? hist + (int64_t)(mgit - mgit0) * (npde + 1) : nullptr;
@@ -4352,6 +4555,7 @@ int orc_smooth_ns(orc_level *h, const cosa_params *p, int ncycles, int mgit0, in
         if (p->harbal) resg_rms_hb_level(L, res, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
         else resg_rms_level(L, res, rhs, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
       }
+      if (p->lomach) lsp_precres_level(L, 1, q, res, h->cut_pgr.data(), h->cut_vis.data(), *p);
       if (p->irsop > 0) irs_level(L, res, dtvol, nullptr, bx, by, bz, nullptr, nullptr, nullptr, *p);
 #pragma omp parallel for schedule(dynamic)
       for (int b = 0; b < L.nb; ++b) update_b(L, b, res, q, qold, dtvol, p->alphas[irk - 1]);
@@ -4390,6 +4594,7 @@ int orc_smooth_rans(orc_level *h, const cosa_params *p, int ncycles, int mgit0, 
         if (p->harbal) resg_rms_hb_level(L, A.res, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
         else resg_rms_level(L, A.res, A.rhs, hist + (int64_t)(mgit - mgit0) * (L.npde + 1));
       }
+      if (p->lomach) lsp_precres_level(L, 1, A.q, A.res, h->cut_pgr.data(), h->cut_vis.data(), *p);
       if (p->irsop > 0)
         irs_level(L, A.res, A.dtvol, kom ? A.dtvolt : nullptr, A.betaxi, A.betaeta, A.betazeta, X.tbx, X.tby, X.tbz,
                   *p);
@@ -4505,7 +4710,8 @@ int orc_smooth_level_rans(orc_level *h, const cosa_params *p, int nl, int nlevel
                           int rms_every, double *hist_row) {
   Level &L = h->L;
   const cosa_level_ptrs &A = *Ap;
-  const VExtra X = vx(*E);
+  VExtra X = vx(*E);
+  X.to_coarse = to_coarse;
   int status = 0;
   const int niterp = to_coarse ? niter + 1 : niter;
   for (int iter = 1; iter <= niterp; ++iter) {
@@ -4529,6 +4735,7 @@ int orc_smooth_level_rans(orc_level *h, const cosa_params *p, int nl, int nlevel
         }
       }
       if (nl == 1 && p->dualt) add_level(L, A.res, A.rhs, -1.0, -1);
+      if (p->lomach) lsp_precres_level(L, nl, A.q, A.res, h->cut_pgr.data(), h->cut_vis.data(), *p);
       if (from_fine && iter == 1 && irk == 1) add_level(L, A.rhs, A.res, 1.0, -1);
       if (nl > 1) add_level(L, A.res, A.rhs, -1.0, -1);
       if (iter == niter + 1) {
@@ -4579,6 +4786,7 @@ int orc_smooth_level_rans(orc_level *h, const cosa_params *p, int nl, int nlevel
 int orc_restrict_rans(orc_level *f, orc_level *c, const cosa_params *p, const cosa_level_ptrs *P1,
                       const cosa_level_ptrs *P2, const orc_vextra *E1, const orc_vextra *E2) {
   orc_rest1(f, c, P1->q, P2->q, P1->vol, P2->vol);
+  lsp_restrict(f, c, p, P1->vol, P2->vol);
   if (!p->prd_all_lvls) {
     orc_rest4(f, c, E1->prd, E2->prd, P1->vol, P2->vol);
     orc_rest4(f, c, E1->delpls, E2->delpls, P1->vol, P2->vol);
@@ -4605,6 +4813,7 @@ int orc_mg_rans(orc_level **lv, int nlevel, const cosa_params *p, const cosa_lev
   int status = 0;
   const int npde = p->npde;
   int last = mgit0 - 1;
+  for (int l = 0; l < nlevel; ++l) lv[l]->nl = l + 1;
   for (int mgit = mgit0; mgit < mgit0 + ncycles; ++mgit) {
     last = mgit;
     double *row = hist ? hist + (int64_t)(mgit - mgit0) * (npde + 1) : nullptr;

@@ -34,7 +34,9 @@ class _LevelPtrs(C.Structure):
 
 
 def build(force: bool = False) -> str:
-    if force or not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(os.path.join(_HERE, "cosa_oracle.cpp")):
+    srcs = [os.path.join(_HERE, f) for f in ("cosa_oracle.cpp", "lsp_oracle.inc", "Makefile")]
+    srcs.append(os.path.join(_HERE, "..", "include", "cosa_gpu.h"))
+    if force or not os.path.exists(_LIB) or any(os.path.getmtime(_LIB) < os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-C", _HERE], check=True, stdout=subprocess.DEVNULL)
     return _LIB
 
@@ -664,3 +666,49 @@ def lu_solve(a, b):
     lib().orc_lu_solve(C.c_int(n), _p(af), _p(bf), C.c_int(nrhs))
     x = bf.reshape((n, nrhs), order="F")
     return x[:, 0] if bb.ndim == 1 else x
+
+
+# ---- low-speed preconditioning (src/losp.f90, src/flux.f90:390-830) ----------
+def m1(O):
+    """An interior-cell array x S (cutoff_pgr / cutoff_vis layout)."""
+    return np.zeros(O.nm1 * O.S)
+
+
+def lm_cutoff_pg(O, q, cut):
+    lib().orc_lm_cutoff_pg(O.h, _par(O.p), _p(q), _p(cut))
+
+
+def lm_viscoff(O, q, si, sj, sk, cut):
+    lib().orc_lm_viscoff(O.h, _par(O.p), _p(q), _p(si), _p(sj), _p(sk), _p(cut))
+
+
+def proflux(O, idir, nl, qr, ql, flux, sijk, cpg, cvs):
+    lib().orc_proflux(O.h, _par(O.p), C.c_int(idir), C.c_int(nl), _p(qr), _p(ql), _p(flux), _p(sijk), _p(cpg),
+                      _p(cvs))
+
+
+def lsp_prec(O, nl, q, cpg, cvs):
+    """blsp's preconditioner of every interior cell of the conservative q,
+    (imax-1, jmax-1, kmax-1, npde, npde, S) per block."""
+    prec = np.zeros(O.nm1 * O.p.npde * O.p.npde * O.S)
+    lib().orc_lsp_prec(O.h, _par(O.p), C.c_int(nl), _p(q), _p(cpg), _p(cvs), _p(prec))
+    return prec
+
+
+def precres(O, res, prec):
+    lib().orc_precres(O.h, _p(res), _p(prec))
+
+
+def rest3(Of, Oc, c1, c2, vol1, vol2):
+    lib().orc_rest3(Of.h, Oc.h, _p(c1), _p(c2), _p(vol1), _p(vol2))
+
+
+def get_cutoffs(O):
+    """The level's own pressure-gradient and viscous cut-offs."""
+    pgr, vis = m1(O), m1(O)
+    lib().orc_get_cutoffs(O.h, _p(pgr), _p(vis))
+    return pgr, vis
+
+
+def set_cutoffs(O, pgr, vis):
+    lib().orc_set_cutoffs(O.h, _p(pgr), _p(vis))

@@ -398,7 +398,7 @@ def test_restart_short_file_fails(tmp_path):
 @pytest.mark.parametrize("edit,code", [
     (lambda s: s.replace("n euler internal", "n spalart internal"), 0x10),
     (lambda s: s.replace("COSA two-block channel\nmesh", "COSA two-block channel\ncgns\ngrid.cgns"), 0x80),
-    (lambda s: s.replace("preconditioning\nnone", "preconditioning\nlomach 1 inviscid"), 0x80),
+    (lambda s: s.replace("preconditioning\nnone", "preconditioning\nlomach 4 inviscid\nepsp\n1e-5"), 0x10),
     (lambda s: s.replace("1 99 1 1 1 1 1", "4 99 1 1 1 1 1"), 0x10),
     (lambda s: s.replace("output\nbin", "output\nvtk"), 0x10),
     (lambda s: s.replace("1 1.0d-6 n\neig_limit_f", "1 1.0d-6 y 1.5 0 0.1 n\neig_limit_f"), 0x10),
@@ -409,6 +409,23 @@ def test_input_errors(tmp_path, edit, code):
     with pytest.raises(cf.CaseFileError) as e:
         cf.read_input(path)
     assert e.value.code == code
+
+
+def test_low_speed_preconditioning_lines(tmp_path):
+    """The lomach line (cut-off type, viscous/inviscid cut-off) and the
+    constant cut-off per level (src/input.f90:3582-3700), read and written
+    back; a viscous cut-off in an inviscid run is refused."""
+    text = CHANNEL_2BLK.replace("preconditioning\nnone", "preconditioning\nlomach 2 inviscid\nepsp\n2.5d-3")
+    p, r, inp = cf.read_input(_write(tmp_path, "input.dat", text))
+    assert (p.lomach, p.cutoff_type, p.visprec, p.mixpi, p.uprv) == (1, 2, 0, 0, 0.0)
+    assert p.epsp[0] == 2.5e-3
+    out = str(tmp_path / "back.dat")
+    cf.write_input(out, p, r, inp)
+    p2, _, _ = cf.read_input(out)
+    assert (p2.lomach, p2.cutoff_type, p2.epsp[0]) == (1, 2, 2.5e-3)
+    bad = CHANNEL_2BLK.replace("preconditioning\nnone", "preconditioning\nlomach 2 viscous\nepsp\n1e-5")
+    with pytest.raises(cf.CaseFileError):
+        cf.read_input(_write(tmp_path, "bad.dat", bad))
 
 
 def test_default_params_match_python_defaults():
