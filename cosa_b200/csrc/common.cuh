@@ -18,6 +18,7 @@ struct DevBlock {
   int I3, J3;              // im+3, jm+3
   int64_t P3;              // (im+3)(jm+3)(km+3)
   int64_t op3, op2, op1, of0;  // setoffs offsets in cells
+  int64_t om1;                 // offset in the interior-cell layout (off_m1)
   int obct, nbcs;          // the block's rows of the level's BC table (offset in ints, count)
   // a per-block kernel launched for this block alone
   __host__ __device__ DevBlock get() const { return *this; }

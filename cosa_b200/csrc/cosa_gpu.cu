@@ -22,10 +22,14 @@
 #include "moving.cuh"
 #include "force.cuh"
 #include "unsteady.cuh"
+#include "lsp.cuh"
 
 namespace {
 // any k-omega variant: Wilcox (kom), BSL (kom_bsl), SST (kom_sst)
 inline bool rans(const cosa_params &p) { return p.kom || p.kom_bsl || p.kom_sst; }
+// the routine-by-routine stage (in place, one launch per pass): k-omega and
+// low-speed preconditioning
+inline bool routine_stage(const cosa_params &p) { return rans(p) || p.lomach; }
 inline bool blend(const cosa_params &p) { return p.kom_bsl || p.kom_sst; }
 // dual time: src_uns enters the residual unless rkimp without IRS on one
 // level, where update_b takes the physical-time term alone (src/cosa.f90:1910-1915)
@@ -35,6 +39,7 @@ constexpr int kTI = 32, kTJ = 7;  // tile of the fused stage kernel (7 rows + th
 
 struct LevelState {
   int nb = 0;
+  int nl = 1;  // the level's index (1 = finest)
   std::vector<DevBlock> hb;
   std::vector<int> nbcs, bct, cut;
   std::vector<int64_t> obct;
@@ -80,6 +85,9 @@ struct LevelState {
   double *d_h0 = nullptr;     // k-omega: h0 of each family's last face (block x 3 x snapshot x 2)
   double *d_rflux = nullptr;  // k-omega: convective and viscous face fluxes of the three families (6 x F0 x npde x S)
   int rflux_S = 0;
+  // low-speed preconditioning: the level's pressure-gradient and viscous
+  // cut-offs (interior layout x S, the reference's p_cutoff_pgr / p_cutoff_vis)
+  double *d_cut_pgr = nullptr, *d_cut_vis = nullptr;
   double *d_tbeta[3] = {nullptr, nullptr, nullptr};
   // stage schedule: 0 = fused tile kernel, 1 = face-split (k_faces + k_cells),
   // set by cosa_gpu_autotune
@@ -182,7 +190,7 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
     if (x.im < 3 || x.jm < 3 || x.km < 2) return COSA_ERR_ARG;
     x.I3 = x.im + 3; x.J3 = x.jm + 3;
     x.P3 = (int64_t)(x.im + 3) * (x.jm + 3) * (x.km + 3);
-    x.op3 = a3; x.op2 = a2; x.op1 = a1; x.of0 = a0;
+    x.op3 = a3; x.op2 = a2; x.op1 = a1; x.of0 = a0; x.om1 = am;
     if (offs) { x.op3 = offs[3 * b]; x.op2 = offs[3 * b + 1]; x.op1 = offs[3 * b + 2]; }
     x.obct = (int)ab; x.nbcs = d.nbcs[b];
     L.hb.push_back(x);
@@ -285,6 +293,7 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
   }
   if (bps)
     for (HaloItem &it : L.items) it.ps = bps[it.dblk];
+  for (HaloItem &it : L.items) it.nl = L.nl;
   // last writer of every halo cell keeps its write (reference order)
   {
     std::unordered_map<int64_t, int64_t> owner;
@@ -544,7 +553,19 @@ int check_rans_supported(const cosa_params &p) {
   return COSA_OK;
 }
 
+// low-speed preconditioning: Euler or laminar flow, explicit stages, fixed
+// grids (update_lsp_b's k-omega and implicit branches and the moving-frame
+// preconditioner are not built); IRS 5 and 6 are refused by the reference
+int check_lsp_supported(const cosa_params &p) {
+  if (p.npde != 5 || rans(p) || p.rkimp || p.moving || p.rgkuns || p.cutoff_type < 1 || p.cutoff_type > 3 ||
+      (p.visprec && !p.viscous) || p.irsop < 0 || p.irsop > 3 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4 ||
+      p.nlevel < 1 || p.nlevel > COSA_MAX_LEVELS || (p.dualt && (p.harbal || p.dt <= 0)))
+    return COSA_ERR_UNSUPPORTED;
+  return COSA_OK;
+}
+
 int check_fused_supported(const cosa_params &p) {
+  if (p.lomach) return check_lsp_supported(p);
   if (rans(p)) return check_rans_supported(p);
   // rkimp: the implicit time-spectral update of harmonic balance (update_bhb,
   // src/update.f90:1564-1604 without IRS on one level, 1771-1836 with IRS or
@@ -960,6 +981,7 @@ struct IterOpts {
   bool copy_qold = true;       // qold = q at stage 1 (iter <= niter)
   double *res_only = nullptr;  // residual pass of to_coarse: stage-1 residual here, no update
   bool first_cycle = false;    // mgit == 1 (k-omega: coarse-level mut at the first visit)
+  bool to_coarse = false;      // smooth()'s to_coarse (fine-level low-speed cut-offs)
 };
 
 int launch_rans_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o);
@@ -1014,7 +1036,7 @@ int dual_tail(cosa_ctx *c, int nl, LevelState &L, const double *q, double *R, co
 // one RK iteration (nstage stages) of the fused path
 int launch_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
   const cosa_params &p = c->p;
-  if (rans(p)) return launch_rans_iteration(c, nl, L, o);
+  if (routine_stage(p)) return launch_rans_iteration(c, nl, L, o);
   double *Q = L.ptrs.q, *T = L.d_T, *QO = L.ptrs.qold;
   const int S = 2 * p.nharms + 1;
   if (p.dualt) {
@@ -1242,6 +1264,34 @@ int ensure_rans(cosa_ctx *c, LevelState &L) {
   return COSA_OK;
 }
 
+// the preconditioned stage's arrays: the level's cut-offs (zero: cut-off
+// type 1 and runs without the viscous cut-off keep them so), the face-flux
+// planes, the norm partials and the IRS scratch
+int ensure_lsp(cosa_ctx *c, LevelState &L) {
+  const cosa_level_ptrs &P = L.ptrs;
+  if (!P.res || !P.qp || !P.dq || !P.vol) return COSA_ERR_ARG;
+  const int S = 2 * c->p.nharms + 1;
+  int r = 0;
+  for (double **a : {&L.d_cut_pgr, &L.d_cut_vis})
+    if (!*a) {
+      drop_graphs(c);
+      if ((r = dalloc(c, a, (size_t)L.nm1 * COSA_MAX_SNAP))) return r;
+      CK(cudaMemset(*a, 0, (size_t)L.nm1 * COSA_MAX_SNAP * sizeof(double)));
+    }
+  if (L.rflux_S < S) {
+    drop_graphs(c);
+    if ((r = dalloc(c, &L.d_rflux, (size_t)6 * L.n0 * c->p.npde * S))) return r;
+    L.rflux_S = S;
+  }
+  if (c->p.irsop > 0 && (r = ensure_irs_scratch(c, L))) return r;
+  if (L.npart_cap < L.nb * 64) {
+    drop_graphs(c);
+    if ((r = dalloc(c, &L.d_part, (size_t)L.nb * 64 * 8))) return r;
+    L.npart_cap = L.nb * 64;
+  }
+  return COSA_OK;
+}
+
 int ensure_hist(cosa_ctx *c, int rows) {
   if (rows <= c->hist_cap) return COSA_OK;
   drop_graphs(c);  // captured graphs hold the old buffer address
@@ -1285,6 +1335,7 @@ int cosa_gpu_init(const cosa_params *p, int32_t nlevels, const cosa_level_desc *
   cudaMemset(c->d_status, 0, sizeof(int));
   cudaMemset(c->d_row, 0, sizeof(int));
   for (int l = 0; l < nlevels; ++l) {
+    c->L[l].nl = l + 1;
     if ((r = build_level(c, c->L[l], levels[l]))) {
       cosa_gpu_finalize(c);
       return r;
@@ -1602,6 +1653,7 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
   if (c->p.viscous && (!P.vol || !L->d_vm)) return COSA_ERR_ARG;
   if (c->p.dualt && (nl != 1 || !P.rhs || !P.vol)) return COSA_ERR_ARG;
   if (rans(c->p) && (r = ensure_rans(c, *L))) return r;
+  if (c->p.lomach && (r = ensure_lsp(c, *L))) return r;
   cudaSetDevice(c->device);
   const int npde = c->p.npde;
   // schedule of printed iterations (src/cosa.f90:1925-1927)
@@ -1647,7 +1699,7 @@ int cosa_gpu_smooth(cosa_ctx *c, int32_t nl, int32_t niter, int32_t mgit0, int32
   }
   // reference state after smooth(): face halos of q in conservative form
   // (the k-omega stage converts them itself, src/update.f90:1875-2084)
-  if (niter > 0 && !L->items.empty() && !rans(c->p)) {
+  if (niter > 0 && !L->items.empty() && !routine_stage(c->p)) {
     double *last_in = (c->p.nstage % 2 == 0) ? L->d_T : L->ptrs.q;
     const int S = 2 * c->p.nharms + 1;
     k_halo_p2c<<<grid_for((int64_t)L->items.size() * S), 256, 0, c->s>>>(L->d_blocks, L->d_items,
@@ -1956,6 +2008,22 @@ int issue_restrict(cosa_ctx *c, int nl) {
   const cosa_level_ptrs &A = L1->ptrs, &B = L2->ptrs;
   if (!A.q || !A.vol || !A.res || !B.q || !B.vol || !B.rhs) return COSA_ERR_ARG;
   if ((r = launch_rest1(c, *L1, *L2, A.q, B.q, A.vol, B.vol))) return r;
+  if (c->p.lomach) {
+    // the low-speed cut-offs (src/cosa.f90:2724-2731)
+    const int S = 2 * c->p.nharms + 1;
+    std::vector<std::pair<const double *, double *>> cuts;
+    if (c->p.cutoff_type == 3) cuts.push_back({L1->d_cut_pgr, L2->d_cut_pgr});
+    if (c->p.visprec) cuts.push_back({L1->d_cut_vis, L2->d_cut_vis});
+    for (auto &f : cuts) {
+      if (!f.first || !f.second) return COSA_ERR_ARG;
+      for (int b = 0; b < L2->nb; ++b) {
+        const DevBlock &g = L2->hb[b];
+        k_rest3<<<grid_for((int64_t)(g.im - 1) * (g.jm - 1) * (g.km - 1) * S), 256, 0, c->s>>>(
+            L1->hb[b], g, S, f.first, f.second, A.vol, B.vol);
+        if ((r = after_launch(c))) return r;
+      }
+    }
+  }
   if (rans(c->p)) {
     // production terms (or mut with prd_all_lvls) restricted as well
     // (src/cosa.f90:2733-2741)
@@ -2022,11 +2090,12 @@ int issue_smooth_level(cosa_ctx *c, int nl, int niter, bool from_fine, bool to_c
     o.want_rms = want_rms && nl == 1 && iter == niter;
     o.res_only = iter == niter + 1 ? L.ptrs.res : nullptr;
     o.first_cycle = first_cycle;
+    o.to_coarse = to_coarse;
     if ((r = launch_iteration(c, nl, L, o))) return r;
   }
   // reference state after smooth(): face halos of q in conservative form
   // (the k-omega stage converts them itself)
-  if (niterp > 0 && !L.items.empty() && !rans(p)) {
+  if (niterp > 0 && !L.items.empty() && !routine_stage(p)) {
     double *last_in = (to_coarse || p.nstage % 2 == 1) ? L.ptrs.q : L.d_T;
     const int S = 2 * p.nharms + 1;
     k_halo_p2c<<<grid_for((int64_t)L.items.size() * S), 256, 0, c->s>>>(L.d_blocks, L.d_items, (int)L.items.size(),
@@ -2188,6 +2257,7 @@ int cosa_gpu_smooth_level(cosa_ctx *c, int32_t nl, int32_t niter, int32_t from_f
   }
   CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
   if (rans(c->p) && (r = ensure_rans(c, *L))) return r;
+  if (c->p.lomach && (r = ensure_lsp(c, *L))) return r;
   const bool first = mgit == 1;
   const int flags = (from_fine ? 1 : 0) | (to_coarse ? 2 : 0) | (want ? 4 : 0) | (first ? 8 : 0);
   r = run_graph(c, graph_key(1, nl, niter, flags),
@@ -2281,6 +2351,7 @@ int cosa_gpu_mg(cosa_ctx *c, int32_t mgit0, int32_t ncycles, int32_t ncycle, int
       Lv.npart_cap = Lv.nb * 64;
     }
     if (rans(c->p) && (r = ensure_rans(c, Lv))) return r;
+    if (c->p.lomach && (r = ensure_lsp(c, Lv))) return r;
   }
   CK(cudaMemsetAsync(c->d_row, 0, sizeof(int), c->s));
   size_t ri = 0;
@@ -2773,6 +2844,93 @@ int cosa_gpu_srckw(cosa_ctx *c, int32_t nl, const double *q, const double *mut, 
   });
 }
 
+// ---- low-speed preconditioning, per routine ----------------------------------------
+int cosa_gpu_lm_cutoff_pg(cosa_ctx *c, int32_t nl, const double *q, double *cutoff_pgr) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !cutoff_pgr) return COSA_ERR_ARG;
+  return for_blocks(c, *L, cnt_cells,
+                    [&](auto b, dim3 g) { k_lm_cutoff_pg<<<g, 256, 0, c->s>>>(b, c->d_p, q, cutoff_pgr); });
+}
+
+int cosa_gpu_lm_viscoff(cosa_ctx *c, int32_t nl, const double *q, const double *si, const double *sj,
+                        const double *sk, double *cutoff_vis) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !si || !sj || !sk || !cutoff_vis) return COSA_ERR_ARG;
+  if (!c->p.viscous) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
+    k_lm_viscoff<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, cutoff_vis);
+  });
+}
+
+int cosa_gpu_rest3(cosa_ctx *c, int32_t nl, const double *cutoff1, double *cutoff2, const double *vol1,
+                   const double *vol2) {
+  LevelState *L1, *L2;
+  int r = level_pair(c, nl, L1, L2);
+  if (r) return r;
+  if (!cutoff1 || !cutoff2 || !vol1 || !vol2) return COSA_ERR_ARG;
+  const int S = 2 * c->p.nharms + 1;
+  for (int b = 0; b < L2->nb; ++b) {
+    const DevBlock &g = L2->hb[b];
+    k_rest3<<<grid_for((int64_t)(g.im - 1) * (g.jm - 1) * (g.km - 1) * S), 256, 0, c->s>>>(L1->hb[b], g, S, cutoff1,
+                                                                                          cutoff2, vol1, vol2);
+    if ((r = after_launch(c))) return r;
+  }
+  return COSA_OK;
+}
+
+int cosa_gpu_proflux(cosa_ctx *c, int32_t idir, int32_t nl, const double *qr, const double *ql, double *flux,
+                     const double *sijk, const double *cutoff_pgr, const double *cutoff_vis) {
+  LevelState *L = level(c, nl);
+  if (!L || idir < 1 || idir > 3 || !qr || !ql || !flux || !sijk || !cutoff_pgr || !cutoff_vis) return COSA_ERR_ARG;
+  if (c->p.moving || nl > COSA_MAX_LEVELS) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_faces, [&](auto b, dim3 g) {
+    k_proflux<<<g, 256, 0, c->s>>>(b, idir, c->d_p, nl, qr, ql, flux, sijk, cutoff_pgr, cutoff_vis);
+  });
+}
+
+int cosa_gpu_lambda_p(cosa_ctx *c, int32_t nl, const double *q, const double *si, const double *sj,
+                      const double *sk, const double *vol, double *lam, double *lamv, const double *cutoff_pgr,
+                      const double *cutoff_vis) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !si || !sj || !sk || !lam || !cutoff_pgr || !cutoff_vis) return COSA_ERR_ARG;
+  if (c->p.moving || rans(c->p) || nl > COSA_MAX_LEVELS) return COSA_ERR_UNSUPPORTED;
+  if (c->p.viscous) {
+    if (!vol || !lamv) return COSA_ERR_ARG;
+    return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
+      k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, vol, nullptr, lam, lamv, cutoff_pgr, cutoff_vis, nl);
+    });
+  }
+  return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
+    k_lambda<<<g, 256, 0, c->s>>>(b, c->d_p, q, si, sj, sk, lam, nullptr, nullptr, nullptr, cutoff_pgr, cutoff_vis, nl);
+  });
+}
+
+int cosa_gpu_lsp(cosa_ctx *c, int32_t nl, const double *q, const double *cutoff_pgr, const double *cutoff_vis,
+                 double *prec) {
+  LevelState *L = level(c, nl);
+  if (!L || !q || !cutoff_pgr || !cutoff_vis || !prec) return COSA_ERR_ARG;
+  if (c->p.moving || nl > COSA_MAX_LEVELS) return COSA_ERR_UNSUPPORTED;
+  return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) {
+    k_lsp_prec<<<g, 256, 0, c->s>>>(b, c->d_p, nl, q, cutoff_pgr, cutoff_vis, prec);
+  });
+}
+
+int cosa_gpu_precres(cosa_ctx *c, int32_t nl, double *res, const double *prec) {
+  LevelState *L = level(c, nl);
+  if (!L || !res || !prec) return COSA_ERR_ARG;
+  return for_blocks(c, *L, cnt_cells, [&](auto b, dim3 g) { k_precres<<<g, 256, 0, c->s>>>(b, c->d_p, res, prec); });
+}
+
+int cosa_gpu_lsp_cutoffs(cosa_ctx *c, int32_t nl, double *cutoff_pgr, double *cutoff_vis) {
+  LevelState *L = level(c, nl);
+  if (!L || !cutoff_pgr || !cutoff_vis) return COSA_ERR_ARG;
+  if (!L->d_cut_pgr || !L->d_cut_vis) return COSA_ERR_ARG;
+  const size_t n = (size_t)L->nm1 * (2 * c->p.nharms + 1) * sizeof(double);
+  CK(cudaMemcpyAsync(cutoff_pgr, L->d_cut_pgr, n, cudaMemcpyDeviceToDevice, c->s));
+  CK(cudaMemcpyAsync(cutoff_vis, L->d_cut_vis, n, cudaMemcpyDeviceToDevice, c->s));
+  return COSA_OK;
+}
+
 int cosa_gpu_update_kom(cosa_ctx *c, int32_t nl, const double *res, double *q, const double *qold, const double *vol,
                         const double *dtvolt, const double *delpls, const double *prd, double ar,
                         const double *ttrm) {
@@ -3134,11 +3292,130 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
   return COSA_OK;
 }
 
+// one RK stage of the low-speed preconditioned path (npde = 5, Euler or
+// laminar), smooth()'s routines with lomach (src/cosa.f90:1719-2016):
+// cons2prim, BCs and cuts, bprtest, the cut-offs, the preconditioned time
+// step, the preconditioned convective fluxes (MUSCL + proflux) and the laminar
+// viscous ones in one launch, resid, prim2cons, the residual norm, lsp +
+// precres, the multigrid forcing, IRS and update_b
+int launch_lsp_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpts &o) {
+  const bool compute_dt = o.compute_dt && irk == 1, want_rms = o.want_rms && irk == o.rms_stage;
+  const cosa_params &p = c->p;
+  const int S = 2 * p.nharms + 1, npde = p.npde;
+  const cosa_level_ptrs &P = L.ptrs;
+  double *q = P.q;
+  const BlockList bl{L.d_blocks};
+  const int *bct = L.d_bct;
+  double *beta[3] = {P.betaxi ? P.betaxi : L.d_beta[0], P.betaeta ? P.betaeta : L.d_beta[1],
+                     P.betazeta ? P.betazeta : L.d_beta[2]};
+  int r = 0;
+  if (irk == 1 && o.copy_qold &&
+      (r = for_blocks(c, L, cnt_interior,
+                      [&](auto b, dim3 g) { k_copy_interior<<<g, 256, 0, c->s>>>(b, npde * S, q, P.qold); })))
+    return r;
+  if ((r = cosa_gpu_cons2prim(c, nl, 0, q))) return r;
+  if (!L.items.empty()) {
+    k_halo<false><<<grid_for((int64_t)L.items.size() * S), 256, 0, c->s>>>(
+        L.d_blocks, L.d_items, (int)L.items.size(), c->d_p, q, P.si, P.sj, P.sk, c->d_status, P.dist,
+        face_vel_of(c, L));
+    if ((r = after_launch(c))) return r;
+  }
+  if ((r = for_blocks(c, L, cnt_all, [&](auto b, dim3 g) { k_prtest<<<g, 256, 0, c->s>>>(b, c->d_p, q, c->d_status); })))
+    return r;
+  // Darmofal's pressure-gradient cut-off (every level, or the fine level of a
+  // cycle that restricts) and the viscous cut-off (src/cosa.f90:1763-1778)
+  const bool fine = (p.nlevel > 1 && nl == 1 && o.to_coarse) || p.nlevel == 1;
+  if (((p.cutoff_type == 3 && fine) || p.cutoff_type == 2) &&
+      (r = for_blocks(c, L, cnt_cells,
+                      [&](auto b, dim3 g) { k_lm_cutoff_pg<<<g, 256, 0, c->s>>>(b, c->d_p, q, L.d_cut_pgr); })))
+    return r;
+  if (p.visprec && fine && (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+                              k_lm_viscoff<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.si, P.sj, P.sk, L.d_cut_vis);
+                            })))
+    return r;
+  if (compute_dt) {
+    // eig_eul_p / eig_ns_p and bdeltat (src/cosa.f90:1447-1590)
+    const bool irs = p.irsop >= 2;
+    if (p.viscous) {
+      if ((r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+             k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.si, P.sj, P.sk, P.vol, nullptr, P.qp, P.dq, L.d_cut_pgr,
+                                              L.d_cut_vis, nl);
+           })) ||
+          (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+             k_deltat_ns<<<g, 256, 0, c->s>>>(b, c->d_p, P.dtvol, P.qp, P.dq, irs ? beta[0] : nullptr, beta[1],
+                                              beta[2], nullptr, nullptr, nullptr, nullptr);
+           })))
+        return r;
+    } else {
+      if ((r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+             k_lambda<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.si, P.sj, P.sk, P.qp, nullptr, nullptr, nullptr, L.d_cut_pgr,
+                                           L.d_cut_vis, nl);
+           })) ||
+          (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+             k_deltat<<<g, 256, 0, c->s>>>(b, c->d_p, P.dtvol, P.qp, irs ? beta[0] : nullptr, beta[1], beta[2]);
+           })))
+        return r;
+    }
+  }
+  if ((r = cosa_gpu_zero(c, nl, P.res))) return r;
+  if (p.viscous && (r = launch_edges(c, L, q, nullptr))) return r;
+  // MUSCL + proflux (and the laminar viscous fluxes) of the three families,
+  // then resid of their sums (src/cosa.f90:1797-1876)
+  if ((r = for_blocks(c, L, cnt_faces, [&](auto b, dim3 g) {
+         (void)b;
+         const dim3 gz(g.x * 2, g.y, p.viscous ? 6 : 3);
+         k_lsp_faces<<<gz, 128, 0, c->s>>>(bl, c->d_p, bct, q, nl, P.si, P.sj, P.sk, L.d_cut_pgr, L.d_cut_vis, L.d_vm,
+                                           L.n0, L.d_rflux);
+       })) ||
+      (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+         (void)b;
+         k_rans_resid<<<g, 256, 0, c->s>>>(bl, c->d_p, L.n0, L.d_rflux, P.res, p.viscous ? 1 : 0);
+       })))
+    return r;
+  if ((r = cosa_gpu_prim2cons(c, nl, q))) return r;
+  // unsteady source terms (src/cosa.f90:1908-1922)
+  if (dual_src_in_res(p) &&
+      (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) { k_src_uns<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.vol, P.res); })))
+    return r;
+  if (p.harbal &&
+      (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) { k_src_hb<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.vol, P.res); })))
+    return r;
+  if (want_rms && (r = launch_norm(c, L, P.res, p.dualt ? P.rhs : nullptr, nullptr))) return r;
+  const int nvs = npde * S;
+  if (p.dualt && nl == 1 &&
+      (r = for_blocks(c, L, cnt_interior,
+                      [&](auto b, dim3 g) { k_add_interior<<<g, 256, 0, c->s>>>(b, nvs, P.res, P.rhs, -1.0); })))
+    return r;
+  // lsp + precres (src/cosa.f90:1943-1947) on the conservative state
+  if ((r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
+         k_lsp_precres<<<g, 256, 0, c->s>>>(b, c->d_p, nl, q, L.d_cut_pgr, L.d_cut_vis, P.res);
+       })))
+    return r;
+  // multigrid forcing (src/cosa.f90:1950-1960)
+  if (o.rhs && o.force && irk == 1 &&
+      (r = for_blocks(c, L, cnt_interior,
+                      [&](auto b, dim3 g) { k_add_interior<<<g, 256, 0, c->s>>>(b, nvs, o.rhs, P.res, 1.0); })))
+    return r;
+  if (o.rhs && nl > 1 &&
+      (r = for_blocks(c, L, cnt_interior,
+                      [&](auto b, dim3 g) { k_add_interior<<<g, 256, 0, c->s>>>(b, nvs, P.res, o.rhs, -1.0); })))
+    return r;
+  if (o.res_only) return COSA_OK;
+  if (p.irsop > 0 && (r = irs_apply(c, L, P.res, L.d_ores, P.dtvol, beta))) return r;
+  // update_lsp_b / update_lsp_bhb without k-omega: q = q^n - ar R dt/V
+  const double ar = p.alphas[irk - 1];
+  return for_blocks(c, L, cnt_interior,
+                    [&](auto b, dim3 g) { k_update<<<g, 256, 0, c->s>>>(b, c->d_p, P.res, q, P.qold, P.dtvol, ar); });
+}
+
 int launch_rans_iteration(cosa_ctx *c, int nl, LevelState &L, const IterOpts &o) {
   if (o.res_only && o.res_only != L.ptrs.res) return COSA_ERR_ARG;  // the residual pass leaves R in res
-  if (o.res_only) return launch_rans_stage(c, nl, L, 1, o);
+  auto stage = [&](int irk) {
+    return rans(c->p) ? launch_rans_stage(c, nl, L, irk, o) : launch_lsp_stage(c, nl, L, irk, o);
+  };
+  if (o.res_only) return stage(1);
   for (int irk = 1; irk <= c->p.nstage; ++irk) {
-    int r = launch_rans_stage(c, nl, L, irk, o);
+    int r = stage(irk);
     if (r) return r;
   }
   return COSA_OK;
@@ -3210,7 +3487,7 @@ extern "C" int cosa_gpu_autotune(cosa_ctx *c, int32_t nl, int32_t niter, double 
   int r = check_fused_supported(c->p);
   if (r) return r;
   ms[0] = ms[1] = 0.0;
-  if (rans(c->p)) {  // the k-omega stage has one schedule
+  if (routine_stage(c->p)) {  // the k-omega and preconditioned stages have one schedule
     L->schedule = 0;
     if (choice) *choice = 0;
     return COSA_OK;

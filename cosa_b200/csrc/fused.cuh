@@ -38,6 +38,7 @@ struct HaloItem {
   int64_t c1, c2;   // interior cells (p3 cell index in sblk)
   int64_t mface;    // metric cell index (i + I2*(j + J2*k)) of the face in dblk
   int ps;           // slot of the flow conditions (BC values) in the params array
+  int nl;           // multigrid level of the item's block (the low-speed cut-off epsp(nl))
 };
 
 struct Tile {
@@ -102,7 +103,7 @@ __global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__re
         const int64_t e = ((db.op2 * S2) + (int64_t)nh * I2 * J2 * K2 + it.mface) * 4;
         nx = s[e] * it.sgn; ny = s[e + 1] * it.sgn; nz = s[e + 2] * it.sgn;
       }
-      const BcPar B = make_bcpar(Pp[it.ps]);
+      const BcPar B = make_bcpar(Pp[it.ps], it.nl);
       int err = 0;
       // moving walls: the velocity of the wall face (snapshot nh)
       double wv[3];

@@ -105,7 +105,9 @@ template <class BS>
 __global__ void k_lambda(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
                          const double *__restrict__ si, const double *__restrict__ sj,
                          const double *__restrict__ sk, double *__restrict__ lam, const double *__restrict__ cvx = nullptr,
-                         const double *__restrict__ cvy = nullptr, const double *__restrict__ cvz = nullptr) {
+                         const double *__restrict__ cvy = nullptr, const double *__restrict__ cvz = nullptr,
+                         const double *__restrict__ cpg = nullptr, const double *__restrict__ cvs = nullptr,
+                         int nl = 1) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
@@ -132,7 +134,14 @@ __global__ void k_lambda(BS bs_, const cosa_params *__restrict__ Pp, const doubl
       const int64_t g = b.op2 * S2 + (int64_t)nh * I2 * J2 * K2 + i + I2 * (j + J2 * (int64_t)k);
       gv[0] = cvx[g]; gv[1] = cvy[g]; gv[2] = cvz[g];
     }
-    eig_eul(P.gamma, qc, sim, sip, sjm, sjp, skm, skp, li, lj, lk, cvx ? gv : nullptr);
+    if (cpg) {
+      // low-speed preconditioning: eig_eul_p with the cell's cut-offs (interior layout)
+      const int64_t m = b.om1 * S + (int64_t)n * ni * nj * nk + (i - 1) + (int64_t)ni * ((j - 1) + (int64_t)nj * (k - 1));
+      eig_eul_p(P.gamma, P.uprv, P.epsp[nl - 1] * P.epsp[nl - 1], fmax(cpg[m], cvs[m]), qc, sim, sip, sjm, sjp, skm,
+                skp, li, lj, lk);
+    } else {
+      eig_eul(P.gamma, qc, sim, sip, sjm, sjp, skm, skp, li, lj, lk, cvx ? gv : nullptr);
+    }
     lam[p3_var(b, npde, S, 1, n) + c] = li;
     lam[p3_var(b, npde, S, 2, n) + c] = lj;
     lam[p3_var(b, npde, S, 3, n) + c] = lk;

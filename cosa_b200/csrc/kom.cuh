@@ -755,8 +755,9 @@ __device__ __forceinline__ void rans_conv_faces(const DevBlock &b, const cosa_pa
 // q_face (+ calmut) / q_der / b_rtst / vflux_b of the faces of family D of
 // block ib: the face state and gradients of the bulk loops, or on strong-BC
 // faces the one-sided wall formulas with the halo mut (src/flux.f90:1848-1962,
-// 2846-2946, 947-1180); the seven viscous face fluxes go to F
-template <int D>
+// 2846-2946, 947-1180); the NV viscous face fluxes go to F.  NV = 7: k-omega
+// (Reynolds stresses, k and omega diffusion); NV = 5: laminar flow (mut null)
+template <int D, int NV = 7>
 __device__ __forceinline__ void rans_visc_faces(const DevBlock &b, int ib, const cosa_params &P,
                                                 const int *__restrict__ bct, const double *__restrict__ q,
                                                 const double *__restrict__ mut, const double *__restrict__ vm,
@@ -770,10 +771,10 @@ __device__ __forceinline__ void rans_visc_faces(const DevBlock &b, int ib, const
     const QView Q = qview(b, q, S, n, npde);
     const int e = D == 1 ? i : (D == 2 ? j : k);
     const int row = strong_row(b, bct, D, e, mx, D == 1 ? j : i, D == 3 ? j : k);
-    double qf[7], g[3][7], mf;
+    double qf[NV], g[3][NV], mf = 0.0;
     if (row < 0) {
-      face_interior<D, 7>(Q, i, j, k, qf, g);
-      mf = (mut[p3s_idx(b, S, i - di, j - dj, k - dk, n)] + mut[p3s_idx(b, S, i, j, k, n)]) / 2;
+      face_interior<D, NV>(Q, i, j, k, qf, g);
+      if (NV == 7) mf = (mut[p3s_idx(b, S, i - di, j - dj, k - dk, n)] + mut[p3s_idx(b, S, i, j, k, n)]) / 2;
     } else {
       const int *rw = bct + b.obct + 10 * row;
       WallFace w;
@@ -781,21 +782,26 @@ __device__ __forceinline__ void rans_visc_faces(const DevBlock &b, int ib, const
       w.fi = i; w.fj = j; w.fk = k;
       w.lo[0] = rw[3]; w.lo[1] = rw[5]; w.lo[2] = rw[7];
       w.hi[0] = rw[4]; w.hi[1] = rw[6]; w.hi[2] = rw[8];
-      face_wall<7>(Q, w, mx, qf, g);
+      face_wall<NV>(Q, w, mx, qf, g);
       const int a = e == 1 ? 0 : mx;
-      mf = mut[p3s_idx(b, S, D == 1 ? a : i, D == 2 ? a : j, D == 3 ? a : k, n)];
+      if (NV == 7) mf = mut[p3s_idx(b, S, D == 1 ? a : i, D == 2 ? a : j, D == 3 ? a : k, n)];
     }
     double vmf[9];
     load_vm(vm, b, n0, D, i, j, k, vmf);
-    double gr[3][3], t6[6], Fv[7];
-#pragma unroll
-    for (int m = 0; m < 3; ++m) { gr[m][0] = g[0][m + 1]; gr[m][1] = g[1][m + 1]; gr[m][2] = g[2][m + 1]; }
-    rtst_face(P, qf[0], qf[5], gr, vmf, mf, t6);
     const int64_t e4 = p2_idx(b, 1, 1, i, j, k, 0);
-    vflux_kom_face(P, V, qf, g, t6, vmf, s[e4], s[e4 + 1], s[e4 + 2], s[e4 + 3], mf,
-                   fdist ? fdist[f0_idx(b, 1, 1, i, j, k, 1, 0)] : -1.0, Fv);
+    double Fv[NV];
+    if constexpr (NV == 7) {
+      double gr[3][3], t6[6];
 #pragma unroll
-    for (int m = 0; m < 7; ++m) F[f0_idx(b, npde, S, i, j, k, m + 1, n)] = Fv[m];
+      for (int m = 0; m < 3; ++m) { gr[m][0] = g[0][m + 1]; gr[m][1] = g[1][m + 1]; gr[m][2] = g[2][m + 1]; }
+      rtst_face(P, qf[0], qf[5], gr, vmf, mf, t6);
+      vflux_kom_face(P, V, qf, g, t6, vmf, s[e4], s[e4 + 1], s[e4 + 2], s[e4 + 3], mf,
+                     fdist ? fdist[f0_idx(b, 1, 1, i, j, k, 1, 0)] : -1.0, Fv);
+    } else {
+      vflux_face(V, qf, g, vmf, s[e4], s[e4 + 1], s[e4 + 2], s[e4 + 3], 0.0, Fv);
+    }
+#pragma unroll
+    for (int m = 0; m < NV; ++m) F[f0_idx(b, npde, S, i, j, k, m + 1, n)] = Fv[m];
   }
 }
 
@@ -830,9 +836,10 @@ __global__ void __launch_bounds__(128, 3) k_rans_faces(BlockList bs_, const cosa
 }
 
 // bresid of the three families on the summed convective + viscous face
-// fluxes of k_rans_faces, families in the reference's order (src/cosa.f90:1149-1200)
+// fluxes of k_rans_faces (visc = 0: the convective ones alone), families in
+// the reference's order (src/cosa.f90:1149-1200)
 __global__ void k_rans_resid(BlockList bs_, const cosa_params *__restrict__ Pp, int64_t n0,
-                             const double *__restrict__ rf, double *__restrict__ res) {
+                             const double *__restrict__ rf, double *__restrict__ res, int visc = 1) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1;
@@ -847,7 +854,8 @@ __global__ void k_rans_resid(BlockList bs_, const cosa_params *__restrict__ Pp, 
         const int64_t fp = f0_idx(b, npde, S, i + (d == 1), j + (d == 2), k + (d == 3), v, n);
         const int64_t fm = f0_idx(b, npde, S, i, j, k, v, n);
         const double *Fc = rf + (d - 1) * plane, *Fv = rf + (d + 2) * plane;
-        x = x + (Fc[fp] + Fv[fp]) - (Fc[fm] + Fv[fm]);
+        if (visc) x = x + (Fc[fp] + Fv[fp]) - (Fc[fm] + Fv[fm]);
+        else x = x + Fc[fp] - Fc[fm];
       }
       res[o] = x;
     }

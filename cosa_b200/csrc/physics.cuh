@@ -517,6 +517,36 @@ __device__ __forceinline__ void eig_eul(double g, const double *qc, const double
   lamk = fabs(u * zetax + v * zetay + w * zetaz) + a * azeta;
 }
 
+// eig_eul_p (src/cosa.f90:4300-4372): the convective spectral radii of the
+// low-speed preconditioned system, with the preconditioned Mach number
+// mp2 = min(max(M^2, (uprv/a)^2, cutoff, epsp(nl)^2), 1)
+__device__ __forceinline__ void eig_eul_p(double g, double uprv, double eps2, double cutoff, const double *qc,
+                                          const double *sim, const double *sip, const double *sjm,
+                                          const double *sjp, const double *skm, const double *skp, double &lami,
+                                          double &lamj, double &lamk) {
+  const double rho = qc[0], p = qc[4], u = qc[1], v = qc[2], w = qc[3];
+  const double a = sqrt(g * p / rho);
+  const double q2 = u * u + v * v + w * w, a2 = a * a;
+  const double ump2 = (uprv / a) * (uprv / a);
+  const double mp2 = fmin(fmax(fmax(fmax(q2 / a2, ump2), cutoff), eps2), 1.0);
+  const double xix = 0.5 * (sim[0] * sim[3] + sip[0] * sip[3]);
+  const double xiy = 0.5 * (sim[1] * sim[3] + sip[1] * sip[3]);
+  const double xiz = 0.5 * (sim[2] * sim[3] + sip[2] * sip[3]);
+  const double etax = 0.5 * (sjm[0] * sjm[3] + sjp[0] * sjp[3]);
+  const double etay = 0.5 * (sjm[1] * sjm[3] + sjp[1] * sjp[3]);
+  const double etaz = 0.5 * (sjm[2] * sjm[3] + sjp[2] * sjp[3]);
+  const double zetax = 0.5 * (skm[0] * skm[3] + skp[0] * skp[3]);
+  const double zetay = 0.5 * (skm[1] * skm[3] + skp[1] * skp[3]);
+  const double zetaz = 0.5 * (skm[2] * skm[3] + skp[2] * skp[3]);
+  const double axi = (sim[3] + sip[3]) / 2, aeta = (sjm[3] + sjp[3]) / 2, azeta = (skm[3] + skp[3]) / 2;
+  const double ui = u * xix + v * xiy + w * xiz, uj = u * etax + v * etay + w * etaz;
+  const double uk = u * zetax + v * zetay + w * zetaz;
+  const double m1 = (1 - mp2) * (1 - mp2);
+  lami = ((1 + mp2) * fabs(ui) + sqrt(ui * ui * m1 + 4 * a2 * mp2 * (axi * axi))) / 2;
+  lamj = ((1 + mp2) * fabs(uj) + sqrt(uj * uj * m1 + 4 * a2 * mp2 * (aeta * aeta))) / 2;
+  lamk = ((1 + mp2) * fabs(uk) + sqrt(uk * uk * m1 + 4 * a2 * mp2 * (azeta * azeta))) / 2;
+}
+
 // ---- boundary conditions (src/bc.f90) --------------------------------------------
 // Each BC maps the primitive interior values next to the face (c1 = first
 // interior cell, c2 = second) and the face normal to the two halo layers
@@ -528,9 +558,12 @@ struct BcPar {
   double pout1, pout3;
   double tkefar, omefar, qmin6, qmin7;
   int npde;
+  // low-speed preconditioning: lomach, mixpi, uprv and epsp(nl)^2 of the level
+  int lomach, mixpi;
+  double uprv, eps2;
 };
 
-__device__ __forceinline__ BcPar make_bcpar(const cosa_params &P) {
+__device__ __forceinline__ BcPar make_bcpar(const cosa_params &P, int nl = 1) {
   BcPar b;
   b.g = P.gamma; b.rhoinf = P.rhoinf; b.ainf = P.ainf; b.pinf = P.pinf;
   b.sinf = P.pinf / pow(P.rhoinf, P.gamma);
@@ -544,6 +577,8 @@ __device__ __forceinline__ BcPar make_bcpar(const cosa_params &P) {
   b.pout1 = P.outlet_p[0]; b.pout3 = P.outlet_p[2];
   b.tkefar = P.tkefar; b.omefar = P.omefar; b.qmin6 = P.qmin[5]; b.qmin7 = P.qmin[6];
   b.npde = P.npde;
+  b.lomach = P.lomach; b.mixpi = P.mixpi; b.uprv = P.uprv;
+  b.eps2 = P.epsp[nl - 1] * P.epsp[nl - 1];
   return b;
 }
 
@@ -587,8 +622,20 @@ __device__ __forceinline__ int bc_insub(const BcPar &B, double nx, double ny, do
   const double un1 = c1[1] * nx + c1[2] * ny + c1[3] * nz;
   const double un2 = c2[1] * nx + c2[2] * ny + c2[3] * nz;
   const double p1 = c1[4], p2 = c2[4];
-  const double rc1 = sqrt(g * p1 * rho1);
-  const double rc2 = sqrt(g * p2 * rho2);
+  double rc1 = sqrt(g * p1 * rho1);
+  double rc2 = sqrt(g * p2 * rho2);
+  if (B.lomach) {
+    // the preconditioned outgoing characteristic (src/bc.f90:1032-1056)
+    auto rc_lsp = [&](const double *c, double un) {
+      const double q2 = c[1] * c[1] + c[2] * c[2] + c[3] * c[3], a2 = g * c[4] / c[0], a = sqrt(a2);
+      const double ump2 = (B.uprv / a) * (B.uprv / a);
+      const double mp2 = fmin(fmax(fmax(q2 / a2, ump2), B.eps2), 1.0);
+      const double lp3 = 0.5 * (un * (1. + mp2) + sqrt(un * un * ((1. - mp2) * (1. - mp2)) + 4. * a2 * mp2));
+      return -(c[0] * (un - lp3));
+    };
+    rc1 = rc_lsp(c1, un1);
+    rc2 = rc_lsp(c2, un2);
+  }
   const double rcun1 = rc1 * un1, rcun2 = rc2 * un2;
   const double h0inl = 1 / (g - 1) * B.t0;
   const double dot = B.sx * nx + B.sy * ny + B.sz * nz;
@@ -685,6 +732,13 @@ __device__ __forceinline__ int bc_outsub(const BcPar &B, const double *c1, const
 // stream; s = face normal times sgnm
 __device__ __forceinline__ int bc_far0(const BcPar &B, double sx, double sy, double sz, const double *c1,
                                        double *h1, double *h2) {
+  if (B.lomach) {
+    // low-speed preconditioning: both layers frozen at the free stream (src/bc.f90:264-276, 409-414)
+    for (int v = 0; v < 5; ++v) h1[v] = B.qfst[v];
+    if (B.npde > 5) { h1[5] = B.tkefar; h1[6] = B.omefar; }
+    for (int v = 0; v < B.npde; ++v) h2[v] = h1[v];
+    return 3;
+  }
   const double g = B.g;
   const double qext = c1[1] * sx + c1[2] * sy + c1[3] * sz;
   const double qinf = B.qfst[1] * sx + B.qfst[2] * sy + B.qfst[3] * sz;
@@ -744,8 +798,20 @@ __device__ __forceinline__ int bc_far1(const BcPar &B, double sx, double sy, dou
   const double qinf = B.qfst[1] * sx + B.qfst[2] * sy + B.qfst[3] * sz;
   const double pext = c1[4], pinf = B.qfst[4], rhoext = c1[0];
   const double a = sqrt(g * pext / rhoext);
-  const double unb = (qext + qinf) / 2 + (pext - pinf) / (2 * rhoext * a);
-  const double pb = (pext + pinf) / 2 + rhoext * a * (qext - qinf) / 2;
+  double unb = (qext + qinf) / 2 + (pext - pinf) / (2 * rhoext * a);
+  double pb = (pext + pinf) / 2 + rhoext * a * (qext - qinf) / 2;
+  if (B.lomach) {
+    // preconditioned characteristics with the artificial sound speed apr
+    // (src/bc.f90:638-667)
+    const double q2 = c1[1] * c1[1] + c1[2] * c1[2] + c1[3] * c1[3];
+    const double a2 = g * pext / rhoext, al = sqrt(a2), un = qext;
+    const double m2 = q2 / a2, ump2 = (B.uprv / al) * (B.uprv / al);
+    const double mp2s = fmin(1.0, fmax(fmax(m2, (1 - B.mixpi) * ump2), B.eps2));
+    const double am = (1 - mp2s) / 2;
+    const double apr = sqrt(am * am * (un * un) + a2 * mp2s);
+    unb = (qext + qinf) / 2 + (pext - pinf) / (2 * rhoext * apr) + (qext - qinf) / 2 * am * un / apr;
+    pb = (pext + pinf) / 2 + rhoext * mp2s * a2 / apr * (qext - qinf) / 2 - (pext - pinf) / 2 * am * un / apr;
+  }
   const double mach = unb / a;
   int mask = 0;
   if (unb <= 0.0) {

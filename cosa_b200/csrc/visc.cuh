@@ -479,7 +479,7 @@ __device__ __forceinline__ void eig_ns_cell(const DevBlock &b, const cosa_params
                                             const double *__restrict__ si, const double *__restrict__ sj,
                                             const double *__restrict__ sk, int S2, int nh, double volc, int i, int j,
                                             int k, double lam[3], double lamv[3], const double *mut = nullptr,
-                                            int S = 1, int n = 0) {
+                                            int S = 1, int n = 0, double lsp_cut = -1.0, double lsp_eps2 = 0.0) {
   const double g = P.gamma, st = P.stemp;
   double qc[5], sm[3][4], sp[3][4];
 #pragma unroll
@@ -490,7 +490,10 @@ __device__ __forceinline__ void eig_ns_cell(const DevBlock &b, const cosa_params
     sm[1][m] = sj[p2_idx(b, S2, m + 1, i, j, k, nh)]; sp[1][m] = sj[p2_idx(b, S2, m + 1, i, j + 1, k, nh)];
     sm[2][m] = sk[p2_idx(b, S2, m + 1, i, j, k, nh)]; sp[2][m] = sk[p2_idx(b, S2, m + 1, i, j, k + 1, nh)];
   }
-  eig_eul(g, qc, sm[0], sp[0], sm[1], sp[1], sm[2], sp[2], lam[0], lam[1], lam[2]);
+  if (lsp_cut >= 0)  // eig_ns_p: the preconditioned convective radii (src/cosa.f90:4374-4460)
+    eig_eul_p(g, P.uprv, lsp_eps2, lsp_cut, qc, sm[0], sp[0], sm[1], sp[1], sm[2], sp[2], lam[0], lam[1], lam[2]);
+  else
+    eig_eul(g, qc, sm[0], sp[0], sm[1], sp[1], sm[2], sp[2], lam[0], lam[1], lam[2]);
   const double rho = qc[0];
   const double mu = sutherland(g * qc[4] / rho, st);
   auto MUT = [&](int a, int c, int e) { return mut ? mut[b.op3 * S + (int64_t)n * b.P3 + p3_cell(b, a, c, e)] : 0.0; };
@@ -567,7 +570,9 @@ template <class BS>
 __global__ void k_lambda_ns(BS bs_, const cosa_params *__restrict__ Pp, const double *__restrict__ q,
                             const double *__restrict__ si, const double *__restrict__ sj,
                             const double *__restrict__ sk, const double *__restrict__ vol,
-                            const double *__restrict__ mut, double *__restrict__ lam, double *__restrict__ lamv) {
+                            const double *__restrict__ mut, double *__restrict__ lam, double *__restrict__ lamv,
+                            const double *__restrict__ cpg = nullptr, const double *__restrict__ cvs = nullptr,
+                            int nl = 1) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
@@ -581,7 +586,13 @@ __global__ void k_lambda_ns(BS bs_, const cosa_params *__restrict__ Pp, const do
     const int n = (int)(r / nk), nh = n * P.hbmove;
     const QView Q = qview(b, q, S, n, npde);
     double l[3], lv[3];
-    eig_ns_cell(b, P, Q, si, sj, sk, S2, nh, vol[p1_idx(b, 1, i, j, k, 0)], i, j, k, l, lv, mut, S, n);
+    double cut = -1.0;
+    if (cpg) {
+      const int64_t m = b.om1 * S + (int64_t)n * ni * nj * nk + (i - 1) + (int64_t)ni * ((j - 1) + (int64_t)nj * (k - 1));
+      cut = fmax(cpg[m], cvs[m]);
+    }
+    eig_ns_cell(b, P, Q, si, sj, sk, S2, nh, vol[p1_idx(b, 1, i, j, k, 0)], i, j, k, l, lv, mut, S, n, cut,
+                P.epsp[nl - 1] * P.epsp[nl - 1]);
     const int64_t c = p3_cell(b, i, j, k);
 #pragma unroll
     for (int m = 0; m < 3; ++m) {

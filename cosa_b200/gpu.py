@@ -65,7 +65,8 @@ SYMBOLS = [
     "cosa_gpu_autotune", "cosa_gpu_set_schedule", "cosa_gpu_force", "cosa_gpu_rest2_ho", "cosa_gpu_bc_res",
     "cosa_gpu_movegrid", "cosa_gpu_face_vel", "cosa_gpu_vert2cell", "cosa_gpu_facedist", "cosa_gpu_update_ttrm",
     "cosa_gpu_srckw_sst", "cosa_gpu_tur_vis_sst", "cosa_gpu_src_uns", "cosa_gpu_rhs_uns", "cosa_gpu_rkuns",
-    "cosa_gpu_copy_interior",
+    "cosa_gpu_copy_interior", "cosa_gpu_lm_cutoff_pg", "cosa_gpu_lm_viscoff", "cosa_gpu_rest3", "cosa_gpu_proflux",
+    "cosa_gpu_lambda_p", "cosa_gpu_lsp", "cosa_gpu_precres", "cosa_gpu_lsp_cutoffs",
 ]
 
 
@@ -429,6 +430,45 @@ class Context:
         self._check(load().cosa_gpu_update_kom(self.h, nl, _ptr(res.ptr), _ptr(q.ptr), _ptr(qold.ptr), _ptr(vol.ptr),
                                                _ptr(dtvolt.ptr), _ptr(delpls.ptr), _ptr(prd.ptr), C.c_double(ar),
                                                _ptr(ttrm.ptr if ttrm is not None else None)), "update_kom")
+
+    # ---- low-speed preconditioning -------------------------------------------------
+    def alloc_m1(self, nl=1, nvar=1):
+        """An interior-cell array x S (x nvar): the cut-off layout; nvar =
+        npde^2 for a preconditioner array."""
+        return DevArray(self, self.sizes(nl)[4] * self.S * nvar)
+
+    def lm_cutoff_pg(self, nl, q, cut):
+        self._check(load().cosa_gpu_lm_cutoff_pg(self.h, nl, _ptr(q.ptr), _ptr(cut.ptr)), "lm_cutoff_pg")
+
+    def lm_viscoff(self, nl, q, si, sj, sk, cut):
+        self._check(load().cosa_gpu_lm_viscoff(self.h, nl, _ptr(q.ptr), _ptr(si.ptr), _ptr(sj.ptr), _ptr(sk.ptr),
+                                               _ptr(cut.ptr)), "lm_viscoff")
+
+    def rest3(self, nl, c1, c2, vol1, vol2):
+        self._check(load().cosa_gpu_rest3(self.h, nl, _ptr(c1.ptr), _ptr(c2.ptr), _ptr(vol1.ptr), _ptr(vol2.ptr)),
+                    "rest3")
+
+    def proflux(self, idir, nl, qr, ql, flux, sijk, cpg, cvs):
+        self._check(load().cosa_gpu_proflux(self.h, idir, nl, _ptr(qr.ptr), _ptr(ql.ptr), _ptr(flux.ptr),
+                                            _ptr(sijk.ptr), _ptr(cpg.ptr), _ptr(cvs.ptr)), "proflux")
+
+    def lambda_p(self, nl, q, si, sj, sk, lam, cpg, cvs, vol=None, lamv=None):
+        self._check(load().cosa_gpu_lambda_p(self.h, nl, _ptr(q.ptr), _ptr(si.ptr), _ptr(sj.ptr), _ptr(sk.ptr),
+                                             _ptr(vol.ptr if vol is not None else None), _ptr(lam.ptr),
+                                             _ptr(lamv.ptr if lamv is not None else None), _ptr(cpg.ptr),
+                                             _ptr(cvs.ptr)), "lambda_p")
+
+    def lsp(self, nl, q, cpg, cvs, prec):
+        self._check(load().cosa_gpu_lsp(self.h, nl, _ptr(q.ptr), _ptr(cpg.ptr), _ptr(cvs.ptr), _ptr(prec.ptr)), "lsp")
+
+    def precres(self, nl, res, prec):
+        self._check(load().cosa_gpu_precres(self.h, nl, _ptr(res.ptr), _ptr(prec.ptr)), "precres")
+
+    def lsp_cutoffs(self, nl=1):
+        """The level's own pressure-gradient and viscous cut-offs (host arrays)."""
+        pgr, vis = self.alloc_m1(nl), self.alloc_m1(nl)
+        self._check(load().cosa_gpu_lsp_cutoffs(self.h, nl, _ptr(pgr.ptr), _ptr(vis.ptr)), "lsp_cutoffs")
+        return pgr.download(), vis.download()
 
     # ---- time-accurate runs -------------------------------------------------------
     def src_uns(self, nl, q, vol, res):

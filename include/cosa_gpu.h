@@ -438,6 +438,38 @@ int cosa_gpu_srckw(cosa_ctx *ctx, int32_t nl, const double *q, const double *mut
 int cosa_gpu_update_kom(cosa_ctx *ctx, int32_t nl, const double *res, double *q, const double *qold,
                         const double *vol, const double *dtvolt, const double *delpls,
                         const double *prd, double ar, const double *ttrm);
+/* ---- low-speed preconditioning (lomach; src/losp.f90, src/flux.f90:390-830).
+   Cut-off arrays are in the reference's interior-cell layout
+   (imax-1, jmax-1, kmax-1, 0:S-1) per block, off_m1 * S (p_cutoff_pgr /
+   p_cutoff_vis); prec is (imax-1, jmax-1, kmax-1, npde, npde, 0:S-1) per
+   block at off_m1 * npde^2 * S (p_prec).  q primitive unless stated. */
+/* lm_cutoff_pg (src/losp.f90:1085-1165): pressure-gradient cut-off */
+int cosa_gpu_lm_cutoff_pg(cosa_ctx *ctx, int32_t nl, const double *q, double *cutoff_pgr);
+/* lm_viscoff (src/losp.f90:1290-1414): viscous cut-off (viscous runs) */
+int cosa_gpu_lm_viscoff(cosa_ctx *ctx, int32_t nl, const double *q, const double *si, const double *sj,
+                        const double *sk, double *cutoff_vis);
+/* rest3 (src/cosa.f90:3014-3088): cut-offs of level nl restricted to nl+1 */
+int cosa_gpu_rest3(cosa_ctx *ctx, int32_t nl, const double *cutoff1, double *cutoff2, const double *vol1,
+                   const double *vol2);
+/* lm_cutoff + proflux (src/losp.f90:1416-1447, src/flux.f90:390-830): the
+   preconditioned Roe flux of family idir from the MUSCL states qr (qp) and
+   ql (qm) */
+int cosa_gpu_proflux(cosa_ctx *ctx, int32_t idir, int32_t nl, const double *qr, const double *ql, double *flux,
+                     const double *sijk, const double *cutoff_pgr, const double *cutoff_vis);
+/* lambda with lomach (src/cosa.f90:1447-1590): eig_eul_p, or with viscous
+   eig_ns_p (vol and lamv then required) */
+int cosa_gpu_lambda_p(cosa_ctx *ctx, int32_t nl, const double *q, const double *si, const double *sj,
+                      const double *sk, const double *vol, double *lam, double *lamv, const double *cutoff_pgr,
+                      const double *cutoff_vis);
+/* lsp (src/losp.f90:2-195): the preconditioner of every interior cell from
+   the conservative q */
+int cosa_gpu_lsp(cosa_ctx *ctx, int32_t nl, const double *q, const double *cutoff_pgr, const double *cutoff_vis,
+                 double *prec);
+/* precres (src/cosa.f90:2446-2521): res <- prec res over the interior cells */
+int cosa_gpu_precres(cosa_ctx *ctx, int32_t nl, double *res, const double *prec);
+/* the level's own cut-offs as the smooth/multigrid drivers left them
+   (device to device copies into the two arrays given) */
+int cosa_gpu_lsp_cutoffs(cosa_ctx *ctx, int32_t nl, double *cutoff_pgr, double *cutoff_vis);
 /* facedist (src/grid.f90:2809-2870): face wall distances of the three
    families from the cell distances dist (P1) */
 int cosa_gpu_facedist(cosa_ctx *ctx, int32_t nl, const double *dist, double *fidist, double *fjdist,

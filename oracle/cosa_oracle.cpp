@@ -4268,6 +4268,13 @@ void orc_precres(orc_level *h, double *res, const double *prec) {
           }
   }
 }
+// lambda with lomach: eig_eul_p, or with viscous eig_ns_p (src/cosa.f90:1447-1590)
+void orc_lambda_p(orc_level *h, const cosa_params *p, int nl, const double *q, const double *si, const double *sj,
+                  const double *sk, const double *vol, double *lam, double *lamv, const double *cpg,
+                  const double *cvs) {
+  if (p->viscous) lambda_ns_level(h->L, q, si, sj, sk, vol, nullptr, lam, lamv, *p, cpg, cvs, nl);
+  else lambda_level(h->L, q, si, sj, sk, lam, *p, cpg, cvs, nl);
+}
 void orc_rest3(orc_level *f, orc_level *c, const double *c1, double *c2, const double *vol1, const double *vol2) {
   for (int b = 0; b < f->L.nb; ++b) rest3_b(f->L, c->L, b, c1, c2, vol1, vol2);
 }

@@ -687,6 +687,11 @@ def proflux(O, idir, nl, qr, ql, flux, sijk, cpg, cvs):
                       _p(cvs))
 
 
+def lambda_p(O, nl, q, si, sj, sk, lam, cpg, cvs, vol=None, lamv=None):
+    lib().orc_lambda_p(O.h, _par(O.p), C.c_int(nl), _p(q), _p(si), _p(sj), _p(sk), _opt(vol), _p(lam), _opt(lamv),
+                       _p(cpg), _p(cvs))
+
+
 def lsp_prec(O, nl, q, cpg, cvs):
     """blsp's preconditioner of every interior cell of the conservative q,
     (imax-1, jmax-1, kmax-1, npde, npde, S) per block."""

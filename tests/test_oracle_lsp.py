@@ -12,7 +12,9 @@ bc_far1 / bc_insub (src/bc.f90):
   (src/losp.f90:196-300) is the identity;
 * the pressure-gradient cut-off of a uniform state is zero and of a single
   pressure jump is the jump over rho a^2; rest3 keeps a constant field;
-* with equal face states proflux is the physical flux;
+* with equal face states proflux is the physical flux, and its dissipation
+  is P^-1 |P A| (q_R - q_L) with P blsp's preconditioner and A the flux
+  Jacobian, both at the Roe-averaged state (the preconditioned Roe scheme);
 * a low-Mach channel is driven further down by the preconditioned cycles.
 """
 import numpy as np
@@ -173,6 +175,54 @@ def test_proflux_of_equal_states_is_physical(oracle_mod):
     np.testing.assert_allclose(F[0, 0, :jm - 1, :], 1.1 * un * ds, rtol=1e-13, atol=1e-16)
     np.testing.assert_allclose(F[1, 0, :jm - 1, :], (1.1 * 0.03 * un + 0.7 * kx) * ds, rtol=1e-13, atol=1e-16)
     np.testing.assert_allclose(F[4, 0, :jm - 1, :], 1.1 * h0 * un * ds, rtol=1e-13, atol=1e-16)
+
+
+def _cons(w, g=1.4):
+    r, u, v, ww, p = w
+    return np.array([r, r * u, r * v, r * ww, p / (g - 1) + 0.5 * r * (u * u + v * v + ww * ww)])
+
+
+def _flux(Q, n, g=1.4):
+    r = Q[0]
+    u, v, w = Q[1:4] / r
+    p = (g - 1) * (Q[4] - 0.5 * r * (u * u + v * v + w * w))
+    U = u * n[0] + v * n[1] + w * n[2]
+    return np.array([r * U, r * u * U + p * n[0], r * v * U + p * n[1], r * w * U + p * n[2], (Q[4] + p) * U])
+
+
+def test_proflux_dissipation_is_preconditioned_roe(oracle_mod):
+    case = casekit.small_channel(4, 4, 2)
+    p = _lsp(case.params, cutoff_type=1, epsp=(0.02,))
+    O = oracle_mod.OracleLevel(case.tables, p)
+    si, sj, sk, vol = O.metrics(case.x, case.y, case.z)
+    wr, wl = np.array([1.02, 0.05, 0.01, 0.0, 0.716]), np.array([0.99, 0.04, -0.01, 0.0, 0.713])
+    qr, ql = O.p3(), O.p3()
+    for m in range(5):
+        qr[m * O.n3:(m + 1) * O.n3], ql[m * O.n3:(m + 1) * O.n3] = wr[m], wl[m]
+    f, zero = O.f0(), oracle_mod.m1(O)
+    oracle_mod.proflux(O, 1, 1, qr, ql, f, si, zero, zero)
+    im, jm, km = case.tables.dims[0]
+    F = f[:im * jm * km * 5].reshape(5, km, jm, im)[:, 0, 1, 2]  # face (3, 2, 1)
+    s = si.reshape(-1)[:4 * (im + 2) * (jm + 2) * (km + 2)].reshape(km + 2, jm + 2, im + 2, 4)[1, 2, 3]
+    n, ds = s[:3], s[3]
+    QR, QL = _cons(wr), _cons(wl)
+    df = _flux(QR, n) + _flux(QL, n) - 2 * F / ds
+    rl, rr = np.sqrt(wl[0]), np.sqrt(wr[0])
+    u = (rl * wl[1:4] + rr * wr[1:4]) / (rl + rr)
+    h0 = (rl * (3.5 * wl[4] / wl[0] + 0.5 * wl[1:4] @ wl[1:4]) + rr * (3.5 * wr[4] / wr[0] + 0.5 * wr[1:4] @ wr[1:4]))
+    h0 /= rl + rr
+    a2 = 0.4 * (h0 - 0.5 * u @ u)
+    Q = _cons(np.array([rl * rr, *u, rl * rr * a2 / 1.4]))
+    A = np.zeros((5, 5))
+    for c in range(5):
+        dq = np.zeros(5)
+        dq[c] = 1e-7 * max(1.0, abs(Q[c]))
+        A[:, c] = (_flux(Q + dq, n) - _flux(Q - dq, n)) / (2 * dq[c])
+    mp2 = min(1.0, max(u @ u / a2, 0.02 ** 2))
+    P = np.linalg.inv(_preci(Q, mp2, 1.4))
+    ev, R = np.linalg.eig(P @ A)
+    D = np.linalg.inv(P) @ (R @ np.diag(np.abs(ev)) @ np.linalg.inv(R)).real @ (QR - QL)
+    np.testing.assert_allclose(df, D, rtol=1e-7, atol=1e-9 * np.abs(D).max())
 
 
 def test_low_mach_cycles_converge_further(oracle_mod):
