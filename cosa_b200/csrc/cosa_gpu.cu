@@ -137,6 +137,7 @@ struct cosa_ctx {
   // residual norms reduced per segment of tiles (one per served solve) when
   // set: segment s = tiles [d_seg[2s], +d_seg[2s+1]) with seg_ncell[s] cells
   int nseg = 0;
+  double *d_cfl_blk = nullptr;  // serving: CFL number of each block's solve
   int *d_seg = nullptr;
   double *d_seg_ncell = nullptr;
   int hist_cap = 0;
@@ -917,6 +918,7 @@ int launch_stage(cosa_ctx *c, int nl, LevelState &L, double *qin, double *qout, 
   A.compute_dt = compute_dt;
   A.first_order = nl >= p.nl_crs;
   A.update = update;
+  A.cfl_blk = c->d_cfl_blk;
   const bool split =
       L.schedule == 1 && c->nseg == 0 && L.d_cflux && (L.d_qprim || !p.viscous) && L.d_ftasks && !p.rkimp;
   if (split && p.viscous) {

@@ -177,6 +177,7 @@ struct StageArgs {
   int compute_dt;
   int first_order;
   int update;            // 0: residual only (restriction pass)
+  const double *cfl_blk; // per-block CFL number (serving: each solve's own), or null for P.cfl
 };
 
 // Thread layout: TJ main warps, warp w holds row j0+w of the tile (lane =
@@ -401,7 +402,7 @@ k_stage_tile(const DevBlock *__restrict__ blocks, const Tile *__restrict__ tiles
         load_metric(A.sk, ci, cj, k, skm); load_metric(A.sk, ci, cj, k + 1, skp);
         double li, lj, lk;
         eig_eul(g, qc, sim, sip, sjm, sjp, skm, skp, li, lj, lk);
-        dt = P.cfl / (li + lj + lk);
+        dt = (A.cfl_blk ? A.cfl_blk[T.blk] : P.cfl) / (li + lj + lk);
         A.dtvol[o1] = dt;
         if (A.bx) {
           double ba, bb_, bc;

@@ -159,7 +159,7 @@ int serve_rebuild(cosa_serve *e) {
   std::vector<int64_t> offs;
   std::vector<int> bps;
   std::vector<int> seg;
-  std::vector<double> segn;
+  std::vector<double> segn, cflb;
   int nb = 0;
   int64_t tile0 = 0;
   for (int a = 0; a < na; ++a) {
@@ -179,6 +179,7 @@ int serve_rebuild(cosa_serve *e) {
       offs.push_back(s.off + s.lop[3 * b + 1]);
       offs.push_back(s.off + s.lop[3 * b + 2]);
       bps.push_back(a);
+      cflb.push_back(s.flow.cfl > 0 ? s.flow.cfl : c->p.cfl);
     }
     seg.push_back((int)tile0);
     seg.push_back((int)s.ntiles);
@@ -202,6 +203,10 @@ int serve_rebuild(cosa_serve *e) {
   c->d_halo_p = e->d_ps;
   // residual-norm segments and their output rows
   if ((r = ensure_hist(c, na))) return r;
+  // each solve's CFL number on its blocks (the flow conditions' cfl, else the scheme's)
+  if (c->d_cfl_blk) { cudaFree(c->d_cfl_blk); c->d_cfl_blk = nullptr; }
+  CK(cudaMalloc(&c->d_cfl_blk, cflb.size() * sizeof(double)));
+  CK(cudaMemcpyAsync(c->d_cfl_blk, cflb.data(), cflb.size() * sizeof(double), cudaMemcpyHostToDevice, c->s));
   if (c->d_seg) { cudaFree(c->d_seg); c->d_seg = nullptr; }
   if (c->d_seg_ncell) { cudaFree(c->d_seg_ncell); c->d_seg_ncell = nullptr; }
   CK(cudaMalloc(&c->d_seg, seg.size() * sizeof(int)));
@@ -359,6 +364,7 @@ int cosa_serve_destroy(cosa_serve *e) {
   if (e->d_bad) cudaFree(e->d_bad);
   if (c->d_seg) cudaFree(c->d_seg);
   if (c->d_seg_ncell) cudaFree(c->d_seg_ncell);
+  if (c->d_cfl_blk) cudaFree(c->d_cfl_blk);
   if (c->L[0].d_part) cudaFree(c->L[0].d_part);
   c->L[0].d_part = nullptr;
   cosa_gpu_finalize(c);
@@ -400,6 +406,7 @@ int cosa_serve_submit(cosa_serve *e, const cosa_level_desc *grid, const double *
   s.flow.rhoinf = flow->rhoinf; s.flow.pinf = flow->pinf; s.flow.ainf = flow->ainf; s.flow.tinf = flow->tinf;
   s.flow.inlet_t0 = flow->inlet_t0; s.flow.inlet_p0 = flow->inlet_p0;
   for (int i = 0; i < 3; ++i) { s.flow.inlet_dir[i] = flow->inlet_dir[i]; s.flow.outlet_p[i] = flow->outlet_p[i]; }
+  if (flow->cfl > 0) s.flow.cfl = flow->cfl;  // the request's own CFL number (local time step)
   s.tol = tol;
   s.max_iter = max_iter;
   s.t_submit = e->now();

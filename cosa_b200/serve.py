@@ -46,11 +46,13 @@ def naca_request(scale: float, mach: float, alpha_deg: float, arrival: float = 0
     """Euler NACA 0012 O-grid of the harmonic-balance family, 256 x 64 x 2
     cells in four blocks (3/16, 5/16, 5/16, 3/16 of the contour) scaled by
     `scale` in i and j, slip wall (14), far field (30) at 20 chords, free
-    stream at `mach` and incidence `alpha_deg`."""
+    stream at `mach` and incidence `alpha_deg`, CFL 1 (each solve's CFL
+    number travels with its flow conditions)."""
     ni, nj = max(16, int(round(256 * scale)) // 16 * 16), max(8, int(round(64 * scale)))
     blocks = (3 * ni // 16, 5 * ni // 16, 5 * ni // 16, 3 * ni // 16)
     p = cases.channel_params(mach)
     p.alpha = float(np.deg2rad(alpha_deg))
+    p.cfl = 1.0  # the O-grids' thin wall cells and closed trailing edge diverge at the channel's CFL 2
     case = cases.naca0012_ogrid(blocks=blocks, nj=nj, nk=2, rfar=20.0, h1=2e-3 / scale, params=p, wall=14)
     return Request(scale, mach, arrival, case, case.params, alpha_deg, "naca")
 
@@ -95,15 +97,19 @@ class SweepResult:
         return {"requests": self.n, "wall_s": self.wall_s, "solves_per_hour": self.solves_per_hour,
                 "p50_latency_s": self.p50_s, "p99_latency_s": self.p99_s,
                 "converged": sum(s == "converged" for s in self.states),
+                "stopped": sum(s == "stopped" for s in self.states),
+                "failed": sum(s == "failed" for s in self.states),
                 "mean_iters": float(np.mean(self.iters)) if self.iters else 0.0,
                 "mcell_stages_per_s": self.cell_stages / self.wall_s / 1e6 if self.wall_s else 0.0}
 
 
 def run_sweep(requests: List[Request], budget_bytes: float = 150e9, tol: float = 1e-8, max_iter: int = 200_000,
-              check_every: int = 10, iters_per_step: int = 50, device: int = 0) -> SweepResult:
+              check_every: int = 10, iters_per_step: int = 50, device: int = 0, precision: int = 0) -> SweepResult:
     """Feed `requests` at their arrival times (seconds after the start) and
-    run the engine until every one has retired."""
-    srv = Server(engine_scheme(), int(budget_bytes), device=device, check_every=check_every)
+    run the engine (precision 0: FP64, 1: mixed) until every one has retired."""
+    scheme = engine_scheme()
+    scheme.precision = precision
+    srv = Server(scheme, int(budget_bytes), device=device, check_every=check_every)
     try:
         ids: List[int] = []
         pending = sorted(range(len(requests)), key=lambda k: requests[k].arrival)
@@ -178,7 +184,7 @@ def batched_vs_plain(requests: List[Request], niter: int = 400, device: int = 0,
         secs, work = 0.0, 0
         for r, nc in zip(requests, cells):
             p = engine_scheme()
-            for k in ("machfs", "alpha", "beta", "rhoinf", "pinf", "ainf", "tinf", "inlet_t0", "inlet_p0"):
+            for k in ("machfs", "alpha", "beta", "rhoinf", "pinf", "ainf", "tinf", "inlet_t0", "inlet_p0", "cfl"):
                 setattr(p, k, getattr(r.flow, k))
             for i in range(3):
                 p.inlet_dir[i] = r.flow.inlet_dir[i]

@@ -607,9 +607,10 @@ int cosa_gpu_resg_rms_noalloc(int32_t nblocks, const int32_t *dims, int32_t npde
  * in the same halo and tile launches) and retire when their total residual
  * norm falls below tol times its first-iteration value (checked every
  * check_every of their own iterations) or after max_iter iterations.  The
- * scheme (gamma, limiter, CFL, RK coefficients) is the engine's; machfs,
- * alpha, beta, the free stream, the inlet total state and the outlet
- * pressure come from each request.  Explicit Euler, single grid, S = 1,
+ * scheme (gamma, limiter, RK coefficients, and the CFL number unless the
+ * request sets cfl > 0) is the engine's; machfs, alpha, beta, the free
+ * stream, the inlet total state, the outlet pressure and the CFL number
+ * come from each request.  Explicit Euler, single grid, S = 1,
  * blocks of at least two cells per direction.
  */
 #define COSA_SOLVE_QUEUED    0

@@ -128,10 +128,11 @@ def test_naca_requests_in_the_mix():
 
 def test_failed_solve_is_isolated():
     """A request whose state loses positivity (Euler NACA at 7.7 deg on the
-    finer grid: the impulsive start drives p below qmin at the leading
-    edge) is retired as failed; the requests beside it converge with the
-    same bits as alone."""
+    finer grid run at CFL 2: the impulsive start drives p below qmin at the
+    leading edge) is retired as failed; the requests beside it converge
+    with the same bits as alone."""
     bad = serve.naca_request(1.0, 0.417, 7.68)
+    bad.flow.cfl = 2.0
     reqs = [serve.channel_request(0.5, 0.45), bad, serve.naca_request(0.5, 0.5, 6.0)]
     alone = {k: _run(reqs, [k], tol=0.3)[k] for k in (0, 2)}
     assert _run(reqs, [1], tol=0.3)[1]["state"] == "failed"
