@@ -17,7 +17,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libcosa_gpu.so")
 SOURCES = ["cosa_gpu.cu", "io.cpp"]
 HEADERS = ["common.cuh", "physics.cuh", "kernels_ref.cuh", "fused.cuh", "mg.cuh", "visc.cuh", "kom.cuh", "split.cuh", "faces.cuh",
-           "moving.cuh", "force.cuh", "serve.cuh", "unsteady.cuh"]
+           "moving.cuh", "force.cuh", "serve.cuh", "unsteady.cuh", "lsp.cuh"]
 
 
 def nvcc() -> str:

@@ -227,7 +227,7 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
       const int type = r[0], idir = r[1], inrout = r[2];
       if (idir < 1 || idir > 3) return COSA_ERR_ARG;
       // viscous walls: the laminar, fixed-grid branch of bc_walvis_15
-      const bool wall15 = type / 100 == 15 && (!c->p.moving || !rans(c->p));
+      const bool wall15 = type / 100 == 15;
       const bool ok = type == 80 || type == 4 || type == 14 || type == 21 || type == 91 || type == 30 || type == 31 ||
                       wall15;
       if (!ok) return COSA_ERR_UNSUPPORTED;
@@ -440,6 +440,25 @@ int build_level(cosa_ctx *c, LevelState &L, const cosa_level_desc &d, const int6
   }
   L.ncutx = (int)cutx.size();
   L.ncutv = (int)cutv.size();
+  // moving grids: the node copies of every snapshot (node arrays of S2
+  // snapshots per block at op2 * S2, snapshot nh at nh * (im+2)(jm+2)(km+2))
+  const int S2m = c->p.moving ? 2 * c->p.nharms * c->p.hbmove + 1 : 1;
+  if (S2m > 1) {
+    std::vector<std::pair<int64_t, int64_t>> base(L.nb);  // (op2, nodes per snapshot)
+    for (int b = 0; b < L.nb; ++b)
+      base[b] = {L.hb[b].op2, (int64_t)(L.hb[b].im + 2) * (L.hb[b].jm + 2) * (L.hb[b].km + 2)};
+    auto shift = [&](int64_t g, int nh) {
+      int b = L.nb - 1;
+      while (b > 0 && base[b].first > g) --b;
+      return g + base[b].first * (S2m - 1) + nh * base[b].second;
+    };
+    std::vector<CopyItem> all;
+    all.reserve(cutx.size() * S2m);
+    for (int nh = 0; nh < S2m; ++nh)
+      for (const CopyItem &it : cutx) all.push_back(CopyItem{shift(it.dst, nh), shift(it.src, nh)});
+    cutx.swap(all);
+    L.ncutx = (int)cutx.size();
+  }
 
   // ---- tiles of the fused stage kernel
   std::vector<Tile> tiles;
@@ -548,8 +567,12 @@ int set_smem_attrs() {
 // BSL and SST
 int check_rans_supported(const cosa_params &p) {
   if (p.npde != 7 || !rans(p) || (p.kom + p.kom_bsl + p.kom_sst) != 1 || !p.viscous ||
-      (p.rkimp && !p.dualt && !p.harbal) || p.moving || (p.dualt && (p.dt <= 0 || p.harbal)) ||
+      (p.rkimp && !p.dualt && !p.harbal) || (p.dualt && (p.dt <= 0 || p.harbal)) ||
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
+    return COSA_ERR_UNSUPPORTED;
+  // moving grids: harmonic balance of a pitching body, explicit stages on one
+  // level in FP64 (the mixed-precision k-omega flux carries no face speed)
+  if (p.moving && (!p.harbal || !p.hbmove || p.rkimp || p.nlevel > 1 || p.precision != COSA_PREC_FP64))
     return COSA_ERR_UNSUPPORTED;
   return COSA_OK;
 }
@@ -2545,15 +2568,29 @@ extern "C" int cosa_gpu_resg_rms_noalloc(int32_t nblocks, const int32_t *dims, i
 // ---- laminar viscous path ---------------------------------------------------------------
 extern "C" {
 
+// a block's view of node snapshot nh of a moving level's node arrays
+// (S2 snapshots per block at op2 * S2)
+static DevBlock node_snapshot(const cosa_ctx *c, const DevBlock &b, int nh) {
+  DevBlock x = b;
+  if (c->p.moving) {
+    const int S2 = 2 * c->p.nharms * c->p.hbmove + 1;
+    x.op2 = b.op2 * S2 + (int64_t)nh * (b.im + 2) * (b.jm + 2) * (b.km + 2);
+  }
+  return x;
+}
+
+static int node_snapshots(const cosa_ctx *c) { return c->p.moving ? 2 * c->p.nharms * c->p.hbmove + 1 : 1; }
+
 int cosa_gpu_coordex(cosa_ctx *c, int32_t nl, double *x, double *y, double *z) {
   LevelState *L = level(c, nl);
   if (!L || !x || !y || !z) return COSA_ERR_ARG;
-  for (const DevBlock &b : L->hb) {
-    const int64_t n = 2 * ((int64_t)b.im * b.km + (int64_t)b.jm * b.km + (int64_t)b.im * b.jm);
-    k_coordex<<<grid_for(n), 256, 0, c->s>>>(b, x, y, z);
-    int r = after_launch(c);
-    if (r) return r;
-  }
+  for (int nh = 0; nh < node_snapshots(c); ++nh)
+    for (const DevBlock &b : L->hb) {
+      const int64_t n = 2 * ((int64_t)b.im * b.km + (int64_t)b.jm * b.km + (int64_t)b.im * b.jm);
+      k_coordex<<<grid_for(n), 256, 0, c->s>>>(node_snapshot(c, b, nh), x, y, z);
+      int r = after_launch(c);
+      if (r) return r;
+    }
   return COSA_OK;
 }
 
@@ -2590,13 +2627,15 @@ int cosa_gpu_vmetrix(cosa_ctx *c, int32_t nl, const double *x, const double *y, 
                      double *vm) {
   LevelState *L = level(c, nl);
   if (!L || !x || !y || !z || !vol || !vm) return COSA_ERR_ARG;
-  if (c->p.moving) return COSA_ERR_UNSUPPORTED;
-  for (const DevBlock &b : L->hb)
-    for (int d = 1; d <= 3; ++d) {
-      k_vmetrix<<<grid_for((int64_t)b.im * b.jm * b.km), 256, 0, c->s>>>(b, d, x, y, z, vol, vm, L->n0);
-      int r = after_launch(c);
-      if (r) return r;
-    }
+  // moving grids: the inverse metrics of every node snapshot, 27 * n0 each
+  for (int nh = 0; nh < node_snapshots(c); ++nh)
+    for (const DevBlock &b : L->hb)
+      for (int d = 1; d <= 3; ++d) {
+        k_vmetrix<<<grid_for((int64_t)b.im * b.jm * b.km), 256, 0, c->s>>>(node_snapshot(c, b, nh), d, x, y, z, vol,
+                                                                           vm + (int64_t)nh * 27 * L->n0, L->n0);
+        int r = after_launch(c);
+        if (r) return r;
+      }
   return COSA_OK;
 }
 
@@ -2952,7 +2991,10 @@ int cosa_gpu_force(cosa_ctx *c, int32_t nl, const double *q, const double *x, co
   if (!L || !q || !x || !y || !z || !si || !sj || !sk || !xmom || !lngth || !coef || isurf < 1) return COSA_ERR_ARG;
   const cosa_params &P = c->p;
   if (P.viscous && !vm) return COSA_ERR_ARG;
-  if (P.moving && P.viscous) return COSA_ERR_UNSUPPORTED;
+  // moving viscous grids: the wall derivative of the velocity relative to the
+  // grid needs the bound level's cell grid velocities
+  const bool mvisc = P.moving && P.viscous;
+  if (mvisc && (!L->ptrs.xdot || !L->ptrs.ydot || !L->ptrs.zdot)) return COSA_ERR_ARG;
   if (lngth[0] == 0.0 || lngth[1] == 0.0 || lngth[2] == 0.0) return COSA_ERR_ARG;
   const int S = 2 * P.nharms + 1, nb = L->nb;
   // moment centre of every snapshot: on a pitching grid it moves with the
@@ -3022,7 +3064,9 @@ int cosa_gpu_force(cosa_ctx *c, int32_t nl, const double *q, const double *x, co
     CK(cudaMemcpyAsync(fl.d_xmom, xms.data(), xms.size() * sizeof(double), cudaMemcpyHostToDevice, c->s));
     k_force_faces<<<grid_for((int64_t)fl.nfaces * S), 256, 0, c->s>>>(L->d_blocks, c->d_p, fl.d_faces, fl.nfaces, q, x,
                                                                        y, z, si, sj, sk, vm, L->n0, fl.d_xmom,
-                                                                       fl.d_buf);
+                                                                       fl.d_buf, mvisc ? L->ptrs.xdot : nullptr,
+                                                                       mvisc ? L->ptrs.ydot : nullptr,
+                                                                       mvisc ? L->ptrs.zdot : nullptr);
     int r = after_launch(c);
     if (r) return r;
     k_force_sum<<<dim3(nb, S), 256, 0, c->s>>>(fl.d_bstart, fl.nfaces, fl.d_buf, fl.d_sums);
@@ -3145,7 +3189,10 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
     return r;
   if (compute_dt) {
     if ((r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
-           k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.si, P.sj, P.sk, P.vol, P.mut, P.qp, P.dq);
+           const bool mv = p.moving;
+           k_lambda_ns<<<g, 256, 0, c->s>>>(b, c->d_p, q, P.si, P.sj, P.sk, P.vol, P.mut, P.qp, P.dq, nullptr,
+                                            nullptr, 1, mv ? P.xdot : nullptr, mv ? P.ydot : nullptr,
+                                            mv ? P.zdot : nullptr);
          })))
       return r;
     const bool irs = p.irsop >= 2 && p.irsop != 4;
@@ -3176,7 +3223,7 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
                                                     L.n0, fd, L.d_rflux);
          else
            k_rans_faces<false><<<g6, 128, 0, c->s>>>(bl, c->d_p, bct, q, nl, P.si, P.sj, P.sk, L.d_h0, P.mut, L.d_vm,
-                                                     L.n0, fd, L.d_rflux);
+                                                     L.n0, fd, L.d_rflux, face_vel_of(c, L));
        })) ||
       (r = for_blocks(c, L, cnt_cells, [&](auto b, dim3 g) {
          (void)b;

@@ -25,10 +25,13 @@ __global__ void k_force_faces(const DevBlock *__restrict__ blocks, const cosa_pa
                               const double *__restrict__ z, const double *__restrict__ si,
                               const double *__restrict__ sj, const double *__restrict__ sk,
                               const double *__restrict__ vm, int64_t n0, const double *__restrict__ xmoms,
-                              double *__restrict__ buf) {
+                              double *__restrict__ buf, const double *__restrict__ cvx = nullptr,
+                              const double *__restrict__ cvy = nullptr, const double *__restrict__ cvz = nullptr) {
   // xmoms: the moment centre of every snapshot (3 doubles each; on moving
   // grids carried with the body, src/output.f90:4476-4485); metrics and
-  // nodes of snapshot n hbmove
+  // nodes of snapshot n hbmove; on moving grids the inverse metrics of
+  // snapshot nh at vm + nh * 27 n0 and the cell grid velocities cv* (node
+  // layout) make the wall derivative one of the velocity relative to the grid
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
   const int64_t total = (int64_t)nfaces * S;
@@ -63,7 +66,7 @@ __global__ void k_force_faces(const DevBlock *__restrict__ blocks, const cosa_pa
     o[4] = (kz * xr - kx * zr) * pw * ds;
     o[5] = (kx * yr - ky * xr) * pw * ds;
     if (P.viscous) {
-      const int64_t vb = ((int64_t)((d - 1) * 3 + (d - 1)) * 3) * n0 + b.of0 * 3 +
+      const int64_t vb = (int64_t)nh * 27 * n0 + ((int64_t)((d - 1) * 3 + (d - 1)) * 3) * n0 + b.of0 * 3 +
                          ((mi - 1) + (int64_t)b.im * ((mj - 1) + (int64_t)b.jm * (mk - 1))) * 3;
       const double ex = vm[vb], ey = vm[vb + 1], ez = vm[vb + 2];
       const double tw = pw * P.gamma / r;
@@ -71,10 +74,19 @@ __global__ void k_force_faces(const DevBlock *__restrict__ blocks, const cosa_pa
       const int64_t c1 = p3_cell(b, F.i + sgn * di, F.j + sgn * dj, F.k + sgn * dk);
       const int64_t c2 = p3_cell(b, F.i + 2 * sgn * di, F.j + 2 * sgn * dj, F.k + 2 * sgn * dk);
       const double r1 = Q(1, c1), r2 = Q(1, c2);
+      // node-layout offsets of the three cells (src/output.f90:4768-4806)
+      const int64_t g0 = b.op2 * S2 + (int64_t)nh * I2 * J2 * (b.km + 2);
+      const int64_t gh = g0 + F.i + I2 * (F.j + J2 * (int64_t)F.k);
+      const int64_t g1 = gh + sgn * (di + I2 * (dj + J2 * (int64_t)dk));
+      const int64_t g2 = gh + 2 * sgn * (di + I2 * (dj + J2 * (int64_t)dk));
       double eta[3];
 #pragma unroll
       for (int m = 0; m < 3; ++m) {
-        const double uw = Q(m + 2, hc) / r, ua = Q(m + 2, c1) / r1, ub = Q(m + 2, c2) / r2;
+        double uw = Q(m + 2, hc) / r, ua = Q(m + 2, c1) / r1, ub = Q(m + 2, c2) / r2;
+        if (cvx) {
+          const double *cv = m == 0 ? cvx : (m == 1 ? cvy : cvz);
+          uw = uw - cv[gh]; ua = ua - cv[g1]; ub = ub - cv[g2];
+        }
         eta[m] = sgn * (-8 * uw + 9 * ua - ub) / 3;
       }
       const double dudx = eta[0] * ex, dudy = eta[0] * ey, dudz = eta[0] * ez;

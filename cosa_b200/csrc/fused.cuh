@@ -132,7 +132,7 @@ __global__ void k_halo(const DevBlock *__restrict__ blocks, const HaloItem *__re
               const int64_t I3 = db.I3, J3 = db.J3;
               const int ci = (int)(it.c1 % I3) - 1, cj = (int)((it.c1 / I3) % J3) - 1;
               const int ck = (int)(it.c1 / (I3 * J3)) - 1;
-              bc_walvis_kom(P, nx, ny, nz, dist[p1_idx(db, 1, ci, cj, ck, 0)], c1, h1, h2);
+              bc_walvis_kom(P, nx, ny, nz, dist[p1_idx(db, 1, ci, cj, ck, 0)], c1, h1, h2, wvp);
             }
           } else {
             st |= COSA_ERR_UNSUPPORTED;

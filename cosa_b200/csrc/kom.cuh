@@ -208,7 +208,7 @@ __global__ void k_rtst(BS bs_, int d, const cosa_params *__restrict__ Pp, const 
     auto Q = [&](const double *a, int v) { return a[p3_var(b, npde, S, v, n) + c]; };
     const double rho = Q(qf, 1), tke = Q(qf, 6), mut = flux[f0_idx(b, npde, S, i, j, k, 1, n)];
     double vmf[9];
-    load_vm(vm, b, n0, d, i, j, k, vmf);
+    load_vm(vm + (int64_t)(n * P.hbmove) * 27 * n0, b, n0, d, i, j, k, vmf);
     double gr[3][3];  // gr[var u,v,w][xi, eta, zeta]
 #pragma unroll
     for (int m = 0; m < 3; ++m) { gr[m][0] = Q(g0, m + 2); gr[m][1] = Q(g1, m + 2); gr[m][2] = Q(g2, m + 2); }
@@ -239,7 +239,7 @@ __global__ void k_vflux_kom(BS bs_, int d, const cosa_params *__restrict__ Pp, c
     const int64_t e = p2_idx(b, S2, 1, i, j, k, nh);
     const double kx = s[e], ky = s[e + 1], kz = s[e + 2], ds = s[e + 3];
     double vmf[9];
-    load_vm(vm, b, n0, d, i, j, k, vmf);
+    load_vm(vm + (int64_t)(n * P.hbmove) * 27 * n0, b, n0, d, i, j, k, vmf);
     const double mut = flux[f0_idx(b, npde, S, i, j, k, 1, n)];
     double f7[7], g[3][7], t6[6], F[7];
 #pragma unroll
@@ -543,7 +543,7 @@ __global__ void k_update_ttrm(BS bs_, const cosa_params *__restrict__ Pp, const 
     const double tt = P.gamma * p / rho;
     const double mu = sutherland(tt, P.stemp);
     double met[3][3];
-    cell_met(vm, b, n0, i, j, k, met);
+    cell_met(vm + (int64_t)(n * P.hbmove) * 27 * n0, b, n0, i, j, k, met);
     const double tkexi = Q(dx, 6), tkeeta = Q(de, 6), tkezeta = Q(dz, 6);
     const double omexi = Q(dx, 7), omeeta = Q(de, 7), omezeta = Q(dz, 7);
     const double dtkedx = tkexi * met[0][0] + tkeeta * met[1][0] + tkezeta * met[2][0];
@@ -582,7 +582,7 @@ __global__ void k_tur_vis_sst(BS bs_, const cosa_params *__restrict__ Pp, const 
     const double tt = P.gamma * p / rho;
     const double mu = sutherland(tt, P.stemp);
     double met[3][3];
-    cell_met(vm, b, n0, i, j, k, met);
+    cell_met(vm + (int64_t)(n * P.hbmove) * 27 * n0, b, n0, i, j, k, met);
     double dv[3][3];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
@@ -733,20 +733,24 @@ __global__ void k_rans_h0(const DevBlock *__restrict__ blocks, int nb, const cos
 template <int D, bool MIXED>
 __device__ __forceinline__ void rans_conv_faces(const DevBlock &b, const cosa_params &P, const int *__restrict__ bct,
                                                 const double *__restrict__ q, int nl, const double *__restrict__ s,
-                                                const double *__restrict__ h0b, double *__restrict__ F) {
+                                                const double *__restrict__ h0b, double *__restrict__ F,
+                                                const double *__restrict__ fv = nullptr) {
   const PhysPar ph = make_phys(P);
-  const int npde = P.npde, S = 2 * P.nharms + 1;
+  const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
   KOM_FACE_LOOP(D)
     double vr[7], vl[7], f[5];
     rans_face_recon<MIXED>(b, P, bct, q, D, nl, i, j, k, n, npde, vr, vl);
-    const int64_t e4 = p2_idx(b, 1, 1, i, j, k, 0);
+    const int nh = n * P.hbmove;
+    const int64_t e4 = p2_idx(b, S2, 1, i, j, k, nh);
     const double kx = s[e4], ky = s[e4 + 1], kz = s[e4 + 2], ds = s[e4 + 3];
+    // the face speed of a moving grid (roflux_b, src/flux.f90:110-113, 262-264)
+    const double ubn = fv ? fv[(e4 >> 2) * 3] * kx + fv[(e4 >> 2) * 3 + 1] * ky + fv[(e4 >> 2) * 3 + 2] * kz : 0.0;
     if (MIXED) roe_flux_mixed_tke(ph, kx, ky, kz, ds, vr, vl, vr[5], vl[5], f);
-    else roe_flux_fp64(ph, kx, ky, kz, ds, vr, vl, vr[5], vl[5], f);
+    else roe_flux_fp64(ph, kx, ky, kz, ds, vr, vl, vr[5], vl[5], f, ubn);
 #pragma unroll
     for (int m = 0; m < 5; ++m) F[f0_idx(b, npde, S, i, j, k, m + 1, n)] = f[m];
     double fk, fw;
-    roe_turb(P, kx, ky, kz, ds, vr, vl, h0b[2 * n], h0b[2 * n + 1], fk, fw);
+    roe_turb(P, kx, ky, kz, ds, vr, vl, h0b[2 * n], h0b[2 * n + 1], fk, fw, ubn);
     F[f0_idx(b, npde, S, i, j, k, 6, n)] = fk;
     F[f0_idx(b, npde, S, i, j, k, 7, n)] = fw;
   }
@@ -787,8 +791,8 @@ __device__ __forceinline__ void rans_visc_faces(const DevBlock &b, int ib, const
       if (NV == 7) mf = mut[p3s_idx(b, S, D == 1 ? a : i, D == 2 ? a : j, D == 3 ? a : k, n)];
     }
     double vmf[9];
-    load_vm(vm, b, n0, D, i, j, k, vmf);
-    const int64_t e4 = p2_idx(b, 1, 1, i, j, k, 0);
+    load_vm(vm + (int64_t)(n * P.hbmove) * 27 * n0, b, n0, D, i, j, k, vmf);
+    const int64_t e4 = p2_idx(b, 2 * P.nharms * P.hbmove + 1, 1, i, j, k, n * P.hbmove);
     double Fv[NV];
     if constexpr (NV == 7) {
       double gr[3][3], t6[6];
@@ -816,7 +820,8 @@ __global__ void __launch_bounds__(128, 3) k_rans_faces(BlockList bs_, const cosa
                                                        const double *__restrict__ sj, const double *__restrict__ sk,
                                                        const double *__restrict__ h0, const double *__restrict__ mut,
                                                        const double *__restrict__ vm, int64_t n0,
-                                                       const double *__restrict__ fd, double *__restrict__ rf) {
+                                                       const double *__restrict__ fd, double *__restrict__ rf,
+                                                       FaceVel fvel = FaceVel{{nullptr, nullptr, nullptr}}) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int S = 2 * P.nharms + 1, z = blockIdx.z, d = z % 3 + 1;
@@ -824,9 +829,10 @@ __global__ void __launch_bounds__(128, 3) k_rans_faces(BlockList bs_, const cosa
   double *F = rf + (int64_t)z * n0 * P.npde * S;
   if (z < 3) {
     const double *h0b = h0 + ((int64_t)blockIdx.y * 3 + (d - 1)) * S * 2;
-    if (d == 1) rans_conv_faces<1, MIXED>(b, P, bct, q, nl, s, h0b, F);
-    else if (d == 2) rans_conv_faces<2, MIXED>(b, P, bct, q, nl, s, h0b, F);
-    else rans_conv_faces<3, MIXED>(b, P, bct, q, nl, s, h0b, F);
+    const double *fv = fvel.f[d - 1];
+    if (d == 1) rans_conv_faces<1, MIXED>(b, P, bct, q, nl, s, h0b, F, fv);
+    else if (d == 2) rans_conv_faces<2, MIXED>(b, P, bct, q, nl, s, h0b, F, fv);
+    else rans_conv_faces<3, MIXED>(b, P, bct, q, nl, s, h0b, F, fv);
   } else {
     const double *fdd = fd ? fd + (int64_t)(d - 1) * n0 : nullptr;
     if (d == 1) rans_visc_faces<1>(b, blockIdx.y, P, bct, q, mut, vm, n0, s, fdd, F);
@@ -955,7 +961,7 @@ __global__ void k_rans_cellsrc(BlockList bs_, const cosa_params *__restrict__ Pp
       }
     }
     double met[3][3];
-    if (own_prod || BLEND) cell_met(vm, b, n0, i, j, k, met);
+    if (own_prod || BLEND) cell_met(vm + (int64_t)(n * P.hbmove) * 27 * n0, b, n0, i, j, k, met);
     double prod, divv;
     if (own_prod) {
       // turprod_b (src/src.f90:40-177)

@@ -863,11 +863,11 @@ __device__ __forceinline__ int bc_walvis(double g, const double *c1, const doubl
 // the snapshot (the reference does not recompute them in this loop).
 __device__ __forceinline__ void roe_turb(const cosa_params &P, double kx, double ky, double kz, double ds,
                                          const double *qr, const double *ql, double h0r_last, double h0l_last,
-                                         double &fk, double &fw) {
+                                         double &fk, double &fw, double ubn = 0.0) {
   const double g = P.gamma;
   const double rhor = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4], tker = qr[5], omer = qr[6];
   const double rhol = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4], tkel = ql[5], omel = ql[6];
-  const double unr = ur * kx + vr * ky + wr * kz, unl = ul * kx + vl * ky + wl * kz;
+  const double unr = ur * kx + vr * ky + wr * kz - ubn, unl = ul * kx + vl * ky + wl * kz - ubn;
   const double frk = rhor * unr * tker, frw = rhor * unr * omer;
   const double flk = rhol * unl * tkel, flw = rhol * unl * omel;
   const double drho = rhor - rhol, dp = pr - pl, dun = unr - unl, dtke = tker - tkel, dome = omer - omel;
@@ -881,10 +881,10 @@ __device__ __forceinline__ void roe_turb(const cosa_params &P, double kx, double
   const double q2 = u * u + v * v + w * w;
   const double a2 = (g - 1) * (h0 - q2 / 2 - tke);
   const double a = sqrt(a2);
-  double rm123 = fabs(un), rm4 = fabs(un + a), rm5 = fabs(un - a);
+  double rm123 = fabs(un - ubn), rm4 = fabs(un + a - ubn), rm5 = fabs(un - a - ubn);
   if (P.efx_setup_t) {
     double rdelta = P.cntrpy_t * (P.entfx_t_w[0] * P.entfxctf_t + P.entfx_t_w[1] * (sqrt(q2) + a) +
-                                  P.entfx_t_w[2] * 0.2 * (fabs(un) + a + 0.0));
+                                  P.entfx_t_w[2] * 0.2 * (fabs(un) + a + fabs(ubn)));
     rdelta = fmax(rdelta, 1.0e-12);
     if (rm123 <= rdelta && P.efx_all_t) rm123 = 0.5 * (rm123 * rm123 + rdelta * rdelta) / rdelta;
     if (rm4 <= rdelta) rm4 = 0.5 * (rm4 * rm4 + rdelta * rdelta) / rdelta;
@@ -912,14 +912,16 @@ __device__ __forceinline__ double face_h0(double g, const double *q) {
 // h1 holds the wall state (laminar part already applied), c1 the first
 // cell; d = wall distance of the first cell, (nx, ny, nz) the face normal
 __device__ __forceinline__ void bc_walvis_kom(const cosa_params &P, double nx, double ny, double nz, double d,
-                                              const double *c1, double *h1, double *h2) {
+                                              const double *c1, double *h1, double *h2,
+                                              const double *wv = nullptr) {
   const double small = 1.0e-12, smasq = 1.0e-24, mor = P.machfs / P.reyno;
   const double rhow = h1[0], pw = h1[4];
   const double tw = pw * P.gamma / rhow;
   const double muw = (P.stemp + 1) / (tw + P.stemp) * pow(tw, 1.5);
   double omew;
   if (P.wallwilc) {
-    const double uc = c1[1], vc = c1[2], wc = c1[3];
+    // the first cell's velocity relative to a moving wall face (src/bc.f90:2346-2394)
+    const double uc = wv ? c1[1] - wv[0] : c1[1], vc = wv ? c1[2] - wv[1] : c1[2], wc = wv ? c1[3] - wv[2] : c1[3];
     const double uorth = nx * uc + ny * vc + nz * wc;
     const double a = uc - uorth * nx, b = vc - uorth * ny, c = wc - uorth * nz;
     const double upar = sqrt(a * a + b * b + c * c);

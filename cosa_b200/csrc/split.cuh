@@ -77,7 +77,10 @@ __global__ void k_dt_euler(const DevBlock *__restrict__ blocks, const cosa_param
 // every interior cell (the tile kernel's epilogue; the time step is already
 // in dtvol); per-CTA norm partials at part[(block * gridDim.x + blockIdx.x) * 8 + m]
 template <bool RMS>
-__global__ void __launch_bounds__(256, 2) k_cells(const DevBlock *__restrict__ blocks, const cosa_params *__restrict__ Pp,
+#ifndef COSA_CELLS_MINB
+#define COSA_CELLS_MINB 2  // resident CTAs per SM k_cells is compiled for
+#endif
+__global__ void __launch_bounds__(256, COSA_CELLS_MINB) k_cells(const DevBlock *__restrict__ blocks, const cosa_params *__restrict__ Pp,
                                                StageArgs A, const double *__restrict__ cf, int64_t n0,
                                                int blk0) {
   __shared__ double red[8][8];

@@ -479,7 +479,8 @@ __device__ __forceinline__ void eig_ns_cell(const DevBlock &b, const cosa_params
                                             const double *__restrict__ si, const double *__restrict__ sj,
                                             const double *__restrict__ sk, int S2, int nh, double volc, int i, int j,
                                             int k, double lam[3], double lamv[3], const double *mut = nullptr,
-                                            int S = 1, int n = 0, double lsp_cut = -1.0, double lsp_eps2 = 0.0) {
+                                            int S = 1, int n = 0, double lsp_cut = -1.0, double lsp_eps2 = 0.0,
+                                            const double *gv = nullptr) {
   const double g = P.gamma, st = P.stemp;
   double qc[5], sm[3][4], sp[3][4];
 #pragma unroll
@@ -493,7 +494,7 @@ __device__ __forceinline__ void eig_ns_cell(const DevBlock &b, const cosa_params
   if (lsp_cut >= 0)  // eig_ns_p: the preconditioned convective radii (src/cosa.f90:4374-4460)
     eig_eul_p(g, P.uprv, lsp_eps2, lsp_cut, qc, sm[0], sp[0], sm[1], sp[1], sm[2], sp[2], lam[0], lam[1], lam[2]);
   else
-    eig_eul(g, qc, sm[0], sp[0], sm[1], sp[1], sm[2], sp[2], lam[0], lam[1], lam[2]);
+    eig_eul(g, qc, sm[0], sp[0], sm[1], sp[1], sm[2], sp[2], lam[0], lam[1], lam[2], gv);
   const double rho = qc[0];
   const double mu = sutherland(g * qc[4] / rho, st);
   auto MUT = [&](int a, int c, int e) { return mut ? mut[b.op3 * S + (int64_t)n * b.P3 + p3_cell(b, a, c, e)] : 0.0; };
@@ -572,7 +573,8 @@ __global__ void k_lambda_ns(BS bs_, const cosa_params *__restrict__ Pp, const do
                             const double *__restrict__ sk, const double *__restrict__ vol,
                             const double *__restrict__ mut, double *__restrict__ lam, double *__restrict__ lamv,
                             const double *__restrict__ cpg = nullptr, const double *__restrict__ cvs = nullptr,
-                            int nl = 1) {
+                            int nl = 1, const double *__restrict__ cvx = nullptr,
+                            const double *__restrict__ cvy = nullptr, const double *__restrict__ cvz = nullptr) {
   const DevBlock b = bs_.get();
   const cosa_params &P = *Pp;
   const int npde = P.npde, S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
@@ -591,8 +593,15 @@ __global__ void k_lambda_ns(BS bs_, const cosa_params *__restrict__ Pp, const do
       const int64_t m = b.om1 * S + (int64_t)n * ni * nj * nk + (i - 1) + (int64_t)ni * ((j - 1) + (int64_t)nj * (k - 1));
       cut = fmax(cpg[m], cvs[m]);
     }
+    double gv[3];
+    if (cvx) {
+      // cell grid velocity of a moving grid (node-array layout, snapshot nh)
+      const int64_t I2 = b.im + 2, J2 = b.jm + 2, K2 = b.km + 2;
+      const int64_t gi = b.op2 * S2 + (int64_t)nh * I2 * J2 * K2 + i + I2 * (j + J2 * (int64_t)k);
+      gv[0] = cvx[gi]; gv[1] = cvy[gi]; gv[2] = cvz[gi];
+    }
     eig_ns_cell(b, P, Q, si, sj, sk, S2, nh, vol[p1_idx(b, 1, i, j, k, 0)], i, j, k, l, lv, mut, S, n, cut,
-                P.epsp[nl - 1] * P.epsp[nl - 1]);
+                P.epsp[nl - 1] * P.epsp[nl - 1], cvx ? gv : nullptr);
     const int64_t c = p3_cell(b, i, j, k);
 #pragma unroll
     for (int m = 0; m < 3; ++m) {

@@ -347,8 +347,10 @@ class Context:
 
     # ---- laminar viscous terms -------------------------------------------------------
     def alloc_vm(self, nl=1):
-        """The nine face inverse-metric arrays of level nl (27 * n0 doubles)."""
-        return DevArray(self, self.sizes(nl)[3] * 27)
+        """The nine face inverse-metric arrays of level nl (27 * n0 doubles);
+        on a moving grid one set per node snapshot."""
+        nsnap = self.S if self.params.moving and self.params.hbmove else 1
+        return DevArray(self, self.sizes(nl)[3] * 27 * nsnap)
 
     def coordex(self, nl, x, y, z):
         self._check(load().cosa_gpu_coordex(self.h, nl, _ptr(x.ptr), _ptr(y.ptr), _ptr(z.ptr)), "coordex")

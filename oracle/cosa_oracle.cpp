@@ -750,7 +750,7 @@ int bc_level(const Level &L, double *qa, const double *si, const double *sj, con
         case 21: status |= bc_insub(pa, q, vi, vj, vk, L, P, nl); break;
         case 91: bc_outsub(pa, q, L, P); break;
         default:
-          if (pa.bctyp / 100 == 15 && (!P.moving || !is_kom(P)) && (!is_kom(P) || dist)) {
+          if (pa.bctyp / 100 == 15 && (!is_kom(P) || dist)) {
             bc_walvis_15(pa, q, L, P);
             if (is_kom(P)) bc_walvis_15_kom(pa, q, vi, vj, vk, dist, L, b, P);
           } else if (pa.bctyp / 100 == 15) {
@@ -1186,13 +1186,14 @@ void roflux_turb(const Level &L, int b, int d, B3 &qr, B3 &ql, B0 &flux, const B
     for (int j = 1; j <= jc; ++j)
       for (int i = 1; i <= ic; ++i) {
         const double kx = s(1, i, j, k, nh), ky = s(2, i, j, k, nh), kz = s(3, i, j, k, nh), ds = s(4, i, j, k, nh);
+        const double ubn = P.moving ? face_ubn(L, b, d, i, j, k, nh, kx, ky, kz) : 0.0;
         const double rhor = qr(i, j, k, 1, n), ur = qr(i, j, k, 2, n), vr = qr(i, j, k, 3, n), wr = qr(i, j, k, 4, n);
         const double pr = qr(i, j, k, 5, n), omer = qr(i, j, k, 7, n), tker = qr(i, j, k, 6, n);
-        const double unr = ur * kx + vr * ky + wr * kz;
+        const double unr = ur * kx + vr * ky + wr * kz - ubn;
         const double frk = rhor * unr * tker, frw = rhor * unr * omer;
         const double rhol = ql(i, j, k, 1, n), ul = ql(i, j, k, 2, n), vl = ql(i, j, k, 3, n), wl = ql(i, j, k, 4, n);
         const double pl = ql(i, j, k, 5, n), omel = ql(i, j, k, 7, n), tkel = ql(i, j, k, 6, n);
-        const double unl = ul * kx + vl * ky + wl * kz;
+        const double unl = ul * kx + vl * ky + wl * kz - ubn;
         const double flk = rhol * unl * tkel, flw = rhol * unl * omel;
         const double drho = rhor - rhol, dp = pr - pl, dun = unr - unl, dtke = tker - tkel, dome = omer - omel;
         const double rhols = std::sqrt(rhol), rhors = std::sqrt(rhor);
@@ -1205,10 +1206,10 @@ void roflux_turb(const Level &L, int b, int d, B3 &qr, B3 &ql, B0 &flux, const B
         const double q2 = u * u + v * v + w * w;
         const double a2 = (g - 1) * (h0 - q2 / 2 - tke);
         const double a = std::sqrt(a2);
-        double rm123 = std::fabs(un), rm4 = std::fabs(un + a), rm5 = std::fabs(un - a);
+        double rm123 = std::fabs(un - ubn), rm4 = std::fabs(un + a - ubn), rm5 = std::fabs(un - a - ubn);
         if (P.efx_setup_t) {
           double rdelta = P.cntrpy_t * (P.entfx_t_w[0] * P.entfxctf_t + P.entfx_t_w[1] * (std::sqrt(q2) + a) +
-                                        P.entfx_t_w[2] * 0.2 * (std::fabs(un) + a + 0.0));
+                                        P.entfx_t_w[2] * 0.2 * (std::fabs(un) + a + std::fabs(ubn)));
           rdelta = std::max(rdelta, 1.0e-12);
           if (rm123 <= rdelta && P.efx_all_t) rm123 = 0.5 * (rm123 * rm123 + rdelta * rdelta) / rdelta;
           if (rm4 <= rdelta) rm4 = 0.5 * (rm4 * rm4 + rdelta * rdelta) / rdelta;
@@ -2490,9 +2491,11 @@ void tur_vis_level(const Level &L, const double *qa, double *muta, const cosa_pa
 }
 
 // ---- viscous set-up (src/grid.f90) -----------------------------------------
-struct BGw {  // writable grid view (0:im+1, 0:jm+1, 0:km+1)
+struct BGw {  // writable grid view (0:im+1, 0:jm+1, 0:km+1) of snapshot nh (moving grids: dim5h snapshots)
   double *p; int I, J;
-  BGw(double *base, const Level &L, int b) : I(L.im[b] + 2), J(L.jm[b] + 2) { p = base + L.op2[b]; }
+  BGw(double *base, const Level &L, int b, int nh = 0) : I(L.im[b] + 2), J(L.jm[b] + 2) {
+    p = base + L.op2[b] * L.dim5h + (int64_t)nh * I * J * (L.km[b] + 2);
+  }
   inline double &operator()(int i, int j, int k) const { return p[i + (int64_t)I * (j + (int64_t)J * k)]; }
 };
 struct BV {  // face inverse metrics (3, imax, jmax, kmax), 1-based face index
@@ -2503,12 +2506,16 @@ struct BV {  // face inverse metrics (3, imax, jmax, kmax), 1-based face index
   }
 };
 
+// the face inverse metrics of grid snapshot nh (moving grids keep one set of
+// 27 n0 values per snapshot, xideri(.., 0:2*nharms*hbmove))
+inline const double *vm_snap(const Level &L, const double *vm, int nh) { return vm + (int64_t)nh * 27 * L.n0; }
+
 // cordex_b (src/grid.f90:20-80): ghost nodes repeat the boundary nodes
-void coordex_level(const Level &L, double *xa, double *ya, double *za) {
+void coordex_level(const Level &L, double *xa, double *ya, double *za, int nh = 0) {
   for (int b = 0; b < L.nb; ++b) {
     const int im = L.im[b], jm = L.jm[b], km = L.km[b];
     for (double *a : {xa, ya, za}) {
-      BGw X(a, L, b);
+      BGw X(a, L, b, nh);
       for (int k = 1; k <= km; ++k) {
         for (int i = 1; i <= im; ++i) { X(i, 0, k) = X(i, 1, k); X(i, jm + 1, k) = X(i, jm, k); }
         for (int j = 1; j <= jm; ++j) { X(0, j, k) = X(1, j, k); X(im + 1, j, k) = X(im, j, k); }
@@ -2521,7 +2528,7 @@ void coordex_level(const Level &L, double *xa, double *ya, double *za) {
 
 // cut_x, in-process branch (src/grid.f90:242-523): the ghost node plane of
 // block 1 takes the nodes one plane inside block 2
-void cutman_x_level(const Level &L, double *xa, double *ya, double *za) {
+void cutman_x_level(const Level &L, double *xa, double *ya, double *za, int nh = 0) {
   for (int icut = 0; icut < L.ncuts; ++icut) {
     const int *c = L.cut.data() + 21 * icut;
     const int b1 = c[0] - 1, b2 = c[9] - 1;
@@ -2545,7 +2552,7 @@ void cutman_x_level(const Level &L, double *xa, double *ya, double *za) {
     const int ic1 = cyc(idir1, 1), ic2 = cyc(idir1, 2), ic3 = cyc(idir1, 3);
     const int jc1 = iord[ic1], jc2 = iord[ic2], jc3 = iord[ic3];
     for (double *a : {xa, ya, za}) {
-      BGw X1(a, L, b1), X2(a, L, b2);
+      BGw X1(a, L, b1, nh), X2(a, L, b2, nh);
       for (int i3 = 0; i3 <= len[ic3]; ++i3)
         for (int i2 = 0; i2 <= len[ic2]; ++i2) {
           const int a2_ = istr1[ic2] + isgn1[ic2] * i2, a3_ = istr1[ic3] + isgn1[ic3] * i3;
@@ -2618,8 +2625,8 @@ void cutman_v_level(const Level &L, double *va) {
 // (coordex), divided by the mean volume of the two cells of the face.
 // vm[m] receives (xi, eta, zeta)_(x, y, z) for m = xi, eta, zeta.
 void vmetrix_b(const Level &L, int b, int d, const double *xa, const double *ya, const double *za,
-               const double *va, double *vm0, double *vm1, double *vm2) {
-  BGw X(const_cast<double *>(xa), L, b), Y(const_cast<double *>(ya), L, b), Z(const_cast<double *>(za), L, b);
+               const double *va, double *vm0, double *vm1, double *vm2, int nh = 0) {
+  BGw X(const_cast<double *>(xa), L, b, nh), Y(const_cast<double *>(ya), L, b, nh), Z(const_cast<double *>(za), L, b, nh);
   B1 vol(const_cast<double *>(va), L, b, 1);
   BV o0(vm0, L, b), o1(vm1, L, b), o2(vm2, L, b);
   const int im = L.im[b], jm = L.jm[b], km = L.km[b];
@@ -2801,7 +2808,7 @@ void vflux_b(const Level &L, int b, int d, const double *qfa, const double *dxa,
              double *fa, const cosa_params &P, bool kom = false) {
   B3 qf(const_cast<double *>(qfa), L, b), dqx(const_cast<double *>(dxa), L, b);
   B3 dqe(const_cast<double *>(dya), L, b), dqz(const_cast<double *>(dza), L, b);
-  BV xv(const_cast<double *>(xd), L, b), ev(const_cast<double *>(ed), L, b), zv(const_cast<double *>(zd), L, b);
+  const int64_t vms = 27 * L.n0;  // per grid snapshot
   B2 s(sijk, L, b);
   B0 flux(fa, L, b);
   const int im = L.im[b], jm = L.jm[b], km = L.km[b];
@@ -2824,6 +2831,8 @@ void vflux_b(const Level &L, int b, int d, const double *qfa, const double *dxa,
           const double t = g * p / rho;
           const double mu = (P.stemp + 1) / (t + P.stemp) * std::pow(t, 1.5);
           const double mut = flux(i, j, k, 1, n);
+          const BV xv(const_cast<double *>(xd) + n * P.hbmove * vms, L, b), ev(const_cast<double *>(ed) + n * P.hbmove * vms, L, b),
+              zv(const_cast<double *>(zd) + n * P.hbmove * vms, L, b);
           const double xix = xv(1, i, j, k), xiy = xv(2, i, j, k), xiz = xv(3, i, j, k);
           const double etax = ev(1, i, j, k), etay = ev(2, i, j, k), etaz = ev(3, i, j, k);
           const double zetax = zv(1, i, j, k), zetay = zv(2, i, j, k), zetaz = zv(3, i, j, k);
@@ -2942,7 +2951,13 @@ void lambda_ns_level(const Level &L, const double *qa, const double *si, const d
               sjm[c] = vj(c, i, j, k, nh); sjp[c] = vj(c, i, j + 1, k, nh);
               skm[c] = vk(c, i, j, k, nh); skp[c] = vk(c, i, j, k + 1, nh);
             }
-            const double u = q(i, j, k, 2, n), v = q(i, j, k, 3, n), w = q(i, j, k, 4, n);
+            double u = q(i, j, k, 2, n), v = q(i, j, k, 3, n), w = q(i, j, k, 4, n);
+            if (P.moving && L.cv[0]) {
+              // eig_ns: velocity relative to the cell's grid velocity (src/cosa.f90:4283-4287)
+              u = u - BGs(L.cv[0], L, b, nh)(i, j, k);
+              v = v - BGs(L.cv[1], L, b, nh)(i, j, k);
+              w = w - BGs(L.cv[2], L, b, nh)(i, j, k);
+            }
             const double a = std::sqrt(t);
             const double xix = 0.5 * (sim[1] * sim[4] + sip[1] * sip[4]);
             const double xiy = 0.5 * (sim[2] * sim[4] + sip[2] * sip[4]);
@@ -3088,7 +3103,14 @@ void bc_walvis_15_kom(const Patch &pa, B3 &q, const B2 &si, const B2 &sj, const 
         double omew;
         if (P.wallwilc) {
           const double nx = sf(1, mi, mj, mk, nh), ny = sf(2, mi, mj, mk, nh), nz = sf(3, mi, mj, mk, nh);
-          const double uc = q(ni_, nj_, nk_, 2, n), vc = q(ni_, nj_, nk_, 3, n), wc = q(ni_, nj_, nk_, 4, n);
+          double uw = 0.0, vw = 0.0, ww = 0.0;
+          if (P.moving && L.fv[pa.idir - 1]) {
+            // velocity relative to the moving wall face (src/bc.f90:2346-2368, 2392-2394)
+            BFv f(L.fv[pa.idir - 1], L, b);
+            uw = f(1, mi, mj, mk, nh); vw = f(2, mi, mj, mk, nh); ww = f(3, mi, mj, mk, nh);
+          }
+          const double uc = q(ni_, nj_, nk_, 2, n) - uw, vc = q(ni_, nj_, nk_, 3, n) - vw;
+          const double wc = q(ni_, nj_, nk_, 4, n) - ww;
           const double uorth = nx * uc + ny * vc + nz * wc;
           const double a = uc - uorth * nx, bb = vc - uorth * ny, c = wc - uorth * nz;
           const double upar = std::sqrt(a * a + bb * bb + c * c);
@@ -3144,7 +3166,7 @@ void rtst_b(const Level &L, int b, int d, const double *qfa, const double *dxa, 
             const cosa_params &P) {
   B3 qf(const_cast<double *>(qfa), L, b), dqx(const_cast<double *>(dxa), L, b);
   B3 dqe(const_cast<double *>(dya), L, b), dqz(const_cast<double *>(dza), L, b), tau(taua, L, b);
-  BV xv(const_cast<double *>(xd), L, b), ev(const_cast<double *>(ed), L, b), zv(const_cast<double *>(zd), L, b);
+  const int64_t vms = 27 * L.n0;  // per grid snapshot
   B0 f(const_cast<double *>(fa), L, b);
   const int im = L.im[b], jm = L.jm[b], km = L.km[b];
   const int ni = d == 1 ? im : im - 1, nj = d == 2 ? jm : jm - 1, nk = d == 3 ? km : km - 1;
@@ -3154,6 +3176,8 @@ void rtst_b(const Level &L, int b, int d, const double *qfa, const double *dxa, 
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) {
           const double rho = qf(i, j, k, 1, n), tke = qf(i, j, k, 6, n), mut = f(i, j, k, 1, n);
+          const BV xv(const_cast<double *>(xd) + n * P.hbmove * vms, L, b), ev(const_cast<double *>(ed) + n * P.hbmove * vms, L, b),
+              zv(const_cast<double *>(zd) + n * P.hbmove * vms, L, b);
           const double xix = xv(1, i, j, k), xiy = xv(2, i, j, k), xiz = xv(3, i, j, k);
           const double etax = ev(1, i, j, k), etay = ev(2, i, j, k), etaz = ev(3, i, j, k);
           const double zetax = zv(1, i, j, k), zetay = zv(2, i, j, k), zetaz = zv(3, i, j, k);
@@ -3191,7 +3215,7 @@ void vflux_kom_b(const Level &L, int b, int d, const double *qfa, const double *
                  const double *sijk, double *fa, const cosa_params &P, const double *fdista = nullptr) {
   B3 qf(const_cast<double *>(qfa), L, b), dqx(const_cast<double *>(dxa), L, b);
   B3 dqe(const_cast<double *>(dya), L, b), dqz(const_cast<double *>(dza), L, b), tau(const_cast<double *>(taua), L, b);
-  BV xv(const_cast<double *>(xd), L, b), ev(const_cast<double *>(ed), L, b), zv(const_cast<double *>(zd), L, b);
+  const int64_t vms = 27 * L.n0;  // per grid snapshot
   B2 s(sijk, L, b);
   B0 flux(fa, L, b);
   const int im = L.im[b], jm = L.jm[b], km = L.km[b];
@@ -3206,6 +3230,8 @@ void vflux_kom_b(const Level &L, int b, int d, const double *qfa, const double *
           const double t = P.gamma * p / rho;
           const double mu = (P.stemp + 1) / (t + P.stemp) * std::pow(t, 1.5);
           const double mut = flux(i, j, k, 1, n);
+          const BV xv(const_cast<double *>(xd) + n * P.hbmove * vms, L, b), ev(const_cast<double *>(ed) + n * P.hbmove * vms, L, b),
+              zv(const_cast<double *>(zd) + n * P.hbmove * vms, L, b);
           const double xix = xv(1, i, j, k), xiy = xv(2, i, j, k), xiz = xv(3, i, j, k);
           const double etax = ev(1, i, j, k), etay = ev(2, i, j, k), etaz = ev(3, i, j, k);
           const double zetax = zv(1, i, j, k), zetay = zv(2, i, j, k), zetaz = zv(3, i, j, k);
@@ -3272,15 +3298,16 @@ void turprod_b(const Level &L, int b, const double *qa, const double *dxa, const
   B3 dqe(const_cast<double *>(dya), L, b), dqz(const_cast<double *>(dza), L, b);
   B3s prd(prda, L, b), dvv(diva, L, b), dpl(dpla, L, b);
   // vm array (d, m): derivative m on faces of family d
-  auto V = [&](int d, int m) { return BV(const_cast<double *>(vm) + (int64_t)((d - 1) * 3 + m) * 3 * L.n0, L, b); };
-  BV xi_i = V(1, 0), xi_j = V(2, 0), xi_k = V(3, 0);
-  BV et_i = V(1, 1), et_j = V(2, 1), et_k = V(3, 1);
-  BV ze_i = V(1, 2), ze_j = V(2, 2), ze_k = V(3, 2);
   const double fact = 2.0 / 3.0;
   for (int n = 0; n < L.S; ++n)
     for (int k = 1; k <= L.km[b] - 1; ++k)
       for (int j = 1; j <= L.jm[b] - 1; ++j)
         for (int i = 1; i <= L.im[b] - 1; ++i) {
+          const double *vmn = vm_snap(L, vm, n * P.hbmove);
+          auto V = [&](int d, int m) { return BV(const_cast<double *>(vmn) + (int64_t)((d - 1) * 3 + m) * 3 * L.n0, L, b); };
+          const BV xi_i = V(1, 0), xi_j = V(2, 0), xi_k = V(3, 0);
+          const BV et_i = V(1, 1), et_j = V(2, 1), et_k = V(3, 1);
+          const BV ze_i = V(1, 2), ze_j = V(2, 2), ze_k = V(3, 2);
           const double xix = (xi_i(1, i + 1, j, k) + xi_i(1, i, j, k)) / 2;
           const double xiy = (xi_j(2, i, j + 1, k) + xi_j(2, i, j, k)) / 2;
           const double xiz = (xi_k(3, i, j, k + 1) + xi_k(3, i, j, k)) / 2;
@@ -3424,7 +3451,7 @@ void update_ttrm_b(const Level &L, int b, const double *qa, const double *dxa, c
           const double rho = q(i, j, k, 1, n), tke = q(i, j, k, 6, n), ome = q(i, j, k, 7, n), p = q(i, j, k, 5, n);
           const double t = P.gamma * p / rho;
           const double mu = (P.stemp + 1) / (t + P.stemp) * std::pow(t, 1.5);
-          const CellMet m = cell_met(L, b, vm, i, j, k);
+          const CellMet m = cell_met(L, b, vm_snap(L, vm, n * P.hbmove), i, j, k);
           const double tkexi = dqx(i, j, k, 6, n), tkeeta = dqe(i, j, k, 6, n), tkezeta = dqz(i, j, k, 6, n);
           const double omexi = dqx(i, j, k, 7, n), omeeta = dqe(i, j, k, 7, n), omezeta = dqz(i, j, k, 7, n);
           const double dtkedx = tkexi * m.xix + tkeeta * m.etax + tkezeta * m.zetax;
@@ -3499,7 +3526,7 @@ void tur_vis_sst_level(const Level &L, const double *qa, double *muta, const dou
             const double rho = q1, tke = q(i, j, k, 6, n) / rho, ome = q(i, j, k, 7, n) / rho;
             const double t = P.gamma * p / rho;
             const double mu = (P.stemp + 1) / (t + P.stemp) * std::pow(t, 1.5);
-            const CellMet m = cell_met(L, b, vm, i, j, k);
+            const CellMet m = cell_met(L, b, vm_snap(L, vm, n * P.hbmove), i, j, k);
             const double uxi = dqx(i, j, k, 2, n), ueta = dqe(i, j, k, 2, n), uzeta = dqz(i, j, k, 2, n);
             const double vxi = dqx(i, j, k, 3, n), veta = dqe(i, j, k, 3, n), vzeta = dqz(i, j, k, 3, n);
             const double wxi = dqx(i, j, k, 4, n), weta = dqe(i, j, k, 4, n), wzeta = dqz(i, j, k, 4, n);
@@ -3611,14 +3638,19 @@ void cutman_mut_level(const Level &L, double *muta) {
 // 300-322): volume and node halos, then the face inverse metrics.
 // vm holds the 9 arrays (xi, eta, zeta derivatives on i-, j-, k-faces),
 // array (d, m) at vm + ((d-1)*3 + m) * 3 * n0.
+// viscous set-up (src/cosa.f90:300-322); moving grids: the ghost nodes and
+// cuts and one set of face inverse metrics per grid snapshot
 void viscous_setup_level(const Level &L, double *x, double *y, double *z, double *vol, double *vm) {
   volex_level(L, vol);
   cutman_v_level(L, vol);
-  coordex_level(L, x, y, z);
-  cutman_x_level(L, x, y, z);
-  for (int d = 1; d <= 3; ++d) {
-    double *a = vm + (int64_t)(d - 1) * 9 * L.n0;
-    for (int b = 0; b < L.nb; ++b) vmetrix_b(L, b, d, x, y, z, vol, a, a + 3 * L.n0, a + 6 * L.n0);
+  for (int nh = 0; nh < L.dim5h; ++nh) {
+    coordex_level(L, x, y, z, nh);
+    cutman_x_level(L, x, y, z, nh);
+    double *vn = vm + (int64_t)nh * 27 * L.n0;
+    for (int d = 1; d <= 3; ++d) {
+      double *a = vn + (int64_t)(d - 1) * 9 * L.n0;
+      for (int b = 0; b < L.nb; ++b) vmetrix_b(L, b, d, x, y, z, vol, a, a + 3 * L.n0, a + 6 * L.n0, nh);
+    }
   }
 }
 
@@ -3696,7 +3728,7 @@ void force_level(const Level &L, const double *qa, const double *xa, const doubl
         const int ibcpt = in1 ? 0 : ijk[d], ibcm = in1 ? 1 : ijk[d], ibcw = in1 ? 0 : ijk[d];
         const int sgn = in1 ? 1 : -1;  // (-1)**(1+1/inrout)
         const B2 &s = sd[d - 1];
-        BV vd(vm ? const_cast<double *>(vm) + (int64_t)((d - 1) * 3 + (d - 1)) * 3 * L.n0 : nullptr, L, b);
+        BV vd(vm ? const_cast<double *>(vm_snap(L, vm, nh)) + (int64_t)((d - 1) * 3 + (d - 1)) * 3 * L.n0 : nullptr, L, b);
         auto pw_of = [&](int i, int j, int k) {
           const double r = q(i, j, k, 1, n);
           return (P.gamma - 1) * (q(i, j, k, 5, n) - q(i, j, k, 2, n) * q(i, j, k, 2, n) / r / 2 -
@@ -3730,8 +3762,8 @@ void force_level(const Level &L, const double *qa, const double *xa, const doubl
             pidx(pa, ibcm, i2, i3, mi, mj, mk);
             pidx(pa, ibcw, i2, i3, wi, wj, wk);
             const int o1[3] = {sgn * krd(d, 1), sgn * krd(d, 2), sgn * krd(d, 3)};
-            const double kx = sgn * s(1, mi, mj, mk, 0), ky = sgn * s(2, mi, mj, mk, 0);
-            const double kz = sgn * s(3, mi, mj, mk, 0), ds = s(4, mi, mj, mk, 0);
+            const double kx = sgn * s(1, mi, mj, mk, nh), ky = sgn * s(2, mi, mj, mk, nh);
+            const double kz = sgn * s(3, mi, mj, mk, nh), ds = s(4, mi, mj, mk, nh);
             const double ex = vd(1, mi, mj, mk), ey = vd(2, mi, mj, mk), ez = vd(3, mi, mj, mk);
             const double rhow = q(hi, hj, hk, 1, n);
             const double pw = pw_of(hi, hj, hk);
@@ -3743,7 +3775,15 @@ void force_level(const Level &L, const double *qa, const double *xa, const doubl
               const double u1 = q(hi + o1[0], hj + o1[1], hk + o1[2], m + 2, n) / q(hi + o1[0], hj + o1[1], hk + o1[2], 1, n);
               const double u2 = q(hi + 2 * o1[0], hj + 2 * o1[1], hk + 2 * o1[2], m + 2, n) /
                                 q(hi + 2 * o1[0], hj + 2 * o1[1], hk + 2 * o1[2], 1, n);
-              eta[m] = sgn * (-8 * uw + 9 * u1 - u2) / 3;
+              double uwm = uw, u1m = u1, u2m = u2;
+              if (P.moving && L.cv[m]) {
+                // velocities relative to the grid (src/output.f90:4768-4806)
+                const BGs G(L.cv[m], L, b, nh);
+                uwm = uw - G(hi, hj, hk);
+                u1m = u1 - G(hi + o1[0], hj + o1[1], hk + o1[2]);
+                u2m = u2 - G(hi + 2 * o1[0], hj + 2 * o1[1], hk + 2 * o1[2]);
+              }
+              eta[m] = sgn * (-8 * uwm + 9 * u1m - u2m) / 3;
             }
             const double dudx = eta[0] * ex, dudy = eta[0] * ey, dudz = eta[0] * ez;
             const double dvdx = eta[1] * ex, dvdy = eta[1] * ey, dvdz = eta[1] * ez;

@@ -402,8 +402,9 @@ def mg(levels, arrays, mgit0, ncycles, ncycle, rms_every=1):
 # ---- viscous path ------------------------------------------------------------------
 def vm_alloc(O):
     """The 9 face inverse-metric arrays (3 x imax x jmax x kmax each) of a level
-    in one buffer: array (d, m) at offset ((d-1)*3 + m) * 3 * n0."""
-    return np.zeros(27 * O.n0)
+    in one buffer: array (d, m) at offset ((d-1)*3 + m) * 3 * n0; on a moving
+    grid (moving_setup) one such set per snapshot, snapshot nh at nh * 27 n0."""
+    return np.zeros(27 * O.n0 * (O.S if getattr(O, "_moving", None) is not None else 1))
 
 
 def coordex(O, x, y, z):
