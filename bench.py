@@ -406,23 +406,27 @@ def main():
 
     serving = None
     if rank == 0 and ws == 1 and not args.no_serve:
-        # continuous batching: 20 Poisson arrivals at 2 req/s, half bump
-        # channels and half Euler NACA 0012 O-grids (alpha ~ U[-4, 8] deg), at
-        # three scales and random Mach numbers, each to a residual drop of
-        # 1e-8 or 60k RK cycles (single-grid explicit scheme), admission
-        # against 150 GB, FP64 and mixed precision, on this GPU after the duct runs
+        # continuous batching: 20 Poisson arrivals at 2 req/s, half k-omega
+        # RANS (NACA 0012) and half Euler (bump channel or NACA 0012, 50/50),
+        # at three scales, random Mach numbers and incidences (U[-4, 8] deg),
+        # each to a residual drop of 1e-8 or a cycle cap (Euler 60k, k-omega
+        # 20k: single-grid explicit schemes), admission against 150 GB split
+        # between the Euler engine and the k-omega lane by the request mix,
+        # FP64 and mixed precision, on this GPU after the duct runs
         from cosa_b200 import serve
         serving = {}
-        reqs = serve.poisson_requests(20, 2.0, 0, naca_fraction=0.5)
+        reqs = serve.poisson_requests(20, 2.0, 0, naca_fraction=0.5, kom_fraction=0.5)
         for name, prec in (("fp64", 0), ("mixed", 1)):
             try:
-                serving[name] = serve.run_sweep(reqs, 150e9, 1e-8, max_iter=60_000, device=dev,
-                                                precision=prec).summary()
+                serving[name] = serve.run_sweep(reqs, 150e9, 1e-8, max_iter=60_000, device=dev, precision=prec,
+                                                kom_max_iter=20_000).summary()
             except Exception as e:  # reported, not fatal
                 serving[name] = {"error": str(e)}
-        serving["workload"] = ("bump channel 128x64x2 (CFL 2) / Euler NACA 0012 256x64x2 (CFL 1) (50/50) "
-                               "x{0.5,1,2} in-plane, M~U[0.3,0.7], alpha~U[-4,8] deg, Poisson 2 req/s, drop 1e-8 "
-                               "or 60k cycles, 150 GB; k-omega requests are not served")
+        serving["workload"] = ("k-omega NACA 0012 256x64x2 (Re 1e6, IRS, CFL 3) / Euler (bump channel 128x64x2 at "
+                               "CFL 2 or NACA 0012 256x64x2 at CFL 1) 50/50, x{0.5,1,2} in-plane, M~U[0.3,0.7], "
+                               "alpha~U[-4,8] deg, Poisson 2 req/s, drop 1e-8 or 60k (Euler) / 20k (k-omega) cycles, "
+                               "150 GB; Euler solves batched in the engine's merged level, k-omega solves each in "
+                               "its own context and stream on a worker thread (the k-omega lane)")
         # the same kind of solves batched in the engine (mixed precision)
         # against the plain single-solve FP64 path, 400 RK cycles each
         try:

@@ -551,8 +551,12 @@ int64_t cnt_all(const DevBlock &b, const cosa_params &p) {
   return (int64_t)(b.im + 3) * (b.jm + 3) * (b.km + 3) * (2 * p.nharms + 1) * p.npde;
 }
 
+// once per process; contexts driven from several host threads (the serving
+// engine's k-omega lane) may reach it together
 int set_smem_attrs() {
+  static std::mutex mu;
   static bool done = false;
+  std::lock_guard<std::mutex> lock(mu);
   if (done) return COSA_OK;
   const int smem = (int)stage_smem_bytes<kTI, kTJ>();
   CK(cudaFuncSetAttribute(k_stage_tile<kTI, kTJ, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -571,9 +575,8 @@ int check_rans_supported(const cosa_params &p) {
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
   // moving grids: harmonic balance of a pitching body, explicit stages on one
-  // level in FP64 (the mixed-precision k-omega flux carries no face speed)
-  if (p.moving && (!p.harbal || !p.hbmove || p.rkimp || p.nlevel > 1 || p.precision != COSA_PREC_FP64))
-    return COSA_ERR_UNSUPPORTED;
+  // level
+  if (p.moving && (!p.harbal || !p.hbmove || p.rkimp || p.nlevel > 1)) return COSA_ERR_UNSUPPORTED;
   return COSA_OK;
 }
 
@@ -3220,7 +3223,7 @@ int launch_rans_stage(cosa_ctx *c, int nl, LevelState &L, int irk, const IterOpt
          const double *fd = blend(p) ? L.d_fdist : nullptr;
          if (mixed)
            k_rans_faces<true><<<g6, 128, 0, c->s>>>(bl, c->d_p, bct, q, nl, P.si, P.sj, P.sk, L.d_h0, P.mut, L.d_vm,
-                                                    L.n0, fd, L.d_rflux);
+                                                    L.n0, fd, L.d_rflux, face_vel_of(c, L));
          else
            k_rans_faces<false><<<g6, 128, 0, c->s>>>(bl, c->d_p, bct, q, nl, P.si, P.sj, P.sk, L.d_h0, P.mut, L.d_vm,
                                                      L.n0, fd, L.d_rflux, face_vel_of(c, L));

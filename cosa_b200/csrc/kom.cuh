@@ -745,7 +745,7 @@ __device__ __forceinline__ void rans_conv_faces(const DevBlock &b, const cosa_pa
     const double kx = s[e4], ky = s[e4 + 1], kz = s[e4 + 2], ds = s[e4 + 3];
     // the face speed of a moving grid (roflux_b, src/flux.f90:110-113, 262-264)
     const double ubn = fv ? fv[(e4 >> 2) * 3] * kx + fv[(e4 >> 2) * 3 + 1] * ky + fv[(e4 >> 2) * 3 + 2] * kz : 0.0;
-    if (MIXED) roe_flux_mixed_tke(ph, kx, ky, kz, ds, vr, vl, vr[5], vl[5], f);
+    if (MIXED) roe_flux_mixed_tke(ph, kx, ky, kz, ds, vr, vl, vr[5], vl[5], f, ubn);
     else roe_flux_fp64(ph, kx, ky, kz, ds, vr, vl, vr[5], vl[5], f, ubn);
 #pragma unroll
     for (int m = 0; m < 5; ++m) F[f0_idx(b, npde, S, i, j, k, m + 1, n)] = f[m];

@@ -430,12 +430,14 @@ __device__ __forceinline__ void roe_flux_mixed(const PhysPar &P, double kx, doub
 // differences (the k-omega path's counterpart of roe_flux_mixed).
 __device__ __forceinline__ void roe_flux_mixed_tke(const PhysPar &P, double kx, double ky, double kz, double ds,
                                                    const double *qr, const double *ql, double tker, double tkel,
-                                                   double *flux) {
+                                                   double *flux, double ubn = 0.0) {
+  // ubn: the face's normal grid speed on moving grids (src/flux.f90:110-113),
+  // FP64 in the central flux, FP32 in the dissipation like the rest of it
   const double g = P.g;
   const double rhor = qr[0], ur = qr[1], vr = qr[2], wr = qr[3], pr = qr[4];
   const double rhol = ql[0], ul = ql[1], vl = ql[2], wl = ql[3], pl = ql[4];
-  const double unr = ur * kx + vr * ky + wr * kz;
-  const double unl = ul * kx + vl * ky + wl * kz;
+  const double unr = ur * kx + vr * ky + wr * kz - ubn;
+  const double unl = ul * kx + vl * ky + wl * kz - ubn;
   const double q2r = ur * ur + vr * vr + wr * wr;
   const double q2l = ul * ul + vl * vl + wl * wl;
   const double h0r = g / (g - 1) * pr / rhor + q2r / 2 + tker;
@@ -457,10 +459,11 @@ __device__ __forceinline__ void roe_flux_mixed_tke(const PhysPar &P, double kx, 
   const float q2 = u * u + v * v + w * w;
   const float a2 = (float)(g - 1) * (h0 - q2 * 0.5f - tke);
   const float a = sqrtf(a2);
-  float rm123 = fabsf(un), rm4 = fabsf(un + a), rm5 = fabsf(un - a);
+  const float fubn = (float)ubn;
+  float rm123 = fabsf(un - fubn), rm4 = fabsf(un + a - fubn), rm5 = fabsf(un - a - fubn);
   if (P.efx_setup_f) {
     float rdelta = (float)P.cntrpy_f * ((float)P.w1 * (float)P.entfxctf_f + (float)P.w2 * (sqrtf(q2) + a) +
-                                        (float)P.w3 * 0.2f * (fabsf(un) + a));
+                                        (float)P.w3 * 0.2f * (fabsf(un) + a + fabsf(fubn)));
     rdelta = fmaxf(rdelta, 1.0e-12f);
     if (rm123 <= rdelta && P.efx_all_f) rm123 = 0.5f * (rm123 * rm123 + rdelta * rdelta) / rdelta;
     if (rm4 <= rdelta) rm4 = 0.5f * (rm4 * rm4 + rdelta * rdelta) / rdelta;
@@ -487,7 +490,7 @@ __device__ __forceinline__ void roe_flux_mixed_tke(const PhysPar &P, double kx, 
   flux[1] = ((rhor * ur * unr + pr * kx) + (rhol * ul * unl + pl * kx) - (double)df2) / 2 * ds;
   flux[2] = ((rhor * vr * unr + pr * ky) + (rhol * vl * unl + pl * ky) - (double)df3) / 2 * ds;
   flux[3] = ((rhor * wr * unr + pr * kz) + (rhol * wl * unl + pl * kz) - (double)df4) / 2 * ds;
-  flux[4] = (rhor * h0r * unr + rhol * h0l * unl - (double)df5) / 2 * ds;
+  flux[4] = (rhor * h0r * unr + pr * ubn + rhol * h0l * unl + pl * ubn - (double)df5) / 2 * ds;
 }
 
 // ---- eig_eul (src/cosa.f90:4183-4233); gv: the cell's grid velocity on

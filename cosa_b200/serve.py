@@ -2,17 +2,29 @@
 
 A seeded Poisson stream of steady solves arrives; each request is the bump
 channel at one of three in-plane scales with its own free-stream Mach
-number (and the matching inlet total state), or an Euler NACA 0012 O-grid
-at one of three scales with its own Mach number and incidence.  Requests are submitted when
-they arrive, admitted by the engine as device memory allows, advanced
-together with whatever else is on the GPU, and retired at convergence.
-Reports throughput (solves per hour) and p50/p99 latency (arrival to
-retirement).  The reference has no serving mode: each of its runs is one
-solve; this is the batched counterpart of running those one after another.
+number (and the matching inlet total state), or a NACA 0012 O-grid at one of
+three scales with its own Mach number and incidence, and is an Euler or a
+k-omega RANS solve.  Requests are submitted when they arrive, admitted as
+device memory allows, advanced together with whatever else is on the GPU,
+and retired at convergence.  Reports throughput (solves per hour) and
+p50/p99 latency (arrival to retirement).  The reference has no serving mode:
+each of its runs is one solve; this is the batched counterpart of running
+those one after another.
+
+Euler solves share the engine's merged level (one halo and one stage launch
+per RK stage for all of them).  k-omega solves run in the k-omega lane
+(KomLane): each is resident in its own context with its own CUDA stream and
+advanced by a worker thread, so their launches overlap on the device with
+one another and with the engine's; the library call releases the
+interpreter lock.  The device budget is split between the engine's pools
+and the lane.
 """
 from __future__ import annotations
 
+import threading
 import time
+from collections import deque
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional
 
@@ -57,6 +69,41 @@ def naca_request(scale: float, mach: float, alpha_deg: float, arrival: float = 0
     return Request(scale, mach, arrival, case, case.params, alpha_deg, "naca")
 
 
+def kom_channel_request(scale: float, mach: float, arrival: float = 0.0, reyno: float = 1.0e5) -> Request:
+    """k-omega (Wilcox, Menter wall omega) bump channel 128 x 64 x 2 cells
+    scaled by `scale` in i and j, no-slip walls (1500) top and bottom, free
+    stream and inlet total state at `mach`, Reynolds number reyno per unit
+    length, CFL 1.5.  Short runs only: the uniform inflow meets the no-slip
+    walls at the inlet corners, where k-omega production runs away (k
+    reaches four times the free-stream kinetic energy near cycle 60, in the
+    oracle as on the device; the production limiters only delay it), so
+    poisson_requests draws its k-omega solves on the NACA grid."""
+    ni, nj = max(8, int(round(128 * scale))), max(4, int(round(64 * scale)))
+    case = cases.turbulent_channel(ni, nj, 2, mach=mach, reyno=reyno)
+    case.params.cfl = case.params.cflt = 1.5
+    return Request(scale, mach, arrival, case, case.params, 0.0, "channel_kom")
+
+
+def kom_naca_request(scale: float, mach: float, alpha_deg: float, arrival: float = 0.0,
+                     reyno: float = 1.0e6) -> Request:
+    """k-omega NACA 0012 O-grid 256 x 64 x 2 cells in four blocks scaled by
+    `scale` in i and j, no-slip wall (1500), far field (30) at 20 chords,
+    first spacing 2e-4 chords at every scale (at 4e-4 on the 128 x 32 grid
+    the trailing-edge cells' k runs away by cycle 300, in the oracle as on
+    the device), free stream at `mach` and incidence `alpha_deg`, Reynolds
+    number reyno, constant-coefficient IRS (0.6) at CFL 3."""
+    ni, nj = max(16, int(round(256 * scale)) // 16 * 16), max(8, int(round(64 * scale)))
+    blocks = (3 * ni // 16, 5 * ni // 16, 5 * ni // 16, 3 * ni // 16)
+    p = cases.naca_params("kom", mach=mach, alpha_deg=alpha_deg, reyno=reyno, cfl=3.0, eps_irs=0.6)
+    case = cases.naca0012_ogrid(blocks=blocks, nj=nj, nk=2, rfar=20.0, h1=2e-4, params=p)
+    return Request(scale, mach, arrival, case, case.params, alpha_deg, "naca_kom")
+
+
+def is_kom(r: Request) -> bool:
+    p = r.flow
+    return bool(p.kom or p.kom_bsl or p.kom_sst)
+
+
 def engine_scheme() -> CosaParams:
     """The engine's scheme: Roe + MUSCL (kappa 1/3, smooth limiter), 4-stage
     RK at CFL 2; flow conditions come with each request."""
@@ -64,21 +111,149 @@ def engine_scheme() -> CosaParams:
 
 
 def poisson_requests(n: int, rate: float, seed: int, scales=(0.5, 1.0, 2.0), mach_range=(0.3, 0.7),
-                     naca_fraction: float = 0.0, alpha_range=(-4.0, 8.0)) -> List[Request]:
-    """n arrivals at `rate` per second (seeded): the bump channel, or with
-    probability naca_fraction the Euler NACA 0012 at an incidence drawn from
-    alpha_range (degrees); scale and Mach number drawn uniformly."""
+                     naca_fraction: float = 0.0, alpha_range=(-4.0, 8.0), kom_fraction: float = 0.0) -> List[Request]:
+    """n arrivals at `rate` per second (seeded): with probability
+    kom_fraction a k-omega RANS solve of the NACA 0012 (kom_naca_request),
+    else an Euler solve of the bump channel or, with probability
+    naca_fraction, of the NACA 0012; incidence drawn from alpha_range
+    (degrees), scale and Mach number uniformly."""
     rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1.0 / rate, size=n))
     t -= t[0]
     out = []
     for k in range(n):
         scale, mach = float(rng.choice(scales)), float(rng.uniform(*mach_range))
-        if rng.uniform() < naca_fraction:
-            out.append(naca_request(scale, mach, float(rng.uniform(*alpha_range)), float(t[k])))
+        naca = rng.uniform() < naca_fraction
+        alpha = float(rng.uniform(*alpha_range))
+        kom = rng.uniform() < kom_fraction
+        if kom:
+            out.append(kom_naca_request(scale, mach, alpha, float(t[k])))
+        elif naca:
+            out.append(naca_request(scale, mach, alpha, float(t[k])))
         else:
             out.append(channel_request(scale, mach, float(t[k])))
     return out
+
+
+def kom_solve_bytes(case: "cases.Case") -> int:
+    """Device bytes of one k-omega solve in its own context, an upper
+    estimate from the arrays SteadySolver binds and the context's own work
+    arrays: 8 states, 7 face-flux planes (one of the caller, six of the
+    fused stage), the IRS pivots (2 per variable) and about 30 scalar arrays
+    per P3 cell, plus the face inverse metrics (27 per face cell): 8 bytes x
+    (8 x 7 + 7 x 7 + 2 x 7 + 30 + 27) = 1408 bytes per P3 cell."""
+    _, tot = case.tables.offsets()
+    return int(8 * (8 * 7 + 7 * 7 + 2 * 7 + 30) * tot["p3"] + 8 * 27 * tot["f0"])
+
+
+class KomLane:
+    """k-omega solves next to the serving engine.  A submitted solve waits
+    in a queue until its device bytes (kom_solve_bytes) fit the lane's
+    budget and a worker is free; it then runs on a worker thread in its own
+    context and stream (SteadySolver: metrics, viscous set-up, wall distance
+    and the initial eddy viscosity on the device), check_every RK cycles per
+    library call, with the same convergence rule as the engine: the total
+    residual norm of its first cycle is the reference, the solve converges
+    when the norm of a checked cycle falls below tol times it, stops at
+    max_iter cycles and fails on a status bit or a non-finite norm.  A
+    retired solve's context is closed at once, so its bytes go back to the
+    lane.  result() gives the engine's fields."""
+
+    def __init__(self, budget_bytes: float, device: int = 0, check_every: int = 10, precision: int = 0,
+                 workers: int = 16):
+        self.budget, self.used = float(budget_bytes), 0.0
+        self.device, self.check_every, self.precision = device, check_every, precision
+        self.solves: List[Dict] = []
+        self.queue: deque = deque()
+        self.lock = threading.Lock()
+        self.running = 0
+        self.workers = workers
+        self.pool = ThreadPoolExecutor(max_workers=workers)
+        self.t0 = time.perf_counter()
+
+    def now(self) -> float:
+        return time.perf_counter() - self.t0
+
+    def submit(self, case: "cases.Case", flow: CosaParams, tol: float, max_iter: int) -> int:
+        nbytes = kom_solve_bytes(case)
+        if nbytes > self.budget:
+            raise ValueError(f"a k-omega solve of {nbytes} bytes exceeds the lane's budget of {self.budget:.0f}")
+        with self.lock:
+            rid = len(self.solves)
+            self.solves.append({"case": case, "flow": flow, "tol": tol, "max_iter": max_iter, "bytes": nbytes,
+                                "state": "queued", "iters": 0, "drop": 0.0, "t_submit": self.now(),
+                                "t_admit": 0.0, "t_done": 0.0, "status": 0, "result": None})
+            self.queue.append(rid)
+        self.admit()
+        return rid
+
+    def admit(self):
+        """Start queued solves in arrival order while the head one fits."""
+        with self.lock:
+            while self.queue and self.running < self.workers:
+                s = self.solves[self.queue[0]]
+                if self.used + s["bytes"] > self.budget:
+                    break
+                rid = self.queue.popleft()
+                self.used += s["bytes"]
+                self.running += 1
+                s["state"], s["t_admit"] = "active", self.now()
+                self.pool.submit(self._run, rid)
+
+    def _run(self, rid: int):
+        from .solver import SteadySolver
+        s = self.solves[rid]
+        solver = None
+        state = "failed"
+        try:
+            p = CosaParams.from_buffer_copy(s["flow"])
+            p.precision = self.precision
+            solver = SteadySolver(s["case"], params=p, device=self.device)
+            npde, rms0 = p.npde, None
+            while True:
+                n = min(self.check_every, s["max_iter"] - s["iters"])
+                hist, st = solver.run(n, rms_every=n)
+                s["iters"] += n
+                if rms0 is None:
+                    rms0 = float(hist[0, npde])
+                rms = float(hist[n - 1, npde])
+                s["drop"] = rms / rms0 if rms0 > 0 else 0.0
+                if st or not np.isfinite(rms):
+                    s["status"] = int(st)
+                    break
+                if rms0 > 0 and rms < s["tol"] * rms0:
+                    state = "converged"
+                    break
+                if s["iters"] >= s["max_iter"]:
+                    state = "stopped"
+                    break
+            if state != "failed":
+                s["result"] = solver.state()
+        except Exception as e:  # a set-up or library error retires the solve as failed
+            s["error"] = repr(e)
+        finally:
+            if solver is not None:
+                solver.close()
+            with self.lock:
+                s["state"], s["t_done"] = state, self.now()
+                s["case"] = None
+                self.used -= s["bytes"]
+                self.running -= 1
+        self.admit()
+
+    def result(self, rid: int) -> Dict:
+        s = self.solves[rid]
+        out = {k: s[k] for k in ("state", "iters", "drop", "t_submit", "t_admit", "t_done", "status")}
+        if "error" in s:
+            out["error"] = s["error"]
+        return out
+
+    def counts(self):
+        with self.lock:
+            return self.running, len(self.queue)
+
+    def close(self):
+        self.pool.shutdown(wait=True)
 
 
 @dataclass
@@ -93,55 +268,91 @@ class SweepResult:
     latencies: List[float] = field(default_factory=list)
     cell_stages: float = 0.0
 
+    kinds: List[str] = field(default_factory=list)
+
     def summary(self) -> Dict:
-        return {"requests": self.n, "wall_s": self.wall_s, "solves_per_hour": self.solves_per_hour,
-                "p50_latency_s": self.p50_s, "p99_latency_s": self.p99_s,
-                "converged": sum(s == "converged" for s in self.states),
-                "stopped": sum(s == "stopped" for s in self.states),
-                "failed": sum(s == "failed" for s in self.states),
-                "mean_iters": float(np.mean(self.iters)) if self.iters else 0.0,
-                "mcell_stages_per_s": self.cell_stages / self.wall_s / 1e6 if self.wall_s else 0.0}
+        out = {"requests": self.n, "wall_s": self.wall_s, "solves_per_hour": self.solves_per_hour,
+               "p50_latency_s": self.p50_s, "p99_latency_s": self.p99_s,
+               "converged": sum(s == "converged" for s in self.states),
+               "stopped": sum(s == "stopped" for s in self.states),
+               "failed": sum(s == "failed" for s in self.states),
+               "mean_iters": float(np.mean(self.iters)) if self.iters else 0.0,
+               "mcell_stages_per_s": self.cell_stages / self.wall_s / 1e6 if self.wall_s else 0.0}
+        for kind in sorted(set(self.kinds)):
+            sel = [i for i, k in enumerate(self.kinds) if k == kind]
+            lat = [self.latencies[i] for i in sel]
+            out[kind] = {"requests": len(sel), "converged": sum(self.states[i] == "converged" for i in sel),
+                         "stopped": sum(self.states[i] == "stopped" for i in sel),
+                         "failed": sum(self.states[i] == "failed" for i in sel),
+                         "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99))}
+        return out
 
 
 def run_sweep(requests: List[Request], budget_bytes: float = 150e9, tol: float = 1e-8, max_iter: int = 200_000,
-              check_every: int = 10, iters_per_step: int = 50, device: int = 0, precision: int = 0) -> SweepResult:
+              check_every: int = 10, iters_per_step: int = 50, device: int = 0, precision: int = 0,
+              kom_share: Optional[float] = None, kom_max_iter: Optional[int] = None) -> SweepResult:
     """Feed `requests` at their arrival times (seconds after the start) and
-    run the engine (precision 0: FP64, 1: mixed) until every one has retired."""
+    run the engine and the k-omega lane (precision 0: FP64, 1: mixed) until
+    every one has retired.  kom_share is the lane's part of the device budget
+    (default: the k-omega fraction of the requests, 0 without any);
+    kom_max_iter caps the k-omega solves' cycles (default max_iter)."""
+    nkom = sum(is_kom(r) for r in requests)
+    share = (nkom / max(len(requests), 1)) if kom_share is None else kom_share
+    share = share if nkom else 0.0
     scheme = engine_scheme()
     scheme.precision = precision
-    srv = Server(scheme, int(budget_bytes), device=device, check_every=check_every)
+    srv = Server(scheme, int(budget_bytes * (1.0 - share)), device=device, check_every=check_every) \
+        if nkom < len(requests) else None
+    lane = KomLane(budget_bytes * share, device=device, check_every=check_every, precision=precision) \
+        if nkom else None
     try:
-        ids: List[int] = []
+        ids: List[tuple] = []  # ("engine" | "kom", id) in submission order
         pending = sorted(range(len(requests)), key=lambda k: requests[k].arrival)
-        order: Dict[int, int] = {}
+        order: Dict[tuple, int] = {}
         t0 = time.perf_counter()
         done = 0
         nxt = 0
+
+        def result(key):
+            return srv.result(key[1]) if key[0] == "engine" else lane.result(key[1])
+
         while done < len(requests):
             now = time.perf_counter() - t0
             while nxt < len(pending) and requests[pending[nxt]].arrival <= now:
                 r = requests[pending[nxt]]
-                rid = srv.submit(r.case.tables, r.case.x, r.case.y, r.case.z, r.case.q0, r.flow, tol, max_iter)
-                order[rid] = pending[nxt]
-                ids.append(rid)
+                if is_kom(r):
+                    key = ("kom", lane.submit(r.case, r.flow, tol, kom_max_iter or max_iter))
+                else:
+                    key = ("engine", srv.submit(r.case.tables, r.case.x, r.case.y, r.case.z, r.case.q0, r.flow, tol,
+                                                max_iter))
+                order[key] = pending[nxt]
+                ids.append(key)
                 nxt += 1
-            na, nq = srv.step(iters_per_step) if ids else (0, 0)
-            done = sum(srv.result(rid)["state"] not in ("queued", "active") for rid in ids)
-            if na == 0 and nq == 0 and nxt < len(pending) and done == len(ids):
+            na, nq = srv.step(iters_per_step) if srv is not None and any(k[0] == "engine" for k in ids) else (0, 0)
+            done = sum(result(k)["state"] not in ("queued", "active") for k in ids)
+            if na == 0 and nq == 0 and done < len(ids):
+                time.sleep(0.005)  # only k-omega solves in flight: their worker threads drive the GPU
+            elif na == 0 and nq == 0 and nxt < len(pending) and done == len(ids):
                 wait = requests[pending[nxt]].arrival - (time.perf_counter() - t0)
                 if wait > 0:
                     time.sleep(wait)
         wall = time.perf_counter() - t0
-        res = [srv.result(rid) for rid in ids]
+        res = [result(k) for k in ids]
         lat = [r["t_done"] - r["t_submit"] for r in res]
         cs = 0.0
-        for rid, r in zip(ids, res):
-            cs += requests[order[rid]].case.ncells * 4 * r["iters"]
-        return SweepResult(len(ids), wall, len(ids) / wall * 3600.0, float(np.percentile(lat, 50)),
-                           float(np.percentile(lat, 99)), [r["iters"] for r in res], [r["state"] for r in res], lat,
-                           cs)
+        for key, r in zip(ids, res):
+            rq = requests[order[key]]
+            cs += rq.case.ncells * int(rq.flow.nstage) * r["iters"]
+        out = SweepResult(len(ids), wall, len(ids) / wall * 3600.0, float(np.percentile(lat, 50)),
+                          float(np.percentile(lat, 99)), [r["iters"] for r in res], [r["state"] for r in res], lat,
+                          cs)
+        out.kinds = ["kom" if k[0] == "kom" else "euler" for k in ids]
+        return out
     finally:
-        srv.close()
+        if srv is not None:
+            srv.close()
+        if lane is not None:
+            lane.close()
 
 
 def main():
@@ -154,8 +365,9 @@ def main():
     ap.add_argument("--tol", type=float, default=0.1)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--naca-fraction", type=float, default=0.5)
+    ap.add_argument("--kom-fraction", type=float, default=0.5)
     a = ap.parse_args()
-    reqs = poisson_requests(a.requests, a.rate, a.seed, naca_fraction=a.naca_fraction)
+    reqs = poisson_requests(a.requests, a.rate, a.seed, naca_fraction=a.naca_fraction, kom_fraction=a.kom_fraction)
     print(json.dumps(run_sweep(reqs, a.budget_gb * 1e9, a.tol).summary()))
 
 

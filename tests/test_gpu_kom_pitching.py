@@ -135,13 +135,24 @@ def test_kom_pitching_hb_cycles_match_oracle(nharms, model):
     ctx.close()
 
 
-def test_mixed_precision_moving_kom_is_refused():
-    """The mixed-precision k-omega flux carries no face speed: the stage
-    refuses a moving grid in that precision instead of dropping the speeds."""
-    case = _case(1)
-    case.params.precision = PREC_MIXED
-    O, A, mo = _oracle_setup(case, case.q0)
-    ctx, m, vm, d = _device_setup(case, A)
-    _, st = ctx.smooth(1, 1, 1, 1)
-    assert st == 0x80  # COSA_ERR_UNSUPPORTED
-    ctx.close()
+def test_mixed_precision_moving_kom_close_to_fp64():
+    """FP32 reconstruction and Roe dissipation (the face speed in both) on
+    the pitching grid: 20 cycles of k-omega HB (S = 3) against the FP64
+    device path, states within 1e-6 of the largest value of each variable
+    and the per-snapshot force and moment coefficients within 1e-6."""
+    out = {}
+    for prec in (0, PREC_MIXED):
+        case = _case(1)
+        case.params.precision = prec
+        q = _state(case, 21)
+        O, A, mo = _oracle_setup(case, q)
+        ctx, m, vm, d = _device_setup(case, A)
+        hg, st = ctx.smooth(1, 20, 1, 20)
+        assert st == 0
+        c = ctx.force(1, d["q"], m["x"], m["y"], m["z"], m["si"], m["sj"], m["sk"], vm=vm, lngth=(1.0, 0.1, 1.0))
+        out[prec] = (d["q"].download(), c, case.tables)
+        ctx.close()
+    (q64, c64, t), (q32, c32, _) = out[0], out[PREC_MIXED]
+    err = _rel(q32, q64, t, 3)
+    assert 0 < err <= 1e-6, err
+    assert np.abs(c32 - c64).max() <= 1e-6, np.abs(c32 - c64).max()

@@ -151,3 +151,58 @@ def test_short_mixed_sweep_reports_latency():
     s = res.summary()
     assert s["requests"] == 6 and s["converged"] == 6, res.states
     assert 0 < s["p50_latency_s"] <= s["p99_latency_s"]
+
+
+def _lane_run(reqs, n, budget=4e9, check_every=10):
+    lane = serve.KomLane(budget, check_every=check_every)
+    try:
+        ids = [lane.submit(r.case, r.flow, 0.0, n) for r in reqs]
+        while any(lane.result(i)["state"] in ("queued", "active") for i in ids):
+            import time
+            time.sleep(0.01)
+        return [dict(lane.result(i), q=lane.solves[i]["result"]) for i in ids]
+    finally:
+        lane.close()
+
+
+def test_kom_lane_matches_plain_solver_alone_and_in_the_mix():
+    """k-omega requests in the lane (each in its own context and stream,
+    advanced by worker threads at the same time): every solve gives the
+    bits of a plain SteadySolver run of the same cycles, alone and beside
+    other k-omega solves."""
+    from cosa_b200.solver import SteadySolver
+    reqs = [serve.kom_channel_request(0.5, 0.45), serve.kom_naca_request(0.5, 0.5, 4.0),
+            serve.kom_channel_request(0.5, 0.4)]
+    n = 60
+    mixed = _lane_run(reqs, n)
+    alone = _lane_run(reqs[1:2], n)[0]
+    s = SteadySolver(reqs[1].case)
+    _, st = s.run(n, rms_every=10)
+    assert st == 0
+    plain = s.state()
+    s.close()
+    assert mixed[1]["state"] == alone["state"] == "stopped" and mixed[1]["iters"] == n
+    for r in (alone, mixed[1]):
+        assert np.array_equal(casekit.interior_cells(reqs[1].case, r["q"], 7),
+                              casekit.interior_cells(reqs[1].case, plain, 7))
+    assert all(m["state"] == "stopped" for m in mixed), [(m["state"], m["status"], m.get("error")) for m in mixed]
+
+
+def test_kom_lane_admission_waits_for_memory():
+    a, b = serve.kom_channel_request(0.5, 0.45), serve.kom_channel_request(0.5, 0.55)
+    budget = serve.kom_solve_bytes(a.case) * 1.5  # room for one solve at a time
+    ra, rb = _lane_run([a, b], 30, budget=budget)
+    assert ra["state"] == rb["state"] == "stopped"
+    assert rb["t_admit"] >= ra["t_done"]
+
+
+def test_euler_and_kom_sweep_retires_every_request():
+    reqs = serve.poisson_requests(8, rate=20.0, seed=3, scales=(0.5,), naca_fraction=0.5, alpha_range=(-4.0, 4.0),
+                                  kom_fraction=0.5)
+    assert any(serve.is_kom(r) for r in reqs) and not all(serve.is_kom(r) for r in reqs)
+    res = serve.run_sweep(reqs, budget_bytes=8e9, tol=0.3, max_iter=20000, iters_per_step=25, kom_max_iter=400)
+    s = res.summary()
+    assert s["requests"] == 8 and s["failed"] == 0, res.states
+    assert s["euler"]["converged"] == s["euler"]["requests"]
+    assert s["kom"]["converged"] + s["kom"]["stopped"] == s["kom"]["requests"]
+    assert 0 < s["p50_latency_s"] <= s["p99_latency_s"]
