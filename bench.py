@@ -46,6 +46,10 @@ B_ALG_STAGE = 234
 # harmonic balance of a pitching body, per cell-snapshot-stage: state 120 +
 # metrics 3 x 7 x 8 = 168 + cell grid velocity 24 + vol 8 + dt/V 8 + 2
 B_ALG_HB_MOVING = 330
+# k-omega on the pitching grid: the k-omega stage's 960 B per cell-stage
+# (7 variables, the face inverse metrics, mut and the k-omega work arrays)
+# per snapshot
+B_ALG_KOM_HB_MOVING = 960
 # bytes the face-split schedule's face kernels (k_faces_line, i-face and
 # marching launches) move per cell: state reads 3 x 40 (once per family) +
 # face metrics 96 + face fluxes written 120
@@ -441,24 +445,27 @@ def main():
         # FP64 and mixed: throughput, roofline and the CL/CM harmonics' gap
         from cosa_b200 import pitching
         hb = {}
-        for nh in (1, 2, 3):
-            try:
-                r = pitching.compare(nh, cycles=args.hb_cycles, chunk=args.hb_cycles, device=dev)
-                f, mx = r["fp64"], r["mixed"]
-                gbs = B_ALG_HB_MOVING * f["mcell_snapshot_stage_s"] * 1e6 / 1e9
-                hb[f"nh{nh}"] = {"snapshots": f["snapshots"], "cells": f["cells"], "cycles": f["cycles"],
-                                 "fp64_mcell_snapshot_stage_s": f["mcell_snapshot_stage_s"],
-                                 "mixed_mcell_snapshot_stage_s": mx["mcell_snapshot_stage_s"],
-                                 "mixed_speedup": r["mixed_speedup"],
-                                 "fp64_stage_gbs_alg": gbs, "fp64_stage_frac": gbs / peak,
-                                 "drop_rho_fp64": f["drop_rho"],
-                                 "cl_harmonics_fp64": f["cl_harmonics"], "cm_harmonics_fp64": f["cm_harmonics"],
-                                 "max_dcl_harmonic_mixed": r["max_dcl_harmonic"],
-                                 "max_dcm_harmonic_mixed": r["max_dcm_harmonic"]}
-            except Exception as e:  # reported, not fatal
-                hb[f"nh{nh}"] = {"error": str(e)}
-        hb["workload"] = ("NACA 0012 O-grid 256x64x2 (4 blocks), Euler, M=0.5, pitching 2.5 deg about c/4 at "
-                          "k=0.08, harmonic balance with one grid per snapshot, CFL 1, 4-stage RK")
+        for model, bpc in (("euler", B_ALG_HB_MOVING), ("kom", B_ALG_KOM_HB_MOVING)):
+            for nh in (1, 2, 3):
+                key = f"nh{nh}" if model == "euler" else f"kom_nh{nh}"
+                try:
+                    r = pitching.compare(nh, cycles=args.hb_cycles, chunk=args.hb_cycles, device=dev, model=model)
+                    f, mx = r["fp64"], r["mixed"]
+                    gbs = bpc * f["mcell_snapshot_stage_s"] * 1e6 / 1e9
+                    hb[key] = {"snapshots": f["snapshots"], "cells": f["cells"], "cycles": f["cycles"],
+                               "fp64_mcell_snapshot_stage_s": f["mcell_snapshot_stage_s"],
+                               "mixed_mcell_snapshot_stage_s": mx["mcell_snapshot_stage_s"],
+                               "mixed_speedup": r["mixed_speedup"],
+                               "fp64_stage_gbs_alg": gbs, "fp64_stage_frac": gbs / peak,
+                               "drop_rho_fp64": f["drop_rho"],
+                               "cl_harmonics_fp64": f["cl_harmonics"], "cm_harmonics_fp64": f["cm_harmonics"],
+                               "max_dcl_harmonic_mixed": r["max_dcl_harmonic"],
+                               "max_dcm_harmonic_mixed": r["max_dcm_harmonic"]}
+                except Exception as e:  # reported, not fatal
+                    hb[key] = {"error": str(e)}
+        hb["workload"] = ("NACA 0012 O-grid 256x64x2 (4 blocks), M=0.5, pitching 2.5 deg about c/4 at k=0.08, "
+                          "harmonic balance with one grid per snapshot, CFL 1, 4-stage RK; nh*: Euler; kom_nh*: "
+                          "k-omega (Wilcox), Re 1e6, first spacing 2e-4 chords, CL/CM with skin friction")
 
     cpu = None
     if rank == 0 and not args.no_cpu:

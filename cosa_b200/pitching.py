@@ -1,14 +1,17 @@
-"""Harmonic balance of a pitching NACA 0012 (the inviscid case of the
-benchmark's harmonic-balance configuration): the O-grid of naca0012_ogrid,
-256 x 64 x 2 cells by default, pitching theta(t) = 2.5 deg sin(omega t)
-about the quarter chord at reduced frequency 0.08 and M = 0.5, with NH
-harmonics (S = 2 NH + 1 snapshots, each on its own rotated grid) solved
-together in one set of stage launches.  Reports the device-timed
+"""Harmonic balance of a pitching NACA 0012 (the benchmark's
+harmonic-balance configuration, Euler or k-omega RANS): the O-grid of
+naca0012_ogrid, 256 x 64 x 2 cells by default, pitching theta(t) = 2.5 deg
+sin(omega t) about the quarter chord at reduced frequency 0.08 and M = 0.5,
+with NH harmonics (S = 2 NH + 1 snapshots, each on its own rotated grid)
+solved together in one set of stage launches.  Reports the device-timed
 throughput in cell-snapshot-stages per second, the residual history, the
 per-snapshot lift and moment coefficients and their harmonics (mathb's E,
-src/input.f90:5240-5251), FP64 and mixed precision side by side.
+src/input.f90:5240-5251), FP64 and mixed precision side by side.  The
+k-omega case (Re 1e6, no-slip wall with first spacing 2e-4 chords) adds the
+viscous set-up of every snapshot, the wall distance and the initial eddy
+viscosity; its coefficients include the skin friction.
 
-    python -m cosa_b200.pitching --nharms 1 2 3 --cycles 4000
+    python -m cosa_b200.pitching --nharms 1 2 3 --cycles 4000 [--model kom]
 
 Needs a GPU.
 """
@@ -26,20 +29,49 @@ from .params import PREC_MIXED, hb_harmonics
 LNGTH = (1.0, 0.1, 1.0)  # chord, span (z extent of the 2-cell O-grid), moment arm reference
 
 
-def run(nharms=1, precision=0, cycles=2000, chunk=500, blocks=(64, 64, 64, 64), nj=64, device=0):
+def _bind_kom(ctx, case, m, q):
+    """The k-omega arrays of a pitching level: the face inverse metrics of
+    every snapshot, the wall distance (rigid motion: that of the grid at
+    rest), the work arrays, and the initial eddy viscosity from the state
+    after the BCs (tur_vis, cut halos copied); returns vm."""
+    vm = ctx.alloc_vm(1)
+    ctx.viscous_setup(1, m["x"], m["y"], m["z"], m["vol"], vm)
+    dist = ctx.alloc_p1().upload(cases.wall_distance(case))
+    mut = ctx.alloc_p3s()
+    ctx.bind_level(1, q=q, qold=ctx.alloc_p3(), res=ctx.alloc_p3(), dtvol=ctx.alloc_p1(nsnap=ctx.S),
+                   dtvolt=ctx.alloc_p1(nsnap=ctx.S), si=m["si"], sj=m["sj"], sk=m["sk"], vol=m["vol"],
+                   qp=ctx.alloc_p3(), qm=ctx.alloc_p3(), dq=ctx.alloc_p3(), dqp=ctx.alloc_p3(), dqm=ctx.alloc_p3(),
+                   flux=ctx.alloc_f0(), mut=mut, dist=dist, xdot=m["xdot"], ydot=m["ydot"], zdot=m["zdot"],
+                   fvi=m["fvi"], fvj=m["fvj"], fvk=m["fvk"])
+    qq = ctx.alloc_p3().upload(q.download())
+    ctx.cons2prim(1, qq)
+    ctx.bc_dist(1, qq, m["si"], m["sj"], m["sk"], dist)
+    ctx.cutman_q(1, qq)
+    ctx.prim2cons(1, qq)
+    ctx.tur_vis(1, qq, mut)
+    ctx.cutman_mut(1, mut)
+    return vm
+
+
+def run(nharms=1, precision=0, cycles=2000, chunk=500, blocks=(64, 64, 64, 64), nj=64, device=0, model="euler"):
     """One pitching solve on the device: returns a dict with the throughput
     (Mcell-snapshot-stage/s, CUDA events on the library's stream), the
     residual drop of rho, the per-snapshot CL and CM and their harmonics."""
     import torch
-    case = cases.naca_pitching(nharms=nharms, blocks=blocks, nj=nj)
+    kom = model == "kom"
+    case = cases.naca_pitching(nharms=nharms, blocks=blocks, nj=nj, model=model, **({"h1": 2e-4} if kom else {}))
     p = case.params
     p.precision = precision
     ctx = gpu.Context([case.tables], p, device=device)
     m = ctx.pitching_setup(1, case)
     q = ctx.alloc_p3().upload(case.q0)
-    ctx.bind_level(1, q=q, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(nsnap=ctx.S), si=m["si"], sj=m["sj"],
-                   sk=m["sk"], vol=m["vol"], xdot=m["xdot"], ydot=m["ydot"], zdot=m["zdot"], fvi=m["fvi"],
-                   fvj=m["fvj"], fvk=m["fvk"])
+    vm = None
+    if kom:
+        vm = _bind_kom(ctx, case, m, q)
+    else:
+        ctx.bind_level(1, q=q, qold=ctx.alloc_p3(), dtvol=ctx.alloc_p1(nsnap=ctx.S), si=m["si"], sj=m["sj"],
+                       sk=m["sk"], vol=m["vol"], xdot=m["xdot"], ydot=m["ydot"], zdot=m["zdot"], fvi=m["fvi"],
+                       fvj=m["fvj"], fvk=m["fvk"])
     stream = torch.cuda.ExternalStream(ctx.stream())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     hist = []
@@ -58,11 +90,12 @@ def run(nharms=1, precision=0, cycles=2000, chunk=500, blocks=(64, 64, 64, 64), 
         if st:
             break
     hist = np.concatenate(hist, axis=0)
-    coef = ctx.force(1, q, m["x"], m["y"], m["z"], m["si"], m["sj"], m["sk"], lngth=LNGTH)
+    coef = ctx.force(1, q, m["x"], m["y"], m["z"], m["si"], m["sj"], m["sk"], vm=vm, lngth=LNGTH)
     ctx.close()
     S = 2 * nharms + 1
-    cl, cm = coef[:, 0], coef[:, 5]
-    return {"nharms": nharms, "snapshots": S, "precision": "mixed" if precision else "fp64", "cycles": done,
+    cl, cm = coef[:, 0] + coef[:, 6], coef[:, 5] + coef[:, 11]  # pressure + skin friction (0 for Euler)
+    return {"nharms": nharms, "model": model, "snapshots": S, "precision": "mixed" if precision else "fp64",
+            "cycles": done,
             "status": int(st), "cells": case.ncells,
             "mcell_snapshot_stage_s": case.ncells * S * p.nstage * done / (ms / 1e3) / 1e6,
             "ms_per_cycle": ms / max(done, 1),
@@ -88,10 +121,11 @@ def main():
     ap.add_argument("--nharms", type=int, nargs="+", default=[1, 2, 3])
     ap.add_argument("--cycles", type=int, default=2000)
     ap.add_argument("--chunk", type=int, default=500)
+    ap.add_argument("--model", choices=("euler", "kom"), default="euler")
     a = ap.parse_args()
     for nh in a.nharms:
         t = time.time()
-        r = compare(nh, a.cycles, chunk=a.chunk)
+        r = compare(nh, a.cycles, chunk=a.chunk, model=a.model)
         r["seconds"] = time.time() - t
         print(json.dumps(r), flush=True)
 
