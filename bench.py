@@ -398,6 +398,12 @@ def main():
     e2e_ms = max(e0.elapsed_time(e1), wall * 1e3)
     e2e_val = ws * ncells * nstage * args.e2e_steps / (e2e_ms / 1e3) / 1e6
     state_bytes = nq * 8
+    # the duct's device arrays and the pinned host copy are not needed by the
+    # legs below: release them, so that the serving sweep's 150 GB budget fits
+    # the device beside the other legs' contexts
+    ctx.close()
+    del hostq
+    torch.cuda.empty_cache()
 
     viscous = {}
     if rank == 0 and ws == 1 and not args.no_viscous:

@@ -269,6 +269,7 @@ class SweepResult:
     cell_stages: float = 0.0
 
     kinds: List[str] = field(default_factory=list)
+    errors: List[str] = field(default_factory=list)
 
     def summary(self) -> Dict:
         out = {"requests": self.n, "wall_s": self.wall_s, "solves_per_hour": self.solves_per_hour,
@@ -278,6 +279,8 @@ class SweepResult:
                "failed": sum(s == "failed" for s in self.states),
                "mean_iters": float(np.mean(self.iters)) if self.iters else 0.0,
                "mcell_stages_per_s": self.cell_stages / self.wall_s / 1e6 if self.wall_s else 0.0}
+        if self.errors:
+            out["errors"] = sorted(set(self.errors))
         for kind in sorted(set(self.kinds)):
             sel = [i for i, k in enumerate(self.kinds) if k == kind]
             lat = [self.latencies[i] for i in sel]
@@ -347,6 +350,7 @@ def run_sweep(requests: List[Request], budget_bytes: float = 150e9, tol: float =
                           float(np.percentile(lat, 99)), [r["iters"] for r in res], [r["state"] for r in res], lat,
                           cs)
         out.kinds = ["kom" if k[0] == "kom" else "euler" for k in ids]
+        out.errors = [r["error"] for r in res if r.get("error")]
         return out
     finally:
         if srv is not None:
