@@ -421,7 +421,7 @@ def main():
         # at three scales, random Mach numbers and incidences (U[-4, 8] deg),
         # each to a residual drop of 1e-8 or a cycle cap (Euler 60k, k-omega
         # 20k: single-grid explicit schemes), admission against 150 GB split
-        # between the Euler engine and the k-omega lane by the request mix,
+        # between the Euler engine and the context lane by the request mix,
         # FP64 and mixed precision, on this GPU after the duct runs
         from cosa_b200 import serve
         serving = {}
@@ -436,7 +436,7 @@ def main():
                                "CFL 2 or NACA 0012 256x64x2 at CFL 1) 50/50, x{0.5,1,2} in-plane, M~U[0.3,0.7], "
                                "alpha~U[-4,8] deg, Poisson 2 req/s, drop 1e-8 or 60k (Euler) / 20k (k-omega) cycles, "
                                "150 GB; Euler solves batched in the engine's merged level, k-omega solves each in "
-                               "its own context and stream on a worker thread (the k-omega lane)")
+                               "its own context and stream on a worker thread (the context lane)")
         # the same kind of solves batched in the engine (mixed precision)
         # against the plain single-solve FP64 path, 400 RK cycles each
         try:

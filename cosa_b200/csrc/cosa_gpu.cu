@@ -552,7 +552,7 @@ int64_t cnt_all(const DevBlock &b, const cosa_params &p) {
 }
 
 // once per process; contexts driven from several host threads (the serving
-// engine's k-omega lane) may reach it together
+// engine's context lane) may reach it together
 int set_smem_attrs() {
   static std::mutex mu;
   static bool done = false;

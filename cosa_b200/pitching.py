@@ -53,6 +53,46 @@ def _bind_kom(ctx, case, m, q):
     return vm
 
 
+class PitchingSolver:
+    """A pitching harmonic-balance solve resident on the device, with the
+    interface of solver.SteadySolver (run, state, close): the moving-grid
+    set-up of every snapshot (and, for k-omega, the viscous set-up, wall
+    distance and initial eddy viscosity), then run() advances it niter
+    explicit cycles through cosa_gpu_smooth."""
+
+    def __init__(self, case: "cases.Case", params=None, device: int = 0):
+        p = params if params is not None else case.params
+        self.case, self.p = case, p
+        self.kom = bool(p.kom or p.kom_bsl or p.kom_sst)
+        self.ctx = gpu.Context([case.tables], p, device=device)
+        self.m = self.ctx.pitching_setup(1, case)
+        self.q = self.ctx.alloc_p3().upload(case.q0)
+        self.vm = None
+        m = self.m
+        if self.kom:
+            self.vm = _bind_kom(self.ctx, case, m, self.q)
+        else:
+            self.ctx.bind_level(1, q=self.q, qold=self.ctx.alloc_p3(), dtvol=self.ctx.alloc_p1(nsnap=self.ctx.S),
+                                si=m["si"], sj=m["sj"], sk=m["sk"], vol=m["vol"], xdot=m["xdot"], ydot=m["ydot"],
+                                zdot=m["zdot"], fvi=m["fvi"], fvj=m["fvj"], fvk=m["fvk"])
+        self.it = 0
+
+    def run(self, niter: int, rms_every: int = 10, want_hist: bool = True):
+        h, st = self.ctx.smooth(1, niter, self.it + 1, rms_every, want_hist=want_hist)
+        self.it += niter
+        return h, st
+
+    def forces(self):
+        m = self.m
+        return self.ctx.force(1, self.q, m["x"], m["y"], m["z"], m["si"], m["sj"], m["sk"], vm=self.vm, lngth=LNGTH)
+
+    def state(self):
+        return self.q.download()
+
+    def close(self):
+        self.ctx.close()
+
+
 def run(nharms=1, precision=0, cycles=2000, chunk=500, blocks=(64, 64, 64, 64), nj=64, device=0, model="euler"):
     """One pitching solve on the device: returns a dict with the throughput
     (Mcell-snapshot-stage/s, CUDA events on the library's stream), the

@@ -11,11 +11,12 @@ p50/p99 latency (arrival to retirement).  The reference has no serving mode:
 each of its runs is one solve; this is the batched counterpart of running
 those one after another.
 
-Euler solves share the engine's merged level (one halo and one stage launch
-per RK stage for all of them).  k-omega solves run in the k-omega lane
-(KomLane): each is resident in its own context with its own CUDA stream and
-advanced by a worker thread, so their launches overlap on the device with
-one another and with the engine's; the library call releases the
+Steady Euler solves share the engine's merged level (one halo and one
+stage launch per RK stage for all of them).  k-omega solves and
+harmonic-balance solves of a pitching aerofoil run in the context lane
+(ContextLane): each is resident in its own context with its own CUDA stream
+and advanced by a worker thread, so their launches overlap on the device
+with one another and with the engine's; the library call releases the
 interpreter lock.  The device budget is split between the engine's pools
 and the lane.
 """
@@ -99,9 +100,29 @@ def kom_naca_request(scale: float, mach: float, alpha_deg: float, arrival: float
     return Request(scale, mach, arrival, case, case.params, alpha_deg, "naca_kom")
 
 
+def hb_request(scale: float, mach: float, alpha_deg: float, nharms: int = 1, arrival: float = 0.0,
+               model: str = "euler") -> Request:
+    """Harmonic balance of the NACA 0012 pitching 2.5 deg about the quarter
+    chord at reduced frequency 0.08 (cases.naca_pitching) with nharms
+    harmonics, mean incidence alpha_deg, on the 256 x 64 x 2 O-grid scaled by
+    `scale` in i and j; Euler (slip wall) or k-omega (Re 1e6, first spacing
+    2e-4 chords), CFL 1."""
+    ni, nj = max(16, int(round(256 * scale)) // 16 * 16), max(8, int(round(64 * scale)))
+    blocks = (ni // 4,) * 4
+    kw = {"h1": 2e-4} if model == "kom" else {}
+    case = cases.naca_pitching(nharms=nharms, blocks=blocks, nj=nj, mach=mach, alpha_deg=alpha_deg, rfar=20.0,
+                               model=model, **kw)
+    return Request(scale, mach, arrival, case, case.params, alpha_deg, "naca_hb" if model == "euler" else "naca_hb_kom")
+
+
 def is_kom(r: Request) -> bool:
     p = r.flow
     return bool(p.kom or p.kom_bsl or p.kom_sst)
+
+
+def in_lane(r: Request) -> bool:
+    """Solves the engine cannot merge: k-omega and harmonic balance."""
+    return is_kom(r) or r.flow.nharms > 0
 
 
 def engine_scheme() -> CosaParams:
@@ -111,12 +132,16 @@ def engine_scheme() -> CosaParams:
 
 
 def poisson_requests(n: int, rate: float, seed: int, scales=(0.5, 1.0, 2.0), mach_range=(0.3, 0.7),
-                     naca_fraction: float = 0.0, alpha_range=(-4.0, 8.0), kom_fraction: float = 0.0) -> List[Request]:
+                     naca_fraction: float = 0.0, alpha_range=(-4.0, 8.0), kom_fraction: float = 0.0,
+                     hb_fraction: float = 0.0, nharms_choices=(1, 2, 3)) -> List[Request]:
     """n arrivals at `rate` per second (seeded): with probability
     kom_fraction a k-omega RANS solve of the NACA 0012 (kom_naca_request),
     else an Euler solve of the bump channel or, with probability
     naca_fraction, of the NACA 0012; incidence drawn from alpha_range
-    (degrees), scale and Mach number uniformly."""
+    (degrees), scale and Mach number uniformly.  With probability
+    hb_fraction (drawn only when it is > 0) the request is instead a pitching
+    harmonic-balance solve (hb_request, Euler or k-omega as drawn) with
+    nharms from nharms_choices."""
     rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1.0 / rate, size=n))
     t -= t[0]
@@ -126,7 +151,10 @@ def poisson_requests(n: int, rate: float, seed: int, scales=(0.5, 1.0, 2.0), mac
         naca = rng.uniform() < naca_fraction
         alpha = float(rng.uniform(*alpha_range))
         kom = rng.uniform() < kom_fraction
-        if kom:
+        if hb_fraction > 0 and rng.uniform() < hb_fraction:
+            out.append(hb_request(scale, mach, alpha, int(rng.choice(nharms_choices)), float(t[k]),
+                                  "kom" if kom else "euler"))
+        elif kom:
             out.append(kom_naca_request(scale, mach, alpha, float(t[k])))
         elif naca:
             out.append(naca_request(scale, mach, alpha, float(t[k])))
@@ -135,24 +163,36 @@ def poisson_requests(n: int, rate: float, seed: int, scales=(0.5, 1.0, 2.0), mac
     return out
 
 
-def kom_solve_bytes(case: "cases.Case") -> int:
-    """Device bytes of one k-omega solve in its own context, an upper
-    estimate from the arrays SteadySolver binds and the context's own work
-    arrays: 8 states, 7 face-flux planes (one of the caller, six of the
-    fused stage), the IRS pivots (2 per variable) and about 30 scalar arrays
-    per P3 cell, plus the face inverse metrics (27 per face cell): 8 bytes x
-    (8 x 7 + 7 x 7 + 2 x 7 + 30 + 27) = 1408 bytes per P3 cell."""
+def lane_solve_bytes(case: "cases.Case") -> int:
+    """Device bytes of one solve in its own context, an upper estimate from
+    the arrays its driver binds and the context's own work arrays, per P3
+    cell and snapshot: k-omega 8 states, 7 face-flux planes (one of the
+    caller, six of the fused stage), the IRS pivots (2 per variable) and
+    about 30 scalar arrays (149 doubles), plus the face inverse metrics (27
+    per face cell); Euler 4 states and 4 scalars (24 doubles); a pitching
+    grid adds its per-snapshot metrics (12), nodes and node velocities (6)
+    and face velocities (9)."""
+    p = case.params
+    S = 2 * p.nharms + 1
     _, tot = case.tables.offsets()
-    return int(8 * (8 * 7 + 7 * 7 + 2 * 7 + 30) * tot["p3"] + 8 * 27 * tot["f0"])
+    kom = bool(p.kom or p.kom_bsl or p.kom_sst)
+    per, face = (8 * 7 + 7 * 7 + 2 * 7 + 30, 27) if kom else (4 * 5 + 4, 0)
+    if p.moving:
+        per += 12 + 6 + 9
+    return int(8 * S * (per * tot["p3"] + face * tot["f0"]))
 
 
-class KomLane:
-    """k-omega solves next to the serving engine.  A submitted solve waits
-    in a queue until its device bytes (kom_solve_bytes) fit the lane's
-    budget and a worker is free; it then runs on a worker thread in its own
-    context and stream (SteadySolver: metrics, viscous set-up, wall distance
-    and the initial eddy viscosity on the device), check_every RK cycles per
-    library call, with the same convergence rule as the engine: the total
+kom_solve_bytes = lane_solve_bytes
+
+
+class ContextLane:
+    """k-omega and harmonic-balance solves next to the serving engine.  A
+    submitted solve waits in a queue until its device bytes
+    (lane_solve_bytes) fit the lane's budget and a worker is free; it then
+    runs on a worker thread in its own context and stream (SteadySolver, or
+    pitching.PitchingSolver on a pitching grid: metrics, viscous set-up,
+    wall distance and the initial eddy viscosity on the device),
+    check_every RK cycles per library call, with the same convergence rule as the engine: the total
     residual norm of its first cycle is the reference, the solve converges
     when the norm of a checked cycle falls below tol times it, stops at
     max_iter cycles and fails on a status bit or a non-finite norm.  A
@@ -175,9 +215,9 @@ class KomLane:
         return time.perf_counter() - self.t0
 
     def submit(self, case: "cases.Case", flow: CosaParams, tol: float, max_iter: int) -> int:
-        nbytes = kom_solve_bytes(case)
+        nbytes = lane_solve_bytes(case)
         if nbytes > self.budget:
-            raise ValueError(f"a k-omega solve of {nbytes} bytes exceeds the lane's budget of {self.budget:.0f}")
+            raise ValueError(f"a solve of {nbytes} bytes exceeds the lane's budget of {self.budget:.0f}")
         with self.lock:
             rid = len(self.solves)
             self.solves.append({"case": case, "flow": flow, "tol": tol, "max_iter": max_iter, "bytes": nbytes,
@@ -206,9 +246,15 @@ class KomLane:
         solver = None
         state = "failed"
         try:
+            import torch
+            torch.cuda.set_device(self.device)  # a new thread starts on device 0; the per-routine entries use the current one
             p = CosaParams.from_buffer_copy(s["flow"])
             p.precision = self.precision
-            solver = SteadySolver(s["case"], params=p, device=self.device)
+            if p.moving:
+                from .pitching import PitchingSolver
+                solver = PitchingSolver(s["case"], params=p, device=self.device)
+            else:
+                solver = SteadySolver(s["case"], params=p, device=self.device)
             npde, rms0 = p.npde, None
             while True:
                 n = min(self.check_every, s["max_iter"] - s["iters"])
@@ -295,21 +341,21 @@ def run_sweep(requests: List[Request], budget_bytes: float = 150e9, tol: float =
               check_every: int = 10, iters_per_step: int = 50, device: int = 0, precision: int = 0,
               kom_share: Optional[float] = None, kom_max_iter: Optional[int] = None) -> SweepResult:
     """Feed `requests` at their arrival times (seconds after the start) and
-    run the engine and the k-omega lane (precision 0: FP64, 1: mixed) until
+    run the engine and the context lane (precision 0: FP64, 1: mixed) until
     every one has retired.  kom_share is the lane's part of the device budget
-    (default: the k-omega fraction of the requests, 0 without any);
-    kom_max_iter caps the k-omega solves' cycles (default max_iter)."""
-    nkom = sum(is_kom(r) for r in requests)
+    (default: the fraction of the requests the lane serves, 0 without any);
+    kom_max_iter caps the lane solves' cycles (default max_iter)."""
+    nkom = sum(in_lane(r) for r in requests)
     share = (nkom / max(len(requests), 1)) if kom_share is None else kom_share
     share = share if nkom else 0.0
     scheme = engine_scheme()
     scheme.precision = precision
     srv = Server(scheme, int(budget_bytes * (1.0 - share)), device=device, check_every=check_every) \
         if nkom < len(requests) else None
-    lane = KomLane(budget_bytes * share, device=device, check_every=check_every, precision=precision) \
+    lane = ContextLane(budget_bytes * share, device=device, check_every=check_every, precision=precision) \
         if nkom else None
     try:
-        ids: List[tuple] = []  # ("engine" | "kom", id) in submission order
+        ids: List[tuple] = []  # ("engine" | "lane", id) in submission order
         pending = sorted(range(len(requests)), key=lambda k: requests[k].arrival)
         order: Dict[tuple, int] = {}
         t0 = time.perf_counter()
@@ -323,8 +369,8 @@ def run_sweep(requests: List[Request], budget_bytes: float = 150e9, tol: float =
             now = time.perf_counter() - t0
             while nxt < len(pending) and requests[pending[nxt]].arrival <= now:
                 r = requests[pending[nxt]]
-                if is_kom(r):
-                    key = ("kom", lane.submit(r.case, r.flow, tol, kom_max_iter or max_iter))
+                if in_lane(r):
+                    key = ("lane", lane.submit(r.case, r.flow, tol, kom_max_iter or max_iter))
                 else:
                     key = ("engine", srv.submit(r.case.tables, r.case.x, r.case.y, r.case.z, r.case.q0, r.flow, tol,
                                                 max_iter))
@@ -349,7 +395,8 @@ def run_sweep(requests: List[Request], budget_bytes: float = 150e9, tol: float =
         out = SweepResult(len(ids), wall, len(ids) / wall * 3600.0, float(np.percentile(lat, 50)),
                           float(np.percentile(lat, 99)), [r["iters"] for r in res], [r["state"] for r in res], lat,
                           cs)
-        out.kinds = ["kom" if k[0] == "kom" else "euler" for k in ids]
+        out.kinds = [("hb_" if requests[order[k]].flow.nharms > 0 else "") +
+                     ("kom" if is_kom(requests[order[k]]) else "euler") for k in ids]
         out.errors = [r["error"] for r in res if r.get("error")]
         return out
     finally:

@@ -154,7 +154,7 @@ def test_short_mixed_sweep_reports_latency():
 
 
 def _lane_run(reqs, n, budget=4e9, check_every=10):
-    lane = serve.KomLane(budget, check_every=check_every)
+    lane = serve.ContextLane(budget, check_every=check_every)
     try:
         ids = [lane.submit(r.case, r.flow, 0.0, n) for r in reqs]
         while any(lane.result(i)["state"] in ("queued", "active") for i in ids):
@@ -206,3 +206,23 @@ def test_euler_and_kom_sweep_retires_every_request():
     assert s["euler"]["converged"] == s["euler"]["requests"]
     assert s["kom"]["converged"] + s["kom"]["stopped"] == s["kom"]["requests"]
     assert 0 < s["p50_latency_s"] <= s["p99_latency_s"]
+
+
+def test_harmonic_balance_requests_in_the_lane():
+    """Pitching harmonic-balance requests (Euler S = 3 and k-omega S = 3) in
+    the context lane beside a steady k-omega solve: each gives the bits of
+    a plain PitchingSolver run of the same cycles."""
+    from cosa_b200.pitching import PitchingSolver
+    reqs = [serve.hb_request(0.25, 0.5, 1.0, 1), serve.hb_request(0.25, 0.5, 0.0, 1, model="kom"),
+            serve.kom_channel_request(0.5, 0.4)]
+    n = 40
+    got = _lane_run(reqs, n)
+    assert all(g["state"] == "stopped" and g["iters"] == n for g in got), got
+    for k in (0, 1):
+        s = PitchingSolver(reqs[k].case)
+        _, st = s.run(n, rms_every=10)
+        assert st == 0
+        plain = s.state()
+        s.close()
+        npde = reqs[k].flow.npde
+        assert np.array_equal(got[k]["q"], plain), k
