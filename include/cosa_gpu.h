@@ -335,7 +335,9 @@ int cosa_gpu_prolong(cosa_ctx *ctx, int32_t nl);
    grid); q in primitive form where the reference has it so ---- */
 /* coordex (src/grid.f90:2-80): ghost nodes 0 and imax+1 (j, k alike)
    repeat the boundary nodes; x, y, z are node arrays of cosa_level_desc's
-   P2 extent (no lmet factor) */
+   P2 extent (no lmet factor).  On a moving grid (moving, hbmove) the node
+   arrays hold every snapshot (P2 x S2, as cosa_gpu_movegrid writes them)
+   and coordex, cutman_x and vmetrix run on every snapshot */
 int cosa_gpu_coordex(cosa_ctx *ctx, int32_t nl, double *x, double *y, double *z);
 /* cutman_x / cut_x (src/grid.f90:242-523): ghost nodes of cut faces from
    the neighbour block's nodes one plane inside */
@@ -349,12 +351,14 @@ int cosa_gpu_cutman_v(cosa_ctx *ctx, int32_t nl, double *vol);
    reference's nine arrays xideri, etaderi, zetaderi, xiderj, ... zetaderk,
    each (3, imax, jmax, kmax) per block at offset off_0*3 of a 3*n0 slab:
    array (d, m) (d = face family 1..3, m = 0 xi, 1 eta, 2 zeta) starts at
-   ((d-1)*3 + m)*3*n0, n0 = sizes[3] of cosa_gpu_level_sizes */
+   ((d-1)*3 + m)*3*n0, n0 = sizes[3] of cosa_gpu_level_sizes; on a moving
+   grid one such set per node snapshot, snapshot nh at nh*27*n0 */
 int cosa_gpu_vmetrix(cosa_ctx *ctx, int32_t nl, const double *x, const double *y,
                      const double *z, const double *vol, double *vm);
 /* the viscous start-up of the solver (src/cosa.f90:300-322): volex,
-   cutman_v, coordex, cutman_x, vmetrix; binds vm (27*n0 doubles, kept by
-   the caller) to level nl for cosa_gpu_smooth / smooth_level / mg */
+   cutman_v, coordex, cutman_x, vmetrix; binds vm (27*n0 doubles, times S2
+   on a moving grid, kept by the caller) to level nl for cosa_gpu_smooth /
+   smooth_level / mg */
 int cosa_gpu_viscous_setup(cosa_ctx *ctx, int32_t nl, double *x, double *y, double *z,
                            double *vol, double *vm);
 /* q_face (src/flux.f90:2391-2801), calmut = .false.: face averages of the
