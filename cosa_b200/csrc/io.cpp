@@ -181,6 +181,110 @@ void mathb(cosa_params &p) {
     }
 }
 
+// ---- Fortran formatted output of the history and force files -------------------
+// A small interpreter of the edit descriptors these files use: Iw, nX, Ew.d,
+// Dw.d and '/', with groups expanded beforehand.  Format control ends at the
+// first data descriptor left without an item (the record being built is still
+// written, as a WRITE statement does); blanks from X editing appear only when
+// a field follows them in the same record.
+struct FItem {
+  char k;     // 'I', 'X', 'E', 'D', '/'
+  int w, d;
+};
+
+// Ew.d / Dw.d editing of v: [-]0.<d digits>E+ee in w columns, right-justified
+// (exponents beyond 99 drop the letter, as Fortran's Ew.d does), asterisks
+// when the field is too narrow
+std::string fortran_e(double v, int w, int d, char letter) {
+  std::string out;
+  if (!std::isfinite(v)) {
+    out = std::isnan(v) ? "NaN" : (v > 0 ? "Infinity" : "-Infinity");
+  } else {
+    char tmp[64];
+    std::snprintf(tmp, sizeof(tmp), "%.*e", d - 1, v);  // d significant digits, d.ddd e+XX
+    std::string t(tmp);
+    const bool neg = t[0] == '-';
+    if (neg) t.erase(0, 1);
+    const size_t ep = t.find('e');
+    std::string mant = t.substr(0, ep), digits;
+    for (char ch : mant)
+      if (ch != '.') digits += ch;
+    int ex = std::atoi(t.c_str() + ep + 1);
+    if (v != 0.0) ex += 1;  // 0.ddd form
+    else ex = 0;
+    char eb[16];
+    if (std::abs(ex) <= 99) std::snprintf(eb, sizeof(eb), "%c%c%02d", letter, ex < 0 ? '-' : '+', std::abs(ex));
+    else std::snprintf(eb, sizeof(eb), "%c%03d", ex < 0 ? '-' : '+', std::abs(ex));
+    out = std::string(neg ? "-" : "") + "0." + digits + eb;
+  }
+  if ((int)out.size() > w) return std::string((size_t)w, '*');
+  return std::string((size_t)(w - (int)out.size()), ' ') + out;
+}
+
+std::string fortran_i(long long v, int w) {
+  std::string t = std::to_string(v);
+  if ((int)t.size() > w) return std::string((size_t)w, '*');
+  return std::string((size_t)(w - (int)t.size()), ' ') + t;
+}
+
+// one WRITE of the integer and real items through the expanded format
+std::string fortran_write(const std::vector<FItem> &fmt, const std::vector<long long> &ints,
+                          const std::vector<double> &reals) {
+  std::string out, rec;
+  int pend = 0;
+  size_t ii = 0, ri = 0;
+  for (const FItem &f : fmt) {
+    if (f.k == '/') { out += rec + "\n"; rec.clear(); pend = 0; continue; }
+    if (f.k == 'X') { pend += f.w; continue; }
+    if (f.k == 'I') {
+      if (ii >= ints.size()) break;
+      rec += std::string((size_t)pend, ' ') + fortran_i(ints[ii++], f.w);
+    } else {
+      if (ri >= reals.size()) break;
+      rec += std::string((size_t)pend, ' ') + fortran_e(reals[ri++], f.w, f.d, f.k);
+    }
+    pend = 0;
+  }
+  return out + rec + "\n";
+}
+
+void push_n(std::vector<FItem> &v, int n, FItem a, FItem b) {
+  for (int i = 0; i < n; ++i) { v.push_back(a); v.push_back(b); }
+}
+
+// (i8,1x,[(1x,d12.5)],4(/12(1x,d12.5)),[/(1x,d12.5)]) and the itime form
+// 2(i8,1x) of formats 212-220 (src/output.f90:4376-4380)
+std::vector<FItem> force_format(bool two_ints, bool time, bool alpha) {
+  std::vector<FItem> f;
+  f.push_back({'I', 8, 0}); f.push_back({'X', 1, 0});
+  if (two_ints) { f.push_back({'I', 8, 0}); f.push_back({'X', 1, 0}); }
+  if (time) push_n(f, 1, {'X', 1, 0}, {'D', 12, 5});
+  for (int g = 0; g < 4; ++g) {
+    f.push_back({'/', 0, 0});
+    push_n(f, 12, {'X', 1, 0}, {'D', 12, 5});
+  }
+  if (alpha) { f.push_back({'/', 0, 0}); push_n(f, 1, {'X', 1, 0}, {'D', 12, 5}); }
+  return f;
+}
+
+int copy_out(const std::string &t, char *buf, int64_t cap) {
+  if (!buf || cap < (int64_t)t.size() + 1) return COSA_ERR_ARG;
+  std::memcpy(buf, t.c_str(), t.size() + 1);
+  return COSA_OK;
+}
+
+// variable names of one surface block of the force files
+std::string force_names(int isurf, int nsurface) {
+  static const char *base[6] = {"Cl", "Cd", "Cz", "Cmx", "Cmy", "Cm"};
+  std::string s;
+  for (int c = 0; c < 6; ++c)
+    for (int pv = 0; pv < 2; ++pv) {
+      std::string nm = std::string(base[c]) + (nsurface > 1 ? std::to_string(isurf) : "") + (pv ? "_v" : "_p");
+      s += ",\"" + nm + "\"";
+    }
+  return s;
+}
+
 }  // namespace
 
 struct cosa_input {
@@ -939,6 +1043,91 @@ int cosa_io_write_restart(const char *path, int32_t nb, const int32_t *dims, int
   }
   ok = (std::fclose(f) == 0) && ok;
   return ok ? COSA_OK : COSA_ERR_ARG;
+}
+
+// history files of output() (src/output.f90:4941-4965): hist.dat holds
+// resrms(1:5), histur.dat resrms(6:npde) of k-omega runs, histg.dat the last
+// cycle's line; format (i7,2x,i7,5(1x,e13.5))
+int cosa_io_hist_record(int32_t itime, int32_t it, const double *res, int32_t n, char *buf, int64_t cap) {
+  if (!res || n < 0 || n > 5) return COSA_ERR_ARG;
+  std::vector<FItem> f = {{'I', 7, 0}, {'X', 2, 0}, {'I', 7, 0}};
+  push_n(f, 5, {'X', 1, 0}, {'E', 13, 5});
+  return copy_out(fortran_write(f, {itime, it}, std::vector<double>(res, res + n)), buf, cap);
+}
+
+// the header force() writes when it creates the force file of snapshot n
+// (src/output.f90:4100-4240): forces_tec.dat for steady and time-accurate
+// runs, forces_hb_<nnn>.dat per snapshot for harmonic balance.  The variable
+// lists keep the reference's spellings, among them the second "it" of the
+// two- and four-surface time-accurate fixed-grid lists, "Cm2_v" for "Cm1_v"
+// in the three-surface steady list and "Cm_p","Cm_v" for surface 1 of the
+// two-surface moving harmonic-balance list; the harmonic-balance title is
+// a 72-character line (trailing blanks kept)
+int cosa_io_force_header(const cosa_params *p, int32_t nsurface, int32_t n, char *buf, int64_t cap) {
+  if (!p || nsurface < 1 || nsurface > 4 || n < 0 || n > 999) return COSA_ERR_ARG;
+  const bool unsteady_t = p->dualt || p->rgkuns;
+  std::string names;
+  for (int is = 1; is <= nsurface; ++is) names += force_names(is, nsurface);
+  std::string t;
+  if (!p->harbal) {
+    t = " TITLE=\"Force coefficients\"\n";
+    std::string head;
+    if (unsteady_t) {
+      head = "\"itime\",\"it\",\"time\"";
+      if (!p->moving && (nsurface == 2 || nsurface == 4)) head += ",\"it\"";
+    } else {
+      head = "\"it\"";
+      if (nsurface == 3) {
+        const size_t at = names.find("\"Cm1_v\"");
+        if (at != std::string::npos) names.replace(at, 7, "\"Cm2_v\"");
+      }
+    }
+    t += " VARIABLES=" + head + names + (unsteady_t && p->moving ? ",\"alpha\"" : "") + "\n";
+  } else {
+    char line[80];
+    std::snprintf(line, sizeof(line), " TITLE=\"Force coefficients, Harmonic %2d\"", n);
+    std::string l(line);
+    l.resize(72, ' ');
+    t = l + "\n";
+    if (p->moving) {
+      if (nsurface == 2) {
+        const size_t at = names.find("\"Cm1_p\",\"Cm1_v\"");
+        if (at != std::string::npos) names.replace(at, 15, "\"Cm_p\",\"Cm_v\"");
+      }
+      t += " VARIABLES=\"it\",\"time\"" + names + ",\"alpha\"\n";
+    } else {
+      t += " VARIABLES=\"it\",\"time\",\"Cl\",\"Cd\",\"Cz\"\n";
+    }
+  }
+  return copy_out(t, buf, cap);
+}
+
+// one record of the force file of snapshot n (src/output.f90:4310-4360,
+// formats 212-220): coef holds per surface cl_p, cl_v, cd_p, cd_v, cz_p, cz_v,
+// cmx_p, cmx_v, cmy_p, cmy_v, cm_p, cm_v; time the physical time of a
+// time-accurate run, zeit the snapshot's time of harmonic balance, alpha_deg
+// the effective incidence of a moving grid
+int cosa_io_force_record(const cosa_params *p, int32_t nsurface, int32_t itime, int32_t it, double time,
+                         double zeit, const double *coef, double alpha_deg, char *buf, int64_t cap) {
+  if (!p || !coef || nsurface < 1 || nsurface > 4) return COSA_ERR_ARG;
+  std::vector<double> v;
+  std::vector<long long> ints;
+  std::vector<FItem> f;
+  if (p->dualt || p->rgkuns) {
+    ints = {itime, it};
+    v.push_back(time);
+    f = force_format(true, true, p->moving);
+  } else if (!p->harbal) {
+    ints = {it};
+    f = force_format(false, false, false);
+  } else {
+    ints = {it};
+    v.push_back(zeit);
+    f = force_format(false, true, p->moving);
+  }
+  v.insert(v.end(), coef, coef + 12 * nsurface);
+  if ((p->dualt || p->rgkuns || p->harbal) && p->moving) v.push_back(alpha_deg);
+  return copy_out(fortran_write(f, ints, v), buf, cap);
 }
 
 }  // extern "C"

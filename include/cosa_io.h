@@ -76,6 +76,20 @@ int cosa_io_write_restart(const char *path, int32_t nblocks, const int32_t *dims
                           int32_t with_q1, int32_t with_mut, const double *q, const double *q1,
                           const double *mut);
 
+/* History and force files, one WRITE each, as text in buf (records end in
+   '\n'; COSA_ERR_ARG when cap is too small).  cosa_io_hist_record: a line of
+   hist.dat (resrms 1..5), histur.dat (6..npde) or histg.dat, format
+   (i7,2x,i7,5(1x,e13.5)) of output() (src/output.f90:4941-4965, 5005).
+   cosa_io_force_header: the title and variable list force() writes when it
+   creates forces_tec.dat or forces_hb_<nnn>.dat of snapshot n
+   (src/output.f90:4100-4240).  cosa_io_force_record: one record of that
+   file (formats 212-220, src/output.f90:4310-4380); coef holds per surface
+   cl_p, cl_v, cd_p, cd_v, cz_p, cz_v, cmx_p, cmx_v, cmy_p, cmy_v, cm_p, cm_v. */
+int cosa_io_hist_record(int32_t itime, int32_t it, const double *res, int32_t n, char *buf, int64_t cap);
+int cosa_io_force_header(const cosa_params *p, int32_t nsurface, int32_t n, char *buf, int64_t cap);
+int cosa_io_force_record(const cosa_params *p, int32_t nsurface, int32_t itime, int32_t it, double time,
+                         double zeit, const double *coef, double alpha_deg, char *buf, int64_t cap);
+
 #ifdef __cplusplus
 }
 #endif

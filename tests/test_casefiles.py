@@ -432,3 +432,65 @@ def test_default_params_match_python_defaults():
     from cosa_b200.params import default_params
     a, b = cf.default_params(), default_params()
     _params_close(a, b)
+
+
+# ---- history and force files (src/output.f90:4100-4386, 4941-4965) --------------
+def test_hist_record_fortran_e_editing():
+    from cosa_b200 import casefiles
+    line = casefiles.hist_record(0, 1, [1.234e-3, 2.0, -3.5e-7, 0.0, 1e-120])
+    assert line == ("      0        1" + "   0.12340E-02" + "   0.20000E+01" + "  -0.35000E-06" + "   0.00000E+00" +
+                    "   0.10000-119\n")
+    # rounding to 5 significant digits carries into the exponent
+    assert casefiles.hist_record(3, 40, [9.999996]) == "      3       40   0.10000E+02\n"
+    # histur.dat: two values end the record after the second field
+    assert casefiles.hist_record(0, 10, [1.0, 0.5]) == "      0       10   0.10000E+01   0.50000E+00\n"
+
+
+def test_force_files_header_and_record():
+    from cosa_b200 import casefiles
+    from cosa_b200.params import CosaParams
+    p = CosaParams()
+    names = ',"Cl_p","Cl_v","Cd_p","Cd_v","Cz_p","Cz_v","Cmx_p","Cmx_v","Cmy_p","Cmy_v","Cm_p","Cm_v"'
+    assert casefiles.force_header(p) == ' TITLE="Force coefficients"\n VARIABLES="it"' + names + "\n"
+    # three surfaces, steady: the reference's list names surface 1's viscous Cm "Cm2_v"
+    h3 = casefiles.force_header(p, 3)
+    assert h3.count('"Cm2_v"') == 2 and '"Cm1_v"' not in h3
+    row = np.arange(12, dtype=float) + 1.0  # gpu.Context.force order
+    rec = casefiles.force_record(p, 7, row)
+    vals = [row[c] for c in casefiles.FORCE_FILE_COLUMNS]
+    body = "".join(" " + ("0.%05dD+%02d" % (round(v * 10 ** (5 - len(str(int(v))))), len(str(int(v))))).rjust(12)
+                   for v in vals)
+    # i8, then the 12 values on the next record; the exhausted list ends the
+    # third record empty (the slash before the second group)
+    assert rec == "       7\n" + body + "\n\n"
+    # harmonic balance on a pitching grid: 72-column title, time and alpha
+    p.harbal, p.moving, p.nharms = 1, 1, 1
+    h = casefiles.force_header(p, 1, 2)
+    title = h.split("\n")[0]
+    assert len(title) == 72 and title.rstrip() == ' TITLE="Force coefficients, Harmonic  2"'
+    assert h.split("\n")[1].endswith(',"Cm_v","alpha"')
+    h2 = casefiles.force_header(p, 2, 0)
+    assert '"Cmy1_v","Cm_p","Cm_v","Cl2_p"' in h2
+    rec = casefiles.force_record(p, 5, row, zeit=1.5, alpha_deg=-2.5)
+    lines = rec.split("\n")
+    assert lines[0] == "       5   0.15000D+01"  # i8, 1x, 1x, d12.5
+    assert lines[1] == body and lines[2] == " -0.25000D+01" and lines[3] == ""
+
+
+def test_output_files_schedule(tmp_path):
+    from cosa_b200 import casefiles
+    from cosa_b200.params import CosaParams
+    p = CosaParams()
+    p.npde, p.kom = 7, 1
+    out = casefiles.OutputFiles(str(tmp_path), p, iprint=2)
+    for it in range(1, 6):
+        row = np.full(8, 1.0 / it)
+        out.hist(it, row, last=(it == 5))
+        out.forces(it, np.ones((1, 12)) * it, last=(it == 5))
+    hist = (tmp_path / "hist.dat").read_text().splitlines()
+    assert [int(l.split()[1]) for l in hist] == [1, 2, 4, 5]
+    assert len((tmp_path / "histur.dat").read_text().splitlines()[0].split()) == 4
+    assert (tmp_path / "histg.dat").read_text().splitlines() == [hist[-1]]
+    f = (tmp_path / "forces_tec.dat").read_text().split("\n")
+    assert f[0] == ' TITLE="Force coefficients"' and f[1].startswith(' VARIABLES="it"')
+    assert [int(l) for l in f[2:] if l.strip() and "D" not in l] == [1, 2, 4, 5]
