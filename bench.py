@@ -432,7 +432,7 @@ def main():
                                                 kom_max_iter=20_000).summary()
             except Exception as e:  # reported, not fatal
                 serving[name] = {"error": str(e)}
-        serving["workload"] = ("k-omega NACA 0012 256x64x2 (Re 1e6, IRS, CFL 3) / Euler (bump channel 128x64x2 at "
+        serving["workload"] = ("k-omega SST NACA 0012 256x64x2 (Re 1e6, IRS, CFL 3) / Euler (bump channel 128x64x2 at "
                                "CFL 2 or NACA 0012 256x64x2 at CFL 1) 50/50, x{0.5,1,2} in-plane, M~U[0.3,0.7], "
                                "alpha~U[-4,8] deg, Poisson 2 req/s, drop 1e-8 or 60k (Euler) / 20k (k-omega) cycles, "
                                "150 GB; Euler solves batched in the engine's merged level, k-omega solves each in "

@@ -86,16 +86,22 @@ def kom_channel_request(scale: float, mach: float, arrival: float = 0.0, reyno: 
 
 
 def kom_naca_request(scale: float, mach: float, alpha_deg: float, arrival: float = 0.0,
-                     reyno: float = 1.0e6) -> Request:
+                     reyno: float = 1.0e6, model: str = "sst") -> Request:
     """k-omega NACA 0012 O-grid 256 x 64 x 2 cells in four blocks scaled by
     `scale` in i and j, no-slip wall (1500), far field (30) at 20 chords,
     first spacing 2e-4 chords at every scale (at 4e-4 on the 128 x 32 grid
     the trailing-edge cells' k runs away by cycle 300, in the oracle as on
     the device), free stream at `mach` and incidence `alpha_deg`, Reynolds
-    number reyno, constant-coefficient IRS (0.6) at CFL 3."""
+    number reyno, constant-coefficient IRS (0.6) at CFL 3.  model "sst"
+    (Menter's SST, the default) or "wilcox": on the 512 x 128 grid at 5-7
+    deg incidence and M 0.33-0.44 Wilcox's k and omega go non-finite after
+    2400-3700 cycles (at CFL 3 and 2; the production limiters save one of
+    two such requests), while SST runs them 20k cycles."""
     ni, nj = max(16, int(round(256 * scale)) // 16 * 16), max(8, int(round(64 * scale)))
     blocks = (3 * ni // 16, 5 * ni // 16, 5 * ni // 16, 3 * ni // 16)
     p = cases.naca_params("kom", mach=mach, alpha_deg=alpha_deg, reyno=reyno, cfl=3.0, eps_irs=0.6)
+    if model == "sst":
+        p.kom, p.kom_sst = 0, 1
     case = cases.naca0012_ogrid(blocks=blocks, nj=nj, nk=2, rfar=20.0, h1=2e-4, params=p)
     return Request(scale, mach, arrival, case, case.params, alpha_deg, "naca_kom")
 
