@@ -11,13 +11,13 @@ p50/p99 latency (arrival to retirement).  The reference has no serving mode:
 each of its runs is one solve; this is the batched counterpart of running
 those one after another.
 
-Steady Euler solves share the engine's merged level (one halo and one
-stage launch per RK stage for all of them).  k-omega solves and
-harmonic-balance solves of a pitching aerofoil run in the context lane
-(ContextLane): each is resident in its own context with its own CUDA stream
-and advanced by a worker thread, so their launches overlap on the device
-with one another and with the engine's; the library call releases the
-interpreter lock.  The device budget is split between the engine's pools
+Steady single-grid Euler solves share the engine's merged level (one halo
+and one stage launch per RK stage for all of them).  k-omega solves,
+multigrid solves and harmonic-balance solves of a pitching aerofoil run in
+the context lane (ContextLane): each is resident in its own context with
+its own CUDA stream and advanced by a worker thread, so their launches
+overlap on the device with one another and with the engine's; the library
+call releases the interpreter lock.  The device budget is split between the engine's pools
 and the lane.
 """
 from __future__ import annotations
@@ -121,14 +121,31 @@ def hb_request(scale: float, mach: float, alpha_deg: float, nharms: int = 1, arr
     return Request(scale, mach, arrival, case, case.params, alpha_deg, "naca_hb" if model == "euler" else "naca_hb_kom")
 
 
+def mg_request(scale: float, mach: float, arrival: float = 0.0, nlevel: int = 2) -> Request:
+    """Euler bump channel (channel_request's grid, in-plane sizes rounded to
+    multiples of 2^(nlevel-1)) solved with nlevel-level multigrid: one pre-,
+    post- and coarsest-level iteration, bilinear prolongation, first order
+    from level 2 on (the 2-cell-thick grid is one cell thick there)."""
+    m = 2 ** (nlevel - 1)
+    ni, nj = max(8 * m, int(round(128 * scale)) // m * m), max(4 * m, int(round(64 * scale)) // m * m)
+    case = cases.bump_channel(ni, nj, 2, mach=mach)
+    p = case.params
+    p.nlevel = nlevel
+    p.nstart = p.npre = p.npost = p.ncrs = 1
+    p.bln_prol = 1
+    p.nl_crs = 2
+    return Request(scale, mach, arrival, case, p, 0.0, "channel_mg")
+
+
 def is_kom(r: Request) -> bool:
     p = r.flow
     return bool(p.kom or p.kom_bsl or p.kom_sst)
 
 
 def in_lane(r: Request) -> bool:
-    """Solves the engine cannot merge: k-omega and harmonic balance."""
-    return is_kom(r) or r.flow.nharms > 0
+    """Solves the engine cannot merge: k-omega, harmonic balance and
+    multigrid."""
+    return is_kom(r) or r.flow.nharms > 0 or r.flow.nlevel > 1
 
 
 def engine_scheme() -> CosaParams:
@@ -177,7 +194,10 @@ def lane_solve_bytes(case: "cases.Case") -> int:
     about 30 scalar arrays (149 doubles), plus the face inverse metrics (27
     per face cell); Euler 4 states and 4 scalars (24 doubles); a pitching
     grid adds its per-snapshot metrics (12), nodes and node velocities (6)
-    and face velocities (9)."""
+    and face velocities (9); multigrid adds the residual and forcing states
+    (10) and counts the coarser levels as half the finest (each level has at
+    most a quarter of the cells of the one above it on these grids, halos
+    included)."""
     p = case.params
     S = 2 * p.nharms + 1
     _, tot = case.tables.offsets()
@@ -185,14 +205,19 @@ def lane_solve_bytes(case: "cases.Case") -> int:
     per, face = (8 * 7 + 7 * 7 + 2 * 7 + 30, 27) if kom else (4 * 5 + 4, 0)
     if p.moving:
         per += 12 + 6 + 9
-    return int(8 * S * (per * tot["p3"] + face * tot["f0"]))
+    levels = 1.0
+    if p.nlevel > 1:
+        per += 10
+        levels = 1.5
+    return int(8 * S * levels * (per * tot["p3"] + face * tot["f0"]))
 
 
 kom_solve_bytes = lane_solve_bytes
 
 
 class ContextLane:
-    """k-omega and harmonic-balance solves next to the serving engine.  A
+    """k-omega, multigrid and harmonic-balance solves next to the serving
+    engine.  A
     submitted solve waits in a queue until its device bytes
     (lane_solve_bytes) fit the lane's budget and a worker is free; it then
     runs on a worker thread in its own context and stream (SteadySolver, or

@@ -226,3 +226,22 @@ def test_harmonic_balance_requests_in_the_lane():
         s.close()
         npde = reqs[k].flow.npde
         assert np.array_equal(got[k]["q"], plain), k
+
+
+def test_multigrid_requests_in_the_lane():
+    """Two-level multigrid Euler requests in the context lane beside a
+    single-grid k-omega solve: each gives the bits of a plain SteadySolver
+    multigrid run of the same cycles."""
+    from cosa_b200.solver import SteadySolver
+    reqs = [serve.mg_request(0.5, 0.45), serve.kom_channel_request(0.5, 0.4), serve.mg_request(0.5, 0.6)]
+    assert all(serve.in_lane(r) for r in reqs)
+    n = 30
+    got = _lane_run(reqs, n)
+    assert all(g["state"] == "stopped" and g["iters"] == n for g in got), got
+    for k in (0, 2):
+        s = SteadySolver(reqs[k].case)
+        _, st = s.run(n, rms_every=10)
+        assert st == 0
+        plain = s.state()
+        s.close()
+        assert np.array_equal(got[k]["q"], plain), k
