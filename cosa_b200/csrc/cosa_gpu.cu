@@ -603,9 +603,9 @@ int check_fused_supported(const cosa_params &p) {
   if (p.npde != 5 || p.kom || p.kom_bsl || p.kom_sst ||
       p.irsop < 0 || p.irsop > 6 || p.irsop == 4 || p.lmet != 4 || p.ilimf < 0 || p.ilimf > 4)
     return COSA_ERR_UNSUPPORTED;
-  // moving grids: inviscid harmonic balance of a pitching body, explicit
-  // (the face-split stage schedule carries the face speeds)
-  if (p.moving && (!p.harbal || !p.hbmove || p.viscous || p.rkimp || p.nlevel > 1)) return COSA_ERR_UNSUPPORTED;
+  // moving grids: harmonic balance of a pitching body (inviscid or laminar),
+  // explicit (the face-split stage schedule carries the face speeds)
+  if (p.moving && (!p.harbal || !p.hbmove || p.rkimp || p.nlevel > 1)) return COSA_ERR_UNSUPPORTED;
   return COSA_OK;
 }
 
@@ -811,8 +811,10 @@ int launch_visc(cosa_ctx *c, LevelState &L, const double *qin, bool dt, double *
   if ((r = launch_edges(c, L, L.d_qprim, nullptr))) return r;
   const cosa_level_ptrs &P = L.ptrs;
   if (dt) {
+    const bool mv = c->p.moving;
     k_dt_ns<<<dim3(grid_x(mc, L.nb), L.nb), 256, 0, c->s>>>(L.d_blocks, c->d_p, L.d_qprim, P.si, P.sj, P.sk, P.vol,
-                                                            P.dtvol, bx, by, bz);
+                                                            P.dtvol, bx, by, bz, mv ? P.xdot : nullptr,
+                                                            mv ? P.ydot : nullptr, mv ? P.zdot : nullptr);
     if ((r = after_launch(c))) return r;
   }
   k_vface<<<dim3(grid_x(mf, L.nb), L.nb, 3), 256, 0, c->s>>>(L.d_blocks, c->d_p, L.d_qprim, P.si, P.sj, P.sk, L.d_vm,
@@ -863,13 +865,16 @@ int launch_split_tail(cosa_ctx *c, int nl, LevelState &L, StageArgs &A, bool wan
   k_faces_line<M, CV, IF><<<(nt[IF ? 0 : 1] + 3) / 4, 128, 0, st>>>(                                           \
       L.d_blocks, tk[IF ? 0 : 1], nt[IF ? 0 : 1], lp, qsrc, A.si, A.sj, A.sk, L.d_strong, L.d_smap,              \
       A.first_order, L.n0, L.d_cflux, c->d_status)
-#define COSA_FACES_MOVING(M, IF)                                                                                \
-  k_faces_line<M, true, IF, true><<<(nt[IF ? 0 : 1] + 3) / 4, 128, 0, st>>>(                                   \
+#define COSA_FACES_MOVING(M, CV, IF)                                                                            \
+  k_faces_line<M, CV, IF, true><<<(nt[IF ? 0 : 1] + 3) / 4, 128, 0, st>>>(                                     \
       L.d_blocks, tk[IF ? 0 : 1], nt[IF ? 0 : 1], lp, qsrc, A.si, A.sj, A.sk, L.d_strong, L.d_smap,              \
       A.first_order, L.n0, L.d_cflux, c->d_status, fvel)
     const FaceVel fvel = face_vel_of(c, L);
-    if (p.moving && conv && mixed) { COSA_FACES_MOVING(true, true); COSA_FACES_MOVING(true, false); }
-    else if (p.moving && conv) { COSA_FACES_MOVING(false, true); COSA_FACES_MOVING(false, false); }
+    // moving grids: the face speeds; viscous runs read the primitive copy (CV false)
+    if (p.moving && conv && mixed) { COSA_FACES_MOVING(true, true, true); COSA_FACES_MOVING(true, true, false); }
+    else if (p.moving && conv) { COSA_FACES_MOVING(false, true, true); COSA_FACES_MOVING(false, true, false); }
+    else if (p.moving && mixed) { COSA_FACES_MOVING(true, false, true); COSA_FACES_MOVING(true, false, false); }
+    else if (p.moving) { COSA_FACES_MOVING(false, false, true); COSA_FACES_MOVING(false, false, false); }
     else if (mixed && conv) { COSA_FACES_LINE(true, true, true); COSA_FACES_LINE(true, true, false); }
     else if (mixed) { COSA_FACES_LINE(true, false, true); COSA_FACES_LINE(true, false, false); }
     else if (conv) { COSA_FACES_LINE(false, true, true); COSA_FACES_LINE(false, true, false); }

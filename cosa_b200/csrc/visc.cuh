@@ -380,7 +380,7 @@ __device__ __forceinline__ void vface_one(const DevBlock &b, const ViscPar &V, c
                                           int64_t n0, int i, int j, int k, int nh, double *__restrict__ F) {
   double qf[5], g[3][5], vmf[9], F5[5];
   face_interior<D>(Q, i, j, k, qf, g);
-  load_vm(vm, b, n0, D, i, j, k, vmf);
+  load_vm(vm + (int64_t)nh * 27 * n0, b, n0, D, i, j, k, vmf);  // inverse metrics of node snapshot nh
   const int64_t e = p2_idx(b, S2, 1, i, j, k, nh);
   const double2 a = __ldg(reinterpret_cast<const double2 *>(s + e));
   const double2 c = __ldg(reinterpret_cast<const double2 *>(s + e + 2));
@@ -435,7 +435,7 @@ __global__ void k_vwall(const DevBlock *__restrict__ blocks, const WallFace *__r
     const int mx = w.d == 1 ? b.im : (w.d == 2 ? b.jm : b.km);
     double qf[5], g[3][5], vmf[9], F[5];
     face_wall(Q, w, mx, qf, g);
-    load_vm(vm, b, n0, w.d, w.fi, w.fj, w.fk, vmf);
+    load_vm(vm + (int64_t)nh * 27 * n0, b, n0, w.d, w.fi, w.fj, w.fk, vmf);
     const double *s = w.d == 1 ? si : (w.d == 2 ? sj : sk);
     const int64_t e = p2_idx(b, S2, 1, w.fi, w.fj, w.fk, nh);
     vflux_face(V, qf, g, vmf, s[e], s[e + 1], s[e + 2], s[e + 3], 0.0, F);
@@ -542,7 +542,9 @@ __device__ __forceinline__ void deltat_ns_cell(const cosa_params &P, const doubl
 __global__ void k_dt_ns(const DevBlock *__restrict__ blocks, const cosa_params *__restrict__ Pp,
                         const double *__restrict__ qp, const double *__restrict__ si, const double *__restrict__ sj,
                         const double *__restrict__ sk, const double *__restrict__ vol, double *__restrict__ dtv,
-                        double *bx, double *by, double *bz) {
+                        double *bx, double *by, double *bz, const double *__restrict__ cvx = nullptr,
+                        const double *__restrict__ cvy = nullptr, const double *__restrict__ cvz = nullptr) {
+  // cv*: the cell grid velocities of a moving grid (node layout, per snapshot)
   const DevBlock b = blocks[blockIdx.y];
   const cosa_params &P = *Pp;
   const int S = 2 * P.nharms + 1, S2 = 2 * P.nharms * P.hbmove + 1;
@@ -555,8 +557,14 @@ __global__ void k_dt_ns(const DevBlock *__restrict__ blocks, const cosa_params *
     const int k = (int)(r % nk) + 1;
     const int n = (int)(r / nk), nh = n * P.hbmove;
     const QView Q = qview(b, qp, S, n);
-    double lam[3], lamv[3];
-    eig_ns_cell(b, P, Q, si, sj, sk, S2, nh, vol[p1_idx(b, 1, i, j, k, 0)], i, j, k, lam, lamv);
+    double lam[3], lamv[3], gv[3];
+    if (cvx) {
+      const int64_t I2 = b.im + 2, J2 = b.jm + 2, K2 = b.km + 2;
+      const int64_t gi = b.op2 * S2 + (int64_t)nh * I2 * J2 * K2 + i + I2 * (j + J2 * (int64_t)k);
+      gv[0] = cvx[gi]; gv[1] = cvy[gi]; gv[2] = cvz[gi];
+    }
+    eig_ns_cell(b, P, Q, si, sj, sk, S2, nh, vol[p1_idx(b, 1, i, j, k, 0)], i, j, k, lam, lamv, nullptr, 1, 0, -1.0,
+                0.0, cvx ? gv : nullptr);
     double dt, a, c, e;
     deltat_ns_cell(P, lam, lamv, dt, a, c, e);
     const int64_t o = p1_idx(b, S, i, j, k, n);
@@ -720,7 +728,7 @@ __global__ void k_vflux_ref(DevBlock b, int d, const cosa_params *__restrict__ P
       const int64_t o = p3_var(b, 5, S, m + 1, n) + c;
       f[m] = qf[o]; g[0][m] = g0[o]; g[1][m] = g1[o]; g[2][m] = g2[o];
     }
-    load_vm(vm, b, n0, d, i, j, k, vmf);
+    load_vm(vm + (int64_t)nh * 27 * n0, b, n0, d, i, j, k, vmf);
     const int64_t e = p2_idx(b, S2, 1, i, j, k, nh);
     vflux_face(V, f, g, vmf, s[e], s[e + 1], s[e + 2], s[e + 3], 0.0, F);
 #pragma unroll

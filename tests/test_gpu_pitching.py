@@ -169,3 +169,37 @@ def test_pitching_mixed_precision_close_to_fp64():
     err = _rel(out[1], out[0], case.tables, S)
     assert 0 < err < 1e-6, err
     assert np.abs(cls[1] - cls[0]).max() < 1e-6
+
+
+@pytest.mark.parametrize("nharms", [1, 2])
+def test_laminar_pitching_hb_cycles_match_oracle(nharms):
+    """Laminar harmonic balance on the pitching grid: the face inverse
+    metrics of every node snapshot, the no-slip wall moving with the body,
+    the grid velocity in the viscous time step, and the skin friction from
+    the velocity relative to the grid."""
+    case = cases.naca_pitching(nharms=nharms, blocks=(16, 16, 16, 16), nj=16, rfar=12.0, h1=5e-3, model="laminar")
+    p = case.params
+    S = 2 * p.nharms + 1
+    O = oracle.OracleLevel(case.tables, p)
+    ones = np.ones(O.n1)
+    mo = oracle.moving_setup(O, case.x, case.y, case.z, ones, ones, ones)
+    vmo = oracle.viscous_setup(O, mo["x"], mo["y"], mo["z"], mo["vol"])
+    q = _state(case, 31 + nharms)
+    qo = q.copy()
+    ncyc = 5
+    hist_o, st_o = oracle.smooth_ns(O, qo, mo["si"], mo["sj"], mo["sk"], mo["vol"], vmo, ncyc, rms_every=1)
+    assert st_o == 0
+    ctx, m = _device(case)
+    vm = ctx.alloc_vm(1)
+    ctx.viscous_setup(1, m["x"], m["y"], m["z"], m["vol"], vm)
+    assert np.abs(vm.download() - vmo).max() <= 1e-12 * np.abs(vmo).max()
+    dq = _bind(ctx, m, q)
+    hist_g, st = ctx.smooth(1, ncyc, 1, 1)
+    assert st == 0
+    assert _rel(dq.download(), qo, case.tables, S) <= TOL
+    np.testing.assert_allclose(hist_g, hist_o, rtol=1e-9)
+    co = oracle.force(O, qo, mo["x"], mo["y"], mo["z"], mo["si"], mo["sj"], mo["sk"], vmo, lngth=(1.0, 0.1, 1.0))
+    cg = ctx.force(1, dq, m["x"], m["y"], m["z"], m["si"], m["sj"], m["sk"], vm=vm, lngth=(1.0, 0.1, 1.0))
+    assert np.abs(cg - co).max() <= 1e-10 * np.abs(co).max()
+    assert np.abs(co[:, 6:]).max() > 0
+    ctx.close()
